@@ -1,0 +1,281 @@
+"""Test infrastructure: ctypes binding of the CPU restatement of the reference
+sheet step (oracle/sheet_oracle.cpp). Only the parity tests, the smoke check and
+the CPU-baseline leg of bench.py load it; the product never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_silt.so")
+
+_f = ctypes.c_float
+_i = ctypes.c_int
+_p = ctypes.c_void_p
+
+
+class CoreCfg(ctypes.Structure):
+    _fields_ = [("res", _i), ("cell", _f), ("fine_res", _i), ("fine_cell", _f),
+                ("layout", _i), ("tire_r", _f), ("soften", _i), ("inner_par", _i),
+                ("center_x", _f), ("center_z", _f)]
+
+
+class Tire(ctypes.Structure):
+    _fields_ = [("x", _f), ("z", _f), ("forward_x", _f), ("forward_z", _f),
+                ("radius", _f), ("width", _f), ("speed", _f), ("slip", _f)]
+
+
+class Spray(ctypes.Structure):
+    _fields_ = [("x", _f), ("y", _f), ("z", _f), ("vx", _f), ("vy", _f), ("vz", _f),
+                ("volume", _f), ("kind", _i)]
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.oracle_scratch_new.restype = _p
+        L.oracle_scratch_free.argtypes = [_p]
+        L.oracle_step_sheet.argtypes = [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _f, _i, _f, _i, _i, _p]
+        L.oracle_transport_open.argtypes = [_p, _p, _p, _i, _f, _f, _i, _i, _i, _i, _i, _p, _f, _i, _p, _p]
+        L.oracle_sheet_work_boxes.argtypes = [_p, _i, _f, _i, _i, _p, _i]
+        L.oracle_awake_work_boxes.argtypes = [_p, _p, _p, _p, _i, _f, _f, _p, _i]
+        L.oracle_dynamic_viscosity.argtypes = [_i, _f]
+        L.oracle_dynamic_viscosity.restype = _f
+        L.oracle_sheet_mobility_for.argtypes = [_f]
+        L.oracle_sheet_mobility_for.restype = _f
+        L.oracle_sheet_damp.argtypes = [_f]
+        L.oracle_sheet_damp.restype = _f
+        L.oracle_soften_border.argtypes = [_p, _p, _i]
+        L.oracle_rut_heal.argtypes = [_i, _f, _p]
+        L.oracle_core_new.argtypes = [ctypes.POINTER(CoreCfg)]
+        L.oracle_core_new.restype = _p
+        L.oracle_core_free.argtypes = [_p]
+        L.oracle_core_map_water_bed.argtypes = [_p, _p, _p]
+        L.oracle_core_map_water_bed.restype = _f
+        L.oracle_core_map_grain.argtypes = [_p, _p]
+        L.oracle_core_map_water_velocity.argtypes = [_p, _p, _p]
+        L.oracle_core_pour.argtypes = [_p, _f, _f, _f, _f, _f, _i, _i, _f]
+        L.oracle_core_pour.restype = _f
+        L.oracle_core_lay_slurry_mask.argtypes = [_p, _p, _i, _f]
+        L.oracle_core_lay_slurry_mask.restype = _f
+        L.oracle_core_read_substrate.argtypes = [_p, _p, _p, _p]
+        L.oracle_core_push_tire.argtypes = [_p, ctypes.POINTER(Tire)]
+        L.oracle_core_step.argtypes = [_p, _f, _p, _i]
+        L.oracle_core_step.restype = _i
+        L.oracle_core_ledger.argtypes = [_p, _p, _p]
+        L.oracle_core_get.argtypes = [_p, _i, _p]
+        L.oracle_core_set.argtypes = [_p, _i, _p]
+        L.oracle_core_get_grain.argtypes = [_p, _p]
+        L.oracle_core_publish.argtypes = [_p, _p, _p]
+        L.oracle_core_set_fine_pace.argtypes = [_p, _i]
+        L.oracle_core_set_fine_sub_cap.argtypes = [_p, _f]
+        L.oracle_core_set_near_field.argtypes = [_p, _i]
+        L.oracle_core_near_tiles.argtypes = [_p]
+        L.oracle_core_near_tiles.restype = _i
+        L.oracle_core_spray_m3.argtypes = [_p]
+        L.oracle_core_spray_m3.restype = _f
+        L.oracle_core_non_finite.argtypes = [_p]
+        L.oracle_core_non_finite.restype = ctypes.c_uint32
+        L.oracle_core_sample.argtypes = [_p, _f, _f, _p]
+        L.oracle_core_fine_water_debug.argtypes = [_p, _p, _i, _i, _p, _p]
+        L.oracle_core_inflow.argtypes = [_p, _i, _f, _f, _f]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_p) if a is not None else None
+
+
+def f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Scratch:
+    """Stands in for the reference's thread-local sheet scratch."""
+
+    def __init__(self):
+        self.h = lib().oracle_scratch_new()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_scratch_free(self.h)
+            self.h = None
+
+
+def step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps=1.0e-6, banks=False,
+               sub_cap=8.0, pace=0, inner_par=True, scratch=None):
+    """In-place `step_sheet_eps` (src/fluid_core.rs:856) on float32 arrays."""
+    sc = scratch or Scratch()
+    lib().oracle_step_sheet(_ptr(h), _ptr(u), _ptr(v), _ptr(bed), _ptr(nu), _ptr(gate), res, cell, dt,
+                            vorticity, eps, int(banks), sub_cap, pace, int(inner_par), sc.h)
+
+
+def transport_open(h, vel, gate, res, cell, dt, box, along_x, bed=None, frac_cap=0.45, serial=False):
+    n = res * res
+    removed = np.zeros(n, np.float32)
+    added = np.zeros(n, np.float32)
+    i0, i1, j0, j1 = box
+    lib().oracle_transport_open(_ptr(h), _ptr(vel), _ptr(gate), res, cell, dt, i0, i1, j0, j1, int(along_x),
+                                _ptr(bed), frac_cap, int(serial), _ptr(removed), _ptr(added))
+    return removed, added
+
+
+def sheet_work_boxes(h, res, eps, allow_split=True, flood=False):
+    out = np.zeros(4 * 4096, np.int32)
+    n = lib().oracle_sheet_work_boxes(_ptr(h), res, eps, int(allow_split), int(flood), _ptr(out), 4096)
+    return [tuple(int(x) for x in out[4 * k:4 * k + 4]) for k in range(n)]
+
+
+def awake_work_boxes(h, u, v, bed, res, cell, eps):
+    out = np.zeros(4 * 4096, np.int32)
+    n = lib().oracle_awake_work_boxes(_ptr(h), _ptr(u), _ptr(v), _ptr(bed), res, cell, eps, _ptr(out), 4096)
+    return [tuple(int(x) for x in out[4 * k:4 * k + 4]) for k in range(n)]
+
+
+def dynamic_viscosity(grain, moisture):
+    return lib().oracle_dynamic_viscosity(grain, moisture)
+
+
+def sheet_damp(nu):
+    return lib().oracle_sheet_damp(nu)
+
+
+def sheet_mobility_for(nu):
+    return lib().oracle_sheet_mobility_for(nu)
+
+
+def rut_heal(grain, moisture):
+    out = np.zeros(4, np.float32)
+    lib().oracle_rut_heal(grain, moisture, _ptr(out))
+    return dict(level_s=float(out[0]), relief0=float(out[1]), relief_8s=float(out[2]),
+                still_deep_at_8s=bool(out[3] > 0.5))
+
+
+FIELDS = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7}
+
+
+class Core:
+    """The reference `FluidCore` subset on the sheet path (window 200 at 0.2 m by default)."""
+
+    def __init__(self, res=200, cell=0.2, fine_res=160, fine_cell=0.02, layout=0, tire_r=0.56,
+                 soften=True, inner_par=False, center=(0.0, 0.0)):
+        self.res = res
+        self.fine_res = fine_res
+        cfg = CoreCfg(res, cell, fine_res, fine_cell, layout, tire_r, int(soften), int(inner_par),
+                      center[0], center[1])
+        self.h = lib().oracle_core_new(ctypes.byref(cfg))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_core_free(self.h)
+            self.h = None
+
+    def map_water_bed(self, bed, water):
+        return lib().oracle_core_map_water_bed(self.h, _ptr(f32(bed)), _ptr(f32(water)))
+
+    def map_grain(self, grain):
+        lib().oracle_core_map_grain(self.h, _ptr(np.ascontiguousarray(grain, np.uint8)))
+
+    def map_water_velocity(self, u, v):
+        lib().oracle_core_map_water_velocity(self.h, _ptr(f32(u)), _ptr(f32(v)))
+
+    def pour_water(self, x0, x1, z0, z1, depth):
+        return lib().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 1, 3, 1.0)
+
+    def pour_slurry(self, x0, x1, z0, z1, depth, grain, moisture):
+        return lib().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 0, grain, moisture)
+
+    def lay_slurry_mask(self, depth, grain, moisture):
+        return lib().oracle_core_lay_slurry_mask(self.h, _ptr(f32(depth)), grain, moisture)
+
+    def read_substrate(self, bed, moisture, grain):
+        lib().oracle_core_read_substrate(self.h, _ptr(f32(bed)), _ptr(f32(moisture)),
+                                         _ptr(np.ascontiguousarray(grain, np.uint8)))
+
+    def push_tire(self, **kw):
+        t = Tire(kw["x"], kw["z"], kw.get("forward_x", 0.0), kw.get("forward_z", 1.0), kw["radius"],
+                 kw["width"], kw["speed"], kw.get("slip", 0.0))
+        lib().oracle_core_push_tire(self.h, ctypes.byref(t))
+
+    def step(self, dt):
+        cap = 65536
+        buf = (Spray * cap)()
+        n = lib().oracle_core_step(self.h, dt, buf, cap)
+        return [(s.x, s.y, s.z, s.vx, s.vy, s.vz, s.volume, s.kind) for s in buf[:min(n, cap)]]
+
+    def ledger(self):
+        o = np.zeros(5, np.float32)
+        o64 = np.zeros(2, np.float64)
+        lib().oracle_core_ledger(self.h, _ptr(o), _ptr(o64))
+        return dict(water_m3=float(o[0]), slurry_m3=float(o[1]), frozen_water_m3=float(o[2]),
+                    frozen_slurry_m3=float(o[3]), spray_m3=float(o[4]), water64=float(o64[0]),
+                    slurry64=float(o64[1]))
+
+    def get(self, name):
+        out = np.zeros(self.res * self.res, np.float32)
+        lib().oracle_core_get(self.h, FIELDS[name], _ptr(out))
+        return out
+
+    def set(self, name, arr):
+        lib().oracle_core_set(self.h, FIELDS[name], _ptr(f32(arr)))
+
+    def grain(self):
+        out = np.zeros(self.res * self.res, np.uint8)
+        lib().oracle_core_get_grain(self.h, _ptr(out))
+        return out
+
+    def publish(self):
+        film = np.zeros(2 * self.res * self.res, np.float32)
+        flow = np.zeros(4 * self.res * self.res, np.float32)
+        lib().oracle_core_publish(self.h, _ptr(film), _ptr(flow))
+        return film, flow
+
+    def set_fine_pace(self, pace):
+        lib().oracle_core_set_fine_pace(self.h, pace)
+
+    def set_fine_sub_cap(self, cap):
+        lib().oracle_core_set_fine_sub_cap(self.h, cap)
+
+    def set_near_field(self, on):
+        lib().oracle_core_set_near_field(self.h, int(on))
+
+    def near_tiles(self):
+        return lib().oracle_core_near_tiles(self.h)
+
+    def spray_m3(self):
+        return lib().oracle_core_spray_m3(self.h)
+
+    def non_finite_count(self):
+        return lib().oracle_core_non_finite(self.h)
+
+    def sample(self, x, z):
+        o = np.zeros(7, np.float32)
+        lib().oracle_core_sample(self.h, x, z, _ptr(o))
+        return dict(water_m=float(o[0]), slurry_m=float(o[1]), u=float(o[2]), v=float(o[3]),
+                    moisture=float(o[5]), bed_m=float(o[6]))
+
+    def fine_water_debug(self, tires, patch=0):
+        arr = (Tire * len(tires))()
+        for k, t in enumerate(tires):
+            arr[k] = Tire(t["x"], t["z"], t.get("forward_x", 0.0), t.get("forward_z", 1.0), t["radius"],
+                          t["width"], t["speed"], t.get("slip", 0.0))
+        out = np.zeros(self.fine_res * self.fine_res, np.float32)
+        org = np.zeros(2, np.float32)
+        lib().oracle_core_fine_water_debug(self.h, arr, len(tires), patch, _ptr(out), _ptr(org))
+        return out, org
+
+    def set_inflow(self, j, x0, x1, rate_m3_s):
+        lib().oracle_core_inflow(self.h, j, x0, x1, rate_m3_s)

@@ -1,0 +1,1897 @@
+// TEST INFRASTRUCTURE ONLY: CPU restatement of the reference sheet step used
+// as the parity checker and the timed CPU baseline. Every function cites the
+// reference file:line it restates (paths inside x3-team/Dirty-gen). The
+// product never links this file.
+//
+// Build: g++ -O2 -ffp-contract=off -fno-fast-math (see oracle/Makefile).
+#include "sheet_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <utility>
+#include <vector>
+
+namespace {
+
+typedef uint8_t u8;
+typedef size_t usize;
+
+// ---------------------------------------------------------------- constants
+// src/fluid_core.rs:69-124
+const float GAUSS[5] = {0.06f, 0.24f, 0.40f, 0.24f, 0.06f};
+const float STEEP[5] = {0.02f, 0.08f, 0.80f, 0.08f, 0.02f};
+const float GRAVITY = 9.81f;
+const float FINE_CELL_M = 0.02f;
+const usize FINE_RES = 160;
+const usize SERIAL_SHEET_MAX = 96;          // :2480
+const float FILM_SPEED_CAP_MPS = 1.6f;      // :10003
+const usize BOX_PAR_GAP = 6;                // :1870
+const usize SLEEP_TILE = 8;                 // :1528
+const float SLEEP_SPEED = 0.05f;            // :1531
+const float SLEEP_SLOPE = 0.02f;            // :1533
+const usize NU_FILL_MARGIN = 8;             // :791
+const float NEAR_RESIDUAL_LIFE_S = 1.5f;    // near.rs:37
+const float NEAR_DROP_M = 1.0e-5f;          // near.rs:39
+const float NEAR_FILM_M = 1.0e-6f;          // near.rs:41
+
+// ------------------------------------------------- Rust f32 helper semantics
+inline float rmax(float a, float b) { return fmaxf(a, b); }   // f32::max (NaN-ignoring)
+inline float rmin(float a, float b) { return fminf(a, b); }   // f32::min
+inline float rclamp(float x, float lo, float hi) {           // f32::clamp (NaN stays)
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+inline bool finite(float x) { return std::isfinite(x); }
+inline float rsignum(float x) {  // f32::signum: +1 for +0.0, -1 for -0.0
+    if (std::isnan(x)) return x;
+    return std::signbit(x) ? -1.0f : 1.0f;
+}
+inline usize sat_sub(usize a, usize b) { return a > b ? a - b : 0; }
+inline usize f2usize(float x) {  // `as usize`, saturating, NaN -> 0
+    if (!(x > 0.0f)) return 0;
+    if (x >= 1.8e19f) return (usize)-1;
+    return (usize)x;
+}
+inline uint32_t fbits(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    return b;
+}
+// Iterator::sum for f32 folds from -0.0 in the reference toolchain.
+inline float rsum(const float* p, usize n) {
+    float s = -0.0f;
+    for (usize k = 0; k < n; ++k) s += p[k];
+    return s;
+}
+
+struct Box {
+    usize i0, i1, j0, j1;
+    bool operator==(const Box& o) const {
+        return i0 == o.i0 && i1 == o.i1 && j0 == o.j0 && j1 == o.j1;
+    }
+};
+
+// -------------------------------------------------------------- material laws
+// src/fluid_core.rs:150-161
+float dynamic_viscosity(u8 grain, float moisture) {
+    float x = rclamp((rclamp(moisture, 0.0f, 1.0f) - 0.22f) / 0.70f, 0.0f, 1.0f);
+    float thin = x * x * (3.0f - 2.0f * x);
+    float stiff, fluid;
+    switch (grain) {
+        case 1: stiff = 220.0f; fluid = 4.0f; break;     // Silt
+        case 2: stiff = 28.0f; fluid = 0.55f; break;     // Sand
+        case 3: stiff = 0.9f; fluid = 0.9f; break;       // Water
+        case 4: stiff = 1.5f; fluid = 0.08f; break;      // Other
+        default: stiff = 420.0f; fluid = 0.35f; break;   // Clay (0 and unknown)
+    }
+    return stiff + (fluid - stiff) * thin;
+}
+
+// src/fluid_core.rs:169-180
+float sheet_mobility_for(float nu) {
+    if (nu < 0.0f) return -nu;
+    float boost;
+    if (nu < 12.0f) {
+        float t = rclamp((12.0f - rmax(nu, 0.0f)) / 12.0f, 0.0f, 1.0f);
+        boost = t * t * 1.6f;
+    } else {
+        boost = 0.0f;
+    }
+    return 0.042f * (1.0f + boost);
+}
+
+// src/fluid_core.rs:184-192
+float sheet_damp(float nu) {
+    float rel = rclamp(rmax(nu, 0.05f) / 231.0f, 0.002f, 12.0f);
+    if (rel >= 0.42f) return 1.70f * powf(rel, 0.30f);
+    float at_silt = 1.70f * powf(0.42f, 0.30f);
+    float t = rclamp(rel / 0.42f, 0.0f, 1.0f);
+    return at_silt * powf(t, 1.15f);
+}
+
+// src/fluid_core.rs:3473-3479
+float finite_speed(float v, float lim) { return finite(v) ? rclamp(v, -lim, lim) : 0.0f; }
+float finite0(float v) { return finite(v) ? v : 0.0f; }
+
+// ------------------------------------------------------------------- scratch
+// src/fluid_core.rs:536-579
+struct Scratch {
+    usize n = 0;
+    std::vector<float> a, b, c, d, e, removed, added, flux_l, flux_r;
+    void fit(usize n_) {
+        if (n == n_) return;
+        n = n_;
+        a.resize(n, 0.0f); b.resize(n, 0.0f); c.resize(n, 0.0f); d.resize(n, 0.0f);
+        e.resize(n, 0.0f); removed.resize(n, 0.0f); added.resize(n, 0.0f);
+    }
+};
+
+// ------------------------------------------------------------------ stencils
+// src/fluid_core.rs:3498-3540
+float vorticity_at(const float* u, const float* v, usize res, usize i, usize j, float cell) {
+    usize ip = std::min(i + 1, res - 1), im = sat_sub(i, 1);
+    usize jp = std::min(j + 1, res - 1), jm = sat_sub(j, 1);
+    float dvdx = (v[j * res + ip] - v[j * res + im]) / (2.0f * cell);
+    float dudz = (u[jp * res + i] - u[jm * res + i]) / (2.0f * cell);
+    return dvdx - dudz;
+}
+void grad(const float* p, usize res, usize i, usize j, float cell, float& dx, float& dz) {
+    usize ip = std::min(i + 1, res - 1), im = sat_sub(i, 1);
+    usize jp = std::min(j + 1, res - 1), jm = sat_sub(j, 1);
+    dx = (p[j * res + ip] - p[j * res + im]) / (2.0f * cell);
+    dz = (p[jp * res + i] - p[jm * res + i]) / (2.0f * cell);
+}
+void grad_vel(const float* u, const float* v, usize res, usize i, usize j, float cell,
+              float& dux, float& dvz) {
+    usize ip = std::min(i + 1, res - 1), im = sat_sub(i, 1);
+    usize jp = std::min(j + 1, res - 1), jm = sat_sub(j, 1);
+    dux = (u[j * res + ip] - u[j * res + im]) / (2.0f * cell);
+    dvz = (v[jp * res + i] - v[jm * res + i]) / (2.0f * cell);
+}
+float lap(const float* p, usize res, usize i, usize j, float cell) {
+    usize idx = j * res + i;
+    usize ip = std::min(i + 1, res - 1), im = sat_sub(i, 1);
+    usize jp = std::min(j + 1, res - 1), jm = sat_sub(j, 1);
+    float s = p[j * res + ip] + p[j * res + im] + p[jp * res + i] + p[jm * res + i] - 4.0f * p[idx];
+    return s / (cell * cell);
+}
+// src/fluid_core.rs:2833-2838
+inline float vort_interior(const float* u, const float* v, usize res, usize i, usize j, float two) {
+    float dvdx = (v[j * res + i + 1] - v[j * res + i - 1]) / two;
+    float dudz = (u[(j + 1) * res + i] - u[(j - 1) * res + i]) / two;
+    return dvdx - dudz;
+}
+
+// Confinement kick shared by the four variants: src/fluid_core.rs:3442-3471,
+// :2805-2831, :2348-2375, :2446-2470. `su,sv` are read, `u,v` written.
+void confine_one(const float* su, const float* sv, float* u, float* v, usize res, usize i,
+                 usize j, float cell, float dt, float eps) {
+    float w = vorticity_at(su, sv, res, i, j, cell);
+    if (!finite(w) || fabsf(w) < 1.0e-4f) return;
+    float wxp = fabsf(vorticity_at(su, sv, res, std::min(i + 1, res - 1), j, cell));
+    float wxm = fabsf(vorticity_at(su, sv, res, sat_sub(i, 1), j, cell));
+    float wzp = fabsf(vorticity_at(su, sv, res, i, std::min(j + 1, res - 1), cell));
+    float wzm = fabsf(vorticity_at(su, sv, res, i, sat_sub(j, 1), cell));
+    float nx = (wxp - wxm) / (2.0f * cell);
+    float nz = (wzp - wzm) / (2.0f * cell);
+    float du = eps * dt * (-nz * w);
+    float dv = eps * dt * (nx * w);
+    if (finite(du) && finite(dv) && du * du + dv * dv <= 0.0625f) {
+        usize idx = j * res + i;
+        u[idx] += du;
+        v[idx] += dv;
+    }
+}
+void confine_interior(const float* su, const float* sv, float* u, float* v, usize res, usize i,
+                      usize j, float dt, float eps, float two) {
+    float w = vort_interior(su, sv, res, i, j, two);
+    if (!finite(w) || fabsf(w) < 1.0e-4f) return;
+    float wxp = fabsf(vort_interior(su, sv, res, i + 1, j, two));
+    float wxm = fabsf(vort_interior(su, sv, res, i - 1, j, two));
+    float wzp = fabsf(vort_interior(su, sv, res, i, j + 1, two));
+    float wzm = fabsf(vort_interior(su, sv, res, i, j - 1, two));
+    float nx = (wxp - wxm) / two;
+    float nz = (wzp - wzm) / two;
+    float du = eps * dt * (-nz * w);
+    float dv = eps * dt * (nx * w);
+    if (finite(du) && finite(dv) && du * du + dv * dv <= 0.0625f) {
+        usize idx = j * res + i;
+        u[idx] += du;
+        v[idx] += dv;
+    }
+}
+
+// ---------------------------------------------------------------------- blur
+// src/fluid_core.rs:3680-3758 (accum5, accum5_clamped, blur_axis_x/z)
+inline float accum5(float a0, float a1, float a2, float a3, float a4, const float* k) {
+    float a = a0 * k[0];
+    a += a1 * k[1];
+    a += a2 * k[2];
+    a += a3 * k[3];
+    a += a4 * k[4];
+    return a;
+}
+inline float accum5_clamped(const float* row, usize r, usize i, const float* k) {
+    float a = 0.0f;
+    for (int t = -2; t <= 2; ++t) {
+        long ii = (long)i + t;
+        if (ii < 0) ii = 0;
+        if (ii > (long)r - 1) ii = (long)r - 1;
+        a += row[ii] * k[t + 2];
+    }
+    return a;
+}
+void blur_axis_x(const float* src, float* tmp, usize res, usize j, usize i0, usize i1, const float* k) {
+    const float* row = src + j * res;
+    float* dst = tmp + j * res;
+    usize lo = std::max(i0, (usize)2);
+    usize hi = std::min(i1, sat_sub(res, 3));
+    for (usize i = i0; i < std::min(lo, i1 + 1); ++i) dst[i] = accum5_clamped(row, res, i, k);
+    if (lo <= hi)
+        for (usize i = lo; i <= hi; ++i)
+            dst[i] = accum5(row[i - 2], row[i - 1], row[i], row[i + 1], row[i + 2], k);
+    usize tail = std::max(hi + 1, lo);
+    for (usize i = tail; i <= i1; ++i) dst[i] = accum5_clamped(row, res, i, k);
+}
+void blur_axis_z(const float* src, float* dst, usize res, usize j, usize i0, usize i1, const float* k) {
+    if (j >= 2 && j <= sat_sub(res, 3)) {
+        const float* r0 = src + (j - 2) * res;
+        const float* r1 = src + (j - 1) * res;
+        const float* r2 = src + j * res;
+        const float* r3 = src + (j + 1) * res;
+        const float* r4 = src + (j + 2) * res;
+        for (usize i = i0; i <= i1; ++i) dst[j * res + i] = accum5(r0[i], r1[i], r2[i], r3[i], r4[i], k);
+    } else {
+        for (usize i = i0; i <= i1; ++i) {
+            float a = 0.0f;
+            for (int t = -2; t <= 2; ++t) {
+                long jj = (long)j + t;
+                if (jj < 0) jj = 0;
+                if (jj > (long)res - 1) jj = (long)res - 1;
+                a += src[jj * res + i] * k[t + 2];
+            }
+            dst[j * res + i] = a;
+        }
+    }
+}
+// src/fluid_core.rs:3541-3569
+void blur_box(const float* src, float* dst, float* tmp, usize res, usize i0, usize i1, usize j0,
+              usize j1, const float* k) {
+    if (i0 > i1 || j0 > j1 || res == 0) return;
+    for (usize j = j0; j <= j1; ++j) blur_axis_x(src, tmp, res, j, i0, i1, k);
+    for (usize j = j0; j <= j1; ++j) blur_axis_z(tmp, dst, res, j, i0, i1, k);
+}
+
+// ------------------------------------------------------------ gravity + confine
+// Snapshot-Jacobi confinement: force_gravity_par (src/fluid_core.rs:2263-2378) and
+// gravity_jacobi_serial/jacobi_confine_box (:2530-2595, :2415-2473) give the same
+// values: every cell reads the post-gravity snapshot.
+void jacobi_confine(const float* h, float* u, float* v, usize res, float cell, float dt,
+                    float vorticity, float eps, usize i0, usize i1, usize j0, usize j1) {
+    usize n = res * res;
+    std::vector<float> su(u, u + n), sv(v, v + n);
+    float two = 2.0f * cell;
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            if (h[idx] <= eps) continue;
+            if (i >= 2 && j >= 2 && i + 2 < res && j + 2 < res)
+                confine_interior(su.data(), sv.data(), u, v, res, i, j, dt, vorticity, two);
+            else
+                confine_one(su.data(), sv.data(), u, v, res, i, j, cell, dt, vorticity);
+        }
+}
+
+// src/fluid_core.rs:2204-2261 (serial sweep) with its two Jacobi branches.
+void force_gravity_open(const float* h, float* u, float* v, const float* nu, const float* p,
+                        usize res, float cell, float dt, float vorticity, float eps, usize i0,
+                        usize i1, usize j0, usize j1, bool inner_par) {
+    float two = 2.0f * cell;
+    bool fine = cell <= FINE_CELL_M + 1.0e-6f;
+    bool par = (j1 - j0 >= 47) && (i1 - i0 >= 31) && inner_par;
+    bool jacobi = fine || par;
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            if (h[idx] <= eps) continue;
+            float px, pz;
+            if (i >= 2 && j >= 2 && i + 2 < res && j + 2 < res) {
+                px = (p[idx + 1] - p[idx - 1]) / two;
+                pz = (p[idx + res] - p[idx - res]) / two;
+            } else {
+                grad(p, res, i, j, cell, px, pz);
+            }
+            float mob = sheet_mobility_for(nu[idx]);
+            u[idx] += -GRAVITY * px * mob * dt;
+            v[idx] += -GRAVITY * pz * mob * dt;
+            if (!jacobi && vorticity > 0.0f) {
+                if (i >= 2 && j >= 2 && i + 2 < res && j + 2 < res)
+                    confine_interior(u, v, u, v, res, i, j, dt, vorticity, two);
+                else
+                    confine_one(u, v, u, v, res, i, j, cell, dt, vorticity);
+            }
+        }
+    if (jacobi && vorticity > 0.0f) jacobi_confine(h, u, v, res, cell, dt, vorticity, eps, i0, i1, j0, j1);
+}
+
+// ------------------------------------------------------------------ transport
+// src/fluid_core.rs:2867-2911 open_edge_dh
+inline float open_edge_dh(bool BED, float hd, float hr, float remd, u8 gate_r, float bed_d,
+                          float bed_r, float speed, float dt, float cell, float frac_cap) {
+    bool live = !(fabsf(speed) < 1.0e-5f);
+    bool bank = BED && hr <= 1.0e-6f && bed_r > bed_d + hd + 1.0e-3f;
+    float room = hd - remd;
+    bool gate_shut = gate_r == 0 && hr <= 1.0e-6f;
+    float frac = rmin(fabsf(speed) * dt / cell, frac_cap);
+    float dh = rmin(hd * frac, room);
+    bool ok = live & !bank & !(room <= 1.0e-8f) & !gate_shut & !(dh <= 1.0e-8f);
+    return ok ? dh : 0.0f;
+}
+
+// src/fluid_core.rs:3025-3137 transport_open_rows_body
+void transport_open_rows(bool BED, float* h, const float* vel, const u8* gate, usize res, float cell,
+                         float dt, usize i0, usize i1, usize j0, usize j1, bool along_x,
+                         const float* bed, float frac_cap, Scratch& sc) {
+    usize m = i1 + 1 - i0;
+    if (along_x) {
+        if (sc.flux_l.size() < m) {
+            sc.flux_l.resize(m, 0.0f);
+            sc.flux_r.resize(m, 0.0f);
+        }
+        for (usize j = j0; j <= j1; ++j) {
+            usize lo = j * res + i0;
+            float* hr = h + lo;
+            const float* vr = vel + lo;
+            const u8* gr = gate + lo;
+            const float* br = BED ? bed + lo : nullptr;
+            float* fl = sc.flux_l.data();
+            float* fr = sc.flux_r.data();
+            usize edges = m - 1;
+            for (usize k = 0; k < edges; ++k) {
+                float speed = 0.5f * (vr[k] + vr[k + 1]);
+                float bd = BED ? br[k + 1] : 0.0f, bc = BED ? br[k] : 0.0f;
+                float dh = open_edge_dh(BED, hr[k + 1], hr[k], 0.0f, gr[k], bd, bc, speed, dt, cell, frac_cap);
+                fl[k] = speed > 0.0f ? 0.0f : dh;
+            }
+            for (usize k = 0; k < edges; ++k) {
+                float speed = 0.5f * (vr[k] + vr[k + 1]);
+                float prev = k > 0 ? fl[k - 1] : 0.0f;
+                float bd = BED ? br[k] : 0.0f, bc = BED ? br[k + 1] : 0.0f;
+                float dh = open_edge_dh(BED, hr[k], hr[k + 1], 0.0f + prev, gr[k + 1], bd, bc, speed, dt, cell, frac_cap);
+                fr[k] = speed > 0.0f ? dh : 0.0f;
+            }
+            fl[edges] = 0.0f;
+            fr[edges] = 0.0f;
+            float* rem = sc.removed.data() + lo;
+            float* add = sc.added.data() + lo;
+            rem[0] = (0.0f + 0.0f) + fr[0];
+            add[0] = (0.0f + 0.0f) + fl[0];
+            for (usize c = 1; c < m; ++c) {
+                rem[c] = (0.0f + fl[c - 1]) + fr[c];
+                add[c] = (0.0f + fr[c - 1]) + fl[c];
+            }
+            for (usize c = 0; c < m; ++c) {
+                float moved = rmax(hr[c] - rem[c] + add[c], 0.0f);
+                hr[c] = (rem[c] > 0.0f || add[c] > 0.0f) ? moved : hr[c];
+            }
+        }
+        return;
+    }
+    for (usize j = j0; j <= j1; ++j) {
+        usize lo = j * res + i0;
+        std::fill(sc.removed.begin() + lo, sc.removed.begin() + lo + m, 0.0f);
+        std::fill(sc.added.begin() + lo, sc.added.begin() + lo + m, 0.0f);
+    }
+    for (usize j = j0; j < j1; ++j) {
+        usize lo = j * res + i0;
+        const float* ha = h + lo;
+        const float* hb = h + lo + res;
+        const float* va = vel + lo;
+        const float* vb = vel + lo + res;
+        const u8* ga = gate + lo;
+        const u8* gb = gate + lo + res;
+        float* ra = sc.removed.data() + lo;
+        float* rb = sc.removed.data() + lo + res;
+        float* aa = sc.added.data() + lo;
+        float* ab = sc.added.data() + lo + res;
+        const float* ba = BED ? bed + lo : nullptr;
+        const float* bb = BED ? bed + lo + res : nullptr;
+        // src/fluid_core.rs:2916-2960 open_row_pair
+        for (usize i = 0; i < m; ++i) {
+            float speed = 0.5f * (va[i] + vb[i]);
+            float bd = BED ? bb[i] : 0.0f, bc = BED ? ba[i] : 0.0f;
+            float dh = open_edge_dh(BED, hb[i], ha[i], 0.0f, ga[i], bd, bc, speed, dt, cell, frac_cap);
+            float up = speed > 0.0f ? 0.0f : dh;
+            rb[i] += up;
+            aa[i] += up;
+        }
+        for (usize i = 0; i < m; ++i) {
+            float speed = 0.5f * (va[i] + vb[i]);
+            float bd = BED ? ba[i] : 0.0f, bc = BED ? bb[i] : 0.0f;
+            float dh = open_edge_dh(BED, ha[i], hb[i], ra[i], gb[i], bd, bc, speed, dt, cell, frac_cap);
+            float down = speed > 0.0f ? dh : 0.0f;
+            ra[i] += down;
+            ab[i] += down;
+        }
+    }
+    for (usize j = j0; j <= j1; ++j) {
+        usize lo = j * res + i0;
+        for (usize c = 0; c < m; ++c) {
+            float r = sc.removed[lo + c], a = sc.added[lo + c];
+            float moved = rmax(h[lo + c] - r + a, 0.0f);
+            h[lo + c] = (r > 0.0f || a > 0.0f) ? moved : h[lo + c];
+        }
+    }
+}
+
+// src/fluid_core.rs:3140-3206 transport_open_ref + flux_open :3411-3440 (serial definition)
+void transport_open_serial(float* h, const float* vel, const u8* gate, usize res, float cell,
+                           float dt, usize i0, usize i1, usize j0, usize j1, bool along_x,
+                           const float* bed, float frac_cap, Scratch& sc) {
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) sc.removed[j * res + i] = sc.added[j * res + i] = 0.0f;
+    auto flux = [&](usize a, usize b, float speed) {
+        usize donor = speed > 0.0f ? a : b, recv = speed > 0.0f ? b : a;
+        float room = h[donor] - sc.removed[donor];
+        if (room <= 1.0e-8f) return;
+        if (gate[recv] == 0 && h[recv] <= 1.0e-6f) return;
+        float frac = rmin(fabsf(speed) * dt / cell, frac_cap);
+        float dh = rmin(h[donor] * frac, room);
+        if (dh <= 1.0e-8f) return;
+        sc.removed[donor] += dh;
+        sc.added[recv] += dh;
+    };
+    auto edge = [&](usize a, usize b) {
+        float speed = 0.5f * (vel[a] + vel[b]);
+        if (fabsf(speed) < 1.0e-5f) return;
+        if (bed) {
+            usize donor = speed > 0.0f ? a : b, recv = speed > 0.0f ? b : a;
+            if (h[recv] <= 1.0e-6f && bed[recv] > bed[donor] + h[donor] + 1.0e-3f) return;
+        }
+        flux(a, b, speed);
+    };
+    if (along_x) {
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i < i1; ++i) edge(j * res + i, j * res + i + 1);
+    } else {
+        for (usize j = j0; j < j1; ++j)
+            for (usize i = i0; i <= i1; ++i) edge(j * res + i, j * res + i + res);
+    }
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            float r = sc.removed[idx], a = sc.added[idx];
+            float moved = rmax(h[idx] - r + a, 0.0f);
+            h[idx] = (r > 0.0f || a > 0.0f) ? moved : h[idx];
+        }
+}
+
+// -------------------------------------------------------------------- substep
+// src/fluid_core.rs:1879-2082, open sheet (no walls), gravity drive.
+void substep(float* h, float* u, float* v, const float* bed, const float* nu, const u8* gate,
+             usize res, float cell, float dt, float vorticity, float eps, usize i0, usize i1,
+             usize j0, usize j1, bool banks, bool do_flux, Scratch& sc, bool inner_par) {
+    usize hi0 = sat_sub(i0, 2), hi1 = std::min(i1 + 2, res - 1);
+    usize hj0 = sat_sub(j0, 2), hj1 = std::min(j1 + 2, res - 1);
+    for (usize j = hj0; j <= hj1; ++j)
+        for (usize i = hi0; i <= hi1; ++i) sc.a[j * res + i] = bed[j * res + i] + h[j * res + i];
+    blur_box(sc.a.data(), sc.b.data(), sc.e.data(), res, i0, i1, j0, j1, GAUSS);
+    blur_box(sc.a.data(), sc.c.data(), sc.e.data(), res, i0, i1, j0, j1, STEEP);
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            float filtered = 0.62f * sc.b[idx] + 0.38f * sc.c[idx];
+            sc.d[idx] = 0.45f * filtered + 0.55f * sc.a[idx];
+        }
+    force_gravity_open(h, u, v, nu, sc.d.data(), res, cell, dt, vorticity, eps, i0, i1, j0, j1, inner_par);
+    bool project = cell > FINE_CELL_M + 1.0e-6f;
+    if (project) {
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float ux, vz;
+                grad_vel(u, v, res, i, j, cell, ux, vz);
+                float div = ux + vz;
+                float lap_h = lap(sc.a.data(), res, i, j, cell);
+                float overload = 1.0f + rclamp(nu[idx] / 231.0f, 0.0f, 6.0f);
+                sc.b[idx] = div * overload - 0.015f * overload * lap_h;
+            }
+        blur_box(sc.b.data(), sc.c.data(), sc.e.data(), res, i0, i1, j0, j1, GAUSS);
+        blur_box(sc.b.data(), sc.a.data(), sc.e.data(), res, i0, i1, j0, j1, STEEP);
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                sc.d[idx] = 0.62f * sc.c[idx] + 0.38f * sc.a[idx];
+            }
+    }
+    uint32_t memo_nu = 0x7fc00000u;  // f32::NAN bits
+    float memo_decay = 1.0f;
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            if (h[idx] <= eps) continue;
+            if (project) {
+                float qx, qz;
+                grad(sc.d.data(), res, i, j, cell, qx, qz);
+                u[idx] += 0.012f * dt * qx;
+                v[idx] += 0.012f * dt * qz;
+            }
+            float nu_here = nu[idx];
+            if (fbits(nu_here) != memo_nu) {
+                memo_nu = fbits(nu_here);
+                memo_decay = expf(-sheet_damp(nu_here) * dt);
+            }
+            float decay = memo_decay;
+            u[idx] = finite_speed(u[idx] * decay, FILM_SPEED_CAP_MPS);
+            v[idx] = finite_speed(v[idx] * decay, FILM_SPEED_CAP_MPS);
+        }
+    if (!do_flux) return;
+    const float* open_bed = banks ? bed : nullptr;
+    transport_open_rows(banks, h, u, gate, res, cell, dt, i0, i1, j0, j1, true, open_bed, 0.45f, sc);
+    transport_open_rows(banks, h, v, gate, res, cell, dt, i0, i1, j0, j1, false, open_bed, 0.45f, sc);
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize idx = j * res + i;
+            if (eps > 0.0f && h[idx] < eps) h[idx] = u[idx] = v[idx] = 0.0f;
+        }
+}
+
+// ---------------------------------------------------------------- work boxes
+// src/fluid_core.rs:1306-1319
+float wet_sum(const float* h, usize n, float eps) {
+    float lanes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    usize chunks = n / 8;
+    for (usize c = 0; c < chunks; ++c)
+        for (int k = 0; k < 8; ++k) {
+            float x = h[c * 8 + k];
+            lanes[k] += x > eps ? x : 0.0f;
+        }
+    float sum = rsum(lanes, 8);
+    for (usize k = chunks * 8; k < n; ++k) {
+        float x = h[k];
+        sum += x > eps ? x : 0.0f;
+    }
+    return sum;
+}
+
+// src/fluid_core.rs:794-818
+bool wet_bounds(const float* h, usize res, usize margin, Box& out) {
+    usize j0 = (usize)-1, j1 = 0, i0 = (usize)-1, i1 = 0;
+    for (usize j = 0; j < res; ++j) {
+        const float* row = h + j * res;
+        long first = -1, last = -1;
+        for (usize i = 0; i < res; ++i)
+            if (row[i] > 0.0f) {
+                if (first < 0) first = (long)i;
+                last = (long)i;
+            }
+        if (first < 0) continue;
+        j0 = std::min(j0, j);
+        j1 = j;
+        i0 = std::min(i0, (usize)first);
+        i1 = std::max(i1, (usize)last);
+    }
+    if (j0 == (usize)-1) return false;
+    out = {sat_sub(i0, margin), std::min(i1 + margin, res - 1), sat_sub(j0, margin), std::min(j1 + margin, res - 1)};
+    return true;
+}
+
+// src/fluid_core.rs:1449-1479
+bool boxes_touch(const Box& a, const Box& b) {
+    return sat_sub(a.i0, 1) <= b.i1 + 1 && sat_sub(b.i0, 1) <= a.i1 + 1 &&
+           sat_sub(a.j0, 1) <= b.j1 + 1 && sat_sub(b.j0, 1) <= a.j1 + 1;
+}
+void merge_boxes(std::vector<Box>& boxes) {
+    for (;;) {
+        bool did = false;
+        usize i = 0;
+        while (i < boxes.size()) {
+            usize j = i + 1;
+            while (j < boxes.size()) {
+                if (boxes_touch(boxes[i], boxes[j])) {
+                    Box a = boxes[i], b = boxes[j];
+                    boxes[i] = {std::min(a.i0, b.i0), std::max(a.i1, b.i1), std::min(a.j0, b.j0), std::max(a.j1, b.j1)};
+                    boxes[j] = boxes.back();  // swap_remove
+                    boxes.pop_back();
+                    did = true;
+                } else {
+                    ++j;
+                }
+            }
+            ++i;
+        }
+        if (!did) break;
+    }
+}
+
+const usize SPLIT_HALO = 6;
+
+// src/fluid_core.rs:1325-1447 (run-length bodies)
+std::vector<Box> sheet_work_boxes(const float* h, usize res, float eps, bool allow_split) {
+    usize i0 = res, i1 = 0, j0 = res, j1 = 0, wet = 0;
+    for (usize j = 0; j < res; ++j) {
+        const float* row = h + j * res;
+        usize c = 0;
+        for (usize i = 0; i < res; ++i) c += row[i] > eps;
+        if (c == 0) continue;
+        wet += c;
+        usize first = 0, last = 0;
+        for (usize i = 0; i < res; ++i) if (row[i] > eps) { first = i; break; }
+        for (usize i = res; i-- > 0;) if (row[i] > eps) { last = i; break; }
+        i0 = std::min(i0, first);
+        i1 = std::max(i1, last);
+        j0 = std::min(j0, j);
+        j1 = std::max(j1, j);
+    }
+    if (wet == 0) return {};
+    Box whole = {sat_sub(i0, 3), std::min(i1 + 3, res - 1), sat_sub(j0, 3), std::min(j1 + 3, res - 1)};
+    bool solid = wet == (i1 - i0 + 1) * (j1 - j0 + 1);
+    if (!allow_split || solid) return {whole};
+    std::vector<std::pair<usize, usize>> all;
+    std::vector<uint32_t> parent;
+    std::vector<Box> bbox;
+    std::vector<usize> first;
+    auto root = [&](uint32_t x) {
+        while (parent[x] != x) {
+            uint32_t up = parent[parent[x]];
+            parent[x] = up;
+            x = up;
+        }
+        return x;
+    };
+    usize prev0 = 0, prev1 = 0;
+    for (usize j = j0; j <= j1; ++j) {
+        const float* row = h + j * res;
+        usize start = all.size();
+        usize i = i0;
+        while (i <= i1) {
+            if (!(row[i] > eps)) { ++i; continue; }
+            usize a = i;
+            while (i <= i1 && row[i] > eps) ++i;
+            usize b = i - 1;
+            uint32_t id = (uint32_t)all.size();
+            all.push_back({a, b});
+            parent.push_back(id);
+            bbox.push_back({a, b, j, j});
+            first.push_back(j * res + a);
+            for (usize k = prev0; k < prev1; ++k) {
+                usize pa = all[k].first, pb = all[k].second;
+                if (pa <= b && a <= pb) {
+                    uint32_t ra = root((uint32_t)k), rb = root(id);
+                    if (ra != rb) {
+                        uint32_t keep = ra < rb ? ra : rb, gone = ra < rb ? rb : ra;
+                        parent[gone] = keep;
+                        Box g = bbox[gone];
+                        Box& kb = bbox[keep];
+                        kb.i0 = std::min(kb.i0, g.i0);
+                        kb.i1 = std::max(kb.i1, g.i1);
+                        kb.j0 = std::min(kb.j0, g.j0);
+                        kb.j1 = std::max(kb.j1, g.j1);
+                        first[keep] = std::min(first[keep], first[gone]);
+                    }
+                }
+            }
+        }
+        prev0 = start;
+        prev1 = all.size();
+    }
+    std::vector<std::pair<usize, Box>> bodies;
+    for (usize k = 0; k < all.size(); ++k)
+        if (parent[k] == (uint32_t)k) bodies.push_back({first[k], bbox[k]});
+    std::sort(bodies.begin(), bodies.end(), [](const std::pair<usize, Box>& x, const std::pair<usize, Box>& y) { return x.first < y.first; });
+    std::vector<Box> boxes;
+    for (auto& bd : bodies) {
+        Box c = bd.second;
+        boxes.push_back({sat_sub(c.i0, SPLIT_HALO), std::min(c.i1 + SPLIT_HALO, res - 1),
+                         sat_sub(c.j0, SPLIT_HALO), std::min(c.j1 + SPLIT_HALO, res - 1)});
+    }
+    merge_boxes(boxes);
+    if (boxes.size() == 1 || boxes.size() > 8) return {whole};
+    return boxes;
+}
+
+// src/fluid_core.rs:11134-11227 (test-only flood-fill definition)
+std::vector<Box> sheet_work_boxes_flood(const float* h, usize res, float eps, bool allow_split) {
+    usize i0 = res, i1 = 0, j0 = res, j1 = 0, wet = 0;
+    for (usize j = 0; j < res; ++j) {
+        const float* row = h + j * res;
+        usize c = 0;
+        for (usize i = 0; i < res; ++i) c += row[i] > eps;
+        if (c == 0) continue;
+        wet += c;
+        usize first = 0, last = 0;
+        for (usize i = 0; i < res; ++i) if (row[i] > eps) { first = i; break; }
+        for (usize i = res; i-- > 0;) if (row[i] > eps) { last = i; break; }
+        i0 = std::min(i0, first); i1 = std::max(i1, last);
+        j0 = std::min(j0, j); j1 = std::max(j1, j);
+    }
+    if (wet == 0) return {};
+    Box whole = {sat_sub(i0, 3), std::min(i1 + 3, res - 1), sat_sub(j0, 3), std::min(j1 + 3, res - 1)};
+    bool solid = wet == (i1 - i0 + 1) * (j1 - j0 + 1);
+    if (!allow_split || solid) return {whole};
+    std::vector<u8> mark(res * res, 0);
+    std::vector<usize> queue;
+    std::vector<Box> boxes;
+    for (usize j = j0; j <= j1; ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize s = j * res + i;
+            if (h[s] <= eps || mark[s]) continue;
+            usize ci0 = i, ci1 = i, cj0 = j, cj1 = j;
+            mark[s] = 1;
+            queue.clear();
+            queue.push_back(s);
+            while (!queue.empty()) {
+                usize cur = queue.back();
+                queue.pop_back();
+                usize cj = cur / res, ci = cur - cj * res;
+                ci0 = std::min(ci0, ci); ci1 = std::max(ci1, ci);
+                cj0 = std::min(cj0, cj); cj1 = std::max(cj1, cj);
+                long neigh[4] = {ci > 0 ? (long)cur - 1 : -1, ci + 1 < res ? (long)cur + 1 : -1,
+                                 cj > 0 ? (long)(cur - res) : -1, cj + 1 < res ? (long)(cur + res) : -1};
+                for (long nidx : neigh)
+                    if (nidx >= 0 && !mark[nidx] && h[nidx] > eps) {
+                        mark[nidx] = 1;
+                        queue.push_back((usize)nidx);
+                    }
+            }
+            boxes.push_back({sat_sub(ci0, SPLIT_HALO), std::min(ci1 + SPLIT_HALO, res - 1),
+                             sat_sub(cj0, SPLIT_HALO), std::min(cj1 + SPLIT_HALO, res - 1)});
+        }
+    merge_boxes(boxes);
+    if (boxes.size() == 1 || boxes.size() > 8) return {whole};
+    return boxes;
+}
+
+// src/fluid_core.rs:1537-1657
+std::vector<Box> awake_work_boxes(const float* h, const float* u, const float* v, const float* bed,
+                                  usize res, float cell, float eps) {
+    usize tiles = (res + SLEEP_TILE - 1) / SLEEP_TILE;
+    usize ntile = tiles * tiles;
+    std::vector<u8> hot(ntile, 0), grown(ntile, 0);
+    for (usize tj = 0; tj < tiles; ++tj)
+        for (usize ti = 0; ti < tiles; ++ti) {
+            usize i0 = ti * SLEEP_TILE, j0 = tj * SLEEP_TILE;
+            usize i1 = std::min(i0 + SLEEP_TILE, res), j1 = std::min(j0 + SLEEP_TILE, res);
+            bool awake = false;
+            for (usize j = j0; j < j1 && !awake; ++j) {
+                usize row = j * res;
+                for (usize i = i0; i < i1; ++i) {
+                    usize idx = row + i;
+                    if (h[idx] <= eps) continue;
+                    if (hypotf(u[idx], v[idx]) > SLEEP_SPEED) { awake = true; break; }
+                    float eta = bed[idx] + h[idx];
+                    usize ip = i + 1 < res ? row + i + 1 : idx;
+                    usize jp = j + 1 < res ? (j + 1) * res + i : idx;
+                    float dex = fabsf(bed[ip] + h[ip] - eta);
+                    float dez = fabsf(bed[jp] + h[jp] - eta);
+                    if (rmax(dex, dez) > SLEEP_SLOPE * cell) { awake = true; break; }
+                }
+            }
+            if (awake) hot[tj * tiles + ti] = 1;
+        }
+    for (usize tj = 0; tj < tiles; ++tj)
+        for (usize ti = 0; ti < tiles; ++ti) {
+            if (!hot[tj * tiles + ti]) continue;
+            for (int dj = -1; dj <= 1; ++dj)
+                for (int di = -1; di <= 1; ++di) {
+                    long ni = (long)ti + di, nj = (long)tj + dj;
+                    if (ni >= 0 && nj >= 0 && ni < (long)tiles && nj < (long)tiles) grown[nj * tiles + ni] = 1;
+                }
+        }
+    std::vector<u8> seen(ntile, 0);
+    std::vector<usize> stack;
+    std::vector<Box> boxes;
+    for (usize s = 0; s < ntile; ++s) {
+        if (!grown[s] || seen[s]) continue;
+        seen[s] = 1;
+        stack.clear();
+        stack.push_back(s);
+        usize ti0 = s % tiles, ti1 = ti0, tj0 = s / tiles, tj1 = tj0;
+        while (!stack.empty()) {
+            usize cur = stack.back();
+            stack.pop_back();
+            usize tj = cur / tiles, ti = cur - tj * tiles;
+            ti0 = std::min(ti0, ti); ti1 = std::max(ti1, ti);
+            tj0 = std::min(tj0, tj); tj1 = std::max(tj1, tj);
+            auto visit = [&](usize nidx) {
+                if (grown[nidx] && !seen[nidx]) { seen[nidx] = 1; stack.push_back(nidx); }
+            };
+            if (ti > 0) visit(tj * tiles + ti - 1);
+            if (ti + 1 < tiles) visit(tj * tiles + ti + 1);
+            if (tj > 0) visit((tj - 1) * tiles + ti);
+            if (tj + 1 < tiles) visit((tj + 1) * tiles + ti);
+        }
+        boxes.push_back({ti0 * SLEEP_TILE, std::min((ti1 + 1) * SLEEP_TILE, res) - 1,
+                         tj0 * SLEEP_TILE, std::min((tj1 + 1) * SLEEP_TILE, res) - 1});
+    }
+    return boxes;
+}
+
+// src/fluid_core.rs:1873-1877
+bool boxes_apart(const Box& a, const Box& b, usize gap) {
+    auto apart = [gap](usize a0, usize a1, usize b0, usize b1) { return a1 + gap < b0 || b1 + gap < a0; };
+    return apart(a.i0, a.i1, b.i0, b.i1) || apart(a.j0, a.j1, b.j0, b.j1);
+}
+
+// src/fluid_core.rs:1836-1868
+void pace3_slices(float* h, float* u, float* v, const u8* gate, usize res, float cell, float dts,
+                  uint32_t nsub, float eps, const Box& bx, Scratch& sc) {
+    for (uint32_t s = 0; s < nsub; ++s) {
+        transport_open_rows(false, h, u, gate, res, cell, dts, bx.i0, bx.i1, bx.j0, bx.j1, true, nullptr, 0.45f, sc);
+        transport_open_rows(false, h, v, gate, res, cell, dts, bx.i0, bx.i1, bx.j0, bx.j1, false, nullptr, 0.45f, sc);
+    }
+    if (eps > 0.0f)
+        for (usize j = bx.j0; j <= bx.j1; ++j)
+            for (usize i = bx.i0; i <= bx.i1; ++i) {
+                usize idx = j * res + i;
+                if (h[idx] < eps) h[idx] = u[idx] = v[idx] = 0.0f;
+            }
+}
+
+// src/fluid_core.rs:1659-1831 step_sheet_scratch (open sheet, gravity drive).
+void step_sheet_scratch(float* h, float* u, float* v, const float* bed, const float* nu,
+                        const u8* gate, usize res, float cell, float dt, float vorticity, float eps,
+                        bool banks, float sub_cap, int pace, Scratch& sc, Scratch* sc2,
+                        bool inner_par) {
+    bool open_fine = cell <= FINE_CELL_M + 1.0e-6f;
+    bool fine_open = open_fine && pace == 0;
+    bool whole_wet = open_fine && (pace == 2 || pace == 3);
+    bool awake = open_fine && !whole_wet && !fine_open;
+    std::vector<Box> boxes = (fine_open || awake) ? awake_work_boxes(h, u, v, bed, res, cell, eps)
+                                                  : sheet_work_boxes(h, res, eps, true);
+    if (boxes.empty()) return;
+    float cap = finite(sub_cap) ? rclamp(sub_cap, 1.0f, 8.0f) : 8.0f;
+    uint32_t nsub;
+    if (fine_open) {
+        nsub = 1;
+    } else {
+        float max_s = 0.15f;
+        float max_s2 = 0.0f;
+        for (const Box& b : boxes)
+            for (usize j = b.j0; j <= b.j1; ++j)
+                for (usize i = b.i0; i <= b.i1; ++i) {
+                    float uu = u[j * res + i], vv = v[j * res + i];
+                    float s2 = uu * uu + vv * vv;
+                    if (s2 > max_s2) max_s2 = s2;
+                }
+        max_s = rmax(max_s, sqrtf(max_s2));
+        float courant = 0.42f;
+        nsub = (uint32_t)rclamp(ceilf((dt * max_s) / (courant * rmax(cell, 1.0e-3f))), 1.0f, cap);
+    }
+    float dts = dt / (float)nsub;
+    if (pace == 3 && whole_wet && nsub > 1) {
+        auto run = [&](const Box& b, Scratch& s) {
+            substep(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, false, s, inner_par);
+            pace3_slices(h, u, v, gate, res, cell, dts, nsub, eps, b, s);
+        };
+        if (sc2 && boxes.size() == 2 && boxes_apart(boxes[0], boxes[1], BOX_PAR_GAP)) {
+            run(boxes[0], sc);
+            run(boxes[1], *sc2);
+            return;
+        }
+        for (const Box& b : boxes) run(b, sc);
+        return;
+    }
+    if (sc2 && boxes.size() == 2 && boxes_apart(boxes[0], boxes[1], BOX_PAR_GAP)) {
+        for (uint32_t s = 0; s < nsub; ++s) {
+            // The two boxes step on two workers with serial inner loops.
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[0].i0, boxes[0].i1, boxes[0].j0, boxes[0].j1, banks, true, sc, false);
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[1].i0, boxes[1].i1, boxes[1].j0, boxes[1].j1, banks, true, *sc2, false);
+        }
+        return;
+    }
+    for (uint32_t s = 0; s < nsub; ++s)
+        for (const Box& b : boxes)
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, true, sc, inner_par);
+}
+
+// src/fluid_core.rs:821-889 step_sheet_eps_in / step_sheet_eps
+void step_sheet_eps(float* h, float* u, float* v, const float* bed, const float* nu, const u8* gate,
+                    usize res, float cell, float dt, float vorticity, float eps, bool banks,
+                    float sub_cap, int pace, Scratch& sc, Scratch* sc2, bool inner_par) {
+    if (dt <= 0.0f || res == 0) return;
+    float sum = wet_sum(h, res * res, eps);
+    if (sum <= eps) return;
+    sc.fit(res * res);
+    if (sc2) sc2->fit(res * res);
+    step_sheet_scratch(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, banks, sub_cap, pace, sc, sc2, inner_par);
+}
+
+// src/fluid_core.rs:9594-9622 (no reach band)
+void soften_border(float* u, float* v, usize res) {
+    usize edge = std::max(res / 12, (usize)2);
+    usize ends = std::min(edge, res);
+    for (usize j = 0; j < res; ++j) {
+        bool row_band = std::min(j, res - 1 - j) < edge;
+        usize left = row_band ? res : ends, right = row_band ? res : res - ends;
+        auto visit = [&](usize i) {
+            usize di = std::min(i, res - 1 - i), dj = std::min(j, res - 1 - j);
+            usize d = std::min(di, dj);
+            if (d >= edge) return;
+            float t = (float)d / (float)edge;
+            float w = t * t * (3.0f - 2.0f * t);
+            usize idx = j * res + i;
+            u[idx] *= w;
+            v[idx] *= w;
+        };
+        for (usize i = 0; i < left; ++i) visit(i);
+        for (usize i = std::max(right, left); i < res; ++i) visit(i);
+    }
+}
+
+// --------------------------------------------------------------- window core
+struct TirePush {
+    float x, z, forward_x, forward_z, radius, width, speed, slip;
+};
+struct Spray {
+    float x, y, z, vx, vy, vz, volume;
+    int kind;
+};
+
+// src/fluid_core.rs:9877-9897
+std::pair<usize, usize> index_span(float origin, float cell, usize res, float center, float reach) {
+    if (!(cell > 0.0f) || res == 0) return {0, 0};
+    float lo = rmax(floorf((center - reach - origin) / cell - 1.0f), 0.0f);
+    float hi = rmax(ceilf((center + reach - origin) / cell + 2.0f), 0.0f);
+    usize l = std::min(f2usize(lo), res);
+    usize hh = std::max(std::min(f2usize(hi), res), l);
+    return {l, hh};
+}
+void snap_origin(float cx, float cz, float extent, float cell, float* out) {
+    float x = cx - extent * 0.5f, z = cz - extent * 0.5f;
+    out[0] = floorf(x / cell) * cell;
+    out[1] = floorf(z / cell) * cell;
+}
+std::pair<int, int> world_key(float x, float z, float cell) {
+    return {(int)floorf(x / cell), (int)floorf(z / cell)};
+}
+// src/fluid_core.rs:9641-9662
+float dist2_segment(float px, float pz, float ax, float az, float bx, float bz) {
+    float abx = bx - ax, abz = bz - az;
+    float ab2 = abx * abx + abz * abz;
+    float t = ab2 < 1.0e-8f ? 0.0f : rclamp(((px - ax) * abx + (pz - az) * abz) / ab2, 0.0f, 1.0f);
+    float dx = px - (ax + abx * t), dz = pz - (az + abz * t);
+    return dx * dx + dz * dz;
+}
+// src/fluid_core.rs:9624-9640
+bool near_tire_zone(const std::vector<TirePush>& pushes, float x, float z, float r2) {
+    for (const auto& p : pushes) {
+        float dx = x - p.x, dz = z - p.z;
+        if (dx * dx + dz * dz <= r2) return true;
+    }
+    for (usize i = 0; i < pushes.size(); ++i)
+        for (usize j = i + 1; j < pushes.size(); ++j) {
+            const TirePush &a = pushes[i], &b = pushes[j];
+            if (fabsf(a.x - b.x) >= 0.45f) continue;
+            if (dist2_segment(x, z, a.x, a.z, b.x, b.z) <= r2) return true;
+        }
+    return false;
+}
+
+// near.rs:43-80
+struct NearTile {
+    std::vector<float> w, s, uw, vw;
+    bool fresh = false;
+    float idle_s = 0.0f;
+    float peak = 0.0f;
+    explicit NearTile(usize n2) : w(n2, 0.0f), s(n2, 0.0f), uw(n2, 0.0f), vw(n2, 0.0f) {}
+    float left() const { return idle_s <= 0.0f ? 1.0f : expf(-idle_s / NEAR_RESIDUAL_LIFE_S); }
+};
+
+// near.rs:118-125
+void recentre(std::vector<float>& r) {
+    double sum = 0.0;
+    for (float x : r) sum += (double)x;
+    float mean = (float)(sum / (double)r.size());
+    for (float& x : r) x -= mean;
+}
+// near.rs:128-137
+float abs_peak(const std::vector<float>& r) {
+    float hi[4] = {0, 0, 0, 0};
+    for (usize c = 0; c + 4 <= r.size(); c += 4)
+        for (int l = 0; l < 4; ++l) {
+            float a = fabsf(r[c + l]);
+            hi[l] = a > hi[l] ? a : hi[l];
+        }
+    return rmax(rmax(rmax(hi[0], hi[1]), hi[2]), hi[3]);
+}
+// near.rs:139-148
+float floor_scale(float base, const std::vector<float>& r) {
+    float low = 0.0f;
+    for (float x : r) low = rmin(low, x);
+    if (low >= 0.0f || base + low >= 0.0f) return 1.0f;
+    if (base <= 0.0f) return 0.0f;
+    return rclamp(base / -low, 0.0f, 1.0f);
+}
+
+struct Patch {
+    float origin[2] = {0, 0};
+    std::vector<float> water, slurry, uw, vw, us, vs, bed, bed_slurry, moisture;
+    std::vector<u8> grain;
+    std::vector<uint16_t> col, row;
+    Scratch sc[2][2];  // [water, slurry][sc, sc2]
+};
+
+struct Core {
+    oracle_core_cfg cfg;
+    usize res, fres, sub;
+    float origin[2];
+    std::vector<float> water, slurry, uw, vw, us, vs, bed, moisture;
+    std::vector<u8> grain, fine_hold;
+    float moisture_ambient = 0.0f;
+    std::vector<Patch> patches;
+    std::vector<int> hold_owner;   // patch that holds each coarse column (per-tire layout)
+    bool fine_on = false;
+    bool near_on = true;
+    std::map<std::pair<int, int>, NearTile> near;
+    std::map<std::pair<int, int>, std::pair<float, float>> parked;  // water, slurry depth
+    float spray_m3 = 0.0f;
+    std::vector<TirePush> pushes;
+    float fine_sub_cap = 8.0f;
+    int fine_pace = 0;
+    Scratch coarse_sc[2][2];
+    std::vector<float> nu_w, nu_s;  // PairScratch rows (src/fluid_core.rs:621-647)
+    std::vector<float> fnu_w, fnu_s;
+    std::vector<u8> gate, fgate;
+    int inflow_j = -1;
+    float inflow_x0 = 0, inflow_x1 = 0, inflow_rate = 0;
+    double opened_m3 = 0.0;
+
+    explicit Core(const oracle_core_cfg& c) : cfg(c) {
+        res = (usize)c.res;
+        fres = (usize)c.fine_res;
+        sub = (usize)lroundf(c.cell / c.fine_cell);
+        usize n = res * res, fn = fres * fres;
+        water.assign(n, 0); slurry.assign(n, 0); uw.assign(n, 0); vw.assign(n, 0);
+        us.assign(n, 0); vs.assign(n, 0); bed.assign(n, 0); moisture.assign(n, 0);
+        grain.assign(n, 4);
+        fine_hold.assign(n, 0);
+        hold_owner.assign(n, -1);
+        snap_origin(c.center_x, c.center_z, (float)res * c.cell, c.cell, origin);
+        float nuw = dynamic_viscosity(3, 1.0f);
+        nu_w.assign(n, nuw); nu_s.assign(n, 0.0f); gate.assign(n, 1);
+        fnu_w.assign(fn, nuw); fnu_s.assign(fn, 0.0f); fgate.assign(fn, 1);
+    }
+    void coarse_xz(usize i, usize j, float& x, float& z) const {
+        x = origin[0] + ((float)i + 0.5f) * cfg.cell;
+        z = origin[1] + ((float)j + 0.5f) * cfg.cell;
+    }
+    long coarse_axis(float o, float p) const {  // src/fluid_core.rs:9546-9557
+        float i = floorf((p - o) / cfg.cell);
+        if (i < 0.0f) return -1;
+        usize ii = f2usize(i);
+        return ii >= res ? -1 : (long)ii;
+    }
+    bool coarse_ij(float x, float z, usize& i, usize& j) const {
+        long a = coarse_axis(origin[0], x), b = coarse_axis(origin[1], z);
+        if (a < 0 || b < 0) return false;
+        i = (usize)a; j = (usize)b;
+        return true;
+    }
+    void make_patch_axes(Patch& P) const {  // src/fluid_core.rs:9518-9535
+        P.col.assign(fres, 0xffff);
+        P.row.assign(fres, 0xffff);
+        for (usize i = 0; i < fres; ++i) {
+            float x = P.origin[0] + ((float)i + 0.5f) * cfg.fine_cell;
+            long ci = coarse_axis(origin[0], x);
+            if (ci >= 0) P.col[i] = (uint16_t)ci;
+        }
+        for (usize j = 0; j < fres; ++j) {
+            float z = P.origin[1] + ((float)j + 0.5f) * cfg.fine_cell;
+            long cj = coarse_axis(origin[1], z);
+            if (cj >= 0) P.row[j] = (uint16_t)cj;
+        }
+    }
+    void ensure_patches(usize k) {
+        usize fn = fres * fres;
+        while (patches.size() < k) {
+            Patch P;
+            P.water.assign(fn, 0); P.slurry.assign(fn, 0); P.uw.assign(fn, 0); P.vw.assign(fn, 0);
+            P.us.assign(fn, 0); P.vs.assign(fn, 0); P.bed.assign(fn, 0); P.bed_slurry.assign(fn, 0);
+            P.moisture.assign(fn, 0); P.grain.assign(fn, 4);
+            patches.push_back(std::move(P));
+        }
+    }
+    usize active_patches() const { return cfg.layout == 0 ? (fine_on ? 1 : 0) : (fine_on ? pushes_in_use : 0); }
+    usize pushes_in_use = 0;
+
+    // near.rs:152-185 near_columns, per patch
+    struct NearCol { usize cidx; std::pair<int, int> key; usize i0, j0; };
+    std::vector<NearCol> near_columns(const Patch& P, int pidx) const {
+        auto runs = [&](const std::vector<uint16_t>& axis) {
+            std::vector<std::pair<uint16_t, usize>> out;
+            usize i = 0;
+            while (i < fres) {
+                uint16_t c = axis[i];
+                usize n = 1;
+                while (i + n < fres && axis[i + n] == c) ++n;
+                if (c != 0xffff && n == sub) out.push_back({c, i});
+                i += n;
+            }
+            return out;
+        };
+        auto cols = runs(P.col), rows = runs(P.row);
+        std::vector<NearCol> out;
+        for (auto& r : rows)
+            for (auto& c : cols) {
+                usize cidx = (usize)r.first * res + c.first;
+                if (fine_hold[cidx] != 1 || hold_owner[cidx] != pidx) continue;
+                float x, z;
+                coarse_xz(c.first, r.first, x, z);
+                out.push_back({cidx, world_key(x, z, cfg.cell), c.second, r.second});
+            }
+        return out;
+    }
+    bool near_inner(usize cidx) const {  // near.rs:188-197
+        usize i = cidx % res, j = cidx / res;
+        if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return false;
+        usize nb[4] = {cidx - 1, cidx + 1, cidx - res, cidx + res};
+        for (usize q : nb)
+            if (fine_hold[q] != 1) return false;
+        return true;
+    }
+    // near.rs:199-273
+    void near_capture() {
+        if (!fine_on || !near_on) return;
+        usize n2 = sub * sub;
+        for (usize pk = 0; pk < active_patches(); ++pk) {
+            Patch& P = patches[pk];
+            for (const NearCol& nc : near_columns(P, cfg.layout == 0 ? -1 : (int)pk)) {
+                float sw = 0.0f, ss = 0.0f;
+                for (usize b = 0; b < sub; ++b) {
+                    usize f = (nc.j0 + b) * fres + nc.i0;
+                    sw += rsum(&P.water[f], sub);
+                    ss += rsum(&P.slurry[f], sub);
+                }
+                if (sw <= 0.0f && ss <= 0.0f) { near.erase(nc.key); continue; }
+                float nn = (float)n2;
+                float mw = sw / nn, ms = ss / nn;
+                std::vector<float> rw(n2), rs(n2);
+                for (usize b = 0; b < sub; ++b) {
+                    usize f = (nc.j0 + b) * fres + nc.i0;
+                    for (usize a = 0; a < sub; ++a) {
+                        rw[b * sub + a] = P.water[f + a] - mw;
+                        rs[b * sub + a] = P.slurry[f + a] - ms;
+                    }
+                }
+                float peak = rmax(abs_peak(rw), abs_peak(rs));
+                bool inner = near_inner(nc.cidx);
+                if (peak <= NEAR_DROP_M && !inner) { near.erase(nc.key); continue; }
+                recentre(rw);
+                recentre(rs);
+                auto it = near.find(nc.key);
+                if (it == near.end()) it = near.emplace(nc.key, NearTile(n2)).first;
+                NearTile& tile = it->second;
+                tile.w = rw;
+                tile.s = rs;
+                if (inner && sw > 1.0e-10f) {
+                    float mu = 0.0f, mv = 0.0f;
+                    for (usize b = 0; b < sub; ++b) {
+                        usize f = (nc.j0 + b) * fres + nc.i0;
+                        for (usize a = 0; a < sub; ++a) {
+                            float w = P.water[f + a];
+                            mu += w * P.uw[f + a];
+                            mv += w * P.vw[f + a];
+                        }
+                    }
+                    float uu = mu / sw, vv = mv / sw;
+                    for (usize b = 0; b < sub; ++b) {
+                        usize f = (nc.j0 + b) * fres + nc.i0;
+                        for (usize a = 0; a < sub; ++a) {
+                            bool wet = P.water[f + a] > NEAR_FILM_M;
+                            tile.uw[b * sub + a] = wet ? P.uw[f + a] - uu : 0.0f;
+                            tile.vw[b * sub + a] = wet ? P.vw[f + a] - vv : 0.0f;
+                        }
+                    }
+                } else {
+                    std::fill(tile.uw.begin(), tile.uw.end(), 0.0f);
+                    std::fill(tile.vw.begin(), tile.vw.end(), 0.0f);
+                }
+                tile.peak = peak;
+                tile.idle_s = 0.0f;
+                tile.fresh = true;
+            }
+        }
+    }
+    // near.rs:311-325
+    void near_fade(float dt) {
+        if (near.empty()) return;
+        dt = (dt > 0.0f && finite(dt)) ? dt : 0.0f;
+        for (auto it = near.begin(); it != near.end();) {
+            NearTile& t = it->second;
+            if (t.fresh) { t.fresh = false; ++it; continue; }
+            t.idle_s += dt;
+            if (t.peak * t.left() > NEAR_DROP_M) ++it;
+            else it = near.erase(it);
+        }
+    }
+    // near.rs:276-308
+    void near_apply(float dt) {
+        if (!near.empty()) {
+            for (usize pk = 0; pk < active_patches(); ++pk) {
+                Patch& P = patches[pk];
+                for (const NearCol& nc : near_columns(P, cfg.layout == 0 ? -1 : (int)pk)) {
+                    auto it = near.find(nc.key);
+                    if (it == near.end()) continue;
+                    const NearTile& tile = it->second;
+                    usize f0 = nc.j0 * fres + nc.i0;
+                    float bw = P.water[f0], bs = P.slurry[f0];
+                    bool inner = near_inner(nc.cidx);
+                    float left = tile.left();
+                    float aw = left * floor_scale(bw / rmax(left, 1.0e-6f), tile.w);
+                    float as_ = left * floor_scale(bs / rmax(left, 1.0e-6f), tile.s);
+                    for (usize b = 0; b < sub; ++b)
+                        for (usize a = 0; a < sub; ++a) {
+                            usize f = (nc.j0 + b) * fres + nc.i0 + a;
+                            usize k = b * sub + a;
+                            float w = rmax(bw + aw * tile.w[k], 0.0f);
+                            float s = rmax(bs + as_ * tile.s[k], 0.0f);
+                            P.water[f] = w;
+                            P.slurry[f] = s;
+                            if (inner && w > NEAR_FILM_M) {
+                                P.uw[f] += left * tile.uw[k];
+                                P.vw[f] += left * tile.vw[k];
+                            }
+                        }
+                }
+            }
+        }
+        near_fade(dt);
+    }
+
+    // src/fluid_core.rs:8462-8555 restrict_fine (all patches)
+    void restrict_fine() {
+        if (!fine_on) return;
+        near_capture();
+        float fine_area = cfg.fine_cell * cfg.fine_cell;
+        float coarse_area = cfg.cell * cfg.cell;
+        usize full = sub * sub;
+        std::map<usize, usize> touch_pos;
+        std::vector<usize> touch;
+        std::vector<float> aw, as, auw, avw, aus, avs;
+        std::vector<uint32_t> cnt;
+        auto mark = [&](usize cidx) {
+            auto it = touch_pos.find(cidx);
+            if (it == touch_pos.end()) {
+                touch_pos[cidx] = touch.size();
+                touch.push_back(cidx);
+                aw.push_back(0); as.push_back(0); auw.push_back(0); avw.push_back(0); aus.push_back(0); avs.push_back(0);
+                cnt.push_back(0);
+                return touch.size() - 1;
+            }
+            return it->second;
+        };
+        for (usize pk = 0; pk < active_patches(); ++pk) {
+            Patch& P = patches[pk];
+            for (usize j = 0; j < fres; ++j) {
+                uint16_t cj = P.row[j];
+                for (usize i = 0; i < fres; ++i) {
+                    uint16_t ci = P.col[i];
+                    usize fidx = j * fres + i;
+                    if (cj == 0xffff || ci == 0xffff) {
+                        float x = P.origin[0] + ((float)i + 0.5f) * cfg.fine_cell;
+                        float z = P.origin[1] + ((float)j + 0.5f) * cfg.fine_cell;
+                        auto& slot = parked[world_key(x, z, cfg.cell)];
+                        slot.first += P.water[fidx] * fine_area / coarse_area;
+                        slot.second += P.slurry[fidx] * fine_area / coarse_area;
+                        continue;
+                    }
+                    usize cidx = (usize)cj * res + ci;
+                    usize t = mark(cidx);
+                    cnt[t] += 1;
+                    float fw = P.water[fidx], fs = P.slurry[fidx];
+                    if (fw == 0.0f && fs == 0.0f) continue;
+                    aw[t] += P.water[fidx] * fine_area;
+                    as[t] += P.slurry[fidx] * fine_area;
+                    auw[t] += P.uw[fidx] * P.water[fidx] * fine_area;
+                    avw[t] += P.vw[fidx] * P.water[fidx] * fine_area;
+                    aus[t] += P.us[fidx] * P.slurry[fidx] * fine_area;
+                    avs[t] += P.vs[fidx] * P.slurry[fidx] * fine_area;
+                }
+            }
+        }
+        for (usize t = 0; t < touch.size(); ++t) {
+            usize idx = touch[t];
+            bool held = fine_hold[idx] == 1;
+            float w = aw[t] / coarse_area, s = as[t] / coarse_area;
+            if (!held && cnt[t] >= full) {
+                if (w <= 0.0f && s <= 0.0f) continue;
+                float old_w = water[idx], old_s = slurry[idx];
+                float new_w = old_w + w, new_s = old_s + s;
+                if (new_w > 1.0e-6f) {
+                    uw[idx] = (old_w * uw[idx] * coarse_area + auw[t]) / (new_w * coarse_area);
+                    vw[idx] = (old_w * vw[idx] * coarse_area + avw[t]) / (new_w * coarse_area);
+                }
+                if (new_s > 1.0e-6f) {
+                    us[idx] = (old_s * us[idx] * coarse_area + aus[t]) / (new_s * coarse_area);
+                    vs[idx] = (old_s * vs[idx] * coarse_area + avs[t]) / (new_s * coarse_area);
+                }
+                water[idx] = new_w;
+                slurry[idx] = new_s;
+                continue;
+            }
+            water[idx] = w;
+            slurry[idx] = s;
+            if (w > 1.0e-6f) {
+                uw[idx] = auw[t] / (w * coarse_area);
+                vw[idx] = avw[t] / (w * coarse_area);
+            }
+            if (s > 1.0e-6f) {
+                us[idx] = aus[t] / (s * coarse_area);
+                vs[idx] = avs[t] / (s * coarse_area);
+            }
+        }
+        for (usize pk = 0; pk < active_patches(); ++pk) {
+            std::fill(patches[pk].water.begin(), patches[pk].water.end(), 0.0f);
+            std::fill(patches[pk].slurry.begin(), patches[pk].slurry.end(), 0.0f);
+        }
+        fine_on = false;
+    }
+
+    // src/fluid_core.rs:8358-8460 refine. Layout 0 follows the reference (one
+    // patch at the mean tire); layout 1 lays one patch per tire and holds a
+    // column for the first patch that covers it and lies near its own tire.
+    void refine(const std::vector<TirePush>& ps, float dt) {
+        restrict_fine();
+        if (ps.empty()) { near_fade(dt); return; }
+        usize np = cfg.layout == 0 ? 1 : ps.size();
+        ensure_patches(np);
+        pushes_in_use = np;
+        float extent = (float)fres * cfg.fine_cell;
+        std::fill(fine_hold.begin(), fine_hold.end(), 0);
+        std::fill(hold_owner.begin(), hold_owner.end(), -1);
+        usize full = sub * sub;
+        float r2 = cfg.tire_r * cfg.tire_r;
+        for (usize pk = 0; pk < np; ++pk) {
+            Patch& P = patches[pk];
+            if (cfg.layout == 0) {
+                float cx = 0.0f, cz = 0.0f;
+                for (auto& p : ps) { cx += p.x; cz += p.z; }
+                float n = (float)ps.size();
+                cx /= n; cz /= n;
+                snap_origin(cx, cz, extent, cfg.cell, P.origin);
+            } else {
+                snap_origin(ps[pk].x, ps[pk].z, extent, cfg.cell, P.origin);
+            }
+            std::fill(P.water.begin(), P.water.end(), 0.0f);
+            std::fill(P.slurry.begin(), P.slurry.end(), 0.0f);
+            std::fill(P.uw.begin(), P.uw.end(), 0.0f);
+            std::fill(P.vw.begin(), P.vw.end(), 0.0f);
+            std::fill(P.us.begin(), P.us.end(), 0.0f);
+            std::fill(P.vs.begin(), P.vs.end(), 0.0f);
+            make_patch_axes(P);
+            std::vector<usize> touch;
+            std::map<usize, uint32_t> cnt;
+            std::vector<std::pair<usize, usize>> hits;
+            for (usize j = 0; j < fres; ++j) {
+                uint16_t cj = P.row[j];
+                if (cj == 0xffff) continue;
+                for (usize i = 0; i < fres; ++i) {
+                    uint16_t ci = P.col[i];
+                    if (ci == 0xffff) continue;
+                    usize cidx = (usize)cj * res + ci;
+                    if (cnt[cidx] == 0) touch.push_back(cidx);
+                    cnt[cidx] += 1;
+                    hits.push_back({j * fres + i, cidx});
+                }
+            }
+            std::vector<TirePush> own;
+            if (cfg.layout == 0) own = ps; else own.push_back(ps[pk]);
+            for (usize cidx : touch) {
+                if (cnt[cidx] != full) continue;
+                if (cfg.layout == 1 && fine_hold[cidx] == 1) continue;
+                float x, z;
+                coarse_xz(cidx % res, cidx / res, x, z);
+                if (near_tire_zone(own, x, z, r2)) {
+                    fine_hold[cidx] = 1;
+                    hold_owner[cidx] = cfg.layout == 0 ? -1 : (int)pk;
+                }
+            }
+            int me = cfg.layout == 0 ? -1 : (int)pk;
+            for (auto& hp : hits) {
+                usize fidx = hp.first, cidx = hp.second;
+                P.moisture[fidx] = moisture[cidx];
+                P.grain[fidx] = grain[cidx];
+                if (!(fine_hold[cidx] == 1 && hold_owner[cidx] == me)) {
+                    P.bed[fidx] = bed[cidx] + water[cidx];
+                    P.bed_slurry[fidx] = bed[cidx] + slurry[cidx];
+                    continue;
+                }
+                P.bed[fidx] = bed[cidx];
+                P.bed_slurry[fidx] = bed[cidx];
+                P.water[fidx] = water[cidx];
+                P.slurry[fidx] = slurry[cidx];
+                P.uw[fidx] = uw[cidx];
+                P.vw[fidx] = vw[cidx];
+                P.us[fidx] = us[cidx];
+                P.vs[fidx] = vs[cidx];
+            }
+            for (usize cidx : touch)
+                if (fine_hold[cidx] == 1 && hold_owner[cidx] == me)
+                    water[cidx] = slurry[cidx] = uw[cidx] = vw[cidx] = us[cidx] = vs[cidx] = 0.0f;
+        }
+        fine_on = true;
+        near_apply(dt);
+    }
+
+    bool fine_held_at(float x, float z) const {
+        usize i, j;
+        if (!coarse_ij(x, z, i, j)) return false;
+        return fine_hold[j * res + i] == 1;
+    }
+    // src/fluid_core.rs:8318-8356 cell_is_refined; returns the patch that holds it or -1.
+    int refined_patch(float x, float z) const {
+        if (!fine_on || !fine_held_at(x, z)) return -1;
+        usize i, j;
+        if (!coarse_ij(x, z, i, j)) return -1;
+        float x0 = origin[0] + (float)i * cfg.cell, z0 = origin[1] + (float)j * cfg.cell;
+        float x1 = x0 + cfg.cell, z1 = z0 + cfg.cell;
+        int pk = cfg.layout == 0 ? 0 : hold_owner[j * res + i];
+        if (pk < 0) return -1;
+        const Patch& P = patches[pk];
+        float extent = (float)fres * cfg.fine_cell;
+        float rect[4] = {P.origin[0], P.origin[0] + extent, P.origin[1], P.origin[1] + extent};
+        if (x0 >= rect[0] - 1.0e-4f && z0 >= rect[2] - 1.0e-4f && x1 <= rect[1] + 1.0e-4f && z1 <= rect[3] + 1.0e-4f)
+            return pk;
+        return -1;
+    }
+
+    // src/fluid_core.rs:8169-8239 push_on
+    void push_on(const TirePush& p, float* w, float* s, float* fuw, float* fvw, float* fus, float* fvs,
+                 usize r, float cell, const float* org) {
+        float fx = p.forward_x, fz = p.forward_z;
+        float len = rmax(sqrtf(fx * fx + fz * fz), 1.0e-4f);
+        fx = fx / len;
+        fz = fz / len;
+        float rx = fz, rz = -fx;
+        float speed = rmax(p.speed, 0.0f);
+        float reach = hypotf(p.radius * 1.4f, p.width * 0.65f + cell) + cell;
+        auto si = index_span(org[0], cell, r, p.x, reach);
+        auto sj = index_span(org[1], cell, r, p.z, reach);
+        for (usize j = sj.first; j < sj.second; ++j)
+            for (usize i = si.first; i < si.second; ++i) {
+                float x = org[0] + ((float)i + 0.5f) * cell;
+                float z = org[1] + ((float)j + 0.5f) * cell;
+                float dx = x - p.x, dz = z - p.z;
+                float along = dx * fx + dz * fz;
+                float lat = dx * rx + dz * rz;
+                if (fabsf(lat) > p.width * 0.65f + cell) continue;
+                if (along < -p.radius * 1.4f || along > p.radius * 1.1f) continue;
+                usize idx = j * r + i;
+                float flank = rclamp(fabsf(lat) / (p.width * 0.65f + cell), 0.0f, 1.0f);
+                float shove = rmax(speed, 0.4f) * (1.0f - flank * flank);
+                if (w[idx] > 0.004f) {
+                    fuw[idx] += fx * shove * 0.85f;
+                    fvw[idx] += fz * shove * 0.85f;
+                    fuw[idx] += rx * rsignum(lat) * shove * 0.18f * flank;
+                    fvw[idx] += rz * rsignum(lat) * shove * 0.18f * flank;
+                }
+                if (s[idx] > 0.004f) {
+                    float fore = along > 0.0f ? 1.0f : 0.72f;
+                    fus[idx] += fx * shove * fore;
+                    fvs[idx] += fz * shove * fore;
+                    fus[idx] += rx * rsignum(lat) * shove * 0.28f * flank;
+                    fvs[idx] += rz * rsignum(lat) * shove * 0.28f * flank;
+                }
+            }
+    }
+
+    // src/fluid_core.rs:8241-8314 peel_spray
+    void peel(const std::vector<TirePush>& ps, float* w, const float* fuw, const float* fvw, usize r,
+              float cell, const float* org, bool skip_held, std::vector<Spray>& out) {
+        float area = cell * cell;
+        for (const auto& p : ps) {
+            if (p.speed < 0.8f) continue;
+            float reach = p.radius * 1.3f + cell;
+            auto si = index_span(org[0], cell, r, p.x, reach);
+            auto sj = index_span(org[1], cell, r, p.z, reach);
+            for (usize j = sj.first; j < sj.second; ++j)
+                for (usize i = si.first; i < si.second; ++i) {
+                    float x = org[0] + ((float)i + 0.5f) * cell;
+                    float z = org[1] + ((float)j + 0.5f) * cell;
+                    if (skip_held) {
+                        float ci = floorf((x - origin[0]) / cfg.cell), cj = floorf((z - origin[1]) / cfg.cell);
+                        if (!(ci < 0.0f || cj < 0.0f)) {
+                            usize ii = f2usize(ci), jj = f2usize(cj);
+                            if (ii < res && jj < res && fine_hold[jj * res + ii] == 1) continue;
+                        }
+                    }
+                    float dx = x - p.x, dz = z - p.z;
+                    if (dx * dx + dz * dz > (p.radius * 1.3f) * (p.radius * 1.3f)) continue;
+                    usize idx = j * r + i;
+                    if (w[idx] < 0.01f) continue;
+                    float take = rmin(w[idx] * 0.04f, 0.004f);
+                    if (take * area < 1.0e-6f) continue;
+                    w[idx] -= take;
+                    out.push_back({x, 0.35f, z, fuw[idx] * 0.3f, 1.4f + p.speed * 0.25f, fvw[idx] * 0.3f, take * area, 0});
+                }
+        }
+    }
+
+    // src/fluid_core.rs:7942-8150 step_pair (open sheets, no bodies).
+    void step_pair(float dt, bool fine) {
+        if (fine && !fine_on) return;
+        float cap = fine ? fine_sub_cap : 8.0f;
+        int pace = fine ? fine_pace : 0;
+        if (!fine) {
+            usize n = res * res;
+            Box wb;
+            if (cfg.soften) soften_border(uw.data(), vw.data(), res);
+            step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0);
+            if (wet_bounds(slurry.data(), res, NU_FILL_MARGIN, wb))
+                for (usize j = wb.j0; j <= wb.j1; ++j)
+                    for (usize i = wb.i0; i <= wb.i1; ++i) {
+                        usize idx = j * res + i;
+                        nu_s[idx] = dynamic_viscosity(grain[idx], moisture[idx]);
+                    }
+            if (cfg.soften) soften_border(us.data(), vs.data(), res);
+            step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0);
+            (void)n;
+            return;
+        }
+        for (usize pk = 0; pk < active_patches(); ++pk) {
+            Patch& P = patches[pk];
+            Box wb;
+            step_sheet_eps(P.water.data(), P.uw.data(), P.vw.data(), P.bed.data(), fnu_w.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.08f, 1.0e-6f, false, cap, pace, P.sc[0][0], &P.sc[0][1], false);
+            if (wet_bounds(P.slurry.data(), fres, NU_FILL_MARGIN, wb))
+                for (usize j = wb.j0; j <= wb.j1; ++j)
+                    for (usize i = wb.i0; i <= wb.i1; ++i) {
+                        usize idx = j * fres + i;
+                        fnu_s[idx] = dynamic_viscosity(P.grain[idx], P.moisture[idx]);
+                    }
+            step_sheet_eps(P.slurry.data(), P.us.data(), P.vs.data(), P.bed_slurry.data(), fnu_s.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.05f, 1.0e-6f, false, cap, pace, P.sc[1][0], &P.sc[1][1], false);
+        }
+    }
+
+    // src/fluid_core.rs:6034-6128, sheet subset.
+    std::vector<Spray> step(float dt) {
+        std::vector<TirePush> ps;
+        ps.swap(pushes);
+        if (inflow_j >= 0 && dt > 0.0f) apply_inflow(dt);
+        refine(ps, dt);
+        // apply_pushes(fine): src/fluid_core.rs:8152-8158
+        for (const auto& p : ps) {
+            int pk = refined_patch(p.x, p.z);
+            if (pk < 0) continue;
+            Patch& P = patches[pk];
+            push_on(p, P.water.data(), P.slurry.data(), P.uw.data(), P.vw.data(), P.us.data(), P.vs.data(), fres, cfg.fine_cell, P.origin);
+        }
+        step_pair(dt, true);
+        std::vector<Spray> spray;
+        if (fine_on)
+            for (usize pk = 0; pk < active_patches(); ++pk) {
+                Patch& P = patches[pk];
+                peel(ps, P.water.data(), P.uw.data(), P.vw.data(), fres, cfg.fine_cell, P.origin, false, spray);
+            }
+        restrict_fine();
+        for (const auto& p : ps) {  // apply_pushes_outside :8160-8167
+            if (fine_held_at(p.x, p.z)) continue;
+            push_on(p, water.data(), slurry.data(), uw.data(), vw.data(), us.data(), vs.data(), res, cfg.cell, origin);
+        }
+        step_pair(dt, false);
+        if (!ps.empty()) peel(ps, water.data(), uw.data(), vw.data(), res, cfg.cell, origin, true, spray);
+        for (const auto& s : spray) spray_m3 += s.volume;
+        return spray;
+    }
+
+    // Inflow strip: one coarse row, water added as depth, booked as opened volume.
+    void apply_inflow(float dt) {
+        std::vector<usize> cells;
+        for (usize i = 0; i < res; ++i) {
+            float x, z;
+            coarse_xz(i, (usize)inflow_j, x, z);
+            if (x >= inflow_x0 && x < inflow_x1) cells.push_back((usize)inflow_j * res + i);
+        }
+        if (cells.empty()) return;
+        float add = inflow_rate * dt / ((float)cells.size() * cfg.cell * cfg.cell);
+        for (usize idx : cells) water[idx] += add;
+        opened_m3 += (double)add * (double)cfg.cell * (double)cfg.cell * (double)cells.size();
+    }
+};
+
+float column_sum(const std::vector<float>& h, float cell) {  // src/fluid_core.rs:4617-4620
+    float area = cell * cell;
+    float s = -0.0f;
+    for (float x : h) s += rmax(x, 0.0f);
+    return s * area;
+}
+
+}  // namespace
+
+// ============================================================== C interface
+extern "C" {
+
+void* oracle_scratch_new(void) { return new Scratch(); }
+void oracle_scratch_free(void* sc) { delete (Scratch*)sc; }
+
+void oracle_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
+                       int res, float cell, float dt, float vorticity, float eps, int banks, float sub_cap,
+                       int pace, int inner_par, void* sc) {
+    if (res <= 0) return;
+    step_sheet_eps(h, u, v, bed, nu, gate, (usize)res, cell, dt, vorticity, eps, banks != 0, sub_cap, pace,
+                   *(Scratch*)sc, nullptr, inner_par != 0);
+}
+
+void oracle_transport_open(float* h, const float* vel, const uint8_t* gate, int res, float cell, float dt,
+                           int i0, int i1, int j0, int j1, int along_x, const float* bed, float frac_cap,
+                           int serial, float* removed, float* added) {
+    Scratch sc;
+    sc.fit((usize)res * res);
+    if (serial)
+        transport_open_serial(h, vel, gate, res, cell, dt, i0, i1, j0, j1, along_x != 0, bed, frac_cap, sc);
+    else
+        transport_open_rows(bed != nullptr, h, vel, gate, res, cell, dt, i0, i1, j0, j1, along_x != 0, bed, frac_cap, sc);
+    memcpy(removed, sc.removed.data(), sizeof(float) * res * res);
+    memcpy(added, sc.added.data(), sizeof(float) * res * res);
+}
+
+static int put_boxes(const std::vector<Box>& b, int* out, int cap) {
+    int n = (int)b.size();
+    for (int k = 0; k < n && k < cap; ++k) {
+        out[4 * k] = (int)b[k].i0; out[4 * k + 1] = (int)b[k].i1;
+        out[4 * k + 2] = (int)b[k].j0; out[4 * k + 3] = (int)b[k].j1;
+    }
+    return n;
+}
+int oracle_sheet_work_boxes(const float* h, int res, float eps, int allow_split, int flood, int* out, int cap) {
+    return put_boxes(flood ? sheet_work_boxes_flood(h, res, eps, allow_split != 0) : sheet_work_boxes(h, res, eps, allow_split != 0), out, cap);
+}
+int oracle_awake_work_boxes(const float* h, const float* u, const float* v, const float* bed, int res, float cell,
+                            float eps, int* out, int cap) {
+    return put_boxes(awake_work_boxes(h, u, v, bed, res, cell, eps), out, cap);
+}
+float oracle_dynamic_viscosity(int grain, float moisture) { return dynamic_viscosity((u8)grain, moisture); }
+float oracle_sheet_mobility_for(float nu) { return sheet_mobility_for(nu); }
+float oracle_sheet_damp(float nu) { return sheet_damp(nu); }
+void oracle_soften_border(float* u, float* v, int res) { soften_border(u, v, (usize)res); }
+
+// src/fluid_core.rs:4673-4760 rut_heal + relief
+static float relief(const std::vector<float>& h, const std::vector<float>& bed, usize res, float cell) {
+    float c = (float)(res / 2);
+    float center = 0, cn = 0, ring = 0, rn = 0;
+    for (usize j = 0; j < res; ++j)
+        for (usize i = 0; i < res; ++i) {
+            float x = ((float)i + 0.5f - c) * cell, z = ((float)j + 0.5f - c) * cell;
+            float r = sqrtf(x * x + z * z);
+            float eta = bed[j * res + i] + h[j * res + i];
+            if (r < 0.12f) { center += eta; cn += 1.0f; }
+            else if (r >= 0.48f && r < 0.68f) { ring += eta; rn += 1.0f; }
+        }
+    if (cn < 1.0f || rn < 1.0f) return 0.0f;
+    return (ring / rn) - (center / cn);
+}
+void oracle_rut_heal(int grain, float moisture, float* out4) {
+    usize res = 48;
+    float cell = 0.06f;
+    usize n = res * res;
+    std::vector<float> h(n, 0), u(n, 0), v(n, 0), bed(n, 0);
+    float nu_v = dynamic_viscosity((u8)grain, moisture);
+    std::vector<float> nu(n, nu_v);
+    std::vector<u8> gate(n, 1);
+    float c = (float)(res / 2);
+    for (usize j = 0; j < res; ++j)
+        for (usize i = 0; i < res; ++i) {
+            float x = ((float)i + 0.5f - c) * cell, z = ((float)j + 0.5f - c) * cell;
+            float r = sqrtf(x * x + z * z);
+            usize idx = j * res + i;
+            float bowl = expf(-(r * r) / (2.0f * 0.42f * 0.42f));
+            bed[idx] = -0.07f * bowl;
+            h[idx] = 0.012f + 0.028f * (1.0f - bowl);
+        }
+    float relief0 = relief(h, bed, res, cell);
+    float level_s = 20.0f, relief_8s = relief0, t = 0.0f, dt = 0.05f;
+    Scratch sc;
+    while (t < 20.0f - 1.0e-4f) {
+        step_sheet_eps(h.data(), u.data(), v.data(), bed.data(), nu.data(), gate.data(), res, cell, dt, 0.0f, 1.0e-6f, false, 8.0f, 0, sc, nullptr, true);
+        t += dt;
+        float r = relief(h, bed, res, cell);
+        if (fabsf(t - 8.0f) <= dt * 0.51f) relief_8s = r;
+        if (level_s > 19.0f && r < relief0 * 0.28f) level_s = t;
+        if (t >= 8.0f && level_s < 19.0f) break;
+    }
+    out4[0] = level_s; out4[1] = relief0; out4[2] = relief_8s; out4[3] = relief_8s > relief0 * 0.38f ? 1.0f : 0.0f;
+}
+
+void* oracle_core_new(const oracle_core_cfg* cfg) { return new Core(*cfg); }
+void oracle_core_free(void* core) { delete (Core*)core; }
+
+// src/fluid_core.rs:5329-5356 map_water_bed (closure values passed per cell)
+float oracle_core_map_water_bed(void* cp, const float* bedv, const float* waterv) {
+    Core& C = *(Core*)cp;
+    C.restrict_fine();
+    float vol = 0.0f, area = C.cfg.cell * C.cfg.cell;
+    for (usize idx = 0; idx < C.res * C.res; ++idx) {
+        C.bed[idx] = finite(bedv[idx]) ? bedv[idx] : 0.0f;
+        float w = finite(waterv[idx]) ? rmax(waterv[idx], 0.0f) : 0.0f;
+        C.water[idx] = w;
+        if (w > 0.0f) {
+            C.moisture[idx] = rmax(C.moisture[idx], 0.8f);
+            if (C.grain[idx] == 4) C.grain[idx] = 1;
+        }
+        vol += w * area;
+    }
+    return vol;
+}
+void oracle_core_map_grain(void* cp, const uint8_t* g) {  // :5318-5327
+    Core& C = *(Core*)cp;
+    C.restrict_fine();
+    memcpy(C.grain.data(), g, C.res * C.res);
+}
+void oracle_core_map_water_velocity(void* cp, const float* u, const float* v) {  // :5358-5372
+    Core& C = *(Core*)cp;
+    C.restrict_fine();
+    for (usize idx = 0; idx < C.res * C.res; ++idx) {
+        if (C.water[idx] <= 1.0e-6f) continue;
+        C.uw[idx] = finite(u[idx]) ? u[idx] : 0.0f;
+        C.vw[idx] = finite(v[idx]) ? v[idx] : 0.0f;
+    }
+}
+// :5424-5435 pour_water / pour_slurry via paint :5820-5849
+float oracle_core_pour(void* cp, float x0, float x1, float z0, float z1, float depth, int water, int grain,
+                       float moisture) {
+    Core& C = *(Core*)cp;
+    depth = rmax(depth, 0.0f);
+    float vol = 0.0f, area = C.cfg.cell * C.cfg.cell;
+    for (usize j = 0; j < C.res; ++j)
+        for (usize i = 0; i < C.res; ++i) {
+            float x, z;
+            C.coarse_xz(i, j, x, z);
+            if (x < x0 || x >= x1 || z < z0 || z >= z1) continue;
+            usize idx = j * C.res + i;
+            if (water) C.water[idx] = depth;
+            else {
+                C.slurry[idx] = depth;
+                C.grain[idx] = (u8)grain;
+                C.moisture[idx] = rclamp(moisture, 0.0f, 1.0f);
+            }
+            vol += depth * area;
+        }
+    return vol;
+}
+// :5854-5877 lay_slurry_mask
+float oracle_core_lay_slurry_mask(void* cp, const float* depth, int grain, float moisture) {
+    Core& C = *(Core*)cp;
+    C.restrict_fine();
+    float vol = 0.0f, area = C.cfg.cell * C.cfg.cell;
+    for (usize idx = 0; idx < C.res * C.res; ++idx) {
+        float d = depth[idx];
+        if (!(finite(d) && d > 0.0f)) continue;
+        C.slurry[idx] += d;
+        C.grain[idx] = (u8)grain;
+        C.moisture[idx] = rmax(C.moisture[idx], rclamp(moisture, 0.0f, 1.0f));
+        vol += d * area;
+    }
+    return vol;
+}
+// :5928-5962 read_substrate_grid
+void oracle_core_read_substrate(void* cp, const float* bedv, const float* moist, const uint8_t* g) {
+    Core& C = *(Core*)cp;
+    C.restrict_fine();
+    uint32_t hist[101] = {0};
+    for (usize idx = 0; idx < C.res * C.res; ++idx) {
+        float m = rclamp(moist[idx], 0.0f, 1.0f);
+        C.bed[idx] = bedv[idx];
+        C.moisture[idx] = m;
+        float pct = m * 100.0f;
+        usize whole = f2usize(pct);
+        usize bucket = pct - (float)whole >= 0.5f ? whole + 1 : whole;
+        hist[std::min(bucket, (usize)100)] += 1;
+        if (C.slurry[idx] > 1.0e-5f) C.grain[idx] = g[idx];
+    }
+    usize best = 0;
+    uint32_t best_n = 0;
+    for (usize i = 0; i < 101; ++i)
+        if (hist[i] > best_n) { best = i; best_n = hist[i]; }
+    C.moisture_ambient = (float)best * 0.01f;
+}
+void oracle_core_push_tire(void* cp, const oracle_tire* t) {
+    ((Core*)cp)->pushes.push_back({t->x, t->z, t->forward_x, t->forward_z, t->radius, t->width, t->speed, t->slip});
+}
+int oracle_core_step(void* cp, float dt, oracle_spray* out, int cap) {
+    std::vector<Spray> s = ((Core*)cp)->step(dt);
+    for (int k = 0; k < (int)s.size() && k < cap; ++k)
+        out[k] = {s[k].x, s[k].y, s[k].z, s[k].vx, s[k].vy, s[k].vz, s[k].volume, s[k].kind};
+    return (int)s.size();
+}
+// :6821-6883, sheet books only (no dust, fog, reach, suspended)
+void oracle_core_ledger(void* cp, float* out5, double* out64) {
+    Core& C = *(Core*)cp;
+    float water = column_sum(C.water, C.cfg.cell), slurry = column_sum(C.slurry, C.cfg.cell);
+    if (C.fine_on)
+        for (usize pk = 0; pk < C.active_patches(); ++pk) {
+            water += column_sum(C.patches[pk].water, C.cfg.fine_cell);
+            slurry += column_sum(C.patches[pk].slurry, C.cfg.fine_cell);
+        }
+    float fw = 0.0f, fs = 0.0f, area = C.cfg.cell * C.cfg.cell;
+    for (auto& kv : C.parked) { fw += kv.second.first * area; fs += kv.second.second * area; }
+    out5[0] = water; out5[1] = slurry; out5[2] = fw; out5[3] = fs; out5[4] = C.spray_m3;
+    double w64 = 0.0, s64 = 0.0;
+    for (float x : C.water) w64 += (double)rmax(x, 0.0f);
+    for (float x : C.slurry) s64 += (double)rmax(x, 0.0f);
+    out64[0] = w64 * (double)C.cfg.cell * (double)C.cfg.cell;
+    out64[1] = s64 * (double)C.cfg.cell * (double)C.cfg.cell;
+}
+static std::vector<float>* core_field(Core& C, int which) {
+    switch (which) {
+        case 0: return &C.water; case 1: return &C.slurry; case 2: return &C.uw; case 3: return &C.vw;
+        case 4: return &C.us; case 5: return &C.vs; case 6: return &C.bed; default: return &C.moisture;
+    }
+}
+void oracle_core_get(void* cp, int which, float* dst) {
+    Core& C = *(Core*)cp;
+    std::vector<float>* f = core_field(C, which);
+    memcpy(dst, f->data(), f->size() * sizeof(float));
+}
+void oracle_core_set(void* cp, int which, const float* src) {
+    Core& C = *(Core*)cp;
+    std::vector<float>* f = core_field(C, which);
+    memcpy(f->data(), src, f->size() * sizeof(float));
+}
+void oracle_core_get_grain(void* cp, uint8_t* dst) { Core& C = *(Core*)cp; memcpy(dst, C.grain.data(), C.grain.size()); }
+// src/render_contract.rs:457-496 film/flow via coarse_cell (:6998-7035). Tracers are
+// not part of the sheet path, so turbidity is 0.
+void oracle_core_publish(void* cp, float* film, float* flow) {
+    Core& C = *(Core*)cp;
+    for (usize idx = 0; idx < C.res * C.res; ++idx) {
+        float water_m = finite0(C.water[idx]), slurry_m = finite0(C.slurry[idx]);
+        float fl = water_m + slurry_m;
+        float u = 0.0f, v = 0.0f;
+        if (!(fl < 1.0e-5f)) {
+            u = finite0((C.uw[idx] * water_m + C.us[idx] * slurry_m) / fl);
+            v = finite0((C.vw[idx] * water_m + C.vs[idx] * slurry_m) / fl);
+        }
+        bool dry = !finite(water_m) || !finite(slurry_m) || water_m + slurry_m < 1.0e-5f;
+        if (dry) { u = 0.0f; v = 0.0f; } else { u = finite0(u); v = finite0(v); }
+        float speed = dry ? 0.0f : finite0(sqrtf(u * u + v * v));
+        film[2 * idx] = finite0(water_m);
+        film[2 * idx + 1] = finite0(slurry_m);
+        flow[4 * idx] = u; flow[4 * idx + 1] = v; flow[4 * idx + 2] = speed; flow[4 * idx + 3] = 0.0f;
+    }
+}
+void oracle_core_set_fine_pace(void* cp, int pace) { ((Core*)cp)->fine_pace = std::min(pace, 3); }
+void oracle_core_set_fine_sub_cap(void* cp, float cap) { ((Core*)cp)->fine_sub_cap = finite(cap) ? rclamp(cap, 1.0f, 8.0f) : 8.0f; }
+void oracle_core_set_near_field(void* cp, int on) {
+    Core& C = *(Core*)cp;
+    C.near_on = on != 0;
+    if (!on) C.near.clear();
+}
+int oracle_core_near_tiles(void* cp) { return (int)((Core*)cp)->near.size(); }
+float oracle_core_spray_m3(void* cp) { return ((Core*)cp)->spray_m3; }
+uint32_t oracle_core_non_finite(void* cp) {
+    Core& C = *(Core*)cp;
+    uint32_t n = 0;
+    for (auto* f : {&C.water, &C.slurry, &C.uw, &C.vw, &C.us, &C.vs, &C.bed, &C.moisture})
+        for (float x : *f) n += !finite(x);
+    return n;
+}
+// :6806-6815 sample (coarse only between steps; the patch is packed)
+void oracle_core_sample(void* cp, float x, float z, float* out7) {
+    Core& C = *(Core*)cp;
+    usize i, j;
+    for (int k = 0; k < 7; ++k) out7[k] = 0.0f;
+    if (!C.coarse_ij(x, z, i, j)) return;
+    usize idx = j * C.res + i;
+    out7[0] = C.water[idx]; out7[1] = C.slurry[idx]; out7[2] = C.us[idx]; out7[3] = C.vs[idx];
+    out7[4] = 0.0f; out7[5] = C.moisture[idx]; out7[6] = C.bed[idx];
+}
+void oracle_core_fine_water_debug(void* cp, const oracle_tire* tires, int n, int patch, float* dst, float* origin2) {
+    Core& C = *(Core*)cp;
+    std::vector<TirePush> ps;
+    for (int k = 0; k < n; ++k)
+        ps.push_back({tires[k].x, tires[k].z, tires[k].forward_x, tires[k].forward_z, tires[k].radius, tires[k].width, tires[k].speed, tires[k].slip});
+    C.refine(ps, 0.0f);
+    if (patch < (int)C.active_patches()) {
+        memcpy(dst, C.patches[patch].water.data(), C.fres * C.fres * sizeof(float));
+        origin2[0] = C.patches[patch].origin[0];
+        origin2[1] = C.patches[patch].origin[1];
+    }
+    C.restrict_fine();
+}
+void oracle_core_inflow(void* cp, int j, float x0, float x1, float rate) {
+    Core& C = *(Core*)cp;
+    C.inflow_j = j; C.inflow_x0 = x0; C.inflow_x1 = x1; C.inflow_rate = rate;
+}
+}
