@@ -1,0 +1,311 @@
+"""Benchmark of the B200 two-layer sheet step.
+
+Workload (one "step" = one FluidCore-style step of the whole grid): a
+2048 x 2048 grid of 0.2 m cells, seeded 4-octave value-noise bed, eight
+seeded puddles 0.05-0.2 m deep and 2-8 m across, a clay slurry rut pair, an
+inflow strip of 0.5 m^3/s on row 0, and four tires (1.5 m x 2.4 m rectangle,
+5 m/s along +z) each with its own 64 x 64 patch of 2 cm cells, dt = 1/120 s.
+Synthetic inputs stand in for scenes: the reference publishes no dataset.
+
+Prints one JSON line. `value` is cell-steps/s with the state resident in HBM
+(a cell-step = one coarse cell, both layers, one substep; nested 2 cm cells
+are counted the same way); `e2e` is the same metric through the public API
+with the per-step tire pushes from pinned host memory and the step's spray
+events and FP64 ledger read back each step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dirty-gen_b200"))
+
+RES = 2048
+CELL = 0.2
+DT = 1.0 / 120.0
+FINE_RES = 64
+INFLOW = (0, -2.0, 2.0, 0.5)
+FORCE_BYTES_PER_CELL = 49  # k_force: h,u,v x2 + bed + grain + moisture read (33 B), u,v x2 written (16 B)
+STEP_BYTES_PER_CELL = 57   # the fused step's algorithmic bytes (both layers)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--res", type=int, default=RES)
+    ap.add_argument("--no-tires", action="store_true")
+    ap.add_argument("--no-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    return {"workload": f"grid{args.res}_8puddles_inflow_4tires64", "res": args.res, "cell_m": CELL,
+            "dt_s": DT, "fine_patches": 0 if args.no_tires else 4, "fine_res": FINE_RES,
+            "layout": "per_tire64", "l2": "inputs larger than L2 (state ~%d MB)" % (args.res * args.res * 56 // 2**20)}
+
+
+def make_scene(args):
+    import silt_scenes
+
+    return silt_scenes.grid(res=args.res, cell=CELL)
+
+
+def tires_for(step, args):
+    import silt_scenes
+
+    if args.no_tires:
+        return []
+    return silt_scenes.tires_at(step * DT, speed=5.0)
+
+
+def seed(core, scene):
+    import silt_scenes
+
+    silt_scenes.seed_core(core, scene)
+    core.set_inflow(*INFLOW)
+
+
+def sample_clocks(stop, out, gpu_index):
+    q = ("--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", q, "--format=csv,noheader,nounits", "-lms", "100", "-i", str(gpu_index)],
+                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return
+    try:
+        while not stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            out.append(line.strip())
+    finally:
+        p.terminate()
+        try:
+            p.wait(timeout=2)
+        except subprocess.TimeoutExpired:
+            p.kill()
+
+
+def summarise_clocks(lines):
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = max(mx, float(f[2]))
+        except ValueError:
+            continue
+        for k, name in enumerate(names):
+            if f[5 + k].lower().startswith("active"):
+                reasons.add(name)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per k_force launch from the committed ncu summary, scaled to this grid."""
+    path = os.path.join(ROOT, "profiles", "k_force_grid_traffic.txt")
+    try:
+        vals = {}
+        for ln in open(path):
+            if ":" in ln:
+                k, v = ln.split(":", 1)
+                vals[k.strip()] = v.strip()
+        per_cell = float(vals["dram_bytes_per_cell"])
+        return per_cell
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_baseline(args, scene, steps=40):
+    """The CPU oracle (restated reference) on this host: same workload, a bounded sample of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    core = oracle.Core(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1)
+    seed(core, scene)
+    core.step(DT)  # warm
+    t0 = time.perf_counter()
+    for k in range(steps):
+        for t in tires_for(k + 1, args):
+            core.push_tire(**t)
+        core.step(DT)
+    el = time.perf_counter() - t0
+    fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
+    value = (args.res * args.res + fine_cells) * steps / el
+    return {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} steps of the same {args.res}^2 workload after 1 warm-up step, single thread "
+                      f"({el:.2f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene = make_scene(args)
+    base = cpu_baseline(args, scene, steps=max(1, min(args.steps, 3)))
+    line = {"metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": max(1, min(args.steps, 3)), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": workload(args), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
+    line["ms_per_step"] = 1000.0 * (args.res * args.res + fine_cells) / base["value"]
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    import silt_b200
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    scene = make_scene(args)
+    fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
+    cells_per_step = args.res * args.res + fine_cells
+    sheet = silt_b200.Sheet(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02,
+                            layout=silt_b200.FINE_PER_TIRE, device=local, stream=stream.cuda_stream)
+    seed(sheet, scene)
+    step_no = 0
+
+    def one_step(want_spray):
+        nonlocal step_no
+        step_no += 1
+        for t in tires_for(step_no, args):
+            sheet.push_tire(**t)
+        return sheet.step(DT, want_spray=want_spray)
+
+    for _ in range(args.warmup):
+        one_step(False)
+    sheet.sync()
+    torch.cuda.synchronize()
+    # Device-resident timed region.
+    stop = threading.Event()
+    clock_lines = []
+    th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, local), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    sheet.set_step_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one_step(False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    parts = sheet.step_parts()
+    sheet.set_step_timing(False)
+    stop.set()
+    th.join(timeout=5)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells_per_step * args.steps / (ms / 1000.0)
+    # End-to-end through the public API: pushes in, spray events and the FP64 ledger out, every step.
+    e2e_steps = max(10, args.steps // 4)
+    pinned = torch.zeros(4 * 8, dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    nev = 0
+    for _ in range(e2e_steps):
+        tires = tires_for(step_no + 1, args)
+        if tires:
+            pinned.copy_(torch.tensor([[t[k] for k in ("x", "z", "forward_x", "forward_z", "radius", "width",
+                                                        "speed", "slip")] for t in tires], dtype=torch.float32).ravel())
+        ev = one_step(True)
+        nev += len(ev)
+        sheet.ledger()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e_value = world * cells_per_step * e2e_steps / (ems / 1000.0)
+    led = sheet.ledger()
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        force_ms = parts["force_ms"] / max(parts["force_launches"], 1)
+        force_bytes = FORCE_BYTES_PER_CELL * args.res * args.res
+        achieved = force_bytes / (force_ms / 1000.0) / 1e9 if force_ms > 0 else None
+        per_cell = profiled_traffic()
+        roof = {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                "traffic": per_cell * args.res * args.res if per_cell else None,
+                "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms,
+                "transport_avg_launch_ms": parts["transport_ms"] / max(parts["force_launches"], 1),
+                "step_algorithmic_gbs": STEP_BYTES_PER_CELL * args.res * args.res * args.steps / (ms / 1000.0) / 1e9}
+        line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": workload(args), "roofline": roof,
+                "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(tires_for(1, args)) * 32,
+                        "d2h_bytes_per_step": 56 + 4 + 32 * (nev // max(e2e_steps, 1)), "steps": e2e_steps},
+                "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
+                "window_steps_per_s": world * args.steps / (ms / 1000.0),
+                "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
+                           "spray_m3": led["spray_m3"]}}
+        if not args.no_baseline:
+            line["cpu_baseline"] = cpu_baseline(args, scene)
+        print(json.dumps(line), flush=True)
+    sheet.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,74 @@
+// Nested 2 cm patches and their two-way coupling with the coarse window
+// (x3-team/Dirty-gen src/fluid_core.rs:8152-8566, src/fluid_core/near.rs).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/silt_sheet.h"
+
+namespace silt {
+namespace fine {
+
+// The coarse window as the patch module sees it (current buffers).
+struct SheetView {
+    cudaStream_t st;
+    int res;
+    size_t n;
+    float cell;
+    float origin[2];
+    float* h[2];
+    float* u[2];
+    float* v[2];
+    float* bed;
+    float* moisture;
+    uint8_t* grain;
+    double* d_acc;
+};
+
+struct StepOut {
+    int spray_events = 0;   // events queued on the device this step
+};
+
+struct PatchState;  // device planes of one patch (sheet_fine.cu)
+
+struct Patches {
+    int layout = SILT_FINE_MEAN_PATCH;
+    int fres = 160;
+    float fcell = 0.02f;
+    int sub = 10;
+    float tire_r = 0.56f;
+    float sub_cap = 8.0f;
+    int pace = 0;
+    bool near_on = true;
+    bool fine_on = false;
+    int active = 0;
+    std::vector<PatchState*> patches;
+    void* impl = nullptr;   // device tables owned by sheet_fine.cu
+};
+
+SheetView view_of(silt_sheet* s);
+int flush(silt_sheet* s);
+void note_speed(silt_sheet* s, float bound);
+void invalidate_ledger(silt_sheet* s);
+
+int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st);
+void destroy(Patches& P);
+// restrict_fine (src/fluid_core.rs:8462) when a patch is laid down.
+int restrict_all(Patches& P, silt_sheet* s);
+// refine, shove, fine pair, fine spray, restrict, shove outside (src/fluid_core.rs:6058-6066).
+int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, float dt, StepOut& out);
+// peel_spray on the coarse window, held columns skipped (src/fluid_core.rs:6071).
+int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, StepOut& out);
+int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out,
+                  double* spray_m3);
+int ledger_parts(Patches& P, silt_sheet* s, double* fine_w, double* fine_s, double* park_w, double* park_s);
+int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, int patch, float* host,
+                float* origin2);
+int near_tiles(Patches& P, silt_sheet* s, int* out);
+int set_near_field(Patches& P, silt_sheet* s, bool on);
+
+}  // namespace fine
+}  // namespace silt

@@ -1,0 +1,459 @@
+// Full-grid sheet substep for the coarse window and large grids.
+//
+// One substep of the reference (`substep`, x3-team/Dirty-gen
+// src/fluid_core.rs:1879-2082) is split in two fused, tiled kernels:
+//
+//   k_force      eta = bed + h, the two 5-tap pressure blurs, gravity,
+//                snapshot-Jacobi vorticity confinement, the divergence
+//                "overload" projection (its own two blurs), damping and the
+//                speed clamp. Reads h, bed, u, v (and grain/moisture for the
+//                slurry), writes the new u, v. All intermediates live in
+//                shared memory; the tile carries a 9-cell halo.
+//   k_transport  donor-cell transport of depth, x pass then z pass, the dry
+//                cut, and the FP64 ledger partial sum. Reads h, u, v, writes h.
+//
+// Both layers (water, slurry) go in one launch (blockIdx.z). Every stencil
+// clamps its index at the grid edge exactly as the reference's edge branches
+// do, so interior and border cells follow one formula.
+//
+// Work-box semantics: the reference steps only cells inside its work boxes
+// (wet bounding box + 3, or split bodies + 6). A wet cell is always at least 3
+// cells inside its box when a step has one substep, so every value a wet cell
+// reads is a value the full-grid pass computes the same way; dry cells carry
+// no flux and no force. The full-grid pass therefore gives the reference's
+// depths and velocities on every cell that holds fluid.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sheet_grid.cuh"
+#include "sheet_math.cuh"
+
+namespace silt {
+
+constexpr int FT = 32;       // force tile edge
+constexpr int FH = 9;        // force halo: p (2) + gravity (1) + vorticity (2) + projection (4)
+constexpr int FW = FT + 2 * FH;
+constexpr int FPLANE = FW * FW;
+constexpr int FORCE_THREADS = 256;
+
+constexpr int TT = 32;       // transport tile edge
+constexpr int TW = TT + 3;   // cells [t0-2, t1+1)
+constexpr int TRANSPORT_THREADS = 256;
+
+size_t force_smem_bytes() { return sizeof(float) * FPLANE * 8; }
+size_t transport_smem_bytes() { return sizeof(float) * TW * TW * 8; }
+
+// Five taps left to right. Away from the edge the reference starts from the
+// first product (accum5); near it from 0.0 (accum5_clamped,
+// src/fluid_core.rs:3680-3697).
+__device__ __forceinline__ float tap5(float a0, float a1, float a2, float a3, float a4, float k0, float k1, float k2,
+                                      bool interior) {
+    float a = interior ? a0 * k0 : 0.0f + a0 * k0;
+    a += a1 * k1;
+    a += a2 * k2;
+    a += a3 * k1;
+    a += a4 * k0;
+    return a;
+}
+
+__device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Cell material: viscosity, mobility and damping factor.
+__device__ __forceinline__ float cell_nu(const LayerParams& P, size_t g) {
+    if (P.nu_mode == NU_CONST) return P.nu_c;
+    if (P.nu_mode == NU_PLANE) return P.nu_plane[g];
+    return dynamic_viscosity(P.grain[g], P.moisture[g]);
+}
+
+__global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
+    const LayerParams& P = L.lay[blockIdx.z];
+    const int res = P.res;
+    const int tx0 = blockIdx.x * FT, ty0 = blockIdx.y * FT;
+    if (tx0 >= res || ty0 >= res || P.skip) return;
+    extern __shared__ float sm[];
+    float* E = sm;               // eta, radius 9
+    float* TG = sm + FPLANE;     // x-pass scratch
+    float* TS = sm + 2 * FPLANE;
+    float* PB = sm + 3 * FPLANE; // pressure p (radius 7), then projection b (radius 3)
+    float* U = sm + 4 * FPLANE;  // u, v: loaded (radius 6), gravity, confinement in place
+    float* V = sm + 5 * FPLANE;
+    float* HS = sm + 6 * FPLANE; // depth
+    float* WQ = sm + 7 * FPLANE; // vorticity (radius 5), then q (radius 1)
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    const float cell = P.cell, dt = P.dt, eps = P.eps;
+    const float two = 2.0f * cell;
+#define SIDX(gx, gy) (((gy) - oy) * FW + ((gx) - ox))
+#define REGION(rx, ry)                                                              \
+    const int x0 = max(0, tx0 - (rx)), x1 = min(res, tx0 + FT + (rx));            \
+    const int y0 = max(0, ty0 - (ry)), y1 = min(res, ty0 + FT + (ry));            \
+    const int nx = x1 - x0, ncell = nx * (y1 - y0);                                \
+    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {                        \
+        const int gy = y0 + k / nx, gx = x0 + k % nx;                              \
+        const size_t g = (size_t)gy * res + gx;                                    \
+        (void)g;
+#define END_REGION }
+
+    // 1. eta and depth on radius 9.
+    { REGION(FH, FH)
+        float hv = P.h[g];
+        HS[SIDX(gx, gy)] = hv;
+        E[SIDX(gx, gy)] = P.bed[g] + hv;
+    END_REGION }
+    __syncthreads();
+    // 2. Velocity on radius 6: the lazy dry cut of the previous substep, then
+    //    the soft window border (src/fluid_core.rs:9594-9622).
+    { REGION(6, 6)
+        float uu = P.u[g], vv = P.v[g];
+        if (P.apply_cut && HS[SIDX(gx, gy)] < eps) { uu = 0.0f; vv = 0.0f; }
+        if (P.soften_edge > 0) {
+            int di = min(gx, res - 1 - gx), dj = min(gy, res - 1 - gy);
+            int d = min(di, dj);
+            if (d < P.soften_edge) {
+                float t = (float)d / (float)P.soften_edge;
+                float w = t * t * (3.0f - 2.0f * t);
+                uu *= w;
+                vv *= w;
+            }
+        }
+        U[SIDX(gx, gy)] = uu;
+        V[SIDX(gx, gy)] = vv;
+    END_REGION }
+    //    x pass of both pressure blurs: rows radius 9, columns radius 7.
+    { REGION(7, FH)
+        const bool in = gx >= 2 && gx <= res - 3;
+        const int s = SIDX(gx, gy);
+        float e0 = E[SIDX(clampi(gx - 2, 0, res - 1), gy)], e1 = E[SIDX(clampi(gx - 1, 0, res - 1), gy)];
+        float e2 = E[s];
+        float e3 = E[SIDX(clampi(gx + 1, 0, res - 1), gy)], e4 = E[SIDX(clampi(gx + 2, 0, res - 1), gy)];
+        TG[s] = tap5(e0, e1, e2, e3, e4, kG0, kG1, kG2, in);
+        TS[s] = tap5(e0, e1, e2, e3, e4, kS0, kS1, kS2, in);
+    END_REGION }
+    __syncthreads();
+    // 3. z pass and the pressure: p = 0.45 (0.62 G + 0.38 S) + 0.55 eta, radius 7.
+    { REGION(7, 7)
+        const bool in = gy >= 2 && gy <= res - 3;
+        const int s = SIDX(gx, gy);
+        const int s0 = SIDX(gx, clampi(gy - 2, 0, res - 1)), s1 = SIDX(gx, clampi(gy - 1, 0, res - 1));
+        const int s3 = SIDX(gx, clampi(gy + 1, 0, res - 1)), s4 = SIDX(gx, clampi(gy + 2, 0, res - 1));
+        float gb = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
+        float sc = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
+        float filtered = 0.62f * gb + 0.38f * sc;
+        PB[s] = 0.45f * filtered + 0.55f * E[s];
+    END_REGION }
+    __syncthreads();
+    // 4. Gravity down the pressure gradient on wet cells, radius 6
+    //    (src/fluid_core.rs:2234-2253).
+    { REGION(6, 6)
+        const int s = SIDX(gx, gy);
+        if (HS[s] > eps) {
+            float px = (PB[SIDX(min(gx + 1, res - 1), gy)] - PB[SIDX(max(gx - 1, 0), gy)]) / two;
+            float pz = (PB[SIDX(gx, min(gy + 1, res - 1))] - PB[SIDX(gx, max(gy - 1, 0))]) / two;
+            float mob = P.nu_mode == NU_CONST ? P.mob_c : sheet_mobility_for(cell_nu(P, g));
+            U[s] += -kGravity * px * mob * dt;
+            V[s] += -kGravity * pz * mob * dt;
+        }
+    END_REGION }
+    __syncthreads();
+    // 5. Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
+    if (P.vort > 0.0f) {
+        REGION(5, 5)
+            float dvdx = (V[SIDX(min(gx + 1, res - 1), gy)] - V[SIDX(max(gx - 1, 0), gy)]) / two;
+            float dudz = (U[SIDX(gx, min(gy + 1, res - 1))] - U[SIDX(gx, max(gy - 1, 0))]) / two;
+            WQ[SIDX(gx, gy)] = dvdx - dudz;
+        END_REGION
+        __syncthreads();
+        // 6. Confinement kick from that snapshot, in place, radius 4
+        //    (src/fluid_core.rs:2348-2375, :2441-2470).
+        {
+            REGION(4, 4)
+            const int s = SIDX(gx, gy);
+            if (HS[s] > eps) {
+                float w = WQ[s];
+                if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
+                    float wxp = fabsf(WQ[SIDX(min(gx + 1, res - 1), gy)]);
+                    float wxm = fabsf(WQ[SIDX(max(gx - 1, 0), gy)]);
+                    float wzp = fabsf(WQ[SIDX(gx, min(gy + 1, res - 1))]);
+                    float wzm = fabsf(WQ[SIDX(gx, max(gy - 1, 0))]);
+                    float nx_ = (wxp - wxm) / two;
+                    float nz_ = (wzp - wzm) / two;
+                    float du = P.vort * dt * (-nz_ * w);
+                    float dv = P.vort * dt * (nx_ * w);
+                    if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
+                        U[s] += du;
+                        V[s] += dv;
+                    }
+                }
+            }
+            END_REGION
+        }
+        __syncthreads();
+    }
+    if (P.project) {
+        // 7. b = div * overload - 0.015 * overload * lap(eta), radius 3
+        //    (src/fluid_core.rs:1992-2003).
+        { REGION(3, 3)
+            const int s = SIDX(gx, gy);
+            const int sxp = SIDX(min(gx + 1, res - 1), gy), sxm = SIDX(max(gx - 1, 0), gy);
+            const int szp = SIDX(gx, min(gy + 1, res - 1)), szm = SIDX(gx, max(gy - 1, 0));
+            float ux = (U[sxp] - U[sxm]) / (2.0f * cell);
+            float vz = (V[szp] - V[szm]) / (2.0f * cell);
+            float div = ux + vz;
+            float lsum = E[sxp] + E[sxm] + E[szp] + E[szm] - 4.0f * E[s];
+            float lap_h = lsum / (cell * cell);
+            float overload = 1.0f + rclamp(cell_nu(P, g) / 231.0f, 0.0f, 6.0f);
+            PB[s] = div * overload - 0.015f * overload * lap_h;
+        END_REGION }
+        __syncthreads();
+        // 8. x pass of both blurs of b: rows radius 3, columns radius 1.
+        { REGION(1, 3)
+            const bool in = gx >= 2 && gx <= res - 3;
+            const int s = SIDX(gx, gy);
+            float b0 = PB[SIDX(clampi(gx - 2, 0, res - 1), gy)], b1 = PB[SIDX(clampi(gx - 1, 0, res - 1), gy)];
+            float b2 = PB[s];
+            float b3 = PB[SIDX(clampi(gx + 1, 0, res - 1), gy)], b4 = PB[SIDX(clampi(gx + 2, 0, res - 1), gy)];
+            TG[s] = tap5(b0, b1, b2, b3, b4, kG0, kG1, kG2, in);
+            TS[s] = tap5(b0, b1, b2, b3, b4, kS0, kS1, kS2, in);
+        END_REGION }
+        __syncthreads();
+        // 9. q = 0.62 G(b) + 0.38 S(b), radius 1 (src/fluid_core.rs:2004-2011).
+        { REGION(1, 1)
+            const bool in = gy >= 2 && gy <= res - 3;
+            const int s = SIDX(gx, gy);
+            const int s0 = SIDX(gx, clampi(gy - 2, 0, res - 1)), s1 = SIDX(gx, clampi(gy - 1, 0, res - 1));
+            const int s3 = SIDX(gx, clampi(gy + 1, 0, res - 1)), s4 = SIDX(gx, clampi(gy + 2, 0, res - 1));
+            float gq = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
+            float sq = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
+            WQ[s] = 0.62f * gq + 0.38f * sq;
+        END_REGION }
+        __syncthreads();
+    }
+    // 10. Projection kick, damping and the speed clamp on wet cells
+    //     (src/fluid_core.rs:2015-2037); every cell of the tile is written.
+    { REGION(0, 0)
+        const int s = SIDX(gx, gy);
+        float uu = U[s], vv = V[s];
+        if (HS[s] > eps) {
+            if (P.project) {
+                float qx = (WQ[SIDX(min(gx + 1, res - 1), gy)] - WQ[SIDX(max(gx - 1, 0), gy)]) / (2.0f * cell);
+                float qz = (WQ[SIDX(gx, min(gy + 1, res - 1))] - WQ[SIDX(gx, max(gy - 1, 0))]) / (2.0f * cell);
+                uu += 0.012f * dt * qx;
+                vv += 0.012f * dt * qz;
+            }
+            float decay = P.nu_mode == NU_CONST ? P.decay_c : expf(-sheet_damp(cell_nu(P, g)) * dt);
+            uu = finite_speed(uu * decay, kSpeedCap);
+            vv = finite_speed(vv * decay, kSpeedCap);
+        }
+        P.u_out[g] = uu;
+        P.v_out[g] = vv;
+    END_REGION }
+#undef SIDX
+#undef REGION
+#undef END_REGION
+}
+
+// Donor-cell transport (src/fluid_core.rs:3025-3137), x pass then z pass on
+// the updated depth, dry cut (src/fluid_core.rs:2072-2081), FP64 ledger sum.
+__global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
+    const TransportParams& P = L.lay[blockIdx.z];
+    const int res = P.res;
+    const int tx0 = blockIdx.x * TT, ty0 = blockIdx.y * TT;
+    if (tx0 >= res || ty0 >= res || P.skip) return;
+    const int tx1 = min(res, tx0 + TT), ty1 = min(res, ty0 + TT);
+    extern __shared__ float sm[];
+    constexpr int PL = TW * TW;
+    float* HSm = sm;            // h on rows [ty0-2, ty1+1), cols [tx0-2, tx1+1)
+    float* US = sm + PL;        // u on the same cells
+    float* FL = sm + 2 * PL;    // left-going flux of edge e (cells e, e+1)
+    float* FR = sm + 3 * PL;    // right-going flux
+    float* HX = sm + 4 * PL;    // depth after the x pass
+    float* VS = sm + 5 * PL;    // v
+    float* UP = sm + 6 * PL;    // up-going flux of row pair (r, r+1)
+    float* DN = sm + 7 * PL;    // down-going flux
+    const int ox = tx0 - 2, oy = ty0 - 2;
+#define TIDX(gx, gy) (((gy) - oy) * TW + ((gx) - ox))
+    const int ry0 = max(0, ty0 - 2), ry1 = min(res, ty1 + 1);
+    const int cx0 = max(0, tx0 - 2), cx1 = min(res, tx1 + 1);
+    const float cell = P.cell, dt = P.dt;
+    const bool with_bed = P.bank_bed != nullptr;
+    const uint8_t* gate = P.gate;
+    // Load h, u (radius 2/1) and v (tile columns).
+    {
+        const int nx = cx1 - cx0, ncell = nx * (ry1 - ry0);
+        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+            int gy = ry0 + k / nx, gx = cx0 + k % nx;
+            size_t g = (size_t)gy * res + gx;
+            HSm[TIDX(gx, gy)] = P.h[g];
+            US[TIDX(gx, gy)] = P.u[g];
+            if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
+        }
+    }
+    __syncthreads();
+    // x pass. Edge e joins cells e and e+1 and exists for 0 <= e < res-1.
+    // Left-going flux first (its donor e+1 has removed nothing yet).
+    const int e0 = max(0, tx0 - 2), e1 = min(res - 2, tx1 - 1);  // inclusive edge range
+    {
+        const int ne = e1 - e0 + 1, nwork = ne * (ry1 - ry0);
+        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
+            int gy = ry0 + k / ne, e = e0 + k % ne;
+            float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
+            size_t g = (size_t)gy * res + e;
+            float bd = with_bed ? P.bank_bed[g + 1] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+            float dh = open_edge_dh(with_bed, HSm[TIDX(e + 1, gy)], HSm[TIDX(e, gy)], 0.0f, gate ? gate[g] : 1, bd, bc,
+                                    speed, dt, cell, 0.45f);
+            FL[TIDX(e, gy)] = speed > 0.0f ? 0.0f : dh;
+        }
+    }
+    __syncthreads();
+    // Right-going: donor e has removed the left-going flux of edge e-1.
+    {
+        const int ne = e1 - e0 + 1, nwork = ne * (ry1 - ry0);
+        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
+            int gy = ry0 + k / ne, e = e0 + k % ne;
+            if (e < tx0 - 1) continue;
+            float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
+            float prev = e > 0 ? FL[TIDX(e - 1, gy)] : 0.0f;
+            size_t g = (size_t)gy * res + e;
+            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + 1] : 0.0f;
+            float dh = open_edge_dh(with_bed, HSm[TIDX(e, gy)], HSm[TIDX(e + 1, gy)], 0.0f + prev,
+                                    gate ? gate[g + 1] : 1, bd, bc, speed, dt, cell, 0.45f);
+            FR[TIDX(e, gy)] = speed > 0.0f ? dh : 0.0f;
+        }
+    }
+    __syncthreads();
+    // Depth after the x pass on rows [ry0, ry1), tile columns.
+    {
+        const int nx = tx1 - tx0, ncell = nx * (ry1 - ry0);
+        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+            int gy = ry0 + k / nx, c = tx0 + k % nx;
+            float flm = c - 1 >= 0 ? FL[TIDX(c - 1, gy)] : 0.0f;
+            float frm = c - 1 >= 0 ? FR[TIDX(c - 1, gy)] : 0.0f;
+            float flc = c <= res - 2 ? FL[TIDX(c, gy)] : 0.0f;
+            float frc = c <= res - 2 ? FR[TIDX(c, gy)] : 0.0f;
+            float rem = (0.0f + flm) + frc;
+            float add = (0.0f + frm) + flc;
+            float hv = HSm[TIDX(c, gy)];
+            float moved = fmaxf(hv - rem + add, 0.0f);
+            HX[TIDX(c, gy)] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        }
+    }
+    __syncthreads();
+    // z pass. Pair r joins rows r and r+1 and exists for 0 <= r < res-1.
+    const int p0 = max(0, ty0 - 2), p1 = min(res - 2, ty1 - 1);
+    {
+        const int nx = tx1 - tx0, nwork = nx * (p1 - p0 + 1);
+        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
+            int r = p0 + k / nx, c = tx0 + k % nx;
+            float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
+            size_t g = (size_t)r * res + c;
+            float bd = with_bed ? P.bank_bed[g + res] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+            float dh = open_edge_dh(with_bed, HX[TIDX(c, r + 1)], HX[TIDX(c, r)], 0.0f, gate ? gate[g] : 1, bd, bc,
+                                    speed, dt, cell, 0.45f);
+            UP[TIDX(c, r)] = speed > 0.0f ? 0.0f : dh;
+        }
+    }
+    __syncthreads();
+    {
+        const int nx = tx1 - tx0, nwork = nx * (p1 - p0 + 1);
+        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
+            int r = p0 + k / nx, c = tx0 + k % nx;
+            if (r < ty0 - 1) continue;
+            float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
+            float ra = r > 0 ? 0.0f + UP[TIDX(c, r - 1)] : 0.0f;
+            size_t g = (size_t)r * res + c;
+            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + res] : 0.0f;
+            float dh = open_edge_dh(with_bed, HX[TIDX(c, r)], HX[TIDX(c, r + 1)], ra, gate ? gate[g + res] : 1, bd,
+                                    bc, speed, dt, cell, 0.45f);
+            DN[TIDX(c, r)] = speed > 0.0f ? dh : 0.0f;
+        }
+    }
+    __syncthreads();
+    double part = 0.0;
+    {
+        const int nx = tx1 - tx0, ncell = nx * (ty1 - ty0);
+        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
+            int r = ty0 + k / nx, c = tx0 + k % nx;
+            float upm = r - 1 >= 0 ? UP[TIDX(c, r - 1)] : 0.0f;
+            float dnm = r - 1 >= 0 ? DN[TIDX(c, r - 1)] : 0.0f;
+            float upc = r <= res - 2 ? UP[TIDX(c, r)] : 0.0f;
+            float dnc = r <= res - 2 ? DN[TIDX(c, r)] : 0.0f;
+            float rem = (0.0f + upm) + dnc;
+            float add = (0.0f + dnm) + upc;
+            float hv = HX[TIDX(c, r)];
+            float moved = fmaxf(hv - rem + add, 0.0f);
+            float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
+            if (P.eps > 0.0f && hn < P.eps) hn = 0.0f;
+            P.h_out[(size_t)r * res + c] = hn;
+            part += (double)fmaxf(hn, 0.0f);
+        }
+    }
+#undef TIDX
+    // Block sum of the depth (FP64), one atomic per block.
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    __shared__ double warp_sum[TRANSPORT_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? warp_sum[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0 && P.ledger) atomicAdd(P.ledger, v);
+    }
+}
+
+// Materialises the lazy dry cut: u = v = 0 where h < eps.
+__global__ void k_apply_cut(const float* h, float* u, float* v, size_t n, float eps) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (h[i] < eps) { u[i] = 0.0f; v[i] = 0.0f; }
+}
+
+// Largest squared speed, for the CFL substep count (src/fluid_core.rs:1723-1744).
+__global__ void k_max_speed2(const float* h, const float* u, const float* v, size_t n, float eps, int apply_cut,
+                             unsigned int* out_bits) {
+    float m = 0.0f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float uu = u[i], vv = v[i];
+        if (apply_cut && h[i] < eps) continue;
+        float s2 = uu * uu + vv * vv;
+        if (s2 > m) m = s2;
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(m));
+}
+
+cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
+        attr = true;
+    }
+    dim3 grid((res + FT - 1) / FT, (res + FT - 1) / FT, layers);
+    k_force<<<grid, FORCE_THREADS, force_smem_bytes(), st>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes());
+        attr = true;
+    }
+    dim3 grid((res + TT - 1) / TT, (res + TT - 1) / TT, layers);
+    k_transport<<<grid, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_cut(const float* h, float* u, float* v, size_t n, float eps, cudaStream_t st) {
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_apply_cut<<<blocks, 256, 0, st>>>(h, u, v, n, eps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_speed2(const float* h, const float* u, const float* v, size_t n, float eps, int apply_cut,
+                              unsigned int* out_bits, cudaStream_t st) {
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_max_speed2<<<blocks, 256, 0, st>>>(h, u, v, n, eps, apply_cut, out_bits);
+    return cudaGetLastError();
+}
+
+}  // namespace silt

@@ -1,0 +1,64 @@
+// Launch parameters of the full-grid sheet kernels (sheet_grid.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace silt {
+
+enum NuMode : int32_t {
+    NU_CONST = 0,   // one viscosity for the whole layer (the water sheet, 0.9 Pa s)
+    NU_PLANE = 1,   // a float viscosity per cell (the free step_sheet operator)
+    NU_GRAIN = 2,   // dynamic_viscosity(grain, moisture) per cell (the slurry sheet)
+};
+
+struct LayerParams {
+    const float* h;
+    const float* bed;
+    const float* u;
+    const float* v;
+    float* u_out;
+    float* v_out;
+    const uint8_t* grain;
+    const float* moisture;
+    const float* nu_plane;
+    int32_t nu_mode;
+    float nu_c, mob_c, decay_c;  // NU_CONST: viscosity, mobility and damping factor
+    int32_t res;
+    float cell, dt, vort, eps;
+    int32_t project;       // divergence projection (cells wider than 2 cm)
+    int32_t soften_edge;   // soft window band width in cells, 0 = off
+    int32_t apply_cut;     // zero u, v where h < eps on load (the previous dry cut)
+    int32_t skip;          // layer has nothing to do this substep
+};
+
+struct ForceLaunch {
+    LayerParams lay[2];
+};
+
+struct TransportParams {
+    const float* h;
+    const float* u;
+    const float* v;
+    float* h_out;
+    const uint8_t* gate;      // nullptr = every receiver open
+    const float* bank_bed;    // nullptr = no dry-bank test (banks off)
+    double* ledger;           // FP64 sum of the new depth, may be nullptr
+    int32_t res;
+    float cell, dt, eps;
+    int32_t skip;
+};
+
+struct TransportLaunch {
+    TransportParams lay[2];
+};
+
+size_t force_smem_bytes();
+size_t transport_smem_bytes();
+cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st);
+cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st);
+cudaError_t launch_apply_cut(const float* h, float* u, float* v, size_t n, float eps, cudaStream_t st);
+cudaError_t launch_max_speed2(const float* h, const float* u, const float* v, size_t n, float eps, int apply_cut,
+                              unsigned int* out_bits, cudaStream_t st);
+
+}  // namespace silt

@@ -1,0 +1,81 @@
+// Device-side scalar laws of the sheet step, written to give the same f32
+// results as the reference (x3-team/Dirty-gen src/fluid_core.rs). The whole
+// library is compiled with -fmad=false so no multiply and add are fused,
+// matching the reference's build (src/fluid_core.rs:2983-2984).
+#pragma once
+#include <cstdint>
+
+namespace silt {
+
+constexpr float kGravity = 9.81f;          // src/fluid_core.rs:111
+constexpr float kFineCell = 0.02f;         // :73
+constexpr float kSpeedCap = 1.6f;          // FILM_SPEED_CAP_MPS :10003
+constexpr float kG0 = 0.06f, kG1 = 0.24f, kG2 = 0.40f;   // GAUSS :108
+constexpr float kS0 = 0.02f, kS1 = 0.08f, kS2 = 0.80f;   // STEEP :109
+
+// f32::clamp: NaN passes through.
+__device__ __forceinline__ float rclamp(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+__device__ __forceinline__ bool finite_f(float x) { return isfinite(x); }
+
+// src/fluid_core.rs:150-161
+__device__ __forceinline__ float dynamic_viscosity(uint8_t grain, float moisture) {
+    float x = rclamp((rclamp(moisture, 0.0f, 1.0f) - 0.22f) / 0.70f, 0.0f, 1.0f);
+    float thin = x * x * (3.0f - 2.0f * x);
+    float stiff, fluid;
+    switch (grain) {
+        case 1: stiff = 220.0f; fluid = 4.0f; break;
+        case 2: stiff = 28.0f; fluid = 0.55f; break;
+        case 3: stiff = 0.9f; fluid = 0.9f; break;
+        case 4: stiff = 1.5f; fluid = 0.08f; break;
+        default: stiff = 420.0f; fluid = 0.35f; break;
+    }
+    return stiff + (fluid - stiff) * thin;
+}
+
+// src/fluid_core.rs:169-180
+__device__ __forceinline__ float sheet_mobility_for(float nu) {
+    if (nu < 0.0f) return -nu;
+    float boost = 0.0f;
+    if (nu < 12.0f) {
+        float t = rclamp((12.0f - fmaxf(nu, 0.0f)) / 12.0f, 0.0f, 1.0f);
+        boost = t * t * 1.6f;
+    }
+    return 0.042f * (1.0f + boost);
+}
+
+// src/fluid_core.rs:184-192. powf here is CUDA's; it can differ from glibc's
+// in the last bit, which is the one place the slurry damping may differ.
+__device__ __forceinline__ float sheet_damp(float nu) {
+    float rel = rclamp(fmaxf(nu, 0.05f) / 231.0f, 0.002f, 12.0f);
+    if (rel >= 0.42f) return 1.70f * powf(rel, 0.30f);
+    const float at_silt = 1.70f * powf(0.42f, 0.30f);
+    float t = rclamp(rel / 0.42f, 0.0f, 1.0f);
+    return at_silt * powf(t, 1.15f);
+}
+
+// src/fluid_core.rs:3473-3479
+__device__ __forceinline__ float finite_speed(float v, float lim) {
+    return finite_f(v) ? rclamp(v, -lim, lim) : 0.0f;
+}
+__device__ __forceinline__ float finite0(float v) { return finite_f(v) ? v : 0.0f; }
+
+// src/fluid_core.rs:2867-2911 open_edge_dh: depth one donor gives across one
+// edge, 0 where the serial loop would skip the edge.
+__device__ __forceinline__ float open_edge_dh(bool with_bed, float hd, float hr, float remd, uint8_t gate_r,
+                                              float bed_d, float bed_r, float speed, float dt, float cell,
+                                              float frac_cap) {
+    bool live = !(fabsf(speed) < 1.0e-5f);
+    bool bank = with_bed && hr <= 1.0e-6f && bed_r > bed_d + hd + 1.0e-3f;
+    float room = hd - remd;
+    bool gate_shut = gate_r == 0 && hr <= 1.0e-6f;
+    float frac = fminf(fabsf(speed) * dt / cell, frac_cap);
+    float dh = fminf(hd * frac, room);
+    bool ok = live & !bank & !(room <= 1.0e-8f) & !gate_shut & !(dh <= 1.0e-8f);
+    return ok ? dh : 0.0f;
+}
+
+}  // namespace silt

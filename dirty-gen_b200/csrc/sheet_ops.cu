@@ -1,0 +1,212 @@
+// Per-cell kernels around the sheet step: seeding (the reference's closure
+// writes), the render-contract publish, map export, the FP64 ledger sum and
+// the non-finite count. Each follows the reference function it names.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sheet_math.cuh"
+#include "sheet_ops.cuh"
+
+namespace silt {
+
+#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
+static int blocks_for(size_t n) {
+    size_t b = (n + 255) / 256;
+    return (int)(b > 148 * 16 ? 148 * 16 : (b == 0 ? 1 : b));
+}
+
+// src/fluid_core.rs:5329-5356 map_water_bed, per cell.
+__global__ void k_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
+                                uint8_t* grain, size_t n) {
+    GRID_STRIDE(i, n) {
+        float b = bed_in[i];
+        bed[i] = finite_f(b) ? b : 0.0f;
+        float w = water_in[i];
+        w = finite_f(w) ? fmaxf(w, 0.0f) : 0.0f;
+        water[i] = w;
+        if (w > 0.0f) {
+            moisture[i] = fmaxf(moisture[i], 0.8f);
+            if (grain[i] == 4) grain[i] = 1;
+        }
+    }
+}
+
+// src/fluid_core.rs:5358-5372 map_water_velocity.
+__global__ void k_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
+                                     size_t n) {
+    GRID_STRIDE(i, n) {
+        if (water[i] <= 1.0e-6f) continue;
+        float u = u_in[i], v = v_in[i];
+        uw[i] = finite_f(u) ? u : 0.0f;
+        vw[i] = finite_f(v) ? v : 0.0f;
+    }
+}
+
+// src/fluid_core.rs:5820-5849 paint (pour_water / pour_slurry).
+__global__ void k_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
+                        float x0, float x1, float z0, float z1, float depth, int water, int g, float m) {
+    size_t n = (size_t)res * res;
+    GRID_STRIDE(k, n) {
+        int i = (int)(k % res), j = (int)(k / res);
+        float x = ox + ((float)i + 0.5f) * cell;
+        float z = oz + ((float)j + 0.5f) * cell;
+        if (x < x0 || x >= x1 || z < z0 || z >= z1) continue;
+        depth_plane[k] = depth;
+        if (!water) {
+            grain[k] = (uint8_t)g;
+            moisture[k] = m;
+        }
+    }
+}
+
+// src/fluid_core.rs:5854-5877 lay_slurry_mask.
+__global__ void k_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g,
+                             float m) {
+    GRID_STRIDE(i, n) {
+        float d = depth[i];
+        if (!(finite_f(d) && d > 0.0f)) continue;
+        slurry[i] += d;
+        grain[i] = (uint8_t)g;
+        moisture[i] = fmaxf(moisture[i], m);
+    }
+}
+
+// src/fluid_core.rs:5928-5950 read_substrate_grid, per cell.
+__global__ void k_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
+                                 float* moisture, uint8_t* grain, const float* slurry, size_t n) {
+    GRID_STRIDE(i, n) {
+        bed[i] = bed_in[i];
+        moisture[i] = rclamp(moist_in[i], 0.0f, 1.0f);
+        if (slurry[i] > 1.0e-5f) grain[i] = grain_in[i];
+    }
+}
+
+// Inflow strip: depth added on one row over [x0, x1).
+__global__ void k_inflow(float* water, int res, int j, int i0, int i1, float add) {
+    int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < i1) water[(size_t)j * res + i] += add;
+}
+
+// coarse_cell (src/fluid_core.rs:6998-7035) feeding render_contract film/flow
+// (src/render_contract.rs:457-496). Tracers are off the sheet path: turbidity 0.
+__global__ void k_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
+                          const float* vs, float* film, float* flow, size_t n) {
+    GRID_STRIDE(i, n) {
+        float water_m = finite0(water[i]), slurry_m = finite0(slurry[i]);
+        float fl = water_m + slurry_m;
+        float u = 0.0f, v = 0.0f;
+        if (!(fl < 1.0e-5f)) {
+            u = finite0((uw[i] * water_m + us[i] * slurry_m) / fl);
+            v = finite0((vw[i] * water_m + vs[i] * slurry_m) / fl);
+        }
+        bool dry = !finite_f(water_m) || !finite_f(slurry_m) || water_m + slurry_m < 1.0e-5f;
+        if (dry) { u = 0.0f; v = 0.0f; }
+        float speed = dry ? 0.0f : finite0(sqrtf(u * u + v * v));
+        reinterpret_cast<float2*>(film)[i] = make_float2(finite0(water_m), finite0(slurry_m));
+        reinterpret_cast<float4*>(flow)[i] = make_float4(u, v, speed, 0.0f);
+    }
+}
+
+// export_maps (src/fluid_core.rs:6941-6975).
+__global__ void k_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
+                         const float* us, const float* vs, const float* moist, float* height, float* vel_u,
+                         float* vel_v, float* moisture, size_t n) {
+    GRID_STRIDE(i, n) {
+        if (height) height[i] = bed[i] + water[i] + slurry[i];
+        float hw = finite0(water[i]), hs = finite0(slurry[i]);
+        float h = hw + hs;
+        float u = 0.0f, v = 0.0f;
+        if (!(h < 1.0e-5f)) {
+            u = finite0((uw[i] * hw + us[i] * hs) / h);
+            v = finite0((vw[i] * hw + vs[i] * hs) / h);
+        }
+        if (vel_u) vel_u[i] = u;
+        if (vel_v) vel_v[i] = v;
+        if (moisture) moisture[i] = moist[i];
+    }
+}
+
+// FP64 sums of max(h, 0) for two planes (the ledger's column_sum, src/fluid_core.rs:4617).
+__global__ void k_sum2(const float* a, const float* b, size_t n, double* out) {
+    double sa = 0.0, sb = 0.0;
+    GRID_STRIDE(i, n) {
+        sa += (double)fmaxf(a[i], 0.0f);
+        sb += (double)fmaxf(b[i], 0.0f);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_down_sync(0xffffffffu, sa, o);
+        sb += __shfl_down_sync(0xffffffffu, sb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, sa);
+        atomicAdd(out + 1, sb);
+    }
+}
+
+__global__ void k_non_finite(const float* const* planes, int np, size_t n, unsigned int* out) {
+    unsigned int c = 0;
+    GRID_STRIDE(i, n) {
+        for (int p = 0; p < np; ++p) c += !finite_f(planes[p][i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
+                             uint8_t* grain, size_t n, cudaStream_t st) {
+    k_map_water_bed<<<blocks_for(n), 256, 0, st>>>(bed_in, water_in, bed, water, moisture, grain, n);
+    return cudaGetLastError();
+}
+cudaError_t op_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
+                                  size_t n, cudaStream_t st) {
+    k_map_water_velocity<<<blocks_for(n), 256, 0, st>>>(u_in, v_in, water, uw, vw, n);
+    return cudaGetLastError();
+}
+cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
+                     float x0, float x1, float z0, float z1, float depth, int water, int g, float m, cudaStream_t st) {
+    k_paint<<<blocks_for((size_t)res * res), 256, 0, st>>>(depth_plane, moisture, grain, res, cell, ox, oz, x0, x1, z0,
+                                                           z1, depth, water, g, m);
+    return cudaGetLastError();
+}
+cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
+                          cudaStream_t st) {
+    k_lay_slurry<<<blocks_for(n), 256, 0, st>>>(depth, slurry, moisture, grain, n, g, m);
+    return cudaGetLastError();
+}
+cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
+                              float* moisture, uint8_t* grain, const float* slurry, size_t n, cudaStream_t st) {
+    k_read_substrate<<<blocks_for(n), 256, 0, st>>>(bed_in, moist_in, grain_in, bed, moisture, grain, slurry, n);
+    return cudaGetLastError();
+}
+cudaError_t op_inflow(float* water, int res, int j, int i0, int i1, float add, cudaStream_t st) {
+    if (i1 <= i0) return cudaSuccess;
+    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, res, j, i0, i1, add);
+    return cudaGetLastError();
+}
+cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
+                       const float* vs, float* film, float* flow, size_t n, cudaStream_t st) {
+    k_publish<<<blocks_for(n), 256, 0, st>>>(water, slurry, uw, vw, us, vs, film, flow, n);
+    return cudaGetLastError();
+}
+cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
+                      const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
+                      float* moisture, size_t n, cudaStream_t st) {
+    k_export<<<blocks_for(n), 256, 0, st>>>(bed, water, slurry, uw, vw, us, vs, moist, height, vel_u, vel_v, moisture,
+                                           n);
+    return cudaGetLastError();
+}
+cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    k_sum2<<<blocks_for(n), 256, 0, st>>>(a, b, n, out);
+    return cudaGetLastError();
+}
+cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    k_non_finite<<<blocks_for(n), 256, 0, st>>>(planes, np, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace silt

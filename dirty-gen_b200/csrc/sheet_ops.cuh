@@ -1,0 +1,28 @@
+// Per-cell kernels around the sheet step (sheet_ops.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace silt {
+
+cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
+                             uint8_t* grain, size_t n, cudaStream_t st);
+cudaError_t op_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
+                                  size_t n, cudaStream_t st);
+cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
+                     float x0, float x1, float z0, float z1, float depth, int water, int g, float m, cudaStream_t st);
+cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
+                          cudaStream_t st);
+cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
+                              float* moisture, uint8_t* grain, const float* slurry, size_t n, cudaStream_t st);
+cudaError_t op_inflow(float* water, int res, int j, int i0, int i1, float add, cudaStream_t st);
+cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
+                       const float* vs, float* film, float* flow, size_t n, cudaStream_t st);
+cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
+                      const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
+                      float* moisture, size_t n, cudaStream_t st);
+cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st);
+cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st);
+
+}  // namespace silt

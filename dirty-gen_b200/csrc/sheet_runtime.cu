@@ -1,0 +1,879 @@
+// Host runtime of the B200 sheet step: the `silt_*` C ABI (include/silt_sheet.h).
+//
+// A handle owns the device state of one window: ping-pong SoA planes for the
+// water and slurry depth and velocity, the bed, moisture and grain, the
+// nested 2 cm patches, and small device accumulators. Every call queues work
+// on the handle's stream; only calls that return host data synchronise.
+//
+// Step order follows FluidCore::step (x3-team/Dirty-gen src/fluid_core.rs:6034),
+// sheet subset: inflow, refine (restrict, lay the patches, near field), tire
+// shove on the patches, fine pair, fine spray, restrict, shove outside the
+// patches, coarse pair, coarse spray.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/silt_sheet.h"
+#include "sheet_fine.cuh"
+#include "sheet_grid.cuh"
+#include "sheet_host_math.h"
+#include "sheet_ops.cuh"
+
+namespace {
+
+thread_local char g_err[256] = "";
+
+int fail_cuda(cudaError_t e, const char* what) {
+    snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
+    return SILT_ECUDA;
+}
+int fail_arg(const char* what) {
+    snprintf(g_err, sizeof g_err, "invalid argument: %s", what);
+    return SILT_EINVAL;
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call);   \
+    } while (0)
+
+struct DevicePlane {
+    void* p = nullptr;
+    ~DevicePlane() {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+using silt::fine::Patches;
+
+struct silt_sheet {
+    silt_cfg cfg;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int res = 0;
+    size_t n = 0;
+    float origin[2] = {0, 0};
+    // [layer][buffer]: layer 0 water, 1 slurry.
+    float* h[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    float* u[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    float* v[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int cur = 0;
+    float* bed = nullptr;
+    float* moisture = nullptr;
+    uint8_t* grain = nullptr;
+    float* staging = nullptr;     // n floats for host uploads
+    float* staging2 = nullptr;
+    uint8_t* staging_u8 = nullptr;
+    double* d_acc = nullptr;      // [0..1] step ledger sums, [2..3] reductions, [4..7] spare
+    unsigned int* d_u32 = nullptr;
+    const float** d_planes = nullptr;
+    double* h_acc = nullptr;      // pinned mirror of d_acc
+    bool cut_pending = false;
+    bool ledger_fresh = false;    // h_acc[0..1] hold the current depth sums
+    float vmax_bound = 0.0f;      // bound on any cell speed, for the one-substep shortcut
+    float moisture_ambient = 0.0f;
+    std::vector<silt_tire_push> pushes;
+    double spray_m3 = 0.0, opened_m3 = 0.0;
+    int inflow_j = -1, inflow_i0 = 0, inflow_i1 = 0;
+    float inflow_rate = 0.0f;
+    Patches fine;
+    // Step timing (silt_set_step_timing): event triples around force/transport.
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<cudaEvent_t> ev_used;   // groups of three: start, after force, after transport
+    silt_step_parts parts;
+
+    float* H(int l) { return h[l][cur]; }
+    float* U(int l) { return u[l][cur]; }
+    float* V(int l) { return v[l][cur]; }
+};
+
+namespace {
+
+float water_nu() { return silt::host::dynamic_viscosity(3, 1.0f); }
+
+// Materialise the lazy dry cut before anything reads or writes the planes.
+int flush_cut(silt_sheet* s) {
+    if (!s->cut_pending) return SILT_OK;
+    for (int l = 0; l < 2; ++l) CK(silt::launch_apply_cut(s->H(l), s->U(l), s->V(l), s->n, 1.0e-6f, s->st));
+    s->cut_pending = false;
+    return SILT_OK;
+}
+
+int upload(silt_sheet* s, float* dst, const float* host) {
+    CK(cudaMemcpyAsync(dst, host, s->n * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    return SILT_OK;
+}
+
+// One coarse-sized pair of sheets for one step (FluidCore::step_pair, src/fluid_core.rs:7942-8150).
+// `soften` is the soft window border, applied once per step before the first substep.
+int step_coarse_pair(silt_sheet* s, float dt) {
+    const int res = s->res;
+    const float cell = s->cfg.cell;
+    const float eps = 1.0e-6f;
+    // Substep count (src/fluid_core.rs:1715-1744). With every speed under the
+    // bound one substep is certain; otherwise measure the largest speed.
+    int nsub[2] = {1, 1};
+    const float cap = 8.0f;
+    float bound = s->vmax_bound * 1.4142137f;
+    if (!(dt * std::max(0.15f, bound) <= 0.42f * std::max(cell, 1.0e-3f))) {
+        for (int l = 0; l < 2; ++l) {
+            CK(cudaMemsetAsync(s->d_u32, 0, sizeof(unsigned int), s->st));
+            CK(silt::launch_max_speed2(s->H(l), s->U(l), s->V(l), s->n, eps, s->cut_pending ? 1 : 0, s->d_u32, s->st));
+            unsigned int bits = 0;
+            CK(cudaMemcpyAsync(&bits, s->d_u32, sizeof bits, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            float m2;
+            memcpy(&m2, &bits, 4);
+            float max_s = std::max(0.15f, sqrtf(m2));
+            float ns = ceilf((dt * max_s) / (0.42f * std::max(cell, 1.0e-3f)));
+            nsub[l] = (int)silt::host::rclamp(ns, 1.0f, cap);
+        }
+    }
+    const int soften_edge = s->cfg.soften_border ? std::max(res / 12, 2) : 0;
+    const int steps = std::max(nsub[0], nsub[1]);
+    const float nu_w = water_nu();
+    for (int k = 0; k < steps; ++k) {
+        silt::ForceLaunch F;
+        silt::TransportLaunch T;
+        memset(&F, 0, sizeof F);
+        memset(&T, 0, sizeof T);
+        const int nxt = s->cur ^ 1;
+        for (int l = 0; l < 2; ++l) {
+            silt::LayerParams& P = F.lay[l];
+            const float dts = dt / (float)nsub[l];
+            P.h = s->h[l][s->cur];
+            P.bed = s->bed;
+            P.u = s->u[l][s->cur];
+            P.v = s->v[l][s->cur];
+            P.u_out = s->u[l][nxt];
+            P.v_out = s->v[l][nxt];
+            P.res = res;
+            P.cell = cell;
+            P.dt = dts;
+            P.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
+            P.eps = eps;
+            P.project = cell > silt::host::kFineCell + 1.0e-6f;
+            P.soften_edge = k == 0 ? soften_edge : 0;
+            P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
+            P.skip = k >= nsub[l];
+            if (l == 0) {
+                P.nu_mode = silt::NU_CONST;
+                P.nu_c = nu_w;
+                P.mob_c = silt::host::sheet_mobility_for(nu_w);
+                P.decay_c = expf(-silt::host::sheet_damp(nu_w) * dts);
+            } else {
+                P.nu_mode = silt::NU_GRAIN;
+                P.grain = s->grain;
+                P.moisture = s->moisture;
+            }
+            silt::TransportParams& Q = T.lay[l];
+            Q.h = s->h[l][s->cur];
+            Q.u = P.u_out;
+            Q.v = P.v_out;
+            Q.h_out = s->h[l][nxt];
+            Q.gate = nullptr;
+            Q.bank_bed = nullptr;
+            Q.ledger = s->d_acc + l;
+            Q.res = res;
+            Q.cell = cell;
+            Q.dt = dts;
+            Q.eps = eps;
+            Q.skip = P.skip;
+        }
+        // A skipped layer keeps its planes (copied across the buffer swap) and its ledger sum.
+        for (int l = 0; l < 2; ++l)
+            if (!F.lay[l].skip) CK(cudaMemsetAsync(s->d_acc + l, 0, sizeof(double), s->st));
+        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        if (s->timing) {
+            for (int q = 0; q < 3; ++q) {
+                if (s->ev_pool.empty()) {
+                    cudaEvent_t e;
+                    CK(cudaEventCreate(&e));
+                    s->ev_pool.push_back(e);
+                }
+                ev[q] = s->ev_pool.back();
+                s->ev_pool.pop_back();
+                s->ev_used.push_back(ev[q]);
+            }
+            CK(cudaEventRecord(ev[0], s->st));
+        }
+        CK(silt::launch_force(F, res, 2, s->st));
+        if (s->timing) CK(cudaEventRecord(ev[1], s->st));
+        CK(silt::launch_transport(T, res, 2, s->st));
+        if (s->timing) CK(cudaEventRecord(ev[2], s->st));
+        s->parts.launches += 2;
+        s->parts.force_launches += 1;
+        s->parts.force_cells += (int64_t)s->n;
+        for (int l = 0; l < 2; ++l)
+            if (F.lay[l].skip) {
+                CK(cudaMemcpyAsync(s->h[l][nxt], s->h[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
+                CK(cudaMemcpyAsync(s->u[l][nxt], s->u[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
+                CK(cudaMemcpyAsync(s->v[l][nxt], s->v[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
+            }
+        s->cur = nxt;
+        s->cut_pending = true;
+    }
+    s->vmax_bound = std::max(silt::host::kSpeedCap, 0.0f);
+    return SILT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* silt_last_error(void) { return g_err; }
+
+void silt_cfg_default(silt_cfg* c) {
+    if (!c) return;
+    c->res = 200;
+    c->cell = 0.20f;
+    c->fine_res = 160;
+    c->fine_cell = 0.02f;
+    c->fine_layout = SILT_FINE_MEAN_PATCH;
+    c->tire_r = 0.56f;
+    c->soften_border = 1;
+    c->center_x = 0.0f;
+    c->center_z = 0.0f;
+    c->device = 0;
+    c->stream = nullptr;
+}
+
+int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
+    if (!cfg || !out) return fail_arg("cfg/out");
+    if (cfg->res < 8 || cfg->res > 32768 || !(cfg->cell > 0.0f)) return fail_arg("res/cell");
+    if (cfg->fine_res < 8 || cfg->fine_res > 1024 || !(cfg->fine_cell > 0.0f)) return fail_arg("fine_res/fine_cell");
+    float ratio = cfg->cell / cfg->fine_cell;
+    if (fabsf(ratio - roundf(ratio)) > 1.0e-3f || roundf(ratio) < 1.0f) return fail_arg("cell/fine_cell not whole");
+    *out = nullptr;
+    CK(cudaSetDevice(cfg->device));
+    silt_sheet* s = new silt_sheet();
+    s->cfg = *cfg;
+    memset(&s->parts, 0, sizeof s->parts);
+    s->res = cfg->res;
+    s->n = (size_t)cfg->res * cfg->res;
+    silt::host::snap_origin(cfg->center_x, cfg->center_z, (float)cfg->res * cfg->cell, cfg->cell, s->origin);
+    if (cfg->stream) {
+        s->st = (cudaStream_t)cfg->stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete s;
+            return fail_cuda(e, "cudaStreamCreate");
+        }
+        s->own_stream = true;
+    }
+    const size_t nb = s->n * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    for (int l = 0; l < 2 && e == cudaSuccess; ++l)
+        for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+            e = cudaMalloc(&s->h[l][b], nb);
+            if (e == cudaSuccess) e = cudaMalloc(&s->u[l][b], nb);
+            if (e == cudaSuccess) e = cudaMalloc(&s->v[l][b], nb);
+        }
+    if (e == cudaSuccess) e = cudaMalloc(&s->bed, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->moisture, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->grain, s->n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->staging, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_acc, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
+    if (e != cudaSuccess) {
+        silt_sheet_destroy(s);
+        return e == cudaErrorMemoryAllocation ? SILT_ENOMEM : fail_cuda(e, "allocate window");
+    }
+    for (int l = 0; l < 2; ++l)
+        for (int b = 0; b < 2; ++b) {
+            cudaMemsetAsync(s->h[l][b], 0, nb, s->st);
+            cudaMemsetAsync(s->u[l][b], 0, nb, s->st);
+            cudaMemsetAsync(s->v[l][b], 0, nb, s->st);
+        }
+    cudaMemsetAsync(s->bed, 0, nb, s->st);
+    cudaMemsetAsync(s->moisture, 0, nb, s->st);
+    cudaMemsetAsync(s->grain, 4, s->n, s->st);  // Grain::Other
+    int rc = silt::fine::create(s->fine, *cfg, s->res, s->st);
+    if (rc != SILT_OK) {
+        silt_sheet_destroy(s);
+        return rc;
+    }
+    e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) {
+        silt_sheet_destroy(s);
+        return fail_cuda(e, "init window");
+    }
+    *out = s;
+    return SILT_OK;
+}
+
+int silt_sheet_destroy(silt_sheet* s) {
+    if (!s) return SILT_OK;
+    cudaSetDevice(s->cfg.device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    silt::fine::destroy(s->fine);
+    for (int l = 0; l < 2; ++l)
+        for (int b = 0; b < 2; ++b) {
+            cudaFree(s->h[l][b]);
+            cudaFree(s->u[l][b]);
+            cudaFree(s->v[l][b]);
+        }
+    cudaFree(s->bed);
+    cudaFree(s->moisture);
+    cudaFree(s->grain);
+    cudaFree(s->staging);
+    cudaFree(s->staging2);
+    cudaFree(s->staging_u8);
+    cudaFree(s->d_acc);
+    cudaFree(s->d_u32);
+    cudaFree(s->d_planes);
+    if (s->h_acc) cudaFreeHost(s->h_acc);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : s->ev_used) cudaEventDestroy(e);
+    if (s->own_stream) cudaStreamDestroy(s->st);
+    delete s;
+    return SILT_OK;
+}
+
+int silt_sheet_sync(silt_sheet* s) {
+    if (!s) return fail_arg("handle");
+    CK(cudaStreamSynchronize(s->st));
+    return SILT_OK;
+}
+
+// Host-side volume of what a seeding call writes, summed in f32 cell order like the reference.
+static float host_volume(const float* w, size_t n, float area, bool clamp_nonneg) {
+    float vol = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+        float x = w[i];
+        if (clamp_nonneg) x = std::isfinite(x) ? std::max(x, 0.0f) : 0.0f;
+        vol += x * area;
+    }
+    return vol;
+}
+
+int silt_map_water_bed(silt_sheet* s, const float* bed, const float* water, float* vol_out) {
+    if (!s || !bed || !water) return fail_arg("map_water_bed");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = flush_cut(s))) return rc;
+    if ((rc = upload(s, s->staging, bed))) return rc;
+    if ((rc = upload(s, s->staging2, water))) return rc;
+    CK(silt::op_map_water_bed(s->staging, s->staging2, s->bed, s->H(0), s->moisture, s->grain, s->n, s->st));
+    CK(cudaStreamSynchronize(s->st));  // the host arrays may be freed on return
+    if (vol_out) *vol_out = host_volume(water, s->n, s->cfg.cell * s->cfg.cell, true);
+    s->ledger_fresh = false;
+    return SILT_OK;
+}
+
+int silt_map_grain(silt_sheet* s, const uint8_t* grain) {
+    if (!s || !grain) return fail_arg("map_grain");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(s->grain, grain, s->n, cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return SILT_OK;
+}
+
+int silt_map_water_velocity(silt_sheet* s, const float* u, const float* v) {
+    if (!s || !u || !v) return fail_arg("map_water_velocity");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = flush_cut(s))) return rc;
+    if ((rc = upload(s, s->staging, u))) return rc;
+    if ((rc = upload(s, s->staging2, v))) return rc;
+    CK(silt::op_map_water_velocity(s->staging, s->staging2, s->H(0), s->U(0), s->V(0), s->n, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    float m = 0.0f;
+    for (size_t i = 0; i < s->n; ++i) {
+        if (std::isfinite(u[i])) m = std::max(m, fabsf(u[i]));
+        if (std::isfinite(v[i])) m = std::max(m, fabsf(v[i]));
+    }
+    s->vmax_bound = std::max(s->vmax_bound, m);
+    return SILT_OK;
+}
+
+static int paint(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, int water, int grain, float m,
+                 float* vol_out) {
+    if (!s) return fail_arg("handle");
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    depth = std::max(depth, 0.0f);  // NaN becomes 0 like f32::max
+    if (std::isnan(depth)) depth = 0.0f;
+    m = silt::host::rclamp(m, 0.0f, 1.0f);
+    CK(silt::op_paint(water ? s->H(0) : s->H(1), s->moisture, s->grain, s->res, s->cfg.cell, s->origin[0],
+                      s->origin[1], x0, x1, z0, z1, depth, water, grain, m, s->st));
+    if (vol_out) {
+        float vol = 0.0f, area = s->cfg.cell * s->cfg.cell;
+        for (int j = 0; j < s->res; ++j)
+            for (int i = 0; i < s->res; ++i) {
+                float x = s->origin[0] + ((float)i + 0.5f) * s->cfg.cell;
+                float z = s->origin[1] + ((float)j + 0.5f) * s->cfg.cell;
+                if (x < x0 || x >= x1 || z < z0 || z >= z1) continue;
+                vol += depth * area;
+            }
+        *vol_out = vol;
+    }
+    s->ledger_fresh = false;
+    return SILT_OK;
+}
+
+int silt_pour_water(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, float* vol_out) {
+    return paint(s, x0, x1, z0, z1, depth, 1, SILT_GRAIN_WATER, 1.0f, vol_out);
+}
+
+int silt_pour_slurry(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, int32_t grain, float moisture,
+                     float* vol_out) {
+    return paint(s, x0, x1, z0, z1, depth, 0, grain, moisture, vol_out);
+}
+
+int silt_lay_slurry_mask(silt_sheet* s, const float* depth, int32_t grain, float moisture, float* vol_out) {
+    if (!s || !depth) return fail_arg("lay_slurry_mask");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = flush_cut(s))) return rc;
+    if ((rc = upload(s, s->staging, depth))) return rc;
+    CK(silt::op_lay_slurry(s->staging, s->H(1), s->moisture, s->grain, s->n, grain,
+                           silt::host::rclamp(moisture, 0.0f, 1.0f), s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (vol_out) {
+        float vol = 0.0f, area = s->cfg.cell * s->cfg.cell;
+        for (size_t i = 0; i < s->n; ++i)
+            if (std::isfinite(depth[i]) && depth[i] > 0.0f) vol += depth[i] * area;
+        *vol_out = vol;
+    }
+    s->ledger_fresh = false;
+    return SILT_OK;
+}
+
+int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moisture, const uint8_t* grain) {
+    if (!s || !bed || !moisture || !grain) return fail_arg("read_substrate_grid");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = upload(s, s->staging, bed))) return rc;
+    if ((rc = upload(s, s->staging2, moisture))) return rc;
+    CK(cudaMemcpyAsync(s->staging_u8, grain, s->n, cudaMemcpyHostToDevice, s->st));
+    CK(silt::op_read_substrate(s->staging, s->staging2, s->staging_u8, s->bed, s->moisture, s->grain, s->H(1), s->n,
+                               s->st));
+    // The pad moisture: the most common whole percent (src/fluid_core.rs:5937-5961).
+    uint32_t hist[101] = {0};
+    for (size_t i = 0; i < s->n; ++i) {
+        float m = silt::host::rclamp(moisture[i], 0.0f, 1.0f);
+        float pct = m * 100.0f;
+        size_t whole = pct > 0.0f ? (size_t)pct : 0;
+        size_t bucket = pct - (float)whole >= 0.5f ? whole + 1 : whole;
+        hist[std::min(bucket, (size_t)100)] += 1;
+    }
+    size_t best = 0;
+    uint32_t best_n = 0;
+    for (size_t i = 0; i < 101; ++i)
+        if (hist[i] > best_n) {
+            best = i;
+            best_n = hist[i];
+        }
+    s->moisture_ambient = (float)best * 0.01f;
+    CK(cudaStreamSynchronize(s->st));
+    return SILT_OK;
+}
+
+int silt_set_inflow(silt_sheet* s, int32_t j, float x0, float x1, float rate) {
+    if (!s) return fail_arg("handle");
+    if (!(rate > 0.0f) || j < 0 || j >= s->res) {
+        s->inflow_j = -1;
+        return SILT_OK;
+    }
+    int i0 = s->res, i1 = 0;
+    for (int i = 0; i < s->res; ++i) {
+        float x = s->origin[0] + ((float)i + 0.5f) * s->cfg.cell;
+        if (x >= x0 && x < x1) {
+            i0 = std::min(i0, i);
+            i1 = std::max(i1, i + 1);
+        }
+    }
+    if (i1 <= i0) return fail_arg("inflow strip covers no cell");
+    s->inflow_j = j;
+    s->inflow_i0 = i0;
+    s->inflow_i1 = i1;
+    s->inflow_rate = rate;
+    return SILT_OK;
+}
+
+int silt_push_tire(silt_sheet* s, const silt_tire_push* p) {
+    if (!s || !p) return fail_arg("push_tire");
+    s->pushes.push_back(*p);
+    return SILT_OK;
+}
+
+int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32_t* n_out) {
+    if (!s) return fail_arg("handle");
+    if (n_out) *n_out = 0;
+    if (!(dt > 0.0f) || !std::isfinite(dt)) {
+        s->pushes.clear();
+        return SILT_OK_NOOP;
+    }
+    std::vector<silt_tire_push> ps;
+    ps.swap(s->pushes);
+    int rc;
+    if (s->inflow_j >= 0) {
+        if ((rc = flush_cut(s))) return rc;
+        int nc = s->inflow_i1 - s->inflow_i0;
+        float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
+        CK(silt::op_inflow(s->H(0), s->res, s->inflow_j, s->inflow_i0, s->inflow_i1, add, s->st));
+        s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
+    }
+    silt::fine::StepOut fo;
+    rc = silt::fine::step_patches(s->fine, s, ps, dt, fo);
+    if (rc) return rc;
+    if ((rc = step_coarse_pair(s, dt))) return rc;
+    rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
+    if (rc) return rc;
+    int32_t nev = 0;
+    rc = silt::fine::collect_spray(s->fine, s, fo, out, cap, &nev, &s->spray_m3);
+    if (rc) return rc;
+    if (n_out) *n_out = nev;
+    s->parts.steps += 1;
+    s->ledger_fresh = fo.spray_events == 0 && ps.empty();
+    return SILT_OK;
+}
+
+int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
+    if (!s || !out) return fail_arg("ledger");
+    double w = 0.0, sl = 0.0;
+    if (s->ledger_fresh) {
+        CK(cudaMemcpyAsync(s->h_acc, s->d_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    } else {
+        CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
+        CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    }
+    double fine_w = 0.0, fine_s = 0.0, park_w = 0.0, park_s = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &fine_w, &fine_s, &park_w, &park_s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    const double area = (double)s->cfg.cell * (double)s->cfg.cell;
+    w = s->h_acc[0] * area + fine_w;
+    sl = s->h_acc[1] * area + fine_s;
+    out->water_m3 = w;
+    out->slurry_m3 = sl;
+    out->frozen_water_m3 = park_w;
+    out->frozen_slurry_m3 = park_s;
+    out->spray_m3 = s->spray_m3;
+    out->opened_m3 = s->opened_m3;
+    out->total_m3 = w + sl + park_w + park_s + s->spray_m3;
+    return SILT_OK;
+}
+
+int silt_get_coarse_cell(silt_sheet* s, int32_t i, int32_t j, silt_coarse_cell* out) {
+    if (!s || !out) return fail_arg("coarse_cell");
+    if (i < 0 || j < 0 || i >= s->res || j >= s->res) return SILT_OK_NOOP;
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    size_t idx = (size_t)j * s->res + i;
+    float vals[8];
+    const float* src[8] = {s->bed + idx, s->H(0) + idx, s->H(1) + idx, s->moisture + idx,
+                           s->U(0) + idx, s->V(0) + idx, s->U(1) + idx, s->V(1) + idx};
+    for (int k = 0; k < 8; ++k) CK(cudaMemcpyAsync(&vals[k], src[k], 4, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    using silt::host::finite0;
+    float water_m = finite0(vals[1]), slurry_m = finite0(vals[2]);
+    float film = water_m + slurry_m;
+    float u = 0.0f, v = 0.0f;
+    if (!(film < 1.0e-5f)) {
+        u = finite0((vals[4] * water_m + vals[6] * slurry_m) / film);
+        v = finite0((vals[5] * water_m + vals[7] * slurry_m) / film);
+    }
+    out->x = s->origin[0] + ((float)i + 0.5f) * s->cfg.cell;
+    out->z = s->origin[1] + ((float)j + 0.5f) * s->cfg.cell;
+    out->bed_m = finite0(vals[0]);
+    out->water_m = water_m;
+    out->slurry_m = slurry_m;
+    out->moisture = finite0(vals[3]);
+    out->u = u;
+    out->v = v;
+    return SILT_OK;
+}
+
+int silt_export_maps(silt_sheet* s, float* height, float* vel_u, float* vel_v, float* moisture) {
+    if (!s) return fail_arg("handle");
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = flush_cut(s))) return rc;
+    // Four planes through the two staging buffers, two at a time.
+    float* outs[4] = {height, vel_u, vel_v, moisture};
+    for (int pass = 0; pass < 2; ++pass) {
+        float* d[4] = {nullptr, nullptr, nullptr, nullptr};
+        d[pass * 2] = s->staging;
+        d[pass * 2 + 1] = s->staging2;
+        if (!outs[pass * 2] && !outs[pass * 2 + 1]) continue;
+        CK(silt::op_export(s->bed, s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), s->moisture, d[0], d[1],
+                           d[2], d[3], s->n, s->st));
+        if (outs[pass * 2])
+            CK(cudaMemcpyAsync(outs[pass * 2], s->staging, s->n * 4, cudaMemcpyDeviceToHost, s->st));
+        if (outs[pass * 2 + 1])
+            CK(cudaMemcpyAsync(outs[pass * 2 + 1], s->staging2, s->n * 4, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    return SILT_OK;
+}
+
+int silt_publish_film_flow_device(silt_sheet* s, float* d_film, float* d_flow) {
+    if (!s || !d_film || !d_flow) return fail_arg("publish");
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    CK(silt::op_publish(s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), d_film, d_flow, s->n, s->st));
+    return SILT_OK;
+}
+
+int silt_publish_film_flow(silt_sheet* s, float* film, float* flow) {
+    if (!s || !film || !flow) return fail_arg("publish");
+    float* d_film = nullptr;
+    float* d_flow = nullptr;
+    CK(cudaMallocAsync((void**)&d_film, s->n * 2 * sizeof(float), s->st));
+    CK(cudaMallocAsync((void**)&d_flow, s->n * 4 * sizeof(float), s->st));
+    int rc = silt_publish_film_flow_device(s, d_film, d_flow);
+    if (rc == SILT_OK) {
+        CK(cudaMemcpyAsync(film, d_film, s->n * 2 * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaMemcpyAsync(flow, d_flow, s->n * 4 * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    }
+    cudaFreeAsync(d_film, s->st);
+    cudaFreeAsync(d_flow, s->st);
+    CK(cudaStreamSynchronize(s->st));
+    return rc;
+}
+
+int silt_non_finite_count(silt_sheet* s, uint32_t* out) {
+    if (!s || !out) return fail_arg("non_finite_count");
+    const float* planes[8] = {s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), s->bed, s->moisture};
+    CK(cudaMemcpyAsync(s->d_planes, planes, sizeof planes, cudaMemcpyHostToDevice, s->st));
+    CK(silt::op_non_finite(s->d_planes, 8, s->n, s->d_u32 + 1, s->st));
+    unsigned int c = 0;
+    CK(cudaMemcpyAsync(&c, s->d_u32 + 1, 4, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    *out = c;
+    return SILT_OK;
+}
+
+int silt_spray_m3(silt_sheet* s, double* out) {
+    if (!s || !out) return fail_arg("spray_m3");
+    *out = s->spray_m3;
+    return SILT_OK;
+}
+
+int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent) {
+    if (!s) return fail_arg("handle");
+    if (ox) *ox = s->origin[0];
+    if (oz) *oz = s->origin[1];
+    if (extent) *extent = (float)s->res * s->cfg.cell;
+    return SILT_OK;
+}
+
+static float* plane_of(silt_sheet* s, int which) {
+    switch (which) {
+        case 0: return s->H(0);
+        case 1: return s->H(1);
+        case 2: return s->U(0);
+        case 3: return s->V(0);
+        case 4: return s->U(1);
+        case 5: return s->V(1);
+        case 6: return s->bed;
+        case 7: return s->moisture;
+        default: return nullptr;
+    }
+}
+
+int silt_read_plane(silt_sheet* s, int32_t which, float* host) {
+    if (!s || !host) return fail_arg("read_plane");
+    float* p = plane_of(s, which);
+    if (!p) return fail_arg("plane index");
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(host, p, s->n * 4, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return SILT_OK;
+}
+
+int silt_write_plane(silt_sheet* s, int32_t which, const float* host) {
+    if (!s || !host) return fail_arg("write_plane");
+    float* p = plane_of(s, which);
+    if (!p) return fail_arg("plane index");
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(p, host, s->n * 4, cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (which >= 2 && which <= 5) {
+        float m = 0.0f;
+        for (size_t i = 0; i < s->n; ++i)
+            if (std::isfinite(host[i])) m = std::max(m, fabsf(host[i]));
+        s->vmax_bound = std::max(s->vmax_bound, m);
+    }
+    s->ledger_fresh = false;
+    return SILT_OK;
+}
+
+int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
+                          float* origin2) {
+    if (!s || (n > 0 && !tires) || !host) return fail_arg("fine_water_debug");
+    std::vector<silt_tire_push> ps(tires, tires + n);
+    return silt::fine::debug_patch(s->fine, s, ps, patch, host, origin2);
+}
+
+int silt_near_tiles(silt_sheet* s, int32_t* out) {
+    if (!s || !out) return fail_arg("near_tiles");
+    return silt::fine::near_tiles(s->fine, s, out);
+}
+
+int silt_set_step_timing(silt_sheet* s, int32_t on) {
+    if (!s) return fail_arg("handle");
+    CK(cudaStreamSynchronize(s->st));
+    for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
+    s->ev_used.clear();
+    memset(&s->parts, 0, sizeof s->parts);
+    s->timing = on != 0;
+    return SILT_OK;
+}
+
+int silt_get_step_parts(silt_sheet* s, silt_step_parts* out) {
+    if (!s || !out) return fail_arg("step_parts");
+    CK(cudaStreamSynchronize(s->st));
+    for (size_t k = 0; k + 2 < s->ev_used.size(); k += 3) {
+        float a = 0.0f, b = 0.0f;
+        CK(cudaEventElapsedTime(&a, s->ev_used[k], s->ev_used[k + 1]));
+        CK(cudaEventElapsedTime(&b, s->ev_used[k + 1], s->ev_used[k + 2]));
+        s->parts.force_ms += a;
+        s->parts.transport_ms += b;
+    }
+    for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
+    s->ev_used.clear();
+    *out = s->parts;
+    return SILT_OK;
+}
+
+int silt_set_fine_sub_cap(silt_sheet* s, float cap) {
+    if (!s) return fail_arg("handle");
+    s->fine.sub_cap = std::isfinite(cap) ? silt::host::rclamp(cap, 1.0f, 8.0f) : 8.0f;
+    return SILT_OK;
+}
+
+int silt_set_fine_pace(silt_sheet* s, int32_t pace) {
+    if (!s) return fail_arg("handle");
+    s->fine.pace = std::min(std::max(pace, 0), 3);
+    return SILT_OK;
+}
+
+int silt_set_near_field(silt_sheet* s, int32_t on) {
+    if (!s) return fail_arg("handle");
+    return silt::fine::set_near_field(s->fine, s, on != 0);
+}
+
+// ---------------------------------------------------------------- free operator
+size_t silt_step_sheet_scratch_bytes(int32_t res) {
+    if (res <= 0) return 0;
+    size_t n = (size_t)res * res;
+    return 256 + 3 * n * sizeof(float);
+}
+
+int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate, int32_t res,
+                    float cell, float dt, float vorticity, void* scratch, void* stream) {
+    if (!h || !u || !v || !bed || !nu || !scratch || res <= 0) return fail_arg("step_sheet");
+    if (!(dt > 0.0f)) return SILT_OK_NOOP;
+    if (!(cell > silt::host::kFineCell + 1.0e-6f))
+        return fail_arg("step_sheet: 2 cm sheets step through the window's nested patch");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = (size_t)res * res;
+    if (((uintptr_t)scratch & 15) != 0) return fail_arg("step_sheet: scratch must be 16-byte aligned");
+    // Scratch layout: [0, 32) speed bits, [32, 48) two FP64 sums, [256, ...) u, v, h planes.
+    unsigned int* d_bits = (unsigned int*)scratch;
+    double* d_sum = (double*)((char*)scratch + 32);
+    float* u_mid = (float*)((char*)scratch + 256);
+    float* v_mid = u_mid + n;
+    float* h_next = v_mid + n;
+    CK(cudaMemsetAsync(d_bits, 0, 32, st));
+    CK(silt::launch_max_speed2(h, u, v, n, 1.0e-6f, 0, d_bits, st));
+    CK(silt::op_sum2(h, h, n, d_sum, st));
+    unsigned int bits = 0;
+    double sums[2];
+    CK(cudaMemcpyAsync(&bits, d_bits, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(sums, d_sum, 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!(sums[0] > 1.0e-6)) return SILT_OK_NOOP;  // nothing wet (src/fluid_core.rs:873-879)
+    float m2;
+    memcpy(&m2, &bits, 4);
+    float max_s = std::max(0.15f, sqrtf(m2));
+    int nsub = (int)silt::host::rclamp(ceilf((dt * max_s) / (0.42f * std::max(cell, 1.0e-3f))), 1.0f, 8.0f);
+    float dts = dt / (float)nsub;
+    for (int k = 0; k < nsub; ++k) {
+        silt::ForceLaunch F;
+        silt::TransportLaunch T;
+        memset(&F, 0, sizeof F);
+        memset(&T, 0, sizeof T);
+        silt::LayerParams& P = F.lay[0];
+        P.h = h;
+        P.bed = bed;
+        P.u = u;
+        P.v = v;
+        P.u_out = u_mid;
+        P.v_out = v_mid;
+        P.nu_plane = nu;
+        P.nu_mode = silt::NU_PLANE;
+        P.res = res;
+        P.cell = cell;
+        P.dt = dts;
+        P.vort = vorticity;
+        P.eps = 1.0e-6f;
+        P.project = 1;
+        silt::TransportParams& Q = T.lay[0];
+        Q.h = h;
+        Q.u = u_mid;
+        Q.v = v_mid;
+        Q.h_out = h_next;
+        Q.gate = gate;
+        Q.res = res;
+        Q.cell = cell;
+        Q.dt = dts;
+        Q.eps = 1.0e-6f;
+        CK(silt::launch_force(F, res, 1, st));
+        CK(silt::launch_transport(T, res, 1, st));
+        CK(cudaMemcpyAsync(h, h_next, n * 4, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(u, u_mid, n * 4, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(v, v_mid, n * 4, cudaMemcpyDeviceToDevice, st));
+        CK(silt::launch_apply_cut(h, u, v, n, 1.0e-6f, st));
+    }
+    return SILT_OK;
+}
+
+}  // extern "C"
+
+// Accessors the nested-patch module uses (sheet_fine.cu).
+namespace silt {
+namespace fine {
+SheetView view_of(silt_sheet* s) {
+    SheetView w;
+    w.st = s->st;
+    w.res = s->res;
+    w.n = s->n;
+    w.cell = s->cfg.cell;
+    w.origin[0] = s->origin[0];
+    w.origin[1] = s->origin[1];
+    for (int l = 0; l < 2; ++l) {
+        w.h[l] = s->H(l);
+        w.u[l] = s->U(l);
+        w.v[l] = s->V(l);
+    }
+    w.bed = s->bed;
+    w.moisture = s->moisture;
+    w.grain = s->grain;
+    w.d_acc = s->d_acc;
+    return w;
+}
+int flush(silt_sheet* s) { return flush_cut(s); }
+void note_speed(silt_sheet* s, float bound) { s->vmax_bound = std::max(s->vmax_bound, bound); }
+void invalidate_ledger(silt_sheet* s) { s->ledger_fresh = false; }
+}  // namespace fine
+}  // namespace silt

@@ -1,0 +1,286 @@
+"""Python binding of libsilt_b200.so, the B200 sheet step behind its C ABI
+(include/silt_sheet.h).
+
+`Sheet` mirrors the reference's `FluidCore` surface on the sheet path
+(x3-team/Dirty-gen src/fluid_core.rs): seeding, push_tire, step, ledger,
+coarse_cell, export_maps and the render-contract film/flow publish. There is
+no CPU fallback: loading fails loudly when the CUDA library is missing.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsilt_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "silt_sheet.h")
+
+SILT_OK, SILT_OK_NOOP, SILT_EINVAL, SILT_ECUDA, SILT_ETIMEOUT, SILT_ENOMEM = 0, 1, -1, -2, -3, -4
+CLAY, SILT, SAND, WATER, OTHER = 0, 1, 2, 3, 4
+FINE_MEAN_PATCH, FINE_PER_TIRE = 0, 1
+
+_f = ctypes.c_float
+_i = ctypes.c_int32
+_p = ctypes.c_void_p
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [("res", _i), ("cell", _f), ("fine_res", _i), ("fine_cell", _f), ("fine_layout", _i),
+                ("tire_r", _f), ("soften_border", _i), ("center_x", _f), ("center_z", _f), ("device", _i),
+                ("stream", _p)]
+
+
+class TirePush(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("x", "z", "forward_x", "forward_z", "radius", "width", "speed", "slip")]
+
+
+class SprayEvent(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("x", "y", "z", "vx", "vy", "vz", "volume")] + [("kind", _i)]
+
+
+class Ledger(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3",
+                                               "spray_m3", "opened_m3", "total_m3")]
+
+
+class CoarseCell(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("x", "z", "bed_m", "water_m", "slurry_m", "moisture", "u", "v")]
+
+
+class StepParts(ctypes.Structure):
+    _fields_ = [("force_ms", ctypes.c_double), ("transport_ms", ctypes.c_double), ("fine_ms", ctypes.c_double),
+                ("steps", ctypes.c_int64), ("launches", ctypes.c_int64), ("force_launches", ctypes.c_int64),
+                ("force_cells", ctypes.c_int64)]
+
+
+class SiltError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def header_functions():
+    """Names of every function include/silt_sheet.h declares."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|size_t|const char\*)\s+(silt_\w+)\s*\(", text, re.M)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SiltError(f"{LIB_PATH} is missing: build it with `make -C dirty-gen_b200` (no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.silt_last_error.restype = ctypes.c_char_p
+        L.silt_cfg_default.argtypes = [ctypes.POINTER(Cfg)]
+        L.silt_cfg_default.restype = None
+        L.silt_sheet_create.argtypes = [ctypes.POINTER(Cfg), ctypes.POINTER(_p)]
+        for name, args in {
+            "silt_sheet_destroy": [_p], "silt_sheet_sync": [_p],
+            "silt_map_water_bed": [_p, _p, _p, _p], "silt_map_grain": [_p, _p],
+            "silt_map_water_velocity": [_p, _p, _p],
+            "silt_pour_water": [_p, _f, _f, _f, _f, _f, _p],
+            "silt_pour_slurry": [_p, _f, _f, _f, _f, _f, _i, _f, _p],
+            "silt_lay_slurry_mask": [_p, _p, _i, _f, _p],
+            "silt_read_substrate_grid": [_p, _p, _p, _p],
+            "silt_set_inflow": [_p, _i, _f, _f, _f],
+            "silt_push_tire": [_p, ctypes.POINTER(TirePush)],
+            "silt_step": [_p, _f, _p, _i, ctypes.POINTER(_i)],
+            "silt_get_ledger": [_p, ctypes.POINTER(Ledger)],
+            "silt_get_coarse_cell": [_p, _i, _i, ctypes.POINTER(CoarseCell)],
+            "silt_export_maps": [_p, _p, _p, _p, _p],
+            "silt_publish_film_flow": [_p, _p, _p],
+            "silt_publish_film_flow_device": [_p, _p, _p],
+            "silt_non_finite_count": [_p, ctypes.POINTER(ctypes.c_uint32)],
+            "silt_spray_m3": [_p, ctypes.POINTER(ctypes.c_double)],
+            "silt_window_bounds": [_p, _p, _p, _p],
+            "silt_read_plane": [_p, _i, _p], "silt_write_plane": [_p, _i, _p],
+            "silt_fine_water_debug": [_p, _p, _i, _i, _p, _p],
+            "silt_near_tiles": [_p, ctypes.POINTER(_i)],
+            "silt_set_fine_sub_cap": [_p, _f], "silt_set_fine_pace": [_p, _i], "silt_set_near_field": [_p, _i],
+            "silt_step_sheet": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p, _p],
+            "silt_set_step_timing": [_p, _i], "silt_get_step_parts": [_p, ctypes.POINTER(StepParts)],
+        }.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.silt_step_sheet_scratch_bytes.argtypes = [_i]
+        L.silt_step_sheet_scratch_bytes.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def check(rc, what=""):
+    if rc < 0:
+        raise SiltError(f"{what}: rc={rc} {lib().silt_last_error().decode()}")
+    return rc
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+PLANES = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7}
+
+
+def make_push(t):
+    return TirePush(t["x"], t["z"], t.get("forward_x", 0.0), t.get("forward_z", 1.0), t["radius"], t["width"],
+                    t["speed"], t.get("slip", 0.0))
+
+
+class Sheet:
+    """A window of the two-layer sheet on the GPU (FluidCore, src/fluid_core.rs:4808)."""
+
+    def __init__(self, res=200, cell=0.2, fine_res=160, fine_cell=0.02, layout=FINE_MEAN_PATCH, tire_r=0.56,
+                 soften=True, center=(0.0, 0.0), device=0, stream=None):
+        L = lib()
+        cfg = Cfg()
+        L.silt_cfg_default(ctypes.byref(cfg))
+        cfg.res, cfg.cell, cfg.fine_res, cfg.fine_cell = res, cell, fine_res, fine_cell
+        cfg.fine_layout, cfg.tire_r, cfg.soften_border = layout, tire_r, int(soften)
+        cfg.center_x, cfg.center_z, cfg.device = center[0], center[1], device
+        cfg.stream = stream
+        h = _p()
+        check(L.silt_sheet_create(ctypes.byref(cfg), ctypes.byref(h)), "silt_sheet_create")
+        self.h = h
+        self.res = res
+        self.fine_res = fine_res
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().silt_sheet_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def sync(self):
+        check(lib().silt_sheet_sync(self.h), "sync")
+
+    def map_water_bed(self, bed, water):
+        vol = _f(0)
+        check(lib().silt_map_water_bed(self.h, _ptr(_f32(bed)), _ptr(_f32(water)), ctypes.byref(vol)), "map_water_bed")
+        return vol.value
+
+    def map_grain(self, grain):
+        check(lib().silt_map_grain(self.h, _ptr(np.ascontiguousarray(grain, np.uint8))), "map_grain")
+
+    def map_water_velocity(self, u, v):
+        check(lib().silt_map_water_velocity(self.h, _ptr(_f32(u)), _ptr(_f32(v))), "map_water_velocity")
+
+    def pour_water(self, x0, x1, z0, z1, depth):
+        vol = _f(0)
+        check(lib().silt_pour_water(self.h, x0, x1, z0, z1, depth, ctypes.byref(vol)), "pour_water")
+        return vol.value
+
+    def pour_slurry(self, x0, x1, z0, z1, depth, grain, moisture):
+        vol = _f(0)
+        check(lib().silt_pour_slurry(self.h, x0, x1, z0, z1, depth, grain, moisture, ctypes.byref(vol)), "pour_slurry")
+        return vol.value
+
+    def lay_slurry_mask(self, depth, grain, moisture):
+        vol = _f(0)
+        check(lib().silt_lay_slurry_mask(self.h, _ptr(_f32(depth)), grain, moisture, ctypes.byref(vol)), "lay_slurry")
+        return vol.value
+
+    def read_substrate(self, bed, moisture, grain):
+        check(lib().silt_read_substrate_grid(self.h, _ptr(_f32(bed)), _ptr(_f32(moisture)),
+                                             _ptr(np.ascontiguousarray(grain, np.uint8))), "read_substrate_grid")
+
+    def set_inflow(self, j, x0, x1, rate_m3_s):
+        check(lib().silt_set_inflow(self.h, j, x0, x1, rate_m3_s), "set_inflow")
+
+    def push_tire(self, **t):
+        p = make_push(t)
+        check(lib().silt_push_tire(self.h, ctypes.byref(p)), "push_tire")
+
+    def step(self, dt, want_spray=True, cap=65536):
+        n = _i(0)
+        if not want_spray:
+            check(lib().silt_step(self.h, dt, None, 0, None), "step")
+            return None
+        buf = (SprayEvent * cap)()
+        check(lib().silt_step(self.h, dt, buf, cap, ctypes.byref(n)), "step")
+        return [(e.x, e.y, e.z, e.vx, e.vy, e.vz, e.volume, e.kind) for e in buf[:min(n.value, cap)]]
+
+    def ledger(self):
+        led = Ledger()
+        check(lib().silt_get_ledger(self.h, ctypes.byref(led)), "ledger")
+        return {k: getattr(led, k) for k, _ in Ledger._fields_}
+
+    def coarse_cell(self, i, j):
+        c = CoarseCell()
+        rc = check(lib().silt_get_coarse_cell(self.h, i, j, ctypes.byref(c)), "coarse_cell")
+        return None if rc == SILT_OK_NOOP else {k: getattr(c, k) for k, _ in CoarseCell._fields_}
+
+    def get(self, name):
+        out = np.zeros(self.res * self.res, np.float32)
+        check(lib().silt_read_plane(self.h, PLANES[name], _ptr(out)), "read_plane")
+        return out
+
+    def set(self, name, arr):
+        check(lib().silt_write_plane(self.h, PLANES[name], _ptr(_f32(arr))), "write_plane")
+
+    def export_maps(self):
+        n = self.res * self.res
+        out = [np.zeros(n, np.float32) for _ in range(4)]
+        check(lib().silt_export_maps(self.h, *[_ptr(o) for o in out]), "export_maps")
+        return dict(zip(("height", "vel_u", "vel_v", "moisture"), out))
+
+    def publish(self):
+        film = np.zeros(2 * self.res * self.res, np.float32)
+        flow = np.zeros(4 * self.res * self.res, np.float32)
+        check(lib().silt_publish_film_flow(self.h, _ptr(film), _ptr(flow)), "publish")
+        return film, flow
+
+    def non_finite_count(self):
+        c = ctypes.c_uint32(0)
+        check(lib().silt_non_finite_count(self.h, ctypes.byref(c)), "non_finite_count")
+        return c.value
+
+    def spray_m3(self):
+        d = ctypes.c_double(0)
+        check(lib().silt_spray_m3(self.h, ctypes.byref(d)), "spray_m3")
+        return d.value
+
+    def set_fine_pace(self, pace):
+        check(lib().silt_set_fine_pace(self.h, pace), "set_fine_pace")
+
+    def set_fine_sub_cap(self, cap):
+        check(lib().silt_set_fine_sub_cap(self.h, cap), "set_fine_sub_cap")
+
+    def set_near_field(self, on):
+        check(lib().silt_set_near_field(self.h, int(on)), "set_near_field")
+
+    def near_tiles(self):
+        c = _i(0)
+        check(lib().silt_near_tiles(self.h, ctypes.byref(c)), "near_tiles")
+        return c.value
+
+    def set_step_timing(self, on):
+        check(lib().silt_set_step_timing(self.h, int(on)), "set_step_timing")
+
+    def step_parts(self):
+        sp = StepParts()
+        check(lib().silt_get_step_parts(self.h, ctypes.byref(sp)), "step_parts")
+        return {k: getattr(sp, k) for k, _ in StepParts._fields_}
+
+    def fine_water_debug(self, tires, patch=0):
+        arr = (TirePush * max(len(tires), 1))()
+        for k, t in enumerate(tires):
+            arr[k] = make_push(t)
+        out = np.zeros(self.fine_res * self.fine_res, np.float32)
+        org = np.zeros(2, np.float32)
+        check(lib().silt_fine_water_debug(self.h, arr, len(tires), patch, _ptr(out), _ptr(org)), "fine_water_debug")
+        return out, org
+
+
+def step_sheet_device(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream=None):
+    """The free one-sheet operator on device pointers (ints)."""
+    return check(lib().silt_step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream),
+                 "step_sheet")

@@ -1,0 +1,184 @@
+/* silt_sheet.h -- C ABI of the B200 two-layer (water + slurry) sheet step.
+ *
+ * Drop-in for the sheet path of x3-team/Dirty-gen's `FluidCore`
+ * (src/fluid_core.rs). Each entry point names the reference interface it
+ * replaces. The handle owns the device state (SoA float planes in HBM); the
+ * caller owns every host buffer passed in. Seeding arrays are the values the
+ * reference's closures would return, one per coarse cell, row-major j*res+i.
+ *
+ * Threading: one handle per CUDA stream, not thread-safe. All work is queued
+ * on the handle's stream; calls that return host data synchronise it.
+ *
+ * Errors: the reference returns silently on dt <= 0 and similar no-ops; here
+ * those return SILT_OK_NOOP. Bad pointers or sizes return SILT_EINVAL, a CUDA
+ * failure SILT_ECUDA, a device wait past its limit SILT_ETIMEOUT.
+ */
+#ifndef SILT_SHEET_H
+#define SILT_SHEET_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SILT_OK 0
+#define SILT_OK_NOOP 1
+#define SILT_EINVAL (-1)
+#define SILT_ECUDA (-2)
+#define SILT_ETIMEOUT (-3)
+#define SILT_ENOMEM (-4)
+
+/* Grain codes, src/fluid_core.rs:116-124 (`Grain`). */
+#define SILT_GRAIN_CLAY 0
+#define SILT_GRAIN_SILT 1
+#define SILT_GRAIN_SAND 2
+#define SILT_GRAIN_WATER 3
+#define SILT_GRAIN_OTHER 4
+
+/* Nested 2 cm layout: 0 = one patch centred on the mean tire (the reference,
+ * src/fluid_core.rs:8358), 1 = one patch per tire. */
+#define SILT_FINE_MEAN_PATCH 0
+#define SILT_FINE_PER_TIRE 1
+
+typedef struct silt_sheet silt_sheet;
+
+/* Window geometry and options. Defaults (silt_cfg_default) are the
+ * reference constants: 200 cells of 0.20 m (src/fluid_core.rs:69-72), a 160
+ * cell 2 cm patch (:73-76), held radius 0.56 m (:80), soft window border
+ * (:9594). */
+typedef struct {
+    int32_t res;          /* coarse cells per side */
+    float cell;           /* coarse cell, m */
+    int32_t fine_res;     /* fine cells per patch side */
+    float fine_cell;      /* fine cell, m; cell / fine_cell must be a whole number */
+    int32_t fine_layout;  /* SILT_FINE_MEAN_PATCH or SILT_FINE_PER_TIRE */
+    float tire_r;         /* held-column radius around a tire, m */
+    int32_t soften_border;/* 1: slow the velocity in the window's edge band each step */
+    float center_x;       /* window centre, m (FluidCore::new(center)) */
+    float center_z;
+    int32_t device;       /* CUDA device ordinal */
+    void* stream;         /* cudaStream_t to queue on; NULL makes a private stream */
+} silt_cfg;
+
+/* One tire shoving the sheet, src/fluid_core.rs:359-368 (`TirePush`). */
+typedef struct {
+    float x, z, forward_x, forward_z, radius, width, speed, slip;
+} silt_tire_push;
+
+/* Volume peeled off the water sheet, src/fluid_core.rs:372-382 (`SprayEvent`). */
+typedef struct {
+    float x, y, z, vx, vy, vz, volume;
+    int32_t kind;
+} silt_spray_event;
+
+/* Volume books, src/fluid_core.rs:485-509 (`FluidLedger`), the sheet part,
+ * accumulated in FP64. `opened_m3` is water added by an inflow strip. */
+typedef struct {
+    double water_m3, slurry_m3, frozen_water_m3, frozen_slurry_m3, spray_m3, opened_m3, total_m3;
+} silt_ledger;
+
+/* src/fluid_core.rs:452-465 (`CoarseCell`), sheet fields. */
+typedef struct {
+    float x, z, bed_m, water_m, slurry_m, moisture, u, v;
+} silt_coarse_cell;
+
+/* -------------------------------------------------------------- lifecycle */
+void silt_cfg_default(silt_cfg* cfg);
+/* FluidCore::new (src/fluid_core.rs:4958). */
+int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out);
+int silt_sheet_destroy(silt_sheet* s);
+/* Waits for all queued work. */
+int silt_sheet_sync(silt_sheet* s);
+/* Last CUDA error string for this thread ("" when none). */
+const char* silt_last_error(void);
+
+/* ---------------------------------------------------------------- seeding */
+/* FluidCore::map_water_bed (src/fluid_core.rs:5329); vol_out may be NULL. */
+int silt_map_water_bed(silt_sheet* s, const float* bed, const float* water, float* vol_out);
+/* FluidCore::map_grain (src/fluid_core.rs:5318). */
+int silt_map_grain(silt_sheet* s, const uint8_t* grain);
+/* FluidCore::map_water_velocity (src/fluid_core.rs:5358). */
+int silt_map_water_velocity(silt_sheet* s, const float* u, const float* v);
+/* FluidCore::pour_water / pour_slurry (src/fluid_core.rs:5424, :5428). */
+int silt_pour_water(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, float* vol_out);
+int silt_pour_slurry(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, int32_t grain,
+                     float moisture, float* vol_out);
+/* FluidCore::lay_slurry_mask (src/fluid_core.rs:5857). */
+int silt_lay_slurry_mask(silt_sheet* s, const float* depth, int32_t grain, float moisture, float* vol_out);
+/* FluidCore::read_substrate_grid (src/fluid_core.rs:5928). */
+int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moisture, const uint8_t* grain);
+/* Inflow strip on coarse row j over world x in [x0, x1), rate m^3/s; rate 0 turns it off.
+ * No reference counterpart (the reference has no inflow source); booked as opened_m3. */
+int silt_set_inflow(silt_sheet* s, int32_t j, float x0, float x1, float rate_m3_s);
+
+/* --------------------------------------------------------------- per step */
+/* FluidCore::push_tire (src/fluid_core.rs:5964). */
+int silt_push_tire(silt_sheet* s, const silt_tire_push* push);
+/* FluidCore::step (src/fluid_core.rs:6034), sheet path. Writes up to `cap`
+ * spray events to `out` (may be NULL when cap is 0) and the total count to
+ * n_out (may be NULL). Synchronises only when events are requested. */
+int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32_t* n_out);
+
+/* ------------------------------------------------------------------ reads */
+/* FluidCore::ledger (src/fluid_core.rs:6821), FP64. */
+int silt_get_ledger(silt_sheet* s, silt_ledger* out);
+/* FluidCore::coarse_cell (src/fluid_core.rs:6998). Returns SILT_OK_NOOP outside the window. */
+int silt_get_coarse_cell(silt_sheet* s, int32_t i, int32_t j, silt_coarse_cell* out);
+/* FluidCore::export_maps (src/fluid_core.rs:6941): height, vel_u, vel_v, moisture (res*res each; any may be NULL). */
+int silt_export_maps(silt_sheet* s, float* height, float* vel_u, float* vel_v, float* moisture);
+/* render_contract::publish_with_snow film/flow (src/render_contract.rs:483-496):
+ * film = (water, slurry) per cell, flow = (vx, vz, speed, turbidity). Host pointers. */
+int silt_publish_film_flow(silt_sheet* s, float* film, float* flow);
+/* Same maps into device memory the caller owns (2*res*res and 4*res*res floats). */
+int silt_publish_film_flow_device(silt_sheet* s, float* d_film, float* d_flow);
+/* FluidCore::non_finite_count (src/fluid_core.rs:5374), sheet planes. */
+int silt_non_finite_count(silt_sheet* s, uint32_t* out);
+/* FluidCore::spray_m3 (src/fluid_core.rs:6817). */
+int silt_spray_m3(silt_sheet* s, double* out);
+/* FluidCore::window_bounds (src/fluid_core.rs:6977): origin x, origin z, extent. */
+int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
+/* Raw plane copy to host for tests and tools: which = 0 water, 1 slurry, 2 uw,
+ * 3 vw, 4 us, 5 vs, 6 bed, 7 moisture. */
+int silt_read_plane(silt_sheet* s, int32_t which, float* host);
+int silt_write_plane(silt_sheet* s, int32_t which, const float* host);
+/* FluidCore::fine_water_debug (src/fluid_core/near.rs:341): lays the patch
+ * down for these tires, copies patch `patch` (fine_res^2 floats) and its
+ * origin, and packs it back. */
+int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
+                          float* origin2);
+/* FluidCore::near_tiles (src/fluid_core/near.rs:328). */
+int silt_near_tiles(silt_sheet* s, int32_t* out);
+
+/* Device time per kernel family since timing was last switched on, measured
+ * with CUDA events on the handle's stream. The GPU counterpart of
+ * FluidCore::step_parts (src/fluid_core.rs:4782-4795, :6130). `launches`
+ * counts this library's kernel launches (always counted). */
+typedef struct {
+    double force_ms, transport_ms, fine_ms;
+    int64_t steps, launches, force_launches, force_cells;
+} silt_step_parts;
+int silt_set_step_timing(silt_sheet* s, int32_t on);
+int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
+
+/* ------------------------------------------------------------------ knobs */
+/* FluidCore::set_fine_sub_cap / set_fine_pace (src/fluid_core.rs:5072, :5085). */
+int silt_set_fine_sub_cap(silt_sheet* s, float cap);
+int silt_set_fine_pace(silt_sheet* s, int32_t pace);
+/* FluidCore::set_near_field (src/fluid_core/near.rs:332). */
+int silt_set_near_field(silt_sheet* s, int32_t on);
+
+/* ------------------------------------------------------ one-sheet operator */
+/* Free `step_sheet` (src/fluid_core.rs:770) with the gravity drive on caller
+ * device arrays (res*res each): h, u, v updated in place; bed, nu, gate read.
+ * `scratch` is device memory of silt_step_sheet_scratch_bytes(res) bytes the
+ * caller allocates once; stream is a cudaStream_t (NULL = legacy stream). */
+size_t silt_step_sheet_scratch_bytes(int32_t res);
+int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
+                    int32_t res, float cell, float dt, float vorticity, void* scratch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SILT_SHEET_H */

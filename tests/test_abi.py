@@ -1,0 +1,26 @@
+"""The C ABI library builds for sm_100a, loads without a GPU, and exports
+every function include/silt_sheet.h declares."""
+import ctypes
+import os
+import subprocess
+
+import silt_b200
+
+
+def test_library_exports_every_declared_symbol():
+    names = silt_b200.header_functions()
+    assert len(names) >= 30
+    lib = ctypes.CDLL(silt_b200.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_is_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", silt_b200.LIB_PATH], capture_output=True, text=True)
+    assert "sm_100a" in out.stdout, out.stdout + out.stderr
+
+
+def test_binding_declares_every_header_function():
+    lib = silt_b200.lib()
+    for n in silt_b200.header_functions():
+        assert getattr(lib, n).restype is not None or n in ("silt_cfg_default",)
