@@ -1,48 +1,1318 @@
-// Nested 2 cm patches (placeholder until the patch kernels land): the window
-// steps without tires; a tire push is refused.
+// Nested 2 cm patches and their two-way coupling with the coarse window
+// (x3-team/Dirty-gen src/fluid_core.rs:8152-8566 and src/fluid_core/near.rs).
+//
+// The host decides the geometry each step from the tire positions: patch
+// origins, the fine-to-coarse axes, the held columns, the near-field columns
+// and which tire shoves which grid. Those small tables go to the device in
+// one copy; the kernels below then move all cell data on the device:
+//
+//   k_refine_lay    coarse -> fine copy of held columns, free-surface bed elsewhere
+//   k_zero_cells    empty the held coarse columns
+//   k_near_apply    lay the kept 10x10 residual tiles back on the patch
+//   k_near_fade     age tiles whose column is not held; recycle dropped slots
+//   k_push_cells    tire shove on velocity, pushes applied in call order
+//   (sheet_patch.cu k_patch_step: the fine sheet step itself)
+//   k_peel          spray peeled off the water, events queued on the device
+//   k_near_capture  residual tiles of held columns
+//   k_restrict      volume- and momentum-weighted sum back into the columns
+//   k_park          fine volume outside the window, booked as parked
+//
+// Near-field tiles live in a device pool with a slot per coarse cell; slots
+// are taken in k_near_capture and returned in k_near_fade, so no kernel both
+// pushes and pops the free stack.
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
 #include "sheet_fine.cuh"
+#include "sheet_host_math.h"
+#include "sheet_math.cuh"
+#include "sheet_patch.cuh"
 
 namespace silt {
 namespace fine {
 
-struct PatchState {};
+namespace {
+
+constexpr int MAX_PATCHES = 16;
+constexpr int NEAR_POOL = 16384;
+constexpr int SPRAY_CAP = 1 << 16;
+constexpr float NEAR_LIFE_S = 1.5f;      // near.rs:37
+constexpr float NEAR_DROP_M = 1.0e-5f;   // near.rs:39
+constexpr float NEAR_FILM_M = 1.0e-6f;   // near.rs:41
+
+thread_local char g_err[200] = "";
+
+#define FCK(call)                                                                     \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            snprintf(g_err, sizeof g_err, "%s: %s", #call, cudaGetErrorString(e_));   \
+            return SILT_ECUDA;                                                        \
+        }                                                                             \
+    } while (0)
+
+}  // namespace
+
+// Device planes of one patch.
+struct PatchState {
+    float* base = nullptr;
+    float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
+    uint8_t* grain;
+    float* sc[2][2][5];   // [layer][set][a..e]
+    float* tmp[2][2];     // [layer][f1, f2]
+    // Host geometry of the current step.
+    float origin[2] = {0, 0};
+    std::vector<int16_t> col, row;
+};
+
+struct PatchRef {
+    float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
+    uint8_t* grain;
+    const int16_t* col;
+    const int16_t* row;
+    float ox, oz;
+};
+
+struct NearCol {
+    int cidx, patch, i0, j0, inner, pad;
+};
+
+struct RestrictEntry {
+    int cidx, cnt, held, seg_off, seg_n, pad;
+};
+
+struct Segment {
+    int patch, i0, i1, j0, j1, pad;
+};
+
+struct PushJob {
+    float x, z, fx, fz, radius, width, speed, slip;
+    int span_i0, span_i1, span_j0, span_j1;  // half-open index spans (index_span)
+    int index;                               // position in the call order
+    int pad[3];
+};
+
+struct SprayRec {
+    float x, y, z, vx, vy, vz, volume;
+    int kind;
+    unsigned long long key;
+};
+
+struct NearMeta {
+    int state;   // 0 free, 1 live, 2 released (back to the free stack at the next fade)
+    int key;     // coarse cell index
+    int fresh;
+    float idle_s;
+    float peak;
+    int pad[3];
+};
+
+struct Impl {
+    int res = 0;
+    int8_t* owner = nullptr;          // per coarse cell: patch that holds it, -1 none
+    std::vector<int8_t> h_owner;      // host mirror
+    std::vector<int> held_now;        // coarse cells held by the last laid patches
+    patch::Job* d_jobs = nullptr;
+    void* host = nullptr;             // HostState: the step plan and its table buffers
+    // Near-field pool.
+    int* slot_map = nullptr;          // per coarse cell
+    float* pool = nullptr;            // NEAR_POOL x 4 x sub^2
+    NearMeta* meta = nullptr;
+    int* free_stack = nullptr;
+    int* counters = nullptr;          // [0] free top, [1] live tiles, [2] overflow, [3] spray count
+    bool near_maybe = false;
+    // Spray.
+    SprayRec* spray = nullptr;
+    double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3
+    double* h_books = nullptr;
+    int* h_counters = nullptr;
+};
+
+static Impl& I(Patches& P) { return *reinterpret_cast<Impl*>(P.impl); }
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_scatter_owner(int8_t* owner, const int* idx, const int8_t* val, int n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) owner[idx[k]] = val[k];
+}
+
+// refine (src/fluid_core.rs:8358-8460), the per-fine-cell copy.
+__global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W, const int8_t* owner) {
+    const size_t fn = (size_t)fres * fres;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(k / fn);
+        const int f = (int)(k % fn);
+        const PatchRef& R = refs[p];
+        R.water[f] = 0.0f;
+        R.slurry[f] = 0.0f;
+        R.uw[f] = 0.0f;
+        R.vw[f] = 0.0f;
+        R.us[f] = 0.0f;
+        R.vs[f] = 0.0f;
+        const int ci = R.col[f % fres], cj = R.row[f / fres];
+        if (ci < 0 || cj < 0) continue;
+        const size_t c = (size_t)cj * W.res + ci;
+        R.moisture[f] = W.moisture[c];
+        R.grain[f] = W.grain[c];
+        if (owner[c] != p) {
+            R.bed[f] = W.bed[c] + W.h[0][c];
+            R.bed_slurry[f] = W.bed[c] + W.h[1][c];
+            continue;
+        }
+        R.bed[f] = W.bed[c];
+        R.bed_slurry[f] = W.bed[c];
+        R.water[f] = W.h[0][c];
+        R.slurry[f] = W.h[1][c];
+        R.uw[f] = W.u[0][c];
+        R.vw[f] = W.v[0][c];
+        R.us[f] = W.u[1][c];
+        R.vs[f] = W.v[1][c];
+    }
+}
+
+__global__ void k_zero_cells(SheetView W, const int* cells, int n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    size_t c = cells[k];
+    W.h[0][c] = 0.0f;
+    W.h[1][c] = 0.0f;
+    W.u[0][c] = 0.0f;
+    W.v[0][c] = 0.0f;
+    W.u[1][c] = 0.0f;
+    W.v[1][c] = 0.0f;
+}
+
+__device__ __forceinline__ float tile_left(float idle) { return idle <= 0.0f ? 1.0f : expf(-idle / NEAR_LIFE_S); }
+
+// near.rs:139-148 floor_scale on one residual.
+__device__ float floor_scale(float base, const float* r, int n) {
+    float low = 0.0f;
+    for (int k = 0; k < n; ++k) low = fminf(low, r[k]);
+    if (low >= 0.0f || base + low >= 0.0f) return 1.0f;
+    if (base <= 0.0f) return 0.0f;
+    return rclamp(base / -low, 0.0f, 1.0f);
+}
+
+// near_apply (near.rs:276-308): one block per held near column.
+__global__ void k_near_apply(const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol,
+                             const int* slot_map, const float* pool, const NearMeta* meta) {
+    const int q = blockIdx.x;
+    if (q >= ncol) return;
+    const NearCol C = cols[q];
+    const int slot = slot_map[C.cidx];
+    if (slot < 0 || meta[slot].state != 1) return;
+    const int n2 = sub * sub;
+    const float* tw = pool + (size_t)slot * 4 * n2;
+    const float* ts = tw + n2;
+    const float* tuw = ts + n2;
+    const float* tvw = tuw + n2;
+    const PatchRef& R = refs[C.patch];
+    __shared__ float scale[2];
+    const int f0 = C.j0 * fres + C.i0;
+    const float bw = R.water[f0], bs = R.slurry[f0];
+    const float left = tile_left(meta[slot].idle_s);
+    if (threadIdx.x == 0) {
+        scale[0] = left * floor_scale(bw / fmaxf(left, 1.0e-6f), tw, n2);
+        scale[1] = left * floor_scale(bs / fmaxf(left, 1.0e-6f), ts, n2);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+        const int b = k / sub, a = k % sub;
+        const int f = (C.j0 + b) * fres + C.i0 + a;
+        float w = fmaxf(bw + scale[0] * tw[k], 0.0f);
+        float s = fmaxf(bs + scale[1] * ts[k], 0.0f);
+        R.water[f] = w;
+        R.slurry[f] = s;
+        if (C.inner && w > NEAR_FILM_M) {
+            R.uw[f] += left * tuw[k];
+            R.vw[f] += left * tvw[k];
+        }
+    }
+}
+
+// near_fade (near.rs:311-325) and slot recycling.
+__global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int* counters, float dt) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= NEAR_POOL) return;
+    NearMeta& M = meta[s];
+    if (M.state == 1) {
+        if (M.fresh) {
+            M.fresh = 0;
+        } else {
+            M.idle_s += dt;
+            if (!(M.peak * tile_left(M.idle_s) > NEAR_DROP_M)) {
+                slot_map[M.key] = -1;
+                M.state = 2;
+                atomicSub(&counters[1], 1);
+            }
+        }
+    }
+    if (M.state == 2) {
+        int top = atomicAdd(&counters[0], 1);
+        free_stack[top] = s;
+        M.state = 0;
+    }
+}
+
+// push_on (src/fluid_core.rs:8169-8239); every thread owns one cell of the
+// pushes' joint span and applies the pushes in call order.
+__global__ void k_push_cells(float* w, float* s, float* uw, float* vw, float* us, float* vs, int res, float cell,
+                             float ox, float oz, const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= bw * bh) return;
+    const int i = bi0 + k % bw, j = bj0 + k / bw;
+    const size_t idx = (size_t)j * res + i;
+    for (int q = 0; q < njobs; ++q) {
+        const PushJob p = jobs[q];
+        if (i < p.span_i0 || i >= p.span_i1 || j < p.span_j0 || j >= p.span_j1) continue;
+        float fx = p.fx, fz = p.fz;
+        float len = fmaxf(sqrtf(fx * fx + fz * fz), 1.0e-4f);
+        fx = fx / len;
+        fz = fz / len;
+        const float rx = fz, rz = -fx;
+        const float speed = fmaxf(p.speed, 0.0f);
+        const float x = ox + ((float)i + 0.5f) * cell;
+        const float z = oz + ((float)j + 0.5f) * cell;
+        const float dx = x - p.x, dz = z - p.z;
+        const float along = dx * fx + dz * fz;
+        const float lat = dx * rx + dz * rz;
+        if (fabsf(lat) > p.width * 0.65f + cell) continue;
+        if (along < -p.radius * 1.4f || along > p.radius * 1.1f) continue;
+        const float flank = rclamp(fabsf(lat) / (p.width * 0.65f + cell), 0.0f, 1.0f);
+        const float shove = fmaxf(speed, 0.4f) * (1.0f - flank * flank);
+        const float sg = isnan(lat) ? lat : (signbit(lat) ? -1.0f : 1.0f);  // f32::signum
+        if (w[idx] > 0.004f) {
+            uw[idx] += fx * shove * 0.85f;
+            vw[idx] += fz * shove * 0.85f;
+            uw[idx] += rx * sg * shove * 0.18f * flank;
+            vw[idx] += rz * sg * shove * 0.18f * flank;
+        }
+        if (s[idx] > 0.004f) {
+            const float fore = along > 0.0f ? 1.0f : 0.72f;
+            us[idx] += fx * shove * fore;
+            vs[idx] += fz * shove * fore;
+            us[idx] += rx * sg * shove * 0.28f * flank;
+            vs[idx] += rz * sg * shove * 0.28f * flank;
+        }
+    }
+}
+
+// peel_spray (src/fluid_core.rs:8241-8314). Events carry a sort key that
+// restores the reference's order (phase, patch, push, row, column).
+__global__ void k_peel(float* w, const float* uw, const float* vw, int res, float cell, float ox, float oz,
+                       const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh, const int8_t* owner,
+                       int coarse_res, float cox, float coz, float coarse_cell, int phase, int patch, SprayRec* out,
+                       int* counters, double* books, double* ledger_depth) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= bw * bh) return;
+    const int i = bi0 + k % bw, j = bj0 + k / bw;
+    const size_t idx = (size_t)j * res + i;
+    const float area = cell * cell;
+    for (int q = 0; q < njobs; ++q) {
+        const PushJob p = jobs[q];
+        if (p.speed < 0.8f) continue;
+        if (i < p.span_i0 || i >= p.span_i1 || j < p.span_j0 || j >= p.span_j1) continue;
+        const float x = ox + ((float)i + 0.5f) * cell;
+        const float z = oz + ((float)j + 0.5f) * cell;
+        if (owner) {  // skip the held columns (coarse_held, src/fluid_core.rs:9664-9672)
+            float ci = floorf((x - cox) / coarse_cell), cj = floorf((z - coz) / coarse_cell);
+            if (!(ci < 0.0f || cj < 0.0f)) {
+                int ii = (int)ci, jj = (int)cj;
+                if (ii < coarse_res && jj < coarse_res && owner[(size_t)jj * coarse_res + ii] >= 0) continue;
+            }
+        }
+        const float dx = x - p.x, dz = z - p.z;
+        if (dx * dx + dz * dz > (p.radius * 1.3f) * (p.radius * 1.3f)) continue;
+        if (w[idx] < 0.01f) continue;
+        const float take = fminf(w[idx] * 0.04f, 0.004f);
+        if (take * area < 1.0e-6f) continue;
+        w[idx] -= take;
+        int slot = atomicAdd(&counters[3], 1);
+        atomicAdd(&books[0], (double)(take * area));
+        if (ledger_depth) atomicAdd(ledger_depth, -(double)take);
+        if (slot < SPRAY_CAP) {
+            SprayRec r;
+            r.x = x;
+            r.y = 0.35f;
+            r.z = z;
+            r.vx = uw[idx] * 0.3f;
+            r.vy = 1.4f + p.speed * 0.25f;
+            r.vz = vw[idx] * 0.3f;
+            r.volume = take * area;
+            r.kind = 0;
+            r.key = ((unsigned long long)phase << 60) | ((unsigned long long)patch << 54) |
+                    ((unsigned long long)p.index << 44) | ((unsigned long long)j << 22) | (unsigned long long)i;
+            out[slot] = r;
+        }
+    }
+}
+
+// near_capture (near.rs:199-273): one block of 128 threads per held near column.
+__global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol, int* slot_map,
+                               float* pool, NearMeta* meta, int* free_stack, int* counters) {
+    const int q = blockIdx.x;
+    if (q >= ncol) return;
+    const NearCol C = cols[q];
+    const PatchRef& R = refs[C.patch];
+    const int n2 = sub * sub;
+    __shared__ float bw_[1024], bs_[1024], bu_[1024], bv_[1024];
+    __shared__ int decision;   // 0 remove, 1 keep
+    __shared__ int slot_s;
+    __shared__ float mw_s, ms_s, uu_s, vv_s, peak_s, sw_s;
+    __shared__ double mean_w, mean_s;
+    for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+        const int f = (C.j0 + k / sub) * fres + C.i0 + k % sub;
+        bw_[k] = R.water[f];
+        bs_[k] = R.slurry[f];
+        bu_[k] = R.uw[f];
+        bv_[k] = R.vw[f];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // Column sums: each row of `sub` summed from -0.0, rows added in order.
+        float sw = 0.0f, ss = 0.0f;
+        for (int b = 0; b < sub; ++b) {
+            float rw = -0.0f, rs = -0.0f;
+            for (int a = 0; a < sub; ++a) {
+                rw += bw_[b * sub + a];
+                rs += bs_[b * sub + a];
+            }
+            sw += rw;
+            ss += rs;
+        }
+        int keep = 1;
+        if (sw <= 0.0f && ss <= 0.0f) keep = 0;
+        const float nn = (float)n2;
+        const float mw = sw / nn, ms = ss / nn;
+        // abs_peak with four lanes (near.rs:128-137).
+        float hw[4] = {0, 0, 0, 0}, hs[4] = {0, 0, 0, 0};
+        for (int c = 0; c + 4 <= n2; c += 4)
+            for (int l = 0; l < 4; ++l) {
+                float a = fabsf(bw_[c + l] - mw);
+                hw[l] = a > hw[l] ? a : hw[l];
+                float b2 = fabsf(bs_[c + l] - ms);
+                hs[l] = b2 > hs[l] ? b2 : hs[l];
+            }
+        float peak = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(hw[0], hw[1]), hw[2]), hw[3]), hs[0]), hs[1]), hs[2]),
+                           hs[3]);
+        if (keep && peak <= NEAR_DROP_M && !C.inner) keep = 0;
+        // recentre (near.rs:118-125): f64 mean of the residual.
+        double sum_w = 0.0, sum_s = 0.0;
+        for (int k = 0; k < n2; ++k) {
+            sum_w += (double)(bw_[k] - mw);
+            sum_s += (double)(bs_[k] - ms);
+        }
+        mean_w = sum_w / (double)n2;
+        mean_s = sum_s / (double)n2;
+        float mu = 0.0f, mv = 0.0f;
+        if (C.inner && sw > 1.0e-10f)
+            for (int k = 0; k < n2; ++k) {
+                mu += bw_[k] * bu_[k];
+                mv += bw_[k] * bv_[k];
+            }
+        uu_s = mu / sw;
+        vv_s = mv / sw;
+        mw_s = mw;
+        ms_s = ms;
+        sw_s = sw;
+        peak_s = peak;
+        int slot = slot_map[C.cidx];
+        if (!keep) {
+            if (slot >= 0) {
+                meta[slot].state = 2;
+                slot_map[C.cidx] = -1;
+                atomicSub(&counters[1], 1);
+            }
+            slot = -1;
+        } else if (slot < 0) {
+            int top = atomicSub(&counters[0], 1);
+            if (top <= 0) {
+                atomicAdd(&counters[0], 1);
+                atomicAdd(&counters[2], 1);
+                keep = 0;
+            } else {
+                slot = free_stack[top - 1];
+                slot_map[C.cidx] = slot;
+                meta[slot].state = 1;
+                meta[slot].key = C.cidx;
+                atomicAdd(&counters[1], 1);
+            }
+        }
+        decision = keep;
+        slot_s = slot;
+        if (keep) {
+            meta[slot].peak = peak;
+            meta[slot].idle_s = 0.0f;
+            meta[slot].fresh = 1;
+        }
+    }
+    __syncthreads();
+    if (!decision) return;
+    float* tw = pool + (size_t)slot_s * 4 * n2;
+    float* ts = tw + n2;
+    float* tuw = ts + n2;
+    float* tvw = tuw + n2;
+    const float mwf = (float)mean_w, msf = (float)mean_s;
+    const bool vel = C.inner && sw_s > 1.0e-10f;
+    for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+        tw[k] = (bw_[k] - mw_s) - mwf;
+        ts[k] = (bs_[k] - ms_s) - msf;
+        if (vel) {
+            const bool wet = bw_[k] > NEAR_FILM_M;
+            tuw[k] = wet ? bu_[k] - uu_s : 0.0f;
+            tvw[k] = wet ? bv_[k] - vv_s : 0.0f;
+        } else {
+            tuw[k] = 0.0f;
+            tvw[k] = 0.0f;
+        }
+    }
+}
+
+// restrict_fine (src/fluid_core.rs:8462-8555): one thread per touched coarse column.
+__global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const RestrictEntry* ents, int nent,
+                           const Segment* segs, float fine_area, float coarse_area, int full) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nent) return;
+    const RestrictEntry E = ents[q];
+    float aw = 0.0f, as = 0.0f, auw = 0.0f, avw = 0.0f, aus = 0.0f, avs = 0.0f;
+    for (int sgi = 0; sgi < E.seg_n; ++sgi) {
+        const Segment S = segs[E.seg_off + sgi];
+        const PatchRef& R = refs[S.patch];
+        for (int j = S.j0; j <= S.j1; ++j)
+            for (int i = S.i0; i <= S.i1; ++i) {
+                const int f = j * fres + i;
+                const float fw = R.water[f], fs = R.slurry[f];
+                if (fw == 0.0f && fs == 0.0f) continue;
+                aw += fw * fine_area;
+                as += fs * fine_area;
+                auw += R.uw[f] * fw * fine_area;
+                avw += R.vw[f] * fw * fine_area;
+                aus += R.us[f] * fs * fine_area;
+                avs += R.vs[f] * fs * fine_area;
+            }
+    }
+    const size_t idx = E.cidx;
+    const float w = aw / coarse_area, s = as / coarse_area;
+    if (!E.held && E.cnt >= full) {
+        if (w <= 0.0f && s <= 0.0f) return;
+        const float old_w = W.h[0][idx], old_s = W.h[1][idx];
+        const float new_w = old_w + w, new_s = old_s + s;
+        if (new_w > 1.0e-6f) {
+            W.u[0][idx] = (old_w * W.u[0][idx] * coarse_area + auw) / (new_w * coarse_area);
+            W.v[0][idx] = (old_w * W.v[0][idx] * coarse_area + avw) / (new_w * coarse_area);
+        }
+        if (new_s > 1.0e-6f) {
+            W.u[1][idx] = (old_s * W.u[1][idx] * coarse_area + aus) / (new_s * coarse_area);
+            W.v[1][idx] = (old_s * W.v[1][idx] * coarse_area + avs) / (new_s * coarse_area);
+        }
+        W.h[0][idx] = new_w;
+        W.h[1][idx] = new_s;
+        return;
+    }
+    W.h[0][idx] = w;
+    W.h[1][idx] = s;
+    if (w > 1.0e-6f) {
+        W.u[0][idx] = auw / (w * coarse_area);
+        W.v[0][idx] = avw / (w * coarse_area);
+    }
+    if (s > 1.0e-6f) {
+        W.u[1][idx] = aus / (s * coarse_area);
+        W.v[1][idx] = avs / (s * coarse_area);
+    }
+}
+
+// Fine cells outside the coarse window: their volume is parked (src/fluid_core.rs:8476-8484).
+__global__ void k_park(const PatchRef* refs, int np, int fres, float fine_area, double* books) {
+    const size_t fn = (size_t)fres * fres;
+    double pw = 0.0, ps = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
+        const PatchRef& R = refs[k / fn];
+        const int f = (int)(k % fn);
+        if (R.col[f % fres] >= 0 && R.row[f / fres] >= 0) continue;
+        pw += (double)R.water[f] * fine_area;
+        ps += (double)R.slurry[f] * fine_area;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        pw += __shfl_down_sync(0xffffffffu, pw, o);
+        ps += __shfl_down_sync(0xffffffffu, ps, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (pw != 0.0 || ps != 0.0)) {
+        atomicAdd(&books[1], pw);
+        atomicAdd(&books[2], ps);
+    }
+}
+
+__global__ void k_init_pool(NearMeta* meta, int* free_stack, int* slot_map, size_t ncells, int* counters) {
+    size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k < NEAR_POOL) {
+        meta[k].state = 0;
+        free_stack[k] = NEAR_POOL - 1 - (int)k;
+    }
+    for (size_t c = k; c < ncells; c += (size_t)gridDim.x * blockDim.x) slot_map[c] = -1;
+    if (k == 0) {
+        counters[0] = NEAR_POOL;
+        counters[1] = 0;
+        counters[2] = 0;
+        counters[3] = 0;
+    }
+}
+
+// ------------------------------------------------------------------- host side
+
+namespace {
+
+std::pair<int, int> index_span(float origin, float cell, int res, float center, float reach) {
+    if (!(cell > 0.0f) || res == 0) return {0, 0};
+    float lo = std::fmax(std::floor((center - reach - origin) / cell - 1.0f), 0.0f);
+    float hi = std::fmax(std::ceil((center + reach - origin) / cell + 2.0f), 0.0f);
+    auto to_i = [](float v) { return v > 0.0f ? (v >= 2.0e9f ? 2000000000 : (int)v) : 0; };
+    int l = std::min(to_i(lo), res);
+    int h = std::max(std::min(to_i(hi), res), l);
+    return {l, h};
+}
+
+float dist2_segment(float px, float pz, float ax, float az, float bx, float bz) {
+    float abx = bx - ax, abz = bz - az;
+    float ab2 = abx * abx + abz * abz;
+    float t = ab2 < 1.0e-8f ? 0.0f : host::rclamp(((px - ax) * abx + (pz - az) * abz) / ab2, 0.0f, 1.0f);
+    float dx = px - (ax + abx * t), dz = pz - (az + abz * t);
+    return dx * dx + dz * dz;
+}
+
+// near_tire_zone (src/fluid_core.rs:9624-9640).
+bool near_tire_zone(const std::vector<silt_tire_push>& ps, float x, float z, float r2) {
+    for (const auto& p : ps) {
+        float dx = x - p.x, dz = z - p.z;
+        if (dx * dx + dz * dz <= r2) return true;
+    }
+    for (size_t i = 0; i < ps.size(); ++i)
+        for (size_t j = i + 1; j < ps.size(); ++j) {
+            if (std::fabs(ps[i].x - ps[j].x) >= 0.45f) continue;
+            if (dist2_segment(x, z, ps[i].x, ps[i].z, ps[j].x, ps[j].z) <= r2) return true;
+        }
+    return false;
+}
+
+// coarse_axis (src/fluid_core.rs:9546-9557).
+long coarse_axis(float origin, float cell, int res, float p) {
+    float i = std::floor((p - origin) / cell);
+    if (i < 0.0f) return -1;
+    long ii = (long)i;
+    return ii >= res ? -1 : ii;
+}
+
+struct Table {
+    std::vector<char> buf;
+    template <class T>
+    size_t put(const T* p, size_t n) {
+        size_t off = (buf.size() + 255) & ~size_t(255);
+        buf.resize(off + std::max<size_t>(n, 1) * sizeof(T));
+        if (n) memcpy(buf.data() + off, p, n * sizeof(T));
+        return off;
+    }
+};
+
+int launch_blocks(size_t n, int per = 256) {
+    return (int)std::max<size_t>(1, std::min<size_t>((n + per - 1) / per, 148 * 8));
+}
+
+PushJob make_job(const silt_tire_push& p, int index, float origin_x, float origin_z, float cell, int res,
+                 float reach) {
+    PushJob J;
+    J.x = p.x;
+    J.z = p.z;
+    J.fx = p.forward_x;
+    J.fz = p.forward_z;
+    J.radius = p.radius;
+    J.width = p.width;
+    J.speed = p.speed;
+    J.slip = p.slip;
+    auto si = index_span(origin_x, cell, res, p.x, reach);
+    auto sj = index_span(origin_z, cell, res, p.z, reach);
+    J.span_i0 = si.first;
+    J.span_i1 = si.second;
+    J.span_j0 = sj.first;
+    J.span_j1 = sj.second;
+    J.index = index;
+    J.pad[0] = J.pad[1] = J.pad[2] = 0;
+    return J;
+}
+
+float push_reach(const silt_tire_push& p, float cell) { return hypotf(p.radius * 1.4f, p.width * 0.65f + cell) + cell; }
+float peel_reach(const silt_tire_push& p, float cell) { return p.radius * 1.3f + cell; }
+
+struct JobList {
+    size_t off = 0;
+    int n = 0, i0 = 0, j0 = 0, w = 0, h = 0;
+};
+
+JobList job_list(Table& tab, const std::vector<PushJob>& jobs) {
+    JobList L;
+    L.n = (int)jobs.size();
+    int a0 = 1 << 30, a1 = -1, b0 = 1 << 30, b1 = -1;
+    for (auto& J : jobs) {
+        if (J.span_i1 <= J.span_i0 || J.span_j1 <= J.span_j0) continue;
+        a0 = std::min(a0, J.span_i0);
+        a1 = std::max(a1, J.span_i1);
+        b0 = std::min(b0, J.span_j0);
+        b1 = std::max(b1, J.span_j1);
+    }
+    if (a1 < 0) {
+        L.n = 0;
+        return L;
+    }
+    L.i0 = a0;
+    L.j0 = b0;
+    L.w = a1 - a0;
+    L.h = b1 - b0;
+    L.off = tab.put(jobs.data(), jobs.size());
+    return L;
+}
+
+}  // namespace
+
+// Per-handle state of one step between laying the patches and packing them.
+struct StepPlan {
+    int np = 0;
+    std::vector<int> held;
+    bool any_park = false;
+    int n_owner = 0, n_near = 0, n_ent = 0;
+    size_t off_refs = 0, off_held = 0, off_oidx = 0, off_oval = 0, off_near = 0, off_ent = 0, off_seg = 0;
+    std::vector<JobList> fine_push, fine_peel;
+    JobList coarse_push, coarse_peel;
+    int slot = 0;
+};
+
+struct HostState {
+    StepPlan plan;
+    char* d_tab[2] = {nullptr, nullptr};
+    char* h_tab[2] = {nullptr, nullptr};
+    size_t cap[2] = {0, 0};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int flip = 0;
+    int jobs_for = -1;   // patch count the device job array was written for
+};
+
+static HostState& H(Patches& P) { return *reinterpret_cast<HostState*>(I(P).host); }
+
+static int ensure_patches(Patches& P, int np, cudaStream_t st) {
+    const size_t fn = (size_t)P.fres * P.fres;
+    while ((int)P.patches.size() < np) {
+        PatchState* S = new PatchState();
+        // 9 planes + a spare + 2 layers x 2 scratch sets x 5 + 2 layers x 2 transient, then grain.
+        const size_t planes = 10 + 20 + 4;
+        cudaError_t e = cudaMalloc(&S->base, planes * fn * sizeof(float) + fn + 256);
+        if (e != cudaSuccess) {
+            delete S;
+            snprintf(g_err, sizeof g_err, "patch alloc: %s", cudaGetErrorString(e));
+            return SILT_ENOMEM;
+        }
+        float* q = S->base;
+        float** named[9] = {&S->water, &S->slurry, &S->uw, &S->vw, &S->us, &S->vs, &S->bed, &S->bed_slurry,
+                            &S->moisture};
+        for (int k = 0; k < 9; ++k) {
+            *named[k] = q;
+            q += fn;
+        }
+        q += fn;
+        for (int l = 0; l < 2; ++l)
+            for (int s2 = 0; s2 < 2; ++s2)
+                for (int a = 0; a < 5; ++a) {
+                    S->sc[l][s2][a] = q;
+                    q += fn;
+                }
+        for (int l = 0; l < 2; ++l)
+            for (int t = 0; t < 2; ++t) {
+                S->tmp[l][t] = q;
+                q += fn;
+            }
+        S->grain = reinterpret_cast<uint8_t*>(q);
+        FCK(cudaMemsetAsync(S->base, 0, planes * fn * sizeof(float), st));
+        FCK(cudaMemsetAsync(S->grain, 4, fn, st));
+        P.patches.push_back(S);
+    }
+    return SILT_OK;
+}
+
+// Plans one step's geometry on the host and ships it in one table copy.
+static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps) {
+    Impl& M = I(P);
+    HostState& HS = H(P);
+    StepPlan& L = HS.plan;
+    L = StepPlan();
+    SheetView W = view_of(s);
+    const int res = W.res, fres = P.fres, sub = P.sub;
+    const float extent = (float)fres * P.fcell;
+    const int full = sub * sub;
+    const float r2 = P.tire_r * P.tire_r;
+    L.np = P.layout == SILT_FINE_MEAN_PATCH ? 1 : std::min((int)ps.size(), MAX_PATCHES);
+    int rc = ensure_patches(P, L.np, W.st);
+    if (rc) return rc;
+    std::vector<int> oidx;
+    std::vector<int8_t> oval;
+    for (int c : M.held_now) {
+        M.h_owner[c] = -1;
+        oidx.push_back(c);
+        oval.push_back(-1);
+    }
+    M.held_now.clear();
+    struct Touch {
+        int cnt = 0;
+        std::vector<Segment> segs;
+    };
+    std::map<int, Touch> touch;
+    std::vector<int16_t> axes((size_t)L.np * 2 * fres);
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        if (P.layout == SILT_FINE_MEAN_PATCH) {
+            float cx = 0.0f, cz = 0.0f;
+            for (const auto& t : ps) {
+                cx += t.x;
+                cz += t.z;
+            }
+            float n = (float)ps.size();
+            cx /= n;
+            cz /= n;
+            host::snap_origin(cx, cz, extent, W.cell, S->origin);
+        } else {
+            host::snap_origin(ps[p].x, ps[p].z, extent, W.cell, S->origin);
+        }
+        S->col.assign(fres, -1);
+        S->row.assign(fres, -1);
+        for (int i = 0; i < fres; ++i) {
+            S->col[i] = (int16_t)coarse_axis(W.origin[0], W.cell, res, S->origin[0] + ((float)i + 0.5f) * P.fcell);
+            S->row[i] = (int16_t)coarse_axis(W.origin[1], W.cell, res, S->origin[1] + ((float)i + 0.5f) * P.fcell);
+            axes[(size_t)p * 2 * fres + i] = S->col[i];
+            axes[(size_t)p * 2 * fres + fres + i] = S->row[i];
+        }
+        auto runs = [&](const std::vector<int16_t>& ax) {
+            std::vector<std::array<int, 3>> out;
+            int i = 0;
+            while (i < fres) {
+                int c = ax[i], n = 1;
+                while (i + n < fres && ax[i + n] == c) ++n;
+                if (c >= 0) out.push_back({c, i, i + n - 1});
+                else L.any_park = true;
+                i += n;
+            }
+            return out;
+        };
+        auto cr = runs(S->col), rr = runs(S->row);
+        std::vector<silt_tire_push> own;
+        if (P.layout == SILT_FINE_MEAN_PATCH)
+            own = ps;
+        else
+            own.push_back(ps[p]);
+        for (auto& r : rr)
+            for (auto& c : cr) {
+                const int cidx = r[0] * res + c[0];
+                const int n = (c[2] - c[1] + 1) * (r[2] - r[1] + 1);
+                Touch& T = touch[cidx];
+                T.cnt += n;
+                T.segs.push_back({p, c[1], c[2], r[1], r[2], 0});
+                if (n != full || M.h_owner[cidx] >= 0) continue;
+                float x = W.origin[0] + ((float)c[0] + 0.5f) * W.cell;
+                float z = W.origin[1] + ((float)r[0] + 0.5f) * W.cell;
+                if (near_tire_zone(own, x, z, r2)) {
+                    M.h_owner[cidx] = (int8_t)p;
+                    M.held_now.push_back(cidx);
+                    L.held.push_back(cidx);
+                    oidx.push_back(cidx);
+                    oval.push_back((int8_t)p);
+                }
+            }
+    }
+    std::vector<NearCol> ncols;
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        auto runs = [&](const std::vector<int16_t>& ax) {
+            std::vector<std::pair<int, int>> out;
+            int i = 0;
+            while (i < fres) {
+                int c = ax[i], n = 1;
+                while (i + n < fres && ax[i + n] == c) ++n;
+                if (c >= 0 && n == sub) out.push_back({c, i});
+                i += n;
+            }
+            return out;
+        };
+        auto cols = runs(S->col), rows = runs(S->row);
+        for (auto& r : rows)
+            for (auto& c : cols) {
+                const int cidx = r.first * res + c.first;
+                if (M.h_owner[cidx] != p) continue;
+                const int i = c.first, j = r.first;
+                int inner = 0;
+                if (i > 0 && j > 0 && i + 1 < res && j + 1 < res)
+                    inner = M.h_owner[cidx - 1] >= 0 && M.h_owner[cidx + 1] >= 0 && M.h_owner[cidx - res] >= 0 &&
+                            M.h_owner[cidx + res] >= 0;
+                ncols.push_back({cidx, p, c.second, r.second, inner, 0});
+            }
+    }
+    std::vector<RestrictEntry> ents;
+    std::vector<Segment> segs;
+    for (auto& kv : touch) {
+        RestrictEntry E;
+        E.cidx = kv.first;
+        E.cnt = kv.second.cnt;
+        E.held = M.h_owner[kv.first] >= 0;
+        E.seg_off = (int)segs.size();
+        E.seg_n = (int)kv.second.segs.size();
+        E.pad = 0;
+        for (auto& sg : kv.second.segs) segs.push_back(sg);
+        ents.push_back(E);
+    }
+    Table tab;
+    // Axes first: the refs below point into the device copy of this table.
+    const size_t off_axes = tab.put(axes.data(), axes.size());
+    L.off_held = tab.put(L.held.data(), L.held.size());
+    L.off_oidx = tab.put(oidx.data(), oidx.size());
+    L.off_oval = tab.put(oval.data(), oval.size());
+    L.off_near = tab.put(ncols.data(), ncols.size());
+    L.off_ent = tab.put(ents.data(), ents.size());
+    L.off_seg = tab.put(segs.data(), segs.size());
+    L.n_owner = (int)oidx.size();
+    L.n_near = (int)ncols.size();
+    L.n_ent = (int)ents.size();
+    // Tire jobs: shove and peel per patch, shove outside, peel on the coarse window.
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        std::vector<PushJob> push, peel;
+        for (size_t q = 0; q < ps.size(); ++q) {
+            peel.push_back(make_job(ps[q], (int)q, S->origin[0], S->origin[1], P.fcell, fres,
+                                    peel_reach(ps[q], P.fcell)));
+            // cell_is_refined (src/fluid_core.rs:8338-8356): held by this patch and inside its rectangle.
+            long ci = coarse_axis(W.origin[0], W.cell, res, ps[q].x);
+            long cj = coarse_axis(W.origin[1], W.cell, res, ps[q].z);
+            if (ci < 0 || cj < 0 || M.h_owner[cj * res + ci] != p) continue;
+            float x0 = W.origin[0] + (float)ci * W.cell, z0 = W.origin[1] + (float)cj * W.cell;
+            float x1 = x0 + W.cell, z1 = z0 + W.cell;
+            if (!(x0 >= S->origin[0] - 1.0e-4f && z0 >= S->origin[1] - 1.0e-4f &&
+                  x1 <= S->origin[0] + extent + 1.0e-4f && z1 <= S->origin[1] + extent + 1.0e-4f))
+                continue;
+            push.push_back(make_job(ps[q], (int)q, S->origin[0], S->origin[1], P.fcell, fres,
+                                    push_reach(ps[q], P.fcell)));
+        }
+        L.fine_push.push_back(job_list(tab, push));
+        L.fine_peel.push_back(job_list(tab, peel));
+    }
+    {
+        std::vector<PushJob> push, peel;
+        for (size_t q = 0; q < ps.size(); ++q) {
+            peel.push_back(make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, peel_reach(ps[q], W.cell)));
+            long ci = coarse_axis(W.origin[0], W.cell, res, ps[q].x);
+            long cj = coarse_axis(W.origin[1], W.cell, res, ps[q].z);
+            if (ci >= 0 && cj >= 0 && M.h_owner[cj * res + ci] >= 0) continue;
+            push.push_back(make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, push_reach(ps[q], W.cell)));
+        }
+        L.coarse_push = job_list(tab, push);
+        L.coarse_peel = job_list(tab, peel);
+    }
+    // Patch references, pointing at the axes inside the device table.
+    const int slot = HS.flip;
+    HS.flip ^= 1;
+    L.slot = slot;
+    size_t need = tab.buf.size() + (size_t)L.np * sizeof(PatchRef) + 512;
+    if (need > HS.cap[slot]) {
+        if (HS.ev[slot]) FCK(cudaEventSynchronize(HS.ev[slot]));
+        if (HS.d_tab[slot]) cudaFree(HS.d_tab[slot]);
+        if (HS.h_tab[slot]) cudaFreeHost(HS.h_tab[slot]);
+        HS.d_tab[slot] = nullptr;
+        HS.h_tab[slot] = nullptr;
+        HS.cap[slot] = std::max(need * 2, (size_t)1 << 20);
+        FCK(cudaMalloc(&HS.d_tab[slot], HS.cap[slot]));
+        FCK(cudaMallocHost(&HS.h_tab[slot], HS.cap[slot]));
+        if (!HS.ev[slot]) FCK(cudaEventCreateWithFlags(&HS.ev[slot], cudaEventDisableTiming));
+    }
+    std::vector<PatchRef> refs;
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        PatchRef r;
+        r.water = S->water;
+        r.slurry = S->slurry;
+        r.uw = S->uw;
+        r.vw = S->vw;
+        r.us = S->us;
+        r.vs = S->vs;
+        r.bed = S->bed;
+        r.bed_slurry = S->bed_slurry;
+        r.moisture = S->moisture;
+        r.grain = S->grain;
+        const int16_t* dax = reinterpret_cast<const int16_t*>(HS.d_tab[slot] + off_axes);
+        r.col = dax + (size_t)p * 2 * fres;
+        r.row = dax + (size_t)p * 2 * fres + fres;
+        r.ox = S->origin[0];
+        r.oz = S->origin[1];
+        refs.push_back(r);
+    }
+    L.off_refs = tab.put(refs.data(), refs.size());
+    // The pinned half in use two steps ago may still feed its copy.
+    FCK(cudaEventSynchronize(HS.ev[slot]));
+    memcpy(HS.h_tab[slot], tab.buf.data(), tab.buf.size());
+    FCK(cudaMemcpyAsync(HS.d_tab[slot], HS.h_tab[slot], tab.buf.size(), cudaMemcpyHostToDevice, W.st));
+    FCK(cudaEventRecord(HS.ev[slot], W.st));
+    // The patch-step job array changes only when the patch set grows.
+    if (HS.jobs_for != L.np) {
+        std::vector<patch::Job> jobs;
+        for (int p = 0; p < L.np; ++p) {
+            PatchState* S = P.patches[p];
+            for (int l = 0; l < 2; ++l) {
+                patch::Job J;
+                memset(&J, 0, sizeof J);
+                J.h = l == 0 ? S->water : S->slurry;
+                J.u = l == 0 ? S->uw : S->us;
+                J.v = l == 0 ? S->vw : S->vs;
+                J.bed = l == 0 ? S->bed : S->bed_slurry;
+                J.grain = S->grain;
+                J.moisture = S->moisture;
+                for (int st = 0; st < 2; ++st)
+                    for (int a = 0; a < 5; ++a) J.sc[st][a] = S->sc[l][st][a];
+                J.f1 = S->tmp[l][0];
+                J.f2 = S->tmp[l][1];
+                J.nu_const = l == 0;
+                J.vort = l == 0 ? 0.08f : 0.05f;
+                J.active = 1;
+                jobs.push_back(J);
+            }
+        }
+        FCK(cudaMemcpyAsync(M.d_jobs, jobs.data(), jobs.size() * sizeof(patch::Job), cudaMemcpyHostToDevice, W.st));
+        FCK(cudaStreamSynchronize(W.st));
+        HS.jobs_for = L.np;
+    }
+    return SILT_OK;
+}
+
+#define TAB(T, off) (reinterpret_cast<const T*>(HS.d_tab[L.slot] + (off)))
+
+static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt) {
+    Impl& M = I(P);
+    int rc = plan_step(P, s, ps);
+    if (rc) return rc;
+    HostState& HS = H(P);
+    const StepPlan& L = HS.plan;
+    SheetView W = view_of(s);
+    const PatchRef* refs = TAB(PatchRef, L.off_refs);
+    if (L.n_owner) {
+        k_scatter_owner<<<launch_blocks(L.n_owner), 256, 0, W.st>>>(M.owner, TAB(int, L.off_oidx),
+                                                                     TAB(int8_t, L.off_oval), L.n_owner);
+        FCK(cudaGetLastError());
+    }
+    k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner);
+    FCK(cudaGetLastError());
+    if (!L.held.empty()) {
+        k_zero_cells<<<launch_blocks(L.held.size()), 256, 0, W.st>>>(W, TAB(int, L.off_held), (int)L.held.size());
+        FCK(cudaGetLastError());
+    }
+    P.fine_on = true;
+    P.active = L.np;
+    if (M.near_maybe) {
+        if (L.n_near) {
+            k_near_apply<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
+                                                     M.slot_map, M.pool, M.meta);
+            FCK(cudaGetLastError());
+        }
+        k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
+                                                              dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+        FCK(cudaGetLastError());
+    }
+    return SILT_OK;
+}
+
+int restrict_all(Patches& P, silt_sheet* s) {
+    if (!P.fine_on) return SILT_OK;
+    Impl& M = I(P);
+    HostState& HS = H(P);
+    const StepPlan& L = HS.plan;
+    SheetView W = view_of(s);
+    const PatchRef* refs = TAB(PatchRef, L.off_refs);
+    if (P.near_on && L.n_near) {
+        k_near_capture<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
+                                                   M.slot_map, M.pool, M.meta, M.free_stack, M.counters);
+        FCK(cudaGetLastError());
+        M.near_maybe = true;
+    }
+    if (L.n_ent) {
+        k_restrict<<<launch_blocks(L.n_ent, 128), 128, 0, W.st>>>(refs, P.fres, W, TAB(RestrictEntry, L.off_ent),
+                                                                 L.n_ent, TAB(Segment, L.off_seg), P.fcell * P.fcell,
+                                                                 W.cell * W.cell, P.sub * P.sub);
+        FCK(cudaGetLastError());
+    }
+    if (L.any_park) {
+        k_park<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres,
+                                                                                P.fcell * P.fcell, M.d_books);
+        FCK(cudaGetLastError());
+    }
+    const size_t fn = (size_t)P.fres * P.fres;
+    for (int p = 0; p < L.np; ++p) {
+        FCK(cudaMemsetAsync(P.patches[p]->water, 0, fn * sizeof(float), W.st));
+        FCK(cudaMemsetAsync(P.patches[p]->slurry, 0, fn * sizeof(float), W.st));
+    }
+    P.fine_on = false;
+    invalidate_ledger(s);
+    return SILT_OK;
+}
+
+static int fade_only(Patches& P, silt_sheet* s, float dt) {
+    Impl& M = I(P);
+    if (!M.near_maybe) return SILT_OK;
+    SheetView W = view_of(s);
+    k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
+                                                          dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+    FCK(cudaGetLastError());
+    return SILT_OK;
+}
+
+int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt, StepOut& out) {
+    Impl& M = I(P);
+    int rc = restrict_all(P, s);
+    if (rc) return rc;
+    SheetView W = view_of(s);
+    FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
+    if (ps.empty()) return fade_only(P, s, dt);
+    if ((rc = flush(s))) return rc;
+    if ((rc = lay_patches(P, s, ps, dt))) return rc;
+    HostState& HS = H(P);
+    const StepPlan& L = HS.plan;
+    W = view_of(s);
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        const JobList& J = L.fine_push[p];
+        if (!J.n) continue;
+        k_push_cells<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(
+            S->water, S->slurry, S->uw, S->vw, S->us, S->vs, P.fres, P.fcell, S->origin[0], S->origin[1],
+            TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w, J.h);
+        FCK(cudaGetLastError());
+    }
+    {
+        patch::Args A;
+        memset(&A, 0, sizeof A);
+        A.jobs = M.d_jobs;
+        A.res = P.fres;
+        A.cell = P.fcell;
+        A.dt = dt;
+        A.sub_cap = P.sub_cap;
+        A.eps = 1.0e-6f;
+        A.pace = P.pace;
+        A.has_sc2 = 1;
+        const float nu_w = host::dynamic_viscosity(3, 1.0f);
+        A.nu_c = nu_w;
+        A.mob_c = host::sheet_mobility_for(nu_w);
+        for (int k = 1; k <= 8; ++k) A.decay_w[k] = expf(-host::sheet_damp(nu_w) * (dt / (float)k));
+        FCK(patch::launch_patch_step(A, 2 * L.np, W.st));
+    }
+    for (int p = 0; p < L.np; ++p) {
+        PatchState* S = P.patches[p];
+        const JobList& J = L.fine_peel[p];
+        if (!J.n) continue;
+        k_peel<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(
+            S->water, S->uw, S->vw, P.fres, P.fcell, S->origin[0], S->origin[1], TAB(PushJob, J.off), J.n, J.i0, J.j0,
+            J.w, J.h, nullptr, W.res, W.origin[0], W.origin[1], W.cell, 0, p, M.spray, M.counters, M.d_books, nullptr);
+        FCK(cudaGetLastError());
+    }
+    if ((rc = restrict_all(P, s))) return rc;
+    if (L.coarse_push.n) {
+        const JobList& J = L.coarse_push;
+        k_push_cells<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(W.h[0], W.h[1], W.u[0], W.v[0], W.u[1],
+                                                                         W.v[1], W.res, W.cell, W.origin[0],
+                                                                         W.origin[1], TAB(PushJob, J.off), J.n, J.i0,
+                                                                         J.j0, J.w, J.h);
+        FCK(cudaGetLastError());
+    }
+    // A shove changes a cell's speed by at most 1.04 max(speed, 0.4)
+    // (|fore f + 0.28 flank r| <= sqrt(1 + 0.28^2)); shoves add up only where
+    // the tires' spans overlap.
+    float add = 0.0f;
+    for (size_t a = 0; a < ps.size(); ++a) {
+        float reach_a = push_reach(ps[a], W.cell);
+        auto ai = index_span(W.origin[0], W.cell, W.res, ps[a].x, reach_a);
+        auto aj = index_span(W.origin[1], W.cell, W.res, ps[a].z, reach_a);
+        float sum = 0.0f;
+        for (size_t b = 0; b < ps.size(); ++b) {
+            float reach_b = push_reach(ps[b], W.cell);
+            auto bi = index_span(W.origin[0], W.cell, W.res, ps[b].x, reach_b);
+            auto bj = index_span(W.origin[1], W.cell, W.res, ps[b].z, reach_b);
+            bool overlap = ai.first < bi.second && bi.first < ai.second && aj.first < bj.second && bj.first < aj.second;
+            if (a == b || overlap) sum += 1.04f * std::max(ps[b].speed, 0.4f);
+        }
+        add = std::max(add, sum);
+    }
+    add_speed(s, add);
+    out.spray_events = 1;
+    return SILT_OK;
+}
+
+int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, StepOut& out) {
+    if (ps.empty()) return SILT_OK;
+    Impl& M = I(P);
+    HostState& HS = H(P);
+    const StepPlan& L = HS.plan;
+    const JobList& J = L.coarse_peel;
+    if (!J.n) return SILT_OK;
+    SheetView W = view_of(s);
+    k_peel<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(W.h[0], W.u[0], W.v[0], W.res, W.cell, W.origin[0],
+                                                               W.origin[1], TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w,
+                                                               J.h, M.owner, W.res, W.origin[0], W.origin[1], W.cell,
+                                                               1, 0, M.spray, M.counters, M.d_books, W.d_acc);
+    FCK(cudaGetLastError());
+    return SILT_OK;
+}
+
+int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out) {
+    Impl& M = I(P);
+    SheetView W = view_of(s);
+    if (!host && !n_out) return SILT_OK;
+    FCK(cudaMemcpyAsync(M.h_counters, M.counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaStreamSynchronize(W.st));
+    int n = std::min(M.h_counters[3], SPRAY_CAP);
+    if (n_out) *n_out = n;
+    if (host && cap > 0 && n > 0) {
+        std::vector<SprayRec> recs(n);
+        FCK(cudaMemcpyAsync(recs.data(), M.spray, n * sizeof(SprayRec), cudaMemcpyDeviceToHost, W.st));
+        FCK(cudaStreamSynchronize(W.st));
+        std::sort(recs.begin(), recs.end(), [](const SprayRec& a, const SprayRec& b) { return a.key < b.key; });
+        for (int k = 0; k < n && k < cap; ++k)
+            host[k] = {recs[k].x, recs[k].y, recs[k].z, recs[k].vx, recs[k].vy, recs[k].vz, recs[k].volume,
+                       recs[k].kind};
+    }
+    return SILT_OK;
+}
+
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s) {
+    Impl& M = I(P);
+    SheetView W = view_of(s);
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 4 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaStreamSynchronize(W.st));
+    *spray = M.h_books[0];
+    *park_w = M.h_books[1];
+    *park_s = M.h_books[2];
+    return SILT_OK;
+}
+
+int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, int patch, float* host,
+                float* origin2) {
+    int rc = restrict_all(P, s);
+    if (rc) return rc;
+    SheetView W = view_of(s);
+    if (ps.empty()) {
+        if ((rc = fade_only(P, s, 0.0f))) return rc;
+        memset(host, 0, (size_t)P.fres * P.fres * sizeof(float));
+        FCK(cudaStreamSynchronize(W.st));
+        return SILT_OK;
+    }
+    if ((rc = flush(s))) return rc;
+    if ((rc = lay_patches(P, s, ps, 0.0f))) return rc;
+    if (patch >= 0 && patch < P.active) {
+        PatchState* S = P.patches[patch];
+        FCK(cudaMemcpyAsync(host, S->water, (size_t)P.fres * P.fres * sizeof(float), cudaMemcpyDeviceToHost, W.st));
+        if (origin2) {
+            origin2[0] = S->origin[0];
+            origin2[1] = S->origin[1];
+        }
+    }
+    rc = restrict_all(P, s);
+    FCK(cudaStreamSynchronize(W.st));
+    return rc;
+}
+
+int near_tiles(Patches& P, silt_sheet* s, int* out) {
+    Impl& M = I(P);
+    SheetView W = view_of(s);
+    FCK(cudaMemcpyAsync(M.h_counters, M.counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaStreamSynchronize(W.st));
+    *out = M.h_counters[1];
+    return SILT_OK;
+}
+
+int set_near_field(Patches& P, silt_sheet* s, bool on) {
+    Impl& M = I(P);
+    P.near_on = on;
+    if (!on) {
+        SheetView W = view_of(s);
+        k_init_pool<<<launch_blocks(std::max<size_t>(W.n, NEAR_POOL)), 256, 0, W.st>>>(M.meta, M.free_stack,
+                                                                                       M.slot_map, W.n, M.counters);
+        FCK(cudaGetLastError());
+        M.near_maybe = false;
+    }
+    return SILT_OK;
+}
 
 int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
-    P.layout = cfg.fine_layout;
+    P.layout = cfg.fine_layout == SILT_FINE_PER_TIRE ? SILT_FINE_PER_TIRE : SILT_FINE_MEAN_PATCH;
     P.fres = cfg.fine_res;
     P.fcell = cfg.fine_cell;
+    P.sub = (int)std::lround(cfg.cell / cfg.fine_cell);
     P.tire_r = cfg.tire_r;
+    if (P.fres > 512 || P.sub > 32) {
+        snprintf(g_err, sizeof g_err, "fine_res above 512 or cell ratio above 32");
+        return SILT_EINVAL;
+    }
+    Impl* M = new Impl();
+    P.impl = M;
+    M->host = new HostState();
+    M->res = res;
+    const size_t n = (size_t)res * res;
+    M->h_owner.assign(n, -1);
+    const int n2 = P.sub * P.sub;
+    FCK(cudaMalloc(&M->owner, n));
+    FCK(cudaMemsetAsync(M->owner, 0xff, n, st));
+    FCK(cudaMalloc(&M->d_jobs, 2 * MAX_PATCHES * sizeof(patch::Job)));
+    FCK(cudaMalloc(&M->slot_map, n * sizeof(int)));
+    FCK(cudaMalloc(&M->pool, (size_t)NEAR_POOL * 4 * n2 * sizeof(float)));
+    FCK(cudaMalloc(&M->meta, NEAR_POOL * sizeof(NearMeta)));
+    FCK(cudaMalloc(&M->free_stack, NEAR_POOL * sizeof(int)));
+    FCK(cudaMalloc(&M->counters, 8 * sizeof(int)));
+    FCK(cudaMalloc(&M->spray, SPRAY_CAP * sizeof(SprayRec)));
+    FCK(cudaMalloc(&M->d_books, 4 * sizeof(double)));
+    FCK(cudaMemsetAsync(M->d_books, 0, 4 * sizeof(double), st));
+    FCK(cudaMallocHost(&M->h_books, 4 * sizeof(double)));
+    FCK(cudaMallocHost(&M->h_counters, 8 * sizeof(int)));
+    k_init_pool<<<launch_blocks(std::max<size_t>(n, NEAR_POOL)), 256, 0, st>>>(M->meta, M->free_stack, M->slot_map, n,
+                                                                               M->counters);
+    FCK(cudaGetLastError());
     return SILT_OK;
 }
-void destroy(Patches& P) {}
-int restrict_all(Patches& P, silt_sheet* s) { return SILT_OK; }
-int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, float dt, StepOut& out) {
-    return pushes.empty() ? SILT_OK : SILT_EINVAL;
+
+void destroy(Patches& P) {
+    for (PatchState* S : P.patches) {
+        cudaFree(S->base);
+        delete S;
+    }
+    P.patches.clear();
+    if (!P.impl) return;
+    Impl* M = (Impl*)P.impl;
+    if (M->host) {
+        HostState* HS = (HostState*)M->host;
+        for (int k = 0; k < 2; ++k) {
+            if (HS->ev[k]) cudaEventDestroy(HS->ev[k]);
+            cudaFree(HS->d_tab[k]);
+            if (HS->h_tab[k]) cudaFreeHost(HS->h_tab[k]);
+        }
+        delete HS;
+    }
+    cudaFree(M->owner);
+    cudaFree(M->d_jobs);
+    cudaFree(M->slot_map);
+    cudaFree(M->pool);
+    cudaFree(M->meta);
+    cudaFree(M->free_stack);
+    cudaFree(M->counters);
+    cudaFree(M->spray);
+    cudaFree(M->d_books);
+    if (M->h_books) cudaFreeHost(M->h_books);
+    if (M->h_counters) cudaFreeHost(M->h_counters);
+    delete M;
+    P.impl = nullptr;
 }
-int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, StepOut& out) {
-    return SILT_OK;
-}
-int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out,
-                  double* spray_m3) {
-    *n_out = 0;
-    return SILT_OK;
-}
-int ledger_parts(Patches& P, silt_sheet* s, double* fine_w, double* fine_s, double* park_w, double* park_s) {
-    *fine_w = *fine_s = *park_w = *park_s = 0.0;
-    return SILT_OK;
-}
-int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, int patch, float* host,
-                float* origin2) {
-    return SILT_EINVAL;
-}
-int near_tiles(Patches& P, silt_sheet* s, int* out) {
-    *out = 0;
-    return SILT_OK;
-}
-int set_near_field(Patches& P, silt_sheet* s, bool on) {
-    P.near_on = on;
-    return SILT_OK;
-}
+
+const char* last_error() { return g_err; }
 
 }  // namespace fine
 }  // namespace silt

@@ -51,7 +51,8 @@ struct Patches {
 
 SheetView view_of(silt_sheet* s);
 int flush(silt_sheet* s);
-void note_speed(silt_sheet* s, float bound);
+// Raises the bound on any cell speed by `add` m/s (a tire shove).
+void add_speed(silt_sheet* s, float add);
 void invalidate_ledger(silt_sheet* s);
 
 int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st);
@@ -62,9 +63,10 @@ int restrict_all(Patches& P, silt_sheet* s);
 int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, float dt, StepOut& out);
 // peel_spray on the coarse window, held columns skipped (src/fluid_core.rs:6071).
 int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, StepOut& out);
-int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out,
-                  double* spray_m3);
-int ledger_parts(Patches& P, silt_sheet* s, double* fine_w, double* fine_s, double* park_w, double* park_s);
+int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out);
+// FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s);
+const char* last_error();
 int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, int patch, float* host,
                 float* origin2);
 int near_tiles(Patches& P, silt_sheet* s, int* out);

@@ -77,10 +77,10 @@ struct silt_sheet {
     double* h_acc = nullptr;      // pinned mirror of d_acc
     bool cut_pending = false;
     bool ledger_fresh = false;    // h_acc[0..1] hold the current depth sums
-    float vmax_bound = 0.0f;      // bound on any cell speed, for the one-substep shortcut
+    float vmax_bound = 0.0f;      // bound on any cell's speed |(u, v)|, for the one-substep shortcut
     float moisture_ambient = 0.0f;
     std::vector<silt_tire_push> pushes;
-    double spray_m3 = 0.0, opened_m3 = 0.0;
+    double opened_m3 = 0.0;
     int inflow_j = -1, inflow_i0 = 0, inflow_i1 = 0;
     float inflow_rate = 0.0f;
     Patches fine;
@@ -122,7 +122,7 @@ int step_coarse_pair(silt_sheet* s, float dt) {
     // bound one substep is certain; otherwise measure the largest speed.
     int nsub[2] = {1, 1};
     const float cap = 8.0f;
-    float bound = s->vmax_bound * 1.4142137f;
+    float bound = s->vmax_bound;
     if (!(dt * std::max(0.15f, bound) <= 0.42f * std::max(cell, 1.0e-3f))) {
         for (int l = 0; l < 2; ++l) {
             CK(cudaMemsetAsync(s->d_u32, 0, sizeof(unsigned int), s->st));
@@ -221,7 +221,8 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         s->cur = nxt;
         s->cut_pending = true;
     }
-    s->vmax_bound = std::max(silt::host::kSpeedCap, 0.0f);
+    // Every component is now clamped to the film speed cap.
+    s->vmax_bound = silt::host::kSpeedCap * 1.4142137f;
     return SILT_OK;
 }
 
@@ -229,7 +230,10 @@ int step_coarse_pair(silt_sheet* s, float dt) {
 
 extern "C" {
 
-const char* silt_last_error(void) { return g_err; }
+const char* silt_last_error(void) {
+    if (g_err[0]) return g_err;
+    return silt::fine::last_error();
+}
 
 void silt_cfg_default(silt_cfg* c) {
     if (!c) return;
@@ -397,7 +401,7 @@ int silt_map_water_velocity(silt_sheet* s, const float* u, const float* v) {
         if (std::isfinite(u[i])) m = std::max(m, fabsf(u[i]));
         if (std::isfinite(v[i])) m = std::max(m, fabsf(v[i]));
     }
-    s->vmax_bound = std::max(s->vmax_bound, m);
+    s->vmax_bound = std::max(s->vmax_bound, m * 1.4142137f);
     return SILT_OK;
 }
 
@@ -536,11 +540,13 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
     int32_t nev = 0;
-    rc = silt::fine::collect_spray(s->fine, s, fo, out, cap, &nev, &s->spray_m3);
-    if (rc) return rc;
+    if (out || n_out) {
+        rc = silt::fine::collect_spray(s->fine, s, fo, out, cap, &nev);
+        if (rc) return rc;
+    }
     if (n_out) *n_out = nev;
     s->parts.steps += 1;
-    s->ledger_fresh = fo.spray_events == 0 && ps.empty();
+    s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
     return SILT_OK;
 }
 
@@ -553,20 +559,20 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    double fine_w = 0.0, fine_s = 0.0, park_w = 0.0, park_s = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &fine_w, &fine_s, &park_w, &park_s);
+    double spray = 0.0, park_w = 0.0, park_s = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s->st));
     const double area = (double)s->cfg.cell * (double)s->cfg.cell;
-    w = s->h_acc[0] * area + fine_w;
-    sl = s->h_acc[1] * area + fine_s;
+    w = s->h_acc[0] * area;
+    sl = s->h_acc[1] * area;
     out->water_m3 = w;
     out->slurry_m3 = sl;
     out->frozen_water_m3 = park_w;
     out->frozen_slurry_m3 = park_s;
-    out->spray_m3 = s->spray_m3;
+    out->spray_m3 = spray;
     out->opened_m3 = s->opened_m3;
-    out->total_m3 = w + sl + park_w + park_s + s->spray_m3;
+    out->total_m3 = w + sl + park_w + park_s + spray;
     return SILT_OK;
 }
 
@@ -662,8 +668,9 @@ int silt_non_finite_count(silt_sheet* s, uint32_t* out) {
 
 int silt_spray_m3(silt_sheet* s, double* out) {
     if (!s || !out) return fail_arg("spray_m3");
-    *out = s->spray_m3;
-    return SILT_OK;
+    double pw = 0.0, ps = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, out, &pw, &ps);
+    return rc;
 }
 
 int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent) {
@@ -711,7 +718,7 @@ int silt_write_plane(silt_sheet* s, int32_t which, const float* host) {
         float m = 0.0f;
         for (size_t i = 0; i < s->n; ++i)
             if (std::isfinite(host[i])) m = std::max(m, fabsf(host[i]));
-        s->vmax_bound = std::max(s->vmax_bound, m);
+        s->vmax_bound = std::max(s->vmax_bound, m * 1.4142137f);
     }
     s->ledger_fresh = false;
     return SILT_OK;
@@ -873,7 +880,7 @@ SheetView view_of(silt_sheet* s) {
     return w;
 }
 int flush(silt_sheet* s) { return flush_cut(s); }
-void note_speed(silt_sheet* s, float bound) { s->vmax_bound = std::max(s->vmax_bound, bound); }
+void add_speed(silt_sheet* s, float add) { s->vmax_bound += add; }
 void invalidate_ledger(silt_sheet* s) { s->ledger_fresh = false; }
 }  // namespace fine
 }  // namespace silt

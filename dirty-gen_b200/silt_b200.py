@@ -199,12 +199,14 @@ class Sheet:
         p = make_push(t)
         check(lib().silt_push_tire(self.h, ctypes.byref(p)), "push_tire")
 
-    def step(self, dt, want_spray=True, cap=65536):
-        n = _i(0)
+    def step(self, dt, want_spray=True, cap=8192):
         if not want_spray:
             check(lib().silt_step(self.h, dt, None, 0, None), "step")
             return None
-        buf = (SprayEvent * cap)()
+        if getattr(self, "_spray_buf", None) is None or len(self._spray_buf) < cap:
+            self._spray_buf = (SprayEvent * cap)()
+        n = _i(0)
+        buf = self._spray_buf
         check(lib().silt_step(self.h, dt, buf, cap, ctypes.byref(n)), "step")
         return [(e.x, e.y, e.z, e.vx, e.vy, e.vz, e.volume, e.kind) for e in buf[:min(n.value, cap)]]
 

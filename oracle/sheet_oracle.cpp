@@ -1334,10 +1334,13 @@ struct Core {
     // src/fluid_core.rs:8358-8460 refine. Layout 0 follows the reference (one
     // patch at the mean tire); layout 1 lays one patch per tire and holds a
     // column for the first patch that covers it and lies near its own tire.
+    // All holds are decided first, then every patch is laid from the coarse
+    // state before any held column is emptied (for one patch this is the
+    // reference's order).
     void refine(const std::vector<TirePush>& ps, float dt) {
         restrict_fine();
         if (ps.empty()) { near_fade(dt); return; }
-        usize np = cfg.layout == 0 ? 1 : ps.size();
+        usize np = cfg.layout == 0 ? 1 : std::min(ps.size(), (usize)16);
         ensure_patches(np);
         pushes_in_use = np;
         float extent = (float)fres * cfg.fine_cell;
@@ -1345,6 +1348,8 @@ struct Core {
         std::fill(hold_owner.begin(), hold_owner.end(), -1);
         usize full = sub * sub;
         float r2 = cfg.tire_r * cfg.tire_r;
+        std::vector<std::vector<usize>> touches(np);
+        std::vector<std::vector<std::pair<usize, usize>>> hits(np);
         for (usize pk = 0; pk < np; ++pk) {
             Patch& P = patches[pk];
             if (cfg.layout == 0) {
@@ -1363,9 +1368,7 @@ struct Core {
             std::fill(P.us.begin(), P.us.end(), 0.0f);
             std::fill(P.vs.begin(), P.vs.end(), 0.0f);
             make_patch_axes(P);
-            std::vector<usize> touch;
             std::map<usize, uint32_t> cnt;
-            std::vector<std::pair<usize, usize>> hits;
             for (usize j = 0; j < fres; ++j) {
                 uint16_t cj = P.row[j];
                 if (cj == 0xffff) continue;
@@ -1373,16 +1376,16 @@ struct Core {
                     uint16_t ci = P.col[i];
                     if (ci == 0xffff) continue;
                     usize cidx = (usize)cj * res + ci;
-                    if (cnt[cidx] == 0) touch.push_back(cidx);
+                    if (cnt[cidx] == 0) touches[pk].push_back(cidx);
                     cnt[cidx] += 1;
-                    hits.push_back({j * fres + i, cidx});
+                    hits[pk].push_back({j * fres + i, cidx});
                 }
             }
             std::vector<TirePush> own;
             if (cfg.layout == 0) own = ps; else own.push_back(ps[pk]);
-            for (usize cidx : touch) {
+            for (usize cidx : touches[pk]) {
                 if (cnt[cidx] != full) continue;
-                if (cfg.layout == 1 && fine_hold[cidx] == 1) continue;
+                if (fine_hold[cidx] == 1) continue;
                 float x, z;
                 coarse_xz(cidx % res, cidx / res, x, z);
                 if (near_tire_zone(own, x, z, r2)) {
@@ -1390,8 +1393,11 @@ struct Core {
                     hold_owner[cidx] = cfg.layout == 0 ? -1 : (int)pk;
                 }
             }
+        }
+        for (usize pk = 0; pk < np; ++pk) {
+            Patch& P = patches[pk];
             int me = cfg.layout == 0 ? -1 : (int)pk;
-            for (auto& hp : hits) {
+            for (auto& hp : hits[pk]) {
                 usize fidx = hp.first, cidx = hp.second;
                 P.moisture[fidx] = moisture[cidx];
                 P.grain[fidx] = grain[cidx];
@@ -1409,10 +1415,11 @@ struct Core {
                 P.us[fidx] = us[cidx];
                 P.vs[fidx] = vs[cidx];
             }
-            for (usize cidx : touch)
-                if (fine_hold[cidx] == 1 && hold_owner[cidx] == me)
-                    water[cidx] = slurry[cidx] = uw[cidx] = vw[cidx] = us[cidx] = vs[cidx] = 0.0f;
         }
+        for (usize pk = 0; pk < np; ++pk)
+            for (usize cidx : touches[pk])
+                if (fine_hold[cidx] == 1)
+                    water[cidx] = slurry[cidx] = uw[cidx] = vw[cidx] = us[cidx] = vs[cidx] = 0.0f;
         fine_on = true;
         near_apply(dt);
     }
