@@ -169,12 +169,15 @@ __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W
         }
         R.bed[f] = W.bed[c];
         R.bed_slurry[f] = W.bed[c];
-        R.water[f] = W.h[0][c];
-        R.slurry[f] = W.h[1][c];
-        R.uw[f] = W.u[0][c];
-        R.vw[f] = W.v[0][c];
-        R.us[f] = W.u[1][c];
-        R.vs[f] = W.v[1][c];
+        const float hw = W.h[0][c], hs = W.h[1][c];
+        R.water[f] = hw;
+        R.slurry[f] = hs;
+        // A coarse cell still waiting for the previous dry cut carries no velocity.
+        const bool cw = W.cut_pending && hw < 1.0e-6f, cs = W.cut_pending && hs < 1.0e-6f;
+        R.uw[f] = cw ? 0.0f : W.u[0][c];
+        R.vw[f] = cw ? 0.0f : W.v[0][c];
+        R.us[f] = cs ? 0.0f : W.u[1][c];
+        R.vs[f] = cs ? 0.0f : W.v[1][c];
     }
 }
 
@@ -501,10 +504,19 @@ __global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const Re
     }
     const size_t idx = E.cidx;
     const float w = aw / coarse_area, s = as / coarse_area;
-    if (!E.held && E.cnt >= full) {
+    // A column the patch does not hold keeps its depth and gains what flowed
+    // onto its fine cells. For patches that are whole multiples of the coarse
+    // cell every touched column is fully covered and this is the reference's
+    // `!held && cnt >= full` branch; a partly covered rim column (64-cell
+    // patches) must not lose the coarse depth it kept.
+    (void)full;
+    if (!E.held) {
         if (w <= 0.0f && s <= 0.0f) return;
         const float old_w = W.h[0][idx], old_s = W.h[1][idx];
         const float new_w = old_w + w, new_s = old_s + s;
+        // Pending dry cut: a cell under eps holds no velocity.
+        if (W.cut_pending && old_w < 1.0e-6f) W.u[0][idx] = W.v[0][idx] = 0.0f;
+        if (W.cut_pending && old_s < 1.0e-6f) W.u[1][idx] = W.v[1][idx] = 0.0f;
         if (new_w > 1.0e-6f) {
             W.u[0][idx] = (old_w * W.u[0][idx] * coarse_area + auw) / (new_w * coarse_area);
             W.v[0][idx] = (old_w * W.v[0][idx] * coarse_area + avw) / (new_w * coarse_area);
@@ -756,12 +768,12 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
     L.np = P.layout == SILT_FINE_MEAN_PATCH ? 1 : std::min((int)ps.size(), MAX_PATCHES);
     int rc = ensure_patches(P, L.np, W.st);
     if (rc) return rc;
-    std::vector<int> oidx;
-    std::vector<int8_t> oval;
+    // Owner changes as one value per cell: last step's holds are released,
+    // this step's holds override (a cell listed twice would race in the scatter).
+    std::map<int, int8_t> changes;
     for (int c : M.held_now) {
         M.h_owner[c] = -1;
-        oidx.push_back(c);
-        oval.push_back(-1);
+        changes[c] = -1;
     }
     M.held_now.clear();
     struct Touch {
@@ -825,8 +837,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                     M.h_owner[cidx] = (int8_t)p;
                     M.held_now.push_back(cidx);
                     L.held.push_back(cidx);
-                    oidx.push_back(cidx);
-                    oval.push_back((int8_t)p);
+                    changes[cidx] = (int8_t)p;
                 }
             }
     }
@@ -869,6 +880,12 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         E.pad = 0;
         for (auto& sg : kv.second.segs) segs.push_back(sg);
         ents.push_back(E);
+    }
+    std::vector<int> oidx;
+    std::vector<int8_t> oval;
+    for (auto& kv : changes) {
+        oidx.push_back(kv.first);
+        oval.push_back(kv.second);
     }
     Table tab;
     // Axes first: the refs below point into the device copy of this table.
@@ -1077,7 +1094,8 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     SheetView W = view_of(s);
     FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
     if (ps.empty()) return fade_only(P, s, dt);
-    if ((rc = flush(s))) return rc;
+    // The coarse planes may still wait for the previous dry cut: the lay,
+    // restrict and shove kernels apply it to the cells they touch.
     if ((rc = lay_patches(P, s, ps, dt))) return rc;
     HostState& HS = H(P);
     const StepPlan& L = HS.plan;

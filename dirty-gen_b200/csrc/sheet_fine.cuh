@@ -26,6 +26,7 @@ struct SheetView {
     float* moisture;
     uint8_t* grain;
     double* d_acc;
+    int cut_pending;   // u, v of cells with h < eps still hold their pre-cut values
 };
 
 struct StepOut {

@@ -82,10 +82,18 @@ __global__ void k_read_substrate(const float* bed_in, const float* moist_in, con
     }
 }
 
-// Inflow strip: depth added on one row over [x0, x1).
-__global__ void k_inflow(float* water, int res, int j, int i0, int i1, float add) {
+// Inflow strip: depth added on one row over [x0, x1). A cell still waiting
+// for the previous dry cut gets it first, so the water lands at rest.
+__global__ void k_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1,
+                         float add) {
     int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < i1) water[(size_t)j * res + i] += add;
+    if (i >= i1) return;
+    size_t c = (size_t)j * res + i;
+    if (cut_pending && water[c] < 1.0e-6f) {
+        uw[c] = 0.0f;
+        vw[c] = 0.0f;
+    }
+    water[c] += add;
 }
 
 // coarse_cell (src/fluid_core.rs:6998-7035) feeding render_contract film/flow
@@ -179,9 +187,10 @@ cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const 
     k_read_substrate<<<blocks_for(n), 256, 0, st>>>(bed_in, moist_in, grain_in, bed, moisture, grain, slurry, n);
     return cudaGetLastError();
 }
-cudaError_t op_inflow(float* water, int res, int j, int i0, int i1, float add, cudaStream_t st) {
+cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
+                      cudaStream_t st) {
     if (i1 <= i0) return cudaSuccess;
-    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, res, j, i0, i1, add);
+    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, uw, vw, cut_pending, res, j, i0, i1, add);
     return cudaGetLastError();
 }
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,

@@ -527,10 +527,10 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     ps.swap(s->pushes);
     int rc;
     if (s->inflow_j >= 0) {
-        if ((rc = flush_cut(s))) return rc;
         int nc = s->inflow_i1 - s->inflow_i0;
         float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
-        CK(silt::op_inflow(s->H(0), s->res, s->inflow_j, s->inflow_i0, s->inflow_i1, add, s->st));
+        CK(silt::op_inflow(s->H(0), s->U(0), s->V(0), s->cut_pending ? 1 : 0, s->res, s->inflow_j, s->inflow_i0,
+                           s->inflow_i1, add, s->st));
         s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
     }
     silt::fine::StepOut fo;
@@ -877,6 +877,7 @@ SheetView view_of(silt_sheet* s) {
     w.moisture = s->moisture;
     w.grain = s->grain;
     w.d_acc = s->d_acc;
+    w.cut_pending = s->cut_pending ? 1 : 0;
     return w;
 }
 int flush(silt_sheet* s) { return flush_cut(s); }

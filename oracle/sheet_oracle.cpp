@@ -1297,7 +1297,12 @@ struct Core {
             usize idx = touch[t];
             bool held = fine_hold[idx] == 1;
             float w = aw[t] / coarse_area, s = as[t] / coarse_area;
-            if (!held && cnt[t] >= full) {
+            // Unheld columns keep their depth and gain what flowed onto their fine
+            // cells. With patches that are whole multiples of the coarse cell (the
+            // reference's 160-cell patch) every touched column is fully covered, so
+            // this is the reference's `!held && cnt >= full` branch; a partly
+            // covered rim column of a 64-cell patch must not lose its coarse depth.
+            if (!held) {
                 if (w <= 0.0f && s <= 0.0f) continue;
                 float old_w = water[idx], old_s = slurry[idx];
                 float new_w = old_w + w, new_s = old_s + s;

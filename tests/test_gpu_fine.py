@@ -109,7 +109,7 @@ def test_detail_survives_refine_and_keeps_volume():
     assert abs(after - before) < 1.0e-6
     assert (fine >= 0).all()
     f = fine.reshape(160, 160)
-    spread = max(float(f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10].ptp()) for cj in range(16) for ci in range(16)
+    spread = max(float(np.ptp(f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10])) for cj in range(16) for ci in range(16)
                  if f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10].max() > 0)
     assert spread > 1.0e-3
 
@@ -143,7 +143,7 @@ def test_near_field_keeps_sub_cell_detail():
             z = np.float32(z + np.float32(SPEED) * np.float32(DT))
         fine, _ = dev.fine_water_debug(four_tires(float(z), SPEED))
         f = fine.reshape(160, 160)
-        spreads = [float(f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10].ptp()) for cj in range(16) for ci in range(16)
+        spreads = [float(np.ptp(f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10])) for cj in range(16) for ci in range(16)
                    if f[cj * 10:cj * 10 + 10, ci * 10:ci * 10 + 10].max() > 1e-4]
         led = dev.ledger()
         return np.mean(spreads), led["water_m3"] + led["frozen_water_m3"] + led["spray_m3"], start
