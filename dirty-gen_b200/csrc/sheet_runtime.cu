@@ -855,6 +855,48 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
     return SILT_OK;
 }
 
+// ------------------------------------------------------ free operator, no alloc
+// Scratch for silt_step_sheet_noalloc: the layout silt_step_sheet expects
+// (256 bytes of reduction words, then the u, v and depth planes) for the
+// largest grid it serves. Every GPU that loads the library holds this array
+// until the process exits. In host code `g_step_sheet_scratch` is only a
+// stand-in symbol, never a device address: the address comes from
+// cudaGetSymbolAddress, looked up once per device with that device current.
+static __device__ __align__(256) unsigned char
+    g_step_sheet_scratch[256 + 3 * (size_t)SILT_STEP_SHEET_STATIC_MAX_RES * SILT_STEP_SHEET_STATIC_MAX_RES *
+                                   sizeof(float)];
+
+static std::mutex g_scratch_mu;
+static void* g_scratch_addr[64] = {nullptr};
+
+int silt_step_sheet_noalloc(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
+                            int32_t res, float cell, float dt, float vorticity, void* stream) {
+    if (res <= 0) return fail_arg("step_sheet_noalloc: res");
+    if (res > SILT_STEP_SHEET_STATIC_MAX_RES) {
+        snprintf(g_err, sizeof g_err,
+                 "invalid argument: step_sheet_noalloc serves grids up to %d cells per side, got %d "
+                 "(use silt_step_sheet with caller scratch)",
+                 SILT_STEP_SHEET_STATIC_MAX_RES, (int)res);
+        return SILT_EINVAL;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail_arg("step_sheet_noalloc: device ordinal");
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        if (!g_scratch_addr[dev]) {
+            // First call on this device (it is current): resolve the array's device address.
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_step_sheet_scratch);
+            if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(g_step_sheet_scratch)");
+            g_scratch_addr[dev] = p;
+        }
+        scratch = g_scratch_addr[dev];
+    }
+    return silt_step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream);
+}
+
 }  // extern "C"
 
 // Accessors the nested-patch module uses (sheet_fine.cu).

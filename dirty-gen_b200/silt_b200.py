@@ -102,6 +102,7 @@ def lib():
             "silt_set_fine_sub_cap": [_p, _f], "silt_set_fine_pace": [_p, _i], "silt_set_near_field": [_p, _i],
             "silt_step_sheet": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p, _p],
             "silt_set_step_timing": [_p, _i], "silt_get_step_parts": [_p, ctypes.POINTER(StepParts)],
+            "silt_step_sheet_noalloc": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args

@@ -178,6 +178,23 @@ size_t silt_step_sheet_scratch_bytes(int32_t res);
 int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
                     int32_t res, float cell, float dt, float vorticity, void* scratch, void* stream);
 
+/* The same operator for callers that cannot allocate GPU memory. No
+ * counterpart in the reference: it exists for code on a fixed-budget frame
+ * loop (a game or simulation tick) where cudaMalloc/cudaFree may not run,
+ * since cudaFree waits for the whole device and an allocation can stall or
+ * fail mid-frame, and for hosts whose GPU memory is all owned by another
+ * allocator. Its scratch is a fixed array compiled into the library, sized
+ * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (3 MiB per
+ * GPU that loads the library, held until the process exits); larger grids
+ * return SILT_EINVAL. The first call on each device looks the array up (with
+ * that device current), so make that first call before any stream capture.
+ * Every call shares the one array: calls whose work overlaps on the GPU race
+ * and must be ordered by the caller (one stream, or events). Calls no
+ * cudaMalloc, cudaFree or other allocating routine. */
+#define SILT_STEP_SHEET_STATIC_MAX_RES 512
+int silt_step_sheet_noalloc(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
+                            int32_t res, float cell, float dt, float vorticity, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
