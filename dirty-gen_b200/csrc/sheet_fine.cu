@@ -33,7 +33,7 @@
 #include "sheet_fine.cuh"
 #include "sheet_host_math.h"
 #include "sheet_math.cuh"
-#include "sheet_patch.cuh"
+#include "sheet_window.cuh"
 
 namespace silt {
 namespace fine {
@@ -65,8 +65,7 @@ struct PatchState {
     float* base = nullptr;
     float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
     uint8_t* grain;
-    float* sc[2][2][5];   // [layer][set][a..e]
-    float* tmp[2][2];     // [layer][f1, f2]
+    float* win[2];        // [layer]: the window engine's scratch planes
     // Host geometry of the current step.
     float origin[2] = {0, 0};
     std::vector<int16_t> col, row;
@@ -119,7 +118,6 @@ struct Impl {
     int8_t* owner = nullptr;          // per coarse cell: patch that holds it, -1 none
     std::vector<int8_t> h_owner;      // host mirror
     std::vector<int> held_now;        // coarse cells held by the last laid patches
-    patch::Job* d_jobs = nullptr;
     void* host = nullptr;             // HostState: the step plan and its table buffers
     // Near-field pool.
     int* slot_map = nullptr;          // per coarse cell
@@ -697,6 +695,7 @@ struct StepPlan {
     std::vector<int> held;
     bool any_park = false;
     int n_owner = 0, n_near = 0, n_ent = 0;
+    size_t off_jobs = 0;
     size_t off_refs = 0, off_held = 0, off_oidx = 0, off_oval = 0, off_near = 0, off_ent = 0, off_seg = 0;
     std::vector<JobList> fine_push, fine_peel;
     JobList coarse_push, coarse_peel;
@@ -710,7 +709,6 @@ struct HostState {
     size_t cap[2] = {0, 0};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int flip = 0;
-    int jobs_for = -1;   // patch count the device job array was written for
 };
 
 static HostState& H(Patches& P) { return *reinterpret_cast<HostState*>(I(P).host); }
@@ -719,8 +717,8 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
     const size_t fn = (size_t)P.fres * P.fres;
     while ((int)P.patches.size() < np) {
         PatchState* S = new PatchState();
-        // 9 planes + a spare + 2 layers x 2 scratch sets x 5 + 2 layers x 2 transient, then grain.
-        const size_t planes = 10 + 20 + 4;
+        // 9 planes + a spare + the window engine's scratch for two layers, then grain.
+        const size_t planes = 10 + 2 * (size_t)window::SCRATCH_PLANES;
         cudaError_t e = cudaMalloc(&S->base, planes * fn * sizeof(float) + fn + 256);
         if (e != cudaSuccess) {
             delete S;
@@ -735,17 +733,10 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
             q += fn;
         }
         q += fn;
-        for (int l = 0; l < 2; ++l)
-            for (int s2 = 0; s2 < 2; ++s2)
-                for (int a = 0; a < 5; ++a) {
-                    S->sc[l][s2][a] = q;
-                    q += fn;
-                }
-        for (int l = 0; l < 2; ++l)
-            for (int t = 0; t < 2; ++t) {
-                S->tmp[l][t] = q;
-                q += fn;
-            }
+        for (int l = 0; l < 2; ++l) {
+            S->win[l] = q;
+            q += (size_t)window::SCRATCH_PLANES * fn;
+        }
         S->grain = reinterpret_cast<uint8_t*>(q);
         FCK(cudaMemsetAsync(S->base, 0, planes * fn * sizeof(float), st));
         FCK(cudaMemsetAsync(S->grain, 4, fn, st));
@@ -755,7 +746,7 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
 }
 
 // Plans one step's geometry on the host and ships it in one table copy.
-static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps) {
+static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt) {
     Impl& M = I(P);
     HostState& HS = H(P);
     StepPlan& L = HS.plan;
@@ -937,7 +928,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
     const int slot = HS.flip;
     HS.flip ^= 1;
     L.slot = slot;
-    size_t need = tab.buf.size() + (size_t)L.np * sizeof(PatchRef) + 512;
+    size_t need = tab.buf.size() + (size_t)L.np * (sizeof(PatchRef) + 2 * sizeof(window::Job)) + 1024;
     if (need > HS.cap[slot]) {
         if (HS.ev[slot]) FCK(cudaEventSynchronize(HS.ev[slot]));
         if (HS.d_tab[slot]) cudaFree(HS.d_tab[slot]);
@@ -971,18 +962,16 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         refs.push_back(r);
     }
     L.off_refs = tab.put(refs.data(), refs.size());
-    // The pinned half in use two steps ago may still feed its copy.
-    FCK(cudaEventSynchronize(HS.ev[slot]));
-    memcpy(HS.h_tab[slot], tab.buf.data(), tab.buf.size());
-    FCK(cudaMemcpyAsync(HS.d_tab[slot], HS.h_tab[slot], tab.buf.size(), cudaMemcpyHostToDevice, W.st));
-    FCK(cudaEventRecord(HS.ev[slot], W.st));
-    // The patch-step job array changes only when the patch set grows.
-    if (HS.jobs_for != L.np) {
-        std::vector<patch::Job> jobs;
+    // The fine pair (src/fluid_core.rs:7942-8150 with fine = true): one window
+    // job per patch and layer.
+    {
+        std::vector<window::Job> jobs;
+        const float nu_w = host::dynamic_viscosity(3, 1.0f);
+        const size_t fn = (size_t)fres * fres;
         for (int p = 0; p < L.np; ++p) {
             PatchState* S = P.patches[p];
             for (int l = 0; l < 2; ++l) {
-                patch::Job J;
+                window::Job J;
                 memset(&J, 0, sizeof J);
                 J.h = l == 0 ? S->water : S->slurry;
                 J.u = l == 0 ? S->uw : S->us;
@@ -990,20 +979,30 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 J.bed = l == 0 ? S->bed : S->bed_slurry;
                 J.grain = S->grain;
                 J.moisture = S->moisture;
-                for (int st = 0; st < 2; ++st)
-                    for (int a = 0; a < 5; ++a) J.sc[st][a] = S->sc[l][st][a];
-                J.f1 = S->tmp[l][0];
-                J.f2 = S->tmp[l][1];
-                J.nu_const = l == 0;
+                window::attach_scratch(J, S->win[l], fn);
+                J.res = fres;
+                J.cell = P.fcell;
+                J.dt = dt;
                 J.vort = l == 0 ? 0.08f : 0.05f;
+                J.sub_cap = P.sub_cap;
+                J.eps = 1.0e-6f;
+                J.nu_mode = l == 0 ? window::NU_CONST : window::NU_GRAIN;
+                J.nu_c = nu_w;
+                J.mob_c = host::sheet_mobility_for(nu_w);
+                for (int k = 1; k <= 8; ++k) J.decay_c[k] = expf(-host::sheet_damp(nu_w) * (dt / (float)k));
+                J.pace = P.pace;
+                J.has_sc2 = 1;
                 J.active = 1;
                 jobs.push_back(J);
             }
         }
-        FCK(cudaMemcpyAsync(M.d_jobs, jobs.data(), jobs.size() * sizeof(patch::Job), cudaMemcpyHostToDevice, W.st));
-        FCK(cudaStreamSynchronize(W.st));
-        HS.jobs_for = L.np;
+        L.off_jobs = tab.put(jobs.data(), jobs.size());
     }
+    // The pinned half in use two steps ago may still feed its copy.
+    FCK(cudaEventSynchronize(HS.ev[slot]));
+    memcpy(HS.h_tab[slot], tab.buf.data(), tab.buf.size());
+    FCK(cudaMemcpyAsync(HS.d_tab[slot], HS.h_tab[slot], tab.buf.size(), cudaMemcpyHostToDevice, W.st));
+    FCK(cudaEventRecord(HS.ev[slot], W.st));
     return SILT_OK;
 }
 
@@ -1011,7 +1010,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
 
 static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt) {
     Impl& M = I(P);
-    int rc = plan_step(P, s, ps);
+    int rc = plan_step(P, s, ps, dt);
     if (rc) return rc;
     HostState& HS = H(P);
     const StepPlan& L = HS.plan;
@@ -1109,23 +1108,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
             TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w, J.h);
         FCK(cudaGetLastError());
     }
-    {
-        patch::Args A;
-        memset(&A, 0, sizeof A);
-        A.jobs = M.d_jobs;
-        A.res = P.fres;
-        A.cell = P.fcell;
-        A.dt = dt;
-        A.sub_cap = P.sub_cap;
-        A.eps = 1.0e-6f;
-        A.pace = P.pace;
-        A.has_sc2 = 1;
-        const float nu_w = host::dynamic_viscosity(3, 1.0f);
-        A.nu_c = nu_w;
-        A.mob_c = host::sheet_mobility_for(nu_w);
-        for (int k = 1; k <= 8; ++k) A.decay_w[k] = expf(-host::sheet_damp(nu_w) * (dt / (float)k));
-        FCK(patch::launch_patch_step(A, 2 * L.np, W.st));
-    }
+    FCK(window::launch_window_step(TAB(window::Job, L.off_jobs), 2 * L.np, W.st));
     for (int p = 0; p < L.np; ++p) {
         PatchState* S = P.patches[p];
         const JobList& J = L.fine_peel[p];
@@ -1281,7 +1264,6 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     const int n2 = P.sub * P.sub;
     FCK(cudaMalloc(&M->owner, n));
     FCK(cudaMemsetAsync(M->owner, 0xff, n, st));
-    FCK(cudaMalloc(&M->d_jobs, 2 * MAX_PATCHES * sizeof(patch::Job)));
     FCK(cudaMalloc(&M->slot_map, n * sizeof(int)));
     FCK(cudaMalloc(&M->pool, (size_t)NEAR_POOL * 4 * n2 * sizeof(float)));
     FCK(cudaMalloc(&M->meta, NEAR_POOL * sizeof(NearMeta)));
@@ -1316,7 +1298,6 @@ void destroy(Patches& P) {
         delete HS;
     }
     cudaFree(M->owner);
-    cudaFree(M->d_jobs);
     cudaFree(M->slot_map);
     cudaFree(M->pool);
     cudaFree(M->meta);

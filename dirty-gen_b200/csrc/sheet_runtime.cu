@@ -22,6 +22,7 @@
 #include "sheet_grid.cuh"
 #include "sheet_host_math.h"
 #include "sheet_ops.cuh"
+#include "sheet_window.cuh"
 
 namespace {
 
@@ -89,6 +90,13 @@ struct silt_sheet {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<cudaEvent_t> ev_used;   // groups of three: start, after force, after transport
     silt_step_parts parts;
+    // Window engine for the coarse pair (SILT_ENGINE_WINDOW).
+    int engine = SILT_ENGINE_GRID;
+    float* win_planes = nullptr;                  // 2 layers x SCRATCH_PLANES x n
+    silt::window::Job* d_win_jobs = nullptr;      // 2 slots x 2 layers
+    silt::window::Job* h_win_jobs = nullptr;      // pinned staging
+    cudaEvent_t win_ev[2] = {nullptr, nullptr};
+    int win_flip = 0;
 
     float* H(int l) { return h[l][cur]; }
     float* U(int l) { return u[l][cur]; }
@@ -226,6 +234,72 @@ int step_coarse_pair(silt_sheet* s, float dt) {
     return SILT_OK;
 }
 
+// The coarse pair on the window engine: one CTA per layer steps it box by
+// box exactly as FluidCore::step_pair does (serial inner loops, so the
+// Gauss-Seidel confinement), in place on the current planes.
+int step_coarse_pair_window(silt_sheet* s, float dt) {
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    const int slot = s->win_flip;
+    s->win_flip ^= 1;
+    CK(cudaEventSynchronize(s->win_ev[slot]));
+    silt::window::Job* jobs = s->h_win_jobs + 2 * slot;
+    const float nu_w = water_nu();
+    for (int l = 0; l < 2; ++l) {
+        silt::window::Job& J = jobs[l];
+        memset(&J, 0, sizeof J);
+        J.h = s->H(l);
+        J.u = s->U(l);
+        J.v = s->V(l);
+        J.bed = s->bed;
+        J.grain = s->grain;
+        J.moisture = s->moisture;
+        silt::window::attach_scratch(J, s->win_planes + (size_t)l * silt::window::SCRATCH_PLANES * s->n, s->n);
+        J.ledger = s->d_acc + l;
+        J.res = s->res;
+        J.cell = s->cfg.cell;
+        J.dt = dt;
+        J.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
+        J.sub_cap = 8.0f;
+        J.eps = 1.0e-6f;
+        J.nu_mode = l == 0 ? silt::window::NU_CONST : silt::window::NU_GRAIN;
+        J.nu_c = nu_w;
+        J.mob_c = silt::host::sheet_mobility_for(nu_w);
+        for (int k = 1; k <= 8; ++k) J.decay_c[k] = expf(-silt::host::sheet_damp(nu_w) * (dt / (float)k));
+        J.soften_edge = s->cfg.soften_border ? std::max(s->res / 12, 2) : 0;
+        J.has_sc2 = 1;
+        J.active = 1;
+    }
+    CK(cudaMemcpyAsync(s->d_win_jobs + 2 * slot, jobs, 2 * sizeof(silt::window::Job), cudaMemcpyHostToDevice, s->st));
+    CK(cudaEventRecord(s->win_ev[slot], s->st));
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (s->timing) {
+        for (cudaEvent_t* e : {&ev0, &ev1}) {
+            if (s->ev_pool.empty()) {
+                cudaEvent_t x;
+                CK(cudaEventCreate(&x));
+                s->ev_pool.push_back(x);
+            }
+            *e = s->ev_pool.back();
+            s->ev_pool.pop_back();
+        }
+        CK(cudaEventRecord(ev0, s->st));
+    }
+    CK(silt::window::launch_window_step(s->d_win_jobs + 2 * slot, 2, s->st));
+    if (s->timing) {
+        CK(cudaEventRecord(ev1, s->st));
+        // Force time only; the transport runs inside the same kernel.
+        s->ev_used.push_back(ev0);
+        s->ev_used.push_back(ev1);
+        s->ev_used.push_back(ev1);
+    }
+    s->parts.launches += 1;
+    s->parts.force_launches += 1;
+    s->parts.force_cells += (int64_t)s->n;
+    s->vmax_bound = silt::host::kSpeedCap * 1.4142137f;
+    return SILT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -248,6 +322,7 @@ void silt_cfg_default(silt_cfg* c) {
     c->center_z = 0.0f;
     c->device = 0;
     c->stream = nullptr;
+    c->engine = SILT_ENGINE_AUTO;
 }
 
 int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
@@ -292,6 +367,21 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 4 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
+    s->engine = cfg->engine == SILT_ENGINE_WINDOW || cfg->engine == SILT_ENGINE_GRID
+                    ? cfg->engine
+                    : (cfg->res <= silt::window::MAX_RES ? SILT_ENGINE_WINDOW : SILT_ENGINE_GRID);
+    if (s->engine == SILT_ENGINE_WINDOW && cfg->res > silt::window::MAX_RES) {
+        silt_sheet_destroy(s);
+        return fail_arg("window engine serves windows up to 512 cells per side");
+    }
+    if (s->engine == SILT_ENGINE_WINDOW) {
+        const size_t wp = 2 * (size_t)silt::window::SCRATCH_PLANES * s->n * sizeof(float);
+        if (e == cudaSuccess) e = cudaMalloc(&s->win_planes, wp);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->win_planes, 0, wp, s->st);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_win_jobs, 4 * sizeof(silt::window::Job));
+        if (e == cudaSuccess) e = cudaMallocHost(&s->h_win_jobs, 4 * sizeof(silt::window::Job));
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&s->win_ev[k], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
         silt_sheet_destroy(s);
         return e == cudaErrorMemoryAllocation ? SILT_ENOMEM : fail_cuda(e, "allocate window");
@@ -340,6 +430,11 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->d_u32);
     cudaFree(s->d_planes);
     if (s->h_acc) cudaFreeHost(s->h_acc);
+    cudaFree(s->win_planes);
+    cudaFree(s->d_win_jobs);
+    if (s->h_win_jobs) cudaFreeHost(s->h_win_jobs);
+    for (int k = 0; k < 2; ++k)
+        if (s->win_ev[k]) cudaEventDestroy(s->win_ev[k]);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_used) cudaEventDestroy(e);
     if (s->own_stream) cudaStreamDestroy(s->st);
@@ -536,7 +631,8 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     silt::fine::StepOut fo;
     rc = silt::fine::step_patches(s->fine, s, ps, dt, fo);
     if (rc) return rc;
-    if ((rc = step_coarse_pair(s, dt))) return rc;
+    rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
+    if (rc) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
     int32_t nev = 0;
@@ -780,10 +876,47 @@ int silt_set_near_field(silt_sheet* s, int32_t on) {
 }
 
 // ---------------------------------------------------------------- free operator
-size_t silt_step_sheet_scratch_bytes(int32_t res) {
+// Free-operator scratch: up to 512 cells per side, a 4 KiB header holding
+// the window job, then the window engine's planes; above, 256 bytes of
+// reduction words and the grid engine's three planes.
+static size_t step_sheet_scratch(int32_t res) {
     if (res <= 0) return 0;
     size_t n = (size_t)res * res;
+    if (res <= silt::window::MAX_RES) return 4096 + (size_t)silt::window::SCRATCH_PLANES * n * sizeof(float);
     return 256 + 3 * n * sizeof(float);
+}
+
+size_t silt_step_sheet_scratch_bytes(int32_t res) { return step_sheet_scratch(res); }
+
+// The free operator on the window engine: exact, asynchronous (the substep
+// count and the wet test are decided on the device).
+static int step_sheet_window(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
+                             int32_t res, float cell, float dt, float vorticity, void* scratch, cudaStream_t st) {
+    const size_t n = (size_t)res * res;
+    silt::window::Job J;
+    memset(&J, 0, sizeof J);
+    J.h = h;
+    J.u = u;
+    J.v = v;
+    J.bed = bed;
+    J.nu_plane = nu;
+    J.gate = gate;
+    silt::window::attach_scratch(J, reinterpret_cast<float*>((char*)scratch + 4096), n);
+    J.res = res;
+    J.cell = cell;
+    J.dt = dt;
+    J.vort = vorticity;
+    J.sub_cap = 8.0f;
+    J.eps = 1.0e-6f;
+    J.nu_mode = silt::window::NU_PLANE;
+    J.inner_par = 1;
+    J.has_sc2 = 0;
+    J.active = 1;
+    silt::window::Job* d_job = reinterpret_cast<silt::window::Job*>(scratch);
+    // From the stack: the copy is staged before this call returns.
+    CK(cudaMemcpyAsync(d_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
+    CK(silt::window::launch_window_step(d_job, 1, st));
+    return SILT_OK;
 }
 
 int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate, int32_t res,
@@ -795,6 +928,8 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)res * res;
     if (((uintptr_t)scratch & 15) != 0) return fail_arg("step_sheet: scratch must be 16-byte aligned");
+    if (res <= silt::window::MAX_RES)
+        return step_sheet_window(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, (cudaStream_t)stream);
     // Scratch layout: [0, 32) speed bits, [32, 48) two FP64 sums, [256, ...) u, v, h planes.
     unsigned int* d_bits = (unsigned int*)scratch;
     double* d_sum = (double*)((char*)scratch + 32);
@@ -857,14 +992,14 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
 
 // ------------------------------------------------------ free operator, no alloc
 // Scratch for silt_step_sheet_noalloc: the layout silt_step_sheet expects
-// (256 bytes of reduction words, then the u, v and depth planes) for the
-// largest grid it serves. Every GPU that loads the library holds this array
+// (a 4 KiB job header, then the window engine's scratch planes) for the
+// largest grid it serves. Zero at load, as a first caller scratch must be. Every GPU that loads the library holds this array
 // until the process exits. In host code `g_step_sheet_scratch` is only a
 // stand-in symbol, never a device address: the address comes from
 // cudaGetSymbolAddress, looked up once per device with that device current.
 static __device__ __align__(256) unsigned char
-    g_step_sheet_scratch[256 + 3 * (size_t)SILT_STEP_SHEET_STATIC_MAX_RES * SILT_STEP_SHEET_STATIC_MAX_RES *
-                                   sizeof(float)];
+    g_step_sheet_scratch[4096 + (size_t)silt::window::SCRATCH_PLANES * SILT_STEP_SHEET_STATIC_MAX_RES *
+                                    SILT_STEP_SHEET_STATIC_MAX_RES * sizeof(float)];
 
 static std::mutex g_scratch_mu;
 static void* g_scratch_addr[64] = {nullptr};

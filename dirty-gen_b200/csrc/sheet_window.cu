@@ -1,0 +1,869 @@
+// Window engine: one CTA steps one layer of one window (up to 512 x 512
+// cells) exactly as the reference's step_sheet does (x3-team/Dirty-gen
+// src/fluid_core.rs:821-2082): work boxes chosen per step, the CFL substep
+// count, then every substep box by box with the per-sheet scratch planes the
+// reference keeps between calls. It serves the nested 2 cm patches, the
+// coarse 20 cm window and batches of windows (one CTA per window layer).
+//
+// Exactness notes, each a property of the reference this engine keeps:
+// * A box-edge cell reads pressure and blur values an earlier box or an
+//   earlier step left in the scratch; the same scratch planes with the same
+//   writes reproduce those reads.
+// * The coarse pair confines vorticity in a raster-order Gauss-Seidel sweep
+//   (force_gravity_open, :2234-2260). Here the sweep is solved as a fixed
+//   point: every wet cell's final velocity is u_grav + kick(final values of
+//   the cells before it, its own post-gravity value, pre-gravity values of
+//   the cells after it). Passes run until one changes no bit, which makes
+//   every cell satisfy its own sweep equation, i.e. the sequential result;
+//   past a pass limit one thread runs the sweep itself.
+// * Fine sheets and the free operator's large boxes confine from a snapshot
+//   (Jacobi), as the reference does there.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sheet_math.cuh"
+#include "sheet_window.cuh"
+
+namespace silt {
+namespace window {
+
+constexpr int NT = 512;            // threads per CTA
+constexpr int SLEEP_TILE = 8;      // src/fluid_core.rs:1528
+constexpr int MAX_TILES = (MAX_RES / SLEEP_TILE) * (MAX_RES / SLEEP_TILE);
+constexpr int MAX_BOXES = 512;
+constexpr int GS_MAX_PASSES = 256;
+
+struct Box {
+    int i0, i1, j0, j1;
+};
+
+struct Shared {
+    int lab[MAX_TILES];
+    unsigned char hot[MAX_TILES];
+    unsigned char grown[MAX_TILES];
+    int bbox[4][MAX_BOXES];
+    int row_count[MAX_RES];
+    int nbox;
+    int changed;
+    float red_f[NT / 32];
+    double red_d[NT / 32];
+    int red_i[4][NT / 32];
+};
+
+#define CTA_RECT(I0, I1, J0, J1, ...)                                               \
+    {                                                                               \
+        const int ri0_ = (I0), rj0_ = (J0);                                         \
+        const int rw_ = (I1) - ri0_ + 1, rh_ = (J1) - rj0_ + 1;                    \
+        if (rw_ > 0 && rh_ > 0) {                                                   \
+            const int rn_ = rw_ * rh_;                                              \
+            for (int k_ = threadIdx.x; k_ < rn_; k_ += NT) {                        \
+                const int j = rj0_ + k_ / rw_;                                      \
+                const int i = ri0_ + k_ % rw_;                                      \
+                const int g = j * res + i;                                          \
+                (void)g;                                                            \
+                __VA_ARGS__                                                         \
+            }                                                                       \
+        }                                                                           \
+    }
+
+__device__ __forceinline__ double block_sum_d(Shared& S, double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) S.red_d[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = S.red_d[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) S.red_d[0] = t;
+    }
+    __syncthreads();
+    double r = S.red_d[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ float block_max_f(Shared& S, float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) S.red_f[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float t = S.red_f[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_down_sync(0xffffffffu, t, o));
+        if (threadIdx.x == 0) S.red_f[0] = t;
+    }
+    __syncthreads();
+    float r = S.red_f[0];
+    __syncthreads();
+    return r;
+}
+
+// Four ints reduced together: op 0 = sum, 1 = min, 2 = max.
+__device__ void block_reduce4(Shared& S, int v[4], const int op[4]) {
+    for (int q = 0; q < 4; ++q)
+        for (int o = 16; o > 0; o >>= 1) {
+            int w = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = op[q] == 0 ? v[q] + w : (op[q] == 1 ? min(v[q], w) : max(v[q], w));
+        }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < 4; ++q) S.red_i[q][threadIdx.x >> 5] = v[q];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        for (int q = 0; q < 4; ++q) {
+            int t = S.red_i[q][threadIdx.x];
+            for (int o = 16; o > 0; o >>= 1) {
+                int w = __shfl_down_sync(0xffffffffu, t, o);
+                t = op[q] == 0 ? t + w : (op[q] == 1 ? min(t, w) : max(t, w));
+            }
+            if (threadIdx.x == 0) S.red_i[q][0] = t;
+        }
+    }
+    __syncthreads();
+    for (int q = 0; q < 4; ++q) v[q] = S.red_i[q][0];
+    __syncthreads();
+}
+
+// Five taps along one axis, clamped at the grid edge. Cells at least 2 from
+// the edge start from the first product (accum5), others from 0.0
+// (accum5_clamped), src/fluid_core.rs:3680-3697.
+__device__ __forceinline__ float tap5c(const float* line, int res, int i, float k0, float k1, float k2, int stride) {
+    const bool in = i >= 2 && i <= res - 3;
+    const int i0 = i < 2 ? 0 : i - 2, i1 = i < 1 ? 0 : i - 1;
+    const int i3 = i + 1 > res - 1 ? res - 1 : i + 1, i4 = i + 2 > res - 1 ? res - 1 : i + 2;
+    float a0 = line[i0 * stride], a1 = line[i1 * stride], a2 = line[i * stride], a3 = line[i3 * stride],
+          a4 = line[i4 * stride];
+    float a = in ? a0 * k0 : 0.0f + a0 * k0;
+    a += a1 * k1;
+    a += a2 * k2;
+    a += a3 * k1;
+    a += a4 * k0;
+    return a;
+}
+
+// blur_box (src/fluid_core.rs:3541-3569): x pass of the box rows into tmp,
+// then the z pass into dst, which reads tmp rows outside the box as they are.
+__device__ void cta_blur(const float* src, float* dst, float* tmp, int res, const Box& b, float k0, float k1,
+                         float k2) {
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, { tmp[g] = tap5c(src + j * res, res, i, k0, k1, k2, 1); })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, { dst[g] = tap5c(tmp + i, res, j, k0, k1, k2, res); })
+    __syncthreads();
+}
+
+__device__ __forceinline__ float job_nu(const Job& J, int g) {
+    if (J.nu_mode == NU_CONST) return J.nu_c;
+    if (J.nu_mode == NU_PLANE) return J.nu_plane[g];
+    return dynamic_viscosity(J.grain[g], J.moisture[g]);
+}
+
+// transport_open_rows (src/fluid_core.rs:3025-3137) on one box (banks off).
+__device__ void cta_transport(const Job& J, const Box& b, float dt) {
+    const int res = J.res;
+    float* h = J.h;
+    float* F1 = J.f1;
+    float* F2 = J.f2;
+    const float cell = J.cell;
+    const uint8_t* gate = J.gate;
+    CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
+        float speed = 0.5f * (J.u[g] + J.u[g + 1]);
+        float dh = open_edge_dh(false, h[g + 1], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
+        F1[g] = speed > 0.0f ? 0.0f : dh;
+    })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
+        float speed = 0.5f * (J.u[g] + J.u[g + 1]);
+        float prev = i > b.i0 ? F1[g - 1] : 0.0f;
+        float dh = open_edge_dh(false, h[g], h[g + 1], 0.0f + prev, gate ? gate[g + 1] : 1, 0.0f, 0.0f, speed, dt,
+                                cell, 0.45f);
+        F2[g] = speed > 0.0f ? dh : 0.0f;
+    })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        float flm = i > b.i0 ? F1[g - 1] : 0.0f, frm = i > b.i0 ? F2[g - 1] : 0.0f;
+        float flc = i < b.i1 ? F1[g] : 0.0f, frc = i < b.i1 ? F2[g] : 0.0f;
+        float rem = (0.0f + flm) + frc, add = (0.0f + frm) + flc;
+        float hv = h[g];
+        float moved = fmaxf(hv - rem + add, 0.0f);
+        h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+    })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
+        float speed = 0.5f * (J.v[g] + J.v[g + res]);
+        float dh = open_edge_dh(false, h[g + res], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
+        F1[g] = speed > 0.0f ? 0.0f : dh;
+    })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
+        float speed = 0.5f * (J.v[g] + J.v[g + res]);
+        float ra = j > b.j0 ? 0.0f + F1[g - res] : 0.0f;
+        float dh = open_edge_dh(false, h[g], h[g + res], ra, gate ? gate[g + res] : 1, 0.0f, 0.0f, speed, dt, cell,
+                                0.45f);
+        F2[g] = speed > 0.0f ? dh : 0.0f;
+    })
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        float upm = j > b.j0 ? F1[g - res] : 0.0f, dnm = j > b.j0 ? F2[g - res] : 0.0f;
+        float upc = j < b.j1 ? F1[g] : 0.0f, dnc = j < b.j1 ? F2[g] : 0.0f;
+        float rem = (0.0f + upm) + dnc, add = (0.0f + dnm) + upc;
+        float hv = h[g];
+        float moved = fmaxf(hv - rem + add, 0.0f);
+        h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+    })
+    __syncthreads();
+}
+
+__device__ void cta_dry_cut(const Job& J, const Box& b) {
+    const int res = J.res;
+    if (!(J.eps > 0.0f)) return;
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (J.h[g] < J.eps) {
+            J.h[g] = 0.0f;
+            J.u[g] = 0.0f;
+            J.v[g] = 0.0f;
+        }
+    })
+    __syncthreads();
+}
+
+// The confinement kick at (i, j) from the velocities `uu`, `vv` return for
+// any cell (src/fluid_core.rs:3442-3471 with clamped indices; the interior
+// form :2805-2831 gives the same values).
+template <class UF, class VF>
+__device__ __forceinline__ bool conf_kick(int i, int j, int res, float two, float dt, float vort, UF uu, VF vv,
+                                          float& du, float& dv) {
+    auto vort_at = [&](int a, int c) {
+        const int ip = min(a + 1, res - 1), im = max(a - 1, 0), jp = min(c + 1, res - 1), jm = max(c - 1, 0);
+        float dvdx = (vv(ip, c) - vv(im, c)) / two;
+        float dudz = (uu(a, jp) - uu(a, jm)) / two;
+        return dvdx - dudz;
+    };
+    float w = vort_at(i, j);
+    if (!finite_f(w) || fabsf(w) < 1.0e-4f) return false;
+    float wxp = fabsf(vort_at(min(i + 1, res - 1), j));
+    float wxm = fabsf(vort_at(max(i - 1, 0), j));
+    float wzp = fabsf(vort_at(i, min(j + 1, res - 1)));
+    float wzm = fabsf(vort_at(i, max(j - 1, 0)));
+    float nx = (wxp - wxm) / two;
+    float nz = (wzp - wzm) / two;
+    du = vort * dt * (-nz * w);
+    dv = vort * dt * (nx * w);
+    return finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f;
+}
+
+// Gravity then the raster-order Gauss-Seidel confinement on one box
+// (force_gravity_open's serial sweep, src/fluid_core.rs:2234-2260).
+__device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float* p, float dt) {
+    const int res = J.res;
+    const float eps = J.eps, two = 2.0f * J.cell;
+    float* U0 = J.gs[0];
+    float* V0 = J.gs[1];
+    float* UG = J.gs[2];
+    float* VG = J.gs[3];
+    {
+        const int x0 = max(b.i0 - 2, 0), x1 = min(b.i1 + 2, res - 1), y0 = max(b.j0 - 2, 0),
+                  y1 = min(b.j1 + 2, res - 1);
+        CTA_RECT(x0, x1, y0, y1, {
+            U0[g] = J.u[g];
+            V0[g] = J.v[g];
+        })
+    }
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (J.h[g] > eps) {
+            const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+            float px = (p[j * res + ip] - p[j * res + im]) / two;
+            float pz = (p[jp * res + i] - p[jm * res + i]) / two;
+            float mob = J.nu_mode == NU_CONST ? J.mob_c : sheet_mobility_for(job_nu(J, g));
+            float ug = J.u[g] + -kGravity * px * mob * dt;
+            float vg = J.v[g] + -kGravity * pz * mob * dt;
+            UG[g] = ug;
+            VG[g] = vg;
+            J.u[g] = ug;
+            J.v[g] = vg;
+        }
+    })
+    __syncthreads();
+    if (!(J.vort > 0.0f)) return 0;
+    // Fixed point of the sweep: cells before (i, j) in raster order read their
+    // final values, (i, j) itself its post-gravity value, cells after it their
+    // pre-gravity values.
+    int passes = 0;
+    for (; passes < GS_MAX_PASSES; ++passes) {
+        if (threadIdx.x == 0) S.changed = 0;
+        __syncthreads();
+        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+            if (J.h[g] > eps) {
+                auto pick = [&](const float* X, const float* G0, const float* SG, int a, int c) {
+                    if (a == i && c == j) return SG[g];
+                    const bool before = c < j || (c == j && a < i);
+                    return before ? X[c * res + a] : G0[c * res + a];
+                };
+                auto uu = [&](int a, int c) { return pick(J.u, U0, UG, a, c); };
+                auto vv = [&](int a, int c) { return pick(J.v, V0, VG, a, c); };
+                float du, dv;
+                float nu_ = UG[g], nv_ = VG[g];
+                if (conf_kick(i, j, res, two, dt, J.vort, uu, vv, du, dv)) {
+                    nu_ = UG[g] + du;
+                    nv_ = VG[g] + dv;
+                }
+                if (__float_as_uint(nu_) != __float_as_uint(J.u[g]) || __float_as_uint(nv_) != __float_as_uint(J.v[g])) {
+                    J.u[g] = nu_;
+                    J.v[g] = nv_;
+                    S.changed = 1;
+                }
+            }
+        })
+        __syncthreads();
+        if (!S.changed) break;
+        __syncthreads();
+    }
+    if (passes < GS_MAX_PASSES) return passes + 1;
+    // Pass limit reached: the sweep itself, in raster order, on one thread.
+    if (threadIdx.x == 0) {
+        for (int j = b.j0; j <= b.j1; ++j)
+            for (int i = b.i0; i <= b.i1; ++i) {
+                const int g = j * res + i;
+                if (!(J.h[g] > eps)) continue;
+                auto pick = [&](const float* X, const float* G0, const float* SG, int a, int c) {
+                    if (a == i && c == j) return SG[g];
+                    const bool before = c < j || (c == j && a < i);
+                    return before ? X[c * res + a] : G0[c * res + a];
+                };
+                auto uu = [&](int a, int c) { return pick(J.u, U0, UG, a, c); };
+                auto vv = [&](int a, int c) { return pick(J.v, V0, VG, a, c); };
+                float du, dv;
+                if (conf_kick(i, j, res, two, dt, J.vort, uu, vv, du, dv)) {
+                    J.u[g] = UG[g] + du;
+                    J.v[g] = VG[g] + dv;
+                } else {
+                    J.u[g] = UG[g];
+                    J.v[g] = VG[g];
+                }
+            }
+    }
+    __syncthreads();
+    return -1;
+}
+
+// Gravity then snapshot-Jacobi confinement (force_gravity_par :2263-2378,
+// gravity_jacobi_serial :2530-2595).
+__device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* p, float dt) {
+    const int res = J.res;
+    const float eps = J.eps, two = 2.0f * J.cell;
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (J.h[g] > eps) {
+            const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+            float px = (p[j * res + ip] - p[j * res + im]) / two;
+            float pz = (p[jp * res + i] - p[jm * res + i]) / two;
+            float mob = J.nu_mode == NU_CONST ? J.mob_c : sheet_mobility_for(job_nu(J, g));
+            J.u[g] += -kGravity * px * mob * dt;
+            J.v[g] += -kGravity * pz * mob * dt;
+        }
+    })
+    __syncthreads();
+    if (!(J.vort > 0.0f)) return;
+    float* W = J.f1;
+    {
+        const int wi0 = max(b.i0 - 1, 0), wi1 = min(b.i1 + 1, res - 1);
+        const int wj0 = max(b.j0 - 1, 0), wj1 = min(b.j1 + 1, res - 1);
+        CTA_RECT(wi0, wi1, wj0, wj1, {
+            const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+            float dvdx = (J.v[j * res + ip] - J.v[j * res + im]) / two;
+            float dudz = (J.u[jp * res + i] - J.u[jm * res + i]) / two;
+            W[g] = dvdx - dudz;
+        })
+    }
+    __syncthreads();
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (J.h[g] > eps) {
+            float w = W[g];
+            if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
+                const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+                float wxp = fabsf(W[j * res + ip]), wxm = fabsf(W[j * res + im]);
+                float wzp = fabsf(W[jp * res + i]), wzm = fabsf(W[jm * res + i]);
+                float nx = (wxp - wxm) / two;
+                float nz = (wzp - wzm) / two;
+                float du = J.vort * dt * (-nz * w);
+                float dv = J.vort * dt * (nx * w);
+                if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
+                    J.u[g] += du;
+                    J.v[g] += dv;
+                }
+            }
+        }
+    })
+    __syncthreads();
+}
+
+// substep (src/fluid_core.rs:1879-2082), open sheet, gravity drive.
+__device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* sc, float dt, float decay_c,
+                           bool do_flux, bool inner_par) {
+    const int res = J.res;
+    float* sa = sc[0];
+    float* sb = sc[1];
+    float* scc = sc[2];
+    float* sd = sc[3];
+    float* se = sc[4];
+    const float eps = J.eps, cell = J.cell;
+    const bool fine = cell <= kFineCell + 1.0e-6f;
+    {
+        const int hi0 = max(b.i0 - 2, 0), hi1 = min(b.i1 + 2, res - 1);
+        const int hj0 = max(b.j0 - 2, 0), hj1 = min(b.j1 + 2, res - 1);
+        CTA_RECT(hi0, hi1, hj0, hj1, { sa[g] = J.bed[g] + J.h[g]; })
+    }
+    __syncthreads();
+    cta_blur(sa, sb, se, res, b, kG0, kG1, kG2);
+    cta_blur(sa, scc, se, res, b, kS0, kS1, kS2);
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        float filtered = 0.62f * sb[g] + 0.38f * scc[g];
+        sd[g] = 0.45f * filtered + 0.55f * sa[g];
+    })
+    __syncthreads();
+    const bool par = (b.j1 - b.j0 >= 47) && (b.i1 - b.i0 >= 31) && inner_par;
+    int passes = 0;
+    if (fine || par)
+        cta_gravity_jacobi(J, b, sd, dt);
+    else
+        passes = cta_gravity_gs(S, J, b, sd, dt);
+    const bool project = !fine;
+    if (project) {
+        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+            const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+            float ux = (J.u[j * res + ip] - J.u[j * res + im]) / (2.0f * cell);
+            float vz = (J.v[jp * res + i] - J.v[jm * res + i]) / (2.0f * cell);
+            float div = ux + vz;
+            float s = sa[j * res + ip] + sa[j * res + im] + sa[jp * res + i] + sa[jm * res + i] - 4.0f * sa[g];
+            float lap_h = s / (cell * cell);
+            float overload = 1.0f + rclamp(job_nu(J, g) / 231.0f, 0.0f, 6.0f);
+            sb[g] = div * overload - 0.015f * overload * lap_h;
+        })
+        __syncthreads();
+        cta_blur(sb, scc, se, res, b, kG0, kG1, kG2);
+        cta_blur(sb, sa, se, res, b, kS0, kS1, kS2);
+        CTA_RECT(b.i0, b.i1, b.j0, b.j1, { sd[g] = 0.62f * scc[g] + 0.38f * sa[g]; })
+        __syncthreads();
+    }
+    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (J.h[g] > eps) {
+            if (project) {
+                const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+                float qx = (sd[j * res + ip] - sd[j * res + im]) / (2.0f * cell);
+                float qz = (sd[jp * res + i] - sd[jm * res + i]) / (2.0f * cell);
+                J.u[g] += 0.012f * dt * qx;
+                J.v[g] += 0.012f * dt * qz;
+            }
+            float decay = J.nu_mode == NU_CONST ? decay_c : expf(-sheet_damp(job_nu(J, g)) * dt);
+            J.u[g] = finite_speed(J.u[g] * decay, kSpeedCap);
+            J.v[g] = finite_speed(J.v[g] * decay, kSpeedCap);
+        }
+    })
+    __syncthreads();
+    if (do_flux) {
+        cta_transport(J, b, dt);
+        cta_dry_cut(J, b);
+    }
+    return passes;
+}
+
+// awake_work_boxes (src/fluid_core.rs:1537-1657).
+__device__ void cta_awake_boxes(Shared& S, const Job& J) {
+    const int res = J.res;
+    const int tiles = (res + SLEEP_TILE - 1) / SLEEP_TILE;
+    const int ntile = tiles * tiles;
+    for (int t = threadIdx.x; t < ntile; t += NT) {
+        S.hot[t] = 0;
+        S.grown[t] = 0;
+    }
+    __syncthreads();
+    const float eps = J.eps, cell = J.cell;
+    CTA_RECT(0, res - 1, 0, res - 1, {
+        float hv = J.h[g];
+        if (hv > eps) {
+            bool awake = hypotf(J.u[g], J.v[g]) > 0.05f;
+            if (!awake) {
+                float eta = J.bed[g] + hv;
+                int ip = i + 1 < res ? g + 1 : g;
+                int jp = j + 1 < res ? g + res : g;
+                float dex = fabsf(J.bed[ip] + J.h[ip] - eta);
+                float dez = fabsf(J.bed[jp] + J.h[jp] - eta);
+                awake = fmaxf(dex, dez) > 0.02f * cell;
+            }
+            if (awake) S.hot[(j / SLEEP_TILE) * tiles + i / SLEEP_TILE] = 1;
+        }
+    })
+    __syncthreads();
+    for (int t = threadIdx.x; t < ntile; t += NT) {
+        int ti = t % tiles, tj = t / tiles;
+        unsigned char gr = 0;
+        for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di) {
+                int ni = ti + di, nj = tj + dj;
+                if (ni >= 0 && nj >= 0 && ni < tiles && nj < tiles && S.hot[nj * tiles + ni]) gr = 1;
+            }
+        S.grown[t] = gr;
+        S.lab[t] = gr ? t : 0x7fffffff;
+    }
+    __syncthreads();
+    // Component label = first tile in raster order, the order the reference's scan finds them.
+    for (int iter = 0; iter < 4 * MAX_TILES; ++iter) {
+        if (threadIdx.x == 0) S.changed = 0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < ntile; t += NT) {
+            if (!S.grown[t]) continue;
+            int ti = t % tiles, tj = t / tiles;
+            int m = S.lab[t];
+            if (ti > 0 && S.grown[t - 1]) m = min(m, S.lab[t - 1]);
+            if (ti + 1 < tiles && S.grown[t + 1]) m = min(m, S.lab[t + 1]);
+            if (tj > 0 && S.grown[t - tiles]) m = min(m, S.lab[t - tiles]);
+            if (tj + 1 < tiles && S.grown[t + tiles]) m = min(m, S.lab[t + tiles]);
+            m = min(m, S.lab[m]);
+            if (m < S.lab[t]) {
+                atomicMin(&S.lab[t], m);
+                S.changed = 1;
+            }
+        }
+        __syncthreads();
+        if (!S.changed) break;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        int nb = 0;
+        for (int t = 0; t < ntile; ++t)
+            if (S.grown[t] && S.lab[t] == t && nb < MAX_BOXES) {
+                S.bbox[0][nb] = t % tiles;
+                S.bbox[1][nb] = t % tiles;
+                S.bbox[2][nb] = t / tiles;
+                S.bbox[3][nb] = t / tiles;
+                S.lab[t] = -(nb + 1);
+                ++nb;
+            }
+        S.nbox = nb;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < ntile; t += NT) {
+        if (!S.grown[t]) continue;
+        int r = S.lab[t];
+        int slot = r < 0 ? -r - 1 : -S.lab[r] - 1;
+        if (slot < 0 || slot >= MAX_BOXES) continue;
+        int ti = t % tiles, tj = t / tiles;
+        atomicMin(&S.bbox[0][slot], ti);
+        atomicMax(&S.bbox[1][slot], ti);
+        atomicMin(&S.bbox[2][slot], tj);
+        atomicMax(&S.bbox[3][slot], tj);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < S.nbox; ++k) {
+            int ti0 = S.bbox[0][k], ti1 = S.bbox[1][k], tj0 = S.bbox[2][k], tj1 = S.bbox[3][k];
+            S.bbox[0][k] = ti0 * SLEEP_TILE;
+            S.bbox[1][k] = min((ti1 + 1) * SLEEP_TILE, res) - 1;
+            S.bbox[2][k] = tj0 * SLEEP_TILE;
+            S.bbox[3][k] = min((tj1 + 1) * SLEEP_TILE, res) - 1;
+        }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool boxes_touch(int a0, int a1, int a2, int a3, int b0, int b1, int b2, int b3) {
+    auto ss = [](int x) { return x > 0 ? x - 1 : 0; };
+    return ss(a0) <= b1 + 1 && ss(b0) <= a1 + 1 && ss(a2) <= b3 + 1 && ss(b2) <= a3 + 1;
+}
+
+__device__ __forceinline__ int uf_find(const int* L, int x) {
+    for (int n = 0; n < (1 << 20); ++n) {
+        int p = L[x];
+        if (p == x || p < 0) return x;
+        x = p;
+    }
+    return x;
+}
+
+__device__ void set_whole(Shared& S, int x0, int x1, int y0, int y1) {
+    if (threadIdx.x == 0) {
+        S.nbox = 1;
+        S.bbox[0][0] = x0;
+        S.bbox[1][0] = x1;
+        S.bbox[2][0] = y0;
+        S.bbox[3][0] = y1;
+    }
+    __syncthreads();
+}
+
+// sheet_work_boxes (src/fluid_core.rs:1325-1447). Wet bodies are labelled in
+// the f2 plane (as ints) by union-find; a body's root is its first wet cell
+// in raster order, the order the reference's run merge keeps.
+__device__ void cta_wet_boxes(Shared& S, const Job& J) {
+    const int res = J.res;
+    const float eps = J.eps;
+    int v[4] = {0, res, 1, res};
+    int vj1 = -1;
+    CTA_RECT(0, res - 1, 0, res - 1, {
+        if (J.h[g] > eps) {
+            v[0] += 1;
+            v[1] = min(v[1], i);
+            v[2] = min(v[2], -i);
+            v[3] = min(v[3], j);
+            vj1 = max(vj1, j);
+        }
+    })
+    {
+        const int op[4] = {0, 1, 1, 1};
+        block_reduce4(S, v, op);
+        int t[4] = {vj1, 0, 0, 0};
+        const int op2[4] = {2, 2, 2, 2};
+        block_reduce4(S, t, op2);
+        vj1 = t[0];
+    }
+    const int wet = v[0], i0 = v[1], i1 = -v[2], j0 = v[3], j1 = vj1;
+    if (wet == 0) {
+        if (threadIdx.x == 0) S.nbox = 0;
+        __syncthreads();
+        return;
+    }
+    const int x0 = max(i0 - 3, 0), x1 = min(i1 + 3, res - 1), y0 = max(j0 - 3, 0), y1 = min(j1 + 3, res - 1);
+    if (wet == (i1 - i0 + 1) * (j1 - j0 + 1)) {
+        set_whole(S, x0, x1, y0, y1);
+        return;
+    }
+    int* L = reinterpret_cast<int*>(J.f2);
+    CTA_RECT(i0, i1, j0, j1, { L[g] = J.h[g] > eps ? g : -1; })
+    __syncthreads();
+    for (int round = 0; round < 4096; ++round) {
+        if (threadIdx.x == 0) S.changed = 0;
+        __syncthreads();
+        CTA_RECT(i0, i1, j0, j1, {
+            if (L[g] >= 0) {
+                if (i < i1 && L[g + 1] >= 0) {
+                    int a = uf_find(L, g), c = uf_find(L, g + 1);
+                    if (a != c) {
+                        atomicMin(&L[max(a, c)], min(a, c));
+                        S.changed = 1;
+                    }
+                }
+                if (j < j1 && L[g + res] >= 0) {
+                    int a = uf_find(L, g), c = uf_find(L, g + res);
+                    if (a != c) {
+                        atomicMin(&L[max(a, c)], min(a, c));
+                        S.changed = 1;
+                    }
+                }
+            }
+        })
+        __syncthreads();
+        CTA_RECT(i0, i1, j0, j1, {
+            if (L[g] >= 0) L[g] = uf_find(L, g);
+        })
+        __syncthreads();
+        if (!S.changed) break;
+        __syncthreads();
+    }
+    // Roots in raster order: count per row, scan, then number them.
+    const int rows = j1 - j0 + 1;
+    for (int r = threadIdx.x; r < rows; r += NT) {
+        int c = 0;
+        const int j = j0 + r;
+        for (int i = i0; i <= i1; ++i) c += L[j * res + i] == j * res + i;
+        S.row_count[r] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int r = 0; r < rows; ++r) {
+            int c = S.row_count[r];
+            S.row_count[r] = acc;
+            acc += c;
+        }
+        S.nbox = acc;
+    }
+    __syncthreads();
+    const int nbodies = S.nbox;
+    if (nbodies > MAX_BOXES) {  // more bodies than slots: the whole box
+        __syncthreads();
+        set_whole(S, x0, x1, y0, y1);
+        return;
+    }
+    for (int r = threadIdx.x; r < rows; r += NT) {
+        int slot = S.row_count[r];
+        const int j = j0 + r;
+        for (int i = i0; i <= i1; ++i) {
+            const int g = j * res + i;
+            if (L[g] == g) {
+                S.bbox[0][slot] = i;
+                S.bbox[1][slot] = i;
+                S.bbox[2][slot] = j;
+                S.bbox[3][slot] = j;
+                L[g] = -(slot + 2);
+                ++slot;
+            }
+        }
+    }
+    __syncthreads();
+    CTA_RECT(i0, i1, j0, j1, {
+        int r = L[g];
+        if (r >= 0 || r <= -2) {
+            int slot = r >= 0 ? -L[r] - 2 : -r - 2;
+            if (slot >= 0 && slot < MAX_BOXES) {
+                atomicMin(&S.bbox[0][slot], i);
+                atomicMax(&S.bbox[1][slot], i);
+                atomicMin(&S.bbox[2][slot], j);
+                atomicMax(&S.bbox[3][slot], j);
+            }
+        }
+    })
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int nb = nbodies;
+        for (int k = 0; k < nb; ++k) {
+            S.bbox[0][k] = max(S.bbox[0][k] - 6, 0);
+            S.bbox[1][k] = min(S.bbox[1][k] + 6, res - 1);
+            S.bbox[2][k] = max(S.bbox[2][k] - 6, 0);
+            S.bbox[3][k] = min(S.bbox[3][k] + 6, res - 1);
+        }
+        // merge_boxes (src/fluid_core.rs:1459-1487), swap_remove order.
+        for (;;) {
+            bool did = false;
+            int a = 0;
+            while (a < nb) {
+                int c = a + 1;
+                while (c < nb) {
+                    if (boxes_touch(S.bbox[0][a], S.bbox[1][a], S.bbox[2][a], S.bbox[3][a], S.bbox[0][c],
+                                    S.bbox[1][c], S.bbox[2][c], S.bbox[3][c])) {
+                        S.bbox[0][a] = min(S.bbox[0][a], S.bbox[0][c]);
+                        S.bbox[1][a] = max(S.bbox[1][a], S.bbox[1][c]);
+                        S.bbox[2][a] = min(S.bbox[2][a], S.bbox[2][c]);
+                        S.bbox[3][a] = max(S.bbox[3][a], S.bbox[3][c]);
+                        for (int q = 0; q < 4; ++q) S.bbox[q][c] = S.bbox[q][nb - 1];
+                        --nb;
+                        did = true;
+                    } else {
+                        ++c;
+                    }
+                }
+                ++a;
+            }
+            if (!did) break;
+        }
+        if (nb == 1 || nb > 8) {
+            nb = 1;
+            S.bbox[0][0] = x0;
+            S.bbox[1][0] = x1;
+            S.bbox[2][0] = y0;
+            S.bbox[3][0] = y1;
+        }
+        S.nbox = nb;
+    }
+    __syncthreads();
+}
+
+// soften_border (src/fluid_core.rs:9594-9622) on the whole layer.
+__device__ void cta_soften(const Job& J) {
+    const int res = J.res, edge = J.soften_edge;
+    CTA_RECT(0, res - 1, 0, res - 1, {
+        int d = min(min(i, res - 1 - i), min(j, res - 1 - j));
+        if (d < edge) {
+            float t = (float)d / (float)edge;
+            float w = t * t * (3.0f - 2.0f * t);
+            J.u[g] *= w;
+            J.v[g] *= w;
+        }
+    })
+    __syncthreads();
+}
+
+__device__ void cta_ledger(Shared& S, const Job& J) {
+    const int res = J.res;
+    double part = 0.0;
+    CTA_RECT(0, res - 1, 0, res - 1, { part += (double)fmaxf(J.h[g], 0.0f); })
+    part = block_sum_d(S, part);
+    if (threadIdx.x == 0 && J.ledger) *J.ledger = part;
+}
+
+// step_sheet_eps_in + step_sheet_scratch (src/fluid_core.rs:821-852, :1659-1831).
+__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
+    const Job J = jobs[blockIdx.x];
+    if (!J.active) return;
+    int gs_passes = 0;
+    __shared__ Shared S;
+    const int res = J.res;
+    const float eps = J.eps;
+    if (J.soften_edge > 0) cta_soften(J);
+    // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844).
+    double ws = 0.0;
+    CTA_RECT(0, res - 1, 0, res - 1, {
+        float hv = J.h[g];
+        if (hv > eps) ws += (double)hv;
+    })
+    ws = block_sum_d(S, ws);
+    if (!(ws > (double)eps)) {
+        cta_ledger(S, J);
+        return;
+    }
+    const bool open_fine = J.cell <= kFineCell + 1.0e-6f;
+    const bool fine_open = open_fine && J.pace == 0;
+    const bool whole_wet = open_fine && (J.pace == 2 || J.pace == 3);
+    const bool awake = open_fine && !whole_wet && !fine_open;
+    if (fine_open || awake)
+        cta_awake_boxes(S, J);
+    else
+        cta_wet_boxes(S, J);
+    const int nb = S.nbox;
+    if (nb <= 0) {
+        cta_ledger(S, J);
+        return;
+    }
+    const float cap = finite_f(J.sub_cap) ? rclamp(J.sub_cap, 1.0f, 8.0f) : 8.0f;
+    int nsub = 1;
+    if (!fine_open) {
+        float m2 = 0.0f;
+        for (int k = 0; k < nb; ++k) {
+            const Box b = {S.bbox[0][k], S.bbox[1][k], S.bbox[2][k], S.bbox[3][k]};
+            CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+                float uu = J.u[g], vv = J.v[g];
+                float s2 = uu * uu + vv * vv;
+                if (s2 > m2) m2 = s2;
+            })
+        }
+        m2 = block_max_f(S, m2);
+        float max_s = fmaxf(0.15f, sqrtf(m2));
+        nsub = (int)rclamp(ceilf((J.dt * max_s) / (0.42f * fmaxf(J.cell, 1.0e-3f))), 1.0f, cap);
+    }
+    const float dts = J.dt / (float)nsub;
+    float* set0[5] = {J.sc[0][0], J.sc[0][1], J.sc[0][2], J.sc[0][3], J.sc[0][4]};
+    float* set1[5] = {J.sc[1][0], J.sc[1][1], J.sc[1][2], J.sc[1][3], J.sc[1][4]};
+    auto ap = [](int a0, int a1, int b0, int b1) { return a1 + 6 < b0 || b1 + 6 < a0; };
+    const bool two_apart = J.has_sc2 && nb == 2 &&
+                           (ap(S.bbox[0][0], S.bbox[1][0], S.bbox[0][1], S.bbox[1][1]) ||
+                            ap(S.bbox[2][0], S.bbox[3][0], S.bbox[2][1], S.bbox[3][1]));
+    // Two far-apart boxes run on two workers with the inner loops serial.
+    const bool inner = two_apart ? false : (J.inner_par != 0);
+    if (J.pace == 3 && whole_wet && nsub > 1) {
+        for (int k = 0; k < nb; ++k) {
+            const Box b = {S.bbox[0][k], S.bbox[1][k], S.bbox[2][k], S.bbox[3][k]};
+            float* const* sc = (two_apart && k == 1) ? set1 : set0;
+            gs_passes = cta_substep(S, J, b, sc, J.dt, J.decay_c[1], false, inner);
+            for (int s = 0; s < nsub; ++s) cta_transport(J, b, dts);
+            cta_dry_cut(J, b);
+        }
+    } else {
+        for (int s = 0; s < nsub; ++s)
+            for (int k = 0; k < nb; ++k) {
+                const Box b = {S.bbox[0][k], S.bbox[1][k], S.bbox[2][k], S.bbox[3][k]};
+                float* const* sc = (two_apart && k == 1) ? set1 : set0;
+                int p = cta_substep(S, J, b, sc, dts, J.decay_c[nsub], true, inner);
+                gs_passes = p < 0 || gs_passes < 0 ? -1 : max(gs_passes, p);
+            }
+    }
+    cta_ledger(S, J);
+    if (threadIdx.x == 0) jobs[blockIdx.x].gs_iters = gs_passes;
+}
+
+cudaError_t launch_window_step(const Job* d_jobs, int njobs, cudaStream_t st) {
+    if (njobs <= 0) return cudaSuccess;
+    k_window_step<<<njobs, NT, 0, st>>>(const_cast<Job*>(d_jobs));
+    return cudaGetLastError();
+}
+
+size_t window_static_smem() { return sizeof(Shared); }
+
+}  // namespace window
+}  // namespace silt

@@ -19,6 +19,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "silt_sheet.h")
 SILT_OK, SILT_OK_NOOP, SILT_EINVAL, SILT_ECUDA, SILT_ETIMEOUT, SILT_ENOMEM = 0, 1, -1, -2, -3, -4
 CLAY, SILT, SAND, WATER, OTHER = 0, 1, 2, 3, 4
 FINE_MEAN_PATCH, FINE_PER_TIRE = 0, 1
+ENGINE_AUTO, ENGINE_WINDOW, ENGINE_GRID = 0, 1, 2
 
 _f = ctypes.c_float
 _i = ctypes.c_int32
@@ -28,7 +29,7 @@ _p = ctypes.c_void_p
 class Cfg(ctypes.Structure):
     _fields_ = [("res", _i), ("cell", _f), ("fine_res", _i), ("fine_cell", _f), ("fine_layout", _i),
                 ("tire_r", _f), ("soften_border", _i), ("center_x", _f), ("center_z", _f), ("device", _i),
-                ("stream", _p)]
+                ("stream", _p), ("engine", _i)]
 
 
 class TirePush(ctypes.Structure):
@@ -139,7 +140,7 @@ class Sheet:
     """A window of the two-layer sheet on the GPU (FluidCore, src/fluid_core.rs:4808)."""
 
     def __init__(self, res=200, cell=0.2, fine_res=160, fine_cell=0.02, layout=FINE_MEAN_PATCH, tire_r=0.56,
-                 soften=True, center=(0.0, 0.0), device=0, stream=None):
+                 soften=True, center=(0.0, 0.0), device=0, stream=None, engine=ENGINE_AUTO):
         L = lib()
         cfg = Cfg()
         L.silt_cfg_default(ctypes.byref(cfg))
@@ -147,6 +148,7 @@ class Sheet:
         cfg.fine_layout, cfg.tire_r, cfg.soften_border = layout, tire_r, int(soften)
         cfg.center_x, cfg.center_z, cfg.device = center[0], center[1], device
         cfg.stream = stream
+        cfg.engine = engine
         h = _p()
         check(L.silt_sheet_create(ctypes.byref(cfg), ctypes.byref(h)), "silt_sheet_create")
         self.h = h

@@ -60,7 +60,18 @@ typedef struct {
     float center_z;
     int32_t device;       /* CUDA device ordinal */
     void* stream;         /* cudaStream_t to queue on; NULL makes a private stream */
+    int32_t engine;       /* SILT_ENGINE_*: how the coarse pair is stepped */
 } silt_cfg;
+
+/* Coarse-pair engines. WINDOW steps each layer box by box exactly as the
+ * reference (work boxes, Gauss-Seidel confinement, per-sheet scratch), one
+ * CTA per layer, windows up to 512 cells per side. GRID steps the whole grid
+ * with tiled kernels on every SM and confines from a snapshot (the
+ * reference's free-operator form), for grids of any size. AUTO picks WINDOW
+ * up to 512 cells per side and GRID above. The nested patches always use WINDOW. */
+#define SILT_ENGINE_AUTO 0
+#define SILT_ENGINE_WINDOW 1
+#define SILT_ENGINE_GRID 2
 
 /* One tire shoving the sheet, src/fluid_core.rs:359-368 (`TirePush`). */
 typedef struct {
@@ -173,7 +184,11 @@ int silt_set_near_field(silt_sheet* s, int32_t on);
 /* Free `step_sheet` (src/fluid_core.rs:770) with the gravity drive on caller
  * device arrays (res*res each): h, u, v updated in place; bed, nu, gate read.
  * `scratch` is device memory of silt_step_sheet_scratch_bytes(res) bytes the
- * caller allocates once; stream is a cudaStream_t (NULL = legacy stream). */
+ * caller allocates once and passes to every call (zeroed before the first):
+ * it plays the reference's per-thread sheet scratch, whose contents one call
+ * leaves for the next. Up to 512 cells per side the window engine steps the
+ * sheet exactly as the reference; above, the grid engine. stream is a
+ * cudaStream_t (NULL = legacy stream). */
 size_t silt_step_sheet_scratch_bytes(int32_t res);
 int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
                     int32_t res, float cell, float dt, float vorticity, void* scratch, void* stream);
@@ -184,14 +199,14 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
  * since cudaFree waits for the whole device and an allocation can stall or
  * fail mid-frame, and for hosts whose GPU memory is all owned by another
  * allocator. Its scratch is a fixed array compiled into the library, sized
- * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (3 MiB per
+ * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (4 MiB per
  * GPU that loads the library, held until the process exits); larger grids
  * return SILT_EINVAL. The first call on each device looks the array up (with
  * that device current), so make that first call before any stream capture.
  * Every call shares the one array: calls whose work overlaps on the GPU race
  * and must be ordered by the caller (one stream, or events). Calls no
  * cudaMalloc, cudaFree or other allocating routine. */
-#define SILT_STEP_SHEET_STATIC_MAX_RES 512
+#define SILT_STEP_SHEET_STATIC_MAX_RES 256
 int silt_step_sheet_noalloc(float* h, float* u, float* v, const float* bed, const float* nu, const uint8_t* gate,
                             int32_t res, float cell, float dt, float vorticity, void* stream);
 

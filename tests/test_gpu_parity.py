@@ -1,10 +1,13 @@
 """Parity of the CUDA sheet step with the CPU oracle (the restated reference).
 
 Tolerance (from the build's pass criteria): max |dh| <= 1e-4 m per layer after
-100 steps. The CUDA path differs from the reference in two documented places
-only: vorticity confinement reads a post-gravity snapshot (Jacobi) where the
-reference's coarse pair sweeps in raster order (Gauss-Seidel), and the slurry
-damping factor uses CUDA's expf/powf. Both move depths by well under 1e-5 m.
+100 steps. The window engine (windows up to 512 cells) steps box by box with
+the reference's Gauss-Seidel confinement; the only source of difference is
+the slurry damping factor, which uses CUDA's expf/powf. The water layer's
+damping factor is computed on the host with the reference's libm, so the
+water depths must match bit for bit. The grid engine (large grids) confines
+from a snapshot, the reference's free-operator form, which moves config-1
+depths by under 1e-6 m.
 """
 import numpy as np
 import pytest
@@ -18,9 +21,9 @@ DT = 1.0 / 120.0
 TOL_H = 1.0e-4
 
 
-def run_pair(steps, scene, check_every=0):
+def run_pair(steps, scene, check_every=0, engine=G.ENGINE_AUTO):
     ref = O.Core()
-    dev = G.Sheet()
+    dev = G.Sheet(engine=engine)
     S.seed_core(ref, scene)
     S.seed_core(dev, scene)
     worst = []
@@ -46,6 +49,23 @@ def test_window200_100_steps_depth_parity():
     assert dev.non_finite_count() == 0
 
 
+def test_window200_water_is_bit_exact_after_100_steps():
+    scene = S.window200()
+    ref, dev, _ = run_pair(100, scene)
+    a, b = ref.get("water"), dev.get("water")
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), float(np.abs(a - b).max())
+    for name in ("uw", "vw"):
+        a, b = ref.get(name), dev.get(name)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (name, float(np.abs(a - b).max()))
+
+
+def test_grid_engine_window200_within_tolerance():
+    scene = S.window200()
+    ref, dev, _ = run_pair(100, scene, engine=G.ENGINE_GRID)
+    for name in ("water", "slurry"):
+        assert np.abs(ref.get(name) - dev.get(name)).max() <= TOL_H, name
+
+
 def test_window200_ledger_matches_oracle_in_fp64():
     scene = S.window200()
     ref, dev, _ = run_pair(20, scene)
@@ -55,15 +75,16 @@ def test_window200_ledger_matches_oracle_in_fp64():
     assert abs(ld["slurry_m3"] - lr["slurry64"]) <= 1e-6 * lr["slurry64"]
 
 
-def test_water_layer_is_bit_exact_on_a_jacobi_sized_box():
-    """The water layer on a pond wider than 48 x 32 cells. The oracle's pair then
-    confines from a snapshot too (force_gravity_par, src/fluid_core.rs:2229-2231)
-    and the water damping factor is computed on the host with the reference's
-    libm, so every operation is the reference's own IEEE sequence and the
-    depths must match bit for bit."""
+def test_grid_engine_water_is_bit_exact_on_a_jacobi_sized_box():
+    """The grid engine on a pond wider than 48 x 32 cells, against the oracle's
+    pair with the free operator's threading: the reference then confines from
+    a snapshot too (force_gravity_par, src/fluid_core.rs:2229-2231) and the
+    water damping factor is computed on the host with the reference's libm, so
+    every operation is the reference's own IEEE sequence and the depths must
+    match bit for bit."""
     scene = S.window200()
     ref = O.Core(inner_par=True)
-    dev = G.Sheet()
+    dev = G.Sheet(engine=G.ENGINE_GRID)
     for core in (ref, dev):
         core.map_water_bed(scene["bed"], np.zeros_like(scene["water"]))
         core.pour_water(-7.0, 7.0, -7.0, 7.0, 0.06)

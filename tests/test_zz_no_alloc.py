@@ -53,7 +53,7 @@ def test_noalloc_matches_caller_scratch_on_two_calls():
 
 def test_noalloc_refuses_grids_above_its_limit():
     res = G.lib().silt_step_sheet_noalloc  # bound
-    big = 513
+    big = 257
     rc = res(None, None, None, None, None, None, big, 0.2, 0.01, 0.0, None)
     assert rc == G.SILT_EINVAL
-    assert b"up to 512" in G.lib().silt_last_error()
+    assert b"up to 256" in G.lib().silt_last_error()
