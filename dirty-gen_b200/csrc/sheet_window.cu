@@ -37,6 +37,8 @@ struct Box {
     int i0, i1, j0, j1;
 };
 
+static_assert(NT % 32 == 0 && NT / 32 <= 32, "one warp reduces the per-warp partials");
+
 struct Shared {
     int lab[MAX_TILES];
     unsigned char hot[MAX_TILES];
@@ -72,7 +74,7 @@ __device__ __forceinline__ double block_sum_d(Shared& S, double v) {
     if ((threadIdx.x & 31) == 0) S.red_d[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x < 32) {
-        double t = S.red_d[threadIdx.x];
+        double t = threadIdx.x < NT / 32 ? S.red_d[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if (threadIdx.x == 0) S.red_d[0] = t;
     }
@@ -88,7 +90,7 @@ __device__ __forceinline__ float block_max_f(Shared& S, float v) {
     if ((threadIdx.x & 31) == 0) S.red_f[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x < 32) {
-        float t = S.red_f[threadIdx.x];
+        float t = threadIdx.x < NT / 32 ? S.red_f[threadIdx.x] : 0.0f;  // values reduced here are >= 0
         for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_down_sync(0xffffffffu, t, o));
         if (threadIdx.x == 0) S.red_f[0] = t;
     }
@@ -111,7 +113,8 @@ __device__ void block_reduce4(Shared& S, int v[4], const int op[4]) {
     __syncthreads();
     if (threadIdx.x < 32) {
         for (int q = 0; q < 4; ++q) {
-            int t = S.red_i[q][threadIdx.x];
+            const int ident = op[q] == 0 ? 0 : (op[q] == 1 ? 0x7fffffff : (int)0x80000000);
+            int t = threadIdx.x < NT / 32 ? S.red_i[q][threadIdx.x] : ident;
             for (int o = 16; o > 0; o >>= 1) {
                 int w = __shfl_down_sync(0xffffffffu, t, o);
                 t = op[q] == 0 ? t + w : (op[q] == 1 ? min(t, w) : max(t, w));
