@@ -34,7 +34,7 @@ constexpr int FT = 32;       // force tile edge
 constexpr int FH = 9;        // force halo: p (2) + gravity (1) + vorticity (2) + projection (4)
 constexpr int FW = FT + 2 * FH;
 constexpr int FPLANE = FW * FW;
-constexpr int FORCE_THREADS = 256;
+constexpr int FORCE_THREADS = 512;
 
 constexpr int TT = 32;       // transport tile edge
 constexpr int TW = TT + 3;   // cells [t0-2, t1+1)
@@ -65,12 +65,13 @@ __device__ __forceinline__ float cell_nu(const LayerParams& P, size_t g) {
     return dynamic_viscosity(P.grain[g], P.moisture[g]);
 }
 
-__global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
-    const LayerParams& P = L.lay[blockIdx.z];
+// One force tile. EDGE = false for tiles whose whole radius-9 region lies at
+// least 2 cells inside the grid: no index is ever clamped there and every
+// blur uses the interior form, so the stencils are plain offsets. Threads
+// walk the regions as rows (one warp per row, lanes along x).
+template <bool EDGE>
+__device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
     const int res = P.res;
-    const int tx0 = blockIdx.x * FT, ty0 = blockIdx.y * FT;
-    if (tx0 >= res || ty0 >= res || P.skip) return;
-    extern __shared__ float sm[];
     float* E = sm;               // eta, radius 9
     float* TG = sm + FPLANE;     // x-pass scratch
     float* TS = sm + 2 * FPLANE;
@@ -82,32 +83,36 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     const int ox = tx0 - FH, oy = ty0 - FH;
     const float cell = P.cell, dt = P.dt, eps = P.eps;
     const float two = 2.0f * cell;
-#define SIDX(gx, gy) (((gy) - oy) * FW + ((gx) - ox))
-#define REGION(rx, ry)                                                              \
-    const int x0 = max(0, tx0 - (rx)), x1 = min(res, tx0 + FT + (rx));            \
-    const int y0 = max(0, ty0 - (ry)), y1 = min(res, ty0 + FT + (ry));            \
-    const int nx = x1 - x0, ncell = nx * (y1 - y0);                                \
-    for (int k = threadIdx.x; k < ncell; k += blockDim.x) {                        \
-        const int gy = y0 + k / nx, gx = x0 + k % nx;                              \
-        const size_t g = (size_t)gy * res + gx;                                    \
-        (void)g;
+    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    constexpr int NW = FORCE_THREADS / 32;
+#define REGION(rx, ry)                                                                  \
+    const int x0 = EDGE ? max(0, tx0 - (rx)) : tx0 - (rx);                              \
+    const int x1 = EDGE ? min(res, tx0 + FT + (rx)) : tx0 + FT + (rx);                  \
+    const int y0 = EDGE ? max(0, ty0 - (ry)) : ty0 - (ry);                              \
+    const int y1 = EDGE ? min(res, ty0 + FT + (ry)) : ty0 + FT + (ry);                  \
+    for (int gy = y0 + wy; gy < y1; gy += NW)                                           \
+        for (int gx = x0 + lane; gx < x1; gx += 32) {                                   \
+            const int s = (gy - oy) * FW + (gx - ox);                                   \
+            const size_t g = (size_t)gy * res + gx;                                     \
+            (void)g;
 #define END_REGION }
+#define NX(d) (EDGE ? (gy - oy) * FW + (clampi(gx + (d), 0, res - 1) - ox) : s + (d))
+#define NZ(d) (EDGE ? (clampi(gy + (d), 0, res - 1) - oy) * FW + (gx - ox) : s + (d) * FW)
 
     // 1. eta and depth on radius 9.
     { REGION(FH, FH)
         float hv = P.h[g];
-        HS[SIDX(gx, gy)] = hv;
-        E[SIDX(gx, gy)] = P.bed[g] + hv;
+        HS[s] = hv;
+        E[s] = P.bed[g] + hv;
     END_REGION }
     __syncthreads();
     // 2. Velocity on radius 6: the lazy dry cut of the previous substep, then
     //    the soft window border (src/fluid_core.rs:9594-9622).
     { REGION(6, 6)
         float uu = P.u[g], vv = P.v[g];
-        if (P.apply_cut && HS[SIDX(gx, gy)] < eps) { uu = 0.0f; vv = 0.0f; }
+        if (P.apply_cut && HS[s] < eps) { uu = 0.0f; vv = 0.0f; }
         if (P.soften_edge > 0) {
-            int di = min(gx, res - 1 - gx), dj = min(gy, res - 1 - gy);
-            int d = min(di, dj);
+            int d = min(min(gx, res - 1 - gx), min(gy, res - 1 - gy));
             if (d < P.soften_edge) {
                 float t = (float)d / (float)P.soften_edge;
                 float w = t * t * (3.0f - 2.0f * t);
@@ -115,26 +120,21 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
                 vv *= w;
             }
         }
-        U[SIDX(gx, gy)] = uu;
-        V[SIDX(gx, gy)] = vv;
+        U[s] = uu;
+        V[s] = vv;
     END_REGION }
     //    x pass of both pressure blurs: rows radius 9, columns radius 7.
     { REGION(7, FH)
-        const bool in = gx >= 2 && gx <= res - 3;
-        const int s = SIDX(gx, gy);
-        float e0 = E[SIDX(clampi(gx - 2, 0, res - 1), gy)], e1 = E[SIDX(clampi(gx - 1, 0, res - 1), gy)];
-        float e2 = E[s];
-        float e3 = E[SIDX(clampi(gx + 1, 0, res - 1), gy)], e4 = E[SIDX(clampi(gx + 2, 0, res - 1), gy)];
+        const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
+        float e0 = E[NX(-2)], e1 = E[NX(-1)], e2 = E[s], e3 = E[NX(1)], e4 = E[NX(2)];
         TG[s] = tap5(e0, e1, e2, e3, e4, kG0, kG1, kG2, in);
         TS[s] = tap5(e0, e1, e2, e3, e4, kS0, kS1, kS2, in);
     END_REGION }
     __syncthreads();
     // 3. z pass and the pressure: p = 0.45 (0.62 G + 0.38 S) + 0.55 eta, radius 7.
     { REGION(7, 7)
-        const bool in = gy >= 2 && gy <= res - 3;
-        const int s = SIDX(gx, gy);
-        const int s0 = SIDX(gx, clampi(gy - 2, 0, res - 1)), s1 = SIDX(gx, clampi(gy - 1, 0, res - 1));
-        const int s3 = SIDX(gx, clampi(gy + 1, 0, res - 1)), s4 = SIDX(gx, clampi(gy + 2, 0, res - 1));
+        const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
+        const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
         float gb = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
         float sc = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
         float filtered = 0.62f * gb + 0.38f * sc;
@@ -144,10 +144,9 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     // 4. Gravity down the pressure gradient on wet cells, radius 6
     //    (src/fluid_core.rs:2234-2253).
     { REGION(6, 6)
-        const int s = SIDX(gx, gy);
         if (HS[s] > eps) {
-            float px = (PB[SIDX(min(gx + 1, res - 1), gy)] - PB[SIDX(max(gx - 1, 0), gy)]) / two;
-            float pz = (PB[SIDX(gx, min(gy + 1, res - 1))] - PB[SIDX(gx, max(gy - 1, 0))]) / two;
+            float px = (PB[NX(1)] - PB[NX(-1)]) / two;
+            float pz = (PB[NZ(1)] - PB[NZ(-1)]) / two;
             float mob = P.nu_mode == NU_CONST ? P.mob_c : sheet_mobility_for(cell_nu(P, g));
             U[s] += -kGravity * px * mob * dt;
             V[s] += -kGravity * pz * mob * dt;
@@ -156,24 +155,20 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     __syncthreads();
     // 5. Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
     if (P.vort > 0.0f) {
-        REGION(5, 5)
-            float dvdx = (V[SIDX(min(gx + 1, res - 1), gy)] - V[SIDX(max(gx - 1, 0), gy)]) / two;
-            float dudz = (U[SIDX(gx, min(gy + 1, res - 1))] - U[SIDX(gx, max(gy - 1, 0))]) / two;
-            WQ[SIDX(gx, gy)] = dvdx - dudz;
-        END_REGION
+        { REGION(5, 5)
+            float dvdx = (V[NX(1)] - V[NX(-1)]) / two;
+            float dudz = (U[NZ(1)] - U[NZ(-1)]) / two;
+            WQ[s] = dvdx - dudz;
+        END_REGION }
         __syncthreads();
         // 6. Confinement kick from that snapshot, in place, radius 4
         //    (src/fluid_core.rs:2348-2375, :2441-2470).
-        {
-            REGION(4, 4)
-            const int s = SIDX(gx, gy);
+        { REGION(4, 4)
             if (HS[s] > eps) {
                 float w = WQ[s];
                 if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
-                    float wxp = fabsf(WQ[SIDX(min(gx + 1, res - 1), gy)]);
-                    float wxm = fabsf(WQ[SIDX(max(gx - 1, 0), gy)]);
-                    float wzp = fabsf(WQ[SIDX(gx, min(gy + 1, res - 1))]);
-                    float wzm = fabsf(WQ[SIDX(gx, max(gy - 1, 0))]);
+                    float wxp = fabsf(WQ[NX(1)]), wxm = fabsf(WQ[NX(-1)]);
+                    float wzp = fabsf(WQ[NZ(1)]), wzm = fabsf(WQ[NZ(-1)]);
                     float nx_ = (wxp - wxm) / two;
                     float nz_ = (wzp - wzm) / two;
                     float du = P.vort * dt * (-nz_ * w);
@@ -184,17 +179,14 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
                     }
                 }
             }
-            END_REGION
-        }
+        END_REGION }
         __syncthreads();
     }
     if (P.project) {
         // 7. b = div * overload - 0.015 * overload * lap(eta), radius 3
         //    (src/fluid_core.rs:1992-2003).
         { REGION(3, 3)
-            const int s = SIDX(gx, gy);
-            const int sxp = SIDX(min(gx + 1, res - 1), gy), sxm = SIDX(max(gx - 1, 0), gy);
-            const int szp = SIDX(gx, min(gy + 1, res - 1)), szm = SIDX(gx, max(gy - 1, 0));
+            const int sxp = NX(1), sxm = NX(-1), szp = NZ(1), szm = NZ(-1);
             float ux = (U[sxp] - U[sxm]) / (2.0f * cell);
             float vz = (V[szp] - V[szm]) / (2.0f * cell);
             float div = ux + vz;
@@ -206,21 +198,16 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
         __syncthreads();
         // 8. x pass of both blurs of b: rows radius 3, columns radius 1.
         { REGION(1, 3)
-            const bool in = gx >= 2 && gx <= res - 3;
-            const int s = SIDX(gx, gy);
-            float b0 = PB[SIDX(clampi(gx - 2, 0, res - 1), gy)], b1 = PB[SIDX(clampi(gx - 1, 0, res - 1), gy)];
-            float b2 = PB[s];
-            float b3 = PB[SIDX(clampi(gx + 1, 0, res - 1), gy)], b4 = PB[SIDX(clampi(gx + 2, 0, res - 1), gy)];
+            const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
+            float b0 = PB[NX(-2)], b1 = PB[NX(-1)], b2 = PB[s], b3 = PB[NX(1)], b4 = PB[NX(2)];
             TG[s] = tap5(b0, b1, b2, b3, b4, kG0, kG1, kG2, in);
             TS[s] = tap5(b0, b1, b2, b3, b4, kS0, kS1, kS2, in);
         END_REGION }
         __syncthreads();
         // 9. q = 0.62 G(b) + 0.38 S(b), radius 1 (src/fluid_core.rs:2004-2011).
         { REGION(1, 1)
-            const bool in = gy >= 2 && gy <= res - 3;
-            const int s = SIDX(gx, gy);
-            const int s0 = SIDX(gx, clampi(gy - 2, 0, res - 1)), s1 = SIDX(gx, clampi(gy - 1, 0, res - 1));
-            const int s3 = SIDX(gx, clampi(gy + 1, 0, res - 1)), s4 = SIDX(gx, clampi(gy + 2, 0, res - 1));
+            const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
+            const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
             float gq = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
             float sq = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
             WQ[s] = 0.62f * gq + 0.38f * sq;
@@ -230,12 +217,11 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     // 10. Projection kick, damping and the speed clamp on wet cells
     //     (src/fluid_core.rs:2015-2037); every cell of the tile is written.
     { REGION(0, 0)
-        const int s = SIDX(gx, gy);
         float uu = U[s], vv = V[s];
         if (HS[s] > eps) {
             if (P.project) {
-                float qx = (WQ[SIDX(min(gx + 1, res - 1), gy)] - WQ[SIDX(max(gx - 1, 0), gy)]) / (2.0f * cell);
-                float qz = (WQ[SIDX(gx, min(gy + 1, res - 1))] - WQ[SIDX(gx, max(gy - 1, 0))]) / (2.0f * cell);
+                float qx = (WQ[NX(1)] - WQ[NX(-1)]) / (2.0f * cell);
+                float qz = (WQ[NZ(1)] - WQ[NZ(-1)]) / (2.0f * cell);
                 uu += 0.012f * dt * qx;
                 vv += 0.012f * dt * qz;
             }
@@ -246,9 +232,23 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
         P.u_out[g] = uu;
         P.v_out[g] = vv;
     END_REGION }
-#undef SIDX
 #undef REGION
 #undef END_REGION
+#undef NX
+#undef NZ
+}
+
+__global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
+    const LayerParams& P = L.lay[blockIdx.z];
+    const int res = P.res;
+    const int tx0 = blockIdx.x * FT, ty0 = blockIdx.y * FT;
+    if (tx0 >= res || ty0 >= res || P.skip) return;
+    extern __shared__ float sm[];
+    const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
+    if (interior)
+        force_tile<false>(P, sm, tx0, ty0);
+    else
+        force_tile<true>(P, sm, tx0, ty0);
 }
 
 // Donor-cell transport (src/fluid_core.rs:3025-3137), x pass then z pass on
@@ -271,122 +271,102 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch
     float* DN = sm + 7 * PL;    // down-going flux
     const int ox = tx0 - 2, oy = ty0 - 2;
 #define TIDX(gx, gy) (((gy) - oy) * TW + ((gx) - ox))
+    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    constexpr int NW = TRANSPORT_THREADS / 32;
+#define ROWS(Y0, Y1, X0, X1) \
+    for (int gy = (Y0) + wy; gy < (Y1); gy += NW) for (int gx = (X0) + lane; gx < (X1); gx += 32)
     const int ry0 = max(0, ty0 - 2), ry1 = min(res, ty1 + 1);
     const int cx0 = max(0, tx0 - 2), cx1 = min(res, tx1 + 1);
     const float cell = P.cell, dt = P.dt;
     const bool with_bed = P.bank_bed != nullptr;
     const uint8_t* gate = P.gate;
-    // Load h, u (radius 2/1) and v (tile columns).
-    {
-        const int nx = cx1 - cx0, ncell = nx * (ry1 - ry0);
-        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
-            int gy = ry0 + k / nx, gx = cx0 + k % nx;
-            size_t g = (size_t)gy * res + gx;
-            HSm[TIDX(gx, gy)] = P.h[g];
-            US[TIDX(gx, gy)] = P.u[g];
-            if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
-        }
+    ROWS(ry0, ry1, cx0, cx1) {
+        size_t g = (size_t)gy * res + gx;
+        HSm[TIDX(gx, gy)] = P.h[g];
+        US[TIDX(gx, gy)] = P.u[g];
+        if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
     }
     __syncthreads();
     // x pass. Edge e joins cells e and e+1 and exists for 0 <= e < res-1.
     // Left-going flux first (its donor e+1 has removed nothing yet).
     const int e0 = max(0, tx0 - 2), e1 = min(res - 2, tx1 - 1);  // inclusive edge range
-    {
-        const int ne = e1 - e0 + 1, nwork = ne * (ry1 - ry0);
-        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
-            int gy = ry0 + k / ne, e = e0 + k % ne;
-            float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
-            size_t g = (size_t)gy * res + e;
-            float bd = with_bed ? P.bank_bed[g + 1] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
-            float dh = open_edge_dh(with_bed, HSm[TIDX(e + 1, gy)], HSm[TIDX(e, gy)], 0.0f, gate ? gate[g] : 1, bd, bc,
-                                    speed, dt, cell, 0.45f);
-            FL[TIDX(e, gy)] = speed > 0.0f ? 0.0f : dh;
-        }
+    ROWS(ry0, ry1, e0, e1 + 1) {
+        const int e = gx;
+        float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
+        size_t g = (size_t)gy * res + e;
+        float bd = with_bed ? P.bank_bed[g + 1] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+        float dh = open_edge_dh(with_bed, HSm[TIDX(e + 1, gy)], HSm[TIDX(e, gy)], 0.0f, gate ? gate[g] : 1, bd, bc,
+                                speed, dt, cell, 0.45f);
+        FL[TIDX(e, gy)] = speed > 0.0f ? 0.0f : dh;
     }
     __syncthreads();
     // Right-going: donor e has removed the left-going flux of edge e-1.
-    {
-        const int ne = e1 - e0 + 1, nwork = ne * (ry1 - ry0);
-        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
-            int gy = ry0 + k / ne, e = e0 + k % ne;
-            if (e < tx0 - 1) continue;
-            float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
-            float prev = e > 0 ? FL[TIDX(e - 1, gy)] : 0.0f;
-            size_t g = (size_t)gy * res + e;
-            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + 1] : 0.0f;
-            float dh = open_edge_dh(with_bed, HSm[TIDX(e, gy)], HSm[TIDX(e + 1, gy)], 0.0f + prev,
-                                    gate ? gate[g + 1] : 1, bd, bc, speed, dt, cell, 0.45f);
-            FR[TIDX(e, gy)] = speed > 0.0f ? dh : 0.0f;
-        }
+    ROWS(ry0, ry1, max(e0, tx0 - 1), e1 + 1) {
+        const int e = gx;
+        float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
+        float prev = e > 0 ? FL[TIDX(e - 1, gy)] : 0.0f;
+        size_t g = (size_t)gy * res + e;
+        float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + 1] : 0.0f;
+        float dh = open_edge_dh(with_bed, HSm[TIDX(e, gy)], HSm[TIDX(e + 1, gy)], 0.0f + prev,
+                                gate ? gate[g + 1] : 1, bd, bc, speed, dt, cell, 0.45f);
+        FR[TIDX(e, gy)] = speed > 0.0f ? dh : 0.0f;
     }
     __syncthreads();
     // Depth after the x pass on rows [ry0, ry1), tile columns.
-    {
-        const int nx = tx1 - tx0, ncell = nx * (ry1 - ry0);
-        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
-            int gy = ry0 + k / nx, c = tx0 + k % nx;
-            float flm = c - 1 >= 0 ? FL[TIDX(c - 1, gy)] : 0.0f;
-            float frm = c - 1 >= 0 ? FR[TIDX(c - 1, gy)] : 0.0f;
-            float flc = c <= res - 2 ? FL[TIDX(c, gy)] : 0.0f;
-            float frc = c <= res - 2 ? FR[TIDX(c, gy)] : 0.0f;
-            float rem = (0.0f + flm) + frc;
-            float add = (0.0f + frm) + flc;
-            float hv = HSm[TIDX(c, gy)];
-            float moved = fmaxf(hv - rem + add, 0.0f);
-            HX[TIDX(c, gy)] = (rem > 0.0f || add > 0.0f) ? moved : hv;
-        }
+    ROWS(ry0, ry1, tx0, tx1) {
+        const int c = gx;
+        float flm = c - 1 >= 0 ? FL[TIDX(c - 1, gy)] : 0.0f;
+        float frm = c - 1 >= 0 ? FR[TIDX(c - 1, gy)] : 0.0f;
+        float flc = c <= res - 2 ? FL[TIDX(c, gy)] : 0.0f;
+        float frc = c <= res - 2 ? FR[TIDX(c, gy)] : 0.0f;
+        float rem = (0.0f + flm) + frc;
+        float add = (0.0f + frm) + flc;
+        float hv = HSm[TIDX(c, gy)];
+        float moved = fmaxf(hv - rem + add, 0.0f);
+        HX[TIDX(c, gy)] = (rem > 0.0f || add > 0.0f) ? moved : hv;
     }
     __syncthreads();
     // z pass. Pair r joins rows r and r+1 and exists for 0 <= r < res-1.
     const int p0 = max(0, ty0 - 2), p1 = min(res - 2, ty1 - 1);
-    {
-        const int nx = tx1 - tx0, nwork = nx * (p1 - p0 + 1);
-        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
-            int r = p0 + k / nx, c = tx0 + k % nx;
-            float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
-            size_t g = (size_t)r * res + c;
-            float bd = with_bed ? P.bank_bed[g + res] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
-            float dh = open_edge_dh(with_bed, HX[TIDX(c, r + 1)], HX[TIDX(c, r)], 0.0f, gate ? gate[g] : 1, bd, bc,
-                                    speed, dt, cell, 0.45f);
-            UP[TIDX(c, r)] = speed > 0.0f ? 0.0f : dh;
-        }
+    ROWS(p0, p1 + 1, tx0, tx1) {
+        const int r = gy, c = gx;
+        float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
+        size_t g = (size_t)r * res + c;
+        float bd = with_bed ? P.bank_bed[g + res] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+        float dh = open_edge_dh(with_bed, HX[TIDX(c, r + 1)], HX[TIDX(c, r)], 0.0f, gate ? gate[g] : 1, bd, bc,
+                                speed, dt, cell, 0.45f);
+        UP[TIDX(c, r)] = speed > 0.0f ? 0.0f : dh;
     }
     __syncthreads();
-    {
-        const int nx = tx1 - tx0, nwork = nx * (p1 - p0 + 1);
-        for (int k = threadIdx.x; k < nwork; k += blockDim.x) {
-            int r = p0 + k / nx, c = tx0 + k % nx;
-            if (r < ty0 - 1) continue;
-            float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
-            float ra = r > 0 ? 0.0f + UP[TIDX(c, r - 1)] : 0.0f;
-            size_t g = (size_t)r * res + c;
-            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + res] : 0.0f;
-            float dh = open_edge_dh(with_bed, HX[TIDX(c, r)], HX[TIDX(c, r + 1)], ra, gate ? gate[g + res] : 1, bd,
-                                    bc, speed, dt, cell, 0.45f);
-            DN[TIDX(c, r)] = speed > 0.0f ? dh : 0.0f;
-        }
+    ROWS(max(p0, ty0 - 1), p1 + 1, tx0, tx1) {
+        const int r = gy, c = gx;
+        float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
+        float ra = r > 0 ? 0.0f + UP[TIDX(c, r - 1)] : 0.0f;
+        size_t g = (size_t)r * res + c;
+        float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + res] : 0.0f;
+        float dh = open_edge_dh(with_bed, HX[TIDX(c, r)], HX[TIDX(c, r + 1)], ra, gate ? gate[g + res] : 1, bd,
+                                bc, speed, dt, cell, 0.45f);
+        DN[TIDX(c, r)] = speed > 0.0f ? dh : 0.0f;
     }
     __syncthreads();
     double part = 0.0;
-    {
-        const int nx = tx1 - tx0, ncell = nx * (ty1 - ty0);
-        for (int k = threadIdx.x; k < ncell; k += blockDim.x) {
-            int r = ty0 + k / nx, c = tx0 + k % nx;
-            float upm = r - 1 >= 0 ? UP[TIDX(c, r - 1)] : 0.0f;
-            float dnm = r - 1 >= 0 ? DN[TIDX(c, r - 1)] : 0.0f;
-            float upc = r <= res - 2 ? UP[TIDX(c, r)] : 0.0f;
-            float dnc = r <= res - 2 ? DN[TIDX(c, r)] : 0.0f;
-            float rem = (0.0f + upm) + dnc;
-            float add = (0.0f + dnm) + upc;
-            float hv = HX[TIDX(c, r)];
-            float moved = fmaxf(hv - rem + add, 0.0f);
-            float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
-            if (P.eps > 0.0f && hn < P.eps) hn = 0.0f;
-            P.h_out[(size_t)r * res + c] = hn;
-            part += (double)fmaxf(hn, 0.0f);
-        }
+    ROWS(ty0, ty1, tx0, tx1) {
+        const int r = gy, c = gx;
+        float upm = r - 1 >= 0 ? UP[TIDX(c, r - 1)] : 0.0f;
+        float dnm = r - 1 >= 0 ? DN[TIDX(c, r - 1)] : 0.0f;
+        float upc = r <= res - 2 ? UP[TIDX(c, r)] : 0.0f;
+        float dnc = r <= res - 2 ? DN[TIDX(c, r)] : 0.0f;
+        float rem = (0.0f + upm) + dnc;
+        float add = (0.0f + dnm) + upc;
+        float hv = HX[TIDX(c, r)];
+        float moved = fmaxf(hv - rem + add, 0.0f);
+        float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        if (P.eps > 0.0f && hn < P.eps) hn = 0.0f;
+        P.h_out[(size_t)r * res + c] = hn;
+        part += (double)fmaxf(hn, 0.0f);
     }
 #undef TIDX
+#undef ROWS
     // Block sum of the depth (FP64), one atomic per block.
     for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
     __shared__ double warp_sum[TRANSPORT_THREADS / 32];
