@@ -502,6 +502,8 @@ __global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const Re
     }
     const size_t idx = E.cidx;
     const float w = aw / coarse_area, s = as / coarse_area;
+    mark_tile(W, 0, (int)(idx % W.res), (int)(idx / W.res));
+    mark_tile(W, 1, (int)(idx % W.res), (int)(idx / W.res));
     // A column the patch does not hold keeps its depth and gains what flowed
     // onto its fine cells. For patches that are whole multiples of the coarse
     // cell every touched column is fully covered and this is the reference's

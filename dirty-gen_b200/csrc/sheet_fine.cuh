@@ -27,7 +27,22 @@ struct SheetView {
     uint8_t* grain;
     double* d_acc;
     int cut_pending;   // u, v of cells with h < eps still hold their pre-cut values
+    // Grid engine tile flags of the current buffers (tiles_x = 0 on the window
+    // engine): a kernel that writes a coarse cell marks its tile.
+    int tiles_x;
+    uint8_t* t_wet[2];
+    uint8_t* t_zuv[2];
+    uint8_t* t_zh[2];
 };
+
+// Marks the tile of coarse cell (i, j) of layer l as possibly wet and not zero.
+__device__ __forceinline__ void mark_tile(const SheetView& W, int l, int i, int j) {
+    if (!W.tiles_x) return;
+    const int t = (j / 32) * W.tiles_x + i / 32;
+    W.t_wet[l][t] = 1;
+    W.t_zuv[l][t] = 0;
+    W.t_zh[l][t] = 0;
+}
 
 struct StepOut {
     int spray_events = 0;   // events queued on the device this step

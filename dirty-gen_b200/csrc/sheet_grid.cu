@@ -238,28 +238,76 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
 #undef NZ
 }
 
+// Persistent over the substep's tile list.
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
-    const LayerParams& P = L.lay[blockIdx.z];
-    const int res = P.res;
-    const int tx0 = blockIdx.x * FT, ty0 = blockIdx.y * FT;
-    if (tx0 >= res || ty0 >= res || P.skip) return;
     extern __shared__ float sm[];
-    const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
-    if (interior)
-        force_tile<false>(P, sm, tx0, ty0);
-    else
-        force_tile<true>(P, sm, tx0, ty0);
+    const int n = *L.tf.count;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = L.tf.list[k];
+        const int l = e >> 30, zero_fill = (e >> 29) & 1, t = e & ((1 << 29) - 1);
+        const LayerParams& P = L.lay[l];
+        const int res = P.res;
+        const int tx0 = (t % L.tf.tiles_x) * FT, ty0 = (t / L.tf.tiles_x) * FT;
+        if (zero_fill) {
+            // A quiet tile: dry in its whole neighbourhood, so after the dry cut
+            // its velocity is zero.
+            const int w = min(FT, res - tx0), h = min(FT, res - ty0);
+            for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+                const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
+                P.u_out[g] = 0.0f;
+                P.v_out[g] = 0.0f;
+            }
+            if (threadIdx.x == 0) L.tf.zero_uv[l][L.nxt][t] = 1;
+            continue;
+        }
+        const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
+        if (interior)
+            force_tile<false>(P, sm, tx0, ty0);
+        else
+            force_tile<true>(P, sm, tx0, ty0);
+        if (threadIdx.x == 0) L.tf.zero_uv[l][L.nxt][t] = 0;
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1) {
+    const int nt = tf.tiles_x * tf.tiles_x;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * nt) return;
+    const int l = k / nt, t = k % nt;
+    if (l == 0 ? skip0 : skip1) return;
+    const int ti = t % tf.tiles_x, tj = t / tf.tiles_x;
+    bool active = all != 0;
+    for (int dj = -1; dj <= 1 && !active; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+            const int a = ti + di, b = tj + dj;
+            if (a < 0 || b < 0 || a >= tf.tiles_x || b >= tf.tiles_x) continue;
+            if (tf.wet[l][cur][b * tf.tiles_x + a]) {
+                active = true;
+                break;
+            }
+        }
+    if (active) {
+        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | t;
+    } else if (!tf.zero_uv[l][nxt][t] || !tf.zero_h[l][nxt][t]) {
+        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | (1 << 29) | t;
+    }
+}
+
+cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(tf.count, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const int n = 2 * tf.tiles_x * tf.tiles_x;
+    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1);
+    return cudaGetLastError();
 }
 
 // Donor-cell transport (src/fluid_core.rs:3025-3137), x pass then z pass on
 // the updated depth, dry cut (src/fluid_core.rs:2072-2081), FP64 ledger sum.
-__global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
-    const TransportParams& P = L.lay[blockIdx.z];
+__device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int ty0, const TileFlags& tf, int l,
+                               int nxt, int t) {
     const int res = P.res;
-    const int tx0 = blockIdx.x * TT, ty0 = blockIdx.y * TT;
-    if (tx0 >= res || ty0 >= res || P.skip) return;
     const int tx1 = min(res, tx0 + TT), ty1 = min(res, ty0 + TT);
-    extern __shared__ float sm[];
     constexpr int PL = TW * TW;
     float* HSm = sm;            // h on rows [ty0-2, ty1+1), cols [tx0-2, tx1+1)
     float* US = sm + PL;        // u on the same cells
@@ -367,7 +415,8 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch
     }
 #undef TIDX
 #undef ROWS
-    // Block sum of the depth (FP64), one atomic per block.
+    // Block sum of the depth (FP64), one atomic per tile; the tile's flags.
+    const int any = __syncthreads_or(part > 0.0);
     for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
     __shared__ double warp_sum[TRANSPORT_THREADS / 32];
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = part;
@@ -375,7 +424,36 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch
     if (threadIdx.x < 32) {
         double v = threadIdx.x < (blockDim.x >> 5) ? warp_sum[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0 && P.ledger) atomicAdd(P.ledger, v);
+        if (threadIdx.x == 0) {
+            if (P.ledger) atomicAdd(P.ledger, v);
+            tf.wet[l][nxt][t] = any ? 1 : 0;
+            tf.zero_h[l][nxt][t] = any ? 0 : 1;
+        }
+    }
+    __syncthreads();  // shared memory is reused by the next tile
+}
+
+// Persistent over the substep's tile list.
+__global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
+    extern __shared__ float sm[];
+    const int n = *L.tf.count;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = L.tf.list[k];
+        const int l = e >> 30, zero_fill = (e >> 29) & 1, t = e & ((1 << 29) - 1);
+        const TransportParams& P = L.lay[l];
+        const int res = P.res;
+        const int tx0 = (t % L.tf.tiles_x) * TT, ty0 = (t / L.tf.tiles_x) * TT;
+        if (zero_fill) {
+            const int w = min(TT, res - tx0), h = min(TT, res - ty0);
+            for (int q = threadIdx.x; q < w * h; q += blockDim.x)
+                P.h_out[(size_t)(ty0 + q / w) * res + tx0 + q % w] = 0.0f;
+            if (threadIdx.x == 0) {
+                L.tf.wet[l][L.nxt][t] = 0;
+                L.tf.zero_h[l][L.nxt][t] = 1;
+            }
+            continue;
+        }
+        transport_tile(P, sm, tx0, ty0, L.tf, l, L.nxt, t);
     }
 }
 
@@ -405,8 +483,9 @@ cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t
         cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
         attr = true;
     }
-    dim3 grid((res + FT - 1) / FT, (res + FT - 1) / FT, layers);
-    k_force<<<grid, FORCE_THREADS, force_smem_bytes(), st>>>(L);
+    (void)res;
+    (void)layers;
+    k_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(L);
     return cudaGetLastError();
 }
 
@@ -416,8 +495,9 @@ cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cuda
         cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes());
         attr = true;
     }
-    dim3 grid((res + TT - 1) / TT, (res + TT - 1) / TT, layers);
-    k_transport<<<grid, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
+    (void)res;
+    (void)layers;
+    k_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
     return cudaGetLastError();
 }
 

@@ -32,8 +32,24 @@ struct LayerParams {
     int32_t skip;          // layer has nothing to do this substep
 };
 
+// Active-tile bookkeeping of the grid engine, per layer and ping-pong buffer,
+// one byte per 32 x 32 tile. A tile is stepped only when some tile of its
+// 3 x 3 neighbourhood may hold water; every other tile is provably unchanged
+// (no depth within the force and transport halos, no velocity after the dry
+// cut) and is written once with zeros, then skipped while its buffer stays zero.
+struct TileFlags {
+    uint8_t* wet[2][2];      // [layer][buffer]: the tile may hold water
+    uint8_t* zero_uv[2][2];  // [layer][buffer]: u and v of the tile are all zero
+    uint8_t* zero_h[2][2];   // [layer][buffer]: h of the tile is all zero
+    int* list;               // entries (layer << 30) | (zero_fill << 29) | tile
+    int* count;
+    int32_t tiles_x;
+};
+
 struct ForceLaunch {
     LayerParams lay[2];
+    TileFlags tf;
+    int32_t nxt;             // buffer being written
 };
 
 struct TransportParams {
@@ -51,9 +67,16 @@ struct TransportParams {
 
 struct TransportLaunch {
     TransportParams lay[2];
+    TileFlags tf;
+    int32_t nxt;
 };
 
+constexpr int GRID_TILE = 32;
+
 size_t force_smem_bytes();
+// Builds the tile list of one substep: active tiles of both layers, then the
+// quiet tiles whose output buffer is not yet zero. `all` marks every tile active.
+cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1, cudaStream_t st);
 size_t transport_smem_bytes();
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st);
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st);

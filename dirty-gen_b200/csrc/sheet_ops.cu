@@ -85,10 +85,16 @@ __global__ void k_read_substrate(const float* bed_in, const float* moist_in, con
 // Inflow strip: depth added on one row over [x0, x1). A cell still waiting
 // for the previous dry cut gets it first, so the water lands at rest.
 __global__ void k_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1,
-                         float add) {
+                         float add, int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh) {
     int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= i1) return;
     size_t c = (size_t)j * res + i;
+    if (tiles_x) {  // the grid engine's tile of this cell now holds water
+        const int t = (j / 32) * tiles_x + i / 32;
+        t_wet[t] = 1;
+        t_zuv[t] = 0;
+        t_zh[t] = 0;
+    }
     if (cut_pending && water[c] < 1.0e-6f) {
         uw[c] = 0.0f;
         vw[c] = 0.0f;
@@ -188,9 +194,10 @@ cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const 
     return cudaGetLastError();
 }
 cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
-                      cudaStream_t st) {
+                      int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh, cudaStream_t st) {
     if (i1 <= i0) return cudaSuccess;
-    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, uw, vw, cut_pending, res, j, i0, i1, add);
+    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, uw, vw, cut_pending, res, j, i0, i1, add, tiles_x, t_wet,
+                                                     t_zuv, t_zh);
     return cudaGetLastError();
 }
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,

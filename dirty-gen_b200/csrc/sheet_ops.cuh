@@ -17,7 +17,7 @@ cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, ui
 cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
                               float* moisture, uint8_t* grain, const float* slurry, size_t n, cudaStream_t st);
 cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
-                      cudaStream_t st);
+                      int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh, cudaStream_t st);
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
                        const float* vs, float* film, float* flow, size_t n, cudaStream_t st);
 cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,

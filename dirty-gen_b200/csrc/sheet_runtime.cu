@@ -97,6 +97,10 @@ struct silt_sheet {
     silt::window::Job* h_win_jobs = nullptr;      // pinned staging
     cudaEvent_t win_ev[2] = {nullptr, nullptr};
     int win_flip = 0;
+    // Grid engine: active-tile flags and the substep's tile list.
+    silt::TileFlags tf;
+    uint8_t* tile_mem = nullptr;
+    bool tiles_all = true;     // next substep steps every tile (after any outside write)
 
     float* H(int l) { return h[l][cur]; }
     float* U(int l) { return u[l][cur]; }
@@ -106,6 +110,21 @@ struct silt_sheet {
 namespace {
 
 float water_nu() { return silt::host::dynamic_viscosity(3, 1.0f); }
+
+// After a write from outside the step (seeding, plane writes) every tile may
+// hold water and no buffer is known to be zero.
+int tiles_dirty(silt_sheet* s) {
+    s->tiles_all = true;
+    if (!s->tile_mem) return SILT_OK;
+    const size_t nt = (size_t)s->tf.tiles_x * s->tf.tiles_x;
+    for (int l = 0; l < 2; ++l)
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMemsetAsync(s->tf.wet[l][b], 1, nt, s->st));
+            CK(cudaMemsetAsync(s->tf.zero_uv[l][b], 0, nt, s->st));
+            CK(cudaMemsetAsync(s->tf.zero_h[l][b], 0, nt, s->st));
+        }
+    return SILT_OK;
+}
 
 // Materialise the lazy dry cut before anything reads or writes the planes.
 int flush_cut(silt_sheet* s) {
@@ -196,9 +215,18 @@ int step_coarse_pair(silt_sheet* s, float dt) {
             Q.eps = eps;
             Q.skip = P.skip;
         }
+        F.tf = s->tf;
+        F.nxt = nxt;
+        T.tf = s->tf;
+        T.nxt = nxt;
         // A skipped layer keeps its planes (copied across the buffer swap) and its ledger sum.
         for (int l = 0; l < 2; ++l)
             if (!F.lay[l].skip) CK(cudaMemsetAsync(s->d_acc + l, 0, sizeof(double), s->st));
+        // A substep that does not start from a dry cut (the first after an
+        // outside write) steps every tile: its dry cells may carry velocity.
+        const int all = (s->tiles_all || !(k > 0 || s->cut_pending)) ? 1 : 0;
+        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, F.lay[0].skip, F.lay[1].skip, s->st));
+        s->tiles_all = false;
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
         if (s->timing) {
             for (int q = 0; q < 3; ++q) {
@@ -225,6 +253,12 @@ int step_coarse_pair(silt_sheet* s, float dt) {
                 CK(cudaMemcpyAsync(s->h[l][nxt], s->h[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
                 CK(cudaMemcpyAsync(s->u[l][nxt], s->u[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
                 CK(cudaMemcpyAsync(s->v[l][nxt], s->v[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
+                const size_t nt = (size_t)s->tf.tiles_x * s->tf.tiles_x;
+                CK(cudaMemcpyAsync(s->tf.wet[l][nxt], s->tf.wet[l][s->cur], nt, cudaMemcpyDeviceToDevice, s->st));
+                CK(cudaMemcpyAsync(s->tf.zero_uv[l][nxt], s->tf.zero_uv[l][s->cur], nt, cudaMemcpyDeviceToDevice,
+                                   s->st));
+                CK(cudaMemcpyAsync(s->tf.zero_h[l][nxt], s->tf.zero_h[l][s->cur], nt, cudaMemcpyDeviceToDevice,
+                                   s->st));
             }
         s->cur = nxt;
         s->cut_pending = true;
@@ -374,6 +408,27 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         silt_sheet_destroy(s);
         return fail_arg("window engine serves windows up to 512 cells per side");
     }
+    if (s->engine == SILT_ENGINE_GRID) {
+        const int tx = (cfg->res + silt::GRID_TILE - 1) / silt::GRID_TILE;
+        const size_t nt = (size_t)tx * tx;
+        if (e == cudaSuccess) e = cudaMalloc(&s->tile_mem, 12 * nt + 2 * nt * sizeof(int) + 256);
+        if (e == cudaSuccess) {
+            uint8_t* q = s->tile_mem;
+            for (int l = 0; l < 2; ++l)
+                for (int b = 0; b < 2; ++b) {
+                    s->tf.wet[l][b] = q;
+                    q += nt;
+                    s->tf.zero_uv[l][b] = q;
+                    q += nt;
+                    s->tf.zero_h[l][b] = q;
+                    q += nt;
+                }
+            q = (uint8_t*)(((uintptr_t)q + 15) & ~uintptr_t(15));
+            s->tf.list = (int*)q;
+            s->tf.count = s->tf.list + 2 * nt;
+            s->tf.tiles_x = tx;
+        }
+    }
     if (s->engine == SILT_ENGINE_WINDOW) {
         const size_t wp = 2 * (size_t)silt::window::SCRATCH_PLANES * s->n * sizeof(float);
         if (e == cudaSuccess) e = cudaMalloc(&s->win_planes, wp);
@@ -395,6 +450,7 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     cudaMemsetAsync(s->bed, 0, nb, s->st);
     cudaMemsetAsync(s->moisture, 0, nb, s->st);
     cudaMemsetAsync(s->grain, 4, s->n, s->st);  // Grain::Other
+    if (e == cudaSuccess && tiles_dirty(s) != SILT_OK) e = cudaErrorUnknown;
     int rc = silt::fine::create(s->fine, *cfg, s->res, s->st);
     if (rc != SILT_OK) {
         silt_sheet_destroy(s);
@@ -431,6 +487,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->d_planes);
     if (s->h_acc) cudaFreeHost(s->h_acc);
     cudaFree(s->win_planes);
+    cudaFree(s->tile_mem);
     cudaFree(s->d_win_jobs);
     if (s->h_win_jobs) cudaFreeHost(s->h_win_jobs);
     for (int k = 0; k < 2; ++k)
@@ -470,6 +527,7 @@ int silt_map_water_bed(silt_sheet* s, const float* bed, const float* water, floa
     CK(cudaStreamSynchronize(s->st));  // the host arrays may be freed on return
     if (vol_out) *vol_out = host_volume(water, s->n, s->cfg.cell * s->cfg.cell, true);
     s->ledger_fresh = false;
+    if (int rc2 = tiles_dirty(s)) return rc2;
     return SILT_OK;
 }
 
@@ -497,7 +555,7 @@ int silt_map_water_velocity(silt_sheet* s, const float* u, const float* v) {
         if (std::isfinite(v[i])) m = std::max(m, fabsf(v[i]));
     }
     s->vmax_bound = std::max(s->vmax_bound, m * 1.4142137f);
-    return SILT_OK;
+    return tiles_dirty(s);
 }
 
 static int paint(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, int water, int grain, float m,
@@ -522,7 +580,7 @@ static int paint(silt_sheet* s, float x0, float x1, float z0, float z1, float de
         *vol_out = vol;
     }
     s->ledger_fresh = false;
-    return SILT_OK;
+    return tiles_dirty(s);
 }
 
 int silt_pour_water(silt_sheet* s, float x0, float x1, float z0, float z1, float depth, float* vol_out) {
@@ -550,7 +608,7 @@ int silt_lay_slurry_mask(silt_sheet* s, const float* depth, int32_t grain, float
         *vol_out = vol;
     }
     s->ledger_fresh = false;
-    return SILT_OK;
+    return tiles_dirty(s);
 }
 
 int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moisture, const uint8_t* grain) {
@@ -624,8 +682,9 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     if (s->inflow_j >= 0) {
         int nc = s->inflow_i1 - s->inflow_i0;
         float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
+        silt::fine::SheetView W = silt::fine::view_of(s);
         CK(silt::op_inflow(s->H(0), s->U(0), s->V(0), s->cut_pending ? 1 : 0, s->res, s->inflow_j, s->inflow_i0,
-                           s->inflow_i1, add, s->st));
+                           s->inflow_i1, add, W.tiles_x, W.t_wet[0], W.t_zuv[0], W.t_zh[0], s->st));
         s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
     }
     silt::fine::StepOut fo;
@@ -817,7 +876,7 @@ int silt_write_plane(silt_sheet* s, int32_t which, const float* host) {
         s->vmax_bound = std::max(s->vmax_bound, m * 1.4142137f);
     }
     s->ledger_fresh = false;
-    return SILT_OK;
+    return tiles_dirty(s);
 }
 
 int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
@@ -883,7 +942,8 @@ static size_t step_sheet_scratch(int32_t res) {
     if (res <= 0) return 0;
     size_t n = (size_t)res * res;
     if (res <= silt::window::MAX_RES) return 4096 + (size_t)silt::window::SCRATCH_PLANES * n * sizeof(float);
-    return 256 + 3 * n * sizeof(float);
+    const size_t tx = (size_t)(res + silt::GRID_TILE - 1) / silt::GRID_TILE;
+    return 256 + 3 * n * sizeof(float) + 12 * tx * tx + 2 * tx * tx * sizeof(int) + 64;
 }
 
 size_t silt_step_sheet_scratch_bytes(int32_t res) { return step_sheet_scratch(res); }
@@ -936,6 +996,26 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
     float* u_mid = (float*)((char*)scratch + 256);
     float* v_mid = u_mid + n;
     float* h_next = v_mid + n;
+    // Tile flags after the planes: every tile is stepped on every call.
+    silt::TileFlags tf;
+    {
+        const int tx = (res + silt::GRID_TILE - 1) / silt::GRID_TILE;
+        const size_t nt = (size_t)tx * tx;
+        uint8_t* q = reinterpret_cast<uint8_t*>(h_next + n);
+        for (int l = 0; l < 2; ++l)
+            for (int b = 0; b < 2; ++b) {
+                tf.wet[l][b] = q;
+                q += nt;
+                tf.zero_uv[l][b] = q;
+                q += nt;
+                tf.zero_h[l][b] = q;
+                q += nt;
+            }
+        q = (uint8_t*)(((uintptr_t)q + 15) & ~uintptr_t(15));
+        tf.list = (int*)q;
+        tf.count = tf.list + 2 * nt;
+        tf.tiles_x = tx;
+    }
     CK(cudaMemsetAsync(d_bits, 0, 32, st));
     CK(silt::launch_max_speed2(h, u, v, n, 1.0e-6f, 0, d_bits, st));
     CK(silt::op_sum2(h, h, n, d_sum, st));
@@ -980,6 +1060,13 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         Q.cell = cell;
         Q.dt = dts;
         Q.eps = 1.0e-6f;
+        F.lay[1].skip = 1;
+        T.lay[1].skip = 1;
+        F.tf = tf;
+        T.tf = tf;
+        F.nxt = 1;
+        T.nxt = 1;
+        CK(silt::launch_tile_list(tf, 0, 1, 1, 0, 1, st));
         CK(silt::launch_force(F, res, 1, st));
         CK(silt::launch_transport(T, res, 1, st));
         CK(cudaMemcpyAsync(h, h_next, n * 4, cudaMemcpyDeviceToDevice, st));
@@ -1055,6 +1142,12 @@ SheetView view_of(silt_sheet* s) {
     w.grain = s->grain;
     w.d_acc = s->d_acc;
     w.cut_pending = s->cut_pending ? 1 : 0;
+    w.tiles_x = s->tile_mem ? s->tf.tiles_x : 0;
+    for (int l = 0; l < 2; ++l) {
+        w.t_wet[l] = s->tile_mem ? s->tf.wet[l][s->cur] : nullptr;
+        w.t_zuv[l] = s->tile_mem ? s->tf.zero_uv[l][s->cur] : nullptr;
+        w.t_zh[l] = s->tile_mem ? s->tf.zero_h[l][s->cur] : nullptr;
+    }
     return w;
 }
 int flush(silt_sheet* s) { return flush_cut(s); }

@@ -154,12 +154,15 @@ def test_near_field_keeps_sub_cell_detail():
         assert abs(water - start) < 1.0e-3 * start
 
 
-def test_ledger_closes_in_fp64_with_tires_and_inflow():
+@pytest.mark.parametrize("engine", [G.ENGINE_WINDOW, G.ENGINE_GRID])
+def test_ledger_closes_in_fp64_with_tires_and_inflow(engine):
     """Per-step conservation: water now = water before + inflow - spray - the
-    volume the dry cut removes, to the f32 rounding of the cell updates."""
+    volume the dry cut removes, to the f32 rounding of the cell updates. On
+    the grid engine this also checks that every write outside the step (the
+    inflow strip, the patch hand-back) wakes the tiles it lands in."""
     dt = 1.0 / 120.0
     scene = S.grid(res=256)
-    dev = G.Sheet(res=256, fine_res=64, layout=G.FINE_PER_TIRE)
+    dev = G.Sheet(res=256, fine_res=64, layout=G.FINE_PER_TIRE, engine=engine)
     S.seed_core(dev, scene)
     dev.set_inflow(0, -2.0, 2.0, 0.5)
     prev = dev.ledger()
@@ -175,3 +178,22 @@ def test_ledger_closes_in_fp64_with_tires_and_inflow():
         prev = led
     print("worst relative gap", worst)
     assert worst < 1e-5
+
+
+def test_grid_engine_tracks_window_engine_with_tires():
+    """The two coarse engines on the same tire drive: they differ only in the
+    confinement form (snapshot vs raster sweep), so depths stay close."""
+    dt = 1.0 / 120.0
+    scene = S.grid(res=256)
+    out = []
+    for engine in (G.ENGINE_WINDOW, G.ENGINE_GRID):
+        dev = G.Sheet(res=256, fine_res=64, layout=G.FINE_PER_TIRE, engine=engine)
+        S.seed_core(dev, scene)
+        dev.set_inflow(0, -2.0, 2.0, 0.5)
+        for k in range(30):
+            for t in S.tires_at(k * dt, speed=5.0, z0=-5.0):
+                dev.push_tire(**t)
+            dev.step(dt, want_spray=False)
+        out.append((dev.get("water"), dev.get("slurry")))
+    assert np.abs(out[0][0] - out[1][0]).max() < 5e-3
+    assert np.abs(out[0][1] - out[1][1]).max() < 5e-3
