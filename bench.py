@@ -32,8 +32,11 @@ CELL = 0.2
 DT = 1.0 / 120.0
 FINE_RES = 64
 INFLOW = (0, -2.0, 2.0, 0.5)
-FORCE_BYTES_PER_CELL = 49  # k_force: h,u,v x2 + bed + grain + moisture read (33 B), u,v x2 written (16 B)
-STEP_BYTES_PER_CELL = 57   # the fused step's algorithmic bytes (both layers)
+# Algorithmic bytes of k_force per stepped cell-layer: water reads h, u, v,
+# bed (16 B) and writes u, v (8 B); slurry also reads grain and moisture (5 B).
+FORCE_BYTES_WATER = 24
+FORCE_BYTES_SLURRY = 29
+STEP_BYTES_PER_CELL = 57   # the fused step's algorithmic bytes (both layers) per coarse cell
 
 
 def parse():
@@ -227,8 +230,10 @@ def run_b200(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    h0 = time.perf_counter()
     for _ in range(args.steps):
         one_step(False)
+    host_ms = (time.perf_counter() - h0) * 1000.0 / args.steps
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -270,16 +275,20 @@ def run_b200(args):
     led = sheet.ledger()
     if rank == 0:
         peak, peak_kind = measured_peak()
-        force_ms = parts["force_ms"] / max(parts["force_launches"], 1)
-        force_bytes = FORCE_BYTES_PER_CELL * args.res * args.res
+        launches = max(parts["force_launches"], 1)
+        force_ms = parts["force_ms"] / launches
+        cw = parts["force_cells_water"] / launches
+        cs = (parts["force_cells"] - parts["force_cells_water"]) / launches
+        force_bytes = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * cs
         achieved = force_bytes / (force_ms / 1000.0) / 1e9 if force_ms > 0 else None
         per_cell = profiled_traffic()
         roof = {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
                 "traffic": per_cell * args.res * args.res if per_cell else None,
                 "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms,
-                "transport_avg_launch_ms": parts["transport_ms"] / max(parts["force_launches"], 1),
-                "step_algorithmic_gbs": STEP_BYTES_PER_CELL * args.res * args.res * args.steps / (ms / 1000.0) / 1e9}
+                "stepped_cell_layers_per_launch": cw + cs,
+                "active_fraction": (cw + cs) / (2.0 * args.res * args.res),
+                "transport_avg_launch_ms": parts["transport_ms"] / max(parts["force_launches"], 1)}
         line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -287,6 +296,7 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(tires_for(1, args)) * 32,
                         "d2h_bytes_per_step": 56 + 4 + 32 * (nev // max(e2e_steps, 1)), "steps": e2e_steps},
                 "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
+                "host_submit_ms_per_step": host_ms,
                 "window_steps_per_s": world * args.steps / (ms / 1000.0),
                 "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
                            "spray_m3": led["spray_m3"]}}

@@ -289,6 +289,7 @@ __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, 
         }
     if (active) {
         tf.list[atomicAdd(tf.count, 1)] = (l << 30) | t;
+        if (tf.stepped) atomicAdd(&tf.stepped[l], 1ull);
     } else if (!tf.zero_uv[l][nxt][t] || !tf.zero_h[l][nxt][t]) {
         tf.list[atomicAdd(tf.count, 1)] = (l << 30) | (1 << 29) | t;
     }

@@ -43,6 +43,7 @@ struct TileFlags {
     uint8_t* zero_h[2][2];   // [layer][buffer]: h of the tile is all zero
     int* list;               // entries (layer << 30) | (zero_fill << 29) | tile
     int* count;
+    unsigned long long* stepped;  // per layer: running total of tiles stepped (may be nullptr)
     int32_t tiles_x;
 };
 

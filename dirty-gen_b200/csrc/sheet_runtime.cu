@@ -245,9 +245,8 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         if (s->timing) CK(cudaEventRecord(ev[1], s->st));
         CK(silt::launch_transport(T, res, 2, s->st));
         if (s->timing) CK(cudaEventRecord(ev[2], s->st));
-        s->parts.launches += 2;
+        s->parts.launches += 3;
         s->parts.force_launches += 1;
-        s->parts.force_cells += (int64_t)s->n;
         for (int l = 0; l < 2; ++l)
             if (F.lay[l].skip) {
                 CK(cudaMemcpyAsync(s->h[l][nxt], s->h[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
@@ -329,7 +328,8 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
     }
     s->parts.launches += 1;
     s->parts.force_launches += 1;
-    s->parts.force_cells += (int64_t)s->n;
+    s->parts.force_cells += 2 * (int64_t)s->n;
+    s->parts.force_cells_water += (int64_t)s->n;
     s->vmax_bound = silt::host::kSpeedCap * 1.4142137f;
     return SILT_OK;
 }
@@ -398,7 +398,7 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_acc, 8 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 8 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
     s->engine = cfg->engine == SILT_ENGINE_WINDOW || cfg->engine == SILT_ENGINE_GRID
@@ -426,6 +426,7 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
             q = (uint8_t*)(((uintptr_t)q + 15) & ~uintptr_t(15));
             s->tf.list = (int*)q;
             s->tf.count = s->tf.list + 2 * nt;
+            s->tf.stepped = reinterpret_cast<unsigned long long*>(s->d_u32 + 4);
             s->tf.tiles_x = tx;
         }
     }
@@ -894,6 +895,7 @@ int silt_near_tiles(silt_sheet* s, int32_t* out) {
 int silt_set_step_timing(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     CK(cudaStreamSynchronize(s->st));
+    if (s->tile_mem) CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, s->st));
     for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
     s->ev_used.clear();
     memset(&s->parts, 0, sizeof s->parts);
@@ -913,6 +915,13 @@ int silt_get_step_parts(silt_sheet* s, silt_step_parts* out) {
     }
     for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
     s->ev_used.clear();
+    if (s->tile_mem) {
+        // Cells of the tiles the force kernel stepped (32 x 32 per tile layer).
+        unsigned long long stepped[2] = {0, 0};
+        CK(cudaMemcpy(stepped, s->d_u32 + 4, 16, cudaMemcpyDeviceToHost));
+        s->parts.force_cells = (int64_t)(stepped[0] + stepped[1]) * silt::GRID_TILE * silt::GRID_TILE;
+        s->parts.force_cells_water = (int64_t)stepped[0] * silt::GRID_TILE * silt::GRID_TILE;
+    }
     *out = s->parts;
     return SILT_OK;
 }

@@ -52,7 +52,7 @@ class CoarseCell(ctypes.Structure):
 class StepParts(ctypes.Structure):
     _fields_ = [("force_ms", ctypes.c_double), ("transport_ms", ctypes.c_double), ("fine_ms", ctypes.c_double),
                 ("steps", ctypes.c_int64), ("launches", ctypes.c_int64), ("force_launches", ctypes.c_int64),
-                ("force_cells", ctypes.c_int64)]
+                ("force_cells", ctypes.c_int64), ("force_cells_water", ctypes.c_int64)]
 
 
 class SiltError(RuntimeError):

@@ -165,10 +165,13 @@ int silt_near_tiles(silt_sheet* s, int32_t* out);
 /* Device time per kernel family since timing was last switched on, measured
  * with CUDA events on the handle's stream. The GPU counterpart of
  * FluidCore::step_parts (src/fluid_core.rs:4782-4795, :6130). `launches`
- * counts this library's kernel launches (always counted). */
+ * counts this library's kernel launches (always counted); `force_cells` the
+ * cell-layers the force kernel stepped (the grid engine's active tiles, or
+ * every window cell on the window engine), `force_cells_water` the water
+ * layer's share. */
 typedef struct {
     double force_ms, transport_ms, fine_ms;
-    int64_t steps, launches, force_launches, force_cells;
+    int64_t steps, launches, force_launches, force_cells, force_cells_water;
 } silt_step_parts;
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
