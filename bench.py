@@ -143,25 +143,43 @@ def profiled_traffic():
         return None
 
 
-def cpu_baseline(args, scene, steps=40):
-    """The CPU oracle (restated reference) on this host: same workload, a bounded sample of steps."""
+def cpu_threads(args):
+    """Threads the oracle runs on: the coarse pair on two (the reference's
+    rayon::join of the two sheets), each fine patch's two sheets on their own."""
+    return 2 if args.no_tires else 2 * 4
+
+
+def cpu_baseline(args, scene, max_steps=40, warmup=1, budget_s=20.0):
+    """The CPU oracle (restated reference) on this host: the same workload for a
+    bounded sample of steps (at most `max_steps`, stopping once `budget_s` has passed)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    core = oracle.Core(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1)
+    threads = cpu_threads(args)
+    core = oracle.Core(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=threads)
     seed(core, scene)
-    core.step(DT)  # warm
-    t0 = time.perf_counter()
-    for k in range(steps):
-        for t in tires_for(k + 1, args):
+    k = 0
+    for _ in range(max(1, warmup)):
+        for t in tires_for(k, args):
             core.push_tire(**t)
         core.step(DT)
-    el = time.perf_counter() - t0
+        k += 1
+    steps = 0
+    t0 = time.perf_counter()
+    el = 0.0
+    while steps < max(1, max_steps) and el < budget_s:
+        for t in tires_for(k, args):
+            core.push_tire(**t)
+        core.step(DT)
+        k += 1
+        steps += 1
+        el = time.perf_counter() - t0
     fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
     value = (args.res * args.res + fine_cells) * steps / el
-    return {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{steps} steps of the same {args.res}^2 workload after 1 warm-up step, single thread "
-                      f"({el:.2f} s)"}
+    return {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "steps": steps, "seconds": el,
+            "sample": f"{steps} steps of the same {args.res}^2 workload after {max(1, warmup)} warm-up step(s); "
+                      f"coarse pair on 2 threads, fine patch sheets on {threads} ({el:.2f} s)"}
 
 
 def run_reference(args):
@@ -169,14 +187,15 @@ def run_reference(args):
     if rank != 0:
         return
     scene = make_scene(args)
-    base = cpu_baseline(args, scene, steps=max(1, min(args.steps, 3)))
-    line = {"metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
-            "steps": max(1, min(args.steps, 3)), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": workload(args), "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    base = cpu_baseline(args, scene, max_steps=args.steps, warmup=args.warmup, budget_s=60.0)
     fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
-    line["ms_per_step"] = 1000.0 * (args.res * args.res + fine_cells) / base["value"]
+    line = {"metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": base["steps"], "warmup": max(1, args.warmup),
+            "ms_per_step": 1000.0 * (args.res * args.res + fine_cells) / base["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference", "config": workload(args), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 

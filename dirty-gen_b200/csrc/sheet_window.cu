@@ -680,7 +680,11 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
     }
     __syncthreads();
     const int nbodies = S.nbox;
-    if (nbodies > MAX_BOXES) {  // more bodies than slots: the whole box
+    // More than MAX_BOXES bodies: step the whole box. The reference merges the
+    // grown bodies first and only then falls back at more than 8 boxes, so
+    // this differs from it only when over 512 separate bodies would merge
+    // into 8 or fewer boxes.
+    if (nbodies > MAX_BOXES) {
         __syncthreads();
         set_whole(S, x0, x1, y0, y1);
         return;

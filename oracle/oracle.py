@@ -19,7 +19,7 @@ _p = ctypes.c_void_p
 class CoreCfg(ctypes.Structure):
     _fields_ = [("res", _i), ("cell", _f), ("fine_res", _i), ("fine_cell", _f),
                 ("layout", _i), ("tire_r", _f), ("soften", _i), ("inner_par", _i),
-                ("center_x", _f), ("center_z", _f)]
+                ("center_x", _f), ("center_z", _f), ("threads", _i)]
 
 
 class Tire(ctypes.Structure):
@@ -171,11 +171,11 @@ class Core:
     """The reference `FluidCore` subset on the sheet path (window 200 at 0.2 m by default)."""
 
     def __init__(self, res=200, cell=0.2, fine_res=160, fine_cell=0.02, layout=0, tire_r=0.56,
-                 soften=True, inner_par=False, center=(0.0, 0.0)):
+                 soften=True, inner_par=False, center=(0.0, 0.0), threads=1):
         self.res = res
         self.fine_res = fine_res
         cfg = CoreCfg(res, cell, fine_res, fine_cell, layout, tire_r, int(soften), int(inner_par),
-                      center[0], center[1])
+                      center[0], center[1], int(threads))
         self.h = lib().oracle_core_new(ctypes.byref(cfg))
 
     def __del__(self):

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -1035,6 +1036,7 @@ struct Core {
     Scratch coarse_sc[2][2];
     std::vector<float> nu_w, nu_s;  // PairScratch rows (src/fluid_core.rs:621-647)
     std::vector<float> fnu_w, fnu_s;
+    std::vector<std::vector<float>> fnu_s_rows;
     std::vector<u8> gate, fgate;
     int inflow_j = -1;
     float inflow_x0 = 0, inflow_x1 = 0, inflow_rate = 0;
@@ -1529,32 +1531,61 @@ struct Core {
         float cap = fine ? fine_sub_cap : 8.0f;
         int pace = fine ? fine_pace : 0;
         if (!fine) {
-            usize n = res * res;
-            Box wb;
-            if (cfg.soften) soften_border(uw.data(), vw.data(), res);
-            step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0);
-            if (wet_bounds(slurry.data(), res, NU_FILL_MARGIN, wb))
-                for (usize j = wb.j0; j <= wb.j1; ++j)
-                    for (usize i = wb.i0; i <= wb.i1; ++i) {
-                        usize idx = j * res + i;
-                        nu_s[idx] = dynamic_viscosity(grain[idx], moisture[idx]);
-                    }
-            if (cfg.soften) soften_border(us.data(), vs.data(), res);
-            step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0);
-            (void)n;
+            auto run_water = [&]() {
+                if (cfg.soften) soften_border(uw.data(), vw.data(), res);
+                step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0);
+            };
+            auto run_slurry = [&]() {
+                Box wb;
+                if (wet_bounds(slurry.data(), res, NU_FILL_MARGIN, wb))
+                    for (usize j = wb.j0; j <= wb.j1; ++j)
+                        for (usize i = wb.i0; i <= wb.i1; ++i) {
+                            usize idx = j * res + i;
+                            nu_s[idx] = dynamic_viscosity(grain[idx], moisture[idx]);
+                        }
+                if (cfg.soften) soften_border(us.data(), vs.data(), res);
+                step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0);
+            };
+            // src/fluid_core.rs:8127-8131: the two sheets on two workers.
+            if (cfg.threads > 1) {
+                std::thread t(run_slurry);
+                run_water();
+                t.join();
+            } else {
+                run_water();
+                run_slurry();
+            }
             return;
         }
-        for (usize pk = 0; pk < active_patches(); ++pk) {
+        // Each patch's slurry reads its own viscosity row (patches run on
+        // their own workers when threads > 1; results do not depend on it).
+        if (fnu_s_rows.size() < active_patches()) fnu_s_rows.resize(active_patches(), std::vector<float>(fres * fres, 0.0f));
+        auto run_patch = [&](usize pk, int layer) {
             Patch& P = patches[pk];
+            if (layer == 0) {
+                step_sheet_eps(P.water.data(), P.uw.data(), P.vw.data(), P.bed.data(), fnu_w.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.08f, 1.0e-6f, false, cap, pace, P.sc[0][0], &P.sc[0][1], false);
+                return;
+            }
+            std::vector<float>& nu = fnu_s_rows[pk];
             Box wb;
-            step_sheet_eps(P.water.data(), P.uw.data(), P.vw.data(), P.bed.data(), fnu_w.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.08f, 1.0e-6f, false, cap, pace, P.sc[0][0], &P.sc[0][1], false);
             if (wet_bounds(P.slurry.data(), fres, NU_FILL_MARGIN, wb))
                 for (usize j = wb.j0; j <= wb.j1; ++j)
                     for (usize i = wb.i0; i <= wb.i1; ++i) {
                         usize idx = j * fres + i;
-                        fnu_s[idx] = dynamic_viscosity(P.grain[idx], P.moisture[idx]);
+                        nu[idx] = dynamic_viscosity(P.grain[idx], P.moisture[idx]);
                     }
-            step_sheet_eps(P.slurry.data(), P.us.data(), P.vs.data(), P.bed_slurry.data(), fnu_s.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.05f, 1.0e-6f, false, cap, pace, P.sc[1][0], &P.sc[1][1], false);
+            step_sheet_eps(P.slurry.data(), P.us.data(), P.vs.data(), P.bed_slurry.data(), nu.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.05f, 1.0e-6f, false, cap, pace, P.sc[1][0], &P.sc[1][1], false);
+        };
+        if (cfg.threads > 1) {
+            std::vector<std::thread> pool;
+            for (usize pk = 0; pk < active_patches(); ++pk)
+                for (int l = 0; l < 2; ++l) pool.emplace_back(run_patch, pk, l);
+            for (auto& t : pool) t.join();
+        } else {
+            for (usize pk = 0; pk < active_patches(); ++pk) {
+                run_patch(pk, 0);
+                run_patch(pk, 1);
+            }
         }
     }
 

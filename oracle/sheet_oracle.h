@@ -65,6 +65,7 @@ typedef struct {
     int soften;        // 1: soften_border on the coarse velocity (reference: 1)
     int inner_par;     // 0: coarse pair runs serial inner loops (reference step_pair)
     float center_x, center_z;
+    int threads;       // >1: each sheet of a pair on its own thread (the reference's rayon::join)
 } oracle_core_cfg;
 
 typedef struct {
