@@ -34,6 +34,7 @@
 #include "sheet_host_math.h"
 #include "sheet_math.cuh"
 #include "sheet_window.cuh"
+#include "launch_count.cuh"
 
 namespace silt {
 namespace fine {
@@ -64,6 +65,7 @@ thread_local char g_err[200] = "";
 struct PatchState {
     float* base = nullptr;
     float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
+    float *nu_s, *mob_s, *damp_s;  // slurry material of each cell, from grain and moisture at lay time
     uint8_t* grain;
     float* win[2];        // [layer]: the window engine's scratch planes
     // Host geometry of the current step.
@@ -73,6 +75,7 @@ struct PatchState {
 
 struct PatchRef {
     float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
+    float *nu_s, *mob_s, *damp_s;
     uint8_t* grain;
     const int16_t* col;
     const int16_t* row;
@@ -156,10 +159,19 @@ __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W
         R.us[f] = 0.0f;
         R.vs[f] = 0.0f;
         const int ci = R.col[f % fres], cj = R.row[f / fres];
+        if (ci >= 0 && cj >= 0) {
+            const size_t c = (size_t)cj * W.res + ci;
+            R.moisture[f] = W.moisture[c];
+            R.grain[f] = W.grain[c];
+        }
+        // The slurry's material laws once per step here, spread over the whole
+        // GPU, instead of once per cell and substep inside the patch's step.
+        const float nu = dynamic_viscosity(R.grain[f], R.moisture[f]);
+        R.nu_s[f] = nu;
+        R.mob_s[f] = sheet_mobility_for(nu);
+        R.damp_s[f] = sheet_damp(nu);
         if (ci < 0 || cj < 0) continue;
         const size_t c = (size_t)cj * W.res + ci;
-        R.moisture[f] = W.moisture[c];
-        R.grain[f] = W.grain[c];
         if (owner[c] != p) {
             R.bed[f] = W.bed[c] + W.h[0][c];
             R.bed_slurry[f] = W.bed[c] + W.h[1][c];
@@ -265,11 +277,8 @@ __global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int*
 
 // push_on (src/fluid_core.rs:8169-8239); every thread owns one cell of the
 // pushes' joint span and applies the pushes in call order.
-__global__ void k_push_cells(float* w, float* s, float* uw, float* vw, float* us, float* vs, int res, float cell,
-                             float ox, float oz, const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= bw * bh) return;
-    const int i = bi0 + k % bw, j = bj0 + k / bw;
+__device__ void push_cell(float* w, float* s, float* uw, float* vw, float* us, float* vs, int res, float cell,
+                          float ox, float oz, const PushJob* jobs, int njobs, int i, int j) {
     const size_t idx = (size_t)j * res + i;
     for (int q = 0; q < njobs; ++q) {
         const PushJob p = jobs[q];
@@ -306,15 +315,35 @@ __global__ void k_push_cells(float* w, float* s, float* uw, float* vw, float* us
     }
 }
 
+__global__ void k_push_cells(float* w, float* s, float* uw, float* vw, float* us, float* vs, int res, float cell,
+                             float ox, float oz, const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bw * bh; k += gridDim.x * blockDim.x)
+        push_cell(w, s, uw, vw, us, vs, res, cell, ox, oz, jobs, njobs, bi0 + k % bw, bj0 + k / bw);
+}
+
+// One patch's shove or peel jobs within a launch over all patches (blockIdx.y).
+struct JobGroup {
+    int patch;          // PatchRef index
+    float ox, oz;       // patch origin
+    int job_off;        // byte offset of its PushJob list in the step table
+    int njobs, i0, j0, w, h;
+};
+
+__global__ void k_push_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int fres, float fcell) {
+    const JobGroup G = groups[blockIdx.y];
+    const PatchRef& R = refs[G.patch];
+    const PushJob* jobs = reinterpret_cast<const PushJob*>(tab + G.job_off);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < G.w * G.h; k += gridDim.x * blockDim.x)
+        push_cell(R.water, R.slurry, R.uw, R.vw, R.us, R.vs, fres, fcell, G.ox, G.oz, jobs, G.njobs,
+                  G.i0 + k % G.w, G.j0 + k / G.w);
+}
+
 // peel_spray (src/fluid_core.rs:8241-8314). Events carry a sort key that
 // restores the reference's order (phase, patch, push, row, column).
-__global__ void k_peel(float* w, const float* uw, const float* vw, int res, float cell, float ox, float oz,
-                       const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh, const int8_t* owner,
-                       int coarse_res, float cox, float coz, float coarse_cell, int phase, int patch, SprayRec* out,
-                       int* counters, double* books, double* ledger_depth) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= bw * bh) return;
-    const int i = bi0 + k % bw, j = bj0 + k / bw;
+__device__ void peel_cell(float* w, const float* uw, const float* vw, int res, float cell, float ox, float oz,
+                          const PushJob* jobs, int njobs, int i, int j, const int8_t* owner, int coarse_res, float cox,
+                          float coz, float coarse_cell, int phase, int patch, SprayRec* out, int* counters,
+                          double* books, double* ledger_depth) {
     const size_t idx = (size_t)j * res + i;
     const float area = cell * cell;
     for (int q = 0; q < njobs; ++q) {
@@ -356,6 +385,26 @@ __global__ void k_peel(float* w, const float* uw, const float* vw, int res, floa
     }
 }
 
+__global__ void k_peel(float* w, const float* uw, const float* vw, int res, float cell, float ox, float oz,
+                       const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh, const int8_t* owner,
+                       int coarse_res, float cox, float coz, float coarse_cell, int phase, int patch, SprayRec* out,
+                       int* counters, double* books, double* ledger_depth) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bw * bh; k += gridDim.x * blockDim.x)
+        peel_cell(w, uw, vw, res, cell, ox, oz, jobs, njobs, bi0 + k % bw, bj0 + k / bw, owner, coarse_res, cox, coz,
+                  coarse_cell, phase, patch, out, counters, books, ledger_depth);
+}
+
+// The fine peel of every patch in one launch (phase 0: no held-column test, no coarse ledger).
+__global__ void k_peel_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int fres, float fcell,
+                               SprayRec* out, int* counters, double* books) {
+    const JobGroup G = groups[blockIdx.y];
+    const PatchRef& R = refs[G.patch];
+    const PushJob* jobs = reinterpret_cast<const PushJob*>(tab + G.job_off);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < G.w * G.h; k += gridDim.x * blockDim.x)
+        peel_cell(R.water, R.uw, R.vw, fres, fcell, G.ox, G.oz, jobs, G.njobs, G.i0 + k % G.w, G.j0 + k / G.w,
+                  nullptr, 0, 0.0f, 0.0f, 1.0f, 0, G.patch, out, counters, books, nullptr);
+}
+
 // near_capture (near.rs:199-273): one block of 128 threads per held near column.
 __global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol, int* slot_map,
                                float* pool, NearMeta* meta, int* free_stack, int* counters) {
@@ -367,7 +416,7 @@ __global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const Ne
     __shared__ float bw_[1024], bs_[1024], bu_[1024], bv_[1024];
     __shared__ int decision;   // 0 remove, 1 keep
     __shared__ int slot_s;
-    __shared__ float mw_s, ms_s, uu_s, vv_s, peak_s, sw_s;
+    __shared__ float mw_s, ms_s, uu_s, vv_s, sw_s;
     __shared__ double mean_w, mean_s;
     for (int k = threadIdx.x; k < n2; k += blockDim.x) {
         const int f = (C.j0 + k / sub) * fres + C.i0 + k % sub;
@@ -424,7 +473,6 @@ __global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const Ne
         mw_s = mw;
         ms_s = ms;
         sw_s = sw;
-        peak_s = peak;
         int slot = slot_map[C.cidx];
         if (!keep) {
             if (slot >= 0) {
@@ -477,29 +525,48 @@ __global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const Ne
     }
 }
 
-// restrict_fine (src/fluid_core.rs:8462-8555): one thread per touched coarse column.
-__global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const RestrictEntry* ents, int nent,
-                           const Segment* segs, float fine_area, float coarse_area, int full) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nent) return;
-    const RestrictEntry E = ents[q];
+__device__ void restrict_column(const PatchRef* refs, int fres, const SheetView& W, const RestrictEntry& E,
+                                const Segment* segs, float fine_area, float coarse_area, int lane) {
     float aw = 0.0f, as = 0.0f, auw = 0.0f, avw = 0.0f, aus = 0.0f, avs = 0.0f;
     for (int sgi = 0; sgi < E.seg_n; ++sgi) {
         const Segment S = segs[E.seg_off + sgi];
         const PatchRef& R = refs[S.patch];
-        for (int j = S.j0; j <= S.j1; ++j)
-            for (int i = S.i0; i <= S.i1; ++i) {
-                const int f = j * fres + i;
+        const int ni = S.i1 - S.i0 + 1, nc = ni * (S.j1 - S.j0 + 1);
+        for (int c0 = 0; c0 < nc; c0 += 32) {
+            const int c = c0 + lane;
+            float pw = 0.0f, ps = 0.0f, puw = 0.0f, pvw = 0.0f, pus = 0.0f, pvs = 0.0f;
+            int take = 0;
+            if (c < nc) {
+                const int f = (S.j0 + c / ni) * fres + S.i0 + c % ni;
                 const float fw = R.water[f], fs = R.slurry[f];
-                if (fw == 0.0f && fs == 0.0f) continue;
-                aw += fw * fine_area;
-                as += fs * fine_area;
-                auw += R.uw[f] * fw * fine_area;
-                avw += R.vw[f] * fw * fine_area;
-                aus += R.us[f] * fs * fine_area;
-                avs += R.vs[f] * fs * fine_area;
+                if (!(fw == 0.0f && fs == 0.0f)) {
+                    take = 1;
+                    pw = fw * fine_area;
+                    ps = fs * fine_area;
+                    puw = R.uw[f] * fw * fine_area;
+                    pvw = R.vw[f] * fw * fine_area;
+                    pus = R.us[f] * fs * fine_area;
+                    pvs = R.vs[f] * fs * fine_area;
+                }
             }
+            const unsigned takes = __ballot_sync(0xffffffffu, take);
+            const int m = min(32, nc - c0);
+            for (int b = 0; b < m; ++b) {
+                const float xw = __shfl_sync(0xffffffffu, pw, b), xs = __shfl_sync(0xffffffffu, ps, b);
+                const float xuw = __shfl_sync(0xffffffffu, puw, b), xvw = __shfl_sync(0xffffffffu, pvw, b);
+                const float xus = __shfl_sync(0xffffffffu, pus, b), xvs = __shfl_sync(0xffffffffu, pvs, b);
+                if ((takes >> b) & 1u) {
+                    aw += xw;
+                    as += xs;
+                    auw += xuw;
+                    avw += xvw;
+                    aus += xus;
+                    avs += xvs;
+                }
+            }
+        }
     }
+    if (lane != 0) return;
     const size_t idx = E.cidx;
     const float w = aw / coarse_area, s = as / coarse_area;
     mark_tile(W, 0, (int)(idx % W.res), (int)(idx / W.res));
@@ -509,7 +576,6 @@ __global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const Re
     // cell every touched column is fully covered and this is the reference's
     // `!held && cnt >= full` branch; a partly covered rim column (64-cell
     // patches) must not lose the coarse depth it kept.
-    (void)full;
     if (!E.held) {
         if (w <= 0.0f && s <= 0.0f) return;
         const float old_w = W.h[0][idx], old_s = W.h[1][idx];
@@ -539,6 +605,19 @@ __global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const Re
         W.u[1][idx] = aus / (s * coarse_area);
         W.v[1][idx] = avs / (s * coarse_area);
     }
+}
+
+// restrict_fine (src/fluid_core.rs:8462-8555): one warp per touched coarse
+// column. The lanes load 32 fine cells at a time and form their products in
+// parallel; the six sums then take the products one by one in the
+// reference's raster order (every lane adds the same sequence).
+__global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const RestrictEntry* ents, int nent,
+                           const Segment* segs, float fine_area, float coarse_area, int full) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (int)((gridDim.x * (size_t)blockDim.x) >> 5);
+    for (int q = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5); q < nent; q += warps)
+        restrict_column(refs, fres, W, ents[q], segs, fine_area, coarse_area, lane);
+    (void)full;
 }
 
 // Fine cells outside the coarse window: their volume is parked (src/fluid_core.rs:8476-8484).
@@ -701,6 +780,8 @@ struct StepPlan {
     size_t off_refs = 0, off_held = 0, off_oidx = 0, off_oval = 0, off_near = 0, off_ent = 0, off_seg = 0;
     std::vector<JobList> fine_push, fine_peel;
     JobList coarse_push, coarse_peel;
+    size_t off_push_groups = 0, off_peel_groups = 0;
+    int n_push_groups = 0, n_peel_groups = 0, push_cells_max = 0, peel_cells_max = 0;
     int slot = 0;
 };
 
@@ -719,8 +800,8 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
     const size_t fn = (size_t)P.fres * P.fres;
     while ((int)P.patches.size() < np) {
         PatchState* S = new PatchState();
-        // 9 planes + a spare + the window engine's scratch for two layers, then grain.
-        const size_t planes = 10 + 2 * (size_t)window::SCRATCH_PLANES;
+        // 12 planes + a spare + the window engine's scratch for two layers, then grain.
+        const size_t planes = 13 + 2 * (size_t)window::SCRATCH_PLANES;
         cudaError_t e = cudaMalloc(&S->base, planes * fn * sizeof(float) + fn + 256);
         if (e != cudaSuccess) {
             delete S;
@@ -728,9 +809,9 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
             return SILT_ENOMEM;
         }
         float* q = S->base;
-        float** named[9] = {&S->water, &S->slurry, &S->uw, &S->vw, &S->us, &S->vs, &S->bed, &S->bed_slurry,
-                            &S->moisture};
-        for (int k = 0; k < 9; ++k) {
+        float** named[12] = {&S->water, &S->slurry, &S->uw, &S->vw, &S->us,      &S->vs,
+                             &S->bed,   &S->bed_slurry, &S->moisture, &S->nu_s, &S->mob_s, &S->damp_s};
+        for (int k = 0; k < 12; ++k) {
             *named[k] = q;
             q += fn;
         }
@@ -915,6 +996,34 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         L.fine_peel.push_back(job_list(tab, peel));
     }
     {
+        std::vector<JobGroup> pg, qg;
+        L.push_cells_max = L.peel_cells_max = 0;
+        for (int p = 0; p < L.np; ++p) {
+            const PatchState* S = P.patches[p];
+            for (int which = 0; which < 2; ++which) {
+                const JobList& J = which ? L.fine_peel[p] : L.fine_push[p];
+                if (!J.n) continue;
+                JobGroup G;
+                G.patch = p;
+                G.ox = S->origin[0];
+                G.oz = S->origin[1];
+                G.job_off = (int)J.off;
+                G.njobs = J.n;
+                G.i0 = J.i0;
+                G.j0 = J.j0;
+                G.w = J.w;
+                G.h = J.h;
+                (which ? qg : pg).push_back(G);
+                int& mx = which ? L.peel_cells_max : L.push_cells_max;
+                mx = std::max(mx, J.w * J.h);
+            }
+        }
+        L.n_push_groups = (int)pg.size();
+        L.n_peel_groups = (int)qg.size();
+        L.off_push_groups = tab.put(pg.data(), pg.size());
+        L.off_peel_groups = tab.put(qg.data(), qg.size());
+    }
+    {
         std::vector<PushJob> push, peel;
         for (size_t q = 0; q < ps.size(); ++q) {
             peel.push_back(make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, peel_reach(ps[q], W.cell)));
@@ -955,6 +1064,9 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         r.bed = S->bed;
         r.bed_slurry = S->bed_slurry;
         r.moisture = S->moisture;
+        r.nu_s = S->nu_s;
+        r.mob_s = S->mob_s;
+        r.damp_s = S->damp_s;
         r.grain = S->grain;
         const int16_t* dax = reinterpret_cast<const int16_t*>(HS.d_tab[slot] + off_axes);
         r.col = dax + (size_t)p * 2 * fres;
@@ -988,7 +1100,10 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 J.vort = l == 0 ? 0.08f : 0.05f;
                 J.sub_cap = P.sub_cap;
                 J.eps = 1.0e-6f;
-                J.nu_mode = l == 0 ? window::NU_CONST : window::NU_GRAIN;
+                J.nu_mode = l == 0 ? window::NU_CONST : window::NU_TABLE;
+                J.nu_plane = S->nu_s;
+                J.mob_plane = S->mob_s;
+                J.damp_plane = S->damp_s;
                 J.nu_c = nu_w;
                 J.mob_c = host::sheet_mobility_for(nu_w);
                 for (int k = 1; k <= 8; ++k) J.decay_c[k] = expf(-host::sheet_damp(nu_w) * (dt / (float)k));
@@ -1021,12 +1136,15 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
     if (L.n_owner) {
         k_scatter_owner<<<launch_blocks(L.n_owner), 256, 0, W.st>>>(M.owner, TAB(int, L.off_oidx),
                                                                      TAB(int8_t, L.off_oval), L.n_owner);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner);
+    ::silt::count_launch();
     FCK(cudaGetLastError());
     if (!L.held.empty()) {
         k_zero_cells<<<launch_blocks(L.held.size()), 256, 0, W.st>>>(W, TAB(int, L.off_held), (int)L.held.size());
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     P.fine_on = true;
@@ -1035,10 +1153,12 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
         if (L.n_near) {
             k_near_apply<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
                                                      M.slot_map, M.pool, M.meta);
+            ::silt::count_launch();
             FCK(cudaGetLastError());
         }
         k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
                                                               dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     return SILT_OK;
@@ -1054,18 +1174,21 @@ int restrict_all(Patches& P, silt_sheet* s) {
     if (P.near_on && L.n_near) {
         k_near_capture<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
                                                    M.slot_map, M.pool, M.meta, M.free_stack, M.counters);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
         M.near_maybe = true;
     }
     if (L.n_ent) {
-        k_restrict<<<launch_blocks(L.n_ent, 128), 128, 0, W.st>>>(refs, P.fres, W, TAB(RestrictEntry, L.off_ent),
+        k_restrict<<<launch_blocks((size_t)L.n_ent * 32, 128), 128, 0, W.st>>>(refs, P.fres, W, TAB(RestrictEntry, L.off_ent),
                                                                  L.n_ent, TAB(Segment, L.off_seg), P.fcell * P.fcell,
                                                                  W.cell * W.cell, P.sub * P.sub);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     if (L.any_park) {
         k_park<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres,
                                                                                 P.fcell * P.fcell, M.d_books);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     const size_t fn = (size_t)P.fres * P.fres;
@@ -1084,6 +1207,7 @@ static int fade_only(Patches& P, silt_sheet* s, float dt) {
     SheetView W = view_of(s);
     k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
                                                           dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+    ::silt::count_launch();
     FCK(cudaGetLastError());
     return SILT_OK;
 }
@@ -1101,23 +1225,20 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     HostState& HS = H(P);
     const StepPlan& L = HS.plan;
     W = view_of(s);
-    for (int p = 0; p < L.np; ++p) {
-        PatchState* S = P.patches[p];
-        const JobList& J = L.fine_push[p];
-        if (!J.n) continue;
-        k_push_cells<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(
-            S->water, S->slurry, S->uw, S->vw, S->us, S->vs, P.fres, P.fcell, S->origin[0], S->origin[1],
-            TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w, J.h);
+    const PatchRef* refs = TAB(PatchRef, L.off_refs);
+    const char* tab = TAB(char, 0);
+    if (L.n_push_groups) {
+        dim3 grid(launch_blocks((size_t)L.push_cells_max), L.n_push_groups);
+        k_push_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_push_groups), P.fres, P.fcell);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    FCK(window::launch_window_step(TAB(window::Job, L.off_jobs), 2 * L.np, W.st));
-    for (int p = 0; p < L.np; ++p) {
-        PatchState* S = P.patches[p];
-        const JobList& J = L.fine_peel[p];
-        if (!J.n) continue;
-        k_peel<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(
-            S->water, S->uw, S->vw, P.fres, P.fcell, S->origin[0], S->origin[1], TAB(PushJob, J.off), J.n, J.i0, J.j0,
-            J.w, J.h, nullptr, W.res, W.origin[0], W.origin[1], W.cell, 0, p, M.spray, M.counters, M.d_books, nullptr);
+    FCK(window::launch_window_step(TAB(window::Job, L.off_jobs), 2 * L.np, P.fres, W.st));
+    if (L.n_peel_groups) {
+        dim3 grid(launch_blocks((size_t)L.peel_cells_max), L.n_peel_groups);
+        k_peel_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_peel_groups), P.fres, P.fcell, M.spray,
+                                               M.counters, M.d_books);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     if ((rc = restrict_all(P, s))) return rc;
@@ -1127,6 +1248,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
                                                                          W.v[1], W.res, W.cell, W.origin[0],
                                                                          W.origin[1], TAB(PushJob, J.off), J.n, J.i0,
                                                                          J.j0, J.w, J.h);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
     }
     // A shove changes a cell's speed by at most 1.04 max(speed, 0.4)
@@ -1164,6 +1286,7 @@ int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps
                                                                W.origin[1], TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w,
                                                                J.h, M.owner, W.res, W.origin[0], W.origin[1], W.cell,
                                                                1, 0, M.spray, M.counters, M.d_books, W.d_acc);
+    ::silt::count_launch();
     FCK(cudaGetLastError());
     return SILT_OK;
 }
@@ -1241,6 +1364,7 @@ int set_near_field(Patches& P, silt_sheet* s, bool on) {
         SheetView W = view_of(s);
         k_init_pool<<<launch_blocks(std::max<size_t>(W.n, NEAR_POOL)), 256, 0, W.st>>>(M.meta, M.free_stack,
                                                                                        M.slot_map, W.n, M.counters);
+        ::silt::count_launch();
         FCK(cudaGetLastError());
         M.near_maybe = false;
     }
@@ -1278,6 +1402,7 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     FCK(cudaMallocHost(&M->h_counters, 8 * sizeof(int)));
     k_init_pool<<<launch_blocks(std::max<size_t>(n, NEAR_POOL)), 256, 0, st>>>(M->meta, M->free_stack, M->slot_map, n,
                                                                                M->counters);
+    ::silt::count_launch();
     FCK(cudaGetLastError());
     return SILT_OK;
 }

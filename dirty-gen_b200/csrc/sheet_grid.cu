@@ -27,6 +27,7 @@
 
 #include "sheet_grid.cuh"
 #include "sheet_math.cuh"
+#include "launch_count.cuh"
 
 namespace silt {
 
@@ -57,6 +58,26 @@ __device__ __forceinline__ float tap5(float a0, float a1, float a2, float a3, fl
 }
 
 __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// The layer's substep count from its largest squared speed, in the host's
+// arithmetic (IEEE sqrt and divide, no contraction).
+__device__ __forceinline__ int device_nsub(const SubstepCount& c, int l) {
+    const float m2 = __uint_as_float(c.speed2[l]);
+    const float max_s = fmaxf(0.15f, sqrtf(m2));
+    const float ns = ceilf((c.dt * max_s) / (0.42f * fmaxf(c.cell, 1.0e-3f)));
+    return (int)rclamp(ns, 1.0f, c.cap);
+}
+
+// One flag plane by layer and buffer, without indexing the parameter array
+// by a runtime value (which would copy it to local memory).
+__device__ __forceinline__ uint8_t* pick(uint8_t* const (&a)[2][2], int l, int b) {
+    return l ? (b ? a[1][1] : a[1][0]) : (b ? a[0][1] : a[0][0]);
+}
+
+// Tile-list entry: layer, zero-fill and copy bits over the tile index.
+constexpr int ENTRY_ZERO = 1 << 29;
+constexpr int ENTRY_COPY = 1 << 28;
+constexpr int ENTRY_TILE = (1 << 28) - 1;
 
 // Cell material: viscosity, mobility and damping factor.
 __device__ __forceinline__ float cell_nu(const LayerParams& P, size_t g) {
@@ -241,13 +262,37 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     extern __shared__ float sm[];
+    __shared__ LayerParams Ps[2];
+    if (threadIdx.x < 2) {
+        const int l = threadIdx.x;
+        LayerParams P = L.lay[l];
+        if (L.sc.speed2) {
+            const int ns = device_nsub(L.sc, l);
+            P.dt = L.sc.dt / (float)ns;
+            if (P.nu_mode == NU_CONST) P.decay_c = L.sc.water_decay[ns];
+            if (L.sc.k == 0 && blockIdx.x == 0 && ns > L.sc.launched) atomicOr(L.sc.overflow, 1u);
+        }
+        Ps[l] = P;
+    }
+    __syncthreads();
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
-        const int l = e >> 30, zero_fill = (e >> 29) & 1, t = e & ((1 << 29) - 1);
-        const LayerParams& P = L.lay[l];
+        const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
+        const LayerParams& P = Ps[l];
         const int res = P.res;
         const int tx0 = (t % L.tf.tiles_x) * FT, ty0 = (t / L.tf.tiles_x) * FT;
+        if (copy) {
+            // Identity substep of a layer that has taken all its substeps.
+            const int w = min(FT, res - tx0), h = min(FT, res - ty0);
+            for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+                const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
+                P.u_out[g] = P.u[g];
+                P.v_out[g] = P.v[g];
+            }
+            if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = pick(L.tf.zero_uv, l, L.nxt ^ 1)[t];
+            continue;
+        }
         if (zero_fill) {
             // A quiet tile: dry in its whole neighbourhood, so after the dry cut
             // its velocity is zero.
@@ -257,7 +302,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
                 P.u_out[g] = 0.0f;
                 P.v_out[g] = 0.0f;
             }
-            if (threadIdx.x == 0) L.tf.zero_uv[l][L.nxt][t] = 1;
+            if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = 1;
             continue;
         }
         const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
@@ -265,24 +310,35 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
             force_tile<false>(P, sm, tx0, ty0);
         else
             force_tile<true>(P, sm, tx0, ty0);
-        if (threadIdx.x == 0) L.tf.zero_uv[l][L.nxt][t] = 0;
+        if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = 0;
         __syncthreads();  // shared memory is reused by the next tile
     }
 }
 
-__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1) {
+__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc) {
     const int nt = tf.tiles_x * tf.tiles_x;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= 2 * nt) return;
     const int l = k / nt, t = k % nt;
     if (l == 0 ? skip0 : skip1) return;
+    if (sc.speed2 && sc.k > 0) {  // substep 0 steps every layer; its list precedes the speed pass
+        const int ns = device_nsub(sc, l);
+        if (sc.k >= ns) {
+            // Identity substep: carry every tile not known to be zero.
+            if (!(pick(tf.zero_h, l, cur)[t] && pick(tf.zero_uv, l, cur)[t]))
+                tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_COPY | t;
+            else if (!(pick(tf.zero_h, l, nxt)[t] && pick(tf.zero_uv, l, nxt)[t]))
+                tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_ZERO | t;
+            return;
+        }
+    }
     const int ti = t % tf.tiles_x, tj = t / tf.tiles_x;
     bool active = all != 0;
     for (int dj = -1; dj <= 1 && !active; ++dj)
         for (int di = -1; di <= 1; ++di) {
             const int a = ti + di, b = tj + dj;
             if (a < 0 || b < 0 || a >= tf.tiles_x || b >= tf.tiles_x) continue;
-            if (tf.wet[l][cur][b * tf.tiles_x + a]) {
+            if (pick(tf.wet, l, cur)[b * tf.tiles_x + a]) {
                 active = true;
                 break;
             }
@@ -290,16 +346,18 @@ __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, 
     if (active) {
         tf.list[atomicAdd(tf.count, 1)] = (l << 30) | t;
         if (tf.stepped) atomicAdd(&tf.stepped[l], 1ull);
-    } else if (!tf.zero_uv[l][nxt][t] || !tf.zero_h[l][nxt][t]) {
-        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | (1 << 29) | t;
+    } else if (!pick(tf.zero_uv, l, nxt)[t] || !pick(tf.zero_h, l, nxt)[t]) {
+        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_ZERO | t;
     }
 }
 
-cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1, cudaStream_t st) {
+cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1,
+                             const SubstepCount& sc, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(tf.count, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     const int n = 2 * tf.tiles_x * tf.tiles_x;
-    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1);
+    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1, sc);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 
@@ -427,30 +485,71 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (threadIdx.x == 0) {
             if (P.ledger) atomicAdd(P.ledger, v);
-            tf.wet[l][nxt][t] = any ? 1 : 0;
-            tf.zero_h[l][nxt][t] = any ? 0 : 1;
+            pick(tf.wet, l, nxt)[t] = any ? 1 : 0;
+            pick(tf.zero_h, l, nxt)[t] = any ? 0 : 1;
         }
     }
     __syncthreads();  // shared memory is reused by the next tile
 }
 
+// Identity substep of one depth tile: copy, ledger sum and flags as
+// transport_tile leaves them.
+__device__ void copy_tile(const TransportParams& P, int tx0, int ty0, const TileFlags& tf, int l, int nxt, int t) {
+    const int res = P.res;
+    const int w = min(TT, res - tx0), h = min(TT, res - ty0);
+    double part = 0.0;
+    for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+        const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
+        const float hv = P.h[g];
+        P.h_out[g] = hv;
+        part += (double)fmaxf(hv, 0.0f);
+    }
+    const int any = __syncthreads_or(part > 0.0);
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    __shared__ double warp_sum[TRANSPORT_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? warp_sum[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) {
+            if (P.ledger) atomicAdd(P.ledger, v);
+            pick(tf.wet, l, nxt)[t] = any ? 1 : 0;
+            pick(tf.zero_h, l, nxt)[t] = any ? 0 : 1;
+        }
+    }
+    __syncthreads();
+}
+
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
     extern __shared__ float sm[];
+    __shared__ TransportParams Ps[2];
+    if (threadIdx.x < 2) {
+        const int l = threadIdx.x;
+        TransportParams P = L.lay[l];
+        if (L.sc.speed2) P.dt = L.sc.dt / (float)device_nsub(L.sc, l);
+        Ps[l] = P;
+    }
+    __syncthreads();
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
-        const int l = e >> 30, zero_fill = (e >> 29) & 1, t = e & ((1 << 29) - 1);
-        const TransportParams& P = L.lay[l];
+        const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
+        const TransportParams& P = Ps[l];
         const int res = P.res;
         const int tx0 = (t % L.tf.tiles_x) * TT, ty0 = (t / L.tf.tiles_x) * TT;
+        if (copy) {
+            copy_tile(P, tx0, ty0, L.tf, l, L.nxt, t);
+            continue;
+        }
         if (zero_fill) {
             const int w = min(TT, res - tx0), h = min(TT, res - ty0);
             for (int q = threadIdx.x; q < w * h; q += blockDim.x)
                 P.h_out[(size_t)(ty0 + q / w) * res + tx0 + q % w] = 0.0f;
             if (threadIdx.x == 0) {
-                L.tf.wet[l][L.nxt][t] = 0;
-                L.tf.zero_h[l][L.nxt][t] = 1;
+                pick(L.tf.wet, l, L.nxt)[t] = 0;
+                pick(L.tf.zero_h, l, L.nxt)[t] = 1;
             }
             continue;
         }
@@ -478,6 +577,54 @@ __global__ void k_max_speed2(const float* h, const float* u, const float* v, siz
     if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(m));
 }
 
+// k_max_speed2 over the stepped tiles of substep 0's list (every tile that
+// may hold water is one of them; a tile without water has no cell at or above
+// eps and, after the dry cut, no velocity). Each thread loads its four cells
+// before comparing, so a tile costs one memory round trip.
+__global__ void __launch_bounds__(256) k_tile_speed2(TileFlags tf, const float* h0, const float* u0, const float* v0,
+                                                     const float* h1, const float* u1, const float* v1, int res,
+                                                     float eps, int apply_cut, unsigned int* bits) {
+    const int n = *tf.count;
+    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = tf.list[k];
+        if (e & (ENTRY_ZERO | ENTRY_COPY)) continue;
+        const int l = e >> 30, t = e & ENTRY_TILE;
+        const float* h = l ? h1 : h0;
+        const float* u = l ? u1 : u0;
+        const float* v = l ? v1 : v0;
+        const int tx0 = (t % tf.tiles_x) * GRID_TILE, ty0 = (t / tf.tiles_x) * GRID_TILE;
+        const int gx = tx0 + lane;
+        float hv[4], uv[4], vv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int gy = ty0 + wy + 8 * r;
+            const bool in = gx < res && gy < res;
+            const size_t g = in ? (size_t)gy * res + gx : 0;
+            hv[r] = in ? h[g] : 0.0f;
+            uv[r] = in ? u[g] : 0.0f;
+            vv[r] = in ? v[g] : 0.0f;
+        }
+        float m = 0.0f;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (apply_cut && hv[r] < eps) continue;
+            const float s2 = uv[r] * uv[r] + vv[r] * vv[r];
+            if (s2 > m) m = s2;
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (lane == 0 && m > 0.0f) atomicMax(&bits[l], __float_as_uint(m));
+    }
+}
+
+cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], const float* const u[2],
+                               const float* const v[2], int res, float eps, int apply_cut, unsigned int* bits,
+                               cudaStream_t st) {
+    k_tile_speed2<<<148 * 8, 256, 0, st>>>(tf, h[0], u[0], v[0], h[1], u[1], v[1], res, eps, apply_cut, bits);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
@@ -487,6 +634,7 @@ cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t
     (void)res;
     (void)layers;
     k_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(L);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 
@@ -499,6 +647,7 @@ cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cuda
     (void)res;
     (void)layers;
     k_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 
@@ -506,6 +655,7 @@ cudaError_t launch_apply_cut(const float* h, float* u, float* v, size_t n, float
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_apply_cut<<<blocks, 256, 0, st>>>(h, u, v, n, eps);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 
@@ -514,6 +664,7 @@ cudaError_t launch_max_speed2(const float* h, const float* u, const float* v, si
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
     k_max_speed2<<<blocks, 256, 0, st>>>(h, u, v, n, eps, apply_cut, out_bits);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 

@@ -47,9 +47,25 @@ struct TileFlags {
     int32_t tiles_x;
 };
 
+// Substep count decided on the device (src/fluid_core.rs:1715-1744). The
+// largest squared speed of each layer, reduced over the tiles that may hold
+// water, gives the layer's count n = clamp(ceil(dt max(0.15, s) / (0.42 cell)),
+// 1, cap); the tile-list, force and transport kernels of substep k read it and
+// step with dt / n while k < n. The host launches `launched` substeps from its
+// own speed bound; a layer that needs fewer copies its tiles through the rest
+// (identity substeps), and one that needs more sets `overflow`.
+struct SubstepCount {
+    const unsigned int* speed2;  // [2] float bits; nullptr = the host's count (LayerParams.dt, skip)
+    unsigned int* overflow;
+    float dt, cell, cap;
+    int32_t k, launched;
+    float water_decay[9];        // [n]: damping factor of the water layer over dt / n
+};
+
 struct ForceLaunch {
     LayerParams lay[2];
     TileFlags tf;
+    SubstepCount sc;
     int32_t nxt;             // buffer being written
 };
 
@@ -69,6 +85,7 @@ struct TransportParams {
 struct TransportLaunch {
     TransportParams lay[2];
     TileFlags tf;
+    SubstepCount sc;
     int32_t nxt;
 };
 
@@ -77,7 +94,14 @@ constexpr int GRID_TILE = 32;
 size_t force_smem_bytes();
 // Builds the tile list of one substep: active tiles of both layers, then the
 // quiet tiles whose output buffer is not yet zero. `all` marks every tile active.
-cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1, cudaStream_t st);
+cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1,
+                             const SubstepCount& sc, cudaStream_t st);
+// Largest squared speed of each layer over the stepped tiles of the current
+// tile list, which must be substep 0's (cells below eps skipped when
+// apply_cut): atomicMax into bits[0..1], which start at zero.
+cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], const float* const u[2],
+                               const float* const v[2], int res, float eps, int apply_cut, unsigned int* bits,
+                               cudaStream_t st);
 size_t transport_smem_bytes();
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st);
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st);

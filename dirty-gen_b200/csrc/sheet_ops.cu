@@ -6,6 +6,7 @@
 
 #include "sheet_math.cuh"
 #include "sheet_ops.cuh"
+#include "launch_count.cuh"
 
 namespace silt {
 
@@ -170,27 +171,32 @@ __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsig
 cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
                              uint8_t* grain, size_t n, cudaStream_t st) {
     k_map_water_bed<<<blocks_for(n), 256, 0, st>>>(bed_in, water_in, bed, water, moisture, grain, n);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
                                   size_t n, cudaStream_t st) {
     k_map_water_velocity<<<blocks_for(n), 256, 0, st>>>(u_in, v_in, water, uw, vw, n);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
                      float x0, float x1, float z0, float z1, float depth, int water, int g, float m, cudaStream_t st) {
     k_paint<<<blocks_for((size_t)res * res), 256, 0, st>>>(depth_plane, moisture, grain, res, cell, ox, oz, x0, x1, z0,
                                                            z1, depth, water, g, m);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
                           cudaStream_t st) {
     k_lay_slurry<<<blocks_for(n), 256, 0, st>>>(depth, slurry, moisture, grain, n, g, m);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
                               float* moisture, uint8_t* grain, const float* slurry, size_t n, cudaStream_t st) {
     k_read_substrate<<<blocks_for(n), 256, 0, st>>>(bed_in, moist_in, grain_in, bed, moisture, grain, slurry, n);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
@@ -198,11 +204,13 @@ cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int r
     if (i1 <= i0) return cudaSuccess;
     k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, uw, vw, cut_pending, res, j, i0, i1, add, tiles_x, t_wet,
                                                      t_zuv, t_zh);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
                        const float* vs, float* film, float* flow, size_t n, cudaStream_t st) {
     k_publish<<<blocks_for(n), 256, 0, st>>>(water, slurry, uw, vw, us, vs, film, flow, n);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
@@ -210,18 +218,21 @@ cudaError_t op_export(const float* bed, const float* water, const float* slurry,
                       float* moisture, size_t n, cudaStream_t st) {
     k_export<<<blocks_for(n), 256, 0, st>>>(bed, water, slurry, uw, vw, us, vs, moist, height, vel_u, vel_v, moisture,
                                            n);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
     if (e != cudaSuccess) return e;
     k_sum2<<<blocks_for(n), 256, 0, st>>>(a, b, n, out);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
     k_non_finite<<<blocks_for(n), 256, 0, st>>>(planes, np, n, out);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 

@@ -9,6 +9,7 @@
 // sheet subset: inflow, refine (restrict, lay the patches, near field), tire
 // shove on the patches, fine pair, fine spray, restrict, shove outside the
 // patches, coarse pair, coarse spray.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "../../include/silt_sheet.h"
 #include "sheet_fine.cuh"
+#include "launch_count.cuh"
 #include "sheet_grid.cuh"
 #include "sheet_host_math.h"
 #include "sheet_ops.cuh"
@@ -73,9 +75,10 @@ struct silt_sheet {
     float* staging2 = nullptr;
     uint8_t* staging_u8 = nullptr;
     double* d_acc = nullptr;      // [0..1] step ledger sums, [2..3] reductions, [4..7] spare
-    unsigned int* d_u32 = nullptr;
+    unsigned int* d_u32 = nullptr;   // [0..1] speed bits, [2] substep overflow, [3] non-finite count, [4..7] tile counters
     const float** d_planes = nullptr;
     double* h_acc = nullptr;      // pinned mirror of d_acc
+    unsigned int* h_flags = nullptr;  // pinned: [0] the device's substep-overflow flag
     bool cut_pending = false;
     bool ledger_fresh = false;    // h_acc[0..1] hold the current depth sums
     float vmax_bound = 0.0f;      // bound on any cell's speed |(u, v)|, for the one-substep shortcut
@@ -146,36 +149,42 @@ int step_coarse_pair(silt_sheet* s, float dt) {
     const float cell = s->cfg.cell;
     const float eps = 1.0e-6f;
     // Substep count (src/fluid_core.rs:1715-1744). With every speed under the
-    // bound one substep is certain; otherwise measure the largest speed.
-    int nsub[2] = {1, 1};
+    // host's bound one substep is certain. Otherwise the device measures each
+    // layer's largest speed and decides its count; the host launches as many
+    // substeps as the bound allows, without waiting for the answer.
     const float cap = 8.0f;
-    float bound = s->vmax_bound;
-    if (!(dt * std::max(0.15f, bound) <= 0.42f * std::max(cell, 1.0e-3f))) {
-        for (int l = 0; l < 2; ++l) {
-            CK(cudaMemsetAsync(s->d_u32, 0, sizeof(unsigned int), s->st));
-            CK(silt::launch_max_speed2(s->H(l), s->U(l), s->V(l), s->n, eps, s->cut_pending ? 1 : 0, s->d_u32, s->st));
-            unsigned int bits = 0;
-            CK(cudaMemcpyAsync(&bits, s->d_u32, sizeof bits, cudaMemcpyDeviceToHost, s->st));
-            CK(cudaStreamSynchronize(s->st));
-            float m2;
-            memcpy(&m2, &bits, 4);
-            float max_s = std::max(0.15f, sqrtf(m2));
-            float ns = ceilf((dt * max_s) / (0.42f * std::max(cell, 1.0e-3f)));
-            nsub[l] = (int)silt::host::rclamp(ns, 1.0f, cap);
-        }
+    const float bound = s->vmax_bound;
+    const float courant_len = 0.42f * std::max(cell, 1.0e-3f);
+    int launched = 1;
+    silt::SubstepCount sc;
+    memset(&sc, 0, sizeof sc);
+    sc.dt = dt;
+    sc.cell = cell;
+    sc.cap = cap;
+    const float nu_w = water_nu();
+    for (int q = 1; q <= 8; ++q) sc.water_decay[q] = expf(-silt::host::sheet_damp(nu_w) * (dt / (float)q));
+    sc.water_decay[0] = sc.water_decay[1];
+    if (!(dt * std::max(0.15f, bound) <= courant_len)) {
+        const float nb = ceilf((dt * std::max(0.15f, bound)) / courant_len);
+        launched = std::isfinite(nb) ? (int)silt::host::rclamp(nb, 1.0f, cap) : (int)cap;
+        sc.speed2 = s->d_u32;
+        sc.overflow = s->d_u32 + 2;
+        sc.launched = launched;
+        s->parts.device_counts += 1;
     }
     const int soften_edge = s->cfg.soften_border ? std::max(res / 12, 2) : 0;
-    const int steps = std::max(nsub[0], nsub[1]);
-    const float nu_w = water_nu();
-    for (int k = 0; k < steps; ++k) {
+    for (int k = 0; k < launched; ++k) {
         silt::ForceLaunch F;
         silt::TransportLaunch T;
         memset(&F, 0, sizeof F);
         memset(&T, 0, sizeof T);
         const int nxt = s->cur ^ 1;
+        sc.k = k;
+        F.sc = sc;
+        T.sc = sc;
         for (int l = 0; l < 2; ++l) {
             silt::LayerParams& P = F.lay[l];
-            const float dts = dt / (float)nsub[l];
+            const float dts = dt;  // the device divides by its count when it decides one
             P.h = s->h[l][s->cur];
             P.bed = s->bed;
             P.u = s->u[l][s->cur];
@@ -190,12 +199,12 @@ int step_coarse_pair(silt_sheet* s, float dt) {
             P.project = cell > silt::host::kFineCell + 1.0e-6f;
             P.soften_edge = k == 0 ? soften_edge : 0;
             P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
-            P.skip = k >= nsub[l];
+            P.skip = 0;
             if (l == 0) {
                 P.nu_mode = silt::NU_CONST;
                 P.nu_c = nu_w;
                 P.mob_c = silt::host::sheet_mobility_for(nu_w);
-                P.decay_c = expf(-silt::host::sheet_damp(nu_w) * dts);
+                P.decay_c = sc.water_decay[1];
             } else {
                 P.nu_mode = silt::NU_GRAIN;
                 P.grain = s->grain;
@@ -219,13 +228,19 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         F.nxt = nxt;
         T.tf = s->tf;
         T.nxt = nxt;
-        // A skipped layer keeps its planes (copied across the buffer swap) and its ledger sum.
-        for (int l = 0; l < 2; ++l)
-            if (!F.lay[l].skip) CK(cudaMemsetAsync(s->d_acc + l, 0, sizeof(double), s->st));
+        CK(cudaMemsetAsync(s->d_acc, 0, 2 * sizeof(double), s->st));
         // A substep that does not start from a dry cut (the first after an
         // outside write) steps every tile: its dry cells may carry velocity.
         const int all = (s->tiles_all || !(k > 0 || s->cut_pending)) ? 1 : 0;
-        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, F.lay[0].skip, F.lay[1].skip, s->st));
+        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, 0, 0, sc, s->st));
+        if (k == 0 && sc.speed2) {
+            // The substep count, from the tiles substep 0 steps.
+            CK(cudaMemsetAsync(s->d_u32, 0, 2 * sizeof(unsigned int), s->st));
+            const float* hh[2] = {s->H(0), s->H(1)};
+            const float* uu[2] = {s->U(0), s->U(1)};
+            const float* vv[2] = {s->V(0), s->V(1)};
+            CK(silt::launch_tile_speed2(s->tf, hh, uu, vv, res, eps, s->cut_pending ? 1 : 0, s->d_u32, s->st));
+        }
         s->tiles_all = false;
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
         if (s->timing) {
@@ -245,20 +260,7 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         if (s->timing) CK(cudaEventRecord(ev[1], s->st));
         CK(silt::launch_transport(T, res, 2, s->st));
         if (s->timing) CK(cudaEventRecord(ev[2], s->st));
-        s->parts.launches += 3;
         s->parts.force_launches += 1;
-        for (int l = 0; l < 2; ++l)
-            if (F.lay[l].skip) {
-                CK(cudaMemcpyAsync(s->h[l][nxt], s->h[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
-                CK(cudaMemcpyAsync(s->u[l][nxt], s->u[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
-                CK(cudaMemcpyAsync(s->v[l][nxt], s->v[l][s->cur], s->n * 4, cudaMemcpyDeviceToDevice, s->st));
-                const size_t nt = (size_t)s->tf.tiles_x * s->tf.tiles_x;
-                CK(cudaMemcpyAsync(s->tf.wet[l][nxt], s->tf.wet[l][s->cur], nt, cudaMemcpyDeviceToDevice, s->st));
-                CK(cudaMemcpyAsync(s->tf.zero_uv[l][nxt], s->tf.zero_uv[l][s->cur], nt, cudaMemcpyDeviceToDevice,
-                                   s->st));
-                CK(cudaMemcpyAsync(s->tf.zero_h[l][nxt], s->tf.zero_h[l][s->cur], nt, cudaMemcpyDeviceToDevice,
-                                   s->st));
-            }
         s->cur = nxt;
         s->cut_pending = true;
     }
@@ -305,28 +307,27 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
     }
     CK(cudaMemcpyAsync(s->d_win_jobs + 2 * slot, jobs, 2 * sizeof(silt::window::Job), cudaMemcpyHostToDevice, s->st));
     CK(cudaEventRecord(s->win_ev[slot], s->st));
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     if (s->timing) {
-        for (cudaEvent_t* e : {&ev0, &ev1}) {
+        for (int q = 0; q < 3; ++q) {
             if (s->ev_pool.empty()) {
                 cudaEvent_t x;
                 CK(cudaEventCreate(&x));
                 s->ev_pool.push_back(x);
             }
-            *e = s->ev_pool.back();
+            ev[q] = s->ev_pool.back();
             s->ev_pool.pop_back();
+            s->ev_used.push_back(ev[q]);
         }
-        CK(cudaEventRecord(ev0, s->st));
+        CK(cudaEventRecord(ev[0], s->st));
     }
-    CK(silt::window::launch_window_step(s->d_win_jobs + 2 * slot, 2, s->st));
+    CK(silt::window::launch_window_step(s->d_win_jobs + 2 * slot, 2, s->res, s->st));
     if (s->timing) {
-        CK(cudaEventRecord(ev1, s->st));
-        // Force time only; the transport runs inside the same kernel.
-        s->ev_used.push_back(ev0);
-        s->ev_used.push_back(ev1);
-        s->ev_used.push_back(ev1);
+        // Force time only: the transport runs inside the same kernel, so the
+        // third event closes an empty transport interval.
+        CK(cudaEventRecord(ev[1], s->st));
+        CK(cudaEventRecord(ev[2], s->st));
     }
-    s->parts.launches += 1;
     s->parts.force_launches += 1;
     s->parts.force_cells += 2 * (int64_t)s->n;
     s->parts.force_cells_water += (int64_t)s->n;
@@ -335,6 +336,10 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
 }
 
 }  // namespace
+
+namespace silt {
+thread_local unsigned long long t_kernel_launches = 0;
+}
 
 extern "C" {
 
@@ -398,9 +403,12 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_acc, 8 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 8 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 16 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_flags, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_u32, 0, 16 * sizeof(unsigned int));
+    if (e == cudaSuccess) memset(s->h_flags, 0, 4 * sizeof(unsigned int));
     s->engine = cfg->engine == SILT_ENGINE_WINDOW || cfg->engine == SILT_ENGINE_GRID
                     ? cfg->engine
                     : (cfg->res <= silt::window::MAX_RES ? SILT_ENGINE_WINDOW : SILT_ENGINE_GRID);
@@ -484,6 +492,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->staging2);
     cudaFree(s->staging_u8);
     cudaFree(s->d_acc);
+    cudaFreeHost(s->h_flags);
     cudaFree(s->d_u32);
     cudaFree(s->d_planes);
     if (s->h_acc) cudaFreeHost(s->h_acc);
@@ -500,10 +509,20 @@ int silt_sheet_destroy(silt_sheet* s) {
     return SILT_OK;
 }
 
+// After a wait on the stream: a step whose layer needed more substeps than
+// the host's speed bound launched leaves the state off the reference's path.
+static int check_substep_overflow(silt_sheet* s) {
+    if (!s->h_flags[0]) return SILT_OK;
+    snprintf(g_err, sizeof g_err, "%s",
+             "a step needed more substeps than its speed bound launched; the state is no longer the reference's");
+    return SILT_EBOUND;
+}
+
 int silt_sheet_sync(silt_sheet* s) {
     if (!s) return fail_arg("handle");
+    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    return SILT_OK;
+    return check_substep_overflow(s);
 }
 
 // Host-side volume of what a seeding call writes, summed in f32 cell order like the reference.
@@ -677,6 +696,9 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         s->pushes.clear();
         return SILT_OK_NOOP;
     }
+    const unsigned long long launches0 = silt::t_kernel_launches;
+    using clock = std::chrono::steady_clock;
+    const clock::time_point t0 = clock::now();
     std::vector<silt_tire_push> ps;
     ps.swap(s->pushes);
     int rc;
@@ -689,8 +711,10 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
     }
     silt::fine::StepOut fo;
+    const clock::time_point t1 = clock::now();
     rc = silt::fine::step_patches(s->fine, s, ps, dt, fo);
     if (rc) return rc;
+    const clock::time_point t2 = clock::now();
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
     if (rc) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
@@ -702,6 +726,12 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     }
     if (n_out) *n_out = nev;
     s->parts.steps += 1;
+    s->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
+    if (s->timing) {
+        const clock::time_point t3 = clock::now();
+        s->parts.host_step_ms += std::chrono::duration<double, std::milli>(t3 - t0).count();
+        s->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+    }
     s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
     return SILT_OK;
 }
@@ -718,7 +748,9 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     double spray = 0.0, park_w = 0.0, park_s = 0.0;
     int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s);
     if (rc) return rc;
+    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    if ((rc = check_substep_overflow(s))) return rc;
     const double area = (double)s->cfg.cell * (double)s->cfg.cell;
     w = s->h_acc[0] * area;
     sl = s->h_acc[1] * area;
@@ -814,9 +846,9 @@ int silt_non_finite_count(silt_sheet* s, uint32_t* out) {
     if (!s || !out) return fail_arg("non_finite_count");
     const float* planes[8] = {s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), s->bed, s->moisture};
     CK(cudaMemcpyAsync(s->d_planes, planes, sizeof planes, cudaMemcpyHostToDevice, s->st));
-    CK(silt::op_non_finite(s->d_planes, 8, s->n, s->d_u32 + 1, s->st));
+    CK(silt::op_non_finite(s->d_planes, 8, s->n, s->d_u32 + 3, s->st));
     unsigned int c = 0;
-    CK(cudaMemcpyAsync(&c, s->d_u32 + 1, 4, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&c, s->d_u32 + 3, 4, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     *out = c;
     return SILT_OK;
@@ -984,7 +1016,7 @@ static int step_sheet_window(float* h, float* u, float* v, const float* bed, con
     silt::window::Job* d_job = reinterpret_cast<silt::window::Job*>(scratch);
     // From the stack: the copy is staged before this call returns.
     CK(cudaMemcpyAsync(d_job, &J, sizeof J, cudaMemcpyHostToDevice, st));
-    CK(silt::window::launch_window_step(d_job, 1, st));
+    CK(silt::window::launch_window_step(d_job, 1, res, st));
     return SILT_OK;
 }
 
@@ -1075,7 +1107,9 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         T.tf = tf;
         F.nxt = 1;
         T.nxt = 1;
-        CK(silt::launch_tile_list(tf, 0, 1, 1, 0, 1, st));
+        silt::SubstepCount host_count;
+        memset(&host_count, 0, sizeof host_count);
+        CK(silt::launch_tile_list(tf, 0, 1, 1, 0, 1, host_count, st));
         CK(silt::launch_force(F, res, 1, st));
         CK(silt::launch_transport(T, res, 1, st));
         CK(cudaMemcpyAsync(h, h_next, n * 4, cudaMemcpyDeviceToDevice, st));

@@ -23,6 +23,7 @@
 
 #include "sheet_math.cuh"
 #include "sheet_window.cuh"
+#include "launch_count.cuh"
 
 namespace silt {
 namespace window {
@@ -52,20 +53,17 @@ struct Shared {
     int red_i[4][NT / 32];
 };
 
+// Every cell of the inclusive rectangle, one warp per row and the lanes along
+// x (no division per cell). Bodies may `continue` to the next cell.
 #define CTA_RECT(I0, I1, J0, J1, ...)                                               \
     {                                                                               \
-        const int ri0_ = (I0), rj0_ = (J0);                                         \
-        const int rw_ = (I1) - ri0_ + 1, rh_ = (J1) - rj0_ + 1;                    \
-        if (rw_ > 0 && rh_ > 0) {                                                   \
-            const int rn_ = rw_ * rh_;                                              \
-            for (int k_ = threadIdx.x; k_ < rn_; k_ += NT) {                        \
-                const int j = rj0_ + k_ / rw_;                                      \
-                const int i = ri0_ + k_ % rw_;                                      \
+        const int ri0_ = (I0), ri1_ = (I1), rj1_ = (J1);                            \
+        for (int j = (J0) + (int)(threadIdx.x >> 5); j <= rj1_; j += NT / 32)       \
+            for (int i = ri0_ + (int)(threadIdx.x & 31); i <= ri1_; i += 32) {      \
                 const int g = j * res + i;                                          \
                 (void)g;                                                            \
                 __VA_ARGS__                                                         \
             }                                                                       \
-        }                                                                           \
     }
 
 __device__ __forceinline__ double block_sum_d(Shared& S, double v) {
@@ -146,8 +144,8 @@ __device__ __forceinline__ float tap5c(const float* line, int res, int i, float 
 
 // blur_box (src/fluid_core.rs:3541-3569): x pass of the box rows into tmp,
 // then the z pass into dst, which reads tmp rows outside the box as they are.
-__device__ void cta_blur(const float* src, float* dst, float* tmp, int res, const Box& b, float k0, float k1,
-                         float k2) {
+__device__ void cta_blur(const float* __restrict__ src, float* __restrict__ dst, float* __restrict__ tmp, int res,
+                         const Box& b, float k0, float k1, float k2) {
     CTA_RECT(b.i0, b.i1, b.j0, b.j1, { tmp[g] = tap5c(src + j * res, res, i, k0, k1, k2, 1); })
     __syncthreads();
     CTA_RECT(b.i0, b.i1, b.j0, b.j1, { dst[g] = tap5c(tmp + i, res, j, k0, k1, k2, res); })
@@ -156,26 +154,44 @@ __device__ void cta_blur(const float* src, float* dst, float* tmp, int res, cons
 
 __device__ __forceinline__ float job_nu(const Job& J, int g) {
     if (J.nu_mode == NU_CONST) return J.nu_c;
-    if (J.nu_mode == NU_PLANE) return J.nu_plane[g];
+    if (J.nu_mode == NU_PLANE || J.nu_mode == NU_TABLE) return J.nu_plane[g];
     return dynamic_viscosity(J.grain[g], J.moisture[g]);
+}
+
+// sheet_mobility_for(nu) of the cell.
+__device__ __forceinline__ float job_mob(const Job& J, int g) {
+    if (J.nu_mode == NU_CONST) return J.mob_c;
+    if (J.nu_mode == NU_TABLE) return J.mob_plane[g];
+    return sheet_mobility_for(job_nu(J, g));
+}
+
+// The cell's damping factor over dt: exp(-sheet_damp(nu) dt).
+__device__ __forceinline__ float job_decay(const Job& J, int g, float dt, float decay_c) {
+    if (J.nu_mode == NU_CONST) return decay_c;
+    const float rate = J.nu_mode == NU_TABLE ? J.damp_plane[g] : sheet_damp(job_nu(J, g));
+    return expf(-rate * dt);
 }
 
 // transport_open_rows (src/fluid_core.rs:3025-3137) on one box (banks off).
 __device__ void cta_transport(const Job& J, const Box& b, float dt) {
+    // The planes are distinct and each phase writes only its own cell, so
+    // the loads of one cell may run ahead of the stores of the previous.
     const int res = J.res;
-    float* h = J.h;
-    float* F1 = J.f1;
-    float* F2 = J.f2;
+    float* __restrict__ h = J.h;
+    const float* __restrict__ U = J.u;
+    const float* __restrict__ V = J.v;
+    float* __restrict__ F1 = J.f1;
+    float* __restrict__ F2 = J.f2;
     const float cell = J.cell;
-    const uint8_t* gate = J.gate;
+    const uint8_t* __restrict__ gate = J.gate;
     CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
-        float speed = 0.5f * (J.u[g] + J.u[g + 1]);
+        float speed = 0.5f * (U[g] + U[g + 1]);
         float dh = open_edge_dh(false, h[g + 1], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
     __syncthreads();
     CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
-        float speed = 0.5f * (J.u[g] + J.u[g + 1]);
+        float speed = 0.5f * (U[g] + U[g + 1]);
         float prev = i > b.i0 ? F1[g - 1] : 0.0f;
         float dh = open_edge_dh(false, h[g], h[g + 1], 0.0f + prev, gate ? gate[g + 1] : 1, 0.0f, 0.0f, speed, dt,
                                 cell, 0.45f);
@@ -192,13 +208,13 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     })
     __syncthreads();
     CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
-        float speed = 0.5f * (J.v[g] + J.v[g + res]);
+        float speed = 0.5f * (V[g] + V[g + res]);
         float dh = open_edge_dh(false, h[g + res], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
     __syncthreads();
     CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
-        float speed = 0.5f * (J.v[g] + J.v[g + res]);
+        float speed = 0.5f * (V[g] + V[g + res]);
         float ra = j > b.j0 ? 0.0f + F1[g - res] : 0.0f;
         float dh = open_edge_dh(false, h[g], h[g + res], ra, gate ? gate[g + res] : 1, 0.0f, 0.0f, speed, dt, cell,
                                 0.45f);
@@ -218,12 +234,16 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
 
 __device__ void cta_dry_cut(const Job& J, const Box& b) {
     const int res = J.res;
-    if (!(J.eps > 0.0f)) return;
+    const float eps = J.eps;
+    if (!(eps > 0.0f)) return;
+    float* __restrict__ h = J.h;
+    float* __restrict__ u = J.u;
+    float* __restrict__ v = J.v;
     CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
-        if (J.h[g] < J.eps) {
-            J.h[g] = 0.0f;
-            J.u[g] = 0.0f;
-            J.v[g] = 0.0f;
+        if (h[g] < eps) {
+            h[g] = 0.0f;
+            u[g] = 0.0f;
+            v[g] = 0.0f;
         }
     })
     __syncthreads();
@@ -277,7 +297,7 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float px = (p[j * res + ip] - p[j * res + im]) / two;
             float pz = (p[jp * res + i] - p[jm * res + i]) / two;
-            float mob = J.nu_mode == NU_CONST ? J.mob_c : sheet_mobility_for(job_nu(J, g));
+            float mob = job_mob(J, g);
             float ug = J.u[g] + -kGravity * px * mob * dt;
             float vg = J.v[g] + -kGravity * pz * mob * dt;
             UG[g] = ug;
@@ -351,35 +371,40 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
 
 // Gravity then snapshot-Jacobi confinement (force_gravity_par :2263-2378,
 // gravity_jacobi_serial :2530-2595).
-__device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* p, float dt) {
+__device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __restrict__ p, float dt) {
+    // Distinct planes; each phase writes only its own cell of u, v or W.
     const int res = J.res;
     const float eps = J.eps, two = 2.0f * J.cell;
+    const float* __restrict__ H = J.h;
+    float* __restrict__ U = J.u;
+    float* __restrict__ V = J.v;
     CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
-        if (J.h[g] > eps) {
+        if (H[g] > eps) {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float px = (p[j * res + ip] - p[j * res + im]) / two;
             float pz = (p[jp * res + i] - p[jm * res + i]) / two;
-            float mob = J.nu_mode == NU_CONST ? J.mob_c : sheet_mobility_for(job_nu(J, g));
-            J.u[g] += -kGravity * px * mob * dt;
-            J.v[g] += -kGravity * pz * mob * dt;
+            float mob = job_mob(J, g);
+            U[g] += -kGravity * px * mob * dt;
+            V[g] += -kGravity * pz * mob * dt;
         }
     })
     __syncthreads();
     if (!(J.vort > 0.0f)) return;
-    float* W = J.f1;
+    float* __restrict__ W = J.f1;
     {
         const int wi0 = max(b.i0 - 1, 0), wi1 = min(b.i1 + 1, res - 1);
         const int wj0 = max(b.j0 - 1, 0), wj1 = min(b.j1 + 1, res - 1);
         CTA_RECT(wi0, wi1, wj0, wj1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float dvdx = (J.v[j * res + ip] - J.v[j * res + im]) / two;
-            float dudz = (J.u[jp * res + i] - J.u[jm * res + i]) / two;
+            float dvdx = (V[j * res + ip] - V[j * res + im]) / two;
+            float dudz = (U[jp * res + i] - U[jm * res + i]) / two;
             W[g] = dvdx - dudz;
         })
     }
     __syncthreads();
+    const float vort = J.vort;
     CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
-        if (J.h[g] > eps) {
+        if (H[g] > eps) {
             float w = W[g];
             if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
                 const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
@@ -387,11 +412,11 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* p, f
                 float wzp = fabsf(W[jp * res + i]), wzm = fabsf(W[jm * res + i]);
                 float nx = (wxp - wxm) / two;
                 float nz = (wzp - wzm) / two;
-                float du = J.vort * dt * (-nz * w);
-                float dv = J.vort * dt * (nx * w);
+                float du = vort * dt * (-nz * w);
+                float dv = vort * dt * (nx * w);
                 if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
-                    J.u[g] += du;
-                    J.v[g] += dv;
+                    U[g] += du;
+                    V[g] += dv;
                 }
             }
         }
@@ -403,17 +428,19 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* p, f
 __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* sc, float dt, float decay_c,
                            bool do_flux, bool inner_par) {
     const int res = J.res;
-    float* sa = sc[0];
-    float* sb = sc[1];
-    float* scc = sc[2];
-    float* sd = sc[3];
-    float* se = sc[4];
+    float* __restrict__ sa = sc[0];
+    float* __restrict__ sb = sc[1];
+    float* __restrict__ scc = sc[2];
+    float* __restrict__ sd = sc[3];
+    float* __restrict__ se = sc[4];
     const float eps = J.eps, cell = J.cell;
     const bool fine = cell <= kFineCell + 1.0e-6f;
     {
+        const float* __restrict__ bed = J.bed;
+        const float* __restrict__ H = J.h;
         const int hi0 = max(b.i0 - 2, 0), hi1 = min(b.i1 + 2, res - 1);
         const int hj0 = max(b.j0 - 2, 0), hj1 = min(b.j1 + 2, res - 1);
-        CTA_RECT(hi0, hi1, hj0, hj1, { sa[g] = J.bed[g] + J.h[g]; })
+        CTA_RECT(hi0, hi1, hj0, hj1, { sa[g] = bed[g] + H[g]; })
     }
     __syncthreads();
     cta_blur(sa, sb, se, res, b, kG0, kG1, kG2);
@@ -447,20 +474,27 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
         CTA_RECT(b.i0, b.i1, b.j0, b.j1, { sd[g] = 0.62f * scc[g] + 0.38f * sa[g]; })
         __syncthreads();
     }
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
-        if (J.h[g] > eps) {
-            if (project) {
-                const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-                float qx = (sd[j * res + ip] - sd[j * res + im]) / (2.0f * cell);
-                float qz = (sd[jp * res + i] - sd[jm * res + i]) / (2.0f * cell);
-                J.u[g] += 0.012f * dt * qx;
-                J.v[g] += 0.012f * dt * qz;
+    {
+        const float* __restrict__ H = J.h;
+        float* __restrict__ U = J.u;
+        float* __restrict__ V = J.v;
+        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+            if (H[g] > eps) {
+                float uu = U[g], vv = V[g];
+                if (project) {
+                    const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1),
+                              jm = max(j - 1, 0);
+                    float qx = (sd[j * res + ip] - sd[j * res + im]) / (2.0f * cell);
+                    float qz = (sd[jp * res + i] - sd[jm * res + i]) / (2.0f * cell);
+                    uu += 0.012f * dt * qx;
+                    vv += 0.012f * dt * qz;
+                }
+                float decay = job_decay(J, g, dt, decay_c);
+                U[g] = finite_speed(uu * decay, kSpeedCap);
+                V[g] = finite_speed(vv * decay, kSpeedCap);
             }
-            float decay = J.nu_mode == NU_CONST ? decay_c : expf(-sheet_damp(job_nu(J, g)) * dt);
-            J.u[g] = finite_speed(J.u[g] * decay, kSpeedCap);
-            J.v[g] = finite_speed(J.v[g] * decay, kSpeedCap);
-        }
-    })
+        })
+    }
     __syncthreads();
     if (do_flux) {
         cta_transport(J, b, dt);
@@ -786,11 +820,9 @@ __device__ void cta_ledger(Shared& S, const Job& J) {
 }
 
 // step_sheet_eps_in + step_sheet_scratch (src/fluid_core.rs:821-852, :1659-1831).
-__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
-    const Job J = jobs[blockIdx.x];
-    if (!J.active) return;
+// One window layer's step; returns the Gauss-Seidel passes of its last box.
+__device__ int window_body(Shared& S, const Job& J) {
     int gs_passes = 0;
-    __shared__ Shared S;
     const int res = J.res;
     const float eps = J.eps;
     if (J.soften_edge > 0) cta_soften(J);
@@ -803,7 +835,7 @@ __global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
     ws = block_sum_d(S, ws);
     if (!(ws > (double)eps)) {
         cta_ledger(S, J);
-        return;
+        return 0;
     }
     const bool open_fine = J.cell <= kFineCell + 1.0e-6f;
     const bool fine_open = open_fine && J.pace == 0;
@@ -816,7 +848,7 @@ __global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
     const int nb = S.nbox;
     if (nb <= 0) {
         cta_ledger(S, J);
-        return;
+        return 0;
     }
     const float cap = finite_f(J.sub_cap) ? rclamp(J.sub_cap, 1.0f, 8.0f) : 8.0f;
     int nsub = 1;
@@ -861,12 +893,59 @@ __global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
             }
     }
     cta_ledger(S, J);
+    return gs_passes;
+}
+
+// Planes a small window keeps in shared memory: h, u, v, the first scratch
+// set (a..e) and the two transient planes.
+constexpr int SMEM_PLANES = 10;
+constexpr int SMEM_CARRIED = 8;  // h, u, v and the scratch set come in and go back out
+
+__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs, int smem_cells) {
+    extern __shared__ float wsm[];
+    __shared__ Shared S;
+    Job J = jobs[blockIdx.x];
+    if (!J.active) return;
+    const int n = J.res * J.res;
+    // A window that fits runs on shared-memory copies of its planes: every
+    // phase of the step then waits on shared memory instead of L2. The
+    // scratch set keeps its values between steps, so it travels both ways.
+    const bool local = n <= smem_cells;
+    float* carried[SMEM_CARRIED] = {J.h, J.u, J.v, J.sc[0][0], J.sc[0][1], J.sc[0][2], J.sc[0][3], J.sc[0][4]};
+    if (local) {
+#pragma unroll
+        for (int q = 0; q < SMEM_CARRIED; ++q)
+            for (int c = threadIdx.x; c < n; c += NT) wsm[(size_t)q * n + c] = carried[q][c];
+        J.h = wsm;
+        J.u = wsm + n;
+        J.v = wsm + 2 * (size_t)n;
+        for (int a = 0; a < 5; ++a) J.sc[0][a] = wsm + (size_t)(3 + a) * n;
+        J.f1 = wsm + 8 * (size_t)n;
+        J.f2 = wsm + 9 * (size_t)n;
+        __syncthreads();
+    }
+    const int gs_passes = window_body(S, J);
+    if (local) {
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < SMEM_CARRIED; ++q)
+            for (int c = threadIdx.x; c < n; c += NT) carried[q][c] = wsm[(size_t)q * n + c];
+    }
     if (threadIdx.x == 0) jobs[blockIdx.x].gs_iters = gs_passes;
 }
 
-cudaError_t launch_window_step(const Job* d_jobs, int njobs, cudaStream_t st) {
+cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st) {
     if (njobs <= 0) return cudaSuccess;
-    k_window_step<<<njobs, NT, 0, st>>>(const_cast<Job*>(d_jobs));
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_window_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(sizeof(float) * SMEM_PLANES * SMEM_RES * SMEM_RES));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int cells = max_res <= SMEM_RES ? max_res * max_res : 0;
+    k_window_step<<<njobs, NT, sizeof(float) * SMEM_PLANES * (size_t)cells, st>>>(const_cast<Job*>(d_jobs), cells);
+    ::silt::count_launch();
     return cudaGetLastError();
 }
 

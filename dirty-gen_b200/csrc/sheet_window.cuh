@@ -10,7 +10,9 @@ namespace window {
 
 constexpr int MAX_RES = 512;  // largest window side the engine steps (tile and row tables)
 
-enum : int32_t { NU_CONST = 0, NU_PLANE = 1, NU_GRAIN = 2 };
+// NU_TABLE: nu_plane, mob_plane and damp_plane hold each cell's viscosity,
+// mobility and damping rate (the material laws applied once beforehand).
+enum : int32_t { NU_CONST = 0, NU_PLANE = 1, NU_GRAIN = 2, NU_TABLE = 3 };
 
 // One layer of one window: its planes, its persistent scratch, its options.
 struct Job {
@@ -21,6 +23,8 @@ struct Job {
     const uint8_t* grain;
     const float* moisture;
     const float* nu_plane;
+    const float* mob_plane;   // NU_TABLE only
+    const float* damp_plane;  // NU_TABLE only
     const uint8_t* gate;   // nullptr: every receiver open
     float* sc[2][5];       // the reference's two scratch sets (sc, sc2): a, b, c, d, e
     float* f1;             // transient: vorticity, edge fluxes
@@ -40,7 +44,10 @@ struct Job {
     int32_t gs_iters;      // out: Gauss-Seidel passes used by the last box (diagnostics)
 };
 
-cudaError_t launch_window_step(const Job* d_jobs, int njobs, cudaStream_t st);
+// Windows up to SMEM_RES cells per side step on shared-memory copies of
+// their planes. `max_res` is the largest window side among the jobs.
+constexpr int SMEM_RES = 64;
+cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st);
 size_t window_static_smem();
 
 // Planes of scratch one window layer needs beyond its own h, u, v: two

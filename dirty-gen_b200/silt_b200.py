@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsilt_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "silt_sheet.h")
 
-SILT_OK, SILT_OK_NOOP, SILT_EINVAL, SILT_ECUDA, SILT_ETIMEOUT, SILT_ENOMEM = 0, 1, -1, -2, -3, -4
+SILT_OK, SILT_OK_NOOP, SILT_EINVAL, SILT_ECUDA, SILT_ETIMEOUT, SILT_ENOMEM, SILT_EBOUND = 0, 1, -1, -2, -3, -4, -5
 CLAY, SILT, SAND, WATER, OTHER = 0, 1, 2, 3, 4
 FINE_MEAN_PATCH, FINE_PER_TIRE = 0, 1
 ENGINE_AUTO, ENGINE_WINDOW, ENGINE_GRID = 0, 1, 2
@@ -52,7 +52,9 @@ class CoarseCell(ctypes.Structure):
 class StepParts(ctypes.Structure):
     _fields_ = [("force_ms", ctypes.c_double), ("transport_ms", ctypes.c_double), ("fine_ms", ctypes.c_double),
                 ("steps", ctypes.c_int64), ("launches", ctypes.c_int64), ("force_launches", ctypes.c_int64),
-                ("force_cells", ctypes.c_int64), ("force_cells_water", ctypes.c_int64)]
+                ("force_cells", ctypes.c_int64), ("force_cells_water", ctypes.c_int64),
+                ("device_counts", ctypes.c_int64), ("host_step_ms", ctypes.c_double),
+                ("host_fine_ms", ctypes.c_double)]
 
 
 class SiltError(RuntimeError):

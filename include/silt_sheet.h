@@ -11,7 +11,9 @@
  *
  * Errors: the reference returns silently on dt <= 0 and similar no-ops; here
  * those return SILT_OK_NOOP. Bad pointers or sizes return SILT_EINVAL, a CUDA
- * failure SILT_ECUDA, a device wait past its limit SILT_ETIMEOUT.
+ * failure SILT_ECUDA, a device wait past its limit SILT_ETIMEOUT. SILT_EBOUND
+ * (from silt_sheet_sync and silt_get_ledger, and sticky) means a step needed
+ * more substeps than the host's speed bound launched for it.
  */
 #ifndef SILT_SHEET_H
 #define SILT_SHEET_H
@@ -29,6 +31,7 @@ extern "C" {
 #define SILT_ECUDA (-2)
 #define SILT_ETIMEOUT (-3)
 #define SILT_ENOMEM (-4)
+#define SILT_EBOUND (-5)
 
 /* Grain codes, src/fluid_core.rs:116-124 (`Grain`). */
 #define SILT_GRAIN_CLAY 0
@@ -172,6 +175,8 @@ int silt_near_tiles(silt_sheet* s, int32_t* out);
 typedef struct {
     double force_ms, transport_ms, fine_ms;
     int64_t steps, launches, force_launches, force_cells, force_cells_water;
+    int64_t device_counts;  /* steps whose substep count the device decided */
+    double host_step_ms, host_fine_ms;  /* host time inside silt_step, and its nested-patch share */
 } silt_step_parts;
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);

@@ -96,6 +96,39 @@ def test_grid_engine_water_is_bit_exact_on_a_jacobi_sized_box():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (k, float(np.abs(a - b).max()))
 
 
+def test_grid_engine_device_substep_count_is_exact():
+    """A fast start (15 m/s water) needs two substeps, which the grid engine
+    decides on the device without waiting: the host launches three from its
+    speed bound and the water layer copies itself through the third. The slurry
+    pool, slow, takes one substep and copies itself through two. With two
+    substeps the cells the first one wets sit two cells inside the reference's
+    work box, where the box edge reaches their pressure solve, so the grid
+    engine (which has no box edge) differs there by float rounding (~3e-8 m);
+    a wrong substep count would move the pond's rim by ~1e-3 m."""
+    scene = S.window200()
+    ref = O.Core(inner_par=True)
+    dev = G.Sheet(engine=G.ENGINE_GRID)
+    dev.set_step_timing(True)
+    n = scene["water"].size
+    fast_u = np.full(n, 15.0, np.float32)
+    fast_v = np.full(n, -2.0, np.float32)
+    for core in (ref, dev):
+        core.map_water_bed(scene["bed"], np.zeros_like(scene["water"]))
+        core.pour_water(-7.0, 7.0, -7.0, 7.0, 0.06)
+        core.pour_slurry(10.0, 13.0, 10.0, 13.0, 0.03, 0, 0.55)
+        core.read_substrate(scene["bed"], scene["moisture"], scene["grain"])
+        core.map_water_velocity(fast_u, fast_v)
+    for k in range(4):
+        ref.step(DT)
+        dev.step(DT, want_spray=False)
+        assert np.abs(ref.get("water") - dev.get("water")).max() <= 1.0e-6, k
+        assert np.abs(ref.get("slurry") - dev.get("slurry")).max() <= TOL_H, k
+    assert dev.step_parts()["device_counts"] >= 1
+    ld, lr = dev.ledger(), ref.ledger()
+    assert abs(ld["water_m3"] - lr["water64"]) <= 1e-6 * lr["water64"]
+    assert abs(ld["slurry_m3"] - lr["slurry64"]) <= 1e-6 * lr["slurry64"]
+
+
 @pytest.mark.parametrize("res,cell,dt,vort", [(48, 0.06, 0.05, 0.0), (96, 0.2, 0.05, 0.02), (160, 0.1, 0.02, 0.08)])
 def test_free_step_sheet_matches_oracle(res, cell, dt, vort):
     import torch
