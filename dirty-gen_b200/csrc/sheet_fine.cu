@@ -15,7 +15,7 @@
 //   k_peel          spray peeled off the water, events queued on the device
 //   k_near_capture  residual tiles of held columns
 //   k_restrict      volume- and momentum-weighted sum back into the columns
-//   k_park          fine volume outside the window, booked as parked
+//   k_release       fine volume outside the window, booked as parked; fine depths cleared
 //
 // Near-field tiles live in a device pool with a slot per coarse cell; slots
 // are taken in k_near_capture and returned in k_near_fade, so no kernel both
@@ -146,8 +146,10 @@ __global__ void k_scatter_owner(int8_t* owner, const int* idx, const int8_t* val
 }
 
 // refine (src/fluid_core.rs:8358-8460), the per-fine-cell copy.
-__global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W, const int8_t* owner) {
+__global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W, const int8_t* owner,
+                             int* spray_count) {
     const size_t fn = (size_t)fres * fres;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *spray_count = 0;  // this step's spray events start here
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
         const int p = (int)(k / fn);
         const int f = (int)(k % fn);
@@ -620,16 +622,20 @@ __global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const Re
     (void)full;
 }
 
-// Fine cells outside the coarse window: their volume is parked (src/fluid_core.rs:8476-8484).
-__global__ void k_park(const PatchRef* refs, int np, int fres, float fine_area, double* books) {
+// After the restrict: fine cells outside the coarse window have their volume
+// parked (src/fluid_core.rs:8476-8484), and every fine depth is released.
+__global__ void k_release(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park) {
     const size_t fn = (size_t)fres * fres;
     double pw = 0.0, ps = 0.0;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
         const PatchRef& R = refs[k / fn];
         const int f = (int)(k % fn);
-        if (R.col[f % fres] >= 0 && R.row[f / fres] >= 0) continue;
-        pw += (double)R.water[f] * fine_area;
-        ps += (double)R.slurry[f] * fine_area;
+        if (park && !(R.col[f % fres] >= 0 && R.row[f / fres] >= 0)) {
+            pw += (double)R.water[f] * fine_area;
+            ps += (double)R.slurry[f] * fine_area;
+        }
+        R.water[f] = 0.0f;
+        R.slurry[f] = 0.0f;
     }
     for (int o = 16; o > 0; o >>= 1) {
         pw += __shfl_down_sync(0xffffffffu, pw, o);
@@ -1139,7 +1145,8 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner);
+    k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner,
+                                                                                 M.counters + 3);
     ::silt::count_launch();
     FCK(cudaGetLastError());
     if (!L.held.empty()) {
@@ -1185,17 +1192,10 @@ int restrict_all(Patches& P, silt_sheet* s) {
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    if (L.any_park) {
-        k_park<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres,
-                                                                                P.fcell * P.fcell, M.d_books);
-        ::silt::count_launch();
-        FCK(cudaGetLastError());
-    }
-    const size_t fn = (size_t)P.fres * P.fres;
-    for (int p = 0; p < L.np; ++p) {
-        FCK(cudaMemsetAsync(P.patches[p]->water, 0, fn * sizeof(float), W.st));
-        FCK(cudaMemsetAsync(P.patches[p]->slurry, 0, fn * sizeof(float), W.st));
-    }
+    k_release<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, P.fcell * P.fcell,
+                                                                              M.d_books, L.any_park ? 1 : 0);
+    ::silt::count_launch();
+    FCK(cudaGetLastError());
     P.fine_on = false;
     invalidate_ledger(s);
     return SILT_OK;
@@ -1217,8 +1217,11 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     int rc = restrict_all(P, s);
     if (rc) return rc;
     SheetView W = view_of(s);
-    FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
-    if (ps.empty()) return fade_only(P, s, dt);
+    if (ps.empty()) {
+        FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
+        return fade_only(P, s, dt);
+    }
+    // With tires, k_refine_lay clears the spray count.
     // The coarse planes may still wait for the previous dry cut: the lay,
     // restrict and shove kernels apply it to the cells they touch.
     if ((rc = lay_patches(P, s, ps, dt))) return rc;

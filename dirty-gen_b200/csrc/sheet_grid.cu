@@ -315,9 +315,15 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     }
 }
 
-__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc) {
+__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc,
+                            int* count_next, double* zero_ledger, unsigned int* zero_bits) {
     const int nt = tf.tiles_x * tf.tiles_x;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) {
+        if (count_next) *count_next = 0;
+        if (zero_ledger) zero_ledger[0] = zero_ledger[1] = 0.0;
+        if (zero_bits) zero_bits[0] = zero_bits[1] = 0u;
+    }
     if (k >= 2 * nt) return;
     const int l = k / nt, t = k % nt;
     if (l == 0 ? skip0 : skip1) return;
@@ -352,11 +358,15 @@ __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, 
 }
 
 cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1,
-                             const SubstepCount& sc, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(tf.count, 0, sizeof(int), st);
-    if (e != cudaSuccess) return e;
+                             const SubstepCount& sc, int* count_next, double* zero_ledger, unsigned int* zero_bits,
+                             cudaStream_t st) {
+    if (!count_next) {
+        cudaError_t e = cudaMemsetAsync(tf.count, 0, sizeof(int), st);
+        if (e != cudaSuccess) return e;
+    }
     const int n = 2 * tf.tiles_x * tf.tiles_x;
-    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1, sc);
+    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1, sc, count_next, zero_ledger,
+                                                 zero_bits);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -94,8 +94,13 @@ constexpr int GRID_TILE = 32;
 size_t force_smem_bytes();
 // Builds the tile list of one substep: active tiles of both layers, then the
 // quiet tiles whose output buffer is not yet zero. `all` marks every tile active.
+// The list's count must be zero on entry. With `count_next` the kernel zeroes
+// the other count slot for the next substep (and `zero_ledger[0..1]`,
+// `zero_bits[0..1]` when given), so a step needs no memset; without it the
+// count is cleared by a memset first.
 cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1,
-                             const SubstepCount& sc, cudaStream_t st);
+                             const SubstepCount& sc, int* count_next, double* zero_ledger, unsigned int* zero_bits,
+                             cudaStream_t st);
 // Largest squared speed of each layer over the stepped tiles of the current
 // tile list, which must be substep 0's (cells below eps skipped when
 // apply_cut): atomicMax into bits[0..1], which start at zero.

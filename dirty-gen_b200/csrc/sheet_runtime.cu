@@ -103,6 +103,8 @@ struct silt_sheet {
     // Grid engine: active-tile flags and the substep's tile list.
     silt::TileFlags tf;
     uint8_t* tile_mem = nullptr;
+    int* tile_count = nullptr;   // two count slots, used alternately by successive substeps
+    unsigned long long tile_seq = 0;
     bool tiles_all = true;     // next substep steps every tile (after any outside write)
 
     float* H(int l) { return h[l][cur]; }
@@ -228,14 +230,19 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         F.nxt = nxt;
         T.tf = s->tf;
         T.nxt = nxt;
-        CK(cudaMemsetAsync(s->d_acc, 0, 2 * sizeof(double), s->st));
         // A substep that does not start from a dry cut (the first after an
         // outside write) steps every tile: its dry cells may carry velocity.
         const int all = (s->tiles_all || !(k > 0 || s->cut_pending)) ? 1 : 0;
-        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, 0, 0, sc, s->st));
+        // The list kernel clears this substep's ledger sums, the next
+        // substep's list count and, before the speed pass, the speed bits.
+        const int slot = (int)(s->tile_seq++ & 1);
+        s->tf.count = s->tile_count + slot;
+        F.tf.count = s->tf.count;
+        T.tf.count = s->tf.count;
+        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, 0, 0, sc, s->tile_count + (slot ^ 1), s->d_acc,
+                                  (k == 0 && sc.speed2) ? s->d_u32 : nullptr, s->st));
         if (k == 0 && sc.speed2) {
             // The substep count, from the tiles substep 0 steps.
-            CK(cudaMemsetAsync(s->d_u32, 0, 2 * sizeof(unsigned int), s->st));
             const float* hh[2] = {s->H(0), s->H(1)};
             const float* uu[2] = {s->U(0), s->U(1)};
             const float* vv[2] = {s->V(0), s->V(1)};
@@ -433,9 +440,11 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
                 }
             q = (uint8_t*)(((uintptr_t)q + 15) & ~uintptr_t(15));
             s->tf.list = (int*)q;
-            s->tf.count = s->tf.list + 2 * nt;
+            s->tile_count = s->tf.list + 2 * nt;
+            s->tf.count = s->tile_count;
             s->tf.stepped = reinterpret_cast<unsigned long long*>(s->d_u32 + 4);
             s->tf.tiles_x = tx;
+            e = cudaMemsetAsync(s->tile_count, 0, 2 * sizeof(int), s->st);
         }
     }
     if (s->engine == SILT_ENGINE_WINDOW) {
@@ -1109,7 +1118,7 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         T.nxt = 1;
         silt::SubstepCount host_count;
         memset(&host_count, 0, sizeof host_count);
-        CK(silt::launch_tile_list(tf, 0, 1, 1, 0, 1, host_count, st));
+        CK(silt::launch_tile_list(tf, 0, 1, 1, 0, 1, host_count, nullptr, nullptr, nullptr, st));
         CK(silt::launch_force(F, res, 1, st));
         CK(silt::launch_transport(T, res, 1, st));
         CK(cudaMemcpyAsync(h, h_next, n * 4, cudaMemcpyDeviceToDevice, st));
