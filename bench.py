@@ -14,6 +14,11 @@ with the per-step tire pushes from pinned host memory and the step's spray
 events and FP64 ledger read back each step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload grid|batch] [--windows 256] [--batch-tires 1|0]
+
+--workload batch: 256 independent windows, sides log-uniform 64..512 cells of
+0.2 m, each with its own seed, 1..4 puddles and 0..4 tires with 64 x 64
+patches, all stepped together (silt_batch_step); a step advances every window.
 """
 import argparse
 import json
@@ -48,6 +53,11 @@ def parse():
     ap.add_argument("--res", type=int, default=RES)
     ap.add_argument("--no-tires", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200"],
+                    help="grid: one 2048^2 grid with four tire patches; batch: many windows stepped together; "
+                         "window200: the reference's own 200^2 window, no tires")
+    ap.add_argument("--windows", type=int, default=256, help="batch: number of windows")
+    ap.add_argument("--batch-tires", type=int, default=1, help="batch: 1 = each window's 0..4 tires, 0 = none")
     return ap.parse_args()
 
 
@@ -328,9 +338,327 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- batched windows
+
+def batch_workload(args):
+    return {"workload": f"batch{args.windows}_side64-512_logu_1-4puddles_" +
+                        ("0-4tires64" if args.batch_tires else "notires"),
+            "windows": args.windows, "cell_m": CELL, "dt_s": DT, "fine_res": FINE_RES, "layout": "per_tire64",
+            "l2": "inputs larger than L2 (state ~1 GB)"}
+
+
+def batch_scene(args, rank=0):
+    import silt_scenes
+
+    wins = silt_scenes.batch_windows(n=args.windows, base_seed=0x9E3779B9 + 1000003 * rank, cell=CELL)
+    if not args.batch_tires:
+        for w in wins:
+            w["tires"] = 0
+    return wins
+
+
+def batch_tires(step, win):
+    import silt_scenes
+
+    if not win["tires"]:
+        return []
+    return silt_scenes.tires_at(step * DT, speed=5.0, z0=-0.5 * win["res"] * CELL)[:win["tires"]]
+
+
+def batch_cells(wins):
+    return sum(w["res"] * w["res"] + w["tires"] * FINE_RES * FINE_RES for w in wins)
+
+
+def batch_cpu(args, wins, max_steps, warmup, budget_s):
+    """The oracle on a bounded sample of the batch: every 16th window, each
+    stepped on its own (the reference steps one FluidCore at a time)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import silt_scenes
+
+    sample = wins[::16]
+    cores = []
+    for w in sample:
+        c = oracle.Core(res=w["res"], cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=2)
+        silt_scenes.seed_core(c, w)
+        cores.append(c)
+    k = 0
+    for _ in range(max(1, warmup)):
+        k += 1
+        for w, c in zip(sample, cores):
+            for t in batch_tires(k, w):
+                c.push_tire(**t)
+            c.step(DT)
+    steps = 0
+    t0 = time.perf_counter()
+    el = 0.0
+    while steps < max(1, max_steps) and el < budget_s:
+        k += 1
+        for w, c in zip(sample, cores):
+            for t in batch_tires(k, w):
+                c.push_tire(**t)
+            c.step(DT)
+        steps += 1
+        el = time.perf_counter() - t0
+    value = batch_cells(sample) * steps / el
+    return {"value": value, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
+            "sample": f"{len(sample)} of the {len(wins)} windows (every 16th), {steps} steps after "
+                      f"{max(1, warmup)} warm-up step(s), one window at a time, each pair on 2 threads ({el:.2f} s)"}
+
+
+def run_batch_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    wins = batch_scene(args)
+    base = batch_cpu(args, wins, max_steps=args.steps, warmup=args.warmup, budget_s=60.0)
+    line = {"metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": base["steps"], "warmup": max(1, args.warmup),
+            "ms_per_step": 1000.0 * batch_cells(wins) / base["value"], "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": batch_workload(args), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    import torch
+
+    import silt_b200
+    import silt_scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    import silt_shard
+
+    all_wins = batch_scene(args)
+    mine = silt_shard.shard(len(all_wins), rank, world)  # round-robin: windows are independent
+    wins = [all_wins[w] for w in mine]
+    sheets = []
+    for w in wins:
+        sh = silt_b200.Sheet(res=w["res"], cell=CELL, fine_res=FINE_RES, fine_cell=0.02,
+                             layout=silt_b200.FINE_PER_TIRE, device=local, stream=stream.cuda_stream,
+                             engine=silt_b200.ENGINE_GRID)
+        silt_scenes.seed_core(sh, w)
+        sheets.append(sh)
+    batch = silt_b200.Batch(sheets)
+    cells = batch_cells(wins)
+    step_no = 0
+
+    def one_step():
+        nonlocal step_no
+        step_no += 1
+        for sh, w in zip(sheets, wins):
+            for t in batch_tires(step_no, w):
+                sh.push_tire(**t)
+        batch.step(DT)
+
+    for _ in range(max(3, args.warmup)):
+        one_step()
+    torch.cuda.synchronize()
+    stop = threading.Event()
+    clock_lines = []
+    th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, local), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    batch.set_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step()
+    host_ms = (time.perf_counter() - h0) * 1000.0 / args.steps
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    parts = batch.parts()
+    batch.set_timing(False)
+    stop.set()
+    th.join(timeout=5)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_cells = batch_cells(all_wins)
+    value = total_cells * args.steps / (ms / 1000.0)
+    # End to end: the pushes in, every window's FP64 ledger back (gathered
+    # over the ranks: the one collective), each step.
+    e2e_steps = max(5, args.steps // 4)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        one_step()
+        led = batch.ledgers()
+        table = silt_shard.gather_ledgers(dict(zip(mine, led)), len(all_wins), dist,
+                                          device="cuda" if dist else "cpu")
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e_value = total_cells * e2e_steps / (ems / 1000.0)
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        launches = max(parts["force_launches"], 1)
+        force_ms = parts["force_ms"] / launches
+        cw = parts["force_cells_water"] / launches
+        cs = (parts["force_cells"] - parts["force_cells_water"]) / launches
+        force_bytes = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * cs
+        achieved = force_bytes / (force_ms / 1000.0) / 1e9 if force_ms > 0 else None
+        coarse = sum(w["res"] * w["res"] for w in wins)
+        roof = {"bound": "hbm", "kernel": "k_batch_force", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms,
+                "stepped_cell_layers_per_launch": cw + cs, "active_fraction": (cw + cs) / (2.0 * coarse),
+                "transport_avg_launch_ms": parts["transport_ms"] / launches}
+        n_tires = sum(w["tires"] for w in wins)
+        line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": batch_workload(args), "roofline": roof,
+                "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * n_tires,
+                        "d2h_bytes_per_step": 40 * len(wins), "steps": e2e_steps},
+                "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
+                "host_submit_ms_per_step": host_ms,
+                "host_ms_per_step": {"batch_step": parts["host_step_ms"] / args.steps,
+                                     "per_window_before_coarse": parts["host_fine_ms"] / args.steps},
+                "window_steps_per_s": len(all_wins) * args.steps / (ms / 1000.0),
+                "windows": len(all_wins), "windows_rank0": len(wins), "coarse_cells_rank0": coarse,
+                "tires_rank0": n_tires, "ledger_total_m3": float(table[:, -1].sum())}
+        if not args.no_baseline:
+            line["cpu_baseline"] = batch_cpu(args, all_wins, max_steps=20, warmup=1, budget_s=20.0)
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for sh in sheets:
+        sh.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- the 200 x 200 window
+
+def run_window200(args):
+    """The reference's CPU-runnable case: one 200 x 200 window (0.2 m cells),
+    ruts, a Gaussian puddle and a rut slurry film, no tires, dt = 1/120 s,
+    stepped on the window engine (the exact box-by-box step)."""
+    import torch
+
+    import silt_b200
+    import silt_scenes
+
+    if int(os.environ.get("RANK", "0")) != 0 and args.impl == "reference":
+        return
+    scene = silt_scenes.window200()
+    res = scene["res"]
+    cfgw = {"workload": "window200_ruts_puddle_slurry", "res": res, "cell_m": CELL, "dt_s": DT,
+            "engine": "window", "l2": "state fits in L2 (~2 MB); no flush between steps"}
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        core = oracle.Core(threads=2)
+        silt_scenes.seed_core(core, scene)
+        for _ in range(max(1, args.warmup)):
+            core.step(DT)
+        steps, t0, el = 0, time.perf_counter(), 0.0
+        while steps < max(1, args.steps) and el < 60.0:
+            core.step(DT)
+            steps += 1
+            el = time.perf_counter() - t0
+        v = res * res * steps / el
+        base = {"value": v, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
+                "sample": f"{steps} steps after {max(1, args.warmup)} warm-up, the pair on 2 threads ({el:.2f} s)"}
+        print(json.dumps({"metric": "cell-steps/s", "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+                          "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": 1000.0 * el / steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "impl": "reference", "config": cfgw, "cpu_baseline": base,
+                          "window_steps_per_s": steps / el,
+                          "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    sheet = silt_b200.Sheet(device=local, stream=stream.cuda_stream)
+    silt_scenes.seed_core(sheet, scene)
+    for _ in range(max(3, args.warmup)):
+        sheet.step(DT, want_spray=False)
+    torch.cuda.synchronize()
+    sheet.set_step_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sheet.step(DT, want_spray=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    parts = sheet.step_parts()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(10, args.steps // 4)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        sheet.step(DT)
+        sheet.ledger()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    line = {"metric": "cell-steps/s", "value": res * res * args.steps / (ms / 1000.0), "unit": "cell-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfgw, "window_steps_per_s": args.steps / (ms / 1000.0),
+            "e2e": {"value": res * res * e2e_steps / (ems / 1000.0), "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 60, "steps": e2e_steps},
+            "gpu_launches": int(parts["launches"])}
+    if not args.no_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        core = oracle.Core(threads=2)
+        silt_scenes.seed_core(core, scene)
+        core.step(DT)
+        t0 = time.perf_counter()
+        for _ in range(20):
+            core.step(DT)
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": res * res * 20 / el, "unit": "cell-steps/s", "cores": 2, "kind": "port",
+                                "sample": f"20 steps after 1 warm-up, the pair on 2 threads ({el:.2f} s)"}
+    print(json.dumps(line), flush=True)
+    sheet.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "window200":
+        run_window200(args)
+    elif args.workload == "batch":
+        if args.impl == "reference":
+            run_batch_reference(args)
+        else:
+            run_batch(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

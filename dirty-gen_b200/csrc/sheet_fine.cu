@@ -1314,6 +1314,8 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
     return SILT_OK;
 }
 
+const double* books(Patches& P) { return I(P).d_books; }
+
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s) {
     Impl& M = I(P);
     SheetView W = view_of(s);

@@ -259,83 +259,80 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
 #undef NZ
 }
 
+// A layer's force parameters for this substep: with a device count, its dt
+// and (constant-viscosity layers) damping factor for that count.
+__device__ __forceinline__ LayerParams force_params(const LayerParams& P0, const SubstepCount& sc, int l,
+                                                    bool report_overflow) {
+    LayerParams P = P0;
+    if (sc.speed2) {
+        const int ns = device_nsub(sc, l);
+        P.dt = sc.dt / (float)ns;
+        if (P.nu_mode == NU_CONST) P.decay_c = sc.water_decay[ns];
+        if (report_overflow && sc.k == 0 && ns > sc.launched) atomicOr(sc.overflow, 1u);
+    }
+    return P;
+}
+
+// One list entry of the force pass. Returns true when it used shared memory.
+__device__ __forceinline__ bool force_entry(const LayerParams& P, const TileFlags& tf, int nxt, int e, float* sm) {
+    const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
+    const int res = P.res;
+    const int tx0 = (t % tf.tiles_x) * FT, ty0 = (t / tf.tiles_x) * FT;
+    if (copy) {
+        // Identity substep of a layer that has taken all its substeps.
+        const int w = min(FT, res - tx0), h = min(FT, res - ty0);
+        for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+            const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
+            P.u_out[g] = P.u[g];
+            P.v_out[g] = P.v[g];
+        }
+        if (threadIdx.x == 0) pick(tf.zero_uv, l, nxt)[t] = pick(tf.zero_uv, l, nxt ^ 1)[t];
+        return false;
+    }
+    if (zero_fill) {
+        // A quiet tile: dry in its whole neighbourhood, so after the dry cut
+        // its velocity is zero.
+        const int w = min(FT, res - tx0), h = min(FT, res - ty0);
+        for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+            const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
+            P.u_out[g] = 0.0f;
+            P.v_out[g] = 0.0f;
+        }
+        if (threadIdx.x == 0) pick(tf.zero_uv, l, nxt)[t] = 1;
+        return false;
+    }
+    const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
+    if (interior)
+        force_tile<false>(P, sm, tx0, ty0);
+    else
+        force_tile<true>(P, sm, tx0, ty0);
+    if (threadIdx.x == 0) pick(tf.zero_uv, l, nxt)[t] = 0;
+    return true;
+}
+
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
     extern __shared__ float sm[];
     __shared__ LayerParams Ps[2];
-    if (threadIdx.x < 2) {
-        const int l = threadIdx.x;
-        LayerParams P = L.lay[l];
-        if (L.sc.speed2) {
-            const int ns = device_nsub(L.sc, l);
-            P.dt = L.sc.dt / (float)ns;
-            if (P.nu_mode == NU_CONST) P.decay_c = L.sc.water_decay[ns];
-            if (L.sc.k == 0 && blockIdx.x == 0 && ns > L.sc.launched) atomicOr(L.sc.overflow, 1u);
-        }
-        Ps[l] = P;
-    }
+    if (threadIdx.x < 2) Ps[threadIdx.x] = force_params(L.lay[threadIdx.x], L.sc, threadIdx.x, blockIdx.x == 0);
     __syncthreads();
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
-        const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
-        const LayerParams& P = Ps[l];
-        const int res = P.res;
-        const int tx0 = (t % L.tf.tiles_x) * FT, ty0 = (t / L.tf.tiles_x) * FT;
-        if (copy) {
-            // Identity substep of a layer that has taken all its substeps.
-            const int w = min(FT, res - tx0), h = min(FT, res - ty0);
-            for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
-                const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
-                P.u_out[g] = P.u[g];
-                P.v_out[g] = P.v[g];
-            }
-            if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = pick(L.tf.zero_uv, l, L.nxt ^ 1)[t];
-            continue;
-        }
-        if (zero_fill) {
-            // A quiet tile: dry in its whole neighbourhood, so after the dry cut
-            // its velocity is zero.
-            const int w = min(FT, res - tx0), h = min(FT, res - ty0);
-            for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
-                const size_t g = (size_t)(ty0 + q / w) * res + tx0 + q % w;
-                P.u_out[g] = 0.0f;
-                P.v_out[g] = 0.0f;
-            }
-            if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = 1;
-            continue;
-        }
-        const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
-        if (interior)
-            force_tile<false>(P, sm, tx0, ty0);
-        else
-            force_tile<true>(P, sm, tx0, ty0);
-        if (threadIdx.x == 0) pick(L.tf.zero_uv, l, L.nxt)[t] = 0;
-        __syncthreads();  // shared memory is reused by the next tile
+        if (force_entry(Ps[e >> 30], L.tf, L.nxt, e, sm)) __syncthreads();  // shared memory is reused by the next tile
     }
 }
 
-__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc,
-                            int* count_next, double* zero_ledger, unsigned int* zero_bits) {
-    const int nt = tf.tiles_x * tf.tiles_x;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0) {
-        if (count_next) *count_next = 0;
-        if (zero_ledger) zero_ledger[0] = zero_ledger[1] = 0.0;
-        if (zero_bits) zero_bits[0] = zero_bits[1] = 0u;
-    }
-    if (k >= 2 * nt) return;
-    const int l = k / nt, t = k % nt;
-    if (l == 0 ? skip0 : skip1) return;
+// The list entry of tile t of layer l for this substep, or -1 for none.
+__device__ __forceinline__ int tile_entry(const TileFlags& tf, int cur, int nxt, int all, const SubstepCount& sc,
+                                          int l, int t) {
     if (sc.speed2 && sc.k > 0) {  // substep 0 steps every layer; its list precedes the speed pass
         const int ns = device_nsub(sc, l);
         if (sc.k >= ns) {
             // Identity substep: carry every tile not known to be zero.
-            if (!(pick(tf.zero_h, l, cur)[t] && pick(tf.zero_uv, l, cur)[t]))
-                tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_COPY | t;
-            else if (!(pick(tf.zero_h, l, nxt)[t] && pick(tf.zero_uv, l, nxt)[t]))
-                tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_ZERO | t;
-            return;
+            if (!(pick(tf.zero_h, l, cur)[t] && pick(tf.zero_uv, l, cur)[t])) return (l << 30) | ENTRY_COPY | t;
+            if (!(pick(tf.zero_h, l, nxt)[t] && pick(tf.zero_uv, l, nxt)[t])) return (l << 30) | ENTRY_ZERO | t;
+            return -1;
         }
     }
     const int ti = t % tf.tiles_x, tj = t / tf.tiles_x;
@@ -350,11 +347,27 @@ __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, 
             }
         }
     if (active) {
-        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | t;
         if (tf.stepped) atomicAdd(&tf.stepped[l], 1ull);
-    } else if (!pick(tf.zero_uv, l, nxt)[t] || !pick(tf.zero_h, l, nxt)[t]) {
-        tf.list[atomicAdd(tf.count, 1)] = (l << 30) | ENTRY_ZERO | t;
+        return (l << 30) | t;
     }
+    if (!pick(tf.zero_uv, l, nxt)[t] || !pick(tf.zero_h, l, nxt)[t]) return (l << 30) | ENTRY_ZERO | t;
+    return -1;
+}
+
+__global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc,
+                            int* count_next, double* zero_ledger, unsigned int* zero_bits) {
+    const int nt = tf.tiles_x * tf.tiles_x;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) {
+        if (count_next) *count_next = 0;
+        if (zero_ledger) zero_ledger[0] = zero_ledger[1] = 0.0;
+        if (zero_bits) zero_bits[0] = zero_bits[1] = 0u;
+    }
+    if (k >= 2 * nt) return;
+    const int l = k / nt, t = k % nt;
+    if (l == 0 ? skip0 : skip1) return;
+    const int e = tile_entry(tf, cur, nxt, all, sc, l, t);
+    if (e >= 0) tf.list[atomicAdd(tf.count, 1)] = e;
 }
 
 cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int skip0, int skip1,
@@ -531,6 +544,29 @@ __device__ void copy_tile(const TransportParams& P, int tx0, int ty0, const Tile
     __syncthreads();
 }
 
+// One list entry of the transport pass.
+__device__ __forceinline__ void transport_entry(const TransportParams& P, const TileFlags& tf, int nxt, int e,
+                                                float* sm) {
+    const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
+    const int res = P.res;
+    const int tx0 = (t % tf.tiles_x) * TT, ty0 = (t / tf.tiles_x) * TT;
+    if (copy) {
+        copy_tile(P, tx0, ty0, tf, l, nxt, t);
+        return;
+    }
+    if (zero_fill) {
+        const int w = min(TT, res - tx0), h = min(TT, res - ty0);
+        for (int q = threadIdx.x; q < w * h; q += blockDim.x)
+            P.h_out[(size_t)(ty0 + q / w) * res + tx0 + q % w] = 0.0f;
+        if (threadIdx.x == 0) {
+            pick(tf.wet, l, nxt)[t] = 0;
+            pick(tf.zero_h, l, nxt)[t] = 1;
+        }
+        return;
+    }
+    transport_tile(P, sm, tx0, ty0, tf, l, nxt, t);
+}
+
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
     extern __shared__ float sm[];
@@ -545,25 +581,7 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
-        const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
-        const TransportParams& P = Ps[l];
-        const int res = P.res;
-        const int tx0 = (t % L.tf.tiles_x) * TT, ty0 = (t / L.tf.tiles_x) * TT;
-        if (copy) {
-            copy_tile(P, tx0, ty0, L.tf, l, L.nxt, t);
-            continue;
-        }
-        if (zero_fill) {
-            const int w = min(TT, res - tx0), h = min(TT, res - ty0);
-            for (int q = threadIdx.x; q < w * h; q += blockDim.x)
-                P.h_out[(size_t)(ty0 + q / w) * res + tx0 + q % w] = 0.0f;
-            if (threadIdx.x == 0) {
-                pick(L.tf.wet, l, L.nxt)[t] = 0;
-                pick(L.tf.zero_h, l, L.nxt)[t] = 1;
-            }
-            continue;
-        }
-        transport_tile(P, sm, tx0, ty0, L.tf, l, L.nxt, t);
+        transport_entry(Ps[e >> 30], L.tf, L.nxt, e, sm);
     }
 }
 
@@ -631,6 +649,152 @@ cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], con
                                const float* const v[2], int res, float eps, int apply_cut, unsigned int* bits,
                                cudaStream_t st) {
     k_tile_speed2<<<148 * 8, 256, 0, st>>>(tf, h[0], u[0], v[0], h[1], u[1], v[1], res, eps, apply_cut, bits);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ batched windows
+
+__global__ void k_batch_tile_list(const WindowSubstep* ws, int* list, int* entry_win, int* count, int* count_next) {
+    const int w = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w == 0 && k == 0) *count_next = 0;
+    const WindowSubstep& D = ws[w];
+    if (D.skip) return;
+    const TileFlags& tf = D.F.tf;
+    if (k == 0) {
+        if (D.zero_ledger) D.zero_ledger[0] = D.zero_ledger[1] = 0.0;
+        if (D.zero_bits) D.zero_bits[0] = D.zero_bits[1] = 0u;
+    }
+    const int nt = tf.tiles_x * tf.tiles_x;
+    if (k >= 2 * nt) return;
+    const int l = k / nt, t = k % nt;
+    const int e = tile_entry(tf, D.cur, D.F.nxt, D.all, D.F.sc, l, t);
+    if (e >= 0) {
+        const int q = atomicAdd(count, 1);
+        list[q] = e;
+        entry_win[q] = w;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_speed2(const WindowSubstep* ws, const int* list, const int* entry_win,
+                                                      const int* count) {
+    const int n = *count;
+    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = list[k];
+        if (e & (ENTRY_ZERO | ENTRY_COPY)) continue;
+        const WindowSubstep& D = ws[entry_win[k]];
+        if (!D.zero_bits) continue;
+        const int l = e >> 30, t = e & ENTRY_TILE;
+        const LayerParams& P = D.F.lay[l];
+        const int res = P.res, tiles_x = D.F.tf.tiles_x;
+        const int tx0 = (t % tiles_x) * GRID_TILE, ty0 = (t / tiles_x) * GRID_TILE;
+        const int gx = tx0 + lane;
+        float hv[4], uv[4], vv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int gy = ty0 + wy + 8 * r;
+            const bool in = gx < res && gy < res;
+            const size_t g = in ? (size_t)gy * res + gx : 0;
+            hv[r] = in ? P.h[g] : 0.0f;
+            uv[r] = in ? P.u[g] : 0.0f;
+            vv[r] = in ? P.v[g] : 0.0f;
+        }
+        float m = 0.0f;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (D.apply_cut && hv[r] < P.eps) continue;
+            const float s2 = uv[r] * uv[r] + vv[r] * vv[r];
+            if (s2 > m) m = s2;
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (lane == 0 && m > 0.0f) atomicMax(&D.zero_bits[l], __float_as_uint(m));
+    }
+}
+
+__global__ void __launch_bounds__(FORCE_THREADS) k_batch_force(const WindowSubstep* ws, const int* list,
+                                                               const int* entry_win, const int* count) {
+    extern __shared__ float sm[];
+    __shared__ LayerParams Ps;
+    __shared__ TileFlags Tf;
+    __shared__ int nxt_s;
+    const int n = *count;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = list[k];
+        if (threadIdx.x == 0) {
+            const WindowSubstep& D = ws[entry_win[k]];
+            Ps = force_params(D.F.lay[e >> 30], D.F.sc, e >> 30, true);
+            Tf = D.F.tf;
+            nxt_s = D.F.nxt;
+        }
+        __syncthreads();
+        force_entry(Ps, Tf, nxt_s, e, sm);
+        __syncthreads();  // the parameters and shared memory are reused by the next entry
+    }
+}
+
+__global__ void __launch_bounds__(TRANSPORT_THREADS) k_batch_transport(const WindowSubstep* ws, const int* list,
+                                                                       const int* entry_win, const int* count) {
+    extern __shared__ float sm[];
+    __shared__ TransportParams Ps;
+    __shared__ TileFlags Tf;
+    __shared__ int nxt_s;
+    const int n = *count;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = list[k];
+        if (threadIdx.x == 0) {
+            const WindowSubstep& D = ws[entry_win[k]];
+            const int l = e >> 30;
+            TransportParams P = D.T.lay[l];
+            if (D.T.sc.speed2) P.dt = D.T.sc.dt / (float)device_nsub(D.T.sc, l);
+            Ps = P;
+            Tf = D.T.tf;
+            nxt_s = D.T.nxt;
+        }
+        __syncthreads();
+        transport_entry(Ps, Tf, nxt_s, e, sm);
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_batch_tile_list(const WindowSubstep* d_ws, int nwin, int max_tiles, int* list, int* entry_win,
+                                   int* count, int* count_next, cudaStream_t st) {
+    if (nwin <= 0) return cudaSuccess;
+    dim3 grid((2 * max_tiles + 255) / 256, nwin);
+    k_batch_tile_list<<<grid, 256, 0, st>>>(d_ws, list, entry_win, count, count_next);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
+                                cudaStream_t st) {
+    k_batch_speed2<<<148 * 8, 256, 0, st>>>(d_ws, list, entry_win, count);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
+                               cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_batch_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
+        attr = true;
+    }
+    k_batch_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(d_ws, list, entry_win, count);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
+                                   const int* count, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_batch_transport, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)transport_smem_bytes());
+        attr = true;
+    }
+    k_batch_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }

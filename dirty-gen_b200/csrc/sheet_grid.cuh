@@ -91,6 +91,30 @@ struct TransportLaunch {
 
 constexpr int GRID_TILE = 32;
 
+// One window's part of a batched substep (many independent windows stepped by
+// the same launches). The list kernel reads it by window (blockIdx.y); the
+// force, speed and transport kernels by each list entry's window.
+struct WindowSubstep {
+    ForceLaunch F;            // layers, the window's tile flags, device count, buffer written
+    TransportLaunch T;
+    int32_t cur, all;
+    int32_t skip;             // the window sits this substep out
+    int32_t apply_cut;        // speed pass: cells below eps are skipped
+    double* zero_ledger;      // the window's ledger sums, cleared by the list kernel
+    unsigned int* zero_bits;  // the window's speed bits, cleared before substep 0's speed pass (or nullptr)
+};
+
+// Batched substep over `nwin` windows: one tile list (entries and their
+// window indices), cleared count slot for the next substep.
+cudaError_t launch_batch_tile_list(const WindowSubstep* d_ws, int nwin, int max_tiles, int* list, int* entry_win,
+                                   int* count, int* count_next, cudaStream_t st);
+cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
+                                cudaStream_t st);
+cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
+                               cudaStream_t st);
+cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
+                                   const int* count, cudaStream_t st);
+
 size_t force_smem_bytes();
 // Builds the tile list of one substep: active tiles of both layers, then the
 // quiet tiles whose output buffer is not yet zero. `all` marks every tile active.

@@ -228,6 +228,22 @@ cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaS
     ::silt::count_launch();
     return cudaGetLastError();
 }
+__global__ void k_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n) return;
+    out[5 * w + 0] = acc[w][0];
+    out[5 * w + 1] = acc[w][1];
+    out[5 * w + 2] = books[w][0];
+    out[5 * w + 3] = books[w][1];
+    out[5 * w + 4] = books[w][2];
+}
+cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
+                              cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_gather_ledgers<<<(n + 127) / 128, 128, 0, st>>>(acc, books, n, out);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;

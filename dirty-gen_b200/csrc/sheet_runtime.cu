@@ -144,111 +144,139 @@ int upload(silt_sheet* s, float* dst, const float* host) {
     return SILT_OK;
 }
 
-// One coarse-sized pair of sheets for one step (FluidCore::step_pair, src/fluid_core.rs:7942-8150).
-// `soften` is the soft window border, applied once per step before the first substep.
-int step_coarse_pair(silt_sheet* s, float dt) {
-    const int res = s->res;
+// Host plan of one sheet's coarse pair for one step: how many substeps to
+// launch and whether the device decides the count.
+struct CoarsePlan {
+    int launched = 1;
+    silt::SubstepCount sc;
+    int soften_edge = 0;
+    float nu_w = 0.0f;
+};
+
+// Substep count (src/fluid_core.rs:1715-1744). With every speed under the
+// host's bound one substep is certain. Otherwise the device measures each
+// layer's largest speed and decides its count; the host launches as many
+// substeps as the bound allows, without waiting for the answer.
+void coarse_plan(silt_sheet* s, float dt, CoarsePlan& cp) {
     const float cell = s->cfg.cell;
-    const float eps = 1.0e-6f;
-    // Substep count (src/fluid_core.rs:1715-1744). With every speed under the
-    // host's bound one substep is certain. Otherwise the device measures each
-    // layer's largest speed and decides its count; the host launches as many
-    // substeps as the bound allows, without waiting for the answer.
     const float cap = 8.0f;
     const float bound = s->vmax_bound;
     const float courant_len = 0.42f * std::max(cell, 1.0e-3f);
-    int launched = 1;
-    silt::SubstepCount sc;
-    memset(&sc, 0, sizeof sc);
-    sc.dt = dt;
-    sc.cell = cell;
-    sc.cap = cap;
-    const float nu_w = water_nu();
-    for (int q = 1; q <= 8; ++q) sc.water_decay[q] = expf(-silt::host::sheet_damp(nu_w) * (dt / (float)q));
-    sc.water_decay[0] = sc.water_decay[1];
+    memset(&cp.sc, 0, sizeof cp.sc);
+    cp.launched = 1;
+    cp.sc.dt = dt;
+    cp.sc.cell = cell;
+    cp.sc.cap = cap;
+    cp.nu_w = water_nu();
+    for (int q = 1; q <= 8; ++q) cp.sc.water_decay[q] = expf(-silt::host::sheet_damp(cp.nu_w) * (dt / (float)q));
+    cp.sc.water_decay[0] = cp.sc.water_decay[1];
     if (!(dt * std::max(0.15f, bound) <= courant_len)) {
         const float nb = ceilf((dt * std::max(0.15f, bound)) / courant_len);
-        launched = std::isfinite(nb) ? (int)silt::host::rclamp(nb, 1.0f, cap) : (int)cap;
-        sc.speed2 = s->d_u32;
-        sc.overflow = s->d_u32 + 2;
-        sc.launched = launched;
+        cp.launched = std::isfinite(nb) ? (int)silt::host::rclamp(nb, 1.0f, cap) : (int)cap;
+        cp.sc.speed2 = s->d_u32;
+        cp.sc.overflow = s->d_u32 + 2;
+        cp.sc.launched = cp.launched;
         s->parts.device_counts += 1;
     }
-    const int soften_edge = s->cfg.soften_border ? std::max(res / 12, 2) : 0;
-    for (int k = 0; k < launched; ++k) {
+    cp.soften_edge = s->cfg.soften_border ? std::max(s->res / 12, 2) : 0;
+}
+
+// Parameters of substep k of FluidCore::step_pair (src/fluid_core.rs:7942-8150)
+// on the sheet's current buffers, writing the other ones. `all`: step every
+// tile (the first substep after an outside write, whose dry cells may carry
+// velocity).
+void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::ForceLaunch& F,
+                    silt::TransportLaunch& T, int& all) {
+    const int res = s->res;
+    const float cell = s->cfg.cell;
+    const float eps = 1.0e-6f;
+    memset(&F, 0, sizeof F);
+    memset(&T, 0, sizeof T);
+    const int nxt = s->cur ^ 1;
+    F.sc = cp.sc;
+    F.sc.k = k;
+    T.sc = F.sc;
+    for (int l = 0; l < 2; ++l) {
+        silt::LayerParams& P = F.lay[l];
+        P.h = s->h[l][s->cur];
+        P.bed = s->bed;
+        P.u = s->u[l][s->cur];
+        P.v = s->v[l][s->cur];
+        P.u_out = s->u[l][nxt];
+        P.v_out = s->v[l][nxt];
+        P.res = res;
+        P.cell = cell;
+        P.dt = dt;  // the device divides by its count when it decides one
+        P.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
+        P.eps = eps;
+        P.project = cell > silt::host::kFineCell + 1.0e-6f;
+        P.soften_edge = k == 0 ? cp.soften_edge : 0;
+        P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
+        P.skip = 0;
+        if (l == 0) {
+            P.nu_mode = silt::NU_CONST;
+            P.nu_c = cp.nu_w;
+            P.mob_c = silt::host::sheet_mobility_for(cp.nu_w);
+            P.decay_c = cp.sc.water_decay[1];
+        } else {
+            P.nu_mode = silt::NU_GRAIN;
+            P.grain = s->grain;
+            P.moisture = s->moisture;
+        }
+        silt::TransportParams& Q = T.lay[l];
+        Q.h = s->h[l][s->cur];
+        Q.u = P.u_out;
+        Q.v = P.v_out;
+        Q.h_out = s->h[l][nxt];
+        Q.gate = nullptr;
+        Q.bank_bed = nullptr;
+        Q.ledger = s->d_acc + l;
+        Q.res = res;
+        Q.cell = cell;
+        Q.dt = dt;
+        Q.eps = eps;
+        Q.skip = 0;
+    }
+    F.tf = s->tf;
+    F.nxt = nxt;
+    T.tf = s->tf;
+    T.nxt = nxt;
+    all = (s->tiles_all || !(k > 0 || s->cut_pending)) ? 1 : 0;
+}
+
+// After substep k: the other buffers are current and wait for the dry cut.
+void coarse_advance(silt_sheet* s) {
+    s->cur ^= 1;
+    s->cut_pending = true;
+    s->tiles_all = false;
+}
+
+// One coarse-sized pair of sheets for one step (FluidCore::step_pair, src/fluid_core.rs:7942-8150).
+int step_coarse_pair(silt_sheet* s, float dt) {
+    const int res = s->res;
+    const float eps = 1.0e-6f;
+    CoarsePlan cp;
+    coarse_plan(s, dt, cp);
+    for (int k = 0; k < cp.launched; ++k) {
         silt::ForceLaunch F;
         silt::TransportLaunch T;
-        memset(&F, 0, sizeof F);
-        memset(&T, 0, sizeof T);
-        const int nxt = s->cur ^ 1;
-        sc.k = k;
-        F.sc = sc;
-        T.sc = sc;
-        for (int l = 0; l < 2; ++l) {
-            silt::LayerParams& P = F.lay[l];
-            const float dts = dt;  // the device divides by its count when it decides one
-            P.h = s->h[l][s->cur];
-            P.bed = s->bed;
-            P.u = s->u[l][s->cur];
-            P.v = s->v[l][s->cur];
-            P.u_out = s->u[l][nxt];
-            P.v_out = s->v[l][nxt];
-            P.res = res;
-            P.cell = cell;
-            P.dt = dts;
-            P.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
-            P.eps = eps;
-            P.project = cell > silt::host::kFineCell + 1.0e-6f;
-            P.soften_edge = k == 0 ? soften_edge : 0;
-            P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
-            P.skip = 0;
-            if (l == 0) {
-                P.nu_mode = silt::NU_CONST;
-                P.nu_c = nu_w;
-                P.mob_c = silt::host::sheet_mobility_for(nu_w);
-                P.decay_c = sc.water_decay[1];
-            } else {
-                P.nu_mode = silt::NU_GRAIN;
-                P.grain = s->grain;
-                P.moisture = s->moisture;
-            }
-            silt::TransportParams& Q = T.lay[l];
-            Q.h = s->h[l][s->cur];
-            Q.u = P.u_out;
-            Q.v = P.v_out;
-            Q.h_out = s->h[l][nxt];
-            Q.gate = nullptr;
-            Q.bank_bed = nullptr;
-            Q.ledger = s->d_acc + l;
-            Q.res = res;
-            Q.cell = cell;
-            Q.dt = dts;
-            Q.eps = eps;
-            Q.skip = P.skip;
-        }
-        F.tf = s->tf;
-        F.nxt = nxt;
-        T.tf = s->tf;
-        T.nxt = nxt;
-        // A substep that does not start from a dry cut (the first after an
-        // outside write) steps every tile: its dry cells may carry velocity.
-        const int all = (s->tiles_all || !(k > 0 || s->cut_pending)) ? 1 : 0;
+        int all = 0;
+        coarse_substep(s, cp, dt, k, F, T, all);
         // The list kernel clears this substep's ledger sums, the next
         // substep's list count and, before the speed pass, the speed bits.
         const int slot = (int)(s->tile_seq++ & 1);
         s->tf.count = s->tile_count + slot;
         F.tf.count = s->tf.count;
         T.tf.count = s->tf.count;
-        CK(silt::launch_tile_list(s->tf, s->cur, nxt, all, 0, 0, sc, s->tile_count + (slot ^ 1), s->d_acc,
-                                  (k == 0 && sc.speed2) ? s->d_u32 : nullptr, s->st));
-        if (k == 0 && sc.speed2) {
+        CK(silt::launch_tile_list(s->tf, s->cur, F.nxt, all, 0, 0, F.sc, s->tile_count + (slot ^ 1), s->d_acc,
+                                  (k == 0 && F.sc.speed2) ? s->d_u32 : nullptr, s->st));
+        if (k == 0 && F.sc.speed2) {
             // The substep count, from the tiles substep 0 steps.
             const float* hh[2] = {s->H(0), s->H(1)};
             const float* uu[2] = {s->U(0), s->U(1)};
             const float* vv[2] = {s->V(0), s->V(1)};
             CK(silt::launch_tile_speed2(s->tf, hh, uu, vv, res, eps, s->cut_pending ? 1 : 0, s->d_u32, s->st));
         }
-        s->tiles_all = false;
         cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
         if (s->timing) {
             for (int q = 0; q < 3; ++q) {
@@ -268,8 +296,7 @@ int step_coarse_pair(silt_sheet* s, float dt) {
         CK(silt::launch_transport(T, res, 2, s->st));
         if (s->timing) CK(cudaEventRecord(ev[2], s->st));
         s->parts.force_launches += 1;
-        s->cur = nxt;
-        s->cut_pending = true;
+        coarse_advance(s);
     }
     // Every component is now clamped to the film speed cap.
     s->vmax_bound = silt::host::kSpeedCap * 1.4142137f;
@@ -698,6 +725,31 @@ int silt_push_tire(silt_sheet* s, const silt_tire_push* p) {
     return SILT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The parts of silt_step before the coarse pair: the tire pushes of the step,
+// the inflow strip, the nested patches (refine, shove, fine pair, peel,
+// restrict, shove outside).
+int step_before_coarse(silt_sheet* s, float dt, std::vector<silt_tire_push>& ps, silt::fine::StepOut& fo) {
+    ps.clear();
+    ps.swap(s->pushes);
+    if (s->inflow_j >= 0) {
+        int nc = s->inflow_i1 - s->inflow_i0;
+        float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
+        silt::fine::SheetView W = silt::fine::view_of(s);
+        CK(silt::op_inflow(s->H(0), s->U(0), s->V(0), s->cut_pending ? 1 : 0, s->res, s->inflow_j, s->inflow_i0,
+                           s->inflow_i1, add, W.tiles_x, W.t_wet[0], W.t_zuv[0], W.t_zh[0], s->st));
+        s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
+    }
+    return silt::fine::step_patches(s->fine, s, ps, dt, fo);
+}
+
+}  // namespace
+
+extern "C" {
+
 int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32_t* n_out) {
     if (!s) return fail_arg("handle");
     if (n_out) *n_out = 0;
@@ -709,19 +761,8 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     using clock = std::chrono::steady_clock;
     const clock::time_point t0 = clock::now();
     std::vector<silt_tire_push> ps;
-    ps.swap(s->pushes);
-    int rc;
-    if (s->inflow_j >= 0) {
-        int nc = s->inflow_i1 - s->inflow_i0;
-        float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
-        silt::fine::SheetView W = silt::fine::view_of(s);
-        CK(silt::op_inflow(s->H(0), s->U(0), s->V(0), s->cut_pending ? 1 : 0, s->res, s->inflow_j, s->inflow_i0,
-                           s->inflow_i1, add, W.tiles_x, W.t_wet[0], W.t_zuv[0], W.t_zh[0], s->st));
-        s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
-    }
     silt::fine::StepOut fo;
-    const clock::time_point t1 = clock::now();
-    rc = silt::fine::step_patches(s->fine, s, ps, dt, fo);
+    int rc = step_before_coarse(s, dt, ps, fo);
     if (rc) return rc;
     const clock::time_point t2 = clock::now();
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
@@ -739,7 +780,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     if (s->timing) {
         const clock::time_point t3 = clock::now();
         s->parts.host_step_ms += std::chrono::duration<double, std::milli>(t3 - t0).count();
-        s->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+        s->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
     }
     s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
     return SILT_OK;
@@ -982,6 +1023,307 @@ int silt_set_fine_pace(silt_sheet* s, int32_t pace) {
 int silt_set_near_field(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     return silt::fine::set_near_field(s->fine, s, on != 0);
+}
+
+// ---------------------------------------------------------------- batched windows
+}  // extern "C"
+
+struct silt_batch {
+    std::vector<silt_sheet*> sheets;
+    cudaStream_t st = nullptr;
+    int device = 0;
+    int max_tiles = 0;              // the largest window's tile count per layer
+    int* list = nullptr;            // tile list of every window, and each entry's window
+    int* entry_win = nullptr;
+    int* count = nullptr;           // two count slots, used alternately by successive substeps
+    unsigned long long seq = 0;
+    silt::WindowSubstep* d_ws[2] = {nullptr, nullptr};
+    silt::WindowSubstep* h_ws[2] = {nullptr, nullptr};  // pinned
+    size_t ws_cap[2] = {0, 0};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int flip = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool, ev_used;  // groups of three: start, after force, after transport
+    silt_step_parts parts;
+    // Ledger gather: per window the depth sums and the books, one copy back.
+    const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
+    double* d_ledgers = nullptr;            // 5 doubles per window
+    double* h_ledgers = nullptr;            // pinned
+};
+
+namespace {
+
+int batch_free(silt_batch* b) {
+    if (!b) return SILT_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    cudaFree(b->list);
+    cudaFree(b->entry_win);
+    cudaFree(b->count);
+    cudaFree(b->d_ledger_src);
+    cudaFree(b->d_ledgers);
+    if (b->h_ledgers) cudaFreeHost(b->h_ledgers);
+    for (int k = 0; k < 2; ++k) {
+        cudaFree(b->d_ws[k]);
+        if (b->h_ws[k]) cudaFreeHost(b->h_ws[k]);
+        if (b->ev[k]) cudaEventDestroy(b->ev[k]);
+    }
+    for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->ev_used) cudaEventDestroy(e);
+    delete b;
+    return SILT_OK;
+}
+
+cudaEvent_t batch_event(silt_batch* b) {
+    cudaEvent_t e = nullptr;
+    if (b->ev_pool.empty()) {
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    } else {
+        e = b->ev_pool.back();
+        b->ev_pool.pop_back();
+    }
+    b->ev_used.push_back(e);
+    return e;
+}
+
+// The coarse pairs of every window, `launched` substeps at most, through the
+// batched list, speed, force and transport kernels.
+int batch_coarse(silt_batch* b, float dt) {
+    const int n = (int)b->sheets.size();
+    std::vector<CoarsePlan> plans(n);
+    int steps = 1;
+    bool device_count = false;
+    for (int w = 0; w < n; ++w) {
+        coarse_plan(b->sheets[w], dt, plans[w]);
+        steps = std::max(steps, plans[w].launched);
+        device_count = device_count || plans[w].sc.speed2 != nullptr;
+    }
+    const int slot = b->flip;
+    b->flip ^= 1;
+    const size_t need = (size_t)steps * n;
+    if (b->ev[slot]) CK(cudaEventSynchronize(b->ev[slot]));  // the descriptors two steps back are copied
+    if (need > b->ws_cap[slot]) {
+        cudaFree(b->d_ws[slot]);
+        if (b->h_ws[slot]) cudaFreeHost(b->h_ws[slot]);
+        b->d_ws[slot] = nullptr;
+        b->h_ws[slot] = nullptr;
+        b->ws_cap[slot] = 0;
+        CK(cudaMalloc(&b->d_ws[slot], need * sizeof(silt::WindowSubstep)));
+        CK(cudaMallocHost(&b->h_ws[slot], need * sizeof(silt::WindowSubstep)));
+        b->ws_cap[slot] = need;
+    }
+    if (!b->ev[slot]) CK(cudaEventCreateWithFlags(&b->ev[slot], cudaEventDisableTiming));
+    for (int k = 0; k < steps; ++k)
+        for (int w = 0; w < n; ++w) {
+            silt_sheet* s = b->sheets[w];
+            silt::WindowSubstep& D = b->h_ws[slot][(size_t)k * n + w];
+            memset(&D, 0, sizeof D);
+            if (k >= plans[w].launched) {
+                D.skip = 1;
+                continue;
+            }
+            int all = 0;
+            coarse_substep(s, plans[w], dt, k, D.F, D.T, all);
+            D.cur = s->cur;
+            D.all = all;
+            D.apply_cut = s->cut_pending ? 1 : 0;
+            D.zero_ledger = s->d_acc;
+            D.zero_bits = (k == 0 && D.F.sc.speed2) ? s->d_u32 : nullptr;
+            s->parts.force_launches += 1;
+            coarse_advance(s);
+        }
+    CK(cudaMemcpyAsync(b->d_ws[slot], b->h_ws[slot], need * sizeof(silt::WindowSubstep), cudaMemcpyHostToDevice,
+                       b->st));
+    CK(cudaEventRecord(b->ev[slot], b->st));
+    for (int k = 0; k < steps; ++k) {
+        const silt::WindowSubstep* d = b->d_ws[slot] + (size_t)k * n;
+        int* count = b->count + (b->seq & 1);
+        int* count_next = b->count + ((b->seq + 1) & 1);
+        ++b->seq;
+        CK(silt::launch_batch_tile_list(d, n, b->max_tiles, b->list, b->entry_win, count, count_next, b->st));
+        if (k == 0 && device_count) CK(silt::launch_batch_speed2(d, b->list, b->entry_win, count, b->st));
+        cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+        if (b->timing) {
+            e0 = batch_event(b);
+            e1 = batch_event(b);
+            e2 = batch_event(b);
+            if (!e0 || !e1 || !e2) return fail_cuda(cudaErrorMemoryAllocation, "batch timing events");
+            CK(cudaEventRecord(e0, b->st));
+        }
+        CK(silt::launch_batch_force(d, b->list, b->entry_win, count, b->st));
+        if (b->timing) CK(cudaEventRecord(e1, b->st));
+        CK(silt::launch_batch_transport(d, b->list, b->entry_win, count, b->st));
+        if (b->timing) CK(cudaEventRecord(e2, b->st));
+        b->parts.force_launches += 1;
+    }
+    for (int w = 0; w < n; ++w) b->sheets[w]->vmax_bound = silt::host::kSpeedCap * 1.4142137f;
+    return SILT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
+    if (!sheets || n <= 0 || !out) return fail_arg("batch");
+    *out = nullptr;
+    silt_batch* b = new silt_batch();
+    memset(&b->parts, 0, sizeof b->parts);
+    size_t tiles = 0;
+    for (int w = 0; w < n; ++w) {
+        silt_sheet* s = sheets[w];
+        if (!s) {
+            batch_free(b);
+            return fail_arg("batch: null sheet");
+        }
+        if (s->engine != SILT_ENGINE_GRID || !s->tile_mem) {
+            batch_free(b);
+            return fail_arg("batch: every sheet must step on the grid engine (SILT_ENGINE_GRID)");
+        }
+        if (w > 0 && (s->st != b->st || s->cfg.device != b->device)) {
+            batch_free(b);
+            return fail_arg("batch: every sheet must share one device and one stream");
+        }
+        if (w == 0) {
+            b->st = s->st;
+            b->device = s->cfg.device;
+        }
+        const int nt = s->tf.tiles_x * s->tf.tiles_x;
+        b->max_tiles = std::max(b->max_tiles, nt);
+        tiles += 2 * (size_t)nt;
+        b->sheets.push_back(s);
+    }
+    if (n > 65535) {
+        batch_free(b);
+        return fail_arg("batch: at most 65535 windows");
+    }
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaMalloc(&b->list, tiles * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->entry_win, tiles * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->count, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->count, 0, 2 * sizeof(int), b->st);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 5 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 5 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) {
+        std::vector<const double*> src(2 * (size_t)n);
+        for (int w = 0; w < n; ++w) {
+            src[w] = b->sheets[w]->d_acc;
+            src[n + w] = silt::fine::books(b->sheets[w]->fine);
+        }
+        e = cudaMemcpy(b->d_ledger_src, src.data(), src.size() * sizeof(double*), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return fail_cuda(e, "batch alloc");
+    }
+    *out = b;
+    return SILT_OK;
+}
+
+int silt_batch_destroy(silt_batch* b) { return batch_free(b); }
+
+int silt_batch_step(silt_batch* b, float dt) {
+    if (!b) return fail_arg("batch");
+    if (!(dt > 0.0f) || !std::isfinite(dt)) {
+        for (silt_sheet* s : b->sheets) s->pushes.clear();
+        return SILT_OK_NOOP;
+    }
+    const unsigned long long launches0 = silt::t_kernel_launches;
+    using clock = std::chrono::steady_clock;
+    const clock::time_point t0 = clock::now();
+    const int n = (int)b->sheets.size();
+    std::vector<std::vector<silt_tire_push>> ps(n);
+    std::vector<silt::fine::StepOut> fo(n);
+    int rc;
+    for (int w = 0; w < n; ++w)
+        if ((rc = step_before_coarse(b->sheets[w], dt, ps[w], fo[w]))) return rc;
+    const clock::time_point t1 = clock::now();
+    if ((rc = batch_coarse(b, dt))) return rc;
+    for (int w = 0; w < n; ++w) {
+        silt_sheet* s = b->sheets[w];
+        if ((rc = silt::fine::peel_coarse(s->fine, s, ps[w], fo[w]))) return rc;
+        s->parts.steps += 1;
+        s->ledger_fresh = true;
+    }
+    b->parts.steps += 1;
+    b->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
+    if (b->timing) {
+        const clock::time_point t2 = clock::now();
+        b->parts.host_step_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
+        b->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    return SILT_OK;
+}
+
+int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
+    if (!b || !out) return fail_arg("batch ledgers");
+    const int n = (int)b->sheets.size();
+    bool fresh = true;
+    for (silt_sheet* s : b->sheets) fresh = fresh && s->ledger_fresh;
+    if (!fresh) {  // before the first step: each window sums its planes
+        for (int w = 0; w < n; ++w) {
+            int rc = silt_get_ledger(b->sheets[w], out + w);
+            if (rc) return rc;
+        }
+        return SILT_OK;
+    }
+    CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
+    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 5 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    for (silt_sheet* s : b->sheets)
+        CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    for (int w = 0; w < n; ++w) {
+        silt_sheet* s = b->sheets[w];
+        int rc = check_substep_overflow(s);
+        if (rc) return rc;
+        const double* g = b->h_ledgers + 5 * (size_t)w;
+        const double area = (double)s->cfg.cell * (double)s->cfg.cell;
+        silt_ledger& L = out[w];
+        L.water_m3 = g[0] * area;
+        L.slurry_m3 = g[1] * area;
+        L.spray_m3 = g[2];
+        L.frozen_water_m3 = g[3];
+        L.frozen_slurry_m3 = g[4];
+        L.opened_m3 = s->opened_m3;
+        L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3;
+    }
+    return SILT_OK;
+}
+
+int silt_batch_set_timing(silt_batch* b, int32_t on) {
+    if (!b) return fail_arg("batch");
+    CK(cudaStreamSynchronize(b->st));
+    b->timing = on != 0;
+    memset(&b->parts, 0, sizeof b->parts);
+    for (cudaEvent_t e : b->ev_used) b->ev_pool.push_back(e);
+    b->ev_used.clear();
+    for (silt_sheet* s : b->sheets)
+        if (s->tile_mem) CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, b->st));
+    return SILT_OK;
+}
+
+int silt_batch_get_parts(silt_batch* b, silt_step_parts* out) {
+    if (!b || !out) return fail_arg("batch parts");
+    CK(cudaStreamSynchronize(b->st));
+    for (size_t k = 0; k + 2 < b->ev_used.size(); k += 3) {
+        float x = 0.0f, y = 0.0f;
+        CK(cudaEventElapsedTime(&x, b->ev_used[k], b->ev_used[k + 1]));
+        CK(cudaEventElapsedTime(&y, b->ev_used[k + 1], b->ev_used[k + 2]));
+        b->parts.force_ms += x;
+        b->parts.transport_ms += y;
+    }
+    for (cudaEvent_t e : b->ev_used) b->ev_pool.push_back(e);
+    b->ev_used.clear();
+    b->parts.force_cells = 0;
+    b->parts.force_cells_water = 0;
+    for (silt_sheet* s : b->sheets) {
+        unsigned long long stepped[2] = {0, 0};
+        CK(cudaMemcpy(stepped, s->d_u32 + 4, 16, cudaMemcpyDeviceToHost));
+        b->parts.force_cells += (int64_t)(stepped[0] + stepped[1]) * silt::GRID_TILE * silt::GRID_TILE;
+        b->parts.force_cells_water += (int64_t)stepped[0] * silt::GRID_TILE * silt::GRID_TILE;
+    }
+    *out = b->parts;
+    return SILT_OK;
 }
 
 // ---------------------------------------------------------------- free operator

@@ -106,6 +106,10 @@ def lib():
             "silt_step_sheet": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p, _p],
             "silt_set_step_timing": [_p, _i], "silt_get_step_parts": [_p, ctypes.POINTER(StepParts)],
             "silt_step_sheet_noalloc": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p],
+            "silt_batch_create": [ctypes.POINTER(_p), _i, ctypes.POINTER(_p)],
+            "silt_batch_destroy": [_p], "silt_batch_step": [_p, _f],
+            "silt_batch_get_ledgers": [_p, ctypes.POINTER(Ledger)],
+            "silt_batch_set_timing": [_p, _i], "silt_batch_get_parts": [_p, ctypes.POINTER(StepParts)],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -291,3 +295,39 @@ def step_sheet_device(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch,
     """The free one-sheet operator on device pointers (ints)."""
     return check(lib().silt_step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream),
                  "step_sheet")
+
+
+class Batch:
+    """Many windows stepped together: each Sheet (grid engine, one stream) keeps
+    its own state; step() advances them all, the coarse pairs through shared
+    launches (silt_batch_step)."""
+
+    def __init__(self, sheets):
+        self.sheets = list(sheets)
+        arr = (_p * len(self.sheets))(*[sh.h for sh in self.sheets])
+        h = _p()
+        check(lib().silt_batch_create(arr, len(self.sheets), ctypes.byref(h)), "batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().silt_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def step(self, dt):
+        return check(lib().silt_batch_step(self.h, dt), "batch_step")
+
+    def ledgers(self):
+        arr = (Ledger * len(self.sheets))()
+        check(lib().silt_batch_get_ledgers(self.h, arr), "batch_ledgers")
+        return [{k: getattr(x, k) for k, _ in Ledger._fields_} for x in arr]
+
+    def set_timing(self, on):
+        check(lib().silt_batch_set_timing(self.h, int(on)), "batch_set_timing")
+
+    def parts(self):
+        sp = StepParts()
+        check(lib().silt_batch_get_parts(self.h, ctypes.byref(sp)), "batch_parts")
+        return {k: getattr(sp, k) for k, _ in StepParts._fields_}

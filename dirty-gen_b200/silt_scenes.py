@@ -10,6 +10,8 @@ feeds to the sheet API (map_water_bed, lay_slurry_mask, read_substrate_grid):
 * grid -- the same bed noise on a large grid with eight seeded puddles
   (0.05..0.2 m deep, radius 2..8 m), plus four tires in a 1.5 m x 2.4 m
   rectangle driving +z and an inflow strip on row 0.
+* batch_windows -- many independent windows of log-uniform sides (64..512
+  cells), each a `grid` scene with its own seed, 1..4 puddles and 0..4 tires.
 
 The value noise is the reference's `hash01`/`relief_value`
 (src/fluid_core.rs:4639-4668) evaluated in float32.
@@ -150,3 +152,18 @@ def seed_core(core, scene):
     core.map_water_bed(scene["bed"], scene["water"])
     core.lay_slurry_mask(scene["slurry"], scene["slurry_grain"], scene["slurry_moisture"])
     core.read_substrate(scene["bed"], scene["moisture"], scene["grain"])
+
+
+def batch_windows(n=256, base_seed=0x9E3779B9, cell=0.2, lo=64, hi=512):
+    """Window k: side round(exp(U(ln lo, ln hi))), seed base_seed + k, 1..4
+    puddles and 0..4 tires (the first of tires_at's four)."""
+    rng = _rng(base_seed + 7)
+    out = []
+    for k in range(n):
+        side = int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+        puddles = int(rng.integers(1, 5))
+        tires = int(rng.integers(0, 5))
+        sc = grid(res=side, cell=cell, seed=base_seed + k, puddles=puddles)
+        sc["tires"] = tires
+        out.append(sc)
+    return out

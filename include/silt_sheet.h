@@ -181,6 +181,28 @@ typedef struct {
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
 
+/* ------------------------------------------------------- batched windows */
+/* Many independent windows stepped together (vehicles or scenes, each its own
+ * FluidCore in the reference, which steps them one after another). A batch
+ * groups sheets created with SILT_ENGINE_GRID on one device and one stream;
+ * each keeps its own state, seeding, tires, ledger and reads through the
+ * calls above. silt_batch_step(b, dt) equals silt_step(s, dt) on every sheet
+ * (same kernels and arithmetic), except that spray events are not returned
+ * (their volume still goes to each sheet's books): the nested patches and
+ * inflow run per sheet, then every window's coarse pair advances through one
+ * tile list and one launch of each grid kernel per substep. */
+typedef struct silt_batch silt_batch;
+int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out);
+int silt_batch_destroy(silt_batch* b);
+int silt_batch_step(silt_batch* b, float dt);
+/* Every window's ledger (out: one per window, in batch order) with one copy
+ * back and one wait, as silt_get_ledger gives them one at a time. */
+int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out);
+/* Device time of the batched force and transport launches, tiles stepped,
+ * launches and host time, as silt_get_step_parts reports for one sheet. */
+int silt_batch_set_timing(silt_batch* b, int32_t on);
+int silt_batch_get_parts(silt_batch* b, silt_step_parts* out);
+
 /* ------------------------------------------------------------------ knobs */
 /* FluidCore::set_fine_sub_cap / set_fine_pace (src/fluid_core.rs:5072, :5085). */
 int silt_set_fine_sub_cap(silt_sheet* s, float cap);

@@ -1,0 +1,68 @@
+"""Batched windows: silt_batch_step must give every window exactly what
+silt_step gives it alone (the same kernels and arithmetic; only the FP64
+ledger sums may differ in their last bits, from the order of the atomics)."""
+import numpy as np
+import pytest
+
+import silt_b200 as G
+import silt_scenes as S
+
+pytestmark = pytest.mark.gpu
+DT = 1.0 / 120.0
+
+
+def make(scene, fast=False, stream=None):
+    sh = G.Sheet(res=scene["res"], cell=0.2, fine_res=64, fine_cell=0.02, layout=G.FINE_PER_TIRE,
+                 engine=G.ENGINE_GRID, stream=stream)
+    S.seed_core(sh, scene)
+    if fast:
+        n = scene["res"] ** 2
+        sh.map_water_velocity(np.full(n, 14.0, np.float32), np.full(n, -3.0, np.float32))
+    return sh
+
+
+def push(sh, k, count):
+    for t in S.tires_at(k * DT, speed=5.0, z0=-3.0)[:count]:
+        sh.push_tire(**t)
+
+
+def test_batch_step_equals_single_steps():
+    scenes = [S.grid(res=r, seed=0x1234 + r, puddles=3) for r in (64, 96, 130, 200)]
+    opts = [dict(), dict(fast=True), dict(tires=True), dict(tires=True, fast=True)]
+    import torch
+
+    stream = torch.cuda.Stream()
+    alone = [make(sc, o.get("fast", False)) for sc, o in zip(scenes, opts)]
+    grouped = [make(sc, o.get("fast", False), stream.cuda_stream) for sc, o in zip(scenes, opts)]
+    batch = G.Batch(grouped)
+    for k in range(1, 25):
+        for w, o in enumerate(opts):
+            if o.get("tires"):
+                push(alone[w], k, 2 + w % 3)
+                push(grouped[w], k, 2 + w % 3)
+            alone[w].step(DT, want_spray=False)
+        batch.step(DT)
+    for w in range(len(scenes)):
+        for name in ("water", "slurry", "uw", "vw", "us", "vs"):
+            a, b = alone[w].get(name), grouped[w].get(name)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (w, name, float(np.abs(a - b).max()))
+        la, lb = alone[w].ledger(), grouped[w].ledger()
+        for key in ("water_m3", "slurry_m3", "spray_m3"):
+            assert abs(la[key] - lb[key]) <= 1e-12 * max(1.0, abs(la[key])), (w, key)
+    gathered = batch.ledgers()
+    for w in range(len(scenes)):
+        single = grouped[w].ledger()
+        for key in ("water_m3", "slurry_m3", "spray_m3", "frozen_water_m3", "opened_m3", "total_m3"):
+            assert gathered[w][key] == single[key], (w, key)
+    parts = batch.parts()
+    assert parts["steps"] == 24 and parts["launches"] > 0
+    batch.close()
+
+
+def test_batch_refuses_window_engine_sheets_and_mixed_streams():
+    sh = G.Sheet(res=64, engine=G.ENGINE_WINDOW)
+    with pytest.raises(G.SiltError):
+        G.Batch([sh])
+    a, b = G.Sheet(res=64, engine=G.ENGINE_GRID), G.Sheet(res=64, engine=G.ENGINE_GRID)
+    with pytest.raises(G.SiltError, match="one stream"):
+        G.Batch([a, b])
