@@ -18,6 +18,8 @@
 //   past a pass limit one thread runs the sweep itself.
 // * Fine sheets and the free operator's large boxes confine from a snapshot
 //   (Jacobi), as the reference does there.
+#include <algorithm>
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -64,6 +66,42 @@ struct Shared {
                 (void)g;                                                            \
                 __VA_ARGS__                                                         \
             }                                                                       \
+    }
+
+namespace cg = cooperative_groups;
+
+// A job is stepped by a cluster of CTAs (its crew). The step's phases split
+// the box rows over every warp of the crew and end at the cluster barrier
+// (release/acquire at cluster scope, so each phase sees the planes the crew
+// wrote in the one before). Work-box selection, the wet and CFL reductions
+// and the ledger read whole planes and run per CTA (identical in every CTA,
+// so the crew's control flow stays uniform) or on rank 0 alone.
+__device__ __forceinline__ int crew_rank() { return (int)cg::this_cluster().block_rank(); }
+__device__ __forceinline__ int crew_size() { return (int)cg::this_cluster().num_blocks(); }
+__device__ __forceinline__ void crew_sync() { cg::this_cluster().sync(); }
+
+// Every cell of the inclusive rectangle, shared by the crew: work items are
+// (row, 32-cell chunk) pairs dealt round-robin to the crew's warps, lanes
+// along x. Bodies may `continue` to the next cell.
+#define CLU_RECT(I0, I1, J0, J1, ...)                                                    \
+    {                                                                                    \
+        const int ri0_ = (I0), ri1_ = (I1), rj0_ = (J0), rj1_ = (J1);                    \
+        if (ri1_ >= ri0_ && rj1_ >= rj0_) {                                              \
+            const int ch_ = (ri1_ - ri0_ + 32) >> 5;                                     \
+            const int items_ = (rj1_ - rj0_ + 1) * ch_;                                  \
+            const int gs_ = crew_size() * (NT / 32);                                     \
+            for (int it_ = crew_rank() * (NT / 32) + (int)(threadIdx.x >> 5); it_ < items_; \
+                 it_ += gs_) {                                                           \
+                const int r_ = it_ / ch_;                                                \
+                const int j = rj0_ + r_;                                                 \
+                const int i = ri0_ + (it_ - r_ * ch_) * 32 + (int)(threadIdx.x & 31);   \
+                if (i <= ri1_) {                                                         \
+                    const int g = j * res + i;                                           \
+                    (void)g;                                                             \
+                    __VA_ARGS__                                                          \
+                }                                                                        \
+            }                                                                            \
+        }                                                                                \
     }
 
 __device__ __forceinline__ double block_sum_d(Shared& S, double v) {
@@ -146,10 +184,10 @@ __device__ __forceinline__ float tap5c(const float* line, int res, int i, float 
 // then the z pass into dst, which reads tmp rows outside the box as they are.
 __device__ void cta_blur(const float* __restrict__ src, float* __restrict__ dst, float* __restrict__ tmp, int res,
                          const Box& b, float k0, float k1, float k2) {
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, { tmp[g] = tap5c(src + j * res, res, i, k0, k1, k2, 1); })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, { dst[g] = tap5c(tmp + i, res, j, k0, k1, k2, res); })
-    __syncthreads();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, { tmp[g] = tap5c(src + j * res, res, i, k0, k1, k2, 1); })
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, { dst[g] = tap5c(tmp + i, res, j, k0, k1, k2, res); })
+    crew_sync();
 }
 
 __device__ __forceinline__ float job_nu(const Job& J, int g) {
@@ -184,21 +222,21 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     float* __restrict__ F2 = J.f2;
     const float cell = J.cell;
     const uint8_t* __restrict__ gate = J.gate;
-    CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
+    CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
         float speed = 0.5f * (U[g] + U[g + 1]);
         float dh = open_edge_dh(false, h[g + 1], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
         float speed = 0.5f * (U[g] + U[g + 1]);
         float prev = i > b.i0 ? F1[g - 1] : 0.0f;
         float dh = open_edge_dh(false, h[g], h[g + 1], 0.0f + prev, gate ? gate[g + 1] : 1, 0.0f, 0.0f, speed, dt,
                                 cell, 0.45f);
         F2[g] = speed > 0.0f ? dh : 0.0f;
     })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         float flm = i > b.i0 ? F1[g - 1] : 0.0f, frm = i > b.i0 ? F2[g - 1] : 0.0f;
         float flc = i < b.i1 ? F1[g] : 0.0f, frc = i < b.i1 ? F2[g] : 0.0f;
         float rem = (0.0f + flm) + frc, add = (0.0f + frm) + flc;
@@ -206,22 +244,22 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
         float moved = fmaxf(hv - rem + add, 0.0f);
         h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
     })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
         float speed = 0.5f * (V[g] + V[g + res]);
         float dh = open_edge_dh(false, h[g + res], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
         float speed = 0.5f * (V[g] + V[g + res]);
         float ra = j > b.j0 ? 0.0f + F1[g - res] : 0.0f;
         float dh = open_edge_dh(false, h[g], h[g + res], ra, gate ? gate[g + res] : 1, 0.0f, 0.0f, speed, dt, cell,
                                 0.45f);
         F2[g] = speed > 0.0f ? dh : 0.0f;
     })
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         float upm = j > b.j0 ? F1[g - res] : 0.0f, dnm = j > b.j0 ? F2[g - res] : 0.0f;
         float upc = j < b.j1 ? F1[g] : 0.0f, dnc = j < b.j1 ? F2[g] : 0.0f;
         float rem = (0.0f + upm) + dnc, add = (0.0f + dnm) + upc;
@@ -229,7 +267,7 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
         float moved = fmaxf(hv - rem + add, 0.0f);
         h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
     })
-    __syncthreads();
+    crew_sync();
 }
 
 __device__ void cta_dry_cut(const Job& J, const Box& b) {
@@ -239,14 +277,14 @@ __device__ void cta_dry_cut(const Job& J, const Box& b) {
     float* __restrict__ h = J.h;
     float* __restrict__ u = J.u;
     float* __restrict__ v = J.v;
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (h[g] < eps) {
             h[g] = 0.0f;
             u[g] = 0.0f;
             v[g] = 0.0f;
         }
     })
-    __syncthreads();
+    crew_sync();
 }
 
 // The confinement kick at (i, j) from the velocities `uu`, `vv` return for
@@ -286,13 +324,13 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
     {
         const int x0 = max(b.i0 - 2, 0), x1 = min(b.i1 + 2, res - 1), y0 = max(b.j0 - 2, 0),
                   y1 = min(b.j1 + 2, res - 1);
-        CTA_RECT(x0, x1, y0, y1, {
+        CLU_RECT(x0, x1, y0, y1, {
             U0[g] = J.u[g];
             V0[g] = J.v[g];
         })
     }
-    __syncthreads();
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    crew_sync();
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (J.h[g] > eps) {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float px = (p[j * res + ip] - p[j * res + im]) / two;
@@ -306,16 +344,19 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
             J.v[g] = vg;
         }
     })
-    __syncthreads();
+    crew_sync();
     if (!(J.vort > 0.0f)) return 0;
     // Fixed point of the sweep: cells before (i, j) in raster order read their
     // final values, (i, j) itself its post-gravity value, cells after it their
     // pre-gravity values.
+    // A pass ends when the whole crew has passed the barrier; its verdict is
+    // the OR of every CTA's flag, read from their shared memory.
+    cg::cluster_group crew = cg::this_cluster();
     int passes = 0;
     for (; passes < GS_MAX_PASSES; ++passes) {
         if (threadIdx.x == 0) S.changed = 0;
-        __syncthreads();
-        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        crew_sync();
+        CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             if (J.h[g] > eps) {
                 auto pick = [&](const float* X, const float* G0, const float* SG, int a, int c) {
                     if (a == i && c == j) return SG[g];
@@ -337,13 +378,15 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
                 }
             }
         })
-        __syncthreads();
-        if (!S.changed) break;
-        __syncthreads();
+        crew_sync();
+        int any = 0;
+        for (int r = 0; r < crew_size(); ++r) any |= *crew.map_shared_rank(&S.changed, r);
+        crew_sync();  // every CTA has read the flags before the next pass clears them
+        if (!any) break;
     }
     if (passes < GS_MAX_PASSES) return passes + 1;
-    // Pass limit reached: the sweep itself, in raster order, on one thread.
-    if (threadIdx.x == 0) {
+    // Pass limit reached: the sweep itself, in raster order, on one thread of the crew.
+    if (crew_rank() == 0 && threadIdx.x == 0) {
         for (int j = b.j0; j <= b.j1; ++j)
             for (int i = b.i0; i <= b.i1; ++i) {
                 const int g = j * res + i;
@@ -365,7 +408,7 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
                 }
             }
     }
-    __syncthreads();
+    crew_sync();
     return -1;
 }
 
@@ -378,7 +421,7 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
     const float* __restrict__ H = J.h;
     float* __restrict__ U = J.u;
     float* __restrict__ V = J.v;
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (H[g] > eps) {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float px = (p[j * res + ip] - p[j * res + im]) / two;
@@ -388,22 +431,22 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
             V[g] += -kGravity * pz * mob * dt;
         }
     })
-    __syncthreads();
+    crew_sync();
     if (!(J.vort > 0.0f)) return;
     float* __restrict__ W = J.f1;
     {
         const int wi0 = max(b.i0 - 1, 0), wi1 = min(b.i1 + 1, res - 1);
         const int wj0 = max(b.j0 - 1, 0), wj1 = min(b.j1 + 1, res - 1);
-        CTA_RECT(wi0, wi1, wj0, wj1, {
+        CLU_RECT(wi0, wi1, wj0, wj1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float dvdx = (V[j * res + ip] - V[j * res + im]) / two;
             float dudz = (U[jp * res + i] - U[jm * res + i]) / two;
             W[g] = dvdx - dudz;
         })
     }
-    __syncthreads();
+    crew_sync();
     const float vort = J.vort;
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (H[g] > eps) {
             float w = W[g];
             if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
@@ -421,7 +464,7 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
             }
         }
     })
-    __syncthreads();
+    crew_sync();
 }
 
 // substep (src/fluid_core.rs:1879-2082), open sheet, gravity drive.
@@ -440,16 +483,16 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
         const float* __restrict__ H = J.h;
         const int hi0 = max(b.i0 - 2, 0), hi1 = min(b.i1 + 2, res - 1);
         const int hj0 = max(b.j0 - 2, 0), hj1 = min(b.j1 + 2, res - 1);
-        CTA_RECT(hi0, hi1, hj0, hj1, { sa[g] = bed[g] + H[g]; })
+        CLU_RECT(hi0, hi1, hj0, hj1, { sa[g] = bed[g] + H[g]; })
     }
-    __syncthreads();
+    crew_sync();
     cta_blur(sa, sb, se, res, b, kG0, kG1, kG2);
     cta_blur(sa, scc, se, res, b, kS0, kS1, kS2);
-    CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         float filtered = 0.62f * sb[g] + 0.38f * scc[g];
         sd[g] = 0.45f * filtered + 0.55f * sa[g];
     })
-    __syncthreads();
+    crew_sync();
     const bool par = (b.j1 - b.j0 >= 47) && (b.i1 - b.i0 >= 31) && inner_par;
     int passes = 0;
     if (fine || par)
@@ -458,7 +501,7 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
         passes = cta_gravity_gs(S, J, b, sd, dt);
     const bool project = !fine;
     if (project) {
-        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
             float ux = (J.u[j * res + ip] - J.u[j * res + im]) / (2.0f * cell);
             float vz = (J.v[jp * res + i] - J.v[jm * res + i]) / (2.0f * cell);
@@ -468,17 +511,17 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
             float overload = 1.0f + rclamp(job_nu(J, g) / 231.0f, 0.0f, 6.0f);
             sb[g] = div * overload - 0.015f * overload * lap_h;
         })
-        __syncthreads();
+        crew_sync();
         cta_blur(sb, scc, se, res, b, kG0, kG1, kG2);
         cta_blur(sb, sa, se, res, b, kS0, kS1, kS2);
-        CTA_RECT(b.i0, b.i1, b.j0, b.j1, { sd[g] = 0.62f * scc[g] + 0.38f * sa[g]; })
-        __syncthreads();
+        CLU_RECT(b.i0, b.i1, b.j0, b.j1, { sd[g] = 0.62f * scc[g] + 0.38f * sa[g]; })
+        crew_sync();
     }
     {
         const float* __restrict__ H = J.h;
         float* __restrict__ U = J.u;
         float* __restrict__ V = J.v;
-        CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+        CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             if (H[g] > eps) {
                 float uu = U[g], vv = V[g];
                 if (project) {
@@ -495,7 +538,7 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
             }
         })
     }
-    __syncthreads();
+    crew_sync();
     if (do_flux) {
         cta_transport(J, b, dt);
         cta_dry_cut(J, b);
@@ -799,7 +842,7 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
 // soften_border (src/fluid_core.rs:9594-9622) on the whole layer.
 __device__ void cta_soften(const Job& J) {
     const int res = J.res, edge = J.soften_edge;
-    CTA_RECT(0, res - 1, 0, res - 1, {
+    CLU_RECT(0, res - 1, 0, res - 1, {
         int d = min(min(i, res - 1 - i), min(j, res - 1 - j));
         if (d < edge) {
             float t = (float)d / (float)edge;
@@ -808,15 +851,16 @@ __device__ void cta_soften(const Job& J) {
             J.v[g] *= w;
         }
     })
-    __syncthreads();
+    crew_sync();
 }
 
+// The layer's FP64 depth sum; each CTA sums the whole plane, rank 0 writes it.
 __device__ void cta_ledger(Shared& S, const Job& J) {
     const int res = J.res;
     double part = 0.0;
     CTA_RECT(0, res - 1, 0, res - 1, { part += (double)fmaxf(J.h[g], 0.0f); })
     part = block_sum_d(S, part);
-    if (threadIdx.x == 0 && J.ledger) *J.ledger = part;
+    if (threadIdx.x == 0 && J.ledger && crew_rank() == 0) *J.ledger = part;
 }
 
 // step_sheet_eps_in + step_sheet_scratch (src/fluid_core.rs:821-852, :1659-1831).
@@ -826,7 +870,7 @@ __device__ int window_body(Shared& S, const Job& J) {
     const int res = J.res;
     const float eps = J.eps;
     if (J.soften_edge > 0) cta_soften(J);
-    // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844).
+    // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844), per CTA.
     double ws = 0.0;
     CTA_RECT(0, res - 1, 0, res - 1, {
         float hv = J.h[g];
@@ -841,10 +885,22 @@ __device__ int window_body(Shared& S, const Job& J) {
     const bool fine_open = open_fine && J.pace == 0;
     const bool whole_wet = open_fine && (J.pace == 2 || J.pace == 3);
     const bool awake = open_fine && !whole_wet && !fine_open;
-    if (fine_open || awake)
-        cta_awake_boxes(S, J);
-    else
-        cta_wet_boxes(S, J);
+    // Work boxes on rank 0 (the wet-body labels use a global plane), then
+    // every other CTA copies them from its shared memory.
+    if (crew_rank() == 0) {
+        if (fine_open || awake)
+            cta_awake_boxes(S, J);
+        else
+            cta_wet_boxes(S, J);
+    }
+    crew_sync();
+    if (crew_rank() != 0) {
+        const Shared* S0 = cg::this_cluster().map_shared_rank(&S, 0);
+        const int n0 = S0->nbox;
+        for (int k = threadIdx.x; k < 4 * n0; k += NT) S.bbox[k / n0][k % n0] = S0->bbox[k / n0][k % n0];
+        if (threadIdx.x == 0) S.nbox = n0;
+        __syncthreads();
+    }
     const int nb = S.nbox;
     if (nb <= 0) {
         cta_ledger(S, J);
@@ -896,56 +952,76 @@ __device__ int window_body(Shared& S, const Job& J) {
     return gs_passes;
 }
 
-// Planes a small window keeps in shared memory: h, u, v, the first scratch
-// set (a..e) and the two transient planes.
-constexpr int SMEM_PLANES = 10;
-constexpr int SMEM_CARRIED = 8;  // h, u, v and the scratch set come in and go back out
-
-__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs, int smem_cells) {
-    extern __shared__ float wsm[];
+__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
     __shared__ Shared S;
-    Job J = jobs[blockIdx.x];
-    if (!J.active) return;
-    const int n = J.res * J.res;
-    // A window that fits runs on shared-memory copies of its planes: every
-    // phase of the step then waits on shared memory instead of L2. The
-    // scratch set keeps its values between steps, so it travels both ways.
-    const bool local = n <= smem_cells;
-    float* carried[SMEM_CARRIED] = {J.h, J.u, J.v, J.sc[0][0], J.sc[0][1], J.sc[0][2], J.sc[0][3], J.sc[0][4]};
-    if (local) {
-#pragma unroll
-        for (int q = 0; q < SMEM_CARRIED; ++q)
-            for (int c = threadIdx.x; c < n; c += NT) wsm[(size_t)q * n + c] = carried[q][c];
-        J.h = wsm;
-        J.u = wsm + n;
-        J.v = wsm + 2 * (size_t)n;
-        for (int a = 0; a < 5; ++a) J.sc[0][a] = wsm + (size_t)(3 + a) * n;
-        J.f1 = wsm + 8 * (size_t)n;
-        J.f2 = wsm + 9 * (size_t)n;
-        __syncthreads();
+    __shared__ Job Js;
+    const int job = (int)(blockIdx.x / (unsigned)crew_size());
+    // The job's fields live in shared memory for the step: every phase reads
+    // them, and a copy on the thread's stack would be reloaded from local
+    // memory after each store through a plane pointer.
+    if (threadIdx.x == 0) Js = jobs[job];
+    __syncthreads();
+    if (!Js.active) return;  // the same for the whole crew
+    const int gs_passes = window_body(S, Js);
+    if (threadIdx.x == 0 && crew_rank() == 0) jobs[job].gs_iters = gs_passes;
+    crew_sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// CTAs per job: enough warps for one (row, 32-cell chunk) item each on a
+// 64-cell patch, up to the portable cluster size.
+static int crew_for(int max_res) {
+    const int items = max_res * ((max_res + 31) / 32);
+    int c = items / (NT / 32);
+    if (c < 1) c = 1;
+    if (c > 8) c = 8;
+    return c;
+}
+
+// The largest crew the device can hold at once (a cluster of full-SM CTAs).
+static int crew_limit(cudaStream_t st) {
+    static int limit = 0;
+    if (limit > 0) return limit;
+    for (int c = 8; c >= 1; --c) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)c, 1, 1);
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_window_step, &cfg) == cudaSuccess && n > 0) {
+            limit = c;
+            return limit;
+        }
+        cudaGetLastError();
     }
-    const int gs_passes = window_body(S, J);
-    if (local) {
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < SMEM_CARRIED; ++q)
-            for (int c = threadIdx.x; c < n; c += NT) carried[q][c] = wsm[(size_t)q * n + c];
-    }
-    if (threadIdx.x == 0) jobs[blockIdx.x].gs_iters = gs_passes;
+    limit = 1;
+    return limit;
 }
 
 cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st) {
     if (njobs <= 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_window_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(sizeof(float) * SMEM_PLANES * SMEM_RES * SMEM_RES));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    const int cells = max_res <= SMEM_RES ? max_res * max_res : 0;
-    k_window_step<<<njobs, NT, sizeof(float) * SMEM_PLANES * (size_t)cells, st>>>(const_cast<Job*>(d_jobs), cells);
+    const int crew = std::min(crew_for(max_res), crew_limit(st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(njobs * crew), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)crew;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step, const_cast<Job*>(d_jobs));
     ::silt::count_launch();
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -44,9 +44,8 @@ struct Job {
     int32_t gs_iters;      // out: Gauss-Seidel passes used by the last box (diagnostics)
 };
 
-// Windows up to SMEM_RES cells per side step on shared-memory copies of
-// their planes. `max_res` is the largest window side among the jobs.
-constexpr int SMEM_RES = 64;
+// One cluster of CTAs steps each job, its size chosen from `max_res`, the
+// largest window side among the jobs.
 cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st);
 size_t window_static_smem();
 
