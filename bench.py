@@ -139,18 +139,29 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per k_force launch from the committed ncu summary, scaled to this grid."""
+    """DRAM bytes per algorithmic byte of k_force, from the committed ncu summary
+    (a capture whose algorithmic bytes are exact: every tile stepped)."""
     path = os.path.join(ROOT, "profiles", "k_force_grid_traffic.txt")
     try:
-        vals = {}
         for ln in open(path):
-            if ":" in ln:
-                k, v = ln.split(":", 1)
-                vals[k.strip()] = v.strip()
-        per_cell = float(vals["dram_bytes_per_cell"])
-        return per_cell
-    except (OSError, KeyError, ValueError):
-        return None
+            if ln.startswith("dram_bytes_per_algorithmic_byte:"):
+                return float(ln.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def host_cpu():
+    """The host CPU the CPU legs ran on: model name and logical cores."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
 
 
 def cpu_threads(args):
@@ -310,7 +321,9 @@ def run_b200(args):
         per_cell = profiled_traffic()
         roof = {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                "traffic": per_cell * args.res * args.res if per_cell else None,
+                "traffic": per_cell * force_bytes if per_cell else None,
+                "traffic_basis": "ncu ratio of DRAM bytes to algorithmic bytes on a 1024^2 launch with every "
+                                 "tile stepped, times this launch's algorithmic bytes",
                 "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms,
                 "stepped_cell_layers_per_launch": cw + cs,
                 "active_fraction": (cw + cs) / (2.0 * args.res * args.res),
@@ -401,7 +414,7 @@ def batch_cpu(args, wins, max_steps, warmup, budget_s):
         steps += 1
         el = time.perf_counter() - t0
     value = batch_cells(sample) * steps / el
-    return {"value": value, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
+    return {"value": value, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el, "host": host_cpu(),
             "sample": f"{len(sample)} of the {len(wins)} windows (every 16th), {steps} steps after "
                       f"{max(1, warmup)} warm-up step(s), one window at a time, each pair on 2 threads ({el:.2f} s)"}
 
@@ -588,6 +601,7 @@ def run_window200(args):
             el = time.perf_counter() - t0
         v = res * res * steps / el
         base = {"value": v, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
+                "host": host_cpu(), "host": host_cpu(),
                 "sample": f"{steps} steps after {max(1, args.warmup)} warm-up, the pair on 2 threads ({el:.2f} s)"}
         print(json.dumps({"metric": "cell-steps/s", "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
                           "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": 1000.0 * el / steps,
@@ -644,6 +658,7 @@ def run_window200(args):
             core.step(DT)
         el = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": res * res * 20 / el, "unit": "cell-steps/s", "cores": 2, "kind": "port",
+                                "host": host_cpu(),
                                 "sample": f"20 steps after 1 warm-up, the pair on 2 threads ({el:.2f} s)"}
     print(json.dumps(line), flush=True)
     sheet.close()
