@@ -198,7 +198,7 @@ def cpu_baseline(args, scene, max_steps=40, warmup=1, budget_s=20.0):
     fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
     value = (args.res * args.res + fine_cells) * steps / el
     return {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-            "steps": steps, "seconds": el,
+            "steps": steps, "seconds": el, "host": host_cpu(),
             "sample": f"{steps} steps of the same {args.res}^2 workload after {max(1, warmup)} warm-up step(s); "
                       f"coarse pair on 2 threads, fine patch sheets on {threads} ({el:.2f} s)"}
 
