@@ -129,6 +129,7 @@ struct Impl {
     int* free_stack = nullptr;
     int* counters = nullptr;          // [0] free top, [1] live tiles, [2] overflow, [3] spray count
     bool near_maybe = false;
+    bool spray_dirty = false;         // the spray count may be non-zero (a step with tires ran)
     // Spray.
     SprayRec* spray = nullptr;
     double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3
@@ -1218,10 +1219,14 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     if (rc) return rc;
     SheetView W = view_of(s);
     if (ps.empty()) {
-        FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
+        if (M.spray_dirty) {
+            FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));
+            M.spray_dirty = false;
+        }
         return fade_only(P, s, dt);
     }
     // With tires, k_refine_lay clears the spray count.
+    M.spray_dirty = true;
     // The coarse planes may still wait for the previous dry cut: the lay,
     // restrict and shove kernels apply it to the cells they touch.
     if ((rc = lay_patches(P, s, ps, dt))) return rc;

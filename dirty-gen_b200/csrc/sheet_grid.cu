@@ -23,6 +23,7 @@
 // no flux and no force. The full-grid pass therefore gives the reference's
 // depths and velocities on every cell that holds fluid.
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "sheet_grid.cuh"
@@ -776,11 +777,8 @@ cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, cons
 
 cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
                                cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_batch_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
-        attr = true;
-    }
+    static std::once_flag attr;
+    std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
     k_batch_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
@@ -788,23 +786,16 @@ cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const
 
 cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
                                    const int* count, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_batch_transport, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)transport_smem_bytes());
-        attr = true;
-    }
+    static std::once_flag attr;
+    std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
     k_batch_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
-        attr = true;
-    }
+    static std::once_flag attr;
+    std::call_once(attr, [] { cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
     (void)res;
     (void)layers;
     k_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(L);
@@ -813,11 +804,8 @@ cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t
 }
 
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes());
-        attr = true;
-    }
+    static std::once_flag attr;
+    std::call_once(attr, [] { cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
     (void)res;
     (void)layers;
     k_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);

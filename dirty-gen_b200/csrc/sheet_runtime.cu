@@ -13,7 +13,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -1028,8 +1032,71 @@ int silt_set_near_field(silt_sheet* s, int32_t on) {
 // ---------------------------------------------------------------- batched windows
 }  // extern "C"
 
+// Host threads for the per-window parts of a batched step (tire pushes,
+// inflow, the nested patches: host planning and a dozen small launches per
+// window with tires). Each worker owns a stream; its windows' work goes there
+// between an event from the batch stream and one back to it.
+struct BatchWorkers {
+    std::vector<std::thread> threads;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> done;
+    std::vector<int> rc;
+    std::vector<std::string> err;
+    std::vector<unsigned long long> launches;
+    std::mutex m;
+    std::condition_variable go, finished;
+    std::function<void(int)> job;
+    unsigned long long gen = 0;
+    int pending = 0;
+    bool quit = false;
+    int device = 0;
+
+    void loop(int k) {
+        cudaSetDevice(device);
+        unsigned long long seen = 0;
+        for (;;) {
+            std::function<void(int)> f;
+            {
+                std::unique_lock<std::mutex> lk(m);
+                go.wait(lk, [&] { return quit || gen != seen; });
+                if (quit) return;
+                seen = gen;
+                f = job;
+            }
+            const unsigned long long l0 = silt::t_kernel_launches;
+            f(k);
+            {
+                std::lock_guard<std::mutex> lk(m);
+                launches[k] += silt::t_kernel_launches - l0;
+                if (--pending == 0) finished.notify_all();
+            }
+        }
+    }
+    // Runs f(k) on every worker and returns when all are done.
+    void run(std::function<void(int)> f) {
+        std::unique_lock<std::mutex> lk(m);
+        job = std::move(f);
+        pending = (int)threads.size();
+        ++gen;
+        go.notify_all();
+        finished.wait(lk, [&] { return pending == 0; });
+    }
+    ~BatchWorkers() {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            quit = true;
+        }
+        go.notify_all();
+        for (auto& t : threads) t.join();
+        for (cudaStream_t st : streams) cudaStreamDestroy(st);
+        for (cudaEvent_t e : done) cudaEventDestroy(e);
+    }
+};
+
 struct silt_batch {
     std::vector<silt_sheet*> sheets;
+    BatchWorkers* workers = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_coarse = nullptr;
     cudaStream_t st = nullptr;
     int device = 0;
     int max_tiles = 0;              // the largest window's tile count per layer
@@ -1056,6 +1123,9 @@ namespace {
 int batch_free(silt_batch* b) {
     if (!b) return SILT_OK;
     if (b->st) cudaStreamSynchronize(b->st);
+    delete b->workers;
+    if (b->ev_start) cudaEventDestroy(b->ev_start);
+    if (b->ev_coarse) cudaEventDestroy(b->ev_coarse);
     cudaFree(b->list);
     cudaFree(b->entry_win);
     cudaFree(b->count);
@@ -1212,6 +1282,29 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
         }
         e = cudaMemcpy(b->d_ledger_src, src.data(), src.size() * sizeof(double*), cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_coarse, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+        unsigned hw = std::thread::hardware_concurrency();
+        const int k = std::max(1, std::min({8, (int)(hw ? hw : 1), n}));
+        BatchWorkers* W = new BatchWorkers();
+        W->device = b->device;
+        b->workers = W;
+        for (int q = 0; q < k && e == cudaSuccess; ++q) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (st) W->streams.push_back(st);
+            if (ev) W->done.push_back(ev);
+        }
+        if (e == cudaSuccess) {
+            W->rc.assign(k, 0);
+            W->err.assign(k, std::string());
+            W->launches.assign(k, 0);
+            for (int q = 0; q < k; ++q) W->threads.emplace_back([W, q] { W->loop(q); });
+        }
+    }
     if (e != cudaSuccess) {
         batch_free(b);
         return fail_cuda(e, "batch alloc");
@@ -1234,19 +1327,56 @@ int silt_batch_step(silt_batch* b, float dt) {
     const int n = (int)b->sheets.size();
     std::vector<std::vector<silt_tire_push>> ps(n);
     std::vector<silt::fine::StepOut> fo(n);
+    BatchWorkers& Wk = *b->workers;
+    const int nk = (int)Wk.threads.size();
+    // One window's part before (phase 0) or after (phase 1) the coarse pairs,
+    // on worker k's stream in place of the sheet's own.
+    auto per_window = [&](int phase, cudaEvent_t after) {
+        Wk.run([&, phase, after](int k) {
+            Wk.rc[k] = 0;
+            cudaStream_t wst = Wk.streams[k];
+            cudaError_t e = cudaStreamWaitEvent(wst, after, 0);
+            for (int w = k; w < n && e == cudaSuccess && Wk.rc[k] == 0; w += nk) {
+                silt_sheet* s = b->sheets[w];
+                if (phase == 1 && ps[w].empty()) continue;
+                cudaStream_t own = s->st;
+                s->st = wst;
+                Wk.rc[k] = phase == 0 ? step_before_coarse(s, dt, ps[w], fo[w])
+                                      : silt::fine::peel_coarse(s->fine, s, ps[w], fo[w]);
+                s->st = own;
+                if (Wk.rc[k]) Wk.err[k] = silt_last_error();
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(Wk.done[k], wst);
+            if (e != cudaSuccess && Wk.rc[k] == 0) {
+                Wk.rc[k] = SILT_ECUDA;
+                Wk.err[k] = std::string("batch worker: ") + cudaGetErrorString(e);
+            }
+        });
+        for (int k = 0; k < nk; ++k) {
+            if (Wk.rc[k]) {
+                snprintf(g_err, sizeof g_err, "%s", Wk.err[k].c_str());
+                return Wk.rc[k];
+            }
+        }
+        for (int k = 0; k < nk; ++k) CK(cudaStreamWaitEvent(b->st, Wk.done[k], 0));
+        return SILT_OK;
+    };
     int rc;
-    for (int w = 0; w < n; ++w)
-        if ((rc = step_before_coarse(b->sheets[w], dt, ps[w], fo[w]))) return rc;
+    for (auto& c : Wk.launches) c = 0;
+    CK(cudaEventRecord(b->ev_start, b->st));
+    if ((rc = per_window(0, b->ev_start))) return rc;
     const clock::time_point t1 = clock::now();
     if ((rc = batch_coarse(b, dt))) return rc;
+    CK(cudaEventRecord(b->ev_coarse, b->st));
+    if ((rc = per_window(1, b->ev_coarse))) return rc;
     for (int w = 0; w < n; ++w) {
         silt_sheet* s = b->sheets[w];
-        if ((rc = silt::fine::peel_coarse(s->fine, s, ps[w], fo[w]))) return rc;
         s->parts.steps += 1;
         s->ledger_fresh = true;
     }
     b->parts.steps += 1;
     b->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
+    for (auto c : Wk.launches) b->parts.launches += (int64_t)c;
     if (b->timing) {
         const clock::time_point t2 = clock::now();
         b->parts.host_step_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();

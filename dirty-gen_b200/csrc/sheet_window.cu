@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cooperative_groups.h>
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "sheet_math.cuh"
@@ -978,9 +979,7 @@ static int crew_for(int max_res) {
 }
 
 // The largest crew the device can hold at once (a cluster of full-SM CTAs).
-static int crew_limit(cudaStream_t st) {
-    static int limit = 0;
-    if (limit > 0) return limit;
+static int crew_limit_query(cudaStream_t st) {
     for (int c = 8; c >= 1; --c) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)c, 1, 1);
@@ -994,13 +993,16 @@ static int crew_limit(cudaStream_t st) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_window_step, &cfg) == cudaSuccess && n > 0) {
-            limit = c;
-            return limit;
-        }
+        if (cudaOccupancyMaxActiveClusters(&n, k_window_step, &cfg) == cudaSuccess && n > 0) return c;
         cudaGetLastError();
     }
-    limit = 1;
+    return 1;
+}
+
+static int crew_limit(cudaStream_t st) {
+    static std::once_flag once;
+    static int limit = 1;
+    std::call_once(once, [st] { limit = crew_limit_query(st); });
     return limit;
 }
 
