@@ -787,6 +787,7 @@ struct StepPlan {
     size_t off_refs = 0, off_held = 0, off_oidx = 0, off_oval = 0, off_near = 0, off_ent = 0, off_seg = 0;
     std::vector<JobList> fine_push, fine_peel;
     JobList coarse_push, coarse_peel;
+    std::vector<int> coarse_pushed;   // tires that shove coarse cells (their cell is not held)
     size_t off_push_groups = 0, off_peel_groups = 0;
     int n_push_groups = 0, n_peel_groups = 0, push_cells_max = 0, peel_cells_max = 0;
     int slot = 0;
@@ -1038,6 +1039,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
             long cj = coarse_axis(W.origin[1], W.cell, res, ps[q].z);
             if (ci >= 0 && cj >= 0 && M.h_owner[cj * res + ci] >= 0) continue;
             push.push_back(make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, push_reach(ps[q], W.cell)));
+            L.coarse_pushed.push_back((int)q);
         }
         L.coarse_push = job_list(tab, push);
         L.coarse_peel = job_list(tab, peel);
@@ -1259,16 +1261,22 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    // A shove changes a cell's speed by at most 1.04 max(speed, 0.4)
-    // (|fore f + 0.28 flank r| <= sqrt(1 + 0.28^2)); shoves add up only where
-    // the tires' spans overlap.
+    // The coarse speed bound after this step's coupling. The restrict hands
+    // each column a depth-weighted mean of its fine cells' velocities and its
+    // own, so it adds nothing above the largest fine speed; after the patch
+    // step every wet fine cell faster than 0.05 m/s lies in a work box and is
+    // clamped to the film cap, and drier cells carry only the laid coarse
+    // velocity (shoves need 4 mm of depth). So only the shoves of tires
+    // outside the patches raise it: each by at most 1.04 max(speed, 0.4)
+    // (|fore f + 0.28 flank r| <= sqrt(1 + 0.28^2)), summed where the tires'
+    // spans overlap.
     float add = 0.0f;
-    for (size_t a = 0; a < ps.size(); ++a) {
+    for (int a : L.coarse_pushed) {
         float reach_a = push_reach(ps[a], W.cell);
         auto ai = index_span(W.origin[0], W.cell, W.res, ps[a].x, reach_a);
         auto aj = index_span(W.origin[1], W.cell, W.res, ps[a].z, reach_a);
         float sum = 0.0f;
-        for (size_t b = 0; b < ps.size(); ++b) {
+        for (int b : L.coarse_pushed) {
             float reach_b = push_reach(ps[b], W.cell);
             auto bi = index_span(W.origin[0], W.cell, W.res, ps[b].x, reach_b);
             auto bj = index_span(W.origin[1], W.cell, W.res, ps[b].z, reach_b);
