@@ -6,20 +6,24 @@
 // and which tire shoves which grid. Those small tables go to the device in
 // one copy; the kernels below then move all cell data on the device:
 //
-//   k_refine_lay    coarse -> fine copy of held columns, free-surface bed elsewhere
-//   k_zero_cells    empty the held coarse columns
-//   k_near_apply    lay the kept 10x10 residual tiles back on the patch
-//   k_near_fade     age tiles whose column is not held; recycle dropped slots
-//   k_push_cells    tire shove on velocity, pushes applied in call order
-//   (sheet_patch.cu k_patch_step: the fine sheet step itself)
-//   k_peel          spray peeled off the water, events queued on the device
-//   k_near_capture  residual tiles of held columns
-//   k_restrict      volume- and momentum-weighted sum back into the columns
+//   k_refine_lay    coarse -> fine copy of held columns, free-surface bed elsewhere,
+//                   the slurry's material tables
+//   k_lay_finish    empty the held coarse columns; lay the kept 10x10 residual
+//                   tiles back on the patch (near_apply)
+//   k_push_patches  tire shoves on every patch's velocity, pushes applied in
+//                   call order; one more row of blocks ages the near-field tiles
+//                   and recycles dropped slots (near_fade)
+//   (sheet_window.cu k_window_step: the fine sheet step itself)
+//   k_peel_patches  spray peeled off the fine water, events queued on the device
+//   k_restrict      residual tiles of held columns (near_capture), then the
+//                   volume- and momentum-weighted sum back into the columns
 //   k_release       fine volume outside the window, booked as parked; fine depths cleared
+//   k_push_cells, k_peel  the same shove and peel on the coarse grid
 //
 // Near-field tiles live in a device pool with a slot per coarse cell; slots
-// are taken in k_near_capture and returned in k_near_fade, so no kernel both
-// pushes and pops the free stack.
+// are taken in the capture (k_restrict) and returned in the fade
+// (k_push_patches, or k_near_fade without tires), so no kernel both pushes and
+// pops the free stack.
 #include <algorithm>
 #include <array>
 #include <cstdio>
@@ -194,33 +198,19 @@ __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W
     }
 }
 
-__global__ void k_zero_cells(SheetView W, const int* cells, int n) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    size_t c = cells[k];
-    W.h[0][c] = 0.0f;
-    W.h[1][c] = 0.0f;
-    W.u[0][c] = 0.0f;
-    W.v[0][c] = 0.0f;
-    W.u[1][c] = 0.0f;
-    W.v[1][c] = 0.0f;
-}
-
 __device__ __forceinline__ float tile_left(float idle) { return idle <= 0.0f ? 1.0f : expf(-idle / NEAR_LIFE_S); }
 
-// near.rs:139-148 floor_scale on one residual.
-__device__ float floor_scale(float base, const float* r, int n) {
-    float low = 0.0f;
-    for (int k = 0; k < n; ++k) low = fminf(low, r[k]);
+// near.rs:139-148 floor_scale on one residual, given its lowest value
+// (the minimum of 0 and every residual).
+__device__ float floor_scale_min(float base, float low) {
     if (low >= 0.0f || base + low >= 0.0f) return 1.0f;
     if (base <= 0.0f) return 0.0f;
     return rclamp(base / -low, 0.0f, 1.0f);
 }
 
 // near_apply (near.rs:276-308): one block per held near column.
-__global__ void k_near_apply(const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol,
-                             const int* slot_map, const float* pool, const NearMeta* meta) {
-    const int q = blockIdx.x;
+__device__ void near_apply_col(int q, const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol,
+                               const int* slot_map, const float* pool, const NearMeta* meta) {
     if (q >= ncol) return;
     const NearCol C = cols[q];
     const int slot = slot_map[C.cidx];
@@ -235,9 +225,22 @@ __global__ void k_near_apply(const PatchRef* refs, int fres, int sub, const Near
     const int f0 = C.j0 * fres + C.i0;
     const float bw = R.water[f0], bs = R.slurry[f0];
     const float left = tile_left(meta[slot].idle_s);
-    if (threadIdx.x == 0) {
-        scale[0] = left * floor_scale(bw / fmaxf(left, 1.0e-6f), tw, n2);
-        scale[1] = left * floor_scale(bs / fmaxf(left, 1.0e-6f), ts, n2);
+    if (threadIdx.x < 32) {
+        // floor_scale's minimum residual of each layer over the first warp (a
+        // minimum: any order gives the same value).
+        float lw = 0.0f, ls = 0.0f;
+        for (int k = threadIdx.x; k < n2; k += 32) {
+            lw = fminf(lw, tw[k]);
+            ls = fminf(ls, ts[k]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lw = fminf(lw, __shfl_down_sync(0xffffffffu, lw, o));
+            ls = fminf(ls, __shfl_down_sync(0xffffffffu, ls, o));
+        }
+        if (threadIdx.x == 0) {
+            scale[0] = left * floor_scale_min(bw / fmaxf(left, 1.0e-6f), lw);
+            scale[1] = left * floor_scale_min(bs / fmaxf(left, 1.0e-6f), ls);
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < n2; k += blockDim.x) {
@@ -254,10 +257,29 @@ __global__ void k_near_apply(const PatchRef* refs, int fres, int sub, const Near
     }
 }
 
+// The end of the lay in one launch: blocks [0, zero_blocks) empty the held
+// coarse columns, the rest apply the near-field residual of one held column
+// each (independent writes: coarse cells, fine cells).
+__global__ void k_lay_finish(SheetView W, const int* held, int n_held, int zero_blocks, const PatchRef* refs,
+                             int fres, int sub, const NearCol* cols, int ncol, const int* slot_map, const float* pool,
+                             const NearMeta* meta) {
+    if ((int)blockIdx.x < zero_blocks) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_held; k += zero_blocks * blockDim.x) {
+            const size_t c = held[k];
+            W.h[0][c] = 0.0f;
+            W.h[1][c] = 0.0f;
+            W.u[0][c] = 0.0f;
+            W.v[0][c] = 0.0f;
+            W.u[1][c] = 0.0f;
+            W.v[1][c] = 0.0f;
+        }
+        return;
+    }
+    near_apply_col((int)blockIdx.x - zero_blocks, refs, fres, sub, cols, ncol, slot_map, pool, meta);
+}
+
 // near_fade (near.rs:311-325) and slot recycling.
-__global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int* counters, float dt) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= NEAR_POOL) return;
+__device__ void near_fade_slot(int s, NearMeta* meta, int* slot_map, int* free_stack, int* counters, float dt) {
     NearMeta& M = meta[s];
     if (M.state == 1) {
         if (M.fresh) {
@@ -276,6 +298,11 @@ __global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int*
         free_stack[top] = s;
         M.state = 0;
     }
+}
+
+__global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int* counters, float dt) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < NEAR_POOL) near_fade_slot(s, meta, slot_map, free_stack, counters, dt);
 }
 
 // push_on (src/fluid_core.rs:8169-8239); every thread owns one cell of the
@@ -332,7 +359,17 @@ struct JobGroup {
     int njobs, i0, j0, w, h;
 };
 
-__global__ void k_push_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int fres, float fcell) {
+// The shoves of every patch (blockIdx.y = group). With `fade`, one more row
+// of blocks runs near_fade over the tile pool (independent of the shoves).
+__global__ void k_push_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int ngroups, int fres,
+                               float fcell, int fade, NearMeta* meta, int* slot_map, int* free_stack, int* counters,
+                               float dt) {
+    if ((int)blockIdx.y == ngroups) {
+        if (fade)
+            for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < NEAR_POOL; q += gridDim.x * blockDim.x)
+                near_fade_slot(q, meta, slot_map, free_stack, counters, dt);
+        return;
+    }
     const JobGroup G = groups[blockIdx.y];
     const PatchRef& R = refs[G.patch];
     const PushJob* jobs = reinterpret_cast<const PushJob*>(tab + G.job_off);
@@ -409,9 +446,8 @@ __global__ void k_peel_patches(const PatchRef* refs, const char* tab, const JobG
 }
 
 // near_capture (near.rs:199-273): one block of 128 threads per held near column.
-__global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol, int* slot_map,
-                               float* pool, NearMeta* meta, int* free_stack, int* counters) {
-    const int q = blockIdx.x;
+__device__ void near_capture_col(int q, const PatchRef* refs, int fres, int sub, const NearCol* cols, int ncol,
+                                 int* slot_map, float* pool, NearMeta* meta, int* free_stack, int* counters) {
     if (q >= ncol) return;
     const NearCol C = cols[q];
     const PatchRef& R = refs[C.patch];
@@ -429,48 +465,77 @@ __global__ void k_near_capture(const PatchRef* refs, int fres, int sub, const Ne
         bv_[k] = R.vw[f];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // Column sums: each row of `sub` summed from -0.0, rows added in order.
-        float sw = 0.0f, ss = 0.0f;
-        for (int b = 0; b < sub; ++b) {
+    // The column's reductions, each in the reference's order, spread over the
+    // first warp: per-row sums on `sub` lanes, then the rest on their own lanes.
+    __shared__ float row_w[32], row_s[32];
+    __shared__ float sw_sh, ss_sh, mu_sh, mv_sh, peak_sh;
+    __shared__ double sum_w_sh, sum_s_sh;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        if (lane < sub) {
+            // Each row of `sub` summed from -0.0 (near.rs column sums).
             float rw = -0.0f, rs = -0.0f;
             for (int a = 0; a < sub; ++a) {
-                rw += bw_[b * sub + a];
-                rs += bs_[b * sub + a];
+                rw += bw_[lane * sub + a];
+                rs += bs_[lane * sub + a];
             }
-            sw += rw;
-            ss += rs;
+            row_w[lane] = rw;
+            row_s[lane] = rs;
         }
+        __syncwarp();
+        if (lane < 2) {  // rows added in order
+            const float* rows = lane == 0 ? row_w : row_s;
+            float acc = 0.0f;
+            for (int b = 0; b < sub; ++b) acc += rows[b];
+            if (lane == 0) sw_sh = acc; else ss_sh = acc;
+        }
+        __syncwarp();
+        const float sw = sw_sh, ss = ss_sh;
+        const float nn = (float)n2;
+        const float mw = sw / nn, ms = ss / nn;
+        // abs_peak (near.rs:128-137): the largest deviation over whole groups
+        // of four, in any order (a maximum).
+        float pk = 0.0f;
+        const int whole = (n2 / 4) * 4;
+        for (int k = lane; k < whole; k += 32) {
+            float a = fabsf(bw_[k] - mw);
+            pk = a > pk ? a : pk;
+            float b2 = fabsf(bs_[k] - ms);
+            pk = b2 > pk ? b2 : pk;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float x = __shfl_down_sync(0xffffffffu, pk, o);
+            pk = x > pk ? x : pk;
+        }
+        if (lane == 0) peak_sh = pk;
+        // recentre (near.rs:118-125): f64 sums of the residual, in order.
+        if (lane == 1 || lane == 2) {
+            const float* b = lane == 1 ? bw_ : bs_;
+            const float m = lane == 1 ? mw : ms;
+            double acc = 0.0;
+            for (int k = 0; k < n2; ++k) acc += (double)(b[k] - m);
+            if (lane == 1) sum_w_sh = acc; else sum_s_sh = acc;
+        }
+        if (lane == 3 || lane == 4) {  // momentum of the water, in order
+            const float* vel = lane == 3 ? bu_ : bv_;
+            float acc = 0.0f;
+            if (C.inner && sw > 1.0e-10f)
+                for (int k = 0; k < n2; ++k) acc += bw_[k] * vel[k];
+            if (lane == 3) mu_sh = acc; else mv_sh = acc;
+        }
+        __syncwarp();
+    }
+    if (threadIdx.x == 0) {
+        const float sw = sw_sh, ss = ss_sh;
         int keep = 1;
         if (sw <= 0.0f && ss <= 0.0f) keep = 0;
         const float nn = (float)n2;
         const float mw = sw / nn, ms = ss / nn;
-        // abs_peak with four lanes (near.rs:128-137).
-        float hw[4] = {0, 0, 0, 0}, hs[4] = {0, 0, 0, 0};
-        for (int c = 0; c + 4 <= n2; c += 4)
-            for (int l = 0; l < 4; ++l) {
-                float a = fabsf(bw_[c + l] - mw);
-                hw[l] = a > hw[l] ? a : hw[l];
-                float b2 = fabsf(bs_[c + l] - ms);
-                hs[l] = b2 > hs[l] ? b2 : hs[l];
-            }
-        float peak = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(hw[0], hw[1]), hw[2]), hw[3]), hs[0]), hs[1]), hs[2]),
-                           hs[3]);
+        const float peak = peak_sh;
         if (keep && peak <= NEAR_DROP_M && !C.inner) keep = 0;
-        // recentre (near.rs:118-125): f64 mean of the residual.
-        double sum_w = 0.0, sum_s = 0.0;
-        for (int k = 0; k < n2; ++k) {
-            sum_w += (double)(bw_[k] - mw);
-            sum_s += (double)(bs_[k] - ms);
-        }
-        mean_w = sum_w / (double)n2;
-        mean_s = sum_s / (double)n2;
-        float mu = 0.0f, mv = 0.0f;
-        if (C.inner && sw > 1.0e-10f)
-            for (int k = 0; k < n2; ++k) {
-                mu += bw_[k] * bu_[k];
-                mv += bw_[k] * bv_[k];
-            }
+        mean_w = sum_w_sh / (double)n2;
+        mean_s = sum_s_sh / (double)n2;
+        const float mu = mu_sh, mv = mv_sh;
         uu_s = mu / sw;
         vv_s = mv / sw;
         mw_s = mw;
@@ -535,36 +600,45 @@ __device__ void restrict_column(const PatchRef* refs, int fres, const SheetView&
         const Segment S = segs[E.seg_off + sgi];
         const PatchRef& R = refs[S.patch];
         const int ni = S.i1 - S.i0 + 1, nc = ni * (S.j1 - S.j0 + 1);
-        for (int c0 = 0; c0 < nc; c0 += 32) {
-            const int c = c0 + lane;
-            float pw = 0.0f, ps = 0.0f, puw = 0.0f, pvw = 0.0f, pus = 0.0f, pvs = 0.0f;
-            int take = 0;
-            if (c < nc) {
-                const int f = (S.j0 + c / ni) * fres + S.i0 + c % ni;
-                const float fw = R.water[f], fs = R.slurry[f];
-                if (!(fw == 0.0f && fs == 0.0f)) {
-                    take = 1;
-                    pw = fw * fine_area;
-                    ps = fs * fine_area;
-                    puw = R.uw[f] * fw * fine_area;
-                    pvw = R.vw[f] * fw * fine_area;
-                    pus = R.us[f] * fs * fine_area;
-                    pvs = R.vs[f] * fs * fine_area;
+        constexpr int G = 4;  // chunks loaded together before they are summed
+        for (int g0 = 0; g0 < nc; g0 += 32 * G) {
+            float pw[G], ps[G], puw[G], pvw[G], pus[G], pvs[G];
+            unsigned takes[G];
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int c = g0 + 32 * q + lane;
+                pw[q] = ps[q] = puw[q] = pvw[q] = pus[q] = pvs[q] = 0.0f;
+                int take = 0;
+                if (c < nc) {
+                    const int f = (S.j0 + c / ni) * fres + S.i0 + c % ni;
+                    const float fw = R.water[f], fs = R.slurry[f];
+                    if (!(fw == 0.0f && fs == 0.0f)) {
+                        take = 1;
+                        pw[q] = fw * fine_area;
+                        ps[q] = fs * fine_area;
+                        puw[q] = R.uw[f] * fw * fine_area;
+                        pvw[q] = R.vw[f] * fw * fine_area;
+                        pus[q] = R.us[f] * fs * fine_area;
+                        pvs[q] = R.vs[f] * fs * fine_area;
+                    }
                 }
+                takes[q] = __ballot_sync(0xffffffffu, take);
             }
-            const unsigned takes = __ballot_sync(0xffffffffu, take);
-            const int m = min(32, nc - c0);
-            for (int b = 0; b < m; ++b) {
-                const float xw = __shfl_sync(0xffffffffu, pw, b), xs = __shfl_sync(0xffffffffu, ps, b);
-                const float xuw = __shfl_sync(0xffffffffu, puw, b), xvw = __shfl_sync(0xffffffffu, pvw, b);
-                const float xus = __shfl_sync(0xffffffffu, pus, b), xvs = __shfl_sync(0xffffffffu, pvs, b);
-                if ((takes >> b) & 1u) {
-                    aw += xw;
-                    as += xs;
-                    auw += xuw;
-                    avw += xvw;
-                    aus += xus;
-                    avs += xvs;
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int m = min(32, nc - (g0 + 32 * q));
+                for (int b = 0; b < m; ++b) {
+                    const float xw = __shfl_sync(0xffffffffu, pw[q], b), xs = __shfl_sync(0xffffffffu, ps[q], b);
+                    const float xuw = __shfl_sync(0xffffffffu, puw[q], b), xvw = __shfl_sync(0xffffffffu, pvw[q], b);
+                    const float xus = __shfl_sync(0xffffffffu, pus[q], b), xvs = __shfl_sync(0xffffffffu, pvs[q], b);
+                    if ((takes[q] >> b) & 1u) {
+                        aw += xw;
+                        as += xs;
+                        auw += xuw;
+                        avw += xvw;
+                        aus += xus;
+                        avs += xvs;
+                    }
                 }
             }
         }
@@ -614,13 +688,22 @@ __device__ void restrict_column(const PatchRef* refs, int fres, const SheetView&
 // column. The lanes load 32 fine cells at a time and form their products in
 // parallel; the six sums then take the products one by one in the
 // reference's raster order (every lane adds the same sequence).
-__global__ void k_restrict(const PatchRef* refs, int fres, SheetView W, const RestrictEntry* ents, int nent,
-                           const Segment* segs, float fine_area, float coarse_area, int full) {
+// Blocks [0, ncap) capture the near-field residual of one held column each
+// (with `ncap` = 0 when the near field is off); the rest restrict, a warp per
+// touched coarse column. Both read the fine cells after the peel and write
+// disjoint state (the tile pool, the coarse columns). 128 threads per block.
+__global__ void k_restrict(const PatchRef* refs, int fres, int sub, SheetView W, const RestrictEntry* ents, int nent,
+                           const Segment* segs, float fine_area, float coarse_area, const NearCol* cols, int ncap,
+                           int* slot_map, float* pool, NearMeta* meta, int* free_stack, int* counters) {
+    if ((int)blockIdx.x < ncap) {
+        near_capture_col(blockIdx.x, refs, fres, sub, cols, ncap, slot_map, pool, meta, free_stack, counters);
+        return;
+    }
     const int lane = threadIdx.x & 31;
-    const int warps = (int)((gridDim.x * (size_t)blockDim.x) >> 5);
-    for (int q = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5); q < nent; q += warps)
+    const int nb = (int)gridDim.x - ncap;
+    const int warps = (int)((nb * (size_t)blockDim.x) >> 5);
+    for (int q = (int)((((int)blockIdx.x - ncap) * (size_t)blockDim.x + threadIdx.x) >> 5); q < nent; q += warps)
         restrict_column(refs, fres, W, ents[q], segs, fine_area, coarse_area, lane);
-    (void)full;
 }
 
 // After the restrict: fine cells outside the coarse window have their volume
@@ -1152,22 +1235,17 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
                                                                                  M.counters + 3);
     ::silt::count_launch();
     FCK(cudaGetLastError());
-    if (!L.held.empty()) {
-        k_zero_cells<<<launch_blocks(L.held.size()), 256, 0, W.st>>>(W, TAB(int, L.off_held), (int)L.held.size());
-        ::silt::count_launch();
-        FCK(cudaGetLastError());
-    }
     P.fine_on = true;
     P.active = L.np;
-    if (M.near_maybe) {
-        if (L.n_near) {
-            k_near_apply<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
-                                                     M.slot_map, M.pool, M.meta);
-            ::silt::count_launch();
-            FCK(cudaGetLastError());
-        }
-        k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
-                                                              dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+    // Empty the held coarse columns and apply the near-field residuals in one
+    // launch (the fade runs with the shoves).
+    const int n_held = (int)L.held.size();
+    const int n_apply = M.near_maybe ? L.n_near : 0;
+    if (n_held || n_apply) {
+        const int zero_blocks = n_held ? launch_blocks((size_t)n_held, 128) : 0;
+        k_lay_finish<<<zero_blocks + n_apply, 128, 0, W.st>>>(W, TAB(int, L.off_held), n_held, zero_blocks, refs,
+                                                             P.fres, P.sub, TAB(NearCol, L.off_near), n_apply,
+                                                             M.slot_map, M.pool, M.meta);
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
@@ -1181,17 +1259,15 @@ int restrict_all(Patches& P, silt_sheet* s) {
     const StepPlan& L = HS.plan;
     SheetView W = view_of(s);
     const PatchRef* refs = TAB(PatchRef, L.off_refs);
-    if (P.near_on && L.n_near) {
-        k_near_capture<<<L.n_near, 128, 0, W.st>>>(refs, P.fres, P.sub, TAB(NearCol, L.off_near), L.n_near,
-                                                   M.slot_map, M.pool, M.meta, M.free_stack, M.counters);
-        ::silt::count_launch();
-        FCK(cudaGetLastError());
-        M.near_maybe = true;
-    }
-    if (L.n_ent) {
-        k_restrict<<<launch_blocks((size_t)L.n_ent * 32, 128), 128, 0, W.st>>>(refs, P.fres, W, TAB(RestrictEntry, L.off_ent),
-                                                                 L.n_ent, TAB(Segment, L.off_seg), P.fcell * P.fcell,
-                                                                 W.cell * W.cell, P.sub * P.sub);
+    // The near-field capture and the restrict in one launch.
+    const int ncap = (P.near_on && L.n_near) ? L.n_near : 0;
+    if (ncap) M.near_maybe = true;
+    if (ncap || L.n_ent) {
+        const int rblocks = L.n_ent ? launch_blocks((size_t)L.n_ent * 32, 128) : 0;
+        k_restrict<<<ncap + rblocks, 128, 0, W.st>>>(refs, P.fres, P.sub, W, TAB(RestrictEntry, L.off_ent), L.n_ent,
+                                                     TAB(Segment, L.off_seg), P.fcell * P.fcell, W.cell * W.cell,
+                                                     TAB(NearCol, L.off_near), ncap, M.slot_map, M.pool, M.meta,
+                                                     M.free_stack, M.counters);
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
@@ -1237,9 +1313,13 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     W = view_of(s);
     const PatchRef* refs = TAB(PatchRef, L.off_refs);
     const char* tab = TAB(char, 0);
-    if (L.n_push_groups) {
-        dim3 grid(launch_blocks((size_t)L.push_cells_max), L.n_push_groups);
-        k_push_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_push_groups), P.fres, P.fcell);
+    // The shoves of every patch, and the near-field fade in one more row of blocks.
+    const int fade = M.near_maybe ? 1 : 0;
+    if (L.n_push_groups || fade) {
+        dim3 grid(launch_blocks((size_t)std::max(L.push_cells_max, 1)), L.n_push_groups + fade);
+        k_push_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_push_groups), L.n_push_groups, P.fres,
+                                               P.fcell, fade, M.meta, M.slot_map, M.free_stack, M.counters,
+                                               dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
