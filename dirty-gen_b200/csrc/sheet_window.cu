@@ -53,6 +53,8 @@ struct Shared {
     int changed;
     float red_f[NT / 32];
     double red_d[NT / 32];
+    double crew_d;   // this CTA's share of a crew-wide sum or maximum, read by the crew
+    float crew_f;
     int red_i[4][NT / 32];
 };
 
@@ -135,6 +137,31 @@ __device__ __forceinline__ float block_max_f(Shared& S, float v) {
     float r = S.red_f[0];
     __syncthreads();
     return r;
+}
+
+// A crew-wide sum of per-thread partials: each CTA reduces its own, then every
+// CTA adds the CTAs' results in rank order (the same value in every CTA).
+__device__ double crew_sum_d(Shared& S, double v) {
+    const double part = block_sum_d(S, v);
+    if (threadIdx.x == 0) S.crew_d = part;
+    crew_sync();
+    cg::cluster_group crew = cg::this_cluster();
+    double tot = 0.0;
+    for (int r = 0; r < crew_size(); ++r) tot += *crew.map_shared_rank(&S.crew_d, r);
+    crew_sync();  // every CTA has read the shares before they are reused
+    return tot;
+}
+
+// A crew-wide maximum of non-negative per-thread values.
+__device__ float crew_max_f(Shared& S, float v) {
+    const float part = block_max_f(S, v);
+    if (threadIdx.x == 0) S.crew_f = part;
+    crew_sync();
+    cg::cluster_group crew = cg::this_cluster();
+    float m = 0.0f;
+    for (int r = 0; r < crew_size(); ++r) m = fmaxf(m, *crew.map_shared_rank(&S.crew_f, r));
+    crew_sync();
+    return m;
 }
 
 // Four ints reduced together: op 0 = sum, 1 = min, 2 = max.
@@ -548,17 +575,21 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
 }
 
 // awake_work_boxes (src/fluid_core.rs:1537-1657).
+// Called by the whole crew: the crew marks rank 0's hot tiles, rank 0 does
+// the rest (labels and boxes in its shared memory).
 __device__ void cta_awake_boxes(Shared& S, const Job& J) {
     const int res = J.res;
     const int tiles = (res + SLEEP_TILE - 1) / SLEEP_TILE;
     const int ntile = tiles * tiles;
-    for (int t = threadIdx.x; t < ntile; t += NT) {
-        S.hot[t] = 0;
-        S.grown[t] = 0;
-    }
-    __syncthreads();
+    if (crew_rank() == 0)
+        for (int t = threadIdx.x; t < ntile; t += NT) {
+            S.hot[t] = 0;
+            S.grown[t] = 0;
+        }
+    crew_sync();
+    Shared* S0 = cg::this_cluster().map_shared_rank(&S, 0);
     const float eps = J.eps, cell = J.cell;
-    CTA_RECT(0, res - 1, 0, res - 1, {
+    CLU_RECT(0, res - 1, 0, res - 1, {
         float hv = J.h[g];
         if (hv > eps) {
             bool awake = hypotf(J.u[g], J.v[g]) > 0.05f;
@@ -570,10 +601,11 @@ __device__ void cta_awake_boxes(Shared& S, const Job& J) {
                 float dez = fabsf(J.bed[jp] + J.h[jp] - eta);
                 awake = fmaxf(dex, dez) > 0.02f * cell;
             }
-            if (awake) S.hot[(j / SLEEP_TILE) * tiles + i / SLEEP_TILE] = 1;
+            if (awake) S0->hot[(j / SLEEP_TILE) * tiles + i / SLEEP_TILE] = 1;
         }
     })
-    __syncthreads();
+    crew_sync();
+    if (crew_rank() != 0) return;
     for (int t = threadIdx.x; t < ntile; t += NT) {
         int ti = t % tiles, tj = t / tiles;
         unsigned char gr = 0;
@@ -855,12 +887,12 @@ __device__ void cta_soften(const Job& J) {
     crew_sync();
 }
 
-// The layer's FP64 depth sum; each CTA sums the whole plane, rank 0 writes it.
+// The layer's FP64 depth sum over the crew; rank 0 writes it.
 __device__ void cta_ledger(Shared& S, const Job& J) {
     const int res = J.res;
     double part = 0.0;
-    CTA_RECT(0, res - 1, 0, res - 1, { part += (double)fmaxf(J.h[g], 0.0f); })
-    part = block_sum_d(S, part);
+    CLU_RECT(0, res - 1, 0, res - 1, { part += (double)fmaxf(J.h[g], 0.0f); })
+    part = crew_sum_d(S, part);
     if (threadIdx.x == 0 && J.ledger && crew_rank() == 0) *J.ledger = part;
 }
 
@@ -871,13 +903,13 @@ __device__ int window_body(Shared& S, const Job& J) {
     const int res = J.res;
     const float eps = J.eps;
     if (J.soften_edge > 0) cta_soften(J);
-    // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844), per CTA.
+    // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844), over the crew.
     double ws = 0.0;
-    CTA_RECT(0, res - 1, 0, res - 1, {
+    CLU_RECT(0, res - 1, 0, res - 1, {
         float hv = J.h[g];
         if (hv > eps) ws += (double)hv;
     })
-    ws = block_sum_d(S, ws);
+    ws = crew_sum_d(S, ws);
     if (!(ws > (double)eps)) {
         cta_ledger(S, J);
         return 0;
@@ -886,14 +918,13 @@ __device__ int window_body(Shared& S, const Job& J) {
     const bool fine_open = open_fine && J.pace == 0;
     const bool whole_wet = open_fine && (J.pace == 2 || J.pace == 3);
     const bool awake = open_fine && !whole_wet && !fine_open;
-    // Work boxes on rank 0 (the wet-body labels use a global plane), then
-    // every other CTA copies them from its shared memory.
-    if (crew_rank() == 0) {
-        if (fine_open || awake)
-            cta_awake_boxes(S, J);
-        else
-            cta_wet_boxes(S, J);
-    }
+    // Work boxes on rank 0 (the wet-body labels use a global plane; the awake
+    // scan is shared by the crew), then every other CTA copies them from its
+    // shared memory.
+    if (fine_open || awake)
+        cta_awake_boxes(S, J);
+    else if (crew_rank() == 0)
+        cta_wet_boxes(S, J);
     crew_sync();
     if (crew_rank() != 0) {
         const Shared* S0 = cg::this_cluster().map_shared_rank(&S, 0);
@@ -913,13 +944,13 @@ __device__ int window_body(Shared& S, const Job& J) {
         float m2 = 0.0f;
         for (int k = 0; k < nb; ++k) {
             const Box b = {S.bbox[0][k], S.bbox[1][k], S.bbox[2][k], S.bbox[3][k]};
-            CTA_RECT(b.i0, b.i1, b.j0, b.j1, {
+            CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
                 float uu = J.u[g], vv = J.v[g];
                 float s2 = uu * uu + vv * vv;
                 if (s2 > m2) m2 = s2;
             })
         }
-        m2 = block_max_f(S, m2);
+        m2 = crew_max_f(S, m2);
         float max_s = fmaxf(0.15f, sqrtf(m2));
         nsub = (int)rclamp(ceilf((J.dt * max_s) / (0.42f * fmaxf(J.cell, 1.0e-3f))), 1.0f, cap);
     }
