@@ -471,9 +471,12 @@ def run_batch(args):
     def one_step():
         nonlocal step_no
         step_no += 1
-        for sh, w in zip(sheets, wins):
+        idx, tires = [], []
+        for k, w in enumerate(wins):
             for t in batch_tires(step_no, w):
-                sh.push_tire(**t)
+                idx.append(k)
+                tires.append(t)
+        batch.push_tires(idx, tires)
         batch.step(DT)
 
     for _ in range(max(3, args.warmup)):

@@ -150,52 +150,53 @@ __global__ void k_scatter_owner(int8_t* owner, const int* idx, const int8_t* val
     if (k < n) owner[idx[k]] = val[k];
 }
 
-// refine (src/fluid_core.rs:8358-8460), the per-fine-cell copy.
+// refine (src/fluid_core.rs:8358-8460), the copy into fine cell f of patch p.
+__device__ __forceinline__ void refine_cell(const PatchRef& R, int p, int f, int fres, const SheetView& W,
+                                            const int8_t* owner) {
+    R.water[f] = 0.0f;
+    R.slurry[f] = 0.0f;
+    R.uw[f] = 0.0f;
+    R.vw[f] = 0.0f;
+    R.us[f] = 0.0f;
+    R.vs[f] = 0.0f;
+    const int ci = R.col[f % fres], cj = R.row[f / fres];
+    if (ci >= 0 && cj >= 0) {
+        const size_t c = (size_t)cj * W.res + ci;
+        R.moisture[f] = W.moisture[c];
+        R.grain[f] = W.grain[c];
+    }
+    // The slurry's material laws once per step here, spread over the whole
+    // GPU, instead of once per cell and substep inside the patch's step.
+    const float nu = dynamic_viscosity(R.grain[f], R.moisture[f]);
+    R.nu_s[f] = nu;
+    R.mob_s[f] = sheet_mobility_for(nu);
+    R.damp_s[f] = sheet_damp(nu);
+    if (ci < 0 || cj < 0) return;
+    const size_t c = (size_t)cj * W.res + ci;
+    if (owner[c] != p) {
+        R.bed[f] = W.bed[c] + W.h[0][c];
+        R.bed_slurry[f] = W.bed[c] + W.h[1][c];
+        return;
+    }
+    R.bed[f] = W.bed[c];
+    R.bed_slurry[f] = W.bed[c];
+    const float hw = W.h[0][c], hs = W.h[1][c];
+    R.water[f] = hw;
+    R.slurry[f] = hs;
+    // A coarse cell still waiting for the previous dry cut carries no velocity.
+    const bool cw = W.cut_pending && hw < 1.0e-6f, cs = W.cut_pending && hs < 1.0e-6f;
+    R.uw[f] = cw ? 0.0f : W.u[0][c];
+    R.vw[f] = cw ? 0.0f : W.v[0][c];
+    R.us[f] = cs ? 0.0f : W.u[1][c];
+    R.vs[f] = cs ? 0.0f : W.v[1][c];
+}
+
 __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W, const int8_t* owner,
                              int* spray_count) {
     const size_t fn = (size_t)fres * fres;
     if (blockIdx.x == 0 && threadIdx.x == 0) *spray_count = 0;  // this step's spray events start here
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
-        const int p = (int)(k / fn);
-        const int f = (int)(k % fn);
-        const PatchRef& R = refs[p];
-        R.water[f] = 0.0f;
-        R.slurry[f] = 0.0f;
-        R.uw[f] = 0.0f;
-        R.vw[f] = 0.0f;
-        R.us[f] = 0.0f;
-        R.vs[f] = 0.0f;
-        const int ci = R.col[f % fres], cj = R.row[f / fres];
-        if (ci >= 0 && cj >= 0) {
-            const size_t c = (size_t)cj * W.res + ci;
-            R.moisture[f] = W.moisture[c];
-            R.grain[f] = W.grain[c];
-        }
-        // The slurry's material laws once per step here, spread over the whole
-        // GPU, instead of once per cell and substep inside the patch's step.
-        const float nu = dynamic_viscosity(R.grain[f], R.moisture[f]);
-        R.nu_s[f] = nu;
-        R.mob_s[f] = sheet_mobility_for(nu);
-        R.damp_s[f] = sheet_damp(nu);
-        if (ci < 0 || cj < 0) continue;
-        const size_t c = (size_t)cj * W.res + ci;
-        if (owner[c] != p) {
-            R.bed[f] = W.bed[c] + W.h[0][c];
-            R.bed_slurry[f] = W.bed[c] + W.h[1][c];
-            continue;
-        }
-        R.bed[f] = W.bed[c];
-        R.bed_slurry[f] = W.bed[c];
-        const float hw = W.h[0][c], hs = W.h[1][c];
-        R.water[f] = hw;
-        R.slurry[f] = hs;
-        // A coarse cell still waiting for the previous dry cut carries no velocity.
-        const bool cw = W.cut_pending && hw < 1.0e-6f, cs = W.cut_pending && hs < 1.0e-6f;
-        R.uw[f] = cw ? 0.0f : W.u[0][c];
-        R.vw[f] = cw ? 0.0f : W.v[0][c];
-        R.us[f] = cs ? 0.0f : W.u[1][c];
-        R.vs[f] = cs ? 0.0f : W.v[1][c];
-    }
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x)
+        refine_cell(refs[k / fn], (int)(k / fn), (int)(k % fn), fres, W, owner);
 }
 
 __device__ __forceinline__ float tile_left(float idle) { return idle <= 0.0f ? 1.0f : expf(-idle / NEAR_LIFE_S); }
@@ -708,10 +709,11 @@ __global__ void k_restrict(const PatchRef* refs, int fres, int sub, SheetView W,
 
 // After the restrict: fine cells outside the coarse window have their volume
 // parked (src/fluid_core.rs:8476-8484), and every fine depth is released.
-__global__ void k_release(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park) {
+__device__ void release_cells(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park,
+                              size_t k0, size_t stride) {
     const size_t fn = (size_t)fres * fres;
     double pw = 0.0, ps = 0.0;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x) {
+    for (size_t k = k0; k < fn * np; k += stride) {
         const PatchRef& R = refs[k / fn];
         const int f = (int)(k % fn);
         if (park && !(R.col[f % fres] >= 0 && R.row[f / fres] >= 0)) {
@@ -729,6 +731,11 @@ __global__ void k_release(const PatchRef* refs, int np, int fres, float fine_are
         atomicAdd(&books[1], pw);
         atomicAdd(&books[2], ps);
     }
+}
+
+__global__ void k_release(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park) {
+    release_cells(refs, np, fres, fine_area, books, park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
+                  (size_t)gridDim.x * blockDim.x);
 }
 
 __global__ void k_init_pool(NearMeta* meta, int* free_stack, int* slot_map, size_t ncells, int* counters) {
@@ -871,6 +878,7 @@ struct StepPlan {
     std::vector<JobList> fine_push, fine_peel;
     JobList coarse_push, coarse_peel;
     std::vector<int> coarse_pushed;   // tires that shove coarse cells (their cell is not held)
+    int b_apply = 0, b_fade = 0, b_ncap = 0;  // batched step: near-field apply, fade and capture counts
     size_t off_push_groups = 0, off_peel_groups = 0;
     int n_push_groups = 0, n_peel_groups = 0, push_cells_max = 0, peel_cells_max = 0;
     int slot = 0;
@@ -1217,6 +1225,33 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
 
 #define TAB(T, off) (reinterpret_cast<const T*>(HS.d_tab[L.slot] + (off)))
 
+// The coarse speed bound's growth from this step's coupling. The restrict
+// hands each column a depth-weighted mean of its fine cells' velocities and
+// its own, so it adds nothing above the largest fine speed; after the patch
+// step every wet fine cell faster than 0.05 m/s lies in a work box and is
+// clamped to the film cap, and drier cells carry only the laid coarse velocity
+// (shoves need 4 mm of depth). So only the shoves of tires outside the patches
+// raise it: each by at most 1.04 max(speed, 0.4) (|fore f + 0.28 flank r| <=
+// sqrt(1 + 0.28^2)), summed where the tires' spans overlap.
+static float coarse_shove_bound(const StepPlan& L, const std::vector<silt_tire_push>& ps, const SheetView& W) {
+    float add = 0.0f;
+    for (int a : L.coarse_pushed) {
+        float reach_a = push_reach(ps[a], W.cell);
+        auto ai = index_span(W.origin[0], W.cell, W.res, ps[a].x, reach_a);
+        auto aj = index_span(W.origin[1], W.cell, W.res, ps[a].z, reach_a);
+        float sum = 0.0f;
+        for (int b : L.coarse_pushed) {
+            float reach_b = push_reach(ps[b], W.cell);
+            auto bi = index_span(W.origin[0], W.cell, W.res, ps[b].x, reach_b);
+            auto bj = index_span(W.origin[1], W.cell, W.res, ps[b].z, reach_b);
+            bool overlap = ai.first < bi.second && bi.first < ai.second && aj.first < bj.second && bj.first < aj.second;
+            if (a == b || overlap) sum += 1.04f * std::max(ps[b].speed, 0.4f);
+        }
+        add = std::max(add, sum);
+    }
+    return add;
+}
+
 static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt) {
     Impl& M = I(P);
     int rc = plan_step(P, s, ps, dt);
@@ -1341,31 +1376,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    // The coarse speed bound after this step's coupling. The restrict hands
-    // each column a depth-weighted mean of its fine cells' velocities and its
-    // own, so it adds nothing above the largest fine speed; after the patch
-    // step every wet fine cell faster than 0.05 m/s lies in a work box and is
-    // clamped to the film cap, and drier cells carry only the laid coarse
-    // velocity (shoves need 4 mm of depth). So only the shoves of tires
-    // outside the patches raise it: each by at most 1.04 max(speed, 0.4)
-    // (|fore f + 0.28 flank r| <= sqrt(1 + 0.28^2)), summed where the tires'
-    // spans overlap.
-    float add = 0.0f;
-    for (int a : L.coarse_pushed) {
-        float reach_a = push_reach(ps[a], W.cell);
-        auto ai = index_span(W.origin[0], W.cell, W.res, ps[a].x, reach_a);
-        auto aj = index_span(W.origin[1], W.cell, W.res, ps[a].z, reach_a);
-        float sum = 0.0f;
-        for (int b : L.coarse_pushed) {
-            float reach_b = push_reach(ps[b], W.cell);
-            auto bi = index_span(W.origin[0], W.cell, W.res, ps[b].x, reach_b);
-            auto bj = index_span(W.origin[1], W.cell, W.res, ps[b].z, reach_b);
-            bool overlap = ai.first < bi.second && bi.first < ai.second && aj.first < bj.second && bj.first < aj.second;
-            if (a == b || overlap) sum += 1.04f * std::max(ps[b].speed, 0.4f);
-        }
-        add = std::max(add, sum);
-    }
-    add_speed(s, add);
+    add_speed(s, coarse_shove_bound(L, ps, W));
     out.spray_events = 1;
     return SILT_OK;
 }
@@ -1537,6 +1548,380 @@ void destroy(Patches& P) {
 }
 
 const char* last_error() { return g_err; }
+
+
+// ------------------------------------------------------------ batched windows
+// Many windows' nested patches stepped by one launch per kernel: each window's
+// tables are planned and uploaded per window (on any host thread), then one
+// record per window tells the batched kernels (blockIdx.z = record) where its
+// tables, planes and books are.
+
+struct FineRec {
+    SheetView W;
+    const PatchRef* refs;
+    const char* tab;
+    int np, fres, sub, park;
+    float fcell, dt;
+    int8_t* owner;
+    const int* oidx;
+    const int8_t* oval;
+    int n_owner;
+    const int* held;
+    int n_held, zero_blocks;
+    const NearCol* near;
+    int n_apply, ncap, fade;
+    const JobGroup* push_groups;
+    int n_push_groups;
+    const JobGroup* peel_groups;
+    int n_peel_groups;
+    const RestrictEntry* ents;
+    int n_ent, rblocks;
+    const Segment* segs;
+    const PushJob* cpush;
+    int cpush_n, cpush_i0, cpush_j0, cpush_w, cpush_h;
+    int* slot_map;
+    float* pool;
+    NearMeta* meta;
+    int* free_stack;
+    int* counters;
+    SprayRec* spray;
+    double* books;
+};
+
+struct PeelRec {
+    SheetView W;
+    const PushJob* jobs;
+    int n, i0, j0, w, h;
+    int8_t* owner;
+    SprayRec* spray;
+    int* counters;
+    double* books;
+};
+
+__global__ void kb_scatter(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.n_owner; k += gridDim.x * blockDim.x)
+        r.owner[r.oidx[k]] = r.oval[k];
+}
+
+__global__ void kb_refine(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    const size_t fn = (size_t)r.fres * r.fres;
+    if (blockIdx.x == 0 && threadIdx.x == 0) r.counters[3] = 0;  // this step's spray events start here
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * r.np; k += (size_t)gridDim.x * blockDim.x)
+        refine_cell(r.refs[k / fn], (int)(k / fn), (int)(k % fn), r.fres, r.W, r.owner);
+}
+
+__global__ void kb_lay_finish(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    const int b = (int)blockIdx.x;
+    if (b < r.zero_blocks) {
+        for (int k = b * blockDim.x + threadIdx.x; k < r.n_held; k += r.zero_blocks * blockDim.x) {
+            const size_t c = r.held[k];
+            r.W.h[0][c] = 0.0f;
+            r.W.h[1][c] = 0.0f;
+            r.W.u[0][c] = 0.0f;
+            r.W.v[0][c] = 0.0f;
+            r.W.u[1][c] = 0.0f;
+            r.W.v[1][c] = 0.0f;
+        }
+        return;
+    }
+    near_apply_col(b - r.zero_blocks, r.refs, r.fres, r.sub, r.near, r.n_apply, r.slot_map, r.pool, r.meta);
+}
+
+__global__ void kb_push(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    const int y = (int)blockIdx.y;
+    if (y == r.n_push_groups) {
+        if (r.fade)
+            for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < NEAR_POOL; q += gridDim.x * blockDim.x)
+                near_fade_slot(q, r.meta, r.slot_map, r.free_stack, r.counters, r.dt);
+        return;
+    }
+    if (y > r.n_push_groups) return;
+    const JobGroup G = r.push_groups[y];
+    const PatchRef& R = r.refs[G.patch];
+    const PushJob* jobs = reinterpret_cast<const PushJob*>(r.tab + G.job_off);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < G.w * G.h; k += gridDim.x * blockDim.x)
+        push_cell(R.water, R.slurry, R.uw, R.vw, R.us, R.vs, r.fres, r.fcell, G.ox, G.oz, jobs, G.njobs,
+                  G.i0 + k % G.w, G.j0 + k / G.w);
+}
+
+__global__ void kb_peel_patches(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    if ((int)blockIdx.y >= r.n_peel_groups) return;
+    const JobGroup G = r.peel_groups[blockIdx.y];
+    const PatchRef& R = r.refs[G.patch];
+    const PushJob* jobs = reinterpret_cast<const PushJob*>(r.tab + G.job_off);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < G.w * G.h; k += gridDim.x * blockDim.x)
+        peel_cell(R.water, R.uw, R.vw, r.fres, r.fcell, G.ox, G.oz, jobs, G.njobs, G.i0 + k % G.w, G.j0 + k / G.w,
+                  nullptr, 0, 0.0f, 0.0f, 1.0f, 0, G.patch, r.spray, r.counters, r.books, nullptr);
+}
+
+__global__ void kb_restrict(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    const int b = (int)blockIdx.x;
+    if (b < r.ncap) {
+        near_capture_col(b, r.refs, r.fres, r.sub, r.near, r.ncap, r.slot_map, r.pool, r.meta, r.free_stack,
+                         r.counters);
+        return;
+    }
+    if (b - r.ncap >= r.rblocks) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = (int)((r.rblocks * (size_t)blockDim.x) >> 5);
+    for (int q = (int)(((b - r.ncap) * (size_t)blockDim.x + threadIdx.x) >> 5); q < r.n_ent; q += warps)
+        restrict_column(r.refs, r.fres, r.W, r.ents[q], r.segs, r.fcell * r.fcell, r.W.cell * r.W.cell, lane);
+}
+
+__global__ void kb_release(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    release_cells(r.refs, r.np, r.fres, r.fcell * r.fcell, r.books, r.park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
+                  (size_t)gridDim.x * blockDim.x);
+}
+
+__global__ void kb_coarse_push(const FineRec* recs) {
+    const FineRec& r = recs[blockIdx.z];
+    const SheetView& W = r.W;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.cpush_w * r.cpush_h; k += gridDim.x * blockDim.x)
+        push_cell(W.h[0], W.h[1], W.u[0], W.v[0], W.u[1], W.v[1], W.res, W.cell, W.origin[0], W.origin[1], r.cpush,
+                  r.cpush_n, r.cpush_i0 + k % r.cpush_w, r.cpush_j0 + k / r.cpush_w);
+}
+
+__global__ void kb_coarse_peel(const PeelRec* recs) {
+    const PeelRec& r = recs[blockIdx.z];
+    const SheetView& W = r.W;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.w * r.h; k += gridDim.x * blockDim.x)
+        peel_cell(W.h[0], W.u[0], W.v[0], W.res, W.cell, W.origin[0], W.origin[1], r.jobs, r.n, r.i0 + k % r.w,
+                  r.j0 + k / r.w, r.owner, W.res, W.origin[0], W.origin[1], W.cell, 1, 0, r.spray, r.counters,
+                  r.books, W.d_acc);
+}
+
+struct FineBatch {
+    // Double-buffered pinned and device staging: records, then job pointers.
+    char* h_buf[2] = {nullptr, nullptr};
+    char* d_buf[2] = {nullptr, nullptr};
+    size_t cap[2] = {0, 0};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int flip = 0;
+    PeelRec* h_peel[2] = {nullptr, nullptr};
+    PeelRec* d_peel[2] = {nullptr, nullptr};
+    size_t peel_cap[2] = {0, 0};
+    cudaEvent_t peel_ev[2] = {nullptr, nullptr};
+    int peel_flip = 0;
+};
+
+FineBatch* batch_new() { return new FineBatch(); }
+
+void batch_free(FineBatch* B) {
+    if (!B) return;
+    for (int k = 0; k < 2; ++k) {
+        if (B->ev[k]) cudaEventSynchronize(B->ev[k]);
+        if (B->peel_ev[k]) cudaEventSynchronize(B->peel_ev[k]);
+        cudaFree(B->d_buf[k]);
+        if (B->h_buf[k]) cudaFreeHost(B->h_buf[k]);
+        cudaFree(B->d_peel[k]);
+        if (B->h_peel[k]) cudaFreeHost(B->h_peel[k]);
+        if (B->ev[k]) cudaEventDestroy(B->ev[k]);
+        if (B->peel_ev[k]) cudaEventDestroy(B->peel_ev[k]);
+    }
+    delete B;
+}
+
+int batch_prepare(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, float dt, StepOut& out,
+                  bool* has_work) {
+    *has_work = false;
+    Impl& M = I(P);
+    int rc = restrict_all(P, s);
+    if (rc) return rc;
+    if (ps.empty()) {
+        if (M.spray_dirty) {
+            FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), view_of(s).st));
+            M.spray_dirty = false;
+        }
+        return fade_only(P, s, dt);
+    }
+    M.spray_dirty = true;
+    if ((rc = plan_step(P, s, ps, dt))) return rc;
+    StepPlan& L = H(P).plan;
+    // The flags the single-window step reads between its launches.
+    L.b_apply = M.near_maybe ? L.n_near : 0;
+    L.b_fade = M.near_maybe ? 1 : 0;
+    L.b_ncap = (P.near_on && L.n_near) ? L.n_near : 0;
+    if (L.b_ncap) M.near_maybe = true;
+    P.active = L.np;
+    P.fine_on = false;  // the batched launches restrict the patches this step
+    invalidate_ledger(s);
+    add_speed(s, coarse_shove_bound(L, ps, view_of(s)));
+    out.spray_events = 1;
+    *has_work = true;
+    return SILT_OK;
+}
+
+int batch_launch(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::vector<Patches*>& patches, float dt,
+                 cudaStream_t st) {
+    const int n = (int)sheets.size();
+    if (n == 0) return SILT_OK;
+    size_t njobs = 0;
+    int max_fres = 0;
+    for (Patches* P : patches) {
+        njobs += 2 * (size_t)H(*P).plan.np;
+        max_fres = std::max(max_fres, P->fres);
+    }
+    const size_t rec_bytes = ((n * sizeof(FineRec)) + 255) & ~size_t(255);
+    const size_t need = rec_bytes + njobs * sizeof(window::Job*);
+    const int slot = B->flip;
+    B->flip ^= 1;
+    if (B->ev[slot]) FCK(cudaEventSynchronize(B->ev[slot]));
+    if (need > B->cap[slot]) {
+        cudaFree(B->d_buf[slot]);
+        if (B->h_buf[slot]) cudaFreeHost(B->h_buf[slot]);
+        B->d_buf[slot] = nullptr;
+        B->h_buf[slot] = nullptr;
+        B->cap[slot] = 0;
+        const size_t cap = std::max(need * 2, (size_t)1 << 16);
+        FCK(cudaMalloc(&B->d_buf[slot], cap));
+        FCK(cudaMallocHost(&B->h_buf[slot], cap));
+        B->cap[slot] = cap;
+    }
+    if (!B->ev[slot]) FCK(cudaEventCreateWithFlags(&B->ev[slot], cudaEventDisableTiming));
+    FineRec* recs = reinterpret_cast<FineRec*>(B->h_buf[slot]);
+    window::Job** jl = reinterpret_cast<window::Job**>(B->h_buf[slot] + rec_bytes);
+    int mx_owner = 1, mx_cells = 1, mx_finish = 1, mx_push = 1, mx_pgroups = 0, mx_peel = 1, mx_qgroups = 0;
+    int mx_restrict = 1, mx_cpush = 1;
+    size_t q = 0;
+    for (int w = 0; w < n; ++w) {
+        silt_sheet* s = sheets[w];
+        Patches& P = *patches[w];
+        Impl& M = I(P);
+        HostState& HS = H(P);
+        const StepPlan& L = HS.plan;
+        FineRec& r = recs[w];
+        memset(&r, 0, sizeof r);
+        r.W = view_of(s);
+        r.refs = TAB(PatchRef, L.off_refs);
+        r.tab = TAB(char, 0);
+        r.np = L.np;
+        r.fres = P.fres;
+        r.sub = P.sub;
+        r.park = L.any_park ? 1 : 0;
+        r.fcell = P.fcell;
+        r.dt = dt > 0.0f && std::isfinite(dt) ? dt : 0.0f;
+        r.owner = M.owner;
+        r.oidx = TAB(int, L.off_oidx);
+        r.oval = TAB(int8_t, L.off_oval);
+        r.n_owner = L.n_owner;
+        r.held = TAB(int, L.off_held);
+        r.n_held = (int)L.held.size();
+        r.zero_blocks = r.n_held ? launch_blocks((size_t)r.n_held, 128) : 0;
+        r.near = TAB(NearCol, L.off_near);
+        r.n_apply = L.b_apply;
+        r.ncap = L.b_ncap;
+        r.fade = L.b_fade;
+        r.push_groups = TAB(JobGroup, L.off_push_groups);
+        r.n_push_groups = L.n_push_groups;
+        r.peel_groups = TAB(JobGroup, L.off_peel_groups);
+        r.n_peel_groups = L.n_peel_groups;
+        r.ents = TAB(RestrictEntry, L.off_ent);
+        r.n_ent = L.n_ent;
+        r.rblocks = L.n_ent ? launch_blocks((size_t)L.n_ent * 32, 128) : 0;
+        r.segs = TAB(Segment, L.off_seg);
+        r.cpush = TAB(PushJob, L.coarse_push.off);
+        r.cpush_n = L.coarse_push.n;
+        r.cpush_i0 = L.coarse_push.i0;
+        r.cpush_j0 = L.coarse_push.j0;
+        r.cpush_w = L.coarse_push.n ? L.coarse_push.w : 0;
+        r.cpush_h = L.coarse_push.n ? L.coarse_push.h : 0;
+        r.slot_map = M.slot_map;
+        r.pool = M.pool;
+        r.meta = M.meta;
+        r.free_stack = M.free_stack;
+        r.counters = M.counters;
+        r.spray = M.spray;
+        r.books = M.d_books;
+        window::Job* jobs = const_cast<window::Job*>(TAB(window::Job, L.off_jobs));
+        for (int k = 0; k < 2 * L.np; ++k) jl[q++] = jobs + k;
+        mx_owner = std::max(mx_owner, r.n_owner);
+        mx_cells = std::max(mx_cells, r.np * r.fres * r.fres);
+        mx_finish = std::max(mx_finish, r.zero_blocks + r.n_apply);
+        mx_push = std::max(mx_push, L.push_cells_max);
+        mx_pgroups = std::max(mx_pgroups, L.n_push_groups);
+        mx_peel = std::max(mx_peel, L.peel_cells_max);
+        mx_qgroups = std::max(mx_qgroups, L.n_peel_groups);
+        mx_restrict = std::max(mx_restrict, r.ncap + r.rblocks);
+        mx_cpush = std::max(mx_cpush, r.cpush_w * r.cpush_h);
+    }
+    FCK(cudaMemcpyAsync(B->d_buf[slot], B->h_buf[slot], need, cudaMemcpyHostToDevice, st));
+    FCK(cudaEventRecord(B->ev[slot], st));
+    const FineRec* d = reinterpret_cast<const FineRec*>(B->d_buf[slot]);
+    window::Job* const* djl = reinterpret_cast<window::Job* const*>(B->d_buf[slot] + rec_bytes);
+    const unsigned nz = (unsigned)n;
+#define BLAUNCH(kern, gx, gy, threads)                                           \
+    do {                                                                          \
+        kern<<<dim3((unsigned)(gx), (unsigned)(gy), nz), (threads), 0, st>>>(d); \
+        ::silt::count_launch();                                                   \
+        FCK(cudaGetLastError());                                                  \
+    } while (0)
+    BLAUNCH(kb_scatter, launch_blocks((size_t)mx_owner), 1, 256);
+    BLAUNCH(kb_refine, launch_blocks((size_t)mx_cells), 1, 256);
+    BLAUNCH(kb_lay_finish, mx_finish, 1, 128);
+    BLAUNCH(kb_push, launch_blocks((size_t)mx_push), mx_pgroups + 1, 256);
+    FCK(window::launch_window_step_list(djl, (int)njobs, max_fres, st));
+    if (mx_qgroups) BLAUNCH(kb_peel_patches, launch_blocks((size_t)mx_peel), mx_qgroups, 256);
+    BLAUNCH(kb_restrict, mx_restrict, 1, 128);
+    BLAUNCH(kb_release, launch_blocks((size_t)mx_cells), 1, 256);
+    BLAUNCH(kb_coarse_push, launch_blocks((size_t)mx_cpush), 1, 256);
+#undef BLAUNCH
+    return SILT_OK;
+}
+
+int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::vector<Patches*>& patches,
+               cudaStream_t st) {
+    const int n = (int)sheets.size();
+    if (n == 0) return SILT_OK;
+    const int slot = B->peel_flip;
+    B->peel_flip ^= 1;
+    if (B->peel_ev[slot]) FCK(cudaEventSynchronize(B->peel_ev[slot]));
+    if ((size_t)n > B->peel_cap[slot]) {
+        cudaFree(B->d_peel[slot]);
+        if (B->h_peel[slot]) cudaFreeHost(B->h_peel[slot]);
+        B->d_peel[slot] = nullptr;
+        B->h_peel[slot] = nullptr;
+        B->peel_cap[slot] = 0;
+        FCK(cudaMalloc(&B->d_peel[slot], 2 * (size_t)n * sizeof(PeelRec)));
+        FCK(cudaMallocHost(&B->h_peel[slot], 2 * (size_t)n * sizeof(PeelRec)));
+        B->peel_cap[slot] = 2 * (size_t)n;
+    }
+    if (!B->peel_ev[slot]) FCK(cudaEventCreateWithFlags(&B->peel_ev[slot], cudaEventDisableTiming));
+    int mx = 1;
+    for (int w = 0; w < n; ++w) {
+        silt_sheet* s = sheets[w];
+        Patches& P = *patches[w];
+        Impl& M = I(P);
+        HostState& HS = H(P);
+        const StepPlan& L = HS.plan;
+        PeelRec& r = B->h_peel[slot][w];
+        memset(&r, 0, sizeof r);
+        r.W = view_of(s);
+        r.jobs = TAB(PushJob, L.coarse_peel.off);
+        r.n = L.coarse_peel.n;
+        r.i0 = L.coarse_peel.i0;
+        r.j0 = L.coarse_peel.j0;
+        r.w = L.coarse_peel.n ? L.coarse_peel.w : 0;
+        r.h = L.coarse_peel.n ? L.coarse_peel.h : 0;
+        r.owner = M.owner;
+        r.spray = M.spray;
+        r.counters = M.counters;
+        r.books = M.d_books;
+        mx = std::max(mx, r.w * r.h);
+    }
+    FCK(cudaMemcpyAsync(B->d_peel[slot], B->h_peel[slot], n * sizeof(PeelRec), cudaMemcpyHostToDevice, st));
+    FCK(cudaEventRecord(B->peel_ev[slot], st));
+    kb_coarse_peel<<<dim3((unsigned)launch_blocks((size_t)mx), 1, (unsigned)n), 256, 0, st>>>(B->d_peel[slot]);
+    ::silt::count_launch();
+    FCK(cudaGetLastError());
+    return SILT_OK;
+}
 
 }  // namespace fine
 }  // namespace silt

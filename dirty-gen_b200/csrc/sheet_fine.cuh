@@ -79,6 +79,23 @@ int restrict_all(Patches& P, silt_sheet* s);
 int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, float dt, StepOut& out);
 // peel_spray on the coarse window, held columns skipped (src/fluid_core.rs:6071).
 int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, StepOut& out);
+
+// Batched windows: step_patches and peel_coarse split so that many windows
+// share each launch. batch_prepare (per window, on any host thread, with the
+// sheet's stream pointing at that thread's stream) plans the patches and
+// uploads the window's tables, or runs the tire-less path; it sets *has_work
+// when the window's patches go to the batched launches. batch_launch then
+// steps every such window's patches on `st` (after the uploads), and
+// batch_peel, after the coarse step, peels their coarse cells.
+struct FineBatch;
+FineBatch* batch_new();
+void batch_free(FineBatch* B);
+int batch_prepare(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, float dt, StepOut& out,
+                  bool* has_work);
+int batch_launch(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::vector<Patches*>& patches, float dt,
+                 cudaStream_t st);
+int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::vector<Patches*>& patches,
+               cudaStream_t st);
 int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out);
 // FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s);

@@ -736,9 +736,18 @@ namespace {
 // The parts of silt_step before the coarse pair: the tire pushes of the step,
 // the inflow strip, the nested patches (refine, shove, fine pair, peel,
 // restrict, shove outside).
+int step_inflow(silt_sheet* s, float dt);
+
 int step_before_coarse(silt_sheet* s, float dt, std::vector<silt_tire_push>& ps, silt::fine::StepOut& fo) {
     ps.clear();
     ps.swap(s->pushes);
+    int rc = step_inflow(s, dt);
+    if (rc) return rc;
+    return silt::fine::step_patches(s->fine, s, ps, dt, fo);
+}
+
+// The inflow strip's share of the step (a build addition, booked as opened).
+int step_inflow(silt_sheet* s, float dt) {
     if (s->inflow_j >= 0) {
         int nc = s->inflow_i1 - s->inflow_i0;
         float add = s->inflow_rate * dt / ((float)nc * s->cfg.cell * s->cfg.cell);
@@ -747,7 +756,7 @@ int step_before_coarse(silt_sheet* s, float dt, std::vector<silt_tire_push>& ps,
                            s->inflow_i1, add, W.tiles_x, W.t_wet[0], W.t_zuv[0], W.t_zh[0], s->st));
         s->opened_m3 += (double)add * (double)s->cfg.cell * (double)s->cfg.cell * (double)nc;
     }
-    return silt::fine::step_patches(s->fine, s, ps, dt, fo);
+    return SILT_OK;
 }
 
 }  // namespace
@@ -1096,7 +1105,8 @@ struct BatchWorkers {
 struct silt_batch {
     std::vector<silt_sheet*> sheets;
     BatchWorkers* workers = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_coarse = nullptr;
+    silt::fine::FineBatch* fine = nullptr;  // staging of the batched nested-patch launches
+    cudaEvent_t ev_start = nullptr;
     cudaStream_t st = nullptr;
     int device = 0;
     int max_tiles = 0;              // the largest window's tile count per layer
@@ -1124,8 +1134,8 @@ int batch_free(silt_batch* b) {
     if (!b) return SILT_OK;
     if (b->st) cudaStreamSynchronize(b->st);
     delete b->workers;
+    silt::fine::batch_free(b->fine);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
-    if (b->ev_coarse) cudaEventDestroy(b->ev_coarse);
     cudaFree(b->list);
     cudaFree(b->entry_win);
     cudaFree(b->count);
@@ -1282,8 +1292,8 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
         }
         e = cudaMemcpy(b->d_ledger_src, src.data(), src.size() * sizeof(double*), cudaMemcpyHostToDevice);
     }
+    b->fine = silt::fine::batch_new();
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_coarse, cudaEventDisableTiming);
     if (e == cudaSuccess) {
         unsigned hw = std::thread::hardware_concurrency();
         const int k = std::max(1, std::min({8, (int)(hw ? hw : 1), n}));
@@ -1329,46 +1339,53 @@ int silt_batch_step(silt_batch* b, float dt) {
     std::vector<silt::fine::StepOut> fo(n);
     BatchWorkers& Wk = *b->workers;
     const int nk = (int)Wk.threads.size();
-    // One window's part before (phase 0) or after (phase 1) the coarse pairs,
-    // on worker k's stream in place of the sheet's own.
-    auto per_window = [&](int phase, cudaEvent_t after) {
-        Wk.run([&, phase, after](int k) {
-            Wk.rc[k] = 0;
-            cudaStream_t wst = Wk.streams[k];
-            cudaError_t e = cudaStreamWaitEvent(wst, after, 0);
-            for (int w = k; w < n && e == cudaSuccess && Wk.rc[k] == 0; w += nk) {
-                silt_sheet* s = b->sheets[w];
-                if (phase == 1 && ps[w].empty()) continue;
-                cudaStream_t own = s->st;
-                s->st = wst;
-                Wk.rc[k] = phase == 0 ? step_before_coarse(s, dt, ps[w], fo[w])
-                                      : silt::fine::peel_coarse(s->fine, s, ps[w], fo[w]);
-                s->st = own;
-                if (Wk.rc[k]) Wk.err[k] = silt_last_error();
-            }
-            if (e == cudaSuccess) e = cudaEventRecord(Wk.done[k], wst);
-            if (e != cudaSuccess && Wk.rc[k] == 0) {
-                Wk.rc[k] = SILT_ECUDA;
-                Wk.err[k] = std::string("batch worker: ") + cudaGetErrorString(e);
-            }
-        });
-        for (int k = 0; k < nk; ++k) {
-            if (Wk.rc[k]) {
-                snprintf(g_err, sizeof g_err, "%s", Wk.err[k].c_str());
-                return Wk.rc[k];
-            }
-        }
-        for (int k = 0; k < nk; ++k) CK(cudaStreamWaitEvent(b->st, Wk.done[k], 0));
-        return SILT_OK;
-    };
-    int rc;
+    std::vector<char> work(n, 0);
     for (auto& c : Wk.launches) c = 0;
-    CK(cudaEventRecord(b->ev_start, b->st));
-    if ((rc = per_window(0, b->ev_start))) return rc;
+    CK(cudaEventRecord(b->ev_start, b->st));  // the workers' streams start after the batch's previous work
+    // Each window's tire pushes, inflow and nested-patch planning on the
+    // workers (the planning uploads the window's tables on the worker's
+    // stream); the patches themselves step in the batched launches below.
+    Wk.run([&](int k) {
+        Wk.rc[k] = 0;
+        cudaStream_t wst = Wk.streams[k];
+        cudaError_t e = cudaStreamWaitEvent(wst, b->ev_start, 0);
+        for (int w = k; w < n && e == cudaSuccess && Wk.rc[k] == 0; w += nk) {
+            silt_sheet* s = b->sheets[w];
+            cudaStream_t own = s->st;
+            s->st = wst;
+            ps[w].clear();
+            ps[w].swap(s->pushes);
+            bool has = false;
+            Wk.rc[k] = step_inflow(s, dt);
+            if (!Wk.rc[k]) Wk.rc[k] = silt::fine::batch_prepare(s->fine, s, ps[w], dt, fo[w], &has);
+            work[w] = has ? 1 : 0;
+            s->st = own;
+            if (Wk.rc[k]) Wk.err[k] = silt_last_error();
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(Wk.done[k], wst);
+        if (e != cudaSuccess && Wk.rc[k] == 0) {
+            Wk.rc[k] = SILT_ECUDA;
+            Wk.err[k] = std::string("batch worker: ") + cudaGetErrorString(e);
+        }
+    });
+    for (int k = 0; k < nk; ++k)
+        if (Wk.rc[k]) {
+            snprintf(g_err, sizeof g_err, "%s", Wk.err[k].c_str());
+            return Wk.rc[k];
+        }
+    int rc;
+    for (int k = 0; k < nk; ++k) CK(cudaStreamWaitEvent(b->st, Wk.done[k], 0));
+    std::vector<silt_sheet*> fs;
+    std::vector<silt::fine::Patches*> fp;
+    for (int w = 0; w < n; ++w)
+        if (work[w]) {
+            fs.push_back(b->sheets[w]);
+            fp.push_back(&b->sheets[w]->fine);
+        }
+    if ((rc = silt::fine::batch_launch(b->fine, fs, fp, dt, b->st))) return rc;
     const clock::time_point t1 = clock::now();
     if ((rc = batch_coarse(b, dt))) return rc;
-    CK(cudaEventRecord(b->ev_coarse, b->st));
-    if ((rc = per_window(1, b->ev_coarse))) return rc;
+    if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
     for (int w = 0; w < n; ++w) {
         silt_sheet* s = b->sheets[w];
         s->parts.steps += 1;
@@ -1417,6 +1434,15 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         L.opened_m3 = s->opened_m3;
         L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3;
     }
+    return SILT_OK;
+}
+
+int silt_batch_push_tires(silt_batch* b, const int32_t* windows, const silt_tire_push* pushes, int32_t n) {
+    if (!b || n < 0 || (n > 0 && (!windows || !pushes))) return fail_arg("batch_push_tires");
+    const int nw = (int)b->sheets.size();
+    for (int k = 0; k < n; ++k)
+        if (windows[k] < 0 || windows[k] >= nw) return fail_arg("batch_push_tires: window index");
+    for (int k = 0; k < n; ++k) b->sheets[windows[k]]->pushes.push_back(pushes[k]);
     return SILT_OK;
 }
 

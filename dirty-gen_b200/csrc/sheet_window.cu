@@ -682,15 +682,6 @@ __device__ __forceinline__ bool boxes_touch(int a0, int a1, int a2, int a3, int 
     return ss(a0) <= b1 + 1 && ss(b0) <= a1 + 1 && ss(a2) <= b3 + 1 && ss(b2) <= a3 + 1;
 }
 
-__device__ __forceinline__ int uf_find(const int* L, int x) {
-    for (int n = 0; n < (1 << 20); ++n) {
-        int p = L[x];
-        if (p == x || p < 0) return x;
-        x = p;
-    }
-    return x;
-}
-
 __device__ void set_whole(Shared& S, int x0, int x1, int y0, int y1) {
     if (threadIdx.x == 0) {
         S.nbox = 1;
@@ -703,8 +694,8 @@ __device__ void set_whole(Shared& S, int x0, int x1, int y0, int y1) {
 }
 
 // sheet_work_boxes (src/fluid_core.rs:1325-1447). Wet bodies are labelled in
-// the f2 plane (as ints) by union-find; a body's root is its first wet cell
-// in raster order, the order the reference's run merge keeps.
+// the f2 plane (as ints) by hooking and pointer jumping; a body's root is its
+// first wet cell in raster order, the order the reference's run merge keeps.
 __device__ void cta_wet_boxes(Shared& S, const Job& J) {
     const int res = J.res;
     const float eps = J.eps;
@@ -741,21 +732,27 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
     int* L = reinterpret_cast<int*>(J.f2);
     CTA_RECT(i0, i1, j0, j1, { L[g] = J.h[g] > eps ? g : -1; })
     __syncthreads();
+    // Hook and jump: each round lowers the label of the larger of two
+    // neighbours' labels to the smaller, then moves every cell one step up its
+    // chain. Labels only fall and stay inside the body; when a round changes
+    // nothing, every cell holds its body's smallest index (its first raster
+    // cell), in O(log) rounds and without walking long chains.
     for (int round = 0; round < 4096; ++round) {
         if (threadIdx.x == 0) S.changed = 0;
         __syncthreads();
         CTA_RECT(i0, i1, j0, j1, {
-            if (L[g] >= 0) {
-                if (i < i1 && L[g + 1] >= 0) {
-                    int a = uf_find(L, g), c = uf_find(L, g + 1);
-                    if (a != c) {
+            const int a = L[g];
+            if (a >= 0) {
+                if (i < i1) {
+                    const int c = L[g + 1];
+                    if (c >= 0 && a != c) {
                         atomicMin(&L[max(a, c)], min(a, c));
                         S.changed = 1;
                     }
                 }
-                if (j < j1 && L[g + res] >= 0) {
-                    int a = uf_find(L, g), c = uf_find(L, g + res);
-                    if (a != c) {
+                if (j < j1) {
+                    const int c = L[g + res];
+                    if (c >= 0 && a != c) {
                         atomicMin(&L[max(a, c)], min(a, c));
                         S.changed = 1;
                     }
@@ -764,7 +761,14 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
         })
         __syncthreads();
         CTA_RECT(i0, i1, j0, j1, {
-            if (L[g] >= 0) L[g] = uf_find(L, g);
+            const int a = L[g];
+            if (a >= 0) {
+                const int c = L[a];
+                if (c != a) {
+                    L[g] = c;
+                    S.changed = 1;
+                }
+            }
         })
         __syncthreads();
         if (!S.changed) break;
@@ -875,15 +879,25 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
 // soften_border (src/fluid_core.rs:9594-9622) on the whole layer.
 __device__ void cta_soften(const Job& J) {
     const int res = J.res, edge = J.soften_edge;
-    CLU_RECT(0, res - 1, 0, res - 1, {
-        int d = min(min(i, res - 1 - i), min(j, res - 1 - j));
-        if (d < edge) {
-            float t = (float)d / (float)edge;
-            float w = t * t * (3.0f - 2.0f * t);
-            J.u[g] *= w;
-            J.v[g] *= w;
-        }
-    })
+    // The band's rows and columns: [0, lo] and [hi, res).
+    const int lo = min(edge, res) - 1, hi = min(max(edge, res - edge), res);
+#define SOFTEN_CELL                                                     \
+    {                                                                   \
+        int d = min(min(i, res - 1 - i), min(j, res - 1 - j));          \
+        if (d < edge) {                                                 \
+            float t = (float)d / (float)edge;                           \
+            float w = t * t * (3.0f - 2.0f * t);                        \
+            J.u[g] *= w;                                                \
+            J.v[g] *= w;                                                \
+        }                                                               \
+    }
+    // Only the band within `edge` of the border: the top and bottom rows,
+    // then the left and right columns of the rows between.
+    CLU_RECT(0, res - 1, 0, lo, SOFTEN_CELL)
+    CLU_RECT(0, res - 1, hi, res - 1, SOFTEN_CELL)
+    CLU_RECT(0, lo, lo + 1, hi - 1, SOFTEN_CELL)
+    CLU_RECT(hi, res - 1, lo + 1, hi - 1, SOFTEN_CELL)
+#undef SOFTEN_CELL
     crew_sync();
 }
 
@@ -984,19 +998,28 @@ __device__ int window_body(Shared& S, const Job& J) {
     return gs_passes;
 }
 
-__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
+__device__ __forceinline__ void window_job(Job* jp) {
     __shared__ Shared S;
     __shared__ Job Js;
-    const int job = (int)(blockIdx.x / (unsigned)crew_size());
     // The job's fields live in shared memory for the step: every phase reads
     // them, and a copy on the thread's stack would be reloaded from local
     // memory after each store through a plane pointer.
-    if (threadIdx.x == 0) Js = jobs[job];
+    if (threadIdx.x == 0) Js = *jp;
     __syncthreads();
     if (!Js.active) return;  // the same for the whole crew
     const int gs_passes = window_body(S, Js);
-    if (threadIdx.x == 0 && crew_rank() == 0) jobs[job].gs_iters = gs_passes;
+    if (threadIdx.x == 0 && crew_rank() == 0) jp->gs_iters = gs_passes;
     crew_sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Job k of an array.
+__global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
+    window_job(jobs + blockIdx.x / (unsigned)crew_size());
+}
+
+// Job k of a list of jobs that live in different tables (batched windows).
+__global__ void __launch_bounds__(NT, 1) k_window_step_list(Job* const* jobs) {
+    window_job(jobs[blockIdx.x / (unsigned)crew_size()]);
 }
 
 // CTAs per job: enough warps for one (row, 32-cell chunk) item each on a
@@ -1037,9 +1060,35 @@ static int crew_limit(cudaStream_t st) {
     return limit;
 }
 
+// The crew for `njobs` jobs: as large as the window and the device allow, and
+// small enough that all the jobs' CTAs fit on the GPU about twice over.
+static int crew_of(int njobs, int max_res, cudaStream_t st) {
+    return std::max(1, std::min({crew_for(max_res), crew_limit(st), 296 / std::max(njobs, 1)}));
+}
+
+cudaError_t launch_window_step_list(Job* const* d_job_list, int njobs, int max_res, cudaStream_t st) {
+    if (njobs <= 0) return cudaSuccess;
+    const int crew = crew_of(njobs, max_res, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(njobs * crew), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)crew;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step_list, d_job_list);
+    ::silt::count_launch();
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st) {
     if (njobs <= 0) return cudaSuccess;
-    const int crew = std::min(crew_for(max_res), crew_limit(st));
+    const int crew = crew_of(njobs, max_res, st);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(njobs * crew), 1, 1);
     cfg.blockDim = dim3(NT, 1, 1);

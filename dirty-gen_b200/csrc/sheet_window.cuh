@@ -47,6 +47,8 @@ struct Job {
 // One cluster of CTAs steps each job, its size chosen from `max_res`, the
 // largest window side among the jobs.
 cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaStream_t st);
+// The same for jobs addressed through a device array of pointers.
+cudaError_t launch_window_step_list(Job* const* d_job_list, int njobs, int max_res, cudaStream_t st);
 size_t window_static_smem();
 
 // Planes of scratch one window layer needs beyond its own h, u, v: two

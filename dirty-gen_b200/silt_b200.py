@@ -109,6 +109,7 @@ def lib():
             "silt_batch_create": [ctypes.POINTER(_p), _i, ctypes.POINTER(_p)],
             "silt_batch_destroy": [_p], "silt_batch_step": [_p, _f],
             "silt_batch_get_ledgers": [_p, ctypes.POINTER(Ledger)],
+            "silt_batch_push_tires": [_p, _p, ctypes.POINTER(TirePush), _i],
             "silt_batch_set_timing": [_p, _i], "silt_batch_get_parts": [_p, ctypes.POINTER(StepParts)],
         }.items():
             fn = getattr(L, name)
@@ -318,6 +319,15 @@ class Batch:
 
     def step(self, dt):
         return check(lib().silt_batch_step(self.h, dt), "batch_step")
+
+    def push_tires(self, windows, tires):
+        """Tire pushes for many windows: tires[k] (a dict as for Sheet.push_tire) goes to window windows[k]."""
+        n = len(tires)
+        if n == 0:
+            return
+        idx = np.ascontiguousarray(windows, dtype=np.int32)
+        arr = (TirePush * n)(*[make_push(t) for t in tires])
+        check(lib().silt_batch_push_tires(self.h, _ptr(idx), arr, n), "batch_push_tires")
 
     def ledgers(self):
         arr = (Ledger * len(self.sheets))()

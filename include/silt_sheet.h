@@ -195,6 +195,9 @@ typedef struct silt_batch silt_batch;
 int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out);
 int silt_batch_destroy(silt_batch* b);
 int silt_batch_step(silt_batch* b, float dt);
+/* silt_push_tire for many windows at once: pushes[k] goes to the window at
+ * batch index windows[k] (in call order within each window). */
+int silt_batch_push_tires(silt_batch* b, const int32_t* windows, const silt_tire_push* pushes, int32_t n);
 /* Every window's ledger (out: one per window, in batch order) with one copy
  * back and one wait, as silt_get_ledger gives them one at a time. */
 int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out);

@@ -36,11 +36,15 @@ def test_batch_step_equals_single_steps():
     grouped = [make(sc, o.get("fast", False), stream.cuda_stream) for sc, o in zip(scenes, opts)]
     batch = G.Batch(grouped)
     for k in range(1, 25):
+        idx, tires = [], []
         for w, o in enumerate(opts):
             if o.get("tires"):
                 push(alone[w], k, 2 + w % 3)
-                push(grouped[w], k, 2 + w % 3)
+                for t in S.tires_at(k * DT, speed=5.0, z0=-3.0)[:2 + w % 3]:
+                    idx.append(w)
+                    tires.append(t)
             alone[w].step(DT, want_spray=False)
+        batch.push_tires(idx, tires)  # the batch's bulk form of push_tire
         batch.step(DT)
     for w in range(len(scenes)):
         for name in ("water", "slurry", "uw", "vw", "us", "vs"):
