@@ -467,16 +467,30 @@ def run_batch(args):
     batch = silt_b200.Batch(sheets)
     cells = batch_cells(wins)
     step_no = 0
+    # Every window's tires as one record array: the same pushes batch_tires
+    # gives, with z advanced in place each step (float32, as tires_at does).
+    import numpy as np
+
+    f32 = np.float32
+    idx, recs, zbase, zrow = [], [], [], []
+    for k, w in enumerate(wins):
+        for q, t in enumerate(batch_tires(0, w)):
+            idx.append(k)
+            recs.append(t)
+            zbase.append(f32(0.0) + f32(-0.5 * w["res"] * CELL))  # center z + z0, as tires_at sums them
+            zrow.append(f32((-0.5, -0.5, 0.5, 0.5)[q] * 2.4))       # the tire's offset along the wheelbase
+    idx = np.asarray(idx, np.int32)
+    push_rec = np.zeros(len(recs), silt_b200.TIRE_DTYPE)
+    for name in silt_b200.TIRE_DTYPE.names:
+        push_rec[name] = [r[name] for r in recs]
+    zbase = np.asarray(zbase, f32)
+    zrow = np.asarray(zrow, f32)
 
     def one_step():
         nonlocal step_no
         step_no += 1
-        idx, tires = [], []
-        for k, w in enumerate(wins):
-            for t in batch_tires(step_no, w):
-                idx.append(k)
-                tires.append(t)
-        batch.push_tires(idx, tires)
+        push_rec["z"] = (zbase + f32(5.0) * f32(step_no * DT)) + zrow
+        batch.push_tires(idx, push_rec)
         batch.step(DT)
 
     for _ in range(max(3, args.warmup)):

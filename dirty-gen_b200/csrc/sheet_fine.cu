@@ -1129,8 +1129,10 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
             long ci = coarse_axis(W.origin[0], W.cell, res, ps[q].x);
             long cj = coarse_axis(W.origin[1], W.cell, res, ps[q].z);
             if (ci >= 0 && cj >= 0 && M.h_owner[cj * res + ci] >= 0) continue;
-            push.push_back(make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, push_reach(ps[q], W.cell)));
-            L.coarse_pushed.push_back((int)q);
+            const PushJob J = make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, push_reach(ps[q], W.cell));
+            push.push_back(J);
+            // A shove whose span misses the window touches no coarse cell.
+            if (J.span_i0 < J.span_i1 && J.span_j0 < J.span_j1) L.coarse_pushed.push_back((int)q);
         }
         L.coarse_push = job_list(tab, push);
         L.coarse_peel = job_list(tab, peel);

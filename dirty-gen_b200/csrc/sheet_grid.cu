@@ -83,8 +83,47 @@ constexpr int ENTRY_TILE = (1 << 28) - 1;
 // Cell material: viscosity, mobility and damping factor.
 __device__ __forceinline__ float cell_nu(const LayerParams& P, size_t g) {
     if (P.nu_mode == NU_CONST) return P.nu_c;
-    if (P.nu_mode == NU_PLANE) return P.nu_plane[g];
+    if (P.nu_mode == NU_PLANE || P.nu_mode == NU_TABLE) return P.nu_plane[g];
     return dynamic_viscosity(P.grain[g], P.moisture[g]);
+}
+
+// sheet_mobility_for(nu) of the cell.
+__device__ __forceinline__ float cell_mob(const LayerParams& P, size_t g) {
+    if (P.nu_mode == NU_CONST) return P.mob_c;
+    if (P.nu_mode == NU_TABLE) return P.mob_plane[g];
+    return sheet_mobility_for(cell_nu(P, g));
+}
+
+// The cell's damping factor over dt: exp(-sheet_damp(nu) dt).
+__device__ __forceinline__ float cell_decay(const LayerParams& P, size_t g, float dt) {
+    if (P.nu_mode == NU_CONST) return P.decay_c;
+    const float rate = P.nu_mode == NU_TABLE ? P.damp_plane[g] : sheet_damp(cell_nu(P, g));
+    return expf(-rate * dt);
+}
+
+// Every cell of the tile's region of radius (RX, RY): f(gx, gy, s, g) with s
+// the shared-memory index and g the global one. Edge tiles clip the region to
+// the grid and walk it one warp per row; interior tiles walk the rectangle as
+// one flat range (a compile-time width), which keeps every lane busy.
+template <bool EDGE, int RX, int RY, class F>
+__device__ __forceinline__ void region(int tx0, int ty0, int res, F f) {
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    if (EDGE) {
+        const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+        constexpr int NW = FORCE_THREADS / 32;
+        const int x0 = max(0, tx0 - RX), x1 = min(res, tx0 + FT + RX);
+        const int y0 = max(0, ty0 - RY), y1 = min(res, ty0 + FT + RY);
+        for (int gy = y0 + wy; gy < y1; gy += NW)
+            for (int gx = x0 + lane; gx < x1; gx += 32)
+                f(gx, gy, (gy - oy) * FW + (gx - ox), (size_t)gy * res + gx);
+    } else {
+        constexpr int W = FT + 2 * RX, H = FT + 2 * RY;
+        for (int k = threadIdx.x; k < W * H; k += FORCE_THREADS) {
+            const int r = k / W;
+            const int gy = ty0 - RY + r, gx = tx0 - RX + (k - r * W);
+            f(gx, gy, (gy - oy) * FW + (gx - ox), (size_t)gy * res + gx);
+        }
+    }
 }
 
 // One force tile. EDGE = false for tiles whose whole radius-9 region lies at
@@ -105,32 +144,19 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
     const int ox = tx0 - FH, oy = ty0 - FH;
     const float cell = P.cell, dt = P.dt, eps = P.eps;
     const float two = 2.0f * cell;
-    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
-    constexpr int NW = FORCE_THREADS / 32;
-#define REGION(rx, ry)                                                                  \
-    const int x0 = EDGE ? max(0, tx0 - (rx)) : tx0 - (rx);                              \
-    const int x1 = EDGE ? min(res, tx0 + FT + (rx)) : tx0 + FT + (rx);                  \
-    const int y0 = EDGE ? max(0, ty0 - (ry)) : ty0 - (ry);                              \
-    const int y1 = EDGE ? min(res, ty0 + FT + (ry)) : ty0 + FT + (ry);                  \
-    for (int gy = y0 + wy; gy < y1; gy += NW)                                           \
-        for (int gx = x0 + lane; gx < x1; gx += 32) {                                   \
-            const int s = (gy - oy) * FW + (gx - ox);                                   \
-            const size_t g = (size_t)gy * res + gx;                                     \
-            (void)g;
-#define END_REGION }
 #define NX(d) (EDGE ? (gy - oy) * FW + (clampi(gx + (d), 0, res - 1) - ox) : s + (d))
 #define NZ(d) (EDGE ? (clampi(gy + (d), 0, res - 1) - oy) * FW + (gx - ox) : s + (d) * FW)
 
     // 1. eta and depth on radius 9.
-    { REGION(FH, FH)
+    region<EDGE, FH, FH>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         float hv = P.h[g];
         HS[s] = hv;
         E[s] = P.bed[g] + hv;
-    END_REGION }
+    });
     __syncthreads();
     // 2. Velocity on radius 6: the lazy dry cut of the previous substep, then
     //    the soft window border (src/fluid_core.rs:9594-9622).
-    { REGION(6, 6)
+    region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         float uu = P.u[g], vv = P.v[g];
         if (P.apply_cut && HS[s] < eps) { uu = 0.0f; vv = 0.0f; }
         if (P.soften_edge > 0) {
@@ -144,48 +170,48 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
         }
         U[s] = uu;
         V[s] = vv;
-    END_REGION }
+    });
     //    x pass of both pressure blurs: rows radius 9, columns radius 7.
-    { REGION(7, FH)
+    region<EDGE, 7, FH>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
         float e0 = E[NX(-2)], e1 = E[NX(-1)], e2 = E[s], e3 = E[NX(1)], e4 = E[NX(2)];
         TG[s] = tap5(e0, e1, e2, e3, e4, kG0, kG1, kG2, in);
         TS[s] = tap5(e0, e1, e2, e3, e4, kS0, kS1, kS2, in);
-    END_REGION }
+    });
     __syncthreads();
     // 3. z pass and the pressure: p = 0.45 (0.62 G + 0.38 S) + 0.55 eta, radius 7.
-    { REGION(7, 7)
+    region<EDGE, 7, 7>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
         const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
         float gb = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
         float sc = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
         float filtered = 0.62f * gb + 0.38f * sc;
         PB[s] = 0.45f * filtered + 0.55f * E[s];
-    END_REGION }
+    });
     __syncthreads();
     // 4. Gravity down the pressure gradient on wet cells, radius 6
     //    (src/fluid_core.rs:2234-2253).
-    { REGION(6, 6)
+    region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         if (HS[s] > eps) {
             float px = (PB[NX(1)] - PB[NX(-1)]) / two;
             float pz = (PB[NZ(1)] - PB[NZ(-1)]) / two;
-            float mob = P.nu_mode == NU_CONST ? P.mob_c : sheet_mobility_for(cell_nu(P, g));
+            float mob = cell_mob(P, g);
             U[s] += -kGravity * px * mob * dt;
             V[s] += -kGravity * pz * mob * dt;
         }
-    END_REGION }
+    });
     __syncthreads();
     // 5. Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
     if (P.vort > 0.0f) {
-        { REGION(5, 5)
+        region<EDGE, 5, 5>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             float dvdx = (V[NX(1)] - V[NX(-1)]) / two;
             float dudz = (U[NZ(1)] - U[NZ(-1)]) / two;
             WQ[s] = dvdx - dudz;
-        END_REGION }
+        });
         __syncthreads();
         // 6. Confinement kick from that snapshot, in place, radius 4
         //    (src/fluid_core.rs:2348-2375, :2441-2470).
-        { REGION(4, 4)
+        region<EDGE, 4, 4>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             if (HS[s] > eps) {
                 float w = WQ[s];
                 if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
@@ -201,13 +227,13 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
                     }
                 }
             }
-        END_REGION }
+        });
         __syncthreads();
     }
     if (P.project) {
         // 7. b = div * overload - 0.015 * overload * lap(eta), radius 3
         //    (src/fluid_core.rs:1992-2003).
-        { REGION(3, 3)
+        region<EDGE, 3, 3>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const int sxp = NX(1), sxm = NX(-1), szp = NZ(1), szm = NZ(-1);
             float ux = (U[sxp] - U[sxm]) / (2.0f * cell);
             float vz = (V[szp] - V[szm]) / (2.0f * cell);
@@ -216,29 +242,29 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
             float lap_h = lsum / (cell * cell);
             float overload = 1.0f + rclamp(cell_nu(P, g) / 231.0f, 0.0f, 6.0f);
             PB[s] = div * overload - 0.015f * overload * lap_h;
-        END_REGION }
+        });
         __syncthreads();
         // 8. x pass of both blurs of b: rows radius 3, columns radius 1.
-        { REGION(1, 3)
+        region<EDGE, 1, 3>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
             float b0 = PB[NX(-2)], b1 = PB[NX(-1)], b2 = PB[s], b3 = PB[NX(1)], b4 = PB[NX(2)];
             TG[s] = tap5(b0, b1, b2, b3, b4, kG0, kG1, kG2, in);
             TS[s] = tap5(b0, b1, b2, b3, b4, kS0, kS1, kS2, in);
-        END_REGION }
+        });
         __syncthreads();
         // 9. q = 0.62 G(b) + 0.38 S(b), radius 1 (src/fluid_core.rs:2004-2011).
-        { REGION(1, 1)
+        region<EDGE, 1, 1>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
             const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
             float gq = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
             float sq = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
             WQ[s] = 0.62f * gq + 0.38f * sq;
-        END_REGION }
+        });
         __syncthreads();
     }
     // 10. Projection kick, damping and the speed clamp on wet cells
     //     (src/fluid_core.rs:2015-2037); every cell of the tile is written.
-    { REGION(0, 0)
+    region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         float uu = U[s], vv = V[s];
         if (HS[s] > eps) {
             if (P.project) {
@@ -247,15 +273,13 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
                 uu += 0.012f * dt * qx;
                 vv += 0.012f * dt * qz;
             }
-            float decay = P.nu_mode == NU_CONST ? P.decay_c : expf(-sheet_damp(cell_nu(P, g)) * dt);
+            float decay = cell_decay(P, g, dt);
             uu = finite_speed(uu * decay, kSpeedCap);
             vv = finite_speed(vv * decay, kSpeedCap);
         }
         P.u_out[g] = uu;
         P.v_out[g] = vv;
-    END_REGION }
-#undef REGION
-#undef END_REGION
+    });
 #undef NX
 #undef NZ
 }
@@ -809,6 +833,24 @@ cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cuda
     (void)res;
     (void)layers;
     k_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_material(const uint8_t* grain, const float* moisture, float* nu, float* mob, float* damp, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float x = dynamic_viscosity(grain[i], moisture[i]);
+        nu[i] = x;
+        mob[i] = sheet_mobility_for(x);
+        damp[i] = sheet_damp(x);
+    }
+}
+
+cudaError_t launch_material(const uint8_t* grain, const float* moisture, float* nu, float* mob, float* damp, size_t n,
+                            cudaStream_t st) {
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_material<<<blocks, 256, 0, st>>>(grain, moisture, nu, mob, damp, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -9,7 +9,8 @@ namespace silt {
 enum NuMode : int32_t {
     NU_CONST = 0,   // one viscosity for the whole layer (the water sheet, 0.9 Pa s)
     NU_PLANE = 1,   // a float viscosity per cell (the free step_sheet operator)
-    NU_GRAIN = 2,   // dynamic_viscosity(grain, moisture) per cell (the slurry sheet)
+    NU_GRAIN = 2,   // dynamic_viscosity(grain, moisture) per cell
+    NU_TABLE = 3,   // nu_plane, mob_plane, damp_plane: the laws evaluated once per cell beforehand (the slurry sheet)
 };
 
 struct LayerParams {
@@ -22,6 +23,8 @@ struct LayerParams {
     const uint8_t* grain;
     const float* moisture;
     const float* nu_plane;
+    const float* mob_plane;   // NU_TABLE
+    const float* damp_plane;  // NU_TABLE
     int32_t nu_mode;
     float nu_c, mob_c, decay_c;  // NU_CONST: viscosity, mobility and damping factor
     int32_t res;
@@ -134,6 +137,10 @@ cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], con
 size_t transport_smem_bytes();
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st);
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st);
+// The slurry's material laws per cell: viscosity, mobility and damping rate
+// from grain and moisture (dynamic_viscosity, sheet_mobility_for, sheet_damp).
+cudaError_t launch_material(const uint8_t* grain, const float* moisture, float* nu, float* mob, float* damp, size_t n,
+                            cudaStream_t st);
 cudaError_t launch_apply_cut(const float* h, float* u, float* v, size_t n, float eps, cudaStream_t st);
 cudaError_t launch_max_speed2(const float* h, const float* u, const float* v, size_t n, float eps, int apply_cut,
                               unsigned int* out_bits, cudaStream_t st);

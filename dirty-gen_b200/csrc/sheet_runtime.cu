@@ -75,6 +75,8 @@ struct silt_sheet {
     float* bed = nullptr;
     float* moisture = nullptr;
     uint8_t* grain = nullptr;
+    float* mat = nullptr;         // slurry material per cell: viscosity, mobility, damping rate (3 planes)
+    bool mat_dirty = true;        // grain or moisture changed since the planes were computed
     float* staging = nullptr;     // n floats for host uploads
     float* staging2 = nullptr;
     uint8_t* staging_u8 = nullptr;
@@ -124,6 +126,7 @@ float water_nu() { return silt::host::dynamic_viscosity(3, 1.0f); }
 // hold water and no buffer is known to be zero.
 int tiles_dirty(silt_sheet* s) {
     s->tiles_all = true;
+    s->mat_dirty = true;
     if (!s->tile_mem) return SILT_OK;
     const size_t nt = (size_t)s->tf.tiles_x * s->tf.tiles_x;
     for (int l = 0; l < 2; ++l)
@@ -145,6 +148,15 @@ int flush_cut(silt_sheet* s) {
 
 int upload(silt_sheet* s, float* dst, const float* host) {
     CK(cudaMemcpyAsync(dst, host, s->n * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    return SILT_OK;
+}
+
+// The slurry's per-cell material planes, recomputed after grain or moisture
+// changed (seeding calls only: the step never changes them).
+int refresh_material(silt_sheet* s) {
+    if (!s->mat_dirty) return SILT_OK;
+    CK(silt::launch_material(s->grain, s->moisture, s->mat, s->mat + s->n, s->mat + 2 * s->n, s->n, s->st));
+    s->mat_dirty = false;
     return SILT_OK;
 }
 
@@ -223,9 +235,12 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
             P.mob_c = silt::host::sheet_mobility_for(cp.nu_w);
             P.decay_c = cp.sc.water_decay[1];
         } else {
-            P.nu_mode = silt::NU_GRAIN;
+            P.nu_mode = silt::NU_TABLE;
             P.grain = s->grain;
             P.moisture = s->moisture;
+            P.nu_plane = s->mat;
+            P.mob_plane = s->mat + s->n;
+            P.damp_plane = s->mat + 2 * s->n;
         }
         silt::TransportParams& Q = T.lay[l];
         Q.h = s->h[l][s->cur];
@@ -259,6 +274,8 @@ void coarse_advance(silt_sheet* s) {
 int step_coarse_pair(silt_sheet* s, float dt) {
     const int res = s->res;
     const float eps = 1.0e-6f;
+    int rc0 = refresh_material(s);
+    if (rc0) return rc0;
     CoarsePlan cp;
     coarse_plan(s, dt, cp);
     for (int k = 0; k < cp.launched; ++k) {
@@ -313,6 +330,7 @@ int step_coarse_pair(silt_sheet* s, float dt) {
 int step_coarse_pair_window(silt_sheet* s, float dt) {
     int rc = flush_cut(s);
     if (rc) return rc;
+    if ((rc = refresh_material(s))) return rc;
     const int slot = s->win_flip;
     s->win_flip ^= 1;
     CK(cudaEventSynchronize(s->win_ev[slot]));
@@ -335,7 +353,10 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         J.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
         J.sub_cap = 8.0f;
         J.eps = 1.0e-6f;
-        J.nu_mode = l == 0 ? silt::window::NU_CONST : silt::window::NU_GRAIN;
+        J.nu_mode = l == 0 ? silt::window::NU_CONST : silt::window::NU_TABLE;
+        J.nu_plane = s->mat;
+        J.mob_plane = s->mat + s->n;
+        J.damp_plane = s->mat + 2 * s->n;
         J.nu_c = nu_w;
         J.mob_c = silt::host::sheet_mobility_for(nu_w);
         for (int k = 1; k <= 8; ++k) J.decay_c[k] = expf(-silt::host::sheet_damp(nu_w) * (dt / (float)k));
@@ -437,6 +458,7 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->bed, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->moisture, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->grain, s->n);
+    if (e == cudaSuccess) e = cudaMalloc(&s->mat, 3 * nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
@@ -528,6 +550,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->bed);
     cudaFree(s->moisture);
     cudaFree(s->grain);
+    cudaFree(s->mat);
     cudaFree(s->staging);
     cudaFree(s->staging2);
     cudaFree(s->staging_u8);
@@ -597,6 +620,7 @@ int silt_map_grain(silt_sheet* s, const uint8_t* grain) {
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->grain, grain, s->n, cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
+    s->mat_dirty = true;
     return SILT_OK;
 }
 
@@ -698,6 +722,7 @@ int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moist
         }
     s->moisture_ambient = (float)best * 0.01f;
     CK(cudaStreamSynchronize(s->st));
+    s->mat_dirty = true;
     return SILT_OK;
 }
 
@@ -1173,6 +1198,8 @@ int batch_coarse(silt_batch* b, float dt) {
     int steps = 1;
     bool device_count = false;
     for (int w = 0; w < n; ++w) {
+        int rc = refresh_material(b->sheets[w]);
+        if (rc) return rc;
         coarse_plan(b->sheets[w], dt, plans[w]);
         steps = std::max(steps, plans[w].launched);
         device_count = device_count || plans[w].sc.speed2 != nullptr;

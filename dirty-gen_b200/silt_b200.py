@@ -138,6 +138,11 @@ def _f32(a):
 PLANES = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7}
 
 
+# A tire push as a numpy record (the layout of silt_tire_push).
+TIRE_DTYPE = np.dtype([("x", np.float32), ("z", np.float32), ("forward_x", np.float32), ("forward_z", np.float32),
+                       ("radius", np.float32), ("width", np.float32), ("speed", np.float32), ("slip", np.float32)])
+
+
 def make_push(t):
     return TirePush(t["x"], t["z"], t.get("forward_x", 0.0), t.get("forward_z", 1.0), t["radius"], t["width"],
                     t["speed"], t.get("slip", 0.0))
@@ -321,12 +326,17 @@ class Batch:
         return check(lib().silt_batch_step(self.h, dt), "batch_step")
 
     def push_tires(self, windows, tires):
-        """Tire pushes for many windows: tires[k] (a dict as for Sheet.push_tire) goes to window windows[k]."""
+        """Tire pushes for many windows: tires[k] goes to window windows[k]. `tires` is a
+        list of dicts as for Sheet.push_tire, or a numpy array of dtype TIRE_DTYPE."""
         n = len(tires)
         if n == 0:
             return
         idx = np.ascontiguousarray(windows, dtype=np.int32)
-        arr = (TirePush * n)(*[make_push(t) for t in tires])
+        if isinstance(tires, np.ndarray):
+            rec = np.ascontiguousarray(tires, dtype=TIRE_DTYPE)
+            arr = rec.ctypes.data_as(ctypes.POINTER(TirePush))
+        else:
+            arr = (TirePush * n)(*[make_push(t) for t in tires])
         check(lib().silt_batch_push_tires(self.h, _ptr(idx), arr, n), "batch_push_tires")
 
     def ledgers(self):
