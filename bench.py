@@ -536,9 +536,8 @@ def run_batch(args):
     f0.record(stream)
     for _ in range(e2e_steps):
         one_step()
-        led = batch.ledgers()
-        table = silt_shard.gather_ledgers(dict(zip(mine, led)), len(all_wins), dist,
-                                          device="cuda" if dist else "cpu")
+        table = silt_shard.gather_ledger_rows(mine, batch.ledger_rows(), len(all_wins), dist,
+                                              device="cuda" if dist else "cpu")
     f1.record(stream)
     torch.cuda.synchronize()
     ems = f0.elapsed_time(f1)

@@ -409,8 +409,31 @@ cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int
     return cudaGetLastError();
 }
 
+// Cells [x0, x0 + W) x [y0, y0 + H) of a transport tile: edge tiles walk
+// clipped rows one warp per row; interior tiles (W, H exact) one flat range
+// of compile-time width, so every lane is busy on the 33-35 wide passes.
+template <bool EDGE, int W, int H, class F>
+__device__ __forceinline__ void trows(int x0, int x1, int y0, int y1, F f) {
+    if (EDGE) {
+        const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+        constexpr int NW = TRANSPORT_THREADS / 32;
+        for (int gy = y0 + wy; gy < y1; gy += NW)
+            for (int gx = x0 + lane; gx < x1; gx += 32) f(gx, gy);
+    } else {
+        for (int k = threadIdx.x; k < W * H; k += TRANSPORT_THREADS) {
+            const int r = k / W;
+            f(x0 + (k - r * W), y0 + r);
+        }
+    }
+}
+
 // Donor-cell transport (src/fluid_core.rs:3025-3137), x pass then z pass on
 // the updated depth, dry cut (src/fluid_core.rs:2072-2081), FP64 ledger sum.
+// An edge moves depth one way only (the sign of its face speed picks the
+// donor), so each flux pass evaluates the edges whose donor it is and writes
+// 0 for the others. EDGE = false: the tile is full and its cells
+// [t0-2, t1+1) lie inside the grid with t1 <= res-1, so no range is clipped.
+template <bool EDGE>
 __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int ty0, const TileFlags& tf, int l,
                                int nxt, int t) {
     const int res = P.res;
@@ -426,50 +449,49 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
     float* DN = sm + 7 * PL;    // down-going flux
     const int ox = tx0 - 2, oy = ty0 - 2;
 #define TIDX(gx, gy) (((gy) - oy) * TW + ((gx) - ox))
-    const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
-    constexpr int NW = TRANSPORT_THREADS / 32;
-#define ROWS(Y0, Y1, X0, X1) \
-    for (int gy = (Y0) + wy; gy < (Y1); gy += NW) for (int gx = (X0) + lane; gx < (X1); gx += 32)
     const int ry0 = max(0, ty0 - 2), ry1 = min(res, ty1 + 1);
     const int cx0 = max(0, tx0 - 2), cx1 = min(res, tx1 + 1);
     const float cell = P.cell, dt = P.dt;
     const bool with_bed = P.bank_bed != nullptr;
     const uint8_t* gate = P.gate;
-    ROWS(ry0, ry1, cx0, cx1) {
+    trows<EDGE, TT + 3, TT + 3>(cx0, cx1, ry0, ry1, [&](int gx, int gy) {
         size_t g = (size_t)gy * res + gx;
         HSm[TIDX(gx, gy)] = P.h[g];
         US[TIDX(gx, gy)] = P.u[g];
         if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
-    }
+    });
     __syncthreads();
     // x pass. Edge e joins cells e and e+1 and exists for 0 <= e < res-1.
     // Left-going flux first (its donor e+1 has removed nothing yet).
     const int e0 = max(0, tx0 - 2), e1 = min(res - 2, tx1 - 1);  // inclusive edge range
-    ROWS(ry0, ry1, e0, e1 + 1) {
-        const int e = gx;
+    trows<EDGE, TT + 2, TT + 3>(e0, e1 + 1, ry0, ry1, [&](int e, int gy) {
         float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
-        size_t g = (size_t)gy * res + e;
-        float bd = with_bed ? P.bank_bed[g + 1] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
-        float dh = open_edge_dh(with_bed, HSm[TIDX(e + 1, gy)], HSm[TIDX(e, gy)], 0.0f, gate ? gate[g] : 1, bd, bc,
-                                speed, dt, cell, 0.45f);
-        FL[TIDX(e, gy)] = speed > 0.0f ? 0.0f : dh;
-    }
+        float dh = 0.0f;
+        if (!(speed > 0.0f)) {
+            size_t g = (size_t)gy * res + e;
+            float bd = with_bed ? P.bank_bed[g + 1] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+            dh = open_edge_dh(with_bed, HSm[TIDX(e + 1, gy)], HSm[TIDX(e, gy)], 0.0f, gate ? gate[g] : 1, bd, bc,
+                              speed, dt, cell, 0.45f);
+        }
+        FL[TIDX(e, gy)] = dh;
+    });
     __syncthreads();
     // Right-going: donor e has removed the left-going flux of edge e-1.
-    ROWS(ry0, ry1, max(e0, tx0 - 1), e1 + 1) {
-        const int e = gx;
+    trows<EDGE, TT + 1, TT + 3>(max(e0, tx0 - 1), e1 + 1, ry0, ry1, [&](int e, int gy) {
         float speed = 0.5f * (US[TIDX(e, gy)] + US[TIDX(e + 1, gy)]);
-        float prev = e > 0 ? FL[TIDX(e - 1, gy)] : 0.0f;
-        size_t g = (size_t)gy * res + e;
-        float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + 1] : 0.0f;
-        float dh = open_edge_dh(with_bed, HSm[TIDX(e, gy)], HSm[TIDX(e + 1, gy)], 0.0f + prev,
-                                gate ? gate[g + 1] : 1, bd, bc, speed, dt, cell, 0.45f);
-        FR[TIDX(e, gy)] = speed > 0.0f ? dh : 0.0f;
-    }
+        float dh = 0.0f;
+        if (speed > 0.0f) {
+            float prev = e > 0 ? FL[TIDX(e - 1, gy)] : 0.0f;
+            size_t g = (size_t)gy * res + e;
+            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + 1] : 0.0f;
+            dh = open_edge_dh(with_bed, HSm[TIDX(e, gy)], HSm[TIDX(e + 1, gy)], 0.0f + prev, gate ? gate[g + 1] : 1,
+                              bd, bc, speed, dt, cell, 0.45f);
+        }
+        FR[TIDX(e, gy)] = dh;
+    });
     __syncthreads();
     // Depth after the x pass on rows [ry0, ry1), tile columns.
-    ROWS(ry0, ry1, tx0, tx1) {
-        const int c = gx;
+    trows<EDGE, TT, TT + 3>(tx0, tx1, ry0, ry1, [&](int c, int gy) {
         float flm = c - 1 >= 0 ? FL[TIDX(c - 1, gy)] : 0.0f;
         float frm = c - 1 >= 0 ? FR[TIDX(c - 1, gy)] : 0.0f;
         float flc = c <= res - 2 ? FL[TIDX(c, gy)] : 0.0f;
@@ -479,34 +501,37 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         float hv = HSm[TIDX(c, gy)];
         float moved = fmaxf(hv - rem + add, 0.0f);
         HX[TIDX(c, gy)] = (rem > 0.0f || add > 0.0f) ? moved : hv;
-    }
+    });
     __syncthreads();
     // z pass. Pair r joins rows r and r+1 and exists for 0 <= r < res-1.
     const int p0 = max(0, ty0 - 2), p1 = min(res - 2, ty1 - 1);
-    ROWS(p0, p1 + 1, tx0, tx1) {
-        const int r = gy, c = gx;
+    trows<EDGE, TT, TT + 2>(tx0, tx1, p0, p1 + 1, [&](int c, int r) {
         float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
-        size_t g = (size_t)r * res + c;
-        float bd = with_bed ? P.bank_bed[g + res] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
-        float dh = open_edge_dh(with_bed, HX[TIDX(c, r + 1)], HX[TIDX(c, r)], 0.0f, gate ? gate[g] : 1, bd, bc,
-                                speed, dt, cell, 0.45f);
-        UP[TIDX(c, r)] = speed > 0.0f ? 0.0f : dh;
-    }
+        float dh = 0.0f;
+        if (!(speed > 0.0f)) {
+            size_t g = (size_t)r * res + c;
+            float bd = with_bed ? P.bank_bed[g + res] : 0.0f, bc = with_bed ? P.bank_bed[g] : 0.0f;
+            dh = open_edge_dh(with_bed, HX[TIDX(c, r + 1)], HX[TIDX(c, r)], 0.0f, gate ? gate[g] : 1, bd, bc, speed,
+                              dt, cell, 0.45f);
+        }
+        UP[TIDX(c, r)] = dh;
+    });
     __syncthreads();
-    ROWS(max(p0, ty0 - 1), p1 + 1, tx0, tx1) {
-        const int r = gy, c = gx;
+    trows<EDGE, TT, TT + 1>(tx0, tx1, max(p0, ty0 - 1), p1 + 1, [&](int c, int r) {
         float speed = 0.5f * (VS[TIDX(c, r)] + VS[TIDX(c, r + 1)]);
-        float ra = r > 0 ? 0.0f + UP[TIDX(c, r - 1)] : 0.0f;
-        size_t g = (size_t)r * res + c;
-        float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + res] : 0.0f;
-        float dh = open_edge_dh(with_bed, HX[TIDX(c, r)], HX[TIDX(c, r + 1)], ra, gate ? gate[g + res] : 1, bd,
-                                bc, speed, dt, cell, 0.45f);
-        DN[TIDX(c, r)] = speed > 0.0f ? dh : 0.0f;
-    }
+        float dh = 0.0f;
+        if (speed > 0.0f) {
+            float ra = r > 0 ? 0.0f + UP[TIDX(c, r - 1)] : 0.0f;
+            size_t g = (size_t)r * res + c;
+            float bd = with_bed ? P.bank_bed[g] : 0.0f, bc = with_bed ? P.bank_bed[g + res] : 0.0f;
+            dh = open_edge_dh(with_bed, HX[TIDX(c, r)], HX[TIDX(c, r + 1)], ra, gate ? gate[g + res] : 1, bd, bc,
+                              speed, dt, cell, 0.45f);
+        }
+        DN[TIDX(c, r)] = dh;
+    });
     __syncthreads();
     double part = 0.0;
-    ROWS(ty0, ty1, tx0, tx1) {
-        const int r = gy, c = gx;
+    trows<EDGE, TT, TT>(tx0, tx1, ty0, ty1, [&](int c, int r) {
         float upm = r - 1 >= 0 ? UP[TIDX(c, r - 1)] : 0.0f;
         float dnm = r - 1 >= 0 ? DN[TIDX(c, r - 1)] : 0.0f;
         float upc = r <= res - 2 ? UP[TIDX(c, r)] : 0.0f;
@@ -519,9 +544,8 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         if (P.eps > 0.0f && hn < P.eps) hn = 0.0f;
         P.h_out[(size_t)r * res + c] = hn;
         part += (double)fmaxf(hn, 0.0f);
-    }
+    });
 #undef TIDX
-#undef ROWS
     // Block sum of the depth (FP64), one atomic per tile; the tile's flags.
     const int any = __syncthreads_or(part > 0.0);
     for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
@@ -589,7 +613,11 @@ __device__ __forceinline__ void transport_entry(const TransportParams& P, const 
         }
         return;
     }
-    transport_tile(P, sm, tx0, ty0, tf, l, nxt, t);
+    const bool interior = tx0 >= 2 && ty0 >= 2 && tx0 + TT + 1 <= res && ty0 + TT + 1 <= res;
+    if (interior)
+        transport_tile<false>(P, sm, tx0, ty0, tf, l, nxt, t);
+    else
+        transport_tile<true>(P, sm, tx0, ty0, tf, l, nxt, t);
 }
 
 // Persistent over the substep's tile list.

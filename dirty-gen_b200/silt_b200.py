@@ -344,6 +344,13 @@ class Batch:
         check(lib().silt_batch_get_ledgers(self.h, arr), "batch_ledgers")
         return [{k: getattr(x, k) for k, _ in Ledger._fields_} for x in arr]
 
+    def ledger_rows(self):
+        """Every window's ledger as one n x 7 FP64 array, columns in the
+        silt_ledger field order."""
+        arr = (Ledger * len(self.sheets))()
+        check(lib().silt_batch_get_ledgers(self.h, arr), "batch_ledgers")
+        return np.frombuffer(arr, dtype=np.float64).reshape(len(self.sheets), len(Ledger._fields_)).copy()
+
     def set_timing(self, on):
         check(lib().silt_batch_set_timing(self.h, int(on)), "batch_set_timing")
 

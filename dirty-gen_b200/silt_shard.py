@@ -19,11 +19,21 @@ def shard(n, rank, world):
 def gather_ledgers(local, n, dist=None, device="cpu"):
     """`local`: {window index: ledger dict} of this rank. Returns an n x 7 FP64
     array (rows in window order, columns LEDGER_KEYS) on every rank."""
+    idx = list(local)
+    rows = np.array([[float(local[w][k]) for k in LEDGER_KEYS] for w in idx], dtype=np.float64)
+    return gather_ledger_rows(idx, rows.reshape(len(idx), len(LEDGER_KEYS)), n, dist, device)
+
+
+def gather_ledger_rows(windows, rows, n, dist=None, device="cpu"):
+    """`rows[k]` (columns LEDGER_KEYS) is window `windows[k]`'s ledger on this
+    rank, e.g. `Batch.ledger_rows()`. Returns the n x 7 FP64 table on every
+    rank."""
     import torch
 
-    t = torch.zeros((n, len(LEDGER_KEYS)), dtype=torch.float64, device=device)
-    for w, led in local.items():
-        t[w] = torch.tensor([float(led[k]) for k in LEDGER_KEYS], dtype=torch.float64)
+    t = torch.zeros((n, len(LEDGER_KEYS)), dtype=torch.float64)
+    if len(windows):
+        t[torch.as_tensor(np.asarray(windows, dtype=np.int64))] = torch.from_numpy(np.asarray(rows, np.float64))
     if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        t = t.to(device)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return t.cpu().numpy()

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import silt_b200 as G
+import silt_shard
 import silt_scenes as S
 
 pytestmark = pytest.mark.gpu
@@ -58,6 +59,9 @@ def test_batch_step_equals_single_steps():
         single = grouped[w].ledger()
         for key in ("water_m3", "slurry_m3", "spray_m3", "frozen_water_m3", "opened_m3", "total_m3"):
             assert gathered[w][key] == single[key], (w, key)
+    rows = batch.ledger_rows()
+    for w in range(len(scenes)):
+        assert list(rows[w]) == [gathered[w][k] for k in silt_shard.LEDGER_KEYS], w
     parts = batch.parts()
     assert parts["steps"] == 24 and parts["launches"] > 0
     batch.close()
