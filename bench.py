@@ -22,6 +22,7 @@ patches, all stepped together (silt_batch_step); a step advances every window.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -53,10 +54,11 @@ def parse():
     ap.add_argument("--res", type=int, default=RES)
     ap.add_argument("--no-tires", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
-    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200"],
+    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200", "closure"],
                     help="grid: one 2048^2 grid with four tire patches; batch: many windows stepped together; "
-                         "window200: the reference's own 200^2 window, no tires")
-    ap.add_argument("--windows", type=int, default=256, help="batch: number of windows")
+                         "window200: the reference's own 200^2 window, no tires; closure: 200^2 windows with "
+                         "four tires each, the learned closure against the nested 2 cm sheets")
+    ap.add_argument("--windows", type=int, default=None, help="batch: number of windows (256); closure: (128)")
     ap.add_argument("--batch-tires", type=int, default=1, help="batch: 1 = each window's 0..4 tires, 0 = none")
     return ap.parse_args()
 
@@ -617,7 +619,7 @@ def run_window200(args):
             el = time.perf_counter() - t0
         v = res * res * steps / el
         base = {"value": v, "unit": "cell-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
-                "host": host_cpu(), "host": host_cpu(),
+                "host": host_cpu(),
                 "sample": f"{steps} steps after {max(1, args.warmup)} warm-up, the pair on 2 threads ({el:.2f} s)"}
         print(json.dumps({"metric": "cell-steps/s", "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
                           "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": 1000.0 * el / steps,
@@ -680,8 +682,274 @@ def run_window200(args):
     sheet.close()
 
 
+CLOSURE_EVAL_SEED = 0xC0FFEE11  # evaluation windows: not among the training windows
+CLOSURE_THRESHOLD = 0.25
+
+
+def closure_workload(args):
+    return {"workload": f"closure{args.windows}_win200_4tires_speed2-10", "windows": args.windows, "res": 200,
+            "cell_m": CELL, "dt_s": DT, "fine_res": FINE_RES, "layout": "per_tire64",
+            "network": "3x3 conv 6(16)-32-32-4(16), bf16, fp32 accumulate", "crop": 32,
+            "residual_threshold": CLOSURE_THRESHOLD,
+            "l2": "inputs larger than L2 (four forms x 128 windows, ~0.7 GB of state)"}
+
+
+def closure_push_records(scenes, silt_b200, T):
+    """Every window's four tires as one record array, with what tires_at adds
+    to z each step kept apart so the per-step z is the same f32 arithmetic."""
+    import numpy as np
+
+    f32 = np.float32
+    idx, recs, zb, spd, zrow = [], [], [], [], []
+    for k, sc in enumerate(scenes):
+        for q, t in enumerate(T.scene_tires(sc, 0)):
+            idx.append(k)
+            recs.append(t)
+            zb.append(f32(0.0) + f32(sc["z0"]))
+            spd.append(f32(sc["speed"]))
+            zrow.append(f32((-0.5, -0.5, 0.5, 0.5)[q] * 2.4))
+    rec = np.zeros(len(recs), silt_b200.TIRE_DTYPE)
+    for name in silt_b200.TIRE_DTYPE.names:
+        rec[name] = [r[name] for r in recs]
+    return np.asarray(idx, np.int32), rec, np.asarray(zb, f32), np.asarray(spd, f32), np.asarray(zrow, f32)
+
+
+def closure_cpu(scenes, T, max_steps, budget_s):
+    """The reference's form (nested 2 cm sheets, one window at a time) on the
+    oracle for every 16th window."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import silt_scenes
+
+    sample = scenes[::16]
+    cores = []
+    for sc in sample:
+        c = oracle.Core(res=200, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=2)
+        silt_scenes.seed_core(c, sc)
+        cores.append(c)
+    for sc, c in zip(sample, cores):
+        for t in T.scene_tires(sc, 1):
+            c.push_tire(**t)
+        c.step(DT)
+    steps, t0, el = 0, time.perf_counter(), 0.0
+    while steps < max(1, max_steps) and el < budget_s:
+        for sc, c in zip(sample, cores):
+            for t in T.scene_tires(sc, 2 + steps):
+                c.push_tire(**t)
+            c.step(DT)
+        steps += 1
+        el = time.perf_counter() - t0
+    v = len(sample) * steps / el
+    return {"value": v, "unit": "window-steps/s", "cores": 2, "kind": "port", "steps": steps, "seconds": el,
+            "host": host_cpu(),
+            "sample": f"{len(sample)} of the {len(scenes)} windows (every 16th), nested per-tire 64^2 sheets, "
+                      f"{steps} steps after 1 warm-up, one window at a time, each pair on 2 threads ({el:.2f} s)"}
+
+
+def run_closure_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "dirty-gen_b200"))
+    import silt_closure_train as T
+
+    scenes = [T.drive_scene(k, CLOSURE_EVAL_SEED) for k in range(args.windows)]
+    base = closure_cpu(scenes, T, args.steps, 60.0)
+    line = {"metric": "window-steps/s", "value": base["value"], "unit": "window-steps/s", "n_gpus": args.gpus,
+            "steps": base["steps"], "warmup": 1, "ms_per_step": 1000.0 * len(scenes) / base["value"],
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": closure_workload(args), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "window-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_closure(args):
+    """Configuration 5: windows of 200^2 with four tires each (speed U(2, 10)
+    m/s), the learned closure against the full nested 64^2 2 cm sheets, from
+    the same start with the same tires; window-steps/s of both forms and the
+    relative L2 depth error of the closure (and of the plain coarse step)
+    against the nested run."""
+    import numpy as np
+    import torch
+
+    import silt_b200
+    import silt_closure as C
+    import silt_closure_train as T
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    wpath = os.path.join(ROOT, "dirty-gen_b200", "closure_weights.npz")
+    if not os.path.exists(wpath):
+        raise SystemExit(f"{wpath} is missing: train it with dirty-gen_b200/silt_closure_train.py")
+    w = np.load(wpath)
+    net = C.Closure(w["params"], w["norm"])
+    zero = C.Closure(np.zeros(C.NPARAM, np.float32), w["norm"])  # the closure's coarse step with no correction
+    scenes = [T.drive_scene(k, CLOSURE_EVAL_SEED) for k in range(args.windows)]
+    forms = {}
+    for name, mode, nn, thr in (("nested", C.COUPLING_NESTED, None, 0.0),
+                                ("closure", C.COUPLING_CLOSURE, net, CLOSURE_THRESHOLD),
+                                ("uncorrected", C.COUPLING_CLOSURE, zero, 1e30),
+                                ("plain", C.COUPLING_NONE, None, 0.0)):
+        sheets = T.make_sheets(scenes, stream.cuda_stream, mode, nn, thr)
+        forms[name] = (sheets, silt_b200.Batch(sheets))
+    idx, rec, zb, spd, zrow = closure_push_records(scenes, silt_b200, T)
+    f32 = np.float32
+    step_of = {name: 0 for name in forms}
+
+    def one_step(name):
+        step_of[name] += 1
+        rec["z"] = (zb + spd * f32(step_of[name] * DT)) + zrow
+        b = forms[name][1]
+        b.push_tires(idx, rec)
+        b.step(DT)
+
+    warm = max(3, args.warmup)
+    timed = {}
+    parts = {}
+    stop = threading.Event()
+    clock_lines = []
+    th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, 0), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    for name in forms:
+        for _ in range(warm):
+            one_step(name)
+        torch.cuda.synchronize()
+        forms[name][1].set_timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            one_step(name)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        timed[name] = e0.elapsed_time(e1)
+        parts[name] = forms[name][1].parts()
+        forms[name][1].set_timing(False)
+    stop.set()
+    th.join(timeout=5)
+    # Depth error against the nested run, every window and both layers.
+    def rel_l2(a, b):
+        num = den = 0.0
+        for sa, sb in zip(forms[a][0], forms[b][0]):
+            for layer in ("water", "slurry"):
+                x, y = sa.plane_device(layer).double(), sb.plane_device(layer).double()
+                num += float(((x - y) ** 2).sum())
+                den += float((y ** 2).sum())
+        return math.sqrt(num / den)
+
+    torch.cuda.synchronize()
+    err_closure = rel_l2("closure", "nested")
+    err_plain = rel_l2("plain", "nested")
+    err_uncorrected = rel_l2("uncorrected", "nested")
+    # End to end through the public API: pushes in from host memory and every
+    # window's FP64 ledger back each step; the ledger gap per step is checked
+    # on the way (volume now against volume before plus what was opened).
+    e2e = {}
+    gaps = {}
+    e2e_steps = max(5, args.steps // 4)
+    for name in ("closure", "nested"):
+        b = forms[name][1]
+        prev = b.ledger_rows()
+        worst = 0.0
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(e2e_steps):
+            one_step(name)
+            rows = b.ledger_rows()
+            tot, opened = rows[:, 6], rows[:, 5]
+            expect = prev[:, 6] + (opened - prev[:, 5])
+            worst = max(worst, float(np.max(np.abs(tot - expect) / np.maximum(expect, 1e-30))))
+            prev = rows
+        f1.record(stream)
+        torch.cuda.synchronize()
+        e2e[name] = args.windows * e2e_steps / (f0.elapsed_time(f1) / 1000.0)
+        gaps[name] = worst
+    cs = [C.stats(sh) for sh in forms["closure"][0]]
+    n_closure = sum(s["closure_steps"] for s in cs)
+    n_fallback = sum(s["fallback_steps"] for s in cs)
+    # The network alone on the windows' crops (tensor-core share of the step).
+    x = torch.zeros((args.windows, C.CROP, C.CROP, C.CIN), dtype=torch.bfloat16, device="cuda")
+    tnet = C.Net(w["params"])
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            tnet.forward(x)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        reps = 20
+        g0.record(stream)
+        for _ in range(reps):
+            tnet.forward(x)
+        g1.record(stream)
+    torch.cuda.synchronize()
+    cnn_ms = g0.elapsed_time(g1) / reps
+    cnn_flops = 2.0 * args.windows * C.CROP * C.CROP * 9 * (C.CIN * C.HID + C.HID * C.HID + C.HID * C.COUT)
+    peak, peak_kind = measured_peak()
+    bf16_peak = None
+    try:
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        bf16_peak = mp.get("bf16_tflops")
+    except Exception:
+        pass
+    pc = parts["closure"]
+    launches = max(pc["force_launches"], 1)
+    force_ms = pc["force_ms"] / launches
+    cw = pc["force_cells_water"] / launches
+    csl = (pc["force_cells"] - pc["force_cells_water"]) / launches
+    force_bytes = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * csl
+    achieved = force_bytes / (force_ms / 1000.0) / 1e9 if force_ms > 0 else None
+    ws_closure = args.windows * args.steps / (timed["closure"] / 1000.0)
+    ws_nested = args.windows * args.steps / (timed["nested"] / 1000.0)
+    ws_plain = args.windows * args.steps / (timed["plain"] / 1000.0)
+    line = {"metric": "window-steps/s", "value": ws_closure, "unit": "window-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": warm, "ms_per_step": timed["closure"] / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32 (network bf16)",
+            "data": "synthetic", "config": closure_workload(args),
+            "roofline": {"bound": "hbm", "kernel": "k_batch_force", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms},
+            "closure_cnn": {"bound": "tensor", "kernel": "k_conv3x3 (tcgen05)", "flops_per_step": cnn_flops,
+                            "ms_per_step": cnn_ms, "achieved_tflops": cnn_flops / (cnn_ms / 1000.0) / 1e12,
+                            "peak_tflops": bf16_peak,
+                            "frac": (cnn_flops / (cnn_ms / 1000.0) / 1e12) / bf16_peak if bf16_peak else None},
+            "e2e": {"value": e2e["closure"], "unit": "window-steps/s", "h2d_bytes_per_step": 32 * len(rec),
+                    "d2h_bytes_per_step": 40 * args.windows, "steps": e2e_steps},
+            "nested": {"window_steps_per_s": ws_nested, "ms_per_step": timed["nested"] / args.steps,
+                       "e2e_window_steps_per_s": e2e["nested"], "ledger_gap_max": gaps["nested"]},
+            "plain_coarse": {"window_steps_per_s": ws_plain, "ms_per_step": timed["plain"] / args.steps,
+                             "depth_rel_l2_vs_nested": err_plain,
+                             "what": "no sheets, tires shove the 20 cm cells"},
+            "uncorrected": {"window_steps_per_s": args.windows * args.steps / (timed["uncorrected"] / 1000.0),
+                            "depth_rel_l2_vs_nested": err_uncorrected,
+                            "what": "the closure's coarse step with a zero network (no tire effect)"},
+            "speedup_vs_nested": ws_closure / ws_nested,
+            "depth_rel_l2_vs_nested": err_closure,
+            "ledger_gap_max": gaps["closure"],
+            "closure_steps": n_closure, "fallback_steps": n_fallback,
+            "steps_compared": warm + args.steps,
+            "gpu_launches": int(pc["launches"]), "clocks": summarise_clocks(clock_lines)}
+    if not args.no_baseline:
+        line["cpu_baseline"] = closure_cpu(scenes, T, 40, 20.0)
+    print(json.dumps(line), flush=True)
+    for name in forms:
+        forms[name][1].close()
+        for sh in forms[name][0]:
+            sh.close()
+    net.close()
+    zero.close()
+
+
 def main():
     args = parse()
+    if args.windows is None:
+        args.windows = 128 if args.workload == "closure" else 256
+    if args.workload == "closure":
+        if args.impl == "reference":
+            run_closure_reference(args)
+        else:
+            run_closure(args)
+        return
     if args.workload == "window200":
         run_window200(args)
     elif args.workload == "batch":

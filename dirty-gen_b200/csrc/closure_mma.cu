@@ -429,6 +429,72 @@ __global__ void k_loss_grad(const float* y, const float* t, const float* wgt, ui
     }
 }
 
+// One crop per block, one cell per thread (the crop edge has no outgoing face).
+__global__ void __launch_bounds__(SILT_CLOSURE_CROP * SILT_CLOSURE_CROP)
+    k_step_loss(const float* y, const float* t, const float* scale, const float* inv_var, float lam, uint16_t* dy,
+                double* loss, float norm) {
+    constexpr int N = SILT_CLOSURE_CROP, NC = N * N, CO = SILT_CLOSURE_COUT, NT = 8;
+    __shared__ float g[4][NC];
+    __shared__ float e[2][NC];
+    __shared__ double red[NC / 32];
+    const int p = threadIdx.x, cx = p % N, cy = p / N;
+    const size_t pix = (size_t)blockIdx.x * NC + p;
+    const float* yo = y + pix * CO;
+    const float* to = t + pix * NT;
+    float yv[8], sc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        yv[c] = yo[c];
+        sc[c] = scale[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const bool edge = (c % 2 == 0) ? cx == N - 1 : cy == N - 1;
+        g[c][p] = edge ? 0.0f : yv[c] * sc[c];
+    }
+    __syncthreads();
+    double part = 0.0;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        const float in = (cx > 0 ? g[2 * l][p - 1] : 0.0f) + (cy > 0 ? g[2 * l + 1][p - N] : 0.0f);
+        const float div = in - g[2 * l][p] - g[2 * l + 1][p];
+        const float r = div - to[l];
+        e[l][p] = r;
+        part += (double)(inv_var[l] * r * r);
+    }
+    float gv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float w = to[6 + k / 2];
+        const float r = yv[4 + k] * sc[4 + k] - to[2 + k];
+        part += (double)(inv_var[2 + k] * w * r * r);
+        gv[k] = 2.0f * inv_var[2 + k] * w * r * sc[4 + k];
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) part += (double)(lam * yv[c] * yv[c]);
+    __syncthreads();
+    uint16_t* out = dy + pix * CO;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        const float gx = cx < N - 1 ? 2.0f * inv_var[l] * (e[l][p + 1] - e[l][p]) : 0.0f;
+        const float gz = cy < N - 1 ? 2.0f * inv_var[l] * (e[l][p + N] - e[l][p]) : 0.0f;
+        out[2 * l] = to_bf16((gx * sc[2 * l] + 2.0f * lam * yv[2 * l]) * norm);
+        out[2 * l + 1] = to_bf16((gz * sc[2 * l + 1] + 2.0f * lam * yv[2 * l + 1]) * norm);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[4 + k] = to_bf16((gv[k] + 2.0f * lam * yv[4 + k]) * norm);
+#pragma unroll
+    for (int c = 8; c < CO; ++c) out[c] = 0;
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((p & 31) == 0) red[p >> 5] = part;
+    __syncthreads();
+    if (p == 0 && loss) {
+        double s = 0.0;
+        for (int w = 0; w < NC / 32; ++w) s += red[w];
+        atomicAdd(loss, s * (double)norm);
+    }
+}
+
 __global__ void k_adam(float* p, float* m, float* v, const float* g, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -583,6 +649,17 @@ int silt_closure_loss_grad(const float* y, const float* target, const float* pix
                                                           cout_pad, n_out, scale);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_loss_grad");
+}
+
+int silt_closure_step_loss_grad(const float* y, const float* t, const float* scale, const float* inv_var,
+                                float lambda, void* dy, double* loss, int32_t n_img, float norm, void* stream) {
+    if (!y || !t || !scale || !inv_var || !dy || n_img < 0)
+        return fail(SILT_EINVAL, "invalid argument: closure_step_loss_grad");
+    if (n_img == 0) return SILT_OK;
+    k_step_loss<<<n_img, SILT_CLOSURE_CROP * SILT_CLOSURE_CROP, 0, (cudaStream_t)stream>>>(
+        y, t, scale, inv_var, lambda, (uint16_t*)dy, loss, norm);
+    ::silt::count_launch();
+    return cuda_rc(cudaGetLastError(), "closure_step_loss_grad");
 }
 
 int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32_t n, float lr, float beta1,

@@ -405,10 +405,12 @@ __device__ void peel_cell(float* w, const float* uw, const float* vw, int res, f
         if (w[idx] < 0.01f) continue;
         const float take = fminf(w[idx] * 0.04f, 0.004f);
         if (take * area < 1.0e-6f) continue;
-        w[idx] -= take;
+        const float before = w[idx], after = before - take;
+        w[idx] = after;
         int slot = atomicAdd(&counters[3], 1);
         atomicAdd(&books[0], (double)(take * area));
-        if (ledger_depth) atomicAdd(ledger_depth, -(double)take);
+        // The depth sum follows the cell's actual (rounded) change.
+        if (ledger_depth) atomicAdd(ledger_depth, (double)after - (double)before);
         if (slot < SPRAY_CAP) {
             SprayRec r;
             r.x = x;
@@ -938,7 +940,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
     const float extent = (float)fres * P.fcell;
     const int full = sub * sub;
     const float r2 = P.tire_r * P.tire_r;
-    L.np = P.layout == SILT_FINE_MEAN_PATCH ? 1 : std::min((int)ps.size(), MAX_PATCHES);
+    L.np = P.patches_off ? 0 : P.layout == SILT_FINE_MEAN_PATCH ? 1 : std::min((int)ps.size(), MAX_PATCHES);
     int rc = ensure_patches(P, L.np, W.st);
     if (rc) return rc;
     // Owner changes as one value per cell: last step's holds are released,
@@ -1129,6 +1131,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
             long ci = coarse_axis(W.origin[0], W.cell, res, ps[q].x);
             long cj = coarse_axis(W.origin[1], W.cell, res, ps[q].z);
             if (ci >= 0 && cj >= 0 && M.h_owner[cj * res + ci] >= 0) continue;
+            if (P.coarse_shove_off) continue;
             const PushJob J = make_job(ps[q], (int)q, W.origin[0], W.origin[1], W.cell, res, push_reach(ps[q], W.cell));
             push.push_back(J);
             // A shove whose span misses the window touches no coarse cell.
@@ -1267,6 +1270,11 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
                                                                      TAB(int8_t, L.off_oval), L.n_owner);
         ::silt::count_launch();
         FCK(cudaGetLastError());
+    }
+    if (L.np == 0) {  // no patch: the released holds above are all there is to lay
+        FCK(cudaMemsetAsync(M.counters + 3, 0, sizeof(int), W.st));  // the spray count k_refine_lay would clear
+        P.active = 0;
+        return SILT_OK;
     }
     k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner,
                                                                                  M.counters + 3);

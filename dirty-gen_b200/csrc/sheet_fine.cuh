@@ -59,6 +59,8 @@ struct Patches {
     float sub_cap = 8.0f;
     int pace = 0;
     bool near_on = true;
+    bool patches_off = false;  // lay no patch this step: every tire shoves the coarse cells (closure coupling)
+    bool coarse_shove_off = false;  // and not even that: the learned closure carries the tires' effect
     bool fine_on = false;
     int active = 0;
     std::vector<PatchState*> patches;

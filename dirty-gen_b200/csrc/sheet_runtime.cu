@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 
 #include "../../include/silt_sheet.h"
+#include "../../include/silt_closure.h"
+#include "closure.cuh"
 #include "sheet_fine.cuh"
 #include "launch_count.cuh"
 #include "sheet_grid.cuh"
@@ -112,6 +114,14 @@ struct silt_sheet {
     int* tile_count = nullptr;   // two count slots, used alternately by successive substeps
     unsigned long long tile_seq = 0;
     bool tiles_all = true;     // next substep steps every tile (after any outside write)
+
+    // Tire coupling (silt_set_coupling): nested sheets, none, or the learned closure.
+    int coupling = SILT_COUPLING_NESTED;
+    silt_closure* net = nullptr;
+    float clos_threshold = 0.25f;
+    silt::closure::Runner* clos = nullptr;
+    bool clos_fallback_next = false;   // the last residual estimate was above the threshold
+    silt_closure_stats cstats = {0, 0, 0.0f, 0.0};
 
     float* H(int l) { return h[l][cur]; }
     float* U(int l) { return u[l][cur]; }
@@ -404,6 +414,7 @@ extern "C" {
 
 const char* silt_last_error(void) {
     if (g_err[0]) return g_err;
+    if (const char* c = silt::closure::last_error()) return c;
     return silt::fine::last_error();
 }
 
@@ -540,6 +551,10 @@ int silt_sheet_destroy(silt_sheet* s) {
     if (!s) return SILT_OK;
     cudaSetDevice(s->cfg.device);
     if (s->st) cudaStreamSynchronize(s->st);
+    if (s->clos) {
+        s->clos->release();
+        delete s->clos;
+    }
     silt::fine::destroy(s->fine);
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
@@ -784,6 +799,58 @@ int step_inflow(silt_sheet* s, float dt) {
     return SILT_OK;
 }
 
+// The coupling of this step's tires: sets whether the nested patches are laid
+// and returns true when the learned closure corrects the step.
+bool closure_begin(silt_sheet* s) {
+    s->fine.patches_off = false;
+    s->fine.coarse_shove_off = false;
+    if (s->coupling == SILT_COUPLING_NESTED) return false;
+    if (s->coupling == SILT_COUPLING_NONE) {
+        s->fine.patches_off = true;
+        return false;
+    }
+    std::vector<float> r;
+    double moved = 0.0;
+    if (s->clos->poll(r, &moved) && !r.empty()) {
+        s->cstats.last_residual = r[0];
+        s->cstats.moved_m3 = moved;
+        s->clos_fallback_next = r[0] > s->clos_threshold;
+    }
+    if (s->pushes.empty()) {  // no tire, nothing to correct: the plain coarse step
+        s->fine.patches_off = true;
+        return false;
+    }
+    if (s->clos_fallback_next) {  // the nested sheets take this step
+        s->clos_fallback_next = false;
+        s->cstats.fallback_steps += 1;
+        return false;
+    }
+    s->fine.patches_off = true;
+    s->fine.coarse_shove_off = true;  // the network carries the tires' effect on the window
+    s->cstats.closure_steps += 1;
+    return true;
+}
+
+silt::closure::FeatureJob closure_job(silt_sheet* s, const std::vector<silt_tire_push>& ps) {
+    silt::closure::FeatureJob J;
+    memset(&J, 0, sizeof J);
+    J.W = silt::fine::view_of(s);
+    silt::closure::crop_origin(ps, s->origin[0], s->origin[1], s->cfg.cell, &J.ci0, &J.cj0);
+    J.ntires = (int)std::min(ps.size(), (size_t)silt::closure::MAX_CROP_TIRES);
+    for (int t = 0; t < J.ntires; ++t) J.tires[t] = ps[t];
+    return J;
+}
+
+int closure_correct(silt_sheet* s, const silt::closure::FeatureJob& F) {
+    std::vector<silt::closure::ApplyJob> A(1);
+    memset(A.data(), 0, sizeof(silt::closure::ApplyJob));
+    A[0].W = silt::fine::view_of(s);
+    A[0].ci0 = F.ci0;
+    A[0].cj0 = F.cj0;
+    CK(s->clos->correct(A, s->net->net, s->st));
+    return SILT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -800,13 +867,22 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     const clock::time_point t0 = clock::now();
     std::vector<silt_tire_push> ps;
     silt::fine::StepOut fo;
-    int rc = step_before_coarse(s, dt, ps, fo);
+    int rc;
+    // The learned closure reads the state the nested sheets would start from.
+    const bool net_on = closure_begin(s);
+    silt::closure::FeatureJob F;
+    if (net_on) {
+        F = closure_job(s, s->pushes);
+        CK(s->clos->features({F}, s->net->net, s->st));
+    }
+    rc = step_before_coarse(s, dt, ps, fo);
     if (rc) return rc;
     const clock::time_point t2 = clock::now();
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
     if (rc) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
+    if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
     if (out || n_out) {
         rc = silt::fine::collect_spray(s->fine, s, fo, out, cap, &nev);
@@ -821,6 +897,58 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         s->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
     }
     s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
+    return SILT_OK;
+}
+
+int silt_set_coupling(silt_sheet* s, int32_t mode, silt_closure* net, float threshold) {
+    if (!s) return fail_arg("handle");
+    if (mode != SILT_COUPLING_NESTED && mode != SILT_COUPLING_NONE && mode != SILT_COUPLING_CLOSURE)
+        return fail_arg("coupling mode");
+    if (mode == SILT_COUPLING_CLOSURE && !net) return fail_arg("closure coupling needs a network");
+    if (!(threshold >= 0.0f) || !std::isfinite(threshold)) return fail_arg("closure threshold");
+    if (net && net->device != s->cfg.device) return fail_arg("closure network on another device");
+    if (mode == SILT_COUPLING_CLOSURE && !s->clos) {
+        s->clos = new silt::closure::Runner();
+        CK(s->clos->reserve(1));
+    }
+    s->coupling = mode;
+    s->net = mode == SILT_COUPLING_CLOSURE ? net : nullptr;
+    s->clos_threshold = threshold;
+    s->clos_fallback_next = false;
+    s->fine.patches_off = mode != SILT_COUPLING_NESTED;
+    s->fine.coarse_shove_off = false;
+    return SILT_OK;
+}
+
+int silt_closure_features(silt_sheet* s, silt_closure* net, void* x, int32_t* origin) {
+    if (!s || !net || !x || !origin) return fail_arg("closure_features");
+    if (((uintptr_t)x & 15u) != 0) return fail_arg("closure_features: x must be 16-byte aligned");
+    if (!s->clos) {
+        s->clos = new silt::closure::Runner();
+        CK(s->clos->reserve(1));
+    }
+    const silt::closure::FeatureJob F = closure_job(s, s->pushes);
+    CK(s->clos->features({F}, net->net, s->st));
+    CK(cudaMemcpyAsync(x, s->clos->x, (size_t)SILT_CLOSURE_CROP * SILT_CLOSURE_CROP * SILT_CLOSURE_CIN * 2,
+                       cudaMemcpyDeviceToDevice, s->st));
+    origin[0] = F.ci0;
+    origin[1] = F.cj0;
+    return SILT_OK;
+}
+
+int silt_get_closure_stats(silt_sheet* s, silt_closure_stats* out) {
+    if (!s || !out) return fail_arg("closure_stats");
+    if (s->clos) {
+        CK(cudaStreamSynchronize(s->st));
+        std::vector<float> r;
+        double moved = 0.0;
+        if (s->clos->poll(r, &moved) && !r.empty()) {
+            s->cstats.last_residual = r[0];
+            s->cstats.moved_m3 = moved;
+            s->clos_fallback_next = r[0] > s->clos_threshold;
+        }
+    }
+    *out = s->cstats;
     return SILT_OK;
 }
 
@@ -1000,6 +1128,33 @@ int silt_write_plane(silt_sheet* s, int32_t which, const float* host) {
     return tiles_dirty(s);
 }
 
+int silt_plane_device(silt_sheet* s, int32_t which, void** out) {
+    if (!s || !out) return fail_arg("plane_device");
+    float* p = plane_of(s, which);
+    if (!p) return fail_arg("plane index");
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    *out = p;
+    return SILT_OK;
+}
+
+int silt_sheet_copy_state(silt_sheet* dst, silt_sheet* src) {
+    if (!dst || !src || dst == src) return fail_arg("copy_state");
+    if (dst->res != src->res || dst->cfg.device != src->cfg.device) return fail_arg("copy_state: different windows");
+    int rc = flush_cut(src);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(src->st));
+    rc = flush_cut(dst);
+    if (rc) return rc;
+    for (int which = 0; which < 8; ++which)
+        CK(cudaMemcpyAsync(plane_of(dst, which), plane_of(src, which), dst->n * 4, cudaMemcpyDeviceToDevice, dst->st));
+    CK(cudaMemcpyAsync(dst->grain, src->grain, dst->n, cudaMemcpyDeviceToDevice, dst->st));
+    dst->vmax_bound = src->vmax_bound;
+    dst->moisture_ambient = src->moisture_ambient;
+    dst->ledger_fresh = false;
+    return tiles_dirty(dst);
+}
+
 int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
                           float* origin2) {
     if (!s || (n > 0 && !tires) || !host) return fail_arg("fine_water_debug");
@@ -1147,6 +1302,9 @@ struct silt_batch {
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool, ev_used;  // groups of three: start, after force, after transport
     silt_step_parts parts;
+    // The learned closure over the windows coupled by it: one crop per window
+    // with tires, every crop through the same launches.
+    silt::closure::Runner* clos = nullptr;
     // Ledger gather: per window the depth sums and the books, one copy back.
     const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
     double* d_ledgers = nullptr;            // 5 doubles per window
@@ -1158,6 +1316,10 @@ namespace {
 int batch_free(silt_batch* b) {
     if (!b) return SILT_OK;
     if (b->st) cudaStreamSynchronize(b->st);
+    if (b->clos) {
+        b->clos->release();
+        delete b->clos;
+    }
     delete b->workers;
     silt::fine::batch_free(b->fine);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
@@ -1188,6 +1350,45 @@ cudaEvent_t batch_event(silt_batch* b) {
     }
     b->ev_used.push_back(e);
     return e;
+}
+
+// Per window of the batch: whether its nested patches are laid this step and
+// whether the closure corrects it (the residual estimates of the last
+// correction decide the fallbacks, as in the single-window step).
+int batch_closure_begin(silt_batch* b, std::vector<int>& net_win, std::vector<silt::closure::FeatureJob>& feats,
+                        const silt_closure** net) {
+    std::vector<float> r;
+    std::vector<int> wins;
+    double moved = 0.0;
+    if (b->clos && b->clos->poll(r, &moved, &wins))
+        for (size_t k = 0; k < r.size() && k < wins.size(); ++k) {
+            silt_sheet* s = b->sheets[wins[k]];
+            s->cstats.last_residual = r[k];
+            s->clos_fallback_next = r[k] > s->clos_threshold;
+        }
+    for (int w = 0; w < (int)b->sheets.size(); ++w) {
+        silt_sheet* s = b->sheets[w];
+        s->fine.patches_off = s->coupling != SILT_COUPLING_NESTED;
+        s->fine.coarse_shove_off = false;
+        if (s->coupling != SILT_COUPLING_CLOSURE || s->pushes.empty()) continue;
+        if (s->clos_fallback_next) {
+            s->clos_fallback_next = false;
+            s->fine.patches_off = false;
+            s->cstats.fallback_steps += 1;
+            continue;
+        }
+        if (*net && *net != s->net) return fail_arg("batch: closure windows must share one network");
+        *net = s->net;
+        s->fine.coarse_shove_off = true;
+        s->cstats.closure_steps += 1;
+        net_win.push_back(w);
+        feats.push_back(closure_job(s, s->pushes));
+    }
+    if (!net_win.empty()) {
+        if (!b->clos) b->clos = new silt::closure::Runner();
+        CK(b->clos->reserve((int)net_win.size()));
+    }
+    return SILT_OK;
 }
 
 // The coarse pairs of every window, `launched` substeps at most, through the
@@ -1353,6 +1554,7 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
 int silt_batch_destroy(silt_batch* b) { return batch_free(b); }
 
 int silt_batch_step(silt_batch* b, float dt) {
+    int rc;
     if (!b) return fail_arg("batch");
     if (!(dt > 0.0f) || !std::isfinite(dt)) {
         for (silt_sheet* s : b->sheets) s->pushes.clear();
@@ -1368,6 +1570,13 @@ int silt_batch_step(silt_batch* b, float dt) {
     const int nk = (int)Wk.threads.size();
     std::vector<char> work(n, 0);
     for (auto& c : Wk.launches) c = 0;
+    // Windows the learned closure corrects this step: their crops are read
+    // from the state before anything of the step touches it.
+    std::vector<int> net_win;
+    std::vector<silt::closure::FeatureJob> feats;
+    const silt_closure* net = nullptr;
+    if ((rc = batch_closure_begin(b, net_win, feats, &net))) return rc;
+    if (!feats.empty()) CK(b->clos->features(feats, net->net, b->st));
     CK(cudaEventRecord(b->ev_start, b->st));  // the workers' streams start after the batch's previous work
     // Each window's tire pushes, inflow and nested-patch planning on the
     // workers (the planning uploads the window's tables on the worker's
@@ -1400,7 +1609,6 @@ int silt_batch_step(silt_batch* b, float dt) {
             snprintf(g_err, sizeof g_err, "%s", Wk.err[k].c_str());
             return Wk.rc[k];
         }
-    int rc;
     for (int k = 0; k < nk; ++k) CK(cudaStreamWaitEvent(b->st, Wk.done[k], 0));
     std::vector<silt_sheet*> fs;
     std::vector<silt::fine::Patches*> fp;
@@ -1413,6 +1621,16 @@ int silt_batch_step(silt_batch* b, float dt) {
     const clock::time_point t1 = clock::now();
     if ((rc = batch_coarse(b, dt))) return rc;
     if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
+    if (!net_win.empty()) {
+        std::vector<silt::closure::ApplyJob> A(net_win.size());
+        memset(A.data(), 0, A.size() * sizeof(silt::closure::ApplyJob));
+        for (size_t k = 0; k < net_win.size(); ++k) {
+            A[k].W = silt::fine::view_of(b->sheets[net_win[k]]);
+            A[k].ci0 = feats[k].ci0;
+            A[k].cj0 = feats[k].cj0;
+        }
+        CK(b->clos->correct(A, net->net, b->st, net_win));
+    }
     for (int w = 0; w < n; ++w) {
         silt_sheet* s = b->sheets[w];
         s->parts.steps += 1;

@@ -111,6 +111,7 @@ def lib():
             "silt_batch_get_ledgers": [_p, ctypes.POINTER(Ledger)],
             "silt_batch_push_tires": [_p, _p, ctypes.POINTER(TirePush), _i],
             "silt_batch_set_timing": [_p, _i], "silt_batch_get_parts": [_p, ctypes.POINTER(StepParts)],
+            "silt_plane_device": [_p, _i, ctypes.POINTER(_p)], "silt_sheet_copy_state": [_p, _p],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -148,6 +149,14 @@ def make_push(t):
                     t["speed"], t.get("slip", 0.0))
 
 
+class _DeviceArray:
+    """A device FP32 array exposed through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
 class Sheet:
     """A window of the two-layer sheet on the GPU (FluidCore, src/fluid_core.rs:4808)."""
 
@@ -166,6 +175,7 @@ class Sheet:
         self.h = h
         self.res = res
         self.fine_res = fine_res
+        self.device = device
 
     def close(self):
         if getattr(self, "h", None):
@@ -242,6 +252,19 @@ class Sheet:
 
     def set(self, name, arr):
         check(lib().silt_write_plane(self.h, PLANES[name], _ptr(_f32(arr))), "write_plane")
+
+    def plane_device(self, name):
+        """The plane's device memory as a torch tensor view (res x res FP32),
+        valid until the next step or write; read it on the sheet's stream."""
+        import torch
+
+        ptr = ctypes.c_void_p()
+        check(lib().silt_plane_device(self.h, PLANES[name], ctypes.byref(ptr)), "plane_device")
+        view = _DeviceArray(ptr.value, (self.res, self.res))
+        return torch.as_tensor(view, device=f"cuda:{self.device}")
+
+    def copy_state_from(self, other):
+        check(lib().silt_sheet_copy_state(self.h, other.h), "copy_state")
 
     def export_maps(self):
         n = self.res * self.res

@@ -18,9 +18,9 @@ import silt_b200
 
 CROP = 32
 CIN, HID, COUT = 16, 32, 16
-IN_USED, OUT_USED = 6, 4
+IN_USED, OUT_USED = 6, 8
 NPARAM = 9 * CIN * HID + HID + 9 * HID * HID + HID + 9 * HID * COUT + COUT
-NNORM = 16
+NNORM = 20
 COUPLING_NESTED, COUPLING_NONE, COUPLING_CLOSURE = 0, 1, 2
 
 # (name, cin, cout) of the three layers, in parameter order.
@@ -38,6 +38,7 @@ _SIGS = {
     "silt_conv3x3_forward": [_p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _p],
     "silt_conv3x3_wgrad": [_p, _p, _p, _p, _i, _i, _i, _i, _i, _p],
     "silt_closure_loss_grad": [_p, _p, _p, _p, _p, _i, _i, _i, _f, _p],
+    "silt_closure_step_loss_grad": [_p, _p, _p, _p, _f, _p, _p, _i, _f, _p],
     "silt_closure_adam": [_p, _p, _p, _p, _i, _f, _f, _f, _f, _i, _p],
     "silt_closure_pack": [_p, _p, _p, _i, _i, _p],
     "silt_closure_create": [_p, _i, _p, _i, ctypes.POINTER(_p)],
@@ -181,6 +182,24 @@ def loss_grad(y, target, weight=None):
     scale = 1.0 / float(n_pix * OUT_USED)
     silt_b200.check(fn("silt_closure_loss_grad")(_ptr(y), _ptr(target), _ptr(weight), _ptr(dy), _ptr(loss), n_pix,
                                                  COUT, OUT_USED, scale, _stream()), "closure_loss_grad")
+    return dy, loss
+
+
+def step_loss_grad(y, t, scale, inv_var, lam=0.0):
+    """Loss of the step correction (mean over the crops' cells): the depth
+    change the predicted transfers make and the predicted velocity change
+    against t [n, 32, 32, 8] FP32 (water and slurry depth change in m; water
+    u, v and slurry u, v change in m/s; water and slurry velocity weights),
+    scale [8] and inv_var [6] FP32 device tensors. Returns (dy BF16, loss FP64)."""
+    import torch
+
+    n = y.shape[0]
+    dy = torch.empty(y.shape, dtype=torch.bfloat16, device=y.device)
+    loss = torch.zeros(1, dtype=torch.float64, device=y.device)
+    norm = 1.0 / float(n * CROP * CROP)
+    silt_b200.check(fn("silt_closure_step_loss_grad")(_ptr(y), _ptr(t), _ptr(scale), _ptr(inv_var), float(lam),
+                                                      _ptr(dy), _ptr(loss), n, norm, _stream()),
+                    "closure_step_loss_grad")
     return dy, loss
 
 

@@ -4,19 +4,21 @@
  * (src/fluid_core.rs:6034-6128: refine -> fine pair -> restrict) on the
  * coarse window: a 3-layer 3 x 3 convolutional network (BF16 weights and
  * activations, FP32 accumulation on the tcgen05 tensor cores) reads the
- * coarse state around the vehicle and predicts, per coarse face, the depth
- * the nested sheets would have moved across it beyond what the plain coarse
- * step moved. The correction moves depth between neighbouring cells only, so
- * the window's volume is conserved to the ledger. The nested sheets remain
- * the fallback: a window whose closure residual estimate exceeds the
- * threshold steps nested on its next step.
+ * coarse state around the vehicle and predicts, per coarse face, depth moved
+ * across it, and per wet cell a velocity change, so that the window after the
+ * coarse step (which then applies no tire shove) matches what the nested
+ * sheets would have left. The correction moves depth between neighbouring
+ * cells only, so the window's volume is conserved to the ledger. The nested sheets remain the fallback:
+ * a window whose closure residual estimate exceeds the threshold steps nested
+ * on one of its next steps.
  *
  * Network (one crop of CROP x CROP coarse cells centred on the vehicle):
  *   in  : 6 channels (water depth, slurry depth, water u, water v, bed,
  *         tire shove field), normalised, zero-padded to 16 channels;
  *   L1  : 3x3 conv 16 -> 32, ReLU;  L2 : 3x3 conv 32 -> 32, ReLU;
- *   L3  : 3x3 conv 32 -> 16 (4 used: water x-face, water z-face, slurry
- *         x-face, slurry z-face depth transfer, normalised).
+ *   L3  : 3x3 conv 32 -> 16 (8 used: water x-face, water z-face, slurry
+ *         x-face, slurry z-face depth transfer; water u, water v, slurry u,
+ *         slurry v change; normalised).
  * Activations are NHWC BF16 ([image][row][col][channel]); weights for the
  * forward pass are [cout][tap][cin] BF16, tap = 3 * (dy + 1) + (dx + 1).
  * The FP32 parameter vector (silt_closure_create, the training entry points)
@@ -42,17 +44,18 @@ extern "C" {
 #define SILT_CLOSURE_HIDDEN 32
 #define SILT_CLOSURE_COUT 16
 #define SILT_CLOSURE_IN_USED 6
-#define SILT_CLOSURE_OUT_USED 4
+#define SILT_CLOSURE_OUT_USED 8
 /* FP32 parameters: 9*16*32 + 32 + 9*32*32 + 32 + 9*32*16 + 16. */
 #define SILT_CLOSURE_NPARAM 18512
-/* Normalisation block: 6 input means, 6 input inverse deviations, 4 output
- * scales (m of depth per unit of network output). */
-#define SILT_CLOSURE_NNORM 16
+/* Normalisation block: 6 input means, 6 input inverse deviations, 8 output
+ * scales (m of depth, then m/s, per unit of network output). */
+#define SILT_CLOSURE_NNORM 20
 
 /* Coupling of the tire sheets into the window (silt_set_coupling). */
 #define SILT_COUPLING_NESTED 0  /* the reference: nested 2 cm sheets */
 #define SILT_COUPLING_NONE 1    /* tires shove the coarse cells directly, no sheets */
-#define SILT_COUPLING_CLOSURE 2 /* NONE plus the learned face-flux correction */
+#define SILT_COUPLING_CLOSURE 2 /* no sheets and no coarse shove: the learned face-flux
+                                 * correction carries the tires' effect */
 
 /* ---- Tensor-core kernels (inference and training) ---------------------- */
 
@@ -77,6 +80,19 @@ int silt_conv3x3_wgrad(const void* x_bf16, const void* dy_bf16, float* dw, float
  * dy = 2 w (y - t) * scale as BF16 (channels >= n_out zero). */
 int silt_closure_loss_grad(const float* y, const float* target, const float* pixel_weight, void* dy_bf16,
                            double* loss, int32_t n_pix, int32_t cout_pad, int32_t n_out, float scale, void* stream);
+
+/* Loss of one closure step's correction, per crop of SILT_CLOSURE_CROP^2
+ * cells. y: n_img crops x CROP^2 x SILT_CLOSURE_COUT FP32 network output
+ * (channels 0..7 as above, in units of scale[c]; faces across the crop's
+ * edge count as 0). t: n_img x CROP^2 x 8 FP32 targets: water and slurry
+ * depth change (m), water u, v and slurry u, v change (m/s), and the water
+ * and slurry weights of the velocity terms (1 where the cell is wet). loss +=
+ * norm * sum over cells of [inv_var[l] (div_l - dh_l)^2 over the two layers +
+ * inv_var[2 + k] w (y[4 + k] scale[4 + k] - dv_k)^2 over the four velocity
+ * channels + lambda * sum of y[0..7]^2], with div the cell's inflow minus
+ * outflow; dy = d loss / d y as BF16 (channels >= 8 zero). */
+int silt_closure_step_loss_grad(const float* y, const float* t, const float* scale, const float* inv_var, float lambda,
+                                void* dy_bf16, double* loss, int32_t n_img, float norm, void* stream);
 
 /* One Adam step (bias-corrected) on n FP32 parameters. */
 int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32_t n, float lr, float beta1,

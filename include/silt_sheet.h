@@ -157,6 +157,14 @@ int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
  * 3 vw, 4 us, 5 vs, 6 bed, 7 moisture. */
 int silt_read_plane(silt_sheet* s, int32_t which, float* host);
 int silt_write_plane(silt_sheet* s, int32_t which, const float* host);
+/* Device pointer of plane `which` (same indices) in the handle's current
+ * buffers, valid until the next step or write; the caller orders its reads
+ * after the handle's stream. */
+int silt_plane_device(silt_sheet* s, int32_t which, void** out);
+/* Device-to-device copy of src's window state (depths, velocities, bed,
+ * moisture, grain) into dst (same size and device); dst's nested patches and
+ * near field are untouched. Used to step one state two ways. */
+int silt_sheet_copy_state(silt_sheet* dst, silt_sheet* src);
 /* FluidCore::fine_water_debug (src/fluid_core/near.rs:341): lays the patch
  * down for these tires, copies patch `patch` (fine_res^2 floats) and its
  * origin, and packs it back. */
