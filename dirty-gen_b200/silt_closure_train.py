@@ -102,22 +102,26 @@ def crop(plane, ci0, cj0):
     return out
 
 
-def generate(n_windows=128, steps=160, base_seed=0x5EED0C10, log=print):
-    """Pairs from n_windows x steps nested steps. Returns (x_raw [N, 32, 32, 16]
-    BF16 raw inputs, targets [N, 32, 32, 8] FP32: water and slurry depth
-    change (m, mean removed), water u, v and slurry u, v change (m/s, where the
-    coarse step left the cell wet), water and slurry wet weights; window
-    index [N], step [N])."""
+def generate(n_windows=128, steps=160, base_seed=0x5EED0C10, log=print, rollout=None):
+    """Pairs from n_windows x steps steps. The states come from the nested run
+    itself, or with `rollout` = (params, norm) from windows the closure with
+    that network drives (each step's state copied into a nested and a
+    coarse-only window for the target), so the network also learns from the
+    states its own corrections lead to. Returns (x_raw [N, 32, 32, 16] BF16
+    raw inputs, targets [N, 32, 32, 8] FP32: water and slurry depth change
+    (m, mean removed), water u, v and slurry u, v change (m/s, where the
+    coarse step left the cell wet), water and slurry wet weights; window index
+    [N], step [N])."""
     import torch
 
     st = torch.cuda.Stream()  # the sheets, batches and crop arithmetic share one stream
     with torch.cuda.stream(st):
-        out = _generate(n_windows, steps, base_seed, st.cuda_stream, log)
+        out = _generate(n_windows, steps, base_seed, st.cuda_stream, log, rollout)
     torch.cuda.synchronize()
     return out
 
 
-def _generate(n_windows, steps, base_seed, stream, log):
+def _generate(n_windows, steps, base_seed, stream, log, rollout):
     import torch
 
     scenes = [drive_scene(k, base_seed) for k in range(n_windows)]
@@ -128,6 +132,12 @@ def _generate(n_windows, steps, base_seed, stream, log):
     nested = make_sheets(scenes, stream)
     plain = make_sheets(scenes, stream, C.COUPLING_CLOSURE, probe, 1e30)
     bn, bp = silt_b200.Batch(nested), silt_b200.Batch(plain)
+    drive_net, driven, bd = None, None, None
+    if rollout is not None:
+        drive_net = C.Closure(rollout[0], rollout[1])
+        driven = make_sheets(scenes, stream, C.COUPLING_CLOSURE, drive_net, 1e30)
+        bd = silt_b200.Batch(driven)
+    src = driven if driven is not None else nested
     N = n_windows * steps
     xs = torch.zeros((N, C.CROP, C.CROP, C.CIN), dtype=torch.bfloat16, device="cuda")
     dhs = torch.zeros((N, C.CROP, C.CROP, 8), dtype=torch.float32, device="cuda")
@@ -137,7 +147,9 @@ def _generate(n_windows, steps, base_seed, stream, log):
     q = 0
     for step in range(1, steps + 1):
         for k in range(n_windows):
-            plain[k].copy_state_from(nested[k])
+            plain[k].copy_state_from(src[k])
+            if driven is not None:
+                nested[k].copy_state_from(src[k])
         push_all(bn, scenes, step)
         origins = []
         for k in range(n_windows):
@@ -145,6 +157,9 @@ def _generate(n_windows, steps, base_seed, stream, log):
         push_all(bp, scenes, step)
         bn.step(DT)
         bp.step(DT)
+        if bd is not None:
+            push_all(bd, scenes, step)
+            bd.step(DT)
         t = torch.zeros((n_windows, 8, C.CROP, C.CROP), dtype=torch.float32, device="cuda")
         for k in range(n_windows):
             ci0, cj0 = origins[k]
@@ -152,8 +167,9 @@ def _generate(n_windows, steps, base_seed, stream, log):
                 hb = crop(plain[k].plane_device(hn), ci0, cj0)
                 t[k, l] = crop(nested[k].plane_device(hn), ci0, cj0) - hb
                 wet = (hb >= 1e-6).float()
-                t[k, 2 + 2 * l] = (crop(nested[k].plane_device(un), ci0, cj0) - crop(plain[k].plane_device(un), ci0, cj0)) * wet
-                t[k, 3 + 2 * l] = (crop(nested[k].plane_device(vn), ci0, cj0) - crop(plain[k].plane_device(vn), ci0, cj0)) * wet
+                for m, name in ((0, un), (1, vn)):
+                    t[k, 2 + 2 * l + m] = (crop(nested[k].plane_device(name), ci0, cj0) -
+                                           crop(plain[k].plane_device(name), ci0, cj0)) * wet
                 t[k, 6 + l] = wet
             wins[q + k] = k
             stp[q + k] = step
@@ -162,11 +178,14 @@ def _generate(n_windows, steps, base_seed, stream, log):
         q += n_windows
         if step % 40 == 0:
             log(f"generate: step {step}/{steps}, {time.time() - t0:.1f} s")
-    bn.close()
-    bp.close()
-    for sh in nested + plain:
+    for b in (bn, bp, bd):
+        if b is not None:
+            b.close()
+    for sh in nested + plain + (driven or []):
         sh.close()
     probe.close()
+    if drive_net is not None:
+        drive_net.close()
     return xs, dhs, wins, stp
 
 
@@ -269,6 +288,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=160)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--held-windows", type=int, default=13)
+    ap.add_argument("--rollouts", type=int, default=1, help="rounds of pairs from closure-driven windows")
     ap.add_argument("--out", default=os.path.join(HERE, "closure_weights.npz"))
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
@@ -277,8 +297,20 @@ def main(argv=None):
     held = (wins >= a.windows - a.held_windows).to("cuda")
     norm = norm_block(xs[~held], dhs[~held])
     params, report = train(xs, dhs, norm, held, epochs=a.epochs)
+    rounds = [report]
+    # Rollout rounds: states the closure's own corrections lead to, targets
+    # from the nested and coarse-only steps of copies of them.
+    for r in range(a.rollouts):
+        xr, dr, wr, _ = generate(a.windows, a.steps, rollout=(params, norm))
+        xs, dhs = torch.cat([xs, xr]), torch.cat([dhs, dr])
+        wins = torch.cat([wins, wr])
+        held = (wins >= a.windows - a.held_windows).to("cuda")
+        params, report = train(xs, dhs, norm, held, epochs=max(1, a.epochs // (r + 2)))
+        rounds.append(report)
+    report = dict(report)
+    report["rounds"] = [{k: v for k, v in rr.items() if k != "history"} for rr in rounds]
     report.update({"windows": a.windows, "steps": a.steps, "pairs": int(xs.shape[0]),
-                   "held_windows": a.held_windows, "norm": norm.tolist()})
+                   "held_windows": a.held_windows, "rollouts": a.rollouts, "norm": norm.tolist()})
     np.savez(a.out, params=params.astype(np.float32), norm=norm)
     print(json.dumps({k: v for k, v in report.items() if k != "history"}), flush=True)
     if a.report:
