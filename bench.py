@@ -60,6 +60,8 @@ def parse():
                          "four tires each, the learned closure against the nested 2 cm sheets")
     ap.add_argument("--windows", type=int, default=None, help="batch: number of windows (256); closure: (128)")
     ap.add_argument("--batch-tires", type=int, default=1, help="batch: 1 = each window's 0..4 tires, 0 = none")
+    ap.add_argument("--closure-threshold", type=float, default=0.1,
+                    help="closure: residual estimate above which a window's next step runs the nested sheets")
     return ap.parse_args()
 
 
@@ -683,14 +685,13 @@ def run_window200(args):
 
 
 CLOSURE_EVAL_SEED = 0xC0FFEE11  # evaluation windows: not among the training windows
-CLOSURE_THRESHOLD = 0.25
 
 
 def closure_workload(args):
     return {"workload": f"closure{args.windows}_win200_4tires_speed2-10", "windows": args.windows, "res": 200,
             "cell_m": CELL, "dt_s": DT, "fine_res": FINE_RES, "layout": "per_tire64",
             "network": "3x3 conv 6(16)-32-32-4(16), bf16, fp32 accumulate", "crop": 32,
-            "residual_threshold": CLOSURE_THRESHOLD,
+            "residual_threshold": args.closure_threshold,
             "l2": "inputs larger than L2 (four forms x 128 windows, ~0.7 GB of state)"}
 
 
@@ -787,7 +788,7 @@ def run_closure(args):
     scenes = [T.drive_scene(k, CLOSURE_EVAL_SEED) for k in range(args.windows)]
     forms = {}
     for name, mode, nn, thr in (("nested", C.COUPLING_NESTED, None, 0.0),
-                                ("closure", C.COUPLING_CLOSURE, net, CLOSURE_THRESHOLD),
+                                ("closure", C.COUPLING_CLOSURE, net, args.closure_threshold),
                                 ("uncorrected", C.COUPLING_CLOSURE, zero, 1e30),
                                 ("plain", C.COUPLING_NONE, None, 0.0)):
         sheets = T.make_sheets(scenes, stream.cuda_stream, mode, nn, thr)
