@@ -301,10 +301,15 @@ def run_b200(args):
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     nev = 0
+    prev = sheet.ledger()
+    gap = 0.0  # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
     for _ in range(e2e_steps):
         ev = one_step(True)
         nev += len(ev)
-        sheet.ledger()
+        led = sheet.ledger()
+        kept = led["total_m3"] + led["cut_m3"] - led["opened_m3"]
+        gap = max(gap, abs(kept - (prev["total_m3"] + prev["cut_m3"] - prev["opened_m3"])) / led["total_m3"])
+        prev = led
     f1.record(stream)
     torch.cuda.synchronize()
     ems = f0.elapsed_time(f1)
@@ -345,7 +350,8 @@ def run_b200(args):
                 "device_counted_steps": int(parts["device_counts"]),
                 "window_steps_per_s": world * args.steps / (ms / 1000.0),
                 "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
-                           "spray_m3": led["spray_m3"]}}
+                           "spray_m3": led["spray_m3"], "cut_m3": led["cut_m3"],
+                           "gap_max_per_step": gap, "gap_steps": e2e_steps}}
         if not args.no_baseline:
             line["cpu_baseline"] = cpu_baseline(args, scene)
         print(json.dumps(line), flush=True)
@@ -577,7 +583,7 @@ def run_batch(args):
                                      "per_window_before_coarse": parts["host_fine_ms"] / args.steps},
                 "window_steps_per_s": len(all_wins) * args.steps / (ms / 1000.0),
                 "windows": len(all_wins), "windows_rank0": len(wins), "coarse_cells_rank0": coarse,
-                "tires_rank0": n_tires, "ledger_total_m3": float(table[:, -1].sum())}
+                "tires_rank0": n_tires, "ledger_total_m3": float(table[:, 6].sum())}
         if not args.no_baseline:
             line["cpu_baseline"] = batch_cpu(args, all_wins, max_steps=20, warmup=1, budget_s=20.0)
         print(json.dumps(line), flush=True)
@@ -859,8 +865,9 @@ def run_closure(args):
         for _ in range(e2e_steps):
             one_step(name)
             rows = b.ledger_rows()
-            tot, opened = rows[:, 6], rows[:, 5]
-            expect = prev[:, 6] + (opened - prev[:, 5])
+            # Books with the dry cut's volume: total + cut - opened is conserved.
+            tot, opened = rows[:, 6] + rows[:, 7], rows[:, 5]
+            expect = prev[:, 6] + prev[:, 7] + (opened - prev[:, 5])
             worst = max(worst, float(np.max(np.abs(tot - expect) / np.maximum(expect, 1e-30))))
             prev = rows
         f1.record(stream)

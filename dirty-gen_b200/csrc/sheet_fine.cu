@@ -136,7 +136,7 @@ struct Impl {
     bool spray_dirty = false;         // the spray count may be non-zero (a step with tires ran)
     // Spray.
     SprayRec* spray = nullptr;
-    double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3
+    double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3, [3] dry cut m3
     double* h_books = nullptr;
     int* h_counters = nullptr;
 };
@@ -408,7 +408,8 @@ __device__ void peel_cell(float* w, const float* uw, const float* vw, int res, f
         const float before = w[idx], after = before - take;
         w[idx] = after;
         int slot = atomicAdd(&counters[3], 1);
-        atomicAdd(&books[0], (double)(take * area));
+        // The spray book takes the cell's actual change, so the FP64 books close.
+        atomicAdd(&books[0], ((double)before - (double)after) * ((double)cell * (double)cell));
         // The depth sum follows the cell's actual (rounded) change.
         if (ledger_depth) atomicAdd(ledger_depth, (double)after - (double)before);
         if (slot < SPRAY_CAP) {
@@ -1201,6 +1202,8 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 window::attach_scratch(J, S->win[l], fn);
                 J.res = fres;
                 J.cell = P.fcell;
+                J.cut = M.d_books + 3;
+                J.cut_area = (double)P.fcell * (double)P.fcell;
                 J.dt = dt;
                 J.vort = l == 0 ? 0.08f : 0.05f;
                 J.sub_cap = P.sub_cap;
@@ -1428,9 +1431,9 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
     return SILT_OK;
 }
 
-const double* books(Patches& P) { return I(P).d_books; }
+double* books(Patches& P) { return I(P).d_books; }
 
-int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s) {
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut) {
     Impl& M = I(P);
     SheetView W = view_of(s);
     FCK(cudaMemcpyAsync(M.h_books, M.d_books, 4 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
@@ -1438,6 +1441,7 @@ int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, doubl
     *spray = M.h_books[0];
     *park_w = M.h_books[1];
     *park_s = M.h_books[2];
+    if (cut) *cut = M.h_books[3];
     return SILT_OK;
 }
 

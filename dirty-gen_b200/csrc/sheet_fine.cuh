@@ -100,9 +100,9 @@ int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::
                cudaStream_t st);
 int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out);
 // FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
-int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s);
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr);
 // Device address of the books: [0] spray, [1] parked water, [2] parked slurry (m^3, FP64).
-const double* books(Patches& P);
+double* books(Patches& P);
 const char* last_error();
 int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, int patch, float* host,
                 float* origin2);

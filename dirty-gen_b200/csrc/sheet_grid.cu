@@ -530,7 +530,7 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         DN[TIDX(c, r)] = dh;
     });
     __syncthreads();
-    double part = 0.0;
+    double part = 0.0, cut = 0.0;
     trows<EDGE, TT, TT>(tx0, tx1, ty0, ty1, [&](int c, int r) {
         float upm = r - 1 >= 0 ? UP[TIDX(c, r - 1)] : 0.0f;
         float dnm = r - 1 >= 0 ? DN[TIDX(c, r - 1)] : 0.0f;
@@ -541,10 +541,15 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         float hv = HX[TIDX(c, r)];
         float moved = fmaxf(hv - rem + add, 0.0f);
         float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
-        if (P.eps > 0.0f && hn < P.eps) hn = 0.0f;
+        if (P.eps > 0.0f && hn < P.eps) {
+            if (hn > 0.0f) cut += (double)hn;  // booked: the dry cut's volume
+            hn = 0.0f;
+        }
         P.h_out[(size_t)r * res + c] = hn;
         part += (double)fmaxf(hn, 0.0f);
     });
+    for (int o = 16; o > 0; o >>= 1) cut += __shfl_down_sync(0xffffffffu, cut, o);
+    if ((threadIdx.x & 31) == 0 && cut > 0.0 && P.cut) atomicAdd(P.cut, cut * P.cut_area);
 #undef TIDX
     // Block sum of the depth (FP64), one atomic per tile; the tile's flags.
     const int any = __syncthreads_or(part > 0.0);

@@ -80,6 +80,8 @@ struct TransportParams {
     const uint8_t* gate;      // nullptr = every receiver open
     const float* bank_bed;    // nullptr = no dry-bank test (banks off)
     double* ledger;           // FP64 sum of the new depth, may be nullptr
+    double* cut;              // FP64 volume the dry cut removed, m^3 (accumulated), may be nullptr
+    double cut_area;          // m^2 of one cell for that book
     int32_t res;
     float cell, dt, eps;
     int32_t skip;

@@ -260,6 +260,8 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         Q.gate = nullptr;
         Q.bank_bed = nullptr;
         Q.ledger = s->d_acc + l;
+        Q.cut = silt::fine::books(s->fine) + 3;
+        Q.cut_area = (double)cell * (double)cell;
         Q.res = res;
         Q.cell = cell;
         Q.dt = dt;
@@ -357,6 +359,8 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         J.moisture = s->moisture;
         silt::window::attach_scratch(J, s->win_planes + (size_t)l * silt::window::SCRATCH_PLANES * s->n, s->n);
         J.ledger = s->d_acc + l;
+        J.cut = silt::fine::books(s->fine) + 3;
+        J.cut_area = (double)s->cfg.cell * (double)s->cfg.cell;
         J.res = s->res;
         J.cell = s->cfg.cell;
         J.dt = dt;
@@ -961,8 +965,8 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    double spray = 0.0, park_w = 0.0, park_s = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s);
+    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -977,6 +981,7 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->spray_m3 = spray;
     out->opened_m3 = s->opened_m3;
     out->total_m3 = w + sl + park_w + park_s + spray;
+    out->cut_m3 = cut;
     return SILT_OK;
 }
 
@@ -1307,7 +1312,7 @@ struct silt_batch {
     silt::closure::Runner* clos = nullptr;
     // Ledger gather: per window the depth sums and the books, one copy back.
     const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
-    double* d_ledgers = nullptr;            // 5 doubles per window
+    double* d_ledgers = nullptr;            // 6 doubles per window
     double* h_ledgers = nullptr;            // pinned
 };
 
@@ -1510,8 +1515,8 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->count, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemsetAsync(b->count, 0, 2 * sizeof(int), b->st);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 5 * (size_t)n * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 5 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 6 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 6 * (size_t)n * sizeof(double));
     if (e == cudaSuccess) {
         std::vector<const double*> src(2 * (size_t)n);
         for (int w = 0; w < n; ++w) {
@@ -1660,7 +1665,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         return SILT_OK;
     }
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
-    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 5 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)
         CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
@@ -1668,7 +1673,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         silt_sheet* s = b->sheets[w];
         int rc = check_substep_overflow(s);
         if (rc) return rc;
-        const double* g = b->h_ledgers + 5 * (size_t)w;
+        const double* g = b->h_ledgers + 6 * (size_t)w;
         const double area = (double)s->cfg.cell * (double)s->cfg.cell;
         silt_ledger& L = out[w];
         L.water_m3 = g[0] * area;
@@ -1678,6 +1683,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         L.frozen_slurry_m3 = g[4];
         L.opened_m3 = s->opened_m3;
         L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3;
+        L.cut_m3 = g[5];
     }
     return SILT_OK;
 }

@@ -305,13 +305,17 @@ __device__ void cta_dry_cut(const Job& J, const Box& b) {
     float* __restrict__ h = J.h;
     float* __restrict__ u = J.u;
     float* __restrict__ v = J.v;
+    double cut = 0.0;  // depth the cut removes, booked so the FP64 books still close
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (h[g] < eps) {
+            if (h[g] > 0.0f) cut += (double)h[g];
             h[g] = 0.0f;
             u[g] = 0.0f;
             v[g] = 0.0f;
         }
     })
+    for (int o = 16; o > 0; o >>= 1) cut += __shfl_down_sync(0xffffffffu, cut, o);
+    if ((threadIdx.x & 31) == 0 && cut > 0.0 && J.cut) atomicAdd(J.cut, cut * J.cut_area);
     crew_sync();
 }
 

@@ -31,6 +31,8 @@ struct Job {
     float* f2;             // transient: edge fluxes, wet-body labels
     float* gs[4];          // Gauss-Seidel confinement: u0, v0, u after gravity, v after gravity
     double* ledger;        // FP64 sum of max(h, 0) after the step, may be nullptr
+    double* cut;           // FP64 volume the dry cut removed, m^3 (accumulated), may be nullptr
+    double cut_area;       // m^2 of one cell for that book
     int32_t res;
     float cell, dt, vort, sub_cap, eps;
     int32_t nu_mode;

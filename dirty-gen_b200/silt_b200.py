@@ -42,7 +42,7 @@ class SprayEvent(ctypes.Structure):
 
 class Ledger(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3",
-                                               "spray_m3", "opened_m3", "total_m3")]
+                                               "spray_m3", "opened_m3", "total_m3", "cut_m3")]
 
 
 class CoarseCell(ctypes.Structure):

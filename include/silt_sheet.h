@@ -91,6 +91,10 @@ typedef struct {
  * accumulated in FP64. `opened_m3` is water added by an inflow strip. */
 typedef struct {
     double water_m3, slurry_m3, frozen_water_m3, frozen_slurry_m3, spray_m3, opened_m3, total_m3;
+    /* Volume the dry cut (src/fluid_core.rs:2072-2081, films under 1e-6 m)
+     * has removed since creation; not in total_m3, which keeps the
+     * reference's books. total_m3 + cut_m3 - opened_m3 is conserved. */
+    double cut_m3;
 } silt_ledger;
 
 /* src/fluid_core.rs:452-465 (`CoarseCell`), sheet fields. */
