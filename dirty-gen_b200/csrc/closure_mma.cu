@@ -150,6 +150,7 @@ struct ConvShape {
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(THREADS) k_conv3x3(ConvArgs a) {
+    ::silt::dep_wait();
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 32, "shape");
     using S = ConvShape<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
@@ -293,6 +294,7 @@ __device__ __forceinline__ void transpose8(const uint4 (&v)[8], uint4 (&out)[8])
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(THREADS) k_conv3x3_wgrad(WgradArgs a) {
+    ::silt::dep_wait();
     using S = WgradShape<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* As = smem;
@@ -405,6 +407,7 @@ __global__ void __launch_bounds__(THREADS) k_conv3x3_wgrad(WgradArgs a) {
 
 __global__ void k_loss_grad(const float* y, const float* t, const float* wgt, uint16_t* dy, double* loss, int n_pix,
                             int cpad, int n_out, float scale) {
+    ::silt::dep_wait();
     double part = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pix; p += gridDim.x * blockDim.x) {
         const float w = wgt ? wgt[p] : 1.0f;
@@ -433,6 +436,7 @@ __global__ void k_loss_grad(const float* y, const float* t, const float* wgt, ui
 __global__ void __launch_bounds__(SILT_CLOSURE_CROP * SILT_CLOSURE_CROP)
     k_step_loss(const float* y, const float* t, const float* scale, const float* inv_var, float lam, uint16_t* dy,
                 double* loss, float norm) {
+    ::silt::dep_wait();
     constexpr int N = SILT_CLOSURE_CROP, NC = N * N, CO = SILT_CLOSURE_COUT, NT = 8;
     __shared__ float g[4][NC];
     __shared__ float e[2][NC];
@@ -497,6 +501,7 @@ __global__ void __launch_bounds__(SILT_CLOSURE_CROP * SILT_CLOSURE_CROP)
 
 __global__ void k_adam(float* p, float* m, float* v, const float* g, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2) {
+    ::silt::dep_wait();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float gi = g[i];
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
@@ -508,6 +513,7 @@ __global__ void k_adam(float* p, float* m, float* v, const float* g, int n, floa
 }
 
 __global__ void k_pack(const float* w, uint16_t* fwd, uint16_t* bwd, int cin, int cout) {
+    ::silt::dep_wait();
     const int n = 9 * cin * cout;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int o = i % cout, c = (i / cout) % cin, tap = i / (cout * cin);
@@ -539,7 +545,7 @@ cudaError_t conv_launch(const ConvArgs& a, cudaStream_t st) {
     if (attr != cudaSuccess) return attr;
     const int tiles = a.n_img * ((a.H + TILE_H - 1) / TILE_H) * ((a.W + TILE_W - 1) / TILE_W);
     const int grid = tiles < 2 * sm_count() ? tiles : 2 * sm_count();
-    k_conv3x3<CIN, COUT><<<grid, THREADS, S::SMEM, st>>>(a);
+    ::silt::launch_dep(k_conv3x3<CIN, COUT>, dim3(grid), dim3(THREADS), S::SMEM, st, a);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -551,7 +557,7 @@ cudaError_t wgrad_launch(const WgradArgs& a, cudaStream_t st) {
     if (attr != cudaSuccess) return attr;
     const int tiles = a.n_img * ((a.H + TILE_H - 1) / TILE_H) * ((a.W + TILE_W - 1) / TILE_W);
     const int grid = tiles < sm_count() ? tiles : sm_count();
-    k_conv3x3_wgrad<CIN, COUT><<<grid, THREADS, S::SMEM, st>>>(a);
+    ::silt::launch_dep(k_conv3x3_wgrad<CIN, COUT>, dim3(grid), dim3(THREADS), S::SMEM, st, a);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -645,7 +651,7 @@ int silt_closure_loss_grad(const float* y, const float* target, const float* pix
         return fail(SILT_EINVAL, "invalid argument: closure_loss_grad");
     if (n_pix == 0) return SILT_OK;
     const int blocks = (n_pix + 255) / 256 < 1184 ? (n_pix + 255) / 256 : 1184;
-    k_loss_grad<<<blocks, 256, 0, (cudaStream_t)stream>>>(y, target, pixel_weight, (uint16_t*)dy, loss, n_pix,
+    ::silt::launch_dep(k_loss_grad, dim3(blocks), dim3(256), 0, (cudaStream_t)stream, y, target, pixel_weight, (uint16_t*)dy, loss, n_pix,
                                                           cout_pad, n_out, scale);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_loss_grad");
@@ -656,7 +662,7 @@ int silt_closure_step_loss_grad(const float* y, const float* t, const float* sca
     if (!y || !t || !scale || !inv_var || !dy || n_img < 0)
         return fail(SILT_EINVAL, "invalid argument: closure_step_loss_grad");
     if (n_img == 0) return SILT_OK;
-    k_step_loss<<<n_img, SILT_CLOSURE_CROP * SILT_CLOSURE_CROP, 0, (cudaStream_t)stream>>>(
+    ::silt::launch_dep(k_step_loss, dim3(n_img), dim3(SILT_CLOSURE_CROP * SILT_CLOSURE_CROP), 0, (cudaStream_t)stream, 
         y, t, scale, inv_var, lambda, (uint16_t*)dy, loss, norm);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_step_loss_grad");
@@ -667,7 +673,7 @@ int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32
     if (!param || !m || !v || !grad || n < 0 || step < 1) return fail(SILT_EINVAL, "invalid argument: closure_adam");
     if (n == 0) return SILT_OK;
     const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
-    k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(param, m, v, grad, n, lr, beta1, beta2, eps, c1, c2);
+    ::silt::launch_dep(k_adam, dim3((n + 255) / 256), dim3(256), 0, (cudaStream_t)stream, param, m, v, grad, n, lr, beta1, beta2, eps, c1, c2);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_adam");
 }
@@ -675,7 +681,7 @@ int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32
 int silt_closure_pack(const float* w, void* w_fwd, void* w_bwd, int32_t cin, int32_t cout, void* stream) {
     if (!w || (!w_fwd && !w_bwd) || cin <= 0 || cout <= 0) return fail(SILT_EINVAL, "invalid argument: closure_pack");
     const int n = 9 * cin * cout;
-    k_pack<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(w, (uint16_t*)w_fwd, (uint16_t*)w_bwd, cin, cout);
+    ::silt::launch_dep(k_pack, dim3((n + 255) / 256), dim3(256), 0, (cudaStream_t)stream, w, (uint16_t*)w_fwd, (uint16_t*)w_bwd, cin, cout);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_pack");
 }

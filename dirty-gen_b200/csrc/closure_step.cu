@@ -45,6 +45,7 @@ constexpr float DONOR_SHARE = 0.25f; // a face moves at most this share of its d
 __device__ __forceinline__ uint16_t bf16_bits(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 
 __global__ void __launch_bounds__(CROP_CELLS) k_features(const FeatureJob* jobs, const float* norm, uint16_t* x) {
+    ::silt::dep_wait();
     const FeatureJob& J = jobs[blockIdx.x];
     const int p = threadIdx.x, cx = p % CROP, cy = p / CROP;
     const int i = J.ci0 + cx, j = J.cj0 + cy;
@@ -101,6 +102,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 
 __global__ void __launch_bounds__(CROP_CELLS) k_apply(const ApplyJob* jobs, const float* y, const float* norm) {
+    ::silt::dep_wait();
     const ApplyJob& J = jobs[blockIdx.x];
     __shared__ float gx[2][CROP_CELLS], gz[2][CROP_CELLS];
     __shared__ double red[CROP_CELLS / 32];
@@ -189,14 +191,14 @@ __global__ void __launch_bounds__(CROP_CELLS) k_apply(const ApplyJob* jobs, cons
 
 cudaError_t launch_features(const FeatureJob* d_jobs, int n, const float* d_norm, uint16_t* x, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    k_features<<<n, CROP_CELLS, 0, st>>>(d_jobs, d_norm, x);
+    ::silt::launch_dep(k_features, dim3(n), dim3(CROP_CELLS), 0, st, d_jobs, d_norm, x);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_apply(const ApplyJob* d_jobs, int n, const float* y, const float* d_norm, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    k_apply<<<n, CROP_CELLS, 0, st>>>(d_jobs, y, d_norm);
+    ::silt::launch_dep(k_apply, dim3(n), dim3(CROP_CELLS), 0, st, d_jobs, y, d_norm);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -146,6 +146,7 @@ static Impl& I(Patches& P) { return *reinterpret_cast<Impl*>(P.impl); }
 // ------------------------------------------------------------------ kernels
 
 __global__ void k_scatter_owner(int8_t* owner, const int* idx, const int8_t* val, int n) {
+    ::silt::dep_wait();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) owner[idx[k]] = val[k];
 }
@@ -193,6 +194,7 @@ __device__ __forceinline__ void refine_cell(const PatchRef& R, int p, int f, int
 
 __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W, const int8_t* owner,
                              int* spray_count) {
+    ::silt::dep_wait();
     const size_t fn = (size_t)fres * fres;
     if (blockIdx.x == 0 && threadIdx.x == 0) *spray_count = 0;  // this step's spray events start here
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < fn * np; k += (size_t)gridDim.x * blockDim.x)
@@ -264,6 +266,7 @@ __device__ void near_apply_col(int q, const PatchRef* refs, int fres, int sub, c
 __global__ void k_lay_finish(SheetView W, const int* held, int n_held, int zero_blocks, const PatchRef* refs,
                              int fres, int sub, const NearCol* cols, int ncol, const int* slot_map, const float* pool,
                              const NearMeta* meta) {
+    ::silt::dep_wait();
     if ((int)blockIdx.x < zero_blocks) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_held; k += zero_blocks * blockDim.x) {
             const size_t c = held[k];
@@ -302,6 +305,7 @@ __device__ void near_fade_slot(int s, NearMeta* meta, int* slot_map, int* free_s
 }
 
 __global__ void k_near_fade(NearMeta* meta, int* slot_map, int* free_stack, int* counters, float dt) {
+    ::silt::dep_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < NEAR_POOL) near_fade_slot(s, meta, slot_map, free_stack, counters, dt);
 }
@@ -348,6 +352,7 @@ __device__ void push_cell(float* w, float* s, float* uw, float* vw, float* us, f
 
 __global__ void k_push_cells(float* w, float* s, float* uw, float* vw, float* us, float* vs, int res, float cell,
                              float ox, float oz, const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh) {
+    ::silt::dep_wait();
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bw * bh; k += gridDim.x * blockDim.x)
         push_cell(w, s, uw, vw, us, vs, res, cell, ox, oz, jobs, njobs, bi0 + k % bw, bj0 + k / bw);
 }
@@ -365,6 +370,7 @@ struct JobGroup {
 __global__ void k_push_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int ngroups, int fres,
                                float fcell, int fade, NearMeta* meta, int* slot_map, int* free_stack, int* counters,
                                float dt) {
+    ::silt::dep_wait();
     if ((int)blockIdx.y == ngroups) {
         if (fade)
             for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < NEAR_POOL; q += gridDim.x * blockDim.x)
@@ -433,6 +439,7 @@ __global__ void k_peel(float* w, const float* uw, const float* vw, int res, floa
                        const PushJob* jobs, int njobs, int bi0, int bj0, int bw, int bh, const int8_t* owner,
                        int coarse_res, float cox, float coz, float coarse_cell, int phase, int patch, SprayRec* out,
                        int* counters, double* books, double* ledger_depth) {
+    ::silt::dep_wait();
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bw * bh; k += gridDim.x * blockDim.x)
         peel_cell(w, uw, vw, res, cell, ox, oz, jobs, njobs, bi0 + k % bw, bj0 + k / bw, owner, coarse_res, cox, coz,
                   coarse_cell, phase, patch, out, counters, books, ledger_depth);
@@ -441,6 +448,7 @@ __global__ void k_peel(float* w, const float* uw, const float* vw, int res, floa
 // The fine peel of every patch in one launch (phase 0: no held-column test, no coarse ledger).
 __global__ void k_peel_patches(const PatchRef* refs, const char* tab, const JobGroup* groups, int fres, float fcell,
                                SprayRec* out, int* counters, double* books) {
+    ::silt::dep_wait();
     const JobGroup G = groups[blockIdx.y];
     const PatchRef& R = refs[G.patch];
     const PushJob* jobs = reinterpret_cast<const PushJob*>(tab + G.job_off);
@@ -699,6 +707,7 @@ __device__ void restrict_column(const PatchRef* refs, int fres, const SheetView&
 __global__ void k_restrict(const PatchRef* refs, int fres, int sub, SheetView W, const RestrictEntry* ents, int nent,
                            const Segment* segs, float fine_area, float coarse_area, const NearCol* cols, int ncap,
                            int* slot_map, float* pool, NearMeta* meta, int* free_stack, int* counters) {
+    ::silt::dep_wait();
     if ((int)blockIdx.x < ncap) {
         near_capture_col(blockIdx.x, refs, fres, sub, cols, ncap, slot_map, pool, meta, free_stack, counters);
         return;
@@ -737,11 +746,13 @@ __device__ void release_cells(const PatchRef* refs, int np, int fres, float fine
 }
 
 __global__ void k_release(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park) {
+    ::silt::dep_wait();
     release_cells(refs, np, fres, fine_area, books, park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
                   (size_t)gridDim.x * blockDim.x);
 }
 
 __global__ void k_init_pool(NearMeta* meta, int* free_stack, int* slot_map, size_t ncells, int* counters) {
+    ::silt::dep_wait();
     size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (k < NEAR_POOL) {
         meta[k].state = 0;
@@ -1269,7 +1280,7 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
     SheetView W = view_of(s);
     const PatchRef* refs = TAB(PatchRef, L.off_refs);
     if (L.n_owner) {
-        k_scatter_owner<<<launch_blocks(L.n_owner), 256, 0, W.st>>>(M.owner, TAB(int, L.off_oidx),
+        ::silt::launch_dep(k_scatter_owner, dim3(launch_blocks(L.n_owner)), dim3(256), 0, W.st, M.owner, TAB(int, L.off_oidx),
                                                                      TAB(int8_t, L.off_oval), L.n_owner);
         ::silt::count_launch();
         FCK(cudaGetLastError());
@@ -1279,7 +1290,7 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
         P.active = 0;
         return SILT_OK;
     }
-    k_refine_lay<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, W, M.owner,
+    ::silt::launch_dep(k_refine_lay, dim3(launch_blocks((size_t)L.np * P.fres * P.fres)), dim3(256), 0, W.st, refs, L.np, P.fres, W, M.owner,
                                                                                  M.counters + 3);
     ::silt::count_launch();
     FCK(cudaGetLastError());
@@ -1291,7 +1302,7 @@ static int lay_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_pu
     const int n_apply = M.near_maybe ? L.n_near : 0;
     if (n_held || n_apply) {
         const int zero_blocks = n_held ? launch_blocks((size_t)n_held, 128) : 0;
-        k_lay_finish<<<zero_blocks + n_apply, 128, 0, W.st>>>(W, TAB(int, L.off_held), n_held, zero_blocks, refs,
+        ::silt::launch_dep(k_lay_finish, dim3(zero_blocks + n_apply), dim3(128), 0, W.st, W, TAB(int, L.off_held), n_held, zero_blocks, refs,
                                                              P.fres, P.sub, TAB(NearCol, L.off_near), n_apply,
                                                              M.slot_map, M.pool, M.meta);
         ::silt::count_launch();
@@ -1312,14 +1323,14 @@ int restrict_all(Patches& P, silt_sheet* s) {
     if (ncap) M.near_maybe = true;
     if (ncap || L.n_ent) {
         const int rblocks = L.n_ent ? launch_blocks((size_t)L.n_ent * 32, 128) : 0;
-        k_restrict<<<ncap + rblocks, 128, 0, W.st>>>(refs, P.fres, P.sub, W, TAB(RestrictEntry, L.off_ent), L.n_ent,
+        ::silt::launch_dep(k_restrict, dim3(ncap + rblocks), dim3(128), 0, W.st, refs, P.fres, P.sub, W, TAB(RestrictEntry, L.off_ent), L.n_ent,
                                                      TAB(Segment, L.off_seg), P.fcell * P.fcell, W.cell * W.cell,
                                                      TAB(NearCol, L.off_near), ncap, M.slot_map, M.pool, M.meta,
                                                      M.free_stack, M.counters);
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    k_release<<<launch_blocks((size_t)L.np * P.fres * P.fres), 256, 0, W.st>>>(refs, L.np, P.fres, P.fcell * P.fcell,
+    ::silt::launch_dep(k_release, dim3(launch_blocks((size_t)L.np * P.fres * P.fres)), dim3(256), 0, W.st, refs, L.np, P.fres, P.fcell * P.fcell,
                                                                               M.d_books, L.any_park ? 1 : 0);
     ::silt::count_launch();
     FCK(cudaGetLastError());
@@ -1332,7 +1343,7 @@ static int fade_only(Patches& P, silt_sheet* s, float dt) {
     Impl& M = I(P);
     if (!M.near_maybe) return SILT_OK;
     SheetView W = view_of(s);
-    k_near_fade<<<(NEAR_POOL + 255) / 256, 256, 0, W.st>>>(M.meta, M.slot_map, M.free_stack, M.counters,
+    ::silt::launch_dep(k_near_fade, dim3((NEAR_POOL + 255) / 256), dim3(256), 0, W.st, M.meta, M.slot_map, M.free_stack, M.counters,
                                                           dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
     ::silt::count_launch();
     FCK(cudaGetLastError());
@@ -1365,7 +1376,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     const int fade = M.near_maybe ? 1 : 0;
     if (L.n_push_groups || fade) {
         dim3 grid(launch_blocks((size_t)std::max(L.push_cells_max, 1)), L.n_push_groups + fade);
-        k_push_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_push_groups), L.n_push_groups, P.fres,
+        ::silt::launch_dep(k_push_patches, dim3(grid), dim3(256), 0, W.st, refs, tab, TAB(JobGroup, L.off_push_groups), L.n_push_groups, P.fres,
                                                P.fcell, fade, M.meta, M.slot_map, M.free_stack, M.counters,
                                                dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
         ::silt::count_launch();
@@ -1374,7 +1385,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     FCK(window::launch_window_step(TAB(window::Job, L.off_jobs), 2 * L.np, P.fres, W.st));
     if (L.n_peel_groups) {
         dim3 grid(launch_blocks((size_t)L.peel_cells_max), L.n_peel_groups);
-        k_peel_patches<<<grid, 256, 0, W.st>>>(refs, tab, TAB(JobGroup, L.off_peel_groups), P.fres, P.fcell, M.spray,
+        ::silt::launch_dep(k_peel_patches, dim3(grid), dim3(256), 0, W.st, refs, tab, TAB(JobGroup, L.off_peel_groups), P.fres, P.fcell, M.spray,
                                                M.counters, M.d_books);
         ::silt::count_launch();
         FCK(cudaGetLastError());
@@ -1382,7 +1393,7 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
     if ((rc = restrict_all(P, s))) return rc;
     if (L.coarse_push.n) {
         const JobList& J = L.coarse_push;
-        k_push_cells<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(W.h[0], W.h[1], W.u[0], W.v[0], W.u[1],
+        ::silt::launch_dep(k_push_cells, dim3(launch_blocks((size_t)J.w * J.h)), dim3(256), 0, W.st, W.h[0], W.h[1], W.u[0], W.v[0], W.u[1],
                                                                          W.v[1], W.res, W.cell, W.origin[0],
                                                                          W.origin[1], TAB(PushJob, J.off), J.n, J.i0,
                                                                          J.j0, J.w, J.h);
@@ -1402,7 +1413,7 @@ int peel_coarse(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps
     const JobList& J = L.coarse_peel;
     if (!J.n) return SILT_OK;
     SheetView W = view_of(s);
-    k_peel<<<launch_blocks((size_t)J.w * J.h), 256, 0, W.st>>>(W.h[0], W.u[0], W.v[0], W.res, W.cell, W.origin[0],
+    ::silt::launch_dep(k_peel, dim3(launch_blocks((size_t)J.w * J.h)), dim3(256), 0, W.st, W.h[0], W.u[0], W.v[0], W.res, W.cell, W.origin[0],
                                                                W.origin[1], TAB(PushJob, J.off), J.n, J.i0, J.j0, J.w,
                                                                J.h, M.owner, W.res, W.origin[0], W.origin[1], W.cell,
                                                                1, 0, M.spray, M.counters, M.d_books, W.d_acc);
@@ -1485,7 +1496,7 @@ int set_near_field(Patches& P, silt_sheet* s, bool on) {
     P.near_on = on;
     if (!on) {
         SheetView W = view_of(s);
-        k_init_pool<<<launch_blocks(std::max<size_t>(W.n, NEAR_POOL)), 256, 0, W.st>>>(M.meta, M.free_stack,
+        ::silt::launch_dep(k_init_pool, dim3(launch_blocks(std::max<size_t>(W.n, NEAR_POOL))), dim3(256), 0, W.st, M.meta, M.free_stack,
                                                                                        M.slot_map, W.n, M.counters);
         ::silt::count_launch();
         FCK(cudaGetLastError());
@@ -1523,7 +1534,7 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     FCK(cudaMemsetAsync(M->d_books, 0, 4 * sizeof(double), st));
     FCK(cudaMallocHost(&M->h_books, 4 * sizeof(double)));
     FCK(cudaMallocHost(&M->h_counters, 8 * sizeof(int)));
-    k_init_pool<<<launch_blocks(std::max<size_t>(n, NEAR_POOL)), 256, 0, st>>>(M->meta, M->free_stack, M->slot_map, n,
+    ::silt::launch_dep(k_init_pool, dim3(launch_blocks(std::max<size_t>(n, NEAR_POOL))), dim3(256), 0, st, M->meta, M->free_stack, M->slot_map, n,
                                                                                M->counters);
     ::silt::count_launch();
     FCK(cudaGetLastError());
@@ -1613,12 +1624,14 @@ struct PeelRec {
 };
 
 __global__ void kb_scatter(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.n_owner; k += gridDim.x * blockDim.x)
         r.owner[r.oidx[k]] = r.oval[k];
 }
 
 __global__ void kb_refine(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     const size_t fn = (size_t)r.fres * r.fres;
     if (blockIdx.x == 0 && threadIdx.x == 0) r.counters[3] = 0;  // this step's spray events start here
@@ -1627,6 +1640,7 @@ __global__ void kb_refine(const FineRec* recs) {
 }
 
 __global__ void kb_lay_finish(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     const int b = (int)blockIdx.x;
     if (b < r.zero_blocks) {
@@ -1645,6 +1659,7 @@ __global__ void kb_lay_finish(const FineRec* recs) {
 }
 
 __global__ void kb_push(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     const int y = (int)blockIdx.y;
     if (y == r.n_push_groups) {
@@ -1663,6 +1678,7 @@ __global__ void kb_push(const FineRec* recs) {
 }
 
 __global__ void kb_peel_patches(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     if ((int)blockIdx.y >= r.n_peel_groups) return;
     const JobGroup G = r.peel_groups[blockIdx.y];
@@ -1674,6 +1690,7 @@ __global__ void kb_peel_patches(const FineRec* recs) {
 }
 
 __global__ void kb_restrict(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     const int b = (int)blockIdx.x;
     if (b < r.ncap) {
@@ -1689,12 +1706,14 @@ __global__ void kb_restrict(const FineRec* recs) {
 }
 
 __global__ void kb_release(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     release_cells(r.refs, r.np, r.fres, r.fcell * r.fcell, r.books, r.park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
                   (size_t)gridDim.x * blockDim.x);
 }
 
 __global__ void kb_coarse_push(const FineRec* recs) {
+    ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
     const SheetView& W = r.W;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.cpush_w * r.cpush_h; k += gridDim.x * blockDim.x)
@@ -1703,6 +1722,7 @@ __global__ void kb_coarse_push(const FineRec* recs) {
 }
 
 __global__ void kb_coarse_peel(const PeelRec* recs) {
+    ::silt::dep_wait();
     const PeelRec& r = recs[blockIdx.z];
     const SheetView& W = r.W;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < r.w * r.h; k += gridDim.x * blockDim.x)
@@ -1872,7 +1892,7 @@ int batch_launch(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std
     const unsigned nz = (unsigned)n;
 #define BLAUNCH(kern, gx, gy, threads)                                           \
     do {                                                                          \
-        kern<<<dim3((unsigned)(gx), (unsigned)(gy), nz), (threads), 0, st>>>(d); \
+        ::silt::launch_dep(kern, dim3(dim3((unsigned)(gx), (unsigned)(gy), nz)), dim3((threads)), 0, st, d); \
         ::silt::count_launch();                                                   \
         FCK(cudaGetLastError());                                                  \
     } while (0)
@@ -1931,7 +1951,7 @@ int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::
     }
     FCK(cudaMemcpyAsync(B->d_peel[slot], B->h_peel[slot], n * sizeof(PeelRec), cudaMemcpyHostToDevice, st));
     FCK(cudaEventRecord(B->peel_ev[slot], st));
-    kb_coarse_peel<<<dim3((unsigned)launch_blocks((size_t)mx), 1, (unsigned)n), 256, 0, st>>>(B->d_peel[slot]);
+    ::silt::launch_dep(kb_coarse_peel, dim3(dim3((unsigned)launch_blocks((size_t)mx), 1, (unsigned)n)), dim3(256), 0, st, B->d_peel[slot]);
     ::silt::count_launch();
     FCK(cudaGetLastError());
     return SILT_OK;

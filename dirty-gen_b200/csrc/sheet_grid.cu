@@ -337,6 +337,7 @@ __device__ __forceinline__ bool force_entry(const LayerParams& P, const TileFlag
 
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(FORCE_THREADS) k_force(ForceLaunch L) {
+    ::silt::dep_wait();
     extern __shared__ float sm[];
     __shared__ LayerParams Ps[2];
     if (threadIdx.x < 2) Ps[threadIdx.x] = force_params(L.lay[threadIdx.x], L.sc, threadIdx.x, blockIdx.x == 0);
@@ -381,6 +382,7 @@ __device__ __forceinline__ int tile_entry(const TileFlags& tf, int cur, int nxt,
 
 __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, int skip1, SubstepCount sc,
                             int* count_next, double* zero_ledger, unsigned int* zero_bits) {
+    ::silt::dep_wait();
     const int nt = tf.tiles_x * tf.tiles_x;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0) {
@@ -403,7 +405,7 @@ cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int
         if (e != cudaSuccess) return e;
     }
     const int n = 2 * tf.tiles_x * tf.tiles_x;
-    k_tile_list<<<(n + 255) / 256, 256, 0, st>>>(tf, cur, nxt, all, skip0, skip1, sc, count_next, zero_ledger,
+    ::silt::launch_dep(k_tile_list, dim3((n + 255) / 256), dim3(256), 0, st, tf, cur, nxt, all, skip0, skip1, sc, count_next, zero_ledger,
                                                  zero_bits);
     ::silt::count_launch();
     return cudaGetLastError();
@@ -627,6 +629,7 @@ __device__ __forceinline__ void transport_entry(const TransportParams& P, const 
 
 // Persistent over the substep's tile list.
 __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
+    ::silt::dep_wait();
     extern __shared__ float sm[];
     __shared__ TransportParams Ps[2];
     if (threadIdx.x < 2) {
@@ -645,6 +648,7 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch
 
 // Materialises the lazy dry cut: u = v = 0 where h < eps.
 __global__ void k_apply_cut(const float* h, float* u, float* v, size_t n, float eps) {
+    ::silt::dep_wait();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         if (h[i] < eps) { u[i] = 0.0f; v[i] = 0.0f; }
 }
@@ -652,6 +656,7 @@ __global__ void k_apply_cut(const float* h, float* u, float* v, size_t n, float 
 // Largest squared speed, for the CFL substep count (src/fluid_core.rs:1723-1744).
 __global__ void k_max_speed2(const float* h, const float* u, const float* v, size_t n, float eps, int apply_cut,
                              unsigned int* out_bits) {
+    ::silt::dep_wait();
     float m = 0.0f;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         float uu = u[i], vv = v[i];
@@ -670,6 +675,7 @@ __global__ void k_max_speed2(const float* h, const float* u, const float* v, siz
 __global__ void __launch_bounds__(256) k_tile_speed2(TileFlags tf, const float* h0, const float* u0, const float* v0,
                                                      const float* h1, const float* u1, const float* v1, int res,
                                                      float eps, int apply_cut, unsigned int* bits) {
+    ::silt::dep_wait();
     const int n = *tf.count;
     const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
@@ -706,7 +712,7 @@ __global__ void __launch_bounds__(256) k_tile_speed2(TileFlags tf, const float* 
 cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], const float* const u[2],
                                const float* const v[2], int res, float eps, int apply_cut, unsigned int* bits,
                                cudaStream_t st) {
-    k_tile_speed2<<<148 * 8, 256, 0, st>>>(tf, h[0], u[0], v[0], h[1], u[1], v[1], res, eps, apply_cut, bits);
+    ::silt::launch_dep(k_tile_speed2, dim3(148 * 8), dim3(256), 0, st, tf, h[0], u[0], v[0], h[1], u[1], v[1], res, eps, apply_cut, bits);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -714,6 +720,7 @@ cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], con
 // ------------------------------------------------------------ batched windows
 
 __global__ void k_batch_tile_list(const WindowSubstep* ws, int* list, int* entry_win, int* count, int* count_next) {
+    ::silt::dep_wait();
     const int w = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (w == 0 && k == 0) *count_next = 0;
@@ -737,6 +744,7 @@ __global__ void k_batch_tile_list(const WindowSubstep* ws, int* list, int* entry
 
 __global__ void __launch_bounds__(256) k_batch_speed2(const WindowSubstep* ws, const int* list, const int* entry_win,
                                                       const int* count) {
+    ::silt::dep_wait();
     const int n = *count;
     const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
@@ -773,6 +781,7 @@ __global__ void __launch_bounds__(256) k_batch_speed2(const WindowSubstep* ws, c
 
 __global__ void __launch_bounds__(FORCE_THREADS) k_batch_force(const WindowSubstep* ws, const int* list,
                                                                const int* entry_win, const int* count) {
+    ::silt::dep_wait();
     extern __shared__ float sm[];
     __shared__ LayerParams Ps;
     __shared__ TileFlags Tf;
@@ -794,6 +803,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_batch_force(const WindowSubst
 
 __global__ void __launch_bounds__(TRANSPORT_THREADS) k_batch_transport(const WindowSubstep* ws, const int* list,
                                                                        const int* entry_win, const int* count) {
+    ::silt::dep_wait();
     extern __shared__ float sm[];
     __shared__ TransportParams Ps;
     __shared__ TileFlags Tf;
@@ -820,14 +830,14 @@ cudaError_t launch_batch_tile_list(const WindowSubstep* d_ws, int nwin, int max_
                                    int* count, int* count_next, cudaStream_t st) {
     if (nwin <= 0) return cudaSuccess;
     dim3 grid((2 * max_tiles + 255) / 256, nwin);
-    k_batch_tile_list<<<grid, 256, 0, st>>>(d_ws, list, entry_win, count, count_next);
+    ::silt::launch_dep(k_batch_tile_list, dim3(grid), dim3(256), 0, st, d_ws, list, entry_win, count, count_next);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
                                 cudaStream_t st) {
-    k_batch_speed2<<<148 * 8, 256, 0, st>>>(d_ws, list, entry_win, count);
+    ::silt::launch_dep(k_batch_speed2, dim3(148 * 8), dim3(256), 0, st, d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -836,7 +846,7 @@ cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const
                                cudaStream_t st) {
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
-    k_batch_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(d_ws, list, entry_win, count);
+    ::silt::launch_dep(k_batch_force, dim3(148 * 2), dim3(FORCE_THREADS), force_smem_bytes(), st, d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -845,7 +855,7 @@ cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, c
                                    const int* count, cudaStream_t st) {
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
-    k_batch_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(d_ws, list, entry_win, count);
+    ::silt::launch_dep(k_batch_transport, dim3(148 * 4), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -855,7 +865,7 @@ cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t
     std::call_once(attr, [] { cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
     (void)res;
     (void)layers;
-    k_force<<<148 * 2, FORCE_THREADS, force_smem_bytes(), st>>>(L);
+    ::silt::launch_dep(k_force, dim3(148 * 2), dim3(FORCE_THREADS), force_smem_bytes(), st, L);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -865,12 +875,13 @@ cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cuda
     std::call_once(attr, [] { cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
     (void)res;
     (void)layers;
-    k_transport<<<148 * 4, TRANSPORT_THREADS, transport_smem_bytes(), st>>>(L);
+    ::silt::launch_dep(k_transport, dim3(148 * 4), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, L);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 
 __global__ void k_material(const uint8_t* grain, const float* moisture, float* nu, float* mob, float* damp, size_t n) {
+    ::silt::dep_wait();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float x = dynamic_viscosity(grain[i], moisture[i]);
         nu[i] = x;
@@ -883,7 +894,7 @@ cudaError_t launch_material(const uint8_t* grain, const float* moisture, float* 
                             cudaStream_t st) {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_material<<<blocks, 256, 0, st>>>(grain, moisture, nu, mob, damp, n);
+    ::silt::launch_dep(k_material, dim3(blocks), dim3(256), 0, st, grain, moisture, nu, mob, damp, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -891,7 +902,7 @@ cudaError_t launch_material(const uint8_t* grain, const float* moisture, float* 
 cudaError_t launch_apply_cut(const float* h, float* u, float* v, size_t n, float eps, cudaStream_t st) {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_apply_cut<<<blocks, 256, 0, st>>>(h, u, v, n, eps);
+    ::silt::launch_dep(k_apply_cut, dim3(blocks), dim3(256), 0, st, h, u, v, n, eps);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -900,7 +911,7 @@ cudaError_t launch_max_speed2(const float* h, const float* u, const float* v, si
                               unsigned int* out_bits, cudaStream_t st) {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
-    k_max_speed2<<<blocks, 256, 0, st>>>(h, u, v, n, eps, apply_cut, out_bits);
+    ::silt::launch_dep(k_max_speed2, dim3(blocks), dim3(256), 0, st, h, u, v, n, eps, apply_cut, out_bits);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -20,6 +20,7 @@ static int blocks_for(size_t n) {
 // src/fluid_core.rs:5329-5356 map_water_bed, per cell.
 __global__ void k_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
                                 uint8_t* grain, size_t n) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         float b = bed_in[i];
         bed[i] = finite_f(b) ? b : 0.0f;
@@ -36,6 +37,7 @@ __global__ void k_map_water_bed(const float* bed_in, const float* water_in, floa
 // src/fluid_core.rs:5358-5372 map_water_velocity.
 __global__ void k_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
                                      size_t n) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         if (water[i] <= 1.0e-6f) continue;
         float u = u_in[i], v = v_in[i];
@@ -47,6 +49,7 @@ __global__ void k_map_water_velocity(const float* u_in, const float* v_in, const
 // src/fluid_core.rs:5820-5849 paint (pour_water / pour_slurry).
 __global__ void k_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
                         float x0, float x1, float z0, float z1, float depth, int water, int g, float m) {
+    ::silt::dep_wait();
     size_t n = (size_t)res * res;
     GRID_STRIDE(k, n) {
         int i = (int)(k % res), j = (int)(k / res);
@@ -64,6 +67,7 @@ __global__ void k_paint(float* depth_plane, float* moisture, uint8_t* grain, int
 // src/fluid_core.rs:5854-5877 lay_slurry_mask.
 __global__ void k_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g,
                              float m) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         float d = depth[i];
         if (!(finite_f(d) && d > 0.0f)) continue;
@@ -76,6 +80,7 @@ __global__ void k_lay_slurry(const float* depth, float* slurry, float* moisture,
 // src/fluid_core.rs:5928-5950 read_substrate_grid, per cell.
 __global__ void k_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
                                  float* moisture, uint8_t* grain, const float* slurry, size_t n) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         bed[i] = bed_in[i];
         moisture[i] = rclamp(moist_in[i], 0.0f, 1.0f);
@@ -87,6 +92,7 @@ __global__ void k_read_substrate(const float* bed_in, const float* moist_in, con
 // for the previous dry cut gets it first, so the water lands at rest.
 __global__ void k_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1,
                          float add, int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh) {
+    ::silt::dep_wait();
     int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= i1) return;
     size_t c = (size_t)j * res + i;
@@ -107,6 +113,7 @@ __global__ void k_inflow(float* water, float* uw, float* vw, int cut_pending, in
 // (src/render_contract.rs:457-496). Tracers are off the sheet path: turbidity 0.
 __global__ void k_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
                           const float* vs, float* film, float* flow, size_t n) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         float water_m = finite0(water[i]), slurry_m = finite0(slurry[i]);
         float fl = water_m + slurry_m;
@@ -127,6 +134,7 @@ __global__ void k_publish(const float* water, const float* slurry, const float* 
 __global__ void k_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
                          const float* us, const float* vs, const float* moist, float* height, float* vel_u,
                          float* vel_v, float* moisture, size_t n) {
+    ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         if (height) height[i] = bed[i] + water[i] + slurry[i];
         float hw = finite0(water[i]), hs = finite0(slurry[i]);
@@ -144,6 +152,7 @@ __global__ void k_export(const float* bed, const float* water, const float* slur
 
 // FP64 sums of max(h, 0) for two planes (the ledger's column_sum, src/fluid_core.rs:4617).
 __global__ void k_sum2(const float* a, const float* b, size_t n, double* out) {
+    ::silt::dep_wait();
     double sa = 0.0, sb = 0.0;
     GRID_STRIDE(i, n) {
         sa += (double)fmaxf(a[i], 0.0f);
@@ -160,6 +169,7 @@ __global__ void k_sum2(const float* a, const float* b, size_t n, double* out) {
 }
 
 __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsigned int* out) {
+    ::silt::dep_wait();
     unsigned int c = 0;
     GRID_STRIDE(i, n) {
         for (int p = 0; p < np; ++p) c += !finite_f(planes[p][i]);
@@ -170,53 +180,53 @@ __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsig
 
 cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
                              uint8_t* grain, size_t n, cudaStream_t st) {
-    k_map_water_bed<<<blocks_for(n), 256, 0, st>>>(bed_in, water_in, bed, water, moisture, grain, n);
+    ::silt::launch_dep(k_map_water_bed, dim3(blocks_for(n)), dim3(256), 0, st, bed_in, water_in, bed, water, moisture, grain, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_map_water_velocity(const float* u_in, const float* v_in, const float* water, float* uw, float* vw,
                                   size_t n, cudaStream_t st) {
-    k_map_water_velocity<<<blocks_for(n), 256, 0, st>>>(u_in, v_in, water, uw, vw, n);
+    ::silt::launch_dep(k_map_water_velocity, dim3(blocks_for(n)), dim3(256), 0, st, u_in, v_in, water, uw, vw, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
                      float x0, float x1, float z0, float z1, float depth, int water, int g, float m, cudaStream_t st) {
-    k_paint<<<blocks_for((size_t)res * res), 256, 0, st>>>(depth_plane, moisture, grain, res, cell, ox, oz, x0, x1, z0,
+    ::silt::launch_dep(k_paint, dim3(blocks_for((size_t)res * res)), dim3(256), 0, st, depth_plane, moisture, grain, res, cell, ox, oz, x0, x1, z0,
                                                            z1, depth, water, g, m);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
                           cudaStream_t st) {
-    k_lay_slurry<<<blocks_for(n), 256, 0, st>>>(depth, slurry, moisture, grain, n, g, m);
+    ::silt::launch_dep(k_lay_slurry, dim3(blocks_for(n)), dim3(256), 0, st, depth, slurry, moisture, grain, n, g, m);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
                               float* moisture, uint8_t* grain, const float* slurry, size_t n, cudaStream_t st) {
-    k_read_substrate<<<blocks_for(n), 256, 0, st>>>(bed_in, moist_in, grain_in, bed, moisture, grain, slurry, n);
+    ::silt::launch_dep(k_read_substrate, dim3(blocks_for(n)), dim3(256), 0, st, bed_in, moist_in, grain_in, bed, moisture, grain, slurry, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
                       int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh, cudaStream_t st) {
     if (i1 <= i0) return cudaSuccess;
-    k_inflow<<<(i1 - i0 + 127) / 128, 128, 0, st>>>(water, uw, vw, cut_pending, res, j, i0, i1, add, tiles_x, t_wet,
+    ::silt::launch_dep(k_inflow, dim3((i1 - i0 + 127) / 128), dim3(128), 0, st, water, uw, vw, cut_pending, res, j, i0, i1, add, tiles_x, t_wet,
                                                      t_zuv, t_zh);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
                        const float* vs, float* film, float* flow, size_t n, cudaStream_t st) {
-    k_publish<<<blocks_for(n), 256, 0, st>>>(water, slurry, uw, vw, us, vs, film, flow, n);
+    ::silt::launch_dep(k_publish, dim3(blocks_for(n)), dim3(256), 0, st, water, slurry, uw, vw, us, vs, film, flow, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
                       const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
                       float* moisture, size_t n, cudaStream_t st) {
-    k_export<<<blocks_for(n), 256, 0, st>>>(bed, water, slurry, uw, vw, us, vs, moist, height, vel_u, vel_v, moisture,
+    ::silt::launch_dep(k_export, dim3(blocks_for(n)), dim3(256), 0, st, bed, water, slurry, uw, vw, us, vs, moist, height, vel_u, vel_v, moisture,
                                            n);
     ::silt::count_launch();
     return cudaGetLastError();
@@ -224,11 +234,12 @@ cudaError_t op_export(const float* bed, const float* water, const float* slurry,
 cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
     if (e != cudaSuccess) return e;
-    k_sum2<<<blocks_for(n), 256, 0, st>>>(a, b, n, out);
+    ::silt::launch_dep(k_sum2, dim3(blocks_for(n)), dim3(256), 0, st, a, b, n, out);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 __global__ void k_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out) {
+    ::silt::dep_wait();
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n) return;
     out[6 * w + 0] = acc[w][0];
@@ -241,14 +252,14 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    k_gather_ledgers<<<(n + 127) / 128, 128, 0, st>>>(acc, books, n, out);
+    ::silt::launch_dep(k_gather_ledgers, dim3((n + 127) / 128), dim3(128), 0, st, acc, books, n, out);
     ::silt::count_launch();
     return cudaGetLastError();
 }
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
-    k_non_finite<<<blocks_for(n), 256, 0, st>>>(planes, np, n, out);
+    ::silt::launch_dep(k_non_finite, dim3(blocks_for(n)), dim3(256), 0, st, planes, np, n, out);
     ::silt::count_launch();
     return cudaGetLastError();
 }

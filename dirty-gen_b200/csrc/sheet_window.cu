@@ -1018,11 +1018,13 @@ __device__ __forceinline__ void window_job(Job* jp) {
 
 // Job k of an array.
 __global__ void __launch_bounds__(NT, 1) k_window_step(Job* jobs) {
+    ::silt::dep_wait();
     window_job(jobs + blockIdx.x / (unsigned)crew_size());
 }
 
 // Job k of a list of jobs that live in different tables (batched windows).
 __global__ void __launch_bounds__(NT, 1) k_window_step_list(Job* const* jobs) {
+    ::silt::dep_wait();
     window_job(jobs[blockIdx.x / (unsigned)crew_size()]);
 }
 
@@ -1077,13 +1079,15 @@ cudaError_t launch_window_step_list(Job* const* d_job_list, int njobs, int max_r
     cfg.gridDim = dim3((unsigned)(njobs * crew), 1, 1);
     cfg.blockDim = dim3(NT, 1, 1);
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)crew;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with dep_wait()
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step_list, d_job_list);
     ::silt::count_launch();
     if (e != cudaSuccess) return e;
@@ -1098,13 +1102,15 @@ cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaSt
     cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)crew;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with dep_wait()
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step, const_cast<Job*>(d_jobs));
     ::silt::count_launch();
     if (e != cudaSuccess) return e;
