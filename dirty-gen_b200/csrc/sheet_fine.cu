@@ -1197,7 +1197,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
     // job per patch and layer.
     {
         std::vector<window::Job> jobs;
-        const float nu_w = host::dynamic_viscosity(3, 1.0f);
+        const float nu_w = P.open_mobility >= 0.0f ? -std::fmax(P.open_mobility, 1.0e-4f) : host::dynamic_viscosity(3, 1.0f);
         const size_t fn = (size_t)fres * fres;
         for (int p = 0; p < L.np; ++p) {
             PatchState* S = P.patches[p];

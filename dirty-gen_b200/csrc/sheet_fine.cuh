@@ -61,6 +61,7 @@ struct Patches {
     bool near_on = true;
     bool patches_off = false;  // lay no patch this step: every tire shoves the coarse cells (closure coupling)
     bool coarse_shove_off = false;  // and not even that: the learned closure carries the tires' effect
+    float open_mobility = -1.0f;    // >= 0: open-water mode, the water row's mobility (src/fluid_core.rs:8015-8017)
     bool fine_on = false;
     int active = 0;
     std::vector<PatchState*> patches;

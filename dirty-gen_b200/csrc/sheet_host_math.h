@@ -11,6 +11,7 @@ namespace host {
 
 constexpr float kFineCell = 0.02f;
 constexpr float kSpeedCap = 1.6f;
+constexpr float kGravityHost = 9.81f;  // GRAVITY, src/fluid_core.rs:111
 
 inline float rclamp(float x, float lo, float hi) {
     if (x < lo) x = lo;

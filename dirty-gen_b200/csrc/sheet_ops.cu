@@ -178,6 +178,123 @@ __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsig
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
+// src/fluid_core.rs:7521-7581 eddy_shear, the snapshot pass: neighbours in
+// the order (-1, 0), (1, 0), (0, -1), (0, 1); a wet neighbour (over 3 mm)
+// gives its velocity, dry ground standing 3 cm above the surface gives 0 (no
+// slip), a dry beach is skipped, the window edge too.
+__global__ void k_eddy(const float* h, const float* u, const float* v, const float* bed, int res, float k, float* du,
+                       float* dv) {
+    ::silt::dep_wait();
+    const size_t n = (size_t)res * res;
+    GRID_STRIDE(idx, n) {
+        const int i = (int)(idx % res), j = (int)(idx / res);
+        float a = 0.0f, b = 0.0f;
+        const float h0 = h[idx];
+        if (h0 > 0.003f) {
+            const float u0 = u[idx], v0 = v[idx];
+            float lu = 0.0f, lv = 0.0f;
+            const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int ni = i + di[q], nj = j + dj[q];
+                if (ni < 0 || nj < 0 || ni >= res || nj >= res) continue;
+                const size_t nidx = (size_t)nj * res + ni;
+                float un, vn;
+                if (h[nidx] > 0.003f) {
+                    un = u[nidx];
+                    vn = v[nidx];
+                } else if (bed[nidx] > bed[idx] + h0 + 0.03f) {
+                    un = 0.0f;
+                    vn = 0.0f;
+                } else {
+                    continue;
+                }
+                lu += un - u0;
+                lv += vn - v0;
+            }
+            a = k * lu;
+            b = k * lv;
+        }
+        du[idx] = a;
+        dv[idx] = b;
+    }
+}
+
+// The eddy change applied (src/fluid_core.rs:7570-7580), then Manning bed
+// friction (:7485-7512): keep = 1 / (1 + dt g n^2 |u| / max(h, 2 mm)^(4/3)).
+__global__ void k_friction(const float* h, float* u, float* v, const float* du, const float* dv, size_t n, float gn2,
+                           float dt) {
+    ::silt::dep_wait();
+    GRID_STRIDE(idx, n) {
+        float uu = u[idx], vv = v[idx];
+        const float a = du[idx], b = dv[idx];
+        if (a != 0.0f || b != 0.0f) {
+            const float nu = uu + a, nv = vv + b;
+            if (isfinite(nu) && isfinite(nv)) {
+                uu = nu;
+                vv = nv;
+            }
+        }
+        if (gn2 > 0.0f) {
+            const float hv = h[idx];
+            if (hv > 1.0e-4f) {
+                const float speed = hypotf(uu, vv);
+                if (speed > 0.0f) {
+                    const float kk = gn2 * speed / powf(fmaxf(hv, 0.002f), 4.0f / 3.0f);
+                    const float keep = 1.0f / (1.0f + dt * kk);
+                    uu = uu * keep;
+                    vv = vv * keep;
+                }
+            }
+        }
+        u[idx] = uu;
+        v[idx] = vv;
+    }
+}
+
+// src/fluid_core.rs:7584-7636 diffuse_surface. The transfer across the face
+// from cell a to its east or north neighbour b, both wet, is k (eta_a -
+// eta_b) limited to a quarter of the donor. Each cell gathers its four faces
+// in the order the reference's raster sweep adds them to it: from the cell
+// below, from the cell to the west, then its own east and north faces.
+__device__ __forceinline__ float surface_flux(const float* h, const float* bed, size_t a, size_t b, float k) {
+    const float ha = h[a], hb = h[b];
+    if (!(ha > 0.003f) || !(hb > 0.003f)) return 0.0f;
+    float f = k * ((bed[a] + ha) - (bed[b] + hb));
+    if (f > 0.0f) f = fminf(f, 0.25f * ha);
+    else f = fmaxf(f, -0.25f * hb);
+    return f;
+}
+
+__global__ void k_diffuse(const float* h, const float* bed, int res, float k, float* delta) {
+    ::silt::dep_wait();
+    const size_t n = (size_t)res * res;
+    GRID_STRIDE(idx, n) {
+        const int i = (int)(idx % res), j = (int)(idx / res);
+        float d = 0.0f;
+        if (j > 0) d += surface_flux(h, bed, idx - res, idx, k);
+        if (i > 0) d += surface_flux(h, bed, idx - 1, idx, k);
+        if (i + 1 < res) d -= surface_flux(h, bed, idx, idx + 1, k);
+        if (j + 1 < res) d -= surface_flux(h, bed, idx, idx + res, k);
+        delta[idx] = d;
+    }
+}
+
+__global__ void k_diffuse_apply(float* h, const float* delta, size_t n, double* ledger) {
+    ::silt::dep_wait();
+    double part = 0.0;
+    GRID_STRIDE(idx, n) {
+        const float d = delta[idx];
+        if (d != 0.0f && isfinite(d)) {
+            const float h0 = h[idx], h1 = fmaxf(h0 + d, 0.0f);
+            h[idx] = h1;
+            part += (double)h1 - (double)h0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0 && part != 0.0 && ledger) atomicAdd(ledger, part);
+}
+
 cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
                              uint8_t* grain, size_t n, cudaStream_t st) {
     ::silt::launch_dep(k_map_water_bed, dim3(blocks_for(n)), dim3(256), 0, st, bed_in, water_in, bed, water, moisture, grain, n);
@@ -253,6 +370,37 @@ cudaError_t op_gather_ledgers(const double* const* acc, const double* const* boo
                               cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     ::silt::launch_dep(k_gather_ledgers, dim3((n + 127) / 128), dim3(128), 0, st, acc, books, n, out);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+cudaError_t op_open_water(const float* h, float* u, float* v, const float* bed, int res, float k_visc, float gn2,
+                          float dt, float* scratch, cudaStream_t st) {
+    const size_t n = (size_t)res * res;
+    float* du = scratch;
+    float* dv = scratch + n;
+    if (k_visc > 0.0f) {
+        ::silt::launch_dep(k_eddy, dim3(blocks_for(n)), dim3(256), 0, st, h, (const float*)u, (const float*)v, bed,
+                           res, k_visc, du, dv);
+        ::silt::count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    } else {
+        cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * n * sizeof(float), st);
+        if (e != cudaSuccess) return e;
+    }
+    ::silt::launch_dep(k_friction, dim3(blocks_for(n)), dim3(256), 0, st, h, u, v, (const float*)du,
+                       (const float*)dv, n, gn2, dt);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+cudaError_t op_diffuse_surface(float* h, const float* bed, int res, float k, float* scratch, double* ledger,
+                               cudaStream_t st) {
+    const size_t n = (size_t)res * res;
+    ::silt::launch_dep(k_diffuse, dim3(blocks_for(n)), dim3(256), 0, st, (const float*)h, bed, res, k, scratch);
+    ::silt::count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ::silt::launch_dep(k_diffuse_apply, dim3(blocks_for(n)), dim3(256), 0, st, h, (const float*)scratch, n, ledger);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -24,9 +24,20 @@ cudaError_t op_export(const float* bed, const float* water, const float* slurry,
                       const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
                       float* moisture, size_t n, cudaStream_t st);
 cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st);
-// out[5 w + 0..1] = acc[w][0..1] (depth sums), out[5 w + 2..4] = books[w][0..2].
+// out[6 w + 0..1] = acc[w][0..1] (depth sums), out[6 w + 2..5] = books[w][0..3].
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st);
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st);
+
+// Open-water drivers of the coarse water sheet (src/fluid_core.rs:7482-7636).
+// eddy: the velocity change of one explicit Laplacian from a snapshot into
+// du, dv (k = min(nu_t dt / cell^2, 0.2)). friction: adds du, dv, then (gn2 >
+// 0) Manning friction, implicit. diffuse: surface-slope transfers between wet
+// neighbours from a snapshot into delta; diffuse_apply adds them and the
+// exact depth change to ledger[0]. scratch: 2 res^2 floats.
+cudaError_t op_open_water(const float* h, float* u, float* v, const float* bed, int res, float k_visc, float gn2,
+                          float dt, float* scratch, cudaStream_t st);
+cudaError_t op_diffuse_surface(float* h, const float* bed, int res, float k, float* scratch, double* ledger,
+                               cudaStream_t st);
 
 }  // namespace silt

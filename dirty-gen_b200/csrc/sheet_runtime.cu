@@ -115,6 +115,13 @@ struct silt_sheet {
     unsigned long long tile_seq = 0;
     bool tiles_all = true;     // next substep steps every tile (after any outside write)
 
+    // Open-water mode of the water sheet (FluidCore::set_open_water,
+    // src/fluid_core.rs:5293-5303) and the surface diffusion (:5284-5286).
+    bool open_water = false;
+    float ow_mobility = 0.0f, ow_manning = 0.0f, ow_eddy = 0.0f;
+    float surface_diffusion = 0.0f;
+    float* ow_scratch = nullptr;   // 2 n floats for the drivers' snapshots
+    bool turbidity = false;        // FluidCore::set_turbidity_enabled (tracers are off this path)
     // Tire coupling (silt_set_coupling): nested sheets, none, or the learned closure.
     int coupling = SILT_COUPLING_NESTED;
     silt_closure* net = nullptr;
@@ -131,6 +138,12 @@ struct silt_sheet {
 namespace {
 
 float water_nu() { return silt::host::dynamic_viscosity(3, 1.0f); }
+
+// The water row's viscosity entry: in open-water mode a negative entry, the
+// mobility itself (src/fluid_core.rs:8015-8017, sheet_mobility_for :169-172).
+float water_nu(const silt_sheet* s) {
+    return s->open_water ? -std::fmax(s->ow_mobility, 1.0e-4f) : water_nu();
+}
 
 // After a write from outside the step (seeding, plane writes) every tile may
 // hold water and no buffer is known to be zero.
@@ -193,7 +206,7 @@ void coarse_plan(silt_sheet* s, float dt, CoarsePlan& cp) {
     cp.sc.dt = dt;
     cp.sc.cell = cell;
     cp.sc.cap = cap;
-    cp.nu_w = water_nu();
+    cp.nu_w = water_nu(s);
     for (int q = 1; q <= 8; ++q) cp.sc.water_decay[q] = expf(-silt::host::sheet_damp(cp.nu_w) * (dt / (float)q));
     cp.sc.water_decay[0] = cp.sc.water_decay[1];
     if (!(dt * std::max(0.15f, bound) <= courant_len)) {
@@ -347,7 +360,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
     s->win_flip ^= 1;
     CK(cudaEventSynchronize(s->win_ev[slot]));
     silt::window::Job* jobs = s->h_win_jobs + 2 * slot;
-    const float nu_w = water_nu();
+    const float nu_w = water_nu(s);
     for (int l = 0; l < 2; ++l) {
         silt::window::Job& J = jobs[l];
         memset(&J, 0, sizeof J);
@@ -559,6 +572,7 @@ int silt_sheet_destroy(silt_sheet* s) {
         s->clos->release();
         delete s->clos;
     }
+    cudaFree(s->ow_scratch);
     silt::fine::destroy(s->fine);
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
@@ -803,6 +817,26 @@ int step_inflow(silt_sheet* s, float dt) {
     return SILT_OK;
 }
 
+// Open-water drivers after the coarse pair (src/fluid_core.rs:6073-6074):
+// bed_friction (eddy shear, then Manning) in open-water mode, then the
+// surface diffusion when it is set.
+int open_water_step(silt_sheet* s, float dt) {
+    if (!s->open_water && !(s->surface_diffusion > 0.0f)) return SILT_OK;
+    if (!s->ow_scratch) CK(cudaMalloc(&s->ow_scratch, 2 * s->n * sizeof(float)));
+    const float cell = s->cfg.cell;
+    if (s->open_water) {
+        const float k = s->ow_eddy > 0.0f ? std::fmin(s->ow_eddy * dt / (cell * cell), 0.2f) : 0.0f;
+        const float gn2 = s->ow_manning > 0.0f ? silt::host::kGravityHost * s->ow_manning * s->ow_manning : 0.0f;
+        if (k > 0.0f || gn2 > 0.0f)
+            CK(silt::op_open_water(s->H(0), s->U(0), s->V(0), s->bed, s->res, k, gn2, dt, s->ow_scratch, s->st));
+    }
+    if (s->surface_diffusion > 0.0f) {
+        const float k = std::fmin(s->surface_diffusion * dt / (cell * cell), 0.12f);
+        CK(silt::op_diffuse_surface(s->H(0), s->bed, s->res, k, s->ow_scratch, s->d_acc, s->st));
+    }
+    return SILT_OK;
+}
+
 // The coupling of this step's tires: sets whether the nested patches are laid
 // and returns true when the learned closure corrects the step.
 bool closure_begin(silt_sheet* s) {
@@ -884,6 +918,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     const clock::time_point t2 = clock::now();
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
     if (rc) return rc;
+    if ((rc = open_water_step(s, dt))) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
     if (net_on && (rc = closure_correct(s, F))) return rc;
@@ -901,6 +936,59 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         s->parts.host_fine_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
     }
     s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
+    return SILT_OK;
+}
+
+int silt_set_open_water(silt_sheet* s, int32_t on, float mobility, float manning_n, float eddy_m2_s) {
+    if (!s) return fail_arg("handle");
+    s->open_water = on != 0 && std::isfinite(mobility) && std::isfinite(manning_n) && std::isfinite(eddy_m2_s);
+    if (s->open_water) {
+        s->ow_mobility = std::fmin(std::fmax(mobility, 0.0f), 1.0f);
+        s->ow_manning = std::fmax(manning_n, 0.0f);
+        s->ow_eddy = std::fmax(eddy_m2_s, 0.0f);
+    }
+    s->fine.open_mobility = s->open_water ? s->ow_mobility : -1.0f;
+    return SILT_OK;
+}
+
+int silt_set_surface_diffusion(silt_sheet* s, float m2_s) {
+    if (!s) return fail_arg("handle");
+    s->surface_diffusion = std::isfinite(m2_s) ? std::fmax(m2_s, 0.0f) : 0.0f;
+    return SILT_OK;
+}
+
+int silt_set_turbidity_enabled(silt_sheet* s, int32_t on) {
+    if (!s) return fail_arg("handle");
+    s->turbidity = on != 0;
+    return SILT_OK;
+}
+
+int silt_sample(silt_sheet* s, float x, float z, silt_ground_sample* out) {
+    if (!s || !out) return fail_arg("sample");
+    memset(out, 0, sizeof *out);
+    auto axis = [&](float o, float p) -> long {  // coarse_axis, src/fluid_core.rs:9546-9557
+        const float i = std::floor((p - o) / s->cfg.cell);
+        if (i < 0.0f) return -1;
+        const double ii = std::isnan(i) ? 0.0 : (double)i;
+        return ii >= (double)s->res ? -1 : (long)ii;
+    };
+    const long i = axis(s->origin[0], x), j = axis(s->origin[1], z);
+    if (i < 0 || j < 0) return SILT_OK_NOOP;  // outside the window: nothing parked per cell here
+    int rc = flush_cut(s);
+    if (rc) return rc;
+    const size_t c = (size_t)j * s->res + (size_t)i;
+    float vals[6];
+    const float* src[6] = {s->H(0) + c, s->H(1) + c, s->U(1) + c, s->V(1) + c, s->moisture + c, s->bed + c};
+    for (int k = 0; k < 6; ++k)
+        CK(cudaMemcpyAsync(vals + k, src[k], sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    out->water_m = vals[0];
+    out->slurry_m = vals[1];
+    out->u = vals[2];
+    out->v = vals[3];
+    out->settled_dust_m = 0.0f;
+    out->moisture = vals[4];
+    out->bed_m = vals[5];
     return SILT_OK;
 }
 
@@ -1625,6 +1713,8 @@ int silt_batch_step(silt_batch* b, float dt) {
     if ((rc = silt::fine::batch_launch(b->fine, fs, fp, dt, b->st))) return rc;
     const clock::time_point t1 = clock::now();
     if ((rc = batch_coarse(b, dt))) return rc;
+    for (silt_sheet* s : b->sheets)
+        if ((rc = open_water_step(s, dt))) return rc;
     if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
     if (!net_win.empty()) {
         std::vector<silt::closure::ApplyJob> A(net_win.size());

@@ -45,6 +45,10 @@ class Ledger(ctypes.Structure):
                                                "spray_m3", "opened_m3", "total_m3", "cut_m3")]
 
 
+class GroundSample(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("water_m", "slurry_m", "u", "v", "settled_dust_m", "moisture", "bed_m")]
+
+
 class CoarseCell(ctypes.Structure):
     _fields_ = [(k, _f) for k in ("x", "z", "bed_m", "water_m", "slurry_m", "moisture", "u", "v")]
 
@@ -112,6 +116,8 @@ def lib():
             "silt_batch_push_tires": [_p, _p, ctypes.POINTER(TirePush), _i],
             "silt_batch_set_timing": [_p, _i], "silt_batch_get_parts": [_p, ctypes.POINTER(StepParts)],
             "silt_plane_device": [_p, _i, ctypes.POINTER(_p)], "silt_sheet_copy_state": [_p, _p],
+            "silt_set_open_water": [_p, _i, _f, _f, _f], "silt_set_surface_diffusion": [_p, _f],
+            "silt_set_turbidity_enabled": [_p, _i], "silt_sample": [_p, _f, _f, ctypes.POINTER(GroundSample)],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -265,6 +271,22 @@ class Sheet:
 
     def copy_state_from(self, other):
         check(lib().silt_sheet_copy_state(self.h, other.h), "copy_state")
+
+    def set_open_water(self, on, mobility=0.0, manning_n=0.0, eddy_m2_s=0.0):
+        """FluidCore::set_open_water (on=False is None)."""
+        check(lib().silt_set_open_water(self.h, int(on), mobility, manning_n, eddy_m2_s), "set_open_water")
+
+    def set_surface_diffusion(self, m2_s):
+        check(lib().silt_set_surface_diffusion(self.h, m2_s), "set_surface_diffusion")
+
+    def set_turbidity_enabled(self, on):
+        check(lib().silt_set_turbidity_enabled(self.h, int(on)), "set_turbidity_enabled")
+
+    def sample(self, x, z):
+        """FluidCore::sample between steps: the coarse cell under (x, z), None outside."""
+        g = GroundSample()
+        rc = check(lib().silt_sample(self.h, x, z, ctypes.byref(g)), "sample")
+        return None if rc == SILT_OK_NOOP else {k: getattr(g, k) for k, _ in GroundSample._fields_}
 
     def export_maps(self):
         n = self.res * self.res

@@ -135,6 +135,31 @@ def grid(res=2048, cell=0.2, seed=0x9E3779B9, puddles=8, center=(0.0, 0.0)):
                 moisture=np.full(res * res, 0.55, F), grain=np.full(res * res, CLAY, np.uint8))
 
 
+def basin(res=200, cell=0.2, level=0.3, speed=0.75, seed=0x9E3779B9, center=(0.0, 0.0)):
+    """Open water: a flat sand floor in a 12 m square with 0.6 banks, a little
+    bed noise, water to `level`, and a current of `speed` m/s along +x in the
+    band |z| < 3 m (the basin of the reference's open-water tests)."""
+    extent = res * cell
+    origin = snap_origin(center[0], center[1], extent, cell)
+    x, z = cell_centres(res, cell, origin)
+    d = np.maximum(np.maximum(np.abs(x) - F(6.0), np.abs(z) - F(6.0)), F(0.0))
+    bed = (d * F(0.6) + F(0.1) * bed_noise(x, z, seed)).astype(F)
+    water = np.maximum(F(level) - bed, F(0.0)).astype(F)
+    u = np.where((np.abs(z) < F(3.0)) & (water > F(0.0)), F(speed), F(0.0)).astype(F)
+    v = np.zeros_like(u)
+    n = res * res
+    return dict(res=res, cell=cell, origin=origin, center=center, bed=bed.ravel(), water=water.ravel(),
+                u=u.ravel(), v=v.ravel(), moisture=np.full(n, 0.9, F), grain=np.full(n, SAND, np.uint8))
+
+
+def seed_basin(core, scene):
+    """Seeds a sheet handle (oracle or device) with a basin scene."""
+    core.read_substrate(scene["bed"], scene["moisture"], scene["grain"])
+    core.map_grain(scene["grain"])
+    core.map_water_bed(scene["bed"], scene["water"])
+    core.map_water_velocity(scene["u"], scene["v"])
+
+
 def tires_at(t, speed=5.0, center=(0.0, 0.0), track=1.5, wheelbase=2.4, radius=0.38, width=0.2, slip=0.3,
              z0=-10.0):
     """Four tires in a track x wheelbase rectangle driving +z at `speed`."""

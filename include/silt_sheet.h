@@ -97,6 +97,11 @@ typedef struct {
     double cut_m3;
 } silt_ledger;
 
+/* src/fluid_core.rs:440-448 (`GroundSample`); settled dust is off this path (0). */
+typedef struct {
+    float water_m, slurry_m, u, v, settled_dust_m, moisture, bed_m;
+} silt_ground_sample;
+
 /* src/fluid_core.rs:452-465 (`CoarseCell`), sheet fields. */
 typedef struct {
     float x, z, bed_m, water_m, slurry_m, moisture, u, v;
@@ -155,6 +160,10 @@ int silt_publish_film_flow_device(silt_sheet* s, float* d_film, float* d_flow);
 int silt_non_finite_count(silt_sheet* s, uint32_t* out);
 /* FluidCore::spray_m3 (src/fluid_core.rs:6817). */
 int silt_spray_m3(silt_sheet* s, double* out);
+/* FluidCore::sample (src/fluid_core.rs:6806-6813, sample_coarse :9428-9454)
+ * between steps (the patches are handed back): the coarse cell under (x, z);
+ * SILT_OK_NOOP and zeros outside the window. */
+int silt_sample(silt_sheet* s, float x, float z, silt_ground_sample* out);
 /* FluidCore::window_bounds (src/fluid_core.rs:6977): origin x, origin z, extent. */
 int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
 /* Raw plane copy to host for tests and tools: which = 0 water, 1 slurry, 2 uw,
@@ -224,6 +233,17 @@ int silt_set_fine_sub_cap(silt_sheet* s, float cap);
 int silt_set_fine_pace(silt_sheet* s, int32_t pace);
 /* FluidCore::set_near_field (src/fluid_core/near.rs:332). */
 int silt_set_near_field(silt_sheet* s, int32_t on);
+/* FluidCore::set_open_water (src/fluid_core.rs:5293-5303; on = 0 is None):
+ * the water sheet runs at `mobility` (clamped to [0, 1]) with Manning bed
+ * friction `manning_n` and eddy viscosity `eddy_m2_s` (m^2/s) after each
+ * coarse pair (bed_friction / eddy_shear, :7485-7581). */
+int silt_set_open_water(silt_sheet* s, int32_t on, float mobility, float manning_n, float eddy_m2_s);
+/* FluidCore::set_surface_diffusion (src/fluid_core.rs:5284-5286, applied by
+ * diffuse_surface :7584-7636), m^2/s; 0 is off. */
+int silt_set_surface_diffusion(silt_sheet* s, float m2_s);
+/* FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097): kept for the
+ * caller; the tracers that read it are not on this path (flow.A stays 0). */
+int silt_set_turbidity_enabled(silt_sheet* s, int32_t on);
 
 /* ------------------------------------------------------ one-sheet operator */
 /* Free `step_sheet` (src/fluid_core.rs:770) with the gravity drive on caller

@@ -82,6 +82,8 @@ def lib():
         L.oracle_core_set_fine_pace.argtypes = [_p, _i]
         L.oracle_core_set_fine_sub_cap.argtypes = [_p, _f]
         L.oracle_core_set_near_field.argtypes = [_p, _i]
+        L.oracle_core_set_open_water.argtypes = [_p, _i, _f, _f, _f]
+        L.oracle_core_set_surface_diffusion.argtypes = [_p, _f]
         L.oracle_core_near_tiles.argtypes = [_p]
         L.oracle_core_near_tiles.restype = _i
         L.oracle_core_spray_m3.argtypes = [_p]
@@ -251,6 +253,12 @@ class Core:
 
     def set_near_field(self, on):
         lib().oracle_core_set_near_field(self.h, int(on))
+
+    def set_open_water(self, on, mobility=0.0, manning_n=0.0, eddy_m2_s=0.0):
+        lib().oracle_core_set_open_water(self.h, int(on), mobility, manning_n, eddy_m2_s)
+
+    def set_surface_diffusion(self, m2_s):
+        lib().oracle_core_set_surface_diffusion(self.h, m2_s)
 
     def near_tiles(self):
         return lib().oracle_core_near_tiles(self.h)

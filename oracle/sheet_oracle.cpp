@@ -1041,6 +1041,10 @@ struct Core {
     int inflow_j = -1;
     float inflow_x0 = 0, inflow_x1 = 0, inflow_rate = 0;
     double opened_m3 = 0.0;
+    // src/fluid_core.rs:333-340 OpenWater, :5284-5303 the setters.
+    bool open_water = false;
+    float ow_mobility = 0.0f, ow_manning = 0.0f, ow_eddy = 0.0f;
+    float surface_diffusion = 0.0f;
 
     explicit Core(const oracle_core_cfg& c) : cfg(c) {
         res = (usize)c.res;
@@ -1528,6 +1532,23 @@ struct Core {
     // src/fluid_core.rs:7942-8150 step_pair (open sheets, no bodies).
     void step_pair(float dt, bool fine) {
         if (fine && !fine_on) return;
+        // An open reach runs the water row at its own mobility (a negative
+        // entry, src/fluid_core.rs:8015-8017) and puts the water value back
+        // after the pair (:8142-8145).
+        struct RestoreWater {
+            Core& c;
+            ~RestoreWater() {
+                if (!c.open_water) return;
+                float nuw = dynamic_viscosity(3, 1.0f);
+                std::fill(c.nu_w.begin(), c.nu_w.end(), nuw);
+                std::fill(c.fnu_w.begin(), c.fnu_w.end(), nuw);
+            }
+        } restore{*this};
+        if (open_water) {
+            float m = -rmax(ow_mobility, 1.0e-4f);
+            std::fill(nu_w.begin(), nu_w.end(), m);
+            std::fill(fnu_w.begin(), fnu_w.end(), m);
+        }
         float cap = fine ? fine_sub_cap : 8.0f;
         int pace = fine ? fine_pace : 0;
         if (!fine) {
@@ -1615,9 +1636,112 @@ struct Core {
             push_on(p, water.data(), slurry.data(), uw.data(), vw.data(), us.data(), vs.data(), res, cfg.cell, origin);
         }
         step_pair(dt, false);
+        bed_friction(dt);
+        diffuse_surface(dt);
         if (!ps.empty()) peel(ps, water.data(), uw.data(), vw.data(), res, cfg.cell, origin, true, spray);
         for (const auto& s : spray) spray_m3 += s.volume;
         return spray;
+    }
+
+    // src/fluid_core.rs:7482-7512 bed_friction: the eddy shear, then Manning
+    // friction, implicit, on the coarse water in open-water mode.
+    void bed_friction(float dt) {
+        if (!open_water) return;
+        if (dt <= 0.0f) return;
+        eddy_shear(ow_eddy, dt);
+        if (ow_manning <= 0.0f) return;
+        float gn2 = GRAVITY * ow_manning * ow_manning;
+        for (usize idx = 0; idx < res * res; ++idx) {
+            float h = water[idx];
+            if (!(h > 1.0e-4f)) continue;
+            float u = uw[idx], v = vw[idx];
+            float speed = hypotf(u, v);
+            if (!(speed > 0.0f)) continue;
+            float k = gn2 * speed / powf(rmax(h, 0.002f), 4.0f / 3.0f);
+            float keep = 1.0f / (1.0f + dt * k);
+            uw[idx] = u * keep;
+            vw[idx] = v * keep;
+        }
+    }
+
+    // src/fluid_core.rs:7514-7581 eddy_shear: one explicit Laplacian of the
+    // water velocity from a snapshot; dry ground standing 3 cm above the
+    // surface is no slip, a beach is skipped.
+    void eddy_shear(float nu_t, float dt) {
+        if (nu_t <= 0.0f) return;
+        const float WET = 0.003f, STANDS_OUT = 0.03f;
+        usize n = res * res;
+        float k = rmin(nu_t * dt / (cfg.cell * cfg.cell), 0.2f);
+        std::vector<float> du(n, 0.0f), dv(n, 0.0f);
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) {
+                usize idx = j * res + i;
+                if (!(water[idx] > WET)) continue;
+                float u0 = uw[idx], v0 = vw[idx];
+                float lu = 0.0f, lv = 0.0f;
+                const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+                for (auto& d : nb) {
+                    long ni = (long)i + d[0], nj = (long)j + d[1];
+                    if (ni < 0 || nj < 0 || ni >= (long)res || nj >= (long)res) continue;
+                    usize nidx = (usize)nj * res + (usize)ni;
+                    float un, vn;
+                    if (water[nidx] > WET) {
+                        un = uw[nidx];
+                        vn = vw[nidx];
+                    } else if (bed[nidx] > bed[idx] + water[idx] + STANDS_OUT) {
+                        un = 0.0f;
+                        vn = 0.0f;
+                    } else {
+                        continue;
+                    }
+                    lu += un - u0;
+                    lv += vn - v0;
+                }
+                du[idx] = k * lu;
+                dv[idx] = k * lv;
+            }
+        for (usize idx = 0; idx < n; ++idx)
+            if (du[idx] != 0.0f || dv[idx] != 0.0f) {
+                float nu = uw[idx] + du[idx], nv = vw[idx] + dv[idx];
+                if (finite(nu) && finite(nv)) {
+                    uw[idx] = nu;
+                    vw[idx] = nv;
+                }
+            }
+    }
+
+    // src/fluid_core.rs:7582-7636 diffuse_surface: surface-slope fluxes from
+    // one snapshot, each east and north face once, a quarter-column donor limit.
+    void diffuse_surface(float dt) {
+        if (surface_diffusion <= 0.0f || dt <= 0.0f) return;
+        float k = rmin(surface_diffusion * dt / (cfg.cell * cfg.cell), 0.12f);
+        const float WET = 0.003f;
+        usize n = res * res;
+        std::vector<float> delta(n, 0.0f);
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) {
+                usize a = j * res + i;
+                float ha = water[a];
+                if (!(ha > WET)) continue;
+                float ea = bed[a] + ha;
+                for (int face = 0; face < 2; ++face) {
+                    if (face == 0 && !(i + 1 < res)) continue;
+                    if (face == 1 && !(j + 1 < res)) continue;
+                    usize b = face == 0 ? a + 1 : a + res;
+                    float hb = water[b];
+                    if (!(hb > WET)) continue;
+                    float eb = bed[b] + hb;
+                    float f = k * (ea - eb);
+                    if (f > 0.0f) f = rmin(f, 0.25f * ha);
+                    else f = rmax(f, -0.25f * hb);
+                    delta[a] -= f;
+                    delta[b] += f;
+                }
+            }
+        for (usize idx = 0; idx < n; ++idx) {
+            float d = delta[idx];
+            if (d != 0.0f && finite(d)) water[idx] = rmax(water[idx] + d, 0.0f);
+        }
     }
 
     // Inflow strip: one coarse row, water added as depth, booked as opened volume.
@@ -1896,6 +2020,20 @@ void oracle_core_publish(void* cp, float* film, float* flow) {
 }
 void oracle_core_set_fine_pace(void* cp, int pace) { ((Core*)cp)->fine_pace = std::min(pace, 3); }
 void oracle_core_set_fine_sub_cap(void* cp, float cap) { ((Core*)cp)->fine_sub_cap = finite(cap) ? rclamp(cap, 1.0f, 8.0f) : 8.0f; }
+// src/fluid_core.rs:5293-5303 set_open_water (on = 0: None).
+void oracle_core_set_open_water(void* cp, int on, float mobility, float manning_n, float eddy_m2_s) {
+    Core& C = *(Core*)cp;
+    C.open_water = on != 0 && finite(mobility) && finite(manning_n) && finite(eddy_m2_s);
+    if (!C.open_water) return;
+    C.ow_mobility = rmin(rmax(mobility, 0.0f), 1.0f);
+    C.ow_manning = rmax(manning_n, 0.0f);
+    C.ow_eddy = rmax(eddy_m2_s, 0.0f);
+}
+// src/fluid_core.rs:5284-5286 set_surface_diffusion.
+void oracle_core_set_surface_diffusion(void* cp, float m2_s) {
+    Core& C = *(Core*)cp;
+    C.surface_diffusion = finite(m2_s) ? rmax(m2_s, 0.0f) : 0.0f;
+}
 void oracle_core_set_near_field(void* cp, int on) {
     Core& C = *(Core*)cp;
     C.near_on = on != 0;

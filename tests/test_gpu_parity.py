@@ -155,3 +155,53 @@ def test_free_step_sheet_matches_oracle(res, cell, dt, vort):
     torch.cuda.synchronize()
     dh = np.abs(dev[0].cpu().numpy() - ref[0]).max()
     assert dh <= TOL_H, dh
+
+
+@pytest.mark.parametrize("engine", [G.ENGINE_WINDOW, G.ENGINE_GRID])
+def test_open_water_and_surface_diffusion_match_oracle(engine):
+    """Open-water mode (mobility 1, Manning 0.035, eddy 0.06 m^2/s, the ford
+    reach's settings, src/ford.rs:338-343) and surface diffusion 0.024 m^2/s on
+    a basin with a 0.75 m/s current: depth within the 1e-4 m criterion after
+    60 steps, velocity within 1e-3 m/s (Manning's powf and hypotf may differ
+    from glibc's by an ulp), and the FP64 books closed. The grid engine runs
+    against the oracle's snapshot-confinement form."""
+    sc = S.basin()
+    dev = G.Sheet(res=sc["res"], cell=sc["cell"], engine=engine)
+    # The grid engine confines from a snapshot: the oracle's pair with the
+    # free operator's form does too on boxes of at least 48 x 32 (the basin's).
+    ref = O.Core(threads=1, inner_par=engine == G.ENGINE_GRID)
+    for c in (dev, ref):
+        S.seed_basin(c, sc)
+        c.set_open_water(True, 1.0, 0.035, 0.06)
+        c.set_surface_diffusion(0.024)
+    v0 = dev.ledger()
+    for _ in range(60):
+        dev.step(DT, want_spray=False)
+        ref.step(DT)
+    for name in ("water", "slurry"):
+        d = float(np.abs(dev.get(name) - ref.get(name)).max())
+        assert d <= 1e-4, (name, d)
+    du = float(np.abs(dev.get("uw") - ref.get("uw")).max())
+    assert du <= 1e-3, du
+    led = dev.ledger()
+    gap = abs(led["total_m3"] + led["cut_m3"] - v0["total_m3"] - v0["cut_m3"]) / v0["total_m3"]
+    assert gap < 1e-6, gap
+    # The current slowed under the bed friction, as on the oracle.
+    assert float(np.abs(dev.get("uw")).max()) < 0.9
+
+
+def test_sample_reads_the_coarse_cell():
+    sc = S.basin()
+    dev = G.Sheet(res=sc["res"], cell=sc["cell"])
+    ref = O.Core(threads=1)
+    for c in (dev, ref):
+        S.seed_basin(c, sc)
+    for _ in range(5):
+        dev.step(DT, want_spray=False)
+        ref.step(DT)
+    for x, z in ((0.3, -1.1), (2.0, 2.5), (-5.9, 0.1)):
+        g = dev.sample(x, z)
+        r = ref.sample(x, z)
+        assert abs(g["water_m"] - r["water_m"]) <= 1e-4 and abs(g["bed_m"] - r["bed_m"]) == 0.0
+        assert abs(g["moisture"] - r["moisture"]) == 0.0
+    assert dev.sample(1000.0, 0.0) is None
