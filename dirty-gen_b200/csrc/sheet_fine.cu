@@ -38,6 +38,7 @@
 #include "sheet_host_math.h"
 #include "sheet_math.cuh"
 #include "sheet_window.cuh"
+#include "sheet_park.cuh"
 #include "launch_count.cuh"
 
 namespace silt {
@@ -122,6 +123,7 @@ struct NearMeta {
 
 struct Impl {
     int res = 0;
+    park::Table park;                 // parked cells by world key (allocated on first use)
     int8_t* owner = nullptr;          // per coarse cell: patch that holds it, -1 none
     std::vector<int8_t> h_owner;      // host mirror
     std::vector<int> held_now;        // coarse cells held by the last laid patches
@@ -721,9 +723,14 @@ __global__ void k_restrict(const PatchRef* refs, int fres, int sub, SheetView W,
 
 // After the restrict: fine cells outside the coarse window have their volume
 // parked (src/fluid_core.rs:8476-8484), and every fine depth is released.
-__device__ void release_cells(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park,
-                              size_t k0, size_t stride) {
+// Empties the patches. With `park`, fine cells outside the window add their
+// depth to the parked slot of the coarse world cell under them
+// (src/fluid_core.rs:8484-8487: water * fine_area / coarse_area), and their
+// volume to the parked books.
+__device__ void release_cells(const PatchRef* refs, int np, int fres, float fcell, float ccell, double* books,
+                              int park, park::Table T, size_t k0, size_t stride) {
     const size_t fn = (size_t)fres * fres;
+    const float fine_area = fcell * fcell, coarse_area = ccell * ccell;
     double pw = 0.0, ps = 0.0;
     for (size_t k = k0; k < fn * np; k += stride) {
         const PatchRef& R = refs[k / fn];
@@ -731,6 +738,17 @@ __device__ void release_cells(const PatchRef* refs, int np, int fres, float fine
         if (park && !(R.col[f % fres] >= 0 && R.row[f / fres] >= 0)) {
             pw += (double)R.water[f] * fine_area;
             ps += (double)R.slurry[f] * fine_area;
+            if (T.cap && (R.water[f] != 0.0f || R.slurry[f] != 0.0f)) {
+                const float x = R.ox + ((float)(f % fres) + 0.5f) * fcell;
+                const float z = R.oz + ((float)(f / fres) + 0.5f) * fcell;
+                bool fresh = false;
+                const int s = park::find_or_insert(T, park::key_of(park::world_axis(x, ccell), park::world_axis(z, ccell)),
+                                                   &fresh);
+                if (s >= 0) {
+                    atomicAdd(&T.vals[(size_t)s * park::NVAL + 0], R.water[f] * fine_area / coarse_area);
+                    atomicAdd(&T.vals[(size_t)s * park::NVAL + 1], R.slurry[f] * fine_area / coarse_area);
+                }
+            }
         }
         R.water[f] = 0.0f;
         R.slurry[f] = 0.0f;
@@ -745,10 +763,37 @@ __device__ void release_cells(const PatchRef* refs, int np, int fres, float fine
     }
 }
 
-__global__ void k_release(const PatchRef* refs, int np, int fres, float fine_area, double* books, int park) {
+__global__ void k_release(const PatchRef* refs, int np, int fres, float fcell, float ccell, double* books, int park,
+                          park::Table T) {
     ::silt::dep_wait();
-    release_cells(refs, np, fres, fine_area, books, park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
+    release_cells(refs, np, fres, fcell, ccell, books, park, T, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
                   (size_t)gridDim.x * blockDim.x);
+}
+
+// A move of the window by (di, dj) cells: near-field tiles follow their
+// coarse cells; tiles whose cell leaves the window (all of them when the
+// window jumps) are released (their residual sums to zero, so no volume
+// goes with them).
+__global__ void k_near_unmap(int* slot_map, size_t n) {
+    ::silt::dep_wait();
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        slot_map[c] = -1;
+}
+
+__global__ void k_near_move(NearMeta* meta, int* slot_map, int* counters, int res, int di, int dj, int keep) {
+    ::silt::dep_wait();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= NEAR_POOL) return;
+    NearMeta& M = meta[s];
+    if (M.state != 1) return;
+    const int i = M.key % res - di, j = M.key / res - dj;
+    if (keep && i >= 0 && j >= 0 && i < res && j < res) {
+        M.key = j * res + i;
+        slot_map[M.key] = s;
+    } else {
+        M.state = 2;  // back to the free stack at the next fade
+        atomicSub(&counters[1], 1);
+    }
 }
 
 __global__ void k_init_pool(NearMeta* meta, int* free_stack, int* slot_map, size_t ncells, int* counters) {
@@ -1074,6 +1119,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         oidx.push_back(kv.first);
         oval.push_back(kv.second);
     }
+    if (L.any_park && !M.park.cap) FCK(park::alloc(M.park, 1u << 16, W.st));
     Table tab;
     // Axes first: the refs below point into the device copy of this table.
     const size_t off_axes = tab.put(axes.data(), axes.size());
@@ -1330,8 +1376,8 @@ int restrict_all(Patches& P, silt_sheet* s) {
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }
-    ::silt::launch_dep(k_release, dim3(launch_blocks((size_t)L.np * P.fres * P.fres)), dim3(256), 0, W.st, refs, L.np, P.fres, P.fcell * P.fcell,
-                                                                              M.d_books, L.any_park ? 1 : 0);
+    ::silt::launch_dep(k_release, dim3(launch_blocks((size_t)L.np * P.fres * P.fres)), dim3(256), 0, W.st, refs, L.np,
+                       P.fres, P.fcell, W.cell, M.d_books, L.any_park ? 1 : 0, M.park);
     ::silt::count_launch();
     FCK(cudaGetLastError());
     P.fine_on = false;
@@ -1443,6 +1489,22 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
 }
 
 double* books(Patches& P) { return I(P).d_books; }
+
+park::Table& park_table(Patches& P) { return I(P).park; }
+
+int move_window(Patches& P, silt_sheet* s, int di, int dj, bool scroll) {
+    Impl& M = I(P);
+    if (!M.near_maybe) return SILT_OK;
+    SheetView W = view_of(s);
+    ::silt::launch_dep(k_near_unmap, dim3(launch_blocks(W.n)), dim3(256), 0, W.st, M.slot_map, W.n);
+    ::silt::count_launch();
+    FCK(cudaGetLastError());
+    ::silt::launch_dep(k_near_move, dim3((NEAR_POOL + 255) / 256), dim3(256), 0, W.st, M.meta, M.slot_map, M.counters,
+                       W.res, di, dj, scroll ? 1 : 0);
+    ::silt::count_launch();
+    FCK(cudaGetLastError());
+    return SILT_OK;
+}
 
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut) {
     Impl& M = I(P);
@@ -1558,6 +1620,7 @@ void destroy(Patches& P) {
         }
         delete HS;
     }
+    park::release(M->park);
     cudaFree(M->owner);
     cudaFree(M->slot_map);
     cudaFree(M->pool);
@@ -1611,6 +1674,7 @@ struct FineRec {
     int* counters;
     SprayRec* spray;
     double* books;
+    park::Table park_table;
 };
 
 struct PeelRec {
@@ -1708,8 +1772,8 @@ __global__ void kb_restrict(const FineRec* recs) {
 __global__ void kb_release(const FineRec* recs) {
     ::silt::dep_wait();
     const FineRec& r = recs[blockIdx.z];
-    release_cells(r.refs, r.np, r.fres, r.fcell * r.fcell, r.books, r.park, blockIdx.x * (size_t)blockDim.x + threadIdx.x,
-                  (size_t)gridDim.x * blockDim.x);
+    release_cells(r.refs, r.np, r.fres, r.fcell, r.W.cell, r.books, r.park, r.park_table,
+                  blockIdx.x * (size_t)blockDim.x + threadIdx.x, (size_t)gridDim.x * blockDim.x);
 }
 
 __global__ void kb_coarse_push(const FineRec* recs) {
@@ -1873,6 +1937,7 @@ int batch_launch(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std
         r.counters = M.counters;
         r.spray = M.spray;
         r.books = M.d_books;
+        r.park_table = M.park;
         window::Job* jobs = const_cast<window::Job*>(TAB(window::Job, L.off_jobs));
         for (int k = 0; k < 2 * L.np; ++k) jl[q++] = jobs + k;
         mx_owner = std::max(mx_owner, r.n_owner);

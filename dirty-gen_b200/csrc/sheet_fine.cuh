@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/silt_sheet.h"
+#include "sheet_park.cuh"
 
 namespace silt {
 namespace fine {
@@ -104,6 +105,11 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr);
 // Device address of the books: [0] spray, [1] parked water, [2] parked slurry (m^3, FP64).
 double* books(Patches& P);
+// The window's parked cells (allocated on first use).
+park::Table& park_table(Patches& P);
+// The near field's part of a window move by (di, dj) cells (scroll = false:
+// a jump, every tile is released).
+int move_window(Patches& P, silt_sheet* s, int di, int dj, bool scroll);
 const char* last_error();
 int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& pushes, int patch, float* host,
                 float* origin2);

@@ -30,6 +30,7 @@
 #include "sheet_grid.cuh"
 #include "sheet_host_math.h"
 #include "sheet_ops.cuh"
+#include "sheet_park.cuh"
 #include "sheet_window.cuh"
 
 namespace {
@@ -122,6 +123,7 @@ struct silt_sheet {
     float surface_diffusion = 0.0f;
     float* ow_scratch = nullptr;   // 2 n floats for the drivers' snapshots
     bool turbidity = false;        // FluidCore::set_turbidity_enabled (tracers are off this path)
+    float center[2] = {0.0f, 0.0f};  // the chase point (set_center / recenter)
     // Tire coupling (silt_set_coupling): nested sheets, none, or the learned closure.
     int coupling = SILT_COUPLING_NESTED;
     silt_closure* net = nullptr;
@@ -937,6 +939,143 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     }
     s->ledger_fresh = true;  // d_acc holds the post-step depth sums (spray already taken off)
     return SILT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// world_key's axis (src/fluid_core.rs:9894-9896) on the host: floor(p / cell)
+// as a saturating i32 cast.
+long long world_axis_host(float p, float cell) {
+    const float f = std::floor(p / cell);
+    if (std::isnan(f)) return 0;
+    if (f >= 2147483648.0f) return 2147483647LL;
+    if (f < -2147483648.0f) return -2147483648LL;
+    return (long long)f;
+}
+
+// uniform_cell_shift (src/fluid_core.rs:9899-9933): the move is a whole number
+// of cells for the window's corners and middle alike.
+bool uniform_cell_shift(const float* o, const float* nw, float cell, int res, int* di, int* dj) {
+    if (res <= 0 || !(std::isfinite(cell) && cell > 0.0f)) return false;
+    auto key = [&](const float* org, int i, int j, long long* kx, long long* kz) {
+        *kx = world_axis_host(org[0] + ((float)i + 0.5f) * cell, cell);
+        *kz = world_axis_host(org[1] + ((float)j + 0.5f) * cell, cell);
+    };
+    long long o0x, o0z, n0x, n0z, o1x, o1z, n1x, n1z, omx, omz, nmx, nmz;
+    key(o, 0, 0, &o0x, &o0z);
+    key(nw, 0, 0, &n0x, &n0z);
+    const long long ddi = n0x - o0x, ddj = n0z - o0z;
+    const int last = res - 1, mid = res / 2;
+    key(o, last, last, &o1x, &o1z);
+    key(nw, last, last, &n1x, &n1z);
+    if (o1x - o0x != last || o1z - o0z != last) return false;
+    if (n1x - n0x != last || n1z - n0z != last) return false;
+    if (n1x - o1x != ddi || n1z - o1z != ddj) return false;
+    key(o, mid, mid, &omx, &omz);
+    key(nw, mid, mid, &nmx, &nmz);
+    if (nmx - omx != ddi || nmz - omz != ddj) return false;
+    if (ddi > INT_MAX || ddi < INT_MIN || ddj > INT_MAX || ddj < INT_MIN) return false;
+    *di = (int)ddi;
+    *dj = (int)ddj;
+    return true;
+}
+
+// Room in the parked table for `incoming` more keys, rebuilding it larger
+// (and without tombstones) when taken slots would pass half of it.
+int park_room(silt_sheet* s, size_t incoming) {
+    silt::park::Table& T = silt::fine::park_table(s->fine);
+    unsigned int used = 0, overflow = 0;
+    if (T.cap) CK(silt::park::usage(T, &used, &overflow, s->st));
+    if (overflow) return fail_cuda(cudaErrorMemoryAllocation, "parked cells: table overflow");
+    size_t want = 2 * ((size_t)used + incoming);
+    if (T.cap && want <= T.cap) return SILT_OK;
+    size_t cap = 1u << 16;
+    while (cap < want) cap <<= 1;
+    if (cap > (1u << 30)) return fail_cuda(cudaErrorMemoryAllocation, "parked cells: table too large");
+    CK(silt::park::rebuild(T, (unsigned int)cap, s->st));
+    return SILT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int silt_set_center(silt_sheet* s, float cx, float cz) {
+    if (!s) return fail_arg("handle");
+    s->center[0] = cx;
+    s->center[1] = cz;
+    return SILT_OK;
+}
+
+int silt_recenter(silt_sheet* s, float cx, float cz) {
+    if (!s) return fail_arg("handle");
+    if (!std::isfinite(cx) || !std::isfinite(cz)) return fail_arg("recenter: centre");
+    int rc = silt::fine::restrict_all(s->fine, s);  // the patches go back first (src/fluid_core.rs:5410-5412)
+    if (rc) return rc;
+    s->center[0] = cx;
+    s->center[1] = cz;
+    float nw[2];
+    silt::host::snap_origin(cx, cz, (float)s->res * s->cfg.cell, s->cfg.cell, nw);
+    if (std::fabs(nw[0] - s->origin[0]) < 1.0e-4f && std::fabs(nw[1] - s->origin[1]) < 1.0e-4f) return SILT_OK;
+    if ((rc = flush_cut(s))) return rc;
+    int di = 0, dj = 0;
+    const bool scroll = uniform_cell_shift(s->origin, nw, s->cfg.cell, s->res, &di, &dj);
+    const size_t n = s->n;
+    size_t incoming = n;
+    if (scroll) {
+        const size_t ai = (size_t)std::min(std::abs(di), s->res), aj = (size_t)std::min(std::abs(dj), s->res);
+        incoming = std::min(n, ai * (size_t)s->res + aj * (size_t)s->res);
+    }
+    if ((rc = park_room(s, incoming))) return rc;
+    silt::park::Table& T = silt::fine::park_table(s->fine);
+    silt::park::Planes P;
+    memset(&P, 0, sizeof P);
+    const int nx = s->cur ^ 1;
+    for (int l = 0; l < 2; ++l) {
+        P.h[l] = s->h[l][s->cur];
+        P.u[l] = s->u[l][s->cur];
+        P.v[l] = s->v[l][s->cur];
+        P.h_out[l] = s->h[l][nx];
+        P.u_out[l] = s->u[l][nx];
+        P.v_out[l] = s->v[l][nx];
+    }
+    P.moisture = s->moisture;
+    P.moisture_out = s->staging;
+    P.res = s->res;
+    P.cell = s->cfg.cell;
+    P.ambient = s->moisture_ambient;
+    P.books = silt::fine::books(s->fine);
+    if (scroll) {
+        // shift_coarse_scroll (src/fluid_core.rs:9024-9145).
+        CK(silt::park::park_cells(P, T, s->origin[0], s->origin[1], di, dj, 0, s->st));
+        CK(silt::park::scroll_cells(P, di, dj, s->st));
+        s->cur = nx;
+        std::swap(s->moisture, s->staging);
+        for (int l = 0; l < 2; ++l) {
+            P.h[l] = s->h[l][s->cur];
+            P.u[l] = s->u[l][s->cur];
+            P.v[l] = s->v[l][s->cur];
+        }
+        P.moisture = s->moisture;
+        s->origin[0] = nw[0];
+        s->origin[1] = nw[1];
+        CK(silt::park::restore_cells(P, T, s->origin[0], s->origin[1], di, dj, 0, s->st));
+    } else {
+        // shift_coarse_hash (src/fluid_core.rs:9147-9222).
+        CK(silt::park::park_cells(P, T, s->origin[0], s->origin[1], 0, 0, 1, s->st));
+        s->origin[0] = nw[0];
+        s->origin[1] = nw[1];
+        CK(silt::park::restore_cells(P, T, s->origin[0], s->origin[1], 0, 0, 1, s->st));
+    }
+    if ((rc = silt::fine::move_window(s->fine, s, di, dj, scroll))) return rc;
+    unsigned int used = 0, overflow = 0;
+    CK(silt::park::usage(T, &used, &overflow, s->st));
+    if (overflow) return fail_cuda(cudaErrorMemoryAllocation, "parked cells: table overflow");
+    s->vmax_bound = std::max(s->vmax_bound, silt::host::kSpeedCap * 1.4142137f);
+    s->ledger_fresh = false;
+    return tiles_dirty(s);
 }
 
 int silt_set_open_water(silt_sheet* s, int32_t on, float mobility, float manning_n, float eddy_m2_s) {

@@ -118,6 +118,7 @@ def lib():
             "silt_plane_device": [_p, _i, ctypes.POINTER(_p)], "silt_sheet_copy_state": [_p, _p],
             "silt_set_open_water": [_p, _i, _f, _f, _f], "silt_set_surface_diffusion": [_p, _f],
             "silt_set_turbidity_enabled": [_p, _i], "silt_sample": [_p, _f, _f, ctypes.POINTER(GroundSample)],
+            "silt_recenter": [_p, _f, _f], "silt_set_center": [_p, _f, _f],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -278,6 +279,18 @@ class Sheet:
 
     def set_surface_diffusion(self, m2_s):
         check(lib().silt_set_surface_diffusion(self.h, m2_s), "set_surface_diffusion")
+
+    def recenter(self, cx, cz):
+        """FluidCore::recenter: move the window; cells that leave are parked, cells that enter restored."""
+        check(lib().silt_recenter(self.h, cx, cz), "recenter")
+
+    def set_center(self, cx, cz):
+        check(lib().silt_set_center(self.h, cx, cz), "set_center")
+
+    def origin(self):
+        ox, oz, ext = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(lib().silt_window_bounds(self.h, ctypes.byref(ox), ctypes.byref(oz), ctypes.byref(ext)), "window_bounds")
+        return ox.value, oz.value
 
     def set_turbidity_enabled(self, on):
         check(lib().silt_set_turbidity_enabled(self.h, int(on)), "set_turbidity_enabled")

@@ -164,6 +164,17 @@ int silt_spray_m3(silt_sheet* s, double* out);
  * between steps (the patches are handed back): the coarse cell under (x, z);
  * SILT_OK_NOOP and zeros outside the window. */
 int silt_sample(silt_sheet* s, float x, float z, silt_ground_sample* out);
+/* FluidCore::recenter (src/fluid_core.rs:5409-5421): moves the window to
+ * the one centred on (cx, cz). Cells that slide off are parked (in a device
+ * table keyed by world cell, booked as frozen volume), cells that slide on
+ * are restored; bed and grain stay on their index (the caller re-reads the
+ * substrate). A whole-cell move scrolls (shift_coarse_scroll :9024), any
+ * other jump re-keys every cell (shift_coarse_hash :9147). Near-field tiles
+ * follow their cells; tiles leaving the window are released. */
+int silt_recenter(silt_sheet* s, float cx, float cz);
+/* FluidCore::set_center (src/fluid_core.rs:5403): track the chase point
+ * without sliding the window. */
+int silt_set_center(silt_sheet* s, float cx, float cz);
 /* FluidCore::window_bounds (src/fluid_core.rs:6977): origin x, origin z, extent. */
 int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
 /* Raw plane copy to host for tests and tools: which = 0 water, 1 slurry, 2 uw,

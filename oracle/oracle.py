@@ -84,6 +84,10 @@ def lib():
         L.oracle_core_set_near_field.argtypes = [_p, _i]
         L.oracle_core_set_open_water.argtypes = [_p, _i, _f, _f, _f]
         L.oracle_core_set_surface_diffusion.argtypes = [_p, _f]
+        L.oracle_core_recenter.argtypes = [_p, _f, _f]
+        L.oracle_core_origin.argtypes = [_p, _p]
+        L.oracle_core_parked_count.argtypes = [_p]
+        L.oracle_core_parked_count.restype = _i
         L.oracle_core_near_tiles.argtypes = [_p]
         L.oracle_core_near_tiles.restype = _i
         L.oracle_core_spray_m3.argtypes = [_p]
@@ -259,6 +263,17 @@ class Core:
 
     def set_surface_diffusion(self, m2_s):
         lib().oracle_core_set_surface_diffusion(self.h, m2_s)
+
+    def recenter(self, cx, cz):
+        lib().oracle_core_recenter(self.h, cx, cz)
+
+    def origin(self):
+        o = np.zeros(2, np.float32)
+        lib().oracle_core_origin(self.h, _ptr(o))
+        return float(o[0]), float(o[1])
+
+    def parked_count(self):
+        return lib().oracle_core_parked_count(self.h)
 
     def near_tiles(self):
         return lib().oracle_core_near_tiles(self.h)

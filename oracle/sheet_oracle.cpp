@@ -1028,7 +1028,12 @@ struct Core {
     bool fine_on = false;
     bool near_on = true;
     std::map<std::pair<int, int>, NearTile> near;
-    std::map<std::pair<int, int>, std::pair<float, float>> parked;  // water, slurry depth
+    // src/fluid_core.rs:4763-4782 Parked (the sheet fields; dust, foam and
+    // the tracers are off this path and stay 0).
+    struct Parked {
+        float water = 0, slurry = 0, uw = 0, vw = 0, us = 0, vs = 0, moisture = 0;
+    };
+    std::map<std::pair<int, int>, Parked> parked;
     float spray_m3 = 0.0f;
     std::vector<TirePush> pushes;
     float fine_sub_cap = 8.0f;
@@ -1281,8 +1286,8 @@ struct Core {
                         float x = P.origin[0] + ((float)i + 0.5f) * cfg.fine_cell;
                         float z = P.origin[1] + ((float)j + 0.5f) * cfg.fine_cell;
                         auto& slot = parked[world_key(x, z, cfg.cell)];
-                        slot.first += P.water[fidx] * fine_area / coarse_area;
-                        slot.second += P.slurry[fidx] * fine_area / coarse_area;
+                        slot.water += P.water[fidx] * fine_area / coarse_area;
+                        slot.slurry += P.slurry[fidx] * fine_area / coarse_area;
                         continue;
                     }
                     usize cidx = (usize)cj * res + ci;
@@ -1744,6 +1749,135 @@ struct Core {
         }
     }
 
+    // src/fluid_core.rs:4797-4805 park_slot (sheet fields).
+    bool park_slot(const Parked& p) const {
+        return p.water > 1.0e-8f || p.slurry > 1.0e-8f || fabsf(p.moisture - moisture_ambient) > 6.0e-3f;
+    }
+    Parked slot_of(usize idx) const {
+        Parked p;
+        p.water = water[idx]; p.slurry = slurry[idx]; p.uw = uw[idx]; p.vw = vw[idx];
+        p.us = us[idx]; p.vs = vs[idx]; p.moisture = moisture[idx];
+        return p;
+    }
+    void put_slot(usize idx, const Parked& p) {
+        water[idx] = p.water; slurry[idx] = p.slurry; uw[idx] = p.uw; vw[idx] = p.vw;
+        us[idx] = p.us; vs[idx] = p.vs; moisture[idx] = p.moisture;
+    }
+    std::pair<int, int> cell_key(const float* o, usize i, usize j) const {
+        return world_key(o[0] + ((float)i + 0.5f) * cfg.cell, o[1] + ((float)j + 0.5f) * cfg.cell, cfg.cell);
+    }
+    void park(usize idx, std::pair<int, int> key) {
+        Parked p = slot_of(idx);
+        if (park_slot(p)) parked[key] = p;
+        else parked.erase(key);
+    }
+
+    // src/fluid_core.rs:9899-9933 uniform_cell_shift.
+    bool uniform_cell_shift(const float* o, const float* nw, int& di, int& dj) const {
+        if (res == 0 || !(finite(cfg.cell) && cfg.cell > 0.0f)) return false;
+        auto o00 = cell_key(o, 0, 0), n00 = cell_key(nw, 0, 0);
+        di = n00.first - o00.first;
+        dj = n00.second - o00.second;
+        usize last = res - 1;
+        auto o11 = cell_key(o, last, last), n11 = cell_key(nw, last, last);
+        if (o11.first - o00.first != (int)last || o11.second - o00.second != (int)last) return false;
+        if (n11.first - n00.first != (int)last || n11.second - n00.second != (int)last) return false;
+        if (n11.first - o11.first != di || n11.second - o11.second != dj) return false;
+        usize mid = res / 2;
+        auto om = cell_key(o, mid, mid), nm = cell_key(nw, mid, mid);
+        return nm.first - om.first == di && nm.second - om.second == dj;
+    }
+
+    // src/fluid_core.rs:9936-9990 each_leaving.
+    template <class F>
+    void each_leaving(int di, int dj, F f) const {
+        int n = (int)res;
+        if (di > 0) {
+            int w = std::min(di, n);
+            for (int j = 0; j < n; ++j) for (int i = 0; i < w; ++i) f(i, j);
+        } else if (di < 0) {
+            int w = std::min(-di, n);
+            for (int j = 0; j < n; ++j) for (int i = n - w; i < n; ++i) f(i, j);
+        }
+        auto covered = [&](int i) { return di > 0 ? i < di : (di < 0 ? i >= n + di : false); };
+        if (dj > 0) {
+            int h = std::min(dj, n);
+            for (int j = 0; j < h; ++j) for (int i = 0; i < n; ++i) if (!covered(i)) f(i, j);
+        } else if (dj < 0) {
+            int h = std::min(-dj, n);
+            for (int j = n - h; j < n; ++j) for (int i = 0; i < n; ++i) if (!covered(i)) f(i, j);
+        }
+    }
+
+    // src/fluid_core.rs:5409-5421 recenter (the sheet part) and :9004-9020 shift_coarse.
+    void recenter(float cx, float cz) {
+        if (fine_on) restrict_fine();
+        float nw[2];
+        snap_origin(cx, cz, (float)res * cfg.cell, cfg.cell, nw);
+        if (fabsf(nw[0] - origin[0]) < 1.0e-4f && fabsf(nw[1] - origin[1]) < 1.0e-4f) return;
+        int di, dj;
+        if (uniform_cell_shift(origin, nw, di, dj)) shift_scroll(nw, di, dj);
+        else shift_hash(nw);
+    }
+
+    // src/fluid_core.rs:9024-9145 shift_coarse_scroll: park the strip that
+    // leaves, copy the overlap by index (bed and grain stay on their index),
+    // restore the strip that enters.
+    void shift_scroll(const float* nw, int di, int dj) {
+        usize n = res * res;
+        each_leaving(di, dj, [&](int i, int j) { park((usize)j * res + i, cell_key(origin, i, j)); });
+        std::vector<float> cw = water, cs = slurry, cuw = uw, cvw = vw, cus = us, cvs = vs, cm = moisture;
+        int rn = (int)res;
+        for (int j = 0; j < rn; ++j)
+            for (int i = 0; i < rn; ++i) {
+                usize dst = (usize)j * res + i;
+                int si = i + di, sj = j + dj;
+                bool keep = false;
+                usize src = 0;
+                if (si >= 0 && si < rn && sj >= 0 && sj < rn) {
+                    src = (usize)sj * res + si;
+                    keep = cw[src] > 1.0e-8f || cs[src] > 1.0e-8f || cm[src] > 1.0e-4f;
+                }
+                if (keep) {
+                    water[dst] = cw[src]; slurry[dst] = cs[src]; uw[dst] = cuw[src]; vw[dst] = cvw[src];
+                    us[dst] = cus[src]; vs[dst] = cvs[src]; moisture[dst] = cm[src];
+                } else {
+                    water[dst] = 0; slurry[dst] = 0; uw[dst] = 0; vw[dst] = 0; us[dst] = 0; vs[dst] = 0;
+                    moisture[dst] = moisture_ambient;
+                }
+            }
+        (void)n;
+        origin[0] = nw[0];
+        origin[1] = nw[1];
+        each_leaving(-di, -dj, [&](int i, int j) {
+            auto it = parked.find(cell_key(origin, i, j));
+            if (it == parked.end()) return;
+            put_slot((usize)j * res + i, it->second);
+            parked.erase(it);
+        });
+    }
+
+    // src/fluid_core.rs:9147-9222 shift_coarse_hash: park everything, restore
+    // what the new window covers.
+    void shift_hash(const float* nw) {
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) park(j * res + i, cell_key(origin, i, j));
+        origin[0] = nw[0];
+        origin[1] = nw[1];
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) {
+                usize idx = j * res + i;
+                Parked p;
+                p.moisture = moisture_ambient;
+                auto it = parked.find(cell_key(origin, i, j));
+                if (it != parked.end()) {
+                    p = it->second;
+                    parked.erase(it);
+                }
+                put_slot(idx, p);
+            }
+    }
+
     // Inflow strip: one coarse row, water added as depth, booked as opened volume.
     void apply_inflow(float dt) {
         std::vector<usize> cells;
@@ -1973,7 +2107,7 @@ void oracle_core_ledger(void* cp, float* out5, double* out64) {
             slurry += column_sum(C.patches[pk].slurry, C.cfg.fine_cell);
         }
     float fw = 0.0f, fs = 0.0f, area = C.cfg.cell * C.cfg.cell;
-    for (auto& kv : C.parked) { fw += kv.second.first * area; fs += kv.second.second * area; }
+    for (auto& kv : C.parked) { fw += kv.second.water * area; fs += kv.second.slurry * area; }
     out5[0] = water; out5[1] = slurry; out5[2] = fw; out5[3] = fs; out5[4] = C.spray_m3;
     double w64 = 0.0, s64 = 0.0;
     for (float x : C.water) w64 += (double)rmax(x, 0.0f);
@@ -2029,6 +2163,14 @@ void oracle_core_set_open_water(void* cp, int on, float mobility, float manning_
     C.ow_manning = rmax(manning_n, 0.0f);
     C.ow_eddy = rmax(eddy_m2_s, 0.0f);
 }
+// src/fluid_core.rs:5409-5421 recenter.
+void oracle_core_recenter(void* cp, float cx, float cz) { ((Core*)cp)->recenter(cx, cz); }
+void oracle_core_origin(void* cp, float* out2) {
+    Core& C = *(Core*)cp;
+    out2[0] = C.origin[0];
+    out2[1] = C.origin[1];
+}
+int oracle_core_parked_count(void* cp) { return (int)((Core*)cp)->parked.size(); }
 // src/fluid_core.rs:5284-5286 set_surface_diffusion.
 void oracle_core_set_surface_diffusion(void* cp, float m2_s) {
     Core& C = *(Core*)cp;

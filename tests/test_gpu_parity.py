@@ -205,3 +205,72 @@ def test_sample_reads_the_coarse_cell():
         assert abs(g["water_m"] - r["water_m"]) <= 1e-4 and abs(g["bed_m"] - r["bed_m"]) == 0.0
         assert abs(g["moisture"] - r["moisture"]) == 0.0
     assert dev.sample(1000.0, 0.0) is None
+
+
+def _pair_planes(ref, dev, names=("water", "slurry", "uw", "vw", "us", "vs", "moisture")):
+    return {k: float(np.abs(ref.get(k) - dev.get(k)).max()) for k in names}
+
+
+def test_recenter_scroll_and_jump_match_oracle():
+    """Window moves between steps: a whole-cell scroll, a jump with no overlap
+    (every cell parked), the way back; depths within the 1e-4 m criterion of
+    the oracle throughout and the FP64 books (frozen included) equal."""
+    scene = S.window200()
+    ref, dev = O.Core(threads=1), G.Sheet()
+    for c in (ref, dev):
+        S.seed_core(c, scene)
+    v0 = dev.ledger()["total_m3"]
+    plan = [(3, None), (10, (3.1, -2.2)), (2, (100.0, 37.0)), (10, (0.0, 0.0)), (5, (-1.4, 0.8))]
+    for steps, move in plan:
+        if move is not None:
+            ref.recenter(*move)
+            dev.recenter(*move)
+            assert dev.origin() == ref.origin()
+            d = _pair_planes(ref, dev)
+            assert d["water"] <= 1e-4 and d["slurry"] <= 1e-4 and d["moisture"] == 0.0, d
+        for _ in range(steps):
+            ref.step(DT)
+            dev.step(DT, want_spray=False)
+        d = _pair_planes(ref, dev)
+        assert d["water"] <= 1e-4 and d["slurry"] <= 1e-4, (move, d)
+        lr, ld = ref.ledger(), dev.ledger()
+        assert abs(ld["frozen_water_m3"] - lr["frozen_water_m3"]) <= 1e-6 + 1e-5 * lr["frozen_water_m3"]
+        assert abs(ld["frozen_slurry_m3"] - lr["frozen_slurry_m3"]) <= 1e-6 + 1e-5 * lr["frozen_slurry_m3"]
+    led = dev.ledger()
+    assert abs(led["total_m3"] + led["cut_m3"] - v0) <= 1e-6 * v0
+
+
+@pytest.mark.parametrize("engine", [G.ENGINE_WINDOW, G.ENGINE_GRID])
+def test_patch_water_outside_the_window_is_parked_and_restored(engine):
+    """Tires at the window's west edge: the per-tire patches reach past it, so
+    their off-window water is parked under its coarse world cell
+    (src/fluid_core.rs:8484-8487); moving the window west restores it. The
+    near field is off on both sides (the device releases tiles that leave the
+    window; the reference keeps them by world cell)."""
+    scene = S.grid(res=128, seed=0xABC, puddles=6)
+    ox = S.snap_origin(0.0, 0.0, 128 * 0.2, 0.2)[0]
+    ref = O.Core(res=128, fine_res=64, layout=1, inner_par=engine == G.ENGINE_GRID, threads=1)
+    dev = G.Sheet(res=128, fine_res=64, layout=G.FINE_PER_TIRE, engine=engine)
+    for c in (ref, dev):
+        S.seed_core(c, scene)
+        c.set_near_field(False)
+        c.pour_water(ox - 1.0, ox + 2.0, -3.0, 3.0, 0.05)
+    v0 = dev.ledger()["total_m3"]
+    for k in range(20):
+        # The west tires 0.2 m inside the window's edge: their patches reach 0.44 m past it.
+        for t in S.tires_at(k * DT, speed=3.0, center=(ox + 0.95, 0.0), z0=-1.2):
+            ref.push_tire(**t)
+            dev.push_tire(**t)
+        ref.step(DT)
+        dev.step(DT, want_spray=False)
+    lr, ld = ref.ledger(), dev.ledger()
+    assert lr["frozen_water_m3"] > 0.0
+    assert abs(ld["frozen_water_m3"] - lr["frozen_water_m3"]) <= 1e-3 * lr["frozen_water_m3"]
+    for c in (ref, dev):
+        c.recenter(-3.0, 0.0)
+    lr, ld = ref.ledger(), dev.ledger()
+    assert abs(ld["frozen_water_m3"] - lr["frozen_water_m3"]) <= 1e-6 + 1e-3 * lr["frozen_water_m3"]
+    d = _pair_planes(ref, dev, ("water", "slurry"))
+    assert d["water"] <= 1e-4 and d["slurry"] <= 1e-4, d
+    led = dev.ledger()
+    assert abs(led["total_m3"] + led["cut_m3"] - led["opened_m3"] - v0) <= 1e-5 * v0
