@@ -138,7 +138,8 @@ struct Impl {
     bool spray_dirty = false;         // the spray count may be non-zero (a step with tires ran)
     // Spray.
     SprayRec* spray = nullptr;
-    double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3, [3] dry cut m3
+    double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3, [3] dry cut m3,
+                                      // [4] river reach bank m3 (FP64 twin of the reference's f32 bank)
     double* h_books = nullptr;
     int* h_counters = nullptr;
 };
@@ -1506,15 +1507,17 @@ int move_window(Patches& P, silt_sheet* s, int di, int dj, bool scroll) {
     return SILT_OK;
 }
 
-int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut) {
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut,
+                 double* reach) {
     Impl& M = I(P);
     SheetView W = view_of(s);
-    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 4 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 5 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
     FCK(cudaStreamSynchronize(W.st));
     *spray = M.h_books[0];
     *park_w = M.h_books[1];
     *park_s = M.h_books[2];
     if (cut) *cut = M.h_books[3];
+    if (reach) *reach = M.h_books[4];
     return SILT_OK;
 }
 
@@ -1592,9 +1595,9 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     FCK(cudaMalloc(&M->free_stack, NEAR_POOL * sizeof(int)));
     FCK(cudaMalloc(&M->counters, 8 * sizeof(int)));
     FCK(cudaMalloc(&M->spray, SPRAY_CAP * sizeof(SprayRec)));
-    FCK(cudaMalloc(&M->d_books, 4 * sizeof(double)));
-    FCK(cudaMemsetAsync(M->d_books, 0, 4 * sizeof(double), st));
-    FCK(cudaMallocHost(&M->h_books, 4 * sizeof(double)));
+    FCK(cudaMalloc(&M->d_books, 8 * sizeof(double)));
+    FCK(cudaMemsetAsync(M->d_books, 0, 8 * sizeof(double), st));
+    FCK(cudaMallocHost(&M->h_books, 8 * sizeof(double)));
     FCK(cudaMallocHost(&M->h_counters, 8 * sizeof(int)));
     ::silt::launch_dep(k_init_pool, dim3(launch_blocks(std::max<size_t>(n, NEAR_POOL))), dim3(256), 0, st, M->meta, M->free_stack, M->slot_map, n,
                                                                                M->counters);

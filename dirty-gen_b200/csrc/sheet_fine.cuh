@@ -102,7 +102,8 @@ int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::
                cudaStream_t st);
 int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_event* host, int cap, int* n_out);
 // FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
-int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr);
+int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr,
+                 double* reach = nullptr);
 // Device address of the books: [0] spray, [1] parked water, [2] parked slurry (m^3, FP64).
 double* books(Patches& P);
 // The window's parked cells (allocated on first use).

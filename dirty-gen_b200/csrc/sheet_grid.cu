@@ -160,7 +160,11 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
         float uu = P.u[g], vv = P.v[g];
         if (P.apply_cut && HS[s] < eps) { uu = 0.0f; vv = 0.0f; }
         if (P.soften_edge > 0) {
-            int d = min(min(gx, res - 1 - gx), min(gy, res - 1 - gy));
+            const int dx = min(gx, res - 1 - gx), dz = min(gy, res - 1 - gy);
+            // soften_border (src/fluid_core.rs:9594-9620): a reach's band keeps its current through the ends.
+            int d = min(dx, dz);
+            if (P.open_axis == 1 && gy >= P.open_c0 && gy < P.open_c1) d = dz;
+            else if (P.open_axis == 2 && gx >= P.open_c0 && gx < P.open_c1) d = dx;
             if (d < P.soften_edge) {
                 float t = (float)d / (float)P.soften_edge;
                 float w = t * t * (3.0f - 2.0f * t);

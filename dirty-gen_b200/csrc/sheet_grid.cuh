@@ -31,6 +31,8 @@ struct LayerParams {
     float cell, dt, vort, eps;
     int32_t project;       // divergence projection (cells wider than 2 cm)
     int32_t soften_edge;   // soft window band width in cells, 0 = off
+    int32_t open_axis;     // a river reach's band through the window ends: 0 none, 1 rows [open_c0, open_c1)
+    int32_t open_c0, open_c1;  // (reach along X), 2 columns (along Z); there only one edge distance softens
     int32_t apply_cut;     // zero u, v where h < eps on load (the previous dry cut)
     int32_t skip;          // layer has nothing to do this substep
 };

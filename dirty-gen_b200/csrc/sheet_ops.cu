@@ -359,12 +359,13 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
     ::silt::dep_wait();
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n) return;
-    out[6 * w + 0] = acc[w][0];
-    out[6 * w + 1] = acc[w][1];
-    out[6 * w + 2] = books[w][0];
-    out[6 * w + 3] = books[w][1];
-    out[6 * w + 4] = books[w][2];
-    out[6 * w + 5] = books[w][3];
+    out[7 * w + 0] = acc[w][0];
+    out[7 * w + 1] = acc[w][1];
+    out[7 * w + 2] = books[w][0];
+    out[7 * w + 3] = books[w][1];
+    out[7 * w + 4] = books[w][2];
+    out[7 * w + 5] = books[w][3];
+    out[7 * w + 6] = books[w][4];
 }
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st) {

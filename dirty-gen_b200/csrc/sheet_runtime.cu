@@ -25,6 +25,7 @@
 #include "../../include/silt_sheet.h"
 #include "../../include/silt_closure.h"
 #include "closure.cuh"
+#include "sheet_drivers.cuh"
 #include "sheet_fine.cuh"
 #include "launch_count.cuh"
 #include "sheet_grid.cuh"
@@ -124,6 +125,12 @@ struct silt_sheet {
     float* ow_scratch = nullptr;   // 2 n floats for the drivers' snapshots
     bool turbidity = false;        // FluidCore::set_turbidity_enabled (tracers are off this path)
     float center[2] = {0.0f, 0.0f};  // the chase point (set_center / recenter)
+    bool reach_on = false;           // FluidCore::set_river_reach
+    silt_river_reach reach;
+    float* d_reach_bank = nullptr;   // the reference's f32 bank (device)
+    bool wave_on = false;            // FluidCore::set_wave_maker
+    silt_wave_maker wave;
+    float wave_t = 0.0f;
     // Tire coupling (silt_set_coupling): nested sheets, none, or the learned closure.
     int coupling = SILT_COUPLING_NESTED;
     silt_closure* net = nullptr;
@@ -140,6 +147,7 @@ struct silt_sheet {
 namespace {
 
 float water_nu() { return silt::host::dynamic_viscosity(3, 1.0f); }
+void reach_band(const silt_sheet* s, int* axis, int* c0, int* c1);
 
 // The water row's viscosity entry: in open-water mode a negative entry, the
 // mobility itself (src/fluid_core.rs:8015-8017, sheet_mobility_for :169-172).
@@ -252,6 +260,7 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         P.eps = eps;
         P.project = cell > silt::host::kFineCell + 1.0e-6f;
         P.soften_edge = k == 0 ? cp.soften_edge : 0;
+        reach_band(s, &P.open_axis, &P.open_c0, &P.open_c1);
         P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
         P.skip = 0;
         if (l == 0) {
@@ -390,6 +399,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         J.mob_c = silt::host::sheet_mobility_for(nu_w);
         for (int k = 1; k <= 8; ++k) J.decay_c[k] = expf(-silt::host::sheet_damp(nu_w) * (dt / (float)k));
         J.soften_edge = s->cfg.soften_border ? std::max(s->res / 12, 2) : 0;
+        reach_band(s, &J.open_axis, &J.open_c0, &J.open_c1);
         J.has_sc2 = 1;
         J.active = 1;
     }
@@ -575,6 +585,7 @@ int silt_sheet_destroy(silt_sheet* s) {
         delete s->clos;
     }
     cudaFree(s->ow_scratch);
+    cudaFree(s->d_reach_bank);
     silt::fine::destroy(s->fine);
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
@@ -839,6 +850,73 @@ int open_water_step(silt_sheet* s, float dt) {
     return SILT_OK;
 }
 
+// The reach's band on the window (src/fluid_core.rs:8018-8033): 0 none, 1 a
+// band of rows (a reach along X), 2 a band of columns (along Z).
+void reach_band(const silt_sheet* s, int* axis, int* c0, int* c1) {
+    *axis = 0;
+    *c0 = *c1 = 0;
+    if (!s->reach_on) return;
+    const float cell = s->cfg.cell;
+    const float o = s->reach.along_z ? s->origin[0] : s->origin[1];
+    const float a = std::fmax(std::floor((s->reach.cross0 - o) / cell), 0.0f);
+    const float b = std::fmax(std::ceil((s->reach.cross1 - o) / cell), 0.0f);
+    *c0 = (int)std::fmin(a, 2.0e9f);
+    *c1 = (int)std::fmin(std::fmin(b, 2.0e9f), (float)s->res);
+    *axis = s->reach.along_z ? 2 : 1;
+}
+
+// drive_waves (src/fluid_core.rs:7420-7480): the step's scalars on the host.
+int wave_step(silt_sheet* s, float dt) {
+    if (!s->wave_on) return SILT_OK;
+    const silt_wave_maker& w = s->wave;
+    if (dt <= 0.0f || w.period_s <= 0.0f) return SILT_OK;
+    s->wave_t += dt;
+    const float len = std::hypot(w.dir_x, w.dir_z);
+    if (len < 1.0e-6f || !std::isfinite(len)) return SILT_OK;
+    silt::drivers::WaveStep q;
+    q.dx = w.dir_x / len;
+    q.dz = w.dir_z / len;
+    const float ramp = w.ramp_s > 0.0f ? silt::host::rclamp(s->wave_t / w.ramp_s, 0.0f, 1.0f) : 1.0f;
+    const float phase = 6.28318548f * s->wave_t / w.period_s;  // TAU in f32
+    q.stroke = w.amplitude_m_s * ramp * std::sin(phase);
+    q.pull = 1.0f - std::exp(-dt / 0.08f);
+    const float cell = s->cfg.cell;
+    q.span_x = std::fmax(w.x1 - w.x0, cell);
+    q.span_z = std::fmax(w.z1 - w.z0, cell);
+    auto idx = [](float f) { return (int)std::fmax(std::fmin(f, 2.0e9f), -2.0e9f); };
+    q.i0 = std::max(idx(std::floor((w.x0 - s->origin[0]) / cell)), 0);
+    q.i1 = std::min(idx(std::ceil((w.x1 - s->origin[0]) / cell)), s->res);
+    q.j0 = std::max(idx(std::floor((w.z0 - s->origin[1]) / cell)), 0);
+    q.j1 = std::min(idx(std::ceil((w.z1 - s->origin[1]) / cell)), s->res);
+    q.x0 = w.x0;
+    q.x1 = w.x1;
+    q.z0 = w.z0;
+    q.z1 = w.z1;
+    if (q.i1 <= q.i0 || q.j1 <= q.j0) return SILT_OK;
+    CK(silt::drivers::wave_step(silt::fine::view_of(s), q, s->st));
+    return SILT_OK;
+}
+
+// feed_reach (src/fluid_core.rs:7638-7745).
+int reach_step(silt_sheet* s) {
+    if (!s->reach_on) return SILT_OK;
+    silt::drivers::ReachStep r;
+    int axis;
+    reach_band(s, &axis, &r.c0, &r.c1);
+    if (r.c1 <= r.c0) return SILT_OK;
+    r.along_z = s->reach.along_z ? 1 : 0;
+    r.positive = s->reach.positive ? 1 : 0;
+    r.rows = std::min(std::max(s->reach.rows, 1), s->res / 4);
+    if (r.rows < 1) return SILT_OK;
+    r.dx = r.along_z ? 0.0f : (r.positive ? 1.0f : -1.0f);
+    r.dz = r.along_z ? (r.positive ? 1.0f : -1.0f) : 0.0f;
+    r.inlet_eta = s->reach.inlet_eta;
+    r.outlet_eta = s->reach.outlet_eta;
+    r.inlet_speed = s->reach.inlet_speed_m_s;
+    CK(silt::drivers::reach_step(silt::fine::view_of(s), r, s->d_reach_bank, silt::fine::books(s->fine), s->st));
+    return SILT_OK;
+}
+
 // The coupling of this step's tires: sets whether the nested patches are laid
 // and returns true when the learned closure corrects the step.
 bool closure_begin(silt_sheet* s) {
@@ -918,11 +996,13 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     rc = step_before_coarse(s, dt, ps, fo);
     if (rc) return rc;
     const clock::time_point t2 = clock::now();
+    if ((rc = wave_step(s, dt))) return rc;
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
     if (rc) return rc;
     if ((rc = open_water_step(s, dt))) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
+    if ((rc = reach_step(s))) return rc;
     if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
     if (out || n_out) {
@@ -1096,6 +1176,27 @@ int silt_set_surface_diffusion(silt_sheet* s, float m2_s) {
     return SILT_OK;
 }
 
+int silt_set_river_reach(silt_sheet* s, const silt_river_reach* reach) {
+    if (!s) return fail_arg("handle");
+    s->reach_on = reach != nullptr;
+    if (reach) {
+        s->reach = *reach;
+        if (!s->d_reach_bank) {
+            CK(cudaMalloc(&s->d_reach_bank, sizeof(float)));
+            CK(cudaMemsetAsync(s->d_reach_bank, 0, sizeof(float), s->st));
+        }
+    }
+    return SILT_OK;
+}
+
+int silt_set_wave_maker(silt_sheet* s, const silt_wave_maker* wave) {
+    if (!s) return fail_arg("handle");
+    s->wave_on = wave != nullptr;
+    if (wave) s->wave = *wave;
+    s->wave_t = 0.0f;
+    return SILT_OK;
+}
+
 int silt_set_turbidity_enabled(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     s->turbidity = on != 0;
@@ -1192,8 +1293,8 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut);
+    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -1207,8 +1308,9 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->frozen_slurry_m3 = park_s;
     out->spray_m3 = spray;
     out->opened_m3 = s->opened_m3;
-    out->total_m3 = w + sl + park_w + park_s + spray;
+    out->total_m3 = w + sl + park_w + park_s + spray + reach;
     out->cut_m3 = cut;
+    out->reach_m3 = reach;
     return SILT_OK;
 }
 
@@ -1539,7 +1641,7 @@ struct silt_batch {
     silt::closure::Runner* clos = nullptr;
     // Ledger gather: per window the depth sums and the books, one copy back.
     const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
-    double* d_ledgers = nullptr;            // 6 doubles per window
+    double* d_ledgers = nullptr;            // 7 doubles per window
     double* h_ledgers = nullptr;            // pinned
 };
 
@@ -1742,8 +1844,8 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->count, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemsetAsync(b->count, 0, 2 * sizeof(int), b->st);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 6 * (size_t)n * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 6 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 7 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 7 * (size_t)n * sizeof(double));
     if (e == cudaSuccess) {
         std::vector<const double*> src(2 * (size_t)n);
         for (int w = 0; w < n; ++w) {
@@ -1851,10 +1953,14 @@ int silt_batch_step(silt_batch* b, float dt) {
         }
     if ((rc = silt::fine::batch_launch(b->fine, fs, fp, dt, b->st))) return rc;
     const clock::time_point t1 = clock::now();
+    for (silt_sheet* s : b->sheets)
+        if ((rc = wave_step(s, dt))) return rc;
     if ((rc = batch_coarse(b, dt))) return rc;
     for (silt_sheet* s : b->sheets)
         if ((rc = open_water_step(s, dt))) return rc;
     if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
+    for (silt_sheet* s : b->sheets)
+        if ((rc = reach_step(s))) return rc;
     if (!net_win.empty()) {
         std::vector<silt::closure::ApplyJob> A(net_win.size());
         memset(A.data(), 0, A.size() * sizeof(silt::closure::ApplyJob));
@@ -1894,7 +2000,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         return SILT_OK;
     }
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
-    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 7 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)
         CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
@@ -1902,7 +2008,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         silt_sheet* s = b->sheets[w];
         int rc = check_substep_overflow(s);
         if (rc) return rc;
-        const double* g = b->h_ledgers + 6 * (size_t)w;
+        const double* g = b->h_ledgers + 7 * (size_t)w;
         const double area = (double)s->cfg.cell * (double)s->cfg.cell;
         silt_ledger& L = out[w];
         L.water_m3 = g[0] * area;
@@ -1911,7 +2017,8 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         L.frozen_water_m3 = g[3];
         L.frozen_slurry_m3 = g[4];
         L.opened_m3 = s->opened_m3;
-        L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3;
+        L.reach_m3 = g[6];
+        L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3 + L.reach_m3;
         L.cut_m3 = g[5];
     }
     return SILT_OK;

@@ -887,7 +887,12 @@ __device__ void cta_soften(const Job& J) {
     const int lo = min(edge, res) - 1, hi = min(max(edge, res - edge), res);
 #define SOFTEN_CELL                                                     \
     {                                                                   \
-        int d = min(min(i, res - 1 - i), min(j, res - 1 - j));          \
+        const int dx_ = min(i, res - 1 - i), dz_ = min(j, res - 1 - j); \
+        int d = min(dx_, dz_);                                          \
+        if (J.open_axis == 1 && j >= J.open_c0 && j < J.open_c1)        \
+            d = dz_;                                                    \
+        else if (J.open_axis == 2 && i >= J.open_c0 && i < J.open_c1)   \
+            d = dx_;                                                    \
         if (d < edge) {                                                 \
             float t = (float)d / (float)edge;                           \
             float w = t * t * (3.0f - 2.0f * t);                        \

@@ -41,6 +41,8 @@ struct Job {
     int32_t pace;          // fine-sheet pace (cells of 2 cm)
     int32_t inner_par;     // 1: the free operator (Jacobi confinement on boxes >= 48 x 32)
     int32_t soften_edge;   // soft window band in cells, 0 = off (step_pair's soften_border)
+    int32_t open_axis;     // a river reach's band through the window ends: 0 none, 1 rows [open_c0, open_c1)
+    int32_t open_c0, open_c1;  // (reach along X), 2 columns (along Z); there only one edge distance softens
     int32_t has_sc2;       // two far-apart boxes step on the second scratch set
     int32_t active;
     int32_t gs_iters;      // out: Gauss-Seidel passes used by the last box (diagnostics)

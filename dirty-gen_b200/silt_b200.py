@@ -42,7 +42,16 @@ class SprayEvent(ctypes.Structure):
 
 class Ledger(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3",
-                                               "spray_m3", "opened_m3", "total_m3", "cut_m3")]
+                                               "spray_m3", "opened_m3", "total_m3", "cut_m3", "reach_m3")]
+
+
+class RiverReach(ctypes.Structure):
+    _fields_ = [("along_z", _i), ("positive", _i), ("cross0", _f), ("cross1", _f), ("rows", _i),
+                ("inlet_eta", _f), ("outlet_eta", _f), ("inlet_speed_m_s", _f), ("inlet_turbidity", _f)]
+
+
+class WaveMaker(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("x0", "x1", "z0", "z1", "dir_x", "dir_z", "amplitude_m_s", "period_s", "ramp_s")]
 
 
 class GroundSample(ctypes.Structure):
@@ -119,6 +128,8 @@ def lib():
             "silt_set_open_water": [_p, _i, _f, _f, _f], "silt_set_surface_diffusion": [_p, _f],
             "silt_set_turbidity_enabled": [_p, _i], "silt_sample": [_p, _f, _f, ctypes.POINTER(GroundSample)],
             "silt_recenter": [_p, _f, _f], "silt_set_center": [_p, _f, _f],
+            "silt_set_river_reach": [_p, ctypes.POINTER(RiverReach)],
+            "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -291,6 +302,25 @@ class Sheet:
         ox, oz, ext = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         check(lib().silt_window_bounds(self.h, ctypes.byref(ox), ctypes.byref(oz), ctypes.byref(ext)), "window_bounds")
         return ox.value, oz.value
+
+    def set_river_reach(self, reach):
+        """FluidCore::set_river_reach: dict of RiverReach fields, or None."""
+        if reach is None:
+            check(lib().silt_set_river_reach(self.h, None), "set_river_reach")
+            return
+        r = RiverReach(int(reach.get("along_z", False)), int(reach.get("positive", True)), reach.get("cross0", 0.0),
+                       reach.get("cross1", 0.0), int(reach.get("rows", 1)), reach.get("inlet_eta", 0.0),
+                       reach.get("outlet_eta", 0.0), reach.get("inlet_speed_m_s", 0.0),
+                       reach.get("inlet_turbidity", 0.0))
+        check(lib().silt_set_river_reach(self.h, ctypes.byref(r)), "set_river_reach")
+
+    def set_wave_maker(self, wave):
+        """FluidCore::set_wave_maker: dict of WaveMaker fields, or None."""
+        if wave is None:
+            check(lib().silt_set_wave_maker(self.h, None), "set_wave_maker")
+            return
+        w = WaveMaker(*[wave.get(k, 0.0) for k, _ in WaveMaker._fields_])
+        check(lib().silt_set_wave_maker(self.h, ctypes.byref(w)), "set_wave_maker")
 
     def set_turbidity_enabled(self, on):
         check(lib().silt_set_turbidity_enabled(self.h, int(on)), "set_turbidity_enabled")

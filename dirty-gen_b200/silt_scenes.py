@@ -152,6 +152,21 @@ def basin(res=200, cell=0.2, level=0.3, speed=0.75, seed=0x9E3779B9, center=(0.0
                 u=u.ravel(), v=v.ravel(), moisture=np.full(n, 0.9, F), grain=np.full(n, SAND, np.uint8))
 
 
+def channel(res=200, cell=0.2, level=0.3, speed=0.5, seed=0x9E3779B9, center=(0.0, 0.0)):
+    """A river channel along x through the whole window: flat sand floor for
+    |z| < 4 m, banks rising 0.6 per metre beyond, a little bed noise, water
+    to `level` and a current of `speed` m/s along +x."""
+    extent = res * cell
+    origin = snap_origin(center[0], center[1], extent, cell)
+    x, z = cell_centres(res, cell, origin)
+    bed = (np.maximum(np.abs(z) - F(4.0), F(0.0)) * F(0.6) + F(0.05) * bed_noise(x, z, seed)).astype(F)
+    water = np.maximum(F(level) - bed, F(0.0)).astype(F)
+    u = np.where(water > F(0.0), F(speed), F(0.0)).astype(F)
+    n = res * res
+    return dict(res=res, cell=cell, origin=origin, center=center, bed=bed.ravel(), water=water.ravel(),
+                u=u.ravel(), v=np.zeros(n, F), moisture=np.full(n, 0.9, F), grain=np.full(n, SAND, np.uint8))
+
+
 def seed_basin(core, scene):
     """Seeds a sheet handle (oracle or device) with a basin scene."""
     core.read_substrate(scene["bed"], scene["moisture"], scene["grain"])

@@ -95,7 +95,23 @@ typedef struct {
      * has removed since creation; not in total_m3, which keeps the
      * reference's books. total_m3 + cut_m3 - opened_m3 is conserved. */
     double cut_m3;
+    /* The river reach's bank (FluidLedger::reach_m3, :6863), in total_m3. */
+    double reach_m3;
 } silt_ledger;
+
+/* src/fluid_core.rs:289-320 (`RiverReach`); inlet_turbidity is kept for the
+ * caller (suspended solids are off this path). */
+typedef struct {
+    int32_t along_z, positive;
+    float cross0, cross1;
+    int32_t rows;
+    float inlet_eta, outlet_eta, inlet_speed_m_s, inlet_turbidity;
+} silt_river_reach;
+
+/* src/fluid_core.rs:274-287 (`WaveMaker`). */
+typedef struct {
+    float x0, x1, z0, z1, dir_x, dir_z, amplitude_m_s, period_s, ramp_s;
+} silt_wave_maker;
 
 /* src/fluid_core.rs:440-448 (`GroundSample`); settled dust is off this path (0). */
 typedef struct {
@@ -252,6 +268,14 @@ int silt_set_open_water(silt_sheet* s, int32_t on, float mobility, float manning
 /* FluidCore::set_surface_diffusion (src/fluid_core.rs:5284-5286, applied by
  * diffuse_surface :7584-7636), m^2/s; 0 is off. */
 int silt_set_surface_diffusion(silt_sheet* s, float m2_s);
+/* FluidCore::set_river_reach (src/fluid_core.rs:5273-5275; NULL is None):
+ * an inlet and an outlet at the window ends (feed_reach :7638-7745, after the
+ * coarse pair) and a border band that lets the current through (:8018-8033). */
+int silt_set_river_reach(silt_sheet* s, const silt_river_reach* reach);
+/* FluidCore::set_wave_maker (src/fluid_core.rs:5306-5309; NULL is None):
+ * a paddle strip (drive_waves :7420-7480, before the coarse pair); restarts
+ * the paddle clock. */
+int silt_set_wave_maker(silt_sheet* s, const silt_wave_maker* wave);
 /* FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097): kept for the
  * caller; the tracers that read it are not on this path (flow.A stays 0). */
 int silt_set_turbidity_enabled(silt_sheet* s, int32_t on);

@@ -85,6 +85,10 @@ def lib():
         L.oracle_core_set_open_water.argtypes = [_p, _i, _f, _f, _f]
         L.oracle_core_set_surface_diffusion.argtypes = [_p, _f]
         L.oracle_core_recenter.argtypes = [_p, _f, _f]
+        L.oracle_core_set_river_reach.argtypes = [_p, _i, _i, _i, _f, _f, _i, _f, _f, _f]
+        L.oracle_core_reach_bank.argtypes = [_p]
+        L.oracle_core_reach_bank.restype = _f
+        L.oracle_core_set_wave_maker.argtypes = [_p, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f]
         L.oracle_core_origin.argtypes = [_p, _p]
         L.oracle_core_parked_count.argtypes = [_p]
         L.oracle_core_parked_count.restype = _i
@@ -263,6 +267,24 @@ class Core:
 
     def set_surface_diffusion(self, m2_s):
         lib().oracle_core_set_surface_diffusion(self.h, m2_s)
+
+    def set_river_reach(self, reach):
+        """reach: dict(along_z, positive, cross0, cross1, rows, inlet_eta, outlet_eta, inlet_speed_m_s) or None."""
+        r = reach or {}
+        lib().oracle_core_set_river_reach(self.h, int(reach is not None), int(r.get("along_z", False)),
+                                          int(r.get("positive", True)), r.get("cross0", 0.0), r.get("cross1", 0.0),
+                                          int(r.get("rows", 1)), r.get("inlet_eta", 0.0), r.get("outlet_eta", 0.0),
+                                          r.get("inlet_speed_m_s", 0.0))
+
+    def reach_bank_m3(self):
+        return lib().oracle_core_reach_bank(self.h)
+
+    def set_wave_maker(self, wave):
+        """wave: dict(x0, x1, z0, z1, dir_x, dir_z, amplitude_m_s, period_s, ramp_s) or None."""
+        w = wave or {}
+        lib().oracle_core_set_wave_maker(self.h, int(wave is not None), w.get("x0", 0.0), w.get("x1", 0.0),
+                                         w.get("z0", 0.0), w.get("z1", 0.0), w.get("dir_x", 0.0), w.get("dir_z", 0.0),
+                                         w.get("amplitude_m_s", 0.0), w.get("period_s", 0.0), w.get("ramp_s", 0.0))
 
     def recenter(self, cx, cz):
         lib().oracle_core_recenter(self.h, cx, cz)

@@ -902,7 +902,9 @@ void step_sheet_eps(float* h, float* u, float* v, const float* bed, const float*
 }
 
 // src/fluid_core.rs:9594-9622 (no reach band)
-void soften_border(float* u, float* v, usize res) {
+// open_axis: -1 none; 0 a reach along X (its band [c0, c1) of rows keeps its
+// current through the window ends: only the row distance counts); 1 along Z.
+void soften_border(float* u, float* v, usize res, int open_axis = -1, usize c0 = 0, usize c1 = 0) {
     usize edge = std::max(res / 12, (usize)2);
     usize ends = std::min(edge, res);
     for (usize j = 0; j < res; ++j) {
@@ -911,6 +913,8 @@ void soften_border(float* u, float* v, usize res) {
         auto visit = [&](usize i) {
             usize di = std::min(i, res - 1 - i), dj = std::min(j, res - 1 - j);
             usize d = std::min(di, dj);
+            if (open_axis == 0 && j >= c0 && j < c1) d = dj;
+            else if (open_axis == 1 && i >= c0 && i < c1) d = di;
             if (d >= edge) return;
             float t = (float)d / (float)edge;
             float w = t * t * (3.0f - 2.0f * t);
@@ -1050,6 +1054,16 @@ struct Core {
     bool open_water = false;
     float ow_mobility = 0.0f, ow_manning = 0.0f, ow_eddy = 0.0f;
     float surface_diffusion = 0.0f;
+    // src/fluid_core.rs:289-320 RiverReach (inlet turbidity is off this path),
+    // :274-287 WaveMaker.
+    bool reach_on = false;
+    bool reach_along_z = false, reach_positive = true;
+    float reach_cross0 = 0, reach_cross1 = 0, reach_inlet_eta = 0, reach_outlet_eta = 0, reach_speed = 0;
+    usize reach_rows = 1;
+    float reach_bank_m3 = 0.0f;
+    bool wave_on = false;
+    float wave_x0 = 0, wave_x1 = 0, wave_z0 = 0, wave_z1 = 0, wave_dx = 0, wave_dz = 0, wave_amp = 0, wave_period = 0,
+          wave_ramp = 0, wave_t = 0;
 
     explicit Core(const oracle_core_cfg& c) : cfg(c) {
         res = (usize)c.res;
@@ -1557,8 +1571,17 @@ struct Core {
         float cap = fine ? fine_sub_cap : 8.0f;
         int pace = fine ? fine_pace : 0;
         if (!fine) {
+            // An open reach keeps its current through the window ends (src/fluid_core.rs:8018-8033).
+            int open_axis = -1;
+            usize oc0 = 0, oc1 = 0;
+            if (reach_on) {
+                float o = reach_along_z ? origin[0] : origin[1];
+                oc0 = f2usize(rmax(floorf((reach_cross0 - o) / cfg.cell), 0.0f));
+                oc1 = std::min(f2usize(rmax(ceilf((reach_cross1 - o) / cfg.cell), 0.0f)), res);
+                open_axis = reach_along_z ? 1 : 0;
+            }
             auto run_water = [&]() {
-                if (cfg.soften) soften_border(uw.data(), vw.data(), res);
+                if (cfg.soften) soften_border(uw.data(), vw.data(), res, open_axis, oc0, oc1);
                 step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0);
             };
             auto run_slurry = [&]() {
@@ -1569,7 +1592,7 @@ struct Core {
                             usize idx = j * res + i;
                             nu_s[idx] = dynamic_viscosity(grain[idx], moisture[idx]);
                         }
-                if (cfg.soften) soften_border(us.data(), vs.data(), res);
+                if (cfg.soften) soften_border(us.data(), vs.data(), res, open_axis, oc0, oc1);
                 step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0);
             };
             // src/fluid_core.rs:8127-8131: the two sheets on two workers.
@@ -1640,10 +1663,12 @@ struct Core {
             if (fine_held_at(p.x, p.z)) continue;
             push_on(p, water.data(), slurry.data(), uw.data(), vw.data(), us.data(), vs.data(), res, cfg.cell, origin);
         }
+        drive_waves(dt);
         step_pair(dt, false);
         bed_friction(dt);
         diffuse_surface(dt);
         if (!ps.empty()) peel(ps, water.data(), uw.data(), vw.data(), res, cfg.cell, origin, true, spray);
+        feed_reach();
         for (const auto& s : spray) spray_m3 += s.volume;
         return spray;
     }
@@ -1747,6 +1772,116 @@ struct Core {
             float d = delta[idx];
             if (d != 0.0f && finite(d)) water[idx] = rmax(water[idx] + d, 0.0f);
         }
+    }
+
+    // src/fluid_core.rs:7420-7480 drive_waves: the paddle strip's water
+    // velocity relaxes toward the stroke, tapered over the strip's outer
+    // quarters.
+    void drive_waves(float dt) {
+        if (!wave_on) return;
+        if (dt <= 0.0f || wave_period <= 0.0f) return;
+        wave_t += dt;
+        float len = hypotf(wave_dx, wave_dz);
+        if (len < 1.0e-6f || !finite(len)) return;
+        float dx = wave_dx / len, dz = wave_dz / len;
+        float ramp = wave_ramp > 0.0f ? rmin(rmax(wave_t / wave_ramp, 0.0f), 1.0f) : 1.0f;
+        float phase = 6.28318548f * wave_t / wave_period;
+        float stroke = wave_amp * ramp * sinf(phase);
+        float pull = 1.0f - expf(-dt / 0.08f);
+        float cell = cfg.cell;
+        float span_x = rmax(wave_x1 - wave_x0, cell), span_z = rmax(wave_z1 - wave_z0, cell);
+        long i0 = std::max((long)floorf((wave_x0 - origin[0]) / cell), 0L);
+        long i1 = std::min((long)ceilf((wave_x1 - origin[0]) / cell), (long)res);
+        long j0 = std::max((long)floorf((wave_z0 - origin[1]) / cell), 0L);
+        long j1 = std::min((long)ceilf((wave_z1 - origin[1]) / cell), (long)res);
+        for (long j = j0; j < j1; ++j)
+            for (long i = i0; i < i1; ++i) {
+                float x, z;
+                coarse_xz((usize)i, (usize)j, x, z);
+                if (x < wave_x0 || x > wave_x1 || z < wave_z0 || z > wave_z1) continue;
+                usize idx = (usize)j * res + (usize)i;
+                if (water[idx] < 0.02f || !finite(water[idx])) continue;
+                float tx = rmin(rmax(rmin(x - wave_x0, wave_x1 - x) / (0.25f * span_x), 0.0f), 1.0f);
+                float tz = rmin(rmax(rmin(z - wave_z0, wave_z1 - z) / (0.25f * span_z), 0.0f), 1.0f);
+                float k = pull * rmin(tx, tz);
+                float u = uw[idx], v = vw[idx];
+                float along = u * dx + v * dz;
+                float d = (stroke - along) * k;
+                float nu = u + d * dx, nv = v + d * dz;
+                if (finite(nu) && finite(nv)) {
+                    uw[idx] = nu;
+                    vw[idx] = nv;
+                }
+            }
+    }
+
+    // src/fluid_core.rs:7638-7745 feed_reach: the outlet rows hold their stage
+    // and copy the interior velocity, banking the excess; the inlet rows fill
+    // from the bank toward their stage and push the water in.
+    void feed_reach() {
+        if (!reach_on) return;
+        usize rows = std::min(std::max(reach_rows, (usize)1), res / 4);
+        float cell = cfg.cell, area = cell * cell;
+        float co = reach_along_z ? origin[0] : origin[1];
+        usize c0 = f2usize(rmax(floorf((reach_cross0 - co) / cell), 0.0f));
+        float c1f = ceilf((reach_cross1 - co) / cell);
+        usize c1 = f2usize(rmin(rmax(c1f, 0.0f), (float)res));
+        if (c1 <= c0) return;
+        auto at = [&](usize along, usize cross) { return reach_along_z ? along * res + cross : cross * res + along; };
+        auto row = [&](usize k) { return reach_positive ? k : res - 1 - k; };
+        float dx = reach_along_z ? 0.0f : (reach_positive ? 1.0f : -1.0f);
+        float dz = reach_along_z ? (reach_positive ? 1.0f : -1.0f) : 0.0f;
+        usize first_out = res - rows;
+        for (usize cross = c0; cross < c1; ++cross) {
+            usize src = at(row(first_out - 1), cross);
+            float su = uw[src], sv = vw[src];
+            float along = rmax(su * dx + sv * dz, 0.0f);
+            for (usize k = first_out; k < res; ++k) {
+                usize idx = at(row(k), cross);
+                float target = rmax(reach_outlet_eta - bed[idx], 0.0f);
+                float h = water[idx];
+                if (!finite(h) || target <= 0.0f) continue;
+                if (h > target) {
+                    reach_bank_m3 += (h - target) * area;
+                    water[idx] = target;
+                } else if (reach_bank_m3 > 0.0f) {
+                    float add = rmin(target - h, reach_bank_m3 / area);
+                    water[idx] = h + add;
+                    reach_bank_m3 -= add * area;
+                }
+                if (finite(su) && finite(sv)) {
+                    float cross_v = reach_along_z ? su : sv;
+                    if (reach_along_z) {
+                        uw[idx] = cross_v;
+                        vw[idx] = along * dz;
+                    } else {
+                        uw[idx] = along * dx;
+                        vw[idx] = cross_v;
+                    }
+                }
+            }
+        }
+        float deep = 0.0f;
+        for (usize cross = c0; cross < c1; ++cross) deep = rmax(deep, rmax(reach_inlet_eta - bed[at(row(0), cross)], 0.0f));
+        if (deep <= 0.0f) return;
+        for (usize k = 0; k < rows; ++k)
+            for (usize cross = c0; cross < c1; ++cross) {
+                usize idx = at(row(k), cross);
+                float target = rmax(reach_inlet_eta - bed[idx], 0.0f);
+                float h = water[idx];
+                if (!finite(h) || target <= 0.0f) continue;
+                if (h > target) {
+                    reach_bank_m3 += (h - target) * area;
+                    water[idx] = target;
+                } else if (reach_bank_m3 > 0.0f) {
+                    float add = rmin(target - h, reach_bank_m3 / area);
+                    water[idx] = h + add;
+                    reach_bank_m3 -= add * area;
+                }
+                float speed = reach_speed * sqrtf(rmin(rmax(water[idx] / deep, 0.0f), 1.0f));
+                uw[idx] = speed * dx;
+                vw[idx] = speed * dz;
+            }
     }
 
     // src/fluid_core.rs:4797-4805 park_slot (sheet fields).
@@ -2162,6 +2297,31 @@ void oracle_core_set_open_water(void* cp, int on, float mobility, float manning_
     C.ow_mobility = rmin(rmax(mobility, 0.0f), 1.0f);
     C.ow_manning = rmax(manning_n, 0.0f);
     C.ow_eddy = rmax(eddy_m2_s, 0.0f);
+}
+// src/fluid_core.rs:5273-5275 set_river_reach (on = 0: None).
+void oracle_core_set_river_reach(void* cp, int on, int along_z, int positive, float cross0, float cross1, int rows,
+                                 float inlet_eta, float outlet_eta, float inlet_speed) {
+    Core& C = *(Core*)cp;
+    C.reach_on = on != 0;
+    C.reach_along_z = along_z != 0;
+    C.reach_positive = positive != 0;
+    C.reach_cross0 = cross0;
+    C.reach_cross1 = cross1;
+    C.reach_rows = rows > 0 ? (usize)rows : 0;
+    C.reach_inlet_eta = inlet_eta;
+    C.reach_outlet_eta = outlet_eta;
+    C.reach_speed = inlet_speed;
+}
+float oracle_core_reach_bank(void* cp) { return ((Core*)cp)->reach_bank_m3; }
+// src/fluid_core.rs:5306-5309 set_wave_maker (restarts the paddle clock).
+void oracle_core_set_wave_maker(void* cp, int on, float x0, float x1, float z0, float z1, float dir_x, float dir_z,
+                                float amplitude, float period, float ramp) {
+    Core& C = *(Core*)cp;
+    C.wave_on = on != 0;
+    C.wave_x0 = x0; C.wave_x1 = x1; C.wave_z0 = z0; C.wave_z1 = z1;
+    C.wave_dx = dir_x; C.wave_dz = dir_z;
+    C.wave_amp = amplitude; C.wave_period = period; C.wave_ramp = ramp;
+    C.wave_t = 0.0f;
 }
 // src/fluid_core.rs:5409-5421 recenter.
 void oracle_core_recenter(void* cp, float cx, float cz) { ((Core*)cp)->recenter(cx, cz); }

@@ -274,3 +274,34 @@ def test_patch_water_outside_the_window_is_parked_and_restored(engine):
     assert d["water"] <= 1e-4 and d["slurry"] <= 1e-4, d
     led = dev.ledger()
     assert abs(led["total_m3"] + led["cut_m3"] - led["opened_m3"] - v0) <= 1e-5 * v0
+
+
+@pytest.mark.parametrize("engine", [G.ENGINE_WINDOW, G.ENGINE_GRID])
+def test_river_reach_and_wave_maker_match_oracle(engine):
+    """A river channel through the window with the reach's inlet and outlet
+    (src/fluid_core.rs:7638-7745), a paddle strip (:7420-7480) and open water:
+    depth within 1e-4 m of the oracle after 60 steps, the reach bank within
+    f32 rounding of the oracle's, and the FP64 books closed (the bank is on
+    the ledger)."""
+    sc = S.channel()
+    reach = dict(along_z=False, positive=True, cross0=-4.0, cross1=4.0, rows=4, inlet_eta=0.3, outlet_eta=0.28,
+                 inlet_speed_m_s=0.75)
+    wave = dict(x0=5.0, x1=7.0, z0=-3.0, z1=3.0, dir_x=1.0, dir_z=0.0, amplitude_m_s=0.3, period_s=0.5, ramp_s=0.2)
+    dev = G.Sheet(res=sc["res"], cell=sc["cell"], engine=engine)
+    ref = O.Core(threads=1, inner_par=engine == G.ENGINE_GRID)
+    for c in (dev, ref):
+        S.seed_basin(c, sc)
+        c.set_open_water(True, 1.0, 0.035, 0.06)
+        c.set_river_reach(reach)
+        c.set_wave_maker(wave)
+    v0 = dev.ledger()
+    for _ in range(60):
+        dev.step(DT, want_spray=False)
+        ref.step(DT)
+    d = _pair_planes(ref, dev, ("water", "uw", "vw"))
+    assert d["water"] <= 1e-4 and d["uw"] <= 1e-3, d
+    led = dev.ledger()
+    assert led["reach_m3"] > 0.0
+    assert abs(led["reach_m3"] - ref.reach_bank_m3()) <= 1e-4 * led["reach_m3"] + 1e-6
+    gap = abs(led["total_m3"] + led["cut_m3"] - v0["total_m3"] - v0["cut_m3"]) / v0["total_m3"]
+    assert gap < 1e-6, gap
