@@ -1,0 +1,84 @@
+// Exhaustive check of the fixed-divisor division against IEEE division.
+#include "sheet_div.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "launch_count.cuh"
+
+namespace silt {
+
+namespace {
+
+__global__ void k_check_div(float d, float r, unsigned long long* counts) {
+    ::silt::dep_wait();
+    unsigned long long local[6] = {0, 0, 0, 0, 0, 0};
+    const FixedDiv D{d, r, 1};
+    const unsigned long long total = 1ull << 32;
+    for (unsigned long long b = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; b < total;
+         b += (unsigned long long)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((unsigned int)b);
+        const float want = x / d;
+        const float got = fdiv(x, D);
+        const bool same = __float_as_uint(want) == __float_as_uint(got) || (want != want && got != got);
+        if (same) continue;
+        local[0] += 1;
+        const float ax = fabsf(x);
+        if (ax == 0.0f) local[1] += 1;
+        else if (ax < 1.17549435e-38f) local[2] += 1;
+        else if (!(ax <= 3.40282347e38f)) local[3] += 1;
+        else if (fabsf(want) < 1.17549435e-38f) local[4] += 1;
+        else local[5] += 1;
+    }
+    for (int k = 0; k < 6; ++k) {
+        unsigned long long v = local[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&counts[k], v);
+    }
+}
+
+std::mutex g_div_mutex;
+std::map<std::pair<int, unsigned int>, int> g_div_exact;  // (device, bits of d) -> exact
+
+}  // namespace
+
+cudaError_t check_fixed_div(float d, unsigned long long* counts6, cudaStream_t st) {
+    unsigned long long* dc = nullptr;
+    cudaError_t e = cudaMalloc(&dc, 6 * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(dc, 0, 6 * sizeof(unsigned long long), st);
+    const float r = 1.0f / d;
+    if (e == cudaSuccess) {
+        ::silt::launch_dep(k_check_div, dim3(148 * 16), dim3(256), 0, st, d, r, dc);
+        ::silt::count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counts6, dc, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dc);
+    return e;
+}
+
+FixedDiv fixed_div_for(float d, cudaStream_t st) {
+    FixedDiv D{d, 1.0f / d, 0};
+    if (!(d > 0.0f) || !std::isfinite(d)) return D;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    unsigned int bits;
+    memcpy(&bits, &d, sizeof bits);
+    std::lock_guard<std::mutex> lock(g_div_mutex);
+    const auto key = std::make_pair(dev, bits);
+    auto it = g_div_exact.find(key);
+    if (it == g_div_exact.end()) {
+        unsigned long long c[6] = {1, 0, 0, 0, 0, 0};
+        const int exact = check_fixed_div(d, c, st) == cudaSuccess && c[0] == 0 ? 1 : 0;
+        it = g_div_exact.emplace(key, exact).first;
+    }
+    D.exact = it->second;
+    return D;
+}
+
+}  // namespace silt

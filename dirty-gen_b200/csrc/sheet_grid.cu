@@ -142,8 +142,7 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
     float* HS = sm + 6 * FPLANE; // depth
     float* WQ = sm + 7 * FPLANE; // vorticity (radius 5), then q (radius 1)
     const int ox = tx0 - FH, oy = ty0 - FH;
-    const float cell = P.cell, dt = P.dt, eps = P.eps;
-    const float two = 2.0f * cell;
+    const float dt = P.dt, eps = P.eps;
 #define NX(d) (EDGE ? (gy - oy) * FW + (clampi(gx + (d), 0, res - 1) - ox) : s + (d))
 #define NZ(d) (EDGE ? (clampi(gy + (d), 0, res - 1) - oy) * FW + (gx - ox) : s + (d) * FW)
 
@@ -197,8 +196,8 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
     //    (src/fluid_core.rs:2234-2253).
     region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         if (HS[s] > eps) {
-            float px = (PB[NX(1)] - PB[NX(-1)]) / two;
-            float pz = (PB[NZ(1)] - PB[NZ(-1)]) / two;
+            float px = fdiv(PB[NX(1)] - PB[NX(-1)], P.div_two);
+            float pz = fdiv(PB[NZ(1)] - PB[NZ(-1)], P.div_two);
             float mob = cell_mob(P, g);
             U[s] += -kGravity * px * mob * dt;
             V[s] += -kGravity * pz * mob * dt;
@@ -208,8 +207,8 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
     // 5. Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
     if (P.vort > 0.0f) {
         region<EDGE, 5, 5>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-            float dvdx = (V[NX(1)] - V[NX(-1)]) / two;
-            float dudz = (U[NZ(1)] - U[NZ(-1)]) / two;
+            float dvdx = fdiv(V[NX(1)] - V[NX(-1)], P.div_two);
+            float dudz = fdiv(U[NZ(1)] - U[NZ(-1)], P.div_two);
             WQ[s] = dvdx - dudz;
         });
         __syncthreads();
@@ -221,8 +220,8 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
                 if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
                     float wxp = fabsf(WQ[NX(1)]), wxm = fabsf(WQ[NX(-1)]);
                     float wzp = fabsf(WQ[NZ(1)]), wzm = fabsf(WQ[NZ(-1)]);
-                    float nx_ = (wxp - wxm) / two;
-                    float nz_ = (wzp - wzm) / two;
+                    float nx_ = fdiv(wxp - wxm, P.div_two);
+                    float nz_ = fdiv(wzp - wzm, P.div_two);
                     float du = P.vort * dt * (-nz_ * w);
                     float dv = P.vort * dt * (nx_ * w);
                     if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
@@ -239,12 +238,12 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
         //    (src/fluid_core.rs:1992-2003).
         region<EDGE, 3, 3>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const int sxp = NX(1), sxm = NX(-1), szp = NZ(1), szm = NZ(-1);
-            float ux = (U[sxp] - U[sxm]) / (2.0f * cell);
-            float vz = (V[szp] - V[szm]) / (2.0f * cell);
+            float ux = fdiv(U[sxp] - U[sxm], P.div_two);
+            float vz = fdiv(V[szp] - V[szm], P.div_two);
             float div = ux + vz;
             float lsum = E[sxp] + E[sxm] + E[szp] + E[szm] - 4.0f * E[s];
-            float lap_h = lsum / (cell * cell);
-            float overload = 1.0f + rclamp(cell_nu(P, g) / 231.0f, 0.0f, 6.0f);
+            float lap_h = fdiv(lsum, P.div_cell2);
+            float overload = 1.0f + rclamp(fdiv(cell_nu(P, g), P.div_231), 0.0f, 6.0f);
             PB[s] = div * overload - 0.015f * overload * lap_h;
         });
         __syncthreads();
@@ -272,8 +271,8 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
         float uu = U[s], vv = V[s];
         if (HS[s] > eps) {
             if (P.project) {
-                float qx = (WQ[NX(1)] - WQ[NX(-1)]) / (2.0f * cell);
-                float qz = (WQ[NZ(1)] - WQ[NZ(-1)]) / (2.0f * cell);
+                float qx = fdiv(WQ[NX(1)] - WQ[NX(-1)], P.div_two);
+                float qz = fdiv(WQ[NZ(1)] - WQ[NZ(-1)], P.div_two);
                 uu += 0.012f * dt * qx;
                 vv += 0.012f * dt * qz;
             }
@@ -457,7 +456,8 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
 #define TIDX(gx, gy) (((gy) - oy) * TW + ((gx) - ox))
     const int ry0 = max(0, ty0 - 2), ry1 = min(res, ty1 + 1);
     const int cx0 = max(0, tx0 - 2), cx1 = min(res, tx1 + 1);
-    const float cell = P.cell, dt = P.dt;
+    const FixedDiv& cell = P.div_cell;
+    const float dt = P.dt;
     const bool with_bed = P.bank_bed != nullptr;
     const uint8_t* gate = P.gate;
     trows<EDGE, TT + 3, TT + 3>(cx0, cx1, ry0, ry1, [&](int gx, int gy) {

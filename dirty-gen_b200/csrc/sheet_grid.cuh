@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "sheet_div.cuh"
+
 namespace silt {
 
 enum NuMode : int32_t {
@@ -29,6 +31,9 @@ struct LayerParams {
     float nu_c, mob_c, decay_c;  // NU_CONST: viscosity, mobility and damping factor
     int32_t res;
     float cell, dt, vort, eps;
+    FixedDiv div_two;      // 2 * cell (the centred differences)
+    FixedDiv div_cell2;    // cell * cell (the laplacian)
+    FixedDiv div_231;      // 231 (the projection's overload)
     int32_t project;       // divergence projection (cells wider than 2 cm)
     int32_t soften_edge;   // soft window band width in cells, 0 = off
     int32_t open_axis;     // a river reach's band through the window ends: 0 none, 1 rows [open_c0, open_c1)
@@ -86,6 +91,7 @@ struct TransportParams {
     double cut_area;          // m^2 of one cell for that book
     int32_t res;
     float cell, dt, eps;
+    FixedDiv div_cell;        // cell (the face fraction speed dt / cell)
     int32_t skip;
 };
 

@@ -5,6 +5,8 @@
 #pragma once
 #include <cstdint>
 
+#include "sheet_div.cuh"
+
 namespace silt {
 
 constexpr float kGravity = 9.81f;          // src/fluid_core.rs:111
@@ -63,16 +65,21 @@ __device__ __forceinline__ float finite_speed(float v, float lim) {
 }
 __device__ __forceinline__ float finite0(float v) { return finite_f(v) ? v : 0.0f; }
 
+__device__ __forceinline__ float divide_by(float x, float d) { return x / d; }
+__device__ __forceinline__ float divide_by(float x, const FixedDiv& d) { return fdiv(x, d); }
+
 // src/fluid_core.rs:2867-2911 open_edge_dh: depth one donor gives across one
-// edge, 0 where the serial loop would skip the edge.
+// edge, 0 where the serial loop would skip the edge. `cell` is a float or a
+// FixedDiv of the cell width.
+template <class Cell>
 __device__ __forceinline__ float open_edge_dh(bool with_bed, float hd, float hr, float remd, uint8_t gate_r,
-                                              float bed_d, float bed_r, float speed, float dt, float cell,
+                                              float bed_d, float bed_r, float speed, float dt, const Cell& cell,
                                               float frac_cap) {
     bool live = !(fabsf(speed) < 1.0e-5f);
     bool bank = with_bed && hr <= 1.0e-6f && bed_r > bed_d + hd + 1.0e-3f;
     float room = hd - remd;
     bool gate_shut = gate_r == 0 && hr <= 1.0e-6f;
-    float frac = fminf(fabsf(speed) * dt / cell, frac_cap);
+    float frac = fminf(divide_by(fabsf(speed) * dt, cell), frac_cap);
     float dh = fminf(hd * frac, room);
     bool ok = live & !bank & !(room <= 1.0e-8f) & !gate_shut & !(dh <= 1.0e-8f);
     return ok ? dh : 0.0f;

@@ -102,6 +102,10 @@ struct silt_sheet {
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<cudaEvent_t> ev_used;   // groups of three: start, after force, after transport
+    // The grid engine's divisors (2 cell, cell^2, 231, cell), set at
+    // creation; each is exact only once checked against IEEE division for
+    // every float.
+    silt::FixedDiv div_two{}, div_cell2{}, div_231{}, div_cell{};
     silt_step_parts parts;
     // Window engine for the coarse pair (SILT_ENGINE_WINDOW).
     int engine = SILT_ENGINE_GRID;
@@ -255,6 +259,9 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         P.v_out = s->v[l][nxt];
         P.res = res;
         P.cell = cell;
+        P.div_two = s->div_two;
+        P.div_cell2 = s->div_cell2;
+        P.div_231 = s->div_231;
         P.dt = dt;  // the device divides by its count when it decides one
         P.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
         P.eps = eps;
@@ -288,6 +295,7 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         Q.cut_area = (double)cell * (double)cell;
         Q.res = res;
         Q.cell = cell;
+        Q.div_cell = s->div_cell;
         Q.dt = dt;
         Q.eps = eps;
         Q.skip = 0;
@@ -567,6 +575,12 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         silt_sheet_destroy(s);
         return rc;
     }
+    // The divisors of the grid engine's kernels, as they divide (2 * cell,
+    // cell * cell, 231, cell).
+    s->div_two = silt::fixed_div_for(2.0f * cfg->cell, s->st);
+    s->div_cell2 = silt::fixed_div_for(cfg->cell * cfg->cell, s->st);
+    s->div_231 = silt::fixed_div_for(231.0f, s->st);
+    s->div_cell = silt::fixed_div_for(cfg->cell, s->st);
     e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) {
         silt_sheet_destroy(s);
@@ -1489,6 +1503,12 @@ int silt_sheet_copy_state(silt_sheet* dst, silt_sheet* src) {
     return tiles_dirty(dst);
 }
 
+int silt_check_fixed_division(float d, unsigned long long* counts6, void* stream) {
+    if (!counts6 || !(d > 0.0f) || !std::isfinite(d)) return fail_arg("check_fixed_division");
+    CK(silt::check_fixed_div(d, counts6, (cudaStream_t)stream));
+    return SILT_OK;
+}
+
 int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
                           float* origin2) {
     if (!s || (n > 0 && !tires) || !host) return fail_arg("fine_water_debug");
@@ -2181,6 +2201,10 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         P.nu_mode = silt::NU_PLANE;
         P.res = res;
         P.cell = cell;
+        // The free operator divides by IEEE division (no check runs here).
+        P.div_two = silt::FixedDiv{2.0f * cell, 1.0f / (2.0f * cell), 0};
+        P.div_cell2 = silt::FixedDiv{cell * cell, 1.0f / (cell * cell), 0};
+        P.div_231 = silt::FixedDiv{231.0f, 1.0f / 231.0f, 0};
         P.dt = dts;
         P.vort = vorticity;
         P.eps = 1.0e-6f;
@@ -2193,6 +2217,7 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         Q.gate = gate;
         Q.res = res;
         Q.cell = cell;
+        Q.div_cell = silt::FixedDiv{cell, 1.0f / cell, 0};
         Q.dt = dts;
         Q.eps = 1.0e-6f;
         F.lay[1].skip = 1;

@@ -130,6 +130,7 @@ def lib():
             "silt_recenter": [_p, _f, _f], "silt_set_center": [_p, _f, _f],
             "silt_set_river_reach": [_p, ctypes.POINTER(RiverReach)],
             "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
+            "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -389,6 +390,15 @@ def step_sheet_device(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch,
     """The free one-sheet operator on device pointers (ints)."""
     return check(lib().silt_step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream),
                  "step_sheet")
+
+
+def check_fixed_division(d, stream=None):
+    """Mismatch counts of the grid engine's fixed-divisor division by d against
+    IEEE division over every float x: (all, x zero, x subnormal, x inf/NaN,
+    subnormal or zero quotient, rest)."""
+    counts = (ctypes.c_ulonglong * 6)()
+    check(lib().silt_check_fixed_division(float(d), counts, stream), "check_fixed_division")
+    return tuple(int(c) for c in counts)
 
 
 class Batch:

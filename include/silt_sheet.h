@@ -205,6 +205,15 @@ int silt_plane_device(silt_sheet* s, int32_t which, void** out);
  * moisture, grain) into dst (same size and device); dst's nested patches and
  * near field are untouched. Used to step one state two ways. */
 int silt_sheet_copy_state(silt_sheet* dst, silt_sheet* src);
+/* Diagnostic of the grid engine's division by a fixed divisor d > 0 (x times
+ * the rounded reciprocal, refined once by the FMA remainder): counts of float
+ * x, over all 2^32 bit patterns, whose result differs from IEEE x / d, written
+ * to the host array counts6: [0] all, [1] x zero, [2] x subnormal, [3] x
+ * infinite or NaN, [4] a subnormal or zero IEEE quotient, [5] the rest. The
+ * engine divides by the product only for divisors whose [0] is 0 (checked
+ * once per divisor at silt_sheet_create). No counterpart in the reference,
+ * which divides by IEEE division throughout. Synchronises `stream`. */
+int silt_check_fixed_division(float d, unsigned long long* counts6, void* stream);
 /* FluidCore::fine_water_debug (src/fluid_core/near.rs:341): lays the patch
  * down for these tires, copies patch `patch` (fine_res^2 floats) and its
  * origin, and packs it back. */
