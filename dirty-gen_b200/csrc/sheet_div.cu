@@ -81,4 +81,13 @@ FixedDiv fixed_div_for(float d, cudaStream_t st) {
     return D;
 }
 
+CellDivisors cell_divisors(float cell, cudaStream_t st) {
+    CellDivisors D;
+    D.two = fixed_div_for(2.0f * cell, st);
+    D.cell2 = fixed_div_for(cell * cell, st);
+    D.d231 = fixed_div_for(231.0f, st);
+    D.cell = fixed_div_for(cell, st);
+    return D;
+}
+
 }  // namespace silt

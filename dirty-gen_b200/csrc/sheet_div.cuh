@@ -32,6 +32,26 @@ __device__ __forceinline__ float fdiv(float x, const FixedDiv& D) {
     return copysignf(__fmaf_rn(rem, D.r, q), x);
 }
 
+// The divisors of one sheet's step for its cell width: 2 cell (the centred
+// differences), cell^2 (the laplacian), 231 (the projection's overload) and
+// cell (the face fraction speed dt / cell).
+struct CellDivisors {
+    FixedDiv two, cell2, d231, cell;
+};
+
+// Every divisor on IEEE division (no check, no device work).
+inline CellDivisors ieee_cell_divisors(float cell) {
+    CellDivisors D;
+    D.two = FixedDiv{2.0f * cell, 1.0f / (2.0f * cell), 0};
+    D.cell2 = FixedDiv{cell * cell, 1.0f / (cell * cell), 0};
+    D.d231 = FixedDiv{231.0f, 1.0f / 231.0f, 0};
+    D.cell = FixedDiv{cell, 1.0f / cell, 0};
+    return D;
+}
+
+// The same divisors, each checked (fixed_div_for).
+CellDivisors cell_divisors(float cell, cudaStream_t st);
+
 // The divisor d with its reciprocal, exact only when the exhaustive check
 // passed (run once per distinct d and device, on `st`, then cached).
 FixedDiv fixed_div_for(float d, cudaStream_t st);

@@ -1260,6 +1260,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 window::attach_scratch(J, S->win[l], fn);
                 J.res = fres;
                 J.cell = P.fcell;
+                J.div = P.fdivs;
                 J.cut = M.d_books + 3;
                 J.cut_area = (double)P.fcell * (double)P.fcell;
                 J.dt = dt;
@@ -1574,6 +1575,7 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     P.layout = cfg.fine_layout == SILT_FINE_PER_TIRE ? SILT_FINE_PER_TIRE : SILT_FINE_MEAN_PATCH;
     P.fres = cfg.fine_res;
     P.fcell = cfg.fine_cell;
+    P.fdivs = cell_divisors(cfg.fine_cell, st);
     P.sub = (int)std::lround(cfg.cell / cfg.fine_cell);
     P.tire_r = cfg.tire_r;
     if (P.fres > 512 || P.sub > 32) {

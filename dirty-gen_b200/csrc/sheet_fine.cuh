@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/silt_sheet.h"
+#include "sheet_div.cuh"
 #include "sheet_park.cuh"
 
 namespace silt {
@@ -55,6 +56,7 @@ struct Patches {
     int layout = SILT_FINE_MEAN_PATCH;
     int fres = 160;
     float fcell = 0.02f;
+    CellDivisors fdivs{};  // the patch step's divisors for fcell (set by create)
     int sub = 10;
     float tire_r = 0.56f;
     float sub_cap = 8.0f;

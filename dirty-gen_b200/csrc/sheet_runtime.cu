@@ -102,10 +102,9 @@ struct silt_sheet {
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<cudaEvent_t> ev_used;   // groups of three: start, after force, after transport
-    // The grid engine's divisors (2 cell, cell^2, 231, cell), set at
-    // creation; each is exact only once checked against IEEE division for
-    // every float.
-    silt::FixedDiv div_two{}, div_cell2{}, div_231{}, div_cell{};
+    // The step's divisors (2 cell, cell^2, 231, cell), set at creation; each
+    // is exact only once checked against IEEE division for every float.
+    silt::CellDivisors div{};
     silt_step_parts parts;
     // Window engine for the coarse pair (SILT_ENGINE_WINDOW).
     int engine = SILT_ENGINE_GRID;
@@ -259,9 +258,9 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         P.v_out = s->v[l][nxt];
         P.res = res;
         P.cell = cell;
-        P.div_two = s->div_two;
-        P.div_cell2 = s->div_cell2;
-        P.div_231 = s->div_231;
+        P.div_two = s->div.two;
+        P.div_cell2 = s->div.cell2;
+        P.div_231 = s->div.d231;
         P.dt = dt;  // the device divides by its count when it decides one
         P.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
         P.eps = eps;
@@ -295,7 +294,7 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         Q.cut_area = (double)cell * (double)cell;
         Q.res = res;
         Q.cell = cell;
-        Q.div_cell = s->div_cell;
+        Q.div_cell = s->div.cell;
         Q.dt = dt;
         Q.eps = eps;
         Q.skip = 0;
@@ -395,6 +394,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         J.cut_area = (double)s->cfg.cell * (double)s->cfg.cell;
         J.res = s->res;
         J.cell = s->cfg.cell;
+        J.div = s->div;
         J.dt = dt;
         J.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
         J.sub_cap = 8.0f;
@@ -575,12 +575,7 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         silt_sheet_destroy(s);
         return rc;
     }
-    // The divisors of the grid engine's kernels, as they divide (2 * cell,
-    // cell * cell, 231, cell).
-    s->div_two = silt::fixed_div_for(2.0f * cfg->cell, s->st);
-    s->div_cell2 = silt::fixed_div_for(cfg->cell * cfg->cell, s->st);
-    s->div_231 = silt::fixed_div_for(231.0f, s->st);
-    s->div_cell = silt::fixed_div_for(cfg->cell, s->st);
+    s->div = silt::cell_divisors(cfg->cell, s->st);
     e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) {
         silt_sheet_destroy(s);
@@ -2119,6 +2114,7 @@ static int step_sheet_window(float* h, float* u, float* v, const float* bed, con
     silt::window::attach_scratch(J, reinterpret_cast<float*>((char*)scratch + 4096), n);
     J.res = res;
     J.cell = cell;
+    J.div = silt::ieee_cell_divisors(cell);  // no check runs here
     J.dt = dt;
     J.vort = vorticity;
     J.sub_cap = 8.0f;
@@ -2202,9 +2198,10 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         P.res = res;
         P.cell = cell;
         // The free operator divides by IEEE division (no check runs here).
-        P.div_two = silt::FixedDiv{2.0f * cell, 1.0f / (2.0f * cell), 0};
-        P.div_cell2 = silt::FixedDiv{cell * cell, 1.0f / (cell * cell), 0};
-        P.div_231 = silt::FixedDiv{231.0f, 1.0f / 231.0f, 0};
+        const silt::CellDivisors ieee = silt::ieee_cell_divisors(cell);
+        P.div_two = ieee.two;
+        P.div_cell2 = ieee.cell2;
+        P.div_231 = ieee.d231;
         P.dt = dts;
         P.vort = vorticity;
         P.eps = 1.0e-6f;
@@ -2217,7 +2214,7 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
         Q.gate = gate;
         Q.res = res;
         Q.cell = cell;
-        Q.div_cell = silt::FixedDiv{cell, 1.0f / cell, 0};
+        Q.div_cell = ieee.cell;
         Q.dt = dts;
         Q.eps = 1.0e-6f;
         F.lay[1].skip = 1;

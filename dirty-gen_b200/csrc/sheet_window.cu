@@ -248,7 +248,7 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     const float* __restrict__ V = J.v;
     float* __restrict__ F1 = J.f1;
     float* __restrict__ F2 = J.f2;
-    const float cell = J.cell;
+    const FixedDiv cell = J.div.cell;
     const uint8_t* __restrict__ gate = J.gate;
     CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
         float speed = 0.5f * (U[g] + U[g + 1]);
@@ -323,12 +323,12 @@ __device__ void cta_dry_cut(const Job& J, const Box& b) {
 // any cell (src/fluid_core.rs:3442-3471 with clamped indices; the interior
 // form :2805-2831 gives the same values).
 template <class UF, class VF>
-__device__ __forceinline__ bool conf_kick(int i, int j, int res, float two, float dt, float vort, UF uu, VF vv,
+__device__ __forceinline__ bool conf_kick(int i, int j, int res, const FixedDiv& two, float dt, float vort, UF uu, VF vv,
                                           float& du, float& dv) {
     auto vort_at = [&](int a, int c) {
         const int ip = min(a + 1, res - 1), im = max(a - 1, 0), jp = min(c + 1, res - 1), jm = max(c - 1, 0);
-        float dvdx = (vv(ip, c) - vv(im, c)) / two;
-        float dudz = (uu(a, jp) - uu(a, jm)) / two;
+        float dvdx = fdiv(vv(ip, c) - vv(im, c), two);
+        float dudz = fdiv(uu(a, jp) - uu(a, jm), two);
         return dvdx - dudz;
     };
     float w = vort_at(i, j);
@@ -337,8 +337,8 @@ __device__ __forceinline__ bool conf_kick(int i, int j, int res, float two, floa
     float wxm = fabsf(vort_at(max(i - 1, 0), j));
     float wzp = fabsf(vort_at(i, min(j + 1, res - 1)));
     float wzm = fabsf(vort_at(i, max(j - 1, 0)));
-    float nx = (wxp - wxm) / two;
-    float nz = (wzp - wzm) / two;
+    float nx = fdiv(wxp - wxm, two);
+    float nz = fdiv(wzp - wzm, two);
     du = vort * dt * (-nz * w);
     dv = vort * dt * (nx * w);
     return finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f;
@@ -348,7 +348,8 @@ __device__ __forceinline__ bool conf_kick(int i, int j, int res, float two, floa
 // (force_gravity_open's serial sweep, src/fluid_core.rs:2234-2260).
 __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float* p, float dt) {
     const int res = J.res;
-    const float eps = J.eps, two = 2.0f * J.cell;
+    const float eps = J.eps;
+    const FixedDiv two = J.div.two;
     float* U0 = J.gs[0];
     float* V0 = J.gs[1];
     float* UG = J.gs[2];
@@ -365,8 +366,8 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (J.h[g] > eps) {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float px = (p[j * res + ip] - p[j * res + im]) / two;
-            float pz = (p[jp * res + i] - p[jm * res + i]) / two;
+            float px = fdiv(p[j * res + ip] - p[j * res + im], two);
+            float pz = fdiv(p[jp * res + i] - p[jm * res + i], two);
             float mob = job_mob(J, g);
             float ug = J.u[g] + -kGravity * px * mob * dt;
             float vg = J.v[g] + -kGravity * pz * mob * dt;
@@ -449,15 +450,16 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
 __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __restrict__ p, float dt) {
     // Distinct planes; each phase writes only its own cell of u, v or W.
     const int res = J.res;
-    const float eps = J.eps, two = 2.0f * J.cell;
+    const float eps = J.eps;
+    const FixedDiv two = J.div.two;
     const float* __restrict__ H = J.h;
     float* __restrict__ U = J.u;
     float* __restrict__ V = J.v;
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
         if (H[g] > eps) {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float px = (p[j * res + ip] - p[j * res + im]) / two;
-            float pz = (p[jp * res + i] - p[jm * res + i]) / two;
+            float px = fdiv(p[j * res + ip] - p[j * res + im], two);
+            float pz = fdiv(p[jp * res + i] - p[jm * res + i], two);
             float mob = job_mob(J, g);
             U[g] += -kGravity * px * mob * dt;
             V[g] += -kGravity * pz * mob * dt;
@@ -471,8 +473,8 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
         const int wj0 = max(b.j0 - 1, 0), wj1 = min(b.j1 + 1, res - 1);
         CLU_RECT(wi0, wi1, wj0, wj1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float dvdx = (V[j * res + ip] - V[j * res + im]) / two;
-            float dudz = (U[jp * res + i] - U[jm * res + i]) / two;
+            float dvdx = fdiv(V[j * res + ip] - V[j * res + im], two);
+            float dudz = fdiv(U[jp * res + i] - U[jm * res + i], two);
             W[g] = dvdx - dudz;
         })
     }
@@ -485,8 +487,8 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
                 const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
                 float wxp = fabsf(W[j * res + ip]), wxm = fabsf(W[j * res + im]);
                 float wzp = fabsf(W[jp * res + i]), wzm = fabsf(W[jm * res + i]);
-                float nx = (wxp - wxm) / two;
-                float nz = (wzp - wzm) / two;
+                float nx = fdiv(wxp - wxm, two);
+                float nz = fdiv(wzp - wzm, two);
                 float du = vort * dt * (-nz * w);
                 float dv = vort * dt * (nx * w);
                 if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
@@ -535,12 +537,12 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
     if (project) {
         CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float ux = (J.u[j * res + ip] - J.u[j * res + im]) / (2.0f * cell);
-            float vz = (J.v[jp * res + i] - J.v[jm * res + i]) / (2.0f * cell);
+            float ux = fdiv(J.u[j * res + ip] - J.u[j * res + im], J.div.two);
+            float vz = fdiv(J.v[jp * res + i] - J.v[jm * res + i], J.div.two);
             float div = ux + vz;
             float s = sa[j * res + ip] + sa[j * res + im] + sa[jp * res + i] + sa[jm * res + i] - 4.0f * sa[g];
-            float lap_h = s / (cell * cell);
-            float overload = 1.0f + rclamp(job_nu(J, g) / 231.0f, 0.0f, 6.0f);
+            float lap_h = fdiv(s, J.div.cell2);
+            float overload = 1.0f + rclamp(fdiv(job_nu(J, g), J.div.d231), 0.0f, 6.0f);
             sb[g] = div * overload - 0.015f * overload * lap_h;
         })
         crew_sync();
@@ -559,8 +561,8 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
                 if (project) {
                     const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1),
                               jm = max(j - 1, 0);
-                    float qx = (sd[j * res + ip] - sd[j * res + im]) / (2.0f * cell);
-                    float qz = (sd[jp * res + i] - sd[jm * res + i]) / (2.0f * cell);
+                    float qx = fdiv(sd[j * res + ip] - sd[j * res + im], J.div.two);
+                    float qz = fdiv(sd[jp * res + i] - sd[jm * res + i], J.div.two);
                     uu += 0.012f * dt * qx;
                     vv += 0.012f * dt * qz;
                 }

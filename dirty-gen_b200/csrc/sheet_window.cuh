@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "sheet_div.cuh"
+
 namespace silt {
 namespace window {
 
@@ -35,6 +37,7 @@ struct Job {
     double cut_area;       // m^2 of one cell for that book
     int32_t res;
     float cell, dt, vort, sub_cap, eps;
+    CellDivisors div;      // 2 cell, cell^2, 231, cell (fdiv)
     int32_t nu_mode;
     float nu_c, mob_c;
     float decay_c[9];      // NU_CONST damping factor for 1..8 substeps
