@@ -72,6 +72,7 @@ struct PatchState {
     float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
     float *nu_s, *mob_s, *damp_s;  // slurry material of each cell, from grain and moisture at lay time
     uint8_t* grain;
+    uint8_t* solid;       // the patch's wall mask
     float* win[2];        // [layer]: the window engine's scratch planes
     // Host geometry of the current step.
     float origin[2] = {0, 0};
@@ -82,6 +83,7 @@ struct PatchRef {
     float *water, *slurry, *uw, *vw, *us, *vs, *bed, *bed_slurry, *moisture;
     float *nu_s, *mob_s, *damp_s;
     uint8_t* grain;
+    uint8_t* solid;
     const int16_t* col;
     const int16_t* row;
     float ox, oz;
@@ -204,7 +206,7 @@ __global__ void k_refine_lay(const PatchRef* refs, int np, int fres, SheetView W
         refine_cell(refs[k / fn], (int)(k / fn), (int)(k % fn), fres, W, owner);
 }
 
-__device__ __forceinline__ float tile_left(float idle) { return idle <= 0.0f ? 1.0f : expf(-idle / NEAR_LIFE_S); }
+__device__ __forceinline__ float tile_left(float idle) { return idle <= 0.0f ? 1.0f : exp_rn(-idle / NEAR_LIFE_S); }
 
 // near.rs:139-148 floor_scale on one residual, given its lowest value
 // (the minimum of 0 and every residual).
@@ -367,6 +369,16 @@ struct JobGroup {
     int job_off;        // byte offset of its PushJob list in the step table
     int njobs, i0, j0, w, h;
 };
+
+// The wall mask of every patch (blockIdx.y), src/fluid_core.rs:7288-7360
+// with fine = true: the patch's water over its bed at its origin.
+__global__ void k_patch_walls(const PatchRef* refs, int fres, float fcell, const walls::SolidGeom* geoms, int n) {
+    ::silt::dep_wait();
+    const PatchRef& r = refs[blockIdx.y];
+    const int cells = fres * fres;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x)
+        r.solid[c] = walls::mask_value(geoms, n, c % fres, c / fres, fres, fcell, r.ox, r.oz, r.water, r.bed);
+}
 
 // The shoves of every patch (blockIdx.y = group). With `fade`, one more row
 // of blocks runs near_fade over the tile pool (independent of the shoves).
@@ -959,9 +971,10 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
     const size_t fn = (size_t)P.fres * P.fres;
     while ((int)P.patches.size() < np) {
         PatchState* S = new PatchState();
-        // 12 planes + a spare + the window engine's scratch for two layers, then grain.
+        // 12 planes + a spare + the window engine's scratch for two layers,
+        // then grain and the wall mask.
         const size_t planes = 13 + 2 * (size_t)window::SCRATCH_PLANES;
-        cudaError_t e = cudaMalloc(&S->base, planes * fn * sizeof(float) + fn + 256);
+        cudaError_t e = cudaMalloc(&S->base, planes * fn * sizeof(float) + 2 * fn + 256);
         if (e != cudaSuccess) {
             delete S;
             snprintf(g_err, sizeof g_err, "patch alloc: %s", cudaGetErrorString(e));
@@ -980,8 +993,10 @@ static int ensure_patches(Patches& P, int np, cudaStream_t st) {
             q += (size_t)window::SCRATCH_PLANES * fn;
         }
         S->grain = reinterpret_cast<uint8_t*>(q);
+        S->solid = S->grain + fn;
         FCK(cudaMemsetAsync(S->base, 0, planes * fn * sizeof(float), st));
         FCK(cudaMemsetAsync(S->grain, 4, fn, st));
+        FCK(cudaMemsetAsync(S->solid, 0, fn, st));
         P.patches.push_back(S);
     }
     return SILT_OK;
@@ -1232,6 +1247,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         r.mob_s = S->mob_s;
         r.damp_s = S->damp_s;
         r.grain = S->grain;
+        r.solid = S->solid;
         const int16_t* dax = reinterpret_cast<const int16_t*>(HS.d_tab[slot] + off_axes);
         r.col = dax + (size_t)p * 2 * fres;
         r.row = dax + (size_t)p * 2 * fres + fres;
@@ -1261,6 +1277,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 J.res = fres;
                 J.cell = P.fcell;
                 J.div = P.fdivs;
+                J.solid = P.n_solids > 0 ? S->solid : nullptr;
                 J.cut = M.d_books + 3;
                 J.cut_area = (double)P.fcell * (double)P.fcell;
                 J.dt = dt;
@@ -1427,6 +1444,14 @@ int step_patches(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& p
         ::silt::launch_dep(k_push_patches, dim3(grid), dim3(256), 0, W.st, refs, tab, TAB(JobGroup, L.off_push_groups), L.n_push_groups, P.fres,
                                                P.fcell, fade, M.meta, M.slot_map, M.free_stack, M.counters,
                                                dt > 0.0f && std::isfinite(dt) ? dt : 0.0f);
+        ::silt::count_launch();
+        FCK(cudaGetLastError());
+    }
+    if (P.n_solids > 0) {
+        // Each patch's wall mask from its water over its bed (solid_mask(true)).
+        dim3 grid(launch_blocks((size_t)P.fres * P.fres), L.np);
+        ::silt::launch_dep(k_patch_walls, dim3(grid), dim3(256), 0, W.st, refs, P.fres, P.fcell, P.d_solids,
+                           P.n_solids);
         ::silt::count_launch();
         FCK(cudaGetLastError());
     }

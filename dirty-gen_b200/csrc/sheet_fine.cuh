@@ -10,6 +10,7 @@
 #include "../../include/silt_sheet.h"
 #include "sheet_div.cuh"
 #include "sheet_park.cuh"
+#include "sheet_walls.cuh"
 
 namespace silt {
 namespace fine {
@@ -65,6 +66,8 @@ struct Patches {
     bool patches_off = false;  // lay no patch this step: every tire shoves the coarse cells (closure coupling)
     bool coarse_shove_off = false;  // and not even that: the learned closure carries the tires' effect
     float open_mobility = -1.0f;    // >= 0: open-water mode, the water row's mobility (src/fluid_core.rs:8015-8017)
+    const walls::SolidGeom* d_solids = nullptr;  // the walls (silt_set_hydro_solids), device
+    int n_solids = 0;
     bool fine_on = false;
     int active = 0;
     std::vector<PatchState*> patches;

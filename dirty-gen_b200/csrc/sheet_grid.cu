@@ -94,7 +94,9 @@ __device__ __forceinline__ float cell_mob(const LayerParams& P, size_t g) {
     return sheet_mobility_for(cell_nu(P, g));
 }
 
-// The cell's damping factor over dt: exp(-sheet_damp(nu) dt).
+// The cell's damping factor over dt: exp(-sheet_damp(nu) dt). The grid engine
+// keeps single-precision expf on this per-cell path (its confinement is the
+// snapshot form, so its parity is within tolerance, not bit for bit).
 __device__ __forceinline__ float cell_decay(const LayerParams& P, size_t g, float dt) {
     if (P.nu_mode == NU_CONST) return P.decay_c;
     const float rate = P.nu_mode == NU_TABLE ? P.damp_plane[g] : sheet_damp(cell_nu(P, g));

@@ -49,14 +49,22 @@ __device__ __forceinline__ float sheet_mobility_for(float nu) {
     return 0.042f * (1.0f + boost);
 }
 
-// src/fluid_core.rs:184-192. powf here is CUDA's; it can differ from glibc's
-// in the last bit, which is the one place the slurry damping may differ.
+// x^y and e^x as floats: the double-precision function rounded once to
+// float. The reference calls the C library's powf and expf, which are
+// correctly rounded on all but a few inputs in 10^4 over the ranges the
+// sheet uses (an exhaustive comparison with the rounded double results:
+// expf on [-100, 0] differs on 0.009% of floats, powf(r, 0.3) on [0.002, 12]
+// on 0.06%); CUDA's single-precision powf and expf differ far more often.
+__device__ __forceinline__ float pow_rn(float x, float y) { return (float)pow((double)x, (double)y); }
+__device__ __forceinline__ float exp_rn(float x) { return (float)exp((double)x); }
+
+// src/fluid_core.rs:184-192
 __device__ __forceinline__ float sheet_damp(float nu) {
     float rel = rclamp(fmaxf(nu, 0.05f) / 231.0f, 0.002f, 12.0f);
-    if (rel >= 0.42f) return 1.70f * powf(rel, 0.30f);
-    const float at_silt = 1.70f * powf(0.42f, 0.30f);
+    if (rel >= 0.42f) return 1.70f * pow_rn(rel, 0.30f);
+    const float at_silt = 1.70f * pow_rn(0.42f, 0.30f);
     float t = rclamp(rel / 0.42f, 0.0f, 1.0f);
-    return at_silt * powf(t, 1.15f);
+    return at_silt * pow_rn(t, 1.15f);
 }
 
 // src/fluid_core.rs:3473-3479

@@ -31,6 +31,7 @@
 #include "sheet_grid.cuh"
 #include "sheet_host_math.h"
 #include "sheet_ops.cuh"
+#include "sheet_walls.cuh"
 #include "sheet_park.cuh"
 #include "sheet_window.cuh"
 
@@ -113,6 +114,14 @@ struct silt_sheet {
     silt::window::Job* h_win_jobs = nullptr;      // pinned staging
     cudaEvent_t win_ev[2] = {nullptr, nullptr};
     int win_flip = 0;
+    // Walls (silt_set_hydro_solids): the bodies in two device slots, each
+    // filled from its pinned half once the copy two updates ago is done.
+    int n_solids = 0;
+    silt::walls::SolidGeom* d_solids = nullptr;  // 2 x MAX_SOLIDS
+    silt::walls::SolidGeom* h_solids = nullptr;  // pinned, 2 x MAX_SOLIDS
+    cudaEvent_t solid_ev[2] = {nullptr, nullptr};
+    int solid_slot = 0;
+    uint8_t* d_wall_mask = nullptr;  // the coarse window's mask (res^2)
     // Grid engine: active-tile flags and the substep's tile list.
     silt::TileFlags tf;
     uint8_t* tile_mem = nullptr;
@@ -395,6 +404,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         J.res = s->res;
         J.cell = s->cfg.cell;
         J.div = s->div;
+        J.solid = s->n_solids > 0 ? s->d_wall_mask : nullptr;
         J.dt = dt;
         J.vort = l == 0 ? 0.08f : 0.05f;  // src/fluid_core.rs:8074, :8116
         J.sub_cap = 8.0f;
@@ -413,6 +423,12 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
     }
     CK(cudaMemcpyAsync(s->d_win_jobs + 2 * slot, jobs, 2 * sizeof(silt::window::Job), cudaMemcpyHostToDevice, s->st));
     CK(cudaEventRecord(s->win_ev[slot], s->st));
+    if (s->n_solids > 0) {
+        // One mask for both sheets, from the water before either steps
+        // (src/fluid_core.rs:7954-7967).
+        CK(silt::walls::launch_mask(s->d_wall_mask, s->res, s->cfg.cell, s->origin[0], s->origin[1], s->H(0), s->bed,
+                                    s->fine.d_solids, s->n_solids, s->st));
+    }
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     if (s->timing) {
         for (int q = 0; q < 3; ++q) {
@@ -618,6 +634,11 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->tile_mem);
     cudaFree(s->d_win_jobs);
     if (s->h_win_jobs) cudaFreeHost(s->h_win_jobs);
+    cudaFree(s->d_solids);
+    if (s->h_solids) cudaFreeHost(s->h_solids);
+    for (int k = 0; k < 2; ++k)
+        if (s->solid_ev[k]) cudaEventDestroy(s->solid_ev[k]);
+    cudaFree(s->d_wall_mask);
     for (int k = 0; k < 2; ++k)
         if (s->win_ev[k]) cudaEventDestroy(s->win_ev[k]);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -1203,6 +1224,38 @@ int silt_set_wave_maker(silt_sheet* s, const silt_wave_maker* wave) {
     s->wave_on = wave != nullptr;
     if (wave) s->wave = *wave;
     s->wave_t = 0.0f;
+    return SILT_OK;
+}
+
+int silt_set_hydro_solids(silt_sheet* s, const silt_hydro_solid* solids, int32_t n) {
+    if (!s || n < 0 || (n > 0 && !solids)) return fail_arg("set_hydro_solids");
+    if (n > silt::walls::MAX_SOLIDS) return fail_arg("set_hydro_solids: more than 64 bodies");
+    if (n > 0 && s->engine != SILT_ENGINE_WINDOW) return fail_arg("set_hydro_solids: walls need the window engine");
+    CK(cudaSetDevice(s->cfg.device));
+    if (n > 0 && !s->d_solids) {
+        const size_t bytes = 2 * silt::walls::MAX_SOLIDS * sizeof(silt::walls::SolidGeom);
+        CK(cudaMalloc(&s->d_solids, bytes));
+        CK(cudaMallocHost(&s->h_solids, bytes));
+        for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&s->solid_ev[k], cudaEventDisableTiming));
+        CK(cudaMalloc(&s->d_wall_mask, s->n));
+    }
+    if (n > 0) {
+        const int slot = s->solid_slot ^ 1;
+        CK(cudaEventSynchronize(s->solid_ev[slot]));
+        silt::walls::SolidGeom* h = s->h_solids + (size_t)slot * silt::walls::MAX_SOLIDS;
+        for (int k = 0; k < n; ++k) {
+            const silt_hydro_solid& b = solids[k];
+            h[k] = silt::walls::make_geom(b.x, b.z, b.yaw, b.half_length, b.half_width, b.bottom_y, b.top_y,
+                                          b.contact);
+        }
+        silt::walls::SolidGeom* d = s->d_solids + (size_t)slot * silt::walls::MAX_SOLIDS;
+        CK(cudaMemcpyAsync(d, h, (size_t)n * sizeof *h, cudaMemcpyHostToDevice, s->st));
+        CK(cudaEventRecord(s->solid_ev[slot], s->st));
+        s->solid_slot = slot;
+    }
+    s->n_solids = n;
+    s->fine.d_solids = n > 0 ? s->d_solids + (size_t)s->solid_slot * silt::walls::MAX_SOLIDS : nullptr;
+    s->fine.n_solids = n;
     return SILT_OK;
 }
 

@@ -235,10 +235,13 @@ __device__ __forceinline__ float job_mob(const Job& J, int g) {
 __device__ __forceinline__ float job_decay(const Job& J, int g, float dt, float decay_c) {
     if (J.nu_mode == NU_CONST) return decay_c;
     const float rate = J.nu_mode == NU_TABLE ? J.damp_plane[g] : sheet_damp(job_nu(J, g));
-    return expf(-rate * dt);
+    return exp_rn(-rate * dt);
 }
 
-// transport_open_rows (src/fluid_core.rs:3025-3137) on one box (banks off).
+// transport_open_rows (src/fluid_core.rs:3025-3137) on one box, banks off;
+// on a walled sheet the same edges as transport/move_edge_bufs (:3894-3963,
+// :4178-4223): an edge touching a wall moves nothing, and a dry bank above the
+// donor's surface takes nothing (banks on the layer's bed).
 __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     // The planes are distinct and each phase writes only its own cell, so
     // the loads of one cell may run ahead of the stores of the previous.
@@ -250,17 +253,25 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     float* __restrict__ F2 = J.f2;
     const FixedDiv cell = J.div.cell;
     const uint8_t* __restrict__ gate = J.gate;
+    const uint8_t* __restrict__ W = J.solid;
+    const float* __restrict__ bed = J.bed;
+    const bool walled = W != nullptr;
+    // dh of the edge from donor d to receiver r, 0 across a wall.
+    auto edge = [&](int d, int r, float remd, float speed) {
+        const float dh = open_edge_dh(walled, h[d], h[r], remd, gate ? gate[r] : 1, walled ? bed[d] : 0.0f,
+                                      walled ? bed[r] : 0.0f, speed, dt, cell, 0.45f);
+        return walled && (W[d] | W[r]) ? 0.0f : dh;
+    };
     CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
         float speed = 0.5f * (U[g] + U[g + 1]);
-        float dh = open_edge_dh(false, h[g + 1], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
+        float dh = edge(g + 1, g, 0.0f, speed);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
     crew_sync();
     CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
         float speed = 0.5f * (U[g] + U[g + 1]);
         float prev = i > b.i0 ? F1[g - 1] : 0.0f;
-        float dh = open_edge_dh(false, h[g], h[g + 1], 0.0f + prev, gate ? gate[g + 1] : 1, 0.0f, 0.0f, speed, dt,
-                                cell, 0.45f);
+        float dh = edge(g, g + 1, 0.0f + prev, speed);
         F2[g] = speed > 0.0f ? dh : 0.0f;
     })
     crew_sync();
@@ -275,15 +286,14 @@ __device__ void cta_transport(const Job& J, const Box& b, float dt) {
     crew_sync();
     CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
         float speed = 0.5f * (V[g] + V[g + res]);
-        float dh = open_edge_dh(false, h[g + res], h[g], 0.0f, gate ? gate[g] : 1, 0.0f, 0.0f, speed, dt, cell, 0.45f);
+        float dh = edge(g + res, g, 0.0f, speed);
         F1[g] = speed > 0.0f ? 0.0f : dh;
     })
     crew_sync();
     CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
         float speed = 0.5f * (V[g] + V[g + res]);
         float ra = j > b.j0 ? 0.0f + F1[g - res] : 0.0f;
-        float dh = open_edge_dh(false, h[g], h[g + res], ra, gate ? gate[g + res] : 1, 0.0f, 0.0f, speed, dt, cell,
-                                0.45f);
+        float dh = edge(g, g + res, ra, speed);
         F2[g] = speed > 0.0f ? dh : 0.0f;
     })
     crew_sync();
@@ -316,6 +326,249 @@ __device__ void cta_dry_cut(const Job& J, const Box& b) {
     })
     for (int o = 16; o > 0; o >>= 1) cut += __shfl_down_sync(0xffffffffu, cut, o);
     if ((threadIdx.x & 31) == 0 && cut > 0.0 && J.cut) atomicAdd(J.cut, cut * J.cut_area);
+    crew_sync();
+}
+
+// ---------------------------------------------------------------- walls
+// The walled sheet's passes (src/fluid_core.rs:4225-4582). Each writes only
+// cells that the pass itself never reads (wall cells from open ones, or a cell
+// from its own values), so it runs in place on the crew; redirect, which
+// moves depth between neighbours, books into scratch first.
+
+// Four-neighbour offsets in the reference's order: (-1,0), (1,0), (0,-1), (0,1).
+__device__ __forceinline__ int nb_di(int k) { return k == 0 ? -1 : (k == 1 ? 1 : 0); }
+__device__ __forceinline__ int nb_dj(int k) { return k == 2 ? -1 : (k == 3 ? 1 : 0); }
+
+__device__ __forceinline__ bool wall_at(const uint8_t* W, int res, int i, int j) {
+    return i >= 0 && j >= 0 && i < res && j < res && W[j * res + i] != 0;
+}
+__device__ __forceinline__ bool open_at(const uint8_t* W, int res, int i, int j) {
+    return i >= 0 && j >= 0 && i < res && j < res && W[j * res + i] == 0;
+}
+
+// solid_near (:4565-4582, radius 1): a wall among the eight neighbours.
+__device__ __forceinline__ bool wall_near(const uint8_t* W, int res, int i, int j) {
+    for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di)
+            if ((di | dj) && wall_at(W, res, i + di, j + dj)) return true;
+    return false;
+}
+
+// displace_occupied (:4382-4444) on the whole window: a covered column goes,
+// in equal shares, to its open four-neighbours (to the open cells of its 5 x 5
+// block when none is open) and the cell empties; with nowhere to go it stays.
+// Each open cell gathers its shares in the reference's order (sources in
+// raster order) into f1, then every cell applies its change.
+__device__ void cta_displace(const Job& J) {
+    const int res = J.res;
+    const uint8_t* __restrict__ W = J.solid;
+    float* __restrict__ H = J.h;
+    float* __restrict__ give = J.f1;
+    // Open cells a wall cell at (si, sj) would give to: its four-neighbours,
+    // or its 5 x 5 block when none of those is open.
+    auto share_count = [&](int si, int sj, bool& four) {
+        int n = 0;
+        for (int k = 0; k < 4; ++k) n += open_at(W, res, si + nb_di(k), sj + nb_dj(k)) ? 1 : 0;
+        four = n > 0;
+        if (four) return n;
+        for (int dj = -2; dj <= 2; ++dj)
+            for (int di = -2; di <= 2; ++di) n += open_at(W, res, si + di, sj + dj) ? 1 : 0;
+        return n;
+    };
+    CLU_RECT(0, res - 1, 0, res - 1, {
+        if (W[g] == 0) {
+            float acc = 0.0f;
+            for (int sj = j - 2; sj <= j + 2; ++sj)
+                for (int si = i - 2; si <= i + 2; ++si) {
+                    if (!wall_at(W, res, si, sj)) continue;
+                    const float vol = H[sj * res + si];
+                    if (vol <= 1.0e-8f) continue;
+                    bool four;
+                    const int n = share_count(si, sj, four);
+                    if (four && abs(si - i) + abs(sj - j) != 1) continue;
+                    acc += vol / (float)n;
+                }
+            give[g] = acc;
+        }
+    })
+    crew_sync();
+    CLU_RECT(0, res - 1, 0, res - 1, {
+        if (W[g] != 0) {
+            const float vol = H[g];
+            bool four;
+            if (vol <= 1.0e-8f || share_count(i, j, four) > 0) {
+                H[g] = 0.0f;
+                J.u[g] = 0.0f;
+                J.v[g] = 0.0f;
+            }
+        } else if (give[g] > 0.0f) {
+            H[g] += give[g];
+        }
+    })
+    crew_sync();
+}
+
+// lift_solid_surface (:4225-4276): a wall cell's surface is the mean of the
+// wet open cells within two cells, its own when there are none.
+__device__ void cta_lift(const Job& J, const Box& b, float* eta) {
+    const int res = J.res;
+    const uint8_t* __restrict__ W = J.solid;
+    const float eps = J.eps;
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (W[g] != 0) {
+            float acc = 0.0f, n = 0.0f;
+            for (int dj = -2; dj <= 2; ++dj)
+                for (int di = -2; di <= 2; ++di) {
+                    if (!(di | dj) || !open_at(W, res, i + di, j + dj)) continue;
+                    const int q = (j + dj) * res + i + di;
+                    if (J.h[q] <= eps) continue;
+                    acc += eta[q];
+                    n += 1.0f;
+                }
+            if (n > 0.0f) eta[g] = acc / n;
+        }
+    })
+}
+
+// write_noslip_ghost (:4278-4326): a wall cell takes minus the mean velocity
+// of its wet open four-neighbours, zero when there are none.
+__device__ void cta_ghost(const Job& J, const Box& b) {
+    const int res = J.res;
+    const uint8_t* __restrict__ W = J.solid;
+    const float eps = J.eps;
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (W[g] != 0) {
+            float au = 0.0f, av = 0.0f, n = 0.0f;
+            for (int k = 0; k < 4; ++k) {
+                const int ni = i + nb_di(k), nj = j + nb_dj(k);
+                if (!open_at(W, res, ni, nj)) continue;
+                const int q = nj * res + ni;
+                if (J.h[q] <= eps) continue;
+                au += J.u[q];
+                av += J.v[q];
+                n += 1.0f;
+            }
+            J.u[g] = n > 0.0f ? -au / n : 0.0f;
+            J.v[g] = n > 0.0f ? -av / n : 0.0f;
+        }
+    })
+}
+
+// block_into_solid (:4328-4380): a wet open cell drops the part of its
+// velocity that points into a wall neighbour, direction by direction.
+__device__ void cta_block(const Job& J, const Box& b) {
+    const int res = J.res;
+    const uint8_t* __restrict__ W = J.solid;
+    const float eps = J.eps;
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        if (W[g] == 0 && J.h[g] > eps) {
+            float ux = J.u[g], vx = J.v[g];
+            bool hit = false;
+            for (int k = 0; k < 4; ++k) {
+                if (!wall_at(W, res, i + nb_di(k), j + nb_dj(k))) continue;
+                const float nx = (float)nb_di(k), nz = (float)nb_dj(k);
+                const float vn = ux * nx + vx * nz;
+                if (vn > 0.0f) {
+                    ux -= vn * nx;
+                    vx -= vn * nz;
+                    hit = true;
+                }
+            }
+            if (hit) {
+                J.u[g] = ux;
+                J.v[g] = vx;
+            }
+        }
+    })
+}
+
+// redirect_into_walls (:4446-4563). Sources are the box's open cells with 2 cm
+// of water; each books its removal and, per direction, the share each accepted
+// flank receives. Receivers (the box and a one-cell rim) then add their shares
+// in the reference's order -- sources in raster order, directions in neighbour
+// order -- and the new depths land in f1 before they are copied back. The
+// books live in the transient planes (the Gauss-Seidel snapshots and f2): the
+// scratch sets keep what the reference's blurs left there, which the next
+// step's blurs read beyond its box.
+__device__ void cta_redirect(const Job& J, const Box& b, float dt) {
+    const int res = J.res;
+    const uint8_t* __restrict__ W = J.solid;
+    float* __restrict__ H = J.h;
+    const float* __restrict__ bed = J.bed;
+    float* __restrict__ removed = J.gs[0];
+    float* const book[4] = {J.gs[1], J.gs[2], J.gs[3], J.f2};
+    // A flank q of source s takes water unless it is a wall or a dry bank
+    // above the source's surface.
+    auto accepts = [&](int q, int s) {
+        return W[q] == 0 && !(H[q] <= 1.0e-6f && bed[q] > bed[s] + H[s] + 1.0e-3f);
+    };
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        float rem = 0.0f;
+        float share[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (W[g] == 0 && !(H[g] < 0.02f)) {
+            for (int k = 0; k < 4; ++k) {
+                const int di = nb_di(k), dj = nb_dj(k);
+                if (!wall_at(W, res, i + di, j + dj)) continue;
+                float vn = J.u[g] * (float)di + J.v[g] * (float)dj;
+                if (open_at(W, res, i - di, j - dj)) {
+                    const int up = (j - dj) * res + (i - di);
+                    const float feed = J.u[up] * (float)di + J.v[up] * (float)dj;
+                    if (feed > vn) vn = feed;
+                }
+                if (vn < 0.05f) continue;
+                // The flanks: across the direction, lower index first.
+                const int pi = di != 0 ? 0 : 1, pj = di != 0 ? 1 : 0;
+                int n_dest = 0;
+                float flank = 0.0f;
+                for (int side = -1; side <= 1; side += 2) {
+                    const int qi = i + side * pi, qj = j + side * pj;
+                    if (qi < 0 || qj < 0 || qi >= res || qj >= res) continue;
+                    const int q = qj * res + qi;
+                    if (!accepts(q, g)) continue;
+                    flank += H[q];
+                    ++n_dest;
+                }
+                if (n_dest == 0) continue;
+                const float excess = H[g] - flank / (float)n_dest;
+                if (excess < 2.0e-3f) continue;
+                const float room = H[g] - rem;
+                if (room < 1.0e-6f) continue;
+                const float frac = fminf(fdiv(vn * dt, J.div.cell), 0.45f);
+                const float dh = fminf(fminf(excess, H[g] * frac), room);
+                if (dh < 1.0e-8f) continue;
+                rem += dh;
+                share[k] = dh / (float)n_dest;
+            }
+        }
+        removed[g] = rem;
+        for (int k = 0; k < 4; ++k) book[k][g] = share[k];
+    })
+    crew_sync();
+    const int ri0 = max(b.i0 - 1, 0), ri1 = min(b.i1 + 1, res - 1);
+    const int rj0 = max(b.j0 - 1, 0), rj1 = min(b.j1 + 1, res - 1);
+    auto in_box = [&](int i, int j) { return i >= b.i0 && i <= b.i1 && j >= b.j0 && j <= b.j1; };
+    CLU_RECT(ri0, ri1, rj0, rj1, {
+        // Sources whose flank this cell is: the cell above (horizontal
+        // directions), left and right (vertical directions), below
+        // (horizontal directions), in raster order.
+        float add = 0.0f;
+        const int si[4] = {i, i - 1, i + 1, i};
+        const int sj[4] = {j - 1, j, j, j + 1};
+        for (int t = 0; t < 4; ++t) {
+            if (!in_box(si[t], sj[t])) continue;
+            const int s = sj[t] * res + si[t];
+            const int k0 = (t == 0 || t == 3) ? 0 : 2;
+            for (int k = k0; k < k0 + 2; ++k) {
+                const float sh = book[k][s];
+                if (sh > 0.0f && accepts(g, s)) add += sh;
+            }
+        }
+        const float rem = in_box(i, j) ? removed[g] : 0.0f;
+        const float hv = H[g];
+        J.f1[g] = (rem > 0.0f || add > 0.0f) ? fmaxf(hv - rem + add, 0.0f) : hv;
+    })
+    crew_sync();
+    CLU_RECT(ri0, ri1, rj0, rj1, { H[g] = J.f1[g]; })
     crew_sync();
 }
 
@@ -369,6 +622,8 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
             float px = fdiv(p[j * res + ip] - p[j * res + im], two);
             float pz = fdiv(p[jp * res + i] - p[jm * res + i], two);
             float mob = job_mob(J, g);
+            // force_gravity_solid (:2084-2129): at least 1 beside a wall.
+            if (J.solid && J.h[g] > 0.08f && wall_near(J.solid, res, i, j)) mob = fmaxf(mob, 1.0f);
             float ug = J.u[g] + -kGravity * px * mob * dt;
             float vg = J.v[g] + -kGravity * pz * mob * dt;
             UG[g] = ug;
@@ -502,7 +757,7 @@ __device__ void cta_gravity_jacobi(const Job& J, const Box& b, const float* __re
 }
 
 // substep (src/fluid_core.rs:1879-2082), open sheet, gravity drive.
-__device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* sc, float dt, float decay_c,
+__device__ __forceinline__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* sc, float dt, float decay_c,
                            bool do_flux, bool inner_par) {
     const int res = J.res;
     float* __restrict__ sa = sc[0];
@@ -512,6 +767,7 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
     float* __restrict__ se = sc[4];
     const float eps = J.eps, cell = J.cell;
     const bool fine = cell <= kFineCell + 1.0e-6f;
+    const bool walled = J.solid != nullptr;
     {
         const float* __restrict__ bed = J.bed;
         const float* __restrict__ H = J.h;
@@ -520,6 +776,10 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
         CLU_RECT(hi0, hi1, hj0, hj1, { sa[g] = bed[g] + H[g]; })
     }
     crew_sync();
+    if (walled) {
+        cta_lift(J, b, sa);
+        crew_sync();
+    }
     cta_blur(sa, sb, se, res, b, kG0, kG1, kG2);
     cta_blur(sa, scc, se, res, b, kS0, kS1, kS2);
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
@@ -529,11 +789,18 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
     crew_sync();
     const bool par = (b.j1 - b.j0 >= 47) && (b.i1 - b.i0 >= 31) && inner_par;
     int passes = 0;
-    if (fine || par)
-        cta_gravity_jacobi(J, b, sd, dt);
-    else
+    if (walled) {
+        // A walled sheet sweeps serially on every grid (the step pair's
+        // serial inner loops; the free operator takes no walls).
+        cta_ghost(J, b);
+        crew_sync();
         passes = cta_gravity_gs(S, J, b, sd, dt);
-    const bool project = !fine;
+    } else if (fine || par) {
+        cta_gravity_jacobi(J, b, sd, dt);
+    } else {
+        passes = cta_gravity_gs(S, J, b, sd, dt);
+    }
+    const bool project = !fine || walled;
     if (project) {
         CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
@@ -573,6 +840,13 @@ __device__ int cta_substep(Shared& S, const Job& J, const Box& b, float* const* 
         })
     }
     crew_sync();
+    if (walled) {
+        cta_redirect(J, b, dt);
+        cta_block(J, b);
+        crew_sync();
+        cta_ghost(J, b);
+        crew_sync();
+    }
     if (do_flux) {
         cta_transport(J, b, dt);
         cta_dry_cut(J, b);
@@ -923,11 +1197,12 @@ __device__ void cta_ledger(Shared& S, const Job& J) {
 
 // step_sheet_eps_in + step_sheet_scratch (src/fluid_core.rs:821-852, :1659-1831).
 // One window layer's step; returns the Gauss-Seidel passes of its last box.
-__device__ int window_body(Shared& S, const Job& J) {
+__device__ __forceinline__ int window_body(Shared& S, const Job& J) {
     int gs_passes = 0;
     const int res = J.res;
     const float eps = J.eps;
     if (J.soften_edge > 0) cta_soften(J);
+    if (J.solid) cta_displace(J);
     // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844), over the crew.
     double ws = 0.0;
     CLU_RECT(0, res - 1, 0, res - 1, {
@@ -939,7 +1214,7 @@ __device__ int window_body(Shared& S, const Job& J) {
         cta_ledger(S, J);
         return 0;
     }
-    const bool open_fine = J.cell <= kFineCell + 1.0e-6f;
+    const bool open_fine = !J.solid && J.cell <= kFineCell + 1.0e-6f;
     const bool fine_open = open_fine && J.pace == 0;
     const bool whole_wet = open_fine && (J.pace == 2 || J.pace == 3);
     const bool awake = open_fine && !whole_wet && !fine_open;

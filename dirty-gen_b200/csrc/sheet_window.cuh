@@ -28,6 +28,7 @@ struct Job {
     const float* mob_plane;   // NU_TABLE only
     const float* damp_plane;  // NU_TABLE only
     const uint8_t* gate;   // nullptr: every receiver open
+    const uint8_t* solid;  // wall mask (0 open, 1 contact, 2 wall), nullptr: an open sheet
     float* sc[2][5];       // the reference's two scratch sets (sc, sc2): a, b, c, d, e
     float* f1;             // transient: vorticity, edge fluxes
     float* f2;             // transient: edge fluxes, wet-body labels

@@ -54,6 +54,11 @@ class WaveMaker(ctypes.Structure):
     _fields_ = [(k, _f) for k in ("x0", "x1", "z0", "z1", "dir_x", "dir_z", "amplitude_m_s", "period_s", "ramp_s")]
 
 
+class HydroSolid(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("x", "z", "yaw", "half_length", "half_width", "bottom_y", "top_y")] + \
+               [("contact", _i), ("radius", _f), ("width", _f)]
+
+
 class GroundSample(ctypes.Structure):
     _fields_ = [(k, _f) for k in ("water_m", "slurry_m", "u", "v", "settled_dust_m", "moisture", "bed_m")]
 
@@ -131,6 +136,7 @@ def lib():
             "silt_set_river_reach": [_p, ctypes.POINTER(RiverReach)],
             "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
             "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
+            "silt_set_hydro_solids": [_p, ctypes.POINTER(HydroSolid), _i],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -314,6 +320,18 @@ class Sheet:
                        reach.get("outlet_eta", 0.0), reach.get("inlet_speed_m_s", 0.0),
                        reach.get("inlet_turbidity", 0.0))
         check(lib().silt_set_river_reach(self.h, ctypes.byref(r)), "set_river_reach")
+
+    def set_hydro_solids(self, solids):
+        """FluidCore::set_hydro_solids: dicts with the HydroSolid fields (x, z,
+        yaw, half_length, half_width, bottom_y, top_y, contact, radius, width);
+        an empty list removes the walls."""
+        arr = (HydroSolid * max(len(solids), 1))()
+        for k, sd in enumerate(solids):
+            arr[k] = HydroSolid(*[float(sd.get(n, 0.0)) for n in ("x", "z", "yaw", "half_length", "half_width",
+                                                                   "bottom_y", "top_y")],
+                                int(bool(sd.get("contact", False))), float(sd.get("radius", 0.0)),
+                                float(sd.get("width", 0.0)))
+        check(lib().silt_set_hydro_solids(self.h, arr, len(solids)), "set_hydro_solids")
 
     def set_wave_maker(self, wave):
         """FluidCore::set_wave_maker: dict of WaveMaker fields, or None."""

@@ -113,6 +113,17 @@ typedef struct {
     float x0, x1, z0, z1, dir_x, dir_z, amplitude_m_s, period_s, ramp_s;
 } silt_wave_maker;
 
+/* src/fluid_core.rs:213-240 (`HydroSolid`): a wheel's or a belly panel's
+ * footprint, a wall in the sheet wherever the free surface stands above
+ * bottom_y (and the bed below top_y). yaw 0 points the long axis along +Z.
+ * contact != 0 marks a tire contact (drawn over walls). radius and width
+ * (the cylinder of a wheel) are kept for the caller; the sheet uses the box. */
+typedef struct {
+    float x, z, yaw, half_length, half_width, bottom_y, top_y;
+    int32_t contact;
+    float radius, width;
+} silt_hydro_solid;
+
 /* src/fluid_core.rs:440-448 (`GroundSample`); settled dust is off this path (0). */
 typedef struct {
     float water_m, slurry_m, u, v, settled_dust_m, moisture, bed_m;
@@ -288,6 +299,15 @@ int silt_set_wave_maker(silt_sheet* s, const silt_wave_maker* wave);
 /* FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097): kept for the
  * caller; the tracers that read it are not on this path (flow.A stays 0). */
 int silt_set_turbidity_enabled(silt_sheet* s, int32_t on);
+/* FluidCore::set_hydro_solids (src/fluid_core.rs:5257-5260): the walls of the
+ * next steps (n = 0 removes them). Each step builds the wall mask of the
+ * coarse window and of every tire patch from the water over its bed
+ * (:7288-7360 solid_mask), pushes covered columns to their open neighbours
+ * (:4382 displace_occupied) and steps the walled sheet (:1879-2082 with
+ * `solid`): lifted surface, no-slip ghosts, the Gauss-Seidel gravity sweep
+ * with the wall mobility, redirect and block at the walls, walled transport.
+ * Up to 64 bodies; the window engine only (SILT_EINVAL on the grid engine). */
+int silt_set_hydro_solids(silt_sheet* s, const silt_hydro_solid* solids, int32_t n);
 
 /* ------------------------------------------------------ one-sheet operator */
 /* Free `step_sheet` (src/fluid_core.rs:770) with the gravity drive on caller

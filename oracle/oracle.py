@@ -101,6 +101,8 @@ def lib():
         L.oracle_core_sample.argtypes = [_p, _f, _f, _p]
         L.oracle_core_fine_water_debug.argtypes = [_p, _p, _i, _i, _p, _p]
         L.oracle_core_inflow.argtypes = [_p, _i, _f, _f, _f]
+        L.oracle_core_set_hydro_solids.argtypes = [_p, _p, _i]
+        L.oracle_core_solid_mask.argtypes = [_p, _p]
         _lib = L
     return _lib
 
@@ -321,6 +323,19 @@ class Core:
         org = np.zeros(2, np.float32)
         lib().oracle_core_fine_water_debug(self.h, arr, len(tires), patch, _ptr(out), _ptr(org))
         return out, org
+
+    SOLID_KEYS = ("x", "z", "yaw", "half_length", "half_width", "bottom_y", "top_y", "contact", "radius", "width")
+
+    def set_hydro_solids(self, solids):
+        """solids: dicts with the HydroSolid fields (src/fluid_core.rs:219-240)."""
+        packed = np.array([[float(sd.get(k, 0.0)) for k in self.SOLID_KEYS] for sd in solids] or [[0.0] * 10],
+                          np.float32)
+        lib().oracle_core_set_hydro_solids(self.h, _ptr(packed), len(solids))
+
+    def solid_mask(self):
+        out = np.zeros(self.res * self.res, np.uint8)
+        lib().oracle_core_solid_mask(self.h, _ptr(out))
+        return out
 
     def set_inflow(self, j, x0, x1, rate_m3_s):
         lib().oracle_core_inflow(self.h, j, x0, x1, rate_m3_s)

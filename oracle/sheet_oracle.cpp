@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <thread>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -470,15 +471,363 @@ void transport_open_serial(float* h, const float* vel, const u8* gate, usize res
         }
 }
 
+// ---------------------------------------------------------------------- walls
+// A body's footprint in the sheet (src/fluid_core.rs:213-240 HydroSolid).
+struct HydroSolid {
+    float x, z, yaw, half_length, half_width, bottom_y, top_y;
+    bool contact;
+    float radius, width;
+};
+
+// src/fluid_core.rs:4584-4594: inside the yawed rectangle (yaw 0 = long axis +Z).
+bool solid_contains(const HydroSolid& s, float x, float z) {
+    const float dx = x - s.x, dz = z - s.z;
+    const float fx = sinf(s.yaw), fz = cosf(s.yaw);
+    const float along = dx * fx + dz * fz;
+    const float lat = dx * fz + dz * (-fx);
+    return fabsf(along) <= rmax(s.half_length, 0.0f) && fabsf(lat) <= rmax(s.half_width, 0.0f);
+}
+
+// src/fluid_core.rs:4596-4604: a wall only where the free surface stands above
+// the underside and the bed below the top.
+bool solid_overlaps(const HydroSolid& s, float x, float z, float eta, float bed) {
+    if (s.half_length <= 1.0e-4f || s.half_width <= 1.0e-4f) return false;
+    if (!solid_contains(s, x, z)) return false;
+    return eta > s.bottom_y + 1.0e-4f && bed < s.top_y;
+}
+
+// src/fluid_core.rs:7288-7360 solid_mask: 2 = wall, 1 = tire contact (contacts
+// are drawn second and win a shared cell). The surface tested is the highest
+// of the cell and its four neighbours (water layer over its bed).
+std::vector<u8> solid_mask(const std::vector<HydroSolid>& solids, usize res, float cell, const float* origin,
+                           const float* water, const float* bed) {
+    std::vector<u8> mask(res * res, 0);
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool contact = pass == 1;
+        const u8 value = contact ? 1 : 2;
+        for (const HydroSolid& s : solids) {
+            if (s.contact != contact) continue;
+            if (s.half_length <= 1.0e-4f || s.half_width <= 1.0e-4f) continue;
+            const float reach = hypotf(rmax(s.half_length, 0.0f), rmax(s.half_width, 0.0f)) + cell;
+            if (!finite(reach) || !finite(s.x) || !finite(s.z)) continue;
+            const float lo_i = floorf((s.x - reach - origin[0]) / cell - 0.5f);
+            const float hi_i = ceilf((s.x + reach - origin[0]) / cell - 0.5f);
+            const float lo_j = floorf((s.z - reach - origin[1]) / cell - 0.5f);
+            const float hi_j = ceilf((s.z + reach - origin[1]) / cell - 0.5f);
+            const float top = (float)(res - 1);
+            if (hi_i < 0.0f || hi_j < 0.0f || lo_i > top || lo_j > top) continue;
+            const usize i0 = f2usize(rmax(lo_i, 0.0f)), i1 = f2usize(rmin(hi_i, top));
+            const usize j0 = f2usize(rmax(lo_j, 0.0f)), j1 = f2usize(rmin(hi_j, top));
+            for (usize j = j0; j <= j1; ++j)
+                for (usize i = i0; i <= i1; ++i) {
+                    const usize idx = j * res + i;
+                    if (mask[idx] == value) continue;
+                    const float x = origin[0] + ((float)i + 0.5f) * cell;
+                    const float z = origin[1] + ((float)j + 0.5f) * cell;
+                    float eta = bed[idx] + water[idx];
+                    if (i > 0) eta = rmax(eta, bed[idx - 1] + water[idx - 1]);
+                    if (i + 1 < res) eta = rmax(eta, bed[idx + 1] + water[idx + 1]);
+                    if (j > 0) eta = rmax(eta, bed[idx - res] + water[idx - res]);
+                    if (j + 1 < res) eta = rmax(eta, bed[idx + res] + water[idx + res]);
+                    if (solid_overlaps(s, x, z, eta, bed[idx])) mask[idx] = value;
+                }
+        }
+    }
+    return mask;
+}
+
+// The four neighbours in the reference's order: (-1,0), (1,0), (0,-1), (0,1).
+static const int NB4[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+
+inline bool in_grid(long i, long j, usize res) { return i >= 0 && j >= 0 && i < (long)res && j < (long)res; }
+
+// src/fluid_core.rs:4382-4444 displace_occupied: a covered column moves, in
+// equal shares, to its open neighbours (the 5 x 5 block when no four-neighbour
+// is open); a column with nowhere to go stays.
+void displace_occupied(float* h, float* u, float* v, const u8* solid, usize res) {
+    std::vector<float> give(res * res, 0.0f);
+    std::vector<usize> neigh;
+    for (usize j = 0; j < res; ++j)
+        for (usize i = 0; i < res; ++i) {
+            const usize idx = j * res + i;
+            if (!solid[idx]) continue;
+            const float vol = h[idx];
+            if (vol <= 1.0e-8f) {
+                h[idx] = u[idx] = v[idx] = 0.0f;
+                continue;
+            }
+            neigh.clear();
+            for (const auto& d : NB4) {
+                const long ni = (long)i + d[0], nj = (long)j + d[1];
+                if (!in_grid(ni, nj, res)) continue;
+                const usize q = (usize)nj * res + (usize)ni;
+                if (!solid[q]) neigh.push_back(q);
+            }
+            if (neigh.empty())
+                for (long dj = -2; dj <= 2; ++dj)
+                    for (long di = -2; di <= 2; ++di) {
+                        const long ni = (long)i + di, nj = (long)j + dj;
+                        if (!in_grid(ni, nj, res)) continue;
+                        const usize q = (usize)nj * res + (usize)ni;
+                        if (!solid[q]) neigh.push_back(q);
+                    }
+            if (neigh.empty()) continue;
+            h[idx] = u[idx] = v[idx] = 0.0f;
+            const float share = vol / (float)neigh.size();
+            for (usize q : neigh) give[q] += share;
+        }
+    for (usize k = 0; k < res * res; ++k)
+        if (give[k] > 0.0f) h[k] += give[k];
+}
+
+// src/fluid_core.rs:4225-4276 lift_solid_surface: a wall cell's surface is the
+// mean of the wet open cells within two cells (its own when there are none).
+void lift_solid_surface(float* eta, const float* h, const u8* solid, usize res, const Box& b, float eps,
+                        float* tmp) {
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (!solid[idx]) continue;
+            float acc = 0.0f, n = 0.0f;
+            for (long dj = -2; dj <= 2; ++dj)
+                for (long di = -2; di <= 2; ++di) {
+                    if (di == 0 && dj == 0) continue;
+                    const long ni = (long)i + di, nj = (long)j + dj;
+                    if (!in_grid(ni, nj, res)) continue;
+                    const usize q = (usize)nj * res + (usize)ni;
+                    if (solid[q] || h[q] <= eps) continue;
+                    acc += eta[q];
+                    n += 1.0f;
+                }
+            tmp[idx] = n > 0.0f ? acc / n : eta[idx];
+        }
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i)
+            if (solid[j * res + i]) eta[j * res + i] = tmp[j * res + i];
+}
+
+// src/fluid_core.rs:4278-4326 write_noslip_ghost: a wall cell takes minus the
+// mean velocity of its wet open four-neighbours (zero when there are none).
+void write_noslip_ghost(float* u, float* v, const float* h, const u8* solid, usize res, const Box& b, float eps) {
+    std::vector<std::tuple<usize, float, float>> ghosts;
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (!solid[idx]) continue;
+            float au = 0.0f, av = 0.0f, n = 0.0f;
+            for (const auto& d : NB4) {
+                const long ni = (long)i + d[0], nj = (long)j + d[1];
+                if (!in_grid(ni, nj, res)) continue;
+                const usize q = (usize)nj * res + (usize)ni;
+                if (solid[q] || h[q] <= eps) continue;
+                au += u[q];
+                av += v[q];
+                n += 1.0f;
+            }
+            if (n > 0.0f)
+                ghosts.emplace_back(idx, -au / n, -av / n);
+            else
+                ghosts.emplace_back(idx, 0.0f, 0.0f);
+        }
+    for (const auto& g : ghosts) {
+        u[std::get<0>(g)] = std::get<1>(g);
+        v[std::get<0>(g)] = std::get<2>(g);
+    }
+}
+
+// src/fluid_core.rs:4328-4380 block_into_solid: a wet open cell loses the
+// part of its velocity that points into a wall neighbour, direction by
+// direction in the neighbour order.
+void block_into_solid(float* u, float* v, const float* h, const u8* solid, usize res, const Box& b, float eps) {
+    std::vector<std::tuple<usize, float, float>> next;
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (solid[idx] || h[idx] <= eps) continue;
+            float ux = u[idx], vx = v[idx];
+            bool hit = false;
+            for (const auto& d : NB4) {
+                const long ni = (long)i + d[0], nj = (long)j + d[1];
+                if (!in_grid(ni, nj, res)) continue;
+                if (!solid[(usize)nj * res + (usize)ni]) continue;
+                const float nx = (float)d[0], nz = (float)d[1];
+                const float vn = ux * nx + vx * nz;
+                if (vn > 0.0f) {
+                    ux -= vn * nx;
+                    vx -= vn * nz;
+                    hit = true;
+                }
+            }
+            if (hit) next.emplace_back(idx, ux, vx);
+        }
+    for (const auto& t : next) {
+        u[std::get<0>(t)] = std::get<1>(t);
+        v[std::get<0>(t)] = std::get<2>(t);
+    }
+}
+
+// src/fluid_core.rs:4446-4563 redirect_into_walls: the discharge aimed at a
+// wall (the cell's own, or the stream feeding it when that is faster) turns
+// aside to the open flanks, as much as stands above their mean depth.
+void redirect_into_walls(float* h, const float* u, const float* v, const u8* solid, const float* bed, usize res,
+                         float cell, float dt, const Box& b, Scratch& sc) {
+    const usize ri0 = sat_sub(b.i0, 1), ri1 = std::min(b.i1 + 1, res - 1);
+    const usize rj0 = sat_sub(b.j0, 1), rj1 = std::min(b.j1 + 1, res - 1);
+    for (usize j = rj0; j <= rj1; ++j)
+        for (usize i = ri0; i <= ri1; ++i) sc.removed[j * res + i] = sc.added[j * res + i] = 0.0f;
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (solid[idx] || h[idx] < 0.02f) continue;
+            for (const auto& d : NB4) {
+                const long di = d[0], dj = d[1];
+                const long ni = (long)i + di, nj = (long)j + dj;
+                if (!in_grid(ni, nj, res)) continue;
+                if (!solid[(usize)nj * res + (usize)ni]) continue;
+                float vn = u[idx] * (float)di + v[idx] * (float)dj;
+                const long ui = (long)i - di, uj = (long)j - dj;
+                if (in_grid(ui, uj, res)) {
+                    const usize up = (usize)uj * res + (usize)ui;
+                    if (!solid[up]) {
+                        const float feed = u[up] * (float)di + v[up] * (float)dj;
+                        if (feed > vn) vn = feed;
+                    }
+                }
+                if (vn < 0.05f) continue;
+                const long perp[2][2] = {{di != 0 ? 0 : -1, di != 0 ? -1 : 0}, {di != 0 ? 0 : 1, di != 0 ? 1 : 0}};
+                usize dest[2] = {0, 0};
+                usize n_dest = 0;
+                float flank = 0.0f;
+                for (const auto& pq : perp) {
+                    const long qi = (long)i + pq[0], qj = (long)j + pq[1];
+                    if (!in_grid(qi, qj, res)) continue;
+                    const usize q = (usize)qj * res + (usize)qi;
+                    if (solid[q]) continue;
+                    if (h[q] <= 1.0e-6f && bed[q] > bed[idx] + h[idx] + 1.0e-3f) continue;
+                    dest[n_dest++] = q;
+                    flank += h[q];
+                }
+                if (n_dest == 0) continue;
+                const float excess = h[idx] - flank / (float)n_dest;
+                if (excess < 2.0e-3f) continue;
+                const float room = h[idx] - sc.removed[idx];
+                if (room < 1.0e-6f) continue;
+                const float frac = rmin(vn * dt / cell, 0.45f);
+                const float dh = rmin(rmin(excess, h[idx] * frac), room);
+                if (dh < 1.0e-8f) continue;
+                sc.removed[idx] += dh;
+                const float share = dh / (float)n_dest;
+                for (usize k = 0; k < n_dest; ++k) sc.added[dest[k]] += share;
+            }
+        }
+    for (usize j = rj0; j <= rj1; ++j)
+        for (usize i = ri0; i <= ri1; ++i) {
+            const usize idx = j * res + i;
+            if (sc.removed[idx] > 0.0f || sc.added[idx] > 0.0f)
+                h[idx] = rmax(h[idx] - sc.removed[idx] + sc.added[idx], 0.0f);
+        }
+}
+
+// src/fluid_core.rs:4565-4582 solid_near (radius 1): a wall among the eight neighbours.
+bool solid_near(const u8* mask, usize res, usize i, usize j) {
+    for (long dj = -1; dj <= 1; ++dj)
+        for (long di = -1; di <= 1; ++di) {
+            if (di == 0 && dj == 0) continue;
+            const long ni = (long)i + di, nj = (long)j + dj;
+            if (in_grid(ni, nj, res) && mask[(usize)nj * res + (usize)ni]) return true;
+        }
+    return false;
+}
+
+// src/fluid_core.rs:2084-2129 force_gravity_solid, the serial sweep (the step
+// pair runs its sheets with serial inner loops): gravity, with the mobility
+// raised to at least 1 beside a wall under 8 cm of water, then the
+// confinement kick, cell by cell in raster order.
+void force_gravity_solid(const float* h, float* u, float* v, const float* nu, const float* p, const u8* mask,
+                         usize res, float cell, float dt, float vorticity, float eps, const Box& b, bool inner_par) {
+    if (b.j1 - b.j0 >= 47 && b.i1 - b.i0 >= 31 && inner_par) {
+        // force_gravity_solid_par (:2131-2202): gravity on every cell first,
+        // then the same forward confinement sweep.
+        for (usize j = b.j0; j <= b.j1; ++j)
+            for (usize i = b.i0; i <= b.i1; ++i) {
+                const usize idx = j * res + i;
+                if (h[idx] <= eps) continue;
+                float px, pz;
+                grad(p, res, i, j, cell, px, pz);
+                float mob = sheet_mobility_for(nu[idx]);
+                if (h[idx] > 0.08f && solid_near(mask, res, i, j)) mob = rmax(mob, 1.0f);
+                u[idx] += -GRAVITY * px * mob * dt;
+                v[idx] += -GRAVITY * pz * mob * dt;
+            }
+        if (vorticity <= 0.0f) return;
+        for (usize j = b.j0; j <= b.j1; ++j)
+            for (usize i = b.i0; i <= b.i1; ++i)
+                if (h[j * res + i] > eps) confine_one(u, v, u, v, res, i, j, cell, dt, vorticity);
+        return;
+    }
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (h[idx] <= eps) continue;
+            float px, pz;
+            grad(p, res, i, j, cell, px, pz);
+            float mob = sheet_mobility_for(nu[idx]);
+            if (h[idx] > 0.08f && solid_near(mask, res, i, j)) mob = rmax(mob, 1.0f);
+            u[idx] += -GRAVITY * px * mob * dt;
+            v[idx] += -GRAVITY * pz * mob * dt;
+            if (vorticity > 0.0f) confine_one(u, v, u, v, res, i, j, cell, dt, vorticity);
+        }
+}
+
+// src/fluid_core.rs:3894-3963 transport with move_edge_bufs (:4178-4223): the
+// walled donor-cell flux. An edge touching a wall moves nothing; a dry bank
+// above the donor's surface takes nothing.
+void transport_walled(float* h, const float* vel, const u8* gate, usize res, float cell, float dt, const Box& b,
+                      bool along_x, const u8* solid, const float* bed, Scratch& sc) {
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) sc.removed[j * res + i] = sc.added[j * res + i] = 0.0f;
+    auto edge = [&](usize a, usize c) {
+        if (solid[a] || solid[c]) return;
+        const float speed = 0.5f * (vel[a] + vel[c]);
+        if (fabsf(speed) < 1.0e-5f) return;
+        const usize donor = speed > 0.0f ? a : c, recv = speed > 0.0f ? c : a;
+        if (h[recv] <= 1.0e-6f && bed[recv] > bed[donor] + h[donor] + 1.0e-3f) return;
+        const float room = h[donor] - sc.removed[donor];
+        if (room <= 1.0e-8f) return;
+        if (gate[recv] == 0 && h[recv] <= 1.0e-6f) return;
+        const float frac = rmin(fabsf(speed) * dt / cell, 0.45f);
+        const float dh = rmin(h[donor] * frac, room);
+        if (dh <= 1.0e-8f) return;
+        sc.removed[donor] += dh;
+        sc.added[recv] += dh;
+    };
+    if (along_x) {
+        for (usize j = b.j0; j <= b.j1; ++j)
+            for (usize i = b.i0; i < b.i1; ++i) edge(j * res + i, j * res + i + 1);
+    } else {
+        for (usize j = b.j0; j < b.j1; ++j)
+            for (usize i = b.i0; i <= b.i1; ++i) edge(j * res + i, (j + 1) * res + i);
+    }
+    for (usize j = b.j0; j <= b.j1; ++j)
+        for (usize i = b.i0; i <= b.i1; ++i) {
+            const usize idx = j * res + i;
+            if (sc.removed[idx] > 0.0f || sc.added[idx] > 0.0f)
+                h[idx] = rmax(h[idx] - sc.removed[idx] + sc.added[idx], 0.0f);
+        }
+}
+
 // -------------------------------------------------------------------- substep
 // src/fluid_core.rs:1879-2082, open sheet (no walls), gravity drive.
 void substep(float* h, float* u, float* v, const float* bed, const float* nu, const u8* gate,
              usize res, float cell, float dt, float vorticity, float eps, usize i0, usize i1,
-             usize j0, usize j1, bool banks, bool do_flux, Scratch& sc, bool inner_par) {
+             usize j0, usize j1, bool banks, bool do_flux, Scratch& sc, bool inner_par,
+             const u8* solid = nullptr) {
+    const Box box{i0, i1, j0, j1};
     usize hi0 = sat_sub(i0, 2), hi1 = std::min(i1 + 2, res - 1);
     usize hj0 = sat_sub(j0, 2), hj1 = std::min(j1 + 2, res - 1);
     for (usize j = hj0; j <= hj1; ++j)
         for (usize i = hi0; i <= hi1; ++i) sc.a[j * res + i] = bed[j * res + i] + h[j * res + i];
+    if (solid) lift_solid_surface(sc.a.data(), h, solid, res, box, eps, sc.e.data());
     blur_box(sc.a.data(), sc.b.data(), sc.e.data(), res, i0, i1, j0, j1, GAUSS);
     blur_box(sc.a.data(), sc.c.data(), sc.e.data(), res, i0, i1, j0, j1, STEEP);
     for (usize j = j0; j <= j1; ++j)
@@ -487,8 +836,13 @@ void substep(float* h, float* u, float* v, const float* bed, const float* nu, co
             float filtered = 0.62f * sc.b[idx] + 0.38f * sc.c[idx];
             sc.d[idx] = 0.45f * filtered + 0.55f * sc.a[idx];
         }
-    force_gravity_open(h, u, v, nu, sc.d.data(), res, cell, dt, vorticity, eps, i0, i1, j0, j1, inner_par);
-    bool project = cell > FINE_CELL_M + 1.0e-6f;
+    if (solid) {
+        write_noslip_ghost(u, v, h, solid, res, box, eps);
+        force_gravity_solid(h, u, v, nu, sc.d.data(), solid, res, cell, dt, vorticity, eps, box, inner_par);
+    } else {
+        force_gravity_open(h, u, v, nu, sc.d.data(), res, cell, dt, vorticity, eps, i0, i1, j0, j1, inner_par);
+    }
+    bool project = solid || cell > FINE_CELL_M + 1.0e-6f;
     if (project) {
         for (usize j = j0; j <= j1; ++j)
             for (usize i = i0; i <= i1; ++i) {
@@ -529,10 +883,20 @@ void substep(float* h, float* u, float* v, const float* bed, const float* nu, co
             u[idx] = finite_speed(u[idx] * decay, FILM_SPEED_CAP_MPS);
             v[idx] = finite_speed(v[idx] * decay, FILM_SPEED_CAP_MPS);
         }
+    if (solid) {
+        redirect_into_walls(h, u, v, solid, bed, res, cell, dt, box, sc);
+        block_into_solid(u, v, h, solid, res, box, eps);
+        write_noslip_ghost(u, v, h, solid, res, box, eps);
+    }
     if (!do_flux) return;
-    const float* open_bed = banks ? bed : nullptr;
-    transport_open_rows(banks, h, u, gate, res, cell, dt, i0, i1, j0, j1, true, open_bed, 0.45f, sc);
-    transport_open_rows(banks, h, v, gate, res, cell, dt, i0, i1, j0, j1, false, open_bed, 0.45f, sc);
+    if (solid) {
+        transport_walled(h, u, gate, res, cell, dt, box, true, solid, bed, sc);
+        transport_walled(h, v, gate, res, cell, dt, box, false, solid, bed, sc);
+    } else {
+        const float* open_bed = banks ? bed : nullptr;
+        transport_open_rows(banks, h, u, gate, res, cell, dt, i0, i1, j0, j1, true, open_bed, 0.45f, sc);
+        transport_open_rows(banks, h, v, gate, res, cell, dt, i0, i1, j0, j1, false, open_bed, 0.45f, sc);
+    }
     for (usize j = j0; j <= j1; ++j)
         for (usize i = i0; i <= i1; ++i) {
             usize idx = j * res + i;
@@ -836,8 +1200,8 @@ void pace3_slices(float* h, float* u, float* v, const u8* gate, usize res, float
 void step_sheet_scratch(float* h, float* u, float* v, const float* bed, const float* nu,
                         const u8* gate, usize res, float cell, float dt, float vorticity, float eps,
                         bool banks, float sub_cap, int pace, Scratch& sc, Scratch* sc2,
-                        bool inner_par) {
-    bool open_fine = cell <= FINE_CELL_M + 1.0e-6f;
+                        bool inner_par, const u8* solid = nullptr) {
+    bool open_fine = !solid && cell <= FINE_CELL_M + 1.0e-6f;
     bool fine_open = open_fine && pace == 0;
     bool whole_wet = open_fine && (pace == 2 || pace == 3);
     bool awake = open_fine && !whole_wet && !fine_open;
@@ -865,7 +1229,7 @@ void step_sheet_scratch(float* h, float* u, float* v, const float* bed, const fl
     float dts = dt / (float)nsub;
     if (pace == 3 && whole_wet && nsub > 1) {
         auto run = [&](const Box& b, Scratch& s) {
-            substep(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, false, s, inner_par);
+            substep(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, false, s, inner_par, solid);
             pace3_slices(h, u, v, gate, res, cell, dts, nsub, eps, b, s);
         };
         if (sc2 && boxes.size() == 2 && boxes_apart(boxes[0], boxes[1], BOX_PAR_GAP)) {
@@ -879,26 +1243,27 @@ void step_sheet_scratch(float* h, float* u, float* v, const float* bed, const fl
     if (sc2 && boxes.size() == 2 && boxes_apart(boxes[0], boxes[1], BOX_PAR_GAP)) {
         for (uint32_t s = 0; s < nsub; ++s) {
             // The two boxes step on two workers with serial inner loops.
-            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[0].i0, boxes[0].i1, boxes[0].j0, boxes[0].j1, banks, true, sc, false);
-            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[1].i0, boxes[1].i1, boxes[1].j0, boxes[1].j1, banks, true, *sc2, false);
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[0].i0, boxes[0].i1, boxes[0].j0, boxes[0].j1, banks, true, sc, false, solid);
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, boxes[1].i0, boxes[1].i1, boxes[1].j0, boxes[1].j1, banks, true, *sc2, false, solid);
         }
         return;
     }
     for (uint32_t s = 0; s < nsub; ++s)
         for (const Box& b : boxes)
-            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, true, sc, inner_par);
+            substep(h, u, v, bed, nu, gate, res, cell, dts, vorticity, eps, b.i0, b.i1, b.j0, b.j1, banks, true, sc, inner_par, solid);
 }
 
 // src/fluid_core.rs:821-889 step_sheet_eps_in / step_sheet_eps
 void step_sheet_eps(float* h, float* u, float* v, const float* bed, const float* nu, const u8* gate,
                     usize res, float cell, float dt, float vorticity, float eps, bool banks,
-                    float sub_cap, int pace, Scratch& sc, Scratch* sc2, bool inner_par) {
+                    float sub_cap, int pace, Scratch& sc, Scratch* sc2, bool inner_par, const u8* solid = nullptr) {
     if (dt <= 0.0f || res == 0) return;
     float sum = wet_sum(h, res * res, eps);
     if (sum <= eps) return;
     sc.fit(res * res);
     if (sc2) sc2->fit(res * res);
-    step_sheet_scratch(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, banks, sub_cap, pace, sc, sc2, inner_par);
+    step_sheet_scratch(h, u, v, bed, nu, gate, res, cell, dt, vorticity, eps, banks, sub_cap, pace, sc, sc2, inner_par,
+                       solid);
 }
 
 // src/fluid_core.rs:9594-9622 (no reach band)
@@ -1064,6 +1429,8 @@ struct Core {
     bool wave_on = false;
     float wave_x0 = 0, wave_x1 = 0, wave_z0 = 0, wave_z1 = 0, wave_dx = 0, wave_dz = 0, wave_amp = 0, wave_period = 0,
           wave_ramp = 0, wave_t = 0;
+    // src/fluid_core.rs:5257-5264 set_hydro_solids: walls in the sheet.
+    std::vector<HydroSolid> solids;
 
     explicit Core(const oracle_core_cfg& c) : cfg(c) {
         res = (usize)c.res;
@@ -1580,9 +1947,16 @@ struct Core {
                 oc1 = std::min(f2usize(rmax(ceilf((reach_cross1 - o) / cfg.cell), 0.0f)), res);
                 open_axis = reach_along_z ? 1 : 0;
             }
+            // src/fluid_core.rs:7954-7967: one wall mask for both sheets, from
+            // the water before either steps; each sheet first pushes its
+            // columns out of the covered cells (:8057-8059, :8098-8100).
+            std::vector<u8> cmask;
+            if (!solids.empty()) cmask = solid_mask(solids, res, cfg.cell, origin, water.data(), bed.data());
+            const u8* cm = cmask.empty() ? nullptr : cmask.data();
             auto run_water = [&]() {
                 if (cfg.soften) soften_border(uw.data(), vw.data(), res, open_axis, oc0, oc1);
-                step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0);
+                if (cm) displace_occupied(water.data(), uw.data(), vw.data(), cm, res);
+                step_sheet_eps(water.data(), uw.data(), vw.data(), bed.data(), nu_w.data(), gate.data(), res, cfg.cell, dt, 0.08f, 1.0e-6f, false, cap, pace, coarse_sc[0][0], &coarse_sc[0][1], cfg.inner_par != 0, cm);
             };
             auto run_slurry = [&]() {
                 Box wb;
@@ -1593,7 +1967,8 @@ struct Core {
                             nu_s[idx] = dynamic_viscosity(grain[idx], moisture[idx]);
                         }
                 if (cfg.soften) soften_border(us.data(), vs.data(), res, open_axis, oc0, oc1);
-                step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0);
+                if (cm) displace_occupied(slurry.data(), us.data(), vs.data(), cm, res);
+                step_sheet_eps(slurry.data(), us.data(), vs.data(), bed.data(), nu_s.data(), gate.data(), res, cfg.cell, dt, 0.05f, 1.0e-6f, false, cap, pace, coarse_sc[1][0], &coarse_sc[1][1], cfg.inner_par != 0, cm);
             };
             // src/fluid_core.rs:8127-8131: the two sheets on two workers.
             if (cfg.threads > 1) {
@@ -1609,10 +1984,18 @@ struct Core {
         // Each patch's slurry reads its own viscosity row (patches run on
         // their own workers when threads > 1; results do not depend on it).
         if (fnu_s_rows.size() < active_patches()) fnu_s_rows.resize(active_patches(), std::vector<float>(fres * fres, 0.0f));
+        // Each patch's wall mask, from its water over its bed (solid_mask(true)).
+        std::vector<std::vector<u8>> fmask(active_patches());
+        if (!solids.empty())
+            for (usize pk = 0; pk < active_patches(); ++pk)
+                fmask[pk] = solid_mask(solids, fres, cfg.fine_cell, patches[pk].origin, patches[pk].water.data(),
+                                       patches[pk].bed.data());
         auto run_patch = [&](usize pk, int layer) {
             Patch& P = patches[pk];
+            const u8* fm = fmask[pk].empty() ? nullptr : fmask[pk].data();
             if (layer == 0) {
-                step_sheet_eps(P.water.data(), P.uw.data(), P.vw.data(), P.bed.data(), fnu_w.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.08f, 1.0e-6f, false, cap, pace, P.sc[0][0], &P.sc[0][1], false);
+                if (fm) displace_occupied(P.water.data(), P.uw.data(), P.vw.data(), fm, fres);
+                step_sheet_eps(P.water.data(), P.uw.data(), P.vw.data(), P.bed.data(), fnu_w.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.08f, 1.0e-6f, false, cap, pace, P.sc[0][0], &P.sc[0][1], false, fm);
                 return;
             }
             std::vector<float>& nu = fnu_s_rows[pk];
@@ -1623,7 +2006,8 @@ struct Core {
                         usize idx = j * fres + i;
                         nu[idx] = dynamic_viscosity(P.grain[idx], P.moisture[idx]);
                     }
-            step_sheet_eps(P.slurry.data(), P.us.data(), P.vs.data(), P.bed_slurry.data(), nu.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.05f, 1.0e-6f, false, cap, pace, P.sc[1][0], &P.sc[1][1], false);
+            if (fm) displace_occupied(P.slurry.data(), P.us.data(), P.vs.data(), fm, fres);
+            step_sheet_eps(P.slurry.data(), P.us.data(), P.vs.data(), P.bed_slurry.data(), nu.data(), fgate.data(), fres, cfg.fine_cell, dt, 0.05f, 1.0e-6f, false, cap, pace, P.sc[1][0], &P.sc[1][1], false, fm);
         };
         if (cfg.threads > 1) {
             std::vector<std::thread> pool;
@@ -2313,6 +2697,22 @@ void oracle_core_set_river_reach(void* cp, int on, int along_z, int positive, fl
     C.reach_speed = inlet_speed;
 }
 float oracle_core_reach_bank(void* cp) { return ((Core*)cp)->reach_bank_m3; }
+// Solids as 10 floats each: x, z, yaw, half_length, half_width, bottom_y,
+// top_y, contact (0/1), radius, width.
+void oracle_core_set_hydro_solids(void* cp, const float* packed, int n) {
+    Core& C = *(Core*)cp;
+    C.solids.clear();
+    for (int k = 0; k < n; ++k) {
+        const float* f = packed + 10 * k;
+        C.solids.push_back(HydroSolid{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7] != 0.0f, f[8], f[9]});
+    }
+}
+// The wall mask the next coarse step pair would use (res^2 bytes).
+void oracle_core_solid_mask(void* cp, uint8_t* out) {
+    Core& C = *(Core*)cp;
+    std::vector<u8> m = solid_mask(C.solids, C.res, C.cfg.cell, C.origin, C.water.data(), C.bed.data());
+    memcpy(out, m.data(), m.size());
+}
 // src/fluid_core.rs:5306-5309 set_wave_maker (restarts the paddle clock).
 void oracle_core_set_wave_maker(void* cp, int on, float x0, float x1, float z0, float z1, float dir_x, float dir_z,
                                 float amplitude, float period, float ramp) {
