@@ -2,12 +2,13 @@
 
 Tolerance (from the build's pass criteria): max |dh| <= 1e-4 m per layer after
 100 steps. The window engine (windows up to 512 cells) steps box by box with
-the reference's Gauss-Seidel confinement; the only source of difference is
-the slurry damping factor, which uses CUDA's expf/powf. The water layer's
-damping factor is computed on the host with the reference's libm, so the
-water depths must match bit for bit. The grid engine (large grids) confines
-from a snapshot, the reference's free-operator form, which moves config-1
-depths by under 1e-6 m.
+the reference's Gauss-Seidel confinement. The water layer's damping factor
+is computed on the host with the reference's libm; the slurry's powf and expf
+are the double-precision functions rounded once, which agree with the C
+library's on all but a few inputs in 10^4, so on these scenes both layers
+match bit for bit. The grid engine (large grids) confines from a snapshot,
+the reference's free-operator form, which moves config-1 depths by under
+1e-6 m.
 """
 import numpy as np
 import pytest
@@ -55,6 +56,14 @@ def test_window200_water_is_bit_exact_after_100_steps():
     a, b = ref.get("water"), dev.get("water")
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), float(np.abs(a - b).max())
     for name in ("uw", "vw"):
+        a, b = ref.get(name), dev.get(name)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (name, float(np.abs(a - b).max()))
+
+
+def test_window200_slurry_is_bit_exact_after_100_steps():
+    scene = S.window200()
+    ref, dev, _ = run_pair(100, scene)
+    for name in ("slurry", "us", "vs"):
         a, b = ref.get(name), dev.get(name)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (name, float(np.abs(a - b).max()))
 
