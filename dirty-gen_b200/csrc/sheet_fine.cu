@@ -1534,16 +1534,17 @@ int move_window(Patches& P, silt_sheet* s, int di, int dj, bool scroll) {
 }
 
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut,
-                 double* reach) {
+                 double* reach, double* eroded) {
     Impl& M = I(P);
     SheetView W = view_of(s);
-    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 5 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 6 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
     FCK(cudaStreamSynchronize(W.st));
     *spray = M.h_books[0];
     *park_w = M.h_books[1];
     *park_s = M.h_books[2];
     if (cut) *cut = M.h_books[3];
     if (reach) *reach = M.h_books[4];
+    if (eroded) *eroded = M.h_books[5];
     return SILT_OK;
 }
 

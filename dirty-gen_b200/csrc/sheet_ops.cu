@@ -238,7 +238,7 @@ __global__ void k_friction(const float* h, float* u, float* v, const float* du, 
         if (gn2 > 0.0f) {
             const float hv = h[idx];
             if (hv > 1.0e-4f) {
-                const float speed = hypotf(uu, vv);
+                const float speed = hypot_rn(uu, vv);
                 if (speed > 0.0f) {
                     const float kk = gn2 * speed / pow_rn(fmaxf(hv, 0.002f), 4.0f / 3.0f);
                     const float keep = 1.0f / (1.0f + dt * kk);

@@ -122,6 +122,10 @@ struct silt_sheet {
     cudaEvent_t solid_ev[2] = {nullptr, nullptr};
     int solid_slot = 0;
     uint8_t* d_wall_mask = nullptr;  // the coarse window's mask (res^2)
+    std::vector<silt_hydro_solid> solids;        // as set, for the buoyancy read-back
+    float* d_bed_drop = nullptr;                 // scour depth per coarse cell (res^2)
+    double* d_wall_out = nullptr;                // hydro_load sums: 4 + 3 x MAX_SOLIDS
+    unsigned int* d_hole_bits = nullptr;         // the deepest scour (float bits)
     // Grid engine: active-tile flags and the substep's tile list.
     silt::TileFlags tf;
     uint8_t* tile_mem = nullptr;
@@ -639,6 +643,9 @@ int silt_sheet_destroy(silt_sheet* s) {
     for (int k = 0; k < 2; ++k)
         if (s->solid_ev[k]) cudaEventDestroy(s->solid_ev[k]);
     cudaFree(s->d_wall_mask);
+    cudaFree(s->d_bed_drop);
+    cudaFree(s->d_wall_out);
+    cudaFree(s->d_hole_bits);
     for (int k = 0; k < 2; ++k)
         if (s->win_ev[k]) cudaEventDestroy(s->win_ev[k]);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -927,6 +934,35 @@ int wave_step(silt_sheet* s, float dt) {
     return SILT_OK;
 }
 
+// scour_contacts (src/fluid_core.rs:7364-7420) after the coarse peel, from
+// the mask of the state the step left.
+int scour_step(silt_sheet* s, float dt) {
+    if (s->n_solids == 0 || !(dt > 0.0f)) return SILT_OK;
+    CK(silt::walls::launch_mask(s->d_wall_mask, s->res, s->cfg.cell, s->origin[0], s->origin[1], s->H(0), s->bed,
+                                s->fine.d_solids, s->n_solids, s->st));
+    silt::walls::ScourPlanes P;
+    P.mask = s->d_wall_mask;
+    P.water = s->H(0);
+    P.uw = s->U(0);
+    P.vw = s->V(0);
+    P.bed = s->bed;
+    P.slurry = s->H(1);
+    P.us = s->U(1);
+    P.vs = s->V(1);
+    P.moisture = s->moisture;
+    P.bed_drop = s->d_bed_drop;
+    P.grain = s->grain;
+    P.res = s->res;
+    P.area = s->cfg.cell * s->cfg.cell;
+    P.dt = dt;
+    P.eroded = silt::fine::books(s->fine) + 5;
+    P.slurry_sum = s->d_acc + 1;
+    P.hole_bits = s->d_hole_bits;
+    CK(silt::walls::launch_scour(P, s->st));
+    s->mat_dirty = true;
+    return SILT_OK;
+}
+
 // feed_reach (src/fluid_core.rs:7638-7745).
 int reach_step(silt_sheet* s) {
     if (!s->reach_on) return SILT_OK;
@@ -1032,6 +1068,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     if ((rc = open_water_step(s, dt))) return rc;
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
+    if ((rc = scour_step(s, dt))) return rc;
     if ((rc = reach_step(s))) return rc;
     if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
@@ -1238,6 +1275,11 @@ int silt_set_hydro_solids(silt_sheet* s, const silt_hydro_solid* solids, int32_t
         CK(cudaMallocHost(&s->h_solids, bytes));
         for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&s->solid_ev[k], cudaEventDisableTiming));
         CK(cudaMalloc(&s->d_wall_mask, s->n));
+        CK(cudaMalloc(&s->d_bed_drop, s->n * sizeof(float)));
+        CK(cudaMemsetAsync(s->d_bed_drop, 0, s->n * sizeof(float), s->st));
+        CK(cudaMalloc(&s->d_wall_out, (4 + 3 * silt::walls::MAX_SOLIDS) * sizeof(double)));
+        CK(cudaMalloc(&s->d_hole_bits, sizeof(unsigned int)));
+        CK(cudaMemsetAsync(s->d_hole_bits, 0, sizeof(unsigned int), s->st));
     }
     if (n > 0) {
         const int slot = s->solid_slot ^ 1;
@@ -1254,8 +1296,74 @@ int silt_set_hydro_solids(silt_sheet* s, const silt_hydro_solid* solids, int32_t
         s->solid_slot = slot;
     }
     s->n_solids = n;
+    s->solids.assign(solids, solids + n);
     s->fine.d_solids = n > 0 ? s->d_solids + (size_t)s->solid_slot * silt::walls::MAX_SOLIDS : nullptr;
     s->fine.n_solids = n;
+    return SILT_OK;
+}
+
+// src/fluid_core.rs:4606-4615 cylinder_segment_volume (C library acosf, sqrtf).
+static float cylinder_segment_volume(float depth, float radius, float width) {
+    const float d = silt::host::rclamp(depth, 0.0f, radius * 2.0f);
+    if (d <= 1.0e-4f || width <= 0.0f || radius <= 1.0e-3f) return 0.0f;
+    const float c = silt::host::rclamp((radius - d) / radius, -1.0f, 1.0f);
+    const float area =
+        radius * radius * std::acos(c) - (radius - d) * std::sqrt(std::fmax(2.0f * radius * d - d * d, 0.0f));
+    return std::fmax(area, 0.0f) * width;
+}
+
+int silt_get_hydro_load(silt_sheet* s, silt_hydro_load* out) {
+    if (!s || !out) return fail_arg("hydro_load");
+    CK(cudaSetDevice(s->cfg.device));
+    memset(out, 0, sizeof *out);
+    const int n = s->n_solids;
+    std::vector<double> acc(4 + 3 * (size_t)n, 0.0);
+    unsigned int hole_bits = 0;
+    if (n > 0) {
+        CK(silt::walls::launch_mask(s->d_wall_mask, s->res, s->cfg.cell, s->origin[0], s->origin[1], s->H(0), s->bed,
+                                    s->fine.d_solids, n, s->st));
+        CK(silt::walls::launch_load(s->d_wall_mask, s->H(0), s->U(0), s->V(0), s->bed, s->res, s->cfg.cell,
+                                    s->origin[0], s->origin[1], s->fine.d_solids, n, s->d_wall_out, s->st));
+        CK(cudaMemcpyAsync(acc.data(), s->d_wall_out, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    }
+    if (s->d_hole_bits)
+        CK(cudaMemcpyAsync(&hole_bits, s->d_hole_bits, sizeof hole_bits, cudaMemcpyDeviceToHost, s->st));
+    double spray = 0.0, park_w = 0.0, park_s = 0.0, eroded = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, nullptr, nullptr, &eroded);
+    if (rc) return rc;
+    out->force_x = (float)acc[0];
+    out->force_z = (float)acc[1];
+    out->wheel_blocks = (uint32_t)acc[2];
+    out->belly_blocks = (uint32_t)acc[3];
+    const float rho_g = 1000.0f * 9.81f;
+    float wheel_b = 0.0f, hull_b = 0.0f, displaced = 0.0f;
+    for (int k = 0; k < n; ++k) {
+        const double cnt = acc[4 + 3 * (size_t)k + 2];
+        if (cnt < 1.0) continue;
+        const float bed = (float)(acc[4 + 3 * (size_t)k] / cnt);
+        const float water = (float)(acc[4 + 3 * (size_t)k + 1] / cnt);
+        const silt_hydro_solid& b = s->solids[k];
+        if (b.radius > 0.0f) {
+            const float vol = cylinder_segment_volume(water, b.radius, b.width);
+            displaced += vol;
+            wheel_b += rho_g * vol;
+        } else {
+            const float eta = bed + water;
+            const float height = std::fmax(b.top_y - b.bottom_y, 0.0f);
+            const float sub = silt::host::rclamp(eta - b.bottom_y, 0.0f, height);
+            const float vol = (b.half_length * 2.0f) * (b.half_width * 2.0f) * sub * 0.36f;
+            displaced += vol;
+            hull_b += rho_g * vol;
+        }
+    }
+    out->buoyancy_n = wheel_b + hull_b;
+    out->hull_buoyancy_n = hull_b;
+    out->wheel_buoyancy_n = wheel_b;
+    out->displaced_m3 = displaced;
+    out->eroded_m3 = (float)eroded;
+    float hole;
+    memcpy(&hole, &hole_bits, sizeof hole);
+    out->hole_m = hole;
     return SILT_OK;
 }
 
@@ -1355,8 +1463,8 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach);
+    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -1369,7 +1477,7 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->frozen_water_m3 = park_w;
     out->frozen_slurry_m3 = park_s;
     out->spray_m3 = spray;
-    out->opened_m3 = s->opened_m3;
+    out->opened_m3 = s->opened_m3 + eroded;
     out->total_m3 = w + sl + park_w + park_s + spray + reach;
     out->cut_m3 = cut;
     out->reach_m3 = reach;

@@ -20,7 +20,7 @@ struct SolidGeom {
     float reach0;       // hypot(hl, hw); the grid adds one cell
     int32_t contact;    // 1: tire contact (drawn over walls)
     int32_t valid;      // 0: skipped (degenerate extent, or x, z not finite)
-    int32_t pad;
+    float ring;         // max(half_length, half_width) + 0.55: ring_surface's reach
 };
 
 constexpr int MAX_SOLIDS = 64;
@@ -68,6 +68,37 @@ __device__ __forceinline__ uint8_t mask_value(const SolidGeom* geoms, int n, int
     }
     return v;
 }
+
+// scour_contacts (src/fluid_core.rs:7364-7420) on the coarse window, from its
+// wall mask: the cut bed goes into the slurry sheet; `eroded` (FP64 m^3) and
+// `hole_bits` (the deepest cut, float bits) accumulate.
+struct ScourPlanes {
+    const uint8_t* mask;
+    const float* water;
+    const float* uw;
+    const float* vw;
+    float* bed;
+    float* slurry;
+    float* us;
+    float* vs;
+    float* moisture;
+    float* bed_drop;
+    uint8_t* grain;
+    int res;
+    float area, dt;
+    double* eroded;       // m^3: each cut cell's actual slurry change times its area
+    double* slurry_sum;   // the step's FP64 slurry depth sum, kept current
+    unsigned int* hole_bits;
+};
+cudaError_t launch_scour(const ScourPlanes& P, cudaStream_t st);
+
+// hydro_load's sums (:7164-7249) from the window's wall mask: out[0..1]
+// force x, z (N, FP64 sums of the reference's f32 terms), out[2..3] contact and
+// wall cell counts, then per body k out[4 + 3k ..] the ring's bed sum, water
+// sum and cell count (:7251-7286).
+cudaError_t launch_load(const uint8_t* mask, const float* water, const float* uw, const float* vw, const float* bed,
+                        int res, float cell, float ox, float oz, const SolidGeom* geoms, int n, double* out,
+                        cudaStream_t st);
 
 // The host form of one body (C library trigonometry and hypot).
 SolidGeom make_geom(float x, float z, float yaw, float half_length, float half_width, float bottom_y, float top_y,

@@ -872,7 +872,7 @@ __device__ void cta_awake_boxes(Shared& S, const Job& J) {
     CLU_RECT(0, res - 1, 0, res - 1, {
         float hv = J.h[g];
         if (hv > eps) {
-            bool awake = hypotf(J.u[g], J.v[g]) > 0.05f;
+            bool awake = hypot_rn(J.u[g], J.v[g]) > 0.05f;
             if (!awake) {
                 float eta = J.bed[g] + hv;
                 int ip = i + 1 < res ? g + 1 : g;

@@ -59,6 +59,12 @@ class HydroSolid(ctypes.Structure):
                [("contact", _i), ("radius", _f), ("width", _f)]
 
 
+class HydroLoad(ctypes.Structure):
+    _fields_ = [(k, _f) for k in ("force_x", "force_z", "buoyancy_n", "hull_buoyancy_n", "wheel_buoyancy_n",
+                                  "displaced_m3", "eroded_m3", "hole_m")] + \
+               [("wheel_blocks", ctypes.c_uint32), ("belly_blocks", ctypes.c_uint32)]
+
+
 class GroundSample(ctypes.Structure):
     _fields_ = [(k, _f) for k in ("water_m", "slurry_m", "u", "v", "settled_dust_m", "moisture", "bed_m")]
 
@@ -137,6 +143,7 @@ def lib():
             "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
             "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
             "silt_set_hydro_solids": [_p, ctypes.POINTER(HydroSolid), _i],
+            "silt_get_hydro_load": [_p, ctypes.POINTER(HydroLoad)],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -332,6 +339,12 @@ class Sheet:
                                 int(bool(sd.get("contact", False))), float(sd.get("radius", 0.0)),
                                 float(sd.get("width", 0.0)))
         check(lib().silt_set_hydro_solids(self.h, arr, len(solids)), "set_hydro_solids")
+
+    def hydro_load(self):
+        """FluidCore::hydro_load: forces, buoyancy and scour as a dict."""
+        o = HydroLoad()
+        check(lib().silt_get_hydro_load(self.h, ctypes.byref(o)), "hydro_load")
+        return {k: getattr(o, k) for k, _ in HydroLoad._fields_}
 
     def set_wave_maker(self, wave):
         """FluidCore::set_wave_maker: dict of WaveMaker fields, or None."""

@@ -124,6 +124,17 @@ typedef struct {
     float radius, width;
 } silt_hydro_solid;
 
+/* src/fluid_core.rs:242-255 (`HydroLoad`): what the walls feel, read back
+ * after a step. */
+typedef struct {
+    float force_x, force_z;   /* N: hydrostatic plus dynamic pressure on the wall faces */
+    float buoyancy_n, hull_buoyancy_n, wheel_buoyancy_n;
+    float displaced_m3;
+    float eroded_m3;          /* bed scoured beside tire contacts since creation */
+    float hole_m;             /* the deepest scour */
+    uint32_t wheel_blocks, belly_blocks;  /* contact and wall cells of the coarse mask */
+} silt_hydro_load;
+
 /* src/fluid_core.rs:440-448 (`GroundSample`); settled dust is off this path (0). */
 typedef struct {
     float water_m, slurry_m, u, v, settled_dust_m, moisture, bed_m;
@@ -308,6 +319,16 @@ int silt_set_turbidity_enabled(silt_sheet* s, int32_t on);
  * with the wall mobility, redirect and block at the walls, walled transport.
  * Up to 64 bodies; the window engine only (SILT_EINVAL on the grid engine). */
 int silt_set_hydro_solids(silt_sheet* s, const silt_hydro_solid* solids, int32_t n);
+/* FluidCore::hydro_load (src/fluid_core.rs:7164-7249): the coarse mask of the
+ * current state, the hydrostatic (rho g h^2 / 2 per face metre) and dynamic
+ * (rho vn^2 h / 2) force on every open wet cell's wall faces, and each body's
+ * buoyancy from the mean surface of its wet ring (:7251-7286; a wheel's
+ * submerged circular segment, a belly's box at 0.36 fill). The reference's
+ * f32 running sums are FP64 sums here. Synchronises the handle's stream.
+ * With walls the step also scours (scour_contacts :7364-7420): shear above
+ * 1.5 Pa beside a contact cuts up to 8 cm of bed per cell into the slurry as
+ * silt; the ledger books that volume in opened_m3. */
+int silt_get_hydro_load(silt_sheet* s, silt_hydro_load* out);
 
 /* ------------------------------------------------------ one-sheet operator */
 /* Free `step_sheet` (src/fluid_core.rs:770) with the gravity drive on caller

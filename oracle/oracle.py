@@ -103,6 +103,7 @@ def lib():
         L.oracle_core_inflow.argtypes = [_p, _i, _f, _f, _f]
         L.oracle_core_set_hydro_solids.argtypes = [_p, _p, _i]
         L.oracle_core_solid_mask.argtypes = [_p, _p]
+        L.oracle_core_hydro_load.argtypes = [_p, _p]
         _lib = L
     return _lib
 
@@ -331,6 +332,16 @@ class Core:
         packed = np.array([[float(sd.get(k, 0.0)) for k in self.SOLID_KEYS] for sd in solids] or [[0.0] * 10],
                           np.float32)
         lib().oracle_core_set_hydro_solids(self.h, _ptr(packed), len(solids))
+
+    LOAD_KEYS = ("force_x", "force_z", "buoyancy_n", "hull_buoyancy_n", "wheel_buoyancy_n", "displaced_m3",
+                 "eroded_m3", "hole_m", "wheel_blocks", "belly_blocks")
+
+    def hydro_load(self):
+        o = np.zeros(10, np.float32)
+        lib().oracle_core_hydro_load(self.h, _ptr(o))
+        d = {k: float(v) for k, v in zip(self.LOAD_KEYS, o)}
+        d["wheel_blocks"], d["belly_blocks"] = int(o[8]), int(o[9])
+        return d
 
     def solid_mask(self):
         out = np.zeros(self.res * self.res, np.uint8)

@@ -1431,12 +1431,16 @@ struct Core {
           wave_ramp = 0, wave_t = 0;
     // src/fluid_core.rs:5257-5264 set_hydro_solids: walls in the sheet.
     std::vector<HydroSolid> solids;
+    // src/fluid_core.rs:4907-4909: scour beside tire contacts.
+    std::vector<float> bed_drop;
+    float eroded_m3 = 0.0f, scour_hole_m = 0.0f;
 
     explicit Core(const oracle_core_cfg& c) : cfg(c) {
         res = (usize)c.res;
         fres = (usize)c.fine_res;
         sub = (usize)lroundf(c.cell / c.fine_cell);
         usize n = res * res, fn = fres * fres;
+        bed_drop.assign(n, 0.0f);
         water.assign(n, 0); slurry.assign(n, 0); uw.assign(n, 0); vw.assign(n, 0);
         us.assign(n, 0); vs.assign(n, 0); bed.assign(n, 0); moisture.assign(n, 0);
         grain.assign(n, 4);
@@ -2052,9 +2056,147 @@ struct Core {
         bed_friction(dt);
         diffuse_surface(dt);
         if (!ps.empty()) peel(ps, water.data(), uw.data(), vw.data(), res, cfg.cell, origin, true, spray);
+        if (!solids.empty()) scour_contacts(dt);
         feed_reach();
         for (const auto& s : spray) spray_m3 += s.volume;
         return spray;
+    }
+
+    // src/fluid_core.rs:7364-7420 scour_contacts: shear above 1.5 Pa on a wet
+    // open cell beside a tire contact cuts the bed into the slurry sheet, at
+    // most 8 cm per cell over the run.
+    void scour_contacts(float dt) {
+        if (dt <= 0.0f || solids.empty()) return;
+        std::vector<u8> mask = solid_mask(solids, res, cfg.cell, origin, water.data(), bed.data());
+        const float area = cfg.cell * cfg.cell;
+        std::vector<float> cut(res * res, 0.0f);
+        for (usize j = 1; j + 1 < res; ++j)
+            for (usize i = 1; i + 1 < res; ++i) {
+                const usize idx = j * res + i;
+                if (mask[idx] != 0 || water[idx] < 0.02f) continue;
+                bool touch = false;
+                for (const auto& d : NB4)
+                    if (mask[(usize)((long)j + d[1]) * res + (usize)((long)i + d[0])] == 1) {
+                        touch = true;
+                        break;
+                    }
+                if (!touch) continue;
+                const float speed = hypotf(uw[idx], vw[idx]);
+                if (!finite(speed)) continue;
+                const float tau = 1000.0f * 0.03f * speed * speed;
+                const float tau_c = 1.5f;
+                if (tau <= tau_c) continue;
+                const float rate = rmin(0.0035f * (tau / tau_c - 1.0f), 0.012f);
+                const float room = rmax(0.08f - bed_drop[idx], 0.0f);
+                cut[idx] = rmin(rate * dt, room);
+            }
+        for (usize idx = 0; idx < res * res; ++idx) {
+            const float dh = cut[idx];
+            if (dh <= 0.0f) continue;
+            bed[idx] -= dh;
+            slurry[idx] += dh;
+            us[idx] = uw[idx];
+            vs[idx] = vw[idx];
+            grain[idx] = 1;  // Grain::Silt
+            moisture[idx] = rmax(moisture[idx], 0.9f);
+            bed_drop[idx] += dh;
+            eroded_m3 += dh * area;
+            scour_hole_m = rmax(scour_hole_m, bed_drop[idx]);
+        }
+    }
+
+    // src/fluid_core.rs:7251-7286 ring_surface: mean bed and water of the wet
+    // cells in a ring around the body.
+    bool ring_surface(const HydroSolid& s, float& bed_out, float& water_out) const {
+        const float reach = rmax(s.half_length, s.half_width) + 0.55f;
+        const long i0 = (long)floorf((s.x - reach - origin[0]) / cfg.cell);
+        const long i1 = (long)floorf((s.x + reach - origin[0]) / cfg.cell);
+        const long j0 = (long)floorf((s.z - reach - origin[1]) / cfg.cell);
+        const long j1 = (long)floorf((s.z + reach - origin[1]) / cfg.cell);
+        float bsum = 0.0f, wsum = 0.0f, n = 0.0f;
+        for (long j = j0; j <= j1; ++j)
+            for (long i = i0; i <= i1; ++i) {
+                if (!in_grid(i, j, res)) continue;
+                const float x = origin[0] + ((float)i + 0.5f) * cfg.cell;
+                const float z = origin[1] + ((float)j + 0.5f) * cfg.cell;
+                if (solid_contains(s, x, z)) continue;
+                if (hypotf(x - s.x, z - s.z) > reach) continue;
+                const usize idx = (usize)j * res + (usize)i;
+                if (water[idx] < 0.01f) continue;
+                bsum += bed[idx];
+                wsum += water[idx];
+                n += 1.0f;
+            }
+        if (n < 1.0f) return false;
+        bed_out = bsum / n;
+        water_out = wsum / n;
+        return true;
+    }
+
+    // src/fluid_core.rs:4606-4615 cylinder_segment_volume
+    static float cylinder_segment_volume(float depth, float radius, float width) {
+        const float d = rclamp(depth, 0.0f, radius * 2.0f);
+        if (d <= 1.0e-4f || width <= 0.0f || radius <= 1.0e-3f) return 0.0f;
+        const float c = rclamp((radius - d) / radius, -1.0f, 1.0f);
+        const float area = radius * radius * acosf(c) - (radius - d) * sqrtf(rmax(2.0f * radius * d - d * d, 0.0f));
+        return rmax(area, 0.0f) * width;
+    }
+
+    // src/fluid_core.rs:7164-7249 hydro_load: out = force_x, force_z,
+    // buoyancy, hull buoyancy, wheel buoyancy, displaced m^3, eroded m^3,
+    // hole m, wheel blocks, belly blocks.
+    void hydro_load(float* out) const {
+        std::vector<u8> mask = solids.empty() ? std::vector<u8>(res * res, 0)
+                                              : solid_mask(solids, res, cfg.cell, origin, water.data(), bed.data());
+        float fx = 0.0f, fz = 0.0f;
+        uint32_t wheel_blocks = 0, belly_blocks = 0;
+        for (u8 m : mask) {
+            if (m == 1) ++wheel_blocks;
+            else if (m == 2) ++belly_blocks;
+        }
+        const float cell = cfg.cell;
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) {
+                const usize idx = j * res + i;
+                if (mask[idx] != 0) continue;
+                const float h = water[idx];
+                if (h < 1.0e-4f || !finite(h)) continue;
+                for (const auto& d : NB4) {
+                    const long ni = (long)i + d[0], nj = (long)j + d[1];
+                    if (!in_grid(ni, nj, res)) continue;
+                    if (mask[(usize)nj * res + (usize)ni] == 0) continue;
+                    const float nx = (float)d[0], nz = (float)d[1];
+                    const float hydro = 1000.0f * GRAVITY * h * h * 0.5f * cell;
+                    fx += nx * hydro;
+                    fz += nz * hydro;
+                    const float vn = uw[idx] * nx + vw[idx] * nz;
+                    if (vn > 0.0f) {
+                        const float dyn_f = 0.5f * 1000.0f * vn * vn * h * cell;
+                        fx += nx * dyn_f;
+                        fz += nz * dyn_f;
+                    }
+                }
+            }
+        float wheel_b = 0.0f, hull_b = 0.0f, displaced = 0.0f;
+        for (const HydroSolid& s : solids) {
+            float rb, rw;
+            if (!ring_surface(s, rb, rw)) continue;
+            if (s.radius > 0.0f) {
+                const float vol = cylinder_segment_volume(rw, s.radius, s.width);
+                displaced += vol;
+                wheel_b += 1000.0f * GRAVITY * vol;
+            } else {
+                const float eta = rb + rw;
+                const float height = rmax(s.top_y - s.bottom_y, 0.0f);
+                const float sub = rclamp(eta - s.bottom_y, 0.0f, height);
+                const float vol = (s.half_length * 2.0f) * (s.half_width * 2.0f) * sub * 0.36f;
+                displaced += vol;
+                hull_b += 1000.0f * GRAVITY * vol;
+            }
+        }
+        const float vals[10] = {fx, fz, wheel_b + hull_b, hull_b, wheel_b, displaced, eroded_m3, scour_hole_m,
+                                (float)wheel_blocks, (float)belly_blocks};
+        memcpy(out, vals, sizeof vals);
     }
 
     // src/fluid_core.rs:7482-7512 bed_friction: the eddy shear, then Manning
@@ -2707,6 +2849,7 @@ void oracle_core_set_hydro_solids(void* cp, const float* packed, int n) {
         C.solids.push_back(HydroSolid{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7] != 0.0f, f[8], f[9]});
     }
 }
+void oracle_core_hydro_load(void* cp, float* out10) { ((Core*)cp)->hydro_load(out10); }
 // The wall mask the next coarse step pair would use (res^2 bytes).
 void oracle_core_solid_mask(void* cp, uint8_t* out) {
     Core& C = *(Core*)cp;

@@ -5,6 +5,7 @@ m^3 with wheels and belly in a current), restated on the sheet alone. The
 reference has no golden vectors for this path; these properties, and the
 GPU parity tests against this restatement, are what pins it."""
 import numpy as np
+import pytest
 
 import oracle as O
 import silt_scenes as S
@@ -93,3 +94,28 @@ def test_displaced_water_goes_to_open_neighbours():
     w = core.get("water")
     assert float(w[reachable_wall(m, 64)].max()) == 0.0
     assert abs(core.ledger()["water64"] - v0) <= 1e-6 * v0
+
+
+WHEEL = dict(yaw=0.0, half_length=0.25, half_width=0.15, bottom_y=-1.0, top_y=2.0, contact=1, radius=0.38, width=0.2)
+
+
+def test_current_loads_the_walls_downstream_and_scours_beside_contacts():
+    """hydro_load (src/fluid_core.rs:7164-7249) in a +x current: the bow
+    upstream and the dynamic pressure push the bodies along +x; wheels in
+    water float on their submerged segments; scour_contacts (:7364-7420)
+    cuts the bed beside the contacts into the slurry as silt."""
+    wheels = [dict(WHEEL, x=x, z=z) for x in (-2.0, 2.0) for z in (-1.5, 1.5)]
+    core, scene = channel_core([dict(BELLY, yaw=0.0)] + wheels)
+    bed0 = core.get("bed").copy()
+    for _ in range(60):
+        core.step(DT)
+    load = core.hydro_load()
+    assert load["force_x"] > 10.0 * abs(load["force_z"]), load
+    assert load["wheel_blocks"] > 0 and load["belly_blocks"] > 0
+    assert load["wheel_buoyancy_n"] > 0.0 and load["hull_buoyancy_n"] > 0.0
+    assert abs(load["buoyancy_n"] - load["wheel_buoyancy_n"] - load["hull_buoyancy_n"]) <= 1e-3 * load["buoyancy_n"]
+    assert load["eroded_m3"] > 0.0 and 0.0 < load["hole_m"] <= 0.08
+    drop = bed0 - core.get("bed")
+    assert float(drop.max()) == pytest.approx(load["hole_m"], rel=1e-6)
+    assert abs(float(drop.astype(np.float64).sum()) * 0.04 - load["eroded_m3"]) <= 1e-5 * load["eroded_m3"] + 1e-9
+    assert (core.grain()[drop > 0] == 1).all()
