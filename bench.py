@@ -54,9 +54,10 @@ def parse():
     ap.add_argument("--res", type=int, default=RES)
     ap.add_argument("--no-tires", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
-    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200", "closure"],
+    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200", "walls200", "closure"],
                     help="grid: one 2048^2 grid with four tire patches; batch: many windows stepped together; "
-                         "window200: the reference's own 200^2 window, no tires; closure: 200^2 windows with "
+                         "window200: the reference's own 200^2 window, no tires; walls200: that window with a "
+                         "current and a vehicle's belly and four wheel contacts as walls; closure: 200^2 windows with "
                          "four tires each, the learned closure against the nested 2 cm sheets")
     ap.add_argument("--windows", type=int, default=None, help="batch: number of windows (256); closure: (128)")
     ap.add_argument("--batch-tires", type=int, default=1, help="batch: 1 = each window's 0..4 tires, 0 = none")
@@ -600,7 +601,9 @@ def run_batch(args):
 def run_window200(args):
     """The reference's CPU-runnable case: one 200 x 200 window (0.2 m cells),
     ruts, a Gaussian puddle and a rut slurry film, no tires, dt = 1/120 s,
-    stepped on the window engine (the exact box-by-box step)."""
+    stepped on the window engine (the exact box-by-box step). walls200 adds a
+    uniform current and a standing vehicle's belly and wheel contacts as
+    walls (the walled step, mask and displacement every step, scour)."""
     import torch
 
     import silt_b200
@@ -610,14 +613,16 @@ def run_window200(args):
         return
     scene = silt_scenes.window200()
     res = scene["res"]
-    cfgw = {"workload": "window200_ruts_puddle_slurry", "res": res, "cell_m": CELL, "dt_s": DT,
-            "engine": "window", "l2": "state fits in L2 (~2 MB); no flush between steps"}
+    walled = args.workload == "walls200"
+    seed_window = silt_scenes.seed_walled if walled else silt_scenes.seed_core
+    cfgw = {"workload": "window200_ruts_puddle_slurry" + ("_current_belly_4wheels" if walled else ""), "res": res,
+            "cell_m": CELL, "dt_s": DT, "engine": "window", "l2": "state fits in L2 (~2 MB); no flush between steps"}
     if args.impl == "reference":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
 
         core = oracle.Core(threads=2)
-        silt_scenes.seed_core(core, scene)
+        seed_window(core, scene)
         for _ in range(max(1, args.warmup)):
             core.step(DT)
         steps, t0, el = 0, time.perf_counter(), 0.0
@@ -641,7 +646,7 @@ def run_window200(args):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     sheet = silt_b200.Sheet(device=local, stream=stream.cuda_stream)
-    silt_scenes.seed_core(sheet, scene)
+    seed_window(sheet, scene)
     for _ in range(max(3, args.warmup)):
         sheet.step(DT, want_spray=False)
     torch.cuda.synchronize()
@@ -677,7 +682,7 @@ def run_window200(args):
         import oracle
 
         core = oracle.Core(threads=2)
-        silt_scenes.seed_core(core, scene)
+        seed_window(core, scene)
         core.step(DT)
         t0 = time.perf_counter()
         for _ in range(20):
@@ -958,7 +963,7 @@ def main():
         else:
             run_closure(args)
         return
-    if args.workload == "window200":
+    if args.workload in ("window200", "walls200"):
         run_window200(args)
     elif args.workload == "batch":
         if args.impl == "reference":

@@ -186,6 +186,26 @@ def tires_at(t, speed=5.0, center=(0.0, 0.0), track=1.5, wheelbase=2.4, radius=0
     return out
 
 
+def vehicle_bodies(x=0.1, z=0.4, yaw=0.35):
+    """A vehicle standing in the window as HydroSolid bodies (the shapes of
+    the reference's Vehicle::hydro_solids, src/vehicle.rs:345-386): the belly
+    (a 2.3 x 1.4 m wall) and four wheel contacts (0.5 x 0.3 m footprints,
+    radius 0.38, width 0.2), undersides below the bed."""
+    belly = dict(x=x, z=z, yaw=yaw, half_length=1.15, half_width=0.70, bottom_y=-1.0, top_y=2.0, contact=0)
+    wheels = [dict(x=x + dx, z=z + dz, yaw=yaw, half_length=0.25, half_width=0.15, bottom_y=-1.0, top_y=2.0,
+                   contact=1, radius=0.38, width=0.2) for dx in (-0.75, 0.75) for dz in (-1.2, 1.2)]
+    return [belly] + wheels
+
+
+def seed_walled(core, scene, u=0.15, v=0.45):
+    """The walled config-1 window: the scene, a uniform current and the
+    vehicle's bodies."""
+    seed_core(core, scene)
+    n = scene["res"] * scene["res"]
+    core.map_water_velocity(np.full(n, u, np.float32), np.full(n, v, np.float32))
+    core.set_hydro_solids(vehicle_bodies())
+
+
 def seed_core(core, scene):
     """Seeds a sheet handle (oracle or device) the same way: bed + water, the
     rut slurry, then the substrate read that fixes moisture and grain."""
