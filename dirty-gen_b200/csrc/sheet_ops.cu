@@ -77,6 +77,23 @@ __global__ void k_lay_slurry(const float* depth, float* slurry, float* moisture,
     }
 }
 
+// src/fluid_core.rs:5236-5254 lay_slurry_on_water, per cell: a slurry film
+// of `depth` on every cell holding more than 12 mm of water; `count` gets the
+// number of such cells.
+__global__ void k_lay_on_water(const float* water, float* slurry, float* moisture, uint8_t* grain, size_t n, float depth,
+                               int g, unsigned int* count) {
+    ::silt::dep_wait();
+    unsigned int c = 0;
+    GRID_STRIDE(i, n) {
+        if (water[i] <= 0.012f) continue;
+        slurry[i] = depth;
+        grain[i] = (uint8_t)g;
+        moisture[i] = fmaxf(moisture[i], 0.90f);
+        ++c;
+    }
+    if (c) atomicAdd(count, c);
+}
+
 // src/fluid_core.rs:5928-5950 read_substrate_grid, per cell.
 __global__ void k_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,
                                  float* moisture, uint8_t* grain, const float* slurry, size_t n) {
@@ -317,6 +334,15 @@ cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int re
 cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
                           cudaStream_t st) {
     ::silt::launch_dep(k_lay_slurry, dim3(blocks_for(n)), dim3(256), 0, st, depth, slurry, moisture, grain, n, g, m);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+cudaError_t op_lay_on_water(const float* water, float* slurry, float* moisture, uint8_t* grain, size_t n, float depth,
+                            int g, unsigned int* count, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    ::silt::launch_dep(k_lay_on_water, dim3(blocks_for(n)), dim3(256), 0, st, water, slurry, moisture, grain, n, depth,
+                       g, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }

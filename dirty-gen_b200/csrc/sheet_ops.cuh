@@ -12,6 +12,10 @@ cudaError_t op_map_water_velocity(const float* u_in, const float* v_in, const fl
                                   size_t n, cudaStream_t st);
 cudaError_t op_paint(float* depth_plane, float* moisture, uint8_t* grain, int res, float cell, float ox, float oz,
                      float x0, float x1, float z0, float z1, float depth, int water, int g, float m, cudaStream_t st);
+// lay_slurry_on_water: slurry `depth` on cells with more than 12 mm of water;
+// `count` (device) receives how many.
+cudaError_t op_lay_on_water(const float* water, float* slurry, float* moisture, uint8_t* grain, size_t n, float depth,
+                            int g, unsigned int* count, cudaStream_t st);
 cudaError_t op_lay_slurry(const float* depth, float* slurry, float* moisture, uint8_t* grain, size_t n, int g, float m,
                           cudaStream_t st);
 cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const uint8_t* grain_in, float* bed,

@@ -778,6 +778,35 @@ int silt_lay_slurry_mask(silt_sheet* s, const float* depth, int32_t grain, float
     return tiles_dirty(s);
 }
 
+int silt_lay_slurry_on_water(silt_sheet* s, float depth, int32_t grain, float* vol_out) {
+    if (!s) return fail_arg("lay_slurry_on_water");
+    if (vol_out) *vol_out = 0.0f;
+    if (!(std::isfinite(depth) && depth > 0.0f)) return SILT_OK_NOOP;
+    int rc = silt::fine::restrict_all(s->fine, s);
+    if (rc) return rc;
+    if ((rc = flush_cut(s))) return rc;
+    CK(silt::op_lay_on_water(s->H(0), s->H(1), s->moisture, s->grain, s->n, depth, grain, s->d_u32 + 8, s->st));
+    unsigned int cells = 0;
+    CK(cudaMemcpyAsync(&cells, s->d_u32 + 8, sizeof cells, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (vol_out) {
+        // The reference's f32 running sum of depth * area over those cells.
+        const float each = depth * (s->cfg.cell * s->cfg.cell);
+        float vol = 0.0f;
+        for (unsigned int k = 0; k < cells; ++k) vol += each;
+        *vol_out = vol;
+    }
+    s->mat_dirty = true;
+    s->ledger_fresh = false;
+    return tiles_dirty(s);
+}
+
+int silt_window_origin(float center_x, float center_z, int32_t res, float cell, float* origin2) {
+    if (!origin2 || res <= 0 || !(cell > 0.0f)) return fail_arg("window_origin");
+    silt::host::snap_origin(center_x, center_z, (float)res * cell, cell, origin2);
+    return SILT_OK;
+}
+
 int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moisture, const uint8_t* grain) {
     if (!s || !bed || !moisture || !grain) return fail_arg("read_substrate_grid");
     int rc = silt::fine::restrict_all(s->fine, s);

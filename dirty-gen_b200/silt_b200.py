@@ -144,6 +144,7 @@ def lib():
             "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
             "silt_set_hydro_solids": [_p, ctypes.POINTER(HydroSolid), _i],
             "silt_get_hydro_load": [_p, ctypes.POINTER(HydroLoad)],
+            "silt_lay_slurry_on_water": [_p, _f, _i, _p], "silt_window_origin": [_f, _f, _i, _f, _p],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -340,6 +341,13 @@ class Sheet:
                                 float(sd.get("width", 0.0)))
         check(lib().silt_set_hydro_solids(self.h, arr, len(solids)), "set_hydro_solids")
 
+    def lay_slurry_on_water(self, depth, grain):
+        """FluidCore::lay_slurry_on_water: returns the laid volume (f32)."""
+        vol = ctypes.c_float(0.0)
+        check(lib().silt_lay_slurry_on_water(self.h, float(depth), int(grain), ctypes.byref(vol)),
+              "lay_slurry_on_water")
+        return vol.value
+
     def hydro_load(self):
         """FluidCore::hydro_load: forces, buoyancy and scour as a dict."""
         o = HydroLoad()
@@ -421,6 +429,13 @@ def step_sheet_device(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch,
     """The free one-sheet operator on device pointers (ints)."""
     return check(lib().silt_step_sheet(h, u, v, bed, nu, gate, res, cell, dt, vorticity, scratch, stream),
                  "step_sheet")
+
+
+def window_origin(center, res=200, cell=0.2):
+    """FluidCore::window_origin: the snapped minimum corner of a window."""
+    o = (ctypes.c_float * 2)()
+    check(lib().silt_window_origin(float(center[0]), float(center[1]), int(res), float(cell), o), "window_origin")
+    return float(o[0]), float(o[1])
 
 
 def check_fixed_division(d, stream=None):

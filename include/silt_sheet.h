@@ -168,6 +168,11 @@ int silt_pour_slurry(silt_sheet* s, float x0, float x1, float z0, float z1, floa
                      float moisture, float* vol_out);
 /* FluidCore::lay_slurry_mask (src/fluid_core.rs:5857). */
 int silt_lay_slurry_mask(silt_sheet* s, const float* depth, int32_t grain, float moisture, float* vol_out);
+/* FluidCore::lay_slurry_on_water (src/fluid_core.rs:5236-5254): the slurry
+ * depth becomes `depth` on every cell holding more than 12 mm of water (grain
+ * `grain`, moisture at least 0.90); *vol_out gets depth * cell area summed
+ * over those cells as the reference's f32 running sum. Synchronises. */
+int silt_lay_slurry_on_water(silt_sheet* s, float depth, int32_t grain, float* vol_out);
 /* FluidCore::read_substrate_grid (src/fluid_core.rs:5928). */
 int silt_read_substrate_grid(silt_sheet* s, const float* bed, const float* moisture, const uint8_t* grain);
 /* Inflow strip on coarse row j over world x in [x0, x1), rate m^3/s; rate 0 turns it off.
@@ -215,6 +220,10 @@ int silt_recenter(silt_sheet* s, float cx, float cz);
 int silt_set_center(silt_sheet* s, float cx, float cz);
 /* FluidCore::window_bounds (src/fluid_core.rs:6977): origin x, origin z, extent. */
 int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
+/* FluidCore::window_origin (src/fluid_core.rs:6987-6990): the minimum corner
+ * of a res x res window of `cell` around the centre, snapped like
+ * silt_sheet_create (snap_origin :9877-9892). Host only. */
+int silt_window_origin(float center_x, float center_z, int32_t res, float cell, float* origin2);
 /* Raw plane copy to host for tests and tools: which = 0 water, 1 slurry, 2 uw,
  * 3 vw, 4 us, 5 vs, 6 bed, 7 moisture. */
 int silt_read_plane(silt_sheet* s, int32_t which, float* host);

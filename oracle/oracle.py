@@ -104,6 +104,8 @@ def lib():
         L.oracle_core_set_hydro_solids.argtypes = [_p, _p, _i]
         L.oracle_core_solid_mask.argtypes = [_p, _p]
         L.oracle_core_hydro_load.argtypes = [_p, _p]
+        L.oracle_core_lay_slurry_on_water.argtypes = [_p, _f, _i]
+        L.oracle_core_lay_slurry_on_water.restype = _f
         _lib = L
     return _lib
 
@@ -335,6 +337,9 @@ class Core:
 
     LOAD_KEYS = ("force_x", "force_z", "buoyancy_n", "hull_buoyancy_n", "wheel_buoyancy_n", "displaced_m3",
                  "eroded_m3", "hole_m", "wheel_blocks", "belly_blocks")
+
+    def lay_slurry_on_water(self, depth, grain):
+        return lib().oracle_core_lay_slurry_on_water(self.h, depth, grain)
 
     def hydro_load(self):
         o = np.zeros(10, np.float32)

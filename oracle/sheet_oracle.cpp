@@ -2849,6 +2849,22 @@ void oracle_core_set_hydro_solids(void* cp, const float* packed, int n) {
         C.solids.push_back(HydroSolid{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7] != 0.0f, f[8], f[9]});
     }
 }
+// src/fluid_core.rs:5236-5254 lay_slurry_on_water.
+float oracle_core_lay_slurry_on_water(void* cp, float depth, int grain) {
+    Core& C = *(Core*)cp;
+    if (!(finite(depth) && depth > 0.0f)) return 0.0f;
+    C.restrict_fine();
+    const float area = C.cfg.cell * C.cfg.cell;
+    float vol = 0.0f;
+    for (usize idx = 0; idx < C.water.size(); ++idx) {
+        if (C.water[idx] <= 0.012f) continue;
+        C.slurry[idx] = depth;
+        C.grain[idx] = (u8)grain;
+        C.moisture[idx] = rmax(C.moisture[idx], 0.90f);
+        vol += depth * area;
+    }
+    return vol;
+}
 void oracle_core_hydro_load(void* cp, float* out10) { ((Core*)cp)->hydro_load(out10); }
 // The wall mask the next coarse step pair would use (res^2 bytes).
 void oracle_core_solid_mask(void* cp, uint8_t* out) {

@@ -24,3 +24,12 @@ def test_binding_declares_every_header_function():
     lib = silt_b200.lib()
     for n in silt_b200.header_functions():
         assert getattr(lib, n).restype is not None or n in ("silt_cfg_default",)
+
+
+def test_window_origin_matches_the_oracle_snap():
+    """silt_window_origin is host code (FluidCore::window_origin,
+    src/fluid_core.rs:6987-6990): the same snap as the oracle's window."""
+    import oracle
+
+    for c in ((0.0, 0.0), (3.3, -7.1), (-125.07, 40.93), (0.1, 0.1), (19.9999, -0.0001)):
+        assert silt_b200.window_origin(c) == oracle.Core(center=c).origin(), c
