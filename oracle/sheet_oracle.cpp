@@ -1644,7 +1644,6 @@ struct Core {
         near_capture();
         float fine_area = cfg.fine_cell * cfg.fine_cell;
         float coarse_area = cfg.cell * cfg.cell;
-        usize full = sub * sub;
         std::map<usize, usize> touch_pos;
         std::vector<usize> touch;
         std::vector<float> aw, as, auw, avw, aus, avs;
