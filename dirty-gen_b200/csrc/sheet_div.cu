@@ -43,7 +43,41 @@ __global__ void k_check_div(float d, float r, unsigned long long* counts) {
 std::mutex g_div_mutex;
 std::map<std::pair<int, unsigned int>, int> g_div_exact;  // (device, bits of d) -> exact
 
+// Divisors already known to pass the exhaustive check: the four of each
+// standard cell width, 0.2 m (coarse) and 0.02 m (tire sheets), as the float
+// products 2 * cell and cell * cell that cell_divisors forms. The check's
+// verdict depends only on IEEE single-precision arithmetic (a correctly
+// rounded product, fused multiply-add and division, no flush to zero), not
+// on the device, so it holds on every GPU; tests/test_gpu_division.py runs
+// the full check on each entry to keep the table honest. A divisor outside
+// the table is checked once per process and device.
+bool known_exact(float d) {
+    const float cells[2] = {0.2f, 0.02f};
+    for (float c : cells) {
+        const float ds[4] = {2.0f * c, c * c, 231.0f, c};
+        for (float x : ds)
+            if (x == d) return true;
+    }
+    return false;
+}
+
 }  // namespace
+
+int known_exact_divisors(float* out, int cap) {
+    const float cells[2] = {0.2f, 0.02f};
+    float uniq[8];
+    int n = 0;
+    for (float c : cells) {
+        const float ds[4] = {2.0f * c, c * c, 231.0f, c};
+        for (float x : ds) {
+            bool seen = false;
+            for (int k = 0; k < n; ++k) seen = seen || uniq[k] == x;
+            if (!seen) uniq[n++] = x;
+        }
+    }
+    for (int k = 0; k < n && k < cap; ++k) out[k] = uniq[k];
+    return n;
+}
 
 cudaError_t check_fixed_div(float d, unsigned long long* counts6, cudaStream_t st) {
     unsigned long long* dc = nullptr;
@@ -69,15 +103,25 @@ FixedDiv fixed_div_for(float d, cudaStream_t st) {
     cudaGetDevice(&dev);
     unsigned int bits;
     memcpy(&bits, &d, sizeof bits);
+    if (known_exact(d)) {
+        D.exact = 1;
+        return D;
+    }
     std::lock_guard<std::mutex> lock(g_div_mutex);
     const auto key = std::make_pair(dev, bits);
     auto it = g_div_exact.find(key);
-    if (it == g_div_exact.end()) {
-        unsigned long long c[6] = {1, 0, 0, 0, 0, 0};
-        const int exact = check_fixed_div(d, c, st) == cudaSuccess && c[0] == 0 ? 1 : 0;
-        it = g_div_exact.emplace(key, exact).first;
+    if (it != g_div_exact.end()) {
+        D.exact = it->second;
+        return D;
     }
-    D.exact = it->second;
+    unsigned long long c[6] = {1, 0, 0, 0, 0, 0};
+    const cudaError_t e = check_fixed_div(d, c, st);
+    // Only a completed check is remembered: a failed one (no memory, a call
+    // under stream capture) leaves this divisor on IEEE division for now and
+    // is retried at the next sheet creation.
+    if (e == cudaSuccess) g_div_exact.emplace(key, c[0] == 0 ? 1 : 0);
+    else cudaGetLastError();
+    D.exact = e == cudaSuccess && c[0] == 0 ? 1 : 0;
     return D;
 }
 

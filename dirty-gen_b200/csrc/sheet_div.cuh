@@ -53,8 +53,13 @@ inline CellDivisors ieee_cell_divisors(float cell) {
 CellDivisors cell_divisors(float cell, cudaStream_t st);
 
 // The divisor d with its reciprocal, exact only when the exhaustive check
-// passed (run once per distinct d and device, on `st`, then cached).
+// passed: divisors of the standard cell widths are known to pass; any other
+// is checked once per distinct d and device, on `st`, and a completed check
+// is cached.
 FixedDiv fixed_div_for(float d, cudaStream_t st);
+// The divisors known to pass without a check at run time (out[0, cap));
+// returns how many there are.
+int known_exact_divisors(float* out, int cap);
 
 // Mismatch counts of fdiv against IEEE division over all 2^32 x: [0] all,
 // [1] x zero, [2] x subnormal, [3] x infinite or NaN, [4] x normal with a

@@ -80,6 +80,14 @@ constexpr int ENTRY_ZERO = 1 << 29;
 constexpr int ENTRY_COPY = 1 << 28;
 constexpr int ENTRY_TILE = (1 << 28) - 1;
 
+// Clears a sweep launch's barrier count and pass verdicts (the tile-list
+// kernel does, before each force launch).
+__device__ __forceinline__ void clear_sweep(SweepState* S) {
+    if (!S) return;
+    S->bar = 0u;
+    S->flag[0] = S->flag[1] = S->flag[2] = 0u;
+}
+
 // Cell material: viscosity, mobility and damping factor.
 __device__ __forceinline__ float cell_nu(const LayerParams& P, size_t g) {
     if (P.nu_mode == NU_CONST) return P.nu_c;
@@ -94,13 +102,12 @@ __device__ __forceinline__ float cell_mob(const LayerParams& P, size_t g) {
     return sheet_mobility_for(cell_nu(P, g));
 }
 
-// The cell's damping factor over dt: exp(-sheet_damp(nu) dt). The grid engine
-// keeps single-precision expf on this per-cell path (its confinement is the
-// snapshot form, so its parity is within tolerance, not bit for bit).
+// The cell's damping factor over dt: exp(-sheet_damp(nu) dt), the
+// double-precision exponential rounded once (as the window engine does).
 __device__ __forceinline__ float cell_decay(const LayerParams& P, size_t g, float dt) {
     if (P.nu_mode == NU_CONST) return P.decay_c;
     const float rate = P.nu_mode == NU_TABLE ? P.damp_plane[g] : sheet_damp(cell_nu(P, g));
-    return expf(-rate * dt);
+    return exp_rn(-rate * dt);
 }
 
 // Every cell of the tile's region of radius (RX, RY): f(gx, gy, s, g) with s
@@ -128,153 +135,128 @@ __device__ __forceinline__ void region(int tx0, int ty0, int res, F f) {
     }
 }
 
-// One force tile. EDGE = false for tiles whose whole radius-9 region lies at
-// least 2 cells inside the grid: no index is ever clamped there and every
-// blur uses the interior form, so the stencils are plain offsets. Threads
-// walk the regions as rows (one warp per row, lanes along x).
-template <bool EDGE>
-__device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
-    const int res = P.res;
-    float* E = sm;               // eta, radius 9
-    float* TG = sm + FPLANE;     // x-pass scratch
-    float* TS = sm + 2 * FPLANE;
-    float* PB = sm + 3 * FPLANE; // pressure p (radius 7), then projection b (radius 3)
-    float* U = sm + 4 * FPLANE;  // u, v: loaded (radius 6), gravity, confinement in place
-    float* V = sm + 5 * FPLANE;
-    float* HS = sm + 6 * FPLANE; // depth
-    float* WQ = sm + 7 * FPLANE; // vorticity (radius 5), then q (radius 1)
-    const int ox = tx0 - FH, oy = ty0 - FH;
-    const float dt = P.dt, eps = P.eps;
+// The velocity a substep starts from at (gx, gy): the lazy dry cut of the
+// previous substep, then the soft window border (src/fluid_core.rs:9594-9622;
+// a river reach's band keeps its current through the window ends).
+__device__ __forceinline__ void start_velocity(const LayerParams& P, int gx, int gy, size_t g, float hv, float& uu,
+                                               float& vv) {
+    uu = P.u[g];
+    vv = P.v[g];
+    if (P.apply_cut && hv < P.eps) {
+        uu = 0.0f;
+        vv = 0.0f;
+    }
+    if (P.soften_edge > 0) {
+        const int res = P.res;
+        const int dx = min(gx, res - 1 - gx), dz = min(gy, res - 1 - gy);
+        int d = min(dx, dz);
+        if (P.open_axis == 1 && gy >= P.open_c0 && gy < P.open_c1) d = dz;
+        else if (P.open_axis == 2 && gx >= P.open_c0 && gx < P.open_c1) d = dx;
+        if (d < P.soften_edge) {
+            float t = (float)d / (float)P.soften_edge;
+            float w = t * t * (3.0f - 2.0f * t);
+            uu *= w;
+            vv *= w;
+        }
+    }
+}
+
+// Shared-memory planes of a force tile (FW x FW floats each, origin at the
+// tile corner minus FH).
+struct ForcePlanes {
+    float* E;   // eta
+    float* TG;  // x-pass scratch
+    float* TS;
+    float* PB;  // pressure p, then projection b
+    float* U;   // u, v
+    float* V;
+    float* HS;  // depth
+    float* WQ;  // vorticity, then q
+    __device__ explicit ForcePlanes(float* sm)
+        : E(sm), TG(sm + FPLANE), TS(sm + 2 * FPLANE), PB(sm + 3 * FPLANE), U(sm + 4 * FPLANE), V(sm + 5 * FPLANE),
+          HS(sm + 6 * FPLANE), WQ(sm + 7 * FPLANE) {}
+};
+
 #define NX(d) (EDGE ? (gy - oy) * FW + (clampi(gx + (d), 0, res - 1) - ox) : s + (d))
 #define NZ(d) (EDGE ? (clampi(gy + (d), 0, res - 1) - oy) * FW + (gx - ox) : s + (d) * FW)
 
-    // 1. eta and depth on radius 9.
-    region<EDGE, FH, FH>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+// Depth and eta on radius R + 2, then the pressure p = 0.45 (0.62 G + 0.38 S)
+// + 0.55 eta on radius R (src/fluid_core.rs:1950-1985): the two 5-tap blurs,
+// x pass then z pass. Ends with a barrier.
+template <bool EDGE, int R>
+__device__ __forceinline__ void pressure_field(const LayerParams& P, const ForcePlanes& F, int tx0, int ty0) {
+    const int res = P.res;
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    region<EDGE, R + 2, R + 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         float hv = P.h[g];
-        HS[s] = hv;
-        E[s] = P.bed[g] + hv;
+        F.HS[s] = hv;
+        F.E[s] = P.bed[g] + hv;
     });
     __syncthreads();
-    // 2. Velocity on radius 6: the lazy dry cut of the previous substep, then
-    //    the soft window border (src/fluid_core.rs:9594-9622).
-    region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-        float uu = P.u[g], vv = P.v[g];
-        if (P.apply_cut && HS[s] < eps) { uu = 0.0f; vv = 0.0f; }
-        if (P.soften_edge > 0) {
-            const int dx = min(gx, res - 1 - gx), dz = min(gy, res - 1 - gy);
-            // soften_border (src/fluid_core.rs:9594-9620): a reach's band keeps its current through the ends.
-            int d = min(dx, dz);
-            if (P.open_axis == 1 && gy >= P.open_c0 && gy < P.open_c1) d = dz;
-            else if (P.open_axis == 2 && gx >= P.open_c0 && gx < P.open_c1) d = dx;
-            if (d < P.soften_edge) {
-                float t = (float)d / (float)P.soften_edge;
-                float w = t * t * (3.0f - 2.0f * t);
-                uu *= w;
-                vv *= w;
-            }
-        }
-        U[s] = uu;
-        V[s] = vv;
-    });
-    //    x pass of both pressure blurs: rows radius 9, columns radius 7.
-    region<EDGE, 7, FH>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+    region<EDGE, R, R + 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
-        float e0 = E[NX(-2)], e1 = E[NX(-1)], e2 = E[s], e3 = E[NX(1)], e4 = E[NX(2)];
-        TG[s] = tap5(e0, e1, e2, e3, e4, kG0, kG1, kG2, in);
-        TS[s] = tap5(e0, e1, e2, e3, e4, kS0, kS1, kS2, in);
+        float e0 = F.E[NX(-2)], e1 = F.E[NX(-1)], e2 = F.E[s], e3 = F.E[NX(1)], e4 = F.E[NX(2)];
+        F.TG[s] = tap5(e0, e1, e2, e3, e4, kG0, kG1, kG2, in);
+        F.TS[s] = tap5(e0, e1, e2, e3, e4, kS0, kS1, kS2, in);
     });
     __syncthreads();
-    // 3. z pass and the pressure: p = 0.45 (0.62 G + 0.38 S) + 0.55 eta, radius 7.
-    region<EDGE, 7, 7>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+    region<EDGE, R, R>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
         const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
-        float gb = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
-        float sc = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
+        float gb = tap5(F.TG[s0], F.TG[s1], F.TG[s], F.TG[s3], F.TG[s4], kG0, kG1, kG2, in);
+        float sc = tap5(F.TS[s0], F.TS[s1], F.TS[s], F.TS[s3], F.TS[s4], kS0, kS1, kS2, in);
         float filtered = 0.62f * gb + 0.38f * sc;
-        PB[s] = 0.45f * filtered + 0.55f * E[s];
+        F.PB[s] = 0.45f * filtered + 0.55f * F.E[s];
     });
     __syncthreads();
-    // 4. Gravity down the pressure gradient on wet cells, radius 6
-    //    (src/fluid_core.rs:2234-2253).
-    region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-        if (HS[s] > eps) {
-            float px = fdiv(PB[NX(1)] - PB[NX(-1)], P.div_two);
-            float pz = fdiv(PB[NZ(1)] - PB[NZ(-1)], P.div_two);
-            float mob = cell_mob(P, g);
-            U[s] += -kGravity * px * mob * dt;
-            V[s] += -kGravity * pz * mob * dt;
-        }
-    });
-    __syncthreads();
-    // 5. Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
-    if (P.vort > 0.0f) {
-        region<EDGE, 5, 5>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-            float dvdx = fdiv(V[NX(1)] - V[NX(-1)], P.div_two);
-            float dudz = fdiv(U[NZ(1)] - U[NZ(-1)], P.div_two);
-            WQ[s] = dvdx - dudz;
-        });
-        __syncthreads();
-        // 6. Confinement kick from that snapshot, in place, radius 4
-        //    (src/fluid_core.rs:2348-2375, :2441-2470).
-        region<EDGE, 4, 4>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-            if (HS[s] > eps) {
-                float w = WQ[s];
-                if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
-                    float wxp = fabsf(WQ[NX(1)]), wxm = fabsf(WQ[NX(-1)]);
-                    float wzp = fabsf(WQ[NZ(1)]), wzm = fabsf(WQ[NZ(-1)]);
-                    float nx_ = fdiv(wxp - wxm, P.div_two);
-                    float nz_ = fdiv(wzp - wzm, P.div_two);
-                    float du = P.vort * dt * (-nz_ * w);
-                    float dv = P.vort * dt * (nx_ * w);
-                    if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
-                        U[s] += du;
-                        V[s] += dv;
-                    }
-                }
-            }
-        });
-        __syncthreads();
-    }
+}
+
+// Projection, damping and the speed clamp from the confined velocity in U, V
+// (radius 4), depth and eta (radius 4) (src/fluid_core.rs:1992-2037). Writes
+// every cell of the tile to u_out, v_out.
+template <bool EDGE>
+__device__ __forceinline__ void finish_tile(const LayerParams& P, const ForcePlanes& F, int tx0, int ty0) {
+    const int res = P.res;
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    const float dt = P.dt, eps = P.eps;
     if (P.project) {
-        // 7. b = div * overload - 0.015 * overload * lap(eta), radius 3
-        //    (src/fluid_core.rs:1992-2003).
+        // b = div * overload - 0.015 * overload * lap(eta), radius 3 (:1992-2003).
         region<EDGE, 3, 3>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const int sxp = NX(1), sxm = NX(-1), szp = NZ(1), szm = NZ(-1);
-            float ux = fdiv(U[sxp] - U[sxm], P.div_two);
-            float vz = fdiv(V[szp] - V[szm], P.div_two);
+            float ux = fdiv(F.U[sxp] - F.U[sxm], P.div_two);
+            float vz = fdiv(F.V[szp] - F.V[szm], P.div_two);
             float div = ux + vz;
-            float lsum = E[sxp] + E[sxm] + E[szp] + E[szm] - 4.0f * E[s];
+            float lsum = F.E[sxp] + F.E[sxm] + F.E[szp] + F.E[szm] - 4.0f * F.E[s];
             float lap_h = fdiv(lsum, P.div_cell2);
             float overload = 1.0f + rclamp(fdiv(cell_nu(P, g), P.div_231), 0.0f, 6.0f);
-            PB[s] = div * overload - 0.015f * overload * lap_h;
+            F.PB[s] = div * overload - 0.015f * overload * lap_h;
         });
         __syncthreads();
-        // 8. x pass of both blurs of b: rows radius 3, columns radius 1.
+        // x pass of both blurs of b: rows radius 3, columns radius 1.
         region<EDGE, 1, 3>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const bool in = EDGE ? (gx >= 2 && gx <= res - 3) : true;
-            float b0 = PB[NX(-2)], b1 = PB[NX(-1)], b2 = PB[s], b3 = PB[NX(1)], b4 = PB[NX(2)];
-            TG[s] = tap5(b0, b1, b2, b3, b4, kG0, kG1, kG2, in);
-            TS[s] = tap5(b0, b1, b2, b3, b4, kS0, kS1, kS2, in);
+            float b0 = F.PB[NX(-2)], b1 = F.PB[NX(-1)], b2 = F.PB[s], b3 = F.PB[NX(1)], b4 = F.PB[NX(2)];
+            F.TG[s] = tap5(b0, b1, b2, b3, b4, kG0, kG1, kG2, in);
+            F.TS[s] = tap5(b0, b1, b2, b3, b4, kS0, kS1, kS2, in);
         });
         __syncthreads();
-        // 9. q = 0.62 G(b) + 0.38 S(b), radius 1 (src/fluid_core.rs:2004-2011).
+        // q = 0.62 G(b) + 0.38 S(b), radius 1 (:2004-2011).
         region<EDGE, 1, 1>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             const bool in = EDGE ? (gy >= 2 && gy <= res - 3) : true;
             const int s0 = NZ(-2), s1 = NZ(-1), s3 = NZ(1), s4 = NZ(2);
-            float gq = tap5(TG[s0], TG[s1], TG[s], TG[s3], TG[s4], kG0, kG1, kG2, in);
-            float sq = tap5(TS[s0], TS[s1], TS[s], TS[s3], TS[s4], kS0, kS1, kS2, in);
-            WQ[s] = 0.62f * gq + 0.38f * sq;
+            float gq = tap5(F.TG[s0], F.TG[s1], F.TG[s], F.TG[s3], F.TG[s4], kG0, kG1, kG2, in);
+            float sq = tap5(F.TS[s0], F.TS[s1], F.TS[s], F.TS[s3], F.TS[s4], kS0, kS1, kS2, in);
+            F.WQ[s] = 0.62f * gq + 0.38f * sq;
         });
         __syncthreads();
     }
-    // 10. Projection kick, damping and the speed clamp on wet cells
-    //     (src/fluid_core.rs:2015-2037); every cell of the tile is written.
+    // Projection kick, damping and the speed clamp on wet cells (:2015-2037).
     region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
-        float uu = U[s], vv = V[s];
-        if (HS[s] > eps) {
+        float uu = F.U[s], vv = F.V[s];
+        if (F.HS[s] > eps) {
             if (P.project) {
-                float qx = fdiv(WQ[NX(1)] - WQ[NX(-1)], P.div_two);
-                float qz = fdiv(WQ[NZ(1)] - WQ[NZ(-1)], P.div_two);
+                float qx = fdiv(F.WQ[NX(1)] - F.WQ[NX(-1)], P.div_two);
+                float qz = fdiv(F.WQ[NZ(1)] - F.WQ[NZ(-1)], P.div_two);
                 uu += 0.012f * dt * qx;
                 vv += 0.012f * dt * qz;
             }
@@ -285,9 +267,209 @@ __device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int 
         P.u_out[g] = uu;
         P.v_out[g] = vv;
     });
+}
+
+// One force tile in the snapshot (Jacobi) form. EDGE = false for tiles whose
+// whole radius-9 region lies at least 2 cells inside the grid: no index is
+// ever clamped there and every blur uses the interior form, so the stencils
+// are plain offsets. Threads walk the regions as rows (one warp per row,
+// lanes along x).
+template <bool EDGE>
+__device__ __forceinline__ void force_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
+    const int res = P.res;
+    const ForcePlanes F(sm);
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    const float dt = P.dt, eps = P.eps;
+    // 1-3. Depth, eta (radius 9) and the pressure (radius 7).
+    pressure_field<EDGE, 7>(P, F, tx0, ty0);
+    // Velocity on radius 6 and gravity down the pressure gradient on wet
+    // cells (src/fluid_core.rs:2234-2253).
+    region<EDGE, 6, 6>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+        float uu, vv;
+        start_velocity(P, gx, gy, g, F.HS[s], uu, vv);
+        if (F.HS[s] > eps) {
+            float px = fdiv(F.PB[NX(1)] - F.PB[NX(-1)], P.div_two);
+            float pz = fdiv(F.PB[NZ(1)] - F.PB[NZ(-1)], P.div_two);
+            float mob = cell_mob(P, g);
+            uu += -kGravity * px * mob * dt;
+            vv += -kGravity * pz * mob * dt;
+        }
+        F.U[s] = uu;
+        F.V[s] = vv;
+    });
+    __syncthreads();
+    // Vorticity of the post-gravity snapshot, radius 5 (src/fluid_core.rs:3498-3506).
+    if (P.vort > 0.0f) {
+        region<EDGE, 5, 5>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+            float dvdx = fdiv(F.V[NX(1)] - F.V[NX(-1)], P.div_two);
+            float dudz = fdiv(F.U[NZ(1)] - F.U[NZ(-1)], P.div_two);
+            F.WQ[s] = dvdx - dudz;
+        });
+        __syncthreads();
+        // Confinement kick from that snapshot, in place, radius 4
+        // (src/fluid_core.rs:2348-2375, :2441-2470).
+        region<EDGE, 4, 4>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+            if (F.HS[s] > eps) {
+                float w = F.WQ[s];
+                if (finite_f(w) && !(fabsf(w) < 1.0e-4f)) {
+                    float wxp = fabsf(F.WQ[NX(1)]), wxm = fabsf(F.WQ[NX(-1)]);
+                    float wzp = fabsf(F.WQ[NZ(1)]), wzm = fabsf(F.WQ[NZ(-1)]);
+                    float nx_ = fdiv(wxp - wxm, P.div_two);
+                    float nz_ = fdiv(wzp - wzm, P.div_two);
+                    float du = P.vort * dt * (-nz_ * w);
+                    float dv = P.vort * dt * (nx_ * w);
+                    if (finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f) {
+                        F.U[s] += du;
+                        F.V[s] += dv;
+                    }
+                }
+            }
+        });
+        __syncthreads();
+    }
+    finish_tile<EDGE>(P, F, tx0, ty0);
+}
+
+// Sweep form, part 1: the post-gravity velocity G of every cell of the tile
+// (gravity on wet cells only; a dry cell keeps its starting velocity), written
+// to u_out, v_out, and the sweep's first iterate F = G to fu, fv.
+template <bool EDGE>
+__device__ __forceinline__ void pre_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
+    const int res = P.res;
+    const ForcePlanes F(sm);
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    const float dt = P.dt, eps = P.eps;
+    pressure_field<EDGE, 1>(P, F, tx0, ty0);
+    region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+        float uu, vv;
+        start_velocity(P, gx, gy, g, F.HS[s], uu, vv);
+        if (F.HS[s] > eps) {
+            float px = fdiv(F.PB[NX(1)] - F.PB[NX(-1)], P.div_two);
+            float pz = fdiv(F.PB[NZ(1)] - F.PB[NZ(-1)], P.div_two);
+            float mob = cell_mob(P, g);
+            uu += -kGravity * px * mob * dt;
+            vv += -kGravity * pz * mob * dt;
+        }
+        P.u_out[g] = uu;
+        P.v_out[g] = vv;
+        P.fu[g] = uu;
+        P.fv[g] = vv;
+    });
+}
+
+// Local passes of the sweep's fixed point on one tile before its values go
+// back to global memory.
+constexpr int SWEEP_LOCAL_PASSES = 16;
+
+// Sweep form, part 2: one pass of the raster-order Gauss-Seidel confinement
+// (force_gravity_open, src/fluid_core.rs:2234-2260) solved as a fixed point.
+// In the reference's sweep a wet cell's final velocity is its post-gravity
+// value G plus the kick computed from the final values of the cells before it
+// in raster order, its own G, and the starting values of the cells after it;
+// dry cells never change. The tile iterates that equation for its own wet
+// cells in shared memory, reading the current iterate of other tiles' cells
+// from fu, fv, until a local pass changes no bit, and writes back what
+// changed. Returns true (block-uniform) when any value of the tile changed.
+// When a whole pass over every tile changes nothing, every cell satisfies its
+// equation with the values it read, and since each cell depends only on
+// earlier cells that solution is the sequential sweep's, bit for bit.
+template <bool EDGE>
+__device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
+    const int res = P.res;
+    float* PU = sm;              // starting velocity (the values of cells after a cell)
+    float* PV = sm + FPLANE;
+    float* FU = sm + 2 * FPLANE;  // current iterate (the values of cells before it)
+    float* FV = sm + 3 * FPLANE;
+    float* GU = sm + 4 * FPLANE;  // post-gravity velocity of the tile's own cells
+    float* GV = sm + 5 * FPLANE;
+    float* WT = sm + 6 * FPLANE;  // 1: wet
+    const int ox = tx0 - FH, oy = ty0 - FH;
+    const float eps = P.eps;
+    region<EDGE, 2, 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+        const float hv = P.h[g];
+        float uu, vv;
+        start_velocity(P, gx, gy, g, hv, uu, vv);
+        const bool wet = hv > eps;
+        PU[s] = uu;
+        PV[s] = vv;
+        WT[s] = wet ? 1.0f : 0.0f;
+        // A wet cell's tile is always stepped this substep, so its iterate
+        // is current; a dry cell keeps its starting velocity.
+        FU[s] = wet ? P.fu[g] : uu;
+        FV[s] = wet ? P.fv[g] : vv;
+        if (wet && gx >= tx0 && gx < tx0 + FT && gy >= ty0 && gy < ty0 + FT) {
+            GU[s] = P.u_out[g];
+            GV[s] = P.v_out[g];
+        }
+    });
+    __syncthreads();
+    bool tile_changed = false;
+    for (int it = 0; it < SWEEP_LOCAL_PASSES; ++it) {
+        int changed = 0;
+        region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+            if (WT[s] == 0.0f) return;
+            auto at = [&](int a, int b) { return (b - oy) * FW + (a - ox); };
+            auto before = [&](int a, int b) { return b < gy || (b == gy && a < gx); };
+            auto uu = [&](int a, int b) {
+                if (a == gx && b == gy) return GU[s];
+                return before(a, b) ? FU[at(a, b)] : PU[at(a, b)];
+            };
+            auto vv = [&](int a, int b) {
+                if (a == gx && b == gy) return GV[s];
+                return before(a, b) ? FV[at(a, b)] : PV[at(a, b)];
+            };
+            float du, dv, nu_ = GU[s], nv_ = GV[s];
+            if (conf_kick(gx, gy, res, P.div_two, P.dt, P.vort, uu, vv, du, dv)) {
+                nu_ = GU[s] + du;
+                nv_ = GV[s] + dv;
+            }
+            if (__float_as_uint(nu_) != __float_as_uint(FU[s]) || __float_as_uint(nv_) != __float_as_uint(FV[s])) {
+                FU[s] = nu_;
+                FV[s] = nv_;
+                changed = 1;
+            }
+        });
+        if (!__syncthreads_or(changed)) break;
+        tile_changed = true;
+    }
+    if (tile_changed) {
+        region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+            if (WT[s] != 0.0f) {
+                P.fu[g] = FU[s];
+                P.fv[g] = FV[s];
+            }
+        });
+    }
+    __syncthreads();  // shared memory is reused by the next tile
+    return tile_changed;
+}
+
+// Sweep form, part 3: projection, damping and clamp from the solved sweep.
+template <bool EDGE>
+__device__ __forceinline__ void post_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
+    const int res = P.res;
+    const ForcePlanes F(sm);
+    const float eps = P.eps;
+    region<EDGE, 4, 4>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+        const float hv = P.h[g];
+        F.HS[s] = hv;
+        F.E[s] = P.bed[g] + hv;
+        float uu, vv;
+        if (hv > eps) {
+            uu = P.fu[g];
+            vv = P.fv[g];
+        } else {
+            start_velocity(P, gx, gy, g, hv, uu, vv);
+        }
+        F.U[s] = uu;
+        F.V[s] = vv;
+    });
+    __syncthreads();
+    finish_tile<EDGE>(P, F, tx0, ty0);
+}
+
 #undef NX
 #undef NZ
-}
 
 // A layer's force parameters for this substep: with a device count, its dt
 // and (constant-viscosity layers) damping factor for that count.
@@ -303,7 +485,14 @@ __device__ __forceinline__ LayerParams force_params(const LayerParams& P0, const
     return P;
 }
 
-// One list entry of the force pass. Returns true when it used shared memory.
+// A tile whose whole radius-9 region lies at least 2 cells inside the grid:
+// no stencil index is clamped there and every blur uses the interior form.
+__device__ __forceinline__ bool tile_interior(int res, int tx0, int ty0) {
+    return tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
+}
+
+// One list entry of the force pass (the sweep form's first part for a
+// sweeping layer). Returns true when it used shared memory.
 __device__ __forceinline__ bool force_entry(const LayerParams& P, const TileFlags& tf, int nxt, int e, float* sm) {
     const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
     const int res = P.res;
@@ -331,13 +520,186 @@ __device__ __forceinline__ bool force_entry(const LayerParams& P, const TileFlag
         if (threadIdx.x == 0) pick(tf.zero_uv, l, nxt)[t] = 1;
         return false;
     }
-    const bool interior = tx0 - FH >= 2 && ty0 - FH >= 2 && tx0 + FT + FH <= res - 2 && ty0 + FT + FH <= res - 2;
-    if (interior)
+    const bool interior = tile_interior(res, tx0, ty0);
+    if (P.sweep) {
+        // Sweep form: this launch's first part; the sweep and the projection follow.
+        if (interior)
+            pre_tile<false>(P, sm, tx0, ty0);
+        else
+            pre_tile<true>(P, sm, tx0, ty0);
+    } else if (interior) {
         force_tile<false>(P, sm, tx0, ty0);
-    else
+    } else {
         force_tile<true>(P, sm, tx0, ty0);
+    }
     if (threadIdx.x == 0) pick(tf.zero_uv, l, nxt)[t] = 0;
     return true;
+}
+
+// A list entry that steps its tile (neither a zero fill nor an identity copy).
+__device__ __forceinline__ bool entry_steps(int e) { return (e & (ENTRY_ZERO | ENTRY_COPY)) == 0; }
+
+// Sweep-form pass over one list entry: the fixed-point pass of a stepped tile
+// of a sweeping layer with confinement on. Block-uniform result.
+__device__ __forceinline__ bool sweep_entry(const LayerParams& P, const TileFlags& tf, int e, float* sm) {
+    if (!entry_steps(e) || !P.sweep || !(P.vort > 0.0f)) return false;
+    const int t = e & ENTRY_TILE;
+    const int tx0 = (t % tf.tiles_x) * FT, ty0 = (t / tf.tiles_x) * FT;
+    return tile_interior(P.res, tx0, ty0) ? sweep_tile<false>(P, sm, tx0, ty0) : sweep_tile<true>(P, sm, tx0, ty0);
+}
+
+// Sweep-form projection of one list entry. Returns true when it used shared memory.
+__device__ __forceinline__ bool post_entry(const LayerParams& P, const TileFlags& tf, int e, float* sm) {
+    if (!entry_steps(e) || !P.sweep) return false;
+    const int t = e & ENTRY_TILE;
+    const int tx0 = (t % tf.tiles_x) * FT, ty0 = (t / tf.tiles_x) * FT;
+    if (tile_interior(P.res, tx0, ty0))
+        post_tile<false>(P, sm, tx0, ty0);
+    else
+        post_tile<true>(P, sm, tx0, ty0);
+    return true;
+}
+
+// ----------------------------------------------- Gauss-Seidel sweep launches
+//
+// The sweep's fixed point couples every stepped tile, so its passes run in
+// one cooperative launch (every CTA resident at once) separated by a grid
+// barrier. Each wait is bounded: past the limit the CTA records the failure
+// in SweepState::err and the launch ends; the host reports SILT_ETIMEOUT.
+
+constexpr int SWEEP_MAX_PASSES = 64;                  // then the sequential sweep
+constexpr unsigned int SWEEP_SPIN_LIMIT = 1u << 22;   // polls of ~0.1 us: about half a second
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier of a cooperative launch: the arrival count only grows within
+// a launch (the tile-list kernel clears it before), so barrier number k waits
+// for k * gridDim.x arrivals. False when the wait gave up.
+__device__ bool grid_barrier(SweepState* S, unsigned int& target) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        target += gridDim.x;
+        __threadfence();
+        atomicAdd(&S->bar, 1u);
+        int good = 1;
+        unsigned int spins = 0;
+        while (ld_acquire_u32(&S->bar) < target) {
+            if (++spins > SWEEP_SPIN_LIMIT) {
+                atomicOr(&S->err, 1u);
+                good = 0;
+                break;
+            }
+            __nanosleep(100);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Passes of the fixed point until one changes nothing anywhere. `visit(k)`
+// runs list entry k's pass and returns whether it changed a value. Returns
+// the number of passes, 0 at the pass limit, -1 after a failed barrier.
+template <class Visit>
+__device__ int sweep_fixed_point(SweepState* S, unsigned int& target, int n, Visit visit) {
+    __shared__ unsigned int verdict;
+    for (int pass = 0; pass < SWEEP_MAX_PASSES; ++pass) {
+        bool changed = false;
+        for (int k = blockIdx.x; k < n; k += gridDim.x) changed |= visit(k);
+        if (threadIdx.x == 0) {
+            if (changed) atomicOr(&S->flag[pass % 3], 1u);
+            // The next pass's verdict starts clear; the one cleared here was
+            // last read before the previous barrier.
+            if (blockIdx.x == 0) S->flag[(pass + 1) % 3] = 0u;
+        }
+        if (!grid_barrier(S, target)) return -1;
+        if (threadIdx.x == 0) verdict = ld_acquire_u32(&S->flag[pass % 3]);
+        __syncthreads();
+        if (verdict == 0u) return pass + 1;
+    }
+    return 0;
+}
+
+// The sequential sweep of one layer on one thread (past the pass limit):
+// every wet cell in raster order, as force_gravity_open does.
+__device__ void sweep_serial(const LayerParams& P) {
+    const int res = P.res;
+    const float eps = P.eps;
+    for (int j = 0; j < res; ++j)
+        for (int i = 0; i < res; ++i) {
+            const size_t g = (size_t)j * res + i;
+            if (!(P.h[g] > eps)) continue;
+            auto val = [&](bool is_u, int a, int b) {
+                const size_t q = (size_t)b * res + a;
+                if (a == i && b == j) return is_u ? P.u_out[q] : P.v_out[q];
+                const float hq = P.h[q];
+                if (hq > eps && (b < j || (b == j && a < i))) return is_u ? P.fu[q] : P.fv[q];
+                float uu, vv;
+                start_velocity(P, a, b, q, hq, uu, vv);
+                return is_u ? uu : vv;
+            };
+            auto uu = [&](int a, int b) { return val(true, a, b); };
+            auto vv = [&](int a, int b) { return val(false, a, b); };
+            float du, dv, nu_ = P.u_out[g], nv_ = P.v_out[g];
+            if (conf_kick(i, j, res, P.div_two, P.dt, P.vort, uu, vv, du, dv)) {
+                nu_ = P.u_out[g] + du;
+                nv_ = P.v_out[g] + dv;
+            }
+            P.fu[g] = nu_;
+            P.fv[g] = nv_;
+        }
+}
+
+// True when layer l takes a real (not identity) substep in this launch.
+__device__ __forceinline__ bool layer_steps(const SubstepCount& sc, int l) {
+    return !(sc.speed2 && sc.k > 0 && sc.k >= device_nsub(sc, l));
+}
+
+__device__ __forceinline__ void sweep_stats(SweepState* S, int passes) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&S->launches, 1u);
+        atomicMax(&S->passes_max, (unsigned int)(passes > 0 ? passes : SWEEP_MAX_PASSES));
+        if (passes == 0) atomicAdd(&S->fallbacks, 1u);
+    }
+}
+
+// One sheet's force pass in the sweep form (cooperative launch): pre-sweep
+// tiles (and the list's zero and copy entries), the fixed point, projection.
+__global__ void __launch_bounds__(FORCE_THREADS) k_force_sweep(ForceLaunch L) {
+    ::silt::dep_wait();
+    extern __shared__ float sm[];
+    __shared__ LayerParams Ps[2];
+    if (threadIdx.x < 2) Ps[threadIdx.x] = force_params(L.lay[threadIdx.x], L.sc, threadIdx.x, blockIdx.x == 0);
+    __syncthreads();
+    SweepState* S = L.tf.sweep;
+    const int n = *L.tf.count;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = L.tf.list[k];
+        if (force_entry(Ps[e >> 30], L.tf, L.nxt, e, sm)) __syncthreads();
+    }
+    unsigned int target = 0;
+    if (!grid_barrier(S, target)) return;
+    const int passes =
+        sweep_fixed_point(S, target, n, [&](int k) { const int e = L.tf.list[k]; return sweep_entry(Ps[e >> 30], L.tf, e, sm); });
+    if (passes < 0) return;
+    if (passes == 0) {
+        if (threadIdx.x == 0 && blockIdx.x < 2) {
+            const LayerParams& P = Ps[blockIdx.x];
+            if (P.sweep && P.vort > 0.0f && !P.skip && layer_steps(L.sc, blockIdx.x)) sweep_serial(P);
+        }
+        if (!grid_barrier(S, target)) return;
+    }
+    sweep_stats(S, passes);
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = L.tf.list[k];
+        if (post_entry(Ps[e >> 30], L.tf, e, sm)) __syncthreads();
+    }
 }
 
 // Persistent over the substep's tile list.
@@ -394,6 +756,7 @@ __global__ void k_tile_list(TileFlags tf, int cur, int nxt, int all, int skip0, 
         if (count_next) *count_next = 0;
         if (zero_ledger) zero_ledger[0] = zero_ledger[1] = 0.0;
         if (zero_bits) zero_bits[0] = zero_bits[1] = 0u;
+        clear_sweep(tf.sweep);
     }
     if (k >= 2 * nt) return;
     const int l = k / nt, t = k % nt;
@@ -725,11 +1088,15 @@ cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], con
 
 // ------------------------------------------------------------ batched windows
 
-__global__ void k_batch_tile_list(const WindowSubstep* ws, int* list, int* entry_win, int* count, int* count_next) {
+__global__ void k_batch_tile_list(const WindowSubstep* ws, int* list, int* entry_win, int* count, int* count_next,
+                                  SweepState* sweep) {
     ::silt::dep_wait();
     const int w = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w == 0 && k == 0) *count_next = 0;
+    if (w == 0 && k == 0) {
+        *count_next = 0;
+        clear_sweep(sweep);
+    }
     const WindowSubstep& D = ws[w];
     if (D.skip) return;
     const TileFlags& tf = D.F.tf;
@@ -807,6 +1174,62 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_batch_force(const WindowSubst
     }
 }
 
+// Every window's force pass in the sweep form (cooperative launch), as
+// k_force_sweep does for one sheet; windows without the sweep take the
+// snapshot form in the first part and sit out the rest.
+__global__ void __launch_bounds__(FORCE_THREADS) k_batch_force_sweep(const WindowSubstep* ws, int nwin, const int* list,
+                                                                     const int* entry_win, const int* count,
+                                                                     SweepState* S) {
+    ::silt::dep_wait();
+    extern __shared__ float sm[];
+    __shared__ LayerParams Ps;
+    __shared__ TileFlags Tf;
+    __shared__ int nxt_s;
+    const int n = *count;
+    auto fetch = [&](int k, bool report) {
+        const int e = list[k];
+        if (threadIdx.x == 0) {
+            const WindowSubstep& D = ws[entry_win[k]];
+            Ps = force_params(D.F.lay[e >> 30], D.F.sc, e >> 30, report);
+            Tf = D.F.tf;
+            nxt_s = D.F.nxt;
+        }
+        __syncthreads();
+        return e;
+    };
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = fetch(k, true);
+        force_entry(Ps, Tf, nxt_s, e, sm);
+        __syncthreads();  // the parameters and shared memory are reused by the next entry
+    }
+    unsigned int target = 0;
+    if (!grid_barrier(S, target)) return;
+    const int passes = sweep_fixed_point(S, target, n, [&](int k) {
+        const int e = fetch(k, false);
+        const bool r = sweep_entry(Ps, Tf, e, sm);
+        __syncthreads();
+        return r;
+    });
+    if (passes < 0) return;
+    if (passes == 0) {
+        for (int u = blockIdx.x; u < 2 * nwin; u += gridDim.x) {
+            if (threadIdx.x != 0) continue;
+            const WindowSubstep& D = ws[u >> 1];
+            const int l = u & 1;
+            if (D.skip) continue;
+            const LayerParams P = force_params(D.F.lay[l], D.F.sc, l, false);
+            if (P.sweep && P.vort > 0.0f && !P.skip && layer_steps(D.F.sc, l)) sweep_serial(P);
+        }
+        if (!grid_barrier(S, target)) return;
+    }
+    sweep_stats(S, passes);
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int e = fetch(k, false);
+        post_entry(Ps, Tf, e, sm);
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(TRANSPORT_THREADS) k_batch_transport(const WindowSubstep* ws, const int* list,
                                                                        const int* entry_win, const int* count) {
     ::silt::dep_wait();
@@ -833,10 +1256,11 @@ __global__ void __launch_bounds__(TRANSPORT_THREADS) k_batch_transport(const Win
 }
 
 cudaError_t launch_batch_tile_list(const WindowSubstep* d_ws, int nwin, int max_tiles, int* list, int* entry_win,
-                                   int* count, int* count_next, cudaStream_t st) {
+                                   int* count, int* count_next, SweepState* sweep, cudaStream_t st) {
     if (nwin <= 0) return cudaSuccess;
     dim3 grid((2 * max_tiles + 255) / 256, nwin);
-    ::silt::launch_dep(k_batch_tile_list, dim3(grid), dim3(256), 0, st, d_ws, list, entry_win, count, count_next);
+    ::silt::launch_dep(k_batch_tile_list, dim3(grid), dim3(256), 0, st, d_ws, list, entry_win, count, count_next,
+                       sweep);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -848,8 +1272,46 @@ cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, cons
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
-                               cudaStream_t st) {
+// Grid of a cooperative force launch: every CTA the device holds at once.
+template <class K>
+int coop_grid(K kernel, size_t smem) {
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, FORCE_THREADS, smem) != cudaSuccess) return 0;
+    return nsm * per;
+}
+
+template <class K, class... Args>
+cudaError_t launch_coop(K kernel, int grid, cudaStream_t st, Args... args) {
+    if (grid <= 0) return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(FORCE_THREADS);
+    cfg.dynamicSmemBytes = force_smem_bytes();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+    ::silt::count_launch();
+    return e;
+}
+
+cudaError_t launch_batch_force(const WindowSubstep* d_ws, int nwin, const int* list, const int* entry_win,
+                               const int* count, SweepState* sweep, cudaStream_t st) {
+    if (sweep) {
+        static std::once_flag sattr;
+        static int grid = 0;
+        std::call_once(sattr, [] {
+            cudaFuncSetAttribute(k_batch_force_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
+            grid = coop_grid(k_batch_force_sweep, force_smem_bytes());
+        });
+        const cudaError_t e = launch_coop(k_batch_force_sweep, grid, st, d_ws, nwin, list, entry_win, count, sweep);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
     ::silt::launch_dep(k_batch_force, dim3(148 * 2), dim3(FORCE_THREADS), force_smem_bytes(), st, d_ws, list, entry_win, count);
@@ -867,6 +1329,17 @@ cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, c
 }
 
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st) {
+    if (L.lay[0].sweep || L.lay[1].sweep) {
+        if (!L.tf.sweep) return cudaErrorInvalidValue;
+        static std::once_flag sattr;
+        static int grid = 0;
+        std::call_once(sattr, [] {
+            cudaFuncSetAttribute(k_force_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
+            grid = coop_grid(k_force_sweep, force_smem_bytes());
+        });
+        const cudaError_t e = launch_coop(k_force_sweep, grid, st, L);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes()); });
     (void)res;

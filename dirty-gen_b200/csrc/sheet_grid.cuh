@@ -40,6 +40,26 @@ struct LayerParams {
     int32_t open_c0, open_c1;  // (reach along X), 2 columns (along Z); there only one edge distance softens
     int32_t apply_cut;     // zero u, v where h < eps on load (the previous dry cut)
     int32_t skip;          // layer has nothing to do this substep
+    // Confinement form. sweep = 1: the reference's raster-order Gauss-Seidel
+    // sweep (force_gravity_open, src/fluid_core.rs:2234-2260), solved on the
+    // grid as a fixed point in the planes fu, fv; sweep = 0: the snapshot
+    // (Jacobi) form of force_gravity_par (:2263).
+    int32_t sweep;
+    float* fu;
+    float* fv;
+};
+
+// Device state of one Gauss-Seidel sweep launch: the grid barrier's arrival
+// count and the pass verdicts (cleared by the tile-list kernel before every
+// force launch), a sticky error for a barrier wait that gave up, and pass
+// statistics.
+struct SweepState {
+    unsigned int bar;         // CTAs arrived at the grid barrier in this launch
+    unsigned int flag[3];     // pass p's verdict in flag[p % 3]: some tile changed
+    unsigned int err;         // a barrier wait ran past its limit (sticky)
+    unsigned int passes_max;  // most passes one launch needed
+    unsigned int fallbacks;   // launches that ran the sequential sweep after the pass limit
+    unsigned int launches;    // sweep launches
 };
 
 // Active-tile bookkeeping of the grid engine, per layer and ping-pong buffer,
@@ -55,6 +75,7 @@ struct TileFlags {
     int* count;
     unsigned long long* stepped;  // per layer: running total of tiles stepped (may be nullptr)
     int32_t tiles_x;
+    SweepState* sweep;       // cleared by the tile-list kernel (may be nullptr)
 };
 
 // Substep count decided on the device (src/fluid_core.rs:1715-1744). The
@@ -120,11 +141,14 @@ struct WindowSubstep {
 // Batched substep over `nwin` windows: one tile list (entries and their
 // window indices), cleared count slot for the next substep.
 cudaError_t launch_batch_tile_list(const WindowSubstep* d_ws, int nwin, int max_tiles, int* list, int* entry_win,
-                                   int* count, int* count_next, cudaStream_t st);
+                                   int* count, int* count_next, SweepState* sweep, cudaStream_t st);
 cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
                                 cudaStream_t st);
-cudaError_t launch_batch_force(const WindowSubstep* d_ws, const int* list, const int* entry_win, const int* count,
-                               cudaStream_t st);
+// `sweep` non-null: some window confines by the Gauss-Seidel sweep, and the
+// force pass runs as one cooperative launch (pre-sweep tiles, the sweep's
+// fixed point, projection) over every window.
+cudaError_t launch_batch_force(const WindowSubstep* d_ws, int nwin, const int* list, const int* entry_win,
+                               const int* count, SweepState* sweep, cudaStream_t st);
 cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
                                    const int* count, cudaStream_t st);
 
@@ -145,6 +169,11 @@ cudaError_t launch_tile_speed2(const TileFlags& tf, const float* const h[2], con
                                const float* const v[2], int res, float eps, int apply_cut, unsigned int* bits,
                                cudaStream_t st);
 size_t transport_smem_bytes();
+// A layer with `sweep` set runs the Gauss-Seidel form: one cooperative
+// launch (every CTA resident) that computes the post-gravity velocity of
+// every stepped tile, solves the raster-order sweep as a fixed point across
+// tiles (grid barriers between passes, bounded waits; L.tf.sweep holds the
+// barrier state), then projects, damps and clamps.
 cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t st);
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st);
 // The slurry's material laws per cell: viscosity, mobility and damping rate

@@ -100,4 +100,29 @@ __device__ __forceinline__ float open_edge_dh(bool with_bed, float hd, float hr,
     return ok ? dh : 0.0f;
 }
 
+// The confinement kick at (i, j) from the velocities `uu`, `vv` return for
+// any cell (src/fluid_core.rs:3442-3471 with clamped indices; the interior
+// form :2805-2831 gives the same values).
+template <class UF, class VF>
+__device__ __forceinline__ bool conf_kick(int i, int j, int res, const FixedDiv& two, float dt, float vort, UF uu, VF vv,
+                                          float& du, float& dv) {
+    auto vort_at = [&](int a, int c) {
+        const int ip = min(a + 1, res - 1), im = max(a - 1, 0), jp = min(c + 1, res - 1), jm = max(c - 1, 0);
+        float dvdx = fdiv(vv(ip, c) - vv(im, c), two);
+        float dudz = fdiv(uu(a, jp) - uu(a, jm), two);
+        return dvdx - dudz;
+    };
+    float w = vort_at(i, j);
+    if (!finite_f(w) || fabsf(w) < 1.0e-4f) return false;
+    float wxp = fabsf(vort_at(min(i + 1, res - 1), j));
+    float wxm = fabsf(vort_at(max(i - 1, 0), j));
+    float wzp = fabsf(vort_at(i, min(j + 1, res - 1)));
+    float wzm = fabsf(vort_at(i, max(j - 1, 0)));
+    float nx = fdiv(wxp - wxm, two);
+    float nz = fdiv(wzp - wzm, two);
+    du = vort * dt * (-nz * w);
+    dv = vort * dt * (nx * w);
+    return finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f;
+}
+
 }  // namespace silt

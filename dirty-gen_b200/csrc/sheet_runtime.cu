@@ -89,7 +89,10 @@ struct silt_sheet {
     unsigned int* d_u32 = nullptr;   // [0..1] speed bits, [2] substep overflow, [3] non-finite count, [4..7] tile counters
     const float** d_planes = nullptr;
     double* h_acc = nullptr;      // pinned mirror of d_acc
-    unsigned int* h_flags = nullptr;  // pinned: [0] the device's substep-overflow flag
+    // d_u32: [0, 2) speed bits, [2] substep overflow, [4, 8) tiles stepped
+    // (two u64), [SWEEP_AT, SWEEP_AT + 8) the sweep launch state.
+    static constexpr int SWEEP_AT = 8;
+    unsigned int* h_flags = nullptr;  // pinned: d_u32[2, 16) as last read (FLAG_* below)
     bool cut_pending = false;
     bool ledger_fresh = false;    // h_acc[0..1] hold the current depth sums
     float vmax_bound = 0.0f;      // bound on any cell's speed |(u, v)|, for the one-substep shortcut
@@ -132,6 +135,12 @@ struct silt_sheet {
     int* tile_count = nullptr;   // two count slots, used alternately by successive substeps
     unsigned long long tile_seq = 0;
     bool tiles_all = true;     // next substep steps every tile (after any outside write)
+    // Confinement form of the grid engine (silt_set_confinement): the
+    // reference step pair's Gauss-Seidel sweep by default, solved in the
+    // iterate planes (2 layers x u, v) with the launch state in d_u32.
+    int confine = SILT_CONFINE_SWEEP;
+    float* sweep_planes = nullptr;
+    silt::SweepState* sweep_state() { return reinterpret_cast<silt::SweepState*>(d_u32 + SWEEP_AT); }
 
     // Open-water mode of the water sheet (FluidCore::set_open_water,
     // src/fluid_core.rs:5293-5303) and the surface diffusion (:5284-5286).
@@ -282,6 +291,12 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         reach_band(s, &P.open_axis, &P.open_c0, &P.open_c1);
         P.apply_cut = (k > 0 || s->cut_pending) ? 1 : 0;
         P.skip = 0;
+        // The step pair runs serial inner loops, so coarse cells confine by
+        // the raster sweep (force_gravity_open :2234-2260); 2 cm cells always
+        // take the snapshot form (gravity_jacobi_serial, :2223-2228).
+        P.sweep = s->confine == SILT_CONFINE_SWEEP && P.project && s->sweep_planes ? 1 : 0;
+        P.fu = s->sweep_planes ? s->sweep_planes + (size_t)(2 * l) * s->n : nullptr;
+        P.fv = s->sweep_planes ? s->sweep_planes + (size_t)(2 * l + 1) * s->n : nullptr;
         if (l == 0) {
             P.nu_mode = silt::NU_CONST;
             P.nu_c = cp.nu_w;
@@ -534,9 +549,9 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 16 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_flags, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_flags, 16 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMemset(s->d_u32, 0, 16 * sizeof(unsigned int));
-    if (e == cudaSuccess) memset(s->h_flags, 0, 4 * sizeof(unsigned int));
+    if (e == cudaSuccess) memset(s->h_flags, 0, 16 * sizeof(unsigned int));
     s->engine = cfg->engine == SILT_ENGINE_WINDOW || cfg->engine == SILT_ENGINE_GRID
                     ? cfg->engine
                     : (cfg->res <= silt::window::MAX_RES ? SILT_ENGINE_WINDOW : SILT_ENGINE_GRID);
@@ -565,8 +580,11 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
             s->tf.count = s->tile_count;
             s->tf.stepped = reinterpret_cast<unsigned long long*>(s->d_u32 + 4);
             s->tf.tiles_x = tx;
+            s->tf.sweep = s->sweep_state();
             e = cudaMemsetAsync(s->tile_count, 0, 2 * sizeof(int), s->st);
         }
+        if (e == cudaSuccess) e = cudaMalloc(&s->sweep_planes, 4 * nb);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->sweep_planes, 0, 4 * nb, s->st);
     }
     if (s->engine == SILT_ENGINE_WINDOW) {
         const size_t wp = 2 * (size_t)silt::window::SCRATCH_PLANES * s->n * sizeof(float);
@@ -636,6 +654,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     if (s->h_acc) cudaFreeHost(s->h_acc);
     cudaFree(s->win_planes);
     cudaFree(s->tile_mem);
+    cudaFree(s->sweep_planes);
     cudaFree(s->d_win_jobs);
     if (s->h_win_jobs) cudaFreeHost(s->h_win_jobs);
     cudaFree(s->d_solids);
@@ -655,9 +674,15 @@ int silt_sheet_destroy(silt_sheet* s) {
     return SILT_OK;
 }
 
-// After a wait on the stream: a step whose layer needed more substeps than
-// the host's speed bound launched leaves the state off the reference's path.
+// After a wait on the stream, with h_flags read back: a sweep launch whose
+// grid barrier gave up (the state of that step is incomplete), or a step
+// whose layer needed more substeps than the host's speed bound launched (the
+// state is off the reference's path).
 static int check_substep_overflow(silt_sheet* s) {
+    if (s->h_flags[silt_sheet::SWEEP_AT + 4 - 2]) {
+        snprintf(g_err, sizeof g_err, "%s", "a Gauss-Seidel sweep launch gave up waiting at its grid barrier");
+        return SILT_ETIMEOUT;
+    }
     if (!s->h_flags[0]) return SILT_OK;
     snprintf(g_err, sizeof g_err, "%s",
              "a step needed more substeps than its speed bound launched; the state is no longer the reference's");
@@ -666,7 +691,7 @@ static int check_substep_overflow(silt_sheet* s) {
 
 int silt_sheet_sync(silt_sheet* s) {
     if (!s) return fail_arg("handle");
-    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     return check_substep_overflow(s);
 }
@@ -1495,7 +1520,7 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0;
     int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if ((rc = check_substep_overflow(s))) return rc;
     const double area = (double)s->cfg.cell * (double)s->cfg.cell;
@@ -1694,6 +1719,11 @@ int silt_check_fixed_division(float d, unsigned long long* counts6, void* stream
     return SILT_OK;
 }
 
+int silt_known_exact_divisors(float* out, int32_t cap) {
+    if (cap < 0 || (cap > 0 && !out)) return fail_arg("known_exact_divisors");
+    return silt::known_exact_divisors(out, cap);
+}
+
 int silt_fine_water_debug(silt_sheet* s, const silt_tire_push* tires, int32_t n, int32_t patch, float* host,
                           float* origin2) {
     if (!s || (n > 0 && !tires) || !host) return fail_arg("fine_water_debug");
@@ -1709,7 +1739,10 @@ int silt_near_tiles(silt_sheet* s, int32_t* out) {
 int silt_set_step_timing(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     CK(cudaStreamSynchronize(s->st));
-    if (s->tile_mem) CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, s->st));
+    if (s->tile_mem) {
+        CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, s->st));
+        CK(cudaMemsetAsync(&s->sweep_state()->passes_max, 0, 3 * sizeof(unsigned int), s->st));
+    }
     for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
     s->ev_used.clear();
     memset(&s->parts, 0, sizeof s->parts);
@@ -1735,6 +1768,11 @@ int silt_get_step_parts(silt_sheet* s, silt_step_parts* out) {
         CK(cudaMemcpy(stepped, s->d_u32 + 4, 16, cudaMemcpyDeviceToHost));
         s->parts.force_cells = (int64_t)(stepped[0] + stepped[1]) * silt::GRID_TILE * silt::GRID_TILE;
         s->parts.force_cells_water = (int64_t)stepped[0] * silt::GRID_TILE * silt::GRID_TILE;
+        silt::SweepState st;
+        CK(cudaMemcpy(&st, s->sweep_state(), sizeof st, cudaMemcpyDeviceToHost));
+        s->parts.sweep_launches = st.launches;
+        s->parts.sweep_passes_max = st.passes_max;
+        s->parts.sweep_fallbacks = st.fallbacks;
     }
     *out = s->parts;
     return SILT_OK;
@@ -1755,6 +1793,13 @@ int silt_set_fine_pace(silt_sheet* s, int32_t pace) {
 int silt_set_near_field(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     return silt::fine::set_near_field(s->fine, s, on != 0);
+}
+
+int silt_set_confinement(silt_sheet* s, int32_t form) {
+    if (!s) return fail_arg("handle");
+    if (form != SILT_CONFINE_SWEEP && form != SILT_CONFINE_SNAPSHOT) return fail_arg("confinement form");
+    s->confine = form;
+    return SILT_OK;
 }
 
 // ---------------------------------------------------------------- batched windows
@@ -1947,6 +1992,10 @@ int batch_coarse(silt_batch* b, float dt) {
     const int slot = b->flip;
     b->flip ^= 1;
     const size_t need = (size_t)steps * n;
+    // The batch's sweep launches keep their state in the first window's
+    // slot, so their errors come back through that window's flags.
+    silt::SweepState* sweep = b->sheets[0]->sweep_state();
+    bool sweeping = false;
     if (b->ev[slot]) CK(cudaEventSynchronize(b->ev[slot]));  // the descriptors two steps back are copied
     if (need > b->ws_cap[slot]) {
         cudaFree(b->d_ws[slot]);
@@ -1970,6 +2019,7 @@ int batch_coarse(silt_batch* b, float dt) {
             }
             int all = 0;
             coarse_substep(s, plans[w], dt, k, D.F, D.T, all);
+            sweeping = sweeping || D.F.lay[0].sweep || D.F.lay[1].sweep;
             D.cur = s->cur;
             D.all = all;
             D.apply_cut = s->cut_pending ? 1 : 0;
@@ -1986,7 +2036,8 @@ int batch_coarse(silt_batch* b, float dt) {
         int* count = b->count + (b->seq & 1);
         int* count_next = b->count + ((b->seq + 1) & 1);
         ++b->seq;
-        CK(silt::launch_batch_tile_list(d, n, b->max_tiles, b->list, b->entry_win, count, count_next, b->st));
+        CK(silt::launch_batch_tile_list(d, n, b->max_tiles, b->list, b->entry_win, count, count_next,
+                                        sweeping ? sweep : nullptr, b->st));
         if (k == 0 && device_count) CK(silt::launch_batch_speed2(d, b->list, b->entry_win, count, b->st));
         cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
         if (b->timing) {
@@ -1996,7 +2047,7 @@ int batch_coarse(silt_batch* b, float dt) {
             if (!e0 || !e1 || !e2) return fail_cuda(cudaErrorMemoryAllocation, "batch timing events");
             CK(cudaEventRecord(e0, b->st));
         }
-        CK(silt::launch_batch_force(d, b->list, b->entry_win, count, b->st));
+        CK(silt::launch_batch_force(d, n, b->list, b->entry_win, count, sweeping ? sweep : nullptr, b->st));
         if (b->timing) CK(cudaEventRecord(e1, b->st));
         CK(silt::launch_batch_transport(d, b->list, b->entry_win, count, b->st));
         if (b->timing) CK(cudaEventRecord(e2, b->st));
@@ -2207,7 +2258,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
     CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 7 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)
-        CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
+        CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     for (int w = 0; w < n; ++w) {
         silt_sheet* s = b->sheets[w];
@@ -2246,7 +2297,10 @@ int silt_batch_set_timing(silt_batch* b, int32_t on) {
     for (cudaEvent_t e : b->ev_used) b->ev_pool.push_back(e);
     b->ev_used.clear();
     for (silt_sheet* s : b->sheets)
-        if (s->tile_mem) CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, b->st));
+        if (s->tile_mem) {
+            CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, b->st));
+            CK(cudaMemsetAsync(&s->sweep_state()->passes_max, 0, 3 * sizeof(unsigned int), b->st));
+        }
     return SILT_OK;
 }
 
@@ -2269,6 +2323,13 @@ int silt_batch_get_parts(silt_batch* b, silt_step_parts* out) {
         CK(cudaMemcpy(stepped, s->d_u32 + 4, 16, cudaMemcpyDeviceToHost));
         b->parts.force_cells += (int64_t)(stepped[0] + stepped[1]) * silt::GRID_TILE * silt::GRID_TILE;
         b->parts.force_cells_water += (int64_t)stepped[0] * silt::GRID_TILE * silt::GRID_TILE;
+        if (s == b->sheets[0]) {
+            silt::SweepState st;
+            CK(cudaMemcpy(&st, s->sweep_state(), sizeof st, cudaMemcpyDeviceToHost));
+            b->parts.sweep_launches = st.launches;
+            b->parts.sweep_passes_max = st.passes_max;
+            b->parts.sweep_fallbacks = st.fallbacks;
+        }
     }
     *out = b->parts;
     return SILT_OK;
@@ -2337,8 +2398,8 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
     float* u_mid = (float*)((char*)scratch + 256);
     float* v_mid = u_mid + n;
     float* h_next = v_mid + n;
-    // Tile flags after the planes: every tile is stepped on every call.
-    silt::TileFlags tf;
+    // Tile flags after the planes: every tile is stepped on every call (no sweep state).
+    silt::TileFlags tf = {};
     {
         const int tx = (res + silt::GRID_TILE - 1) / silt::GRID_TILE;
         const size_t nt = (size_t)tx * tx;

@@ -20,6 +20,7 @@ SILT_OK, SILT_OK_NOOP, SILT_EINVAL, SILT_ECUDA, SILT_ETIMEOUT, SILT_ENOMEM, SILT
 CLAY, SILT, SAND, WATER, OTHER = 0, 1, 2, 3, 4
 FINE_MEAN_PATCH, FINE_PER_TIRE = 0, 1
 ENGINE_AUTO, ENGINE_WINDOW, ENGINE_GRID = 0, 1, 2
+CONFINE_SWEEP, CONFINE_SNAPSHOT = 0, 1
 
 _f = ctypes.c_float
 _i = ctypes.c_int32
@@ -78,7 +79,8 @@ class StepParts(ctypes.Structure):
                 ("steps", ctypes.c_int64), ("launches", ctypes.c_int64), ("force_launches", ctypes.c_int64),
                 ("force_cells", ctypes.c_int64), ("force_cells_water", ctypes.c_int64),
                 ("device_counts", ctypes.c_int64), ("host_step_ms", ctypes.c_double),
-                ("host_fine_ms", ctypes.c_double)]
+                ("host_fine_ms", ctypes.c_double), ("sweep_launches", ctypes.c_int64),
+                ("sweep_passes_max", ctypes.c_int64), ("sweep_fallbacks", ctypes.c_int64)]
 
 
 class SiltError(RuntimeError):
@@ -127,6 +129,7 @@ def lib():
             "silt_fine_water_debug": [_p, _p, _i, _i, _p, _p],
             "silt_near_tiles": [_p, ctypes.POINTER(_i)],
             "silt_set_fine_sub_cap": [_p, _f], "silt_set_fine_pace": [_p, _i], "silt_set_near_field": [_p, _i],
+            "silt_set_confinement": [_p, _i],
             "silt_step_sheet": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p, _p],
             "silt_set_step_timing": [_p, _i], "silt_get_step_parts": [_p, ctypes.POINTER(StepParts)],
             "silt_step_sheet_noalloc": [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _p],
@@ -142,6 +145,7 @@ def lib():
             "silt_set_river_reach": [_p, ctypes.POINTER(RiverReach)],
             "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
             "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
+            "silt_known_exact_divisors": [_p, _i],
             "silt_set_hydro_solids": [_p, ctypes.POINTER(HydroSolid), _i],
             "silt_get_hydro_load": [_p, ctypes.POINTER(HydroLoad)],
             "silt_lay_slurry_on_water": [_p, _f, _i, _p], "silt_window_origin": [_f, _f, _i, _f, _p],
@@ -402,6 +406,11 @@ class Sheet:
     def set_near_field(self, on):
         check(lib().silt_set_near_field(self.h, int(on)), "set_near_field")
 
+    def set_confinement(self, form):
+        """CONFINE_SWEEP (the reference step pair's Gauss-Seidel sweep, the
+        default) or CONFINE_SNAPSHOT (the Jacobi form) on the grid engine."""
+        check(lib().silt_set_confinement(self.h, int(form)), "set_confinement")
+
     def near_tiles(self):
         c = _i(0)
         check(lib().silt_near_tiles(self.h, ctypes.byref(c)), "near_tiles")
@@ -436,6 +445,14 @@ def window_origin(center, res=200, cell=0.2):
     o = (ctypes.c_float * 2)()
     check(lib().silt_window_origin(float(center[0]), float(center[1]), int(res), float(cell), o), "window_origin")
     return float(o[0]), float(o[1])
+
+
+def known_exact_divisors():
+    """The divisors the library takes as checked without running the check."""
+    n = lib().silt_known_exact_divisors(None, 0)
+    out = np.zeros(max(n, 1), np.float32)
+    check(lib().silt_known_exact_divisors(_ptr(out), n), "known_exact_divisors")
+    return [float(x) for x in out[:n]]
 
 
 def check_fixed_division(d, stream=None):

@@ -68,9 +68,10 @@ typedef struct {
 
 /* Coarse-pair engines. WINDOW steps each layer box by box exactly as the
  * reference (work boxes, Gauss-Seidel confinement, per-sheet scratch), one
- * CTA per layer, windows up to 512 cells per side. GRID steps the whole grid
- * with tiled kernels on every SM and confines from a snapshot (the
- * reference's free-operator form), for grids of any size. AUTO picks WINDOW
+ * crew of CTAs per layer, windows up to 512 cells per side. GRID steps the
+ * whole grid with tiled kernels on every SM, for grids of any size; it
+ * confines by the reference step pair's raster-order Gauss-Seidel sweep
+ * unless silt_set_confinement selects the snapshot form. AUTO picks WINDOW
  * up to 512 cells per side and GRID above. The nested patches always use WINDOW. */
 #define SILT_ENGINE_AUTO 0
 #define SILT_ENGINE_WINDOW 1
@@ -245,6 +246,13 @@ int silt_sheet_copy_state(silt_sheet* dst, silt_sheet* src);
  * once per divisor at silt_sheet_create). No counterpart in the reference,
  * which divides by IEEE division throughout. Synchronises `stream`. */
 int silt_check_fixed_division(float d, unsigned long long* counts6, void* stream);
+/* The divisors the library treats as checked without running the check:
+ * 2 cell, cell^2, 231 and cell for the standard cells of 0.2 m and 0.02 m,
+ * as the float products the step forms. The check's verdict depends only on
+ * IEEE single-precision arithmetic, not on the GPU; every other divisor is
+ * checked once per process and device. Writes up to cap values to out and
+ * returns how many there are (no device work). */
+int silt_known_exact_divisors(float* out, int32_t cap);
 /* FluidCore::fine_water_debug (src/fluid_core/near.rs:341): lays the patch
  * down for these tires, copies patch `patch` (fine_res^2 floats) and its
  * origin, and packs it back. */
@@ -265,6 +273,10 @@ typedef struct {
     int64_t steps, launches, force_launches, force_cells, force_cells_water;
     int64_t device_counts;  /* steps whose substep count the device decided */
     double host_step_ms, host_fine_ms;  /* host time inside silt_step, and its nested-patch share */
+    /* Grid engine, Gauss-Seidel sweep: launches, the most fixed-point passes
+     * one launch needed, launches that reached the pass limit and ran the
+     * sequential sweep. */
+    int64_t sweep_launches, sweep_passes_max, sweep_fallbacks;
 } silt_step_parts;
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
@@ -300,6 +312,17 @@ int silt_set_fine_sub_cap(silt_sheet* s, float cap);
 int silt_set_fine_pace(silt_sheet* s, int32_t pace);
 /* FluidCore::set_near_field (src/fluid_core/near.rs:332). */
 int silt_set_near_field(silt_sheet* s, int32_t on);
+/* Vorticity confinement of the grid engine's coarse pair. SWEEP (default) is
+ * the reference step pair's form: step_pair runs its sheets' inner loops
+ * serially, so force_gravity_open (src/fluid_core.rs:2234-2260) confines in a
+ * raster-order Gauss-Seidel sweep; the grid engine solves that sweep as a
+ * fixed point across tiles and gives its result bit for bit. SNAPSHOT is the
+ * Jacobi form of force_gravity_par (:2263), which the reference takes for
+ * boxes of at least 48 x 32 outside a step pair. The window engine always
+ * sweeps as the reference does; this knob does not change it. */
+#define SILT_CONFINE_SWEEP 0
+#define SILT_CONFINE_SNAPSHOT 1
+int silt_set_confinement(silt_sheet* s, int32_t form);
 /* FluidCore::set_open_water (src/fluid_core.rs:5293-5303; on = 0 is None):
  * the water sheet runs at `mobility` (clamped to [0, 1]) with Manning bed
  * friction `manning_n` and eddy viscosity `eddy_m2_s` (m^2/s) after each
@@ -361,7 +384,10 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
  * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (4 MiB per
  * GPU that loads the library, held until the process exits); larger grids
  * return SILT_EINVAL. The first call on each device looks the array up (with
- * that device current), so make that first call before any stream capture.
+ * that device current) and keeps its address for the rest of the process,
+ * so make that first call before any stream capture begins; nothing here
+ * states whether later calls can be captured. After cudaDeviceReset the kept
+ * address is stale: do not call this entry point on a device that was reset.
  * Every call shares the one array: calls whose work overlaps on the GPU race
  * and must be ordered by the caller (one stream, or events). Calls no
  * cudaMalloc, cudaFree or other allocating routine. */

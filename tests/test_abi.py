@@ -33,3 +33,14 @@ def test_window_origin_matches_the_oracle_snap():
 
     for c in ((0.0, 0.0), (3.3, -7.1), (-125.07, 40.93), (0.1, 0.1), (19.9999, -0.0001)):
         assert silt_b200.window_origin(c) == oracle.Core(center=c).origin(), c
+
+
+def test_known_exact_divisors_need_no_device():
+    """The table of divisors taken as checked is host data: 2 cell, cell^2,
+    231 and cell of the 0.2 m and 0.02 m sheets, each once."""
+    import numpy as np
+
+    got = silt_b200.known_exact_divisors()
+    f = np.float32
+    assert len(got) == len(set(got)) == 7
+    assert float(f(0.2) * f(0.2)) in got and float(f(0.02) * f(0.02)) in got and 231.0 in got
