@@ -318,9 +318,13 @@ class Sheet:
         check(lib().silt_set_center(self.h, cx, cz), "set_center")
 
     def origin(self):
+        return self.window_bounds()[:2]
+
+    def window_bounds(self):
+        """FluidCore::window_bounds: origin x, origin z, extent (m)."""
         ox, oz, ext = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         check(lib().silt_window_bounds(self.h, ctypes.byref(ox), ctypes.byref(oz), ctypes.byref(ext)), "window_bounds")
-        return ox.value, oz.value
+        return ox.value, oz.value, ext.value
 
     def set_river_reach(self, reach):
         """FluidCore::set_river_reach: dict of RiverReach fields, or None."""

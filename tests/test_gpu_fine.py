@@ -40,14 +40,21 @@ def compare(ref, dev, tol=TOL_H):
     return out
 
 
-@pytest.mark.parametrize("pace", [0, 1])
+@pytest.mark.parametrize("pace", [0, 1, 2, 3])
 def test_mean_patch_drive_matches_oracle(pace):
+    """Pace 0 and 1 step the open 2 cm sheet on its awake tiles; pace 2 and 3
+    split the whole wet rectangle by adaptive CFL (pace 3: one pressure solve,
+    then a flux per Courant slice, pace3_slices src/fluid_core.rs:1836),
+    capped at eight substeps as the reference's ThroughDrive sets it
+    (src/world.rs:4307-4308)."""
     dt = 1.0 / 30.0
     ref, dev = O.Core(), G.Sheet()
     for c in (ref, dev):
         c.pour_water(-3.0, 3.0, -2.0, 8.0, 0.08)
         c.pour_slurry(-1.0, 1.0, -2.0, 6.0, 0.03, 0, 0.6)
         c.set_fine_pace(pace)
+        if pace >= 2:
+            c.set_fine_sub_cap(8.0)
     ev_r = drive(ref, 20, dt)
     ev_d = drive(dev, 20, dt)
     d = compare(ref, dev)
