@@ -43,6 +43,10 @@ INFLOW = (0, -2.0, 2.0, 0.5)
 FORCE_BYTES_WATER = 24
 FORCE_BYTES_SLURRY = 29
 STEP_BYTES_PER_CELL = 57   # the fused step's algorithmic bytes (both layers) per coarse cell
+# Per stepped cell-layer and substep, as each layer steps on its own: water
+# reads h, u, v, bed and writes h, u, v; slurry also reads grain and moisture.
+STEP_BYTES_WATER = 28
+STEP_BYTES_SLURRY = 33
 
 
 def parse():
@@ -54,6 +58,8 @@ def parse():
     ap.add_argument("--res", type=int, default=RES)
     ap.add_argument("--no-tires", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--no-batch-roofline", action="store_true",
+                    help="grid: skip the second roofline entry (the batched force kernel on the 256-window batch)")
     ap.add_argument("--workload", default="grid", choices=["grid", "batch", "window200", "walls200", "closure"],
                     help="grid: one 2048^2 grid with four tire patches; batch: many windows stepped together; "
                          "window200: the reference's own 200^2 window, no tires; walls200: that window with a "
@@ -175,37 +181,51 @@ def cpu_threads(args):
     return 2 if args.no_tires else 2 * 4
 
 
-def cpu_baseline(args, scene, max_steps=40, warmup=1, budget_s=20.0):
+def cpu_baseline(args, scene, max_steps=40, warmup=1, budget_s=15.0, single=True):
     """The CPU oracle (restated reference) on this host: the same workload for a
-    bounded sample of steps (at most `max_steps`, stopping once `budget_s` has passed)."""
+    bounded sample of steps (at most `max_steps`, stopping once `budget_s` has
+    passed), built -O3 -march=native here. Two variants: the reference's
+    threading (the two sheets of each pair on their own threads, as its
+    rayon::join does) and, with `single`, one thread."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    threads = cpu_threads(args)
-    core = oracle.Core(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=threads)
-    seed(core, scene)
-    k = 0
-    for _ in range(max(1, warmup)):
-        for t in tires_for(k, args):
-            core.push_tire(**t)
-        core.step(DT)
-        k += 1
-    steps = 0
-    t0 = time.perf_counter()
-    el = 0.0
-    while steps < max(1, max_steps) and el < budget_s:
-        for t in tires_for(k, args):
-            core.push_tire(**t)
-        core.step(DT)
-        k += 1
-        steps += 1
-        el = time.perf_counter() - t0
+    flags = oracle.use_native_build()
+
+    def run(threads):
+        core = oracle.Core(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=threads)
+        seed(core, scene)
+        k = 0
+        for _ in range(max(1, warmup)):
+            for t in tires_for(k, args):
+                core.push_tire(**t)
+            core.step(DT)
+            k += 1
+        steps = 0
+        t0 = time.perf_counter()
+        el = 0.0
+        while steps < max(1, max_steps) and el < budget_s:
+            for t in tires_for(k, args):
+                core.push_tire(**t)
+            core.step(DT)
+            k += 1
+            steps += 1
+            el = time.perf_counter() - t0
+        return steps, el
+
     fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
-    value = (args.res * args.res + fine_cells) * steps / el
-    return {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-            "steps": steps, "seconds": el, "host": host_cpu(),
-            "sample": f"{steps} steps of the same {args.res}^2 workload after {max(1, warmup)} warm-up step(s); "
-                      f"coarse pair on 2 threads, fine patch sheets on {threads} ({el:.2f} s)"}
+    cells = args.res * args.res + fine_cells
+    threads = cpu_threads(args)
+    steps, el = run(threads)
+    out = {"value": cells * steps / el, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+           "steps": steps, "seconds": el, "host": host_cpu(), "build": flags,
+           "sample": f"{steps} steps of the same {args.res}^2 workload after {max(1, warmup)} warm-up step(s); "
+                     f"coarse pair on 2 threads, fine patch sheets on {threads} ({el:.2f} s)"}
+    if single:
+        s1, e1 = run(1)
+        out["single_thread"] = {"value": cells * s1 / e1, "unit": "cell-steps/s", "cores": 1, "steps": s1,
+                                "seconds": e1, "ms_per_step": 1000.0 * e1 / s1}
+    return out
 
 
 def run_reference(args):
@@ -213,7 +233,7 @@ def run_reference(args):
     if rank != 0:
         return
     scene = make_scene(args)
-    base = cpu_baseline(args, scene, max_steps=args.steps, warmup=args.warmup, budget_s=60.0)
+    base = cpu_baseline(args, scene, max_steps=args.steps, warmup=args.warmup, budget_s=60.0, single=False)
     fine_cells = 0 if args.no_tires else 4 * FINE_RES * FINE_RES
     line = {"metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
             "steps": base["steps"], "warmup": max(1, args.warmup),
@@ -258,17 +278,18 @@ def run_b200(args):
             sheet.push_tire(**t)
         return sheet.step(DT, want_spray=want_spray)
 
-    for _ in range(args.warmup):
+    for _ in range(max(3, args.warmup)):
         one_step(False)
     sheet.sync()
     torch.cuda.synchronize()
-    # Device-resident timed region.
+    # Device-resident timed region: K steps, no events inside; the library's
+    # counters (launches, stepped tiles) are read before and after it.
+    p0 = sheet.step_parts()
     stop = threading.Event()
     clock_lines = []
     th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, local), daemon=True)
     th.start()
     time.sleep(0.3)
-    sheet.set_step_timing(True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -282,34 +303,44 @@ def run_b200(args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    parts = sheet.step_parts()
-    sheet.set_step_timing(False)
     stop.set()
     th.join(timeout=5)
+    p1 = sheet.step_parts()
+    parts = {k: p1[k] - p0[k] for k in ("launches", "force_launches", "force_cells", "force_cells_water",
+                                        "device_counts", "steps")}
+    parts["sweep_passes_max"] = p1["sweep_passes_max"]
+    parts["sweep_fallbacks"] = p1["sweep_fallbacks"]
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * cells_per_step * args.steps / (ms / 1000.0)
-    # End-to-end through the public API: pushes in, spray events and the FP64 ledger out, every step.
-    # The pushes reach the device inside silt_step (its pinned step table);
-    # spray events and the ledger come back through pinned buffers.
-    e2e_steps = max(10, args.steps // 4)
+    # Kernel pass: the same K steps again with two CUDA events around every
+    # launch on its stream, for each kernel's device time and share.
+    silt_b200.set_kernel_timing(True)
+    for _ in range(args.steps):
+        one_step(False)
+    kt = silt_b200.kernel_times()
+    silt_b200.set_kernel_timing(False)
+    # End to end through the public API, every timed step: the tire pushes go
+    # in (inside silt_step, from its pinned step table), the spray events and
+    # the FP64 ledger come back, and the ledger's closure is checked each step.
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = args.steps
+    prev = sheet.ledger()
     f0.record(stream)
     nev = 0
-    prev = sheet.ledger()
-    gap = 0.0  # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
+    gaps = []  # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
     for _ in range(e2e_steps):
         ev = one_step(True)
         nev += len(ev)
         led = sheet.ledger()
         kept = led["total_m3"] + led["cut_m3"] - led["opened_m3"]
-        gap = max(gap, abs(kept - (prev["total_m3"] + prev["cut_m3"] - prev["opened_m3"])) / led["total_m3"])
+        gaps.append(abs(kept - (prev["total_m3"] + prev["cut_m3"] - prev["opened_m3"])) / led["total_m3"])
         prev = led
     f1.record(stream)
     torch.cuda.synchronize()
@@ -323,36 +354,43 @@ def run_b200(args):
     if rank == 0:
         peak, peak_kind = measured_peak()
         launches = max(parts["force_launches"], 1)
-        force_ms = parts["force_ms"] / launches
-        cw = parts["force_cells_water"] / launches
+        cw = parts["force_cells_water"] / launches          # stepped cell-layers per coarse substep
         cs = (parts["force_cells"] - parts["force_cells_water"]) / launches
-        force_bytes = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * cs
-        achieved = force_bytes / (force_ms / 1000.0) / 1e9 if force_ms > 0 else None
-        per_cell = profiled_traffic()
-        roof = {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                "traffic": per_cell * force_bytes if per_cell else None,
-                "traffic_basis": "ncu ratio of DRAM bytes to algorithmic bytes on a 1024^2 launch with every "
-                                 "tile stepped, times this launch's algorithmic bytes",
-                "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": force_ms,
-                "stepped_cell_layers_per_launch": cw + cs,
-                "active_fraction": (cw + cs) / (2.0 * args.res * args.res),
-                "transport_avg_launch_ms": parts["transport_ms"] / max(parts["force_launches"], 1)}
+        substeps_per_step = parts["force_launches"] / max(parts["steps"], 1)
+        fine_layers = 0 if args.no_tires else 4 * FINE_RES * FINE_RES  # per layer, one patch pass
+        models = kernel_bytes_models(cw, cs, fine_layers)
+        roof, kernels = kernel_roofline(kt, models, peak, peak_kind)
+        step_bytes = substeps_per_step * (STEP_BYTES_WATER * cw + STEP_BYTES_SLURRY * cs) + \
+            (STEP_BYTES_WATER + STEP_BYTES_SLURRY) * fine_layers
+        step_ms = ms / args.steps
+        roof["step"] = {"algorithmic_bytes_per_step": step_bytes, "ms_per_step": step_ms,
+                        "achieved": step_bytes / (step_ms / 1000.0) / 1e9, "unit": "GB/s",
+                        "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak,
+                        "basis": "28 B per stepped water cell-layer, 33 B per slurry cell-layer per substep "
+                                 "(reads h, u, v, bed [+ grain, moisture], writes h, u, v), coarse tiles the "
+                                 "step stepped plus every 2 cm patch cell"}
+        stepped_per_step = substeps_per_step * (cw + cs) + 2 * fine_layers
         line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": workload(args), "roofline": roof,
+                "data": "synthetic", "config": workload(args), "roofline": roof, "kernels": kernels,
+                "stepped_cell_layers_per_s": world * stepped_per_step * args.steps / (ms / 1000.0),
                 "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(tires_for(1, args)) * 32,
                         "d2h_bytes_per_step": 56 + 4 + 32 * (nev // max(e2e_steps, 1)), "steps": e2e_steps},
                 "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
-                "host_ms_per_step": {"silt_step": parts["host_step_ms"] / args.steps,
-                                     "nested_patches": parts["host_fine_ms"] / args.steps},
                 "device_counted_steps": int(parts["device_counts"]),
+                "confinement": {"form": "gauss-seidel sweep (step_pair)",
+                                "most_fixed_point_passes": int(parts["sweep_passes_max"]),
+                                "sequential_fallbacks": int(parts["sweep_fallbacks"])},
                 "window_steps_per_s": world * args.steps / (ms / 1000.0),
                 "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
                            "spray_m3": led["spray_m3"], "cut_m3": led["cut_m3"],
-                           "gap_max_per_step": gap, "gap_steps": e2e_steps}}
+                           "gap_max_per_step": max(gaps), "gap_median_per_step": statistics.median(gaps),
+                           "gap_steps": len(gaps), "gap_target": 1e-9}}
+        if not args.no_batch_roofline and world == 1:
+            sheet.sync()
+            line["roofline_batch"] = batch_roofline(args, local, peak, peak_kind)
         if not args.no_baseline:
             line["cpu_baseline"] = cpu_baseline(args, scene)
         print(json.dumps(line), flush=True)
@@ -360,6 +398,125 @@ def run_b200(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def kernel_bytes_models(cw, cs, fine_layers):
+    """Algorithmic bytes of one launch, by kernel name, for the grid step:
+    cw, cs = stepped water and slurry cell-layers of one coarse substep,
+    fine_layers = 2 cm patch cells per layer."""
+    force = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * cs
+    window = (STEP_BYTES_WATER + STEP_BYTES_SLURRY) * fine_layers
+    return {"k_force_sweep": (force, "24 B per stepped water cell-layer, 29 B per slurry cell-layer: reads h, u, v, "
+                                     "bed (+ grain, moisture), writes u, v"),
+            "k_force": (force, "as k_force_sweep"),
+            "k_transport": (16 * (cw + cs), "16 B per stepped cell-layer: reads h, u, v, writes h"),
+            "k_window_step": (window, "28 B per 2 cm water cell, 33 B per slurry cell (reads h, u, v, bed [+ grain, "
+                                      "moisture], writes h, u, v), every patch cell of both layers")}
+
+
+def kernel_roofline(kt, models, peak, peak_kind):
+    """The roofline of the kernel with the largest device time in the kernel
+    pass, and every kernel's launches, average and share."""
+    total = sum(k["ms"] for k in kt) or 1.0
+    kernels = [{"name": k["name"], "launches": k["launches"], "avg_ms": k["ms"] / max(k["launches"], 1),
+                "share": k["ms"] / total} for k in kt]
+    roof = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+            "timing": "CUDA events around every launch on its stream, in a pass of the same K steps after the "
+                      "timed one"}
+    if kt:
+        top = kt[0]
+        short = top["name"].split("::")[-1]
+        roof["kernel"] = top["name"]
+        roof["share"] = top["ms"] / total
+        avg_ms = top["ms"] / max(top["launches"], 1)
+        roof["avg_launch_ms"] = avg_ms
+        model = models.get(short)
+        if model:
+            roof["algorithmic_bytes_per_launch"] = model[0]
+            roof["bytes_basis"] = model[1]
+            roof["achieved"] = model[0] / (avg_ms / 1000.0) / 1e9
+            roof["frac"] = roof["achieved"] / peak
+        else:
+            roof["achieved"] = roof["frac"] = None
+        roof["traffic"] = profiled_kernel_traffic(short)
+    return roof, kernels
+
+
+def profiled_kernel_traffic(short):
+    """DRAM bytes per launch (read + write) of the kernel from the committed
+    ncu summary profiles/kernel_traffic.txt (lines `name: bytes`), or None."""
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", "kernel_traffic.txt")):
+            if ln.split(":", 1)[0].strip() == short:
+                return float(ln.split(":", 1)[1].split()[0])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
+def batch_roofline(args, local, peak, peak_kind):
+    """The batched force kernel on the 256-window batch (sides log-uniform
+    64..512, 0..4 tires): its kernel pass and roofline."""
+    import numpy as np
+    import torch
+
+    import silt_b200
+    import silt_scenes
+
+    stream = torch.cuda.Stream()
+    wins = silt_scenes.batch_windows(n=256, base_seed=0x9E3779B9, cell=CELL)
+    sheets = []
+    for w in wins:
+        sh = silt_b200.Sheet(res=w["res"], cell=CELL, fine_res=FINE_RES, fine_cell=0.02,
+                             layout=silt_b200.FINE_PER_TIRE, device=local, stream=stream.cuda_stream,
+                             engine=silt_b200.ENGINE_GRID)
+        silt_scenes.seed_core(sh, w)
+        sheets.append(sh)
+    batch = silt_b200.Batch(sheets)
+    step_no = 0
+
+    def one_step():
+        nonlocal step_no
+        step_no += 1
+        idx, ts = [], []
+        for k, w in enumerate(wins):
+            for t in batch_tires(step_no, w):
+                idx.append(k)
+                ts.append(t)
+        batch.push_tires(idx, ts)
+        batch.step(DT)
+
+    for _ in range(3):
+        one_step()
+    steps = 10
+    p0 = batch.parts()
+    silt_b200.set_kernel_timing(True)
+    for _ in range(steps):
+        one_step()
+    kt = silt_b200.kernel_times()
+    silt_b200.set_kernel_timing(False)
+    p1 = batch.parts()
+    launches = max(p1["force_launches"] - p0["force_launches"], 1)
+    cw = (p1["force_cells_water"] - p0["force_cells_water"]) / launches
+    cs = (p1["force_cells"] - p1["force_cells_water"] - (p0["force_cells"] - p0["force_cells_water"])) / launches
+    force = FORCE_BYTES_WATER * cw + FORCE_BYTES_SLURRY * cs
+    out = {"workload": "batch256_side64-512_logu_1-4puddles_0-4tires64", "steps": steps}
+    for k in kt:
+        short = k["name"].split("::")[-1]
+        if short in ("k_batch_force_sweep", "k_batch_force"):
+            avg = k["ms"] / max(k["launches"], 1)
+            out.update({"kernel": k["name"], "avg_launch_ms": avg, "algorithmic_bytes_per_launch": force,
+                        "stepped_cell_layers_per_launch": cw + cs, "achieved": force / (avg / 1000.0) / 1e9,
+                        "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+                        "share": k["ms"] / (sum(x["ms"] for x in kt) or 1.0),
+                        "traffic": profiled_kernel_traffic(short)})
+            out["frac"] = out["achieved"] / peak
+    out["kernels"] = [{"name": k["name"], "launches": k["launches"], "avg_ms": k["ms"] / max(k["launches"], 1)}
+                      for k in kt[:8]]
+    batch.close()
+    for sh in sheets:
+        sh.close()
+    return out
 
 
 # ---------------------------------------------------------------- batched windows
@@ -398,6 +555,7 @@ def batch_cpu(args, wins, max_steps, warmup, budget_s):
     stepped on its own (the reference steps one FluidCore at a time)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    oracle.use_native_build()
     import silt_scenes
 
     sample = wins[::16]
@@ -620,6 +778,7 @@ def run_window200(args):
     if args.impl == "reference":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
+        oracle.use_native_build()
 
         core = oracle.Core(threads=2)
         seed_window(core, scene)
@@ -680,6 +839,7 @@ def run_window200(args):
     if not args.no_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
+        oracle.use_native_build()
 
         core = oracle.Core(threads=2)
         seed_window(core, scene)
@@ -731,6 +891,7 @@ def closure_cpu(scenes, T, max_steps, budget_s):
     oracle for every 16th window."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    oracle.use_native_build()
     import silt_scenes
 
     sample = scenes[::16]

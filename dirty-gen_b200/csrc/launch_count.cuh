@@ -29,6 +29,23 @@ __device__ __forceinline__ void dep_wait() {
 #endif
 }
 
+// Per-launch device timing (silt_set_kernel_timing, kernel_timer.cu): while
+// it is on, every launch of the library is bracketed by two CUDA events on
+// its own stream, and the elapsed time is booked to the kernel.
+bool kernel_timing_on();
+void kernel_timing_begin(cudaStream_t st);
+void kernel_timing_end(cudaStream_t st, const void* kernel);
+
+// cudaLaunchKernelEx with the optional timing around it.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_ex(const cudaLaunchConfig_t& cfg, void (*kernel)(KArgs...), Args&&... args) {
+    const bool timed = kernel_timing_on();
+    if (timed) kernel_timing_begin(cfg.stream);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    if (timed) kernel_timing_end(cfg.stream, reinterpret_cast<const void*>(kernel));
+    return e;
+}
+
 template <typename... KArgs, typename... Args>
 cudaError_t launch_dep(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                        Args&&... args) {
@@ -42,7 +59,7 @@ cudaError_t launch_dep(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    return launch_ex(cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace silt

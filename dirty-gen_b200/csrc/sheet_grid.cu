@@ -1295,7 +1295,7 @@ cudaError_t launch_coop(K kernel, int grid, cudaStream_t st, Args... args) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+    const cudaError_t e = ::silt::launch_ex(cfg, kernel, args...);
     ::silt::count_launch();
     return e;
 }

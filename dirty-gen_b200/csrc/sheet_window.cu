@@ -1345,7 +1345,7 @@ cudaError_t launch_window_step_list(Job* const* d_job_list, int njobs, int max_r
     attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 2;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step_list, d_job_list);
+    cudaError_t e = ::silt::launch_ex(cfg, k_window_step_list, d_job_list);
     ::silt::count_launch();
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
@@ -1368,7 +1368,7 @@ cudaError_t launch_window_step(const Job* d_jobs, int njobs, int max_res, cudaSt
     attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 2;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_window_step, const_cast<Job*>(d_jobs));
+    cudaError_t e = ::silt::launch_ex(cfg, k_window_step, const_cast<Job*>(d_jobs));
     ::silt::count_launch();
     if (e != cudaSuccess) return e;
     return cudaGetLastError();

@@ -83,6 +83,10 @@ class StepParts(ctypes.Structure):
                 ("sweep_passes_max", ctypes.c_int64), ("sweep_fallbacks", ctypes.c_int64)]
 
 
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 96), ("launches", ctypes.c_int64), ("ms", ctypes.c_double)]
+
+
 class SiltError(RuntimeError):
     pass
 
@@ -146,6 +150,7 @@ def lib():
             "silt_set_wave_maker": [_p, ctypes.POINTER(WaveMaker)],
             "silt_check_fixed_division": [_f, ctypes.POINTER(ctypes.c_ulonglong), _p],
             "silt_known_exact_divisors": [_p, _i],
+            "silt_set_kernel_timing": [_i], "silt_get_kernel_times": [_p, _i, ctypes.POINTER(_i)],
             "silt_set_hydro_solids": [_p, ctypes.POINTER(HydroSolid), _i],
             "silt_get_hydro_load": [_p, ctypes.POINTER(HydroLoad)],
             "silt_lay_slurry_on_water": [_p, _f, _i, _p], "silt_window_origin": [_f, _f, _i, _f, _p],
@@ -449,6 +454,21 @@ def window_origin(center, res=200, cell=0.2):
     o = (ctypes.c_float * 2)()
     check(lib().silt_window_origin(float(center[0]), float(center[1]), int(res), float(cell), o), "window_origin")
     return float(o[0]), float(o[1])
+
+
+def set_kernel_timing(on):
+    """Per-launch device timing of every library kernel (process-wide)."""
+    check(lib().silt_set_kernel_timing(int(on)), "set_kernel_timing")
+
+
+def kernel_times():
+    """Totals by kernel since timing was switched on: [{name, launches, ms}],
+    largest total first. Waits for the device."""
+    n = _i(0)
+    check(lib().silt_get_kernel_times(None, 0, ctypes.byref(n)), "kernel_times")
+    rows = (KernelTime * max(n.value, 1))()
+    check(lib().silt_get_kernel_times(ctypes.cast(rows, _p), n.value, ctypes.byref(n)), "kernel_times")
+    return [dict(name=r.name.decode(), launches=int(r.launches), ms=float(r.ms)) for r in rows[:n.value]]
 
 
 def known_exact_divisors():

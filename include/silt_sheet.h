@@ -281,6 +281,21 @@ typedef struct {
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
 
+/* Device time of every kernel this library launches, from any handle or
+ * thread, while on: each launch is bracketed by two CUDA events on its own
+ * stream (which costs the overlap of back-to-back launches, so time a pass of
+ * its own). on = 1 clears earlier totals. silt_get_kernel_times waits for the
+ * device and writes up to cap rows, largest total first; *n_out is the
+ * number of kernels seen. A GPU counterpart of the reference's per-part step
+ * timing (FluidCore::step_parts, src/fluid_core.rs:4782-4795), by kernel. */
+typedef struct {
+    char name[96];     /* qualified kernel name, no argument list */
+    int64_t launches;
+    double ms;         /* summed device time */
+} silt_kernel_time;
+int silt_set_kernel_timing(int32_t on);
+int silt_get_kernel_times(silt_kernel_time* out, int32_t cap, int32_t* n_out);
+
 /* ------------------------------------------------------- batched windows */
 /* Many independent windows stepped together (vehicles or scenes, each its own
  * FluidCore in the reference, which steps them one after another). A batch

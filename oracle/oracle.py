@@ -16,27 +16,57 @@ _i = ctypes.c_int
 _p = ctypes.c_void_p
 
 
-class CoreCfg(ctypes.Structure):
-    _fields_ = [("res", _i), ("cell", _f), ("fine_res", _i), ("fine_cell", _f),
-                ("layout", _i), ("tire_r", _f), ("soften", _i), ("inner_par", _i),
-                ("center_x", _f), ("center_z", _f), ("threads", _i)]
+def _structs(real):
+    """The interface's structures with `real` for every float field (the
+    FP64 build's interface carries doubles)."""
+
+    class CoreCfg(ctypes.Structure):
+        _fields_ = [("res", _i), ("cell", real), ("fine_res", _i), ("fine_cell", real),
+                    ("layout", _i), ("tire_r", real), ("soften", _i), ("inner_par", _i),
+                    ("center_x", real), ("center_z", real), ("threads", _i)]
+
+    class Tire(ctypes.Structure):
+        _fields_ = [("x", real), ("z", real), ("forward_x", real), ("forward_z", real),
+                    ("radius", real), ("width", real), ("speed", real), ("slip", real)]
+
+    class Spray(ctypes.Structure):
+        _fields_ = [("x", real), ("y", real), ("z", real), ("vx", real), ("vy", real), ("vz", real),
+                    ("volume", real), ("kind", _i)]
+
+    return CoreCfg, Tire, Spray
 
 
-class Tire(ctypes.Structure):
-    _fields_ = [("x", _f), ("z", _f), ("forward_x", _f), ("forward_z", _f),
-                ("radius", _f), ("width", _f), ("speed", _f), ("slip", _f)]
-
-
-class Spray(ctypes.Structure):
-    _fields_ = [("x", _f), ("y", _f), ("z", _f), ("vx", _f), ("vy", _f), ("vz", _f),
-                ("volume", _f), ("kind", _i)]
+CoreCfg, Tire, Spray = _structs(_f)
+CoreCfg64, Tire64, Spray64 = _structs(ctypes.c_double)
 
 
 def build():
     subprocess.check_call(["make", "-s", "-C", HERE])
 
 
+NATIVE_PATH = os.path.join(HERE, "_native", "liboracle_silt.so")
+NATIVE_FLAGS = "-O3 -march=native -ffp-contract=off"
+
+
+def use_native_build(timeout=300):
+    """Loads the -O3 -march=native build (compiled here on first use) in
+    place of the portable one; must come before the first call. Returns the
+    flags of the build in use."""
+    global LIB_PATH
+    if _lib is not None:
+        return NATIVE_FLAGS if LIB_PATH == NATIVE_PATH else "-O2 -ffp-contract=off"
+    try:
+        subprocess.run(["make", "-s", "-C", HERE, "native"], check=True, timeout=timeout,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        LIB_PATH = NATIVE_PATH
+        return NATIVE_FLAGS
+    except (subprocess.SubprocessError, OSError):
+        return "-O2 -ffp-contract=off"
+
+
 _lib = None
+_lib64 = None
+LIB64_PATH = os.path.join(HERE, "liboracle_silt_f64.so")
 
 
 def lib():
@@ -44,7 +74,22 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = ctypes.CDLL(LIB_PATH)
+        _lib = _bind(ctypes.CDLL(LIB_PATH), _f, CoreCfg, Tire)
+    return _lib
+
+
+def lib64():
+    """The FP64 restatement (same source, built with -DORACLE_F64)."""
+    global _lib64
+    if _lib64 is None:
+        if not os.path.exists(LIB64_PATH):
+            build()
+        _lib64 = _bind(ctypes.CDLL(LIB64_PATH), ctypes.c_double, CoreCfg64, Tire64)
+    return _lib64
+
+
+def _bind(L, _f, CoreCfg, Tire):
+    if True:
         L.oracle_scratch_new.restype = _p
         L.oracle_scratch_free.argtypes = [_p]
         L.oracle_step_sheet.argtypes = [_p, _p, _p, _p, _p, _p, _i, _f, _f, _f, _f, _i, _f, _i, _i, _p]
@@ -106,8 +151,7 @@ def lib():
         L.oracle_core_hydro_load.argtypes = [_p, _p]
         L.oracle_core_lay_slurry_on_water.argtypes = [_p, _f, _i]
         L.oracle_core_lay_slurry_on_water.restype = _f
-        _lib = L
-    return _lib
+    return L
 
 
 def _ptr(a):
@@ -185,146 +229,153 @@ FIELDS = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6,
 class Core:
     """The reference `FluidCore` subset on the sheet path (window 200 at 0.2 m by default)."""
 
+    _L = staticmethod(lib)
+    _np = np.float32
+    _Cfg, _Tire, _Spray = CoreCfg, Tire, Spray
+
+    def _arr(self, a):
+        return np.ascontiguousarray(a, dtype=self._np)
+
     def __init__(self, res=200, cell=0.2, fine_res=160, fine_cell=0.02, layout=0, tire_r=0.56,
                  soften=True, inner_par=False, center=(0.0, 0.0), threads=1):
         self.res = res
         self.fine_res = fine_res
-        cfg = CoreCfg(res, cell, fine_res, fine_cell, layout, tire_r, int(soften), int(inner_par),
+        cfg = self._Cfg(res, cell, fine_res, fine_cell, layout, tire_r, int(soften), int(inner_par),
                       center[0], center[1], int(threads))
-        self.h = lib().oracle_core_new(ctypes.byref(cfg))
+        self.h = self._L().oracle_core_new(ctypes.byref(cfg))
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().oracle_core_free(self.h)
+            self._L().oracle_core_free(self.h)
             self.h = None
 
     def map_water_bed(self, bed, water):
-        return lib().oracle_core_map_water_bed(self.h, _ptr(f32(bed)), _ptr(f32(water)))
+        return self._L().oracle_core_map_water_bed(self.h, _ptr(self._arr(bed)), _ptr(self._arr(water)))
 
     def map_grain(self, grain):
-        lib().oracle_core_map_grain(self.h, _ptr(np.ascontiguousarray(grain, np.uint8)))
+        self._L().oracle_core_map_grain(self.h, _ptr(np.ascontiguousarray(grain, np.uint8)))
 
     def map_water_velocity(self, u, v):
-        lib().oracle_core_map_water_velocity(self.h, _ptr(f32(u)), _ptr(f32(v)))
+        self._L().oracle_core_map_water_velocity(self.h, _ptr(self._arr(u)), _ptr(self._arr(v)))
 
     def pour_water(self, x0, x1, z0, z1, depth):
-        return lib().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 1, 3, 1.0)
+        return self._L().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 1, 3, 1.0)
 
     def pour_slurry(self, x0, x1, z0, z1, depth, grain, moisture):
-        return lib().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 0, grain, moisture)
+        return self._L().oracle_core_pour(self.h, x0, x1, z0, z1, depth, 0, grain, moisture)
 
     def lay_slurry_mask(self, depth, grain, moisture):
-        return lib().oracle_core_lay_slurry_mask(self.h, _ptr(f32(depth)), grain, moisture)
+        return self._L().oracle_core_lay_slurry_mask(self.h, _ptr(self._arr(depth)), grain, moisture)
 
     def read_substrate(self, bed, moisture, grain):
-        lib().oracle_core_read_substrate(self.h, _ptr(f32(bed)), _ptr(f32(moisture)),
+        self._L().oracle_core_read_substrate(self.h, _ptr(self._arr(bed)), _ptr(self._arr(moisture)),
                                          _ptr(np.ascontiguousarray(grain, np.uint8)))
 
     def push_tire(self, **kw):
-        t = Tire(kw["x"], kw["z"], kw.get("forward_x", 0.0), kw.get("forward_z", 1.0), kw["radius"],
+        t = self._Tire(kw["x"], kw["z"], kw.get("forward_x", 0.0), kw.get("forward_z", 1.0), kw["radius"],
                  kw["width"], kw["speed"], kw.get("slip", 0.0))
-        lib().oracle_core_push_tire(self.h, ctypes.byref(t))
+        self._L().oracle_core_push_tire(self.h, ctypes.byref(t))
 
     def step(self, dt):
         cap = 65536
-        buf = (Spray * cap)()
-        n = lib().oracle_core_step(self.h, dt, buf, cap)
+        buf = (self._Spray * cap)()
+        n = self._L().oracle_core_step(self.h, dt, buf, cap)
         return [(s.x, s.y, s.z, s.vx, s.vy, s.vz, s.volume, s.kind) for s in buf[:min(n, cap)]]
 
     def ledger(self):
-        o = np.zeros(5, np.float32)
+        o = np.zeros(5, self._np)
         o64 = np.zeros(2, np.float64)
-        lib().oracle_core_ledger(self.h, _ptr(o), _ptr(o64))
+        self._L().oracle_core_ledger(self.h, _ptr(o), _ptr(o64))
         return dict(water_m3=float(o[0]), slurry_m3=float(o[1]), frozen_water_m3=float(o[2]),
                     frozen_slurry_m3=float(o[3]), spray_m3=float(o[4]), water64=float(o64[0]),
                     slurry64=float(o64[1]))
 
     def get(self, name):
-        out = np.zeros(self.res * self.res, np.float32)
-        lib().oracle_core_get(self.h, FIELDS[name], _ptr(out))
+        out = np.zeros(self.res * self.res, self._np)
+        self._L().oracle_core_get(self.h, FIELDS[name], _ptr(out))
         return out
 
     def set(self, name, arr):
-        lib().oracle_core_set(self.h, FIELDS[name], _ptr(f32(arr)))
+        self._L().oracle_core_set(self.h, FIELDS[name], _ptr(self._arr(arr)))
 
     def grain(self):
         out = np.zeros(self.res * self.res, np.uint8)
-        lib().oracle_core_get_grain(self.h, _ptr(out))
+        self._L().oracle_core_get_grain(self.h, _ptr(out))
         return out
 
     def publish(self):
-        film = np.zeros(2 * self.res * self.res, np.float32)
-        flow = np.zeros(4 * self.res * self.res, np.float32)
-        lib().oracle_core_publish(self.h, _ptr(film), _ptr(flow))
+        film = np.zeros(2 * self.res * self.res, self._np)
+        flow = np.zeros(4 * self.res * self.res, self._np)
+        self._L().oracle_core_publish(self.h, _ptr(film), _ptr(flow))
         return film, flow
 
     def set_fine_pace(self, pace):
-        lib().oracle_core_set_fine_pace(self.h, pace)
+        self._L().oracle_core_set_fine_pace(self.h, pace)
 
     def set_fine_sub_cap(self, cap):
-        lib().oracle_core_set_fine_sub_cap(self.h, cap)
+        self._L().oracle_core_set_fine_sub_cap(self.h, cap)
 
     def set_near_field(self, on):
-        lib().oracle_core_set_near_field(self.h, int(on))
+        self._L().oracle_core_set_near_field(self.h, int(on))
 
     def set_open_water(self, on, mobility=0.0, manning_n=0.0, eddy_m2_s=0.0):
-        lib().oracle_core_set_open_water(self.h, int(on), mobility, manning_n, eddy_m2_s)
+        self._L().oracle_core_set_open_water(self.h, int(on), mobility, manning_n, eddy_m2_s)
 
     def set_surface_diffusion(self, m2_s):
-        lib().oracle_core_set_surface_diffusion(self.h, m2_s)
+        self._L().oracle_core_set_surface_diffusion(self.h, m2_s)
 
     def set_river_reach(self, reach):
         """reach: dict(along_z, positive, cross0, cross1, rows, inlet_eta, outlet_eta, inlet_speed_m_s) or None."""
         r = reach or {}
-        lib().oracle_core_set_river_reach(self.h, int(reach is not None), int(r.get("along_z", False)),
+        self._L().oracle_core_set_river_reach(self.h, int(reach is not None), int(r.get("along_z", False)),
                                           int(r.get("positive", True)), r.get("cross0", 0.0), r.get("cross1", 0.0),
                                           int(r.get("rows", 1)), r.get("inlet_eta", 0.0), r.get("outlet_eta", 0.0),
                                           r.get("inlet_speed_m_s", 0.0))
 
     def reach_bank_m3(self):
-        return lib().oracle_core_reach_bank(self.h)
+        return self._L().oracle_core_reach_bank(self.h)
 
     def set_wave_maker(self, wave):
         """wave: dict(x0, x1, z0, z1, dir_x, dir_z, amplitude_m_s, period_s, ramp_s) or None."""
         w = wave or {}
-        lib().oracle_core_set_wave_maker(self.h, int(wave is not None), w.get("x0", 0.0), w.get("x1", 0.0),
+        self._L().oracle_core_set_wave_maker(self.h, int(wave is not None), w.get("x0", 0.0), w.get("x1", 0.0),
                                          w.get("z0", 0.0), w.get("z1", 0.0), w.get("dir_x", 0.0), w.get("dir_z", 0.0),
                                          w.get("amplitude_m_s", 0.0), w.get("period_s", 0.0), w.get("ramp_s", 0.0))
 
     def recenter(self, cx, cz):
-        lib().oracle_core_recenter(self.h, cx, cz)
+        self._L().oracle_core_recenter(self.h, cx, cz)
 
     def origin(self):
-        o = np.zeros(2, np.float32)
-        lib().oracle_core_origin(self.h, _ptr(o))
+        o = np.zeros(2, self._np)
+        self._L().oracle_core_origin(self.h, _ptr(o))
         return float(o[0]), float(o[1])
 
     def parked_count(self):
-        return lib().oracle_core_parked_count(self.h)
+        return self._L().oracle_core_parked_count(self.h)
 
     def near_tiles(self):
-        return lib().oracle_core_near_tiles(self.h)
+        return self._L().oracle_core_near_tiles(self.h)
 
     def spray_m3(self):
-        return lib().oracle_core_spray_m3(self.h)
+        return self._L().oracle_core_spray_m3(self.h)
 
     def non_finite_count(self):
-        return lib().oracle_core_non_finite(self.h)
+        return self._L().oracle_core_non_finite(self.h)
 
     def sample(self, x, z):
-        o = np.zeros(7, np.float32)
-        lib().oracle_core_sample(self.h, x, z, _ptr(o))
+        o = np.zeros(7, self._np)
+        self._L().oracle_core_sample(self.h, x, z, _ptr(o))
         return dict(water_m=float(o[0]), slurry_m=float(o[1]), u=float(o[2]), v=float(o[3]),
                     moisture=float(o[5]), bed_m=float(o[6]))
 
     def fine_water_debug(self, tires, patch=0):
-        arr = (Tire * len(tires))()
+        arr = (self._Tire * len(tires))()
         for k, t in enumerate(tires):
-            arr[k] = Tire(t["x"], t["z"], t.get("forward_x", 0.0), t.get("forward_z", 1.0), t["radius"],
+            arr[k] = self._Tire(t["x"], t["z"], t.get("forward_x", 0.0), t.get("forward_z", 1.0), t["radius"],
                           t["width"], t["speed"], t.get("slip", 0.0))
-        out = np.zeros(self.fine_res * self.fine_res, np.float32)
-        org = np.zeros(2, np.float32)
-        lib().oracle_core_fine_water_debug(self.h, arr, len(tires), patch, _ptr(out), _ptr(org))
+        out = np.zeros(self.fine_res * self.fine_res, self._np)
+        org = np.zeros(2, self._np)
+        self._L().oracle_core_fine_water_debug(self.h, arr, len(tires), patch, _ptr(out), _ptr(org))
         return out, org
 
     SOLID_KEYS = ("x", "z", "yaw", "half_length", "half_width", "bottom_y", "top_y", "contact", "radius", "width")
@@ -332,26 +383,36 @@ class Core:
     def set_hydro_solids(self, solids):
         """solids: dicts with the HydroSolid fields (src/fluid_core.rs:219-240)."""
         packed = np.array([[float(sd.get(k, 0.0)) for k in self.SOLID_KEYS] for sd in solids] or [[0.0] * 10],
-                          np.float32)
-        lib().oracle_core_set_hydro_solids(self.h, _ptr(packed), len(solids))
+                          self._np)
+        self._L().oracle_core_set_hydro_solids(self.h, _ptr(packed), len(solids))
 
     LOAD_KEYS = ("force_x", "force_z", "buoyancy_n", "hull_buoyancy_n", "wheel_buoyancy_n", "displaced_m3",
                  "eroded_m3", "hole_m", "wheel_blocks", "belly_blocks")
 
     def lay_slurry_on_water(self, depth, grain):
-        return lib().oracle_core_lay_slurry_on_water(self.h, depth, grain)
+        return self._L().oracle_core_lay_slurry_on_water(self.h, depth, grain)
 
     def hydro_load(self):
-        o = np.zeros(10, np.float32)
-        lib().oracle_core_hydro_load(self.h, _ptr(o))
+        o = np.zeros(10, self._np)
+        self._L().oracle_core_hydro_load(self.h, _ptr(o))
         d = {k: float(v) for k, v in zip(self.LOAD_KEYS, o)}
         d["wheel_blocks"], d["belly_blocks"] = int(o[8]), int(o[9])
         return d
 
     def solid_mask(self):
         out = np.zeros(self.res * self.res, np.uint8)
-        lib().oracle_core_solid_mask(self.h, _ptr(out))
+        self._L().oracle_core_solid_mask(self.h, _ptr(out))
         return out
 
     def set_inflow(self, j, x0, x1, rate_m3_s):
-        lib().oracle_core_inflow(self.h, j, x0, x1, rate_m3_s)
+        self._L().oracle_core_inflow(self.h, j, x0, x1, rate_m3_s)
+
+
+class Core64(Core):
+    """The same FluidCore subset computed in FP64 throughout (liboracle_silt_f64):
+    the nested-sheet oracle that the learned closure's flux and depth errors
+    are stated against. Fields come back as float64."""
+
+    _L = staticmethod(lib64)
+    _np = np.float64
+    _Cfg, _Tire, _Spray = CoreCfg64, Tire64, Spray64

@@ -4,16 +4,41 @@
 // product never links this file.
 //
 // Build: g++ -O2 -ffp-contract=off -fno-fast-math (see oracle/Makefile).
-#include "sheet_oracle.h"
-
+//
+// With -DORACLE_F64 the same source builds the FP64 restatement (the nested-
+// sheet oracle the learned closure is judged against): every float of the
+// step, the interface included, becomes a double and each single-precision
+// libm call its double form. The model's constants keep their float values
+// (the `f` literals), so only the arithmetic's precision changes.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <thread>
 #include <tuple>
 #include <utility>
 #include <vector>
+
+#ifdef ORACLE_F64
+#define float double
+#define expf exp
+#define powf pow
+#define sqrtf sqrt
+#define hypotf hypot
+#define floorf floor
+#define ceilf ceil
+#define fabsf fabs
+#define fminf fmin
+#define fmaxf fmax
+#define acosf acos
+#define cosf cos
+#define sinf sin
+#define finite oracle_finite  // glibc declares finite(double)
+#endif
+
+#include "sheet_oracle.h"
 
 namespace {
 
@@ -57,9 +82,10 @@ inline usize f2usize(float x) {  // `as usize`, saturating, NaN -> 0
     if (x >= 1.8e19f) return (usize)-1;
     return (usize)x;
 }
-inline uint32_t fbits(float x) {
-    uint32_t b;
-    memcpy(&b, &x, 4);
+// The bit pattern of a value (memo keys compare values bit for bit).
+inline uint64_t fbits(float x) {
+    uint64_t b = 0;
+    memcpy(&b, &x, sizeof x);
     return b;
 }
 // Iterator::sum for f32 folds from -0.0 in the reference toolchain.
@@ -862,7 +888,7 @@ void substep(float* h, float* u, float* v, const float* bed, const float* nu, co
                 sc.d[idx] = 0.62f * sc.c[idx] + 0.38f * sc.a[idx];
             }
     }
-    uint32_t memo_nu = 0x7fc00000u;  // f32::NAN bits
+    uint64_t memo_nu = fbits(std::numeric_limits<float>::quiet_NaN());  // f32::NAN
     float memo_decay = 1.0f;
     for (usize j = j0; j <= j1; ++j)
         for (usize i = i0; i <= i1; ++i) {

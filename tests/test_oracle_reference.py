@@ -5,6 +5,8 @@ is the reference test's assertion, with its seeds, sizes and tolerances
 (src/fluid_core.rs:11126-11817, src/fluid_core/near.rs:349-447,
 tests/near_field.rs). No GPU is needed.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -297,3 +299,27 @@ def test_soften_border_keeps_interior():
     t = F(1) / F(edge)
     assert u2[1, 100] == t * t * (F(3) - F(2) * t)
     assert u2[edge, edge] == 1.0
+
+
+def test_native_build_gives_the_portable_builds_bits(tmp_path):
+    """The timed CPU baseline loads the oracle built -O3 -march=native (still
+    without contraction); it must step the reference's window to the same
+    bits as the portable -O2 build the parity tests use."""
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    prog = (
+        "import sys, numpy as np\n"
+        f"sys.path[:0] = [{os.path.join(root, 'oracle')!r}, {os.path.join(root, 'dirty-gen_b200')!r}]\n"
+        "import oracle, silt_scenes as S\n"
+        "if sys.argv[1] == 'native': assert oracle.use_native_build().startswith('-O3')\n"
+        "sc = S.window200(); c = oracle.Core(); S.seed_core(c, sc)\n"
+        "for _ in range(20): c.step(1 / 120)\n"
+        "np.save(sys.argv[2], np.stack([c.get(n) for n in ('water', 'slurry', 'uw', 'vw', 'us', 'vs')]))\n")
+    outs = []
+    for kind in ("native", "port"):
+        path = str(tmp_path / f"{kind}.npy")
+        subprocess.run([sys.executable, "-c", prog, kind, path], check=True, timeout=600)
+        outs.append(np.load(path))
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
