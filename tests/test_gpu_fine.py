@@ -193,8 +193,10 @@ def test_ledger_closes_in_fp64_with_tires_and_inflow(engine):
 
 
 def test_grid_engine_tracks_window_engine_with_tires():
-    """The two coarse engines on the same tire drive: they differ only in the
-    confinement form (snapshot vs raster sweep), so depths stay close."""
+    """The two coarse engines on the same tire drive: both step the
+    reference's pair with its Gauss-Seidel confinement (the window engine box
+    by box, the grid engine as a fixed point over tiles), so their depths
+    agree to the pass criterion."""
     dt = 1.0 / 120.0
     scene = S.grid(res=256)
     out = []
@@ -207,5 +209,5 @@ def test_grid_engine_tracks_window_engine_with_tires():
                 dev.push_tire(**t)
             dev.step(dt, want_spray=False)
         out.append((dev.get("water"), dev.get("slurry")))
-    assert np.abs(out[0][0] - out[1][0]).max() < 5e-3
-    assert np.abs(out[0][1] - out[1][1]).max() < 5e-3
+    assert np.abs(out[0][0] - out[1][0]).max() <= TOL_H
+    assert np.abs(out[0][1] - out[1][1]).max() <= TOL_H

@@ -2,13 +2,13 @@
 
 Tolerance (from the build's pass criteria): max |dh| <= 1e-4 m per layer after
 100 steps. The window engine (windows up to 512 cells) steps box by box with
-the reference's Gauss-Seidel confinement. The water layer's damping factor
+the reference's Gauss-Seidel confinement, and the grid engine (any size)
+solves the same sweep as a fixed point. The water layer's damping factor
 is computed on the host with the reference's libm; the slurry's powf and expf
 are the double-precision functions rounded once, which agree with the C
 library's on all but a few inputs in 10^4, so on these scenes both layers
-match bit for bit. The grid engine (large grids) confines from a snapshot,
-the reference's free-operator form, which moves config-1 depths by under
-1e-6 m.
+match bit for bit. The grid engine's snapshot form (the reference's
+free-operator confinement) stays selectable.
 """
 import numpy as np
 import pytest
@@ -85,15 +85,16 @@ def test_window200_ledger_matches_oracle_in_fp64():
 
 
 def test_grid_engine_water_is_bit_exact_on_a_jacobi_sized_box():
-    """The grid engine on a pond wider than 48 x 32 cells, against the oracle's
-    pair with the free operator's threading: the reference then confines from
-    a snapshot too (force_gravity_par, src/fluid_core.rs:2229-2231) and the
+    """The grid engine's snapshot form (SILT_CONFINE_SNAPSHOT) on a pond wider
+    than 48 x 32 cells, against the oracle's pair with the free operator's
+    threading: the reference then confines from a snapshot too (force_gravity_par, src/fluid_core.rs:2229-2231) and the
     water damping factor is computed on the host with the reference's libm, so
     every operation is the reference's own IEEE sequence and the depths must
     match bit for bit."""
     scene = S.window200()
     ref = O.Core(inner_par=True)
     dev = G.Sheet(engine=G.ENGINE_GRID)
+    dev.set_confinement(G.CONFINE_SNAPSHOT)
     for core in (ref, dev):
         core.map_water_bed(scene["bed"], np.zeros_like(scene["water"]))
         core.pour_water(-7.0, 7.0, -7.0, 7.0, 0.06)
@@ -115,7 +116,7 @@ def test_grid_engine_device_substep_count_is_exact():
     engine (which has no box edge) differs there by float rounding (~3e-8 m);
     a wrong substep count would move the pond's rim by ~1e-3 m."""
     scene = S.window200()
-    ref = O.Core(inner_par=True)
+    ref = O.Core()
     dev = G.Sheet(engine=G.ENGINE_GRID)
     dev.set_step_timing(True)
     n = scene["water"].size
@@ -178,7 +179,7 @@ def test_open_water_and_surface_diffusion_match_oracle(engine):
     dev = G.Sheet(res=sc["res"], cell=sc["cell"], engine=engine)
     # The grid engine confines from a snapshot: the oracle's pair with the
     # free operator's form does too on boxes of at least 48 x 32 (the basin's).
-    ref = O.Core(threads=1, inner_par=engine == G.ENGINE_GRID)
+    ref = O.Core(threads=1)
     for c in (dev, ref):
         S.seed_basin(c, sc)
         c.set_open_water(True, 1.0, 0.035, 0.06)
@@ -258,7 +259,7 @@ def test_patch_water_outside_the_window_is_parked_and_restored(engine):
     window; the reference keeps them by world cell)."""
     scene = S.grid(res=128, seed=0xABC, puddles=6)
     ox = S.snap_origin(0.0, 0.0, 128 * 0.2, 0.2)[0]
-    ref = O.Core(res=128, fine_res=64, layout=1, inner_par=engine == G.ENGINE_GRID, threads=1)
+    ref = O.Core(res=128, fine_res=64, layout=1, threads=1)
     dev = G.Sheet(res=128, fine_res=64, layout=G.FINE_PER_TIRE, engine=engine)
     for c in (ref, dev):
         S.seed_core(c, scene)
@@ -297,7 +298,7 @@ def test_river_reach_and_wave_maker_match_oracle(engine):
                  inlet_speed_m_s=0.75)
     wave = dict(x0=5.0, x1=7.0, z0=-3.0, z1=3.0, dir_x=1.0, dir_z=0.0, amplitude_m_s=0.3, period_s=0.5, ramp_s=0.2)
     dev = G.Sheet(res=sc["res"], cell=sc["cell"], engine=engine)
-    ref = O.Core(threads=1, inner_par=engine == G.ENGINE_GRID)
+    ref = O.Core(threads=1)
     for c in (dev, ref):
         S.seed_basin(c, sc)
         c.set_open_water(True, 1.0, 0.035, 0.06)
