@@ -334,13 +334,16 @@ def run_b200(args):
     prev = sheet.ledger()
     f0.record(stream)
     nev = 0
-    gaps = []  # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
+    gaps = []   # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
+    rgaps = []  # the same with the transport rounding book taken off
     for _ in range(e2e_steps):
         ev = one_step(True)
         nev += len(ev)
         led = sheet.ledger()
         kept = led["total_m3"] + led["cut_m3"] - led["opened_m3"]
-        gaps.append(abs(kept - (prev["total_m3"] + prev["cut_m3"] - prev["opened_m3"])) / led["total_m3"])
+        kept0 = prev["total_m3"] + prev["cut_m3"] - prev["opened_m3"]
+        gaps.append(abs(kept - kept0) / led["total_m3"])
+        rgaps.append(abs((kept - led["round_m3"]) - (kept0 - prev["round_m3"])) / led["total_m3"])
         prev = led
     f1.record(stream)
     torch.cuda.synchronize()
@@ -387,7 +390,11 @@ def run_b200(args):
                 "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
                            "spray_m3": led["spray_m3"], "cut_m3": led["cut_m3"],
                            "gap_max_per_step": max(gaps), "gap_median_per_step": statistics.median(gaps),
-                           "gap_steps": len(gaps), "gap_target": 1e-9}}
+                           "gap_steps": len(gaps), "gap_target": 1e-9, "round_m3": led["round_m3"],
+                           "gap_max_per_step_after_rounding_book": max(rgaps),
+                           "gap_what": "per step |(total + cut - opened) now - before| / total; the f32 transport "
+                                       "updates' own rounding is booked in FP64 (round_m3) and taken off in the "
+                                       "second figure"}}
         if not args.no_batch_roofline and world == 1:
             sheet.sync()
             line["roofline_batch"] = batch_roofline(args, local, peak, peak_kind)
@@ -919,6 +926,86 @@ def closure_cpu(scenes, T, max_steps, budget_s):
                       f"{steps} steps after 1 warm-up, one window at a time, each pair on 2 threads ({el:.2f} s)"}
 
 
+def closure_fp64_judge(scenes, T, C, net, zero, forms, steps, every=16, probe_every=5):
+    """The closure judged against the FP64 nested-sheet oracle (oracle.Core64:
+    the same restated step in double, per-tire 64 x 64 2 cm sheets) on every
+    `every`-th window:
+
+    * depth error: relative L2 of both layers' depth after `steps` steps, of
+      the closure run and of the f32 GPU nested run, against the FP64 run;
+    * flux error: every `probe_every` steps the FP64 state is loaded into two
+      GPU windows, one stepped with the closure and one with a zero network
+      (the closure's coarse step alone); the correction the closure's face
+      transfers make (closure minus uncorrected depth change) is compared with
+      the correction the FP64 nested sheets make (FP64 nested minus uncorrected
+      depth change) over the window, as a relative L2."""
+    import numpy as np
+    import torch
+
+    import silt_b200
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import silt_scenes
+
+    picked = list(range(0, len(scenes), every))
+    names = ("water", "slurry", "uw", "vw", "us", "vs")
+    num = {"closure": 0.0, "nested_f32": 0.0}
+    den = 0.0
+    fnum = fden = 0.0
+    probes = 0
+    for w in picked:
+        sc = scenes[w]
+        ref = oracle.Core64(res=200, cell=CELL, fine_res=FINE_RES, fine_cell=0.02, layout=1, threads=2)
+        silt_scenes.seed_core(ref, sc)
+        pair = []
+        for nn in (net, zero):
+            sh = silt_b200.Sheet(res=200, cell=CELL, fine_res=FINE_RES, fine_cell=0.02,
+                                 layout=silt_b200.FINE_PER_TIRE, engine=silt_b200.ENGINE_GRID)
+            silt_scenes.seed_core(sh, sc)
+            C.set_coupling(sh, C.COUPLING_CLOSURE, nn, 1e30)
+            pair.append(sh)
+        for k in range(1, steps + 1):
+            tires = T.scene_tires(sc, k)
+            if (k - 1) % probe_every == 0:
+                before = {n: ref.get(n) for n in names}
+                for sh in pair:
+                    for n in names:
+                        sh.set(n, before[n].astype(np.float32))
+                    for t in tires:
+                        sh.push_tire(**t)
+                    sh.step(DT, want_spray=False)
+            for t in tires:
+                ref.push_tire(**t)
+            ref.step(DT)
+            if (k - 1) % probe_every == 0:
+                for layer in ("water", "slurry"):
+                    h0 = before[layer]
+                    d_ref = ref.get(layer) - h0
+                    d_cl = pair[0].get(layer).astype(np.float64) - h0
+                    d_un = pair[1].get(layer).astype(np.float64) - h0
+                    target, pred = d_ref - d_un, d_cl - d_un
+                    fnum += float(((pred - target) ** 2).sum())
+                    fden += float((target ** 2).sum())
+                probes += 1
+        for layer in ("water", "slurry"):
+            y = ref.get(layer)
+            den += float((y ** 2).sum())
+            for name, key in (("closure", "closure"), ("nested", "nested_f32")):
+                x = forms[name][0][w].get(layer).astype(np.float64)
+                num[key] += float(((x - y) ** 2).sum())
+        for sh in pair:
+            sh.close()
+    torch.cuda.synchronize()
+    return {"oracle": "FP64 restatement of the step (oracle.Core64), nested per-tire 64^2 2 cm sheets",
+            "windows": len(picked), "steps": steps,
+            "depth_rel_l2_closure": math.sqrt(num["closure"] / den),
+            "depth_rel_l2_nested_f32": math.sqrt(num["nested_f32"] / den),
+            "flux_correction_rel_l2": math.sqrt(fnum / fden) if fden > 0 else None,
+            "flux_probes": probes,
+            "flux_what": "closure's depth correction (its face transfers) against the FP64 nested sheets' "
+                         "correction of the same coarse step, one step from the FP64 state"}
+
+
 def run_closure_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -1103,6 +1190,8 @@ def run_closure(args):
             "closure_steps": n_closure, "fallback_steps": n_fallback,
             "steps_compared": warm + args.steps,
             "gpu_launches": int(pc["launches"]), "clocks": summarise_clocks(clock_lines)}
+    assert step_of["closure"] == step_of["nested"]
+    line["vs_fp64_nested"] = closure_fp64_judge(scenes, T, C, net, zero, forms, step_of["closure"])
     if not args.no_baseline:
         line["cpu_baseline"] = closure_cpu(scenes, T, 40, 20.0)
     print(json.dumps(line), flush=True)

@@ -99,9 +99,9 @@ __device__ __forceinline__ void bar_init(uint64_t* bar, uint32_t count) {
 
 // Waits for the barrier phase with a bounded number of polls; false if it
 // never completed.
-__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, int limit = WAIT_LIMIT) {
     uint32_t done = 0;
-    for (int k = 0; k < WAIT_LIMIT && !done; ++k)
+    for (int k = 0; k < limit && !done; ++k)
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
@@ -523,6 +523,19 @@ __global__ void k_pack(const float* w, uint16_t* fwd, uint16_t* bwd, int cin, in
     }
 }
 
+// The bounded wait on a barrier phase that never completes (nothing arrives
+// on it): every thread gives up after `polls` polls and the error slot is
+// set, as a convolution's wait would set it. Nothing is in flight and no
+// tensor memory is held, so the kernel ends and the context stays usable.
+__global__ void k_wait_probe(int* err, int polls) {
+    ::silt::dep_wait();
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) bar_init(&bar, 1);
+    __syncthreads();
+    const bool ok = bar_wait(&bar, 0, polls);
+    if (!ok && threadIdx.x == 0 && err) atomicExch(err, 1);
+}
+
 template <class K>
 cudaError_t set_smem(K kernel, int bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -676,6 +689,28 @@ int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32
     ::silt::launch_dep(k_adam, dim3((n + 255) / 256), dim3(256), 0, (cudaStream_t)stream, param, m, v, grad, n, lr, beta1, beta2, eps, c1, c2);
     ::silt::count_launch();
     return cuda_rc(cudaGetLastError(), "closure_adam");
+}
+
+int silt_closure_wait_status(int32_t* gave_up, void* stream) {
+    if (!gave_up) return fail(SILT_EINVAL, "invalid argument: closure_wait_status");
+    int* d = err_slot();
+    if (!d) return fail(SILT_ECUDA, "closure_wait_status: no error slot");
+    int flag = 0;
+    const cudaStream_t st = (cudaStream_t)stream;
+    int rc = cuda_rc(cudaMemcpyAsync(&flag, d, sizeof(int), cudaMemcpyDeviceToHost, st), "closure_wait_status");
+    if (rc == SILT_OK) rc = cuda_rc(cudaMemsetAsync(d, 0, sizeof(int), st), "closure_wait_status");
+    if (rc == SILT_OK) rc = cuda_rc(cudaStreamSynchronize(st), "closure_wait_status");
+    *gave_up = flag;
+    return rc;
+}
+
+int silt_closure_wait_probe(int32_t polls, void* stream) {
+    if (polls < 1 || polls > (1 << 20)) return fail(SILT_EINVAL, "invalid argument: closure_wait_probe polls");
+    int* d = err_slot();
+    if (!d) return fail(SILT_ECUDA, "closure_wait_probe: no error slot");
+    ::silt::launch_dep(k_wait_probe, dim3(1), dim3(32), 0, (cudaStream_t)stream, d, (int)polls);
+    ::silt::count_launch();
+    return cuda_rc(cudaGetLastError(), "closure_wait_probe");
 }
 
 int silt_closure_pack(const float* w, void* w_fwd, void* w_bwd, int32_t cin, int32_t cout, void* stream) {

@@ -141,7 +141,8 @@ struct Impl {
     // Spray.
     SprayRec* spray = nullptr;
     double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3, [3] dry cut m3,
-                                      // [4] river reach bank m3 (FP64 twin of the reference's f32 bank)
+                                      // [4] river reach bank m3 (FP64 twin of the reference's f32 bank),
+                                      // [5] eroded bed m3, [6] transport rounding m3
     double* h_books = nullptr;
     int* h_counters = nullptr;
 };
@@ -1279,6 +1280,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
                 J.div = P.fdivs;
                 J.solid = P.n_solids > 0 ? S->solid : nullptr;
                 J.cut = M.d_books + 3;
+                J.round = M.d_books + 6;
                 J.cut_area = (double)P.fcell * (double)P.fcell;
                 J.dt = dt;
                 J.vort = l == 0 ? 0.08f : 0.05f;
@@ -1534,10 +1536,10 @@ int move_window(Patches& P, silt_sheet* s, int di, int dj, bool scroll) {
 }
 
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut,
-                 double* reach, double* eroded) {
+                 double* reach, double* eroded, double* round) {
     Impl& M = I(P);
     SheetView W = view_of(s);
-    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 6 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 7 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
     FCK(cudaStreamSynchronize(W.st));
     *spray = M.h_books[0];
     *park_w = M.h_books[1];
@@ -1545,6 +1547,7 @@ int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, doubl
     if (cut) *cut = M.h_books[3];
     if (reach) *reach = M.h_books[4];
     if (eroded) *eroded = M.h_books[5];
+    if (round) *round = M.h_books[6];
     return SILT_OK;
 }
 

@@ -861,7 +861,11 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         FR[TIDX(e, gy)] = dh;
     });
     __syncthreads();
-    // Depth after the x pass on rows [ry0, ry1), tile columns.
+    // Depth after the x pass on rows [ry0, ry1), tile columns. The rounding
+    // book takes, for the tile's own cells, each cell's f32 change less the
+    // exact (FP64) sum of the fluxes across its faces.
+    double rnd = 0.0;
+    const bool book_round = P.round != nullptr;
     trows<EDGE, TT, TT + 3>(tx0, tx1, ry0, ry1, [&](int c, int gy) {
         float flm = c - 1 >= 0 ? FL[TIDX(c - 1, gy)] : 0.0f;
         float frm = c - 1 >= 0 ? FR[TIDX(c - 1, gy)] : 0.0f;
@@ -871,7 +875,10 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         float add = (0.0f + frm) + flc;
         float hv = HSm[TIDX(c, gy)];
         float moved = fmaxf(hv - rem + add, 0.0f);
-        HX[TIDX(c, gy)] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        const float hx = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        HX[TIDX(c, gy)] = hx;
+        if (book_round && gy >= ty0 && gy < ty1)
+            rnd += ((double)hx - (double)hv) - (((double)frm + (double)flc) - ((double)flm + (double)frc));
     });
     __syncthreads();
     // z pass. Pair r joins rows r and r+1 and exists for 0 <= r < res-1.
@@ -912,6 +919,8 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
         float hv = HX[TIDX(c, r)];
         float moved = fmaxf(hv - rem + add, 0.0f);
         float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        if (book_round)
+            rnd += ((double)hn - (double)hv) - (((double)dnm + (double)upc) - ((double)upm + (double)dnc));
         if (P.eps > 0.0f && hn < P.eps) {
             if (hn > 0.0f) cut += (double)hn;  // booked: the dry cut's volume
             hn = 0.0f;
@@ -921,6 +930,10 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
     });
     for (int o = 16; o > 0; o >>= 1) cut += __shfl_down_sync(0xffffffffu, cut, o);
     if ((threadIdx.x & 31) == 0 && cut > 0.0 && P.cut) atomicAdd(P.cut, cut * P.cut_area);
+    if (book_round) {
+        for (int o = 16; o > 0; o >>= 1) rnd += __shfl_down_sync(0xffffffffu, rnd, o);
+        if ((threadIdx.x & 31) == 0 && rnd != 0.0) atomicAdd(P.round, rnd * P.cut_area);
+    }
 #undef TIDX
     // Block sum of the depth (FP64), one atomic per tile; the tile's flags.
     const int any = __syncthreads_or(part > 0.0);

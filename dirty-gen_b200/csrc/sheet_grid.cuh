@@ -109,7 +109,9 @@ struct TransportParams {
     const float* bank_bed;    // nullptr = no dry-bank test (banks off)
     double* ledger;           // FP64 sum of the new depth, may be nullptr
     double* cut;              // FP64 volume the dry cut removed, m^3 (accumulated), may be nullptr
-    double cut_area;          // m^2 of one cell for that book
+    double cut_area;          // m^2 of one cell for the cut and rounding books
+    double* round;            // FP64 rounding book, m^3 (accumulated), may be nullptr: each updated
+                              // cell's f32 change minus the exact sum of its face fluxes
     int32_t res;
     float cell, dt, eps;
     FixedDiv div_cell;        // cell (the face fraction speed dt / cell)

@@ -385,13 +385,14 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
     ::silt::dep_wait();
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n) return;
-    out[7 * w + 0] = acc[w][0];
-    out[7 * w + 1] = acc[w][1];
-    out[7 * w + 2] = books[w][0];
-    out[7 * w + 3] = books[w][1];
-    out[7 * w + 4] = books[w][2];
-    out[7 * w + 5] = books[w][3];
-    out[7 * w + 6] = books[w][4];
+    out[8 * w + 0] = acc[w][0];
+    out[8 * w + 1] = acc[w][1];
+    out[8 * w + 2] = books[w][0];
+    out[8 * w + 3] = books[w][1];
+    out[8 * w + 4] = books[w][2];
+    out[8 * w + 5] = books[w][3];
+    out[8 * w + 6] = books[w][4];
+    out[8 * w + 7] = books[w][6];
 }
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st) {

@@ -28,7 +28,8 @@ cudaError_t op_export(const float* bed, const float* water, const float* slurry,
                       const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
                       float* moisture, size_t n, cudaStream_t st);
 cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st);
-// out[7 w + 0..1] = acc[w][0..1] (depth sums), out[7 w + 2..6] = books[w][0..4].
+// out[8 w + 0..1] = acc[w][0..1] (depth sums), out[8 w + 2..6] = books[w][0..4],
+// out[8 w + 7] = books[w][6] (the transport rounding book).
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st);
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st);

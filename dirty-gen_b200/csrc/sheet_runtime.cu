@@ -319,6 +319,7 @@ void coarse_substep(silt_sheet* s, const CoarsePlan& cp, float dt, int k, silt::
         Q.bank_bed = nullptr;
         Q.ledger = s->d_acc + l;
         Q.cut = silt::fine::books(s->fine) + 3;
+        Q.round = silt::fine::books(s->fine) + 6;
         Q.cut_area = (double)cell * (double)cell;
         Q.res = res;
         Q.cell = cell;
@@ -419,6 +420,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         silt::window::attach_scratch(J, s->win_planes + (size_t)l * silt::window::SCRATCH_PLANES * s->n, s->n);
         J.ledger = s->d_acc + l;
         J.cut = silt::fine::books(s->fine) + 3;
+        J.round = silt::fine::books(s->fine) + 6;
         J.cut_area = (double)s->cfg.cell * (double)s->cfg.cell;
         J.res = s->res;
         J.cell = s->cfg.cell;
@@ -1517,8 +1519,8 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded);
+    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0, rounding = 0.0;
+    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded, &rounding);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -1535,6 +1537,7 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->total_m3 = w + sl + park_w + park_s + spray + reach;
     out->cut_m3 = cut;
     out->reach_m3 = reach;
+    out->round_m3 = rounding;
     return SILT_OK;
 }
 
@@ -1891,7 +1894,7 @@ struct silt_batch {
     silt::closure::Runner* clos = nullptr;
     // Ledger gather: per window the depth sums and the books, one copy back.
     const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
-    double* d_ledgers = nullptr;            // 7 doubles per window
+    double* d_ledgers = nullptr;            // 8 doubles per window
     double* h_ledgers = nullptr;            // pinned
 };
 
@@ -2100,8 +2103,8 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->count, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemsetAsync(b->count, 0, 2 * sizeof(int), b->st);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 7 * (size_t)n * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 7 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 8 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 8 * (size_t)n * sizeof(double));
     if (e == cudaSuccess) {
         std::vector<const double*> src(2 * (size_t)n);
         for (int w = 0; w < n; ++w) {
@@ -2256,7 +2259,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         return SILT_OK;
     }
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
-    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 7 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 8 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)
         CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
@@ -2264,7 +2267,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         silt_sheet* s = b->sheets[w];
         int rc = check_substep_overflow(s);
         if (rc) return rc;
-        const double* g = b->h_ledgers + 7 * (size_t)w;
+        const double* g = b->h_ledgers + 8 * (size_t)w;
         const double area = (double)s->cfg.cell * (double)s->cfg.cell;
         silt_ledger& L = out[w];
         L.water_m3 = g[0] * area;
@@ -2276,6 +2279,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         L.reach_m3 = g[6];
         L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3 + L.reach_m3;
         L.cut_m3 = g[5];
+        L.round_m3 = g[7];
     }
     return SILT_OK;
 }

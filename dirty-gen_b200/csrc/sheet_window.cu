@@ -51,6 +51,7 @@ struct Shared {
     int row_count[MAX_RES];
     int nbox;
     int changed;
+    int chg[3];      // Gauss-Seidel pass verdicts, rotating (pass k uses chg[k % 3])
     float red_f[NT / 32];
     double red_d[NT / 32];
     double crew_d;   // this CTA's share of a crew-wide sum or maximum, read by the crew
@@ -208,13 +209,49 @@ __device__ __forceinline__ float tap5c(const float* line, int res, int i, float 
     return a;
 }
 
-// blur_box (src/fluid_core.rs:3541-3569): x pass of the box rows into tmp,
-// then the z pass into dst, which reads tmp rows outside the box as they are.
-__device__ void cta_blur(const float* __restrict__ src, float* __restrict__ dst, float* __restrict__ tmp, int res,
-                         const Box& b, float k0, float k1, float k2) {
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1, { tmp[g] = tap5c(src + j * res, res, i, k0, k1, k2, 1); })
+// tap5c down column i where rows [lo, hi] come from `in_box` and the other
+// rows from `outside`.
+__device__ __forceinline__ float tap5c_pick(const float* in_box, const float* outside, int lo, int hi, int res, int i,
+                                            int j, float k0, float k1, float k2) {
+    const bool in = j >= 2 && j <= res - 3;
+    const int r0 = j < 2 ? 0 : j - 2, r1 = j < 1 ? 0 : j - 1;
+    const int r3 = j + 1 > res - 1 ? res - 1 : j + 1, r4 = j + 2 > res - 1 ? res - 1 : j + 2;
+    auto at = [&](int r) { return (r >= lo && r <= hi ? in_box : outside)[r * res + i]; };
+    float a0 = at(r0), a1 = at(r1), a2 = at(j), a3 = at(r3), a4 = at(r4);
+    float a = in ? a0 * k0 : 0.0f + a0 * k0;
+    a += a1 * k1;
+    a += a2 * k2;
+    a += a3 * k1;
+    a += a4 * k0;
+    return a;
+}
+
+// The reference's two blurs of one source in a row, blur_box with GAUSS into
+// dst_g and then with STEEP into dst_s, both through the scratch `tmp`
+// (src/fluid_core.rs:3541-3569), in two crew phases instead of four. The x
+// passes of the box rows go to tmp_g (GAUSS, a transient plane) and tmp
+// (STEEP, where the reference's second blur leaves it). Each z pass reads box
+// rows from its own x pass and the rows outside the box from tmp as they are:
+// the reference's x passes write only the box, so both of its z passes see
+// the same stale rows there. `combine(g, gauss, steep)` runs on each box cell
+// in the z phase.
+template <class Comb>
+__device__ void cta_blur_pair(const float* __restrict__ src, float* __restrict__ dst_g, float* __restrict__ dst_s,
+                              float* __restrict__ tmp, float* __restrict__ tmp_g, int res, const Box& b,
+                              Comb combine) {
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        const float* line = src + j * res;
+        tmp_g[g] = tap5c(line, res, i, kG0, kG1, kG2, 1);
+        tmp[g] = tap5c(line, res, i, kS0, kS1, kS2, 1);
+    })
     crew_sync();
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1, { dst[g] = tap5c(tmp + i, res, j, k0, k1, k2, res); })
+    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
+        const float gv = tap5c_pick(tmp_g, tmp, b.j0, b.j1, res, i, j, kG0, kG1, kG2);
+        const float sv = tap5c(tmp + i, res, j, kS0, kS1, kS2, res);
+        dst_g[g] = gv;
+        dst_s[g] = sv;
+        combine(g, gv, sv);
+    })
     crew_sync();
 }
 
@@ -243,68 +280,86 @@ __device__ __forceinline__ float job_decay(const Job& J, int g, float dt, float 
 // :4178-4223): an edge touching a wall moves nothing, and a dry bank above the
 // donor's surface takes nothing (banks on the layer's bed).
 __device__ void cta_transport(const Job& J, const Box& b, float dt) {
-    // The planes are distinct and each phase writes only its own cell, so
-    // the loads of one cell may run ahead of the stores of the previous.
+    // Two crew phases. Each cell recomputes the fluxes of the edges it needs
+    // (its own two and, for the donor's room, the left flux one edge further)
+    // from the depths before the pass, exactly as the reference's flux
+    // buffers hold them, so no flux plane and no barrier sits between the
+    // fluxes and the update. The x pass writes its depths to f1; the z pass
+    // reads them there and writes h.
     const int res = J.res;
     float* __restrict__ h = J.h;
     const float* __restrict__ U = J.u;
     const float* __restrict__ V = J.v;
-    float* __restrict__ F1 = J.f1;
-    float* __restrict__ F2 = J.f2;
+    float* __restrict__ HX = J.f1;
     const FixedDiv cell = J.div.cell;
     const uint8_t* __restrict__ gate = J.gate;
     const uint8_t* __restrict__ W = J.solid;
     const float* __restrict__ bed = J.bed;
     const bool walled = W != nullptr;
-    // dh of the edge from donor d to receiver r, 0 across a wall.
-    auto edge = [&](int d, int r, float remd, float speed) {
-        const float dh = open_edge_dh(walled, h[d], h[r], remd, gate ? gate[r] : 1, walled ? bed[d] : 0.0f,
+    // The rounding book: each updated cell's f32 change less the exact
+    // (FP64) sum of the fluxes across its faces.
+    const bool book_round = J.round != nullptr;
+    double rnd = 0.0;
+    // dh of the edge from donor d to receiver r on depths hp, 0 across a wall.
+    auto edge = [&](const float* hp, int d, int r, float remd, float speed) {
+        const float dh = open_edge_dh(walled, hp[d], hp[r], remd, gate ? gate[r] : 1, walled ? bed[d] : 0.0f,
                                       walled ? bed[r] : 0.0f, speed, dt, cell, 0.45f);
         return walled && (W[d] | W[r]) ? 0.0f : dh;
     };
-    CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
-        float speed = 0.5f * (U[g] + U[g + 1]);
-        float dh = edge(g + 1, g, 0.0f, speed);
-        F1[g] = speed > 0.0f ? 0.0f : dh;
-    })
-    crew_sync();
-    CLU_RECT(b.i0, b.i1 - 1, b.j0, b.j1, {
-        float speed = 0.5f * (U[g] + U[g + 1]);
-        float prev = i > b.i0 ? F1[g - 1] : 0.0f;
-        float dh = edge(g, g + 1, 0.0f + prev, speed);
-        F2[g] = speed > 0.0f ? dh : 0.0f;
-    })
-    crew_sync();
+    // x pass. Edge e joins cells e and e+1 of the row, e in [i0, i1 - 1]: its
+    // left-going flux (donor e+1) when the face speed is not positive, else
+    // its right-going flux (donor e, after what e gave across edge e-1).
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
-        float flm = i > b.i0 ? F1[g - 1] : 0.0f, frm = i > b.i0 ? F2[g - 1] : 0.0f;
-        float flc = i < b.i1 ? F1[g] : 0.0f, frc = i < b.i1 ? F2[g] : 0.0f;
-        float rem = (0.0f + flm) + frc, add = (0.0f + frm) + flc;
-        float hv = h[g];
-        float moved = fmaxf(hv - rem + add, 0.0f);
-        h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        const int row = j * res;
+        auto speed = [&](int e) { return 0.5f * (U[row + e] + U[row + e + 1]); };
+        auto left = [&](int e) {
+            const float sp = speed(e);
+            const float dh = edge(h, row + e + 1, row + e, 0.0f, sp);
+            return sp > 0.0f ? 0.0f : dh;
+        };
+        auto right = [&](int e) {
+            const float sp = speed(e);
+            const float prev = e > b.i0 ? left(e - 1) : 0.0f;
+            const float dh = edge(h, row + e, row + e + 1, 0.0f + prev, sp);
+            return sp > 0.0f ? dh : 0.0f;
+        };
+        const float flm = i > b.i0 ? left(i - 1) : 0.0f, frm = i > b.i0 ? right(i - 1) : 0.0f;
+        const float flc = i < b.i1 ? left(i) : 0.0f, frc = i < b.i1 ? right(i) : 0.0f;
+        const float rem = (0.0f + flm) + frc, add = (0.0f + frm) + flc;
+        const float hv = h[g];
+        const float moved = fmaxf(hv - rem + add, 0.0f);
+        const float hx = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        HX[g] = hx;
+        if (book_round) rnd += ((double)hx - (double)hv) - (((double)frm + (double)flc) - ((double)flm + (double)frc));
     })
     crew_sync();
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
-        float speed = 0.5f * (V[g] + V[g + res]);
-        float dh = edge(g + res, g, 0.0f, speed);
-        F1[g] = speed > 0.0f ? 0.0f : dh;
-    })
-    crew_sync();
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1 - 1, {
-        float speed = 0.5f * (V[g] + V[g + res]);
-        float ra = j > b.j0 ? 0.0f + F1[g - res] : 0.0f;
-        float dh = edge(g, g + res, ra, speed);
-        F2[g] = speed > 0.0f ? dh : 0.0f;
-    })
-    crew_sync();
+    // z pass on the x pass's depths: row pair r joins rows r and r+1, r in [j0, j1 - 1].
     CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
-        float upm = j > b.j0 ? F1[g - res] : 0.0f, dnm = j > b.j0 ? F2[g - res] : 0.0f;
-        float upc = j < b.j1 ? F1[g] : 0.0f, dnc = j < b.j1 ? F2[g] : 0.0f;
-        float rem = (0.0f + upm) + dnc, add = (0.0f + dnm) + upc;
-        float hv = h[g];
-        float moved = fmaxf(hv - rem + add, 0.0f);
-        h[g] = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        auto speed = [&](int r) { return 0.5f * (V[r * res + i] + V[(r + 1) * res + i]); };
+        auto up = [&](int r) {
+            const float sp = speed(r);
+            const float dh = edge(HX, (r + 1) * res + i, r * res + i, 0.0f, sp);
+            return sp > 0.0f ? 0.0f : dh;
+        };
+        auto down = [&](int r) {
+            const float sp = speed(r);
+            const float ra = r > b.j0 ? 0.0f + up(r - 1) : 0.0f;
+            const float dh = edge(HX, r * res + i, (r + 1) * res + i, ra, sp);
+            return sp > 0.0f ? dh : 0.0f;
+        };
+        const float upm = j > b.j0 ? up(j - 1) : 0.0f, dnm = j > b.j0 ? down(j - 1) : 0.0f;
+        const float upc = j < b.j1 ? up(j) : 0.0f, dnc = j < b.j1 ? down(j) : 0.0f;
+        const float rem = (0.0f + upm) + dnc, add = (0.0f + dnm) + upc;
+        const float hv = HX[g];
+        const float moved = fmaxf(hv - rem + add, 0.0f);
+        const float hn = (rem > 0.0f || add > 0.0f) ? moved : hv;
+        h[g] = hn;
+        if (book_round) rnd += ((double)hn - (double)hv) - (((double)dnm + (double)upc) - ((double)upm + (double)dnc));
     })
+    if (book_round) {
+        for (int o = 16; o > 0; o >>= 1) rnd += __shfl_down_sync(0xffffffffu, rnd, o);
+        if ((threadIdx.x & 31) == 0 && rnd != 0.0) atomicAdd(J.round, rnd * J.cut_area);
+    }
     crew_sync();
 }
 
@@ -583,42 +638,47 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
     float* UG = J.gs[2];
     float* VG = J.gs[3];
     {
+        // The starting velocity on the box and its 2-cell rim, and gravity on
+        // the box's wet cells, in one phase: each cell's thread copies its
+        // velocity before it changes it, and gravity reads only p.
         const int x0 = max(b.i0 - 2, 0), x1 = min(b.i1 + 2, res - 1), y0 = max(b.j0 - 2, 0),
                   y1 = min(b.j1 + 2, res - 1);
+        if (threadIdx.x == 0) S.chg[0] = S.chg[1] = S.chg[2] = 0;
         CLU_RECT(x0, x1, y0, y1, {
-            U0[g] = J.u[g];
-            V0[g] = J.v[g];
+            const float u0 = J.u[g], v0 = J.v[g];
+            U0[g] = u0;
+            V0[g] = v0;
+            if (i >= b.i0 && i <= b.i1 && j >= b.j0 && j <= b.j1 && J.h[g] > eps) {
+                const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
+                float px = fdiv(p[j * res + ip] - p[j * res + im], two);
+                float pz = fdiv(p[jp * res + i] - p[jm * res + i], two);
+                float mob = job_mob(J, g);
+                // force_gravity_solid (:2084-2129): at least 1 beside a wall.
+                if (J.solid && J.h[g] > 0.08f && wall_near(J.solid, res, i, j)) mob = fmaxf(mob, 1.0f);
+                float ug = u0 + -kGravity * px * mob * dt;
+                float vg = v0 + -kGravity * pz * mob * dt;
+                UG[g] = ug;
+                VG[g] = vg;
+                J.u[g] = ug;
+                J.v[g] = vg;
+            }
         })
     }
-    crew_sync();
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
-        if (J.h[g] > eps) {
-            const int ip = min(i + 1, res - 1), im = max(i - 1, 0), jp = min(j + 1, res - 1), jm = max(j - 1, 0);
-            float px = fdiv(p[j * res + ip] - p[j * res + im], two);
-            float pz = fdiv(p[jp * res + i] - p[jm * res + i], two);
-            float mob = job_mob(J, g);
-            // force_gravity_solid (:2084-2129): at least 1 beside a wall.
-            if (J.solid && J.h[g] > 0.08f && wall_near(J.solid, res, i, j)) mob = fmaxf(mob, 1.0f);
-            float ug = J.u[g] + -kGravity * px * mob * dt;
-            float vg = J.v[g] + -kGravity * pz * mob * dt;
-            UG[g] = ug;
-            VG[g] = vg;
-            J.u[g] = ug;
-            J.v[g] = vg;
-        }
-    })
     crew_sync();
     if (!(J.vort > 0.0f)) return 0;
     // Fixed point of the sweep: cells before (i, j) in raster order read their
     // final values, (i, j) itself its post-gravity value, cells after it their
     // pre-gravity values.
-    // A pass ends when the whole crew has passed the barrier; its verdict is
-    // the OR of every CTA's flag, read from their shared memory.
+    // A pass ends at the crew barrier; its verdict is the OR of every CTA's
+    // flag for that pass, read from their shared memory. Flags rotate over
+    // three slots, so a pass needs one barrier: pass k sets chg[k % 3] and
+    // clears chg[(k + 1) % 3], which the crew last read before the barrier
+    // that ended pass k - 1.
     cg::cluster_group crew = cg::this_cluster();
     int passes = 0;
     for (; passes < GS_MAX_PASSES; ++passes) {
-        if (threadIdx.x == 0) S.changed = 0;
-        crew_sync();
+        const int slot = passes % 3;
+        if (threadIdx.x == 0) S.chg[(slot + 1) % 3] = 0;
         CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
             if (J.h[g] > eps) {
                 auto pick = [&](const float* X, const float* G0, const float* SG, int a, int c) {
@@ -637,14 +697,13 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
                 if (__float_as_uint(nu_) != __float_as_uint(J.u[g]) || __float_as_uint(nv_) != __float_as_uint(J.v[g])) {
                     J.u[g] = nu_;
                     J.v[g] = nv_;
-                    S.changed = 1;
+                    S.chg[slot] = 1;
                 }
             }
         })
         crew_sync();
         int any = 0;
-        for (int r = 0; r < crew_size(); ++r) any |= *crew.map_shared_rank(&S.changed, r);
-        crew_sync();  // every CTA has read the flags before the next pass clears them
+        for (int r = 0; r < crew_size(); ++r) any |= crew.map_shared_rank(S.chg, r)[slot];
         if (!any) break;
     }
     if (passes < GS_MAX_PASSES) return passes + 1;
@@ -755,13 +814,10 @@ __device__ __forceinline__ int cta_substep(Shared& S, const Job& J, const Box& b
         cta_lift(J, b, sa);
         crew_sync();
     }
-    cta_blur(sa, sb, se, res, b, kG0, kG1, kG2);
-    cta_blur(sa, scc, se, res, b, kS0, kS1, kS2);
-    CLU_RECT(b.i0, b.i1, b.j0, b.j1, {
-        float filtered = 0.62f * sb[g] + 0.38f * scc[g];
+    cta_blur_pair(sa, sb, scc, se, J.f1, res, b, [&](int g, float gauss, float steep) {
+        float filtered = 0.62f * gauss + 0.38f * steep;
         sd[g] = 0.45f * filtered + 0.55f * sa[g];
-    })
-    crew_sync();
+    });
     const bool par = (b.j1 - b.j0 >= 47) && (b.i1 - b.i0 >= 31) && inner_par;
     int passes = 0;
     if (walled) {
@@ -788,10 +844,8 @@ __device__ __forceinline__ int cta_substep(Shared& S, const Job& J, const Box& b
             sb[g] = div * overload - 0.015f * overload * lap_h;
         })
         crew_sync();
-        cta_blur(sb, scc, se, res, b, kG0, kG1, kG2);
-        cta_blur(sb, sa, se, res, b, kS0, kS1, kS2);
-        CLU_RECT(b.i0, b.i1, b.j0, b.j1, { sd[g] = 0.62f * scc[g] + 0.38f * sa[g]; })
-        crew_sync();
+        cta_blur_pair(sb, scc, sa, se, J.f1, res, b,
+                      [&](int g, float gauss, float steep) { sd[g] = 0.62f * gauss + 0.38f * steep; });
     }
     {
         const float* __restrict__ H = J.h;

@@ -35,7 +35,9 @@ struct Job {
     float* gs[4];          // Gauss-Seidel confinement: u0, v0, u after gravity, v after gravity
     double* ledger;        // FP64 sum of max(h, 0) after the step, may be nullptr
     double* cut;           // FP64 volume the dry cut removed, m^3 (accumulated), may be nullptr
-    double cut_area;       // m^2 of one cell for that book
+    double cut_area;       // m^2 of one cell for the cut and rounding books
+    double* round;         // FP64 rounding book, m^3 (accumulated), may be nullptr: each updated
+                           // cell's f32 change minus the exact sum of its face fluxes
     int32_t res;
     float cell, dt, vort, sub_cap, eps;
     CellDivisors div;      // 2 cell, cell^2, 231, cell (fdiv)

@@ -43,7 +43,8 @@ class SprayEvent(ctypes.Structure):
 
 class Ledger(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3",
-                                               "spray_m3", "opened_m3", "total_m3", "cut_m3", "reach_m3")]
+                                               "spray_m3", "opened_m3", "total_m3", "cut_m3", "reach_m3",
+                                               "round_m3")]
 
 
 class RiverReach(ctypes.Structure):
@@ -530,7 +531,7 @@ class Batch:
         return [{k: getattr(x, k) for k, _ in Ledger._fields_} for x in arr]
 
     def ledger_rows(self):
-        """Every window's ledger as one n x 7 FP64 array, columns in the
+        """Every window's ledger as one n x 10 FP64 array, columns in the
         silt_ledger field order."""
         arr = (Ledger * len(self.sheets))()
         check(lib().silt_batch_get_ledgers(self.h, arr), "batch_ledgers")

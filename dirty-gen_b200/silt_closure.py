@@ -46,6 +46,8 @@ _SIGS = {
     "silt_set_coupling": [_p, _i, _p, _f],
     "silt_closure_features": [_p, _p, _p, _p],
     "silt_get_closure_stats": [_p, ctypes.POINTER(ClosureStats)],
+    "silt_closure_wait_status": [ctypes.POINTER(_i), _p],
+    "silt_closure_wait_probe": [_i, _p],
 }
 _bound = {}
 
@@ -91,6 +93,18 @@ def wgrad(x, dy, dw, db):
     cout = dy.shape[-1]
     silt_b200.check(fn("silt_conv3x3_wgrad")(_ptr(x), _ptr(dy), _ptr(dw), _ptr(db), n, h, wd, cin, cout,
                                              _stream()), "conv3x3_wgrad")
+
+
+def wait_status():
+    """1 if a tensor-core kernel gave up a bounded wait since the last call (reads and clears)."""
+    g = _i(0)
+    silt_b200.check(fn("silt_closure_wait_status")(ctypes.byref(g), _stream()), "closure_wait_status")
+    return g.value
+
+
+def wait_probe(polls):
+    """One CTA waits at most `polls` polls on an mbarrier phase nothing completes."""
+    silt_b200.check(fn("silt_closure_wait_probe")(int(polls), _stream()), "closure_wait_probe")
 
 
 def pack(w32, cin, cout, fwd=None, bwd=None):

@@ -102,6 +102,17 @@ int silt_closure_adam(float* param, float* m, float* v, const float* grad, int32
  * input-gradient [cin][8 - tap][cout] (the flipped, transposed kernel). */
 int silt_closure_pack(const float* w, void* w_fwd_bf16, void* w_bwd_bf16, int32_t cin, int32_t cout, void* stream);
 
+/* Whether a tensor-core kernel of this library gave up a bounded wait (its
+ * mbarrier phase did not complete within the poll limit; the kernel then
+ * skips its epilogue, frees its tensor memory and returns) since the last
+ * call: *gave_up = 1 if so. Reads and clears the flag; synchronises stream.
+ * No counterpart in the reference (it has no GPU kernels). */
+int silt_closure_wait_status(int32_t* gave_up, void* stream);
+/* Diagnostic of that path without a fault: one CTA waits, `polls` polls at
+ * most (1..2^20), on an mbarrier phase nothing completes, gives up and sets
+ * the flag silt_closure_wait_status reads. */
+int silt_closure_wait_probe(int32_t polls, void* stream);
+
 /* ---- The closure in the step -------------------------------------------- */
 
 typedef struct silt_closure silt_closure;

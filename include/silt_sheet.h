@@ -98,6 +98,14 @@ typedef struct {
     double cut_m3;
     /* The river reach's bank (FluidLedger::reach_m3, :6863), in total_m3. */
     double reach_m3;
+    /* Volume the f32 transport updates created (+) or removed (-) by
+     * rounding since creation: each updated cell's f32 depth change less the
+     * exact (FP64) sum of the fluxes across its faces, summed in FP64. The
+     * state is the reference's f32 arithmetic, so this is the part of the
+     * books' per-step gap its transport explains; not in total_m3.
+     * total_m3 + cut_m3 - opened_m3 - round_m3 is conserved but for the
+     * rounding of the other f32 updates (coupling, seeding). */
+    double round_m3;
 } silt_ledger;
 
 /* src/fluid_core.rs:289-320 (`RiverReach`); inlet_turbidity is kept for the

@@ -143,3 +143,24 @@ def test_adam_training_reduces_the_loss():
     p = C.split_params(net.p)
     assert float(p["W1"][:, C.IN_USED:, :].abs().max()) == 0.0
     assert float(p["W3"][:, :, C.OUT_USED:].abs().max()) == 0.0
+
+
+def test_bounded_wait_gives_up_and_reports_without_a_fault():
+    """The tensor-core kernels wait on mbarrier phases with a poll limit. A
+    probe waits on a phase nothing completes, with a tiny limit: it must give
+    up, the status must come back to the host (and clear on reading), and the
+    context must stay usable: a convolution afterwards still matches the
+    FP32 reference and reports no give-up."""
+    assert C.wait_status() == 0
+    C.wait_probe(1000)
+    torch.cuda.synchronize()
+    assert C.wait_status() == 1
+    assert C.wait_status() == 0
+    x = rand_bf16((2, 16, 16, 16), seed=5)
+    w32 = rand_bf16((9, 16, 32), 0.2, seed=6).float()
+    wf = torch.empty((32, 9, 16), dtype=torch.bfloat16, device="cuda")
+    C.pack(w32.contiguous(), 16, 32, fwd=wf)
+    _, y32 = C.conv3x3(x, wf, want_bf16=False, want_f32=True)
+    ok, err = close(y32, ref_conv(x.float(), w32), 1e-4)
+    assert ok, err
+    assert C.wait_status() == 0
