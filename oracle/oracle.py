@@ -125,6 +125,9 @@ def _bind(L, _f, CoreCfg, Tire):
         L.oracle_core_get_grain.argtypes = [_p, _p]
         L.oracle_core_publish.argtypes = [_p, _p, _p]
         L.oracle_core_set_fine_pace.argtypes = [_p, _i]
+        L.oracle_core_set_turbidity.argtypes = [_p, _i]
+        L.oracle_core_set_reach_turbidity.argtypes = [_p, _f]
+        L.oracle_core_tracer_books.argtypes = [_p, _p, _p]
         L.oracle_core_set_fine_sub_cap.argtypes = [_p, _f]
         L.oracle_core_set_near_field.argtypes = [_p, _i]
         L.oracle_core_set_open_water.argtypes = [_p, _i, _f, _f, _f]
@@ -223,7 +226,10 @@ def rut_heal(grain, moisture):
                 still_deep_at_8s=bool(out[3] > 0.5))
 
 
-FIELDS = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7}
+FIELDS = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7, "foam": 8,
+          "turbid": 9, "susp": 10}
+TRACER_BOOKS = ("suspended_m3", "settled_suspended_m3", "frozen_suspended_m3", "entrained_m3", "turbid_m3",
+                "turbid_settled_m3", "stirred_m3", "frozen_turbid_m3")
 
 
 class Core:
@@ -311,6 +317,21 @@ class Core:
 
     def set_fine_pace(self, pace):
         self._L().oracle_core_set_fine_pace(self.h, pace)
+
+    def set_turbidity_enabled(self, on):
+        self._L().oracle_core_set_turbidity(self.h, int(on))
+
+    def set_reach_turbidity(self, c):
+        self._L().oracle_core_set_reach_turbidity(self.h, c)
+
+    def tracer_books(self):
+        """The tracer books: f32 as the reference keeps them, and '<name>64' in FP64."""
+        o = np.zeros(8, self._np if self._np == np.float64 else np.float32)
+        o64 = np.zeros(8, np.float64)
+        self._L().oracle_core_tracer_books(self.h, _ptr(o), _ptr(o64))
+        d = {k: float(v) for k, v in zip(TRACER_BOOKS, o)}
+        d.update({k + "64": float(v) for k, v in zip(TRACER_BOOKS, o64)})
+        return d
 
     def set_fine_sub_cap(self, cap):
         self._L().oracle_core_set_fine_sub_cap(self.h, cap)

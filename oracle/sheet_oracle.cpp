@@ -62,6 +62,12 @@ const usize NU_FILL_MARGIN = 8;             // :791
 const float NEAR_RESIDUAL_LIFE_S = 1.5f;    // near.rs:37
 const float NEAR_DROP_M = 1.0e-5f;          // near.rs:39
 const float NEAR_FILM_M = 1.0e-6f;          // near.rs:41
+const float FOAM_LIFE_S = 1.8f;             // :112
+const float FOAM_EQ = 0.85f;                // :115
+const float FOAM_TAU_S = 0.35f;             // :117
+const float SILT_SETTLE_S = 4.0f;           // :119
+const float SUSP_FALL_M_S = 0.004f;         // :122
+const float SILT_COLUMN_CAP_M = 0.028f;     // :124
 
 // ------------------------------------------------- Rust f32 helper semantics
 inline float rmax(float a, float b) { return fmaxf(a, b); }   // f32::max (NaN-ignoring)
@@ -143,6 +149,120 @@ float sheet_damp(float nu) {
 // src/fluid_core.rs:3473-3479
 float finite_speed(float v, float lim) { return finite(v) ? rclamp(v, -lim, lim) : 0.0f; }
 float finite0(float v) { return finite(v) ? v : 0.0f; }
+
+// ------------------------------------------------------- tracer helpers
+// src/fluid_core.rs:9688-9691
+float smoothstep(float e0, float e1, float x) {
+    float t = rclamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+// src/fluid_core.rs:9676-9686
+float breaking_foam(float speed, float thickness) {
+    if (!finite(speed) || !finite(thickness) || thickness < 0.004f || speed <= 0.05f) return 0.0f;
+    float froude = speed / sqrtf(9.81f * thickness);
+    return smoothstep(0.85f, 1.45f, froude);
+}
+// src/fluid_core.rs:9693-9712
+float sample_foam(const float* src, usize res, float x, float z) {
+    if (!finite(x) || !finite(z) || x < 0.0f || z < 0.0f) return 0.0f;
+    usize i0 = f2usize(floorf(x)), j0 = f2usize(floorf(z));
+    if (i0 >= res || j0 >= res) return 0.0f;
+    usize i1 = std::min(i0 + 1, res - 1), j1 = std::min(j0 + 1, res - 1);
+    float tx = rclamp(x - (float)i0, 0.0f, 1.0f), tz = rclamp(z - (float)j0, 0.0f, 1.0f);
+    float a = src[j0 * res + i0], b = src[j0 * res + i1], c = src[j1 * res + i0], d = src[j1 * res + i1];
+    float v = a + (b - a) * tx + (c - a) * tz + (a - b - c + d) * tx * tz;
+    return finite(v) ? rclamp(v, 0.0f, 1.0f) : 0.0f;
+}
+// src/fluid_core.rs:9857-9876 flux_edge
+void flux_edge(const float* h, float* scratch, usize n, usize a, usize b, float vel, float cell, float dt) {
+    if (!finite(vel) || fabsf(vel) < 1.0e-5f) return;
+    usize donor = vel > 0.0f ? a : b, recv = vel > 0.0f ? b : a;
+    float column = finite(h[donor]) ? h[donor] : 0.0f;
+    float room = column - scratch[donor];
+    if (room <= 1.0e-8f) return;
+    float frac = rmin(fabsf(vel) * dt / cell, 0.45f);
+    float dh = rmin(column * frac, room);
+    if (dh <= 1.0e-8f || !finite(dh)) return;
+    scratch[donor] += dh;
+    scratch[n + recv] += dh;
+}
+// src/fluid_core.rs:9716-9748 flux_thickness
+void flux_thickness(const float* h, const float* u, const float* v, usize res, float cell, float dt, usize i0,
+                    usize i1, usize j0, usize j1, float* scratch) {
+    usize n = res * res;
+    for (usize j = j0; j <= j1; ++j) {
+        usize row = j * res;
+        for (usize i = i0; i < std::min(i1, res - 1); ++i) {
+            usize a = row + i, b = a + 1;
+            float vel = 0.5f * (u[a] + u[b]);
+            flux_edge(h, scratch, n, a, b, vel, cell, dt);
+        }
+    }
+    for (usize j = j0; j < std::min(j1, res - 1); ++j)
+        for (usize i = i0; i <= i1; ++i) {
+            usize a = j * res + i, b = a + res;
+            float vel = 0.5f * (v[a] + v[b]);
+            flux_edge(h, scratch, n, a, b, vel, cell, dt);
+        }
+}
+// src/fluid_core.rs:9752-9764
+bool shore_wet_cell(const float* water, usize res, usize i, usize j) {
+    if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return false;
+    const int d[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    for (auto& o : d) {
+        float nh = water[(usize)((int)j + o[1]) * res + (usize)((int)i + o[0])];
+        if (finite(nh) && nh < 0.004f) return true;
+    }
+    return false;
+}
+// src/fluid_core.rs:9766-9795 (inclusive box of cells above 1e-8, grown by one)
+bool turbid_span(const float* h, usize res, usize& i0, usize& i1, usize& j0, usize& j1) {
+    i0 = res; i1 = 0; j0 = res; j1 = 0;
+    for (usize j = 0; j < res; ++j) {
+        const float* row = h + j * res;
+        float m = 0.0f;
+        for (usize i = 0; i < res; ++i) m = rmax(m, row[i]);
+        if (m <= 1.0e-8f) continue;
+        usize first = 0, last = 0;
+        for (usize i = 0; i < res; ++i) if (row[i] > 1.0e-8f) { first = i; break; }
+        for (usize i = res; i-- > 0;) if (row[i] > 1.0e-8f) { last = i; break; }
+        i0 = std::min(i0, first); i1 = std::max(i1, last); j0 = std::min(j0, j); j1 = std::max(j1, j);
+    }
+    if (i0 > i1) return false;
+    i0 = sat_sub(i0, 1); i1 = std::min(i1 + 1, res - 1); j0 = sat_sub(j0, 1); j1 = std::min(j1 + 1, res - 1);
+    return true;
+}
+// src/fluid_core.rs:9826-9872 shore_cell: (foam production, silt lift rate)
+void shore_cell(const float* water, const float* uw, const float* vw, usize res, usize idx, float& foam,
+                float& rate) {
+    foam = 0.0f; rate = 0.0f;
+    usize i = idx % res, j = idx / res;
+    if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return;
+    float h = water[idx];
+    if (!finite(h) || h < 0.004f) return;
+    float nx = 0.0f, nz = 0.0f;
+    bool edge = false;
+    const int d[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    for (auto& o : d) {
+        float nh = water[(usize)((int)j + o[1]) * res + (usize)((int)i + o[0])];
+        if (finite(nh) && nh < 0.004f) { edge = true; nx += (float)o[0]; nz += (float)o[1]; }
+    }
+    if (!edge) return;
+    float u = uw[idx], v = vw[idx];
+    if (!finite(u) || !finite(v)) return;
+    float film = hypotf(u, v);
+    float nlen = rmax(hypotf(nx, nz), 1.0e-4f);
+    float into = rmax((u * nx + v * nz) / nlen, 0.0f);
+    float strain = fabsf(uw[idx + 1] - uw[idx - 1]) + fabsf(vw[idx + res] - vw[idx - res]);
+    float shear_v = rmax(film, strain);
+    if (shear_v < 0.2f && into < 0.2f) return;
+    float prod = rmax(breaking_foam(rmax(shear_v, into), h), smoothstep(0.25f, 1.1f, into));
+    foam = prod > 0.02f ? prod : 0.0f;
+    if (h > 0.012f && h < 0.055f && (shear_v > 0.45f || into > 0.4f)) {
+        float tau = 1000.0f * 0.025f * shear_v * shear_v;
+        if (tau > 3.0f || into > 0.45f) rate = rmin(0.006f * (into + shear_v * 0.35f), 0.01f);
+    }
+}
 
 // ------------------------------------------------------------------- scratch
 // src/fluid_core.rs:536-579
@@ -1423,10 +1543,10 @@ struct Core {
     bool fine_on = false;
     bool near_on = true;
     std::map<std::pair<int, int>, NearTile> near;
-    // src/fluid_core.rs:4763-4782 Parked (the sheet fields; dust, foam and
-    // the tracers are off this path and stay 0).
+    // src/fluid_core.rs:4763-4782 Parked (the sheet fields and the tracers;
+    // settled dust is off this path).
     struct Parked {
-        float water = 0, slurry = 0, uw = 0, vw = 0, us = 0, vs = 0, moisture = 0;
+        float water = 0, slurry = 0, uw = 0, vw = 0, us = 0, vs = 0, moisture = 0, foam = 0, turbid = 0, susp = 0;
     };
     std::map<std::pair<int, int>, Parked> parked;
     float spray_m3 = 0.0f;
@@ -1460,6 +1580,18 @@ struct Core {
     // src/fluid_core.rs:4907-4909: scour beside tire contacts.
     std::vector<float> bed_drop;
     float eroded_m3 = 0.0f, scour_hole_m = 0.0f;
+    // src/fluid_core.rs:4832-4860: the tracers. Foam (a 0..1 cover), stirred
+    // silt (`turbid`, metres of soil in the water) and wheel-lifted suspended
+    // solids (`susp`, metres), with their books in f32 as the reference keeps
+    // them and FP64 twins of the same terms.
+    std::vector<float> foam, turbid, susp, susp_next, susp_taken, tracer_scratch;
+    std::vector<uint32_t> foam_live, wet_idx, shore_idx;
+    std::vector<u8> foam_live_mark;
+    float turbid_settled_m3 = 0.0f, stirred_m3 = 0.0f, entrained_m3 = 0.0f, settled_suspended_m3 = 0.0f;
+    double turbid_settled64 = 0.0, stirred64 = 0.0, entrained64 = 0.0, settled_suspended64 = 0.0;
+    uint32_t last_susp_capped = 0;
+    bool turbidity_enabled = true;   // :4994
+    float reach_inlet_turbidity = 0.0f;
 
     explicit Core(const oracle_core_cfg& c) : cfg(c) {
         res = (usize)c.res;
@@ -1467,6 +1599,8 @@ struct Core {
         sub = (usize)lroundf(c.cell / c.fine_cell);
         usize n = res * res, fn = fres * fres;
         bed_drop.assign(n, 0.0f);
+        foam.assign(n, 0.0f); turbid.assign(n, 0.0f); susp.assign(n, 0.0f);
+        susp_next.assign(n, 0.0f); susp_taken.assign(n, 0.0f); foam_live_mark.assign(n, 0);
         water.assign(n, 0); slurry.assign(n, 0); uw.assign(n, 0); vw.assign(n, 0);
         us.assign(n, 0); vs.assign(n, 0); bed.assign(n, 0); moisture.assign(n, 0);
         grain.assign(n, 4);
@@ -2055,6 +2189,8 @@ struct Core {
     std::vector<Spray> step(float dt) {
         std::vector<TirePush> ps;
         ps.swap(pushes);
+        // Lift from the column the tire rolls into, before the sheet shoves it (:6051-6053).
+        if (turbidity_enabled && dt > 0.0f && finite(dt) && !ps.empty()) entrain_wake(ps, dt);
         if (inflow_j >= 0 && dt > 0.0f) apply_inflow(dt);
         refine(ps, dt);
         // apply_pushes(fine): src/fluid_core.rs:8152-8158
@@ -2082,7 +2218,9 @@ struct Core {
         diffuse_surface(dt);
         if (!ps.empty()) peel(ps, water.data(), uw.data(), vw.data(), res, cfg.cell, origin, true, spray);
         if (!solids.empty()) scour_contacts(dt);
+        step_tracers(dt, ps);         // :6080
         feed_reach();
+        if (turbidity_enabled) step_suspended(dt);  // :6087-6089
         for (const auto& s : spray) spray_m3 += s.volume;
         return spray;
     }
@@ -2412,6 +2550,8 @@ struct Core {
                 }
             }
         }
+        float inflow_c = turbidity_enabled && finite(reach_inlet_turbidity) ? rclamp(reach_inlet_turbidity, 0.0f, 1.0f) : 0.0f;
+        double inflow_m3 = 0.0;
         float deep = 0.0f;
         for (usize cross = c0; cross < c1; ++cross) deep = rmax(deep, rmax(reach_inlet_eta - bed[at(row(0), cross)], 0.0f));
         if (deep <= 0.0f) return;
@@ -2432,22 +2572,43 @@ struct Core {
                 float speed = reach_speed * sqrtf(rmin(rmax(water[idx] / deep, 0.0f), 1.0f));
                 uw[idx] = speed * dx;
                 vw[idx] = speed * dz;
+                if (inflow_c > 0.0f) {  // :7712-7757, the inlet's suspended load
+                    float w = water[idx];
+                    float want = inflow_c * w;
+                    float have = susp[idx];
+                    if (w >= 1.0e-5f && finite(have) && have < want) {
+                        susp[idx] = want;
+                        inflow_m3 += (double)((want - have) * area);
+                    }
+                }
             }
+        entrained_m3 += (float)inflow_m3;
+        entrained64 += inflow_m3;
     }
 
-    // src/fluid_core.rs:4797-4805 park_slot (sheet fields).
+    // src/fluid_core.rs:4797-4805 park_slot (settled dust is off this path and 0).
     bool park_slot(const Parked& p) const {
-        return p.water > 1.0e-8f || p.slurry > 1.0e-8f || fabsf(p.moisture - moisture_ambient) > 6.0e-3f;
+        return p.water > 1.0e-8f || p.slurry > 1.0e-8f || p.susp > 1.0e-8f ||
+               fabsf(p.moisture - moisture_ambient) > 6.0e-3f || p.foam > 1.0e-4f || p.turbid > 1.0e-8f;
     }
     Parked slot_of(usize idx) const {
         Parked p;
         p.water = water[idx]; p.slurry = slurry[idx]; p.uw = uw[idx]; p.vw = vw[idx];
         p.us = us[idx]; p.vs = vs[idx]; p.moisture = moisture[idx];
+        p.foam = foam[idx]; p.turbid = turbid[idx]; p.susp = susp[idx];
         return p;
     }
     void put_slot(usize idx, const Parked& p) {
         water[idx] = p.water; slurry[idx] = p.slurry; uw[idx] = p.uw; vw[idx] = p.vw;
         us[idx] = p.us; vs[idx] = p.vs; moisture[idx] = p.moisture;
+        foam[idx] = p.foam; turbid[idx] = p.turbid; susp[idx] = p.susp;
+    }
+    // src/fluid_core.rs:9228-9233 reset_tracer_indices.
+    void reset_tracer_indices() {
+        wet_idx.clear();
+        shore_idx.clear();
+        foam_live.clear();
+        std::fill(foam_live_mark.begin(), foam_live_mark.end(), 0);
     }
     std::pair<int, int> cell_key(const float* o, usize i, usize j) const {
         return world_key(o[0] + ((float)i + 0.5f) * cfg.cell, o[1] + ((float)j + 0.5f) * cfg.cell, cfg.cell);
@@ -2513,6 +2674,8 @@ struct Core {
         usize n = res * res;
         each_leaving(di, dj, [&](int i, int j) { park((usize)j * res + i, cell_key(origin, i, j)); });
         std::vector<float> cw = water, cs = slurry, cuw = uw, cvw = vw, cus = us, cvs = vs, cm = moisture;
+        std::vector<float> cf = foam, ct = turbid, cp = susp;
+        const bool track_susp = turbidity_enabled;
         int rn = (int)res;
         for (int j = 0; j < rn; ++j)
             for (int i = 0; i < rn; ++i) {
@@ -2522,19 +2685,23 @@ struct Core {
                 usize src = 0;
                 if (si >= 0 && si < rn && sj >= 0 && sj < rn) {
                     src = (usize)sj * res + si;
-                    keep = cw[src] > 1.0e-8f || cs[src] > 1.0e-8f || cm[src] > 1.0e-4f;
+                    keep = cw[src] > 1.0e-8f || cs[src] > 1.0e-8f || cm[src] > 1.0e-4f || cf[src] > 1.0e-5f ||
+                           ct[src] > 1.0e-8f || (track_susp && cp[src] > 1.0e-8f);
                 }
                 if (keep) {
                     water[dst] = cw[src]; slurry[dst] = cs[src]; uw[dst] = cuw[src]; vw[dst] = cvw[src];
                     us[dst] = cus[src]; vs[dst] = cvs[src]; moisture[dst] = cm[src];
+                    foam[dst] = cf[src]; turbid[dst] = ct[src]; susp[dst] = track_susp ? cp[src] : 0.0f;
                 } else {
                     water[dst] = 0; slurry[dst] = 0; uw[dst] = 0; vw[dst] = 0; us[dst] = 0; vs[dst] = 0;
                     moisture[dst] = moisture_ambient;
+                    foam[dst] = 0; turbid[dst] = 0; susp[dst] = 0;
                 }
             }
         (void)n;
         origin[0] = nw[0];
         origin[1] = nw[1];
+        reset_tracer_indices();
         each_leaving(-di, -dj, [&](int i, int j) {
             auto it = parked.find(cell_key(origin, i, j));
             if (it == parked.end()) return;
@@ -2550,6 +2717,7 @@ struct Core {
             for (usize i = 0; i < res; ++i) park(j * res + i, cell_key(origin, i, j));
         origin[0] = nw[0];
         origin[1] = nw[1];
+        reset_tracer_indices();
         for (usize j = 0; j < res; ++j)
             for (usize i = 0; i < res; ++i) {
                 usize idx = j * res + i;
@@ -2562,6 +2730,472 @@ struct Core {
                 }
                 put_slot(idx, p);
             }
+    }
+
+    // ------------------------------------------------------------ tracers
+    bool surface_driven() const { return wave_on || reach_on; }  // :6240-6244
+    static bool wake_push(const TirePush& p) {
+        return (finite(p.speed) && p.speed >= 0.25f) || (finite(p.slip) && fabsf(p.slip) >= 0.05f);
+    }
+
+    // src/fluid_core.rs:8758-8815 entrain_wake: the aft plume of each tire
+    // lifts solids into the water column it rolls through.
+    void entrain_wake(const std::vector<TirePush>& ps, float dt) {
+        const int r = (int)res;
+        const float cell = cfg.cell, area = cell * cell;
+        for (const auto& p : ps) {
+            if (p.speed < 0.3f) continue;
+            float fl = rmax(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
+            float fx = p.forward_x / fl, fz = p.forward_z / fl;
+            float rx = fz, rz = -fx;
+            float reach = p.radius * 3.4f + cell;
+            int i0 = (int)floorf(((p.x - reach) - origin[0]) / cell);
+            int i1 = (int)floorf(((p.x + reach) - origin[0]) / cell);
+            int j0 = (int)floorf(((p.z - reach) - origin[1]) / cell);
+            int j1 = (int)floorf(((p.z + reach) - origin[1]) / cell);
+            float aft = p.radius * 3.2f;
+            float half = p.width * 0.55f + 0.08f;
+            for (int j = std::max(j0, 0); j <= std::min(j1, r - 1); ++j)
+                for (int i = std::max(i0, 0); i <= std::min(i1, r - 1); ++i) {
+                    float x = origin[0] + ((float)i + 0.5f) * cell;
+                    float z = origin[1] + ((float)j + 0.5f) * cell;
+                    float dx = x - p.x, dz = z - p.z;
+                    float along = dx * fx + dz * fz;
+                    if (along > -0.05f || along < -aft) continue;
+                    float lat = fabsf(dx * rx + dz * rz);
+                    if (lat > half) continue;
+                    usize idx = (usize)j * res + (usize)i;
+                    float w = water[idx];
+                    if (!finite(w) || w < 0.004f) continue;
+                    float along_t = rclamp((-along) / aft, 0.0f, 1.0f);
+                    float lat_t = rclamp(lat / half, 0.0f, 1.0f);
+                    float core = (1.0f - along_t) * (1.0f - lat_t);
+                    float room = rmax(w - susp[idx], 0.0f);
+                    float add = rmin(4.0f * dt * core * w, room);
+                    if (add <= 1.0e-8f) continue;
+                    susp[idx] += add;
+                    entrained_m3 += add * area;
+                    entrained64 += (double)add * (double)area;
+                }
+        }
+    }
+
+    // src/fluid_core.rs:6210-6237 step_tracers.
+    void step_tracers(float dt, const std::vector<TirePush>& ps) {
+        if (dt <= 0.0f || !finite(dt)) return;
+        bool wake = surface_driven();
+        for (const auto& p : ps) wake = wake || wake_push(p);
+        bool live_silt = false;
+        for (float t : turbid) live_silt = live_silt || (finite(t) && t > 1.0e-8f);
+        bool live_foam = !foam_live.empty();
+        if (!wake && !live_silt && !live_foam) return;
+        collect_tracer_wet(ps);
+        if (wet_idx.empty() && !live_silt) return;
+        if (live_foam) advect_foam(dt);
+        advect_turbid(dt);
+        settle_turbid(dt);
+        for (const auto& p : ps) spawn_tire_tracers(p, dt, cfg.cell * cfg.cell);
+        spawn_shore_tracers(dt, cfg.cell * cfg.cell);
+        spawn_breaking_speed(dt);
+        clear_dry_tracers();
+        sync_foam_live();
+    }
+
+    // src/fluid_core.rs:6248-6293 collect_tracer_wet.
+    void collect_tracer_wet(const std::vector<TirePush>& ps) {
+        wet_idx.clear();
+        shore_idx.clear();
+        bool wake = surface_driven();
+        for (const auto& p : ps) wake = wake || wake_push(p);
+        usize i0, i1, j0, j1;
+        if (wake) {
+            i0 = 0; i1 = res - 1; j0 = 0; j1 = res - 1;
+        } else if (tracer_visit_box(ps, i0, i1, j0, j1)) {
+            const usize M = 2;
+            i0 = sat_sub(i0, M); j0 = sat_sub(j0, M);
+            i1 = std::min(i1 + M, res - 1); j1 = std::min(j1 + M, res - 1);
+        } else {
+            return;
+        }
+        for (usize j = j0; j <= j1; ++j) {
+            usize row = j * res;
+            float peak = 0.0f;
+            for (usize i = i0; i <= i1; ++i) peak = rmax(peak, water[row + i] + slurry[row + i]);
+            if (peak < 0.004f) continue;
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = row + i;
+                float h = water[idx] + slurry[idx];
+                if (!finite(h) || h < 0.004f) continue;
+                wet_idx.push_back((uint32_t)idx);
+                if (shore_wet_cell(water.data(), res, i, j)) shore_idx.push_back((uint32_t)idx);
+            }
+        }
+    }
+
+    // src/fluid_core.rs:6296-6337 tracer_visit_box.
+    bool tracer_visit_box(const std::vector<TirePush>& ps, usize& i0, usize& i1, usize& j0, usize& j1) const {
+        i0 = res; i1 = 0; j0 = res; j1 = 0;
+        bool any = false;
+        for (uint32_t id : foam_live) {
+            usize i = id % res, j = id / res;
+            i0 = std::min(i0, i); i1 = std::max(i1, i); j0 = std::min(j0, j); j1 = std::max(j1, j);
+            any = true;
+        }
+        usize ti0, ti1, tj0, tj1;
+        if (turbid_span(turbid.data(), res, ti0, ti1, tj0, tj1)) {
+            i0 = std::min(i0, ti0); i1 = std::max(i1, ti1); j0 = std::min(j0, tj0); j1 = std::max(j1, tj1);
+            any = true;
+        }
+        int reach = (int)ceilf(8.0f / cfg.cell);
+        for (const auto& p : ps) {
+            usize ci, cj;
+            if (!coarse_ij(p.x, p.z, ci, cj)) continue;
+            int a = (int)ci, b = (int)cj, r = (int)res;
+            i0 = std::min(i0, (usize)std::max(a - reach, 0)); i1 = std::max(i1, (usize)std::min(a + reach, r - 1));
+            j0 = std::min(j0, (usize)std::max(b - reach, 0)); j1 = std::max(j1, (usize)std::min(b + reach, r - 1));
+            any = true;
+        }
+        return any;
+    }
+
+    // src/fluid_core.rs:6339-6349 sync_foam_live.
+    void sync_foam_live() {
+        foam_live.clear();
+        std::fill(foam_live_mark.begin(), foam_live_mark.end(), 0);
+        for (uint32_t id : wet_idx)
+            if (finite(foam[id]) && foam[id] > 1.0e-4f) {
+                foam_live_mark[id] = 1;
+                foam_live.push_back(id);
+            }
+    }
+
+    // src/fluid_core.rs:6352-6397 advect_foam: semi-Lagrangian on the wet cells.
+    void advect_foam(float dt) {
+        const float cell = cfg.cell;
+        std::vector<float> src = foam;
+        std::vector<float> samp(wet_idx.size(), 0.0f);
+        for (usize k = 0; k < wet_idx.size(); ++k) {
+            usize idx = wet_idx[k];
+            float u = uw[idx], v = vw[idx];
+            float sample = 0.0f;
+            if (finite(u) && finite(v)) {
+                usize i = idx % res, j = idx / res;
+                float x = (float)i - u * dt / cell;
+                float z = (float)j - v * dt / cell;
+                sample = sample_foam(src.data(), res, x, z);
+            }
+            samp[k] = sample;
+        }
+        std::vector<float> next = src;
+        for (uint32_t id : foam_live) next[id] = 0.0f;
+        for (uint32_t id : wet_idx) next[id] = 0.0f;
+        float decay = expf(-dt / FOAM_LIFE_S);
+        for (usize k = 0; k < wet_idx.size(); ++k) {
+            float v = samp[k] * decay;
+            if (v > 1.0e-4f && finite(v)) next[wet_idx[k]] = rmin(v, FOAM_EQ);
+        }
+        foam = next;
+    }
+
+    // src/fluid_core.rs:6400-6418 add_foam.
+    void add_foam(usize idx, float prod, float dt) {
+        if (prod <= 0.0f || !finite(prod) || !(dt > 0.0f)) return;
+        float cur = finite(foam[idx]) ? rclamp(foam[idx], 0.0f, FOAM_EQ) : 0.0f;
+        float room = FOAM_EQ - cur;
+        if (room <= 1.0e-5f) return;
+        float grown = cur + room * prod * rmin(dt / FOAM_TAU_S, 1.0f);
+        foam[idx] = finite(grown) ? rmin(grown, FOAM_EQ) : 0.0f;
+    }
+
+    // src/fluid_core.rs:6421-6470 advect_turbid: donor-cell transport of the silt column.
+    void advect_turbid(float dt) {
+        usize i0, i1, j0, j1;
+        if (!turbid_span(turbid.data(), res, i0, i1, j0, j1)) return;
+        usize n = res * res;
+        std::vector<float> scratch(2 * n, 0.0f);
+        flux_thickness(turbid.data(), uw.data(), vw.data(), res, cfg.cell, dt, i0, i1, j0, j1, scratch.data());
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float removed = scratch[idx], added = scratch[n + idx];
+                if (removed == 0.0f && added == 0.0f) {
+                    if (!finite(turbid[idx])) turbid[idx] = 0.0f;
+                    continue;
+                }
+                float next = turbid[idx] - removed + added;
+                turbid[idx] = finite(next) ? rmax(next, 0.0f) : 0.0f;
+            }
+    }
+
+    // src/fluid_core.rs:6473-6509 settle_turbid.
+    void settle_turbid(float dt) {
+        const float area = cfg.cell * cfg.cell;
+        float keep = expf(-dt / SILT_SETTLE_S);
+        float settled = 0.0f;
+        double settled64 = 0.0;
+        usize i0, i1, j0, j1;
+        if (!turbid_span(turbid.data(), res, i0, i1, j0, j1)) return;
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float h = water[idx] + slurry[idx];
+                float column = finite(turbid[idx]) ? rmax(turbid[idx], 0.0f) : 0.0f;
+                if (column <= 0.0f) { turbid[idx] = 0.0f; continue; }
+                if (!finite(h) || h < 1.0e-5f) {
+                    settled += column * area;
+                    settled64 += (double)(column * area);
+                    turbid[idx] = 0.0f;
+                    continue;
+                }
+                float stay = column * keep;
+                settled += (column - stay) * area;
+                settled64 += (double)((column - stay) * area);
+                turbid[idx] = stay;
+            }
+        if (finite(settled)) {
+            turbid_settled_m3 += settled;
+            turbid_settled64 += settled64;
+        }
+    }
+
+    // src/fluid_core.rs:6545-6558 spawn_breaking_speed.
+    void spawn_breaking_speed(float dt) {
+        for (uint32_t id : wet_idx) {
+            float h = water[id] + slurry[id];
+            if (!finite(h) || h < 0.004f) continue;
+            float u = uw[id], v = vw[id];
+            if (!finite(u) || !finite(v) || hypotf(u, v) <= 0.05f) continue;
+            float speed = hypotf(u, v);
+            add_foam(id, breaking_foam(speed, h), dt);
+        }
+    }
+
+    // src/fluid_core.rs:6599-6665 spawn_tire_tracers.
+    void spawn_tire_tracers(const TirePush& p, float dt, float area) {
+        float speed = finite(p.speed) ? rmax(p.speed, 0.0f) : 0.0f;
+        float slip = finite(p.slip) ? rmin(fabsf(p.slip), 1.5f) : 0.0f;
+        if (speed < 0.25f && slip < 0.05f) return;
+        float radius = rmax(p.radius, 0.05f);
+        float len = rmax(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
+        float fx = p.forward_x / len, fz = p.forward_z / len;
+        float rx = fz, rz = -fx;
+        const float cell = cfg.cell;
+        float reach = radius * 1.15f + cell;
+        float reach2 = reach * reach;
+        float slip_v = speed * slip;
+        for (uint32_t id : wet_idx) {
+            usize idx = id;
+            float h = water[idx];
+            if (!finite(h) || h < 0.004f) continue;
+            usize i = idx % res, j = idx / res;
+            float x = origin[0] + ((float)i + 0.5f) * cell;
+            float z = origin[1] + ((float)j + 0.5f) * cell;
+            float dx = x - p.x, dz = z - p.z;
+            if (dx * dx + dz * dz > reach2) continue;
+            float along = dx * fx + dz * fz;
+            float lat = dx * rx + dz * rz;
+            float dist = hypotf(dx, dz);
+            float film = hypotf(uw[idx], vw[idx]);
+            film = finite(film) ? film : 0.0f;
+            float immerse = rmin(h, radius * 0.9f);
+            float r_line = sqrtf(rmax(2.0f * radius * immerse - immerse * immerse, 0.0f));
+            float band = 1.0f - rclamp(fabsf(dist - r_line) / (cell * 1.35f), 0.0f, 1.0f);
+            if (band > 0.0f) {
+                float motion = rmax(rmax(slip_v, speed * 0.45f), film);
+                float prod = breaking_foam(motion, h) * band;
+                add_foam(idx, prod, dt);
+            }
+            bool on_patch = fabsf(lat) <= p.width * 0.55f + cell * 0.35f && along >= -radius * 0.55f &&
+                            along <= radius * 0.35f;
+            if (on_patch && h > 0.02f) {
+                float shear_v = rmax(slip_v, film * 0.35f);
+                lift_silt(idx, shear_v, dt, area, 0.015f, 6.0f);
+            }
+        }
+    }
+
+    // src/fluid_core.rs:6667-6684 spawn_shore_tracers.
+    void spawn_shore_tracers(float dt, float area) {
+        for (uint32_t id : shore_idx) {
+            float prod, silt_add;
+            shore_cell(water.data(), uw.data(), vw.data(), res, id, prod, silt_add);
+            add_foam(id, prod, dt);
+            if (silt_add > 0.0f) add_silt(id, rmin(silt_add * dt, 0.0012f), area);
+        }
+    }
+
+    // src/fluid_core.rs:6686-6697 lift_silt.
+    void lift_silt(usize idx, float shear_v, float dt, float area, float rate_cap, float tau_c) {
+        if (!finite(shear_v) || shear_v <= 0.0f) return;
+        float tau = 1000.0f * 0.035f * shear_v * shear_v;
+        if (tau <= tau_c) return;
+        float rate = rmin(0.008f * (tau / tau_c - 1.0f), rate_cap);
+        add_silt(idx, rmin(rate * dt, 0.0025f), area);
+    }
+
+    // src/fluid_core.rs:6699-6710 add_silt.
+    void add_silt(usize idx, float dh, float area) {
+        if (dh <= 0.0f || !finite(dh)) return;
+        float room = rmax(SILT_COLUMN_CAP_M - rmax(turbid[idx], 0.0f), 0.0f);
+        float add = rmin(dh, room);
+        if (add <= 0.0f) return;
+        turbid[idx] += add;
+        stirred_m3 += add * area;
+        stirred64 += (double)(add * area);
+    }
+
+    // src/fluid_core.rs:6712-6739 clear_dry_tracers.
+    void clear_dry_tracers() {
+        const float area = cfg.cell * cfg.cell;
+        for (uint32_t id : wet_idx) {
+            float h = water[id] + slurry[id];
+            if (!finite(h) || h < 0.004f) foam[id] = 0.0f;
+            else if (!finite(foam[id])) foam[id] = 0.0f;
+        }
+        usize i0, i1, j0, j1;
+        if (!turbid_span(turbid.data(), res, i0, i1, j0, j1)) return;
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float h = water[idx] + slurry[idx];
+                if (!finite(h) || h < 1.0e-5f) {
+                    if (turbid[idx] > 0.0f) {
+                        turbid_settled_m3 += turbid[idx] * area;
+                        turbid_settled64 += (double)(turbid[idx] * area);
+                        turbid[idx] = 0.0f;
+                    }
+                } else if (!finite(turbid[idx])) {
+                    turbid[idx] = 0.0f;
+                }
+            }
+    }
+
+    // src/fluid_core.rs:8817-9002 advect_suspended (step_suspended :8750-8756).
+    void step_suspended(float dt) {
+        last_susp_capped = 0;
+        if (dt <= 0.0f || !finite(dt)) return;
+        const float cell = cfg.cell, area = cell * cell;
+        usize i0 = res, i1 = 0, j0 = res, j1 = 0;
+        double landed_m3 = 0.0;
+        for (usize j = 0; j < res; ++j)
+            for (usize i = 0; i < res; ++i) {
+                usize idx = j * res + i;
+                float sv = susp[idx];
+                if (!finite(sv) || sv <= 1.0e-12f) { susp[idx] = 0.0f; continue; }
+                float w = water[idx];
+                if (!finite(w) || w < 1.0e-5f || sv > w) {
+                    settled_suspended_m3 += sv * area;
+                    settled_suspended64 += (double)(sv * area);
+                    susp[idx] = 0.0f;
+                    continue;
+                }
+                float keep = expf(-dt * SUSP_FALL_M_S / w);
+                float landed = sv * (1.0f - keep);
+                if (landed > 0.0f) {
+                    landed_m3 += (double)landed * (double)area;
+                    sv -= landed;
+                    susp[idx] = sv;
+                }
+                if (sv > 1.0e-8f) {
+                    i0 = std::min(i0, i); i1 = std::max(i1, i); j0 = std::min(j0, j); j1 = std::max(j1, j);
+                }
+            }
+        settled_suspended_m3 += (float)landed_m3;
+        settled_suspended64 += landed_m3;
+        if (i0 > i1) return;
+        i0 = sat_sub(i0, 1); j0 = sat_sub(j0, 1);
+        i1 = std::min(i1 + 1, res - 1); j1 = std::min(j1 + 1, res - 1);
+        susp_next = susp;
+        std::fill(susp_taken.begin(), susp_taken.end(), 0.0f);
+        const bool open = surface_driven();
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float depth = susp[idx], w = water[idx];
+                if (depth <= 1.0e-12f || !finite(depth) || !finite(w) || w < 1.0e-5f) continue;
+                // film_uv(water, 0, uw, vw, 0, 0) (:3490-3501)
+                float u = 0.0f, v = 0.0f;
+                {
+                    float hh = w + 0.0f;
+                    if (finite(hh) && !(hh < 1.0e-5f)) {
+                        u = finite0((uw[idx] * w + 0.0f * 0.0f) / hh);
+                        v = finite0((vw[idx] * w + 0.0f * 0.0f) / hh);
+                    }
+                }
+                u = open && finite(u) ? u : 0.0f;
+                v = finite(v) ? v : 0.0f;
+                float c = depth / w;
+                float fu = fabsf(u) * dt / cell, fv = fabsf(v) * dt / cell;
+                float sum = fu + fv;
+                if (sum > 0.45f) { fu *= 0.45f / sum; fv *= 0.45f / sum; }
+                long up_i = u > 0.0f ? (i + 1 < res ? (long)(idx + 1) : -1) : (i > 0 ? (long)(idx - 1) : -1);
+                long up_j = v > 0.0f ? (j + 1 < res ? (long)(idx + res) : -1) : (j > 0 ? (long)(idx - res) : -1);
+                const float fr[2] = {fu, fv};
+                const long rv[2] = {up_i, up_j};
+                for (int q = 0; q < 2; ++q) {
+                    float give = depth * fr[q];
+                    if (give <= 1.0e-12f) continue;
+                    if (rv[q] < 0) {
+                        settled_suspended_m3 += give * area;
+                        settled_suspended64 += (double)(give * area);
+                        susp_next[idx] -= give;
+                        continue;
+                    }
+                    usize nn = (usize)rv[q];
+                    float wr = water[nn];
+                    if (!finite(wr) || wr < 1.0e-5f) continue;
+                    float have = susp[nn] + susp_taken[nn];
+                    float room = rmax(c * wr - have, 0.0f);
+                    float accept = rmin(rmin(give, room), rmax(wr - have, 0.0f));
+                    if (accept <= 1.0e-12f) continue;
+                    susp_next[idx] -= accept;
+                    susp_taken[nn] += accept;
+                }
+                if (!open) continue;
+                float speed = sqrtf(u * u + v * v);
+                float k = 0.01f + 0.2f * speed * w;
+                float fd = rmin(k * dt / (cell * cell), 0.1f);
+                const long nb[4] = {i + 1 < res ? (long)(idx + 1) : -1, i > 0 ? (long)(idx - 1) : -1,
+                                    j + 1 < res ? (long)(idx + res) : -1, j > 0 ? (long)(idx - res) : -1};
+                for (long nl : nb) {
+                    if (nl < 0) continue;
+                    usize nn = (usize)nl;
+                    float wr = water[nn];
+                    if (!finite(wr) || wr < 1.0e-5f) continue;
+                    float cn = susp[nn] / wr;
+                    if (!(c > cn)) continue;
+                    float give = fd * (c - cn) * rmin(w, wr);
+                    float have = susp[nn] + susp_taken[nn];
+                    float accept = rmin(give, rmax(wr - have, 0.0f));
+                    if (accept <= 1.0e-12f) continue;
+                    susp_next[idx] -= accept;
+                    susp_taken[nn] += accept;
+                }
+            }
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) susp_next[j * res + i] += susp_taken[j * res + i];
+        uint32_t capped = 0;
+        for (usize j = j0; j <= j1; ++j)
+            for (usize i = i0; i <= i1; ++i) {
+                usize idx = j * res + i;
+                float sv = susp_next[idx];
+                if (!finite(sv) || sv <= 0.0f) { susp_next[idx] = 0.0f; continue; }
+                float w = water[idx];
+                if (!finite(w) || w < 1.0e-5f) {
+                    settled_suspended_m3 += sv * area;
+                    settled_suspended64 += (double)(sv * area);
+                    sv = 0.0f;
+                } else if (sv > w) {
+                    float excess = sv - w;
+                    settled_suspended_m3 += excess * area;
+                    settled_suspended64 += (double)(excess * area);
+                    if (excess > 1.0e-5f) capped += 1;
+                    sv = w;
+                }
+                susp_next[idx] = sv;
+            }
+        last_susp_capped += capped;
+        std::swap(susp, susp_next);
     }
 
     // Inflow strip: one coarse row, water added as depth, booked as opened volume.
@@ -2804,7 +3438,8 @@ void oracle_core_ledger(void* cp, float* out5, double* out64) {
 static std::vector<float>* core_field(Core& C, int which) {
     switch (which) {
         case 0: return &C.water; case 1: return &C.slurry; case 2: return &C.uw; case 3: return &C.vw;
-        case 4: return &C.us; case 5: return &C.vs; case 6: return &C.bed; default: return &C.moisture;
+        case 4: return &C.us; case 5: return &C.vs; case 6: return &C.bed; case 8: return &C.foam;
+        case 9: return &C.turbid; case 10: return &C.susp; default: return &C.moisture;
     }
 }
 void oracle_core_get(void* cp, int which, float* dst) {
@@ -2818,12 +3453,18 @@ void oracle_core_set(void* cp, int which, const float* src) {
     memcpy(f->data(), src, f->size() * sizeof(float));
 }
 void oracle_core_get_grain(void* cp, uint8_t* dst) { Core& C = *(Core*)cp; memcpy(dst, C.grain.data(), C.grain.size()); }
-// src/render_contract.rs:457-496 film/flow via coarse_cell (:6998-7035). Tracers are
-// not part of the sheet path, so turbidity is 0.
+// src/render_contract.rs:457-496 film/flow via coarse_cell (:6998-7035), the
+// turbidity channel from the suspended and stirred columns (:7024-7032).
 void oracle_core_publish(void* cp, float* film, float* flow) {
     Core& C = *(Core*)cp;
     for (usize idx = 0; idx < C.res * C.res; ++idx) {
         float water_m = finite0(C.water[idx]), slurry_m = finite0(C.slurry[idx]);
+        float turbidity = water_m < 1.0e-5f
+                              ? 0.0f
+                              : rclamp((rmax(finite0(C.susp[idx]), 0.0f) + rmax(finite0(C.turbid[idx]), 0.0f)) /
+                                           water_m,
+                                       0.0f, 1.0f);
+        float turb = (!finite(water_m) || water_m < 1.0e-5f) ? 0.0f : rclamp(finite0(turbidity), 0.0f, 1.0f);
         float fl = water_m + slurry_m;
         float u = 0.0f, v = 0.0f;
         if (!(fl < 1.0e-5f)) {
@@ -2835,8 +3476,48 @@ void oracle_core_publish(void* cp, float* film, float* flow) {
         float speed = dry ? 0.0f : finite0(sqrtf(u * u + v * v));
         film[2 * idx] = finite0(water_m);
         film[2 * idx + 1] = finite0(slurry_m);
-        flow[4 * idx] = u; flow[4 * idx + 1] = v; flow[4 * idx + 2] = speed; flow[4 * idx + 3] = 0.0f;
+        flow[4 * idx] = u; flow[4 * idx + 1] = v; flow[4 * idx + 2] = speed; flow[4 * idx + 3] = turb;
     }
+}
+// src/fluid_core.rs:5097-5099 set_turbidity_enabled.
+void oracle_core_set_turbidity(void* cp, int on) { ((Core*)cp)->turbidity_enabled = on != 0; }
+// RiverReach::inlet_turbidity (src/fluid_core.rs:319).
+void oracle_core_set_reach_turbidity(void* cp, float c) { ((Core*)cp)->reach_inlet_turbidity = c; }
+// The tracer books (src/fluid_core.rs:6171-6195 silt book, :6821-6884 the
+// suspended part of the ledger), out8 in f32 as the reference keeps them and
+// out64 the same terms in FP64: [0] suspended in the column, [1] settled
+// suspended, [2] parked suspended, [3] entrained, [4] stirred silt in the
+// column, [5] settled silt, [6] stirred, [7] parked silt.
+void oracle_core_tracer_books(void* cp, float* out8, double* out64) {
+    Core& C = *(Core*)cp;
+    const float area = C.cfg.cell * C.cfg.cell;
+    float susp_sum = -0.0f, turbid_sum = 0.0f;
+    double susp64 = 0.0, turbid64 = 0.0;
+    for (usize k = 0; k < C.res * C.res; ++k) {
+        susp_sum += rmax(C.susp[k], 0.0f);
+        susp64 += (double)rmax(C.susp[k], 0.0f);
+        float t = finite(C.turbid[k]) ? rmax(C.turbid[k], 0.0f) : 0.0f;
+        turbid_sum = turbid_sum + t;
+        turbid64 += (double)t;
+    }
+    float fsusp = 0.0f, fturb = 0.0f;
+    double fsusp64 = 0.0, fturb64 = 0.0;
+    for (const auto& kv : C.parked) {
+        fsusp += kv.second.susp * area;
+        fsusp64 += (double)kv.second.susp * (double)area;
+        if (finite(kv.second.turbid)) {
+            fturb += rmax(kv.second.turbid, 0.0f) * area;
+            fturb64 += (double)rmax(kv.second.turbid, 0.0f) * (double)area;
+        }
+    }
+    out8[0] = susp_sum * area; out64[0] = susp64 * (double)area;
+    out8[1] = C.settled_suspended_m3; out64[1] = C.settled_suspended64;
+    out8[2] = fsusp; out64[2] = fsusp64;
+    out8[3] = C.entrained_m3; out64[3] = C.entrained64;
+    out8[4] = turbid_sum * area; out64[4] = turbid64 * (double)area;
+    out8[5] = C.turbid_settled_m3; out64[5] = C.turbid_settled64;
+    out8[6] = C.stirred_m3; out64[6] = C.stirred64;
+    out8[7] = fturb; out64[7] = fturb64;
 }
 void oracle_core_set_fine_pace(void* cp, int pace) { ((Core*)cp)->fine_pace = std::min(pace, 3); }
 void oracle_core_set_fine_sub_cap(void* cp, float cap) { ((Core*)cp)->fine_sub_cap = finite(cap) ? rclamp(cap, 1.0f, 8.0f) : 8.0f; }

@@ -92,12 +92,16 @@ int oracle_core_step(void* core, float dt, oracle_spray* out, int cap);
 // out[0..4]: water_m3, slurry_m3, frozen_water_m3, frozen_slurry_m3, spray_m3,
 // in f32 as the reference sums them; out64[0..2]: water, slurry in f64.
 void oracle_core_ledger(void* core, float* out5, double* out64_2);
-// which: 0 water 1 slurry 2 uw 3 vw 4 us 5 vs 6 bed 7 moisture; dst res*res floats.
+// which: 0 water 1 slurry 2 uw 3 vw 4 us 5 vs 6 bed 7 moisture 8 foam 9 turbid
+// (stirred silt) 10 susp (suspended solids); dst res*res floats.
 void oracle_core_get(void* core, int which, float* dst);
 void oracle_core_set(void* core, int which, const float* src);
 void oracle_core_get_grain(void* core, uint8_t* dst);
 void oracle_core_publish(void* core, float* film, float* flow);
 void oracle_core_set_fine_pace(void* core, int pace);
+void oracle_core_set_turbidity(void* core, int on);
+void oracle_core_set_reach_turbidity(void* core, float inlet_turbidity);
+void oracle_core_tracer_books(void* core, float* out8, double* out64_8);
 void oracle_core_set_fine_sub_cap(void* core, float cap);
 void oracle_core_set_near_field(void* core, int on);
 int oracle_core_near_tiles(void* core);
