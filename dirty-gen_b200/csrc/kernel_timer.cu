@@ -60,7 +60,10 @@ std::string kernel_name(const void* k) {
     char* dem = abi::__cxa_demangle(raw, nullptr, nullptr, &st);
     std::string out = (st == 0 && dem) ? dem : raw;
     std::free(dem);
-    // Keep the qualified name, drop the argument list.
+    // Keep the qualified name, drop the argument list (and anonymous
+    // namespaces, whose parentheses would end the name early).
+    const std::string anon = "(anonymous namespace)::";
+    for (size_t at = out.find(anon); at != std::string::npos; at = out.find(anon)) out.erase(at, anon.size());
     const size_t paren = out.find('(');
     if (paren != std::string::npos) out.resize(paren);
     return out;

@@ -71,6 +71,7 @@ __global__ void k_reach(fine::SheetView W, ReachStep r, float* bank, double* boo
     const float area = W.cell * W.cell;
     float b = *bank;
     double moved = 0.0;
+    double inflow_m3 = 0.0;
     auto at = [&](int along, int cross) -> size_t {
         return r.along_z ? (size_t)along * res + cross : (size_t)cross * res + along;
     };
@@ -114,7 +115,18 @@ __global__ void k_reach(fine::SheetView W, ReachStep r, float* bank, double* boo
                 W.u[0][idx] = speed * r.dx;
                 W.v[0][idx] = speed * r.dz;
                 fine::mark_tile(W, 0, cell_i(idx), cell_j(idx));
+                if (r.inflow_c > 0.0f) {
+                    // The water arrives carrying its load (src/fluid_core.rs:7746-7755).
+                    const float w = W.h[0][idx];
+                    const float want = r.inflow_c * w;
+                    const float have = r.susp[idx];
+                    if (w >= 1.0e-5f && isfinite(have) && have < want) {
+                        r.susp[idx] = want;
+                        inflow_m3 += (double)((want - have) * area);
+                    }
+                }
             }
+    if (inflow_m3 != 0.0) *r.entrained += inflow_m3;
     *bank = b;
     if (moved != 0.0) {
         if (W.d_acc) W.d_acc[0] += moved;

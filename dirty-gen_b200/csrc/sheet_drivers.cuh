@@ -24,6 +24,9 @@ struct ReachStep {
     int c0, c1, rows;           // cross band and end rows on the window
     float dx, dz;               // downstream unit vector
     float inlet_eta, outlet_eta, inlet_speed;
+    float inflow_c;             // the inlet's suspended load as a fraction of the water column (0: none)
+    float* susp;                // the suspended-solids plane (when inflow_c > 0)
+    double* entrained;          // its FP64 book of solids that entered the window
 };
 
 cudaError_t wave_step(const fine::SheetView& W, const WaveStep& w, cudaStream_t st);

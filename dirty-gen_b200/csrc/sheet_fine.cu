@@ -142,7 +142,9 @@ struct Impl {
     SprayRec* spray = nullptr;
     double* d_books = nullptr;        // [0] spray m3, [1] parked water m3, [2] parked slurry m3, [3] dry cut m3,
                                       // [4] river reach bank m3 (FP64 twin of the reference's f32 bank),
-                                      // [5] eroded bed m3, [6] transport rounding m3
+                                      // [5] eroded bed m3, [6] transport rounding m3, [7..10] the
+                                      // tracers' entrained, settled suspended, stirred and settled silt,
+                                      // [11] parked suspended, [12] parked silt
     double* h_books = nullptr;
     int* h_counters = nullptr;
 };
@@ -1539,7 +1541,7 @@ int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, doubl
                  double* reach, double* eroded, double* round) {
     Impl& M = I(P);
     SheetView W = view_of(s);
-    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 7 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 16 * sizeof(double), cudaMemcpyDeviceToHost, W.st));
     FCK(cudaStreamSynchronize(W.st));
     *spray = M.h_books[0];
     *park_w = M.h_books[1];
@@ -1550,6 +1552,8 @@ int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, doubl
     if (round) *round = M.h_books[6];
     return SILT_OK;
 }
+
+const double* books_host(Patches& P) { return I(P).h_books; }
 
 int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, int patch, float* host,
                 float* origin2) {
@@ -1626,9 +1630,9 @@ int create(Patches& P, const silt_cfg& cfg, int res, cudaStream_t st) {
     FCK(cudaMalloc(&M->free_stack, NEAR_POOL * sizeof(int)));
     FCK(cudaMalloc(&M->counters, 8 * sizeof(int)));
     FCK(cudaMalloc(&M->spray, SPRAY_CAP * sizeof(SprayRec)));
-    FCK(cudaMalloc(&M->d_books, 8 * sizeof(double)));
-    FCK(cudaMemsetAsync(M->d_books, 0, 8 * sizeof(double), st));
-    FCK(cudaMallocHost(&M->h_books, 8 * sizeof(double)));
+    FCK(cudaMalloc(&M->d_books, 16 * sizeof(double)));
+    FCK(cudaMemsetAsync(M->d_books, 0, 16 * sizeof(double), st));
+    FCK(cudaMallocHost(&M->h_books, 16 * sizeof(double)));
     FCK(cudaMallocHost(&M->h_counters, 8 * sizeof(int)));
     ::silt::launch_dep(k_init_pool, dim3(launch_blocks(std::max<size_t>(n, NEAR_POOL))), dim3(256), 0, st, M->meta, M->free_stack, M->slot_map, n,
                                                                                M->counters);

@@ -109,6 +109,8 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
 // FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr,
                  double* reach = nullptr, double* eroded = nullptr, double* round = nullptr);
+// The host copy of all 16 books as the last ledger_parts read them.
+const double* books_host(Patches& P);
 // Device address of the books: [0] spray, [1] parked water, [2] parked slurry,
 // [3] dry cut, [4] river reach bank, [5] bed scoured into the slurry (m^3, FP64).
 double* books(Patches& P);

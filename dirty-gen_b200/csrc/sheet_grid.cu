@@ -539,13 +539,48 @@ __device__ __forceinline__ bool force_entry(const LayerParams& P, const TileFlag
 // A list entry that steps its tile (neither a zero fill nor an identity copy).
 __device__ __forceinline__ bool entry_steps(int e) { return (e & (ENTRY_ZERO | ENTRY_COPY)) == 0; }
 
-// Sweep-form pass over one list entry: the fixed-point pass of a stepped tile
-// of a sweeping layer with confinement on. Block-uniform result.
-__device__ __forceinline__ bool sweep_entry(const LayerParams& P, const TileFlags& tf, int e, float* sm) {
+// Sweep-form pass `pass` over one list entry: the fixed-point pass of a
+// stepped tile of a sweeping layer with confinement on. After the first
+// pass a tile is solved again only when some tile of its 3 x 3
+// neighbourhood (itself included) changed since the previous pass began: it
+// is otherwise still at the fixed point of the values around it. Returns
+// whether the tile changed (block-uniform) and stamps it when it did.
+__device__ __forceinline__ bool sweep_entry(const LayerParams& P, const TileFlags& tf, int e, float* sm, int pass,
+                                            unsigned int epoch) {
     if (!entry_steps(e) || !P.sweep || !(P.vort > 0.0f)) return false;
-    const int t = e & ENTRY_TILE;
-    const int tx0 = (t % tf.tiles_x) * FT, ty0 = (t / tf.tiles_x) * FT;
-    return tile_interior(P.res, tx0, ty0) ? sweep_tile<false>(P, sm, tx0, ty0) : sweep_tile<true>(P, sm, tx0, ty0);
+    const int l = e >> 30, t = e & ENTRY_TILE;
+    const int nt = tf.tiles_x * tf.tiles_x;
+    const int ti = t % tf.tiles_x, tj = t / tf.tiles_x;
+    unsigned int* stamp = tf.stamp ? tf.stamp + (size_t)l * nt : nullptr;
+    if (pass > 0 && stamp) {
+        __shared__ int again;
+        if (threadIdx.x == 0) {
+            const unsigned int since = epoch * 256u + (unsigned int)pass;
+            int a = 0;
+            for (int dj = -1; dj <= 1 && !a; ++dj)
+                for (int di = -1; di <= 1; ++di) {
+                    const int x = ti + di, y = tj + dj;
+                    if (x < 0 || y < 0 || x >= tf.tiles_x || y >= tf.tiles_x) continue;
+                    if (*(volatile unsigned int*)&stamp[y * tf.tiles_x + x] >= since) {
+                        a = 1;
+                        break;
+                    }
+                }
+            again = a;
+        }
+        __syncthreads();
+        const int go = again;
+        __syncthreads();
+        if (!go) return false;
+    }
+    const int tx0 = ti * FT, ty0 = tj * FT;
+    const bool changed =
+        tile_interior(P.res, tx0, ty0) ? sweep_tile<false>(P, sm, tx0, ty0) : sweep_tile<true>(P, sm, tx0, ty0);
+    if (changed && stamp && threadIdx.x == 0) {
+        __threadfence();
+        stamp[t] = epoch * 256u + (unsigned int)pass + 1u;
+    }
+    return changed;
 }
 
 // Sweep-form projection of one list entry. Returns true when it used shared memory.
@@ -611,7 +646,7 @@ __device__ int sweep_fixed_point(SweepState* S, unsigned int& target, int n, Vis
     __shared__ unsigned int verdict;
     for (int pass = 0; pass < SWEEP_MAX_PASSES; ++pass) {
         bool changed = false;
-        for (int k = blockIdx.x; k < n; k += gridDim.x) changed |= visit(k);
+        for (int k = blockIdx.x; k < n; k += gridDim.x) changed |= visit(k, pass);
         if (threadIdx.x == 0) {
             if (changed) atomicOr(&S->flag[pass % 3], 1u);
             // The next pass's verdict starts clear; the one cleared here was
@@ -664,6 +699,7 @@ __device__ __forceinline__ bool layer_steps(const SubstepCount& sc, int l) {
 __device__ __forceinline__ void sweep_stats(SweepState* S, int passes) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&S->launches, 1u);
+        atomicAdd(&S->epoch, 1u);  // every CTA read the epoch at the launch's start, two barriers ago
         atomicMax(&S->passes_max, (unsigned int)(passes > 0 ? passes : SWEEP_MAX_PASSES));
         if (passes == 0) atomicAdd(&S->fallbacks, 1u);
     }
@@ -678,6 +714,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force_sweep(ForceLaunch L) {
     if (threadIdx.x < 2) Ps[threadIdx.x] = force_params(L.lay[threadIdx.x], L.sc, threadIdx.x, blockIdx.x == 0);
     __syncthreads();
     SweepState* S = L.tf.sweep;
+    const unsigned int epoch = ld_acquire_u32(&S->epoch);
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
@@ -685,8 +722,10 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force_sweep(ForceLaunch L) {
     }
     unsigned int target = 0;
     if (!grid_barrier(S, target)) return;
-    const int passes =
-        sweep_fixed_point(S, target, n, [&](int k) { const int e = L.tf.list[k]; return sweep_entry(Ps[e >> 30], L.tf, e, sm); });
+    const int passes = sweep_fixed_point(S, target, n, [&](int k, int pass) {
+        const int e = L.tf.list[k];
+        return sweep_entry(Ps[e >> 30], L.tf, e, sm, pass, epoch);
+    });
     if (passes < 0) return;
     if (passes == 0) {
         if (threadIdx.x == 0 && blockIdx.x < 2) {
@@ -1216,10 +1255,11 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_batch_force_sweep(const Windo
         __syncthreads();  // the parameters and shared memory are reused by the next entry
     }
     unsigned int target = 0;
+    const unsigned int epoch = ld_acquire_u32(&S->epoch);
     if (!grid_barrier(S, target)) return;
-    const int passes = sweep_fixed_point(S, target, n, [&](int k) {
+    const int passes = sweep_fixed_point(S, target, n, [&](int k, int pass) {
         const int e = fetch(k, false);
-        const bool r = sweep_entry(Ps, Tf, e, sm);
+        const bool r = sweep_entry(Ps, Tf, e, sm, pass, epoch);
         __syncthreads();
         return r;
     });

@@ -60,6 +60,7 @@ struct SweepState {
     unsigned int passes_max;  // most passes one launch needed
     unsigned int fallbacks;   // launches that ran the sequential sweep after the pass limit
     unsigned int launches;    // sweep launches
+    unsigned int epoch;       // launches ever (never reset): the base of the tiles' change stamps
 };
 
 // Active-tile bookkeeping of the grid engine, per layer and ping-pong buffer,
@@ -76,6 +77,10 @@ struct TileFlags {
     unsigned long long* stepped;  // per layer: running total of tiles stepped (may be nullptr)
     int32_t tiles_x;
     SweepState* sweep;       // cleared by the tile-list kernel (may be nullptr)
+    // Per layer and tile (stamp[l * tiles_x^2 + t]): when the sweep last
+    // changed the tile, as epoch * 256 + pass + 1. A later pass solves a tile
+    // again only when its 3 x 3 neighbourhood changed since it was solved.
+    unsigned int* stamp;
 };
 
 // Substep count decided on the device (src/fluid_core.rs:1715-1744). The

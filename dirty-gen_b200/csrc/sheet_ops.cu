@@ -1,6 +1,7 @@
 // Per-cell kernels around the sheet step: seeding (the reference's closure
 // writes), the render-contract publish, map export, the FP64 ledger sum and
 // the non-finite count. Each follows the reference function it names.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -129,7 +130,7 @@ __global__ void k_inflow(float* water, float* uw, float* vw, int cut_pending, in
 // coarse_cell (src/fluid_core.rs:6998-7035) feeding render_contract film/flow
 // (src/render_contract.rs:457-496). Tracers are off the sheet path: turbidity 0.
 __global__ void k_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
-                          const float* vs, float* film, float* flow, size_t n) {
+                          const float* vs, const float* susp, const float* turbid, float* film, float* flow, size_t n) {
     ::silt::dep_wait();
     GRID_STRIDE(i, n) {
         float water_m = finite0(water[i]), slurry_m = finite0(slurry[i]);
@@ -142,8 +143,15 @@ __global__ void k_publish(const float* water, const float* slurry, const float* 
         bool dry = !finite_f(water_m) || !finite_f(slurry_m) || water_m + slurry_m < 1.0e-5f;
         if (dry) { u = 0.0f; v = 0.0f; }
         float speed = dry ? 0.0f : finite0(sqrtf(u * u + v * v));
+        // coarse_cell's turbidity (src/fluid_core.rs:7024-7032): suspended load
+        // and stirred silt over the water column; the publish clamps it again.
+        const float turbidity =
+            water_m < 1.0e-5f
+                ? 0.0f
+                : rclamp((fmaxf(finite0(susp[i]), 0.0f) + fmaxf(finite0(turbid[i]), 0.0f)) / water_m, 0.0f, 1.0f);
+        const float turb = (!finite_f(water_m) || water_m < 1.0e-5f) ? 0.0f : rclamp(finite0(turbidity), 0.0f, 1.0f);
         reinterpret_cast<float2*>(film)[i] = make_float2(finite0(water_m), finite0(slurry_m));
-        reinterpret_cast<float4*>(flow)[i] = make_float4(u, v, speed, 0.0f);
+        reinterpret_cast<float4*>(flow)[i] = make_float4(u, v, speed, turb);
     }
 }
 
@@ -361,8 +369,10 @@ cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int r
     return cudaGetLastError();
 }
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
-                       const float* vs, float* film, float* flow, size_t n, cudaStream_t st) {
-    ::silt::launch_dep(k_publish, dim3(blocks_for(n)), dim3(256), 0, st, water, slurry, uw, vw, us, vs, film, flow, n);
+                       const float* vs, const float* susp, const float* turbid, float* film, float* flow, size_t n,
+                       cudaStream_t st) {
+    ::silt::launch_dep(k_publish, dim3(blocks_for(n)), dim3(256), 0, st, water, slurry, uw, vw, us, vs, susp, turbid,
+                       film, flow, n);
     ::silt::count_launch();
     return cudaGetLastError();
 }
@@ -385,14 +395,46 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
     ::silt::dep_wait();
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n) return;
-    out[8 * w + 0] = acc[w][0];
-    out[8 * w + 1] = acc[w][1];
-    out[8 * w + 2] = books[w][0];
-    out[8 * w + 3] = books[w][1];
-    out[8 * w + 4] = books[w][2];
-    out[8 * w + 5] = books[w][3];
-    out[8 * w + 6] = books[w][4];
-    out[8 * w + 7] = books[w][6];
+    double* o = out + 16 * (size_t)w;
+    o[0] = acc[w][0];
+    o[1] = acc[w][1];
+    o[2] = books[w][0];
+    o[3] = books[w][1];
+    o[4] = books[w][2];
+    o[5] = books[w][3];
+    o[6] = books[w][4];
+    o[7] = books[w][6];
+    for (int k = 0; k < 6; ++k) o[8 + k] = books[w][7 + k];  // the tracers' books
+}
+// Every window's suspended and silt column sums (FP64 of the clamped cells)
+// into out[16 w + 14], [16 w + 15], which start at zero.
+__global__ void k_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, double* out) {
+    ::silt::dep_wait();
+    const int w = blockIdx.y;
+    const float* a = susp[w];
+    const float* b = turbid[w];
+    const size_t n = (size_t)cells[w];
+    double sa = 0.0, sb = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        sa += (double)fmaxf(a[i], 0.0f);
+        sb += (double)fmaxf(b[i], 0.0f);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_down_sync(0xffffffffu, sa, o);
+        sb += __shfl_down_sync(0xffffffffu, sb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (sa != 0.0) atomicAdd(out + 16 * (size_t)w + 14, sa);
+        if (sb != 0.0) atomicAdd(out + 16 * (size_t)w + 15, sb);
+    }
+}
+cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, int n, double* out,
+                           cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int per = std::max(1, std::min(64, 2368 / n));
+    ::silt::launch_dep(k_sum_tracers, dim3(per, n), dim3(256), 0, st, susp, turbid, cells, out);
+    ::silt::count_launch();
+    return cudaGetLastError();
 }
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st) {

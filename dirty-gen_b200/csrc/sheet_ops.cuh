@@ -23,13 +23,17 @@ cudaError_t op_read_substrate(const float* bed_in, const float* moist_in, const 
 cudaError_t op_inflow(float* water, float* uw, float* vw, int cut_pending, int res, int j, int i0, int i1, float add,
                       int tiles_x, uint8_t* t_wet, uint8_t* t_zuv, uint8_t* t_zh, cudaStream_t st);
 cudaError_t op_publish(const float* water, const float* slurry, const float* uw, const float* vw, const float* us,
-                       const float* vs, float* film, float* flow, size_t n, cudaStream_t st);
+                       const float* vs, const float* susp, const float* turbid, float* film, float* flow, size_t n,
+                       cudaStream_t st);
 cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
                       const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
                       float* moisture, size_t n, cudaStream_t st);
 cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st);
-// out[8 w + 0..1] = acc[w][0..1] (depth sums), out[8 w + 2..6] = books[w][0..4],
-// out[8 w + 7] = books[w][6] (the transport rounding book).
+// Every window's suspended and silt column sums into out[16 w + 14, 15] (zeroed first).
+cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, int n, double* out,
+                           cudaStream_t st);
+// out[16 w + 0..1] = acc[w][0..1] (depth sums), out[16 w + 2..6] = books[w][0..4],
+// out[16 w + 7] = books[w][6] (the transport rounding book), out[16 w + 8..13] = books[w][7..12] (tracers).
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st);
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st);

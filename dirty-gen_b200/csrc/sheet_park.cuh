@@ -16,7 +16,8 @@ namespace park {
 
 constexpr unsigned long long EMPTY = ~0ull;
 constexpr unsigned long long TOMB = ~0ull - 1ull;
-constexpr int NVAL = 8;  // water, slurry, uw, vw, us, vs, moisture, unused
+// water, slurry, uw, vw, us, vs, moisture, unused, foam, stirred silt, suspended solids, unused
+constexpr int NVAL = 12;
 
 struct Table {
     unsigned long long* keys = nullptr;
@@ -101,10 +102,20 @@ struct Planes {
     float* u_out[2];
     float* v_out[2];
     float* moisture_out;
+    // The tracers (src/fluid_core.rs:4763-4782 Parked: foam, turbid, susp),
+    // and the planes a scroll writes them to; track_susp is the turbidity
+    // switch (a scroll carries the suspended load only with it on).
+    float* foam;
+    float* turbid;
+    float* susp;
+    float* foam_out;
+    float* turbid_out;
+    float* susp_out;
+    int track_susp;
     int res;
     float cell;
     float ambient;
-    double* books;  // [1] parked water m^3, [2] parked slurry m^3
+    double* books;  // [1] parked water m^3, [2] parked slurry m^3, [11] parked suspended, [12] parked silt
 };
 
 // Parks the cells of the window at origin (ox, oz) that leave it when its

@@ -33,6 +33,7 @@
 #include "sheet_ops.cuh"
 #include "sheet_walls.cuh"
 #include "sheet_park.cuh"
+#include "sheet_tracers.cuh"
 #include "sheet_window.cuh"
 
 namespace {
@@ -90,7 +91,7 @@ struct silt_sheet {
     const float** d_planes = nullptr;
     double* h_acc = nullptr;      // pinned mirror of d_acc
     // d_u32: [0, 2) speed bits, [2] substep overflow, [4, 8) tiles stepped
-    // (two u64), [SWEEP_AT, SWEEP_AT + 8) the sweep launch state.
+    // (two u64), [SWEEP_AT, SWEEP_AT + 9) the sweep launch state.
     static constexpr int SWEEP_AT = 8;
     unsigned int* h_flags = nullptr;  // pinned: d_u32[2, 16) as last read (FLAG_* below)
     bool cut_pending = false;
@@ -140,6 +141,7 @@ struct silt_sheet {
     // iterate planes (2 layers x u, v) with the launch state in d_u32.
     int confine = SILT_CONFINE_SWEEP;
     float* sweep_planes = nullptr;
+    unsigned int* sweep_stamp = nullptr;  // the sweep's per-tile change stamps (2 layers)
     silt::SweepState* sweep_state() { return reinterpret_cast<silt::SweepState*>(d_u32 + SWEEP_AT); }
 
     // Open-water mode of the water sheet (FluidCore::set_open_water,
@@ -148,7 +150,13 @@ struct silt_sheet {
     float ow_mobility = 0.0f, ow_manning = 0.0f, ow_eddy = 0.0f;
     float surface_diffusion = 0.0f;
     float* ow_scratch = nullptr;   // 2 n floats for the drivers' snapshots
-    bool turbidity = false;        // FluidCore::set_turbidity_enabled (tracers are off this path)
+    // FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097, on by
+    // default :4994): the wake's suspended load and its transport.
+    bool turbidity = true;
+    // The tracers on the coarse window: foam, stirred silt, suspended solids.
+    void* tr_mem = nullptr;
+    silt::tracers::Planes tr;
+    silt::tracers::Runner tr_run;
     float center[2] = {0.0f, 0.0f};  // the chase point (set_center / recenter)
     bool reach_on = false;           // FluidCore::set_river_reach
     silt_river_reach reach;
@@ -216,6 +224,25 @@ int refresh_material(silt_sheet* s) {
     CK(silt::launch_material(s->grain, s->moisture, s->mat, s->mat + s->n, s->mat + 2 * s->n, s->n, s->st));
     s->mat_dirty = false;
     return SILT_OK;
+}
+
+// The coarse window as the tracers see it (the current planes).
+silt::tracers::Window tracer_window(silt_sheet* s, const std::vector<silt_tire_push>& ps) {
+    silt::tracers::Window w;
+    w.S.water = s->H(0);
+    w.S.slurry = s->H(1);
+    w.S.uw = s->U(0);
+    w.S.vw = s->V(0);
+    w.S.res = s->res;
+    w.S.cell = s->cfg.cell;
+    w.S.ox = s->origin[0];
+    w.S.oz = s->origin[1];
+    w.S.cut_pending = s->cut_pending ? 1 : 0;
+    w.S.surface_driven = (s->wave_on || s->reach_on) ? 1 : 0;
+    w.T = s->tr;
+    w.push = ps.empty() ? nullptr : ps.data();
+    w.npush = (int)ps.size();
+    return w;
 }
 
 // Host plan of one sheet's coarse pair for one step: how many substeps to
@@ -548,11 +575,11 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_acc, 8 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 16 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 24 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_flags, 16 * sizeof(unsigned int));
-    if (e == cudaSuccess) e = cudaMemset(s->d_u32, 0, 16 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_u32, 0, 24 * sizeof(unsigned int));
     if (e == cudaSuccess) memset(s->h_flags, 0, 16 * sizeof(unsigned int));
     s->engine = cfg->engine == SILT_ENGINE_WINDOW || cfg->engine == SILT_ENGINE_GRID
                     ? cfg->engine
@@ -587,6 +614,9 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         }
         if (e == cudaSuccess) e = cudaMalloc(&s->sweep_planes, 4 * nb);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->sweep_planes, 0, 4 * nb, s->st);
+        if (e == cudaSuccess) e = cudaMalloc(&s->sweep_stamp, 2 * nt * sizeof(unsigned int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->sweep_stamp, 0, 2 * nt * sizeof(unsigned int), s->st);
+        s->tf.stamp = s->sweep_stamp;
     }
     if (s->engine == SILT_ENGINE_WINDOW) {
         const size_t wp = 2 * (size_t)silt::window::SCRATCH_PLANES * s->n * sizeof(float);
@@ -615,6 +645,12 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         silt_sheet_destroy(s);
         return rc;
     }
+    e = cudaMalloc(&s->tr_mem, silt::tracers::plane_bytes(s->res));
+    if (e == cudaSuccess) e = silt::tracers::attach(s->tr, s->tr_mem, s->res, silt::fine::books(s->fine) + 7, s->st);
+    if (e != cudaSuccess) {
+        silt_sheet_destroy(s);
+        return e == cudaErrorMemoryAllocation ? SILT_ENOMEM : fail_cuda(e, "allocate tracers");
+    }
     s->div = silt::cell_divisors(cfg->cell, s->st);
     e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) {
@@ -635,6 +671,8 @@ int silt_sheet_destroy(silt_sheet* s) {
     }
     cudaFree(s->ow_scratch);
     cudaFree(s->d_reach_bank);
+    s->tr_run.release();
+    cudaFree(s->tr_mem);
     silt::fine::destroy(s->fine);
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
@@ -657,6 +695,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->win_planes);
     cudaFree(s->tile_mem);
     cudaFree(s->sweep_planes);
+    cudaFree(s->sweep_stamp);
     cudaFree(s->d_win_jobs);
     if (s->h_win_jobs) cudaFreeHost(s->h_win_jobs);
     cudaFree(s->d_solids);
@@ -1035,6 +1074,10 @@ int reach_step(silt_sheet* s) {
     r.inlet_eta = s->reach.inlet_eta;
     r.outlet_eta = s->reach.outlet_eta;
     r.inlet_speed = s->reach.inlet_speed_m_s;
+    const float c = s->reach.inlet_turbidity;
+    r.inflow_c = s->turbidity && std::isfinite(c) ? silt::host::rclamp(c, 0.0f, 1.0f) : 0.0f;
+    r.susp = s->tr.susp[0];
+    r.entrained = silt::fine::books(s->fine) + 7;
     CK(silt::drivers::reach_step(silt::fine::view_of(s), r, s->d_reach_bank, silt::fine::books(s->fine), s->st));
     return SILT_OK;
 }
@@ -1108,6 +1151,12 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     std::vector<silt_tire_push> ps;
     silt::fine::StepOut fo;
     int rc;
+    // Lift from the column the tire rolls into, before the sheet shoves it
+    // (entrain_wake, src/fluid_core.rs:6051-6053).
+    if (s->turbidity && !s->pushes.empty()) {
+        const silt::tracers::Window w = tracer_window(s, s->pushes);
+        CK(silt::tracers::entrain(s->tr_run, &w, 1, dt, s->st));
+    }
     // The learned closure reads the state the nested sheets would start from.
     const bool net_on = closure_begin(s);
     silt::closure::FeatureJob F;
@@ -1125,7 +1174,17 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
     if ((rc = scour_step(s, dt))) return rc;
+    {
+        // step_tracers (src/fluid_core.rs:6080), then the reach, then the
+        // suspended load (:6082-6089).
+        const silt::tracers::Window w = tracer_window(s, ps);
+        CK(silt::tracers::step_tracers(s->tr_run, &w, 1, dt, s->st));
+    }
     if ((rc = reach_step(s))) return rc;
+    if (s->turbidity) {
+        const silt::tracers::Window w = tracer_window(s, ps);
+        CK(silt::tracers::step_suspended(s->tr_run, &w, 1, dt, s->st));
+    }
     if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
     if (out || n_out) {
@@ -1246,6 +1305,13 @@ int silt_recenter(silt_sheet* s, float cx, float cz) {
     }
     P.moisture = s->moisture;
     P.moisture_out = s->staging;
+    P.foam = s->tr.foam[0];
+    P.turbid = s->tr.turbid[0];
+    P.susp = s->tr.susp[0];
+    P.foam_out = s->tr.foam[1];
+    P.turbid_out = s->tr.turbid[1];
+    P.susp_out = s->tr.susp[1];
+    P.track_susp = s->turbidity ? 1 : 0;
     P.res = s->res;
     P.cell = s->cfg.cell;
     P.ambient = s->moisture_ambient;
@@ -1256,6 +1322,11 @@ int silt_recenter(silt_sheet* s, float cx, float cz) {
         CK(silt::park::scroll_cells(P, di, dj, s->st));
         s->cur = nx;
         std::swap(s->moisture, s->staging);
+        // The tracers scrolled into their scratch planes; the fields keep their addresses.
+        for (int q = 0; q < 3; ++q) {
+            float* const* pl = q == 0 ? s->tr.foam : (q == 1 ? s->tr.turbid : s->tr.susp);
+            CK(cudaMemcpyAsync(pl[0], pl[1], s->n * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+        }
         for (int l = 0; l < 2; ++l) {
             P.h[l] = s->h[l][s->cur];
             P.u[l] = s->u[l][s->cur];
@@ -1273,6 +1344,7 @@ int silt_recenter(silt_sheet* s, float cx, float cz) {
         CK(silt::park::restore_cells(P, T, s->origin[0], s->origin[1], 0, 0, 1, s->st));
     }
     if ((rc = silt::fine::move_window(s->fine, s, di, dj, scroll))) return rc;
+    CK(silt::tracers::reset_indices(s->tr, s->res, s->st));  // reset_tracer_indices (src/fluid_core.rs:9125, :9225)
     unsigned int used = 0, overflow = 0;
     CK(silt::park::usage(T, &used, &overflow, s->st));
     if (overflow) return fail_cuda(cudaErrorMemoryAllocation, "parked cells: table overflow");
@@ -1519,6 +1591,9 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
         CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
+    CK(cudaMemsetAsync(s->d_acc + 4, 0, 2 * sizeof(double), s->st));
+    CK(silt::op_sum2(s->tr.susp[0], s->tr.turbid[0], s->n, s->d_acc + 4, s->st));
+    CK(cudaMemcpyAsync(s->h_acc + 4, s->d_acc + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0, rounding = 0.0;
     int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded, &rounding);
     if (rc) return rc;
@@ -1538,6 +1613,18 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->cut_m3 = cut;
     out->reach_m3 = reach;
     out->round_m3 = rounding;
+    const double* bk = silt::fine::books_host(s->fine);
+    // The tracers' books take the reference's f32 cell area (cell * cell in
+    // f32), so the standing load and its running books use one area.
+    const double tracer_area = (double)(s->cfg.cell * s->cfg.cell);
+    out->suspended_m3 = s->h_acc[4] * tracer_area;
+    out->settled_suspended_m3 = bk[8];
+    out->frozen_suspended_m3 = bk[11];
+    out->entrained_m3 = bk[7];
+    out->turbid_m3 = s->h_acc[5] * tracer_area;
+    out->turbid_settled_m3 = bk[10];
+    out->frozen_turbid_m3 = bk[12];
+    out->stirred_m3 = bk[9];
     return SILT_OK;
 }
 
@@ -1547,10 +1634,11 @@ int silt_get_coarse_cell(silt_sheet* s, int32_t i, int32_t j, silt_coarse_cell* 
     int rc = flush_cut(s);
     if (rc) return rc;
     size_t idx = (size_t)j * s->res + i;
-    float vals[8];
-    const float* src[8] = {s->bed + idx, s->H(0) + idx, s->H(1) + idx, s->moisture + idx,
-                           s->U(0) + idx, s->V(0) + idx, s->U(1) + idx, s->V(1) + idx};
-    for (int k = 0; k < 8; ++k) CK(cudaMemcpyAsync(&vals[k], src[k], 4, cudaMemcpyDeviceToHost, s->st));
+    float vals[10];
+    const float* src[10] = {s->bed + idx, s->H(0) + idx, s->H(1) + idx, s->moisture + idx,
+                            s->U(0) + idx, s->V(0) + idx, s->U(1) + idx, s->V(1) + idx,
+                            s->tr.susp[0] + idx, s->tr.turbid[0] + idx};
+    for (int k = 0; k < 10; ++k) CK(cudaMemcpyAsync(&vals[k], src[k], 4, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     using silt::host::finite0;
     float water_m = finite0(vals[1]), slurry_m = finite0(vals[2]);
@@ -1568,6 +1656,12 @@ int silt_get_coarse_cell(silt_sheet* s, int32_t i, int32_t j, silt_coarse_cell* 
     out->moisture = finite0(vals[3]);
     out->u = u;
     out->v = v;
+    // Suspended load plus stirred silt over the water column (:7024-7032).
+    out->turbidity = water_m < 1.0e-5f
+                         ? 0.0f
+                         : silt::host::rclamp((std::fmax(finite0(vals[8]), 0.0f) + std::fmax(finite0(vals[9]), 0.0f)) /
+                                                  water_m,
+                                              0.0f, 1.0f);
     return SILT_OK;
 }
 
@@ -1598,7 +1692,8 @@ int silt_publish_film_flow_device(silt_sheet* s, float* d_film, float* d_flow) {
     if (!s || !d_film || !d_flow) return fail_arg("publish");
     int rc = flush_cut(s);
     if (rc) return rc;
-    CK(silt::op_publish(s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), d_film, d_flow, s->n, s->st));
+    CK(silt::op_publish(s->H(0), s->H(1), s->U(0), s->V(0), s->U(1), s->V(1), s->tr.susp[0], s->tr.turbid[0], d_film,
+                        d_flow, s->n, s->st));
     return SILT_OK;
 }
 
@@ -1656,6 +1751,9 @@ static float* plane_of(silt_sheet* s, int which) {
         case 5: return s->V(1);
         case 6: return s->bed;
         case 7: return s->moisture;
+        case 8: return s->tr.foam[0];
+        case 9: return s->tr.turbid[0];
+        case 10: return s->tr.susp[0];
         default: return nullptr;
     }
 }
@@ -1894,7 +1992,10 @@ struct silt_batch {
     silt::closure::Runner* clos = nullptr;
     // Ledger gather: per window the depth sums and the books, one copy back.
     const double** d_ledger_src = nullptr;  // [0, n) depth sums, [n, 2n) books
-    double* d_ledgers = nullptr;            // 8 doubles per window
+    double* d_ledgers = nullptr;            // 16 doubles per window
+    silt::tracers::Runner tr_run;           // the windows' tracer launches
+    const float** d_tr_src = nullptr;       // [0, n) suspended planes, [n, 2n) silt planes
+    int* d_tr_cells = nullptr;              // cells per window
     double* h_ledgers = nullptr;            // pinned
 };
 
@@ -1915,6 +2016,9 @@ int batch_free(silt_batch* b) {
     cudaFree(b->count);
     cudaFree(b->d_ledger_src);
     cudaFree(b->d_ledgers);
+    cudaFree(b->d_tr_src);
+    cudaFree(b->d_tr_cells);
+    b->tr_run.release();
     if (b->h_ledgers) cudaFreeHost(b->h_ledgers);
     for (int k = 0; k < 2; ++k) {
         cudaFree(b->d_ws[k]);
@@ -2103,8 +2207,21 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->count, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemsetAsync(b->count, 0, 2 * sizeof(int), b->st);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 8 * (size_t)n * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 8 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 16 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 16 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_src, 2 * (size_t)n * sizeof(float*));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_cells, (size_t)n * sizeof(int));
+    if (e == cudaSuccess) {
+        std::vector<const float*> src(2 * (size_t)n);
+        std::vector<int> cells(n);
+        for (int w = 0; w < n; ++w) {
+            src[w] = b->sheets[w]->tr.susp[0];
+            src[n + w] = b->sheets[w]->tr.turbid[0];
+            cells[w] = (int)b->sheets[w]->n;
+        }
+        e = cudaMemcpy(b->d_tr_src, src.data(), src.size() * sizeof(float*), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_tr_cells, cells.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) {
         std::vector<const double*> src(2 * (size_t)n);
         for (int w = 0; w < n; ++w) {
@@ -2170,6 +2287,13 @@ int silt_batch_step(silt_batch* b, float dt) {
     const silt_closure* net = nullptr;
     if ((rc = batch_closure_begin(b, net_win, feats, &net))) return rc;
     if (!feats.empty()) CK(b->clos->features(feats, net->net, b->st));
+    {
+        // entrain_wake (src/fluid_core.rs:6051-6053) of every window with tires, one launch.
+        std::vector<silt::tracers::Window> tw;
+        for (silt_sheet* s : b->sheets)
+            if (s->turbidity && !s->pushes.empty()) tw.push_back(tracer_window(s, s->pushes));
+        if (!tw.empty()) CK(silt::tracers::entrain(b->tr_run, tw.data(), (int)tw.size(), dt, b->st));
+    }
     CK(cudaEventRecord(b->ev_start, b->st));  // the workers' streams start after the batch's previous work
     // Each window's tire pushes, inflow and nested-patch planning on the
     // workers (the planning uploads the window's tables on the worker's
@@ -2218,8 +2342,20 @@ int silt_batch_step(silt_batch* b, float dt) {
     for (silt_sheet* s : b->sheets)
         if ((rc = open_water_step(s, dt))) return rc;
     if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
-    for (silt_sheet* s : b->sheets)
-        if ((rc = reach_step(s))) return rc;
+    {
+        // step_tracers of every window in one launch sequence, the reach, then
+        // the suspended load of the windows with turbidity on.
+        std::vector<silt::tracers::Window> tw;
+        tw.reserve(n);
+        for (int w = 0; w < n; ++w) tw.push_back(tracer_window(b->sheets[w], ps[w]));
+        CK(silt::tracers::step_tracers(b->tr_run, tw.data(), n, dt, b->st));
+        for (silt_sheet* s : b->sheets)
+            if ((rc = reach_step(s))) return rc;
+        std::vector<silt::tracers::Window> sw;
+        for (int w = 0; w < n; ++w)
+            if (b->sheets[w]->turbidity) sw.push_back(tracer_window(b->sheets[w], ps[w]));
+        if (!sw.empty()) CK(silt::tracers::step_suspended(b->tr_run, sw.data(), (int)sw.size(), dt, b->st));
+    }
     if (!net_win.empty()) {
         std::vector<silt::closure::ApplyJob> A(net_win.size());
         memset(A.data(), 0, A.size() * sizeof(silt::closure::ApplyJob));
@@ -2258,8 +2394,10 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         }
         return SILT_OK;
     }
+    CK(cudaMemsetAsync(b->d_ledgers, 0, 16 * (size_t)n * sizeof(double), b->st));
+    CK(silt::op_sum_tracers(b->d_tr_src, b->d_tr_src + n, b->d_tr_cells, n, b->d_ledgers, b->st));
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
-    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 8 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 16 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)
         CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
@@ -2267,7 +2405,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         silt_sheet* s = b->sheets[w];
         int rc = check_substep_overflow(s);
         if (rc) return rc;
-        const double* g = b->h_ledgers + 8 * (size_t)w;
+        const double* g = b->h_ledgers + 16 * (size_t)w;
         const double area = (double)s->cfg.cell * (double)s->cfg.cell;
         silt_ledger& L = out[w];
         L.water_m3 = g[0] * area;
@@ -2280,6 +2418,14 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         L.total_m3 = L.water_m3 + L.slurry_m3 + L.frozen_water_m3 + L.frozen_slurry_m3 + L.spray_m3 + L.reach_m3;
         L.cut_m3 = g[5];
         L.round_m3 = g[7];
+        L.entrained_m3 = g[8];
+        L.settled_suspended_m3 = g[9];
+        L.stirred_m3 = g[10];
+        L.turbid_settled_m3 = g[11];
+        L.frozen_suspended_m3 = g[12];
+        L.frozen_turbid_m3 = g[13];
+        L.suspended_m3 = g[14] * (double)(s->cfg.cell * s->cfg.cell);  // the tracers' f32 cell area
+        L.turbid_m3 = g[15] * (double)(s->cfg.cell * s->cfg.cell);
     }
     return SILT_OK;
 }

@@ -1,0 +1,1276 @@
+// The sheet's tracers on the coarse window: foam, stirred silt (`turbid`)
+// and wheel-lifted suspended solids (`susp`), as x3-team/Dirty-gen steps them
+// (src/fluid_core.rs:6210-6739 step_tracers and its parts, :8758-8815
+// entrain_wake, :8817-9002 advect_suspended).
+//
+// The reference walks index lists and applies each update in place, in order.
+// Here every update is a per-cell kernel that reproduces that order:
+//   * a cell's foam and silt sources (every tire in push order, then the
+//     shore, then Froude breaking) run in one thread for that cell;
+//   * the silt transport (flux_thickness) accumulates each donor's removals
+//     in the reference's edge order, so a cell recomputes, for itself and its
+//     four neighbours, the donor sequence up to the edge it shares;
+//   * the suspended transport lets a receiver take from its neighbours in the
+//     reference's raster order of donors (a receiver's room depends on what
+//     earlier donors gave it): receivers write each accepted give into the
+//     donor's slot, then each donor subtracts its slots in its own order.
+// Books that the reference sums in f32 in list order are FP64 sums of the
+// same f32 terms. Index boxes (the live silt span, the visit box) are device
+// reductions, and every kernel reads the step's control flags on the device,
+// so the host never waits.
+#include "sheet_tracers.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "launch_count.cuh"
+#include "sheet_math.cuh"
+
+namespace silt {
+namespace tracers {
+
+namespace {
+
+constexpr float FOAM_EQ = 0.85f;             // src/fluid_core.rs:115
+constexpr float FOAM_TAU_S = 0.35f;          // :117
+constexpr float SUSP_FALL_M_S = 0.004f;      // :122
+constexpr float SILT_COLUMN_CAP_M = 0.028f;  // :124
+
+enum : uint8_t { WET = 1, SHORE = 2, LIVE = 4 };
+
+// Per-step control, in State plus these words (kept after State in memory).
+struct Ctl {
+    int active;     // the tracer step runs at all (wake, live silt or live foam)
+    int go;         // ... and has wet cells or live silt
+    int cbox[4];    // the step's collection box
+    int tspan2[4];  // silt span after the transport
+    int tspan3[4];  // silt span after the sources
+    int mbox[4];    // where wet and shore marks may be set (the last collection box)
+    unsigned int live_foam_prev;
+};
+
+__device__ __forceinline__ Ctl* ctl_of(State* s) { return reinterpret_cast<Ctl*>(s + 1); }
+
+__device__ __forceinline__ float vel(const float* u, const Sheet& S, size_t g) {
+    // The grid engine's pending dry cut: a cell under eps carries no velocity.
+    return (S.cut_pending && S.water[g] < 1.0e-6f) ? 0.0f : u[g];
+}
+
+__device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {  // :9688-9691
+    float t = rclamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+__device__ __forceinline__ float breaking_foam(float speed, float thickness) {  // :9676-9686
+    if (!finite_f(speed) || !finite_f(thickness) || thickness < 0.004f || speed <= 0.05f) return 0.0f;
+    const float froude = speed / sqrtf(9.81f * thickness);
+    return smoothstep_f(0.85f, 1.45f, froude);
+}
+
+__device__ __forceinline__ float sample_foam(const float* src, int res, float x, float z) {  // :9693-9712
+    if (!finite_f(x) || !finite_f(z) || x < 0.0f || z < 0.0f) return 0.0f;
+    const float fx = floorf(x), fz = floorf(z);
+    if (fx >= (float)res || fz >= (float)res) return 0.0f;
+    const int i0 = (int)fx, j0 = (int)fz;
+    const int i1 = min(i0 + 1, res - 1), j1 = min(j0 + 1, res - 1);
+    const float tx = rclamp(x - (float)i0, 0.0f, 1.0f), tz = rclamp(z - (float)j0, 0.0f, 1.0f);
+    const float a = src[(size_t)j0 * res + i0], b = src[(size_t)j0 * res + i1];
+    const float c = src[(size_t)j1 * res + i0], d = src[(size_t)j1 * res + i1];
+    const float v = a + (b - a) * tx + (c - a) * tz + (a - b - c + d) * tx * tz;
+    return finite_f(v) ? rclamp(v, 0.0f, 1.0f) : 0.0f;
+}
+
+__device__ __forceinline__ bool shore_wet_cell(const float* water, int res, int i, int j) {  // :9752-9764
+    if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return false;
+    const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+    for (int k = 0; k < 4; ++k) {
+        const float nh = water[(size_t)(j + dj[k]) * res + (i + di[k])];
+        if (finite_f(nh) && nh < 0.004f) return true;
+    }
+    return false;
+}
+
+// shore_cell (:9826-9872): foam production and silt lift rate of a wet cell.
+__device__ __forceinline__ void shore_cell(const Sheet& S, int i, int j, float& foam, float& rate) {
+    foam = 0.0f;
+    rate = 0.0f;
+    const int res = S.res;
+    if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return;
+    const size_t g = (size_t)j * res + i;
+    const float h = S.water[g];
+    if (!finite_f(h) || h < 0.004f) return;
+    float nx = 0.0f, nz = 0.0f;
+    bool edge = false;
+    const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+    for (int k = 0; k < 4; ++k) {
+        const float nh = S.water[(size_t)(j + dj[k]) * res + (i + di[k])];
+        if (finite_f(nh) && nh < 0.004f) {
+            edge = true;
+            nx += (float)di[k];
+            nz += (float)dj[k];
+        }
+    }
+    if (!edge) return;
+    const float u = vel(S.uw, S, g), v = vel(S.vw, S, g);
+    if (!finite_f(u) || !finite_f(v)) return;
+    const float film = hypot_rn(u, v);
+    const float nlen = fmaxf(hypot_rn(nx, nz), 1.0e-4f);
+    const float into = fmaxf((u * nx + v * nz) / nlen, 0.0f);
+    const float strain = fabsf(vel(S.uw, S, g + 1) - vel(S.uw, S, g - 1)) + fabsf(vel(S.vw, S, g + res) - vel(S.vw, S, g - res));
+    const float shear_v = fmaxf(film, strain);
+    if (shear_v < 0.2f && into < 0.2f) return;
+    const float prod = fmaxf(breaking_foam(fmaxf(shear_v, into), h), smoothstep_f(0.25f, 1.1f, into));
+    foam = prod > 0.02f ? prod : 0.0f;
+    if (h > 0.012f && h < 0.055f && (shear_v > 0.45f || into > 0.4f)) {
+        const float tau = 1000.0f * 0.025f * shear_v * shear_v;
+        if (tau > 3.0f || into > 0.45f) rate = fminf(0.006f * (into + shear_v * 0.35f), 0.01f);
+    }
+}
+
+// add_foam (:6400-6418) on the cell's value.
+__device__ __forceinline__ void add_foam(float& f, float prod, float dt) {
+    if (prod <= 0.0f || !finite_f(prod) || !(dt > 0.0f)) return;
+    const float cur = finite_f(f) ? rclamp(f, 0.0f, FOAM_EQ) : 0.0f;
+    const float room = FOAM_EQ - cur;
+    if (room <= 1.0e-5f) return;
+    const float grown = cur + room * prod * fminf(dt / FOAM_TAU_S, 1.0f);
+    f = finite_f(grown) ? fminf(grown, FOAM_EQ) : 0.0f;
+}
+
+// add_silt (:6699-6710); the stirred volume goes to `book`.
+__device__ __forceinline__ void add_silt(float& t, float dh, float area, double& book) {
+    if (dh <= 0.0f || !finite_f(dh)) return;
+    const float room = fmaxf(SILT_COLUMN_CAP_M - fmaxf(t, 0.0f), 0.0f);
+    const float add = fminf(dh, room);
+    if (add <= 0.0f) return;
+    t += add;
+    book += (double)(add * area);
+}
+
+// Block-wide reductions to one atomic per block: thousands of warps adding
+// into one word would serialise on it. Every thread of the block calls them.
+template <typename V>
+__device__ __forceinline__ V block_sum(V v) {
+    __shared__ V part[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    v = V(0);
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? part[lane] : V(0);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;  // the sum, in thread 0
+}
+
+__device__ __forceinline__ void block_book(double v, double* book) {
+    v = block_sum(v);
+    if (threadIdx.x == 0 && v != 0.0) atomicAdd(book, v);
+}
+
+__device__ __forceinline__ void block_count(unsigned int v, unsigned int* to) {
+    v = block_sum(v);
+    if (threadIdx.x == 0 && v) atomicAdd(to, v);
+}
+
+// Sets *flag when any thread of the block passes `any`.
+__device__ __forceinline__ void block_flag(bool any, unsigned int* flag) {
+    if (__syncthreads_or(any) && threadIdx.x == 0) *flag = 1u;
+}
+
+
+// A thread's own box of cells, merged over the warp and added with one
+// atomic per bound.
+struct LocalBox {
+    int b[4] = {0x7fffffff, -1, 0x7fffffff, -1};
+    __device__ __forceinline__ void add(int i, int j) {
+        b[0] = min(b[0], i);
+        b[1] = max(b[1], i);
+        b[2] = min(b[2], j);
+        b[3] = max(b[3], j);
+    }
+    // Merged over the block, then one atomic per bound. Every thread of the
+    // block calls it.
+    __device__ __forceinline__ void commit(int* box) {
+        __shared__ int part[4][32];
+        for (int o = 16; o > 0; o >>= 1) {
+            b[0] = min(b[0], __shfl_down_sync(0xffffffffu, b[0], o));
+            b[1] = max(b[1], __shfl_down_sync(0xffffffffu, b[1], o));
+            b[2] = min(b[2], __shfl_down_sync(0xffffffffu, b[2], o));
+            b[3] = max(b[3], __shfl_down_sync(0xffffffffu, b[3], o));
+        }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0)
+            for (int k = 0; k < 4; ++k) part[k][warp] = b[k];
+        __syncthreads();
+        if (warp == 0) {
+            const bool have = lane < (int)(blockDim.x >> 5);
+            b[0] = have ? part[0][lane] : 0x7fffffff;
+            b[1] = have ? part[1][lane] : -1;
+            b[2] = have ? part[2][lane] : 0x7fffffff;
+            b[3] = have ? part[3][lane] : -1;
+            for (int o = 16; o > 0; o >>= 1) {
+                b[0] = min(b[0], __shfl_down_sync(0xffffffffu, b[0], o));
+                b[1] = max(b[1], __shfl_down_sync(0xffffffffu, b[1], o));
+                b[2] = min(b[2], __shfl_down_sync(0xffffffffu, b[2], o));
+                b[3] = max(b[3], __shfl_down_sync(0xffffffffu, b[3], o));
+            }
+            if (lane == 0 && b[1] >= 0) {
+                atomicMin(&box[0], b[0]);
+                atomicMax(&box[1], b[1]);
+                atomicMin(&box[2], b[2]);
+                atomicMax(&box[3], b[3]);
+            }
+        }
+        __syncthreads();
+    }
+};
+
+__device__ __forceinline__ void box_clear(int* box, int res) {
+    box[0] = res;
+    box[1] = -1;
+    box[2] = res;
+    box[3] = -1;
+}
+
+__device__ __forceinline__ bool box_empty(const int* b) { return b[0] > b[1]; }
+
+// turbid_span's result (:9766-9795): the box grown by one, clamped.
+__device__ __forceinline__ void grown(const int* b, int res, int& i0, int& i1, int& j0, int& j1) {
+    i0 = max(b[0] - 1, 0);
+    i1 = min(b[1] + 1, res - 1);
+    j0 = max(b[2] - 1, 0);
+    j1 = min(b[3] + 1, res - 1);
+}
+
+// Every cell of the job's window (blockIdx.y is the job, blockIdx.x strides
+// its cells). Indices are 32-bit: a window holds fewer than 2^32 cells.
+#define CELLS(S)                                                                                                  \
+    for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x, n_ = (unsigned)(S).res * (unsigned)(S).res; g < n_; \
+         g += gridDim.x * blockDim.x)
+
+// The cells (i, j, g) of the box [i0, i1] x [j0, j1] (inclusive) of a window
+// `res` cells wide; `continue` moves to the next cell.
+#define BOX_CELLS(res, i0, i1, j0, j1)                                                                  \
+    for (unsigned q_ = blockIdx.x * blockDim.x + threadIdx.x, w_ = (unsigned)max((i1) - (i0) + 1, 0),    \
+                  n_ = w_ * (unsigned)max((j1) - (j0) + 1, 0);                                          \
+         q_ < n_; q_ += gridDim.x * blockDim.x)                                                        \
+        for (int once_ = 1, i = (i0) + (int)(q_ % w_), j = (j0) + (int)(q_ / w_); once_; once_ = 0)        \
+            for (unsigned g = (unsigned)j * (unsigned)(res) + (unsigned)i; once_; once_ = 0)
+
+// The job is copied into registers: the planes' stores would otherwise make
+// the compiler reload its fields from memory after every write.
+#define JOB                              \
+    const Job J = jobs[blockIdx.y];      \
+    const Sheet& S = J.S;                \
+    const Planes& T = J.T;               \
+    (void)S;                             \
+    (void)T
+
+// A box read from device memory into registers.
+struct Box {
+    int i0, i1, j0, j1;
+    __device__ __forceinline__ bool empty() const { return i0 > i1 || j0 > j1; }
+};
+__device__ __forceinline__ Box box_of(const int* b) { return Box{b[0], b[1], b[2], b[3]}; }
+__device__ __forceinline__ Box grown_box(const int* b, int res) {
+    Box r;
+    grown(b, res, r.i0, r.i1, r.j0, r.j1);
+    return r;
+}
+__device__ __forceinline__ Box box_union(Box a, Box b) {
+    if (a.empty()) return b;
+    if (b.empty()) return a;
+    return Box{min(a.i0, b.i0), max(a.i1, b.i1), min(a.j0, b.j0), max(a.j1, b.j1)};
+}
+__device__ __forceinline__ bool in_box(const Box& b, int i, int j) {
+    return i >= b.i0 && i <= b.i1 && j >= b.j0 && j <= b.j1;
+}
+
+// ------------------------------------------------------------ entrain_wake
+
+__global__ void k_entrain(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    float* susp = T.susp[0];
+    const float dt = J.dt;
+    const int res = S.res;
+    const float cell = S.cell, area = cell * cell;
+    double b = 0.0;
+    BOX_CELLS(res, J.ebox[0], J.ebox[1], J.ebox[2], J.ebox[3]) {
+        for (int k = 0; k < J.npush; ++k) {
+            const silt_tire_push& p = J.push[k];
+            if (p.speed < 0.3f) continue;
+            const float fl = fmaxf(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
+            const float fx = p.forward_x / fl, fz = p.forward_z / fl;
+            const float rx = fz, rz = -fx;
+            const float reach = p.radius * 3.4f + cell;
+            const int i0 = (int)floorf(((p.x - reach) - S.ox) / cell);
+            const int i1 = (int)floorf(((p.x + reach) - S.ox) / cell);
+            const int j0 = (int)floorf(((p.z - reach) - S.oz) / cell);
+            const int j1 = (int)floorf(((p.z + reach) - S.oz) / cell);
+            if (i < max(i0, 0) || i > min(i1, res - 1) || j < max(j0, 0) || j > min(j1, res - 1)) continue;
+            const float aft = p.radius * 3.2f;
+            const float half = p.width * 0.55f + 0.08f;
+            const float x = S.ox + ((float)i + 0.5f) * cell;
+            const float z = S.oz + ((float)j + 0.5f) * cell;
+            const float dx = x - p.x, dz = z - p.z;
+            const float along = dx * fx + dz * fz;
+            if (along > -0.05f || along < -aft) continue;
+            const float lat = fabsf(dx * rx + dz * rz);
+            if (lat > half) continue;
+            const float water = S.water[g];
+            if (!finite_f(water) || water < 0.004f) continue;
+            const float along_t = rclamp((-along) / aft, 0.0f, 1.0f);
+            const float lat_t = rclamp(lat / half, 0.0f, 1.0f);
+            const float core = (1.0f - along_t) * (1.0f - lat_t);
+            const float room = fmaxf(water - susp[g], 0.0f);
+            const float add = fminf(4.0f * dt * core * water, room);
+            if (add <= 1.0e-8f) continue;
+            susp[g] += add;
+            b += (double)(add * area);
+        }
+    }
+    block_book(b, T.books + 0);
+}
+
+// ------------------------------------------------------------ step_tracers
+
+__global__ void k_begin(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    const int res = S.res;
+    Ctl* c = ctl_of(st);
+    box_clear(st->tspan, res);
+    box_clear(c->tspan2, res);
+    box_clear(c->tspan3, res);
+    box_clear(c->cbox, res);
+    st->live_silt = 0;
+    st->wet_any = 0;
+    c->active = 0;
+    c->go = 0;
+    c->live_foam_prev = st->live_foam;
+}
+
+// Silt cells above 1e-8 into `box` (which==0: the step's start, also the
+// live-silt flag; 1: after the transport; 2: after the sources).
+__global__ void k_scan(const Job* jobs, int which) {
+    ::silt::dep_wait();
+    JOB;
+    const float* turbid = T.turbid[0];
+    State* st = T.st;
+    Ctl* c = ctl_of(st);
+    if (which > 0 && !c->go) return;
+    int* box = which == 0 ? st->tspan : (which == 1 ? c->tspan2 : c->tspan3);
+    const int res = S.res;
+    LocalBox lb;
+    CELLS(S) {
+        if (turbid[g] > 1.0e-8f) lb.add((int)(g % res), (int)(g / res));
+    }
+    const bool any = lb.b[1] >= 0;
+    lb.commit(box);
+    if (which == 0) block_flag(any, &st->live_silt);
+}
+
+// collect_tracer_wet (:6248-6293) and tracer_visit_box (:6296-6337).
+// `wake`: a tire with speed or slip, or a surface drive (host-known);
+// `pbox`: the tires' reach boxes (host-computed; empty when none).
+__global__ void k_collect_box(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    const int res = S.res, wake = J.wake;
+    Ctl* c = ctl_of(st);
+    c->active = (wake || st->live_silt || c->live_foam_prev) ? 1 : 0;
+    if (!c->active) return;
+    if (wake) {
+        c->cbox[0] = 0;
+        c->cbox[1] = res - 1;
+        c->cbox[2] = 0;
+        c->cbox[3] = res - 1;
+        return;
+    }
+    int b[4] = {res, -1, res, -1};
+    bool any = false;
+    auto take = [&](int i0, int i1, int j0, int j1) {
+        b[0] = min(b[0], i0);
+        b[1] = max(b[1], i1);
+        b[2] = min(b[2], j0);
+        b[3] = max(b[3], j1);
+        any = true;
+    };
+    if (c->live_foam_prev) take(st->live_box[0], st->live_box[1], st->live_box[2], st->live_box[3]);
+    if (!box_empty(st->tspan)) {
+        int i0, i1, j0, j1;
+        grown(st->tspan, res, i0, i1, j0, j1);
+        take(i0, i1, j0, j1);
+    }
+    if (J.pbox[0] <= J.pbox[1]) take(J.pbox[0], J.pbox[1], J.pbox[2], J.pbox[3]);
+    if (!any) return;  // cbox stays empty
+    c->cbox[0] = max(b[0] - 2, 0);
+    c->cbox[1] = min(b[1] + 2, res - 1);
+    c->cbox[2] = max(b[2] - 2, 0);
+    c->cbox[3] = min(b[3] + 2, res - 1);
+}
+
+__global__ void k_collect(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    uint8_t* mark = T.mark;
+    State* st = T.st;
+    Ctl* c = ctl_of(st);
+    if (!c->active) return;
+    const int res = S.res;
+    // Wet and shore marks are cleared where the last collection may have set
+    // them and set inside this step's box; live marks stay.
+    const Box b = box_of(c->cbox);
+    const Box u = box_union(b, box_of(c->mbox));
+    bool any = false;
+    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
+        uint8_t m = mark[g] & LIVE;
+        if (in_box(b, i, j)) {
+            const float h = S.water[g] + S.slurry[g];
+            if (finite_f(h) && !(h < 0.004f)) {
+                m |= WET;
+                any = true;
+                if (shore_wet_cell(S.water, res, i, j)) m |= SHORE;
+            }
+        }
+        mark[g] = m;
+    }
+    block_flag(any, &st->wet_any);
+}
+
+__global__ void k_go(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    Ctl* c = ctl_of(st);
+    c->go = (c->active && (st->wet_any || st->live_silt)) ? 1 : 0;
+    if (c->active) {
+        for (int k = 0; k < 4; ++k) c->mbox[k] = c->cbox[k];
+    }
+}
+
+// advect_foam (:6352-6397), first half: the new value of every wet or
+// foam-live cell into `tmp` (the field itself is read).
+__global__ void k_foam_advect(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    const float* foam = T.foam[0];
+    float* tmp = T.foam[1];
+    const uint8_t* mark = T.mark;
+    const float dt = J.dt, decay = J.foam_decay;
+    Ctl* c = ctl_of(T.st);
+    if (!c->go || !c->live_foam_prev) return;
+    const int res = S.res;
+    const Box b = box_of(c->cbox);  // the wet and foam-live cells lie inside
+    BOX_CELLS(res, b.i0, b.i1, b.j0, b.j1) {
+        const uint8_t m = mark[g];
+        if (m & WET) {
+            const float u = S.uw[g], v = S.vw[g];  // wet cells are far above the dry cut
+            float sample = 0.0f;
+            if (finite_f(u) && finite_f(v)) {
+                const float x = (float)i - u * dt / S.cell;
+                const float z = (float)j - v * dt / S.cell;
+                sample = sample_foam(foam, res, x, z);
+            }
+            const float vv = sample * decay;
+            tmp[g] = (vv > 1.0e-4f && finite_f(vv)) ? fminf(vv, FOAM_EQ) : 0.0f;
+        } else if (m & LIVE) {
+            tmp[g] = 0.0f;
+        }
+    }
+}
+
+// Second half: the new values replace the field.
+__global__ void k_foam_commit(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    float* foam = T.foam[0];
+    const float* tmp = T.foam[1];
+    const uint8_t* mark = T.mark;
+    Ctl* c = ctl_of(T.st);
+    if (!c->go || !c->live_foam_prev) return;
+    const Box b = box_of(c->cbox);
+    BOX_CELLS(S.res, b.i0, b.i1, b.j0, b.j1) {
+        if (mark[g] & (WET | LIVE)) foam[g] = tmp[g];
+    }
+}
+
+// The silt a donor cell gives across its four edges in flux_thickness's
+// order (x edges before z edges, each axis in index order): to the left,
+// right, up and down neighbour (0 where it is not the donor or the edge lies
+// outside the box). flux_edge (:9857-9876) with the donor's running removal.
+__device__ __forceinline__ void donor_flux(const Sheet& S, const float* T, int i, int j, int bi0, int bi1, int bj0,
+                                           int bj1, float dt, float out[4]) {
+    const int res = S.res;
+    const size_t d = (size_t)j * res + i;
+    const float column = finite_f(T[d]) ? T[d] : 0.0f;
+    float removed = 0.0f;
+    out[0] = out[1] = out[2] = out[3] = 0.0f;
+    auto edge = [&](float v, bool donor_is_me) -> float {
+        if (!finite_f(v) || fabsf(v) < 1.0e-5f || !donor_is_me) return 0.0f;
+        const float room = column - removed;
+        if (room <= 1.0e-8f) return 0.0f;
+        const float frac = fminf(fabsf(v) * dt / S.cell, 0.45f);
+        const float dh = fminf(column * frac, room);
+        if (dh <= 1.0e-8f || !finite_f(dh)) return 0.0f;
+        removed += dh;
+        return dh;
+    };
+    if (i - 1 >= bi0 && i <= bi1) {  // edge (i-1, i): this cell donates when the face speed is not positive
+        const float v = 0.5f * (vel(S.uw, S, d - 1) + vel(S.uw, S, d));
+        out[0] = edge(v, !(v > 0.0f));
+    }
+    if (i >= bi0 && i <= bi1 - 1) {  // edge (i, i+1)
+        const float v = 0.5f * (vel(S.uw, S, d) + vel(S.uw, S, d + 1));
+        out[1] = edge(v, v > 0.0f);
+    }
+    if (j - 1 >= bj0 && j <= bj1) {  // edge (j-1, j)
+        const float v = 0.5f * (vel(S.vw, S, d - res) + vel(S.vw, S, d));
+        out[2] = edge(v, !(v > 0.0f));
+    }
+    if (j >= bj0 && j <= bj1 - 1) {  // edge (j, j+1)
+        const float v = 0.5f * (vel(S.vw, S, d) + vel(S.vw, S, d + res));
+        out[3] = edge(v, v > 0.0f);
+    }
+}
+
+// advect_turbid (:6421-6470): new silt of the span's cells into `tmp`.
+__global__ void k_turbid_advect(const Job* jobs) {
+    ::silt::dep_wait();
+    const Job J = jobs[blockIdx.y];
+    const Sheet& S = J.S;
+    const float* T = J.T.turbid[0];
+    float* tmp = J.T.turbid[1];
+    State* st = J.T.st;
+    const float dt = J.dt;
+    Ctl* c = ctl_of(st);
+    if (!c->go || box_empty(st->tspan)) return;
+    const int res = S.res;
+    int bi0, bi1, bj0, bj1;
+    grown(st->tspan, res, bi0, bi1, bj0, bj1);
+    BOX_CELLS(res, bi0, bi1, bj0, bj1) {
+        float own[4], nb[4];
+        donor_flux(S, T, i, j, bi0, bi1, bj0, bj1, dt, own);
+        float removed = 0.0f;
+        for (int k = 0; k < 4; ++k)
+            if (own[k] > 0.0f) removed += own[k];
+        // What the neighbours give this cell, in the reference's edge order.
+        float added = 0.0f;
+        if (i - 1 >= bi0) {
+            donor_flux(S, T, i - 1, j, bi0, bi1, bj0, bj1, dt, nb);
+            if (nb[1] > 0.0f) added += nb[1];
+        }
+        if (i + 1 <= bi1) {
+            donor_flux(S, T, i + 1, j, bi0, bi1, bj0, bj1, dt, nb);
+            if (nb[0] > 0.0f) added += nb[0];
+        }
+        if (j - 1 >= bj0) {
+            donor_flux(S, T, i, j - 1, bi0, bi1, bj0, bj1, dt, nb);
+            if (nb[3] > 0.0f) added += nb[3];
+        }
+        if (j + 1 <= bj1) {
+            donor_flux(S, T, i, j + 1, bi0, bi1, bj0, bj1, dt, nb);
+            if (nb[2] > 0.0f) added += nb[2];
+        }
+        float t = T[g];
+        if (removed == 0.0f && added == 0.0f) {
+            if (!finite_f(t)) t = 0.0f;
+        } else {
+            const float next = t - removed + added;
+            t = finite_f(next) ? fmaxf(next, 0.0f) : 0.0f;
+        }
+        tmp[g] = t;
+    }
+}
+
+__global__ void k_turbid_commit(const Job* jobs) {
+    ::silt::dep_wait();
+    const Job J = jobs[blockIdx.y];
+    const Sheet& S = J.S;
+    float* T = J.T.turbid[0];
+    const float* tmp = J.T.turbid[1];
+    State* st = J.T.st;
+    Ctl* c = ctl_of(st);
+    if (!c->go || box_empty(st->tspan)) return;
+    const int res = S.res;
+    int bi0, bi1, bj0, bj1;
+    grown(st->tspan, res, bi0, bi1, bj0, bj1);
+    BOX_CELLS(res, bi0, bi1, bj0, bj1) T[g] = tmp[g];
+}
+
+// settle_turbid (:6473-6509) on the span after the transport.
+__global__ void k_settle(const Job* jobs) {
+    ::silt::dep_wait();
+    const Job J = jobs[blockIdx.y];
+    const Sheet& S = J.S;
+    float* T = J.T.turbid[0];
+    State* st = J.T.st;
+    const float keep = J.silt_keep;
+    double* book = J.T.books + 3;
+    Ctl* c = ctl_of(st);
+    if (!c->go || box_empty(c->tspan2)) return;
+    const int res = S.res;
+    const float area = S.cell * S.cell;
+    int bi0, bi1, bj0, bj1;
+    grown(c->tspan2, res, bi0, bi1, bj0, bj1);
+    double b = 0.0;
+    BOX_CELLS(res, bi0, bi1, bj0, bj1) {
+        const float h = S.water[g] + S.slurry[g];
+        const float column = finite_f(T[g]) ? fmaxf(T[g], 0.0f) : 0.0f;
+        if (column <= 0.0f) {
+            T[g] = 0.0f;
+            continue;
+        }
+        if (!finite_f(h) || h < 1.0e-5f) {
+            b += (double)(column * area);
+            T[g] = 0.0f;
+            continue;
+        }
+        const float stay = column * keep;
+        b += (double)((column - stay) * area);
+        T[g] = stay;
+    }
+    block_book(b, book);
+}
+
+// spawn_foam_and_silt (:6511-6520) on each wet cell: the tires of this
+// launch in push order (spawn_tire_tracers :6599-6665), then, in the last
+// launch, the shore (spawn_shore_tracers :6667-6684) and Froude breaking
+// (spawn_breaking_speed :6545-6558).
+__global__ void k_spawn(const Job* jobs) {
+    ::silt::dep_wait();
+    const Job J = jobs[blockIdx.y];
+    const Sheet& S = J.S;
+    float* foam = J.T.foam[0];
+    float* T = J.T.turbid[0];
+    const uint8_t* mark = J.T.mark;
+    const float dt = J.dt;
+    double* book = J.T.books + 2;
+    Ctl* c = ctl_of(J.T.st);
+    if (!c->go) return;
+    const int res = S.res;
+    const float cell = S.cell, area = cell * cell;
+    double b = 0.0;
+    const Box cb = box_of(c->cbox);  // the wet cells lie inside
+    BOX_CELLS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
+        const uint8_t m = mark[g];
+        if (!(m & WET)) continue;
+        float f = foam[g], t = T[g];
+        for (int k = 0; k < J.npush; ++k) {
+            const silt_tire_push& p = J.push[k];
+            const float speed = finite_f(p.speed) ? fmaxf(p.speed, 0.0f) : 0.0f;
+            const float slip = finite_f(p.slip) ? fminf(fabsf(p.slip), 1.5f) : 0.0f;
+            if (speed < 0.25f && slip < 0.05f) continue;
+            const float h = S.water[g];
+            if (!finite_f(h) || h < 0.004f) continue;
+            const float radius = fmaxf(p.radius, 0.05f);
+            const float len = fmaxf(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
+            const float fx = p.forward_x / len, fz = p.forward_z / len;
+            const float rx = fz, rz = -fx;
+            const float reach = radius * 1.15f + cell;
+            const float reach2 = reach * reach;
+            const float slip_v = speed * slip;
+            const float x = S.ox + ((float)i + 0.5f) * cell;
+            const float z = S.oz + ((float)j + 0.5f) * cell;
+            const float dx = x - p.x, dz = z - p.z;
+            if (dx * dx + dz * dz > reach2) continue;
+            const float along = dx * fx + dz * fz;
+            const float lat = dx * rx + dz * rz;
+            const float dist = hypot_rn(dx, dz);
+            float film = hypot_rn(S.uw[g], S.vw[g]);
+            film = finite_f(film) ? film : 0.0f;
+            const float immerse = fminf(h, radius * 0.9f);
+            const float r_line = sqrtf(fmaxf(2.0f * radius * immerse - immerse * immerse, 0.0f));
+            const float band = 1.0f - rclamp(fabsf(dist - r_line) / (cell * 1.35f), 0.0f, 1.0f);
+            if (band > 0.0f) {
+                const float motion = fmaxf(fmaxf(slip_v, speed * 0.45f), film);
+                add_foam(f, breaking_foam(motion, h) * band, dt);
+            }
+            const bool on_patch = fabsf(lat) <= p.width * 0.55f + cell * 0.35f && along >= -radius * 0.55f &&
+                                  along <= radius * 0.35f;
+            if (on_patch && h > 0.02f) {
+                // lift_silt (:6686-6697), rate cap 0.015, critical stress 6 Pa.
+                const float shear_v = fmaxf(slip_v, film * 0.35f);
+                if (finite_f(shear_v) && shear_v > 0.0f) {
+                    const float tau = 1000.0f * 0.035f * shear_v * shear_v;
+                    if (tau > 6.0f) {
+                        const float rate = fminf(0.008f * (tau / 6.0f - 1.0f), 0.015f);
+                        add_silt(t, fminf(rate * dt, 0.0025f), area, b);
+                    }
+                }
+            }
+        }
+        {
+            if (m & SHORE) {
+                float prod, silt_add;
+                shore_cell(S, i, j, prod, silt_add);
+                add_foam(f, prod, dt);
+                if (silt_add > 0.0f) add_silt(t, fminf(silt_add * dt, 0.0012f), area, b);
+            }
+            const float h = S.water[g] + S.slurry[g];
+            if (finite_f(h) && !(h < 0.004f)) {
+                const float u = S.uw[g], v = S.vw[g];
+                if (finite_f(u) && finite_f(v) && !(hypot_rn(u, v) <= 0.05f)) add_foam(f, breaking_foam(hypot_rn(u, v), h), dt);
+            }
+        }
+        foam[g] = f;
+        T[g] = t;
+    }
+    block_book(b, book);
+}
+
+// clear_dry_tracers (:6712-6739).
+__global__ void k_clear(const Job* jobs) {
+    ::silt::dep_wait();
+    const Job J = jobs[blockIdx.y];
+    const Sheet& S = J.S;
+    float* foam = J.T.foam[0];
+    float* T = J.T.turbid[0];
+    const uint8_t* mark = J.T.mark;
+    double* book = J.T.books + 3;
+    Ctl* c = ctl_of(J.T.st);
+    if (!c->go) return;
+    const int res = S.res;
+    const float area = S.cell * S.cell;
+    const Box sb = box_empty(c->tspan3) ? Box{0, -1, 0, -1} : grown_box(c->tspan3, res);
+    const Box u = box_union(box_of(c->cbox), sb);  // the wet cells lie in the collection box
+    double b = 0.0;
+    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
+        const float h = S.water[g] + S.slurry[g];
+        if (mark[g] & WET) {
+            if (!finite_f(h) || h < 0.004f || !finite_f(foam[g])) foam[g] = 0.0f;
+        }
+        if (!in_box(sb, i, j)) continue;
+        if (!finite_f(h) || h < 1.0e-5f) {
+            if (T[g] > 0.0f) {
+                b += (double)(T[g] * area);
+                T[g] = 0.0f;
+            }
+        } else if (!finite_f(T[g])) {
+            T[g] = 0.0f;
+        }
+    }
+    block_book(b, book);
+}
+
+__global__ void k_sync_begin(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    const int res = S.res;
+    if (!ctl_of(st)->go) return;
+    st->live_foam = 0;
+    box_clear(st->live_box, res);
+}
+
+// sync_foam_live (:6339-6349).
+__global__ void k_sync(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    const float* foam = T.foam[0];
+    uint8_t* mark = T.mark;
+    State* st = T.st;
+    if (!ctl_of(st)->go) return;
+    const int res = S.res;
+    unsigned int cnt = 0;
+    LocalBox lb;
+    // Outside the collection box no cell is wet, and the live cells of the
+    // last sync lie inside it (it covers their box), so every mark there is 0.
+    const Box cb = box_of(ctl_of(st)->cbox);
+    BOX_CELLS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
+        uint8_t m = mark[g] & (WET | SHORE);
+        if ((m & WET) && finite_f(foam[g]) && foam[g] > 1.0e-4f) {
+            m |= LIVE;
+            ++cnt;
+            lb.add(i, j);
+        }
+        mark[g] = m;
+    }
+    lb.commit(st->live_box);
+    block_count(cnt, &st->live_foam);
+}
+
+// ---------------------------------------------------------- step_suspended
+
+__global__ void k_susp_begin(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    box_clear(st->sbox, S.res);
+    st->capped = 0;
+}
+
+// advect_suspended's first loop (:8826-8870): grains fall out at their fall
+// speed; a dry cell or a load above the water settles whole.
+__global__ void k_susp_settle(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    float* susp = T.susp[0];
+    State* st = T.st;
+    const float dt = J.dt;
+    double* book = T.books + 1;
+    const int res = S.res;
+    const float area = S.cell * S.cell;
+    double b = 0.0;
+    LocalBox lb;
+    CELLS(S) {
+        float s = susp[g];
+        if (!finite_f(s) || s <= 1.0e-12f) {
+            if (__float_as_uint(s) != 0u) susp[g] = 0.0f;
+            continue;
+        }
+        const float w = S.water[g];
+        if (!finite_f(w) || w < 1.0e-5f || s > w) {
+            b += (double)(s * area);
+            susp[g] = 0.0f;
+            continue;
+        }
+        const float keep = exp_rn(-dt * SUSP_FALL_M_S / w);
+        const float landed = s * (1.0f - keep);
+        if (landed > 0.0f) {
+            b += (double)landed * (double)area;
+            s -= landed;
+            susp[g] = s;
+        }
+        if (s > 1.0e-8f) lb.add((int)(g % res), (int)(g / res));
+    }
+    lb.commit(st->sbox);
+    block_book(b, book);
+}
+
+// One donor's part of advect_suspended's transport (:8894-8969).
+struct Donor {
+    bool live;
+    float depth, w, c, fu, fv, fd;
+    int up_i, up_j;  // receivers of the advected gives (-1: off the window)
+};
+
+__device__ __forceinline__ Donor donor_of(const Sheet& S, const float* susp, int i, int j, float dt) {
+    const int res = S.res;
+    const size_t d = (size_t)j * res + i;
+    Donor D;
+    D.depth = susp[d];
+    D.w = S.water[d];
+    D.live = !(D.depth <= 1.0e-12f || !finite_f(D.depth) || !finite_f(D.w) || D.w < 1.0e-5f);
+    if (!D.live) return D;
+    // film_uv(water, 0, uw, vw, 0, 0) (:3490-3501): the water film's own velocity.
+    float u = 0.0f, v = 0.0f;
+    const float hh = D.w + 0.0f;
+    if (finite_f(hh) && !(hh < 1.0e-5f)) {
+        u = finite0((S.uw[d] * D.w + 0.0f * 0.0f) / hh);
+        v = finite0((S.vw[d] * D.w + 0.0f * 0.0f) / hh);
+    }
+    u = S.surface_driven && finite_f(u) ? u : 0.0f;
+    v = finite_f(v) ? v : 0.0f;
+    D.c = D.depth / D.w;
+    float fu = fabsf(u) * dt / S.cell, fv = fabsf(v) * dt / S.cell;
+    const float sum = fu + fv;
+    if (sum > 0.45f) {
+        fu *= 0.45f / sum;
+        fv *= 0.45f / sum;
+    }
+    D.fu = fu;
+    D.fv = fv;
+    D.up_i = u > 0.0f ? (i + 1 < res ? (int)d + 1 : -1) : (i > 0 ? (int)d - 1 : -1);
+    D.up_j = v > 0.0f ? (j + 1 < res ? (int)d + res : -1) : (j > 0 ? (int)d - res : -1);
+    const float speed = sqrtf(u * u + v * v);
+    const float k = 0.01f + 0.2f * speed * D.w;
+    D.fd = fminf(k * dt / (S.cell * S.cell), 0.1f);
+    return D;
+}
+
+// Receivers: each cell takes from its neighbour donors in raster order of
+// the donors, each donor's gives in its own order (advection x, z, then
+// mixing +x, -x, +z, -z), and records every accepted give in the donor's
+// slot; its total goes to `taken`.
+__global__ void k_susp_take(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    const float* susp = T.susp[0];
+    float* taken = T.taken;
+    float* acc = T.acc;
+    State* st = T.st;
+    const float dt = J.dt;
+    if (box_empty(st->sbox)) return;
+    const int res = S.res;
+    const size_t n = (size_t)res * res;
+    int bi0, bi1, bj0, bj1;
+    grown(st->sbox, res, bi0, bi1, bj0, bj1);
+    const bool open = S.surface_driven != 0;
+    BOX_CELLS(res, max(bi0 - 1, 0), min(bi1 + 1, res - 1), max(bj0 - 1, 0), min(bj1 + 1, res - 1)) {
+        const float wr = S.water[g];
+        const bool can = finite_f(wr) && !(wr < 1.0e-5f);
+        float tk = 0.0f;
+        const int di[4] = {0, -1, 1, 0}, dj[4] = {-1, 0, 0, 1};  // donors in raster order
+        for (int q = 0; q < 4; ++q) {
+            const int a = i + di[q], c2 = j + dj[q];
+            if (a < bi0 || a > bi1 || c2 < bj0 || c2 > bj1) continue;  // donors are the box's cells
+            const Donor D = donor_of(S, susp, a, c2, dt);
+            if (!D.live) continue;
+            const size_t d = (size_t)c2 * res + a;
+            const float fr[2] = {D.fu, D.fv};
+            const int rv[2] = {D.up_i, D.up_j};
+            for (int s = 0; s < 2; ++s) {
+                if (rv[s] != (int)g) continue;
+                const float give = D.depth * fr[s];
+                if (give <= 1.0e-12f) continue;
+                float accept = 0.0f;
+                if (can) {
+                    const float have = susp[g] + tk;
+                    const float room = fmaxf(D.c * wr - have, 0.0f);
+                    accept = fminf(fminf(give, room), fmaxf(wr - have, 0.0f));
+                    if (accept <= 1.0e-12f) accept = 0.0f;
+                    else tk += accept;
+                }
+                acc[(size_t)s * n + d] = accept;
+            }
+            if (!open) continue;
+            // The donor's mixing neighbours: +x, -x, +z, -z.
+            const int mk = (g == d + 1) ? 0 : (g + 1 == d ? 1 : (g == d + res ? 2 : 3));
+            float accept = 0.0f;
+            if (can) {
+                const float cn = susp[g] / wr;
+                if (D.c > cn) {
+                    const float give = D.fd * (D.c - cn) * fminf(D.w, wr);
+                    const float have = susp[g] + tk;
+                    accept = fminf(give, fmaxf(wr - have, 0.0f));
+                    if (accept <= 1.0e-12f) accept = 0.0f;
+                    else tk += accept;
+                }
+            }
+            acc[(size_t)(2 + mk) * n + d] = accept;
+        }
+        taken[g] = tk;
+    }
+}
+
+// Donors: each box cell gives its slots away in its own order, takes what
+// its neighbours gave it, then the load above the water or on a dry cell
+// settles (:8971-9000).
+__global__ void k_susp_give(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    float* susp = T.susp[0];
+    const float* taken = T.taken;
+    const float* acc = T.acc;
+    State* st = T.st;
+    const float dt = J.dt;
+    double* book = T.books + 1;
+    if (box_empty(st->sbox)) return;
+    const int res = S.res;
+    const size_t n = (size_t)res * res;
+    const float area = S.cell * S.cell;
+    int bi0, bi1, bj0, bj1;
+    grown(st->sbox, res, bi0, bi1, bj0, bj1);
+    const bool open = S.surface_driven != 0;
+    double b = 0.0;
+    unsigned int capped = 0;
+    BOX_CELLS(res, bi0, bi1, bj0, bj1) {
+        float next = susp[g];
+        const Donor D = donor_of(S, susp, i, j, dt);
+        if (D.live) {
+            const float fr[2] = {D.fu, D.fv};
+            const int rv[2] = {D.up_i, D.up_j};
+            for (int s = 0; s < 2; ++s) {
+                const float give = D.depth * fr[s];
+                if (give <= 1.0e-12f) continue;
+                if (rv[s] < 0) {
+                    b += (double)(give * area);
+                    next -= give;
+                    continue;
+                }
+                const float wrr = S.water[rv[s]];
+                if (!finite_f(wrr) || wrr < 1.0e-5f) continue;
+                const float a = acc[(size_t)s * n + g];
+                if (a > 0.0f) next -= a;
+            }
+            if (open) {
+                const bool has[4] = {i + 1 < res, i > 0, j + 1 < res, j > 0};
+                const int off[4] = {1, -1, res, -res};
+                for (int k = 0; k < 4; ++k) {
+                    if (!has[k]) continue;
+                    const float wrr = S.water[g + off[k]];
+                    if (!finite_f(wrr) || wrr < 1.0e-5f) continue;
+                    const float a = acc[(size_t)(2 + k) * n + g];
+                    if (a > 0.0f) next -= a;
+                }
+            }
+        }
+        next += taken[g];
+        float s = next;
+        if (!finite_f(s) || s <= 0.0f) {
+            susp[g] = 0.0f;
+            continue;
+        }
+        const float w = S.water[g];
+        if (!finite_f(w) || w < 1.0e-5f) {
+            b += (double)(s * area);
+            s = 0.0f;
+        } else if (s > w) {
+            const float excess = s - w;
+            b += (double)(excess * area);
+            if (excess > 1.0e-5f) ++capped;
+            s = w;
+        }
+        susp[g] = s;
+    }
+    block_book(b, book);
+    block_count(capped, &st->capped);
+}
+
+__global__ void k_reset_live(uint8_t* mark, State* st, int res, size_t n) {
+    ::silt::dep_wait();
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x)
+        mark[g] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->live_foam = 0;
+        box_clear(st->live_box, res);
+        box_clear(ctl_of(st)->mbox, res);
+    }
+}
+
+// tracer_visit_box's tire part (:6320-6331) on the host: each tire inside
+// the window reaches ceil(8 m / cell) cells around its own.
+void push_box(const Sheet& S, const silt_tire_push* p, int n, int* b) {
+    b[0] = S.res;
+    b[1] = -1;
+    b[2] = S.res;
+    b[3] = -1;
+    const int reach = (int)ceilf(8.0f / S.cell);
+    for (int k = 0; k < n; ++k) {
+        const float fi = floorf((p[k].x - S.ox) / S.cell), fj = floorf((p[k].z - S.oz) / S.cell);
+        if (!(fi >= 0.0f) || !(fj >= 0.0f) || fi >= (float)S.res || fj >= (float)S.res) continue;
+        const int ci = (int)fi, cj = (int)fj;
+        b[0] = std::min(b[0], std::max(ci - reach, 0));
+        b[1] = std::max(b[1], std::min(ci + reach, S.res - 1));
+        b[2] = std::min(b[2], std::max(cj - reach, 0));
+        b[3] = std::max(b[3], std::min(cj + reach, S.res - 1));
+    }
+}
+
+// entrain_wake's cells (:8766-8776): the union of the tires' reach boxes,
+// one cell wider on each side and clamped to the window (each cell still
+// tests every tire's own box, so the margin only covers host rounding).
+void entrain_box(const Sheet& S, const silt_tire_push* p, int n, int* b) {
+    b[0] = S.res;
+    b[1] = -1;
+    b[2] = S.res;
+    b[3] = -1;
+    for (int k = 0; k < n; ++k) {
+        if (!(p[k].speed >= 0.3f)) continue;
+        const float reach = p[k].radius * 3.4f + S.cell;
+        const float lo_x = floorf(((p[k].x - reach) - S.ox) / S.cell), hi_x = floorf(((p[k].x + reach) - S.ox) / S.cell);
+        const float lo_z = floorf(((p[k].z - reach) - S.oz) / S.cell), hi_z = floorf(((p[k].z + reach) - S.oz) / S.cell);
+        if (!(lo_x <= hi_x) || !(lo_z <= hi_z)) continue;
+        if (hi_x < 0.0f || hi_z < 0.0f || lo_x >= (float)S.res || lo_z >= (float)S.res) continue;
+        b[0] = std::min(b[0], (int)std::max(lo_x - 1.0f, 0.0f));
+        b[1] = std::max(b[1], (int)std::min(hi_x + 1.0f, (float)(S.res - 1)));
+        b[2] = std::min(b[2], (int)std::max(lo_z - 1.0f, 0.0f));
+        b[3] = std::max(b[3], (int)std::min(hi_z + 1.0f, (float)(S.res - 1)));
+    }
+}
+
+// Blocks per window of a launch over n windows: enough for the largest
+// window, about 2400 blocks of 256 threads in all.
+int blocks_x(const Window* w, int n) {
+    size_t most = 1;
+    for (int k = 0; k < n; ++k) most = std::max(most, (size_t)w[k].S.res * w[k].S.res);
+    const size_t per = std::max<size_t>(1, 2368 / (size_t)std::max(n, 1));
+    return (int)std::min((most + 255) / 256, per);
+}
+
+// Uploads the jobs (and their pushes) of one launch sequence; returns the
+// device array.
+cudaError_t upload(Runner& R, const Window* w, int n, float dt, float foam_decay, float silt_keep, cudaStream_t st,
+                   const Job** out) {
+    const int slot = R.flip;
+    R.flip ^= 1;
+    cudaError_t e;
+    if (R.ev[slot]) {
+        if ((e = cudaEventSynchronize(R.ev[slot])) != cudaSuccess) return e;  // the copy two sequences back is done
+    } else if ((e = cudaEventCreateWithFlags(&R.ev[slot], cudaEventDisableTiming)) != cudaSuccess) {
+        return e;
+    }
+    size_t np = 0;
+    for (int k = 0; k < n; ++k) np += (size_t)w[k].npush;
+    if ((size_t)n > R.cap_jobs[slot]) {
+        cudaFree(R.d_jobs[slot]);
+        if (R.h_jobs[slot]) cudaFreeHost(R.h_jobs[slot]);
+        R.d_jobs[slot] = nullptr;
+        R.h_jobs[slot] = nullptr;
+        R.cap_jobs[slot] = 0;
+        const size_t cap = (size_t)n * 2;
+        if ((e = cudaMalloc(&R.d_jobs[slot], cap * sizeof(Job))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&R.h_jobs[slot], cap * sizeof(Job))) != cudaSuccess) return e;
+        R.cap_jobs[slot] = cap;
+    }
+    if (np > R.cap_push[slot]) {
+        cudaFree(R.d_push[slot]);
+        if (R.h_push[slot]) cudaFreeHost(R.h_push[slot]);
+        R.d_push[slot] = nullptr;
+        R.h_push[slot] = nullptr;
+        R.cap_push[slot] = 0;
+        const size_t cap = np * 2 + 16;
+        if ((e = cudaMalloc(&R.d_push[slot], cap * sizeof(silt_tire_push))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&R.h_push[slot], cap * sizeof(silt_tire_push))) != cudaSuccess) return e;
+        R.cap_push[slot] = cap;
+    }
+    size_t q = 0;
+    for (int k = 0; k < n; ++k) {
+        Job& J = R.h_jobs[slot][k];
+        memset(&J, 0, sizeof J);
+        J.S = w[k].S;
+        J.T = w[k].T;
+        J.npush = w[k].npush;
+        J.push = w[k].npush ? R.d_push[slot] + q : nullptr;
+        if (w[k].npush) memcpy(R.h_push[slot] + q, w[k].push, (size_t)w[k].npush * sizeof(silt_tire_push));
+        q += (size_t)w[k].npush;
+        bool wake = w[k].S.surface_driven != 0;
+        for (int t = 0; t < w[k].npush; ++t) {
+            const silt_tire_push& p = w[k].push[t];
+            wake = wake || (std::isfinite(p.speed) && p.speed >= 0.25f) ||
+                   (std::isfinite(p.slip) && fabsf(p.slip) >= 0.05f);
+        }
+        J.wake = wake ? 1 : 0;
+        push_box(w[k].S, w[k].push, w[k].npush, J.pbox);
+        entrain_box(w[k].S, w[k].push, w[k].npush, J.ebox);
+        J.dt = dt;
+        J.foam_decay = foam_decay;
+        J.silt_keep = silt_keep;
+    }
+    if (np && (e = cudaMemcpyAsync(R.d_push[slot], R.h_push[slot], np * sizeof(silt_tire_push),
+                                   cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(R.d_jobs[slot], R.h_jobs[slot], (size_t)n * sizeof(Job), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaEventRecord(R.ev[slot], st)) != cudaSuccess) return e;
+    *out = R.d_jobs[slot];
+    return cudaSuccess;
+}
+
+#define LAUNCH(kernel, bx, ...)                                                                \
+    do {                                                                                       \
+        ::silt::launch_dep(kernel, dim3((bx), (unsigned)n), dim3(256), 0, st, __VA_ARGS__);    \
+        ::silt::count_launch();                                                                \
+        const cudaError_t e_ = cudaGetLastError();                                             \
+        if (e_ != cudaSuccess) return e_;                                                      \
+    } while (0)
+
+}  // namespace
+
+size_t plane_bytes(int res) {
+    const size_t n = (size_t)res * res;
+    return 256 + 6 * n * sizeof(float) + 6 * n * sizeof(float) + n + 256;
+}
+
+cudaError_t attach(Planes& T, void* mem, int res, double* books, cudaStream_t st) {
+    const size_t n = (size_t)res * res;
+    char* q = (char*)mem;
+    T.st = reinterpret_cast<State*>(q);  // State then Ctl, within the first 256 bytes
+    static_assert(sizeof(State) + sizeof(Ctl) <= 256, "tracer state");
+    q += 256;
+    float* f = reinterpret_cast<float*>(q);
+    T.foam[0] = f;
+    T.foam[1] = f + n;
+    T.turbid[0] = f + 2 * n;
+    T.turbid[1] = f + 3 * n;
+    T.susp[0] = f + 4 * n;
+    T.susp[1] = f + 5 * n;
+    T.taken = T.susp[1];
+    T.acc = f + 6 * n;
+    T.mark = reinterpret_cast<uint8_t*>(f + 12 * n);
+    T.books = books;
+    cudaError_t e = cudaMemsetAsync(mem, 0, plane_bytes(res), st);
+    if (e != cudaSuccess) return e;
+    return reset_indices(T, res, st);
+}
+
+void Runner::release() {
+    for (int k = 0; k < 2; ++k) {
+        cudaFree(d_jobs[k]);
+        cudaFree(d_push[k]);
+        if (h_jobs[k]) cudaFreeHost(h_jobs[k]);
+        if (h_push[k]) cudaFreeHost(h_push[k]);
+        if (ev[k]) cudaEventDestroy(ev[k]);
+        d_jobs[k] = h_jobs[k] = nullptr;
+        d_push[k] = h_push[k] = nullptr;
+        cap_jobs[k] = cap_push[k] = 0;
+        ev[k] = nullptr;
+    }
+}
+
+cudaError_t entrain(Runner& R, const Window* w, int n, float dt, cudaStream_t st) {
+    if (n <= 0 || !(dt > 0.0f) || !std::isfinite(dt)) return cudaSuccess;
+    const Job* jobs = nullptr;
+    cudaError_t e = upload(R, w, n, dt, 0.0f, 0.0f, st, &jobs);
+    if (e != cudaSuccess) return e;
+    LAUNCH(k_entrain, blocks_x(w, n), jobs);
+    return cudaSuccess;
+}
+
+cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream_t st) {
+    if (n <= 0 || !(dt > 0.0f) || !std::isfinite(dt)) return cudaSuccess;
+    // The per-step factors, with the C library's expf as the reference's f32::exp.
+    const float foam_decay = expf(-dt / 1.8f);  // FOAM_LIFE_S :112
+    const float silt_keep = expf(-dt / 4.0f);   // SILT_SETTLE_S :119
+    const Job* jobs = nullptr;
+    cudaError_t e = upload(R, w, n, dt, foam_decay, silt_keep, st, &jobs);
+    if (e != cudaSuccess) return e;
+    const int bx = blocks_x(w, n);
+    LAUNCH(k_begin, 1, jobs);
+    LAUNCH(k_scan, bx, jobs, 0);
+    LAUNCH(k_collect_box, 1, jobs);
+    LAUNCH(k_collect, bx, jobs);
+    LAUNCH(k_go, 1, jobs);
+    LAUNCH(k_foam_advect, bx, jobs);
+    LAUNCH(k_foam_commit, bx, jobs);
+    LAUNCH(k_turbid_advect, bx, jobs);
+    LAUNCH(k_turbid_commit, bx, jobs);
+    LAUNCH(k_scan, bx, jobs, 1);
+    LAUNCH(k_settle, bx, jobs);
+    LAUNCH(k_spawn, bx, jobs);
+    LAUNCH(k_scan, bx, jobs, 2);
+    LAUNCH(k_clear, bx, jobs);
+    LAUNCH(k_sync_begin, 1, jobs);
+    LAUNCH(k_sync, bx, jobs);
+    return cudaSuccess;
+}
+
+cudaError_t step_suspended(Runner& R, const Window* w, int n, float dt, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const Job* jobs = nullptr;
+    cudaError_t e = upload(R, w, n, dt, 0.0f, 0.0f, st, &jobs);
+    if (e != cudaSuccess) return e;
+    LAUNCH(k_susp_begin, 1, jobs);
+    if (!(dt > 0.0f) || !std::isfinite(dt)) return cudaSuccess;
+    const int bx = blocks_x(w, n);
+    LAUNCH(k_susp_settle, bx, jobs);
+    LAUNCH(k_susp_take, bx, jobs);
+    LAUNCH(k_susp_give, bx, jobs);
+    return cudaSuccess;
+}
+
+cudaError_t reset_indices(Planes& T, int res, cudaStream_t st) {
+    const size_t cells = (size_t)res * res;
+    const size_t b = (cells + 255) / 256;
+    ::silt::launch_dep(k_reset_live, dim3((unsigned)std::min<size_t>(std::max<size_t>(b, 1), 1184)), dim3(256), 0, st,
+                       T.mark, T.st, res, cells);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace tracers
+}  // namespace silt

@@ -44,7 +44,9 @@ class SprayEvent(ctypes.Structure):
 class Ledger(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3",
                                                "spray_m3", "opened_m3", "total_m3", "cut_m3", "reach_m3",
-                                               "round_m3")]
+                                               "round_m3", "suspended_m3", "settled_suspended_m3",
+                                               "frozen_suspended_m3", "entrained_m3", "turbid_m3",
+                                               "turbid_settled_m3", "frozen_turbid_m3", "stirred_m3")]
 
 
 class RiverReach(ctypes.Structure):
@@ -72,7 +74,7 @@ class GroundSample(ctypes.Structure):
 
 
 class CoarseCell(ctypes.Structure):
-    _fields_ = [(k, _f) for k in ("x", "z", "bed_m", "water_m", "slurry_m", "moisture", "u", "v")]
+    _fields_ = [(k, _f) for k in ("x", "z", "bed_m", "water_m", "slurry_m", "moisture", "u", "v", "turbidity")]
 
 
 class StepParts(ctypes.Structure):
@@ -179,7 +181,8 @@ def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-PLANES = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7}
+PLANES = {"water": 0, "slurry": 1, "uw": 2, "vw": 3, "us": 4, "vs": 5, "bed": 6, "moisture": 7, "foam": 8,
+          "turbid": 9, "susp": 10}
 
 
 # A tire push as a numpy record (the layout of silt_tire_push).
@@ -531,8 +534,8 @@ class Batch:
         return [{k: getattr(x, k) for k, _ in Ledger._fields_} for x in arr]
 
     def ledger_rows(self):
-        """Every window's ledger as one n x 10 FP64 array, columns in the
-        silt_ledger field order."""
+        """Every window's ledger as one FP64 array (a row per window), columns
+        in the silt_ledger field order."""
         arr = (Ledger * len(self.sheets))()
         check(lib().silt_batch_get_ledgers(self.h, arr), "batch_ledgers")
         return np.frombuffer(arr, dtype=np.float64).reshape(len(self.sheets), len(Ledger._fields_)).copy()

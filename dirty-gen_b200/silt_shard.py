@@ -7,7 +7,8 @@ the sum is exact)."""
 import numpy as np
 
 LEDGER_KEYS = ("water_m3", "slurry_m3", "frozen_water_m3", "frozen_slurry_m3", "spray_m3", "opened_m3", "total_m3",
-               "cut_m3", "reach_m3", "round_m3")
+               "cut_m3", "reach_m3", "round_m3", "suspended_m3", "settled_suspended_m3", "frozen_suspended_m3",
+               "entrained_m3", "turbid_m3", "turbid_settled_m3", "frozen_turbid_m3", "stirred_m3")
 
 
 def shard(n, rank, world):
@@ -18,7 +19,7 @@ def shard(n, rank, world):
 
 
 def gather_ledgers(local, n, dist=None, device="cpu"):
-    """`local`: {window index: ledger dict} of this rank. Returns an n x 10 FP64
+    """`local`: {window index: ledger dict} of this rank. Returns an n x len(LEDGER_KEYS) FP64
     array (rows in window order, columns LEDGER_KEYS) on every rank."""
     idx = list(local)
     rows = np.array([[float(local[w][k]) for k in LEDGER_KEYS] for w in idx], dtype=np.float64)
@@ -27,7 +28,7 @@ def gather_ledgers(local, n, dist=None, device="cpu"):
 
 def gather_ledger_rows(windows, rows, n, dist=None, device="cpu"):
     """`rows[k]` (columns LEDGER_KEYS) is window `windows[k]`'s ledger on this
-    rank, e.g. `Batch.ledger_rows()`. Returns the n x 10 FP64 table on every
+    rank, e.g. `Batch.ledger_rows()`. Returns the n x len(LEDGER_KEYS) FP64 table on every
     rank."""
     import torch
 

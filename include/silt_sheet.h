@@ -106,10 +106,21 @@ typedef struct {
      * total_m3 + cut_m3 - opened_m3 - round_m3 is conserved but for the
      * rounding of the other f32 updates (coupling, seeding). */
     double round_m3;
+    /* The tracers' books (FluidLedger's suspended part, src/fluid_core.rs:
+     * 496-505, and the silt book, :6171-6195), FP64: suspended solids in the
+     * water column, settled out of it, parked off the window, and lifted into
+     * suspension in all (wheel wakes, a river reach's inlet load); stirred silt
+     * in the column, settled, parked, and stirred in all. The reference adds
+     * the suspended account to its total; total_m3 here keeps the water and
+     * slurry books only, so it closes without them (the lifted solids come
+     * from the bed, not from the water). Each account closes on its own:
+     * suspended + settled + parked = entrained, and the same for the silt. */
+    double suspended_m3, settled_suspended_m3, frozen_suspended_m3, entrained_m3;
+    double turbid_m3, turbid_settled_m3, frozen_turbid_m3, stirred_m3;
 } silt_ledger;
 
-/* src/fluid_core.rs:289-320 (`RiverReach`); inlet_turbidity is kept for the
- * caller (suspended solids are off this path). */
+/* src/fluid_core.rs:289-320 (`RiverReach`); with turbidity on, the inlet's
+ * water arrives carrying inlet_turbidity of its column as suspended solids. */
 typedef struct {
     int32_t along_z, positive;
     float cross0, cross1;
@@ -152,6 +163,7 @@ typedef struct {
 /* src/fluid_core.rs:452-465 (`CoarseCell`), sheet fields. */
 typedef struct {
     float x, z, bed_m, water_m, slurry_m, moisture, u, v;
+    float turbidity;  /* suspended load plus stirred silt over the water column, 0..1 */
 } silt_coarse_cell;
 
 /* -------------------------------------------------------------- lifecycle */
@@ -204,7 +216,8 @@ int silt_get_coarse_cell(silt_sheet* s, int32_t i, int32_t j, silt_coarse_cell* 
 /* FluidCore::export_maps (src/fluid_core.rs:6941): height, vel_u, vel_v, moisture (res*res each; any may be NULL). */
 int silt_export_maps(silt_sheet* s, float* height, float* vel_u, float* vel_v, float* moisture);
 /* render_contract::publish_with_snow film/flow (src/render_contract.rs:483-496):
- * film = (water, slurry) per cell, flow = (vx, vz, speed, turbidity). Host pointers. */
+ * film = (water, slurry) per cell, flow = (vx, vz, speed, turbidity), the
+ * turbidity from the tracers' suspended load and stirred silt. Host pointers. */
 int silt_publish_film_flow(silt_sheet* s, float* film, float* flow);
 /* Same maps into device memory the caller owns (2*res*res and 4*res*res floats). */
 int silt_publish_film_flow_device(silt_sheet* s, float* d_film, float* d_flow);
@@ -234,7 +247,8 @@ int silt_window_bounds(silt_sheet* s, float* ox, float* oz, float* extent);
  * silt_sheet_create (snap_origin :9877-9892). Host only. */
 int silt_window_origin(float center_x, float center_z, int32_t res, float cell, float* origin2);
 /* Raw plane copy to host for tests and tools: which = 0 water, 1 slurry, 2 uw,
- * 3 vw, 4 us, 5 vs, 6 bed, 7 moisture. */
+ * 3 vw, 4 us, 5 vs, 6 bed, 7 moisture, 8 foam, 9 stirred silt (m), 10
+ * suspended solids (m). */
 int silt_read_plane(silt_sheet* s, int32_t which, float* host);
 int silt_write_plane(silt_sheet* s, int32_t which, const float* host);
 /* Device pointer of plane `which` (same indices) in the handle's current
@@ -362,8 +376,10 @@ int silt_set_river_reach(silt_sheet* s, const silt_river_reach* reach);
  * a paddle strip (drive_waves :7420-7480, before the coarse pair); restarts
  * the paddle clock. */
 int silt_set_wave_maker(silt_sheet* s, const silt_wave_maker* wave);
-/* FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097): kept for the
- * caller; the tracers that read it are not on this path (flow.A stays 0). */
+/* FluidCore::set_turbidity_enabled (src/fluid_core.rs:5097; on by default,
+ * :4994): the tires' wake lifts solids into suspension, which the sheet
+ * carries and settles (step_suspended :8750). Foam and stirred silt
+ * (step_tracers :6210) run either way. */
 int silt_set_turbidity_enabled(silt_sheet* s, int32_t on);
 /* FluidCore::set_hydro_solids (src/fluid_core.rs:5257-5260): the walls of the
  * next steps (n = 0 removes them). Each step builds the wall mask of the

@@ -88,6 +88,20 @@ def lib64():
     return _lib64
 
 
+_lib_rn = None
+LIB_RN_PATH = os.path.join(HERE, "liboracle_silt_rn.so")
+
+
+def lib_rn():
+    """The step with the device's elementary functions (-DORACLE_ELEM_RN)."""
+    global _lib_rn
+    if _lib_rn is None:
+        if not os.path.exists(LIB_RN_PATH):
+            build()
+        _lib_rn = _bind(ctypes.CDLL(LIB_RN_PATH), _f, CoreCfg, Tire)
+    return _lib_rn
+
+
 def _bind(L, _f, CoreCfg, Tire):
     if True:
         L.oracle_scratch_new.restype = _p
@@ -346,12 +360,14 @@ class Core:
         self._L().oracle_core_set_surface_diffusion(self.h, m2_s)
 
     def set_river_reach(self, reach):
-        """reach: dict(along_z, positive, cross0, cross1, rows, inlet_eta, outlet_eta, inlet_speed_m_s) or None."""
+        """reach: dict(along_z, positive, cross0, cross1, rows, inlet_eta, outlet_eta, inlet_speed_m_s[,
+        inlet_turbidity]) or None."""
         r = reach or {}
         self._L().oracle_core_set_river_reach(self.h, int(reach is not None), int(r.get("along_z", False)),
                                           int(r.get("positive", True)), r.get("cross0", 0.0), r.get("cross1", 0.0),
                                           int(r.get("rows", 1)), r.get("inlet_eta", 0.0), r.get("outlet_eta", 0.0),
                                           r.get("inlet_speed_m_s", 0.0))
+        self.set_reach_turbidity(r.get("inlet_turbidity", 0.0))
 
     def reach_bank_m3(self):
         return self._L().oracle_core_reach_bank(self.h)
@@ -427,6 +443,16 @@ class Core:
 
     def set_inflow(self, j, x0, x1, rate_m3_s):
         self._L().oracle_core_inflow(self.h, j, x0, x1, rate_m3_s)
+
+
+class CoreRN(Core):
+    """The same step with e^x, x^y and hypot as the double result rounded
+    once to float, the device's forms (liboracle_silt_rn). The C library's
+    expf differs from that on ~1e-4 of inputs; where such a 1-ulp factor is
+    absorbed by the f32 update the planes stay equal but an FP64 book moves,
+    and this build shows which."""
+
+    _L = staticmethod(lib_rn)
 
 
 class Core64(Core):

@@ -10,6 +10,9 @@
 // step, the interface included, becomes a double and each single-precision
 // libm call its double form. The model's constants keep their float values
 // (the `f` literals), so only the arithmetic's precision changes.
+//
+// With -DORACLE_ELEM_RN it builds the step with the device's elementary
+// functions (below), which attributes a book difference to them.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -36,6 +39,23 @@
 #define cosf cos
 #define sinf sin
 #define finite oracle_finite  // glibc declares finite(double)
+#endif
+
+#ifdef ORACLE_ELEM_RN
+// The same step with e^x, x^y and hypot taken as the double-precision result
+// rounded once to float, as the device computes them: the C library's expf,
+// powf and hypotf differ from that on a few inputs in 10^4. Used only to
+// attribute an FP64 book difference to those functions; the parity oracle is
+// the default build.
+static inline float oracle_exp_rn(float x) { return (float)std::exp((double)x); }
+static inline float oracle_pow_rn(float x, float y) { return (float)std::pow((double)x, (double)y); }
+static inline float oracle_hypot_rn(float x, float y) {
+    const double dx = (double)x, dy = (double)y;
+    return (float)std::sqrt(dx * dx + dy * dy);
+}
+#define expf oracle_exp_rn
+#define powf oracle_pow_rn
+#define hypotf oracle_hypot_rn
 #endif
 
 #include "sheet_oracle.h"
@@ -2775,7 +2795,7 @@ struct Core {
                     if (add <= 1.0e-8f) continue;
                     susp[idx] += add;
                     entrained_m3 += add * area;
-                    entrained64 += (double)add * (double)area;
+                    entrained64 += (double)(add * area);
                 }
         }
     }

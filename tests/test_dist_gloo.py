@@ -31,7 +31,8 @@ def step_windows(idx, wins):
         out[w] = dict(water_m3=led["water64"], slurry_m3=led["slurry64"], frozen_water_m3=0.0,
                       frozen_slurry_m3=0.0, spray_m3=led["spray_m3"], opened_m3=0.0,
                       total_m3=led["water64"] + led["slurry64"] + led["spray_m3"], cut_m3=0.0, reach_m3=0.0,
-                      round_m3=0.0)
+                      round_m3=0.0, suspended_m3=0.0, settled_suspended_m3=0.0, frozen_suspended_m3=0.0,
+                      entrained_m3=0.0, turbid_m3=0.0, turbid_settled_m3=0.0, frozen_turbid_m3=0.0, stirred_m3=0.0)
     return out
 
 

@@ -154,3 +154,34 @@ def test_turbidity_switch_turns_the_suspended_load_off():
     b = c.tracer_books()
     assert b["entrained_m3"] == 0.0 and b["suspended_m3"] == 0.0
     assert b["stirred_m3"] > 0.0
+
+
+def test_device_function_build_moves_only_a_book():
+    """The oracle built with e^x, x^y and hypot as the double result rounded
+    once (oracle.CoreRN, the device's forms) keeps every plane of a tire drive
+    bit for bit and moves only the settled-suspended book, by parts in 10^9:
+    a 1-ulp settling factor from the C library's expf is absorbed by the f32
+    update of the column but not by the FP64 book of what landed."""
+    F = np.float32
+
+    def drive(C):
+        c = C()
+        c.pour_water(-3.0, 3.0, -2.0, 8.0, 0.08)
+        c.pour_slurry(-1.0, 1.0, -2.0, 6.0, 0.03, 0, 0.6)
+        z = F(-1.0)
+        for k in range(24):
+            if k < 16:
+                for x, dz in ((-0.7, -1.2), (0.7, -1.2), (-0.7, 1.2), (0.7, 1.2)):
+                    c.push_tire(x=x, z=float(z + F(dz)), forward_x=0.0, forward_z=1.0, radius=0.38, width=0.2,
+                                speed=3.0, slip=0.6)
+            c.step(1.0 / 30.0)
+            z = F(z + F(3.0) * F(1.0 / 30.0))
+        return c
+
+    a, b = drive(O.Core), drive(O.CoreRN)
+    for n in ("water", "slurry", "uw", "vw", "foam", "turbid", "susp"):
+        assert np.array_equal(a.get(n).view(np.uint32), b.get(n).view(np.uint32)), n
+    ba, bb = a.tracer_books(), b.tracer_books()
+    for k in O.TRACER_BOOKS:
+        rel = abs(ba[k + "64"] - bb[k + "64"]) / max(abs(ba[k + "64"]), 1e-30)
+        assert rel < 1e-8, (k, rel)
