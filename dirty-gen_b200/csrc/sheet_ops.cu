@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "block_sum.cuh"
 #include "sheet_math.cuh"
 #include "sheet_ops.cuh"
 #include "launch_count.cuh"
@@ -183,14 +184,8 @@ __global__ void k_sum2(const float* a, const float* b, size_t n, double* out) {
         sa += (double)fmaxf(a[i], 0.0f);
         sb += (double)fmaxf(b[i], 0.0f);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        sa += __shfl_down_sync(0xffffffffu, sa, o);
-        sb += __shfl_down_sync(0xffffffffu, sb, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(out, sa);
-        atomicAdd(out + 1, sb);
-    }
+    ::silt::block_add(sa, out);
+    ::silt::block_add(sb, out + 1);
 }
 
 __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsigned int* out) {
@@ -199,8 +194,7 @@ __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsig
     GRID_STRIDE(i, n) {
         for (int p = 0; p < np; ++p) c += !finite_f(planes[p][i]);
     }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+    ::silt::block_add(c, out);
 }
 
 // src/fluid_core.rs:7521-7581 eddy_shear, the snapshot pass: neighbours in
@@ -316,8 +310,7 @@ __global__ void k_diffuse_apply(float* h, const float* delta, size_t n, double* 
             part += (double)h1 - (double)h0;
         }
     }
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
-    if ((threadIdx.x & 31) == 0 && part != 0.0 && ledger) atomicAdd(ledger, part);
+    if (ledger) ::silt::block_add(part, ledger);
 }
 
 cudaError_t op_map_water_bed(const float* bed_in, const float* water_in, float* bed, float* water, float* moisture,
@@ -419,14 +412,8 @@ __global__ void k_sum_tracers(const float* const* susp, const float* const* turb
         sa += (double)fmaxf(a[i], 0.0f);
         sb += (double)fmaxf(b[i], 0.0f);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        sa += __shfl_down_sync(0xffffffffu, sa, o);
-        sb += __shfl_down_sync(0xffffffffu, sb, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (sa != 0.0) atomicAdd(out + 16 * (size_t)w + 14, sa);
-        if (sb != 0.0) atomicAdd(out + 16 * (size_t)w + 15, sb);
-    }
+    ::silt::block_add(sa, out + 16 * (size_t)w + 14);
+    ::silt::block_add(sb, out + 16 * (size_t)w + 15);
 }
 cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, int n, double* out,
                            cudaStream_t st) {

@@ -157,6 +157,7 @@ struct silt_sheet {
     void* tr_mem = nullptr;
     silt::tracers::Planes tr;
     silt::tracers::Runner tr_run;
+    bool tr_rescan = true;  // the tracer planes were rewritten (attach, move): scan the silt span once
     float center[2] = {0.0f, 0.0f};  // the chase point (set_center / recenter)
     bool reach_on = false;           // FluidCore::set_river_reach
     silt_river_reach reach;
@@ -242,6 +243,9 @@ silt::tracers::Window tracer_window(silt_sheet* s, const std::vector<silt_tire_p
     w.T = s->tr;
     w.push = ps.empty() ? nullptr : ps.data();
     w.npush = (int)ps.size();
+    w.rescan = s->tr_rescan ? 1 : 0;
+    // A river inlet carrying a load writes its rows' suspended solids.
+    w.sup_all = (s->reach_on && s->reach.inlet_turbidity != 0.0f) ? 1 : 0;
     return w;
 }
 
@@ -1179,6 +1183,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         // suspended load (:6082-6089).
         const silt::tracers::Window w = tracer_window(s, ps);
         CK(silt::tracers::step_tracers(s->tr_run, &w, 1, dt, s->st));
+        s->tr_rescan = false;
     }
     if ((rc = reach_step(s))) return rc;
     if (s->turbidity) {
@@ -1345,6 +1350,7 @@ int silt_recenter(silt_sheet* s, float cx, float cz) {
     }
     if ((rc = silt::fine::move_window(s->fine, s, di, dj, scroll))) return rc;
     CK(silt::tracers::reset_indices(s->tr, s->res, s->st));  // reset_tracer_indices (src/fluid_core.rs:9125, :9225)
+    s->tr_rescan = true;
     unsigned int used = 0, overflow = 0;
     CK(silt::park::usage(T, &used, &overflow, s->st));
     if (overflow) return fail_cuda(cudaErrorMemoryAllocation, "parked cells: table overflow");
@@ -2349,6 +2355,7 @@ int silt_batch_step(silt_batch* b, float dt) {
         tw.reserve(n);
         for (int w = 0; w < n; ++w) tw.push_back(tracer_window(b->sheets[w], ps[w]));
         CK(silt::tracers::step_tracers(b->tr_run, tw.data(), n, dt, b->st));
+        for (silt_sheet* s : b->sheets) s->tr_rescan = false;
         for (silt_sheet* s : b->sheets)
             if ((rc = reach_step(s))) return rc;
         std::vector<silt::tracers::Window> sw;

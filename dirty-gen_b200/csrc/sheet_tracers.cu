@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "block_sum.cuh"
 #include "launch_count.cuh"
 #include "sheet_math.cuh"
 
@@ -47,6 +48,8 @@ struct Ctl {
     int tspan2[4];  // silt span after the transport
     int tspan3[4];  // silt span after the sources
     int mbox[4];    // where wet and shore marks may be set (the last collection box)
+    int ssup[4];    // this step's suspended pass: a box holding every cell whose load is not 0
+    int ssup_next[4];  // the same for the next step, grown by every writer of the load
     unsigned int live_foam_prev;
 };
 
@@ -148,33 +151,8 @@ __device__ __forceinline__ void add_silt(float& t, float dh, float area, double&
     book += (double)(add * area);
 }
 
-// Block-wide reductions to one atomic per block: thousands of warps adding
-// into one word would serialise on it. Every thread of the block calls them.
-template <typename V>
-__device__ __forceinline__ V block_sum(V v) {
-    __shared__ V part[32];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) part[warp] = v;
-    __syncthreads();
-    v = V(0);
-    if (warp == 0) {
-        v = lane < (int)(blockDim.x >> 5) ? part[lane] : V(0);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    }
-    __syncthreads();
-    return v;  // the sum, in thread 0
-}
-
-__device__ __forceinline__ void block_book(double v, double* book) {
-    v = block_sum(v);
-    if (threadIdx.x == 0 && v != 0.0) atomicAdd(book, v);
-}
-
-__device__ __forceinline__ void block_count(unsigned int v, unsigned int* to) {
-    v = block_sum(v);
-    if (threadIdx.x == 0 && v) atomicAdd(to, v);
-}
+__device__ __forceinline__ void block_book(double v, double* book) { ::silt::block_add(v, book); }
+__device__ __forceinline__ void block_count(unsigned int v, unsigned int* to) { ::silt::block_add(v, to); }
 
 // Sets *flag when any thread of the block passes `any`.
 __device__ __forceinline__ void block_flag(bool any, unsigned int* flag) {
@@ -300,6 +278,13 @@ __global__ void k_entrain(const Job* jobs) {
     const int res = S.res;
     const float cell = S.cell, area = cell * cell;
     double b = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && J.ebox[0] <= J.ebox[1]) {
+        int* sup = ctl_of(T.st)->ssup_next;  // the wake's cells may now hold a load
+        atomicMin(&sup[0], J.ebox[0]);
+        atomicMax(&sup[1], J.ebox[1]);
+        atomicMin(&sup[2], J.ebox[2]);
+        atomicMax(&sup[3], J.ebox[3]);
+    }
     BOX_CELLS(res, J.ebox[0], J.ebox[1], J.ebox[2], J.ebox[3]) {
         for (int k = 0; k < J.npush; ++k) {
             const silt_tire_push& p = J.push[k];
@@ -338,6 +323,29 @@ __global__ void k_entrain(const Job* jobs) {
 }
 
 // ------------------------------------------------------------ step_tracers
+//
+// The silt span at a step's start (turbid_span, :9766-9795) is kept exact
+// between steps instead of scanned: every kernel that changes silt records
+// the box of the cells it leaves above 1e-8, and a cell outside the region a
+// kernel touches keeps a value that was already at most 1e-8. A scan of the
+// whole window runs only after the planes were rewritten wholesale (attach,
+// window moves). Launches: [scan], begin, box, collect (with both advections
+// into scratch), go, commit, settle, spawn, sync begin, clear and sync.
+
+// The start span of the jobs whose planes were rewritten (`rescan`); the
+// reset that rewrote them left the span empty.
+__global__ void k_scan(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (!J.rescan) return;
+    const float* turbid = T.turbid[0];
+    const int res = S.res;
+    LocalBox lb;
+    CELLS(S) {
+        if (turbid[g] > 1.0e-8f) lb.add((int)(g % res), (int)(g / res));
+    }
+    lb.commit(T.st->tspan);
+}
 
 __global__ void k_begin(const Job* jobs) {
     ::silt::dep_wait();
@@ -346,35 +354,14 @@ __global__ void k_begin(const Job* jobs) {
     State* st = T.st;
     const int res = S.res;
     Ctl* c = ctl_of(st);
-    box_clear(st->tspan, res);
     box_clear(c->tspan2, res);
     box_clear(c->tspan3, res);
     box_clear(c->cbox, res);
-    st->live_silt = 0;
+    st->live_silt = box_empty(st->tspan) ? 0u : 1u;
     st->wet_any = 0;
     c->active = 0;
     c->go = 0;
     c->live_foam_prev = st->live_foam;
-}
-
-// Silt cells above 1e-8 into `box` (which==0: the step's start, also the
-// live-silt flag; 1: after the transport; 2: after the sources).
-__global__ void k_scan(const Job* jobs, int which) {
-    ::silt::dep_wait();
-    JOB;
-    const float* turbid = T.turbid[0];
-    State* st = T.st;
-    Ctl* c = ctl_of(st);
-    if (which > 0 && !c->go) return;
-    int* box = which == 0 ? st->tspan : (which == 1 ? c->tspan2 : c->tspan3);
-    const int res = S.res;
-    LocalBox lb;
-    CELLS(S) {
-        if (turbid[g] > 1.0e-8f) lb.add((int)(g % res), (int)(g / res));
-    }
-    const bool any = lb.b[1] >= 0;
-    lb.commit(box);
-    if (which == 0) block_flag(any, &st->live_silt);
 }
 
 // collect_tracer_wet (:6248-6293) and tracer_visit_box (:6296-6337).
@@ -419,92 +406,6 @@ __global__ void k_collect_box(const Job* jobs) {
     c->cbox[3] = min(b[3] + 2, res - 1);
 }
 
-__global__ void k_collect(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    uint8_t* mark = T.mark;
-    State* st = T.st;
-    Ctl* c = ctl_of(st);
-    if (!c->active) return;
-    const int res = S.res;
-    // Wet and shore marks are cleared where the last collection may have set
-    // them and set inside this step's box; live marks stay.
-    const Box b = box_of(c->cbox);
-    const Box u = box_union(b, box_of(c->mbox));
-    bool any = false;
-    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
-        uint8_t m = mark[g] & LIVE;
-        if (in_box(b, i, j)) {
-            const float h = S.water[g] + S.slurry[g];
-            if (finite_f(h) && !(h < 0.004f)) {
-                m |= WET;
-                any = true;
-                if (shore_wet_cell(S.water, res, i, j)) m |= SHORE;
-            }
-        }
-        mark[g] = m;
-    }
-    block_flag(any, &st->wet_any);
-}
-
-__global__ void k_go(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    State* st = T.st;
-    Ctl* c = ctl_of(st);
-    c->go = (c->active && (st->wet_any || st->live_silt)) ? 1 : 0;
-    if (c->active) {
-        for (int k = 0; k < 4; ++k) c->mbox[k] = c->cbox[k];
-    }
-}
-
-// advect_foam (:6352-6397), first half: the new value of every wet or
-// foam-live cell into `tmp` (the field itself is read).
-__global__ void k_foam_advect(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    const float* foam = T.foam[0];
-    float* tmp = T.foam[1];
-    const uint8_t* mark = T.mark;
-    const float dt = J.dt, decay = J.foam_decay;
-    Ctl* c = ctl_of(T.st);
-    if (!c->go || !c->live_foam_prev) return;
-    const int res = S.res;
-    const Box b = box_of(c->cbox);  // the wet and foam-live cells lie inside
-    BOX_CELLS(res, b.i0, b.i1, b.j0, b.j1) {
-        const uint8_t m = mark[g];
-        if (m & WET) {
-            const float u = S.uw[g], v = S.vw[g];  // wet cells are far above the dry cut
-            float sample = 0.0f;
-            if (finite_f(u) && finite_f(v)) {
-                const float x = (float)i - u * dt / S.cell;
-                const float z = (float)j - v * dt / S.cell;
-                sample = sample_foam(foam, res, x, z);
-            }
-            const float vv = sample * decay;
-            tmp[g] = (vv > 1.0e-4f && finite_f(vv)) ? fminf(vv, FOAM_EQ) : 0.0f;
-        } else if (m & LIVE) {
-            tmp[g] = 0.0f;
-        }
-    }
-}
-
-// Second half: the new values replace the field.
-__global__ void k_foam_commit(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    float* foam = T.foam[0];
-    const float* tmp = T.foam[1];
-    const uint8_t* mark = T.mark;
-    Ctl* c = ctl_of(T.st);
-    if (!c->go || !c->live_foam_prev) return;
-    const Box b = box_of(c->cbox);
-    BOX_CELLS(S.res, b.i0, b.i1, b.j0, b.j1) {
-        if (mark[g] & (WET | LIVE)) foam[g] = tmp[g];
-    }
-}
-
 // The silt a donor cell gives across its four edges in flux_thickness's
 // order (x edges before z edges, each axis in index order): to the left,
 // right, up and down neighbour (0 where it is not the donor or the edge lies
@@ -544,71 +445,145 @@ __device__ __forceinline__ void donor_flux(const Sheet& S, const float* T, int i
     }
 }
 
-// advect_turbid (:6421-6470): new silt of the span's cells into `tmp`.
-__global__ void k_turbid_advect(const Job* jobs) {
+// advect_turbid (:6421-6470) of cell (i, j) of the grown span: its new silt.
+__device__ __forceinline__ float turbid_after(const Sheet& S, const float* T, int i, int j, int bi0, int bi1, int bj0,
+                                              int bj1, float dt) {
+    const size_t g = (size_t)j * S.res + i;
+    float own[4], nb[4];
+    donor_flux(S, T, i, j, bi0, bi1, bj0, bj1, dt, own);
+    float removed = 0.0f;
+    for (int k = 0; k < 4; ++k)
+        if (own[k] > 0.0f) removed += own[k];
+    // What the neighbours give this cell, in the reference's edge order.
+    float added = 0.0f;
+    if (i - 1 >= bi0) {
+        donor_flux(S, T, i - 1, j, bi0, bi1, bj0, bj1, dt, nb);
+        if (nb[1] > 0.0f) added += nb[1];
+    }
+    if (i + 1 <= bi1) {
+        donor_flux(S, T, i + 1, j, bi0, bi1, bj0, bj1, dt, nb);
+        if (nb[0] > 0.0f) added += nb[0];
+    }
+    if (j - 1 >= bj0) {
+        donor_flux(S, T, i, j - 1, bi0, bi1, bj0, bj1, dt, nb);
+        if (nb[3] > 0.0f) added += nb[3];
+    }
+    if (j + 1 <= bj1) {
+        donor_flux(S, T, i, j + 1, bi0, bi1, bj0, bj1, dt, nb);
+        if (nb[2] > 0.0f) added += nb[2];
+    }
+    float t = T[g];
+    if (removed == 0.0f && added == 0.0f) {
+        if (!finite_f(t)) t = 0.0f;
+    } else {
+        const float next = t - removed + added;
+        t = finite_f(next) ? fmaxf(next, 0.0f) : 0.0f;
+    }
+    return t;
+}
+
+// The wet set (marks) and, into scratch, both advections: advect_foam
+// (:6352-6397) of every wet or foam-live cell and advect_turbid of the grown
+// span. They read only fields no step kernel has changed yet; whether they
+// take effect is decided after the wet set is known (k_go, k_commit). The
+// grown span lies inside the collection box.
+__global__ void k_collect(const Job* jobs) {
     ::silt::dep_wait();
-    const Job J = jobs[blockIdx.y];
-    const Sheet& S = J.S;
-    const float* T = J.T.turbid[0];
-    float* tmp = J.T.turbid[1];
-    State* st = J.T.st;
-    const float dt = J.dt;
+    JOB;
+    uint8_t* mark = T.mark;
+    State* st = T.st;
     Ctl* c = ctl_of(st);
-    if (!c->go || box_empty(st->tspan)) return;
+    if (!c->active) return;
     const int res = S.res;
-    int bi0, bi1, bj0, bj1;
-    grown(st->tspan, res, bi0, bi1, bj0, bj1);
-    BOX_CELLS(res, bi0, bi1, bj0, bj1) {
-        float own[4], nb[4];
-        donor_flux(S, T, i, j, bi0, bi1, bj0, bj1, dt, own);
-        float removed = 0.0f;
-        for (int k = 0; k < 4; ++k)
-            if (own[k] > 0.0f) removed += own[k];
-        // What the neighbours give this cell, in the reference's edge order.
-        float added = 0.0f;
-        if (i - 1 >= bi0) {
-            donor_flux(S, T, i - 1, j, bi0, bi1, bj0, bj1, dt, nb);
-            if (nb[1] > 0.0f) added += nb[1];
+    const float dt = J.dt, decay = J.foam_decay;
+    const float* foam = T.foam[0];
+    float* ftmp = T.foam[1];
+    const float* silt = T.turbid[0];
+    float* ttmp = T.turbid[1];
+    const bool foam_on = c->live_foam_prev != 0;
+    const Box tb = box_empty(st->tspan) ? Box{0, -1, 0, -1} : grown_box(st->tspan, res);
+    // Wet and shore marks are cleared where the last collection may have set
+    // them and set inside this step's box; live marks stay.
+    const Box b = box_of(c->cbox);
+    const Box u = box_union(b, box_of(c->mbox));
+    bool any = false;
+    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
+        uint8_t m = mark[g] & LIVE;
+        if (in_box(b, i, j)) {
+            const float h = S.water[g] + S.slurry[g];
+            if (finite_f(h) && !(h < 0.004f)) {
+                m |= WET;
+                any = true;
+                if (shore_wet_cell(S.water, res, i, j)) m |= SHORE;
+            }
         }
-        if (i + 1 <= bi1) {
-            donor_flux(S, T, i + 1, j, bi0, bi1, bj0, bj1, dt, nb);
-            if (nb[0] > 0.0f) added += nb[0];
+        mark[g] = m;
+        if (foam_on) {
+            if (m & WET) {
+                const float uu = S.uw[g], vv = S.vw[g];  // wet cells are far above the dry cut
+                float sample = 0.0f;
+                if (finite_f(uu) && finite_f(vv)) {
+                    const float x = (float)i - uu * dt / S.cell;
+                    const float z = (float)j - vv * dt / S.cell;
+                    sample = sample_foam(foam, res, x, z);
+                }
+                const float fv = sample * decay;
+                ftmp[g] = (fv > 1.0e-4f && finite_f(fv)) ? fminf(fv, FOAM_EQ) : 0.0f;
+            } else if (m & LIVE) {
+                ftmp[g] = 0.0f;
+            }
         }
-        if (j - 1 >= bj0) {
-            donor_flux(S, T, i, j - 1, bi0, bi1, bj0, bj1, dt, nb);
-            if (nb[3] > 0.0f) added += nb[3];
-        }
-        if (j + 1 <= bj1) {
-            donor_flux(S, T, i, j + 1, bi0, bi1, bj0, bj1, dt, nb);
-            if (nb[2] > 0.0f) added += nb[2];
-        }
-        float t = T[g];
-        if (removed == 0.0f && added == 0.0f) {
-            if (!finite_f(t)) t = 0.0f;
-        } else {
-            const float next = t - removed + added;
-            t = finite_f(next) ? fmaxf(next, 0.0f) : 0.0f;
-        }
-        tmp[g] = t;
+        if (in_box(tb, i, j)) ttmp[g] = turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, dt);
+    }
+    block_flag(any, &st->wet_any);
+}
+
+__global__ void k_go(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State* st = T.st;
+    Ctl* c = ctl_of(st);
+    c->go = (c->active && (st->wet_any || st->live_silt)) ? 1 : 0;
+    if (c->active) {
+        for (int k = 0; k < 4; ++k) c->mbox[k] = c->cbox[k];
     }
 }
 
-__global__ void k_turbid_commit(const Job* jobs) {
+// The advections take effect: foam on every wet or foam-live cell, silt on
+// the grown span, whose cells above 1e-8 are the span after the transport
+// (outside it no cell holds more than 1e-8).
+__global__ void k_commit(const Job* jobs) {
     ::silt::dep_wait();
-    const Job J = jobs[blockIdx.y];
-    const Sheet& S = J.S;
-    float* T = J.T.turbid[0];
-    const float* tmp = J.T.turbid[1];
-    State* st = J.T.st;
+    JOB;
+    State* st = T.st;
     Ctl* c = ctl_of(st);
-    if (!c->go || box_empty(st->tspan)) return;
+    if (!c->go) return;
     const int res = S.res;
-    int bi0, bi1, bj0, bj1;
-    grown(st->tspan, res, bi0, bi1, bj0, bj1);
-    BOX_CELLS(res, bi0, bi1, bj0, bj1) T[g] = tmp[g];
+    const bool foam_on = c->live_foam_prev != 0, silt_on = !box_empty(st->tspan);
+    if (!foam_on && !silt_on) return;
+    const Box fb = foam_on ? box_of(c->cbox) : Box{0, -1, 0, -1};
+    const Box tb = silt_on ? grown_box(st->tspan, res) : Box{0, -1, 0, -1};
+    const Box u = box_union(fb, tb);
+    float* foam = T.foam[0];
+    const float* ftmp = T.foam[1];
+    float* silt = T.turbid[0];
+    const float* ttmp = T.turbid[1];
+    const uint8_t* mark = T.mark;
+    LocalBox lb;
+    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
+        if (in_box(fb, i, j) && (mark[g] & (WET | LIVE))) foam[g] = ftmp[g];
+        if (in_box(tb, i, j)) {
+            const float t = ttmp[g];
+            silt[g] = t;
+            if (t > 1.0e-8f) lb.add(i, j);
+        }
+    }
+    lb.commit(c->tspan2);
 }
 
-// settle_turbid (:6473-6509) on the span after the transport.
+// settle_turbid (:6473-6509) on the span after the transport; the cells it
+// leaves above 1e-8 go into the span after the sources.
 __global__ void k_settle(const Job* jobs) {
     ::silt::dep_wait();
     const Job J = jobs[blockIdx.y];
@@ -624,6 +599,7 @@ __global__ void k_settle(const Job* jobs) {
     int bi0, bi1, bj0, bj1;
     grown(c->tspan2, res, bi0, bi1, bj0, bj1);
     double b = 0.0;
+    LocalBox lb;
     BOX_CELLS(res, bi0, bi1, bj0, bj1) {
         const float h = S.water[g] + S.slurry[g];
         const float column = finite_f(T[g]) ? fmaxf(T[g], 0.0f) : 0.0f;
@@ -639,14 +615,17 @@ __global__ void k_settle(const Job* jobs) {
         const float stay = column * keep;
         b += (double)((column - stay) * area);
         T[g] = stay;
+        if (stay > 1.0e-8f) lb.add(i, j);
     }
+    lb.commit(c->tspan3);
     block_book(b, book);
 }
 
-// spawn_foam_and_silt (:6511-6520) on each wet cell: the tires of this
-// launch in push order (spawn_tire_tracers :6599-6665), then, in the last
-// launch, the shore (spawn_shore_tracers :6667-6684) and Froude breaking
-// (spawn_breaking_speed :6545-6558).
+// spawn_foam_and_silt (:6511-6520) on each wet cell: the tires in push order
+// (spawn_tire_tracers :6599-6665), then the shore (spawn_shore_tracers
+// :6667-6684) and Froude breaking (spawn_breaking_speed :6545-6558). Sources
+// only add silt, so a cell above 1e-8 after the settling stays above it; the
+// wet cells that end above it join the span after the sources.
 __global__ void k_spawn(const Job* jobs) {
     ::silt::dep_wait();
     const Job J = jobs[blockIdx.y];
@@ -661,6 +640,7 @@ __global__ void k_spawn(const Job* jobs) {
     const int res = S.res;
     const float cell = S.cell, area = cell * cell;
     double b = 0.0;
+    LocalBox lb;
     const Box cb = box_of(c->cbox);  // the wet cells lie inside
     BOX_CELLS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
         const uint8_t m = mark[g];
@@ -725,41 +705,9 @@ __global__ void k_spawn(const Job* jobs) {
         }
         foam[g] = f;
         T[g] = t;
+        if (t > 1.0e-8f) lb.add(i, j);
     }
-    block_book(b, book);
-}
-
-// clear_dry_tracers (:6712-6739).
-__global__ void k_clear(const Job* jobs) {
-    ::silt::dep_wait();
-    const Job J = jobs[blockIdx.y];
-    const Sheet& S = J.S;
-    float* foam = J.T.foam[0];
-    float* T = J.T.turbid[0];
-    const uint8_t* mark = J.T.mark;
-    double* book = J.T.books + 3;
-    Ctl* c = ctl_of(J.T.st);
-    if (!c->go) return;
-    const int res = S.res;
-    const float area = S.cell * S.cell;
-    const Box sb = box_empty(c->tspan3) ? Box{0, -1, 0, -1} : grown_box(c->tspan3, res);
-    const Box u = box_union(box_of(c->cbox), sb);  // the wet cells lie in the collection box
-    double b = 0.0;
-    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
-        const float h = S.water[g] + S.slurry[g];
-        if (mark[g] & WET) {
-            if (!finite_f(h) || h < 0.004f || !finite_f(foam[g])) foam[g] = 0.0f;
-        }
-        if (!in_box(sb, i, j)) continue;
-        if (!finite_f(h) || h < 1.0e-5f) {
-            if (T[g] > 0.0f) {
-                b += (double)(T[g] * area);
-                T[g] = 0.0f;
-            }
-        } else if (!finite_f(T[g])) {
-            T[g] = 0.0f;
-        }
-    }
+    lb.commit(c->tspan3);  // with the settled cells': the silt span after the sources
     block_book(b, book);
 }
 
@@ -772,33 +720,70 @@ __global__ void k_sync_begin(const Job* jobs) {
     if (!ctl_of(st)->go) return;
     st->live_foam = 0;
     box_clear(st->live_box, res);
+    box_clear(st->tspan, res);  // rebuilt by the clear: the next step's start span
 }
 
-// sync_foam_live (:6339-6349).
-__global__ void k_sync(const Job* jobs) {
+// clear_dry_tracers (:6712-6739) then sync_foam_live (:6339-6349), per cell.
+// The clear only lowers silt, so the grown span after the sources holds every
+// cell above 1e-8 after it: those cells are the next step's start span.
+// Outside the collection box no cell is wet, and the live cells of the last
+// sync lie inside it (it covers their box), so every mark there is 0.
+__global__ void k_clear_sync(const Job* jobs) {
     ::silt::dep_wait();
     JOB;
-    const float* foam = T.foam[0];
+    float* foam = T.foam[0];
+    float* silt = T.turbid[0];
     uint8_t* mark = T.mark;
     State* st = T.st;
-    if (!ctl_of(st)->go) return;
+    Ctl* c = ctl_of(st);
+    double* book = T.books + 3;
+    if (!c->go) return;
     const int res = S.res;
+    const float area = S.cell * S.cell;
+    const Box cb = box_of(c->cbox);
+    const Box sb = box_empty(c->tspan3) ? Box{0, -1, 0, -1} : grown_box(c->tspan3, res);
+    const Box u = box_union(cb, sb);
+    double b = 0.0;
     unsigned int cnt = 0;
-    LocalBox lb;
-    // Outside the collection box no cell is wet, and the live cells of the
-    // last sync lie inside it (it covers their box), so every mark there is 0.
-    const Box cb = box_of(ctl_of(st)->cbox);
-    BOX_CELLS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
-        uint8_t m = mark[g] & (WET | SHORE);
-        if ((m & WET) && finite_f(foam[g]) && foam[g] > 1.0e-4f) {
-            m |= LIVE;
-            ++cnt;
-            lb.add(i, j);
+    LocalBox live, span;
+    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
+        const float h = S.water[g] + S.slurry[g];
+        const uint8_t m = mark[g];
+        float f = foam[g];
+        if (m & WET) {
+            if (!finite_f(h) || h < 0.004f || !finite_f(f)) {
+                f = 0.0f;
+                foam[g] = 0.0f;
+            }
         }
-        mark[g] = m;
+        if (in_box(sb, i, j)) {
+            float t = silt[g];
+            if (!finite_f(h) || h < 1.0e-5f) {
+                if (t > 0.0f) {
+                    b += (double)(t * area);
+                    t = 0.0f;
+                    silt[g] = 0.0f;
+                }
+            } else if (!finite_f(t)) {
+                t = 0.0f;
+                silt[g] = 0.0f;
+            }
+            if (t > 1.0e-8f) span.add(i, j);
+        }
+        if (in_box(cb, i, j)) {
+            uint8_t mm = m & (WET | SHORE);
+            if ((mm & WET) && finite_f(f) && f > 1.0e-4f) {
+                mm |= LIVE;
+                ++cnt;
+                live.add(i, j);
+            }
+            mark[g] = mm;
+        }
     }
-    lb.commit(st->live_box);
+    live.commit(st->live_box);
+    span.commit(st->tspan);
     block_count(cnt, &st->live_foam);
+    block_book(b, book);
 }
 
 // ---------------------------------------------------------- step_suspended
@@ -808,24 +793,39 @@ __global__ void k_susp_begin(const Job* jobs) {
     JOB;
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     State* st = T.st;
-    box_clear(st->sbox, S.res);
+    const int res = S.res;
+    Ctl* c = ctl_of(st);
+    box_clear(st->sbox, res);
     st->capped = 0;
+    // The cells that may hold a load: every writer since the last pass grew
+    // the next box; a river inlet carrying a load writes its rows.
+    for (int k = 0; k < 4; ++k) c->ssup[k] = c->ssup_next[k];
+    if (J.sup_all) {
+        c->ssup[0] = 0;
+        c->ssup[1] = res - 1;
+        c->ssup[2] = 0;
+        c->ssup[3] = res - 1;
+    }
+    box_clear(c->ssup_next, res);
 }
 
 // advect_suspended's first loop (:8826-8870): grains fall out at their fall
-// speed; a dry cell or a load above the water settles whole.
+// speed; a dry cell or a load above the water settles whole. Cells outside
+// the support box hold no load, and the loop leaves them as they are.
 __global__ void k_susp_settle(const Job* jobs) {
     ::silt::dep_wait();
     JOB;
     float* susp = T.susp[0];
     State* st = T.st;
+    Ctl* c = ctl_of(st);
     const float dt = J.dt;
     double* book = T.books + 1;
     const int res = S.res;
     const float area = S.cell * S.cell;
+    const Box sup = box_of(c->ssup);
     double b = 0.0;
-    LocalBox lb;
-    CELLS(S) {
+    LocalBox lb, held;
+    BOX_CELLS(res, sup.i0, sup.i1, sup.j0, sup.j1) {
         float s = susp[g];
         if (!finite_f(s) || s <= 1.0e-12f) {
             if (__float_as_uint(s) != 0u) susp[g] = 0.0f;
@@ -844,9 +844,11 @@ __global__ void k_susp_settle(const Job* jobs) {
             s -= landed;
             susp[g] = s;
         }
-        if (s > 1.0e-8f) lb.add((int)(g % res), (int)(g / res));
+        if (s > 1.0e-8f) lb.add(i, j);
+        if (s != 0.0f) held.add(i, j);
     }
     lb.commit(st->sbox);
+    held.commit(c->ssup_next);
     block_book(b, book);
 }
 
@@ -977,6 +979,7 @@ __global__ void k_susp_give(const Job* jobs) {
     const bool open = S.surface_driven != 0;
     double b = 0.0;
     unsigned int capped = 0;
+    LocalBox held;
     BOX_CELLS(res, bi0, bi1, bj0, bj1) {
         float next = susp[g];
         const Donor D = donor_of(S, susp, i, j, dt);
@@ -1025,7 +1028,9 @@ __global__ void k_susp_give(const Job* jobs) {
             s = w;
         }
         susp[g] = s;
+        if (s != 0.0f) held.add(i, j);
     }
+    held.commit(ctl_of(st)->ssup_next);
     block_book(b, book);
     block_count(capped, &st->capped);
 }
@@ -1035,9 +1040,17 @@ __global__ void k_reset_live(uint8_t* mark, State* st, int res, size_t n) {
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x)
         mark[g] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // The planes were rewritten: the silt span is scanned again before the
+        // next tracer step, and any cell may hold a suspended load.
+        Ctl* c = ctl_of(st);
         st->live_foam = 0;
         box_clear(st->live_box, res);
-        box_clear(ctl_of(st)->mbox, res);
+        box_clear(st->tspan, res);
+        box_clear(c->mbox, res);
+        c->ssup_next[0] = 0;
+        c->ssup_next[1] = res - 1;
+        c->ssup_next[2] = 0;
+        c->ssup_next[3] = res - 1;
     }
 }
 
@@ -1144,6 +1157,8 @@ cudaError_t upload(Runner& R, const Window* w, int n, float dt, float foam_decay
                    (std::isfinite(p.slip) && fabsf(p.slip) >= 0.05f);
         }
         J.wake = wake ? 1 : 0;
+        J.rescan = w[k].rescan;
+        J.sup_all = w[k].sup_all;
         push_box(w[k].S, w[k].push, w[k].npush, J.pbox);
         entrain_box(w[k].S, w[k].push, w[k].npush, J.ebox);
         J.dt = dt;
@@ -1230,22 +1245,18 @@ cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream
     cudaError_t e = upload(R, w, n, dt, foam_decay, silt_keep, st, &jobs);
     if (e != cudaSuccess) return e;
     const int bx = blocks_x(w, n);
+    bool rescan = false;
+    for (int k = 0; k < n; ++k) rescan = rescan || w[k].rescan;
+    if (rescan) LAUNCH(k_scan, bx, jobs);
     LAUNCH(k_begin, 1, jobs);
-    LAUNCH(k_scan, bx, jobs, 0);
     LAUNCH(k_collect_box, 1, jobs);
     LAUNCH(k_collect, bx, jobs);
     LAUNCH(k_go, 1, jobs);
-    LAUNCH(k_foam_advect, bx, jobs);
-    LAUNCH(k_foam_commit, bx, jobs);
-    LAUNCH(k_turbid_advect, bx, jobs);
-    LAUNCH(k_turbid_commit, bx, jobs);
-    LAUNCH(k_scan, bx, jobs, 1);
+    LAUNCH(k_commit, bx, jobs);
     LAUNCH(k_settle, bx, jobs);
     LAUNCH(k_spawn, bx, jobs);
-    LAUNCH(k_scan, bx, jobs, 2);
-    LAUNCH(k_clear, bx, jobs);
     LAUNCH(k_sync_begin, 1, jobs);
-    LAUNCH(k_sync, bx, jobs);
+    LAUNCH(k_clear_sync, bx, jobs);
     return cudaSuccess;
 }
 

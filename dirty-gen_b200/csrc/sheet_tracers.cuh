@@ -59,6 +59,8 @@ struct Job {
     int wake;                    // a tire with speed or slip, or a surface drive
     int pbox[4];                 // the tires' reach boxes (tracer_visit_box's tire part; empty when none)
     int ebox[4];                 // entrain_wake's cells: the union of the tires' wake boxes (empty when none)
+    int rescan;                  // the planes were rewritten: scan the silt span before the step
+    int sup_all;                 // something outside the tracer kernels wrote the suspended load (a river inlet)
     float dt, foam_decay, silt_keep;
 };
 
@@ -81,6 +83,8 @@ struct Window {
     Planes T;
     const silt_tire_push* push;
     int npush;
+    int rescan = 0;   // the planes were rewritten since the last tracer step (attach, window move)
+    int sup_all = 0;  // a river inlet writes the suspended load outside the tracer kernels
 };
 
 size_t plane_bytes(int res);  // device bytes of one window's tracer planes
