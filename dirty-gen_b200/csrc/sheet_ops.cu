@@ -188,6 +188,51 @@ __global__ void k_sum2(const float* a, const float* b, size_t n, double* out) {
     ::silt::block_add(sb, out + 1);
 }
 
+// The last block of a launch to finish (the ticket counts finished blocks)
+// adds the blocks' partial pairs part[2k], part[2k + 1], k < nb, in a fixed
+// order into out[0], out[1] and re-arms the ticket, so the sum does not
+// depend on the order the blocks ran in. Every thread of the block calls it.
+__device__ __forceinline__ void ordered_finish(double sa, double sb, double* part, unsigned int* ticket, int k,
+                                               int nb, double* out) {
+    __shared__ int last;
+    sa = ::silt::block_sum(sa);
+    sb = ::silt::block_sum(sb);
+    if (threadIdx.x == 0) {
+        part[2 * k] = sa;
+        part[2 * k + 1] = sb;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned int)(nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double ta = 0.0, tb = 0.0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+        ta += ((volatile double*)part)[2 * q];
+        tb += ((volatile double*)part)[2 * q + 1];
+    }
+    ta = ::silt::block_sum(ta);
+    tb = ::silt::block_sum(tb);
+    if (threadIdx.x == 0) {
+        out[0] = ta;
+        out[1] = tb;
+        *ticket = 0u;
+    }
+}
+
+// k_sum2 with a fixed grid and an ordered finish: the same planes give the
+// same bits on every call.
+__global__ void k_sum2_ordered(const float* a, const float* b, size_t n, double* out, double* part,
+                               unsigned int* ticket) {
+    ::silt::dep_wait();
+    double sa = 0.0, sb = 0.0;
+    GRID_STRIDE(i, n) {
+        sa += (double)fmaxf(a[i], 0.0f);
+        sb += (double)fmaxf(b[i], 0.0f);
+    }
+    ordered_finish(sa, sb, part, ticket, blockIdx.x, gridDim.x, out);
+}
+
 __global__ void k_non_finite(const float* const* planes, int np, size_t n, unsigned int* out) {
     ::silt::dep_wait();
     unsigned int c = 0;
@@ -377,7 +422,14 @@ cudaError_t op_export(const float* bed, const float* water, const float* slurry,
     ::silt::count_launch();
     return cudaGetLastError();
 }
-cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st) {
+cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st, double* scratch) {
+    if (scratch) {
+        const int nb = std::min(blocks_for(n), SUM_BLOCKS);
+        unsigned int* ticket = reinterpret_cast<unsigned int*>(scratch + 2 * SUM_BLOCKS);
+        ::silt::launch_dep(k_sum2_ordered, dim3(nb), dim3(256), 0, st, a, b, n, out, scratch, ticket);
+        ::silt::count_launch();
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
     if (e != cudaSuccess) return e;
     ::silt::launch_dep(k_sum2, dim3(blocks_for(n)), dim3(256), 0, st, a, b, n, out);
@@ -400,8 +452,10 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
     for (int k = 0; k < 6; ++k) o[8 + k] = books[w][7 + k];  // the tracers' books
 }
 // Every window's suspended and silt column sums (FP64 of the clamped cells)
-// into out[16 w + 14], [16 w + 15], which start at zero.
-__global__ void k_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, double* out) {
+// into out[16 w + 14], [16 w + 15], in a fixed order (ordered_finish per
+// window; part holds gridDim.x pairs per window, then the windows' tickets).
+__global__ void k_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, double* out,
+                              double* part) {
     ::silt::dep_wait();
     const int w = blockIdx.y;
     const float* a = susp[w];
@@ -412,14 +466,19 @@ __global__ void k_sum_tracers(const float* const* susp, const float* const* turb
         sa += (double)fmaxf(a[i], 0.0f);
         sb += (double)fmaxf(b[i], 0.0f);
     }
-    ::silt::block_add(sa, out + 16 * (size_t)w + 14);
-    ::silt::block_add(sb, out + 16 * (size_t)w + 15);
+    unsigned int* tickets = reinterpret_cast<unsigned int*>(part + 2 * (size_t)gridDim.x * gridDim.y);
+    ordered_finish(sa, sb, part + 2 * (size_t)gridDim.x * w, tickets + w, blockIdx.x, gridDim.x,
+                   out + 16 * (size_t)w + 14);
+}
+size_t sum_tracers_scratch_bytes(int n) {
+    const int per = std::max(1, std::min(64, 2368 / std::max(n, 1)));
+    return (2 * (size_t)per * n) * sizeof(double) + (size_t)n * sizeof(unsigned int);
 }
 cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, int n, double* out,
-                           cudaStream_t st) {
+                           double* scratch, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int per = std::max(1, std::min(64, 2368 / n));
-    ::silt::launch_dep(k_sum_tracers, dim3(per, n), dim3(256), 0, st, susp, turbid, cells, out);
+    ::silt::launch_dep(k_sum_tracers, dim3(per, n), dim3(256), 0, st, susp, turbid, cells, out, scratch);
     ::silt::count_launch();
     return cudaGetLastError();
 }

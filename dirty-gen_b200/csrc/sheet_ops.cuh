@@ -28,10 +28,18 @@ cudaError_t op_publish(const float* water, const float* slurry, const float* uw,
 cudaError_t op_export(const float* bed, const float* water, const float* slurry, const float* uw, const float* vw,
                       const float* us, const float* vs, const float* moist, float* height, float* vel_u, float* vel_v,
                       float* moisture, size_t n, cudaStream_t st);
-cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st);
-// Every window's suspended and silt column sums into out[16 w + 14, 15] (zeroed first).
+// Blocks of an ordered plane sum; its scratch holds 2 * SUM_BLOCKS doubles and
+// a ticket (SUM_SCRATCH_BYTES, zeroed once).
+constexpr int SUM_BLOCKS = 1184;
+constexpr size_t SUM_SCRATCH_BYTES = (2 * SUM_BLOCKS + 2) * sizeof(double);
+// out[0..1] = FP64 sums of max(a, 0) and max(b, 0). With `scratch` the sum
+// is ordered (the same bits on every call); without it, blocks add atomically.
+cudaError_t op_sum2(const float* a, const float* b, size_t n, double* out, cudaStream_t st, double* scratch = nullptr);
+// Every window's suspended and silt column sums into out[16 w + 14, 15], in
+// a fixed order; `scratch` (sum_tracers_scratch_bytes(n), zeroed once).
+size_t sum_tracers_scratch_bytes(int n);
 cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid, const int* cells, int n, double* out,
-                           cudaStream_t st);
+                           double* scratch, cudaStream_t st);
 // out[16 w + 0..1] = acc[w][0..1] (depth sums), out[16 w + 2..6] = books[w][0..4],
 // out[16 w + 7] = books[w][6] (the transport rounding book), out[16 w + 8..13] = books[w][7..12] (tracers).
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,

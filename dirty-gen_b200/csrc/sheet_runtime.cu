@@ -90,6 +90,7 @@ struct silt_sheet {
     unsigned int* d_u32 = nullptr;   // [0..1] speed bits, [2] substep overflow, [3] non-finite count, [4..7] tile counters
     const float** d_planes = nullptr;
     double* h_acc = nullptr;      // pinned mirror of d_acc
+    double* d_sum_scratch = nullptr;  // the ordered plane sums' partials (SUM_SCRATCH_BYTES)
     // d_u32: [0, 2) speed bits, [2] substep overflow, [4, 8) tiles stepped
     // (two u64), [SWEEP_AT, SWEEP_AT + 9) the sweep launch state.
     static constexpr int SWEEP_AT = 8;
@@ -579,6 +580,8 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->staging2, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->staging_u8, s->n);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_acc, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_sum_scratch, silt::SUM_SCRATCH_BYTES);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_sum_scratch, 0, silt::SUM_SCRATCH_BYTES, s->st);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_u32, 24 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_planes, 8 * sizeof(float*));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_acc, 8 * sizeof(double));
@@ -692,6 +695,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->staging2);
     cudaFree(s->staging_u8);
     cudaFree(s->d_acc);
+    cudaFree(s->d_sum_scratch);
     cudaFreeHost(s->h_flags);
     cudaFree(s->d_u32);
     cudaFree(s->d_planes);
@@ -1594,11 +1598,10 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     if (s->ledger_fresh) {
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     } else {
-        CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st));
+        CK(silt::op_sum2(s->H(0), s->H(1), s->n, s->d_acc + 2, s->st, s->d_sum_scratch));
         CK(cudaMemcpyAsync(s->h_acc, s->d_acc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
-    CK(cudaMemsetAsync(s->d_acc + 4, 0, 2 * sizeof(double), s->st));
-    CK(silt::op_sum2(s->tr.susp[0], s->tr.turbid[0], s->n, s->d_acc + 4, s->st));
+    CK(silt::op_sum2(s->tr.susp[0], s->tr.turbid[0], s->n, s->d_acc + 4, s->st, s->d_sum_scratch));
     CK(cudaMemcpyAsync(s->h_acc + 4, s->d_acc + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0, rounding = 0.0;
     int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded, &rounding);
@@ -2002,6 +2005,7 @@ struct silt_batch {
     silt::tracers::Runner tr_run;           // the windows' tracer launches
     const float** d_tr_src = nullptr;       // [0, n) suspended planes, [n, 2n) silt planes
     int* d_tr_cells = nullptr;              // cells per window
+    double* d_tr_sum = nullptr;             // the ordered tracer sums' scratch
     double* h_ledgers = nullptr;            // pinned
 };
 
@@ -2024,6 +2028,7 @@ int batch_free(silt_batch* b) {
     cudaFree(b->d_ledgers);
     cudaFree(b->d_tr_src);
     cudaFree(b->d_tr_cells);
+    cudaFree(b->d_tr_sum);
     b->tr_run.release();
     if (b->h_ledgers) cudaFreeHost(b->h_ledgers);
     for (int k = 0; k < 2; ++k) {
@@ -2217,6 +2222,8 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 16 * (size_t)n * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_src, 2 * (size_t)n * sizeof(float*));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_cells, (size_t)n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_sum, silt::sum_tracers_scratch_bytes(n));
+    if (e == cudaSuccess) e = cudaMemset(b->d_tr_sum, 0, silt::sum_tracers_scratch_bytes(n));
     if (e == cudaSuccess) {
         std::vector<const float*> src(2 * (size_t)n);
         std::vector<int> cells(n);
@@ -2402,7 +2409,7 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
         return SILT_OK;
     }
     CK(cudaMemsetAsync(b->d_ledgers, 0, 16 * (size_t)n * sizeof(double), b->st));
-    CK(silt::op_sum_tracers(b->d_tr_src, b->d_tr_src + n, b->d_tr_cells, n, b->d_ledgers, b->st));
+    CK(silt::op_sum_tracers(b->d_tr_src, b->d_tr_src + n, b->d_tr_cells, n, b->d_ledgers, b->d_tr_sum, b->st));
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
     CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 16 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     for (silt_sheet* s : b->sheets)

@@ -84,16 +84,6 @@ __device__ __forceinline__ float sample_foam(const float* src, int res, float x,
     return finite_f(v) ? rclamp(v, 0.0f, 1.0f) : 0.0f;
 }
 
-__device__ __forceinline__ bool shore_wet_cell(const float* water, int res, int i, int j) {  // :9752-9764
-    if (i == 0 || j == 0 || i + 1 >= res || j + 1 >= res) return false;
-    const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
-    for (int k = 0; k < 4; ++k) {
-        const float nh = water[(size_t)(j + dj[k]) * res + (i + di[k])];
-        if (finite_f(nh) && nh < 0.004f) return true;
-    }
-    return false;
-}
-
 // shore_cell (:9826-9872): foam production and silt lift rate of a wet cell.
 __device__ __forceinline__ void shore_cell(const Sheet& S, int i, int j, float& foam, float& rate) {
     foam = 0.0f;
@@ -239,6 +229,17 @@ __device__ __forceinline__ void grown(const int* b, int res, int& i0, int& i1, i
         for (int once_ = 1, i = (i0) + (int)(q_ % w_), j = (j0) + (int)(q_ / w_); once_; once_ = 0)        \
             for (unsigned g = (unsigned)j * (unsigned)(res) + (unsigned)i; once_; once_ = 0)
 
+// Four cells per thread for the passes over whole windows: a warp takes 128
+// consecutive cells of a row of the box, lane l the cells ib, ib + 32,
+// ib + 64, ib + 96 with ib = start + l (each load coalesced; a thread's four
+// loads independent). Declares j and ib.
+#define QUAD_ROWS(res, i0, i1, j0, j1)                                                                          \
+    for (unsigned it_ = (blockIdx.x * blockDim.x + threadIdx.x) >> 5,                                           \
+                  nx_ = (unsigned)max((i1) - (i0) + 128, 0) / 128u, n_ = nx_ * (unsigned)max((j1) - (j0) + 1, 0); \
+         it_ < n_; it_ += (gridDim.x * blockDim.x) >> 5)                                                        \
+        for (int once_ = 1, j = (j0) + (int)(it_ / nx_), ib = (i0) + (int)(it_ % nx_) * 128 + (int)(threadIdx.x & 31); \
+             once_; once_ = 0)
+
 // The job is copied into registers: the planes' stores would otherwise make
 // the compiler reload its fields from memory after every write.
 #define JOB                              \
@@ -329,8 +330,9 @@ __global__ void k_entrain(const Job* jobs) {
 // the box of the cells it leaves above 1e-8, and a cell outside the region a
 // kernel touches keeps a value that was already at most 1e-8. A scan of the
 // whole window runs only after the planes were rewritten wholesale (attach,
-// window moves). Launches: [scan], begin, box, collect (with both advections
-// into scratch), go, commit, settle, spawn, sync begin, clear and sync.
+// window moves). Launches: [scan], begin, box, collect (with the foam
+// advection into scratch), the silt advection into scratch, go, commit,
+// settle, spawn, sync begin, clear and sync.
 
 // The start span of the jobs whose planes were rewritten (`rescan`); the
 // reset that rewrote them left the span empty.
@@ -482,12 +484,11 @@ __device__ __forceinline__ float turbid_after(const Sheet& S, const float* T, in
     return t;
 }
 
-// The wet set (marks) and, into scratch, both advections: advect_foam
-// (:6352-6397) of every wet or foam-live cell and advect_turbid of the grown
-// span. They read only fields no step kernel has changed yet; whether they
-// take effect is decided after the wet set is known (k_go, k_commit). The
-// grown span lies inside the collection box.
-__global__ void k_collect(const Job* jobs) {
+// The wet set (marks) and, into scratch, advect_foam (:6352-6397) of every
+// wet or foam-live cell; k_turbid_advect puts advect_turbid of the grown span
+// beside it. Both read only fields no step kernel has changed yet; whether
+// they take effect is decided once the wet set is known (k_go, k_commit).
+__global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
     ::silt::dep_wait();
     JOB;
     uint8_t* mark = T.mark;
@@ -498,44 +499,102 @@ __global__ void k_collect(const Job* jobs) {
     const float dt = J.dt, decay = J.foam_decay;
     const float* foam = T.foam[0];
     float* ftmp = T.foam[1];
-    const float* silt = T.turbid[0];
-    float* ttmp = T.turbid[1];
     const bool foam_on = c->live_foam_prev != 0;
-    const Box tb = box_empty(st->tspan) ? Box{0, -1, 0, -1} : grown_box(st->tspan, res);
     // Wet and shore marks are cleared where the last collection may have set
     // them and set inside this step's box; live marks stay.
     const Box b = box_of(c->cbox);
     const Box u = box_union(b, box_of(c->mbox));
     bool any = false;
-    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
-        uint8_t m = mark[g] & LIVE;
-        if (in_box(b, i, j)) {
-            const float h = S.water[g] + S.slurry[g];
-            if (finite_f(h) && !(h < 0.004f)) {
+    QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+        // The four cells' loads in two rounds: marks and depths, then, for the
+        // wet cells only, the four neighbours' water of the shore test
+        // (shore_wet_cell, :9752-9764: a cell on the window's border is never
+        // shore) and the velocity the foam advection reads.
+        uint8_t mk[4];
+        float hw[4], hs[4], nb[4][4], uw4[4], vw4[4];
+        bool here[4], wet[4], inner[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            here[k] = i <= u.i1;
+            wet[k] = false;
+            if (here[k]) mk[k] = mark[g];
+            if (here[k] && in_box(b, i, j)) {
+                hw[k] = S.water[g];
+                hs[k] = S.slurry[g];
+                wet[k] = true;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            if (wet[k]) {
+                const float h = hw[k] + hs[k];
+                wet[k] = finite_f(h) && !(h < 0.004f);
+            }
+            inner[k] = i > 0 && j > 0 && i + 1 < res && j + 1 < res;
+            if (!wet[k]) continue;
+            if (inner[k]) {
+                nb[k][0] = S.water[g - 1];
+                nb[k][1] = S.water[g + 1];
+                nb[k][2] = S.water[g - res];
+                nb[k][3] = S.water[g + res];
+            }
+            if (foam_on) {
+                uw4[k] = S.uw[g];
+                vw4[k] = S.vw[g];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!here[k]) continue;
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            uint8_t m = mk[k] & LIVE;
+            if (wet[k]) {
                 m |= WET;
                 any = true;
-                if (shore_wet_cell(S.water, res, i, j)) m |= SHORE;
+                bool shore = false;
+                if (inner[k])
+                    for (int q = 0; q < 4; ++q) shore = shore || (finite_f(nb[k][q]) && nb[k][q] < 0.004f);
+                if (shore) m |= SHORE;
             }
-        }
-        mark[g] = m;
-        if (foam_on) {
-            if (m & WET) {
-                const float uu = S.uw[g], vv = S.vw[g];  // wet cells are far above the dry cut
-                float sample = 0.0f;
-                if (finite_f(uu) && finite_f(vv)) {
-                    const float x = (float)i - uu * dt / S.cell;
-                    const float z = (float)j - vv * dt / S.cell;
-                    sample = sample_foam(foam, res, x, z);
+            mark[g] = m;
+            if (foam_on) {
+                if (m & WET) {
+                    const float uu = uw4[k], vv = vw4[k];  // wet cells are far above the dry cut
+                    float sample = 0.0f;
+                    if (finite_f(uu) && finite_f(vv)) {
+                        const float x = (float)i - uu * dt / S.cell;
+                        const float z = (float)j - vv * dt / S.cell;
+                        sample = sample_foam(foam, res, x, z);
+                    }
+                    const float fv = sample * decay;
+                    ftmp[g] = (fv > 1.0e-4f && finite_f(fv)) ? fminf(fv, FOAM_EQ) : 0.0f;
+                } else if (m & LIVE) {
+                    ftmp[g] = 0.0f;
                 }
-                const float fv = sample * decay;
-                ftmp[g] = (fv > 1.0e-4f && finite_f(fv)) ? fminf(fv, FOAM_EQ) : 0.0f;
-            } else if (m & LIVE) {
-                ftmp[g] = 0.0f;
             }
         }
-        if (in_box(tb, i, j)) ttmp[g] = turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, dt);
     }
     block_flag(any, &st->wet_any);
+}
+
+// advect_turbid of the grown span into scratch, spread over every block of
+// the launch (a cell's donor sequences are long; in the wet-set pass the
+// few warps holding the span's rows would carry all of them).
+__global__ void k_turbid_advect(const Job* jobs) {
+    ::silt::dep_wait();
+    JOB;
+    State* st = T.st;
+    if (!ctl_of(st)->active || box_empty(st->tspan)) return;
+    const int res = S.res;
+    const Box tb = grown_box(st->tspan, res);
+    const float* silt = T.turbid[0];
+    float* ttmp = T.turbid[1];
+    BOX_CELLS(res, tb.i0, tb.i1, tb.j0, tb.j1) ttmp[g] = turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, J.dt);
 }
 
 __global__ void k_go(const Job* jobs) {
@@ -571,12 +630,30 @@ __global__ void k_commit(const Job* jobs) {
     const float* ttmp = T.turbid[1];
     const uint8_t* mark = T.mark;
     LocalBox lb;
-    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
-        if (in_box(fb, i, j) && (mark[g] & (WET | LIVE))) foam[g] = ftmp[g];
-        if (in_box(tb, i, j)) {
-            const float t = ttmp[g];
-            silt[g] = t;
-            if (t > 1.0e-8f) lb.add(i, j);
+    QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+        bool fo[4];
+        float fv[4], tv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            fo[k] = i <= u.i1 && in_box(fb, i, j) && (mark[(unsigned)j * (unsigned)res + (unsigned)i] & (WET | LIVE));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            if (fo[k]) fv[k] = ftmp[g];
+            if (i <= u.i1 && in_box(tb, i, j)) tv[k] = ttmp[g];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            if (fo[k]) foam[g] = fv[k];
+            if (i <= u.i1 && in_box(tb, i, j)) {
+                silt[g] = tv[k];
+                if (tv[k] > 1.0e-8f) lb.add(i, j);
+            }
         }
     }
     lb.commit(c->tspan2);
@@ -621,12 +698,94 @@ __global__ void k_settle(const Job* jobs) {
     block_book(b, book);
 }
 
-// spawn_foam_and_silt (:6511-6520) on each wet cell: the tires in push order
-// (spawn_tire_tracers :6599-6665), then the shore (spawn_shore_tracers
-// :6667-6684) and Froude breaking (spawn_breaking_speed :6545-6558). Sources
-// only add silt, so a cell above 1e-8 after the settling stays above it; the
-// wet cells that end above it join the span after the sources.
-__global__ void k_spawn(const Job* jobs) {
+// A tire push's constants for spawn_tire_tracers (:6599-6665), computed once
+// per block; `live`: the tire moves or slips.
+struct PushK {
+    float x, z, speed, radius, fx, fz, rx, rz, reach2, slip_v, width;
+    int live;
+};
+
+__device__ __forceinline__ PushK push_k(const silt_tire_push& p, float cell) {
+    PushK q;
+    q.speed = finite_f(p.speed) ? fmaxf(p.speed, 0.0f) : 0.0f;
+    const float slip = finite_f(p.slip) ? fminf(fabsf(p.slip), 1.5f) : 0.0f;
+    q.live = !(q.speed < 0.25f && slip < 0.05f);
+    q.radius = fmaxf(p.radius, 0.05f);
+    const float len = fmaxf(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
+    q.fx = p.forward_x / len;
+    q.fz = p.forward_z / len;
+    q.rx = q.fz;
+    q.rz = -q.fx;
+    const float reach = q.radius * 1.15f + cell;
+    q.reach2 = reach * reach;
+    q.slip_v = q.speed * slip;
+    q.x = p.x;
+    q.z = p.z;
+    q.width = p.width;
+    return q;
+}
+
+constexpr int SPAWN_SHARED_PUSHES = 32;
+
+// spawn_foam_and_silt (:6511-6520) on one wet cell (water h, film velocity
+// u, v, slurry hs): the tires in push order (spawn_tire_tracers :6599-6665),
+// then the shore (spawn_shore_tracers :6667-6684) and Froude breaking
+// (spawn_breaking_speed :6545-6558). `table`: the pushes' constants, or null
+// to compute them from `push` here.
+__device__ __forceinline__ void spawn_cell(const Sheet& S, int i, int j, uint8_t m, float h, float hs, float u,
+                                           float v, const PushK* table, const silt_tire_push* push, int np, float dt,
+                                           float& f, float& t, double& b) {
+    const float cell = S.cell, area = cell * cell;
+    for (int k = 0; k < np; ++k) {
+        const PushK q = table ? table[k] : push_k(push[k], cell);
+        if (!q.live) continue;
+        if (!finite_f(h) || h < 0.004f) continue;
+        const float x = S.ox + ((float)i + 0.5f) * cell;
+        const float z = S.oz + ((float)j + 0.5f) * cell;
+        const float dx = x - q.x, dz = z - q.z;
+        if (dx * dx + dz * dz > q.reach2) continue;
+        const float along = dx * q.fx + dz * q.fz;
+        const float lat = dx * q.rx + dz * q.rz;
+        const float dist = hypot_rn(dx, dz);
+        float film = hypot_rn(u, v);
+        film = finite_f(film) ? film : 0.0f;
+        const float immerse = fminf(h, q.radius * 0.9f);
+        const float r_line = sqrtf(fmaxf(2.0f * q.radius * immerse - immerse * immerse, 0.0f));
+        const float band = 1.0f - rclamp(fabsf(dist - r_line) / (cell * 1.35f), 0.0f, 1.0f);
+        if (band > 0.0f) {
+            const float motion = fmaxf(fmaxf(q.slip_v, q.speed * 0.45f), film);
+            add_foam(f, breaking_foam(motion, h) * band, dt);
+        }
+        const bool on_patch = fabsf(lat) <= q.width * 0.55f + cell * 0.35f && along >= -q.radius * 0.55f &&
+                              along <= q.radius * 0.35f;
+        if (on_patch && h > 0.02f) {
+            // lift_silt (:6686-6697), rate cap 0.015, critical stress 6 Pa.
+            const float shear_v = fmaxf(q.slip_v, film * 0.35f);
+            if (finite_f(shear_v) && shear_v > 0.0f) {
+                const float tau = 1000.0f * 0.035f * shear_v * shear_v;
+                if (tau > 6.0f) {
+                    const float rate = fminf(0.008f * (tau / 6.0f - 1.0f), 0.015f);
+                    add_silt(t, fminf(rate * dt, 0.0025f), area, b);
+                }
+            }
+        }
+    }
+    if (m & SHORE) {
+        float prod, silt_add;
+        shore_cell(S, i, j, prod, silt_add);
+        add_foam(f, prod, dt);
+        if (silt_add > 0.0f) add_silt(t, fminf(silt_add * dt, 0.0012f), area, b);
+    }
+    const float hh = h + hs;
+    if (finite_f(hh) && !(hh < 0.004f)) {
+        if (finite_f(u) && finite_f(v) && !(hypot_rn(u, v) <= 0.05f)) add_foam(f, breaking_foam(hypot_rn(u, v), hh), dt);
+    }
+}
+
+// The sources on every wet cell. They only add silt, so a cell above 1e-8
+// after the settling stays above it; the wet cells that end above it join
+// the span after the sources.
+__global__ void __launch_bounds__(256, 3) k_spawn(const Job* jobs) {
     ::silt::dep_wait();
     const Job J = jobs[blockIdx.y];
     const Sheet& S = J.S;
@@ -637,75 +796,46 @@ __global__ void k_spawn(const Job* jobs) {
     double* book = J.T.books + 2;
     Ctl* c = ctl_of(J.T.st);
     if (!c->go) return;
+    __shared__ PushK table[SPAWN_SHARED_PUSHES];
+    const int np = J.npush;
+    const bool shared_table = np <= SPAWN_SHARED_PUSHES;
+    if (shared_table && (int)threadIdx.x < np) table[threadIdx.x] = push_k(J.push[threadIdx.x], S.cell);
+    __syncthreads();
     const int res = S.res;
-    const float cell = S.cell, area = cell * cell;
     double b = 0.0;
     LocalBox lb;
     const Box cb = box_of(c->cbox);  // the wet cells lie inside
-    BOX_CELLS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
-        const uint8_t m = mark[g];
-        if (!(m & WET)) continue;
-        float f = foam[g], t = T[g];
-        for (int k = 0; k < J.npush; ++k) {
-            const silt_tire_push& p = J.push[k];
-            const float speed = finite_f(p.speed) ? fmaxf(p.speed, 0.0f) : 0.0f;
-            const float slip = finite_f(p.slip) ? fminf(fabsf(p.slip), 1.5f) : 0.0f;
-            if (speed < 0.25f && slip < 0.05f) continue;
-            const float h = S.water[g];
-            if (!finite_f(h) || h < 0.004f) continue;
-            const float radius = fmaxf(p.radius, 0.05f);
-            const float len = fmaxf(sqrtf(p.forward_x * p.forward_x + p.forward_z * p.forward_z), 1.0e-4f);
-            const float fx = p.forward_x / len, fz = p.forward_z / len;
-            const float rx = fz, rz = -fx;
-            const float reach = radius * 1.15f + cell;
-            const float reach2 = reach * reach;
-            const float slip_v = speed * slip;
-            const float x = S.ox + ((float)i + 0.5f) * cell;
-            const float z = S.oz + ((float)j + 0.5f) * cell;
-            const float dx = x - p.x, dz = z - p.z;
-            if (dx * dx + dz * dz > reach2) continue;
-            const float along = dx * fx + dz * fz;
-            const float lat = dx * rx + dz * rz;
-            const float dist = hypot_rn(dx, dz);
-            float film = hypot_rn(S.uw[g], S.vw[g]);
-            film = finite_f(film) ? film : 0.0f;
-            const float immerse = fminf(h, radius * 0.9f);
-            const float r_line = sqrtf(fmaxf(2.0f * radius * immerse - immerse * immerse, 0.0f));
-            const float band = 1.0f - rclamp(fabsf(dist - r_line) / (cell * 1.35f), 0.0f, 1.0f);
-            if (band > 0.0f) {
-                const float motion = fmaxf(fmaxf(slip_v, speed * 0.45f), film);
-                add_foam(f, breaking_foam(motion, h) * band, dt);
-            }
-            const bool on_patch = fabsf(lat) <= p.width * 0.55f + cell * 0.35f && along >= -radius * 0.55f &&
-                                  along <= radius * 0.35f;
-            if (on_patch && h > 0.02f) {
-                // lift_silt (:6686-6697), rate cap 0.015, critical stress 6 Pa.
-                const float shear_v = fmaxf(slip_v, film * 0.35f);
-                if (finite_f(shear_v) && shear_v > 0.0f) {
-                    const float tau = 1000.0f * 0.035f * shear_v * shear_v;
-                    if (tau > 6.0f) {
-                        const float rate = fminf(0.008f * (tau / 6.0f - 1.0f), 0.015f);
-                        add_silt(t, fminf(rate * dt, 0.0025f), area, b);
-                    }
-                }
-            }
+    QUAD_ROWS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
+        uint8_t mk[4];
+        float hw[4], hs[4], u4[4], v4[4], f4[4], t4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            mk[k] = i <= cb.i1 ? mark[(unsigned)j * (unsigned)res + (unsigned)i] : (uint8_t)0;
         }
-        {
-            if (m & SHORE) {
-                float prod, silt_add;
-                shore_cell(S, i, j, prod, silt_add);
-                add_foam(f, prod, dt);
-                if (silt_add > 0.0f) add_silt(t, fminf(silt_add * dt, 0.0012f), area, b);
-            }
-            const float h = S.water[g] + S.slurry[g];
-            if (finite_f(h) && !(h < 0.004f)) {
-                const float u = S.uw[g], v = S.vw[g];
-                if (finite_f(u) && finite_f(v) && !(hypot_rn(u, v) <= 0.05f)) add_foam(f, breaking_foam(hypot_rn(u, v), h), dt);
-            }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!(mk[k] & WET)) continue;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)(ib + 32 * k);
+            hw[k] = S.water[g];
+            hs[k] = S.slurry[g];
+            u4[k] = S.uw[g];
+            v4[k] = S.vw[g];
+            f4[k] = foam[g];
+            t4[k] = T[g];
         }
-        foam[g] = f;
-        T[g] = t;
-        if (t > 1.0e-8f) lb.add(i, j);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!(mk[k] & WET)) continue;
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            float f = f4[k], t = t4[k];
+            spawn_cell(S, i, j, mk[k], hw[k], hs[k], u4[k], v4[k], shared_table ? table : nullptr, J.push, np, dt, f,
+                       t, b);
+            foam[g] = f;
+            T[g] = t;
+            if (t > 1.0e-8f) lb.add(i, j);
+        }
     }
     lb.commit(c->tspan3);  // with the settled cells': the silt span after the sources
     block_book(b, book);
@@ -728,7 +858,7 @@ __global__ void k_sync_begin(const Job* jobs) {
 // cell above 1e-8 after it: those cells are the next step's start span.
 // Outside the collection box no cell is wet, and the live cells of the last
 // sync lie inside it (it covers their box), so every mark there is 0.
-__global__ void k_clear_sync(const Job* jobs) {
+__global__ void __launch_bounds__(256, 4) k_clear_sync(const Job* jobs) {
     ::silt::dep_wait();
     JOB;
     float* foam = T.foam[0];
@@ -746,38 +876,70 @@ __global__ void k_clear_sync(const Job* jobs) {
     double b = 0.0;
     unsigned int cnt = 0;
     LocalBox live, span;
-    BOX_CELLS(res, u.i0, u.i1, u.j0, u.j1) {
-        const float h = S.water[g] + S.slurry[g];
-        const uint8_t m = mark[g];
-        float f = foam[g];
-        if (m & WET) {
-            if (!finite_f(h) || h < 0.004f || !finite_f(f)) {
-                f = 0.0f;
-                foam[g] = 0.0f;
-            }
+    QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+        // Loads in two rounds: the marks, then what the wet cells and the
+        // span's cells read.
+        float hw[4], hs[4], f4[4], t4[4];
+        uint8_t mk[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            mk[k] = i <= u.i1 ? mark[(unsigned)j * (unsigned)res + (unsigned)i] : (uint8_t)0;
         }
-        if (in_box(sb, i, j)) {
-            float t = silt[g];
-            if (!finite_f(h) || h < 1.0e-5f) {
-                if (t > 0.0f) {
-                    b += (double)(t * area);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            if (i > u.i1) continue;
+            const bool in_span = in_box(sb, i, j);
+            if (!(mk[k] & WET) && !in_span) continue;
+            hw[k] = S.water[g];
+            hs[k] = S.slurry[g];
+            if (mk[k] & WET) f4[k] = foam[g];
+            if (in_span) t4[k] = silt[g];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = ib + 32 * k;
+            const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
+            if (i > u.i1) continue;
+            const uint8_t m = mk[k];
+            const bool in_span = in_box(sb, i, j);
+            if (!(m & WET) && !in_span) {
+                if (m != 0 && in_box(cb, i, j)) mark[g] = 0;  // a dry cell's marks (sync below)
+                continue;
+            }
+            const float h = hw[k] + hs[k];
+            float f = (m & WET) ? f4[k] : 0.0f;
+            if (m & WET) {
+                if (!finite_f(h) || h < 0.004f || !finite_f(f)) {
+                    f = 0.0f;
+                    foam[g] = 0.0f;
+                }
+            }
+            if (in_span) {
+                float t = t4[k];
+                if (!finite_f(h) || h < 1.0e-5f) {
+                    if (t > 0.0f) {
+                        b += (double)(t * area);
+                        t = 0.0f;
+                        silt[g] = 0.0f;
+                    }
+                } else if (!finite_f(t)) {
                     t = 0.0f;
                     silt[g] = 0.0f;
                 }
-            } else if (!finite_f(t)) {
-                t = 0.0f;
-                silt[g] = 0.0f;
+                if (t > 1.0e-8f) span.add(i, j);
             }
-            if (t > 1.0e-8f) span.add(i, j);
-        }
-        if (in_box(cb, i, j)) {
-            uint8_t mm = m & (WET | SHORE);
-            if ((mm & WET) && finite_f(f) && f > 1.0e-4f) {
-                mm |= LIVE;
-                ++cnt;
-                live.add(i, j);
+            if (in_box(cb, i, j)) {
+                uint8_t mm = m & (WET | SHORE);
+                if ((mm & WET) && finite_f(f) && f > 1.0e-4f) {
+                    mm |= LIVE;
+                    ++cnt;
+                    live.add(i, j);
+                }
+                mark[g] = mm;
             }
-            mark[g] = mm;
         }
     }
     live.commit(st->live_box);
@@ -1251,6 +1413,7 @@ cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream
     LAUNCH(k_begin, 1, jobs);
     LAUNCH(k_collect_box, 1, jobs);
     LAUNCH(k_collect, bx, jobs);
+    LAUNCH(k_turbid_advect, bx, jobs);
     LAUNCH(k_go, 1, jobs);
     LAUNCH(k_commit, bx, jobs);
     LAUNCH(k_settle, bx, jobs);
