@@ -307,7 +307,8 @@ def run_b200(args):
     th.join(timeout=5)
     p1 = sheet.step_parts()
     parts = {k: p1[k] - p0[k] for k in ("launches", "force_launches", "force_cells", "force_cells_water",
-                                        "device_counts", "steps")}
+                                        "device_counts", "steps", "sweep_launches", "sweep_solves",
+                                        "sweep_local_passes")}
     parts["sweep_passes_max"] = p1["sweep_passes_max"]
     parts["sweep_fallbacks"] = p1["sweep_fallbacks"]
     if dist:
@@ -385,7 +386,9 @@ def run_b200(args):
                 "device_counted_steps": int(parts["device_counts"]),
                 "confinement": {"form": "gauss-seidel sweep (step_pair)",
                                 "most_fixed_point_passes": int(parts["sweep_passes_max"]),
-                                "sequential_fallbacks": int(parts["sweep_fallbacks"])},
+                                "sequential_fallbacks": int(parts["sweep_fallbacks"]),
+                                "tile_solves_per_launch": int(parts["sweep_solves"]) / max(int(parts["sweep_launches"]), 1),
+                                "local_passes_per_solve": int(parts["sweep_local_passes"]) / max(int(parts["sweep_solves"]), 1)},
                 "window_steps_per_s": world * args.steps / (ms / 1000.0),
                 "ledger": {"water_m3": led["water_m3"], "slurry_m3": led["slurry_m3"], "opened_m3": led["opened_m3"],
                            "spray_m3": led["spray_m3"], "cut_m3": led["cut_m3"],

@@ -359,7 +359,10 @@ __device__ __forceinline__ void pre_tile(const LayerParams& P, float* sm, int tx
 
 // Local passes of the sweep's fixed point on one tile before its values go
 // back to global memory.
-constexpr int SWEEP_LOCAL_PASSES = 16;
+#ifndef SILT_SWEEP_LOCAL_PASSES
+#define SILT_SWEEP_LOCAL_PASSES 16
+#endif
+constexpr int SWEEP_LOCAL_PASSES = SILT_SWEEP_LOCAL_PASSES;
 
 // Sweep form, part 2: one pass of the raster-order Gauss-Seidel confinement
 // (force_gravity_open, src/fluid_core.rs:2234-2260) solved as a fixed point.
@@ -373,8 +376,12 @@ constexpr int SWEEP_LOCAL_PASSES = 16;
 // When a whole pass over every tile changes nothing, every cell satisfies its
 // equation with the values it read, and since each cell depends only on
 // earlier cells that solution is the sequential sweep's, bit for bit.
+// `reuse`: this CTA's shared memory still holds this tile from an earlier
+// pass of the launch (the CTA solves no other tile), so only the ring of
+// other tiles' wet cells around it is read again; the starting and
+// post-gravity velocities and the tile's own iterate are current.
 template <bool EDGE>
-__device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
+__device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0, bool reuse, int& passes) {
     const int res = P.res;
     float* PU = sm;              // starting velocity (the values of cells after a cell)
     float* PV = sm + FPLANE;
@@ -385,7 +392,15 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
     float* WT = sm + 6 * FPLANE;  // 1: wet
     const int ox = tx0 - FH, oy = ty0 - FH;
     const float eps = P.eps;
-    region<EDGE, 2, 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+    if (reuse) {
+        region<EDGE, 2, 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
+            if (gx >= tx0 && gx < tx0 + FT && gy >= ty0 && gy < ty0 + FT) return;
+            if (WT[s] != 0.0f) {
+                FU[s] = P.fu[g];
+                FV[s] = P.fv[g];
+            }
+        });
+    } else region<EDGE, 2, 2>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
         const float hv = P.h[g];
         float uu, vv;
         start_velocity(P, gx, gy, g, hv, uu, vv);
@@ -404,7 +419,9 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
     });
     __syncthreads();
     bool tile_changed = false;
+    passes = 0;
     for (int it = 0; it < SWEEP_LOCAL_PASSES; ++it) {
+        ++passes;
         int changed = 0;
         region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             if (WT[s] == 0.0f) return;
@@ -440,7 +457,7 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0) {
             }
         });
     }
-    __syncthreads();  // shared memory is reused by the next tile
+    __syncthreads();  // shared memory is read again by the next tile or pass
     return tile_changed;
 }
 
@@ -545,40 +562,40 @@ __device__ __forceinline__ bool entry_steps(int e) { return (e & (ENTRY_ZERO | E
 // neighbourhood (itself included) changed since the previous pass began: it
 // is otherwise still at the fixed point of the values around it. Returns
 // whether the tile changed (block-uniform) and stamps it when it did.
+// `reuse`: the CTA solves only this entry in the launch, so its shared
+// memory keeps the tile between passes.
 __device__ __forceinline__ bool sweep_entry(const LayerParams& P, const TileFlags& tf, int e, float* sm, int pass,
-                                            unsigned int epoch) {
+                                            unsigned int epoch, bool reuse) {
     if (!entry_steps(e) || !P.sweep || !(P.vort > 0.0f)) return false;
     const int l = e >> 30, t = e & ENTRY_TILE;
     const int nt = tf.tiles_x * tf.tiles_x;
     const int ti = t % tf.tiles_x, tj = t / tf.tiles_x;
     unsigned int* stamp = tf.stamp ? tf.stamp + (size_t)l * nt : nullptr;
     if (pass > 0 && stamp) {
-        __shared__ int again;
-        if (threadIdx.x == 0) {
+        // Nine threads read the nine stamps at once.
+        bool hit = false;
+        if (threadIdx.x < 9) {
+            const int x = ti + (int)(threadIdx.x % 3) - 1, y = tj + (int)(threadIdx.x / 3) - 1;
             const unsigned int since = epoch * 256u + (unsigned int)pass;
-            int a = 0;
-            for (int dj = -1; dj <= 1 && !a; ++dj)
-                for (int di = -1; di <= 1; ++di) {
-                    const int x = ti + di, y = tj + dj;
-                    if (x < 0 || y < 0 || x >= tf.tiles_x || y >= tf.tiles_x) continue;
-                    if (*(volatile unsigned int*)&stamp[y * tf.tiles_x + x] >= since) {
-                        a = 1;
-                        break;
-                    }
-                }
-            again = a;
+            hit = x >= 0 && y >= 0 && x < tf.tiles_x && y < tf.tiles_x &&
+                  *(volatile unsigned int*)&stamp[y * tf.tiles_x + x] >= since;
         }
-        __syncthreads();
-        const int go = again;
-        __syncthreads();
-        if (!go) return false;
+        if (!__syncthreads_or(hit)) return false;
     }
     const int tx0 = ti * FT, ty0 = tj * FT;
-    const bool changed =
-        tile_interior(P.res, tx0, ty0) ? sweep_tile<false>(P, sm, tx0, ty0) : sweep_tile<true>(P, sm, tx0, ty0);
-    if (changed && stamp && threadIdx.x == 0) {
-        __threadfence();
-        stamp[t] = epoch * 256u + (unsigned int)pass + 1u;
+    int passes = 0;
+    const bool keep = reuse && pass > 0;
+    const bool changed = tile_interior(P.res, tx0, ty0) ? sweep_tile<false>(P, sm, tx0, ty0, keep, passes)
+                                                        : sweep_tile<true>(P, sm, tx0, ty0, keep, passes);
+    if (threadIdx.x == 0) {
+        if (changed && stamp) {
+            __threadfence();
+            stamp[t] = epoch * 256u + (unsigned int)pass + 1u;
+        }
+        if (tf.sweep) {
+            atomicAdd(&tf.sweep->solves, 1u);
+            atomicAdd(&tf.sweep->local_passes, (unsigned int)passes);
+        }
     }
     return changed;
 }
@@ -629,7 +646,7 @@ __device__ bool grid_barrier(SweepState* S, unsigned int& target) {
                 good = 0;
                 break;
             }
-            __nanosleep(100);
+            if (spins > 256) __nanosleep(64);  // short waits poll without sleeping
         }
         __threadfence();
         ok = good;
@@ -722,9 +739,10 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force_sweep(ForceLaunch L) {
     }
     unsigned int target = 0;
     if (!grid_barrier(S, target)) return;
+    const bool reuse = n <= (int)gridDim.x;  // one entry per CTA: its tile stays in shared memory
     const int passes = sweep_fixed_point(S, target, n, [&](int k, int pass) {
         const int e = L.tf.list[k];
-        return sweep_entry(Ps[e >> 30], L.tf, e, sm, pass, epoch);
+        return sweep_entry(Ps[e >> 30], L.tf, e, sm, pass, epoch, reuse);
     });
     if (passes < 0) return;
     if (passes == 0) {
@@ -1257,9 +1275,10 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_batch_force_sweep(const Windo
     unsigned int target = 0;
     const unsigned int epoch = ld_acquire_u32(&S->epoch);
     if (!grid_barrier(S, target)) return;
+    const bool reuse = n <= (int)gridDim.x;  // one entry per CTA: its tile stays in shared memory
     const int passes = sweep_fixed_point(S, target, n, [&](int k, int pass) {
         const int e = fetch(k, false);
-        const bool r = sweep_entry(Ps, Tf, e, sm, pass, epoch);
+        const bool r = sweep_entry(Ps, Tf, e, sm, pass, epoch, reuse);
         __syncthreads();
         return r;
     });

@@ -92,8 +92,11 @@ struct silt_sheet {
     double* h_acc = nullptr;      // pinned mirror of d_acc
     double* d_sum_scratch = nullptr;  // the ordered plane sums' partials (SUM_SCRATCH_BYTES)
     // d_u32: [0, 2) speed bits, [2] substep overflow, [4, 8) tiles stepped
-    // (two u64), [SWEEP_AT, SWEEP_AT + 9) the sweep launch state.
+    // (two u64), [SWEEP_AT, SWEEP_AT + 11) the sweep launch state, [COUNT_AT]
+    // a seeding call's cell count.
     static constexpr int SWEEP_AT = 8;
+    static constexpr int COUNT_AT = 20;
+    static_assert(SWEEP_AT + sizeof(silt::SweepState) / sizeof(unsigned int) <= COUNT_AT, "d_u32 slots");
     unsigned int* h_flags = nullptr;  // pinned: d_u32[2, 16) as last read (FLAG_* below)
     bool cut_pending = false;
     bool ledger_fresh = false;    // h_acc[0..1] hold the current depth sums
@@ -859,9 +862,9 @@ int silt_lay_slurry_on_water(silt_sheet* s, float depth, int32_t grain, float* v
     int rc = silt::fine::restrict_all(s->fine, s);
     if (rc) return rc;
     if ((rc = flush_cut(s))) return rc;
-    CK(silt::op_lay_on_water(s->H(0), s->H(1), s->moisture, s->grain, s->n, depth, grain, s->d_u32 + 8, s->st));
+    CK(silt::op_lay_on_water(s->H(0), s->H(1), s->moisture, s->grain, s->n, depth, grain, s->d_u32 + silt_sheet::COUNT_AT, s->st));
     unsigned int cells = 0;
-    CK(cudaMemcpyAsync(&cells, s->d_u32 + 8, sizeof cells, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&cells, s->d_u32 + silt_sheet::COUNT_AT, sizeof cells, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if (vol_out) {
         // The reference's f32 running sum of depth * area over those cells.
@@ -1883,6 +1886,8 @@ int silt_get_step_parts(silt_sheet* s, silt_step_parts* out) {
         s->parts.sweep_launches = st.launches;
         s->parts.sweep_passes_max = st.passes_max;
         s->parts.sweep_fallbacks = st.fallbacks;
+        s->parts.sweep_solves = st.solves;
+        s->parts.sweep_local_passes = st.local_passes;
     }
     *out = s->parts;
     return SILT_OK;
@@ -2493,6 +2498,8 @@ int silt_batch_get_parts(silt_batch* b, silt_step_parts* out) {
             b->parts.sweep_launches = st.launches;
             b->parts.sweep_passes_max = st.passes_max;
             b->parts.sweep_fallbacks = st.fallbacks;
+            b->parts.sweep_solves = st.solves;
+            b->parts.sweep_local_passes = st.local_passes;
         }
     }
     *out = b->parts;

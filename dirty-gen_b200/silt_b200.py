@@ -83,7 +83,8 @@ class StepParts(ctypes.Structure):
                 ("force_cells", ctypes.c_int64), ("force_cells_water", ctypes.c_int64),
                 ("device_counts", ctypes.c_int64), ("host_step_ms", ctypes.c_double),
                 ("host_fine_ms", ctypes.c_double), ("sweep_launches", ctypes.c_int64),
-                ("sweep_passes_max", ctypes.c_int64), ("sweep_fallbacks", ctypes.c_int64)]
+                ("sweep_passes_max", ctypes.c_int64), ("sweep_fallbacks", ctypes.c_int64),
+                ("sweep_solves", ctypes.c_int64), ("sweep_local_passes", ctypes.c_int64)]
 
 
 class KernelTime(ctypes.Structure):

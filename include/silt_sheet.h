@@ -297,8 +297,9 @@ typedef struct {
     double host_step_ms, host_fine_ms;  /* host time inside silt_step, and its nested-patch share */
     /* Grid engine, Gauss-Seidel sweep: launches, the most fixed-point passes
      * one launch needed, launches that reached the pass limit and ran the
-     * sequential sweep. */
-    int64_t sweep_launches, sweep_passes_max, sweep_fallbacks;
+     * sequential sweep, tile solves (a tile in one pass) and their local
+     * passes in shared memory. */
+    int64_t sweep_launches, sweep_passes_max, sweep_fallbacks, sweep_solves, sweep_local_passes;
 } silt_step_parts;
 int silt_set_step_timing(silt_sheet* s, int32_t on);
 int silt_get_step_parts(silt_sheet* s, silt_step_parts* out);
