@@ -1339,19 +1339,27 @@ __global__ void __launch_bounds__(NT, 1) k_window_step_list(Job* const* jobs) {
     window_job(jobs[blockIdx.x / (unsigned)crew_size()]);
 }
 
+// Largest crew: 16 CTAs, the non-portable cluster size B200 allows.
+constexpr int MAX_CREW = 16;
+
 // CTAs per job: enough warps for one (row, 32-cell chunk) item each on a
-// 64-cell patch, up to the portable cluster size.
+// 64-cell patch, up to the largest crew.
 static int crew_for(int max_res) {
     const int items = max_res * ((max_res + 31) / 32);
     int c = items / (NT / 32);
     if (c < 1) c = 1;
-    if (c > 8) c = 8;
+    if (c > MAX_CREW) c = MAX_CREW;
     return c;
 }
 
 // The largest crew the device can hold at once (a cluster of full-SM CTAs).
 static int crew_limit_query(cudaStream_t st) {
-    for (int c = 8; c >= 1; --c) {
+    if (cudaFuncSetAttribute(k_window_step, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+        cudaFuncSetAttribute(k_window_step_list, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 8;  // the portable size
+    }
+    for (int c = MAX_CREW; c >= 1; --c) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)c, 1, 1);
         cfg.blockDim = dim3(NT, 1, 1);
