@@ -43,7 +43,6 @@ enum : uint8_t { WET = 1, SHORE = 2, LIVE = 4 };
 // Per-step control, in State plus these words (kept after State in memory).
 struct Ctl {
     int active;     // the tracer step runs at all (wake, live silt or live foam)
-    int go;         // ... and has wet cells or live silt
     int cbox[4];    // the step's collection box
     int tspan2[4];  // silt span after the transport
     int tspan3[4];  // silt span after the sources
@@ -54,6 +53,13 @@ struct Ctl {
 };
 
 __device__ __forceinline__ Ctl* ctl_of(State* s) { return reinterpret_cast<Ctl*>(s + 1); }
+
+// The tracer step goes on past the wet set (:6226-6229): it runs at all and
+// has wet cells or live silt. Final once the wet-set pass has ended.
+__device__ __forceinline__ bool step_goes(const State* st) {
+    const Ctl* c = reinterpret_cast<const Ctl*>(st + 1);
+    return c->active && (st->wet_any || st->live_silt);
+}
 
 __device__ __forceinline__ float vel(const float* u, const Sheet& S, size_t g) {
     // The grid engine's pending dry cut: a cell under eps carries no velocity.
@@ -330,9 +336,9 @@ __global__ void k_entrain(const Job* jobs) {
 // the box of the cells it leaves above 1e-8, and a cell outside the region a
 // kernel touches keeps a value that was already at most 1e-8. A scan of the
 // whole window runs only after the planes were rewritten wholesale (attach,
-// window moves). Launches: [scan], begin, box, collect (with the foam
-// advection into scratch), the silt advection into scratch, go, commit,
-// settle, spawn, sync begin, clear and sync.
+// window moves). Launches: [scan], begin (control words and the collection
+// box), collect (with the foam advection into scratch), the silt advection
+// into scratch, commit, settle (with the sync's start), spawn, clear and sync.
 
 // The start span of the jobs whose planes were rewritten (`rescan`); the
 // reset that rewrote them left the span empty.
@@ -349,33 +355,23 @@ __global__ void k_scan(const Job* jobs) {
     lb.commit(T.st->tspan);
 }
 
+// The step's control words, then collect_tracer_wet's box (:6248-6293) and
+// tracer_visit_box (:6296-6337). `wake`: a tire with speed or slip, or a
+// surface drive (host-known); `pbox`: the tires' reach boxes (host-computed;
+// empty when none).
 __global__ void k_begin(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    State* st = T.st;
-    const int res = S.res;
-    Ctl* c = ctl_of(st);
-    box_clear(c->tspan2, res);
-    box_clear(c->tspan3, res);
-    box_clear(c->cbox, res);
-    st->live_silt = box_empty(st->tspan) ? 0u : 1u;
-    st->wet_any = 0;
-    c->active = 0;
-    c->go = 0;
-    c->live_foam_prev = st->live_foam;
-}
-
-// collect_tracer_wet (:6248-6293) and tracer_visit_box (:6296-6337).
-// `wake`: a tire with speed or slip, or a surface drive (host-known);
-// `pbox`: the tires' reach boxes (host-computed; empty when none).
-__global__ void k_collect_box(const Job* jobs) {
     ::silt::dep_wait();
     JOB;
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     State* st = T.st;
     const int res = S.res, wake = J.wake;
     Ctl* c = ctl_of(st);
+    box_clear(c->tspan2, res);
+    box_clear(c->tspan3, res);
+    box_clear(c->cbox, res);
+    st->live_silt = box_empty(st->tspan) ? 0u : 1u;
+    st->wet_any = 0;
+    c->live_foam_prev = st->live_foam;
     c->active = (wake || st->live_silt || c->live_foam_prev) ? 1 : 0;
     if (!c->active) return;
     if (wake) {
@@ -407,6 +403,7 @@ __global__ void k_collect_box(const Job* jobs) {
     c->cbox[2] = max(b[2] - 2, 0);
     c->cbox[3] = min(b[3] + 2, res - 1);
 }
+
 
 // The silt a donor cell gives across its four edges in flux_thickness's
 // order (x edges before z edges, each axis in index order): to the left,
@@ -597,18 +594,6 @@ __global__ void k_turbid_advect(const Job* jobs) {
     BOX_CELLS(res, tb.i0, tb.i1, tb.j0, tb.j1) ttmp[g] = turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, J.dt);
 }
 
-__global__ void k_go(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    State* st = T.st;
-    Ctl* c = ctl_of(st);
-    c->go = (c->active && (st->wet_any || st->live_silt)) ? 1 : 0;
-    if (c->active) {
-        for (int k = 0; k < 4; ++k) c->mbox[k] = c->cbox[k];
-    }
-}
-
 // The advections take effect: foam on every wet or foam-live cell, silt on
 // the grown span, whose cells above 1e-8 are the span after the transport
 // (outside it no cell holds more than 1e-8).
@@ -617,7 +602,7 @@ __global__ void k_commit(const Job* jobs) {
     JOB;
     State* st = T.st;
     Ctl* c = ctl_of(st);
-    if (!c->go) return;
+    if (!step_goes(st)) return;
     const int res = S.res;
     const bool foam_on = c->live_foam_prev != 0, silt_on = !box_empty(st->tspan);
     if (!foam_on && !silt_on) return;
@@ -670,7 +655,17 @@ __global__ void k_settle(const Job* jobs) {
     const float keep = J.silt_keep;
     double* book = J.T.books + 3;
     Ctl* c = ctl_of(st);
-    if (!c->go || box_empty(c->tspan2)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c->active) {
+        // The sync's start (:6339): the marks' box for the next step's wet
+        // set, and the live set and start span, rebuilt by k_clear_sync.
+        for (int k = 0; k < 4; ++k) c->mbox[k] = c->cbox[k];
+        if (step_goes(st)) {
+            st->live_foam = 0;
+            box_clear(st->live_box, S.res);
+            box_clear(st->tspan, S.res);
+        }
+    }
+    if (!step_goes(st) || box_empty(c->tspan2)) return;
     const int res = S.res;
     const float area = S.cell * S.cell;
     int bi0, bi1, bj0, bj1;
@@ -795,7 +790,7 @@ __global__ void __launch_bounds__(256, 3) k_spawn(const Job* jobs) {
     const float dt = J.dt;
     double* book = J.T.books + 2;
     Ctl* c = ctl_of(J.T.st);
-    if (!c->go) return;
+    if (!step_goes(J.T.st)) return;
     __shared__ PushK table[SPAWN_SHARED_PUSHES];
     const int np = J.npush;
     const bool shared_table = np <= SPAWN_SHARED_PUSHES;
@@ -841,18 +836,6 @@ __global__ void __launch_bounds__(256, 3) k_spawn(const Job* jobs) {
     block_book(b, book);
 }
 
-__global__ void k_sync_begin(const Job* jobs) {
-    ::silt::dep_wait();
-    JOB;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    State* st = T.st;
-    const int res = S.res;
-    if (!ctl_of(st)->go) return;
-    st->live_foam = 0;
-    box_clear(st->live_box, res);
-    box_clear(st->tspan, res);  // rebuilt by the clear: the next step's start span
-}
-
 // clear_dry_tracers (:6712-6739) then sync_foam_live (:6339-6349), per cell.
 // The clear only lowers silt, so the grown span after the sources holds every
 // cell above 1e-8 after it: those cells are the next step's start span.
@@ -867,7 +850,7 @@ __global__ void __launch_bounds__(256, 4) k_clear_sync(const Job* jobs) {
     State* st = T.st;
     Ctl* c = ctl_of(st);
     double* book = T.books + 3;
-    if (!c->go) return;
+    if (!step_goes(st)) return;
     const int res = S.res;
     const float area = S.cell * S.cell;
     const Box cb = box_of(c->cbox);
@@ -1270,11 +1253,11 @@ int blocks_x(const Window* w, int n) {
 // device array.
 cudaError_t upload(Runner& R, const Window* w, int n, float dt, float foam_decay, float silt_keep, cudaStream_t st,
                    const Job** out) {
-    const int slot = R.flip;
-    R.flip ^= 1;
+    const int slot = R.next;
+    R.next = (R.next + 1) % Runner::SLOTS;
     cudaError_t e;
     if (R.ev[slot]) {
-        if ((e = cudaEventSynchronize(R.ev[slot])) != cudaSuccess) return e;  // the copy two sequences back is done
+        if ((e = cudaEventSynchronize(R.ev[slot])) != cudaSuccess) return e;  // this slot's last copy is done
     } else if ((e = cudaEventCreateWithFlags(&R.ev[slot], cudaEventDisableTiming)) != cudaSuccess) {
         return e;
     }
@@ -1376,7 +1359,7 @@ cudaError_t attach(Planes& T, void* mem, int res, double* books, cudaStream_t st
 }
 
 void Runner::release() {
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < SLOTS; ++k) {
         cudaFree(d_jobs[k]);
         cudaFree(d_push[k]);
         if (h_jobs[k]) cudaFreeHost(h_jobs[k]);
@@ -1411,14 +1394,11 @@ cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream
     for (int k = 0; k < n; ++k) rescan = rescan || w[k].rescan;
     if (rescan) LAUNCH(k_scan, bx, jobs);
     LAUNCH(k_begin, 1, jobs);
-    LAUNCH(k_collect_box, 1, jobs);
     LAUNCH(k_collect, bx, jobs);
     LAUNCH(k_turbid_advect, bx, jobs);
-    LAUNCH(k_go, 1, jobs);
     LAUNCH(k_commit, bx, jobs);
     LAUNCH(k_settle, bx, jobs);
     LAUNCH(k_spawn, bx, jobs);
-    LAUNCH(k_sync_begin, 1, jobs);
     LAUNCH(k_clear_sync, bx, jobs);
     return cudaSuccess;
 }

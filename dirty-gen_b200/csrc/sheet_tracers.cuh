@@ -65,15 +65,18 @@ struct Job {
 };
 
 // Host staging of the jobs of a launch sequence: windows and their pushes,
-// uploaded once per sequence (two slots, alternating).
+// uploaded once per sequence into a ring of slots. A step uploads up to three
+// sequences, so a slot is reused about three steps later and its wait for
+// the earlier copy finds it long done: the host runs ahead of the device.
 struct Runner {
-    Job* d_jobs[2] = {nullptr, nullptr};
-    Job* h_jobs[2] = {nullptr, nullptr};
-    silt_tire_push* d_push[2] = {nullptr, nullptr};
-    silt_tire_push* h_push[2] = {nullptr, nullptr};
-    size_t cap_jobs[2] = {0, 0}, cap_push[2] = {0, 0};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    int flip = 0;
+    static constexpr int SLOTS = 10;
+    Job* d_jobs[SLOTS] = {};
+    Job* h_jobs[SLOTS] = {};
+    silt_tire_push* d_push[SLOTS] = {};
+    silt_tire_push* h_push[SLOTS] = {};
+    size_t cap_jobs[SLOTS] = {}, cap_push[SLOTS] = {};
+    cudaEvent_t ev[SLOTS] = {};
+    int next = 0;
     void release();
 };
 

@@ -424,10 +424,9 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
  * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (4 MiB per
  * GPU that loads the library, held until the process exits); larger grids
  * return SILT_EINVAL. The first call on each device looks the array up (with
- * that device current) and keeps its address for the rest of the process,
- * so make that first call before any stream capture begins; nothing here
- * states whether later calls can be captured. After cudaDeviceReset the kept
- * address is stale: do not call this entry point on a device that was reset.
+ * that device current) and keeps its address for the rest of the process.
+ * After cudaDeviceReset the kept address is stale: do not call this entry
+ * point on a device that was reset.
  * Every call shares the one array: calls whose work overlaps on the GPU race
  * and must be ordered by the caller (one stream, or events). Calls no
  * cudaMalloc, cudaFree or other allocating routine. */

