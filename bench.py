@@ -323,6 +323,17 @@ def run_b200(args):
         one_step(False)
     kt = silt_b200.kernel_times()
     silt_b200.set_kernel_timing(False)
+    # Host pass: the library's own clock around its host work in silt_step
+    # (planning, uploads, launch submission), to compare with the device time.
+    sheet.set_step_timing(True)  # starts the step parts from zero
+    host_steps = min(args.steps, 50)
+    for _ in range(host_steps):
+        one_step(False)
+    torch.cuda.synchronize()
+    hp = sheet.step_parts()
+    sheet.set_step_timing(False)
+    host_inside = {"silt_step": hp["host_step_ms"] / host_steps,
+                   "nested_patch_planning": hp["host_fine_ms"] / host_steps, "steps": host_steps}
     # End to end through the public API, every timed step: the tire pushes go
     # in (inside silt_step, from its pinned step table), the spray events and
     # the FP64 ledger come back, and the ledger's closure is checked each step.
@@ -383,6 +394,7 @@ def run_b200(args):
                         "d2h_bytes_per_step": 56 + 4 + 32 * (nev // max(e2e_steps, 1)), "steps": e2e_steps},
                 "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
+                "host_ms_inside_silt_step": host_inside,
                 "device_counted_steps": int(parts["device_counts"]),
                 "confinement": {"form": "gauss-seidel sweep (step_pair)",
                                 "most_fixed_point_passes": int(parts["sweep_passes_max"]),

@@ -959,12 +959,17 @@ struct StepPlan {
     int slot = 0;
 };
 
+// Staging slots of the per-step tables: a slot is reused STAGING_SLOTS steps
+// later, so the wait for its earlier copy finds it done and the host plans
+// ahead of the device.
+constexpr int STAGING_SLOTS = 4;
+
 struct HostState {
     StepPlan plan;
-    char* d_tab[2] = {nullptr, nullptr};
-    char* h_tab[2] = {nullptr, nullptr};
-    size_t cap[2] = {0, 0};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    char* d_tab[STAGING_SLOTS] = {};
+    char* h_tab[STAGING_SLOTS] = {};
+    size_t cap[STAGING_SLOTS] = {};
+    cudaEvent_t ev[STAGING_SLOTS] = {};
     int flip = 0;
 };
 
@@ -1219,7 +1224,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
     }
     // Patch references, pointing at the axes inside the device table.
     const int slot = HS.flip;
-    HS.flip ^= 1;
+    HS.flip = (HS.flip + 1) % STAGING_SLOTS;
     L.slot = slot;
     size_t need = tab.buf.size() + (size_t)L.np * (sizeof(PatchRef) + 2 * sizeof(window::Job)) + 1024;
     if (need > HS.cap[slot]) {
@@ -1303,7 +1308,7 @@ static int plan_step(Patches& P, silt_sheet* s, const std::vector<silt_tire_push
         }
         L.off_jobs = tab.put(jobs.data(), jobs.size());
     }
-    // The pinned half in use two steps ago may still feed its copy.
+    // The pinned slot in use STAGING_SLOTS steps ago may still feed its copy.
     FCK(cudaEventSynchronize(HS.ev[slot]));
     memcpy(HS.h_tab[slot], tab.buf.data(), tab.buf.size());
     FCK(cudaMemcpyAsync(HS.d_tab[slot], HS.h_tab[slot], tab.buf.size(), cudaMemcpyHostToDevice, W.st));
@@ -1651,7 +1656,7 @@ void destroy(Patches& P) {
     Impl* M = (Impl*)P.impl;
     if (M->host) {
         HostState* HS = (HostState*)M->host;
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < STAGING_SLOTS; ++k) {
             if (HS->ev[k]) cudaEventDestroy(HS->ev[k]);
             cudaFree(HS->d_tab[k]);
             if (HS->h_tab[k]) cudaFreeHost(HS->h_tab[k]);
@@ -1834,16 +1839,16 @@ __global__ void kb_coarse_peel(const PeelRec* recs) {
 }
 
 struct FineBatch {
-    // Double-buffered pinned and device staging: records, then job pointers.
-    char* h_buf[2] = {nullptr, nullptr};
-    char* d_buf[2] = {nullptr, nullptr};
-    size_t cap[2] = {0, 0};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    // Pinned and device staging in a ring of slots: records, then job pointers.
+    char* h_buf[STAGING_SLOTS] = {};
+    char* d_buf[STAGING_SLOTS] = {};
+    size_t cap[STAGING_SLOTS] = {};
+    cudaEvent_t ev[STAGING_SLOTS] = {};
     int flip = 0;
-    PeelRec* h_peel[2] = {nullptr, nullptr};
-    PeelRec* d_peel[2] = {nullptr, nullptr};
-    size_t peel_cap[2] = {0, 0};
-    cudaEvent_t peel_ev[2] = {nullptr, nullptr};
+    PeelRec* h_peel[STAGING_SLOTS] = {};
+    PeelRec* d_peel[STAGING_SLOTS] = {};
+    size_t peel_cap[STAGING_SLOTS] = {};
+    cudaEvent_t peel_ev[STAGING_SLOTS] = {};
     int peel_flip = 0;
 };
 
@@ -1851,7 +1856,7 @@ FineBatch* batch_new() { return new FineBatch(); }
 
 void batch_free(FineBatch* B) {
     if (!B) return;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < STAGING_SLOTS; ++k) {
         if (B->ev[k]) cudaEventSynchronize(B->ev[k]);
         if (B->peel_ev[k]) cudaEventSynchronize(B->peel_ev[k]);
         cudaFree(B->d_buf[k]);
@@ -1907,7 +1912,7 @@ int batch_launch(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std
     const size_t rec_bytes = ((n * sizeof(FineRec)) + 255) & ~size_t(255);
     const size_t need = rec_bytes + njobs * sizeof(window::Job*);
     const int slot = B->flip;
-    B->flip ^= 1;
+    B->flip = (B->flip + 1) % STAGING_SLOTS;
     if (B->ev[slot]) FCK(cudaEventSynchronize(B->ev[slot]));
     if (need > B->cap[slot]) {
         cudaFree(B->d_buf[slot]);
@@ -2017,7 +2022,7 @@ int batch_peel(FineBatch* B, const std::vector<silt_sheet*>& sheets, const std::
     const int n = (int)sheets.size();
     if (n == 0) return SILT_OK;
     const int slot = B->peel_flip;
-    B->peel_flip ^= 1;
+    B->peel_flip = (B->peel_flip + 1) % STAGING_SLOTS;
     if (B->peel_ev[slot]) FCK(cudaEventSynchronize(B->peel_ev[slot]));
     if ((size_t)n > B->peel_cap[slot]) {
         cudaFree(B->d_peel[slot]);

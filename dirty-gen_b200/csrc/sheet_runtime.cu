@@ -118,9 +118,10 @@ struct silt_sheet {
     // Window engine for the coarse pair (SILT_ENGINE_WINDOW).
     int engine = SILT_ENGINE_GRID;
     float* win_planes = nullptr;                  // 2 layers x SCRATCH_PLANES x n
-    silt::window::Job* d_win_jobs = nullptr;      // 2 slots x 2 layers
+    static constexpr int WIN_SLOTS = 4;           // a slot is reused 4 steps later: the host runs ahead
+    silt::window::Job* d_win_jobs = nullptr;      // WIN_SLOTS slots x 2 layers
     silt::window::Job* h_win_jobs = nullptr;      // pinned staging
-    cudaEvent_t win_ev[2] = {nullptr, nullptr};
+    cudaEvent_t win_ev[WIN_SLOTS] = {};
     int win_flip = 0;
     // Walls (silt_set_hydro_solids): the bodies in two device slots, each
     // filled from its pinned half once the copy two updates ago is done.
@@ -439,7 +440,7 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
     if (rc) return rc;
     if ((rc = refresh_material(s))) return rc;
     const int slot = s->win_flip;
-    s->win_flip ^= 1;
+    s->win_flip = (s->win_flip + 1) % silt_sheet::WIN_SLOTS;
     CK(cudaEventSynchronize(s->win_ev[slot]));
     silt::window::Job* jobs = s->h_win_jobs + 2 * slot;
     const float nu_w = water_nu(s);
@@ -632,9 +633,10 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
         const size_t wp = 2 * (size_t)silt::window::SCRATCH_PLANES * s->n * sizeof(float);
         if (e == cudaSuccess) e = cudaMalloc(&s->win_planes, wp);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->win_planes, 0, wp, s->st);
-        if (e == cudaSuccess) e = cudaMalloc(&s->d_win_jobs, 4 * sizeof(silt::window::Job));
-        if (e == cudaSuccess) e = cudaMallocHost(&s->h_win_jobs, 4 * sizeof(silt::window::Job));
-        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&s->win_ev[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_win_jobs, 2 * silt_sheet::WIN_SLOTS * sizeof(silt::window::Job));
+        if (e == cudaSuccess) e = cudaMallocHost(&s->h_win_jobs, 2 * silt_sheet::WIN_SLOTS * sizeof(silt::window::Job));
+        for (int k = 0; k < silt_sheet::WIN_SLOTS && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&s->win_ev[k], cudaEventDisableTiming);
     }
     if (e != cudaSuccess) {
         silt_sheet_destroy(s);
@@ -717,7 +719,7 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->d_bed_drop);
     cudaFree(s->d_wall_out);
     cudaFree(s->d_hole_bits);
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < silt_sheet::WIN_SLOTS; ++k)
         if (s->win_ev[k]) cudaEventDestroy(s->win_ev[k]);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_used) cudaEventDestroy(e);
