@@ -2663,8 +2663,11 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
 // ------------------------------------------------------ free operator, no alloc
 // Scratch for silt_step_sheet_noalloc: the layout silt_step_sheet expects
 // (a 4 KiB job header, then the window engine's scratch planes) for the
-// largest grid it serves. Zero at load, as a first caller scratch must be. Every GPU that loads the library holds this array
-// until the process exits. In host code `g_step_sheet_scratch` is only a
+// largest grid it serves. Zero at load, as a caller's scratch must be before
+// its first use; the header is rewritten by every call and the planes keep
+// what the last call left, like the reference's per-thread sheet scratch.
+// Every GPU that loads the library holds this array until the process
+// exits. In host code `g_step_sheet_scratch` is only a
 // stand-in symbol, never a device address: the address comes from
 // cudaGetSymbolAddress, looked up once per device with that device current.
 static __device__ __align__(256) unsigned char

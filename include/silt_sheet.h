@@ -423,10 +423,13 @@ int silt_step_sheet(float* h, float* u, float* v, const float* bed, const float*
  * allocator. Its scratch is a fixed array compiled into the library, sized
  * for grids up to SILT_STEP_SHEET_STATIC_MAX_RES cells per side (4 MiB per
  * GPU that loads the library, held until the process exits); larger grids
- * return SILT_EINVAL. The first call on each device looks the array up (with
- * that device current) and keeps its address for the rest of the process.
- * After cudaDeviceReset the kept address is stale: do not call this entry
- * point on a device that was reset.
+ * return SILT_EINVAL. The first call on each device does a one-time set-up:
+ * with that device current it looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it for the rest of the process, so make
+ * that first call before any stream capture begins. After cudaDeviceReset
+ * the kept address is stale: do not call this entry point on a device that
+ * was reset. The array keeps what the last call left in it, as the
+ * reference's per-thread sheet scratch does.
  * Every call shares the one array: calls whose work overlaps on the GPU race
  * and must be ordered by the caller (one stream, or events). Calls no
  * cudaMalloc, cudaFree or other allocating routine. */
