@@ -49,6 +49,10 @@ STEP_BYTES_WATER = 28
 STEP_BYTES_SLURRY = 33
 
 
+BATCH_PHASES = ["closure crops + wake entrainment", "per-window planning (workers)", "nested patch launches",
+                "coarse pair + open water", "patch peel", "tracers + reach", "closure correction + books"]
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -692,7 +696,6 @@ def run_batch(args):
     th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, local), daemon=True)
     th.start()
     time.sleep(0.3)
-    batch.set_timing(True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -706,8 +709,18 @@ def run_batch(args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    # The library's step parts (events around the force and transport
+    # launches, host clocks per phase) in a pass of their own after the timed
+    # one, whose region they would otherwise slow; per-step figures below.
+    batch.set_timing(True)
+    part_steps = min(args.steps, 10)
+    for _ in range(part_steps):
+        one_step()
+    torch.cuda.synchronize()
     parts = batch.parts()
     batch.set_timing(False)
+    parts = {k: ([x * args.steps / part_steps for x in v] if isinstance(v, list) else v * args.steps / part_steps)
+             for k, v in parts.items()}
     stop.set()
     th.join(timeout=5)
     if dist:
@@ -761,7 +774,9 @@ def run_batch(args):
                 "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
                 "host_ms_per_step": {"batch_step": parts["host_step_ms"] / args.steps,
-                                     "per_window_before_coarse": parts["host_fine_ms"] / args.steps},
+                                     "per_window_before_coarse": parts["host_fine_ms"] / args.steps,
+                                     "phases": [round(x / args.steps, 4) for x in parts["host_phase_ms"][:7]],
+                                     "phase_names": BATCH_PHASES},
                 "window_steps_per_s": len(all_wins) * args.steps / (ms / 1000.0),
                 "windows": len(all_wins), "windows_rank0": len(wins), "coarse_cells_rank0": coarse,
                 "tires_rank0": n_tires, "ledger_total_m3": float(table[:, 6].sum())}
@@ -1086,11 +1101,11 @@ def run_closure(args):
     th = threading.Thread(target=sample_clocks, args=(stop, clock_lines, 0), daemon=True)
     th.start()
     time.sleep(0.3)
+    part_steps = {}
     for name in forms:
         for _ in range(warm):
             one_step(name)
         torch.cuda.synchronize()
-        forms[name][1].set_timing(True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -1099,6 +1114,13 @@ def run_closure(args):
         e1.record(stream)
         torch.cuda.synchronize()
         timed[name] = e0.elapsed_time(e1)
+        # The library's step parts (per-launch events, host clocks) in a
+        # short pass of their own: their events would slow the timed one.
+        forms[name][1].set_timing(True)
+        part_steps[name] = min(args.steps, 10)
+        for _ in range(part_steps[name]):
+            one_step(name)
+        torch.cuda.synchronize()
         parts[name] = forms[name][1].parts()
         forms[name][1].set_timing(False)
     stop.set()
@@ -1203,8 +1225,14 @@ def run_closure(args):
             "depth_rel_l2_vs_nested": err_closure,
             "ledger_gap_max": gaps["closure"],
             "closure_steps": n_closure, "fallback_steps": n_fallback,
-            "steps_compared": warm + args.steps,
-            "gpu_launches": int(pc["launches"]), "clocks": summarise_clocks(clock_lines)}
+            "steps_compared": warm + args.steps + part_steps["closure"],
+            "gpu_launches": int(pc["launches"]) * args.steps // max(part_steps["closure"], 1),
+            "host_ms_per_step": {name: {"step": parts[name]["host_step_ms"] / max(part_steps[name], 1),
+                                        "phases": [round(x / max(part_steps[name], 1), 4)
+                                                   for x in parts[name]["host_phase_ms"][:7]]}
+                                 for name in forms},
+            "host_phase_names": BATCH_PHASES,
+            "clocks": summarise_clocks(clock_lines)}
     assert step_of["closure"] == step_of["nested"]
     line["vs_fp64_nested"] = closure_fp64_judge(scenes, T, C, net, zero, forms, step_of["closure"])
     if not args.no_baseline:

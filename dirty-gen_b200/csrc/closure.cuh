@@ -53,13 +53,14 @@ struct ApplyJob {
 cudaError_t launch_features(const FeatureJob* d_jobs, int n, const float* d_norm, uint16_t* x, cudaStream_t st);
 cudaError_t launch_apply(const ApplyJob* d_jobs, int n, const float* y, const float* d_norm, cudaStream_t st);
 
-// Per-step records through pinned memory: two slots, each reused only after
-// the copy two puts back has left it.
+// Per-step records through pinned memory: a ring of slots, each reused only
+// after its last copy has left it.
 struct Staging {
-    void* dev[2] = {nullptr, nullptr};
-    void* host[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    size_t cap[2] = {0, 0};
+    static constexpr int SLOTS = 4;  // a slot is reused four puts later: its copy is long done
+    void* dev[SLOTS] = {};
+    void* host[SLOTS] = {};
+    cudaEvent_t ev[SLOTS] = {};
+    size_t cap[SLOTS] = {};
     int flip = 0;
     cudaError_t put(const void* data, size_t bytes, cudaStream_t st, void** out);
     void release();

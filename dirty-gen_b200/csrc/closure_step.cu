@@ -206,7 +206,7 @@ cudaError_t launch_apply(const ApplyJob* d_jobs, int n, const float* y, const fl
 // ---- Staging of per-step job records ---------------------------------------
 
 void Staging::release() {
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < SLOTS; ++k) {
         if (ev[k]) cudaEventSynchronize(ev[k]);
         cudaFree(dev[k]);
         if (host[k]) cudaFreeHost(host[k]);
@@ -220,9 +220,9 @@ void Staging::release() {
 
 cudaError_t Staging::put(const void* data, size_t bytes, cudaStream_t st, void** out) {
     const int k = flip;
-    flip ^= 1;
+    flip = (flip + 1) % SLOTS;
     cudaError_t e = cudaSuccess;
-    if (ev[k]) e = cudaEventSynchronize(ev[k]);  // the copy two puts back has left the pinned buffer
+    if (ev[k]) e = cudaEventSynchronize(ev[k]);  // this slot's last copy has left the pinned buffer
     if (e != cudaSuccess) return e;
     if (bytes > cap[k]) {
         cudaFree(dev[k]);

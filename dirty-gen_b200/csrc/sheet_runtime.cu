@@ -1995,10 +1995,13 @@ struct silt_batch {
     int* entry_win = nullptr;
     int* count = nullptr;           // two count slots, used alternately by successive substeps
     unsigned long long seq = 0;
-    silt::WindowSubstep* d_ws[2] = {nullptr, nullptr};
-    silt::WindowSubstep* h_ws[2] = {nullptr, nullptr};  // pinned
-    size_t ws_cap[2] = {0, 0};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    // Substep descriptors in a ring of slots, reused WS_SLOTS steps later, so
+    // the wait for a slot's earlier copy finds it done and the host plans ahead.
+    static constexpr int WS_SLOTS = 4;
+    silt::WindowSubstep* d_ws[WS_SLOTS] = {};
+    silt::WindowSubstep* h_ws[WS_SLOTS] = {};  // pinned
+    size_t ws_cap[WS_SLOTS] = {};
+    cudaEvent_t ev[WS_SLOTS] = {};
     int flip = 0;
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool, ev_used;  // groups of three: start, after force, after transport
@@ -2038,7 +2041,7 @@ int batch_free(silt_batch* b) {
     cudaFree(b->d_tr_sum);
     b->tr_run.release();
     if (b->h_ledgers) cudaFreeHost(b->h_ledgers);
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < silt_batch::WS_SLOTS; ++k) {
         cudaFree(b->d_ws[k]);
         if (b->h_ws[k]) cudaFreeHost(b->h_ws[k]);
         if (b->ev[k]) cudaEventDestroy(b->ev[k]);
@@ -2115,13 +2118,13 @@ int batch_coarse(silt_batch* b, float dt) {
         device_count = device_count || plans[w].sc.speed2 != nullptr;
     }
     const int slot = b->flip;
-    b->flip ^= 1;
+    b->flip = (b->flip + 1) % silt_batch::WS_SLOTS;
     const size_t need = (size_t)steps * n;
     // The batch's sweep launches keep their state in the first window's
     // slot, so their errors come back through that window's flags.
     silt::SweepState* sweep = b->sheets[0]->sweep_state();
     bool sweeping = false;
-    if (b->ev[slot]) CK(cudaEventSynchronize(b->ev[slot]));  // the descriptors two steps back are copied
+    if (b->ev[slot]) CK(cudaEventSynchronize(b->ev[slot]));  // this slot's last copy has left its pinned half
     if (need > b->ws_cap[slot]) {
         cudaFree(b->d_ws[slot]);
         if (b->h_ws[slot]) cudaFreeHost(b->h_ws[slot]);
@@ -2293,6 +2296,15 @@ int silt_batch_step(silt_batch* b, float dt) {
     const unsigned long long launches0 = silt::t_kernel_launches;
     using clock = std::chrono::steady_clock;
     const clock::time_point t0 = clock::now();
+    clock::time_point tp = t0;
+    // Host time per phase of the step (with timing on): the time since the
+    // last mark goes to phase k.
+    auto phase = [&](int k) {
+        if (!b->timing) return;
+        const clock::time_point t = clock::now();
+        b->parts.host_phase_ms[k] += std::chrono::duration<double, std::milli>(t - tp).count();
+        tp = t;
+    };
     const int n = (int)b->sheets.size();
     std::vector<std::vector<silt_tire_push>> ps(n);
     std::vector<silt::fine::StepOut> fo(n);
@@ -2314,6 +2326,7 @@ int silt_batch_step(silt_batch* b, float dt) {
             if (s->turbidity && !s->pushes.empty()) tw.push_back(tracer_window(s, s->pushes));
         if (!tw.empty()) CK(silt::tracers::entrain(b->tr_run, tw.data(), (int)tw.size(), dt, b->st));
     }
+    phase(0);
     CK(cudaEventRecord(b->ev_start, b->st));  // the workers' streams start after the batch's previous work
     // Each window's tire pushes, inflow and nested-patch planning on the
     // workers (the planning uploads the window's tables on the worker's
@@ -2347,6 +2360,7 @@ int silt_batch_step(silt_batch* b, float dt) {
             return Wk.rc[k];
         }
     for (int k = 0; k < nk; ++k) CK(cudaStreamWaitEvent(b->st, Wk.done[k], 0));
+    phase(1);
     std::vector<silt_sheet*> fs;
     std::vector<silt::fine::Patches*> fp;
     for (int w = 0; w < n; ++w)
@@ -2355,13 +2369,16 @@ int silt_batch_step(silt_batch* b, float dt) {
             fp.push_back(&b->sheets[w]->fine);
         }
     if ((rc = silt::fine::batch_launch(b->fine, fs, fp, dt, b->st))) return rc;
+    phase(2);
     const clock::time_point t1 = clock::now();
     for (silt_sheet* s : b->sheets)
         if ((rc = wave_step(s, dt))) return rc;
     if ((rc = batch_coarse(b, dt))) return rc;
     for (silt_sheet* s : b->sheets)
         if ((rc = open_water_step(s, dt))) return rc;
+    phase(3);
     if ((rc = silt::fine::batch_peel(b->fine, fs, fp, b->st))) return rc;
+    phase(4);
     {
         // step_tracers of every window in one launch sequence, the reach, then
         // the suspended load of the windows with turbidity on.
@@ -2377,6 +2394,7 @@ int silt_batch_step(silt_batch* b, float dt) {
             if (b->sheets[w]->turbidity) sw.push_back(tracer_window(b->sheets[w], ps[w]));
         if (!sw.empty()) CK(silt::tracers::step_suspended(b->tr_run, sw.data(), (int)sw.size(), dt, b->st));
     }
+    phase(5);
     if (!net_win.empty()) {
         std::vector<silt::closure::ApplyJob> A(net_win.size());
         memset(A.data(), 0, A.size() * sizeof(silt::closure::ApplyJob));
@@ -2395,6 +2413,7 @@ int silt_batch_step(silt_batch* b, float dt) {
     b->parts.steps += 1;
     b->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
     for (auto c : Wk.launches) b->parts.launches += (int64_t)c;
+    phase(6);
     if (b->timing) {
         const clock::time_point t2 = clock::now();
         b->parts.host_step_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();

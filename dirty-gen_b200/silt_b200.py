@@ -84,7 +84,17 @@ class StepParts(ctypes.Structure):
                 ("device_counts", ctypes.c_int64), ("host_step_ms", ctypes.c_double),
                 ("host_fine_ms", ctypes.c_double), ("sweep_launches", ctypes.c_int64),
                 ("sweep_passes_max", ctypes.c_int64), ("sweep_fallbacks", ctypes.c_int64),
-                ("sweep_solves", ctypes.c_int64), ("sweep_local_passes", ctypes.c_int64)]
+                ("sweep_solves", ctypes.c_int64), ("sweep_local_passes", ctypes.c_int64),
+                ("host_phase_ms", ctypes.c_double * 8)]
+
+
+def parts_dict(sp):
+    """A StepParts as a dict (arrays as lists)."""
+    out = {}
+    for k, _ in StepParts._fields_:
+        v = getattr(sp, k)
+        out[k] = list(v) if isinstance(v, ctypes.Array) else v
+    return out
 
 
 class KernelTime(ctypes.Structure):
@@ -436,7 +446,7 @@ class Sheet:
     def step_parts(self):
         sp = StepParts()
         check(lib().silt_get_step_parts(self.h, ctypes.byref(sp)), "step_parts")
-        return {k: getattr(sp, k) for k, _ in StepParts._fields_}
+        return parts_dict(sp)
 
     def fine_water_debug(self, tires, patch=0):
         arr = (TirePush * max(len(tires), 1))()
@@ -547,4 +557,4 @@ class Batch:
     def parts(self):
         sp = StepParts()
         check(lib().silt_batch_get_parts(self.h, ctypes.byref(sp)), "batch_parts")
-        return {k: getattr(sp, k) for k, _ in StepParts._fields_}
+        return parts_dict(sp)
