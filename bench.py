@@ -721,6 +721,15 @@ def run_batch(args):
     batch.set_timing(False)
     parts = {k: ([x * args.steps / part_steps for x in v] if isinstance(v, list) else v * args.steps / part_steps)
              for k, v in parts.items()}
+    # Kernel pass: CUDA events around every launch, each kernel's device time.
+    silt_b200.set_kernel_timing(True)
+    for _ in range(part_steps):
+        one_step()
+    kt = silt_b200.kernel_times()
+    silt_b200.set_kernel_timing(False)
+    ktotal = sum(k["ms"] for k in kt) or 1.0
+    kernels = [{"name": k["name"], "launches": k["launches"], "avg_ms": k["ms"] / max(k["launches"], 1),
+                "ms_per_step": k["ms"] / part_steps, "share": k["ms"] / ktotal} for k in kt[:16]]
     stop.set()
     th.join(timeout=5)
     if dist:
@@ -771,7 +780,7 @@ def run_batch(args):
                 "data": "synthetic", "config": batch_workload(args), "roofline": roof,
                 "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * n_tires,
                         "d2h_bytes_per_step": 40 * len(wins), "steps": e2e_steps},
-                "gpu_launches": int(parts["launches"]), "clocks": summarise_clocks(clock_lines),
+                "gpu_launches": int(parts["launches"]), "kernels": kernels, "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
                 "host_ms_per_step": {"batch_step": parts["host_step_ms"] / args.steps,
                                      "per_window_before_coarse": parts["host_fine_ms"] / args.steps,
