@@ -153,19 +153,6 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per algorithmic byte of k_force, from the committed ncu summary
-    (a capture whose algorithmic bytes are exact: every tile stepped)."""
-    path = os.path.join(ROOT, "profiles", "k_force_grid_traffic.txt")
-    try:
-        for ln in open(path):
-            if ln.startswith("dram_bytes_per_algorithmic_byte:"):
-                return float(ln.split(":", 1)[1])
-    except (OSError, ValueError):
-        pass
-    return None
-
-
 def host_cpu():
     """The host CPU the CPU legs ran on: model name and logical cores."""
     model = "unknown"
