@@ -675,6 +675,14 @@ def run_batch(args):
         batch.push_tires(idx, push_rec)
         batch.step(DT)
 
+    # The launch settings come from the library's autotuner, which times the
+    # first steps under each candidate (every candidate gives the same bits);
+    # the warm-up steps follow once it has chosen.
+    batch.autotune(True)
+    for _ in range(40):
+        if batch.tune()["tuned"]:
+            break
+        one_step()
     for _ in range(max(3, args.warmup)):
         one_step()
     torch.cuda.synchronize()
@@ -767,7 +775,8 @@ def run_batch(args):
                 "data": "synthetic", "config": batch_workload(args), "roofline": roof,
                 "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * n_tires,
                         "d2h_bytes_per_step": 40 * len(wins), "steps": e2e_steps},
-                "gpu_launches": int(parts["launches"]), "kernels": kernels, "clocks": summarise_clocks(clock_lines),
+                "gpu_launches": int(parts["launches"]), "kernels": kernels, "launch_settings": batch.tune(),
+                "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
                 "host_ms_per_step": {"batch_step": parts["host_step_ms"] / args.steps,
                                      "per_window_before_coarse": parts["host_fine_ms"] / args.steps,

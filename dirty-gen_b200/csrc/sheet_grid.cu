@@ -1373,15 +1373,22 @@ cudaError_t launch_coop(K kernel, int grid, cudaStream_t st, Args... args) {
 }
 
 cudaError_t launch_batch_force(const WindowSubstep* d_ws, int nwin, const int* list, const int* entry_win,
-                               const int* count, SweepState* sweep, cudaStream_t st) {
+                               const int* count, SweepState* sweep, cudaStream_t st, int ctas_per_sm) {
     if (sweep) {
         static std::once_flag sattr;
-        static int grid = 0;
+        static int grid = 0, nsm = 148;
         std::call_once(sattr, [] {
             cudaFuncSetAttribute(k_batch_force_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)force_smem_bytes());
             grid = coop_grid(k_batch_force_sweep, force_smem_bytes());
+            int dev = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+                nsm = 148;
+            cudaGetLastError();
         });
-        const cudaError_t e = launch_coop(k_batch_force_sweep, grid, st, d_ws, nwin, list, entry_win, count, sweep);
+        // Fewer CTAs than the device holds stay co-resident: the launch is still cooperative.
+        const int g = ctas_per_sm > 0 ? std::min(grid, ctas_per_sm * nsm) : grid;
+        const cudaError_t e = launch_coop(k_batch_force_sweep, g, st, d_ws, nwin, list, entry_win, count, sweep);
         return e != cudaSuccess ? e : cudaGetLastError();
     }
     static std::once_flag attr;
@@ -1392,10 +1399,11 @@ cudaError_t launch_batch_force(const WindowSubstep* d_ws, int nwin, const int* l
 }
 
 cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
-                                   const int* count, cudaStream_t st) {
+                                   const int* count, cudaStream_t st, int blocks) {
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_batch_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
-    ::silt::launch_dep(k_batch_transport, dim3(148 * 4), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, d_ws, list, entry_win, count);
+    const unsigned grid = blocks > 0 ? (unsigned)blocks : 148u * 4u;
+    ::silt::launch_dep(k_batch_transport, dim3(grid), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, d_ws, list, entry_win, count);
     ::silt::count_launch();
     return cudaGetLastError();
 }

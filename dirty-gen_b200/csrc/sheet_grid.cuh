@@ -156,10 +156,13 @@ cudaError_t launch_batch_speed2(const WindowSubstep* d_ws, const int* list, cons
 // `sweep` non-null: some window confines by the Gauss-Seidel sweep, and the
 // force pass runs as one cooperative launch (pre-sweep tiles, the sweep's
 // fixed point, projection) over every window.
+// `ctas_per_sm` caps the cooperative launch's CTAs per SM (at most what the
+// device holds at once; 0 = that maximum); `blocks` sizes the transport's
+// persistent grid (0 = four per SM). Every setting gives the same bits.
 cudaError_t launch_batch_force(const WindowSubstep* d_ws, int nwin, const int* list, const int* entry_win,
-                               const int* count, SweepState* sweep, cudaStream_t st);
+                               const int* count, SweepState* sweep, cudaStream_t st, int ctas_per_sm = 0);
 cudaError_t launch_batch_transport(const WindowSubstep* d_ws, const int* list, const int* entry_win,
-                                   const int* count, cudaStream_t st);
+                                   const int* count, cudaStream_t st, int blocks = 0);
 
 size_t force_smem_bytes();
 // Builds the tile list of one substep: active tiles of both layers, then the

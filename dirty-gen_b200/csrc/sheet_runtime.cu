@@ -15,6 +15,7 @@
 #include <cstring>
 #include <condition_variable>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -1983,8 +1984,20 @@ struct BatchWorkers {
     }
 };
 
+// Batch autotuner state (silt_batch_autotune).
+struct BatchTuner {
+    static constexpr int KNOBS = 3, REPS = 2, SKIP = 6;
+    bool active = false;
+    int knob = 0, cand = 0, rep = 0, skip = SKIP;
+    float best_rep = 0.0f;     // the current candidate's best step so far
+    cudaEvent_t e0[REPS] = {}, e1[REPS] = {};
+    std::vector<float> cand_ms;  // the current knob's candidates' best times
+};
+
 struct silt_batch {
     std::vector<silt_sheet*> sheets;
+    silt_batch_tune tune = {2, 148 * 4, 2368, 0, 0, {}};  // launch settings in force
+    BatchTuner tuner;
     BatchWorkers* workers = nullptr;
     silt::fine::FineBatch* fine = nullptr;  // staging of the batched nested-patch launches
     cudaEvent_t ev_start = nullptr;
@@ -2024,6 +2037,10 @@ namespace {
 int batch_free(silt_batch* b) {
     if (!b) return SILT_OK;
     if (b->st) cudaStreamSynchronize(b->st);
+    for (int r = 0; r < BatchTuner::REPS; ++r) {
+        if (b->tuner.e0[r]) cudaEventDestroy(b->tuner.e0[r]);
+        if (b->tuner.e1[r]) cudaEventDestroy(b->tuner.e1[r]);
+    }
     if (b->clos) {
         b->clos->release();
         delete b->clos;
@@ -2105,6 +2122,109 @@ int batch_closure_begin(silt_batch* b, std::vector<int>& net_win, std::vector<si
 
 // The coarse pairs of every window, `launched` substeps at most, through the
 // batched list, speed, force and transport kernels.
+// ------------------------------------------------------- batch autotuner
+// Candidates of each launch setting, the default first.
+const std::vector<int>& tune_cands(int knob) {
+    static const std::vector<int> c[BatchTuner::KNOBS] = {{2, 1}, {148 * 4, 148 * 2, 148 * 8}, {2368, 1184, 4736}};
+    return c[knob];
+}
+
+int& tune_field(silt_batch_tune& t, int knob) {
+    return knob == 0 ? t.sweep_ctas_per_sm : (knob == 1 ? t.transport_blocks : t.tracer_blocks);
+}
+
+// The size class a choice is kept for: device, window count, coarse cells.
+std::string tune_key(silt_batch* b) {
+    size_t cells = 0;
+    for (silt_sheet* s : b->sheets) cells += s->n;
+    char k[96];
+    snprintf(k, sizeof k, "dev%d_win%zu_cells%zu", b->device, b->sheets.size(), cells);
+    return k;
+}
+
+std::mutex g_tune_mu;
+std::map<std::string, silt_batch_tune> g_tune_cache;
+bool g_tune_loaded = false;
+
+// SILT_TUNE_CACHE: one line per choice, "key sweep_ctas_per_sm transport_blocks tracer_blocks".
+void tune_cache_load() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = getenv("SILT_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = fopen(path, "r");
+    if (!f) return;
+    char key[96];
+    int a = 0, c = 0, d = 0;
+    while (fscanf(f, "%95s %d %d %d", key, &a, &c, &d) == 4) {
+        if (a < 1 || a > 2 || c < 1 || d < 1) continue;
+        silt_batch_tune t = {a, c, d, 1, 0, {}};
+        g_tune_cache[key] = t;
+    }
+    fclose(f);
+}
+
+void tune_cache_store(const std::string& key, const silt_batch_tune& t) {
+    g_tune_cache[key] = t;
+    const char* path = getenv("SILT_TUNE_CACHE");
+    if (!path || !*path) return;
+    if (FILE* f = fopen(path, "a")) {
+        fprintf(f, "%s %d %d %d\n", key.c_str(), t.sweep_ctas_per_sm, t.transport_blocks, t.tracer_blocks);
+        fclose(f);
+    }
+}
+
+// Before a step's work: set the candidate under trial and mark the start.
+// Returns whether this step is timed.
+int tune_before(silt_batch* b, bool* timed) {
+    *timed = false;
+    BatchTuner& T = b->tuner;
+    if (!T.active) return SILT_OK;
+    if (T.skip > 0) {
+        --T.skip;
+        return SILT_OK;
+    }
+    tune_field(b->tune, T.knob) = tune_cands(T.knob)[T.cand];
+    for (int r = 0; r < BatchTuner::REPS; ++r) {
+        if (!T.e0[r]) CK(cudaEventCreate(&T.e0[r]));
+        if (!T.e1[r]) CK(cudaEventCreate(&T.e1[r]));
+    }
+    CK(cudaEventRecord(T.e0[T.rep], b->st));
+    *timed = true;
+    return SILT_OK;
+}
+
+// After a timed step: once a candidate has run its steps, keep its best
+// time; once a setting's candidates are done, fix the fastest.
+int tune_after(silt_batch* b) {
+    BatchTuner& T = b->tuner;
+    CK(cudaEventRecord(T.e1[T.rep], b->st));
+    if (++T.rep < BatchTuner::REPS) return SILT_OK;
+    T.rep = 0;
+    CK(cudaEventSynchronize(T.e1[BatchTuner::REPS - 1]));
+    float best = 0.0f;
+    for (int r = 0; r < BatchTuner::REPS; ++r) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, T.e0[r], T.e1[r]));
+        best = r == 0 ? ms : std::min(best, ms);
+    }
+    if (b->tune.trials < 16) b->tune.trial_ms[b->tune.trials] = best;
+    b->tune.trials += 1;
+    T.cand_ms.push_back(best);
+    const std::vector<int>& c = tune_cands(T.knob);
+    if (++T.cand < (int)c.size()) return SILT_OK;
+    const int pick = (int)(std::min_element(T.cand_ms.begin(), T.cand_ms.end()) - T.cand_ms.begin());
+    tune_field(b->tune, T.knob) = c[pick];
+    T.cand_ms.clear();
+    T.cand = 0;
+    if (++T.knob < BatchTuner::KNOBS) return SILT_OK;
+    T.active = false;
+    b->tune.tuned = 1;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_cache_store(tune_key(b), b->tune);
+    return SILT_OK;
+}
+
 int batch_coarse(silt_batch* b, float dt) {
     const int n = (int)b->sheets.size();
     std::vector<CoarsePlan> plans(n);
@@ -2175,9 +2295,10 @@ int batch_coarse(silt_batch* b, float dt) {
             if (!e0 || !e1 || !e2) return fail_cuda(cudaErrorMemoryAllocation, "batch timing events");
             CK(cudaEventRecord(e0, b->st));
         }
-        CK(silt::launch_batch_force(d, n, b->list, b->entry_win, count, sweeping ? sweep : nullptr, b->st));
+        CK(silt::launch_batch_force(d, n, b->list, b->entry_win, count, sweeping ? sweep : nullptr, b->st,
+                                    b->tune.sweep_ctas_per_sm));
         if (b->timing) CK(cudaEventRecord(e1, b->st));
-        CK(silt::launch_batch_transport(d, b->list, b->entry_win, count, b->st));
+        CK(silt::launch_batch_transport(d, b->list, b->entry_win, count, b->st, b->tune.transport_blocks));
         if (b->timing) CK(cudaEventRecord(e2, b->st));
         b->parts.force_launches += 1;
     }
@@ -2297,6 +2418,9 @@ int silt_batch_step(silt_batch* b, float dt) {
     using clock = std::chrono::steady_clock;
     const clock::time_point t0 = clock::now();
     clock::time_point tp = t0;
+    bool tune_timed = false;
+    if ((rc = tune_before(b, &tune_timed))) return rc;
+    b->tr_run.blocks_total = b->tune.tracer_blocks;
     // Host time per phase of the step (with timing on): the time since the
     // last mark goes to phase k.
     auto phase = [&](int k) {
@@ -2414,6 +2538,7 @@ int silt_batch_step(silt_batch* b, float dt) {
     b->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
     for (auto c : Wk.launches) b->parts.launches += (int64_t)c;
     phase(6);
+    if (tune_timed && (rc = tune_after(b))) return rc;
     if (b->timing) {
         const clock::time_point t2 = clock::now();
         b->parts.host_step_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
@@ -2491,6 +2616,51 @@ int silt_batch_set_timing(silt_batch* b, int32_t on) {
             CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, b->st));
             CK(cudaMemsetAsync(&s->sweep_state()->passes_max, 0, 3 * sizeof(unsigned int), b->st));
         }
+    return SILT_OK;
+}
+
+int silt_batch_autotune(silt_batch* b, int32_t on) {
+    if (!b) return fail_arg("batch");
+    BatchTuner& T = b->tuner;
+    if (!on) {
+        T.active = false;
+        return SILT_OK;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_cache_load();
+        auto it = g_tune_cache.find(tune_key(b));
+        if (it != g_tune_cache.end()) {
+            b->tune = it->second;
+            b->tune.tuned = 1;
+            b->tune.trials = 0;
+            T.active = false;
+            return SILT_OK;
+        }
+    }
+    T.active = true;
+    T.knob = T.cand = T.rep = 0;
+    T.skip = BatchTuner::SKIP;
+    T.cand_ms.clear();
+    b->tune = silt_batch_tune{2, 148 * 4, 2368, 0, 0, {}};
+    return SILT_OK;
+}
+
+int silt_batch_get_tune(silt_batch* b, silt_batch_tune* out) {
+    if (!b || !out) return fail_arg("batch tune");
+    *out = b->tune;
+    return SILT_OK;
+}
+
+int silt_batch_set_tune(silt_batch* b, const silt_batch_tune* in) {
+    if (!b || !in) return fail_arg("batch tune");
+    if (in->sweep_ctas_per_sm < 0 || in->sweep_ctas_per_sm > 2 || in->transport_blocks < 0 ||
+        in->transport_blocks > 65535 || in->tracer_blocks < 0 || in->tracer_blocks > 65535)
+        return fail_arg("batch tune: sweep_ctas_per_sm 1..2, blocks 1..65535 (0 keeps the default)");
+    b->tuner.active = false;
+    b->tune = silt_batch_tune{in->sweep_ctas_per_sm > 0 ? in->sweep_ctas_per_sm : 2,
+                              in->transport_blocks > 0 ? in->transport_blocks : 148 * 4,
+                              in->tracer_blocks > 0 ? in->tracer_blocks : 2368, 0, 0, {}};
     return SILT_OK;
 }
 

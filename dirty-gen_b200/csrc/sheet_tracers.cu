@@ -1241,11 +1241,11 @@ void entrain_box(const Sheet& S, const silt_tire_push* p, int n, int* b) {
 }
 
 // Blocks per window of a launch over n windows: enough for the largest
-// window, about 2400 blocks of 256 threads in all.
-int blocks_x(const Window* w, int n) {
+// window, about `total` blocks of 256 threads in all.
+int blocks_x(const Window* w, int n, int total) {
     size_t most = 1;
     for (int k = 0; k < n; ++k) most = std::max(most, (size_t)w[k].S.res * w[k].S.res);
-    const size_t per = std::max<size_t>(1, 2368 / (size_t)std::max(n, 1));
+    const size_t per = std::max<size_t>(1, (size_t)std::max(total, 1) / (size_t)std::max(n, 1));
     return (int)std::min((most + 255) / 256, per);
 }
 
@@ -1377,7 +1377,7 @@ cudaError_t entrain(Runner& R, const Window* w, int n, float dt, cudaStream_t st
     const Job* jobs = nullptr;
     cudaError_t e = upload(R, w, n, dt, 0.0f, 0.0f, st, &jobs);
     if (e != cudaSuccess) return e;
-    LAUNCH(k_entrain, blocks_x(w, n), jobs);
+    LAUNCH(k_entrain, blocks_x(w, n, R.blocks_total), jobs);
     return cudaSuccess;
 }
 
@@ -1389,7 +1389,7 @@ cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream
     const Job* jobs = nullptr;
     cudaError_t e = upload(R, w, n, dt, foam_decay, silt_keep, st, &jobs);
     if (e != cudaSuccess) return e;
-    const int bx = blocks_x(w, n);
+    const int bx = blocks_x(w, n, R.blocks_total);
     bool rescan = false;
     for (int k = 0; k < n; ++k) rescan = rescan || w[k].rescan;
     if (rescan) LAUNCH(k_scan, bx, jobs);
@@ -1410,7 +1410,7 @@ cudaError_t step_suspended(Runner& R, const Window* w, int n, float dt, cudaStre
     if (e != cudaSuccess) return e;
     LAUNCH(k_susp_begin, 1, jobs);
     if (!(dt > 0.0f) || !std::isfinite(dt)) return cudaSuccess;
-    const int bx = blocks_x(w, n);
+    const int bx = blocks_x(w, n, R.blocks_total);
     LAUNCH(k_susp_settle, bx, jobs);
     LAUNCH(k_susp_take, bx, jobs);
     LAUNCH(k_susp_give, bx, jobs);

@@ -88,6 +88,11 @@ class StepParts(ctypes.Structure):
                 ("host_phase_ms", ctypes.c_double * 8)]
 
 
+class BatchTune(ctypes.Structure):
+    _fields_ = [("sweep_ctas_per_sm", _i), ("transport_blocks", _i), ("tracer_blocks", _i), ("tuned", _i),
+                ("trials", _i), ("trial_ms", ctypes.c_float * 16)]
+
+
 def parts_dict(sp):
     """A StepParts as a dict (arrays as lists)."""
     out = {}
@@ -156,6 +161,8 @@ def lib():
             "silt_batch_get_ledgers": [_p, ctypes.POINTER(Ledger)],
             "silt_batch_push_tires": [_p, _p, ctypes.POINTER(TirePush), _i],
             "silt_batch_set_timing": [_p, _i], "silt_batch_get_parts": [_p, ctypes.POINTER(StepParts)],
+            "silt_batch_autotune": [_p, _i], "silt_batch_get_tune": [_p, ctypes.POINTER(BatchTune)],
+            "silt_batch_set_tune": [_p, ctypes.POINTER(BatchTune)],
             "silt_plane_device": [_p, _i, ctypes.POINTER(_p)], "silt_sheet_copy_state": [_p, _p],
             "silt_set_open_water": [_p, _i, _f, _f, _f], "silt_set_surface_diffusion": [_p, _f],
             "silt_set_turbidity_enabled": [_p, _i], "silt_sample": [_p, _f, _f, ctypes.POINTER(GroundSample)],
@@ -514,6 +521,22 @@ class Batch:
         h = _p()
         check(lib().silt_batch_create(arr, len(self.sheets), ctypes.byref(h)), "batch_create")
         self.h = h
+
+    def autotune(self, on=True):
+        """Times the next steps under each candidate launch setting and keeps
+        the fastest (silt_batch_autotune); every setting gives the same bits."""
+        check(lib().silt_batch_autotune(self.h, int(on)), "batch_autotune")
+
+    def tune(self):
+        t = BatchTune()
+        check(lib().silt_batch_get_tune(self.h, ctypes.byref(t)), "batch_get_tune")
+        return {"sweep_ctas_per_sm": t.sweep_ctas_per_sm, "transport_blocks": t.transport_blocks,
+                "tracer_blocks": t.tracer_blocks, "tuned": bool(t.tuned), "trials": t.trials,
+                "trial_ms": [round(float(x), 4) for x in t.trial_ms[:min(t.trials, 16)]]}
+
+    def set_tune(self, sweep_ctas_per_sm=0, transport_blocks=0, tracer_blocks=0):
+        t = BatchTune(sweep_ctas_per_sm, transport_blocks, tracer_blocks, 0, 0)
+        check(lib().silt_batch_set_tune(self.h, ctypes.byref(t)), "batch_set_tune")
 
     def close(self):
         if getattr(self, "h", None):

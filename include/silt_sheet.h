@@ -349,6 +349,30 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out);
  * launches and host time, as silt_get_step_parts reports for one sheet. */
 int silt_batch_set_timing(silt_batch* b, int32_t on);
 int silt_batch_get_parts(silt_batch* b, silt_step_parts* out);
+/* The batch's launch settings, picked by timed trials. No counterpart in the
+ * reference, which steps its windows one after another. Every setting gives
+ * the same bits, so the autotuner times ordinary steps: after six untimed
+ * steps it varies one setting at a time (coordinate descent), runs each
+ * candidate for two steps, keeps the faster candidate's best time, fixes the
+ * best candidate before the next setting, and stops after 16 timed steps.
+ * The choice is kept for the process per device and size class (window
+ * count and coarse cells), and appended to the file named by the
+ * environment variable SILT_TUNE_CACHE when set (read at the first tuning);
+ * a later batch of the same class takes it without trials. */
+typedef struct {
+    int32_t sweep_ctas_per_sm;  /* CTAs per SM of the batched Gauss-Seidel launch (1 or 2) */
+    int32_t transport_blocks;   /* blocks of the batched transport's persistent grid */
+    int32_t tracer_blocks;      /* blocks of a tracer pass over all the windows */
+    int32_t tuned;              /* 1: chosen by trials or taken from the cache; 0: defaults or set */
+    int32_t trials;             /* candidates timed */
+    float trial_ms[16];         /* each candidate's best step time (device, ms), in trial order */
+} silt_batch_tune;
+/* on != 0 starts the trials with the next steps (or takes a cached choice);
+ * 0 stops them and keeps the settings in force. */
+int silt_batch_autotune(silt_batch* b, int32_t on);
+int silt_batch_get_tune(silt_batch* b, silt_batch_tune* out);
+/* Sets the three settings directly (0 keeps a setting's default). */
+int silt_batch_set_tune(silt_batch* b, const silt_batch_tune* in);
 
 /* ------------------------------------------------------------------ knobs */
 /* FluidCore::set_fine_sub_cap / set_fine_pace (src/fluid_core.rs:5072, :5085). */

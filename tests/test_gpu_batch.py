@@ -74,3 +74,59 @@ def test_batch_refuses_window_engine_sheets_and_mixed_streams():
     a, b = G.Sheet(res=64, engine=G.ENGINE_GRID), G.Sheet(res=64, engine=G.ENGINE_GRID)
     with pytest.raises(G.SiltError, match="one stream"):
         G.Batch([a, b])
+
+
+def _batch_of(scenes, stream):
+    sheets = [make(sc, False, stream.cuda_stream) for sc in scenes]
+    return sheets, G.Batch(sheets)
+
+
+def _drive(batch, n_win, steps):
+    for k in range(1, steps + 1):
+        idx, tires = [], []
+        for w in range(n_win):
+            for t in S.tires_at(k * DT, speed=5.0, z0=-3.0)[:1 + w % 3]:
+                idx.append(w)
+                tires.append(t)
+        batch.push_tires(idx, tires)
+        batch.step(DT)
+
+
+def test_batch_autotuner_times_real_steps_and_changes_no_bit():
+    """The autotuner (silt_batch_autotune) picks the batched sweep's CTAs per
+    SM, the transport's grid and the tracer passes' blocks by timing the
+    batch's own steps; every candidate computes the same bits, so a tuned
+    batch, one with explicit settings and one on the defaults end equal. A
+    second batch of the same size class takes the kept choice without trials."""
+    import torch
+
+    scenes = [S.grid(res=r, seed=0x77 + r, puddles=3) for r in (64, 100, 160)]
+    stream = torch.cuda.Stream()
+    runs = {}
+    for mode in ("default", "tuned", "set"):
+        sheets, b = _batch_of(scenes, stream)
+        if mode == "tuned":
+            b.autotune(True)
+        elif mode == "set":
+            b.set_tune(sweep_ctas_per_sm=1, transport_blocks=296, tracer_blocks=1184)
+        _drive(b, len(scenes), 26)  # six untimed steps, then 8 candidates x 2 timed steps
+        runs[mode] = (sheets, b, b.tune())
+    t = runs["tuned"][2]
+    assert t["tuned"] and t["trials"] == 8 and all(x > 0.0 for x in t["trial_ms"]), t
+    assert t["sweep_ctas_per_sm"] in (1, 2) and t["transport_blocks"] in (296, 592, 1184)
+    assert t["tracer_blocks"] in (1184, 2368, 4736)
+    assert runs["set"][2]["sweep_ctas_per_sm"] == 1 and not runs["set"][2]["tuned"]
+    for mode in ("tuned", "set"):
+        for w in range(len(scenes)):
+            for name in ("water", "slurry", "uw", "vw", "foam", "turbid", "susp"):
+                a, c = runs["default"][0][w].get(name), runs[mode][0][w].get(name)
+                assert np.array_equal(a.view(np.uint32), c.view(np.uint32)), (mode, w, name)
+    sheets, b = _batch_of(scenes, stream)
+    b.autotune(True)
+    again = b.tune()
+    assert again["tuned"] and again["trials"] == 0
+    for k in ("sweep_ctas_per_sm", "transport_blocks", "tracer_blocks"):
+        assert again[k] == t[k]
+    b.close()
+    for _, bb, _ in runs.values():
+        bb.close()
