@@ -324,7 +324,9 @@ def run_b200(args):
     hp = sheet.step_parts()
     sheet.set_step_timing(False)
     host_inside = {"silt_step": hp["host_step_ms"] / host_steps,
-                   "nested_patch_planning": hp["host_fine_ms"] / host_steps, "steps": host_steps}
+                   "nested_patch_planning": hp["host_fine_ms"] / host_steps, "steps": host_steps,
+                   "phases": [round(x / host_steps, 4) for x in hp["host_phase_ms"][:7]],
+                   "phase_names": BATCH_PHASES}
     # End to end through the public API, every timed step: the tire pushes go
     # in (inside silt_step, from its pinned step table), the spray events and
     # the FP64 ledger come back, and the ledger's closure is checked each step.
@@ -851,7 +853,6 @@ def run_window200(args):
     for _ in range(max(3, args.warmup)):
         sheet.step(DT, want_spray=False)
     torch.cuda.synchronize()
-    sheet.set_step_timing(True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -860,7 +861,18 @@ def run_window200(args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    # The library's step parts in a pass of their own (timing mode reads back
+    # each step's Gauss-Seidel pass count, which waits for the step).
+    sheet.set_step_timing(True)
+    part_steps = min(args.steps, 20)
+    for _ in range(part_steps):
+        sheet.step(DT, want_spray=False)
+    torch.cuda.synchronize()
     parts = sheet.step_parts()
+    sheet.set_step_timing(False)
+    gs = {"most_passes": int(parts["sweep_passes_max"]),
+          "mean_passes_per_layer_step": parts["sweep_local_passes"] / max(parts["sweep_solves"], 1),
+          "sequential_fallbacks": int(parts["sweep_fallbacks"]), "steps": part_steps}
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     e2e_steps = max(10, args.steps // 4)
@@ -877,7 +889,8 @@ def run_window200(args):
             "config": cfgw, "window_steps_per_s": args.steps / (ms / 1000.0),
             "e2e": {"value": res * res * e2e_steps / (ems / 1000.0), "unit": "cell-steps/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 60, "steps": e2e_steps},
-            "gpu_launches": int(parts["launches"])}
+            "gpu_launches": int(parts["launches"]) * args.steps // max(part_steps, 1),
+            "gauss_seidel": gs}
     if not args.no_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle

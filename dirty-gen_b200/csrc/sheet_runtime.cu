@@ -507,6 +507,18 @@ int step_coarse_pair_window(silt_sheet* s, float dt) {
         // third event closes an empty transport interval.
         CK(cudaEventRecord(ev[1], s->st));
         CK(cudaEventRecord(ev[2], s->st));
+        // The Gauss-Seidel passes each layer's last box needed (diagnostics;
+        // timing mode only, as this read waits for the step).
+        silt::window::Job done[2];
+        CK(cudaMemcpyAsync(done, s->d_win_jobs + 2 * slot, sizeof done, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        for (int l = 0; l < 2; ++l) {
+            s->parts.sweep_launches += 1;
+            s->parts.sweep_solves += 1;
+            s->parts.sweep_local_passes += done[l].gs_iters > 0 ? done[l].gs_iters : 0;
+            s->parts.sweep_passes_max = std::max<int64_t>(s->parts.sweep_passes_max, done[l].gs_iters);
+            if (done[l].gs_iters < 0) s->parts.sweep_fallbacks += 1;
+        }
     }
     s->parts.force_launches += 1;
     s->parts.force_cells += 2 * (int64_t)s->n;
@@ -1162,6 +1174,15 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     const unsigned long long launches0 = silt::t_kernel_launches;
     using clock = std::chrono::steady_clock;
     const clock::time_point t0 = clock::now();
+    clock::time_point tp = t0;
+    // Host time per phase (with timing on): the time since the last mark goes
+    // to phase k (the same slots as a batch's, where they apply).
+    auto phase = [&](int k) {
+        if (!s->timing) return;
+        const clock::time_point t = clock::now();
+        s->parts.host_phase_ms[k] += std::chrono::duration<double, std::milli>(t - tp).count();
+        tp = t;
+    };
     std::vector<silt_tire_push> ps;
     silt::fine::StepOut fo;
     int rc;
@@ -1178,16 +1199,20 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         F = closure_job(s, s->pushes);
         CK(s->clos->features({F}, s->net->net, s->st));
     }
+    phase(0);
     rc = step_before_coarse(s, dt, ps, fo);
     if (rc) return rc;
+    phase(2);
     const clock::time_point t2 = clock::now();
     if ((rc = wave_step(s, dt))) return rc;
     rc = s->engine == SILT_ENGINE_WINDOW ? step_coarse_pair_window(s, dt) : step_coarse_pair(s, dt);
     if (rc) return rc;
     if ((rc = open_water_step(s, dt))) return rc;
+    phase(3);
     rc = silt::fine::peel_coarse(s->fine, s, ps, fo);
     if (rc) return rc;
     if ((rc = scour_step(s, dt))) return rc;
+    phase(4);
     {
         // step_tracers (src/fluid_core.rs:6080), then the reach, then the
         // suspended load (:6082-6089).
@@ -1200,6 +1225,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         const silt::tracers::Window w = tracer_window(s, ps);
         CK(silt::tracers::step_suspended(s->tr_run, &w, 1, dt, s->st));
     }
+    phase(5);
     if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
     if (out || n_out) {
@@ -1207,6 +1233,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
         if (rc) return rc;
     }
     if (n_out) *n_out = nev;
+    phase(6);
     s->parts.steps += 1;
     s->parts.launches += (int64_t)(silt::t_kernel_launches - launches0);
     if (s->timing) {

@@ -300,11 +300,12 @@ typedef struct {
      * sequential sweep, tile solves (a tile in one pass) and their local
      * passes in shared memory. */
     int64_t sweep_launches, sweep_passes_max, sweep_fallbacks, sweep_solves, sweep_local_passes;
-    /* Batches: host time per phase of silt_batch_step (ms, summed over the
-     * steps): [0] closure crops and wake entrainment, [1] per-window planning
-     * on the workers, [2] the nested patches' launches, [3] the coarse pair
-     * and open-water drivers, [4] the patches' peel, [5] tracers and reach,
-     * [6] the closure's correction and the books. */
+    /* Host time per phase of a step (ms, summed over the steps; with step
+     * timing on): [0] closure crops and wake entrainment, [1] per-window
+     * planning on a batch's workers, [2] the nested patches (a single sheet:
+     * their planning and launches, with the inflow), [3] the coarse pair and
+     * open-water drivers, [4] the patches' peel (and scour), [5] tracers and
+     * reach, [6] the closure's correction, spray and the books. */
     double host_phase_ms[8];
 } silt_step_parts;
 int silt_set_step_timing(silt_sheet* s, int32_t on);
