@@ -52,9 +52,11 @@ struct Shared {
     int nbox;
     int changed;
     int chg[3];      // Gauss-Seidel pass verdicts, rotating (pass k uses chg[k % 3])
+    int lchg[3];     // wet-body label rounds' verdicts, rotating the same way
     float red_f[NT / 32];
     double red_d[NT / 32];
     double crew_d;   // this CTA's share of a crew-wide sum or maximum, read by the crew
+    int crew_ext[5]; // this CTA's share of the wet extent: count, i0, -i1, j0, j1
     float crew_f;
     int red_i[4][NT / 32];
 };
@@ -140,15 +142,30 @@ __device__ __forceinline__ float block_max_f(Shared& S, float v) {
     return r;
 }
 
+// Every crew CTA's copy of one shared-memory value, combined in rank order:
+// lane r of each warp loads rank r's copy (the loads overlap instead of
+// following one another), then the values are folded through shuffles in rank
+// order, so the result is exactly the one a loop over the ranks gives. Called
+// by every thread after the barrier that published the copies; at most 32
+// CTAs in a crew.
+template <typename T, typename F>
+__device__ __forceinline__ T crew_fold(const T* mine, T init, F combine) {
+    cg::cluster_group crew = cg::this_cluster();
+    const int lane = threadIdx.x & 31, n = crew_size();
+    T got = init;
+    if (lane < n) got = *crew.map_shared_rank(mine, lane);
+    T acc = init;
+    for (int r = 0; r < n; ++r) acc = combine(acc, __shfl_sync(0xffffffffu, got, r));
+    return acc;
+}
+
 // A crew-wide sum of per-thread partials: each CTA reduces its own, then every
 // CTA adds the CTAs' results in rank order (the same value in every CTA).
 __device__ double crew_sum_d(Shared& S, double v) {
     const double part = block_sum_d(S, v);
     if (threadIdx.x == 0) S.crew_d = part;
     crew_sync();
-    cg::cluster_group crew = cg::this_cluster();
-    double tot = 0.0;
-    for (int r = 0; r < crew_size(); ++r) tot += *crew.map_shared_rank(&S.crew_d, r);
+    const double tot = crew_fold(&S.crew_d, 0.0, [](double a, double b) { return a + b; });
     crew_sync();  // every CTA has read the shares before they are reused
     return tot;
 }
@@ -158,9 +175,7 @@ __device__ float crew_max_f(Shared& S, float v) {
     const float part = block_max_f(S, v);
     if (threadIdx.x == 0) S.crew_f = part;
     crew_sync();
-    cg::cluster_group crew = cg::this_cluster();
-    float m = 0.0f;
-    for (int r = 0; r < crew_size(); ++r) m = fmaxf(m, *crew.map_shared_rank(&S.crew_f, r));
+    const float m = crew_fold(&S.crew_f, 0.0f, [](float a, float b) { return fmaxf(a, b); });
     crew_sync();
     return m;
 }
@@ -191,6 +206,35 @@ __device__ void block_reduce4(Shared& S, int v[4], const int op[4]) {
     for (int q = 0; q < 4; ++q) v[q] = S.red_i[q][0];
     __syncthreads();
 }
+
+// The crew-wide wet sum and wet extent of one pass: ws summed as crew_sum_d
+// does; ext = {wet cells, min i, -max i, min j, max j} over the crew, in the
+// same barriers.
+__device__ double crew_sum_extent(Shared& S, double v, int ext[5]) {
+    const double part = block_sum_d(S, v);
+    int a[4] = {ext[0], ext[1], ext[2], ext[3]};
+    const int op[4] = {0, 1, 1, 1};
+    block_reduce4(S, a, op);
+    int b[4] = {ext[4], 0, 0, 0};
+    const int op2[4] = {2, 2, 2, 2};
+    block_reduce4(S, b, op2);
+    if (threadIdx.x == 0) {
+        S.crew_d = part;
+        for (int q = 0; q < 4; ++q) S.crew_ext[q] = a[q];
+        S.crew_ext[4] = b[0];
+    }
+    crew_sync();
+    const double tot = crew_fold(&S.crew_d, 0.0, [](double a, double b) { return a + b; });
+    auto mn = [](int a, int b) { return min(a, b); };
+    ext[0] = crew_fold(&S.crew_ext[0], 0, [](int a, int b) { return a + b; });
+    ext[1] = crew_fold(&S.crew_ext[1], 0x7fffffff, mn);
+    ext[2] = crew_fold(&S.crew_ext[2], 0x7fffffff, mn);
+    ext[3] = crew_fold(&S.crew_ext[3], 0x7fffffff, mn);
+    ext[4] = crew_fold(&S.crew_ext[4], -1, [](int a, int b) { return max(a, b); });
+    crew_sync();  // every CTA has read the shares before they are reused
+    return tot;
+}
+
 
 // Five taps along one axis, clamped at the grid edge. Cells at least 2 from
 // the edge start from the first product (accum5), others from 0.0
@@ -702,8 +746,7 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
             }
         })
         crew_sync();
-        int any = 0;
-        for (int r = 0; r < crew_size(); ++r) any |= crew.map_shared_rank(S.chg, r)[slot];
+        const int any = crew_fold(&S.chg[slot], 0, [](int a, int b) { return a | b; });
         if (!any) break;
     }
     if (passes < GS_MAX_PASSES) return passes + 1;
@@ -1005,29 +1048,67 @@ __device__ void set_whole(Shared& S, int x0, int x1, int y0, int y1) {
 // sheet_work_boxes (src/fluid_core.rs:1325-1447). Wet bodies are labelled in
 // the f2 plane (as ints) by hooking and pointer jumping; a body's root is its
 // first wet cell in raster order, the order the reference's run merge keeps.
-__device__ void cta_wet_boxes(Shared& S, const Job& J) {
+// The wet-body labels of sheet_work_boxes (src/fluid_core.rs:1378-1457) over
+// the wet extent, by the whole crew, into the plane f2: every wet cell ends
+// holding its body's smallest index (its first raster cell). Hook and jump:
+// each round lowers the label of the larger of two neighbours' labels to the
+// smaller, then moves every cell one step up its chain. Labels only fall and
+// stay inside the body, so the rounds end at that fixed point in O(log)
+// rounds without walking long chains. Nothing to label when no cell is wet or
+// every cell of the extent is (cta_wet_boxes then takes the whole box).
+__device__ void crew_label_bodies(Shared& S, const Job& J, const int ext[5]) {
     const int res = J.res;
     const float eps = J.eps;
-    int v[4] = {0, res, 1, res};
-    int vj1 = -1;
-    CTA_RECT(0, res - 1, 0, res - 1, {
-        if (J.h[g] > eps) {
-            v[0] += 1;
-            v[1] = min(v[1], i);
-            v[2] = min(v[2], -i);
-            v[3] = min(v[3], j);
-            vj1 = max(vj1, j);
-        }
-    })
-    {
-        const int op[4] = {0, 1, 1, 1};
-        block_reduce4(S, v, op);
-        int t[4] = {vj1, 0, 0, 0};
-        const int op2[4] = {2, 2, 2, 2};
-        block_reduce4(S, t, op2);
-        vj1 = t[0];
+    const int wet = ext[0], i0 = ext[1], i1 = -ext[2], j0 = ext[3], j1 = ext[4];
+    if (wet == 0 || wet == (i1 - i0 + 1) * (j1 - j0 + 1)) return;
+    int* L = reinterpret_cast<int*>(J.f2);
+    CLU_RECT(i0, i1, j0, j1, { L[g] = J.h[g] > eps ? g : -1; })
+    if (threadIdx.x == 0) S.lchg[0] = S.lchg[1] = S.lchg[2] = 0;
+    crew_sync();
+    for (int round = 0; round < 4096; ++round) {
+        const int slot = round % 3;
+        // Round k sets lchg[k % 3] and clears lchg[(k + 1) % 3], which the
+        // crew last read in round k - 2, two barriers ago.
+        if (threadIdx.x == 0) S.lchg[(slot + 1) % 3] = 0;
+        CLU_RECT(i0, i1, j0, j1, {
+            const int a = L[g];
+            if (a >= 0) {
+                if (i < i1) {
+                    const int c = L[g + 1];
+                    if (c >= 0 && a != c) {
+                        atomicMin(&L[max(a, c)], min(a, c));
+                        S.lchg[slot] = 1;
+                    }
+                }
+                if (j < j1) {
+                    const int c = L[g + res];
+                    if (c >= 0 && a != c) {
+                        atomicMin(&L[max(a, c)], min(a, c));
+                        S.lchg[slot] = 1;
+                    }
+                }
+            }
+        })
+        crew_sync();
+        CLU_RECT(i0, i1, j0, j1, {
+            const int a = L[g];
+            if (a >= 0) {
+                const int c = L[a];
+                if (c != a) {
+                    L[g] = c;
+                    S.lchg[slot] = 1;
+                }
+            }
+        })
+        crew_sync();
+        if (!crew_fold(&S.lchg[slot], 0, [](int x, int y) { return x | y; })) break;
     }
-    const int wet = v[0], i0 = v[1], i1 = -v[2], j0 = v[3], j1 = vj1;
+}
+
+// `ext`: the crew's wet extent of the layer (crew_sum_extent).
+__device__ void cta_wet_boxes(Shared& S, const Job& J, const int ext[5]) {
+    const int res = J.res;
+    const int wet = ext[0], i0 = ext[1], i1 = -ext[2], j0 = ext[3], j1 = ext[4];
     if (wet == 0) {
         if (threadIdx.x == 0) S.nbox = 0;
         __syncthreads();
@@ -1038,51 +1119,9 @@ __device__ void cta_wet_boxes(Shared& S, const Job& J) {
         set_whole(S, x0, x1, y0, y1);
         return;
     }
+    // The crew has labelled every wet cell of the box with its body's first
+    // raster cell (crew_label_bodies).
     int* L = reinterpret_cast<int*>(J.f2);
-    CTA_RECT(i0, i1, j0, j1, { L[g] = J.h[g] > eps ? g : -1; })
-    __syncthreads();
-    // Hook and jump: each round lowers the label of the larger of two
-    // neighbours' labels to the smaller, then moves every cell one step up its
-    // chain. Labels only fall and stay inside the body; when a round changes
-    // nothing, every cell holds its body's smallest index (its first raster
-    // cell), in O(log) rounds and without walking long chains.
-    for (int round = 0; round < 4096; ++round) {
-        if (threadIdx.x == 0) S.changed = 0;
-        __syncthreads();
-        CTA_RECT(i0, i1, j0, j1, {
-            const int a = L[g];
-            if (a >= 0) {
-                if (i < i1) {
-                    const int c = L[g + 1];
-                    if (c >= 0 && a != c) {
-                        atomicMin(&L[max(a, c)], min(a, c));
-                        S.changed = 1;
-                    }
-                }
-                if (j < j1) {
-                    const int c = L[g + res];
-                    if (c >= 0 && a != c) {
-                        atomicMin(&L[max(a, c)], min(a, c));
-                        S.changed = 1;
-                    }
-                }
-            }
-        })
-        __syncthreads();
-        CTA_RECT(i0, i1, j0, j1, {
-            const int a = L[g];
-            if (a >= 0) {
-                const int c = L[a];
-                if (c != a) {
-                    L[g] = c;
-                    S.changed = 1;
-                }
-            }
-        })
-        __syncthreads();
-        if (!S.changed) break;
-        __syncthreads();
-    }
     // Roots in raster order: count per row, scan, then number them.
     const int rows = j1 - j0 + 1;
     for (int r = threadIdx.x; r < rows; r += NT) {
@@ -1234,11 +1273,19 @@ __device__ __forceinline__ int window_body(Shared& S, const Job& J) {
     if (J.solid) cta_displace(J);
     // wet_sum early out (src/fluid_core.rs:1306-1319, :840-844), over the crew.
     double ws = 0.0;
+    int ext[5] = {0, res, 1, res, -1};  // wet cells, min i, -max i, min j, max j
     CLU_RECT(0, res - 1, 0, res - 1, {
         float hv = J.h[g];
-        if (hv > eps) ws += (double)hv;
+        if (hv > eps) {
+            ws += (double)hv;
+            ext[0] += 1;
+            ext[1] = min(ext[1], i);
+            ext[2] = min(ext[2], -i);
+            ext[3] = min(ext[3], j);
+            ext[4] = max(ext[4], j);
+        }
     })
-    ws = crew_sum_d(S, ws);
+    ws = crew_sum_extent(S, ws, ext);
     if (!(ws > (double)eps)) {
         cta_ledger(S, J);
         return 0;
@@ -1250,10 +1297,12 @@ __device__ __forceinline__ int window_body(Shared& S, const Job& J) {
     // Work boxes on rank 0 (the wet-body labels use a global plane; the awake
     // scan is shared by the crew), then every other CTA copies them from its
     // shared memory.
-    if (fine_open || awake)
+    if (fine_open || awake) {
         cta_awake_boxes(S, J);
-    else if (crew_rank() == 0)
-        cta_wet_boxes(S, J);
+    } else {
+        crew_label_bodies(S, J, ext);
+        if (crew_rank() == 0) cta_wet_boxes(S, J, ext);
+    }
     crew_sync();
     if (crew_rank() != 0) {
         const Shared* S0 = cg::this_cluster().map_shared_rank(&S, 0);
