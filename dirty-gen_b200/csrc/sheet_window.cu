@@ -1052,9 +1052,11 @@ __device__ void set_whole(Shared& S, int x0, int x1, int y0, int y1) {
 // the wet extent, by the whole crew, into the plane f2: every wet cell ends
 // holding its body's smallest index (its first raster cell). Hook and jump:
 // each round lowers the label of the larger of two neighbours' labels to the
-// smaller, then moves every cell one step up its chain. Labels only fall and
-// stay inside the body, so the rounds end at that fixed point in O(log)
-// rounds without walking long chains. Nothing to label when no cell is wet or
+// smaller root (each cell walks to its root first), then points every cell
+// at its root. Labels only fall and stay inside the body, so the rounds end
+// at that fixed point, in a few rounds. A run's cells start with the same
+// label, which only shortens the rounds: the fixed point is the same. Nothing
+// to label when no cell is wet or
 // every cell of the extent is (cta_wet_boxes then takes the whole box).
 __device__ void crew_label_bodies(Shared& S, const Job& J, const int ext[5]) {
     const int res = J.res;
@@ -1062,40 +1064,76 @@ __device__ void crew_label_bodies(Shared& S, const Job& J, const int ext[5]) {
     const int wet = ext[0], i0 = ext[1], i1 = -ext[2], j0 = ext[3], j1 = ext[4];
     if (wet == 0 || wet == (i1 - i0 + 1) * (j1 - j0 + 1)) return;
     int* L = reinterpret_cast<int*>(J.f2);
-    CLU_RECT(i0, i1, j0, j1, { L[g] = J.h[g] > eps ? g : -1; })
+    // Start from runs: a wet cell takes the index of the first cell of its
+    // horizontal run within its warp's 32-cell chunk (a ballot finds it), so
+    // the rounds only join runs.
+    {
+        const int ch = (i1 - i0 + 32) >> 5;
+        const int items = (j1 - j0 + 1) * ch;
+        const int lane = (int)(threadIdx.x & 31);
+        for (int it = crew_rank() * (NT / 32) + (int)(threadIdx.x >> 5); it < items; it += crew_size() * (NT / 32)) {
+            const int r = it / ch;
+            const int j = j0 + r;
+            const int ib = i0 + (it - r * ch) * 32;
+            const int i = ib + lane;
+            const bool in = i <= i1;
+            const int g = j * res + i;
+            const bool wet = in && J.h[g] > eps;
+            const unsigned m = __ballot_sync(0xffffffffu, wet);
+            // The run's first lane: the lowest lane at or below this one such
+            // that every lane from it up to this one is wet.
+            const unsigned dry_below = ~m & ((lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1u));
+            const int first = dry_below ? (32 - __clz(dry_below)) : 0;
+            if (in) L[g] = wet ? j * res + ib + first : -1;
+        }
+    }
     if (threadIdx.x == 0) S.lchg[0] = S.lchg[1] = S.lchg[2] = 0;
     crew_sync();
+    // A cell's root: follow the labels down (they only fall, so the walk
+    // ends; the cap only bounds a walk, the rounds still reach the fixed point).
+    auto root = [&](int x) {
+        for (int k = 0; k < 4096; ++k) {
+            const int y = ((volatile int*)L)[x];
+            if (y == x) break;
+            x = y;
+        }
+        return x;
+    };
     for (int round = 0; round < 4096; ++round) {
         const int slot = round % 3;
         // Round k sets lchg[k % 3] and clears lchg[(k + 1) % 3], which the
         // crew last read in round k - 2, two barriers ago.
         if (threadIdx.x == 0) S.lchg[(slot + 1) % 3] = 0;
+        // Hook: two wet neighbours with different roots hang the larger root
+        // under the smaller.
         CLU_RECT(i0, i1, j0, j1, {
             const int a = L[g];
             if (a >= 0) {
-                if (i < i1) {
-                    const int c = L[g + 1];
-                    if (c >= 0 && a != c) {
-                        atomicMin(&L[max(a, c)], min(a, c));
+                const int ra = root(a);
+                if (i < i1 && L[g + 1] >= 0) {
+                    const int rc = root(L[g + 1]);
+                    if (rc != ra) {
+                        atomicMin(&L[max(ra, rc)], min(ra, rc));
                         S.lchg[slot] = 1;
                     }
                 }
-                if (j < j1) {
-                    const int c = L[g + res];
-                    if (c >= 0 && a != c) {
-                        atomicMin(&L[max(a, c)], min(a, c));
+                if (j < j1 && L[g + res] >= 0) {
+                    const int rc = root(L[g + res]);
+                    if (rc != ra) {
+                        atomicMin(&L[max(ra, rc)], min(ra, rc));
                         S.lchg[slot] = 1;
                     }
                 }
             }
         })
         crew_sync();
+        // Compress: every cell points at its root.
         CLU_RECT(i0, i1, j0, j1, {
             const int a = L[g];
             if (a >= 0) {
-                const int c = L[a];
-                if (c != a) {
-                    L[g] = c;
+                const int r = root(a);
+                if (r != a) {
+                    L[g] = r;
                     S.lchg[slot] = 1;
                 }
             }
