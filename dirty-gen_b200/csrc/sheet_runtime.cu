@@ -164,6 +164,21 @@ struct silt_sheet {
     silt::tracers::Planes tr;
     silt::tracers::Runner tr_run;
     bool tr_rescan = true;  // the tracer planes were rewritten (attach, move): scan the silt span once
+    // What the host knows of the tracers' idleness from the device's reports
+    // (silt::tracers::step_suspended), so that silt_step can skip tracer
+    // steps that would change nothing.
+    struct TracerIdle {
+        static constexpr int SLOTS = 8;
+        unsigned int* d_flag = nullptr;   // SLOTS report words
+        unsigned int* h_flag = nullptr;   // their pinned mirror
+        cudaEvent_t ev[SLOTS] = {};
+        long long step_of[SLOTS] = {-1, -1, -1, -1, -1, -1, -1, -1};  // the step a slot reports (-1: none)
+        int next = 0;
+        long long steps = 0;          // steps counted at their start
+        long long last_trigger = 0;   // the last step with a wake, rewritten planes or a tracer switch
+        long long idle_through = -1;  // the tracers are known idle after this step
+    } tri;
+    bool tr_poke = false;  // something outside a step changed what the tracers would do
     float center[2] = {0.0f, 0.0f};  // the chase point (set_center / recenter)
     bool reach_on = false;           // FluidCore::set_river_reach
     silt_river_reach reach;
@@ -253,6 +268,54 @@ silt::tracers::Window tracer_window(silt_sheet* s, const std::vector<silt_tire_p
     // A river inlet carrying a load writes its rows' suspended solids.
     w.sup_all = (s->reach_on && s->reach.inlet_turbidity != 0.0f) ? 1 : 0;
     return w;
+}
+
+// At a step's start: whether its tracer kernels can be skipped. They can when
+// the tracers are known idle after the previous step (a device report of an
+// earlier step said idle, and no step since had a trigger) and this step has
+// no trigger: without a wake the tracer step does not run at all
+// (src/fluid_core.rs:6213-6218), the suspended pass finds no load, and an
+// idle state stays idle. Triggers: tire pushes, a surface drive, rewritten
+// planes, the tracer switch. Reports arrive through pinned memory and are
+// only polled, so the host never waits for one.
+bool tracers_skip(silt_sheet* s, bool wake) {
+    silt_sheet::TracerIdle& I = s->tri;
+    if (!I.d_flag) return false;
+    const long long n = ++I.steps;
+    for (int k = 0; k < silt_sheet::TracerIdle::SLOTS; ++k) {
+        if (I.step_of[k] < 0) continue;
+        const cudaError_t q = cudaEventQuery(I.ev[k]);
+        if (q == cudaErrorNotReady) continue;
+        if (q == cudaSuccess && I.h_flag[k] && I.step_of[k] >= I.last_trigger) I.idle_through = n - 1;
+        if (q != cudaSuccess) cudaGetLastError();
+        I.step_of[k] = -1;
+    }
+    const bool trigger = wake || s->tr_rescan || s->tr_poke;
+    s->tr_poke = false;
+    if (trigger) I.last_trigger = n;
+    if (!trigger && I.idle_through == n - 1) {
+        I.idle_through = n;
+        return true;
+    }
+    return false;
+}
+
+// The report word of this step's tracer launches (nullptr: no report).
+unsigned int* tracers_report_word(silt_sheet* s) {
+    silt_sheet::TracerIdle& I = s->tri;
+    return I.d_flag ? I.d_flag + I.next : nullptr;
+}
+
+// After this step's tracer launches: bring the report back.
+int tracers_report(silt_sheet* s) {
+    silt_sheet::TracerIdle& I = s->tri;
+    if (!I.d_flag) return SILT_OK;
+    const int k = I.next;
+    I.next = (I.next + 1) % silt_sheet::TracerIdle::SLOTS;
+    CK(cudaMemcpyAsync(I.h_flag + k, I.d_flag + k, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaEventRecord(I.ev[k], s->st));
+    I.step_of[k] = I.steps;
+    return SILT_OK;
 }
 
 // Host plan of one sheet's coarse pair for one step: how many substeps to
@@ -672,6 +735,11 @@ int silt_sheet_create(const silt_cfg* cfg, silt_sheet** out) {
     }
     e = cudaMalloc(&s->tr_mem, silt::tracers::plane_bytes(s->res));
     if (e == cudaSuccess) e = silt::tracers::attach(s->tr, s->tr_mem, s->res, silt::fine::books(s->fine) + 7, s->st);
+    if (e == cudaSuccess) e = cudaMalloc(&s->tri.d_flag, silt_sheet::TracerIdle::SLOTS * sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&s->tri.h_flag, silt_sheet::TracerIdle::SLOTS * sizeof(unsigned int));
+    for (int k = 0; k < silt_sheet::TracerIdle::SLOTS && e == cudaSuccess; ++k)
+        e = cudaEventCreateWithFlags(&s->tri.ev[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         silt_sheet_destroy(s);
         return e == cudaErrorMemoryAllocation ? SILT_ENOMEM : fail_cuda(e, "allocate tracers");
@@ -698,6 +766,10 @@ int silt_sheet_destroy(silt_sheet* s) {
     cudaFree(s->d_reach_bank);
     s->tr_run.release();
     cudaFree(s->tr_mem);
+    cudaFree(s->tri.d_flag);
+    if (s->tri.h_flag) cudaFreeHost(s->tri.h_flag);
+    for (int k = 0; k < silt_sheet::TracerIdle::SLOTS; ++k)
+        if (s->tri.ev[k]) cudaEventDestroy(s->tri.ev[k]);
     silt::fine::destroy(s->fine);
     for (int l = 0; l < 2; ++l)
         for (int b = 0; b < 2; ++b) {
@@ -1186,6 +1258,7 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     std::vector<silt_tire_push> ps;
     silt::fine::StepOut fo;
     int rc;
+    const bool skip_tracers = tracers_skip(s, !s->pushes.empty() || s->wave_on || s->reach_on);
     // Lift from the column the tire rolls into, before the sheet shoves it
     // (entrain_wake, src/fluid_core.rs:6051-6053).
     if (s->turbidity && !s->pushes.empty()) {
@@ -1213,18 +1286,23 @@ int silt_step(silt_sheet* s, float dt, silt_spray_event* out, int32_t cap, int32
     if (rc) return rc;
     if ((rc = scour_step(s, dt))) return rc;
     phase(4);
-    {
+    if (!skip_tracers) {
         // step_tracers (src/fluid_core.rs:6080), then the reach, then the
         // suspended load (:6082-6089).
-        const silt::tracers::Window w = tracer_window(s, ps);
+        silt::tracers::Window w = tracer_window(s, ps);
+        w.susp_on = s->turbidity ? 1 : 0;
+        w.idle_out = tracers_report_word(s);
         CK(silt::tracers::step_tracers(s->tr_run, &w, 1, dt, s->st));
         s->tr_rescan = false;
     }
     if ((rc = reach_step(s))) return rc;
-    if (s->turbidity) {
-        const silt::tracers::Window w = tracer_window(s, ps);
+    if (s->turbidity && !skip_tracers) {
+        silt::tracers::Window w = tracer_window(s, ps);
+        w.susp_on = 1;
+        w.idle_out = tracers_report_word(s);
         CK(silt::tracers::step_suspended(s->tr_run, &w, 1, dt, s->st));
     }
+    if (!skip_tracers && (rc = tracers_report(s))) return rc;
     phase(5);
     if (net_on && (rc = closure_correct(s, F))) return rc;
     int32_t nev = 0;
@@ -1541,6 +1619,7 @@ int silt_get_hydro_load(silt_sheet* s, silt_hydro_load* out) {
 int silt_set_turbidity_enabled(silt_sheet* s, int32_t on) {
     if (!s) return fail_arg("handle");
     s->turbidity = on != 0;
+    s->tr_poke = true;
     return SILT_OK;
 }
 
@@ -1817,6 +1896,7 @@ int silt_write_plane(silt_sheet* s, int32_t which, const float* host) {
     if (!p) return fail_arg("plane index");
     int rc = flush_cut(s);
     if (rc) return rc;
+    s->tr_poke = true;  // a tracer plane, or the water they ride on, changed outside a step
     CK(cudaMemcpyAsync(p, host, s->n * 4, cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
     if (which >= 2 && which <= 5) {
@@ -2537,7 +2617,10 @@ int silt_batch_step(silt_batch* b, float dt) {
         tw.reserve(n);
         for (int w = 0; w < n; ++w) tw.push_back(tracer_window(b->sheets[w], ps[w]));
         CK(silt::tracers::step_tracers(b->tr_run, tw.data(), n, dt, b->st));
-        for (silt_sheet* s : b->sheets) s->tr_rescan = false;
+        for (silt_sheet* s : b->sheets) {
+            s->tr_rescan = false;
+            s->tr_poke = true;  // stepped by the batch, which sends no idle reports
+        }
         for (silt_sheet* s : b->sheets)
             if ((rc = reach_step(s))) return rc;
         std::vector<silt::tracers::Window> sw;

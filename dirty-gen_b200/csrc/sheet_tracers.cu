@@ -1180,6 +1180,20 @@ __global__ void k_susp_give(const Job* jobs) {
     block_count(capped, &st->capped);
 }
 
+// The idle report of every job with a report word: `last` 0 = the jobs
+// without a suspended pass (after step_tracers), 1 = the rest (after
+// step_suspended).
+__global__ void k_idle(const Job* jobs, int last) {
+    ::silt::dep_wait();
+    const Job& J = jobs[blockIdx.y];
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !J.idle_out || (J.susp_on != 0) != (last != 0)) return;
+    const State* st = J.T.st;
+    const Ctl* c = reinterpret_cast<const Ctl*>(st + 1);
+    const bool idle = st->live_foam == 0u && box_empty(st->tspan) && !J.rescan &&
+                      (!J.susp_on || box_empty(c->ssup_next));
+    *J.idle_out = idle ? 1u : 0u;
+}
+
 __global__ void k_reset_live(uint8_t* mark, State* st, int res, size_t n) {
     ::silt::dep_wait();
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x)
@@ -1304,6 +1318,8 @@ cudaError_t upload(Runner& R, const Window* w, int n, float dt, float foam_decay
         J.wake = wake ? 1 : 0;
         J.rescan = w[k].rescan;
         J.sup_all = w[k].sup_all;
+        J.susp_on = w[k].susp_on;
+        J.idle_out = w[k].idle_out;
         push_box(w[k].S, w[k].push, w[k].npush, J.pbox);
         entrain_box(w[k].S, w[k].push, w[k].npush, J.ebox);
         J.dt = dt;
@@ -1400,6 +1416,9 @@ cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream
     LAUNCH(k_settle, bx, jobs);
     LAUNCH(k_spawn, bx, jobs);
     LAUNCH(k_clear_sync, bx, jobs);
+    bool report = false;
+    for (int k = 0; k < n; ++k) report = report || (w[k].idle_out && !w[k].susp_on);
+    if (report) LAUNCH(k_idle, 1, jobs, 0);
     return cudaSuccess;
 }
 
@@ -1414,6 +1433,9 @@ cudaError_t step_suspended(Runner& R, const Window* w, int n, float dt, cudaStre
     LAUNCH(k_susp_settle, bx, jobs);
     LAUNCH(k_susp_take, bx, jobs);
     LAUNCH(k_susp_give, bx, jobs);
+    bool report = false;
+    for (int k = 0; k < n; ++k) report = report || w[k].idle_out;
+    if (report) LAUNCH(k_idle, 1, jobs, 1);
     return cudaSuccess;
 }
 

@@ -60,6 +60,8 @@ struct Job {
     int pbox[4];                 // the tires' reach boxes (tracer_visit_box's tire part; empty when none)
     int ebox[4];                 // entrain_wake's cells: the union of the tires' wake boxes (empty when none)
     int rescan;                  // the planes were rewritten: scan the silt span before the step
+    int susp_on;                 // the suspended load is stepped (turbidity on)
+    unsigned int* idle_out;      // device word: after the step, 1 when the tracers have nothing left to do
     int sup_all;                 // something outside the tracer kernels wrote the suspended load (a river inlet)
     float dt, foam_decay, silt_keep;
 };
@@ -89,6 +91,8 @@ struct Window {
     int npush;
     int rescan = 0;   // the planes were rewritten since the last tracer step (attach, window move)
     int sup_all = 0;  // a river inlet writes the suspended load outside the tracer kernels
+    int susp_on = 0;  // turbidity on: step_suspended follows step_tracers this step
+    unsigned int* idle_out = nullptr;  // device word for the idle report (see step_tracers)
 };
 
 size_t plane_bytes(int res);  // device bytes of one window's tracer planes
@@ -97,8 +101,14 @@ cudaError_t attach(Planes& T, void* mem, int res, double* books, cudaStream_t st
 // entrain_wake (src/fluid_core.rs:8758-8815) on every window, before the step.
 cudaError_t entrain(Runner& R, const Window* w, int n, float dt, cudaStream_t st);
 // step_tracers (src/fluid_core.rs:6210-6237) after the coarse pair and its peel.
+// A window without turbidity then reports whether it is idle (below).
 cudaError_t step_tracers(Runner& R, const Window* w, int n, float dt, cudaStream_t st);
-// step_suspended (src/fluid_core.rs:8750-8756 with advect_suspended :8817-9002).
+// step_suspended (src/fluid_core.rs:8750-8756 with advect_suspended :8817-9002),
+// then every window reports whether it is idle: no live foam, no silt above
+// 1e-8 and no suspended load. An idle window whose next step has no wake (no
+// tire, no surface drive) and no rewritten planes stays idle through that
+// step, whose tracer kernels would change nothing, so the caller may skip
+// them; a window stays idle until such a trigger.
 cudaError_t step_suspended(Runner& R, const Window* w, int n, float dt, cudaStream_t st);
 // Clears the foam-live set (reset_tracer_indices, src/fluid_core.rs:9228-9233) after a window move.
 cudaError_t reset_indices(Planes& T, int res, cudaStream_t st);

@@ -249,3 +249,37 @@ def test_wheel_cloud_settles_and_ledgers_close():
     assert abs(led["suspended_m3"] + led["settled_suspended_m3"] + led["frozen_suspended_m3"]
                - led["entrained_m3"]) <= 1e-6
     assert abs(led["turbid_m3"] + led["turbid_settled_m3"] + led["frozen_turbid_m3"] - led["stirred_m3"]) <= 1e-6
+
+
+def test_idle_tracer_steps_are_skipped_and_change_nothing():
+    """With nothing to carry (no foam, no silt above 1e-8, no suspended load)
+    and no tire or surface drive, a tracer step changes nothing; the library
+    learns that from the device's report of an earlier step and then skips
+    those launches until a trigger. The 200 window without tires goes idle;
+    tires then wake the tracers again; the oracle runs every step throughout."""
+    dt = 1.0 / 120.0
+    sc = S.window200()
+    ref, dev = Pair(), G.Sheet()
+    for c in (ref, dev):
+        S.seed_core(c, sc)
+    for _ in range(12):
+        for c in (ref, dev):
+            c.step(dt)
+    dev.set_step_timing(True)
+    for _ in range(6):
+        for c in (ref, dev):
+            c.step(dt)
+    idle = dev.step_parts()
+    dev.set_step_timing(False)
+    push = dict(x=0.15, z=0.2, forward_x=0.0, forward_z=1.0, radius=0.38, width=0.28, speed=8.0, slip=1.2)
+    dev.set_step_timing(True)
+    for _ in range(6):
+        for c in (ref, dev):
+            c.push_tire(**push)
+            c.step(dt)
+    busy = dev.step_parts()
+    dev.set_step_timing(False)
+    ref.check(dev)
+    assert float(dev.get("foam").max()) > 0.0
+    # The idle steps launched only the window engine (and no tracer kernel).
+    assert idle["launches"] / 6 < busy["launches"] / 6 - 8, (idle["launches"], busy["launches"])
