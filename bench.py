@@ -778,6 +778,10 @@ def run_batch(args):
                 "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * n_tires,
                         "d2h_bytes_per_step": 40 * len(wins), "steps": e2e_steps},
                 "gpu_launches": int(parts["launches"]), "kernels": kernels, "launch_settings": batch.tune(),
+                "confinement": {"form": "gauss-seidel sweep (step_pair)",
+                                "most_fixed_point_passes": int(parts["sweep_passes_max"] * part_steps / args.steps),
+                                "tile_solves_per_launch": parts["sweep_solves"] / max(parts["sweep_launches"], 1),
+                                "local_passes_per_solve": parts["sweep_local_passes"] / max(parts["sweep_solves"], 1)},
                 "clocks": summarise_clocks(clock_lines),
                 "host_submit_ms_per_step": host_ms,
                 "host_ms_per_step": {"batch_step": parts["host_step_ms"] / args.steps,

@@ -61,8 +61,8 @@ struct SweepState {
     unsigned int fallbacks;   // launches that ran the sequential sweep after the pass limit
     unsigned int launches;    // sweep launches
     unsigned int epoch;       // launches ever (never reset): the base of the tiles' change stamps
-    unsigned int solves;      // tile solves (a tile in a pass), all launches
-    unsigned int local_passes;  // local passes of those solves, all launches
+    unsigned int solves;      // tile solves (a tile in a pass) since step timing was last set
+    unsigned int local_passes;  // local passes of those solves
 };
 
 // Active-tile bookkeeping of the grid engine, per layer and ping-pong buffer,

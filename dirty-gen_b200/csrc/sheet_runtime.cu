@@ -1965,6 +1965,7 @@ int silt_set_step_timing(silt_sheet* s, int32_t on) {
     if (s->tile_mem) {
         CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, s->st));
         CK(cudaMemsetAsync(&s->sweep_state()->passes_max, 0, 3 * sizeof(unsigned int), s->st));
+        CK(cudaMemsetAsync(&s->sweep_state()->solves, 0, 2 * sizeof(unsigned int), s->st));
     }
     for (cudaEvent_t e : s->ev_used) s->ev_pool.push_back(e);
     s->ev_used.clear();
@@ -2725,6 +2726,7 @@ int silt_batch_set_timing(silt_batch* b, int32_t on) {
         if (s->tile_mem) {
             CK(cudaMemsetAsync(s->d_u32 + 4, 0, 16, b->st));
             CK(cudaMemsetAsync(&s->sweep_state()->passes_max, 0, 3 * sizeof(unsigned int), b->st));
+            CK(cudaMemsetAsync(&s->sweep_state()->solves, 0, 2 * sizeof(unsigned int), b->st));
         }
     return SILT_OK;
 }
