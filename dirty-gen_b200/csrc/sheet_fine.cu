@@ -1558,6 +1558,12 @@ int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, doubl
     return SILT_OK;
 }
 
+int books_enqueue(Patches& P, silt_sheet* s) {
+    Impl& M = I(P);
+    FCK(cudaMemcpyAsync(M.h_books, M.d_books, 16 * sizeof(double), cudaMemcpyDeviceToHost, view_of(s).st));
+    return SILT_OK;
+}
+
 const double* books_host(Patches& P) { return I(P).h_books; }
 
 int debug_patch(Patches& P, silt_sheet* s, const std::vector<silt_tire_push>& ps, int patch, float* host,

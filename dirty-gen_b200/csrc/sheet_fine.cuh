@@ -109,7 +109,11 @@ int collect_spray(Patches& P, silt_sheet* s, const StepOut& out, silt_spray_even
 // FP64 books kept on the device: spray volume and parked (off-window) water and slurry.
 int ledger_parts(Patches& P, silt_sheet* s, double* spray, double* park_w, double* park_s, double* cut = nullptr,
                  double* reach = nullptr, double* eroded = nullptr, double* round = nullptr);
-// The host copy of all 16 books as the last ledger_parts read them.
+// Queues the copy of all 16 books to their host copy on the sheet's stream
+// without waiting: books_host holds them once the stream has reached it.
+int books_enqueue(Patches& P, silt_sheet* s);
+// The host copy of all 16 books as the last ledger_parts (or books_enqueue,
+// after a wait on the stream) brought them.
 const double* books_host(Patches& P);
 // Device address of the books: [0] spray, [1] parked water, [2] parked slurry,
 // [3] dry cut, [4] river reach bank, [5] bed scoured into the slurry (m^3, FP64).

@@ -425,6 +425,21 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0, bo
         int changed = 0;
         region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             if (WT[s] == 0.0f) return;
+            if (!EDGE) {
+                // Interior tile: no stencil index is clamped.
+                float du, dv, nu_ = GU[s], nv_ = GV[s];
+                if (conf_kick_inner(P.div_two, P.dt, P.vort, SweepRead{FU, PU, GU, s, FW},
+                                    SweepRead{FV, PV, GV, s, FW}, du, dv)) {
+                    nu_ = GU[s] + du;
+                    nv_ = GV[s] + dv;
+                }
+                if (__float_as_uint(nu_) != __float_as_uint(FU[s]) || __float_as_uint(nv_) != __float_as_uint(FV[s])) {
+                    FU[s] = nu_;
+                    FV[s] = nv_;
+                    changed = 1;
+                }
+                return;
+            }
             auto at = [&](int a, int b) { return (b - oy) * FW + (a - ox); };
             auto before = [&](int a, int b) { return b < gy || (b == gy && a < gx); };
             auto uu = [&](int a, int b) {

@@ -125,4 +125,49 @@ __device__ __forceinline__ bool conf_kick(int i, int j, int res, const FixedDiv&
     return finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f;
 }
 
+// What one cell of the Gauss-Seidel sweep reads at offset (DX, DY) from it
+// (force_gravity_open's raster order, src/fluid_core.rs:2234-2260): its own
+// post-gravity value at (0, 0), the current iterate of a cell before it, the
+// starting value of a cell after it. The offsets are compile-time constants,
+// so each read is one load at a fixed distance from the cell.
+struct SweepRead {
+    const float* cur;    // current iterate
+    const float* start;  // starting values
+    const float* own;    // post-gravity values
+    int s;               // the cell's index
+    int stride;          // the row stride
+    template <int DX, int DY>
+    __device__ __forceinline__ float at() const {
+        if constexpr (DX == 0 && DY == 0)
+            return own[s];
+        else if constexpr (DY < 0 || (DY == 0 && DX < 0))
+            return cur[s + DY * stride + DX];
+        else
+            return start[s + DY * stride + DX];
+    }
+};
+
+// conf_kick at a cell at least two cells inside the grid, where no stencil
+// index is clamped: the same arithmetic in the same order, reading the nine
+// neighbours through SweepRead's fixed offsets.
+__device__ __forceinline__ bool conf_kick_inner(const FixedDiv& two, float dt, float vort, const SweepRead& uu,
+                                                const SweepRead& vv, float& du, float& dv) {
+    auto vort_of = [&](float vp, float vm, float up, float um) {
+        float dvdx = fdiv(vp - vm, two);
+        float dudz = fdiv(up - um, two);
+        return dvdx - dudz;
+    };
+    float w = vort_of(vv.at<1, 0>(), vv.at<-1, 0>(), uu.at<0, 1>(), uu.at<0, -1>());
+    if (!finite_f(w) || fabsf(w) < 1.0e-4f) return false;
+    float wxp = fabsf(vort_of(vv.at<2, 0>(), vv.at<0, 0>(), uu.at<1, 1>(), uu.at<1, -1>()));
+    float wxm = fabsf(vort_of(vv.at<0, 0>(), vv.at<-2, 0>(), uu.at<-1, 1>(), uu.at<-1, -1>()));
+    float wzp = fabsf(vort_of(vv.at<1, 1>(), vv.at<-1, 1>(), uu.at<0, 2>(), uu.at<0, 0>()));
+    float wzm = fabsf(vort_of(vv.at<1, -1>(), vv.at<-1, -1>(), uu.at<0, 0>(), uu.at<0, -2>()));
+    float nx = fdiv(wxp - wxm, two);
+    float nz = fdiv(wzp - wzm, two);
+    du = vort * dt * (-nz * w);
+    dv = vort * dt * (nx * w);
+    return finite_f(du) && finite_f(dv) && du * du + dv * dv <= 0.0625f;
+}
+
 }  // namespace silt

@@ -1715,12 +1715,15 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     }
     CK(silt::op_sum2(s->tr.susp[0], s->tr.turbid[0], s->n, s->d_acc + 4, s->st, s->d_sum_scratch));
     CK(cudaMemcpyAsync(s->h_acc + 4, s->d_acc + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
-    double spray = 0.0, park_w = 0.0, park_s = 0.0, cut = 0.0, reach = 0.0, eroded = 0.0, rounding = 0.0;
-    int rc = silt::fine::ledger_parts(s->fine, s, &spray, &park_w, &park_s, &cut, &reach, &eroded, &rounding);
+    // Every copy is queued first and the stream waited on once.
+    int rc = silt::fine::books_enqueue(s->fine, s);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if ((rc = check_substep_overflow(s))) return rc;
+    const double* bk = silt::fine::books_host(s->fine);
+    const double spray = bk[0], park_w = bk[1], park_s = bk[2], cut = bk[3], reach = bk[4], eroded = bk[5],
+                 rounding = bk[6];
     const double area = (double)s->cfg.cell * (double)s->cfg.cell;
     w = s->h_acc[0] * area;
     sl = s->h_acc[1] * area;
@@ -1734,7 +1737,6 @@ int silt_get_ledger(silt_sheet* s, silt_ledger* out) {
     out->cut_m3 = cut;
     out->reach_m3 = reach;
     out->round_m3 = rounding;
-    const double* bk = silt::fine::books_host(s->fine);
     // The tracers' books take the reference's f32 cell area (cell * cell in
     // f32), so the standing load and its running books use one area.
     const double tracer_area = (double)(s->cfg.cell * s->cfg.cell);

@@ -734,7 +734,11 @@ __device__ int cta_gravity_gs(Shared& S, const Job& J, const Box& b, const float
                 auto vv = [&](int a, int c) { return pick(J.v, V0, VG, a, c); };
                 float du, dv;
                 float nu_ = UG[g], nv_ = VG[g];
-                if (conf_kick(i, j, res, two, dt, J.vort, uu, vv, du, dv)) {
+                // Two cells inside the window no stencil index is clamped.
+                const bool inner = i >= 2 && j >= 2 && i + 2 < res && j + 2 < res;
+                if (inner ? conf_kick_inner(two, dt, J.vort, SweepRead{J.u, U0, UG, g, res},
+                                            SweepRead{J.v, V0, VG, g, res}, du, dv)
+                          : conf_kick(i, j, res, two, dt, J.vort, uu, vv, du, dv)) {
                     nu_ = UG[g] + du;
                     nv_ = VG[g] + dv;
                 }
