@@ -262,12 +262,15 @@ def run_b200(args):
     seed(sheet, scene)
     step_no = 0
 
+    def step_on(sh, n, want_spray):
+        for t in tires_for(n, args):
+            sh.push_tire(**t)
+        return sh.step(DT, want_spray=want_spray)
+
     def one_step(want_spray):
         nonlocal step_no
         step_no += 1
-        for t in tires_for(step_no, args):
-            sheet.push_tire(**t)
-        return sheet.step(DT, want_spray=want_spray)
+        return step_on(sheet, step_no, want_spray)
 
     for _ in range(max(3, args.warmup)):
         one_step(False)
@@ -330,6 +333,14 @@ def run_b200(args):
     # End to end through the public API, every timed step: the tire pushes go
     # in (inside silt_step, from its pinned step table), the spray events and
     # the FP64 ledger come back, and the ledger's closure is checked each step.
+    # A second sheet, seeded and warmed up the same way, takes the timed loop's
+    # own steps (the cost of a step changes as the water and silt spread).
+    sheet.close()
+    sheet = silt_b200.Sheet(res=args.res, cell=CELL, fine_res=FINE_RES, fine_cell=0.02,
+                            layout=silt_b200.FINE_PER_TIRE, device=local, stream=stream.cuda_stream)
+    seed(sheet, scene)
+    for n in range(1, max(3, args.warmup) + 1):
+        step_on(sheet, n, False)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -341,8 +352,8 @@ def run_b200(args):
     nev = 0
     gaps = []   # per step: |(total + cut - opened) now - before| / total, the FP64 books' closure
     rgaps = []  # the same with the transport rounding book taken off
-    for _ in range(e2e_steps):
-        ev = one_step(True)
+    for n in range(max(3, args.warmup) + 1, max(3, args.warmup) + 1 + e2e_steps):
+        ev = step_on(sheet, n, True)
         nev += len(ev)
         led = sheet.ledger()
         kept = led["total_m3"] + led["cut_m3"] - led["opened_m3"]

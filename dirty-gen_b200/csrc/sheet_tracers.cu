@@ -235,6 +235,20 @@ __device__ __forceinline__ void grown(const int* b, int res, int& i0, int& i1, i
         for (int once_ = 1, i = (i0) + (int)(q_ % w_), j = (j0) + (int)(q_ / w_); once_; once_ = 0)        \
             for (unsigned g = (unsigned)j * (unsigned)(res) + (unsigned)i; once_; once_ = 0)
 
+// The 128-cell segments of a row of a `res`-wide window (cells 128 s .. 128 s + 127).
+__host__ __device__ __forceinline__ int segments(int res) { return (res + 127) / 128; }
+
+// QUAD_ROWS over whole segments: every segment that meets the columns
+// [i0, i1], in the rows [j0, j1], one per warp iteration. Declares j, s and
+// ib = 128 s + lane; the cells outside [i0, i1] are the caller's to skip.
+#define QUAD_SEGS(res, i0, i1, j0, j1)                                                                          \
+    for (unsigned it_ = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, s0_ = (unsigned)max((i0), 0) >> 7,        \
+                  nx_ = (i1) >= (i0) ? ((unsigned)(i1) >> 7) - s0_ + 1u : 0u,                                 \
+                  n_ = nx_ * (unsigned)max((j1) - (j0) + 1, 0);                                               \
+         it_ < n_; it_ += (gridDim.x * blockDim.x) >> 5)                                                        \
+        for (int once_ = 1, j = (j0) + (int)(it_ / nx_), s = (int)(s0_ + it_ % nx_), ib = s * 128 + (int)(threadIdx.x & 31); \
+             once_; once_ = 0)
+
 // Four cells per thread for the passes over whole windows: a warp takes 128
 // consecutive cells of a row of the box, lane l the cells ib, ib + 32,
 // ib + 64, ib + 96 with ib = start + l (each load coalesced; a thread's four
@@ -270,6 +284,19 @@ __device__ __forceinline__ Box box_union(Box a, Box b) {
     if (a.empty()) return b;
     if (b.empty()) return a;
     return Box{min(a.i0, b.i0), max(a.i1, b.i1), min(a.j0, b.j0), max(a.j1, b.j1)};
+}
+
+// True when the warp's 128 cells of row j from column ib0 on hold no wet or
+// foam-live mark (the flags of the one or two segments they meet, as this
+// step's wet-set pass left them) and meet no cell of box b: a pass that acts
+// only on such marks and on the cells of b has nothing to do there. Flags of
+// segments the wet-set pass did not visit may be stale, but such segments
+// lie outside its box, where no cell carries a mark.
+__device__ __forceinline__ bool quiet_run(const uint8_t* occ, int res, int j, int ib0, const Box& b) {
+    const int ns = segments(res);
+    const int s0 = ib0 >> 7, s1 = min((ib0 + 127) >> 7, ns - 1);
+    if (occ[j * ns + s0] | occ[j * ns + s1]) return false;
+    return b.empty() || j < b.j0 || j > b.j1 || ib0 + 127 < b.i0 || ib0 > b.i1;
 }
 __device__ __forceinline__ bool in_box(const Box& b, int i, int j) {
     return i >= b.i0 && i <= b.i1 && j >= b.j0 && j <= b.j1;
@@ -502,7 +529,8 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
     const Box b = box_of(c->cbox);
     const Box u = box_union(b, box_of(c->mbox));
     bool any = false;
-    QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+    const int ns = segments(res);
+    QUAD_SEGS(res, u.i0, u.i1, u.j0, u.j1) {
         // The four cells' loads in two rounds: marks and depths, then, for the
         // wet cells only, the four neighbours' water of the shore test
         // (shore_wet_cell, :9752-9764: a cell on the window's border is never
@@ -514,7 +542,7 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
         for (int k = 0; k < 4; ++k) {
             const int i = ib + 32 * k;
             const unsigned g = (unsigned)j * (unsigned)res + (unsigned)i;
-            here[k] = i <= u.i1;
+            here[k] = i >= u.i0 && i <= u.i1;
             wet[k] = false;
             if (here[k]) mk[k] = mark[g];
             if (here[k] && in_box(b, i, j)) {
@@ -544,6 +572,7 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
                 vw4[k] = S.vw[g];
             }
         }
+        bool marked = false;  // a wet or foam-live mark among this thread's cells
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (!here[k]) continue;
@@ -559,6 +588,7 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
                 if (shore) m |= SHORE;
             }
             mark[g] = m;
+            marked = marked || m != 0;
             if (foam_on) {
                 if (m & WET) {
                     const float uu = uw4[k], vv = vw4[k];  // wet cells are far above the dry cut
@@ -575,6 +605,9 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
                 }
             }
         }
+        // The warp holds the whole segment (the cells outside the box carry no mark).
+        const unsigned seg = __ballot_sync(0xffffffffu, marked);
+        if ((threadIdx.x & 31) == 0) T.occ[j * ns + s] = seg != 0u ? 1 : 0;
     }
     block_flag(any, &st->wet_any);
 }
@@ -591,7 +624,14 @@ __global__ void k_turbid_advect(const Job* jobs) {
     const Box tb = grown_box(st->tspan, res);
     const float* silt = T.turbid[0];
     float* ttmp = T.turbid[1];
-    BOX_CELLS(res, tb.i0, tb.i1, tb.j0, tb.j1) ttmp[g] = turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, J.dt);
+    BOX_CELLS(res, tb.i0, tb.i1, tb.j0, tb.j1) {
+        // A cell without silt beside neighbours without silt (those inside the
+        // span) keeps its value: every edge of those columns gives 0.
+        const bool still = silt[g] == 0.0f && (i - 1 < tb.i0 || silt[g - 1] == 0.0f) &&
+                           (i + 1 > tb.i1 || silt[g + 1] == 0.0f) && (j - 1 < tb.j0 || silt[g - res] == 0.0f) &&
+                           (j + 1 > tb.j1 || silt[g + res] == 0.0f);
+        ttmp[g] = still ? silt[g] : turbid_after(S, silt, i, j, tb.i0, tb.i1, tb.j0, tb.j1, J.dt);
+    }
 }
 
 // The advections take effect: foam on every wet or foam-live cell, silt on
@@ -616,6 +656,7 @@ __global__ void k_commit(const Job* jobs) {
     const uint8_t* mark = T.mark;
     LocalBox lb;
     QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+        if (quiet_run(T.occ, res, j, ib - (int)(threadIdx.x & 31), tb)) continue;
         bool fo[4];
         float fv[4], tv[4];
 #pragma unroll
@@ -801,6 +842,7 @@ __global__ void __launch_bounds__(256, 3) k_spawn(const Job* jobs) {
     LocalBox lb;
     const Box cb = box_of(c->cbox);  // the wet cells lie inside
     QUAD_ROWS(res, cb.i0, cb.i1, cb.j0, cb.j1) {
+        if (quiet_run(J.T.occ, res, j, ib - (int)(threadIdx.x & 31), Box{0, -1, 0, -1})) continue;
         uint8_t mk[4];
         float hw[4], hs[4], u4[4], v4[4], f4[4], t4[4];
 #pragma unroll
@@ -860,6 +902,7 @@ __global__ void __launch_bounds__(256, 4) k_clear_sync(const Job* jobs) {
     unsigned int cnt = 0;
     LocalBox live, span;
     QUAD_ROWS(res, u.i0, u.i1, u.j0, u.j1) {
+        if (quiet_run(T.occ, res, j, ib - (int)(threadIdx.x & 31), sb)) continue;
         // Loads in two rounds: the marks, then what the wet cells and the
         // span's cells read.
         float hw[4], hs[4], f4[4], t4[4];
@@ -1349,7 +1392,7 @@ cudaError_t upload(Runner& R, const Window* w, int n, float dt, float foam_decay
 
 size_t plane_bytes(int res) {
     const size_t n = (size_t)res * res;
-    return 256 + 6 * n * sizeof(float) + 6 * n * sizeof(float) + n + 256;
+    return 256 + 6 * n * sizeof(float) + 6 * n * sizeof(float) + n + (size_t)res * segments(res) + 256;
 }
 
 cudaError_t attach(Planes& T, void* mem, int res, double* books, cudaStream_t st) {
@@ -1368,6 +1411,7 @@ cudaError_t attach(Planes& T, void* mem, int res, double* books, cudaStream_t st
     T.taken = T.susp[1];
     T.acc = f + 6 * n;
     T.mark = reinterpret_cast<uint8_t*>(f + 12 * n);
+    T.occ = T.mark + n;
     T.books = books;
     cudaError_t e = cudaMemsetAsync(mem, 0, plane_bytes(res), st);
     if (e != cudaSuccess) return e;

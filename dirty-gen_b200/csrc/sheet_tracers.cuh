@@ -33,6 +33,8 @@ struct Planes {
     float* taken;       // suspended solids a cell takes from its neighbours this step
     float* acc;         // 6 planes: each donor's accepted gives (advection x, z; mixing +x, -x, +z, -z)
     uint8_t* mark;      // bit 0 wet, bit 1 shore, bit 2 foam-live
+    uint8_t* occ;       // per row and 128-cell segment (cells 128 s .. 128 s + 127): 1 when the wet-set pass
+                        // left a wet or foam-live mark in it (res x ceil(res / 128))
     State* st;
     double* books;      // [0] entrained, [1] settled suspended, [2] stirred, [3] settled silt (m^3, FP64)
 };

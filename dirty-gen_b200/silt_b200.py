@@ -237,14 +237,16 @@ class Sheet:
         h = _p()
         check(L.silt_sheet_create(ctypes.byref(cfg), ctypes.byref(h)), "silt_sheet_create")
         self.h = h
+        self._destroy = L.silt_sheet_destroy  # kept: at interpreter exit the module's globals may be gone
         self.res = res
         self.fine_res = fine_res
         self.device = device
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().silt_sheet_destroy(self.h)
+        h = getattr(self, "h", None)
+        if h:
             self.h = None
+            self._destroy(h)
 
     __del__ = close
 
@@ -521,6 +523,7 @@ class Batch:
         h = _p()
         check(lib().silt_batch_create(arr, len(self.sheets), ctypes.byref(h)), "batch_create")
         self.h = h
+        self._destroy = lib().silt_batch_destroy
 
     def autotune(self, on=True):
         """Times the next steps under each candidate launch setting and keeps
@@ -539,9 +542,10 @@ class Batch:
         check(lib().silt_batch_set_tune(self.h, ctypes.byref(t)), "batch_set_tune")
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().silt_batch_destroy(self.h)
+        h = getattr(self, "h", None)
+        if h:
             self.h = None
+            self._destroy(h)
 
     __del__ = close
 
