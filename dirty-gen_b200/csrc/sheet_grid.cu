@@ -24,6 +24,9 @@
 // depths and velocities on every cell that holds fluid.
 #include <cstdint>
 #include <mutex>
+#include <vector>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "sheet_grid.cuh"
@@ -39,11 +42,16 @@ constexpr int FPLANE = FW * FW;
 constexpr int FORCE_THREADS = 512;
 
 constexpr int TT = 32;       // transport tile edge
-constexpr int TW = TT + 3;   // cells [t0-2, t1+1)
+constexpr int TW = TT + 3;   // rows [t0-2, t1+1)
+// A transport plane in shared memory: rows [ty0-2, ty0+33), each TS cells from
+// column tx0-4 (16 bytes below tx0-2, so that a 2D TMA box can start there),
+// padded to 128 bytes.
+constexpr int TS = TT + 8;
+constexpr int TPL = (TS * TW + 31) / 32 * 32;
 constexpr int TRANSPORT_THREADS = 256;
 
 size_t force_smem_bytes() { return sizeof(float) * FPLANE * 8; }
-size_t transport_smem_bytes() { return sizeof(float) * TW * TW * 8; }
+size_t transport_smem_bytes() { return sizeof(float) * TPL * 8; }
 
 // Five taps left to right. Away from the edge the reference starts from the
 // first product (accum5); near it from 0.0 (accum5_clamped,
@@ -851,6 +859,74 @@ cudaError_t launch_tile_list(const TileFlags& tf, int cur, int nxt, int all, int
     return cudaGetLastError();
 }
 
+// ------------------------------------------------- TMA staging of halo tiles
+
+constexpr int TMA_WAIT_LIMIT = 1 << 22;  // mbarrier polls before a CTA gives up on a copy
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Waits for the barrier phase with a bounded number of polls; false if it
+// never completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (int k = 0; k < TMA_WAIT_LIMIT && !done; ++k)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+    return done != 0;
+}
+
+// One 2D tile copy global -> this CTA's shared memory (no multicast), counted
+// on `bar`. x must be a multiple of 4 floats (16 bytes).
+__device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// The mbarrier of a CTA's tile copies and the parity of its next phase.
+struct TileStage {
+    uint64_t* bar;
+    uint32_t phase;
+    bool off;  // a copy did not arrive in time: this CTA loads its tiles itself
+};
+
+// h, u and v of a transport tile, rows [ty0-2, ty0+33) x columns
+// [tx0-4, tx0+36), into their shared planes: three TMA copies (h, u, v
+// tensor maps of the layer) completing one phase of the stage's barrier.
+// Columns past the grid's edge read 0 and are not used. False when the copies
+// did not arrive within the poll limit, twice: the error word gets bit 1 and
+// the caller loads the planes itself.
+__device__ bool tma_stage_transport(const CUtensorMap* maps, float* HSm, float* US, float* VS, int tx0, int ty0,
+                                    TileStage& ts, unsigned int* err) {
+    // Every thread's earlier writes of these planes come before the copies' writes.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(ts.bar)),
+                     "r"(3 * TS * TW * (int)sizeof(float))
+                     : "memory");
+        tma_load_2d(HSm, maps + 0, tx0 - 4, ty0 - 2, ts.bar);
+        tma_load_2d(US, maps + 1, tx0 - 4, ty0 - 2, ts.bar);
+        tma_load_2d(VS, maps + 2, tx0 - 4, ty0 - 2, ts.bar);
+    }
+    bool ok = __syncthreads_and(mbar_wait(ts.bar, ts.phase) ? 1 : 0) != 0;
+    if (!ok) ok = __syncthreads_and(mbar_wait(ts.bar, ts.phase) ? 1 : 0) != 0;
+    if (!ok) {
+        if (threadIdx.x == 0 && err) atomicOr(err, 2u);
+        ts.off = true;  // the phases are no longer known: no more copies
+        return false;
+    }
+    ts.phase ^= 1u;
+    return true;
+}
+
 // Cells [x0, x0 + W) x [y0, y0 + H) of a transport tile: edge tiles walk
 // clipped rows one warp per row; interior tiles (W, H exact) one flat range
 // of compile-time width, so every lane is busy on the 33-35 wide passes.
@@ -876,11 +952,12 @@ __device__ __forceinline__ void trows(int x0, int x1, int y0, int y1, F f) {
 // 0 for the others. EDGE = false: the tile is full and its cells
 // [t0-2, t1+1) lie inside the grid with t1 <= res-1, so no range is clipped.
 template <bool EDGE>
-__device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int ty0, const TileFlags& tf, int l,
-                               int nxt, int t) {
+__device__ __forceinline__ void transport_tile(const TransportParams& P, float* sm, int tx0, int ty0,
+                                               const TileFlags& tf, int l, int nxt, int t, const CUtensorMap* maps,
+                                               TileStage* ts) {
     const int res = P.res;
     const int tx1 = min(res, tx0 + TT), ty1 = min(res, ty0 + TT);
-    constexpr int PL = TW * TW;
+    constexpr int PL = TPL;
     float* HSm = sm;            // h on rows [ty0-2, ty1+1), cols [tx0-2, tx1+1)
     float* US = sm + PL;        // u on the same cells
     float* FL = sm + 2 * PL;    // left-going flux of edge e (cells e, e+1)
@@ -889,21 +966,26 @@ __device__ void transport_tile(const TransportParams& P, float* sm, int tx0, int
     float* VS = sm + 5 * PL;    // v
     float* UP = sm + 6 * PL;    // up-going flux of row pair (r, r+1)
     float* DN = sm + 7 * PL;    // down-going flux
-    const int ox = tx0 - 2, oy = ty0 - 2;
-#define TIDX(gx, gy) (((gy) - oy) * TW + ((gx) - ox))
+    const int ox = tx0 - 4, oy = ty0 - 2;
+#define TIDX(gx, gy) (((gy) - oy) * TS + ((gx) - ox))
     const int ry0 = max(0, ty0 - 2), ry1 = min(res, ty1 + 1);
     const int cx0 = max(0, tx0 - 2), cx1 = min(res, tx1 + 1);
     const FixedDiv& cell = P.div_cell;
     const float dt = P.dt;
     const bool with_bed = P.bank_bed != nullptr;
     const uint8_t* gate = P.gate;
-    trows<EDGE, TT + 3, TT + 3>(cx0, cx1, ry0, ry1, [&](int gx, int gy) {
-        size_t g = (size_t)gy * res + gx;
-        HSm[TIDX(gx, gy)] = P.h[g];
-        US[TIDX(gx, gy)] = P.u[g];
-        if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
-    });
-    __syncthreads();
+    // An interior tile of a layer with tensor maps arrives by TMA.
+    const bool staged = !EDGE && maps && ts && !ts->off &&
+                        tma_stage_transport(maps, HSm, US, VS, tx0, ty0, *ts, tf.sweep ? &tf.sweep->err : nullptr);
+    if (!staged) {
+        trows<EDGE, TT + 3, TT + 3>(cx0, cx1, ry0, ry1, [&](int gx, int gy) {
+            size_t g = (size_t)gy * res + gx;
+            HSm[TIDX(gx, gy)] = P.h[g];
+            US[TIDX(gx, gy)] = P.u[g];
+            if (gx >= tx0 && gx < tx1) VS[TIDX(gx, gy)] = P.v[g];
+        });
+        __syncthreads();
+    }
     // x pass. Edge e joins cells e and e+1 and exists for 0 <= e < res-1.
     // Left-going flux first (its donor e+1 has removed nothing yet).
     const int e0 = max(0, tx0 - 2), e1 = min(res - 2, tx1 - 1);  // inclusive edge range
@@ -1056,7 +1138,8 @@ __device__ void copy_tile(const TransportParams& P, int tx0, int ty0, const Tile
 
 // One list entry of the transport pass.
 __device__ __forceinline__ void transport_entry(const TransportParams& P, const TileFlags& tf, int nxt, int e,
-                                                float* sm) {
+                                                float* sm, const CUtensorMap* maps = nullptr,
+                                                TileStage* ts = nullptr) {
     const int l = e >> 30, zero_fill = (e & ENTRY_ZERO) != 0, copy = (e & ENTRY_COPY) != 0, t = e & ENTRY_TILE;
     const int res = P.res;
     const int tx0 = (t % tf.tiles_x) * TT, ty0 = (t / tf.tiles_x) * TT;
@@ -1076,27 +1159,36 @@ __device__ __forceinline__ void transport_entry(const TransportParams& P, const 
     }
     const bool interior = tx0 >= 2 && ty0 >= 2 && tx0 + TT + 1 <= res && ty0 + TT + 1 <= res;
     if (interior)
-        transport_tile<false>(P, sm, tx0, ty0, tf, l, nxt, t);
+        transport_tile<false>(P, sm, tx0, ty0, tf, l, nxt, t, maps, ts);
     else
-        transport_tile<true>(P, sm, tx0, ty0, tf, l, nxt, t);
+        transport_tile<true>(P, sm, tx0, ty0, tf, l, nxt, t, nullptr, nullptr);
 }
 
 // Persistent over the substep's tile list.
-__global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L) {
+__global__ void __launch_bounds__(TRANSPORT_THREADS) k_transport(TransportLaunch L,
+                                                                   const __grid_constant__ TransportMaps M) {
     ::silt::dep_wait();
-    extern __shared__ float sm[];
+    extern __shared__ __align__(128) float sm[];
     __shared__ TransportParams Ps[2];
+    __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x < 2) {
         const int l = threadIdx.x;
         TransportParams P = L.lay[l];
         if (L.sc.speed2) P.dt = L.sc.dt / (float)device_nsub(L.sc, l);
         Ps[l] = P;
     }
+    const bool tma = (M.on[0] || M.on[1]) && (smem_addr(sm) & 127u) == 0;
+    if (tma && threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
+    TileStage ts{&bar, 0u, !tma};
     const int n = *L.tf.count;
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
         const int e = L.tf.list[k];
-        transport_entry(Ps[e >> 30], L.tf, L.nxt, e, sm);
+        const int l = e >> 30;
+        transport_entry(Ps[l], L.tf, L.nxt, e, sm, M.on[l] ? M.map[l] : nullptr, &ts);
     }
 }
 
@@ -1444,12 +1536,72 @@ cudaError_t launch_force(const ForceLaunch& L, int res, int layers, cudaStream_t
     return cudaGetLastError();
 }
 
+namespace {
+
+// cuTensorMapEncodeTiled from the driver (through the runtime: no link to libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// The transport's tensor map of a res x res FP32 plane: boxes of TS x TW
+// cells, out-of-grid cells read as 0. Maps are kept per (plane, res): the
+// step alternates between a few fixed buffers.
+bool transport_map(const float* plane, int res, CUtensorMap* out) {
+    struct Entry {
+        const float* plane;
+        int res;
+        CUtensorMap map;
+    };
+    static std::mutex m;
+    static std::vector<Entry> cache;
+    std::lock_guard<std::mutex> lock(m);
+    for (const Entry& e : cache)
+        if (e.plane == plane && e.res == res) {
+            *out = e.map;
+            return true;
+        }
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (res % 4) != 0 || (reinterpret_cast<uintptr_t>(plane) % 16) != 0) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)res, (cuuint64_t)res};
+    const cuuint64_t strides[1] = {(cuuint64_t)res * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)TS, (cuuint32_t)TW};
+    const cuuint32_t elem[2] = {1, 1};
+    Entry e{plane, res, {}};
+    if (enc(&e.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(plane), dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    if (cache.size() >= 64) cache.erase(cache.begin());
+    cache.push_back(e);
+    *out = e.map;
+    return true;
+}
+
+}  // namespace
+
 cudaError_t launch_transport(const TransportLaunch& L, int res, int layers, cudaStream_t st) {
     static std::once_flag attr;
     std::call_once(attr, [] { cudaFuncSetAttribute(k_transport, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)transport_smem_bytes()); });
-    (void)res;
     (void)layers;
-    ::silt::launch_dep(k_transport, dim3(148 * 4), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, L);
+    // Interior tiles of a grid a multiple of 4 cells wide arrive by TMA.
+    TransportMaps M;
+    for (int l = 0; l < 2; ++l) {
+        const TransportParams& P = L.lay[l];
+        M.on[l] = P.res == res && P.h && P.u && P.v && transport_map(P.h, res, &M.map[l][0]) &&
+                  transport_map(P.u, res, &M.map[l][1]) && transport_map(P.v, res, &M.map[l][2]);
+    }
+    ::silt::launch_dep(k_transport, dim3(148 * 4), dim3(TRANSPORT_THREADS), transport_smem_bytes(), st, L, M);
     ::silt::count_launch();
     return cudaGetLastError();
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "sheet_div.cuh"
@@ -56,7 +57,8 @@ struct LayerParams {
 struct SweepState {
     unsigned int bar;         // CTAs arrived at the grid barrier in this launch
     unsigned int flag[3];     // pass p's verdict in flag[p % 3]: some tile changed
-    unsigned int err;         // a barrier wait ran past its limit (sticky)
+    unsigned int err;         // sticky: bit 0 a barrier wait ran past its limit, bit 1 a transport tile's
+                              // TMA copies did not arrive within theirs
     unsigned int passes_max;  // most passes one launch needed
     unsigned int fallbacks;   // launches that ran the sequential sweep after the pass limit
     unsigned int launches;    // sweep launches
@@ -130,6 +132,13 @@ struct TransportLaunch {
     TileFlags tf;
     SubstepCount sc;
     int32_t nxt;
+};
+
+// TMA descriptors of a transport launch's input planes: h, u, v of each
+// layer (valid where on[layer]; built by launch_transport).
+struct TransportMaps {
+    CUtensorMap map[2][3];
+    int32_t on[2];
 };
 
 constexpr int GRID_TILE = 32;

@@ -451,6 +451,12 @@ __global__ void k_gather_ledgers(const double* const* acc, const double* const* 
     o[7] = books[w][6];
     for (int k = 0; k < 6; ++k) o[8 + k] = books[w][7 + k];  // the tracers' books
 }
+__global__ void k_gather_words(const unsigned int* const* src, int n, int words, unsigned int* out) {
+    ::silt::dep_wait();
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * words) return;
+    out[q] = src[q / words][q % words];
+}
 // Every window's suspended and silt column sums (FP64 of the clamped cells)
 // into out[16 w + 14], [16 w + 15], in a fixed order (ordered_finish per
 // window; part holds gridDim.x pairs per window, then the windows' tickets).
@@ -486,6 +492,12 @@ cudaError_t op_gather_ledgers(const double* const* acc, const double* const* boo
                               cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     ::silt::launch_dep(k_gather_ledgers, dim3((n + 127) / 128), dim3(128), 0, st, acc, books, n, out);
+    ::silt::count_launch();
+    return cudaGetLastError();
+}
+cudaError_t op_gather_words(const unsigned int* const* src, int n, int words, unsigned int* out, cudaStream_t st) {
+    if (n <= 0 || words <= 0) return cudaSuccess;
+    ::silt::launch_dep(k_gather_words, dim3((n * words + 255) / 256), dim3(256), 0, st, src, n, words, out);
     ::silt::count_launch();
     return cudaGetLastError();
 }

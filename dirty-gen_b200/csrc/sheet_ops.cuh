@@ -44,6 +44,8 @@ cudaError_t op_sum_tracers(const float* const* susp, const float* const* turbid,
 // out[16 w + 7] = books[w][6] (the transport rounding book), out[16 w + 8..13] = books[w][7..12] (tracers).
 cudaError_t op_gather_ledgers(const double* const* acc, const double* const* books, int n, double* out,
                               cudaStream_t st);
+// out[words w + k] = src[w][k] for k < words: each window's flag words in one block.
+cudaError_t op_gather_words(const unsigned int* const* src, int n, int words, unsigned int* out, cudaStream_t st);
 cudaError_t op_non_finite(const float* const* planes, int np, size_t n, unsigned int* out, cudaStream_t st);
 
 // Open-water drivers of the coarse water sheet (src/fluid_core.rs:7482-7636).

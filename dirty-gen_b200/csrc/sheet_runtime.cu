@@ -818,8 +818,10 @@ int silt_sheet_destroy(silt_sheet* s) {
 // whose layer needed more substeps than the host's speed bound launched (the
 // state is off the reference's path).
 static int check_substep_overflow(silt_sheet* s) {
-    if (s->h_flags[silt_sheet::SWEEP_AT + 4 - 2]) {
-        snprintf(g_err, sizeof g_err, "%s", "a Gauss-Seidel sweep launch gave up waiting at its grid barrier");
+    if (const unsigned int err = s->h_flags[silt_sheet::SWEEP_AT + 4 - 2]) {
+        snprintf(g_err, sizeof g_err, "%s",
+                 (err & 1u) ? "a Gauss-Seidel sweep launch gave up waiting at its grid barrier"
+                            : "a transport tile's TMA copies did not arrive in time");
         return SILT_ETIMEOUT;
     }
     if (!s->h_flags[0]) return SILT_OK;
@@ -2140,6 +2142,10 @@ struct silt_batch {
     int* d_tr_cells = nullptr;              // cells per window
     double* d_tr_sum = nullptr;             // the ordered tracer sums' scratch
     double* h_ledgers = nullptr;            // pinned
+    // Every window's 14 flag words (d_u32[2, 16)) in one block, one copy back.
+    const unsigned int** d_flag_src = nullptr;
+    unsigned int* d_flags = nullptr;
+    unsigned int* h_flags = nullptr;        // pinned
 };
 
 namespace {
@@ -2168,6 +2174,9 @@ int batch_free(silt_batch* b) {
     cudaFree(b->d_tr_sum);
     b->tr_run.release();
     if (b->h_ledgers) cudaFreeHost(b->h_ledgers);
+    cudaFree(b->d_flag_src);
+    cudaFree(b->d_flags);
+    if (b->h_flags) cudaFreeHost(b->h_flags);
     for (int k = 0; k < silt_batch::WS_SLOTS; ++k) {
         cudaFree(b->d_ws[k]);
         if (b->h_ws[k]) cudaFreeHost(b->h_ws[k]);
@@ -2461,6 +2470,14 @@ int silt_batch_create(silt_sheet* const* sheets, int32_t n, silt_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledger_src, 2 * (size_t)n * sizeof(double*));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ledgers, 16 * (size_t)n * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_ledgers, 16 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_flag_src, (size_t)n * sizeof(unsigned int*));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_flags, 14 * (size_t)n * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_flags, 14 * (size_t)n * sizeof(unsigned int));
+    if (e == cudaSuccess) {
+        std::vector<const unsigned int*> src(n);
+        for (int w = 0; w < n; ++w) src[w] = b->sheets[w]->d_u32 + 2;
+        e = cudaMemcpy(b->d_flag_src, src.data(), src.size() * sizeof(unsigned int*), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_src, 2 * (size_t)n * sizeof(float*));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_cells, (size_t)n * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tr_sum, silt::sum_tracers_scratch_bytes(n));
@@ -2676,11 +2693,12 @@ int silt_batch_get_ledgers(silt_batch* b, silt_ledger* out) {
     CK(silt::op_sum_tracers(b->d_tr_src, b->d_tr_src + n, b->d_tr_cells, n, b->d_ledgers, b->d_tr_sum, b->st));
     CK(silt::op_gather_ledgers(b->d_ledger_src, b->d_ledger_src + n, n, b->d_ledgers, b->st));
     CK(cudaMemcpyAsync(b->h_ledgers, b->d_ledgers, 16 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, b->st));
-    for (silt_sheet* s : b->sheets)
-        CK(cudaMemcpyAsync(s->h_flags, s->d_u32 + 2, 14 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
+    CK(silt::op_gather_words(b->d_flag_src, n, 14, b->d_flags, b->st));
+    CK(cudaMemcpyAsync(b->h_flags, b->d_flags, 14 * (size_t)n * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     for (int w = 0; w < n; ++w) {
         silt_sheet* s = b->sheets[w];
+        memcpy(s->h_flags, b->h_flags + 14 * (size_t)w, 14 * sizeof(unsigned int));
         int rc = check_substep_overflow(s);
         if (rc) return rc;
         const double* g = b->h_ledgers + 16 * (size_t)w;
