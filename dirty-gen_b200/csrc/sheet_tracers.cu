@@ -551,6 +551,24 @@ __global__ void __launch_bounds__(256, 3) k_collect(const Job* jobs) {
                 wet[k] = true;
             }
         }
+        // A segment with no wet cell and no foam-live mark: its cells' marks
+        // become 0 and nothing else happens there.
+        bool busy = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (here[k] && (mk[k] & LIVE)) busy = true;
+            if (wet[k]) {
+                const float h = hw[k] + hs[k];
+                if (finite_f(h) && !(h < 0.004f)) busy = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (here[k] && mk[k] != 0) mark[(unsigned)j * (unsigned)res + (unsigned)(ib + 32 * k)] = 0;
+            if ((threadIdx.x & 31) == 0) T.occ[j * ns + s] = 0;
+            continue;
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int i = ib + 32 * k;
