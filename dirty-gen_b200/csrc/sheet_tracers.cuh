@@ -81,7 +81,9 @@ struct Runner {
     size_t cap_jobs[SLOTS] = {}, cap_push[SLOTS] = {};
     cudaEvent_t ev[SLOTS] = {};
     int next = 0;
-    int blocks_total = 2368;  // blocks of a pass over all the windows of a launch (any value gives the same bits)
+    // Blocks of a pass over all the windows of a launch: 8 per SM (measured
+    // on config 2 against 16 and 32; any value gives the same planes).
+    int blocks_total = 1184;
     void release();
 };
 
