@@ -428,13 +428,27 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0, bo
     __syncthreads();
     bool tile_changed = false;
     passes = 0;
+    // Interior tiles recompute, after the first local pass, only the cells
+    // one of whose earlier-cell reads changed since they were last computed:
+    // a cell whose inputs did not change keeps its value. A change at c
+    // marks the cells that read c's iterate: c + (1,0), (2,0), (0,1),
+    // (-1,1), (1,1), (0,2). Marks for pass it + 1 go to one byte plane while
+    // pass it reads the other (plane 7 of the force layout, unused here).
+    uint8_t* const marks = reinterpret_cast<uint8_t*>(sm + 7 * FPLANE);
     for (int it = 0; it < SWEEP_LOCAL_PASSES; ++it) {
         ++passes;
         int changed = 0;
+        const uint8_t* dirty = marks + (it & 1) * FPLANE;
+        uint8_t* dirty_next = marks + ((it + 1) & 1) * FPLANE;
+        if (!EDGE) {
+            region<false, 0, 0>(tx0, ty0, res, [&](int, int, int s, size_t) { dirty_next[s] = 0; });
+            __syncthreads();
+        }
         region<EDGE, 0, 0>(tx0, ty0, res, [&](int gx, int gy, int s, size_t g) {
             if (WT[s] == 0.0f) return;
             if (!EDGE) {
                 // Interior tile: no stencil index is clamped.
+                if (it > 0 && !dirty[s]) return;
                 float du, dv, nu_ = GU[s], nv_ = GV[s];
                 if (conf_kick_inner(P.div_two, P.dt, P.vort, SweepRead{FU, PU, GU, s, FW},
                                     SweepRead{FV, PV, GV, s, FW}, du, dv)) {
@@ -445,6 +459,12 @@ __device__ bool sweep_tile(const LayerParams& P, float* sm, int tx0, int ty0, bo
                     FU[s] = nu_;
                     FV[s] = nv_;
                     changed = 1;
+                    dirty_next[s + 1] = 1;
+                    dirty_next[s + 2] = 1;
+                    dirty_next[s + FW - 1] = 1;
+                    dirty_next[s + FW] = 1;
+                    dirty_next[s + FW + 1] = 1;
+                    dirty_next[s + 2 * FW] = 1;
                 }
                 return;
             }
