@@ -48,6 +48,9 @@ constexpr int TW = TT + 3;   // rows [t0-2, t1+1)
 // padded to 128 bytes.
 constexpr int TS = TT + 8;
 constexpr int TPL = (TS * TW + 31) / 32 * 32;
+static_assert((TS * sizeof(float)) % 16 == 0, "a TMA box row is a multiple of 16 bytes");
+static_assert((TPL * sizeof(float)) % 128 == 0, "each transport plane starts 128-byte aligned");
+static_assert(TS * TW * sizeof(float) <= TPL * sizeof(float), "a TMA box fits its plane");
 constexpr int TRANSPORT_THREADS = 256;
 
 size_t force_smem_bytes() { return sizeof(float) * FPLANE * 8; }
