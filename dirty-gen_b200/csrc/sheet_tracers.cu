@@ -443,6 +443,7 @@ __device__ __forceinline__ void donor_flux(const Sheet& S, const float* T, int i
     const float column = finite_f(T[d]) ? T[d] : 0.0f;
     float removed = 0.0f;
     out[0] = out[1] = out[2] = out[3] = 0.0f;
+    if (column <= 1.0e-8f) return;  // every edge finds no room: nothing to read
     auto edge = [&](float v, bool donor_is_me) -> float {
         if (!finite_f(v) || fabsf(v) < 1.0e-5f || !donor_is_me) return 0.0f;
         const float room = column - removed;
