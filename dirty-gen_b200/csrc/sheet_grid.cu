@@ -904,7 +904,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 
-// One 2D tile copy global -> this CTA's shared memory (no multicast), counted
+// One 2D tile copy global -> this CTA's own shared memory only, counted
 // on `bar`. x must be a multiple of 4 floats (16 bytes).
 __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
     asm volatile(
